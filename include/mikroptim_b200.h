@@ -1,0 +1,166 @@
+/*
+ * mikroptim_b200.h -- C ABI of the B200 (sm_100a) batched trace-and-optimise path.
+ *
+ * Plain C: pointers, sizes and status codes, no C++ or torch types. Every entry point
+ * returns MKB_OK (0) or a negative mkb_status; mkb_last_error() gives a one-line reason
+ * for the calling thread's last failure. Arguments are checked on the host before any
+ * device work is queued, as the reference does (it throws std::invalid_argument before a
+ * launch; here that is MKB_ERR_ARGUMENT).
+ *
+ * Device entry points (suffix _device) take device pointers and a CUDA stream passed as
+ * `void*` (a cudaStream_t; NULL is the legacy default stream) and only enqueue work: the
+ * results are valid once the stream has been synchronised. They allocate nothing; the
+ * scratch memory a kernel needs is passed in as `workspace` of at least the size the
+ * matching *_workspace_bytes function reports.
+ *
+ * Layout terms follow the reference (names in parentheses):
+ *   V variants, S table surfaces incl. the stop (surface 0), L wavelengths, F fields,
+ *   G ghost plates, K ghost terms, P variables, R rows per variant.
+ *   Per-variant arrays are variant-major: curvature[v*S+s], index[(v*S+s)*L+l], ...
+ *   (include/mikroptim/batch/system_batch_view.hpp:29-95).
+ *   Residual rows per variant: tuples (f, l) f-major then l, inside a tuple the pupil
+ *   sample k = i*M + j; in soft-failure mode the penalty rows follow the ray rows
+ *   (include/mikroptim/batch/batch_residuals.hpp:47-62).
+ */
+#ifndef MIKROPTIM_B200_H
+#define MIKROPTIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- limits of this build ------------------------------------------------------------ */
+#define MKB_MAX_SURFACES 64     /* kMaxSurfaces, include/mikroptim/trace/surface_table.hpp:15 */
+#define MKB_MAX_RINGS 32        /* the reference caps at 16 (pupil/quadrature.hpp:21) */
+#define MKB_MAX_SPOKES 64
+#define MKB_MAX_FIELDS 16
+#define MKB_MAX_WAVELENGTHS 16
+#define MKB_MAX_TUPLES 128      /* F * L */
+#define MKB_MAX_VARIABLES 64    /* P */
+
+/* ---- status codes --------------------------------------------------------------------- */
+typedef enum mkb_status {
+    MKB_OK = 0,
+    MKB_ERR_ARGUMENT = -1,    /* bad argument; nothing was enqueued */
+    MKB_ERR_CUDA = -2,        /* CUDA runtime error (launch or sticky device error) */
+    MKB_ERR_WORKSPACE = -3,   /* workspace missing or too small */
+    MKB_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
+    MKB_ERR_UNSUPPORTED = -5  /* a feature of the input that this build does not trace */
+} mkb_status;
+
+/* Values are stable and equal to the reference enums. */
+enum { MKB_SURFACE_STOP = 0, MKB_SURFACE_PLANE = 1, MKB_SURFACE_SPHERE = 2,
+       MKB_SURFACE_GHOST_PLATE = 3 };                  /* SurfaceKind, surface_table.hpp:25 */
+enum { MKB_PUPIL_HALF = 0, MKB_PUPIL_FULL = 1, MKB_PUPIL_AXIS = 2 };
+                                                       /* PupilMode, pupil/quadrature.hpp:24 */
+enum { MKB_FAILURE_SOFT = 0, MKB_FAILURE_HARD = 1 };   /* FailureMode, surface_ops.hpp:74 */
+enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_BACKWARD = 3,
+       MKB_STATUS_UNSUPPORTED = 4, MKB_STATUS_SOFT_MISSED = 5, MKB_STATUS_SOFT_TIR = 6 };
+                                                       /* TraceStatus, surface_ops.hpp:24 */
+enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1 };
+enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2 };
+                                                       /* VariableType, model/variables.hpp:18 */
+
+/* ---- batch ------------------------------------------------------------------------------
+ * Mirrors SystemBatchView<double> (include/mikroptim/batch/system_batch_view.hpp:108) for a
+ * collimated source with the reference sphere through the vertex of the last surface
+ * (ReferenceSphereKind::LastSurface) and the ideal image point h_f = field_target. All
+ * pointers are host pointers when passed to mkb_pack_batch_host. */
+typedef struct mkb_batch_view {
+    int32_t variants, surfaces, wavelengths, fields, ghost_plates, ghost_terms;
+    double reference_wavelength_nm;
+    const uint8_t* type;              /* [S]  surface kind                              */
+    const double* wavelength_weight;  /* [L]                                            */
+    const double* field_weight;       /* [F]                                            */
+    const double* curvature;          /* [V][S]                                         */
+    const double* thickness;          /* [V][S]  thickness[S-1] = working distance      */
+    const double* index;              /* [V][S][L] medium after surface s               */
+    const double* pupil_radius;       /* [V]                                            */
+    const double* field_angle;        /* [V][F] radians                                 */
+    const double* field_target;       /* [V][F] ideal image height h_f (mm)             */
+} mkb_batch_view;
+
+/* The device-resident batch: one 16-byte aligned record of `record_stride` doubles per
+ * variant (so that a CTA stages its variant with one bulk copy), plus the shared arrays.
+ * Record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
+ * sin(field_angle)[F] | cos(field_angle)[F] | field_target[F] | padding. */
+typedef struct mkb_device_batch {
+    int32_t variants, surfaces, wavelengths, fields;
+    int32_t record_stride;            /* doubles per variant, even                      */
+    int32_t reserved;
+    const double* records;            /* device [V][record_stride], 16-byte aligned     */
+    const uint8_t* type;              /* host [S] (copied into the kernel parameters)   */
+} mkb_device_batch;
+
+/* Doubles per packed variant record for a batch shape (>= 2, even). */
+int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields);
+
+/* Packs a host SoA view into host records [V][record_stride] (sin/cos of the field angles
+ * are taken here with the host libm, so the start rays are those of the CPU reference). */
+int mkb_pack_batch_host(const mkb_batch_view* view, double* records);
+
+/* Writes the curvature/thickness/working-distance entries of `x` ([runs][P]) into the
+ * packed device records of the matching variants (variant v = first_variant + run) --
+ * VariableSet::apply (src/optim/variable_set.cpp:237) for these variable types. */
+typedef struct mkb_variables {
+    int32_t count;                    /* P                                               */
+    const int32_t* type;              /* host [P] MKB_VAR_*                              */
+    const int32_t* surface;           /* host [P] table surface (batch_surface)          */
+    const double* lower;              /* host [P] (-inf allowed)                         */
+    const double* upper;              /* host [P] (+inf allowed)                         */
+    const double* typical;            /* host [P] > 0                                    */
+} mkb_variables;
+
+/* ---- residual plan -----------------------------------------------------------------------
+ * ResidualSettings + ResidualLayout (include/mikroptim/batch/batch_residuals.hpp:24,62)
+ * plus the shared weights of the batch. quad_u / quad_w are the Gauss-Legendre radial nodes
+ * u_i = rho_i^2 (ascending) and weights W_i (sum 1) for `rings` (pupil/quadrature.hpp:40). */
+typedef struct mkb_residual_plan {
+    int32_t rings, spokes;
+    int32_t failure;                  /* MKB_FAILURE_*                                   */
+    int32_t precision;                /* MKB_PRECISION_*                                 */
+    double fail_weight;               /* w_fail (ray_residual.hpp:175), >= 0             */
+    double reference_wavelength_nm;   /* lambda_ref (residuals in waves at lambda_ref)   */
+    int32_t fields, wavelengths;
+    const uint8_t* pupil_mode;        /* host [F]                                        */
+    const double* field_weight;       /* host [F]                                        */
+    const double* wavelength_weight;  /* host [L]                                        */
+    const double* quad_u;             /* host [rings]                                    */
+    const double* quad_w;             /* host [rings]                                    */
+} mkb_residual_plan;
+
+/* Rays per variant (ResidualLayout::rays_per_variant) and trace rows (rays + penalty rows). */
+int64_t mkb_rays_per_variant(const mkb_residual_plan* plan);
+int64_t mkb_trace_rows(const mkb_residual_plan* plan);
+
+/* ---- forward trace -------------------------------------------------------------------------
+ * RESIDUALS: replaces DeviceResiduals::run (src/cuda/residuals.cu:240) behind
+ * TraceEngine::run(batch, TraceMode::Residuals, ...) (include/mikroptim/cuda/trace_engine.hpp).
+ * residuals [V][stride] (stride >= trace_rows; rows past trace_rows are left untouched),
+ * opd [V][rays] (may be NULL), status [V][rays] (may be NULL). */
+int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                         double* residuals, int64_t stride, double* opd, uint8_t* status,
+                         void* stream);
+
+/* MERIT: replaces DeviceMerit::run (src/cuda/merit.cu:339): merit[v] = sum_(f,l) (sum_k r_k^2
+ * + sum_k p_k^2), failed[v] / hard_failed[v] ray counts (batch_merit.hpp:32). Scratch: the
+ * per-tuple partial sums, mkb_merit_workspace_bytes(V, plan) bytes. */
+size_t mkb_merit_workspace_bytes(int32_t variants, const mkb_residual_plan* plan);
+int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                     double* merit, int64_t* failed, int64_t* hard_failed,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- diagnostics ----------------------------------------------------------------------- */
+const char* mkb_last_error(void);
+const char* mkb_version(void);
+/* Number of kernel launches this library has enqueued in the calling process. */
+int64_t mkb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MIKROPTIM_B200_H */

@@ -1,0 +1,150 @@
+"""ctypes binding of the C ABI declared in include/mikroptim_b200.h.
+
+The library ``libmikroptim_b200.so`` is built in-tree (``python -m mikroptim_b200.build``)
+and loaded from this package directory. There is no fallback: if the library is missing,
+``lib()`` raises, so nothing silently runs on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmikroptim_b200.so")
+
+MKB_OK = 0
+MKB_ERR_ARGUMENT = -1
+MKB_ERR_CUDA = -2
+MKB_ERR_WORKSPACE = -3
+MKB_ERR_TIMEOUT = -4
+MKB_ERR_UNSUPPORTED = -5
+
+P_double = C.POINTER(C.c_double)
+P_int64 = C.POINTER(C.c_int64)
+P_int32 = C.POINTER(C.c_int32)
+P_uint8 = C.POINTER(C.c_uint8)
+
+
+class BatchView(C.Structure):
+    """mkb_batch_view (SystemBatchView<double>, system_batch_view.hpp:108)."""
+
+    _fields_ = [
+        ("variants", C.c_int32), ("surfaces", C.c_int32), ("wavelengths", C.c_int32),
+        ("fields", C.c_int32), ("ghost_plates", C.c_int32), ("ghost_terms", C.c_int32),
+        ("reference_wavelength_nm", C.c_double),
+        ("type", P_uint8),
+        ("wavelength_weight", P_double),
+        ("field_weight", P_double),
+        ("curvature", P_double),
+        ("thickness", P_double),
+        ("index", P_double),
+        ("pupil_radius", P_double),
+        ("field_angle", P_double),
+        ("field_target", P_double),
+    ]
+
+
+class DeviceBatch(C.Structure):
+    """mkb_device_batch: packed per-variant records in device memory."""
+
+    _fields_ = [
+        ("variants", C.c_int32), ("surfaces", C.c_int32), ("wavelengths", C.c_int32),
+        ("fields", C.c_int32), ("record_stride", C.c_int32), ("reserved", C.c_int32),
+        ("records", C.c_void_p),
+        ("type", P_uint8),
+    ]
+
+
+class ResidualPlan(C.Structure):
+    """mkb_residual_plan (ResidualSettings + ResidualLayout, batch_residuals.hpp:24,62)."""
+
+    _fields_ = [
+        ("rings", C.c_int32), ("spokes", C.c_int32),
+        ("failure", C.c_int32), ("precision", C.c_int32),
+        ("fail_weight", C.c_double),
+        ("reference_wavelength_nm", C.c_double),
+        ("fields", C.c_int32), ("wavelengths", C.c_int32),
+        ("pupil_mode", P_uint8),
+        ("field_weight", P_double),
+        ("wavelength_weight", P_double),
+        ("quad_u", P_double),
+        ("quad_w", P_double),
+    ]
+
+
+class Variables(C.Structure):
+    """mkb_variables (VariableSet for curvature / thickness / working distance)."""
+
+    _fields_ = [
+        ("count", C.c_int32),
+        ("type", P_int32),
+        ("surface", P_int32),
+        ("lower", P_double),
+        ("upper", P_double),
+        ("typical", P_double),
+    ]
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(lib: C.CDLL) -> None:
+    c = C
+    lib.mkb_last_error.restype = c.c_char_p
+    lib.mkb_version.restype = c.c_char_p
+    lib.mkb_launch_count.restype = c.c_int64
+    lib.mkb_record_stride.restype = c.c_int32
+    lib.mkb_record_stride.argtypes = [c.c_int32, c.c_int32, c.c_int32]
+    lib.mkb_pack_batch_host.restype = c.c_int
+    lib.mkb_pack_batch_host.argtypes = [C.POINTER(BatchView), P_double]
+    lib.mkb_rays_per_variant.restype = c.c_int64
+    lib.mkb_rays_per_variant.argtypes = [C.POINTER(ResidualPlan)]
+    lib.mkb_trace_rows.restype = c.c_int64
+    lib.mkb_trace_rows.argtypes = [C.POINTER(ResidualPlan)]
+    lib.mkb_residuals_device.restype = c.c_int
+    lib.mkb_residuals_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                         c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p,
+                                         c.c_void_p]
+    lib.mkb_merit_workspace_bytes.restype = c.c_size_t
+    lib.mkb_merit_workspace_bytes.argtypes = [c.c_int32, C.POINTER(ResidualPlan)]
+    lib.mkb_merit_device.restype = c.c_int
+    lib.mkb_merit_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                     c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+                                     c.c_size_t, c.c_void_p]
+
+
+def lib() -> C.CDLL:
+    """The loaded CUDA library; raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"mikroptim_b200: CUDA library not built ({LIB_PATH}); run "
+                    "`python -m mikroptim_b200.build` (there is no CPU fallback)")
+            handle = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
+            _declare(handle)
+            _lib = handle
+        return _lib
+
+
+def check(status: int, what: str) -> None:
+    """Raise the reference-style exception for a non-zero mkb_status."""
+    if status == MKB_OK:
+        return
+    msg = lib().mkb_last_error().decode(errors="replace")
+    if status == MKB_ERR_ARGUMENT:
+        raise ValueError(f"{what}: {msg}")
+    if status == MKB_ERR_UNSUPPORTED:
+        raise NotImplementedError(f"{what}: {msg}")
+    raise RuntimeError(f"{what} (status {status}): {msg}")
+
+
+def ptr(array, ctype=C.c_double):
+    """ctypes pointer to a contiguous numpy array (None for None)."""
+    if array is None:
+        return None
+    return array.ctypes.data_as(C.POINTER(ctype))

@@ -1,0 +1,365 @@
+"""Host-side batch model mirroring the reference's SystemBatch API.
+
+Names and meaning follow the reference:
+  BatchTopology      include/mikroptim/batch/system_batch.hpp:229
+  SystemBatchHost    include/mikroptim/batch/system_batch.hpp:268 (FP64 SoA, variant-major)
+  ResidualSettings   include/mikroptim/batch/batch_residuals.hpp:24
+  ResidualLayout     include/mikroptim/batch/batch_residuals.hpp:62 (src/batch/batch_residuals.cpp:25)
+  VariableSet        include/mikroptim/optim/variable_set.hpp:63 (curvature, thickness and
+                     working-distance variables; Variable.batch_surface is the table surface)
+
+Errors are raised before any device work: ValueError where the reference throws
+std::invalid_argument, IndexError for std::out_of_range.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from . import _capi
+from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_legendre_unit,
+                         sample_count)
+
+SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
+FAILURE_SOFT, FAILURE_HARD = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE = 0, 1, 2
+
+MAX_SURFACES = 64
+MAX_FIELDS = 16
+MAX_WAVELENGTHS = 16
+MAX_TUPLES = 128
+MAX_VARIABLES = 64
+
+# TraceStatus values (include/mikroptim/trace/surface_ops.hpp:24)
+STATUS_OK, STATUS_MISSED, STATUS_TIR, STATUS_BACKWARD = 0, 1, 2, 3
+STATUS_UNSUPPORTED, STATUS_SOFT_MISSED, STATUS_SOFT_TIR = 4, 5, 6
+DEFAULT_FAIL_WEIGHT = 1e6  # kDefaultFailWeight, merit/ray_residual.hpp:175
+
+
+def in_piston(status: np.ndarray) -> np.ndarray:
+    """Ok or soft failure (surface_ops.hpp:66)."""
+    return (status == STATUS_OK) | (status == STATUS_SOFT_MISSED) | (status == STATUS_SOFT_TIR)
+
+
+@dataclass
+class BatchTopology:
+    """Everything all variants of one launch share (ADR-0004 of the reference)."""
+
+    surfaces: int
+    wavelengths: int
+    fields: int
+    type: list[int]
+    pupil_mode: list[int]
+
+    def validate(self) -> None:
+        if not 2 <= self.surfaces <= MAX_SURFACES:
+            raise ValueError(f"BatchTopology: surfaces must be in [2, {MAX_SURFACES}]")
+        if not 1 <= self.wavelengths <= MAX_WAVELENGTHS:
+            raise ValueError(f"BatchTopology: wavelengths must be in [1, {MAX_WAVELENGTHS}]")
+        if not 1 <= self.fields <= MAX_FIELDS:
+            raise ValueError(f"BatchTopology: fields must be in [1, {MAX_FIELDS}]")
+        if self.fields * self.wavelengths > MAX_TUPLES:
+            raise ValueError(f"BatchTopology: fields * wavelengths must be <= {MAX_TUPLES}")
+        if len(self.type) != self.surfaces:
+            raise ValueError("BatchTopology: type needs one entry per surface")
+        if self.type[0] != SURFACE_STOP:
+            raise ValueError("BatchTopology: surface 0 must be the stop")
+        for s, t in enumerate(self.type[1:], start=1):
+            if t not in (SURFACE_PLANE, SURFACE_SPHERE):
+                raise NotImplementedError(
+                    f"BatchTopology: surface {s} has kind {t}; this build traces stop, plane "
+                    "and sphere surfaces")
+        if len(self.pupil_mode) != self.fields:
+            raise ValueError("BatchTopology: pupil_mode needs one entry per field")
+        for m in self.pupil_mode:
+            if m not in (PUPIL_HALF, PUPIL_FULL, PUPIL_AXIS):
+                raise ValueError("BatchTopology: unknown pupil mode")
+
+
+class SystemBatchHost:
+    """V variants of one topology as FP64 structure of arrays (variant outermost)."""
+
+    def __init__(self, topology: BatchTopology, variants: int):
+        topology.validate()
+        if variants < 0:
+            raise ValueError("SystemBatchHost: variants must be >= 0")
+        self.topology = topology
+        S, L, F = topology.surfaces, topology.wavelengths, topology.fields
+        self.reference_wavelength_nm = 0.0
+        self.type = np.asarray(topology.type, dtype=np.uint8)
+        self.wavelength_nm = np.zeros(L)
+        self.wavelength_weight = np.zeros(L)
+        self.field_weight = np.zeros(F)
+        self.curvature = np.zeros((variants, S))
+        self.thickness = np.zeros((variants, S))
+        self.index = np.zeros((variants, S, L))
+        self.pupil_radius = np.zeros(variants)
+        self.field_angle = np.zeros((variants, F))
+        self.field_target = np.zeros((variants, F))
+
+    # ---- shape --------------------------------------------------------------------------
+    @property
+    def variants(self) -> int:
+        return self.curvature.shape[0]
+
+    @property
+    def surfaces(self) -> int:
+        return self.topology.surfaces
+
+    @property
+    def wavelengths(self) -> int:
+        return self.topology.wavelengths
+
+    @property
+    def fields(self) -> int:
+        return self.topology.fields
+
+    def subset(self, first: int, count: int) -> "SystemBatchHost":
+        """Variants [first, first + count) as a new batch (assign_variants)."""
+        if first < 0 or count < 0 or first + count > self.variants:
+            raise IndexError("SystemBatchHost.subset: range out of bounds")
+        out = SystemBatchHost(self.topology, 0)
+        out.reference_wavelength_nm = self.reference_wavelength_nm
+        out.wavelength_nm = self.wavelength_nm.copy()
+        out.wavelength_weight = self.wavelength_weight.copy()
+        out.field_weight = self.field_weight.copy()
+        sl = slice(first, first + count)
+        for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                     "field_target"):
+            setattr(out, name, np.ascontiguousarray(getattr(self, name)[sl]))
+        return out
+
+    def take(self, variants) -> "SystemBatchHost":
+        """Batch made of the listed variants (in that order)."""
+        idx = np.asarray(variants, dtype=np.int64)
+        out = self.subset(0, 0)
+        for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                     "field_target"):
+            setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
+        return out
+
+    def validate_values(self) -> None:
+        """validate_values (src/batch/system_batch.cpp:558) for the fields traced here."""
+        for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                     "field_target", "wavelength_weight", "field_weight"):
+            a = getattr(self, name)
+            if not np.all(np.isfinite(a)):
+                bad = np.argwhere(~np.isfinite(a))[0]
+                raise ValueError(f"SystemBatchHost: {name}{list(bad)} is not finite")
+        if np.any(self.pupil_radius <= 0):
+            raise ValueError("SystemBatchHost: pupil radius must be > 0")
+        if np.any(self.index <= 0):
+            raise ValueError("SystemBatchHost: refractive indices must be > 0")
+        if np.any(self.wavelength_weight < 0) or np.any(self.field_weight < 0):
+            raise ValueError("SystemBatchHost: weights must be >= 0")
+        if not self.reference_wavelength_nm > 0:
+            raise ValueError("SystemBatchHost: reference wavelength must be > 0")
+        for f, m in enumerate(self.topology.pupil_mode):
+            if m == PUPIL_AXIS and np.any(self.field_angle[:, f] != 0.0):
+                raise ValueError(f"SystemBatchHost: field {f} is an axis field but a variant "
+                                 "has a non-zero field angle (check_pupil_modes)")
+
+    # ---- C ABI views ----------------------------------------------------------------------
+    def view(self) -> _capi.BatchView:
+        """mkb_batch_view over the host arrays (valid while this batch is alive)."""
+        arrays = {}
+        for name in ("type", "wavelength_weight", "field_weight", "curvature", "thickness",
+                     "index", "pupil_radius", "field_angle", "field_target"):
+            a = getattr(self, name)
+            if not a.flags.c_contiguous:
+                a = np.ascontiguousarray(a)
+                setattr(self, name, a)
+            arrays[name] = a
+        v = _capi.BatchView()
+        v.variants = self.variants
+        v.surfaces, v.wavelengths, v.fields = self.surfaces, self.wavelengths, self.fields
+        v.ghost_plates = v.ghost_terms = 0
+        v.reference_wavelength_nm = self.reference_wavelength_nm
+        v.type = _capi.ptr(arrays["type"], C.c_uint8)
+        for name in ("wavelength_weight", "field_weight", "curvature", "thickness", "index",
+                     "pupil_radius", "field_angle", "field_target"):
+            setattr(v, name, _capi.ptr(arrays[name]))
+        v._keep = arrays  # keep the arrays alive with the struct
+        return v
+
+
+@dataclass
+class ResidualSettings:
+    """ResidualSettings (batch_residuals.hpp:24)."""
+
+    rings: int = 10
+    spokes: int = 8
+    failure: int = FAILURE_SOFT
+    fail_weight: float = DEFAULT_FAIL_WEIGHT
+    precision: int = PRECISION_FP64
+
+
+class ResidualLayout:
+    """Row layout of one variant's residual vector (batch_residuals.hpp:62)."""
+
+    def __init__(self, topology: BatchTopology, settings: ResidualSettings | None = None):
+        settings = settings or ResidualSettings()
+        topology.validate()
+        if not 1 <= settings.rings <= MAX_RINGS:
+            raise ValueError(f"ResidualLayout: rings must be in [1, {MAX_RINGS}]")
+        if settings.spokes < 1:
+            raise ValueError("ResidualLayout: spokes must be >= 1")
+        if any(m != PUPIL_AXIS for m in topology.pupil_mode) and settings.spokes > 64:
+            raise ValueError("ResidualLayout: spokes must be <= 64 in this build")
+        if settings.failure not in (FAILURE_SOFT, FAILURE_HARD):
+            raise ValueError("ResidualLayout: unknown failure mode")
+        if not (settings.fail_weight >= 0 and math.isfinite(settings.fail_weight)):
+            raise ValueError("ResidualLayout: fail_weight must be finite and >= 0")
+        if settings.precision not in (PRECISION_FP64, PRECISION_MIXED):
+            raise ValueError("ResidualLayout: unknown precision")
+        self.topology = topology
+        self.settings = settings
+        self.fields = topology.fields
+        self.wavelengths = topology.wavelengths
+        self.samples = [sample_count(settings.rings, settings.spokes, m)
+                        for m in topology.pupil_mode]
+        self.field_offset = []
+        off = 0
+        for n in self.samples:
+            self.field_offset.append(off)
+            off += self.wavelengths * n
+        self.rays_per_variant = off
+
+    def offset(self, f: int, l: int) -> int:
+        if not 0 <= f < self.fields:
+            raise IndexError(f"ResidualLayout: field {f} does not exist")
+        if not 0 <= l < self.wavelengths:
+            raise IndexError(f"ResidualLayout: wavelength {l} does not exist")
+        return self.field_offset[f] + l * self.samples[f]
+
+    @property
+    def soft_failure(self) -> bool:
+        return self.settings.failure == FAILURE_SOFT
+
+    @property
+    def penalty_rows(self) -> int:
+        return self.rays_per_variant if self.soft_failure else 0
+
+    @property
+    def trace_rows(self) -> int:
+        return self.rays_per_variant + self.penalty_rows
+
+    def plan(self, batch: SystemBatchHost) -> _capi.ResidualPlan:
+        """mkb_residual_plan for this layout and the shared weights of `batch`."""
+        u, w = gauss_legendre_unit(self.settings.rings)
+        keep = {
+            "pupil_mode": np.asarray(self.topology.pupil_mode, dtype=np.uint8),
+            "field_weight": np.ascontiguousarray(batch.field_weight, dtype=np.float64),
+            "wavelength_weight": np.ascontiguousarray(batch.wavelength_weight,
+                                                      dtype=np.float64),
+            "quad_u": np.asarray(u, dtype=np.float64),
+            "quad_w": np.asarray(w, dtype=np.float64),
+        }
+        p = _capi.ResidualPlan()
+        p.rings, p.spokes = self.settings.rings, self.settings.spokes
+        p.failure, p.precision = self.settings.failure, self.settings.precision
+        p.fail_weight = self.settings.fail_weight
+        p.reference_wavelength_nm = batch.reference_wavelength_nm
+        p.fields, p.wavelengths = self.fields, self.wavelengths
+        p.pupil_mode = _capi.ptr(keep["pupil_mode"], C.c_uint8)
+        for name in ("field_weight", "wavelength_weight", "quad_u", "quad_w"):
+            setattr(p, name, _capi.ptr(keep[name]))
+        p._keep = keep
+        return p
+
+
+@dataclass
+class Variable:
+    """One LM variable (variable_set.hpp:20): type, table surface, bounds, typical size."""
+
+    type: int
+    surface: int
+    lower: float = -math.inf
+    upper: float = math.inf
+    typical: float = 1.0
+
+
+@dataclass
+class VariableSet:
+    """Fixed list of P variables for batches of one topology (variable_set.hpp:63)."""
+
+    topology: BatchTopology
+    variables: list[Variable] = field(default_factory=list)
+
+    def __post_init__(self):
+        S = self.topology.surfaces
+        if len(self.variables) > MAX_VARIABLES:
+            raise ValueError(f"VariableSet: at most {MAX_VARIABLES} variables")
+        seen = set()
+        for k, v in enumerate(self.variables):
+            if v.type == VAR_CURVATURE:
+                if not (1 <= v.surface < S and self.topology.type[v.surface] == SURFACE_SPHERE):
+                    raise ValueError(f"VariableSet: variable {k}: curvature needs a sphere")
+            elif v.type == VAR_THICKNESS:
+                if not 0 <= v.surface < S - 1:
+                    raise ValueError(f"VariableSet: variable {k}: thickness surface out of range")
+            elif v.type == VAR_WORKING_DISTANCE:
+                v.surface = S - 1
+            else:
+                raise NotImplementedError(f"VariableSet: variable type {v.type}")
+            key = (v.type == VAR_CURVATURE, v.surface)
+            if key in seen:
+                raise ValueError(f"VariableSet: parameter of variable {k} already used")
+            seen.add(key)
+            if math.isnan(v.lower) or math.isnan(v.upper) or v.lower > v.upper:
+                raise ValueError(f"VariableSet: invalid bounds of variable {k}")
+            if not (v.typical > 0 and math.isfinite(v.typical)):
+                raise ValueError(f"VariableSet: typical size of variable {k} must be > 0")
+
+    @property
+    def size(self) -> int:
+        return len(self.variables)
+
+    def lower(self) -> np.ndarray:
+        return np.array([v.lower for v in self.variables])
+
+    def upper(self) -> np.ndarray:
+        return np.array([v.upper for v in self.variables])
+
+    def typical(self) -> np.ndarray:
+        return np.array([v.typical for v in self.variables])
+
+    def extract(self, batch: SystemBatchHost, v: int) -> np.ndarray:
+        """x from variant v (VariableSet::extract, variable_set.cpp:222)."""
+        x = np.empty(self.size)
+        for k, var in enumerate(self.variables):
+            x[k] = (batch.curvature[v, var.surface] if var.type == VAR_CURVATURE
+                    else batch.thickness[v, var.surface])
+        return x
+
+    def apply(self, batch: SystemBatchHost, v: int, x) -> None:
+        """Writes x into variant v (VariableSet::apply, variable_set.cpp:237)."""
+        x = np.asarray(x, dtype=np.float64)
+        if x.shape != (self.size,):
+            raise ValueError("VariableSet.apply: x has the wrong length")
+        if not np.all(np.isfinite(x)):
+            raise ValueError("VariableSet.apply: x is not finite")
+        for k, var in enumerate(self.variables):
+            if var.type == VAR_CURVATURE:
+                batch.curvature[v, var.surface] = x[k]
+            else:
+                batch.thickness[v, var.surface] = x[k]
+
+    def c_struct(self) -> _capi.Variables:
+        keep = {
+            "type": np.array([v.type for v in self.variables], dtype=np.int32),
+            "surface": np.array([v.surface for v in self.variables], dtype=np.int32),
+            "lower": self.lower(), "upper": self.upper(), "typical": self.typical(),
+        }
+        s = _capi.Variables()
+        s.count = self.size
+        s.type = _capi.ptr(keep["type"], C.c_int32)
+        s.surface = _capi.ptr(keep["surface"], C.c_int32)
+        s.lower, s.upper, s.typical = (_capi.ptr(keep[n]) for n in ("lower", "upper", "typical"))
+        s._keep = keep
+        return s

@@ -1,0 +1,245 @@
+"""Seeded synthetic workloads (lens systems) with the shapes of the benchmark configurations.
+
+One generator feeds the CUDA path and the CPU oracles byte-identically. Random numbers come
+from a counter-based splitmix64 stream (portable, no std:: distribution), Gaussian noise from
+Box-Muller on it. Seeds: configuration k uses 20261203 + k unless given.
+
+  singlet(...)    1024 biconvex singlets: stop plane at the first vertex, c = +1/50, -1/50,
+                  t = 6 mm, image plane at the paraxial focus of each variant, 2-term Cauchy
+                  n = 1.5046 + 0.00420 / lambda^2 (um) at 486.1 / 587.6 / 656.3 nm, fields
+                  0, 0.7, 1.0 degree, pupil radius 5 mm, c1, c2, t perturbed by 5 % Gaussian
+                  noise, quadrature 6 rings x 12 spokes.
+  objective(...)  4096 seven-element (14-sphere) objectives with curvatures U(-1/15, 1/15),
+                  air gaps U(0.1, 5), glass thickness U(1, 8), 3-term Sellmeier glasses fitted
+                  to n_d U(1.45, 1.90), V_d U(25, 95), 7 wavelengths 405..700 nm, 5 fields,
+                  16 rings x 32 spokes, entrance pupil sized for image-side NA 0.95, image
+                  plane at the paraxial focus, soft failure.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .batch import (BatchTopology, FAILURE_SOFT, PRECISION_FP64, ResidualSettings,
+                    SURFACE_SPHERE, SURFACE_STOP, SystemBatchHost, VAR_CURVATURE,
+                    VAR_THICKNESS, VAR_WORKING_DISTANCE, Variable, VariableSet)
+from .quadrature import PUPIL_AXIS, PUPIL_HALF
+
+_M64 = (1 << 64) - 1
+_GOLDEN = 0x9E3779B97F4A7C15
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser (Steele, Lea, Flood 2014) on uint64 arrays."""
+    with np.errstate(over="ignore"):
+        z = (x + np.uint64(_GOLDEN)).astype(np.uint64)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+class Stream:
+    """Counter-based stream: draw n values for a named purpose, independent of call order."""
+
+    def __init__(self, seed: int):
+        self.seed = np.uint64(seed & _M64)
+
+    def _bits(self, tag: int, n: int) -> np.ndarray:
+        with np.errstate(over="ignore"):
+            base = splitmix64(np.array([self.seed ^ np.uint64(tag * 0x632BE59BD9B4E019 & _M64)],
+                                       dtype=np.uint64))[0]
+            ctr = np.arange(n, dtype=np.uint64) * np.uint64(_GOLDEN) + base
+        return splitmix64(ctr)
+
+    def uniform(self, tag: int, n: int) -> np.ndarray:
+        """U[0, 1) with 53 bits: (bits >> 11) * 2^-53."""
+        return (self._bits(tag, n) >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+    def normal(self, tag: int, n: int) -> np.ndarray:
+        """N(0, 1) by Box-Muller on two uniform streams."""
+        u1 = 1.0 - self.uniform(tag * 2 + 1, n)  # (0, 1]
+        u2 = self.uniform(tag * 2 + 2, n)
+        return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+def cauchy_index(lambda_nm, a: float = 1.5046, b: float = 0.00420) -> np.ndarray:
+    lam_um = np.asarray(lambda_nm, dtype=np.float64) * 1e-3
+    return a + b / (lam_um * lam_um)
+
+
+def paraxial(curvature: np.ndarray, thickness: np.ndarray, index_ref: np.ndarray):
+    """Paraxial y-nu trace of a collimated ray (y = 1) for [V][S] systems at one wavelength.
+
+    index_ref[v][s] is the medium after surface s (air before surface 0). Returns (efl, bfd):
+    effective focal length -1/u' and back focal distance -y/u' after the last surface.
+    """
+    V, S = curvature.shape
+    y = np.ones(V)
+    nu = np.zeros(V)  # n * u
+    n_prev = index_ref[:, 0]
+    for s in range(1, S):
+        y = y + thickness[:, s - 1] * nu / n_prev
+        n_after = index_ref[:, s]
+        nu = nu - y * curvature[:, s] * (n_after - n_prev)
+        n_prev = n_after
+    u_last = nu / n_prev
+    with np.errstate(divide="ignore", invalid="ignore"):
+        efl = -1.0 / u_last
+        bfd = -y / u_last
+    return efl, bfd
+
+
+# ---- configuration 1: biconvex singlets --------------------------------------------------
+
+SINGLET_WAVELENGTHS = (486.1, 587.6, 656.3)
+
+
+def singlet(variants: int = 1024, seed: int = 20261203 + 1, sigma: float = 0.05,
+            failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+    """Configuration 1. Returns (batch, settings, variables, x0 [V][P])."""
+    topo = BatchTopology(surfaces=3, wavelengths=3, fields=3,
+                         type=[SURFACE_STOP, SURFACE_SPHERE, SURFACE_SPHERE],
+                         pupil_mode=[PUPIL_AXIS, PUPIL_HALF, PUPIL_HALF])
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.6
+    b.wavelength_nm[:] = SINGLET_WAVELENGTHS
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    noise = rng.normal(1, 3 * variants).reshape(variants, 3)
+    c1 = (1.0 / 50.0) * (1.0 + sigma * noise[:, 0])
+    c2 = (-1.0 / 50.0) * (1.0 + sigma * noise[:, 1])
+    t = 6.0 * (1.0 + sigma * noise[:, 2])
+    b.curvature[:, 1] = c1
+    b.curvature[:, 2] = c2
+    b.thickness[:, 0] = 0.0  # stop plane at the first vertex
+    b.thickness[:, 1] = t
+    n = cauchy_index(SINGLET_WAVELENGTHS)
+    b.index[:, 0, :] = 1.0
+    b.index[:, 1, :] = n[None, :]
+    b.index[:, 2, :] = 1.0
+    n_ref = np.ones((variants, 3))
+    n_ref[:, 1] = cauchy_index(587.6)
+    efl, bfd = paraxial(b.curvature, b.thickness, n_ref)
+    b.thickness[:, 2] = bfd
+    b.pupil_radius[:] = 5.0
+    angles = np.deg2rad(np.array([0.0, 0.7, 1.0]))
+    b.field_angle[:, :] = angles[None, :]
+    b.field_target[:, :] = efl[:, None] * np.tan(angles)[None, :]
+    settings = ResidualSettings(rings=6, spokes=12, failure=failure, precision=precision)
+    vs = VariableSet(topo, [
+        Variable(VAR_CURVATURE, 1, -0.2, 0.2, 0.01),
+        Variable(VAR_CURVATURE, 2, -0.2, 0.2, 0.01),
+        Variable(VAR_THICKNESS, 1, 0.5, 20.0, 1.0),
+        Variable(VAR_WORKING_DISTANCE, 2, 1.0, 500.0, 1.0),
+    ])
+    x0 = np.stack([vs.extract(b, v) for v in range(variants)])
+    return b, settings, vs, x0
+
+
+# ---- configuration 2: seven-element objectives ---------------------------------------------
+
+OBJECTIVE_WAVELENGTHS = tuple(float(x) for x in np.linspace(405.0, 700.0, 7))
+_SELLMEIER_C = (0.0060, 0.0200, 103.56)  # um^2, poles of the 3-term Sellmeier model
+_SELLMEIER_B3 = 1.03
+
+
+def sellmeier_index(b1, b2, lambda_nm):
+    """n(lambda) of n^2 - 1 = sum_i B_i l^2 / (l^2 - C_i) with B3 and C_i fixed."""
+    l2 = (np.asarray(lambda_nm, dtype=np.float64) * 1e-3) ** 2
+    c1, c2, c3 = _SELLMEIER_C
+    n2 = 1.0 + b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2) + _SELLMEIER_B3 * l2 / (l2 - c3)
+    return np.sqrt(n2)
+
+
+def sellmeier_fit(nd, vd):
+    """B1, B2 so that n(587.56) = n_d and n_F^2 - n_C^2 = 2 n_d (n_d - 1) / V_d.
+
+    The second condition is the first-order form of n_F - n_C = (n_d - 1) / V_d; both are
+    linear in (B1, B2) for fixed poles, so the fit is a 2x2 solve per glass.
+    """
+    nd = np.asarray(nd, dtype=np.float64)
+    vd = np.asarray(vd, dtype=np.float64)
+    c1, c2, c3 = _SELLMEIER_C
+
+    def terms(lam_nm):
+        l2 = (lam_nm * 1e-3) ** 2
+        return l2 / (l2 - c1), l2 / (l2 - c2), _SELLMEIER_B3 * l2 / (l2 - c3)
+
+    ad1, ad2, ad3 = terms(587.56)
+    af1, af2, af3 = terms(486.13)
+    ac1, ac2, ac3 = terms(656.27)
+    r1 = nd * nd - 1.0 - ad3
+    r2 = 2.0 * nd * (nd - 1.0) / vd - (af3 - ac3)
+    m11, m12, m21, m22 = ad1, ad2, af1 - ac1, af2 - ac2
+    det = m11 * m22 - m12 * m21
+    b1 = (r1 * m22 - m12 * r2) / det
+    b2 = (m11 * r2 - m21 * r1) / det
+    return b1, b2
+
+
+def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
+              spokes: int = 32, na: float = 0.95, max_field_deg: float = 1.0,
+              failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+    """Configuration 2. Returns (batch, settings, variables, x0 [V][P])."""
+    S = 15
+    topo = BatchTopology(surfaces=S, wavelengths=7, fields=5,
+                         type=[SURFACE_STOP] + [SURFACE_SPHERE] * 14,
+                         pupil_mode=[PUPIL_AXIS] + [PUPIL_HALF] * 4)
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.56
+    b.wavelength_nm[:] = OBJECTIVE_WAVELENGTHS
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    # Draw candidates in rounds; keep the first candidate of each variant whose paraxial
+    # focal length and back focus are usable (5 <= f' <= 200 mm, BFD > 0.5 mm).
+    todo = np.arange(variants)
+    attempt = 0
+    while todo.size:
+        if attempt >= 64:
+            raise RuntimeError("objective(): could not draw usable systems")
+        n = todo.size
+        tag = 100 * (attempt + 1)
+        curv = (rng.uniform(tag + 1, variants * 14).reshape(variants, 14)[todo] * 2.0 - 1.0) / 15.0
+        gaps = 0.1 + 4.9 * rng.uniform(tag + 2, variants * 8).reshape(variants, 8)[todo]
+        glass_t = 1.0 + 7.0 * rng.uniform(tag + 3, variants * 7).reshape(variants, 7)[todo]
+        nd = 1.45 + 0.45 * rng.uniform(tag + 4, variants * 7).reshape(variants, 7)[todo]
+        vd = 25.0 + 70.0 * rng.uniform(tag + 5, variants * 7).reshape(variants, 7)[todo]
+        c = np.zeros((n, S))
+        t = np.zeros((n, S))
+        c[:, 1:] = curv
+        t[:, 0] = gaps[:, 0]
+        for e in range(7):
+            t[:, 1 + 2 * e] = glass_t[:, e]
+            if e < 6:
+                t[:, 2 + 2 * e] = gaps[:, e + 1]
+        b1, b2 = sellmeier_fit(nd, vd)
+        idx = np.ones((n, S, 7))
+        n_ref = np.ones((n, S))
+        for e in range(7):
+            idx[:, 1 + 2 * e, :] = sellmeier_index(b1[:, e, None], b2[:, e, None],
+                                                   np.array(OBJECTIVE_WAVELENGTHS)[None, :])
+            n_ref[:, 1 + 2 * e] = sellmeier_index(b1[:, e], b2[:, e], 587.56)
+        efl, bfd = paraxial(c, t, n_ref)
+        ok = np.isfinite(efl) & (efl >= 5.0) & (efl <= 200.0) & np.isfinite(bfd) & (bfd > 0.5)
+        sel = todo[ok]
+        b.curvature[sel] = c[ok]
+        t[ok, S - 1] = bfd[ok]
+        b.thickness[sel] = t[ok]
+        b.index[sel] = idx[ok]
+        b.pupil_radius[sel] = na * efl[ok]
+        b.field_target[sel] = efl[ok, None] * np.tan(
+            np.deg2rad(max_field_deg * np.linspace(0.0, 1.0, 5)))[None, :]
+        todo = todo[~ok]
+        attempt += 1
+    b.field_angle[:, :] = np.deg2rad(max_field_deg * np.linspace(0.0, 1.0, 5))[None, :]
+    settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
+    variables = [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, S)]
+    variables += [Variable(VAR_THICKNESS, s, 0.05, 50.0, 1.0) for s in range(0, S - 1)]
+    variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1000.0, 1.0)]
+    vs = VariableSet(topo, variables)
+    x0 = np.stack([vs.extract(b, v) for v in range(variants)])
+    return b, settings, vs, x0

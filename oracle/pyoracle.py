@@ -1,0 +1,216 @@
+"""ctypes front end of the two CPU oracles (test infrastructure only).
+
+``port()`` loads liboracle.so (the C restatement), ``reference()`` loads _ref/libmko_ref.so
+(the reference's own sources); both expose the same calls on SystemBatchHost inputs.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from mikroptim_b200 import _capi
+from mikroptim_b200.batch import ResidualLayout, SystemBatchHost, VariableSet
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libmko_ref.so")
+REFERENCE_TREE = "/root/reference"
+
+
+def build(reference: bool = True) -> None:
+    """Compile liboracle.so and, where the reference tree exists, _ref/libmko_ref.so."""
+    targets = ["oracle"]
+    if reference and os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}", *targets],
+                   check=True)
+
+
+_PB = C.POINTER(_capi.BatchView)
+_PP = C.POINTER(_capi.ResidualPlan)
+_PV = C.POINTER(_capi.Variables)
+
+
+class _Oracle:
+    prefix = ""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        p = self.prefix
+        L = self.lib
+        getattr(L, p + "residuals").argtypes = [_PB, _PP, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int]
+        getattr(L, p + "merit").argtypes = [_PB, _PP, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_int]
+        getattr(L, p + "normal_equations").argtypes = [C.c_void_p, C.c_void_p, C.c_int,
+                                                       C.c_int64, C.c_void_p, C.c_void_p]
+        for fn in ("residuals", "merit", "normal_equations", "fd_jacobian", "adjoint_jacobian"):
+            getattr(L, p + fn).restype = C.c_int
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise ValueError(f"{type(self).__name__}.{what} failed: {self.error()}")
+
+    def error(self) -> str:
+        return "bad argument"
+
+    # ---- forward ------------------------------------------------------------------------
+    def residuals(self, batch: SystemBatchHost, layout: ResidualLayout, threads: int = 1):
+        V, rays, rows = batch.variants, layout.rays_per_variant, layout.trace_rows
+        res = np.zeros((V, rows))
+        opd = np.zeros((V, rays))
+        st = np.zeros((V, rays), dtype=np.uint8)
+        view, plan = batch.view(), layout.plan(batch)
+        rc = getattr(self.lib, self.prefix + "residuals")(
+            C.byref(view), C.byref(plan), res.ctypes.data, opd.ctypes.data, st.ctypes.data,
+            threads)
+        self._check(rc, "residuals")
+        return res, opd, st
+
+    def merit(self, batch: SystemBatchHost, layout: ResidualLayout, threads: int = 1):
+        V = batch.variants
+        merit = np.zeros(V)
+        failed = np.zeros(V, dtype=np.int64)
+        hard = np.zeros(V, dtype=np.int64)
+        view, plan = batch.view(), layout.plan(batch)
+        rc = getattr(self.lib, self.prefix + "merit")(
+            C.byref(view), C.byref(plan), merit.ctypes.data, failed.ctypes.data,
+            hard.ctypes.data, threads)
+        self._check(rc, "merit")
+        return merit, failed, hard
+
+    # ---- Jacobians ----------------------------------------------------------------------
+    def _jac_args(self, batch, layout, vs: VariableSet, x0):
+        x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, vs.size)
+        runs = x0.shape[0]
+        R = layout.trace_rows
+        J = np.zeros((runs, vs.size, R))
+        r0 = np.zeros((runs, R))
+        return x0, runs, R, J, r0, batch.view(), layout.plan(batch), vs.c_struct()
+
+    def normal_equations(self, J: np.ndarray, r: np.ndarray):
+        P, R = J.shape
+        J = np.ascontiguousarray(J)
+        r = np.ascontiguousarray(r)
+        A = np.zeros((P, P))
+        g = np.zeros(P)
+        rc = getattr(self.lib, self.prefix + "normal_equations")(
+            J.ctypes.data, r.ctypes.data, P, R, A.ctypes.data, g.ctypes.data)
+        self._check(rc, "normal_equations")
+        return A, g
+
+
+class Port(_Oracle):
+    """liboracle.so: the plain-C restatement."""
+
+    prefix = "mko_port_"
+
+    def __init__(self, path: str = PORT_LIB):
+        super().__init__(path)
+        self.lib.mko_port_fd_jacobian.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        self.lib.mko_port_adjoint_jacobian.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int,
+                                                       C.c_void_p, C.c_void_p, C.c_void_p,
+                                                       C.c_int]
+
+    def fd_jacobian(self, batch, layout, vs, x0, threads: int = 1):
+        x0, runs, R, J, r0, view, plan, vars_ = self._jac_args(batch, layout, vs, x0)
+        ch = np.zeros((runs, vs.size), dtype=np.int64)
+        rc = self.lib.mko_port_fd_jacobian(C.byref(view), C.byref(plan), C.byref(vars_),
+                                           x0.ctypes.data, runs, J.ctypes.data, r0.ctypes.data,
+                                           ch.ctypes.data, threads)
+        self._check(rc, "fd_jacobian")
+        return J, r0, ch
+
+    def adjoint_jacobian(self, batch, layout, vs, x0, threads: int = 1):
+        x0, runs, R, J, r0, view, plan, vars_ = self._jac_args(batch, layout, vs, x0)
+        st = np.zeros((runs, layout.rays_per_variant), dtype=np.uint8)
+        rc = self.lib.mko_port_adjoint_jacobian(C.byref(view), C.byref(plan), C.byref(vars_),
+                                                x0.ctypes.data, runs, J.ctypes.data,
+                                                r0.ctypes.data, st.ctypes.data, threads)
+        self._check(rc, "adjoint_jacobian")
+        return J, r0, st
+
+
+class Reference(_Oracle):
+    """_ref/libmko_ref.so: the reference's own CPU sources."""
+
+    prefix = "mko_ref_"
+
+    def __init__(self, path: str = REF_LIB):
+        super().__init__(path)
+        L = self.lib
+        L.mko_ref_last_error.restype = C.c_char_p
+        L.mko_ref_fd_jacobian.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]
+        L.mko_ref_adjoint_jacobian.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_int]
+        L.mko_ref_optimize_lm.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mko_ref_optimize_lm.restype = C.c_int
+
+    def error(self) -> str:
+        return self.lib.mko_ref_last_error().decode(errors="replace")
+
+    def fd_jacobian(self, batch, layout, vs, x0, threads: int = 1):
+        x0, runs, R, J, r0, view, plan, vars_ = self._jac_args(batch, layout, vs, x0)
+        ch = np.zeros((runs, vs.size), dtype=np.int64)
+        rc = self.lib.mko_ref_fd_jacobian(C.byref(view), C.byref(plan), C.byref(vars_),
+                                          x0.ctypes.data, runs, J.ctypes.data, r0.ctypes.data,
+                                          ch.ctypes.data)
+        self._check(rc, "fd_jacobian")
+        return J, r0, ch
+
+    def adjoint_jacobian(self, batch, layout, vs, x0, threads: int = 1):
+        x0, runs, R, J, r0, view, plan, vars_ = self._jac_args(batch, layout, vs, x0)
+        st = np.zeros((runs, layout.rays_per_variant), dtype=np.uint8)
+        rc = self.lib.mko_ref_adjoint_jacobian(C.byref(view), C.byref(plan), C.byref(vars_),
+                                               x0.ctypes.data, runs, J.ctypes.data,
+                                               r0.ctypes.data, st.ctypes.data, threads)
+        self._check(rc, "adjoint_jacobian")
+        return J, r0, st
+
+    def optimize_lm(self, batch, layout, vs, x0, max_iterations: int = 100,
+                    method: str = "adjoint", penalty_rounds: int = 1, threads: int = 0):
+        x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, vs.size)
+        runs, P = x0.shape
+        x = np.zeros((runs, P))
+        merit = np.zeros(runs)
+        status = np.zeros(runs, dtype=np.int32)
+        its = np.zeros(runs, dtype=np.int32)
+        acc = np.zeros(runs, dtype=np.int32)
+        hist = np.zeros((runs, max_iterations + 1))
+        view, plan, vars_ = batch.view(), layout.plan(batch), vs.c_struct()
+        rc = self.lib.mko_ref_optimize_lm(
+            C.byref(view), C.byref(plan), C.byref(vars_), x0.ctypes.data, runs, max_iterations,
+            1 if method == "adjoint" else 0, penalty_rounds, threads, x.ctypes.data,
+            merit.ctypes.data, status.ctypes.data, its.ctypes.data, acc.ctypes.data,
+            hist.ctypes.data)
+        self._check(rc, "optimize_lm")
+        return dict(x=x, merit=merit, status=status, iterations=its, accepted=acc,
+                    history=hist)
+
+
+_port = None
+_reference = None
+
+
+def port() -> Port:
+    global _port
+    if _port is None:
+        _port = Port()
+    return _port
+
+
+def reference() -> Reference:
+    global _reference
+    if _reference is None:
+        _reference = Reference()
+    return _reference

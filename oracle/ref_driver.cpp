@@ -1,0 +1,339 @@
+// Test infrastructure (the oracle), not product code.
+//
+// C-ABI driver around the reference's own CPU implementation of the trace-and-optimise path,
+// compiled from the reference sources where they lie (oracle/Makefile) into
+// oracle/_ref/libmko_ref.so. It turns the flat mkb_batch_view / mkb_residual_plan /
+// mkb_variables structs of include/mikroptim_b200.h into the reference's SystemBatchHost,
+// ResidualLayout and VariableSet and calls:
+//   residuals_cpu          src/batch/batch_residuals.cpp:272
+//   merit_cpu              src/batch/batch_merit.cpp:61
+//   fd_jacobian_cpu        src/optim/fd_jacobian.cpp:182
+//   adjoint_jacobian_cpu   src/optim/adjoint_jacobian.cpp:370
+//   normal_equations_host  include/mikroptim/optim/normal_equations.hpp:33
+//   optimize_lm_cpu        src/optim/levenberg_marquardt.cpp:972
+// Only tests/, the golden-fixture script and bench.py's CPU legs load this library.
+
+#include "mikroptim_b200.h"
+
+#include "mikroptim/batch/batch_merit.hpp"
+#include "mikroptim/batch/batch_residuals.hpp"
+#include "mikroptim/batch/system_batch.hpp"
+#include "mikroptim/model/system.hpp"
+#include "mikroptim/optim/adjoint_jacobian.hpp"
+#include "mikroptim/optim/fd_jacobian.hpp"
+#include "mikroptim/optim/levenberg_marquardt.hpp"
+#include "mikroptim/optim/normal_equations.hpp"
+#include "mikroptim/optim/variable_set.hpp"
+#include "optim/parallel_variants.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(const std::exception& e) {
+    g_error = e.what();
+    return -1;
+}
+
+mko::BatchTopology topology_of_view(const mkb_batch_view& v, const mkb_residual_plan& plan) {
+    mko::BatchTopology t;
+    t.surfaces = v.surfaces;
+    t.wavelengths = v.wavelengths;
+    t.fields = v.fields;
+    t.ghost_plates = 0;
+    t.ghost_terms = 0;
+    t.source = mko::SourceKind::Collimated;
+    for (int s = 0; s < v.surfaces; ++s) {
+        t.type.push_back(static_cast<mko::SurfaceKind>(v.type[s]));
+    }
+    for (int f = 0; f < v.fields; ++f) {
+        t.pupil_mode.push_back(static_cast<mko::PupilMode>(plan.pupil_mode[f]));
+    }
+    return t;
+}
+
+mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_plan& plan) {
+    mko::SystemBatchHost b(topology_of_view(v, plan), v.variants);
+    const int S = v.surfaces, L = v.wavelengths, F = v.fields;
+    b.reference_wavelength_nm = v.reference_wavelength_nm;
+    for (int l = 0; l < L; ++l) {
+        b.wavelength_weight(l) = v.wavelength_weight[l];
+        b.wavelength_nm(l) = 500.0 + l; // not read by the trace (index is given directly)
+    }
+    for (int f = 0; f < F; ++f) {
+        b.field_weight(f) = v.field_weight[f];
+    }
+    for (int i = 0; i < v.variants; ++i) {
+        for (int s = 0; s < S; ++s) {
+            b.curvature(i, s) = v.curvature[i * S + s];
+            b.thickness(i, s) = v.thickness[i * S + s];
+            for (int l = 0; l < L; ++l) {
+                b.index(i, s, l) = v.index[(static_cast<std::size_t>(i) * S + s) * L + l];
+            }
+            b.paraxial_index(i, s) = v.index[(static_cast<std::size_t>(i) * S + s) * L];
+        }
+        b.pupil_radius(i) = v.pupil_radius[i];
+        for (int f = 0; f < F; ++f) {
+            b.field_angle(i, f) = v.field_angle[i * F + f];
+            b.field_target(i, f) = v.field_target[i * F + f];
+        }
+    }
+    return b;
+}
+
+mko::ResidualSettings settings_of(const mkb_residual_plan& plan) {
+    mko::ResidualSettings s;
+    s.rings = plan.rings;
+    s.spokes = plan.spokes;
+    s.failure = plan.failure == MKB_FAILURE_HARD ? mko::FailureMode::Hard : mko::FailureMode::Soft;
+    s.fail_weight = plan.fail_weight;
+    return s;
+}
+
+// A file-model description whose surfaces match the batch (variant 0 values), with one
+// variable item per entry of `vars`. Only used to build the reference VariableSet.
+mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_variables& vars,
+                                       const double* x0) {
+    mko::SystemDescription d;
+    d.name = "oracle";
+    d.spectrum.reference_nm = b.reference_wavelength_nm;
+    for (int l = 0; l < b.wavelengths(); ++l) {
+        d.spectrum.wavelengths_nm.push_back(b.wavelength_nm(l));
+        d.spectrum.weights.push_back(b.wavelength_weight(l));
+    }
+    d.source.type = mko::SourceType::Collimated;
+    for (int f = 0; f < b.fields(); ++f) {
+        d.source.field_angles_deg.push_back(b.field_angle(0, f) * 180.0 / M_PI);
+        d.source.field_weights.push_back(b.field_weight(f));
+    }
+    for (int s = 0; s < b.surfaces(); ++s) {
+        mko::Surface surf;
+        const auto kind = b.type(s);
+        surf.type = kind == mko::SurfaceKind::Stop    ? mko::SurfaceType::Stop
+                    : kind == mko::SurfaceKind::Plane ? mko::SurfaceType::Plane
+                                                      : mko::SurfaceType::Sphere;
+        surf.curvature = b.curvature(0, s);
+        surf.thickness = b.thickness(0, s);
+        const double n = b.index(0, s, 0);
+        if (n == 1.0) {
+            surf.material.kind = mko::MaterialKind::Air;
+        } else {
+            surf.material.kind = mko::MaterialKind::Constant;
+            surf.material.n = n;
+        }
+        surf.semi_diameter = s == 0 ? b.pupil_radius(0) : 100.0;
+        d.surfaces.push_back(surf);
+    }
+    // start values of the description = x0 of run 0 (resolve_variables checks the bounds)
+    mko::Variables items;
+    for (int k = 0; k < vars.count; ++k) {
+        mko::VariableSpec spec;
+        const int s = vars.surface[k];
+        if (vars.type[k] == MKB_VAR_CURVATURE) {
+            spec.type = mko::VariableType::Curvature;
+            spec.selection = mko::SurfaceSelection::One;
+            spec.surfaces = {s};
+            d.surfaces[s].curvature = x0[k];
+        } else if (vars.type[k] == MKB_VAR_THICKNESS) {
+            spec.type = mko::VariableType::Thickness;
+            spec.selection = mko::SurfaceSelection::One;
+            spec.surfaces = {s};
+            d.surfaces[s].thickness = x0[k];
+        } else {
+            spec.type = mko::VariableType::WorkingDistance;
+            spec.selection = mko::SurfaceSelection::None;
+            d.surfaces[b.surfaces() - 1].thickness = x0[k];
+        }
+        if (std::isfinite(vars.lower[k])) {
+            spec.min = vars.lower[k];
+        }
+        if (std::isfinite(vars.upper[k])) {
+            spec.max = vars.upper[k];
+        }
+        spec.typical = vars.typical[k];
+        items.items.push_back(spec);
+    }
+    d.variables = items;
+    return d;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* mko_ref_last_error(void) {
+    return g_error.c_str();
+}
+
+int64_t mko_ref_rays_per_variant(const mkb_batch_view* view, const mkb_residual_plan* plan) {
+    try {
+        const mko::ResidualLayout layout(topology_of_view(*view, *plan), settings_of(*plan));
+        return layout.rays_per_variant();
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// residuals [V][trace_rows], opd [V][rays], status [V][rays]; variants split over `threads`
+// host threads with the reference's own parallel_for_variants.
+int mko_ref_residuals(const mkb_batch_view* view, const mkb_residual_plan* plan, double* residuals,
+                      double* opd, uint8_t* status, int threads) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
+        const std::int64_t rows = layout.trace_rows();
+        const std::int64_t rays = layout.rays_per_variant();
+        mko::detail::parallel_for_variants(0, b.variants(), threads, [&](int v) {
+            const mko::ResidualResult r = mko::residuals_cpu(b, v, layout);
+            std::memcpy(residuals + v * rows, r.residuals.data(), sizeof(double) * rows);
+            if (opd != nullptr) {
+                std::memcpy(opd + v * rays, r.opd.data(), sizeof(double) * rays);
+            }
+            if (status != nullptr) {
+                std::memcpy(status + v * rays, r.status.data(), rays);
+            }
+        });
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int mko_ref_merit(const mkb_batch_view* view, const mkb_residual_plan* plan, double* merit,
+                  int64_t* failed, int64_t* hard_failed, int threads) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
+        mko::detail::parallel_for_variants(0, b.variants(), threads, [&](int v) {
+            const mko::MeritResult r = mko::merit_cpu(b, v, layout, false);
+            merit[v] = r.merit[0];
+            failed[v] = r.failed[0];
+            hard_failed[v] = r.hard_failed[0];
+        });
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// FD Jacobian (central scheme) of `runs` runs; base has 1 variant or one per run.
+// J [runs][P][R], r0 [runs][R], status_changes [runs][P], R = trace_rows.
+int mko_ref_fd_jacobian(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const double* x0, int runs, double* J,
+                        double* r0, int64_t* status_changes) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::SystemDescription d = description_of(b, *vars, x0);
+        const mko::VariableSet set(d, b.topology());
+        mko::FdJacobianOptions opt;
+        opt.quadrature = settings_of(*plan);
+        const auto P = static_cast<std::size_t>(vars->count);
+        const mko::FdJacobian fd = mko::fd_jacobian_cpu(
+            set, b, std::span<const double>(x0, P * static_cast<std::size_t>(runs)), opt);
+        std::memcpy(J, fd.jacobian.data(), sizeof(double) * fd.jacobian.size());
+        std::memcpy(r0, fd.residuals.data(), sizeof(double) * fd.residuals.size());
+        if (status_changes != nullptr) {
+            std::memcpy(status_changes, fd.status_changes.data(),
+                        sizeof(int64_t) * fd.status_changes.size());
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Adjoint Jacobian of `runs` runs (one variant per run at x0). Same layout as the FD one,
+// status [runs][rays].
+int mko_ref_adjoint_jacobian(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const double* x0, int runs, double* J,
+                             double* r0, uint8_t* status, int threads) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::SystemDescription d = description_of(b, *vars, x0);
+        const mko::VariableSet set(d, b.topology());
+        mko::AdjointJacobianOptions opt;
+        opt.quadrature = settings_of(*plan);
+        opt.threads = threads;
+        const auto P = static_cast<std::size_t>(vars->count);
+        const mko::AdjointJacobian aj = mko::adjoint_jacobian_cpu(
+            set, b, std::span<const double>(x0, P * static_cast<std::size_t>(runs)), opt);
+        std::memcpy(J, aj.jacobian.data(), sizeof(double) * aj.jacobian.size());
+        std::memcpy(r0, aj.residuals.data(), sizeof(double) * aj.residuals.size());
+        if (status != nullptr) {
+            std::memcpy(status, aj.status.data(), aj.status.size());
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int mko_ref_normal_equations(const double* J, const double* r, int P, int64_t R, double* A,
+                             double* g) {
+    try {
+        const auto n = static_cast<std::size_t>(P);
+        const auto rows = static_cast<std::size_t>(R);
+        mko::normal_equations_host(std::span<const double>(J, n * rows),
+                                   std::span<const double>(r, rows), P,
+                                   std::span<double>(A, n * n), std::span<double>(g, n));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Batched LM on the CPU (optimize_lm_cpu) for `runs` runs. method 0 = FD, 1 = adjoint.
+// Outputs per run: x [runs][P], merit, status (LmStatus value), iterations, accepted and the
+// merit history [runs][max_iterations + 1] padded with NaN (first penalty round only).
+int mko_ref_optimize_lm(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const double* x0, int runs, int max_iterations,
+                        int method, int penalty_rounds, int threads, double* x_out,
+                        double* merit_out, int32_t* status_out, int32_t* iterations_out,
+                        int32_t* accepted_out, double* history_out) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::SystemDescription d = description_of(b, *vars, x0);
+        const mko::VariableSet set(d, b.topology());
+        mko::LmOptions opt;
+        opt.max_iterations = max_iterations;
+        opt.jacobian.quadrature = settings_of(*plan);
+        opt.jacobian_method = method == 1 ? mko::JacobianMethod::Adjoint
+                                          : mko::JacobianMethod::FiniteDifferences;
+        opt.threads = threads;
+        opt.jacobian.extra_threads = threads;
+        if (penalty_rounds <= 1) {
+            opt.fail_weight_factor = 1.0; // one pass, no outer penalty rounds
+        }
+        const auto P = static_cast<std::size_t>(vars->count);
+        const mko::LmResult res = mko::optimize_lm_cpu(
+            set, b, std::span<const double>(x0, P * static_cast<std::size_t>(runs)), opt);
+        const auto H = static_cast<std::size_t>(max_iterations) + 1;
+        for (int i = 0; i < runs; ++i) {
+            const mko::LmRunResult& r = res.runs[static_cast<std::size_t>(i)];
+            std::memcpy(x_out + i * P, r.x.data(), sizeof(double) * P);
+            merit_out[i] = r.merit;
+            status_out[i] = static_cast<int32_t>(r.status);
+            iterations_out[i] = r.iterations;
+            accepted_out[i] = r.accepted;
+            if (history_out != nullptr) {
+                for (std::size_t h = 0; h < H; ++h) {
+                    history_out[i * H + h] = h < r.history.size()
+                                                 ? r.history[h]
+                                                 : std::numeric_limits<double>::quiet_NaN();
+                }
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+} // extern "C"
