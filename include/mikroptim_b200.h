@@ -156,6 +156,9 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);
 const char* mkb_version(void);
+/* Reads and clears the device-side error words (synchronising): MKB_OK, or MKB_ERR_TIMEOUT
+ * when a bounded wait inside a kernel gave up since the last call. */
+int mkb_device_status(void);
 /* Number of kernel launches this library has enqueued in the calling process. */
 int64_t mkb_launch_count(void);
 

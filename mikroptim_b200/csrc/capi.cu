@@ -1,0 +1,368 @@
+// C ABI entry points (include/mikroptim_b200.h): argument checks, parameter blocks, pack
+// plans, error reporting. Every check runs on the host before anything is enqueued.
+#include "common.cuh"
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+namespace mkb {
+
+int launch_residuals(const TraceParams& p, const double* records, double* residuals,
+                     int64_t stride, double* opd, uint8_t* status, cudaStream_t stream);
+int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
+                 int64_t* hard, void* workspace, size_t ws_bytes, cudaStream_t stream);
+size_t merit_workspace_bytes(int V, int n_tuples);
+int pack_rays_default();
+int trace_device_error();
+
+namespace {
+thread_local std::string g_error;
+std::atomic<int64_t> g_launches{0};
+}  // namespace
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void set_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+
+int cuda_status(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return MKB_OK;
+    set_error("%s: %s", what, cudaGetErrorString(err));
+    return MKB_ERR_CUDA;
+}
+
+namespace {
+
+int sample_count(const mkb_residual_plan* plan, int f) {
+    return plan->pupil_mode[f] == MKB_PUPIL_AXIS ? plan->rings : plan->rings * plan->spokes;
+}
+
+// tuple_weight, residual_scale, penalty_scale (reference merit/ray_residual.hpp:98,127,186):
+// same operations and order as the CPU reference, so the factors are bit-identical.
+double tuple_weight(const mkb_residual_plan* p, int f, int l) {
+    const double wf = p->field_weight[f];
+    const double wl = p->wavelength_weight[l];
+    if (!(wf > 0.0) || !(wl > 0.0)) return 0.0;
+    double sum_f = 0.0, sum_l = 0.0;
+    for (int i = 0; i < p->fields; ++i) sum_f += p->field_weight[i];
+    for (int i = 0; i < p->wavelengths; ++i) sum_l += p->wavelength_weight[i];
+    return (wf / sum_f) * (wl / sum_l);
+}
+
+int check_plan(const mkb_residual_plan* plan) {
+    if (plan == nullptr) {
+        set_error("residual plan is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (plan->rings < 1 || plan->rings > kMaxRings) {
+        set_error("rings must be in [1, %d], got %d", kMaxRings, plan->rings);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (plan->spokes < 1 || plan->spokes > kMaxSpokes) {
+        set_error("spokes must be in [1, %d], got %d", kMaxSpokes, plan->spokes);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (plan->fields < 1 || plan->fields > kMaxFields || plan->wavelengths < 1 ||
+        plan->wavelengths > MKB_MAX_WAVELENGTHS ||
+        plan->fields * plan->wavelengths > kMaxTuples) {
+        set_error("fields (%d) or wavelengths (%d) out of range", plan->fields,
+                  plan->wavelengths);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (plan->failure != MKB_FAILURE_SOFT && plan->failure != MKB_FAILURE_HARD) {
+        set_error("unknown failure mode %d", plan->failure);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (!(plan->fail_weight >= 0.0) || !std::isfinite(plan->fail_weight)) {
+        set_error("fail_weight must be finite and >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (!(plan->reference_wavelength_nm > 0.0) || !std::isfinite(plan->reference_wavelength_nm)) {
+        set_error("reference wavelength must be > 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (!plan->pupil_mode || !plan->field_weight || !plan->wavelength_weight || !plan->quad_u ||
+        !plan->quad_w) {
+        set_error("residual plan has a null array");
+        return MKB_ERR_ARGUMENT;
+    }
+    for (int f = 0; f < plan->fields; ++f) {
+        const int m = plan->pupil_mode[f];
+        if (m != MKB_PUPIL_HALF && m != MKB_PUPIL_FULL && m != MKB_PUPIL_AXIS) {
+            set_error("unknown pupil mode %d of field %d", m, f);
+            return MKB_ERR_ARGUMENT;
+        }
+        if (!(plan->field_weight[f] >= 0.0)) {
+            set_error("field weight %d must be >= 0", f);
+            return MKB_ERR_ARGUMENT;
+        }
+    }
+    for (int l = 0; l < plan->wavelengths; ++l)
+        if (!(plan->wavelength_weight[l] >= 0.0)) {
+            set_error("wavelength weight %d must be >= 0", l);
+            return MKB_ERR_ARGUMENT;
+        }
+    return MKB_OK;
+}
+
+}  // namespace
+
+int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                      int pack_rays, TraceParams* out) {
+    if (batch == nullptr) {
+        set_error("batch is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    int rc = check_plan(plan);
+    if (rc != MKB_OK) return rc;
+    const int S = batch->surfaces, L = batch->wavelengths, F = batch->fields;
+    if (S < 2 || S > kMaxSurfaces) {
+        set_error("surfaces must be in [2, %d], got %d", kMaxSurfaces, S);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (L != plan->wavelengths || F != plan->fields) {
+        set_error("plan (F=%d, L=%d) does not match the batch (F=%d, L=%d)", plan->fields,
+                  plan->wavelengths, F, L);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (batch->variants < 0) {
+        set_error("variants must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    const RecordLayout lay = record_layout(S, L, F);
+    if (batch->record_stride != lay.stride) {
+        set_error("record_stride %d does not match the shape (expected %d)",
+                  batch->record_stride, lay.stride);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (batch->variants > 0 && (batch->records == nullptr ||
+                                (reinterpret_cast<uintptr_t>(batch->records) & 15u) != 0)) {
+        set_error("records must be a 16-byte aligned device pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (batch->type == nullptr) {
+        set_error("type array is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (batch->type[0] != MKB_SURFACE_STOP) {
+        set_error("surface 0 must be the stop");
+        return MKB_ERR_ARGUMENT;
+    }
+    for (int s = 1; s < S; ++s) {
+        const int t = batch->type[s];
+        if (t == MKB_SURFACE_GHOST_PLATE) {
+            set_error("surface %d is a ghost plate; this build traces stop, plane and sphere",
+                      s);
+            return MKB_ERR_UNSUPPORTED;
+        }
+        if (t != MKB_SURFACE_PLANE && t != MKB_SURFACE_SPHERE) {
+            set_error("surface %d has unknown kind %d", s, t);
+            return MKB_ERR_ARGUMENT;
+        }
+    }
+    TraceParams& p = *out;
+    std::memset(&p, 0, sizeof(p));
+    p.V = batch->variants;
+    p.S = S;
+    p.L = L;
+    p.F = F;
+    p.stride = lay.stride;
+    p.failure = plan->failure;
+    p.rings = plan->rings;
+    p.spokes = plan->spokes;
+    for (int s = 0; s < S; ++s) p.type[s] = batch->type[s];
+    int offset = 0;
+    for (int f = 0; f < F; ++f) {
+        p.pupil_mode[f] = plan->pupil_mode[f];
+        p.sample_count[f] = sample_count(plan, f);
+        p.field_offset[f] = offset;
+        offset += L * p.sample_count[f];
+    }
+    p.rays = offset;
+    // pupil tables (pupil/quadrature.hpp:71): rho = sqrt(u), weight = W / M, phi per mode
+    const double pi = 3.14159265358979323846264338327950288;
+    for (int i = 0; i < plan->rings; ++i) {
+        p.rho[i] = std::sqrt(plan->quad_u[i]);
+        p.w_axis[i] = plan->quad_w[i] / 1.0;
+        p.rw_axis[i] = std::sqrt(p.w_axis[i]);
+        p.w_spoke[i] = plan->quad_w[i] / static_cast<double>(plan->spokes);
+        p.rw_spoke[i] = std::sqrt(p.w_spoke[i]);
+    }
+    for (int j = 0; j < plan->spokes; ++j) {
+        const double half = static_cast<double>(2 * j + 1) * pi / static_cast<double>(2 * plan->spokes);
+        const double full = static_cast<double>(2 * j + 1) * pi / static_cast<double>(plan->spokes);
+        p.sin_half[j] = std::sin(half);
+        p.cos_half[j] = std::cos(half);
+        p.sin_full[j] = std::sin(full);
+        p.cos_full[j] = std::cos(full);
+    }
+    p.n_tuples = F * L;
+    const double lambda_ref_mm = plan->reference_wavelength_nm * 1e-6;
+    for (int f = 0; f < F; ++f)
+        for (int l = 0; l < L; ++l) {
+            const double w = tuple_weight(plan, f, l);
+            p.scale[f * L + l] = w > 0.0 ? std::sqrt(w) / lambda_ref_mm : 0.0;
+            p.pscale[f * L + l] = w > 0.0 ? std::sqrt(plan->fail_weight * w) : 0.0;
+        }
+    // pack plan: consecutive tuples until pack_rays rays or kMaxPackTuples tuples
+    int packs = 0;
+    int t = 0;
+    while (t < p.n_tuples) {
+        const int n0 = p.sample_count[t / L];
+        if (packs >= kMaxPacks) {
+            set_error("too many packs (%d tuples)", p.n_tuples);
+            return MKB_ERR_ARGUMENT;
+        }
+        Pack& pk = p.packs[packs];
+        pk.first_tuple = static_cast<int16_t>(t);
+        pk.first_ray = p.field_offset[t / L] + (t % L) * n0;
+        int rays = 0, tuples = 0;
+        while (t < p.n_tuples && tuples < kMaxPackTuples) {
+            const int n = p.sample_count[t / L];
+            if (tuples > 0 && rays + n > pack_rays) break;
+            if (n > pack_rays) {
+                set_error("a tuple has %d rays; at most %d per block", n, pack_rays);
+                return MKB_ERR_UNSUPPORTED;
+            }
+            rays += n;
+            ++tuples;
+            ++t;
+        }
+        pk.tuples = static_cast<int16_t>(tuples);
+        pk.rays = rays;
+        ++packs;
+    }
+    p.n_packs = packs;
+    return MKB_OK;
+}
+
+}  // namespace mkb
+
+using namespace mkb;
+
+extern "C" {
+
+const char* mkb_last_error(void) { return g_error.c_str(); }
+const char* mkb_version(void) { return "mikroptim_b200 0.1 (sm_100a)"; }
+int64_t mkb_launch_count(void) { return g_launches.load(); }
+
+int mkb_device_status(void) {
+    int (*readers[])() = {trace_device_error};
+    int status = MKB_OK;
+    for (auto read : readers) {
+        const int v = read();
+        if (v != MKB_OK && status == MKB_OK) status = v;
+    }
+    if (status != MKB_OK) set_error("a bounded device-side wait gave up (status %d)", status);
+    return status;
+}
+
+int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields) {
+    return record_layout(surfaces, wavelengths, fields).stride;
+}
+
+int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
+    if (v == nullptr || records == nullptr) {
+        set_error("pack: null argument");
+        return MKB_ERR_ARGUMENT;
+    }
+    const int S = v->surfaces, L = v->wavelengths, F = v->fields;
+    if (S < 2 || S > kMaxSurfaces || L < 1 || L > MKB_MAX_WAVELENGTHS || F < 1 ||
+        F > kMaxFields || v->variants < 0) {
+        set_error("pack: shape out of range (S=%d, L=%d, F=%d)", S, L, F);
+        return MKB_ERR_ARGUMENT;
+    }
+    const RecordLayout lay = record_layout(S, L, F);
+    for (int64_t i = 0; i < v->variants; ++i) {
+        double* r = records + i * lay.stride;
+        std::memset(r, 0, sizeof(double) * lay.stride);
+        for (int s = 0; s < S; ++s) {
+            r[lay.curvature + s] = v->curvature[i * S + s];
+            r[lay.thickness + s] = v->thickness[i * S + s];
+            for (int l = 0; l < L; ++l)
+                r[lay.index + s * L + l] = v->index[(i * S + s) * L + l];
+        }
+        r[lay.pupil] = v->pupil_radius[i];
+        for (int f = 0; f < F; ++f) {
+            const double th = v->field_angle[i * F + f];
+            r[lay.sin_theta + f] = std::sin(th);
+            r[lay.cos_theta + f] = std::cos(th);
+            r[lay.target + f] = v->field_target[i * F + f];
+        }
+    }
+    return MKB_OK;
+}
+
+int64_t mkb_rays_per_variant(const mkb_residual_plan* plan) {
+    if (check_plan(plan) != MKB_OK) return MKB_ERR_ARGUMENT;
+    int64_t n = 0;
+    for (int f = 0; f < plan->fields; ++f) n += static_cast<int64_t>(plan->wavelengths) * sample_count(plan, f);
+    return n;
+}
+
+int64_t mkb_trace_rows(const mkb_residual_plan* plan) {
+    const int64_t r = mkb_rays_per_variant(plan);
+    if (r < 0) return r;
+    return plan->failure == MKB_FAILURE_SOFT ? 2 * r : r;
+}
+
+int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                         double* residuals, int64_t stride, double* opd, uint8_t* status,
+                         void* stream) {
+    TraceParams p;
+    int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64) {
+        set_error("residuals: precision %d not available for RESIDUALS", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * static_cast<int64_t>(p.rays) : p.rays;
+    if (stride < rows) {
+        set_error("residuals: stride %lld < trace rows %lld", static_cast<long long>(stride),
+                  static_cast<long long>(rows));
+        return MKB_ERR_ARGUMENT;
+    }
+    if (p.V == 0) return MKB_OK;
+    if (residuals == nullptr) {
+        set_error("residuals: output is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    return launch_residuals(p, batch->records, residuals, stride, opd, status,
+                            static_cast<cudaStream_t>(stream));
+}
+
+size_t mkb_merit_workspace_bytes(int32_t variants, const mkb_residual_plan* plan) {
+    if (check_plan(plan) != MKB_OK || variants < 0) return 0;
+    return merit_workspace_bytes(variants, plan->fields * plan->wavelengths);
+}
+
+int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* plan, double* merit,
+                     int64_t* failed, int64_t* hard_failed, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+    TraceParams p;
+    int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64) {
+        set_error("merit: precision %d not built yet", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    if (p.V == 0) return MKB_OK;
+    if (!merit || !failed || !hard_failed) {
+        set_error("merit: output is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    return launch_merit(p, batch->records, merit, failed, hard_failed, workspace,
+                        workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,284 @@
+// Shared device code of the B200 trace kernels: kernel parameter block, record layout, the
+// per-surface ray step in FP64, bulk-copy staging with bounded mbarrier waits, and the
+// host-side helpers shared by the entry points.
+#pragma once
+
+#include "mikroptim_b200.h"
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mkb {
+
+// ---- limits ------------------------------------------------------------------------------
+constexpr int kMaxSurfaces = MKB_MAX_SURFACES;
+constexpr int kMaxRings = MKB_MAX_RINGS;
+constexpr int kMaxSpokes = MKB_MAX_SPOKES;
+constexpr int kMaxFields = MKB_MAX_FIELDS;
+constexpr int kMaxTuples = MKB_MAX_TUPLES;
+constexpr int kMaxPacks = 256;
+constexpr int kMaxPackTuples = 16;
+
+// Trace status and soft-failure branch codes (reference: trace/surface_ops.hpp:24,113).
+enum : int { kOk = 0, kMissed = 1, kTir = 2, kBackward = 3, kUnsupported = 4,
+             kSoftMissed = 5, kSoftTir = 6 };
+enum : int { kBranchRegular = 0, kBranchSoftMissed = 1, kBranchSoftTir = 2 };
+
+__host__ __device__ inline bool is_soft(int s) { return s == kSoftMissed || s == kSoftTir; }
+__host__ __device__ inline bool in_piston(int s) { return s == kOk || is_soft(s); }
+
+// ---- record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
+//      sin theta[F] | cos theta[F] | field_target[F] | pad to even --------------------------
+struct RecordLayout {
+    int curvature, thickness, index, pupil, sin_theta, cos_theta, target, stride;
+};
+
+__host__ __device__ inline RecordLayout record_layout(int S, int L, int F) {
+    RecordLayout r;
+    r.curvature = 0;
+    r.thickness = S;
+    r.index = 2 * S;
+    r.pupil = 2 * S + S * L;
+    r.sin_theta = r.pupil + 1;
+    r.cos_theta = r.sin_theta + F;
+    r.target = r.cos_theta + F;
+    const int n = r.target + F;
+    r.stride = (n + 1) & ~1;
+    return r;
+}
+
+// ---- kernel parameter block (passed by value; < 16 KB) -----------------------------------
+struct Pack {
+    int16_t first_tuple;  // first tuple (f * L + l) of the pack
+    int16_t tuples;       // tuples in the pack (<= kMaxPackTuples)
+    int32_t first_ray;    // offset of the pack's first ray in the variant's ray rows
+    int32_t rays;         // rays of the pack (<= rays per CTA)
+};
+
+struct TraceParams {
+    int V, S, L, F;
+    int stride;             // doubles per variant record
+    int failure;            // MKB_FAILURE_*
+    int rays;               // rays per variant
+    int rings, spokes;
+    int n_tuples, n_packs;
+    int sample_count[kMaxFields];   // n_f
+    int field_offset[kMaxFields];   // ray offset of tuple (f, 0)
+    uint8_t pupil_mode[kMaxFields];
+    uint8_t type[kMaxSurfaces];
+    // pupil tables: radial rho_i, weights W_i/M and sqrt, azimuth sin/cos per mode
+    double rho[kMaxRings];
+    double w_axis[kMaxRings], rw_axis[kMaxRings];
+    double w_spoke[kMaxRings], rw_spoke[kMaxRings];
+    double sin_half[kMaxSpokes], cos_half[kMaxSpokes];
+    double sin_full[kMaxSpokes], cos_full[kMaxSpokes];
+    double scale[kMaxTuples];       // residual_scale per tuple
+    double pscale[kMaxTuples];      // penalty_scale per tuple
+    Pack packs[kMaxPacks];
+};
+
+// ---- error word written by bounded waits that gave up -------------------------------------
+// One word per translation unit (no relocatable device code); each .cu file that launches
+// kernels defines a reader with MKB_DEFINE_ERROR_READER and lists it in capi.cu, and
+// mkb_device_status() polls them all.
+static __device__ int g_device_error = 0;
+
+#define MKB_DEFINE_ERROR_READER(name)                                                     \
+    int name() {                                                                           \
+        int value = 0;                                                                     \
+        if (cudaMemcpyFromSymbol(&value, g_device_error, sizeof(int)) != cudaSuccess)      \
+            return MKB_ERR_CUDA;                                                           \
+        if (value != 0) {                                                                  \
+            const int zero = 0;                                                            \
+            cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int));                        \
+        }                                                                                  \
+        return value;                                                                      \
+    }
+
+// ---- bulk copy into shared memory with an mbarrier (no multicast) ------------------------
+__device__ inline uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ inline void mbar_init(uint64_t* bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ inline void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Waits for phase `parity` of the barrier; gives up after `limit` polls. Returns true when
+// the phase completed.
+__device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Stages `bytes` (multiple of 16, both addresses 16-byte aligned) from global into shared
+// memory with one bulk copy issued by thread 0. Every thread of the block calls it. On a
+// timed-out wait the block records MKB_ERR_TIMEOUT, waits once more (bounded) for the copy
+// still in flight, and the function returns false: the caller must return without touching
+// the staged data.
+__device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t bytes,
+                                       uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, bytes);
+        bulk_copy_g2s(dst, src, bytes, bar);
+    }
+    constexpr uint32_t kPolls = 1u << 24;
+    bool ok = mbar_wait(bar, 0, kPolls);
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_TIMEOUT);
+        mbar_wait(bar, 0, kPolls);
+        __syncthreads();
+    }
+    return ok;
+}
+
+// ---- FP64 ray state and surface step ------------------------------------------------------
+// Formulas and order of operations: transfer_to_tangent_plane, intersect_sphere and
+// refract_sphere (reference trace/surface_ops.hpp:122,144,181), propagate_surface_local
+// (trace/trace.hpp:174), reference_sphere_step (trace/reference_sphere.hpp:55).
+struct Ray64 {
+    double px, py, pz, dx, dy, dz, opl;
+};
+
+struct Soft64 {
+    double penalty;
+    int first;
+    __device__ void add(double amount, int kind) {
+        penalty += amount;
+        if (first == kOk) first = kind;
+    }
+};
+
+// One surface step (stop/plane: c = 0). Returns the status; `branch` gets the taken
+// soft-failure continuation. With soft == nullptr the hard-failure rules apply.
+__device__ __forceinline__ int step_surface64(Ray64& r, double t, double c, double n_before,
+                                              double n_after, Soft64* soft, int& branch) {
+    if (!(r.dz > 0.0)) return kBackward;
+    // transfer to the tangent plane
+    r.pz -= t;
+    const double s0 = -r.pz / r.dz;
+    r.px = r.px + s0 * r.dx;
+    r.py = r.py + s0 * r.dy;
+    r.pz = 0.0;
+    // intersection with the sphere (Spencer-Murty form)
+    const double H = c * (r.px * r.px + r.py * r.py);
+    const double B = r.dz - c * (r.px * r.dx + r.py * r.dy);
+    const double D = B * B - c * H;
+    double s;
+    bool missed = false;
+    if (D < 0.0) {
+        if (soft == nullptr || (!(c > 0.0) && !(c < 0.0))) return kMissed;
+        soft->add(-D, kSoftMissed);
+        s = B / c;
+        missed = true;
+    } else {
+        const double denom = B + sqrt(D);
+        if (!(denom > 0.0)) return kMissed;
+        s = H / denom;
+    }
+    r.px = r.px + s * r.dx;
+    r.py = r.py + s * r.dy;
+    r.pz = r.pz + s * r.dz;
+    r.opl += n_before * (s0 + s);
+    // refraction, mu = n / n'
+    const double mu = n_before / n_after;
+    double nx = -c * r.px, ny = -c * r.py, nz = 1.0 - c * r.pz;
+    if (missed) {
+        const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+        nx = inv * nx;
+        ny = inv * ny;
+        nz = inv * nz;
+    }
+    const double cos_i = r.dx * nx + r.dy * ny + r.dz * nz;
+    const double k = 1.0 - mu * mu * (1.0 - cos_i * cos_i);
+    branch = missed ? kBranchSoftMissed : kBranchRegular;
+    if (k < 0.0) {
+        if (soft == nullptr) return kTir;
+        soft->add(-k, kSoftTir);
+        const double tx = r.dx - cos_i * nx, ty = r.dy - cos_i * ny, tz = r.dz - cos_i * nz;
+        const double inv = 1.0 / sqrt(tx * tx + ty * ty + tz * tz);
+        r.dx = inv * tx;
+        r.dy = inv * ty;
+        r.dz = inv * tz;
+        branch |= kBranchSoftTir;
+        return kOk;
+    }
+    const double a = sqrt(k) - mu * cos_i;
+    r.dx = mu * r.dx + a * nx;
+    r.dy = mu * r.dy + a * ny;
+    r.dz = mu * r.dz + a * nz;
+    return kOk;
+}
+
+// Step onto the reference sphere about M = (0, h, w) through the vertex of the last surface.
+__device__ __forceinline__ int reference_step64(Ray64& r, double h, double w, double n_image,
+                                                Soft64* soft, int& branch) {
+    const double qx = r.px, qy = r.py - h, qz = r.pz - w;
+    const double b = -(qx * r.dx + qy * r.dy + qz * r.dz);
+    const double g = r.px * r.px + r.py * (r.py - 2.0 * h) + r.pz * (r.pz - 2.0 * w);
+    const double disc = b * b - g;
+    branch = kBranchRegular;
+    if (disc < 0.0) {
+        const double radius_sq = h * h + w * w;
+        if (soft == nullptr || !(radius_sq > 0.0)) return kMissed;
+        soft->add(-disc / radius_sq, kSoftMissed);
+        r.px = r.px + b * r.dx;
+        r.py = r.py + b * r.dy;
+        r.pz = r.pz + b * r.dz;
+        r.opl += n_image * b;
+        branch = kBranchSoftMissed;
+        return kSoftMissed;
+    }
+    const double root = sqrt(disc);
+    const bool real_image = w >= 0.0;
+    const double denom = real_image ? b + root : b - root;
+    if (!(real_image ? denom > 0.0 : denom < 0.0)) return kMissed;
+    const double s = g / denom;
+    r.px = r.px + s * r.dx;
+    r.py = r.py + s * r.dy;
+    r.pz = r.pz + s * r.dz;
+    r.opl += n_image * s;
+    return kOk;
+}
+
+// ---- launch bookkeeping (host) -------------------------------------------------------------
+void count_launch(int n = 1);
+void set_error(const char* fmt, ...);
+int cuda_status(cudaError_t err, const char* what);
+
+// Builds the parameter block from the batch and plan; returns MKB_OK or MKB_ERR_ARGUMENT.
+// `pack_rays` = rays one CTA traces (tuples are packed until this many rays).
+int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                      int pack_rays, TraceParams* out);
+
+}  // namespace mkb

@@ -1,0 +1,340 @@
+// RESIDUALS and MERIT forward trace for sm_100a.
+//
+// Work decomposition: one CTA per (variant, pack). A pack is a run of consecutive tuples
+// (field f, wavelength l) of one variant with at most kPackRays rays in total, fixed for the
+// whole batch (the topology fixes the layout). The CTA stages its variant's record (surface
+// table, indices, pupil radius, field data) into shared memory with one bulk copy, traces its
+// rays (thread t takes pack rays t, t + T, ...), keeps OPL / status / penalty in shared
+// memory, and then one warp per tuple reduces the piston and writes the residual rows
+// (RESIDUALS) or the tuple's sum of squares (MERIT) in a fixed order: lane-strided partial
+// sums in ascending sample order, then a fixed xor-shuffle tree. Results are bit-identical
+// across runs, batch positions and tranches.
+//
+// Reference behaviour restated: residuals_kernel / merit_kernel + merit_finalize_kernel
+// (src/cuda/residuals.cu:57, src/cuda/merit.cu:62,206), batch_ray_opl (merit/ray_residual.hpp:69),
+// opd_statistics (merit/opd.hpp:37), ray_residual / ray_penalty (merit/ray_residual.hpp:131,199).
+#include "common.cuh"
+
+#include <cstdio>
+
+namespace mkb {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kRaysPerThread = 4;
+constexpr int kPackRays = kThreads * kRaysPerThread;
+
+// Shared pupil tables copied from the parameter block once per CTA.
+struct SharedTables {
+    double rho[kMaxRings];
+    double w_axis[kMaxRings], rw_axis[kMaxRings];
+    double w_spoke[kMaxRings], rw_spoke[kMaxRings];
+    double sin_half[kMaxSpokes], cos_half[kMaxSpokes];
+    double sin_full[kMaxSpokes], cos_full[kMaxSpokes];
+};
+
+struct alignas(16) SharedTrace {
+    uint64_t bar;
+    double record[2 * kMaxSurfaces + kMaxSurfaces * MKB_MAX_WAVELENGTHS + 1 + 3 * kMaxFields + 1];
+    SharedTables tab;
+    double opl[kPackRays];
+    double pen[kPackRays];
+    uint8_t status[kPackRays];
+    int tuple_start[kMaxPackTuples + 1];
+};
+
+__device__ inline void copy_tables(const TraceParams& p, SharedTables& t) {
+    for (int i = threadIdx.x; i < kMaxRings; i += blockDim.x) {
+        t.rho[i] = p.rho[i];
+        t.w_axis[i] = p.w_axis[i];
+        t.rw_axis[i] = p.rw_axis[i];
+        t.w_spoke[i] = p.w_spoke[i];
+        t.rw_spoke[i] = p.rw_spoke[i];
+    }
+    for (int i = threadIdx.x; i < kMaxSpokes; i += blockDim.x) {
+        t.sin_half[i] = p.sin_half[i];
+        t.cos_half[i] = p.cos_half[i];
+        t.sin_full[i] = p.sin_full[i];
+        t.cos_full[i] = p.cos_full[i];
+    }
+}
+
+// Sample k of field f: rho, weight and sin/cos of the azimuth (pupil/quadrature.hpp:71).
+struct Sample {
+    double rho, weight, root_weight, sin_phi, cos_phi;
+};
+
+__device__ inline Sample pupil_sample(const TraceParams& p, const SharedTables& t, int f, int k) {
+    Sample s;
+    const int mode = p.pupil_mode[f];
+    if (mode == MKB_PUPIL_AXIS) {
+        s.rho = t.rho[k];
+        s.weight = t.w_axis[k];
+        s.root_weight = t.rw_axis[k];
+        s.sin_phi = 0.0;
+        s.cos_phi = 1.0;
+    } else {
+        const int i = k / p.spokes;
+        const int j = k - i * p.spokes;
+        s.rho = t.rho[i];
+        s.weight = t.w_spoke[i];
+        s.root_weight = t.rw_spoke[i];
+        if (mode == MKB_PUPIL_HALF) {
+            s.sin_phi = t.sin_half[j];
+            s.cos_phi = t.cos_half[j];
+        } else {
+            s.sin_phi = t.sin_full[j];
+            s.cos_phi = t.cos_full[j];
+        }
+    }
+    return s;
+}
+
+// Full FP64 trace of one ray to the reference sphere (trace_to_reference_sphere,
+// reference_sphere.hpp:181): returns the status, opl and the soft penalty.
+__device__ inline int trace_ray64(const TraceParams& p, const double* rec, const RecordLayout& lay,
+                                  int f, int l, const Sample& smp, bool soft_mode, double& opl,
+                                  double& penalty) {
+    const int S = p.S, L = p.L;
+    const double a = rec[lay.pupil];
+    const double st = rec[lay.sin_theta + f];
+    const double ct = rec[lay.cos_theta + f];
+    const double r0 = a * smp.rho;
+    Ray64 r;
+    r.px = r0 * smp.sin_phi;
+    r.py = r0 * smp.cos_phi;
+    r.pz = 0.0;
+    r.dx = 0.0;
+    r.dy = st;
+    r.dz = ct;
+    r.opl = r.py * st;  // p . d with p_z = d_x = 0
+    Soft64 soft{0.0, kOk};
+    Soft64* sp = soft_mode ? &soft : nullptr;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    double n_before = idx[l];
+    for (int s = 1; s < S; ++s) {
+        const double n_after = idx[s * L + l];
+        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        int branch;
+        status = step_surface64(r, thick[s - 1], c, n_before, n_after, sp, branch);
+        if (status != kOk) break;
+        n_before = n_after;
+    }
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > 0.0)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step64(r, rec[lay.target + f], thick[S - 1], n_before, sp,
+                                             branch);
+            if (!in_piston(rst)) status = rst;
+            else if (status == kOk) status = rst;
+        }
+    }
+    opl = r.opl;
+    penalty = soft.penalty;
+    return status;
+}
+
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ inline int warp_sum_int(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct TupleOut {
+    double* residuals;  // RESIDUALS: [V][stride]
+    int64_t stride;
+    double* opd;        // [V][rays] or null
+    uint8_t* status;    // [V][rays] or null
+    double* part;       // MERIT: [V][n_tuples] tuple sums
+    int* part_failed;   // MERIT: [V][n_tuples]
+    int* part_hard;     // MERIT: [V][n_tuples]
+};
+
+template <bool kResiduals>
+__global__ void __launch_bounds__(kThreads)
+trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
+             TupleOut out) {
+    __shared__ SharedTrace sh;
+    const int v = blockIdx.x / p.n_packs;
+    const int pk = blockIdx.x - v * p.n_packs;
+    const Pack pack = p.packs[pk];
+    const RecordLayout lay = record_layout(p.S, p.L, p.F);
+    const double* src = records + static_cast<int64_t>(v) * p.stride;
+    if (threadIdx.x <= pack.tuples) {
+        int start = 0;
+        for (int t = 0; t < static_cast<int>(threadIdx.x); ++t) {
+            const int tu = pack.first_tuple + t;
+            start += p.sample_count[tu / p.L];
+        }
+        sh.tuple_start[threadIdx.x] = start;
+    }
+    copy_tables(p, sh.tab);
+    if (!stage_to_shared(sh.record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
+                         &sh.bar))
+        return;
+    const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
+
+    // ---- phase 1: trace ---------------------------------------------------------------
+    for (int i = threadIdx.x; i < pack.rays; i += kThreads) {
+        int t = 0;
+        while (t + 1 < pack.tuples && i >= sh.tuple_start[t + 1]) ++t;
+        const int tu = pack.first_tuple + t;
+        const int f = tu / p.L;
+        const int l = tu - f * p.L;
+        const int k = i - sh.tuple_start[t];
+        const Sample smp = pupil_sample(p, sh.tab, f, k);
+        double opl, pen;
+        const int st = trace_ray64(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
+        sh.opl[i] = opl;
+        sh.pen[i] = pen;
+        sh.status[i] = static_cast<uint8_t>(st);
+    }
+    __syncthreads();
+
+    // ---- phase 2: one warp per tuple ----------------------------------------------------
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int t = warp; t < pack.tuples; t += kThreads / 32) {
+        const int tu = pack.first_tuple + t;
+        const int f = tu / p.L;
+        const int l = tu - f * p.L;
+        const int n = p.sample_count[f];
+        const int base = sh.tuple_start[t];
+        const int64_t row0 = p.field_offset[f] + static_cast<int64_t>(l) * n;  // in the variant
+        double vw = 0.0, vs = 0.0;
+        int failed = 0, hard = 0;
+        for (int k = lane; k < n; k += 32) {
+            const int st = sh.status[base + k];
+            if (in_piston(st)) {
+                const Sample smp = pupil_sample(p, sh.tab, f, k);
+                vw += smp.weight;
+                vs += smp.weight * sh.opl[base + k];
+            }
+            failed += st != kOk;
+            hard += !in_piston(st);
+        }
+        vw = warp_sum(vw);
+        vs = warp_sum(vs);
+        const bool valid = vw > 0.0;
+        const double piston = valid ? vs / vw : 0.0;
+        const double scale = p.scale[tu];
+        const double pscale = p.pscale[tu];
+        double sq = 0.0, psq = 0.0;
+        for (int k = lane; k < n; k += 32) {
+            const int st = sh.status[base + k];
+            const Sample smp = pupil_sample(p, sh.tab, f, k);
+            const double e = (valid && in_piston(st)) ? sh.opl[base + k] - piston : 0.0;
+            const double r = scale * smp.root_weight * e;
+            sq += r * r;
+            double pr = 0.0;
+            if (soft_mode) {
+                const double fp = st == kOk ? 0.0
+                                  : is_soft(st) ? sh.pen[base + k]
+                                                : sh.pen[base + k] + 1.0;
+                pr = pscale * smp.root_weight * fp;
+                psq += pr * pr;
+            }
+            if (kResiduals) {
+                const int64_t row = static_cast<int64_t>(v) * out.stride + row0 + k;
+                out.residuals[row] = r;
+                if (soft_mode) out.residuals[row + p.rays] = pr;
+                const int64_t ray = static_cast<int64_t>(v) * p.rays + row0 + k;
+                if (out.opd) out.opd[ray] = e;
+                if (out.status) out.status[ray] = static_cast<uint8_t>(st);
+            }
+        }
+        if (!kResiduals) {
+            sq = warp_sum(sq);
+            psq = warp_sum(psq);
+            failed = warp_sum_int(failed);
+            hard = warp_sum_int(hard);
+            if (lane == 0) {
+                const int64_t slot = static_cast<int64_t>(v) * p.n_tuples + tu;
+                double tuple = sq;
+                tuple += psq;
+                out.part[slot] = tuple;
+                out.part_failed[slot] = failed;
+                out.part_hard[slot] = hard;
+            }
+        }
+    }
+}
+
+// merit[v] = sum over tuples in order (f-major, then l); counts likewise.
+__global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
+                                      const int* part_failed, const int* part_hard,
+                                      double* merit, int64_t* failed, int64_t* hard) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    double sum = 0.0;
+    int64_t nf = 0, nh = 0;
+    const int64_t o = static_cast<int64_t>(v) * n_tuples;
+    for (int t = 0; t < n_tuples; ++t) {
+        sum += part[o + t];
+        nf += part_failed[o + t];
+        nh += part_hard[o + t];
+    }
+    merit[v] = sum;
+    failed[v] = nf;
+    hard[v] = nh;
+}
+
+size_t merit_workspace(int V, int n_tuples) {
+    const size_t slots = static_cast<size_t>(V) * n_tuples;
+    return slots * (sizeof(double) + 2 * sizeof(int)) + 256;
+}
+
+}  // namespace
+
+int launch_residuals(const TraceParams& p, const double* records, double* residuals,
+                     int64_t stride, double* opd, uint8_t* status, cudaStream_t stream) {
+    TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr};
+    const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
+    trace_kernel<true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "residuals kernel launch");
+}
+
+int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
+                 int64_t* hard, void* workspace, size_t ws_bytes, cudaStream_t stream) {
+    const size_t need = merit_workspace(p.V, p.n_tuples);
+    if (workspace == nullptr || ws_bytes < need) {
+        set_error("merit: workspace of %zu bytes needed, %zu given", need, ws_bytes);
+        return MKB_ERR_WORKSPACE;
+    }
+    const size_t slots = static_cast<size_t>(p.V) * p.n_tuples;
+    char* ws = static_cast<char*>(workspace);
+    TupleOut out{nullptr, 0, nullptr, nullptr, reinterpret_cast<double*>(ws),
+                 reinterpret_cast<int*>(ws + slots * sizeof(double)),
+                 reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int)))};
+    const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
+    trace_kernel<false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    count_launch();
+    int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
+    if (rc != MKB_OK) return rc;
+    merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(
+        p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "merit finalize launch");
+}
+
+size_t merit_workspace_bytes(int V, int n_tuples) { return merit_workspace(V, n_tuples); }
+
+int pack_rays_default() { return kPackRays; }
+
+MKB_DEFINE_ERROR_READER(trace_device_error)
+
+}  // namespace mkb

@@ -1,0 +1,150 @@
+"""CPU tests: the oracle is pinned to the reference before anything is checked against it.
+
+* the host quadrature equals the reference's generated Gauss-Legendre table bit for bit;
+* the C restatement (liboracle.so) reproduces the golden fixtures, which were produced by the
+  reference's own CPU code (tests/golden/make_golden.py), bit for bit;
+* where the reference build is present, restatement and reference agree bit for bit on more
+  variants, including every soft- and hard-failure branch;
+* the adjoint Jacobian of the oracle agrees with its central finite differences.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import has_reference_build
+from mikroptim_b200 import workloads
+from mikroptim_b200.batch import (ResidualLayout, STATUS_BACKWARD, STATUS_MISSED,
+                                  STATUS_SOFT_MISSED, STATUS_SOFT_TIR)
+from mikroptim_b200.quadrature import gauss_legendre_unit
+import oracle.pyoracle as po
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, name)))
+
+
+def test_gauss_legendre_table_matches_reference():
+    table = json.load(open(os.path.join(GOLDEN, "gauss_legendre.json")))["orders"]
+    for n in range(1, 17):
+        u, w = gauss_legendre_unit(n)
+        assert list(u) == [float(x) for x in table[str(n)]["u"]], n
+        assert list(w) == [float(x) for x in table[str(n)]["w"]], n
+
+
+@pytest.mark.parametrize("n", [17, 24, 32])
+def test_gauss_legendre_beyond_reference_is_exact_on_polynomials(n):
+    u, w = gauss_legendre_unit(n)
+    u, w = np.array(u), np.array(w)
+    assert abs(w.sum() - 1) < 1e-15
+    for k in range(2 * n):  # exact for degree <= 2n - 1
+        assert abs((w * u ** k).sum() - 1.0 / (k + 1)) < 1e-14
+
+
+def test_generator_reproduces_golden_inputs():
+    g = load("singlet.npz")
+    b, st, vs, x0 = workloads.singlet(1024)
+    b = b.subset(0, 8)
+    for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                 "field_target"):
+        assert np.array_equal(getattr(b, name), g[name]), name
+    assert np.array_equal(x0[:8], g["x0"])
+    g = load("objective.npz")
+    b, st, vs, x0 = workloads.objective(4096, rings=3, spokes=6)
+    assert np.array_equal(b.subset(0, 2).curvature, g["curvature"])
+    assert np.array_equal(b.subset(0, 2).thickness, g["thickness"])
+    assert np.array_equal(b.subset(0, 2).index, g["index"])
+
+
+def test_port_matches_golden_singlet_bitwise():
+    g = load("singlet.npz")
+    b, st, vs, x0 = workloads.singlet(1024)
+    b = b.subset(0, 8)
+    lay = ResidualLayout(b.topology, st)
+    P = po.port()
+    res, opd, status = P.residuals(b, lay)
+    assert np.array_equal(res, g["residuals"])
+    assert np.array_equal(opd, g["opd"])
+    assert np.array_equal(status, g["status"])
+    merit, failed, hard = P.merit(b, lay, threads=2)
+    assert np.array_equal(merit, g["merit"])
+    assert np.array_equal(failed, g["failed"]) and np.array_equal(hard, g["hard_failed"])
+    J, r0, ch = P.fd_jacobian(b.subset(0, 2), lay, vs, x0[:2])
+    assert np.array_equal(J, g["fd_jacobian"]) and np.array_equal(r0, g["fd_r0"])
+    assert np.array_equal(ch, g["fd_changes"])
+    J, r0, _ = P.adjoint_jacobian(b.subset(0, 2), lay, vs, x0[:2])
+    assert np.array_equal(J, g["adjoint_jacobian"]) and np.array_equal(r0, g["adjoint_r0"])
+
+
+def test_port_matches_golden_objective_bitwise():
+    g = load("objective.npz")
+    b, st, vs, x0 = workloads.objective(4096, rings=3, spokes=6)
+    b = b.subset(0, 2)
+    lay = ResidualLayout(b.topology, st)
+    P = po.port()
+    res, opd, status = P.residuals(b, lay)
+    assert np.array_equal(res, g["residuals"]) and np.array_equal(status, g["status"])
+    merit, failed, hard = P.merit(b, lay)
+    assert np.array_equal(merit, g["merit"])
+    one = b.subset(0, 1)
+    J, r0, _ = P.adjoint_jacobian(one, lay, vs, x0[:1])
+    assert np.array_equal(J, g["adjoint_jacobian"]) and np.array_equal(r0, g["adjoint_r0"])
+    J, r0, ch = P.fd_jacobian(one, lay, vs, x0[:1])
+    assert np.array_equal(J, g["fd_jacobian"]) and np.array_equal(ch, g["fd_changes"])
+
+
+@pytest.mark.skipif(not has_reference_build(), reason="reference build not present")
+def test_port_matches_reference_on_failure_branches():
+    """64 objectives at the full 16 x 32 quadrature hit every soft and hard branch."""
+    b, st, vs, x0 = workloads.objective(64)
+    lay = ResidualLayout(b.topology, st)
+    rp = po.port().residuals(b, lay, threads=8)
+    rr = po.reference().residuals(b, lay, threads=8)
+    for a, c in zip(rp, rr):
+        assert np.array_equal(a, c)
+    counts = np.bincount(rr[2].ravel(), minlength=7)
+    for s in (STATUS_MISSED, STATUS_BACKWARD, STATUS_SOFT_MISSED, STATUS_SOFT_TIR):
+        assert counts[s] > 0, s
+    one = b.subset(3, 1)
+    Jp = po.port().adjoint_jacobian(one, lay, vs, x0[3:4])
+    Jr = po.reference().adjoint_jacobian(one, lay, vs, x0[3:4])
+    assert np.array_equal(Jp[0], Jr[0]) and np.array_equal(Jp[1], Jr[1])
+
+
+@pytest.mark.skipif(not has_reference_build(), reason="reference build not present")
+def test_port_matches_reference_hard_mode():
+    b, st, vs, x0 = workloads.singlet(1024)
+    st.failure = 1  # hard
+    b = b.subset(100, 32)
+    lay = ResidualLayout(b.topology, st)
+    for a, c in zip(po.port().residuals(b, lay), po.reference().residuals(b, lay)):
+        assert np.array_equal(a, c)
+
+
+def test_adjoint_matches_central_differences():
+    """Criterion of the reference (tests/test_adjoint_jacobian.cpp:675): the adjoint and FD
+    Jacobians agree to the FD truncation error on a smooth, failure-free case."""
+    b, st, vs, x0 = workloads.singlet(16)
+    lay = ResidualLayout(b.topology, st)
+    P = po.port()
+    Ja, r0a, _ = P.adjoint_jacobian(b.subset(0, 4), lay, vs, x0[:4])
+    Jf, r0f, _ = P.fd_jacobian(b.subset(0, 4), lay, vs, x0[:4])
+    assert np.array_equal(r0a, r0f)
+    scale = np.abs(Jf).max(axis=2, keepdims=True)
+    assert np.max(np.abs(Ja - Jf) / scale) < 1e-6
+
+
+def test_normal_equations_fma_chain():
+    rng = np.random.default_rng(5)
+    J = rng.standard_normal((6, 40))
+    r = rng.standard_normal(40)
+    A, g = po.port().normal_equations(J, r)
+    assert np.allclose(A, J @ J.T, rtol=1e-14, atol=1e-13)
+    assert np.allclose(g, J @ r, rtol=1e-14, atol=1e-13)
+    if has_reference_build():
+        Ar, gr = po.reference().normal_equations(J, r)
+        assert np.array_equal(A, Ar) and np.array_equal(g, gr)
