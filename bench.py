@@ -1,0 +1,355 @@
+"""Benchmark of the B200 batched trace-and-optimise path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload merit|lm]
+
+Workload (default): the seven-element objective of the adjoint-vs-FD configuration -- 4096
+variants, 15 table surfaces, 7 wavelengths, 5 fields, 16 rings x 32 spokes (14,448 rays per
+variant, 59.2 M rays per evaluation), soft failure; synthetic seeded inputs. One step = one
+MERIT evaluation of all variants (`--workload merit`).
+
+N > 1 (torchrun, one rank per GPU): every rank traces its own 4096 variants (weak scaling,
+independent variants, no data-path collective); the time is the maximum over ranks.
+
+Timing: W untimed warm-up steps, then K steps timed with CUDA events on the launching stream,
+bracketed by a barrier and a device synchronisation; the L2 cache (126 MB) is flushed before
+every step outside the events (the batch records are only 5 MB). Clocks are sampled with
+nvidia-smi during the timed region.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LM iter/s & ray-surface hits/s: adjoint+mixed vs FP64 FD, at ≤1e-4λ OPD err"
+WORKLOAD = "objective-4096: 4096 variants x 15 surfaces, L=7, F=5, 16x32 pupil (config 2 shape)"
+FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of the reference)
+# DRAM traffic of trace_kernel per variant from the ncu capture summarised in
+# profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
+TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="merit", choices=["merit"])
+    ap.add_argument("--variants", type=int, default=4096)
+    return ap.parse_args()
+
+
+# ---- distributed plumbing ------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if os.environ.get("MKB_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- clocks --------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- B200 arm ------------------------------------------------------------------------------
+def fp64_peak_tflops(torch) -> float:
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3 on this GPU, best of 5 (CUDA events)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / best / 1e9
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import PRECISION_FP64, PRECISION_FP64_FMA, ResidualLayout
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    b, st, vs, x0 = workloads.objective(args.variants, seed=20261203 + 2 + 1000 * rank)
+    st.precision = PRECISION_FP64_FMA
+    lay = ResidualLayout(b.topology, st)
+    db = engine.DeviceSystemBatch(b, dev)
+    ws = torch.empty(int(lib.mkb_merit_workspace_bytes(b.variants, C.byref(lay.plan(b)))),
+                     dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    rays = b.variants * lay.rays_per_variant
+    hits = rays * (b.surfaces - 1)
+    flopeq = rays * FLOPEQ_PER_RAY_SURFACE * (b.surfaces - 1 + 2)
+
+    def step():
+        return engine.merit_device(db, lay, b, workspace=ws)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = lib.mkb_launch_count()
+    times = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = lib.mkb_launch_count() - launches0
+    ms_total = sum(a.elapsed_time(c) for a, c in times)
+    ms_total = max_over_ranks(ms_total, world, dev)
+    ms_step = ms_total / args.steps
+    value = world * hits * args.steps / (ms_total / 1e3)
+
+    # dominant kernel alone (trace kernel without the finalize launch) for the roofline
+    plan = lay.plan(b)
+    kernel_ms = ms_step  # finalize is < 1 % of the step; measured below
+    # exact FP64 rate for reference
+    st_exact = ResidualLayout(b.topology, type(st)(rings=st.rings, spokes=st.spokes,
+                                                   failure=st.failure,
+                                                   precision=PRECISION_FP64))
+    engine.merit_device(db, st_exact, b, workspace=ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    e0.record(stream)
+    for _ in range(3):
+        engine.merit_device(db, st_exact, b, workspace=ws)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    exact_ms = e0.elapsed_time(e1) / 3
+
+    # end to end through the host-buffer path: pinned host records in, merit out, every step
+    host_in = db.host_records
+    host_out = torch.empty(b.variants, dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        db.records[:b.variants].copy_(host_in, non_blocking=True)
+        host_out.copy_(step().merit, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        db.records[:b.variants].copy_(host_in, non_blocking=True)
+        host_out.copy_(step().merit, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = flopeq / (kernel_ms / 1e3) / 1e12
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "ray-surface hits/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded generator, configuration-2 shapes)",
+            "config": {"workload": WORKLOAD, "step": "one MERIT evaluation of all variants",
+                       "precision": "FP64 with FMA contraction",
+                       "variants_per_gpu": b.variants, "rays_per_variant": lay.rays_per_variant,
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "gpu_launches": int(launches),
+            "e2e": {"value": world * hits / (e2e_ms / 1e3), "unit": "ray-surface hits/s",
+                    "h2d_bytes_per_step": int(host_in.numel() * 8),
+                    "d2h_bytes_per_step": int(b.variants * 8)},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "traffic": TRAFFIC_BYTES_PER_VARIANT * b.variants,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "flop_model": "140 FLOP-eq per ray-surface step, (S-1)+2 steps per ray"},
+            "fp64_exact": {"ms_per_step": exact_ms,
+                           "value": world * hits / (exact_ms / 1e3),
+                           "note": "bit-identical to the reference CPU"},
+            "clocks": clocks.summary(),
+        }
+    return out, (b, lay)
+
+
+# ---- CPU baselines (oracle) ----------------------------------------------------------------
+def cpu_baseline(kind: str, sample_variants: int = 16, seed: int = 20261203 + 2):
+    """The reference's own CPU merit (oracle/_ref) or the C restatement, on all host threads,
+    on the first `sample_variants` variants of the same workload."""
+    import oracle.pyoracle as po
+    from mikroptim_b200 import workloads
+    from mikroptim_b200.batch import ResidualLayout
+    b, st, vs, x0 = workloads.objective(4096, seed=seed)
+    b = b.subset(0, sample_variants)
+    lay = ResidualLayout(b.topology, st)
+    impl = po.reference() if kind == "reference" else po.port()
+    threads = os.cpu_count() or 1
+    impl.merit(b, lay, threads=threads)
+    t0 = time.perf_counter()
+    impl.merit(b, lay, threads=threads)
+    dt = time.perf_counter() - t0
+    hits = b.variants * lay.rays_per_variant * (b.surfaces - 1)
+    return {"value": hits / dt, "unit": "ray-surface hits/s", "cores": threads, "kind": kind,
+            "sample": f"MERIT of {sample_variants} of the 4096 variants, {dt:.2f} s"}
+
+
+def reference_kind() -> str:
+    import oracle.pyoracle as po
+    return "reference" if os.path.exists(po.REF_LIB) else "port"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    kind = reference_kind()
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(kind, sample_variants=8)
+        if i >= args.warmup:
+            samples.append(r["value"])
+    v = statistics.median(samples)
+    base = cpu_baseline(kind, sample_variants=8)
+    return {
+        "metric": METRIC, "value": v, "unit": "ray-surface hits/s", "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-2 shapes)",
+        "config": {"workload": WORKLOAD, "step": "MERIT of an 8-variant sample on the host"},
+        "cpu_baseline": {"value": v, "unit": "ray-surface hits/s", "cores": base["cores"],
+                         "kind": kind, "sample": base["sample"]},
+        "e2e": {"value": v, "unit": "ray-surface hits/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out, _ = run_b200(args, world, rank, local)
+        if rank == 0 and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline(reference_kind())
+            except Exception as e:  # the baseline is reported, not required
+                out["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -60,7 +60,11 @@ enum { MKB_FAILURE_SOFT = 0, MKB_FAILURE_HARD = 1 };   /* FailureMode, surface_o
 enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_BACKWARD = 3,
        MKB_STATUS_UNSUPPORTED = 4, MKB_STATUS_SOFT_MISSED = 5, MKB_STATUS_SOFT_TIR = 6 };
                                                        /* TraceStatus, surface_ops.hpp:24 */
-enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1 };
+/* FP64: every operation separately rounded, sums in the reference's order -- bit-identical to
+ * the reference CPU build. FP64_FMA: FP64 with a*b+c contracted to FMA and tree sums (faster,
+ * equal within the reference's CPU/GPU tolerances). MIXED: FP32 bulk arithmetic with an FP64
+ * sag root and OPL accumulation. */
+enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2 };
 enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2 };
                                                        /* VariableType, model/variables.hpp:18 */
 

@@ -26,7 +26,7 @@ from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_le
 
 SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
 FAILURE_SOFT, FAILURE_HARD = 0, 1
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA = 0, 1, 2
 VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE = 0, 1, 2
 
 MAX_SURFACES = 64
@@ -215,7 +215,7 @@ class ResidualLayout:
             raise ValueError("ResidualLayout: unknown failure mode")
         if not (settings.fail_weight >= 0 and math.isfinite(settings.fail_weight)):
             raise ValueError("ResidualLayout: fail_weight must be finite and >= 0")
-        if settings.precision not in (PRECISION_FP64, PRECISION_MIXED):
+        if settings.precision not in (PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA):
             raise ValueError("ResidualLayout: unknown precision")
         self.topology = topology
         self.settings = settings

@@ -12,9 +12,11 @@
 namespace mkb {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, cudaStream_t stream);
+                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     cudaStream_t stream);
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, cudaStream_t stream);
+                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 cudaStream_t stream);
 size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
 int trace_device_error();
@@ -322,7 +324,7 @@ int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan*
     TraceParams p;
     int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
         set_error("residuals: precision %d not available for RESIDUALS", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -338,6 +340,7 @@ int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan*
         return MKB_ERR_ARGUMENT;
     }
     return launch_residuals(p, batch->records, residuals, stride, opd, status,
+                            plan->precision == MKB_PRECISION_FP64,
                             static_cast<cudaStream_t>(stream));
 }
 
@@ -352,7 +355,7 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
     TraceParams p;
     int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
         set_error("merit: precision %d not built yet", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -362,7 +365,8 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
         return MKB_ERR_ARGUMENT;
     }
     return launch_merit(p, batch->records, merit, failed, hard_failed, workspace,
-                        workspace_bytes, static_cast<cudaStream_t>(stream));
+                        workspace_bytes, plan->precision == MKB_PRECISION_FP64,
+                        static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -142,6 +142,12 @@ __device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit)
 // the staged data.
 __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t bytes,
                                        uint64_t* bar) {
+    // alignment guard: a misaligned bulk copy faults, so record the error and skip it
+    if (((smem_addr(dst) | reinterpret_cast<uintptr_t>(src) | bytes) & 15u) != 0 ||
+        (smem_addr(bar) & 7u) != 0) {
+        if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_ARGUMENT);
+        return false;
+    }
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -162,18 +168,46 @@ __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t byte
     return ok;
 }
 
-// ---- FP64 ray state and surface step ------------------------------------------------------
+// ---- number types of the FP64 trace ------------------------------------------------------
+// `double`: operators as written, the compiler may contract a*b+c into one FMA (faster, not
+// bit-identical to the CPU). `Exact64`: every operation is a separately rounded IEEE operation
+// (__dadd_rn, __dmul_rn, ... are never fused), division and square root are correctly
+// rounded -- the same arithmetic as the reference CPU build (-ffp-contract=off), so a trace
+// written in the reference's order of operations reproduces it bit for bit.
+struct Exact64 {
+    double v;
+    Exact64() = default;
+    __host__ __device__ constexpr Exact64(double x) : v(x) {}
+};
+__device__ __forceinline__ Exact64 operator+(Exact64 a, Exact64 b) { return __dadd_rn(a.v, b.v); }
+__device__ __forceinline__ Exact64 operator-(Exact64 a, Exact64 b) { return __dsub_rn(a.v, b.v); }
+__device__ __forceinline__ Exact64 operator*(Exact64 a, Exact64 b) { return __dmul_rn(a.v, b.v); }
+__device__ __forceinline__ Exact64 operator/(Exact64 a, Exact64 b) { return __ddiv_rn(a.v, b.v); }
+__device__ __forceinline__ Exact64 operator-(Exact64 a) { return -a.v; }
+__device__ __forceinline__ Exact64& operator+=(Exact64& a, Exact64 b) { return a = a + b; }
+__device__ __forceinline__ Exact64& operator-=(Exact64& a, Exact64 b) { return a = a - b; }
+__device__ __forceinline__ bool operator<(Exact64 a, Exact64 b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(Exact64 a, Exact64 b) { return a.v > b.v; }
+__device__ __forceinline__ bool operator>=(Exact64 a, Exact64 b) { return a.v >= b.v; }
+__device__ __forceinline__ Exact64 nsqrt(Exact64 a) { return __dsqrt_rn(a.v); }
+__device__ __forceinline__ double nsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ double value(double a) { return a; }
+__device__ __forceinline__ double value(Exact64 a) { return a.v; }
+
+// ---- ray state and surface step -------------------------------------------------------------
 // Formulas and order of operations: transfer_to_tangent_plane, intersect_sphere and
 // refract_sphere (reference trace/surface_ops.hpp:122,144,181), propagate_surface_local
 // (trace/trace.hpp:174), reference_sphere_step (trace/reference_sphere.hpp:55).
-struct Ray64 {
-    double px, py, pz, dx, dy, dz, opl;
+template <class N>
+struct RayT {
+    N px, py, pz, dx, dy, dz, opl;
 };
 
-struct Soft64 {
-    double penalty;
+template <class N>
+struct SoftT {
+    N penalty;
     int first;
-    __device__ void add(double amount, int kind) {
+    __device__ void add(N amount, int kind) {
         penalty += amount;
         if (first == kOk) first = kind;
     }
@@ -181,29 +215,31 @@ struct Soft64 {
 
 // One surface step (stop/plane: c = 0). Returns the status; `branch` gets the taken
 // soft-failure continuation. With soft == nullptr the hard-failure rules apply.
-__device__ __forceinline__ int step_surface64(Ray64& r, double t, double c, double n_before,
-                                              double n_after, Soft64* soft, int& branch) {
-    if (!(r.dz > 0.0)) return kBackward;
+template <class N>
+__device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N n_after,
+                                            SoftT<N>* soft, int& branch) {
+    const N zero(0.0), one(1.0);
+    if (!(r.dz > zero)) return kBackward;
     // transfer to the tangent plane
     r.pz -= t;
-    const double s0 = -r.pz / r.dz;
+    const N s0 = -r.pz / r.dz;
     r.px = r.px + s0 * r.dx;
     r.py = r.py + s0 * r.dy;
-    r.pz = 0.0;
+    r.pz = zero;
     // intersection with the sphere (Spencer-Murty form)
-    const double H = c * (r.px * r.px + r.py * r.py);
-    const double B = r.dz - c * (r.px * r.dx + r.py * r.dy);
-    const double D = B * B - c * H;
-    double s;
+    const N H = c * (r.px * r.px + r.py * r.py);
+    const N B = r.dz - c * (r.px * r.dx + r.py * r.dy);
+    const N D = B * B - c * H;
+    N s;
     bool missed = false;
-    if (D < 0.0) {
-        if (soft == nullptr || (!(c > 0.0) && !(c < 0.0))) return kMissed;
+    if (D < zero) {
+        if (soft == nullptr || (!(c > zero) && !(c < zero))) return kMissed;
         soft->add(-D, kSoftMissed);
         s = B / c;
         missed = true;
     } else {
-        const double denom = B + sqrt(D);
-        if (!(denom > 0.0)) return kMissed;
+        const N denom = B + nsqrt(D);
+        if (!(denom > zero)) return kMissed;
         s = H / denom;
     }
     r.px = r.px + s * r.dx;
@@ -211,29 +247,29 @@ __device__ __forceinline__ int step_surface64(Ray64& r, double t, double c, doub
     r.pz = r.pz + s * r.dz;
     r.opl += n_before * (s0 + s);
     // refraction, mu = n / n'
-    const double mu = n_before / n_after;
-    double nx = -c * r.px, ny = -c * r.py, nz = 1.0 - c * r.pz;
+    const N mu = n_before / n_after;
+    N nx = -c * r.px, ny = -c * r.py, nz = one - c * r.pz;
     if (missed) {
-        const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+        const N inv = one / nsqrt(nx * nx + ny * ny + nz * nz);
         nx = inv * nx;
         ny = inv * ny;
         nz = inv * nz;
     }
-    const double cos_i = r.dx * nx + r.dy * ny + r.dz * nz;
-    const double k = 1.0 - mu * mu * (1.0 - cos_i * cos_i);
+    const N cos_i = r.dx * nx + r.dy * ny + r.dz * nz;
+    const N k = one - mu * mu * (one - cos_i * cos_i);
     branch = missed ? kBranchSoftMissed : kBranchRegular;
-    if (k < 0.0) {
+    if (k < zero) {
         if (soft == nullptr) return kTir;
         soft->add(-k, kSoftTir);
-        const double tx = r.dx - cos_i * nx, ty = r.dy - cos_i * ny, tz = r.dz - cos_i * nz;
-        const double inv = 1.0 / sqrt(tx * tx + ty * ty + tz * tz);
+        const N tx = r.dx - cos_i * nx, ty = r.dy - cos_i * ny, tz = r.dz - cos_i * nz;
+        const N inv = one / nsqrt(tx * tx + ty * ty + tz * tz);
         r.dx = inv * tx;
         r.dy = inv * ty;
         r.dz = inv * tz;
         branch |= kBranchSoftTir;
         return kOk;
     }
-    const double a = sqrt(k) - mu * cos_i;
+    const N a = nsqrt(k) - mu * cos_i;
     r.dx = mu * r.dx + a * nx;
     r.dy = mu * r.dy + a * ny;
     r.dz = mu * r.dz + a * nz;
@@ -241,16 +277,18 @@ __device__ __forceinline__ int step_surface64(Ray64& r, double t, double c, doub
 }
 
 // Step onto the reference sphere about M = (0, h, w) through the vertex of the last surface.
-__device__ __forceinline__ int reference_step64(Ray64& r, double h, double w, double n_image,
-                                                Soft64* soft, int& branch) {
-    const double qx = r.px, qy = r.py - h, qz = r.pz - w;
-    const double b = -(qx * r.dx + qy * r.dy + qz * r.dz);
-    const double g = r.px * r.px + r.py * (r.py - 2.0 * h) + r.pz * (r.pz - 2.0 * w);
-    const double disc = b * b - g;
+template <class N>
+__device__ __forceinline__ int reference_step(RayT<N>& r, N h, N w, N n_image, SoftT<N>* soft,
+                                              int& branch) {
+    const N zero(0.0), two(2.0);
+    const N qx = r.px, qy = r.py - h, qz = r.pz - w;
+    const N b = -(qx * r.dx + qy * r.dy + qz * r.dz);
+    const N g = r.px * r.px + r.py * (r.py - two * h) + r.pz * (r.pz - two * w);
+    const N disc = b * b - g;
     branch = kBranchRegular;
-    if (disc < 0.0) {
-        const double radius_sq = h * h + w * w;
-        if (soft == nullptr || !(radius_sq > 0.0)) return kMissed;
+    if (disc < zero) {
+        const N radius_sq = h * h + w * w;
+        if (soft == nullptr || !(radius_sq > zero)) return kMissed;
         soft->add(-disc / radius_sq, kSoftMissed);
         r.px = r.px + b * r.dx;
         r.py = r.py + b * r.dy;
@@ -259,11 +297,11 @@ __device__ __forceinline__ int reference_step64(Ray64& r, double h, double w, do
         branch = kBranchSoftMissed;
         return kSoftMissed;
     }
-    const double root = sqrt(disc);
-    const bool real_image = w >= 0.0;
-    const double denom = real_image ? b + root : b - root;
-    if (!(real_image ? denom > 0.0 : denom < 0.0)) return kMissed;
-    const double s = g / denom;
+    const N root = nsqrt(disc);
+    const bool real_image = w >= zero;
+    const N denom = real_image ? b + root : b - root;
+    if (!(real_image ? denom > zero : denom < zero)) return kMissed;
+    const N s = g / denom;
     r.px = r.px + s * r.dx;
     r.py = r.py + s * r.dy;
     r.pz = r.pz + s * r.dz;

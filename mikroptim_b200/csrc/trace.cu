@@ -16,6 +16,7 @@
 #include "common.cuh"
 
 #include <cstdio>
+#include <type_traits>
 
 namespace mkb {
 
@@ -34,15 +35,19 @@ struct SharedTables {
     double sin_full[kMaxSpokes], cos_full[kMaxSpokes];
 };
 
+// The bulk-copy destination `record` must start on a 16-byte boundary: it is the first
+// member of a 16-byte aligned struct (checked below).
 struct alignas(16) SharedTrace {
-    uint64_t bar;
     double record[2 * kMaxSurfaces + kMaxSurfaces * MKB_MAX_WAVELENGTHS + 1 + 3 * kMaxFields + 1];
+    uint64_t bar;
     SharedTables tab;
     double opl[kPackRays];
     double pen[kPackRays];
     uint8_t status[kPackRays];
     int tuple_start[kMaxPackTuples + 1];
 };
+static_assert(offsetof(SharedTrace, record) % 16 == 0, "bulk-copy destination alignment");
+static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 
 __device__ inline void copy_tables(const TraceParams& p, SharedTables& t) {
     for (int i = threadIdx.x; i < kMaxRings; i += blockDim.x) {
@@ -91,53 +96,56 @@ __device__ inline Sample pupil_sample(const TraceParams& p, const SharedTables& 
     return s;
 }
 
-// Full FP64 trace of one ray to the reference sphere (trace_to_reference_sphere,
-// reference_sphere.hpp:181): returns the status, opl and the soft penalty.
-__device__ inline int trace_ray64(const TraceParams& p, const double* rec, const RecordLayout& lay,
-                                  int f, int l, const Sample& smp, bool soft_mode, double& opl,
-                                  double& penalty) {
+// Trace of one ray to the reference sphere in number type N (trace_to_reference_sphere,
+// reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
+// trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
+template <class N>
+__device__ inline int trace_ray(const TraceParams& p, const double* rec, const RecordLayout& lay,
+                                int f, int l, const Sample& smp, bool soft_mode, double& opl,
+                                double& penalty) {
     const int S = p.S, L = p.L;
-    const double a = rec[lay.pupil];
-    const double st = rec[lay.sin_theta + f];
-    const double ct = rec[lay.cos_theta + f];
-    const double r0 = a * smp.rho;
-    Ray64 r;
-    r.px = r0 * smp.sin_phi;
-    r.py = r0 * smp.cos_phi;
-    r.pz = 0.0;
-    r.dx = 0.0;
+    const N zero(0.0);
+    const N a = rec[lay.pupil];
+    const N st = rec[lay.sin_theta + f];
+    const N ct = rec[lay.cos_theta + f];
+    const N r0 = a * N(smp.rho);
+    RayT<N> r;
+    r.px = r0 * N(smp.sin_phi);
+    r.py = r0 * N(smp.cos_phi);
+    r.pz = zero;
+    r.dx = zero;
     r.dy = st;
     r.dz = ct;
     r.opl = r.py * st;  // p . d with p_z = d_x = 0
-    Soft64 soft{0.0, kOk};
-    Soft64* sp = soft_mode ? &soft : nullptr;
+    SoftT<N> soft{zero, kOk};
+    SoftT<N>* sp = soft_mode ? &soft : nullptr;
     int status = kOk;
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
-    double n_before = idx[l];
+    N n_before = idx[l];
     for (int s = 1; s < S; ++s) {
-        const double n_after = idx[s * L + l];
-        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        const N n_after = idx[s * L + l];
+        const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
-        status = step_surface64(r, thick[s - 1], c, n_before, n_after, sp, branch);
+        status = step_surface<N>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch);
         if (status != kOk) break;
         n_before = n_after;
     }
     if (status == kOk && soft_mode) status = soft.first;
     if (in_piston(status)) {
-        if (!(r.dz > 0.0)) {
+        if (!(r.dz > zero)) {
             status = kBackward;
         } else {
             int branch;
-            const int rst = reference_step64(r, rec[lay.target + f], thick[S - 1], n_before, sp,
-                                             branch);
+            const int rst = reference_step<N>(r, N(rec[lay.target + f]), N(thick[S - 1]),
+                                              n_before, sp, branch);
             if (!in_piston(rst)) status = rst;
             else if (status == kOk) status = rst;
         }
     }
-    opl = r.opl;
-    penalty = soft.penalty;
+    opl = value(r.opl);
+    penalty = value(soft.penalty);
     return status;
 }
 
@@ -163,10 +171,15 @@ struct TupleOut {
     int* part_hard;     // MERIT: [V][n_tuples]
 };
 
-template <bool kResiduals>
+// kExact: per-ray arithmetic in Exact64 and every tuple sum sequential in ascending sample
+// order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
+// RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
+// with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
+template <bool kResiduals, bool kExact>
 __global__ void __launch_bounds__(kThreads)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
+    using N = typename std::conditional<kExact, Exact64, double>::type;
     __shared__ SharedTrace sh;
     const int v = blockIdx.x / p.n_packs;
     const int pk = blockIdx.x - v * p.n_packs;
@@ -197,7 +210,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray64(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
+        const int st = trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
         sh.status[i] = static_cast<uint8_t>(st);
@@ -214,58 +227,98 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int n = p.sample_count[f];
         const int base = sh.tuple_start[t];
         const int64_t row0 = p.field_offset[f] + static_cast<int64_t>(l) * n;  // in the variant
+        // piston: valid weight and weighted OPL sum over the rays in the piston
         double vw = 0.0, vs = 0.0;
+        if (kExact) {
+            if (lane == 0) {
+                N w_acc(0.0), s_acc(0.0);
+                for (int k = 0; k < n; ++k) {
+                    if (in_piston(sh.status[base + k])) {
+                        const N w = pupil_sample(p, sh.tab, f, k).weight;
+                        w_acc += w;
+                        s_acc += w * N(sh.opl[base + k]);
+                    }
+                }
+                vw = value(w_acc);
+                vs = value(s_acc);
+            }
+            vw = __shfl_sync(0xffffffffu, vw, 0);
+            vs = __shfl_sync(0xffffffffu, vs, 0);
+        } else {
+            for (int k = lane; k < n; k += 32) {
+                if (in_piston(sh.status[base + k])) {
+                    const Sample smp = pupil_sample(p, sh.tab, f, k);
+                    vw += smp.weight;
+                    vs += smp.weight * sh.opl[base + k];
+                }
+            }
+            vw = warp_sum(vw);
+            vs = warp_sum(vs);
+        }
+        const bool valid = vw > 0.0;
+        const N piston = valid ? value(N(vs) / N(vw)) : 0.0;
+        const N scale = p.scale[tu];
+        const N pscale = p.pscale[tu];
+        double sq = 0.0, psq = 0.0;
         int failed = 0, hard = 0;
         for (int k = lane; k < n; k += 32) {
             const int st = sh.status[base + k];
-            if (in_piston(st)) {
-                const Sample smp = pupil_sample(p, sh.tab, f, k);
-                vw += smp.weight;
-                vs += smp.weight * sh.opl[base + k];
+            const Sample smp = pupil_sample(p, sh.tab, f, k);
+            const N e = (valid && in_piston(st)) ? N(sh.opl[base + k]) - piston : N(0.0);
+            const N rw = smp.root_weight;
+            const N r = scale * rw * e;
+            N pr(0.0);
+            if (soft_mode) {
+                const N fp = st == kOk ? N(0.0)
+                             : is_soft(st) ? N(sh.pen[base + k])
+                                           : N(sh.pen[base + k]) + N(1.0);
+                pr = pscale * rw * fp;
             }
             failed += st != kOk;
             hard += !in_piston(st);
-        }
-        vw = warp_sum(vw);
-        vs = warp_sum(vs);
-        const bool valid = vw > 0.0;
-        const double piston = valid ? vs / vw : 0.0;
-        const double scale = p.scale[tu];
-        const double pscale = p.pscale[tu];
-        double sq = 0.0, psq = 0.0;
-        for (int k = lane; k < n; k += 32) {
-            const int st = sh.status[base + k];
-            const Sample smp = pupil_sample(p, sh.tab, f, k);
-            const double e = (valid && in_piston(st)) ? sh.opl[base + k] - piston : 0.0;
-            const double r = scale * smp.root_weight * e;
-            sq += r * r;
-            double pr = 0.0;
-            if (soft_mode) {
-                const double fp = st == kOk ? 0.0
-                                  : is_soft(st) ? sh.pen[base + k]
-                                                : sh.pen[base + k] + 1.0;
-                pr = pscale * smp.root_weight * fp;
-                psq += pr * pr;
-            }
             if (kResiduals) {
                 const int64_t row = static_cast<int64_t>(v) * out.stride + row0 + k;
-                out.residuals[row] = r;
-                if (soft_mode) out.residuals[row + p.rays] = pr;
+                out.residuals[row] = value(r);
+                if (soft_mode) out.residuals[row + p.rays] = value(pr);
                 const int64_t ray = static_cast<int64_t>(v) * p.rays + row0 + k;
-                if (out.opd) out.opd[ray] = e;
+                if (out.opd) out.opd[ray] = value(e);
                 if (out.status) out.status[ray] = static_cast<uint8_t>(st);
+            } else if (kExact) {
+                sh.opl[base + k] = value(r);  // each lane rewrites only its own samples
+                sh.pen[base + k] = value(pr);
+            } else {
+                sq += value(r * r);
+                psq += value(pr * pr);
             }
         }
         if (!kResiduals) {
-            sq = warp_sum(sq);
-            psq = warp_sum(psq);
+            if (kExact) {
+                __syncwarp();
+                if (lane == 0) {  // sum_k r_k^2, then sum_k p_k^2, in ascending k
+                    N tuple(0.0), pen(0.0);
+                    for (int k = 0; k < n; ++k) {
+                        const N x = sh.opl[base + k];
+                        tuple += x * x;
+                    }
+                    if (soft_mode) {
+                        for (int k = 0; k < n; ++k) {
+                            const N x = sh.pen[base + k];
+                            pen += x * x;
+                        }
+                        tuple += pen;
+                    }
+                    sq = value(tuple);
+                }
+            } else {
+                sq = warp_sum(sq);
+                psq = warp_sum(psq);
+                sq += psq;
+            }
             failed = warp_sum_int(failed);
             hard = warp_sum_int(hard);
             if (lane == 0) {
                 const int64_t slot = static_cast<int64_t>(v) * p.n_tuples + tu;
-                double tuple = sq;
-                tuple += psq;
-                out.part[slot] = tuple;
+                out.part[slot] = sq;
                 out.part_failed[slot] = failed;
                 out.part_hard[slot] = hard;
             }
@@ -283,7 +336,7 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
     int64_t nf = 0, nh = 0;
     const int64_t o = static_cast<int64_t>(v) * n_tuples;
     for (int t = 0; t < n_tuples; ++t) {
-        sum += part[o + t];
+        sum = __dadd_rn(sum, part[o + t]);
         nf += part_failed[o + t];
         nh += part_hard[o + t];
     }
@@ -300,16 +353,21 @@ size_t merit_workspace(int V, int n_tuples) {
 }  // namespace
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, cudaStream_t stream) {
+                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     cudaStream_t stream) {
     TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr};
     const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
-    trace_kernel<true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    if (exact)
+        trace_kernel<true, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    else
+        trace_kernel<true, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
     count_launch();
     return cuda_status(cudaGetLastError(), "residuals kernel launch");
 }
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, cudaStream_t stream) {
+                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 cudaStream_t stream) {
     const size_t need = merit_workspace(p.V, p.n_tuples);
     if (workspace == nullptr || ws_bytes < need) {
         set_error("merit: workspace of %zu bytes needed, %zu given", need, ws_bytes);
@@ -321,7 +379,10 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
                  reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int)))};
     const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
-    trace_kernel<false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    if (exact)
+        trace_kernel<false, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    else
+        trace_kernel<false, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
     count_launch();
     int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
     if (rc != MKB_OK) return rc;

@@ -1,9 +1,10 @@
 """GPU parity of the forward trace (RESIDUALS, MERIT) against the CPU oracle.
 
-Tolerances are the reference's own CPU/GPU FP64 tolerances (tests/tolerances.hpp of the
-reference): OPD within 1e-12 mm absolute + 1e-11 relative, merit equal to the sum of the
-squared residual rows within 1e-13 relative, statuses identical. Results must be
-bit-identical across repeated runs and independent of the variant's position in the batch.
+Precision FP64 (the default) must reproduce the oracle -- and so the reference CPU build --
+bit for bit: statuses, OPD, residual and penalty rows, merit and failure counts. Precision
+FP64_FMA is checked against the reference's own CPU/GPU tolerances (tests/tolerances.hpp of
+the reference). Both must be bit-identical across repeated runs and independent of a
+variant's position in the batch.
 """
 
 import os
@@ -13,14 +14,17 @@ import pytest
 import torch
 
 from mikroptim_b200 import engine, workloads
-from mikroptim_b200.batch import FAILURE_HARD, ResidualLayout, in_piston
+from mikroptim_b200.batch import (FAILURE_HARD, PRECISION_FP64, PRECISION_FP64_FMA,
+                                  ResidualLayout)
 import oracle.pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
-OPD_ABS = 1e-12    # mm, kCpuGpuFp64
-OPD_REL = 1e-11    # kCpuGpuFp64Relative
-MERIT_REL = 1e-12
+OPD_ABS = 1e-12         # mm, kCpuGpuFp64
+OPD_REL = 1e-11         # kCpuGpuFp64Relative
+SOFT_TUPLE_ABS = 1e-9   # mm, kCpuGpuSoftTuple: tuples with soft-failed rays
+PENALTY_REL = 1e-6      # kCpuGpuPenaltyRelative
+MERIT_VS_ROWS = 1e-13   # kMeritVsResidualSum
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
@@ -36,98 +40,168 @@ def gpu_merit(b, lay):
     return out.merit, out.failed, out.hard_failed
 
 
-def row_factor(res, opd, rays):
-    """|residual / OPD| per ray row (the weight s * sqrt(W) in waves per mm)."""
-    with np.errstate(divide="ignore", invalid="ignore"):
-        f = np.abs(res[:, :rays] / opd)
-    return np.nan_to_num(f, nan=0.0, posinf=0.0)
+def tuple_tolerance(lay, opd_o, status_o):
+    """Per-ray OPD bound of the reference: max(abs, 1e-11 |OPD|), abs = 1e-12 mm, or 1e-9 mm
+    for every ray of a tuple that contains a soft-failed ray."""
+    abs_part = np.full(opd_o.shape, OPD_ABS)
+    soft = (status_o == 5) | (status_o == 6)
+    for f in range(lay.fields):
+        for l in range(lay.wavelengths):
+            o0, n = lay.offset(f, l), lay.samples[f]
+            has_soft = soft[:, o0:o0 + n].any(axis=1)
+            abs_part[has_soft, o0:o0 + n] = SOFT_TUPLE_ABS
+    return np.maximum(abs_part, OPD_REL * np.abs(opd_o))
 
 
-def check_residuals(g, o, lay):
+def check_residuals(g, o, lay, mask=None):
+    """Statuses equal; OPD, wavefront rows and penalty rows within the reference's CPU/GPU
+    tolerances. `mask` (rays) restricts the comparison to tuples whose statuses all agree."""
     res_g, opd_g, st_g = g
     res_o, opd_o, st_o = o
     rays = lay.rays_per_variant
-    assert np.array_equal(st_g, st_o)
-    tol = OPD_ABS + OPD_REL * np.abs(opd_o)
-    assert np.all(np.abs(opd_g - opd_o) <= tol), np.max(np.abs(opd_g - opd_o) - tol)
-    fac = row_factor(res_o, opd_o, rays).max()
-    tol_r = fac * OPD_ABS + OPD_REL * np.abs(res_o[:, :rays])
-    assert np.all(np.abs(res_g[:, :rays] - res_o[:, :rays]) <= tol_r)
+    if mask is None:
+        assert np.array_equal(st_g, st_o)
+        mask = np.ones(st_o.shape, dtype=bool)
+    tol = tuple_tolerance(lay, opd_o, st_o)
+    bad = (np.abs(opd_g - opd_o) > tol) & mask
+    assert not bad.any(), (np.argwhere(bad)[:5], (np.abs(opd_g - opd_o) - tol)[bad].max())
+    wave_f, pen_f = row_factors(lay)
+    # wavefront rows r = s sqrt(W) OPD: the OPD bound times the row factor s sqrt(W)
+    bad = (np.abs(res_g[:, :rays] - res_o[:, :rays]) > wave_f * tol * (1 + 1e-9)) & mask
+    assert not bad.any(), np.argwhere(bad)[:5]
     if lay.soft_failure:
-        pen_o = res_o[:, rays:]
-        assert np.allclose(res_g[:, rays:], pen_o, rtol=1e-12, atol=1e-12 * np.abs(pen_o).max())
+        # penalty rows p = s_p sqrt(W) pi: bound max(1e-12, 1e-6 |pi|) on pi
+        pen_g, pen_o = res_g[:, rays:], res_o[:, rays:]
+        bound = np.maximum(OPD_ABS * pen_f, PENALTY_REL * np.abs(pen_o))
+        bad = (np.abs(pen_g - pen_o) > bound) & mask
+        assert not bad.any(), np.argwhere(bad)[:5]
 
 
-def test_singlet_residuals_match_oracle():
-    b, st, vs, x0 = workloads.singlet(1024)
-    lay = ResidualLayout(b.topology, st)
-    check_residuals(gpu_residuals(b, lay), po.port().residuals(b, lay, threads=8), lay)
+def row_factors(lay):
+    """s_(f,l) sqrt(W_k) of every wavefront row and s_p sqrt(W_k) of every penalty row, with
+    the tuple weights of the workload generators (all field and wavelength weights 1)."""
+    from mikroptim_b200.quadrature import samples
+    F, L = lay.fields, lay.wavelengths
+    w = 1.0 / (F * L)
+    lam = 1e-6 * 587.6 if F == 3 else 1e-6 * 587.56
+    wave = np.zeros(lay.rays_per_variant)
+    pen = np.zeros(lay.rays_per_variant)
+    for f in range(F):
+        smp = samples(lay.settings.rings, lay.settings.spokes, lay.topology.pupil_mode[f])
+        for l in range(L):
+            o0, n = lay.offset(f, l), lay.samples[f]
+            wave[o0:o0 + n] = np.sqrt(w) / lam * np.sqrt(smp[:, 2])
+            pen[o0:o0 + n] = np.sqrt(lay.settings.fail_weight * w) * np.sqrt(smp[:, 2])
+    return wave[None, :], pen[None, :]
 
 
-def test_singlet_matches_reference_golden():
-    g = dict(np.load(os.path.join(GOLDEN, "singlet.npz")))
-    b, st, vs, x0 = workloads.singlet(1024)
-    b = b.subset(0, 8)
-    lay = ResidualLayout(b.topology, st)
-    check_residuals(gpu_residuals(b, lay), (g["residuals"], g["opd"], g["status"]), lay)
-    m, f, h = gpu_merit(b, lay)
-    assert np.allclose(m, g["merit"], rtol=MERIT_REL, atol=0)
-    assert np.array_equal(f, g["failed"]) and np.array_equal(h, g["hard_failed"])
-
-
-def test_singlet_hard_mode():
-    b, st, vs, x0 = workloads.singlet(256, failure=FAILURE_HARD)
-    lay = ResidualLayout(b.topology, st)
-    check_residuals(gpu_residuals(b, lay), po.port().residuals(b, lay, threads=8), lay)
-
-
-def test_objective_soft_failures_match_oracle():
-    b, st, vs, x0 = workloads.objective(48)
-    lay = ResidualLayout(b.topology, st)
-    g = gpu_residuals(b, lay)
-    o = po.port().residuals(b, lay, threads=8)
-    # rays whose soft/hard branch sits within rounding of a decision boundary may flip; the
-    # fraction is checked, and the tuples whose statuses all agree are compared fully
-    same = g[2] == o[2]
-    assert same.mean() > 0.9999
-    check_residuals_masked(g, o, lay, same)
-
-
-def check_residuals_masked(g, o, lay, same):
-    rays = lay.rays_per_variant
-    res_g, opd_g, st_g = g
-    res_o, opd_o, st_o = o
-    # tuple mask: all rays of the tuple agree on their status
+def tuple_mask(lay, same):
     ok = np.ones_like(same)
     for f in range(lay.fields):
         for l in range(lay.wavelengths):
-            o0 = lay.offset(f, l)
-            n = lay.samples[f]
-            t = same[:, o0:o0 + n].all(axis=1)
-            ok[:, o0:o0 + n] = t[:, None]
-    tol = OPD_ABS + OPD_REL * np.abs(opd_o)
-    assert np.all((np.abs(opd_g - opd_o) <= tol) | ~ok)
+            o0, n = lay.offset(f, l), lay.samples[f]
+            ok[:, o0:o0 + n] = same[:, o0:o0 + n].all(axis=1)[:, None]
+    return ok
 
 
-def test_objective_merit_matches_oracle():
-    b, st, vs, x0 = workloads.objective(32)
-    lay = ResidualLayout(b.topology, st)
-    m, f, h = gpu_merit(b, lay)
-    mo, fo, ho = po.port().merit(b, lay, threads=8)
-    assert np.allclose(m, mo, rtol=1e-10, atol=0)
-    assert np.abs(f - fo).max() <= 2 and np.abs(h - ho).max() <= 2
+def exact(st):
+    st.precision = PRECISION_FP64
+    return st
+
+
+def fma(st):
+    st.precision = PRECISION_FP64_FMA
+    return st
+
+
+def assert_bitwise(g, o):
+    for x, y in zip(g, o):
+        assert x.shape == y.shape
+        assert np.array_equal(x, y), np.argwhere(x != y)[:5]
+
+
+def test_fp64_residuals_bitwise_singlet():
+    b, st, vs, x0 = workloads.singlet(1024)
+    lay = ResidualLayout(b.topology, exact(st))
+    assert_bitwise(gpu_residuals(b, lay), po.port().residuals(b, lay, threads=8))
+
+
+def test_fp64_residuals_bitwise_objective_all_failure_branches():
+    b, st, vs, x0 = workloads.objective(48)
+    lay = ResidualLayout(b.topology, exact(st))
+    g = gpu_residuals(b, lay)
+    assert_bitwise(g, po.port().residuals(b, lay, threads=8))
+    counts = np.bincount(g[2].ravel(), minlength=7)
+    assert counts[[1, 3, 5, 6]].min() > 0
+
+
+def test_fp64_merit_bitwise():
+    for b, st, vs, x0 in (workloads.singlet(1024), workloads.objective(32)):
+        lay = ResidualLayout(b.topology, exact(st))
+        assert_bitwise(gpu_merit(b, lay), po.port().merit(b, lay, threads=8))
+
+
+def test_fp64_matches_reference_golden_bitwise():
+    g = dict(np.load(os.path.join(GOLDEN, "singlet.npz")))
+    b, st, vs, x0 = workloads.singlet(1024)
+    b = b.subset(0, 8)
+    lay = ResidualLayout(b.topology, exact(st))
+    assert_bitwise(gpu_residuals(b, lay), (g["residuals"], g["opd"], g["status"]))
+    assert_bitwise(gpu_merit(b, lay), (g["merit"], g["failed"], g["hard_failed"]))
+    g = dict(np.load(os.path.join(GOLDEN, "objective.npz")))
+    b, st, vs, x0 = workloads.objective(4096, rings=3, spokes=6)
+    b = b.subset(0, 2)
+    lay = ResidualLayout(b.topology, exact(st))
+    assert_bitwise(gpu_residuals(b, lay), (g["residuals"], g["opd"], g["status"]))
+
+
+def test_fp64_hard_mode_bitwise():
+    b, st, vs, x0 = workloads.singlet(256, failure=FAILURE_HARD)
+    lay = ResidualLayout(b.topology, exact(st))
+    assert_bitwise(gpu_residuals(b, lay), po.port().residuals(b, lay, threads=8))
+
+
+def test_fma_singlet_within_reference_tolerances():
+    b, st, vs, x0 = workloads.singlet(1024)
+    lay = ResidualLayout(b.topology, fma(st))
+    check_residuals(gpu_residuals(b, lay), po.port().residuals(b, lay, threads=8), lay)
+    m = gpu_merit(b, lay)[0]
+    mo = po.port().merit(b, lay, threads=8)[0]
+    assert np.allclose(m, mo, rtol=1e-11, atol=0)
+
+
+def test_fma_objective_statistics():
+    """FMA contraction moves rays that sit within rounding of a soft/hard decision, and
+    continuations far outside the system amplify rounding (the reference widens its bound to
+    1e-9 mm there); most rays and tuples still agree to the reference tolerances."""
+    b, st, vs, x0 = workloads.objective(48)
+    lay = ResidualLayout(b.topology, fma(st))
+    g = gpu_residuals(b, lay)
+    o = po.port().residuals(b, lay, threads=8)
+    same = g[2] == o[2]
+    assert same.mean() > 0.9999
+    ok = tuple_mask(lay, same)
+    tol = tuple_tolerance(lay, o[1], o[2])
+    within = (np.abs(g[1] - o[1]) <= tol) | ~ok
+    assert within.mean() > 0.97
+    # the tuples of well-behaved variants (no soft failure at all) meet the bound fully
+    clean = ~((o[2] == 5) | (o[2] == 6)).any(axis=1)
+    assert within[clean].all()
 
 
 def test_merit_is_sum_of_squared_rows():
     b, st, vs, x0 = workloads.singlet(512)
-    lay = ResidualLayout(b.topology, st)
-    res = gpu_residuals(b, lay)[0]
-    m = gpu_merit(b, lay)[0]
-    assert np.allclose(m, (res ** 2).sum(axis=1), rtol=1e-13, atol=0)
+    for s in (exact(st), fma(workloads.singlet(4)[1])):
+        lay = ResidualLayout(b.topology, s)
+        res = gpu_residuals(b, lay)[0]
+        m = gpu_merit(b, lay)[0]
+        assert np.allclose(m, (res ** 2).sum(axis=1), rtol=MERIT_VS_ROWS, atol=0)
 
 
-def test_repeated_runs_and_batch_position_bit_identical():
+@pytest.mark.parametrize("precision", [0, 2])
+def test_repeated_runs_and_batch_position_bit_identical(precision):
     b, st, vs, x0 = workloads.objective(40)
+    st.precision = precision
     lay = ResidualLayout(b.topology, st)
     r1 = gpu_residuals(b, lay)
     r2 = gpu_residuals(b, lay)
