@@ -157,6 +157,21 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
                      double* merit, int64_t* failed, int64_t* hard_failed,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* MERIT for callers that cannot allocate device memory. No counterpart in the reference.
+ * Some callers cannot call cudaMalloc: a host application that gives the library a fixed
+ * memory budget and owns the rest of the GPU, or a loop that must never wait on an
+ * allocation. This entry point takes the same batch, plan and outputs as mkb_merit_device but
+ * no workspace: the per-tuple partial sums go to a 4 MiB array compiled into the library
+ * (every GPU that loads the library keeps it until the process exits). Limit: variants x
+ * fields x wavelengths <= MKB_NOALLOC_MERIT_MAX_SLOTS per call; larger batches are rejected
+ * with MKB_ERR_ARGUMENT before anything is enqueued. The array is shared by all calls, so
+ * calls that overlap on the GPU race: run one at a time per device. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, no allocation) with that
+ * device current; make that first call before any stream capture. */
+#define MKB_NOALLOC_MERIT_MAX_SLOTS 262144
+int mkb_merit_noalloc_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                             double* merit, int64_t* failed, int64_t* hard_failed, void* stream);
+
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);
 const char* mkb_version(void);

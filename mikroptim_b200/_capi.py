@@ -114,6 +114,10 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                      c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
                                      c.c_size_t, c.c_void_p]
+    lib.mkb_merit_noalloc_device.restype = c.c_int
+    lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                             c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
+    lib.mkb_device_status.restype = c.c_int
 
 
 def lib() -> C.CDLL:

@@ -16,6 +16,7 @@
 #include "common.cuh"
 
 #include <cstdio>
+#include <mutex>
 #include <type_traits>
 
 namespace mkb {
@@ -394,8 +395,84 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
 
 size_t merit_workspace_bytes(int V, int n_tuples) { return merit_workspace(V, n_tuples); }
 
+// ---- MERIT without a caller workspace --------------------------------------------------------
+// Some callers cannot allocate device memory: a host application that hands the library a
+// fixed pool at start-up and owns every other byte of the GPU, or a tight optimisation loop
+// that must never stall in cudaMalloc. For them MERIT keeps its per-tuple partial sums in this
+// array, which lives in the library's own device image: every GPU that loads the library holds
+// it (4 MiB + 256 B) until the process exits. All calls share it, so two calls that overlap on
+// the GPU (different streams, or different host threads on one device) race; the caller runs
+// one at a time per device. Nothing in it needs to start at zero: each call writes every
+// partial sum before the finalize kernel reads it.
+constexpr int64_t kNoAllocMeritSlots = MKB_NOALLOC_MERIT_MAX_SLOTS;
+constexpr size_t kNoAllocScratchBytes =
+    static_cast<size_t>(kNoAllocMeritSlots) * (sizeof(double) + 2 * sizeof(int)) + 256;
+static __device__ __align__(256) unsigned char g_noalloc_merit_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kMaxDevices] = {};
+}  // namespace
+
+// Device address of the scratch array on the current device. In host code the array's name
+// is only a host-side stand-in, so the address is looked up once per device (with that device
+// current) and cached; the lookup itself allocates nothing.
+int noalloc_merit_scratch(void** out) {
+    int dev = 0;
+    int rc = cuda_status(cudaGetDevice(&dev), "no-allocation MERIT: cudaGetDevice");
+    if (rc != MKB_OK) return rc;
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("no-allocation MERIT: device %d out of range", dev);
+        return MKB_ERR_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[dev] == nullptr) {
+        void* p = nullptr;
+        rc = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_merit_scratch),
+                         "no-allocation MERIT: cudaGetSymbolAddress");
+        if (rc != MKB_OK) return rc;
+        g_noalloc_address[dev] = p;
+    }
+    *out = g_noalloc_address[dev];
+    return MKB_OK;
+}
+
 int pack_rays_default() { return kPackRays; }
 
 MKB_DEFINE_ERROR_READER(trace_device_error)
 
 }  // namespace mkb
+
+// No counterpart in the reference: MERIT for callers that cannot allocate device memory.
+extern "C" int mkb_merit_noalloc_device(const mkb_device_batch* batch,
+                                        const mkb_residual_plan* plan, double* merit,
+                                        int64_t* failed, int64_t* hard_failed, void* stream) {
+    using namespace mkb;
+    TraceParams p;
+    int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+        set_error("no-allocation MERIT: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    if (p.V == 0) return MKB_OK;
+    if (!merit || !failed || !hard_failed) {
+        set_error("no-allocation MERIT: output is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    const int64_t slots = static_cast<int64_t>(p.V) * p.n_tuples;
+    if (slots > kNoAllocMeritSlots) {
+        set_error("no-allocation MERIT: %d variants x %d tuples = %lld partial sums exceed the "
+                  "built-in limit of %lld; split the batch or use mkb_merit_device",
+                  p.V, p.n_tuples, static_cast<long long>(slots),
+                  static_cast<long long>(kNoAllocMeritSlots));
+        return MKB_ERR_ARGUMENT;
+    }
+    void* scratch = nullptr;
+    rc = noalloc_merit_scratch(&scratch);
+    if (rc != MKB_OK) return rc;
+    return launch_merit(p, batch->records, merit, failed, hard_failed, scratch,
+                        kNoAllocScratchBytes, plan->precision == MKB_PRECISION_FP64,
+                        static_cast<cudaStream_t>(stream));
+}
