@@ -157,6 +157,45 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
                      double* merit, int64_t* failed, int64_t* hard_failed,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- Jacobians ------------------------------------------------------------------------------
+ * Both take `templates` (1 variant for all runs, or one per run), the plan, the variables and
+ * the run points x0 [runs][P] (device), and write J [runs][P][R] (column p of run i at
+ * J + (i*P + p)*R, R = trace rows) and r0 [runs][R] = residuals at x0 -- the layout of the
+ * reference's FdJacobian / AdjointJacobian (include/mikroptim/optim/fd_jacobian.hpp:118). */
+
+/* Finite differences, central scheme with the reference's stencils at bounds: replaces
+ * DeviceFdJacobian::compute (src/cuda/fd_jacobian.cu:203, fd_jacobian_cpu in
+ * src/optim/fd_jacobian.cpp:182). 2P + 1 traced variants per run; runs are processed in
+ * chunks that fit the workspace (mkb_fd_jacobian_workspace_bytes for a chunk size).
+ * status_changes [runs][P] (may be NULL): rays whose Ok-status differs between x0 and a
+ * perturbed point of the column. */
+size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
+                                       const mkb_residual_plan* plan, int32_t P, int32_t runs,
+                                       int32_t runs_per_chunk);
+int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                           const mkb_variables* vars, const double* x0, int32_t runs, double* J,
+                           double* r0, int64_t* status_changes, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* Adjoint sweep with checkpoints every 4 surfaces, then the piston projection: replaces
+ * DeviceAdjointJacobian::compute (src/cuda/adjoint_jacobian.cu:401) and
+ * adjoint_jacobian_cpu (src/optim/adjoint_jacobian.cpp:370). status [runs][rays]. */
+size_t mkb_adjoint_jacobian_workspace_bytes(const mkb_device_batch* templates, int32_t runs);
+int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                                const mkb_variables* vars, const double* x0, int32_t runs,
+                                double* J, double* r0, uint8_t* status, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/* ---- normal equations --------------------------------------------------------------------
+ * gram [runs][P+1][P+1] = [J r]^T [J r] for J [runs][P][R] (column p of run i at
+ * J + (i*P + p)*R) and r [runs][R]: A = J^T J in the top-left block, g = J^T r in column P.
+ * Replaces DeviceNormalEquations::compute (src/cuda/normal_equations.cu:48, gram_kernel).
+ * exact != 0: every entry one FMA chain over the rows in ascending order, bit-identical to
+ * normal_equations_host (include/mikroptim/optim/normal_equations.hpp:33); exact == 0: FP64
+ * tensor cores (mma.sync m8n8k4 f64), deterministic. */
+int mkb_normal_equations_device(const double* J, const double* r, int32_t runs, int32_t P,
+                                int64_t R, double* gram, int32_t exact, void* stream);
+
 /* MERIT for callers that cannot allocate device memory. No counterpart in the reference.
  * Some callers cannot call cudaMalloc: a host application that gives the library a fixed
  * memory budget and owns the rest of the GPU, or a loop that must never wait on an

@@ -118,6 +118,24 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     lib.mkb_device_status.restype = c.c_int
+    PV = C.POINTER(Variables)
+    PB = C.POINTER(DeviceBatch)
+    PP = C.POINTER(ResidualPlan)
+    lib.mkb_fd_jacobian_workspace_bytes.restype = c.c_size_t
+    lib.mkb_fd_jacobian_workspace_bytes.argtypes = [PB, PP, c.c_int32, c.c_int32, c.c_int32]
+    lib.mkb_fd_jacobian_device.restype = c.c_int
+    lib.mkb_fd_jacobian_device.argtypes = [PB, PP, PV, c.c_void_p, c.c_int32, c.c_void_p,
+                                           c.c_void_p, c.c_void_p, c.c_void_p, c.c_size_t,
+                                           c.c_void_p]
+    lib.mkb_adjoint_jacobian_workspace_bytes.restype = c.c_size_t
+    lib.mkb_adjoint_jacobian_workspace_bytes.argtypes = [PB, c.c_int32]
+    lib.mkb_adjoint_jacobian_device.restype = c.c_int
+    lib.mkb_adjoint_jacobian_device.argtypes = [PB, PP, PV, c.c_void_p, c.c_int32, c.c_void_p,
+                                                c.c_void_p, c.c_void_p, c.c_void_p, c.c_size_t,
+                                                c.c_void_p]
+    lib.mkb_normal_equations_device.restype = c.c_int
+    lib.mkb_normal_equations_device.argtypes = [c.c_void_p, c.c_void_p, c.c_int32, c.c_int32,
+                                                c.c_int64, c.c_void_p, c.c_int32, c.c_void_p]
 
 
 def lib() -> C.CDLL:

@@ -20,6 +20,9 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
 size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
 int trace_device_error();
+int gram_device_error();
+int adjoint_device_error();
+int jacobian_device_error();
 
 namespace {
 thread_local std::string g_error;
@@ -248,6 +251,59 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     return MKB_OK;
 }
 
+int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out) {
+    if (vars == nullptr || vars->count < 1 || vars->count > MKB_MAX_VARIABLES) {
+        set_error("variables: count must be in [1, %d]", MKB_MAX_VARIABLES);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (!vars->type || !vars->surface || !vars->lower || !vars->upper || !vars->typical) {
+        set_error("variables: null array");
+        return MKB_ERR_ARGUMENT;
+    }
+    VarParams& v = *out;
+    std::memset(&v, 0, sizeof(v));
+    v.P = vars->count;
+    for (int s = 0; s < kMaxSurfaces; ++s) v.col_curvature[s] = v.col_thickness[s] = -1;
+    for (int k = 0; k < v.P; ++k) {
+        const int t = vars->type[k];
+        int s = vars->surface[k];
+        if (t == MKB_VAR_WORKING_DISTANCE) s = S - 1;
+        if (t != MKB_VAR_CURVATURE && t != MKB_VAR_THICKNESS && t != MKB_VAR_WORKING_DISTANCE) {
+            set_error("variable %d: unknown type %d (curvature, thickness, working distance)", k,
+                      t);
+            return MKB_ERR_UNSUPPORTED;
+        }
+        if (s < 0 || s >= S || (t == MKB_VAR_THICKNESS && s == S - 1)) {
+            set_error("variable %d: surface %d out of range", k, s);
+            return MKB_ERR_ARGUMENT;
+        }
+        if (t == MKB_VAR_CURVATURE && type[s] != MKB_SURFACE_SPHERE) {
+            set_error("variable %d: curvature of surface %d, which is not a sphere", k, s);
+            return MKB_ERR_ARGUMENT;
+        }
+        int8_t& slot = t == MKB_VAR_CURVATURE ? v.col_curvature[s] : v.col_thickness[s];
+        if (slot >= 0) {
+            set_error("variable %d: its parameter already belongs to variable %d", k, slot);
+            return MKB_ERR_ARGUMENT;
+        }
+        slot = static_cast<int8_t>(k);
+        v.type[k] = static_cast<int8_t>(t == MKB_VAR_CURVATURE ? MKB_VAR_CURVATURE : MKB_VAR_THICKNESS);
+        v.surface[k] = static_cast<int8_t>(s);
+        v.lower[k] = vars->lower[k];
+        v.upper[k] = vars->upper[k];
+        v.typical[k] = vars->typical[k];
+        if (std::isnan(v.lower[k]) || std::isnan(v.upper[k]) || v.lower[k] > v.upper[k]) {
+            set_error("variable %d: invalid bounds", k);
+            return MKB_ERR_ARGUMENT;
+        }
+        if (!(v.typical[k] > 0.0) || !std::isfinite(v.typical[k])) {
+            set_error("variable %d: typical size must be > 0", k);
+            return MKB_ERR_ARGUMENT;
+        }
+    }
+    return MKB_OK;
+}
+
 }  // namespace mkb
 
 using namespace mkb;
@@ -259,7 +315,8 @@ const char* mkb_version(void) { return "mikroptim_b200 0.1 (sm_100a)"; }
 int64_t mkb_launch_count(void) { return g_launches.load(); }
 
 int mkb_device_status(void) {
-    int (*readers[])() = {trace_device_error};
+    int (*readers[])() = {trace_device_error, gram_device_error, adjoint_device_error,
+                              jacobian_device_error};
     int status = MKB_OK;
     for (auto read : readers) {
         const int v = read();

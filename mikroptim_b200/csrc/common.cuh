@@ -191,8 +191,8 @@ __device__ __forceinline__ bool operator>(Exact64 a, Exact64 b) { return a.v > b
 __device__ __forceinline__ bool operator>=(Exact64 a, Exact64 b) { return a.v >= b.v; }
 __device__ __forceinline__ Exact64 nsqrt(Exact64 a) { return __dsqrt_rn(a.v); }
 __device__ __forceinline__ double nsqrt(double a) { return sqrt(a); }
-__device__ __forceinline__ double value(double a) { return a; }
-__device__ __forceinline__ double value(Exact64 a) { return a.v; }
+__device__ __forceinline__ double value_of(double a) { return a; }
+__device__ __forceinline__ double value_of(Exact64 a) { return a.v; }
 
 // ---- ray state and surface step -------------------------------------------------------------
 // Formulas and order of operations: transfer_to_tangent_plane, intersect_sphere and
@@ -307,6 +307,29 @@ __device__ __forceinline__ int reference_step(RayT<N>& r, N h, N w, N n_image, S
     r.pz = r.pz + s * r.dz;
     r.opl += n_image * s;
     return kOk;
+}
+
+// ---- optimiser variables (VariableSet, reference include/mikroptim/optim/variable_set.hpp:63)
+struct VarParams {
+    int P;
+    int8_t type[MKB_MAX_VARIABLES];       // MKB_VAR_*
+    int8_t surface[MKB_MAX_VARIABLES];    // table surface of the parameter
+    int8_t col_curvature[kMaxSurfaces];   // column of curvature[s], -1 if none
+    int8_t col_thickness[kMaxSurfaces];   // column of thickness[s], -1 if none
+    double lower[MKB_MAX_VARIABLES], upper[MKB_MAX_VARIABLES], typical[MKB_MAX_VARIABLES];
+};
+
+// Builds the variable block for a batch with S surfaces; MKB_OK or MKB_ERR_ARGUMENT.
+int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out);
+
+// Writes x into a packed record (VariableSet::apply, src/optim/variable_set.cpp:237).
+__device__ __forceinline__ void apply_variables(const VarParams& v, const RecordLayout& lay,
+                                                const double* x, double* rec) {
+    for (int k = 0; k < v.P; ++k) {
+        const int s = v.surface[k];
+        if (v.type[k] == MKB_VAR_CURVATURE) rec[lay.curvature + s] = x[k];
+        else rec[lay.thickness + s] = x[k];
+    }
 }
 
 // ---- launch bookkeeping (host) -------------------------------------------------------------

@@ -1,0 +1,353 @@
+// Jacobian entry points: finite differences (the reference method) and the adjoint sweep.
+//
+// FD (central scheme, 2P + 1 variants per run; reference: fd_pattern and write_fd_variants,
+// src/optim/variant_generator.cpp:177,248; fd_jacobian_from_residuals,
+// src/optim/fd_jacobian.cpp:80; fd_difference_kernel, src/cuda/fd_jacobian.cu:65):
+//   1. fd_pattern_kernel  one thread per (run, variable): step h, stencil, points, steps
+//   2. fd_build_kernel    one CTA per FD variant: template record + x0 + the perturbed entry
+//   3. RESIDUALS          the trace kernel over all FD variants of a chunk of runs
+//   4. fd_difference_kernel / fd_changes_kernel: columns by fd_derivative, status changes
+// Runs are processed in chunks sized by the workspace the caller passes.
+//
+// Adjoint (reference: DeviceAdjointJacobian::compute, src/cuda/adjoint_jacobian.cu:401):
+//   apply x0 -> RESIDUALS (r0, status) -> adjoint rows -> piston projection.
+#include "common.cuh"
+
+#include <algorithm>
+#include <type_traits>
+
+namespace mkb {
+
+int launch_residuals(const TraceParams& p, const double* records, double* residuals,
+                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     cudaStream_t stream);
+int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
+                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
+int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
+                        const double* records, double* J, bool exact, cudaStream_t stream);
+int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
+                      const uint8_t* status, double* J, bool exact, cudaStream_t stream);
+int pack_rays_default();
+
+namespace {
+
+enum : int { kCentral = 0, kOneSided = 1, kTruncated = 2 };  // FdStencil, optim/fd_formula.hpp:16
+
+struct FdPattern {
+    double xa, xb, da, db;
+    int stencil;
+    int pad;
+};
+
+// fd_step + fd_pattern (central), every operation separately rounded.
+__global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const double* x0, int runs,
+                                  FdPattern* pattern) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= runs * vp.P) return;
+    const int k = id % vp.P;
+    const Exact64 x = x0[id];
+    const Exact64 lo = vp.lower[k], up = vp.upper[k];
+    const double ax = fabs(x.v);
+    const double typ = vp.typical[k];
+    const Exact64 h = Exact64(6.0554544523933395e-06) * Exact64(ax < typ ? typ : ax);
+    const Exact64 plus = x + h, minus = x - h;
+    FdPattern out;
+    out.stencil = kCentral;
+    out.pad = 0;
+    Exact64 a, b;
+    if (plus.v <= up.v && minus.v >= lo.v) {
+        a = plus;
+        b = minus;
+    } else {
+        const bool towards_upper = (up - x).v >= (x - lo).v;
+        const Exact64 two_h = Exact64(2.0) * h;
+        const Exact64 far = towards_upper ? x + two_h : x - two_h;
+        if (towards_upper ? far.v <= up.v : far.v >= lo.v) {
+            out.stencil = kOneSided;
+            a = towards_upper ? plus : minus;
+            b = far;
+        } else {
+            out.stencil = kTruncated;
+            a = plus.v <= up.v ? plus : up;
+            b = minus.v >= lo.v ? minus : lo;
+        }
+    }
+    out.xa = a.v;
+    out.xb = b.v;
+    out.da = (a - x).v;
+    out.db = (b - x).v;
+    pattern[id] = out;
+}
+
+// One CTA per FD variant j of run i (variant i*n + j): template record, x0 applied, entry k
+// replaced by x_a (j = 2k + 1) or x_b (j = 2k + 2).
+__global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayout lay,
+                                const double* __restrict__ templates, int n_templates,
+                                const double* __restrict__ x0, const FdPattern* __restrict__ pat,
+                                int first_run, int runs, double* __restrict__ out) {
+    const int n = 2 * vp.P + 1;
+    const int local = blockIdx.x / n;
+    const int j = blockIdx.x - local * n;
+    const int run = first_run + local;
+    const double* src = templates + static_cast<int64_t>(n_templates == 1 ? 0 : run) * lay.stride;
+    double* dst = out + static_cast<int64_t>(blockIdx.x) * lay.stride;
+    for (int i = threadIdx.x; i < lay.stride; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double* x = x0 + static_cast<int64_t>(run) * vp.P;
+        apply_variables(vp, lay, x, dst);
+        if (j > 0) {
+            const int k = (j - 1) / 2;
+            const FdPattern& p = pat[static_cast<int64_t>(run) * vp.P + k];
+            const double y = (j & 1) ? p.xa : p.xb;
+            const int s = vp.surface[k];
+            if (vp.type[k] == MKB_VAR_CURVATURE) dst[lay.curvature + s] = y;
+            else dst[lay.thickness + s] = y;
+        }
+    }
+}
+
+// J(r, k) = fd_derivative(stencil, r0, r_a, r_b, d_a, d_b) (optim/fd_formula.hpp:40), r0 rows.
+template <bool kExact>
+__global__ void fd_difference_kernel(const double* __restrict__ res, const FdPattern* __restrict__ pat,
+                                     int P, int64_t R, int first_run, int runs,
+                                     double* __restrict__ J, double* __restrict__ r0) {
+    using N = typename std::conditional<kExact, Exact64, double>::type;
+    const int n = 2 * P + 1;
+    const int64_t total = static_cast<int64_t>(runs) * (P + 1) * R;
+    for (int64_t id = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; id < total;
+         id += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t r = id % R;
+        const int64_t ck = id / R;
+        const int c = static_cast<int>(ck % (P + 1));
+        const int local = static_cast<int>(ck / (P + 1));
+        const int run = first_run + local;
+        const double* base = res + static_cast<int64_t>(local) * n * R;
+        if (c == P) {
+            r0[static_cast<int64_t>(run) * R + r] = base[r];
+            continue;
+        }
+        const FdPattern p = pat[static_cast<int64_t>(run) * P + c];
+        const N v0 = base[r];
+        const N va = base[static_cast<int64_t>(2 * c + 1) * R + r];
+        const N vb = base[static_cast<int64_t>(2 * c + 2) * R + r];
+        const N da = p.da, db = p.db;
+        N d;
+        if (p.stencil == kOneSided) {
+            const N ga = va - v0;
+            const N gb = vb - v0;
+            d = (db * db * ga - da * da * gb) / (da * db * (db - da));
+        } else {
+            d = (va - vb) / (da - db);
+        }
+        J[(static_cast<int64_t>(run) * P + c) * R + r] = value_of(d);
+    }
+}
+
+// Rays whose validity (status Ok) changes between x0 and a perturbed point of column k.
+__global__ void fd_changes_kernel(const uint8_t* __restrict__ status, int P, int64_t rays,
+                                  int first_run, int64_t* __restrict__ changes) {
+    const int n = 2 * P + 1;
+    const int local = blockIdx.x / P;
+    const int k = blockIdx.x - local * P;
+    const uint8_t* s0 = status + static_cast<int64_t>(local) * n * rays;
+    const uint8_t* sa = s0 + static_cast<int64_t>(2 * k + 1) * rays;
+    const uint8_t* sb = s0 + static_cast<int64_t>(2 * k + 2) * rays;
+    int count = 0;
+    for (int64_t r = threadIdx.x; r < rays; r += blockDim.x) {
+        const bool ok0 = s0[r] == kOk;
+        count += ((sa[r] == kOk) != ok0) || ((sb[r] == kOk) != ok0);
+    }
+    __shared__ int part[256];
+    part[threadIdx.x] = count;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (static_cast<int>(threadIdx.x) < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) changes[static_cast<int64_t>(first_run + local) * P + k] = part[0];
+}
+
+size_t align256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+
+struct FdSizes {
+    size_t pattern, records, residuals, status, total_fixed, per_run;
+};
+
+FdSizes fd_sizes(int stride, int P, int64_t R, int64_t rays, int runs) {
+    FdSizes z;
+    const int n = 2 * P + 1;
+    z.pattern = align256(sizeof(FdPattern) * static_cast<size_t>(runs) * P);
+    z.per_run = align256(sizeof(double) * static_cast<size_t>(n) * stride) +
+                align256(sizeof(double) * static_cast<size_t>(n) * R) +
+                align256(static_cast<size_t>(n) * rays);
+    z.total_fixed = z.pattern;
+    return z;
+}
+
+int check_templates(const mkb_device_batch* t, int runs) {
+    if (t == nullptr || (t->variants != 1 && t->variants != runs)) {
+        set_error("templates must hold 1 variant or one per run (%d runs)", runs);
+        return MKB_ERR_ARGUMENT;
+    }
+    return MKB_OK;
+}
+
+}  // namespace
+
+MKB_DEFINE_ERROR_READER(jacobian_device_error)
+
+}  // namespace mkb
+
+using namespace mkb;
+
+extern "C" {
+
+size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
+                                       const mkb_residual_plan* plan, int32_t P, int32_t runs,
+                                       int32_t runs_per_chunk) {
+    TraceParams tp;
+    if (templates == nullptr || P < 1 || runs < 1 || runs_per_chunk < 1) return 0;
+    mkb_device_batch one = *templates;
+    one.variants = 1;
+    if (make_trace_params(&one, plan, pack_rays_default(), &tp) != MKB_OK) return 0;
+    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const FdSizes z = fd_sizes(tp.stride, P, rows, tp.rays, runs);
+    return z.total_fixed + z.per_run * static_cast<size_t>(runs_per_chunk < runs ? runs_per_chunk : runs);
+}
+
+int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                           const mkb_variables* vars, const double* x0, int32_t runs, double* J,
+                           double* r0, int64_t* status_changes, void* workspace,
+                           size_t workspace_bytes, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    if (runs < 0) {
+        set_error("fd jacobian: runs must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (runs == 0) return MKB_OK;
+    int rc = check_templates(templates, runs);
+    if (rc != MKB_OK) return rc;
+    TraceParams tp;
+    mkb_device_batch fdb = *templates;
+    fdb.variants = 1;
+    rc = make_trace_params(&fdb, plan, pack_rays_default(), &tp);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+        set_error("fd jacobian: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    VarParams vp;
+    rc = make_var_params(vars, tp.S, templates->type, &vp);
+    if (rc != MKB_OK) return rc;
+    if (!x0 || !J || !r0) {
+        set_error("fd jacobian: null pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    const bool exact = plan->precision == MKB_PRECISION_FP64;
+    const int P = vp.P, n = 2 * P + 1;
+    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const FdSizes z = fd_sizes(tp.stride, P, R, tp.rays, runs);
+    if (workspace == nullptr || workspace_bytes < z.total_fixed + z.per_run) {
+        set_error("fd jacobian: workspace of at least %zu bytes needed (one run per chunk)",
+                  z.total_fixed + z.per_run);
+        return MKB_ERR_WORKSPACE;
+    }
+    const int chunk = static_cast<int>(
+        std::min<size_t>((workspace_bytes - z.total_fixed) / z.per_run, static_cast<size_t>(runs)));
+    char* ws = static_cast<char*>(workspace);
+    FdPattern* pattern = reinterpret_cast<FdPattern*>(ws);
+    char* chunk_base = ws + z.pattern;
+    double* records = reinterpret_cast<double*>(chunk_base);
+    double* res = reinterpret_cast<double*>(
+        chunk_base + align256(sizeof(double) * static_cast<size_t>(chunk) * n * tp.stride));
+    uint8_t* status = reinterpret_cast<uint8_t*>(
+        reinterpret_cast<char*>(res) + align256(sizeof(double) * static_cast<size_t>(chunk) * n * R));
+    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+
+    fd_pattern_kernel<<<(runs * P + 127) / 128, 128, 0, stream>>>(vp, x0, runs, pattern);
+    count_launch();
+    rc = cuda_status(cudaGetLastError(), "fd pattern launch");
+    for (int first = 0; rc == MKB_OK && first < runs; first += chunk) {
+        const int cnt = std::min(chunk, runs - first);
+        fd_build_kernel<<<cnt * n, 128, 0, stream>>>(vp, lay, templates->records,
+                                                     templates->variants, x0, pattern, first,
+                                                     cnt, records);
+        count_launch();
+        rc = cuda_status(cudaGetLastError(), "fd build launch");
+        if (rc != MKB_OK) break;
+        TraceParams chunk_tp = tp;
+        chunk_tp.V = cnt * n;
+        rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, exact, stream);
+        if (rc != MKB_OK) break;
+        const int64_t total = static_cast<int64_t>(cnt) * (P + 1) * R;
+        const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 64));
+        if (exact)
+            fd_difference_kernel<true><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0);
+        else
+            fd_difference_kernel<false><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0);
+        count_launch();
+        rc = cuda_status(cudaGetLastError(), "fd difference launch");
+        if (rc != MKB_OK || status_changes == nullptr) continue;
+        fd_changes_kernel<<<cnt * P, 256, 0, stream>>>(status, P, tp.rays, first, status_changes);
+        count_launch();
+        rc = cuda_status(cudaGetLastError(), "fd status-change launch");
+    }
+    return rc;
+}
+
+size_t mkb_adjoint_jacobian_workspace_bytes(const mkb_device_batch* templates, int32_t runs) {
+    if (templates == nullptr || runs < 0) return 0;
+    return align256(sizeof(double) * static_cast<size_t>(runs) * templates->record_stride);
+}
+
+int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                                const mkb_variables* vars, const double* x0, int32_t runs,
+                                double* J, double* r0, uint8_t* status, void* workspace,
+                                size_t workspace_bytes, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    if (runs < 0) {
+        set_error("adjoint jacobian: runs must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (runs == 0) return MKB_OK;
+    int rc = check_templates(templates, runs);
+    if (rc != MKB_OK) return rc;
+    TraceParams tp;
+    mkb_device_batch b = *templates;
+    b.variants = runs;
+    rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+        set_error("adjoint jacobian: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    VarParams vp;
+    rc = make_var_params(vars, tp.S, templates->type, &vp);
+    if (rc != MKB_OK) return rc;
+    if (!x0 || !J || !r0 || !status) {
+        set_error("adjoint jacobian: null pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    const size_t need = mkb_adjoint_jacobian_workspace_bytes(templates, runs);
+    if (workspace == nullptr || workspace_bytes < need) {
+        set_error("adjoint jacobian: workspace of %zu bytes needed", need);
+        return MKB_ERR_WORKSPACE;
+    }
+    const bool exact = plan->precision == MKB_PRECISION_FP64;
+    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    double* records = static_cast<double*>(workspace);
+    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
+    if (rc != MKB_OK) return rc;
+    rc = cuda_status(cudaMemsetAsync(J, 0, sizeof(double) * static_cast<size_t>(runs) * vp.P * R,
+                                     stream), "adjoint jacobian: clear J");
+    if (rc != MKB_OK) return rc;
+    rc = launch_residuals(tp, records, r0, R, nullptr, status, exact, stream);
+    if (rc != MKB_OK) return rc;
+    rc = launch_adjoint_rows(tp, vp, R, records, J, exact, stream);
+    if (rc != MKB_OK) return rc;
+    return launch_projection(tp, vp, R, status, J, exact, stream);
+}
+
+}  // extern "C"

@@ -14,6 +14,7 @@
 // (src/cuda/residuals.cu:57, src/cuda/merit.cu:62,206), batch_ray_opl (merit/ray_residual.hpp:69),
 // opd_statistics (merit/opd.hpp:37), ray_residual / ray_penalty (merit/ray_residual.hpp:131,199).
 #include "common.cuh"
+#include "pupil.cuh"
 
 #include <cstdio>
 #include <mutex>
@@ -26,15 +27,6 @@ namespace {
 constexpr int kThreads = 128;
 constexpr int kRaysPerThread = 4;
 constexpr int kPackRays = kThreads * kRaysPerThread;
-
-// Shared pupil tables copied from the parameter block once per CTA.
-struct SharedTables {
-    double rho[kMaxRings];
-    double w_axis[kMaxRings], rw_axis[kMaxRings];
-    double w_spoke[kMaxRings], rw_spoke[kMaxRings];
-    double sin_half[kMaxSpokes], cos_half[kMaxSpokes];
-    double sin_full[kMaxSpokes], cos_full[kMaxSpokes];
-};
 
 // The bulk-copy destination `record` must start on a 16-byte boundary: it is the first
 // member of a 16-byte aligned struct (checked below).
@@ -49,53 +41,6 @@ struct alignas(16) SharedTrace {
 };
 static_assert(offsetof(SharedTrace, record) % 16 == 0, "bulk-copy destination alignment");
 static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
-
-__device__ inline void copy_tables(const TraceParams& p, SharedTables& t) {
-    for (int i = threadIdx.x; i < kMaxRings; i += blockDim.x) {
-        t.rho[i] = p.rho[i];
-        t.w_axis[i] = p.w_axis[i];
-        t.rw_axis[i] = p.rw_axis[i];
-        t.w_spoke[i] = p.w_spoke[i];
-        t.rw_spoke[i] = p.rw_spoke[i];
-    }
-    for (int i = threadIdx.x; i < kMaxSpokes; i += blockDim.x) {
-        t.sin_half[i] = p.sin_half[i];
-        t.cos_half[i] = p.cos_half[i];
-        t.sin_full[i] = p.sin_full[i];
-        t.cos_full[i] = p.cos_full[i];
-    }
-}
-
-// Sample k of field f: rho, weight and sin/cos of the azimuth (pupil/quadrature.hpp:71).
-struct Sample {
-    double rho, weight, root_weight, sin_phi, cos_phi;
-};
-
-__device__ inline Sample pupil_sample(const TraceParams& p, const SharedTables& t, int f, int k) {
-    Sample s;
-    const int mode = p.pupil_mode[f];
-    if (mode == MKB_PUPIL_AXIS) {
-        s.rho = t.rho[k];
-        s.weight = t.w_axis[k];
-        s.root_weight = t.rw_axis[k];
-        s.sin_phi = 0.0;
-        s.cos_phi = 1.0;
-    } else {
-        const int i = k / p.spokes;
-        const int j = k - i * p.spokes;
-        s.rho = t.rho[i];
-        s.weight = t.w_spoke[i];
-        s.root_weight = t.rw_spoke[i];
-        if (mode == MKB_PUPIL_HALF) {
-            s.sin_phi = t.sin_half[j];
-            s.cos_phi = t.cos_half[j];
-        } else {
-            s.sin_phi = t.sin_full[j];
-            s.cos_phi = t.cos_full[j];
-        }
-    }
-    return s;
-}
 
 // Trace of one ray to the reference sphere in number type N (trace_to_reference_sphere,
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
@@ -145,8 +90,8 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const R
             else if (status == kOk) status = rst;
         }
     }
-    opl = value(r.opl);
-    penalty = value(soft.penalty);
+    opl = value_of(r.opl);
+    penalty = value_of(soft.penalty);
     return status;
 }
 
@@ -240,8 +185,8 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                         s_acc += w * N(sh.opl[base + k]);
                     }
                 }
-                vw = value(w_acc);
-                vs = value(s_acc);
+                vw = value_of(w_acc);
+                vs = value_of(s_acc);
             }
             vw = __shfl_sync(0xffffffffu, vw, 0);
             vs = __shfl_sync(0xffffffffu, vs, 0);
@@ -257,7 +202,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
             vs = warp_sum(vs);
         }
         const bool valid = vw > 0.0;
-        const N piston = valid ? value(N(vs) / N(vw)) : 0.0;
+        const N piston = valid ? value_of(N(vs) / N(vw)) : 0.0;
         const N scale = p.scale[tu];
         const N pscale = p.pscale[tu];
         double sq = 0.0, psq = 0.0;
@@ -279,17 +224,17 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
             hard += !in_piston(st);
             if (kResiduals) {
                 const int64_t row = static_cast<int64_t>(v) * out.stride + row0 + k;
-                out.residuals[row] = value(r);
-                if (soft_mode) out.residuals[row + p.rays] = value(pr);
+                out.residuals[row] = value_of(r);
+                if (soft_mode) out.residuals[row + p.rays] = value_of(pr);
                 const int64_t ray = static_cast<int64_t>(v) * p.rays + row0 + k;
-                if (out.opd) out.opd[ray] = value(e);
+                if (out.opd) out.opd[ray] = value_of(e);
                 if (out.status) out.status[ray] = static_cast<uint8_t>(st);
             } else if (kExact) {
-                sh.opl[base + k] = value(r);  // each lane rewrites only its own samples
-                sh.pen[base + k] = value(pr);
+                sh.opl[base + k] = value_of(r);  // each lane rewrites only its own samples
+                sh.pen[base + k] = value_of(pr);
             } else {
-                sq += value(r * r);
-                psq += value(pr * pr);
+                sq += value_of(r * r);
+                psq += value_of(pr * pr);
             }
         }
         if (!kResiduals) {
@@ -308,7 +253,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                         }
                         tuple += pen;
                     }
-                    sq = value(tuple);
+                    sq = value_of(tuple);
                 }
             } else {
                 sq = warp_sum(sq);

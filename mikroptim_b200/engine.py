@@ -170,3 +170,73 @@ def _device_status() -> None:
     lib = _capi.lib()
     lib.mkb_device_status.restype = C.c_int
     _capi.check(lib.mkb_device_status(), "device status")
+
+
+# ---- Jacobians and normal equations (device) --------------------------------------------
+def _dev_f64(a, device):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(device)
+
+
+def fd_jacobian_device(templates: DeviceSystemBatch, layout: ResidualLayout,
+                       host: SystemBatchHost, variables, x0, chunk_runs: int | None = None,
+                       stream=None):
+    """Central-difference Jacobian of runs x0 [runs][P] (DeviceFdJacobian::compute).
+    Returns device tensors J [runs][P][R], r0 [runs][R], status_changes [runs][P]."""
+    lib = _capi.lib()
+    dev = templates.device
+    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    runs, P = x0.shape
+    R = layout.trace_rows
+    b = templates.c_struct()
+    plan = layout.plan(host)
+    chunk = runs if chunk_runs is None else chunk_runs
+    need = int(lib.mkb_fd_jacobian_workspace_bytes(C.byref(b), C.byref(plan), P, runs, chunk))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    J = torch.empty((runs, P, R), dtype=torch.float64, device=dev)
+    r0 = torch.empty((runs, R), dtype=torch.float64, device=dev)
+    ch = torch.empty((runs, P), dtype=torch.int64, device=dev)
+    vs = variables.c_struct()
+    rc = lib.mkb_fd_jacobian_device(C.byref(b), C.byref(plan), C.byref(vs),
+                                    C.c_void_p(x0.data_ptr()), runs, C.c_void_p(J.data_ptr()),
+                                    C.c_void_p(r0.data_ptr()), C.c_void_p(ch.data_ptr()),
+                                    C.c_void_p(ws.data_ptr()), ws.numel(), _stream_handle(stream))
+    _capi.check(rc, "fd jacobian")
+    return J, r0, ch
+
+
+def adjoint_jacobian_device(templates: DeviceSystemBatch, layout: ResidualLayout,
+                            host: SystemBatchHost, variables, x0, stream=None):
+    """Adjoint Jacobian of runs x0 [runs][P] (DeviceAdjointJacobian::compute).
+    Returns device tensors J [runs][P][R], r0 [runs][R], status [runs][rays]."""
+    lib = _capi.lib()
+    dev = templates.device
+    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    runs, P = x0.shape
+    R = layout.trace_rows
+    b = templates.c_struct()
+    plan = layout.plan(host)
+    need = int(lib.mkb_adjoint_jacobian_workspace_bytes(C.byref(b), runs))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    J = torch.empty((runs, P, R), dtype=torch.float64, device=dev)
+    r0 = torch.empty((runs, R), dtype=torch.float64, device=dev)
+    st = torch.empty((runs, layout.rays_per_variant), dtype=torch.uint8, device=dev)
+    vs = variables.c_struct()
+    rc = lib.mkb_adjoint_jacobian_device(C.byref(b), C.byref(plan), C.byref(vs),
+                                         C.c_void_p(x0.data_ptr()), runs,
+                                         C.c_void_p(J.data_ptr()), C.c_void_p(r0.data_ptr()),
+                                         C.c_void_p(st.data_ptr()), C.c_void_p(ws.data_ptr()),
+                                         ws.numel(), _stream_handle(stream))
+    _capi.check(rc, "adjoint jacobian")
+    return J, r0, st
+
+
+def normal_equations_device(J: torch.Tensor, r: torch.Tensor, exact: bool = True, stream=None):
+    """gram [runs][P+1][P+1] = [J r]^T [J r] (DeviceNormalEquations::compute)."""
+    lib = _capi.lib()
+    runs, P, R = J.shape
+    gram = torch.empty((runs, P + 1, P + 1), dtype=torch.float64, device=J.device)
+    rc = lib.mkb_normal_equations_device(C.c_void_p(J.data_ptr()), C.c_void_p(r.data_ptr()),
+                                         runs, P, R, C.c_void_p(gram.data_ptr()), int(exact),
+                                         _stream_handle(stream))
+    _capi.check(rc, "normal equations")
+    return gram
