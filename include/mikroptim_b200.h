@@ -186,6 +186,50 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
                                 double* J, double* r0, uint8_t* status, void* workspace,
                                 size_t workspace_bytes, void* stream);
 
+/* ---- batched Levenberg-Marquardt ------------------------------------------------------------
+ * LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85) for one pass (no outer
+ * soft-failure penalty rounds), and the per-run state kept in a caller workspace. The device
+ * loop replaces the host loop of levenberg_marquardt (src/optim/levenberg_marquardt.cpp:332)
+ * with GpuLmBackend (src/cuda/levenberg_marquardt.cpp): mkb_lm_start_device evaluates the
+ * merit at x0, each mkb_lm_cycle_device performs one LM cycle for every run (Jacobian and
+ * normal equations, damped active-set Cholesky step, trial MERIT, acceptance with Nielsen
+ * damping) as a fixed sequence of launches, so cycles can be captured in a CUDA graph.
+ * With precision FP64 and gram_exact = 1 every run follows the reference's trajectory bit
+ * for bit. Status values are LmStatus (0 running, 1 converged_merit, 2 converged_step,
+ * 3 converged_gradient, 5 max_iterations, 6 damping_limit, 7 numerical_error). */
+enum { MKB_JACOBIAN_FD = 0, MKB_JACOBIAN_ADJOINT = 1 };
+typedef struct mkb_lm_options {
+    int32_t max_iterations;           /* 100 */
+    int32_t reject_new_failures;      /* 1 */
+    double ftol, xtol, gtol;          /* 1e-10 each */
+    double initial_damping;           /* 1e-3 */
+    double max_damping;               /* 1e16 */
+    double diag_floor;                /* 1e-12 */
+    int32_t jacobian;                 /* MKB_JACOBIAN_* */
+    int32_t gram_exact;               /* 1: FMA-chain normal equations, 0: FP64 DMMA */
+} mkb_lm_options;
+
+size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                              const mkb_variables* vars, const mkb_lm_options* options,
+                              int32_t runs);
+int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options,
+                        const double* x0, int32_t runs, void* workspace, size_t workspace_bytes,
+                        void* stream);
+int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                        void* workspace, size_t workspace_bytes, void* stream);
+/* Copies the run results out of the workspace (any output may be NULL; host or device
+ * pointers): x [runs][P], merit, status, iterations, accepted, jacobians, damping mu,
+ * history [runs][max_iterations + 1] (NaN-padded), failed / hard-failed rays, and `running`
+ * (one int: runs still running after the last cycle). */
+int mkb_lm_results_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                          const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                          const void* workspace, double* x, double* merit, int32_t* status,
+                          int32_t* iterations, int32_t* accepted, int32_t* jacobians,
+                          double* damping, double* history, int64_t* failed,
+                          int64_t* hard_failed, int32_t* running, void* stream);
+
 /* ---- normal equations --------------------------------------------------------------------
  * gram [runs][P+1][P+1] = [J r]^T [J r] for J [runs][P][R] (column p of run i at
  * J + (i*P + p)*R) and r [runs][R]: A = J^T J in the top-left block, g = J^T r in column P.

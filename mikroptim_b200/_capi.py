@@ -87,6 +87,18 @@ class Variables(C.Structure):
     ]
 
 
+class LmOptions(C.Structure):
+    """mkb_lm_options (LmOptions, levenberg_marquardt.hpp:85)."""
+
+    _fields_ = [
+        ("max_iterations", C.c_int32), ("reject_new_failures", C.c_int32),
+        ("ftol", C.c_double), ("xtol", C.c_double), ("gtol", C.c_double),
+        ("initial_damping", C.c_double), ("max_damping", C.c_double),
+        ("diag_floor", C.c_double),
+        ("jacobian", C.c_int32), ("gram_exact", C.c_int32),
+    ]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -133,6 +145,18 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_adjoint_jacobian_device.argtypes = [PB, PP, PV, c.c_void_p, c.c_int32, c.c_void_p,
                                                 c.c_void_p, c.c_void_p, c.c_void_p, c.c_size_t,
                                                 c.c_void_p]
+    PO = C.POINTER(LmOptions)
+    lib.mkb_lm_workspace_bytes.restype = c.c_size_t
+    lib.mkb_lm_workspace_bytes.argtypes = [PB, PP, PV, PO, c.c_int32]
+    lib.mkb_lm_start_device.restype = c.c_int
+    lib.mkb_lm_start_device.argtypes = [PB, PP, PV, PO, c.c_void_p, c.c_int32, c.c_void_p,
+                                        c.c_size_t, c.c_void_p]
+    lib.mkb_lm_cycle_device.restype = c.c_int
+    lib.mkb_lm_cycle_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,
+                                        c.c_void_p]
+    lib.mkb_lm_results_device.restype = c.c_int
+    lib.mkb_lm_results_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p] + \
+        [c.c_void_p] * 11 + [c.c_void_p]
     lib.mkb_normal_equations_device.restype = c.c_int
     lib.mkb_normal_equations_device.argtypes = [c.c_void_p, c.c_void_p, c.c_int32, c.c_int32,
                                                 c.c_int64, c.c_void_p, c.c_int32, c.c_void_p]

@@ -23,6 +23,7 @@ int trace_device_error();
 int gram_device_error();
 int adjoint_device_error();
 int jacobian_device_error();
+int lm_device_error();
 
 namespace {
 thread_local std::string g_error;
@@ -316,7 +317,7 @@ int64_t mkb_launch_count(void) { return g_launches.load(); }
 
 int mkb_device_status(void) {
     int (*readers[])() = {trace_device_error, gram_device_error, adjoint_device_error,
-                              jacobian_device_error};
+                              jacobian_device_error, lm_device_error};
     int status = MKB_OK;
     for (auto read : readers) {
         const int v = read();

@@ -1,0 +1,718 @@
+// Batched Levenberg-Marquardt on the device.
+//
+// The control logic of the reference's levenberg_marquardt (src/optim/levenberg_marquardt.cpp:
+// 332-589) runs per run on the GPU, with every run's decisions depending only on its own state:
+//   lm_update_kernel  one CTA per run: new normal equations -> prepare_step (Marquardt scaling,
+//                     projected gradient), the Gauss-Newton model solve (mu = 1e-12) and the
+//                     gtol / ftol / xtol tests, then the damped active-set step solve_step(mu)
+//                     with the trial point clamp(x + delta)
+//   (trial MERIT)     the trace kernels, launched by the entry point
+//   lm_accept_kernel  one thread per run: gain ratio, acceptance, Nielsen damping update
+// Every operation of prepare_step, cholesky, cholesky_solve and solve_step is a separately
+// rounded IEEE operation in the reference's order (sequential where the reference sums
+// sequentially), so with bit-identical normal equations and merits the run trajectories equal
+// the reference's host loop bit for bit. One cycle is a fixed sequence of launches with
+// per-run masks (no host decisions), so a cycle can be captured in a CUDA graph.
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace mkb {
+
+// LmStatus (include/mikroptim/optim/levenberg_marquardt.hpp:26)
+enum : int { kRunning = 0, kConvergedMerit = 1, kConvergedStep = 2, kConvergedGradient = 3,
+             kConvergedStall = 4, kMaxIterations = 5, kDampingLimit = 6, kNumericalError = 7 };
+
+struct LmOptionsDev {
+    int max_iterations;
+    double ftol, xtol, gtol, initial_damping, max_damping, diag_floor;
+    int reject_new_failures;
+};
+
+// Per-run LM state in the workspace (structure of arrays).
+struct LmState {
+    double* x;          // [runs][P]
+    double* trial;      // [runs][P]
+    double* a;          // [runs][P][P]   J^T J (column-major, as the reference)
+    double* g;          // [runs][P]
+    double* d;          // [runs][P]      Marquardt scaling
+    double* merit;      // [runs]
+    double* mu;         // [runs]
+    double* nu;         // [runs]
+    double* predicted;  // [runs]
+    double* step_norm;  // [runs]
+    double* step_damping;
+    double* gradient_norm;
+    double* model_decrease;
+    double* history;    // [runs][max_iterations + 1]
+    int64_t* failed;    // [runs]
+    int64_t* hard;      // [runs]
+    int* status;        // [runs] LmStatus
+    int* iterations;
+    int* accepted;
+    int* jacobians;
+    int* need_jacobian;
+    int* rejected;
+    int* solved;
+    int* in_cycle;      // this cycle took a trial step
+    int* evaluate;      // this cycle's trial point is evaluated
+    int* running;       // [1] runs still running after the last cycle
+};
+
+namespace {
+
+constexpr int kStepThreads = 64;
+constexpr int kMaxP = MKB_MAX_VARIABLES;
+constexpr double kModelDamping = 1e-12;
+
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }  // std::max
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }  // std::min
+
+__device__ __forceinline__ Exact64 scale_of(double x, double typical) {
+    return Exact64(dmax(fabs(x), typical));
+}
+
+__device__ __forceinline__ bool bound_blocks(const VarParams& v, int k, double x, double dir) {
+    if (v.lower[k] == v.upper[k]) return true;
+    return (x <= v.lower[k] && dir < 0.0) || (x >= v.upper[k] && dir > 0.0);
+}
+
+struct StepShared {
+    double m[kMaxP * kMaxP];  // damped free block, column-major lower triangle
+    double rhs[kMaxP];
+    double delta[kMaxP];
+    double step[kMaxP];
+    double aq[kMaxP];
+    int idx[kMaxP];
+    int fixed[kMaxP];
+    int f;
+    int changed;
+    int ok;
+};
+
+// solve_step (levenberg_marquardt.cpp:149) for one run, by one CTA. a, g, d, x of the run.
+// Writes trial, and returns solved / step_norm / predicted through shared memory.
+__device__ void solve_step(const VarParams& v, const double* a, const double* g, const double* d,
+                           const double* x, double mu, double* trial, StepShared& sh,
+                           int& solved, double& step_norm, double& predicted) {
+    const int n = v.P;
+    const int tid = threadIdx.x;
+    for (int k = tid; k < n; k += blockDim.x) sh.fixed[k] = bound_blocks(v, k, x[k], -g[k]) ? 1 : 0;
+    __syncthreads();
+    solved = 1;
+    for (int round = 0; round <= n; ++round) {
+        if (tid == 0) {
+            int f = 0;
+            for (int k = 0; k < n; ++k)
+                if (!sh.fixed[k]) sh.idx[f++] = k;
+            sh.f = f;
+        }
+        for (int k = tid; k < n; k += blockDim.x) sh.delta[k] = 0.0;
+        __syncthreads();
+        const int f = sh.f;
+        if (f == 0) break;
+        // m = lower triangle of A_FF + mu D_FF, rhs = -g_F
+        for (int e = tid; e < f * f; e += blockDim.x) {
+            const int j = e / f, i = e - j * f;
+            if (i >= j) {
+                double val = a[sh.idx[j] * n + sh.idx[i]];
+                if (i == j) val = (Exact64(val) + Exact64(mu) * Exact64(d[sh.idx[j]])).v;
+                sh.m[j * f + i] = val;
+            }
+        }
+        for (int j = tid; j < f; j += blockDim.x) sh.rhs[j] = -g[sh.idx[j]];
+        if (tid == 0) sh.ok = 1;
+        __syncthreads();
+        // cholesky (levenberg_marquardt.cpp:70): column j, diagonal by one thread, then the
+        // rows i > j in parallel; every sum in ascending k
+        for (int j = 0; j < f; ++j) {
+            if (tid == 0) {
+                Exact64 diag = sh.m[j * f + j];
+                for (int k = 0; k < j; ++k) diag -= Exact64(sh.m[k * f + j]) * Exact64(sh.m[k * f + j]);
+                if (!(diag.v > 0.0) || !isfinite(diag.v)) sh.ok = 0;
+                else sh.m[j * f + j] = nsqrt(diag).v;
+            }
+            __syncthreads();
+            if (!sh.ok) break;
+            const Exact64 ljj = sh.m[j * f + j];
+            for (int i = j + 1 + tid; i < f; i += blockDim.x) {
+                Exact64 s = sh.m[j * f + i];
+                for (int k = 0; k < j; ++k) s -= Exact64(sh.m[k * f + i]) * Exact64(sh.m[k * f + j]);
+                sh.m[j * f + i] = (s / ljj).v;
+            }
+            __syncthreads();
+        }
+        if (!sh.ok) {
+            solved = 0;
+            __syncthreads();
+            return;
+        }
+        // cholesky_solve (levenberg_marquardt.cpp:94): L z = b column-oriented (each b[j]
+        // subtracts l[k][j] b[k] for k ascending, as the row loop does), L^T y = z row by row
+        for (int i = 0; i < f; ++i) {
+            if (tid == 0) sh.rhs[i] = (Exact64(sh.rhs[i]) / Exact64(sh.m[i * f + i])).v;
+            __syncthreads();
+            const Exact64 bi = sh.rhs[i];
+            for (int j = i + 1 + tid; j < f; j += blockDim.x)
+                sh.rhs[j] = (Exact64(sh.rhs[j]) - Exact64(sh.m[i * f + j]) * bi).v;
+            __syncthreads();
+        }
+        if (tid == 0) {
+            for (int i = f - 1; i >= 0; --i) {
+                Exact64 s = sh.rhs[i];
+                for (int k = i + 1; k < f; ++k) s -= Exact64(sh.m[i * f + k]) * Exact64(sh.rhs[k]);
+                sh.rhs[i] = (s / Exact64(sh.m[i * f + i])).v;
+            }
+            sh.changed = 0;
+        }
+        __syncthreads();
+        for (int j = tid; j < f; j += blockDim.x) sh.delta[sh.idx[j]] = sh.rhs[j];
+        __syncthreads();
+        if (tid == 0) {
+            int changed = 0;
+            for (int j = 0; j < f; ++j) {
+                const int k = sh.idx[j];
+                if (bound_blocks(v, k, x[k], sh.delta[k])) {
+                    sh.fixed[k] = 1;
+                    changed = 1;
+                }
+            }
+            sh.changed = changed;
+        }
+        __syncthreads();
+        if (!sh.changed) break;
+    }
+    // trial point, step norm, predicted decrease -(2 step.g + step.A.step)
+    for (int k = tid; k < n; k += blockDim.x) {
+        const double t = dmin(dmax((Exact64(x[k]) + Exact64(sh.delta[k])).v, v.lower[k]), v.upper[k]);
+        trial[k] = t;
+        sh.step[k] = (Exact64(t) - Exact64(x[k])).v;
+    }
+    __syncthreads();
+    for (int q = tid; q < n; q += blockDim.x) {
+        Exact64 s = 0.0;
+        for (int p = 0; p < n; ++p) s += Exact64(a[q * n + p]) * Exact64(sh.step[p]);
+        sh.aq[q] = s.v;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double norm = 0.0;
+        for (int k = 0; k < n; ++k)
+            norm = dmax(norm, (Exact64(fabs(sh.step[k])) / scale_of(x[k], v.typical[k])).v);
+        Exact64 lin = 0.0, quad = 0.0;
+        for (int q = 0; q < n; ++q) {
+            lin += Exact64(sh.step[q]) * Exact64(g[q]);
+            quad += Exact64(sh.step[q]) * Exact64(sh.aq[q]);
+        }
+        step_norm = norm;
+        predicted = (-(Exact64(2.0) * lin + quad)).v;
+        sh.ok = 1;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kStepThreads)
+lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st,
+                 const double* __restrict__ gram, int runs) {
+    __shared__ StepShared sh;
+    __shared__ double s_pred, s_norm;
+    __shared__ int s_solved, s_status;
+    const int run = blockIdx.x;
+    if (run >= runs) return;
+    const int n = v.P;
+    const int tid = threadIdx.x;
+    double* x = st.x + static_cast<int64_t>(run) * n;
+    double* trial = st.trial + static_cast<int64_t>(run) * n;
+    double* a = st.a + static_cast<int64_t>(run) * n * n;
+    double* g = st.g + static_cast<int64_t>(run) * n;
+    double* d = st.d + static_cast<int64_t>(run) * n;
+    int status = st.status[run];
+    const double merit = st.merit[run];
+    // ---- new normal equations ----
+    if (status == kRunning && st.need_jacobian[run] && st.iterations[run] < o.max_iterations) {
+        const double* G = gram + static_cast<int64_t>(run) * (n + 1) * (n + 1);
+        __shared__ int s_finite;
+        if (tid == 0) s_finite = 1;
+        __syncthreads();
+        for (int e = tid; e < n * n; e += blockDim.x) {
+            const int q = e / n, p = e - q * n;
+            const double val = G[q * (n + 1) + p];
+            a[e] = val;
+            if (!isfinite(val)) s_finite = 0;
+        }
+        for (int q = tid; q < n; q += blockDim.x) {
+            const double val = G[q * (n + 1) + n];
+            g[q] = val;
+            if (!isfinite(val)) s_finite = 0;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            st.need_jacobian[run] = 0;
+            st.jacobians[run] += 1;
+        }
+        if (!s_finite) {
+            status = kNumericalError;
+        } else {
+            // prepare_step (levenberg_marquardt.cpp:122)
+            if (tid == 0) {
+                double smax = 0.0;
+                for (int k = 0; k < n; ++k) {
+                    const Exact64 sk = scale_of(x[k], v.typical[k]);
+                    smax = dmax(smax, (Exact64(a[k * n + k]) * sk * sk).v);
+                }
+                double gmax = 0.0;
+                for (int k = 0; k < n; ++k) {
+                    const Exact64 sk = scale_of(x[k], v.typical[k]);
+                    const double akk = a[k * n + k];
+                    const double floor = smax > 0.0
+                                             ? (Exact64(o.diag_floor) * Exact64(smax) / (sk * sk)).v
+                                             : (Exact64(1.0) / (sk * sk)).v;
+                    d[k] = dmax(akk, floor);
+                    if (!bound_blocks(v, k, x[k], -g[k])) {
+                        const double denom = nsqrt(Exact64(akk) * Exact64(merit)).v;
+                        if (denom > 0.0) gmax = dmax(gmax, (Exact64(fabs(g[k])) / Exact64(denom)).v);
+                    }
+                }
+                st.gradient_norm[run] = gmax;
+            }
+            __syncthreads();
+            int solved;
+            double norm, pred;
+            solve_step(v, a, g, d, x, kModelDamping, trial, sh, solved, norm, pred);
+            if (tid == 0) {
+                st.model_decrease[run] = solved ? (Exact64(pred) / Exact64(merit)).v : nan("");
+                if (st.gradient_norm[run] <= o.gtol) status = kConvergedGradient;
+                else if (solved && pred >= 0.0 && pred <= (Exact64(o.ftol) * Exact64(merit)).v)
+                    status = kConvergedMerit;
+                else if (solved && norm <= o.xtol) status = kConvergedStep;
+                s_status = status;
+            }
+            __syncthreads();
+            status = s_status;
+        }
+    }
+    // ---- trial step ----
+    int in_cycle = 0, evaluate = 0;
+    if (status == kRunning) {
+        if (st.iterations[run] >= o.max_iterations) {
+            status = kMaxIterations;
+        } else {
+            in_cycle = 1;
+            int solved;
+            double norm, pred;
+            solve_step(v, a, g, d, x, st.mu[run], trial, sh, solved, norm, pred);
+            if (tid == 0) {
+                s_solved = solved;
+                s_norm = norm;
+                s_pred = pred;
+            }
+            __syncthreads();
+            if (s_solved && st.rejected[run] && s_norm <= o.xtol) status = kConvergedStep;
+            else if (s_solved) evaluate = 1;
+        }
+    }
+    if (tid == 0) {
+        st.status[run] = status;
+        st.in_cycle[run] = in_cycle && status != kConvergedStep;
+        st.evaluate[run] = evaluate;
+        if (in_cycle) {
+            st.solved[run] = s_solved;
+            st.step_norm[run] = s_norm;
+            st.predicted[run] = s_pred;
+            st.step_damping[run] = st.mu[run];
+        }
+    }
+}
+
+// Acceptance (levenberg_marquardt.cpp:518-545) after the trial MERIT.
+__global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double* trial_merit,
+                                 const int64_t* trial_failed, const int64_t* trial_hard,
+                                 int runs) {
+    const int run = blockIdx.x * blockDim.x + threadIdx.x;
+    if (run >= runs) return;
+    if (!st.in_cycle[run]) {
+        if (st.status[run] == kRunning) atomicAdd(st.running, 1);
+        return;
+    }
+    st.iterations[run] += 1;
+    bool accept = false;
+    if (st.solved[run]) {
+        const double f_new = trial_merit[run];
+        const double merit = st.merit[run];
+        const double pred = st.predicted[run];
+        const double rho = (Exact64(merit) - Exact64(f_new)).v / pred;
+        accept = isfinite(f_new) && pred > 0.0 && f_new < merit &&
+                 !(o.reject_new_failures && trial_hard[run] > st.hard[run]);
+        if (accept) {
+            for (int k = 0; k < P; ++k)
+                st.x[static_cast<int64_t>(run) * P + k] = st.trial[static_cast<int64_t>(run) * P + k];
+            st.merit[run] = f_new;
+            st.failed[run] = trial_failed[run];
+            st.hard[run] = trial_hard[run];
+            const Exact64 t = Exact64(2.0) * Exact64(rho) - Exact64(1.0);
+            st.mu[run] = (Exact64(st.mu[run]) *
+                          Exact64(dmax(1.0 / 3.0, (Exact64(1.0) - t * t * t).v))).v;
+            st.nu[run] = 2.0;
+            st.need_jacobian[run] = 1;
+            st.rejected[run] = 0;
+            st.accepted[run] += 1;
+            if (f_new == 0.0) st.status[run] = kConvergedMerit;
+        }
+    }
+    if (!accept) {
+        st.mu[run] = (Exact64(st.mu[run]) * Exact64(st.nu[run])).v;
+        st.nu[run] = (Exact64(st.nu[run]) * Exact64(2.0)).v;
+        st.rejected[run] = 1;
+        if (st.mu[run] > o.max_damping) st.status[run] = kDampingLimit;
+    }
+    st.history[static_cast<int64_t>(run) * (o.max_iterations + 1) + st.iterations[run]] =
+        st.merit[run];
+    if (st.status[run] == kRunning) atomicAdd(st.running, 1);
+}
+
+// Start: merit at x0 (already evaluated into merit/failed/hard), status, damping.
+__global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* x0, int runs) {
+    const int run = blockIdx.x * blockDim.x + threadIdx.x;
+    if (run >= runs) return;
+    for (int k = 0; k < P; ++k) {
+        const double xv = x0[static_cast<int64_t>(run) * P + k];
+        st.x[static_cast<int64_t>(run) * P + k] = xv;
+        st.trial[static_cast<int64_t>(run) * P + k] = xv;
+    }
+    const double m = st.merit[run];
+    int status = kRunning;
+    if (!isfinite(m)) status = kNumericalError;
+    else if (m == 0.0) status = kConvergedMerit;
+    st.status[run] = status;
+    st.mu[run] = o.initial_damping;
+    st.nu[run] = 2.0;
+    st.need_jacobian[run] = 1;
+    st.rejected[run] = 0;
+    st.iterations[run] = st.accepted[run] = st.jacobians[run] = 0;
+    st.gradient_norm[run] = 0.0;
+    st.model_decrease[run] = nan("");
+    st.history[static_cast<int64_t>(run) * (o.max_iterations + 1)] = m;
+    for (int h = 1; h <= o.max_iterations; ++h)
+        st.history[static_cast<int64_t>(run) * (o.max_iterations + 1) + h] = nan("");
+    if (status == kRunning) atomicAdd(st.running, 1);
+}
+
+}  // namespace
+
+int launch_lm_init(const LmOptionsDev& o, const LmState& st, int P, const double* x0, int runs,
+                   cudaStream_t stream) {
+    lm_init_kernel<<<(runs + 127) / 128, 128, 0, stream>>>(o, st, P, x0, runs);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "lm init launch");
+}
+
+int launch_lm_update(const VarParams& v, const LmOptionsDev& o, const LmState& st,
+                     const double* gram, int runs, cudaStream_t stream) {
+    lm_update_kernel<<<runs, kStepThreads, 0, stream>>>(v, o, st, gram, runs);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "lm update launch");
+}
+
+int launch_lm_accept(const LmOptionsDev& o, const LmState& st, int P, const double* trial_merit,
+                     const int64_t* trial_failed, const int64_t* trial_hard, int runs,
+                     cudaStream_t stream) {
+    lm_accept_kernel<<<(runs + 127) / 128, 128, 0, stream>>>(o, st, P, trial_merit, trial_failed,
+                                                             trial_hard, runs);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "lm accept launch");
+}
+
+MKB_DEFINE_ERROR_READER(lm_device_error)
+
+}  // namespace mkb
+
+// ---- entry points ------------------------------------------------------------------------------
+namespace mkb {
+
+int launch_residuals(const TraceParams& p, const double* records, double* residuals,
+                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     cudaStream_t stream);
+int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
+                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 cudaStream_t stream);
+size_t merit_workspace_bytes(int V, int n_tuples);
+int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
+                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
+int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
+                        const double* records, double* J, bool exact, cudaStream_t stream);
+int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
+                      const uint8_t* status, double* J, bool exact, cudaStream_t stream);
+int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
+                bool exact, cudaStream_t stream);
+int pack_rays_default();
+
+namespace {
+
+size_t al(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+
+struct LmLayout {
+    size_t total;
+    LmState st;
+    double* gram;
+    double* J;
+    double* r0;
+    uint8_t* status;
+    double* records;
+    void* merit_ws;
+    size_t merit_ws_bytes;
+    double* trial_merit;
+    int64_t* trial_failed;
+    int64_t* trial_hard;
+    void* fd_ws;
+    size_t fd_ws_bytes;
+};
+
+constexpr int kFdChunkRuns = 64;
+
+// Carves the workspace (base may be null to only size it).
+LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_it, bool fd,
+                   const mkb_device_batch* templates, const mkb_residual_plan* plan) {
+    LmLayout L{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base ? base + off : nullptr;
+        off += al(bytes);
+        return p;
+    };
+    const size_t r = static_cast<size_t>(runs);
+    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    L.st.x = reinterpret_cast<double*>(take(8 * r * P));
+    L.st.trial = reinterpret_cast<double*>(take(8 * r * P));
+    L.st.a = reinterpret_cast<double*>(take(8 * r * P * P));
+    L.st.g = reinterpret_cast<double*>(take(8 * r * P));
+    L.st.d = reinterpret_cast<double*>(take(8 * r * P));
+    L.st.merit = reinterpret_cast<double*>(take(8 * r));
+    L.st.mu = reinterpret_cast<double*>(take(8 * r));
+    L.st.nu = reinterpret_cast<double*>(take(8 * r));
+    L.st.predicted = reinterpret_cast<double*>(take(8 * r));
+    L.st.step_norm = reinterpret_cast<double*>(take(8 * r));
+    L.st.step_damping = reinterpret_cast<double*>(take(8 * r));
+    L.st.gradient_norm = reinterpret_cast<double*>(take(8 * r));
+    L.st.model_decrease = reinterpret_cast<double*>(take(8 * r));
+    L.st.history = reinterpret_cast<double*>(take(8 * r * (max_it + 1)));
+    L.st.failed = reinterpret_cast<int64_t*>(take(8 * r));
+    L.st.hard = reinterpret_cast<int64_t*>(take(8 * r));
+    L.st.status = reinterpret_cast<int*>(take(4 * r));
+    L.st.iterations = reinterpret_cast<int*>(take(4 * r));
+    L.st.accepted = reinterpret_cast<int*>(take(4 * r));
+    L.st.jacobians = reinterpret_cast<int*>(take(4 * r));
+    L.st.need_jacobian = reinterpret_cast<int*>(take(4 * r));
+    L.st.rejected = reinterpret_cast<int*>(take(4 * r));
+    L.st.solved = reinterpret_cast<int*>(take(4 * r));
+    L.st.in_cycle = reinterpret_cast<int*>(take(4 * r));
+    L.st.evaluate = reinterpret_cast<int*>(take(4 * r));
+    L.st.running = reinterpret_cast<int*>(take(4));
+    L.gram = reinterpret_cast<double*>(take(8 * r * (P + 1) * (P + 1)));
+    L.J = reinterpret_cast<double*>(take(8 * r * P * R));
+    L.r0 = reinterpret_cast<double*>(take(8 * r * R));
+    L.status = reinterpret_cast<uint8_t*>(take(r * tp.rays));
+    L.records = reinterpret_cast<double*>(take(8 * r * tp.stride));
+    L.merit_ws_bytes = merit_workspace_bytes(runs, tp.n_tuples);
+    L.merit_ws = take(L.merit_ws_bytes);
+    L.trial_merit = reinterpret_cast<double*>(take(8 * r));
+    L.trial_failed = reinterpret_cast<int64_t*>(take(8 * r));
+    L.trial_hard = reinterpret_cast<int64_t*>(take(8 * r));
+    L.fd_ws_bytes = 0;
+    if (fd) {
+        mkb_device_batch t = *templates;
+        L.fd_ws_bytes = mkb_fd_jacobian_workspace_bytes(&t, plan, P, runs,
+                                                        runs < kFdChunkRuns ? runs : kFdChunkRuns);
+        L.fd_ws = take(L.fd_ws_bytes);
+    }
+    L.total = off;
+    return L;
+}
+
+struct LmSetup {
+    TraceParams tp;
+    VarParams vp;
+    LmOptionsDev o;
+    bool fd, exact, gram_exact;
+    int64_t R;
+};
+
+int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+             const mkb_variables* vars, const mkb_lm_options* options, int runs, LmSetup& s) {
+    if (templates == nullptr || options == nullptr || runs < 1) {
+        set_error("lm: null templates/options or runs < 1");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (templates->variants != 1 && templates->variants != runs) {
+        set_error("lm: templates must hold 1 variant or one per run");
+        return MKB_ERR_ARGUMENT;
+    }
+    mkb_device_batch b = *templates;
+    b.variants = runs;
+    int rc = make_trace_params(&b, plan, pack_rays_default(), &s.tp);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+        set_error("lm: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    rc = make_var_params(vars, s.tp.S, templates->type, &s.vp);
+    if (rc != MKB_OK) return rc;
+    const mkb_lm_options& o = *options;
+    auto ok = [](double v) { return std::isfinite(v) && v >= 0.0; };
+    if (o.max_iterations < 0 || !ok(o.ftol) || !ok(o.xtol) || !ok(o.gtol) || !ok(o.diag_floor) ||
+        !(o.initial_damping > 0.0) || !std::isfinite(o.initial_damping) ||
+        !(o.max_damping > o.initial_damping)) {
+        set_error("lm: invalid options (check_options, levenberg_marquardt.cpp:226)");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (o.jacobian != MKB_JACOBIAN_FD && o.jacobian != MKB_JACOBIAN_ADJOINT) {
+        set_error("lm: unknown jacobian method %d", o.jacobian);
+        return MKB_ERR_ARGUMENT;
+    }
+    s.o = {o.max_iterations, o.ftol, o.xtol, o.gtol, o.initial_damping, o.max_damping,
+           o.diag_floor, o.reject_new_failures};
+    s.fd = o.jacobian == MKB_JACOBIAN_FD;
+    s.exact = plan->precision == MKB_PRECISION_FP64;
+    s.gram_exact = o.gram_exact != 0;
+    s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
+    return MKB_OK;
+}
+
+// merit at the run points `x` (applied to the templates) into merit/failed/hard
+int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates,
+                const double* x, int runs, double* merit, int64_t* failed, int64_t* hard,
+                cudaStream_t stream) {
+    const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+    int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
+                          stream);
+    if (rc != MKB_OK) return rc;
+    return launch_merit(s.tp, L.records, merit, failed, hard, L.merit_ws, L.merit_ws_bytes,
+                        s.exact, stream);
+}
+
+}  // namespace
+}  // namespace mkb
+
+using namespace mkb;
+
+extern "C" {
+
+size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                              const mkb_variables* vars, const mkb_lm_options* options,
+                              int32_t runs) {
+    LmSetup s;
+    if (lm_setup(templates, plan, vars, options, runs, s) != MKB_OK) return 0;
+    return lm_layout(nullptr, s.tp, s.vp.P, runs, s.o.max_iterations, s.fd, templates, plan).total;
+}
+
+int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options,
+                        const double* x0, int32_t runs, void* workspace, size_t workspace_bytes,
+                        void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmSetup s;
+    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    if (rc != MKB_OK) return rc;
+    const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
+                                 s.o.max_iterations, s.fd, templates, plan);
+    if (workspace == nullptr || workspace_bytes < L.total || x0 == nullptr) {
+        set_error("lm: workspace of %zu bytes and x0 needed", L.total);
+        return MKB_ERR_WORKSPACE;
+    }
+    rc = lm_merit_at(s, L, templates, x0, runs, L.st.merit, L.st.failed, L.st.hard, stream);
+    if (rc != MKB_OK) return rc;
+    rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
+    if (rc != MKB_OK) return rc;
+    return launch_lm_init(s.o, L.st, s.vp.P, x0, runs, stream);
+}
+
+int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                        void* workspace, size_t workspace_bytes, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmSetup s;
+    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    if (rc != MKB_OK) return rc;
+    const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
+                                 s.o.max_iterations, s.fd, templates, plan);
+    if (workspace == nullptr || workspace_bytes < L.total) {
+        set_error("lm: workspace of %zu bytes needed", L.total);
+        return MKB_ERR_WORKSPACE;
+    }
+    // 1. Jacobian at x (every run; only runs that need one use it) and normal equations
+    if (s.fd) {
+        mkb_device_batch t = *templates;
+        mkb_residual_plan pl = *plan;
+        mkb_variables v = *vars;
+        rc = mkb_fd_jacobian_device(&t, &pl, &v, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
+                                    L.fd_ws_bytes, stream);
+    } else {
+        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
+                          runs, stream);
+        if (rc == MKB_OK)
+            rc = cuda_status(cudaMemsetAsync(L.J, 0, sizeof(double) * size_t(runs) * s.vp.P * s.R,
+                                             stream), "lm: clear J");
+        if (rc == MKB_OK)
+            rc = launch_residuals(s.tp, L.records, L.r0, s.R, nullptr, L.status, s.exact, stream);
+        if (rc == MKB_OK)
+            rc = launch_adjoint_rows(s.tp, s.vp, s.R, L.records, L.J, s.exact, stream);
+        if (rc == MKB_OK)
+            rc = launch_projection(s.tp, s.vp, s.R, L.status, L.J, s.exact, stream);
+    }
+    if (rc != MKB_OK) return rc;
+    rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream);
+    if (rc != MKB_OK) return rc;
+    // 2. step
+    rc = launch_lm_update(s.vp, s.o, L.st, L.gram, runs, stream);
+    if (rc != MKB_OK) return rc;
+    // 3. trial MERIT, 4. acceptance
+    rc = lm_merit_at(s, L, templates, L.st.trial, runs, L.trial_merit, L.trial_failed,
+                     L.trial_hard, stream);
+    if (rc != MKB_OK) return rc;
+    rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
+    if (rc != MKB_OK) return rc;
+    return launch_lm_accept(s.o, L.st, s.vp.P, L.trial_merit, L.trial_failed, L.trial_hard, runs,
+                            stream);
+}
+
+int mkb_lm_results_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                          const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                          const void* workspace, double* x, double* merit, int32_t* status,
+                          int32_t* iterations, int32_t* accepted, int32_t* jacobians,
+                          double* damping, double* history, int64_t* failed,
+                          int64_t* hard_failed, int32_t* running, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmSetup s;
+    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    if (rc != MKB_OK) return rc;
+    const LmLayout L = lm_layout(static_cast<char*>(const_cast<void*>(workspace)), s.tp, s.vp.P,
+                                 runs, s.o.max_iterations, s.fd, templates, plan);
+    const size_t r = static_cast<size_t>(runs);
+    struct Copy {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } copies[] = {
+        {x, L.st.x, 8 * r * s.vp.P},
+        {merit, L.st.merit, 8 * r},
+        {status, L.st.status, 4 * r},
+        {iterations, L.st.iterations, 4 * r},
+        {accepted, L.st.accepted, 4 * r},
+        {jacobians, L.st.jacobians, 4 * r},
+        {damping, L.st.mu, 8 * r},
+        {history, L.st.history, 8 * r * (s.o.max_iterations + 1)},
+        {failed, L.st.failed, 8 * r},
+        {hard_failed, L.st.hard, 8 * r},
+        {running, L.st.running, 4},
+    };
+    for (const Copy& c : copies) {
+        if (c.dst == nullptr) continue;
+        rc = cuda_status(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDefault, stream),
+                         "lm results copy");
+        if (rc != MKB_OK) return rc;
+    }
+    return MKB_OK;
+}
+
+}  // extern "C"

@@ -240,3 +240,129 @@ def normal_equations_device(J: torch.Tensor, r: torch.Tensor, exact: bool = True
                                          _stream_handle(stream))
     _capi.check(rc, "normal equations")
     return gram
+
+
+# ---- batched Levenberg-Marquardt (device) -------------------------------------------------
+JACOBIAN_FD, JACOBIAN_ADJOINT = 0, 1
+LM_STATUS = {0: "running", 1: "converged_merit", 2: "converged_step", 3: "converged_gradient",
+             4: "converged_stall", 5: "max_iterations", 6: "damping_limit",
+             7: "numerical_error"}
+
+
+@dataclass
+class LmOptions:
+    """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85), one penalty pass."""
+
+    max_iterations: int = 100
+    ftol: float = 1e-10
+    xtol: float = 1e-10
+    gtol: float = 1e-10
+    initial_damping: float = 1e-3
+    max_damping: float = 1e16
+    diag_floor: float = 1e-12
+    reject_new_failures: bool = True
+    jacobian: int = JACOBIAN_ADJOINT
+    gram_exact: bool = True
+
+    def c_struct(self) -> "_capi.LmOptions":
+        o = _capi.LmOptions()
+        o.max_iterations = self.max_iterations
+        o.reject_new_failures = int(self.reject_new_failures)
+        o.ftol, o.xtol, o.gtol = self.ftol, self.xtol, self.gtol
+        o.initial_damping, o.max_damping = self.initial_damping, self.max_damping
+        o.diag_floor = self.diag_floor
+        o.jacobian = self.jacobian
+        o.gram_exact = int(self.gram_exact)
+        return o
+
+
+class DeviceLm:
+    """Batched LM state on the device: start(x0), cycle(), results(). One object per problem;
+    the workspace is allocated once and reused by every cycle."""
+
+    def __init__(self, templates: DeviceSystemBatch, layout: ResidualLayout,
+                 host: SystemBatchHost, variables, options: LmOptions, runs: int,
+                 stream=None):
+        self.lib = _capi.lib()
+        self.templates, self.layout, self.host = templates, layout, host
+        self.variables, self.options, self.runs = variables, options, runs
+        self.stream = stream
+        self._b = templates.c_struct()
+        self._plan = layout.plan(host)
+        self._vars = variables.c_struct()
+        self._opt = options.c_struct()
+        need = int(self.lib.mkb_lm_workspace_bytes(C.byref(self._b), C.byref(self._plan),
+                                                   C.byref(self._vars), C.byref(self._opt),
+                                                   runs))
+        if need == 0:
+            raise ValueError(f"lm: {self.lib.mkb_last_error().decode()}")
+        self.workspace = torch.empty(need, dtype=torch.uint8, device=templates.device)
+        self.cycles = 0
+
+    def _args(self):
+        return (C.byref(self._b), C.byref(self._plan), C.byref(self._vars), C.byref(self._opt))
+
+    def start(self, x0) -> None:
+        x0 = _dev_f64(np.asarray(x0).reshape(self.runs, self.variables.size),
+                      self.templates.device)
+        self._x0 = x0
+        rc = self.lib.mkb_lm_start_device(*self._args(), C.c_void_p(x0.data_ptr()), self.runs,
+                                          C.c_void_p(self.workspace.data_ptr()),
+                                          self.workspace.numel(), _stream_handle(self.stream))
+        _capi.check(rc, "lm start")
+
+    def cycle(self) -> None:
+        rc = self.lib.mkb_lm_cycle_device(*self._args(), self.runs,
+                                          C.c_void_p(self.workspace.data_ptr()),
+                                          self.workspace.numel(), _stream_handle(self.stream))
+        _capi.check(rc, "lm cycle")
+        self.cycles += 1
+
+    def running(self) -> int:
+        out = np.zeros(1, dtype=np.int32)
+        torch.cuda.synchronize(self.templates.device)
+        rc = self.lib.mkb_lm_results_device(*self._args(), self.runs,
+                                            C.c_void_p(self.workspace.data_ptr()),
+                                            *([None] * 10), _capi.ptr(out, C.c_int32),
+                                            _stream_handle(self.stream))
+        _capi.check(rc, "lm results")
+        torch.cuda.synchronize(self.templates.device)
+        return int(out[0])
+
+    def results(self) -> dict:
+        R, P, H = self.runs, self.variables.size, self.options.max_iterations + 1
+        out = dict(x=np.zeros((R, P)), merit=np.zeros(R), status=np.zeros(R, np.int32),
+                   iterations=np.zeros(R, np.int32), accepted=np.zeros(R, np.int32),
+                   jacobians=np.zeros(R, np.int32), damping=np.zeros(R),
+                   history=np.zeros((R, H)), failed=np.zeros(R, np.int64),
+                   hard_failed=np.zeros(R, np.int64))
+        torch.cuda.synchronize(self.templates.device)
+        rc = self.lib.mkb_lm_results_device(
+            *self._args(), self.runs, C.c_void_p(self.workspace.data_ptr()),
+            _capi.ptr(out["x"]), _capi.ptr(out["merit"]), _capi.ptr(out["status"], C.c_int32),
+            _capi.ptr(out["iterations"], C.c_int32), _capi.ptr(out["accepted"], C.c_int32),
+            _capi.ptr(out["jacobians"], C.c_int32), _capi.ptr(out["damping"]),
+            _capi.ptr(out["history"]), _capi.ptr(out["failed"], C.c_int64),
+            _capi.ptr(out["hard_failed"], C.c_int64), None, _stream_handle(self.stream))
+        _capi.check(rc, "lm results")
+        torch.cuda.synchronize(self.templates.device)
+        return out
+
+
+def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x0,
+                    options: LmOptions | None = None, device: int = 0) -> dict:
+    """optimize_lm_gpu (include/mikroptim/cuda/levenberg_marquardt.hpp): batched LM of the runs
+    x0 [runs][P] on `batch` (1 variant for all runs or one per run), one penalty pass."""
+    options = options or LmOptions()
+    dev = _require_cuda(f"cuda:{device}")
+    x0 = np.asarray(x0, dtype=np.float64).reshape(-1, variables.size)
+    with torch.cuda.device(dev):
+        templates = DeviceSystemBatch(batch, dev)
+        lm = DeviceLm(templates, layout, batch, variables, options, x0.shape[0])
+        lm.start(x0)
+        while lm.running() > 0:
+            lm.cycle()
+        res = lm.results()
+        res["cycles"] = lm.cycles
+        _device_status()
+        return res
