@@ -186,6 +186,17 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
                                 double* J, double* r0, uint8_t* status, void* workspace,
                                 size_t workspace_bytes, void* stream);
 
+/* Adjoint Jacobian fused with its normal equations: gram [runs][P+1][P+1] = [J r]^T [J r] of
+ * the piston-projected adjoint rows (and the penalty rows), J never written to memory.
+ * Replaces DeviceAdjointJacobian::compute + DeviceNormalEquations::compute for the LM. The
+ * rows are computed in the plan's precision (FP64: the rows of the exact path; FP64_FMA:
+ * contracted), the contraction runs on FP64 tensor cores; the workspace is
+ * mkb_adjoint_jacobian_workspace_bytes(templates, runs). */
+int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
+                                        const mkb_residual_plan* plan, const mkb_variables* vars,
+                                        const double* x0, int32_t runs, double* gram,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- batched Levenberg-Marquardt ------------------------------------------------------------
  * LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85) for one pass (no outer
  * soft-failure penalty rounds), and the per-run state kept in a caller workspace. The device
@@ -206,7 +217,9 @@ typedef struct mkb_lm_options {
     double max_damping;               /* 1e16 */
     double diag_floor;                /* 1e-12 */
     int32_t jacobian;                 /* MKB_JACOBIAN_* */
-    int32_t gram_exact;               /* 1: FMA-chain normal equations, 0: FP64 DMMA */
+    int32_t gram_exact;               /* 1: FMA-chain normal equations, 0: FP64 DMMA; with
+                                         the adjoint, 0 selects the fused adjoint +
+                                         normal-equation kernel (no J in memory) */
 } mkb_lm_options;
 
 size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,

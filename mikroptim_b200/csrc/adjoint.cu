@@ -343,3 +343,430 @@ int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
 MKB_DEFINE_ERROR_READER(adjoint_device_error)
 
 }  // namespace mkb
+
+namespace mkb {
+// ---- fused adjoint + normal equations ---------------------------------------------------------
+// One CTA per run streams the run's rays in chunks of kFusedThreads (one ray per thread):
+//   A  forward with checkpoints in shared memory, then the OPL-seed reverse sweep writes the
+//      row y_k = [dOPL_k/dx | OPL_k] into shared memory (rays outside the piston: weight 0);
+//   B  per tuple segment of the chunk (threads = columns): weighted mean mu_seg, rows centred
+//      and scaled in place, x_k = s sqrt(W_k) (y_k - mu_seg), and the segment merged into the
+//      tuple's running mean with one extra row s sqrt(W_t W_seg / (W_t + W_seg)) (mu_seg - mu_t)
+//      (Chan, Golub, LeVeque): summed over the chunks, sum x x^T is s^2 sum_k W_k (y_k - ybar)
+//      (y_k - ybar)^T over the tuple -- exactly [J r]^T [J r] of the piston-projected rows
+//      J_k = s sqrt(W_k) (g_k - gbar), r_k = s sqrt(W_k) (OPL_k - piston), without a second
+//      pass over the tuple and without J in memory;
+//   C  FP64 tensor cores accumulate sum x x^T (mma.sync m8n8k4, 8 x 8 tiles of the upper
+//      triangle in registers, owned by the CTA's warps);
+//   D  in soft-failure mode, when the chunk has failed rays, the penalty rows
+//      [s_p sqrt(W) dpi/dx | p_k] (uncentred) are accumulated the same way.
+// Output: gram [runs][P+1][P+1] as the normal-equation kernels write it.
+namespace {
+
+constexpr int kFusedThreads = 128;
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr int kExtraRows = 8;
+constexpr int kFusedMinBlocks = 3;  // CTAs per SM the register budget is sized for
+constexpr int kMaxTileCols = (MKB_MAX_VARIABLES + 1 + 7) / 8;                   // 9
+constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 45
+
+struct FusedShared {
+    uint64_t bar;
+    SharedTables tab;
+    double w[kFusedThreads];      // sample weight if the ray is in the piston, else 0
+    int tuple[kFusedThreads];     // tuple of the ray (-1 past the end)
+    double seg_w;                 // weight of the current segment
+    double open_w;                // running weight of the open tuple
+    int open_tuple;               // tuple whose running mean is kept
+    int extra;                    // extra rows pending
+    int any_failed;               // chunk has a ray with status != Ok (soft mode)
+    int2 tiles[kMaxTilePairs];    // (row tile, column tile) of every upper-triangle pair
+};
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// acc += X^T X for X stored column-major, X(k, c) = xt[c * ld + k], k < n (n a multiple of 4;
+// the caller pads with zero rows). Warp w owns tile pairs w, w + 4, ...; the 8 x 8 accumulator
+// tiles live in shared memory in fragment order (acc[pair][lane][2]), loaded and stored around
+// the k loop.
+__device__ __forceinline__ void accumulate(const double* xt, int ld, int n, int pairs,
+                                           const int2* tiles, double* acc) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gid = lane >> 2, tig = lane & 3;
+    for (int e = warp; e < pairs; e += kFusedWarps) {
+        const double* ca = xt + (tiles[e].x * 8 + gid) * ld + tig;
+        const double* cb = xt + (tiles[e].y * 8 + gid) * ld + tig;
+        double* a = acc + (e * 32 + lane) * 2;
+        double d0 = a[0], d1 = a[1];
+        for (int k0 = 0; k0 < n; k0 += 4) dmma(d0, d1, ca[k0], cb[k0]);
+        a[0] = d0;
+        a[1] = d1;
+    }
+}
+
+template <class N>
+__device__ void fused_forward(const TraceParams& p, const double* rec, const RecordLayout& lay,
+                              int f, int l, const Sample& smp, bool soft_mode, double* ck,
+                              int stride_ck, uint64_t& br_lo, uint64_t& br_hi, int& count,
+                              int& image_branch, int& status_out, int& soft_first, double& opl,
+                              double& penalty) {
+    const int S = p.S, L = p.L;
+    const N zero(0.0);
+    const N a = rec[lay.pupil];
+    const N st = rec[lay.sin_theta + f];
+    const N ct = rec[lay.cos_theta + f];
+    const N r0 = a * N(smp.rho);
+    RayT<N> r;
+    r.px = r0 * N(smp.sin_phi);
+    r.py = r0 * N(smp.cos_phi);
+    r.pz = zero;
+    r.dx = zero;
+    r.dy = st;
+    r.dz = ct;
+    r.opl = r.py * st;
+    SoftT<N> soft{zero, kOk};
+    SoftT<N>* sp = soft_mode ? &soft : nullptr;
+    auto save = [&](int c) {
+        double* q = ck + c * stride_ck;
+        q[0] = value_of(r.px);
+        q[1 * kFusedThreads] = value_of(r.py);
+        q[2 * kFusedThreads] = value_of(r.pz);
+        q[3 * kFusedThreads] = value_of(r.dx);
+        q[4 * kFusedThreads] = value_of(r.dy);
+        q[5 * kFusedThreads] = value_of(r.dz);
+    };
+    br_lo = br_hi = 0;
+    count = 1;
+    image_branch = kBranchRegular;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    N n_before = idx[l];
+    for (int s = 1; s < S; ++s) {
+        const N n_after = idx[s * L + l];
+        const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        int branch;
+        status = step_surface<N>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch);
+        if (status != kOk) break;
+        count = s + 1;
+        if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
+        else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
+        if (s % kInterval == 0) save(s / kInterval);
+        n_before = n_after;
+    }
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > zero)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step<N>(r, N(rec[lay.target + f]), N(thick[S - 1]),
+                                              n_before, sp, branch);
+            if (!in_piston(rst)) {
+                status = rst;
+            } else {
+                image_branch = branch;
+                if (status == kOk) status = rst;
+            }
+        }
+    }
+    status_out = status;
+    soft_first = soft.first;
+    opl = value_of(r.opl);
+    penalty = value_of(soft.penalty);
+}
+
+// Reverse sweep of one seed writing factor * dPhi/dx into row[col * ld]. One out-of-line copy
+// serves both seeds (keeps the kernel's instruction footprint small).
+template <class N>
+__device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v, const double* rec,
+                               const RecordLayout& lay, int f, int l, const Sample& smp,
+                               const double* ck,
+                               int stride_ck, uint64_t br_lo, uint64_t br_hi, int count,
+                               int image_branch, bool reached_image, bool soft_mode, N seed_opl,
+                               N seed_pen, N factor, double* row, int ld) {
+    const int S = p.S, L = p.L;
+    const N zero(0.0);
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    RayAdj<N> adj{{zero, zero, zero}, {zero, zero, zero}};
+    int next_branch = kBranchRegular;
+    const Vec<N> center{zero, N(rec[lay.target + f]), N(thick[S - 1])};
+    auto branch_of = [&](int s) {
+        return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
+                      : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
+    };
+    for (int c = (count - 1) / kInterval; c >= 0; --c) {
+        const int first = c * kInterval;
+        const int n = (count - first) < kInterval ? (count - first) : kInterval;
+        Vec<N> sp[kInterval], sd[kInterval];
+        if (c == 0) {  // the start ray is recomputed (collimated_ray), not stored
+            const N r0 = N(rec[lay.pupil]) * N(smp.rho);
+            sp[0] = {r0 * N(smp.sin_phi), r0 * N(smp.cos_phi), zero};
+            sd[0] = {zero, N(rec[lay.sin_theta + f]), N(rec[lay.cos_theta + f])};
+        } else {
+            const double* q = ck + c * stride_ck;
+            sp[0] = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
+            sd[0] = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
+        }
+        RayT<N> r{sp[0].x, sp[0].y, sp[0].z, sd[0].x, sd[0].y, sd[0].z, zero};
+        SoftT<N> dummy{zero, kOk};
+#pragma unroll
+        for (int i = 1; i < kInterval; ++i) {
+            if (i < n) {
+                const int s = first + i;
+                const N cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+                int branch;
+                step_surface<N>(r, N(thick[s - 1]), cs, N(idx[(s - 1) * L + l]),
+                                N(idx[s * L + l]), soft_mode ? &dummy : nullptr, branch);
+                sp[i] = {r.px, r.py, r.pz};
+                sd[i] = {r.dx, r.dy, r.dz};
+            }
+        }
+#pragma unroll
+        for (int i = kInterval - 1; i >= 0; --i) {
+            if (i < n) {
+                const int s = first + i;
+                if (s == count - 1) {
+                    if (reached_image && count == S) {
+                        Vec<N> center_adj{zero, zero, zero};
+                        N n_image_adj = zero;
+                        reference_step_backward<N>(sp[i], sd[i], center, N(idx[(S - 1) * L + l]),
+                                                   image_branch, seed_opl, seed_pen, adj,
+                                                   center_adj, n_image_adj);
+                        const int col = v.col_thickness[S - 1];
+                        if (col >= 0) row[col * ld] = value_of(factor * center_adj.z);
+                    }
+                } else {
+                    const int j = s + 1;
+                    const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
+                    const N cj = sphere ? curv[j] : 0.0;
+                    StepAdj<N> par{zero, zero, zero, zero};
+                    refracting_step_backward<N>(sp[i], sd[i], N(thick[s]), cj, N(idx[s * L + l]),
+                                                N(idx[j * L + l]), next_branch, seed_opl,
+                                                seed_pen, adj, par);
+                    if (sphere && v.col_curvature[j] >= 0)
+                        row[v.col_curvature[j] * ld] = value_of(factor * par.curvature);
+                    if (v.col_thickness[s] >= 0)
+                        row[v.col_thickness[s] * ld] = value_of(factor * par.thickness);
+                }
+                next_branch = branch_of(s);
+            }
+        }
+    }
+}
+
+template <class N>
+__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
+adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __restrict__ records,
+                    double* __restrict__ gram) {
+    const TraceParams& p = ap.t;
+    const VarParams& v = ap.v;
+    __shared__ FusedShared sh;
+    extern __shared__ __align__(16) double dyn[];
+    const int P = v.P;
+    const int NP = ((P + 1 + 7) / 8) * 8;
+    const int ncols = NP / 8;
+    const int pairs = ncols * (ncols + 1) / 2;
+    const int nck = (p.S - 1) / kInterval + 1;
+    const int stride_ck = 6 * kFusedThreads;
+    constexpr int TS = kFusedThreads + 1;              // column stride of Y (odd: no conflicts)
+    constexpr int ES = kExtraRows + 1;                 // column stride of E
+    double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
+    double* Y = record + p.stride;                     // column-major [NP][TS]
+    double* E = Y + NP * TS;                           // column-major [NP][ES]
+    double* mu_open = E + NP * ES;                     // [NP]
+    double* mu_seg = mu_open + NP;                     // [NP]
+    double* acc = mu_seg + NP;                         // [pairs][32][2] DMMA accumulators
+    double* ckpt = acc + pairs * 64;                   // [nck][6][T], checkpoint 0 unused
+    const int tid = threadIdx.x;
+    const int run = blockIdx.x;
+    const RecordLayout lay = record_layout(p.S, p.L, p.F);
+    copy_tables(p, sh.tab);
+    if (tid == 0) {
+        sh.open_tuple = -1;
+        sh.open_w = 0.0;
+        sh.extra = 0;
+    }
+    if (!stage_to_shared(record, records + static_cast<int64_t>(run) * p.stride,
+                         static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar))
+        return;
+    const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
+    for (int e = tid; e < pairs; e += kFusedThreads) {
+        int j = 0, rem = e;
+        while (rem >= j + 1) {
+            rem -= j + 1;
+            ++j;
+        }
+        sh.tiles[e] = make_int2(rem, j);
+    }
+    for (int i = tid; i < pairs * 64; i += kFusedThreads) acc[i] = 0.0;
+    __syncthreads();
+    double* my_ck = ckpt + tid;
+    for (int base = 0; base < p.rays; base += kFusedThreads) {
+        const int q = base + tid;
+        double* row = Y + tid;  // this ray's row, column c at row[c * TS]
+        for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
+        int f = 0, l = 0, k = 0, tu = -1;
+        int status = kMissed, soft_first = kOk, count = 0, image_branch = 0;
+        uint64_t br_lo = 0, br_hi = 0;
+        double opl = 0.0, penalty = 0.0;
+        Sample smp{};
+        if (q < p.rays) {
+            while (f + 1 < p.F && q >= p.field_offset[f + 1]) ++f;
+            const int within = q - p.field_offset[f];
+            l = within / p.sample_count[f];
+            k = within - l * p.sample_count[f];
+            tu = f * p.L + l;
+            smp = pupil_sample(p, sh.tab, f, k);
+            fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
+                             br_hi, count, image_branch, status, soft_first, opl, penalty);
+            if (in_piston(status)) {
+                fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo, br_hi,
+                                  count, image_branch, true, soft_mode, N(1.0), N(0.0), N(1.0),
+                                  row, TS);
+                row[P * TS] = opl;
+            }
+        }
+        sh.w[tid] = (q < p.rays && in_piston(status)) ? smp.weight : 0.0;
+        sh.tuple[tid] = tu;
+        if (tid == 0) sh.any_failed = 0;
+        __syncthreads();
+        if (soft_mode && q < p.rays && status != kOk) sh.any_failed = 1;
+        // ---- B: segments (threads = columns) ----
+        const int rows_here = p.rays - base < kFusedThreads ? p.rays - base : kFusedThreads;
+        int start = 0;
+        while (start < rows_here) {
+            const int t = sh.tuple[start];
+            int end = start + 1;
+            while (end < rows_here && sh.tuple[end] == t) ++end;
+            if (tid == 0) {
+                double w = 0.0;
+                for (int r = start; r < end; ++r) w += sh.w[r];
+                sh.seg_w = w;
+            }
+            __syncthreads();
+            const double wseg = sh.seg_w;
+            const double scale = p.scale[t];
+            if (wseg > 0.0) {
+                if (tid < NP) {
+                    double s = 0.0;
+                    double* col = Y + tid * TS;
+                    for (int r = start; r < end; ++r) s += sh.w[r] * col[r];
+                    const double mean = s / wseg;
+                    mu_seg[tid] = mean;
+                    for (int r = start; r < end; ++r) {
+                        const double x = col[r];
+                        col[r] = sh.w[r] > 0.0 ? scale * sqrt(sh.w[r]) * (x - mean) : 0.0;
+                    }
+                    if (sh.open_tuple == t && sh.open_w > 0.0) {
+                        const double wt = sh.open_w;
+                        const double fac = scale * sqrt(wt * wseg / (wt + wseg));
+                        E[tid * ES + sh.extra] = fac * (mean - mu_open[tid]);
+                        mu_open[tid] += (wseg / (wt + wseg)) * (mean - mu_open[tid]);
+                    } else {
+                        mu_open[tid] = mean;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    if (sh.open_tuple == t && sh.open_w > 0.0) {
+                        sh.extra += 1;
+                        sh.open_w += wseg;
+                    } else {
+                        sh.open_tuple = t;
+                        sh.open_w = wseg;
+                    }
+                }
+            } else if (tid < NP) {
+                for (int r = start; r < end; ++r) Y[tid * TS + r] = 0.0;
+            }
+            __syncthreads();
+            if (sh.extra == kExtraRows) {  // flush the extra rows
+                accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
+                __syncthreads();
+                if (tid == 0) sh.extra = 0;
+                __syncthreads();
+            }
+            start = end;
+        }
+        // ---- C: accumulate the centred rows and the pending extra rows ----
+        for (int r = rows_here + tid; r < ((rows_here + 3) & ~3); r += kFusedThreads)
+            for (int c = 0; c < NP; ++c) Y[c * TS + r] = 0.0;
+        const int ne = sh.extra;
+        for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
+            for (int c = 0; c < NP; ++c) E[c * ES + r] = 0.0;
+        __syncthreads();
+        accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+        if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
+        __syncthreads();
+        if (tid == 0) sh.extra = 0;
+        // ---- D: penalty rows ----
+        if (sh.any_failed) {
+            for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
+            if (q < p.rays && status != kOk) {
+                const N factor = N(p.pscale[tu]) * N(smp.root_weight);
+                if (soft_first != kOk)
+                    fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                      br_hi, count, image_branch, in_piston(status), soft_mode,
+                                      N(0.0), N(1.0), factor, row, TS);
+                const double fp = is_soft(status) ? penalty : penalty + 1.0;
+                row[P * TS] = value_of(factor * N(fp));
+            }
+            __syncthreads();
+            accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+        }
+        __syncthreads();
+    }
+    // ---- write the (P+1) x (P+1) symmetric gram ----
+    const int n = P + 1;
+    double* G = gram + static_cast<int64_t>(run) * n * n;
+    __syncthreads();
+    for (int i = tid; i < pairs * 64; i += kFusedThreads) {
+        const int e = i / 64, lane = (i / 2) & 31, h = i & 1;
+        const int r = sh.tiles[e].x * 8 + (lane >> 2);
+        const int c = sh.tiles[e].y * 8 + 2 * (lane & 3) + h;
+        if (r < n && c < n) {
+            G[static_cast<int64_t>(c) * n + r] = acc[i];
+            G[static_cast<int64_t>(r) * n + c] = acc[i];
+        }
+    }
+}
+
+}  // namespace
+
+size_t fused_adjoint_smem(const TraceParams& tp, int P) {
+    const int NP = ((P + 1 + 7) / 8) * 8;
+    const int nck = (tp.S - 1) / kInterval + 1;
+    const int ncols = NP / 8;
+    const int pairs = ncols * (ncols + 1) / 2;
+    return sizeof(double) * (static_cast<size_t>(tp.stride) +
+                             static_cast<size_t>(kFusedThreads + 1) * NP +
+                             (kExtraRows + 1) * NP + 2 * NP +
+                             static_cast<size_t>(pairs) * 64 +
+                             static_cast<size_t>(nck) * 6 * kFusedThreads);
+}
+
+int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
+                        double* gram, bool exact, cudaStream_t stream) {
+    AdjointParams ap;
+    ap.t = tp;
+    ap.v = vp;
+    ap.rows = 0;
+    const size_t smem = fused_adjoint_smem(tp, vp.P);
+    auto kernel = exact ? adjoint_gram_kernel<Exact64> : adjoint_gram_kernel<double>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(smem));
+    if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");
+    kernel<<<tp.V, kFusedThreads, smem, stream>>>(ap, records, gram);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "fused adjoint launch");
+}
+
+}  // namespace mkb

@@ -27,6 +27,8 @@ int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows
                         const double* records, double* J, bool exact, cudaStream_t stream);
 int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
                       const uint8_t* status, double* J, bool exact, cudaStream_t stream);
+int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
+                        double* gram, bool exact, cudaStream_t stream);
 int pack_rays_default();
 
 namespace {
@@ -348,6 +350,48 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
     rc = launch_adjoint_rows(tp, vp, R, records, J, exact, stream);
     if (rc != MKB_OK) return rc;
     return launch_projection(tp, vp, R, status, J, exact, stream);
+}
+
+int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
+                                        const mkb_residual_plan* plan, const mkb_variables* vars,
+                                        const double* x0, int32_t runs, double* gram,
+                                        void* workspace, size_t workspace_bytes,
+                                        void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    if (runs < 0) {
+        set_error("adjoint normal equations: runs must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (runs == 0) return MKB_OK;
+    int rc = check_templates(templates, runs);
+    if (rc != MKB_OK) return rc;
+    TraceParams tp;
+    mkb_device_batch b = *templates;
+    b.variants = runs;
+    rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+        set_error("adjoint normal equations: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    VarParams vp;
+    rc = make_var_params(vars, tp.S, templates->type, &vp);
+    if (rc != MKB_OK) return rc;
+    if (!x0 || !gram) {
+        set_error("adjoint normal equations: null pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    const size_t need = mkb_adjoint_jacobian_workspace_bytes(templates, runs);
+    if (workspace == nullptr || workspace_bytes < need) {
+        set_error("adjoint normal equations: workspace of %zu bytes needed", need);
+        return MKB_ERR_WORKSPACE;
+    }
+    double* records = static_cast<double*>(workspace);
+    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
+    if (rc != MKB_OK) return rc;
+    return launch_adjoint_gram(tp, vp, records, gram, plan->precision == MKB_PRECISION_FP64,
+                               stream);
 }
 
 }  // extern "C"

@@ -445,6 +445,8 @@ int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
                       const uint8_t* status, double* J, bool exact, cudaStream_t stream);
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
                 bool exact, cudaStream_t stream);
+int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
+                        double* gram, bool exact, cudaStream_t stream);
 int pack_rays_default();
 
 namespace {
@@ -472,7 +474,8 @@ constexpr int kFdChunkRuns = 64;
 
 // Carves the workspace (base may be null to only size it).
 LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_it, bool fd,
-                   const mkb_device_batch* templates, const mkb_residual_plan* plan) {
+                   bool fused, const mkb_device_batch* templates,
+                   const mkb_residual_plan* plan) {
     LmLayout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -509,9 +512,10 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     L.st.evaluate = reinterpret_cast<int*>(take(4 * r));
     L.st.running = reinterpret_cast<int*>(take(4));
     L.gram = reinterpret_cast<double*>(take(8 * r * (P + 1) * (P + 1)));
-    L.J = reinterpret_cast<double*>(take(8 * r * P * R));
-    L.r0 = reinterpret_cast<double*>(take(8 * r * R));
-    L.status = reinterpret_cast<uint8_t*>(take(r * tp.rays));
+    const size_t jr = fused ? 0 : r;  // the fused adjoint keeps J out of memory
+    L.J = reinterpret_cast<double*>(take(8 * jr * P * R));
+    L.r0 = reinterpret_cast<double*>(take(8 * jr * R));
+    L.status = reinterpret_cast<uint8_t*>(take(jr * tp.rays));
     L.records = reinterpret_cast<double*>(take(8 * r * tp.stride));
     L.merit_ws_bytes = merit_workspace_bytes(runs, tp.n_tuples);
     L.merit_ws = take(L.merit_ws_bytes);
@@ -533,7 +537,7 @@ struct LmSetup {
     TraceParams tp;
     VarParams vp;
     LmOptionsDev o;
-    bool fd, exact, gram_exact;
+    bool fd, exact, gram_exact, fused;
     int64_t R;
 };
 
@@ -574,6 +578,7 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     s.fd = o.jacobian == MKB_JACOBIAN_FD;
     s.exact = plan->precision == MKB_PRECISION_FP64;
     s.gram_exact = o.gram_exact != 0;
+    s.fused = !s.fd && !s.gram_exact;
     s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
     return MKB_OK;
 }
@@ -602,7 +607,7 @@ size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_resid
                               int32_t runs) {
     LmSetup s;
     if (lm_setup(templates, plan, vars, options, runs, s) != MKB_OK) return 0;
-    return lm_layout(nullptr, s.tp, s.vp.P, runs, s.o.max_iterations, s.fd, templates, plan).total;
+    return lm_layout(nullptr, s.tp, s.vp.P, runs, s.o.max_iterations, s.fd, s.fused, templates, plan).total;
 }
 
 int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
@@ -614,7 +619,7 @@ int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_pl
     int rc = lm_setup(templates, plan, vars, options, runs, s);
     if (rc != MKB_OK) return rc;
     const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
-                                 s.o.max_iterations, s.fd, templates, plan);
+                                 s.o.max_iterations, s.fd, s.fused, templates, plan);
     if (workspace == nullptr || workspace_bytes < L.total || x0 == nullptr) {
         set_error("lm: workspace of %zu bytes and x0 needed", L.total);
         return MKB_ERR_WORKSPACE;
@@ -634,7 +639,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     int rc = lm_setup(templates, plan, vars, options, runs, s);
     if (rc != MKB_OK) return rc;
     const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
-                                 s.o.max_iterations, s.fd, templates, plan);
+                                 s.o.max_iterations, s.fd, s.fused, templates, plan);
     if (workspace == nullptr || workspace_bytes < L.total) {
         set_error("lm: workspace of %zu bytes needed", L.total);
         return MKB_ERR_WORKSPACE;
@@ -646,6 +651,12 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         mkb_variables v = *vars;
         rc = mkb_fd_jacobian_device(&t, &pl, &v, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
                                     L.fd_ws_bytes, stream);
+    } else if (s.fused) {
+        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
+                          runs, stream);
+        if (rc == MKB_OK)
+            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, s.exact, stream);
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
@@ -661,8 +672,10 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
             rc = launch_projection(s.tp, s.vp, s.R, L.status, L.J, s.exact, stream);
     }
     if (rc != MKB_OK) return rc;
-    rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream);
-    if (rc != MKB_OK) return rc;
+    if (!s.fused) {
+        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream);
+        if (rc != MKB_OK) return rc;
+    }
     // 2. step
     rc = launch_lm_update(s.vp, s.o, L.st, L.gram, runs, stream);
     if (rc != MKB_OK) return rc;
@@ -687,7 +700,7 @@ int mkb_lm_results_device(const mkb_device_batch* templates, const mkb_residual_
     int rc = lm_setup(templates, plan, vars, options, runs, s);
     if (rc != MKB_OK) return rc;
     const LmLayout L = lm_layout(static_cast<char*>(const_cast<void*>(workspace)), s.tp, s.vp.P,
-                                 runs, s.o.max_iterations, s.fd, templates, plan);
+                                 runs, s.o.max_iterations, s.fd, s.fused, templates, plan);
     const size_t r = static_cast<size_t>(runs);
     struct Copy {
         void* dst;

@@ -366,3 +366,25 @@ def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x
         res["cycles"] = lm.cycles
         _device_status()
         return res
+
+
+def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: ResidualLayout,
+                                    host: SystemBatchHost, variables, x0, stream=None):
+    """Fused adjoint + normal equations (FP64_FMA, DMMA): gram [runs][P+1][P+1]."""
+    lib = _capi.lib()
+    dev = templates.device
+    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    runs, P = x0.shape
+    b = templates.c_struct()
+    plan = layout.plan(host)
+    need = int(lib.mkb_adjoint_jacobian_workspace_bytes(C.byref(b), runs))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    gram = torch.empty((runs, P + 1, P + 1), dtype=torch.float64, device=dev)
+    vs = variables.c_struct()
+    rc = lib.mkb_adjoint_normal_equations_device(C.byref(b), C.byref(plan), C.byref(vs),
+                                                 C.c_void_p(x0.data_ptr()), runs,
+                                                 C.c_void_p(gram.data_ptr()),
+                                                 C.c_void_p(ws.data_ptr()), ws.numel(),
+                                                 _stream_handle(stream))
+    _capi.check(rc, "adjoint normal equations")
+    return gram

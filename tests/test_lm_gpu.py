@@ -19,13 +19,15 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not has_reference_build(), reason="reference build missing")]
 
 
-def run_both(method, runs=6, max_iterations=25, gram_exact=True):
+def run_both(method, runs=6, max_iterations=25, gram_exact=True, precision=0):
     b, st, vs, x0 = workloads.singlet(runs)
     lay = ResidualLayout(b.topology, st)
+    lay_gpu = ResidualLayout(b.topology, type(st)(rings=st.rings, spokes=st.spokes,
+                                                  failure=st.failure, precision=precision))
     opt = engine.LmOptions(max_iterations=max_iterations,
                            jacobian=engine.JACOBIAN_ADJOINT if method == "adjoint"
                            else engine.JACOBIAN_FD, gram_exact=gram_exact)
-    g = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
+    g = engine.optimize_lm_gpu(b, lay_gpu, vs, x0, opt)
     r = po.reference().optimize_lm(b, lay, vs, x0, max_iterations=max_iterations,
                                    method=method, penalty_rounds=1, threads=4)
     return g, r
@@ -48,5 +50,13 @@ def test_lm_trajectories_bitwise_equal_reference(method):
 
 def test_lm_dmma_normal_equations_reach_same_optimum():
     g, r = run_both("adjoint", gram_exact=False)
+    assert np.allclose(g["merit"], r["merit"], rtol=1e-6, atol=1e-12)
+    assert np.allclose(g["x"], r["x"], rtol=1e-6, atol=1e-9)
+
+
+def test_lm_fused_adjoint_fma_reaches_same_optimum():
+    """FMA arithmetic with the fused adjoint + DMMA normal equations (the fast path)."""
+    g, r = run_both("adjoint", gram_exact=False, precision=2)
+    assert np.all(g["status"] > 0)
     assert np.allclose(g["merit"], r["merit"], rtol=1e-6, atol=1e-12)
     assert np.allclose(g["x"], r["x"], rtol=1e-6, atol=1e-9)
