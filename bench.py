@@ -3,10 +3,17 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload merit|lm]
 
-Workload (default): the seven-element objective of the adjoint-vs-FD configuration -- 4096
-variants, 15 table surfaces, 7 wavelengths, 5 fields, 16 rings x 32 spokes (14,448 rays per
-variant, 59.2 M rays per evaluation), soft failure; synthetic seeded inputs. One step = one
-MERIT evaluation of all variants (`--workload merit`).
+Workload: the seven-element objective of the adjoint-vs-FD configuration -- 4096 runs (one
+variant each), 15 table surfaces, 7 wavelengths, 5 fields, 16 rings x 32 spokes (14,448 rays
+per variant, 59.2 M rays per evaluation), 29 variables (14 curvatures, 15 thicknesses incl. the
+working distance), soft failure; synthetic seeded inputs.
+
+  --workload lm (default): one step = one batched Levenberg-Marquardt cycle of all 4096 runs
+      (adjoint Jacobian fused with its FP64-tensor-core normal equations, damped Cholesky step,
+      trial MERIT, acceptance), FP64 with FMA contraction. The same cycle with the central-
+      difference Jacobian (the reference method, 2P + 1 = 59 traced variants per run) is timed
+      on the same GPU beside it (`fd_fp64`), on 512 runs (its cost is linear in the runs).
+  --workload merit: one step = one MERIT evaluation of all variants.
 
 N > 1 (torchrun, one rank per GPU): every rank traces its own 4096 variants (weak scaling,
 independent variants, no data-path collective); the time is the maximum over ranks.
@@ -35,7 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "LM iter/s & ray-surface hits/s: adjoint+mixed vs FP64 FD, at ≤1e-4λ OPD err"
-WORKLOAD = "objective-4096: 4096 variants x 15 surfaces, L=7, F=5, 16x32 pupil (config 2 shape)"
+WORKLOAD = "objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=29 (config 2 shape)"
 FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of the reference)
 # DRAM traffic of trace_kernel per variant from the ncu capture summarised in
 # profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
@@ -48,7 +55,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="merit", choices=["merit"])
+    ap.add_argument("--workload", default="lm", choices=["lm", "merit"])
     ap.add_argument("--variants", type=int, default=4096)
     return ap.parse_args()
 
@@ -282,6 +289,166 @@ def run_b200(args, world, rank, local):
     return out, (b, lay)
 
 
+def run_lm(args, world, rank, local):
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import PRECISION_FP64_FMA, ResidualLayout
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    b, st, vs, x0 = workloads.objective(args.variants, seed=20261203 + 2 + 1000 * rank)
+    st.precision = PRECISION_FP64_FMA
+    lay = ResidualLayout(b.topology, st)
+    runs = b.variants
+    db = engine.DeviceSystemBatch(b, dev)
+    opt = engine.LmOptions(max_iterations=args.warmup + args.steps + 100,
+                           jacobian=engine.JACOBIAN_ADJOINT, gram_exact=False)
+    lm = engine.DeviceLm(db, lay, b, vs, opt, runs)
+    lm.start(x0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    rays = runs * lay.rays_per_variant
+    steps_per_ray = b.surfaces - 1
+    for _ in range(args.warmup):
+        lm.cycle()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = lib.mkb_launch_count()
+    times = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lm.cycle()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = lib.mkb_launch_count() - launches0
+    ms_total = max_over_ranks(sum(a.elapsed_time(c) for a, c in times), world, dev)
+    ms_step = ms_total / args.steps
+    value = world * runs * args.steps / (ms_total / 1e3)
+
+    # the dominant kernel alone: fused adjoint + normal equations at the current points
+    x_now = torch.empty((runs, vs.size), dtype=torch.float64, device=dev)
+    lib.mkb_lm_results_device(*lm._args(), runs, C.c_void_p(lm.workspace.data_ptr()),
+                              C.c_void_p(x_now.data_ptr()), *([None] * 10),
+                              C.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize()
+    x_np = x_now.cpu().numpy()
+    engine.adjoint_normal_equations_device(db, lay, b, vs, x_np)
+    torch.cuda.synchronize()
+    kt = []
+    for _ in range(3):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        engine.adjoint_normal_equations_device(db, lay, b, vs, x_np)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kt.append(e0.elapsed_time(e1))
+    kernel_ms = min(kt)
+    # FLOP model (reference cost model): adjoint = 3 x FLOPeq(ray), FLOPeq = 140 (S_steps + 2),
+    # plus 4 P per ray (projection) and 2 P^2 per row (rows: rays and penalty rows)
+    P = vs.size
+    flop = rays * (3 * FLOPEQ_PER_RAY_SURFACE * (steps_per_ray + 2) + 4 * P) + \
+        2 * P * P * runs * lay.trace_rows
+
+    # MERIT rate (ray-surface hits/s) on the same points
+    mws = None
+    engine.merit_device(db, lay, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        engine.merit_device(db, lay, b)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    merit_ms = e0.elapsed_time(e1) / 3
+
+    # the reference method on the same GPU: FD Jacobian (59 traced variants per run), FP64
+    fd_runs = min(512, runs)
+    fd_b = b.subset(0, fd_runs)
+    fd_db = engine.DeviceSystemBatch(fd_b, dev)
+    fd_opt = engine.LmOptions(max_iterations=100, jacobian=engine.JACOBIAN_FD, gram_exact=False)
+    fd = engine.DeviceLm(fd_db, lay, fd_b, vs, fd_opt, fd_runs)
+    fd.start(x0[:fd_runs])
+    fd.cycle()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(2):
+        fd.cycle()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fd_ms = e0.elapsed_time(e1) / 2
+    fd_value = fd_runs / (fd_ms / 1e3)
+    del fd
+
+    # end to end through the host-buffer path: pinned x in, cycle, x and merit out per step
+    host_x = torch.from_numpy(x_np.copy()).pin_memory()
+    host_out = torch.empty((runs, P + 1), dtype=torch.float64).pin_memory()
+    dev_x = torch.empty_like(x_now)
+    lm2 = engine.DeviceLm(db, lay, b, vs, opt, runs)
+    lm2.start(x_np)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_x.copy_(host_x, non_blocking=True)
+        lm2.cycle()
+        lib.mkb_lm_results_device(*lm2._args(), runs, C.c_void_p(lm2.workspace.data_ptr()),
+                                  C.c_void_p(host_out.data_ptr()),
+                                  C.c_void_p(host_out.data_ptr() + runs * P * 8),
+                                  *([None] * 9), C.c_void_p(stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = flop / (kernel_ms / 1e3) / 1e12
+    if rank != 0:
+        return None, None
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": "LM run-iterations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-2 shapes)",
+        "config": {"workload": WORKLOAD, "step": "one batched LM cycle of all runs",
+                   "runs_per_gpu": runs, "variables": P, "rays_per_run": lay.rays_per_variant,
+                   "jacobian": "adjoint fused with FP64 tensor-core normal equations",
+                   "precision": "FP64 with FMA contraction",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(launches),
+        "ray_surface_hits_per_s": world * rays * steps_per_ray / (merit_ms / 1e3),
+        "fd_fp64": {"value": world * fd_value, "unit": "LM run-iterations/s",
+                    "ms_per_cycle_512_runs": fd_ms, "speedup_adjoint_vs_fd": value / (world * fd_value)},
+        "e2e": {"value": world * runs / (e2e_ms / 1e3), "unit": "LM run-iterations/s",
+                "h2d_bytes_per_step": int(runs * P * 8),
+                "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "adjoint_gram_kernel (fused adjoint + DMMA normal equations)",
+                     "kernel_ms": kernel_ms,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "flop_model": "3 x 140 (S-1+2) FLOP-eq per ray + 4P per ray + 2P^2 per row"},
+        "clocks": clocks.summary(),
+    }, None
+
+
 # ---- CPU baselines (oracle) ----------------------------------------------------------------
 def cpu_baseline(kind: str, sample_variants: int = 16, seed: int = 20261203 + 2):
     """The reference's own CPU merit (oracle/_ref) or the C restatement, on all host threads,
@@ -303,6 +470,29 @@ def cpu_baseline(kind: str, sample_variants: int = 16, seed: int = 20261203 + 2)
             "sample": f"MERIT of {sample_variants} of the 4096 variants, {dt:.2f} s"}
 
 
+def cpu_baseline_lm(kind: str, runs: int = 256, seed: int = 20261203 + 2):
+    """LM cycles (adjoint Jacobian, normal equations, step, trial merit) of `runs` runs of the
+    same workload on all host threads: the reference's own optimize_lm_cpu (oracle/_ref).
+    Three cycles minus one cycle, halved, isolates the cost of a cycle from the start-up."""
+    import oracle.pyoracle as po
+    from mikroptim_b200 import workloads
+    from mikroptim_b200.batch import ResidualLayout
+    b, st, vs, x0 = workloads.objective(4096, seed=seed)
+    b = b.subset(0, runs)
+    lay = ResidualLayout(b.topology, st)
+    threads = os.cpu_count() or 1
+    ref = po.reference()
+    t0 = time.perf_counter()
+    ref.optimize_lm(b, lay, vs, x0[:runs], max_iterations=1, method="adjoint", threads=threads)
+    t1 = time.perf_counter()
+    ref.optimize_lm(b, lay, vs, x0[:runs], max_iterations=3, method="adjoint", threads=threads)
+    t2 = time.perf_counter()
+    per_cycle = max(((t2 - t1) - (t1 - t0)) / 2, 1e-9)
+    return {"value": runs / per_cycle, "unit": "LM run-iterations/s", "cores": threads,
+            "kind": kind, "sample": f"optimize_lm_cpu (adjoint) of {runs} of the 4096 runs, "
+                                     f"1 and 3 cycles, {t2 - t0:.1f} s"}
+
+
 def reference_kind() -> str:
     import oracle.pyoracle as po
     return "reference" if os.path.exists(po.REF_LIB) else "port"
@@ -312,6 +502,23 @@ def run_reference(args, world, rank):
     if rank != 0:
         return None
     kind = reference_kind()
+    if args.workload == "lm":
+        if kind != "reference":
+            return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
+        base = cpu_baseline_lm(kind, runs=128)
+        samples = [base["value"]]
+        v = base["value"]
+        return {
+            "metric": METRIC, "value": v, "unit": "LM run-iterations/s", "impl": "reference",
+            "n_gpus": world, "steps": len(samples), "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, configuration-2 shapes)",
+            "config": {"workload": WORKLOAD, "step": "one LM cycle of a 128-run sample on the host"},
+            "cpu_baseline": {"value": v, "unit": "LM run-iterations/s", "cores": base["cores"],
+                             "kind": kind, "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "LM run-iterations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
     samples = []
     for i in range(args.warmup + args.steps):
         r = cpu_baseline(kind, sample_variants=8)
@@ -337,6 +544,13 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "lm":
+        out, _ = run_lm(args, world, rank, local)
+        if rank == 0 and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline_lm(reference_kind())
+            except Exception as e:  # the baseline is reported, not required
+                out["cpu_baseline"] = {"value": None, "error": str(e)}
     else:
         out, _ = run_b200(args, world, rank, local)
         if rank == 0 and world == 1:
