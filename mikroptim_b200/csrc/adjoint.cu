@@ -562,6 +562,174 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
     }
 }
 
+// Mixed precision: forward in the mixed scheme (FP64 positions, sag root and OPL, FP32
+// directions and refraction; checkpoints keep the FP64 position and the FP32 direction), the
+// reverse sweep entirely in FP32 on the states rounded to FP32.
+struct MixedPrecision {};
+
+__device__ void fused_forward_mixed(const TraceParams& p, const double* rec,
+                                    const RecordLayout& lay, int f, int l, const Sample& smp,
+                                    bool soft_mode, double* ck, int stride_ck, uint64_t& br_lo,
+                                    uint64_t& br_hi, int& count, int& image_branch,
+                                    int& status_out, int& soft_first, double& opl,
+                                    double& penalty) {
+    const int S = p.S, L = p.L;
+    const double a = rec[lay.pupil];
+    const double st = rec[lay.sin_theta + f];
+    const double ct = rec[lay.cos_theta + f];
+    const double r0 = a * smp.rho;
+    RayMixed r;
+    r.px = r0 * smp.sin_phi;
+    r.py = r0 * smp.cos_phi;
+    r.pz = 0.0;
+    r.dx = 0.0f;
+    r.dy = static_cast<float>(st);
+    r.dz = static_cast<float>(ct);
+    r.opl = r.py * st;
+    SoftT<double> soft{0.0, kOk};
+    SoftT<double>* sp = soft_mode ? &soft : nullptr;
+    br_lo = br_hi = 0;
+    count = 1;
+    image_branch = kBranchRegular;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    double n_before = idx[l];
+    for (int s = 1; s < S; ++s) {
+        const double n_after = idx[s * L + l];
+        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        int branch;
+        status = step_surface_mixed(r, thick[s - 1], c, n_before, n_after, sp, branch);
+        if (status != kOk) break;
+        count = s + 1;
+        if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
+        else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
+        if (s % kInterval == 0) {
+            double* q = ck + (s / kInterval) * stride_ck;
+            q[0] = r.px;
+            q[1 * kFusedThreads] = r.py;
+            q[2 * kFusedThreads] = r.pz;
+            q[3 * kFusedThreads] = r.dx;
+            q[4 * kFusedThreads] = r.dy;
+            q[5 * kFusedThreads] = r.dz;
+        }
+        n_before = n_after;
+    }
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > 0.0f)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step_mixed(r, rec[lay.target + f], thick[S - 1], n_before,
+                                                 sp, branch);
+            if (!in_piston(rst)) {
+                status = rst;
+            } else {
+                image_branch = branch;
+                if (status == kOk) status = rst;
+            }
+        }
+    }
+    status_out = status;
+    soft_first = soft.first;
+    opl = r.opl;
+    penalty = soft.penalty;
+}
+
+__device__ __noinline__ void fused_backward_mixed(const TraceParams& p, const VarParams& v,
+                                                  const double* rec, const RecordLayout& lay,
+                                                  int f, int l, const Sample& smp,
+                                                  const double* ck, int stride_ck,
+                                                  uint64_t br_lo, uint64_t br_hi, int count,
+                                                  int image_branch, bool reached_image,
+                                                  bool soft_mode, float seed_opl, float seed_pen,
+                                                  float factor, double* row, int ld) {
+    using F = float;
+    const int S = p.S, L = p.L;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    RayAdj<F> adj{{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    int next_branch = kBranchRegular;
+    const Vec<F> center{0.f, static_cast<F>(rec[lay.target + f]), static_cast<F>(thick[S - 1])};
+    auto branch_of = [&](int s) {
+        return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
+                      : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
+    };
+    for (int c = (count - 1) / kInterval; c >= 0; --c) {
+        const int first = c * kInterval;
+        const int n = (count - first) < kInterval ? (count - first) : kInterval;
+        Vec<F> sp[kInterval], sd[kInterval];
+        RayMixed r;
+        if (c == 0) {
+            const double r0 = rec[lay.pupil] * smp.rho;
+            r.px = r0 * smp.sin_phi;
+            r.py = r0 * smp.cos_phi;
+            r.pz = 0.0;
+            r.dx = 0.0f;
+            r.dy = static_cast<float>(rec[lay.sin_theta + f]);
+            r.dz = static_cast<float>(rec[lay.cos_theta + f]);
+        } else {
+            const double* q = ck + c * stride_ck;
+            r.px = q[0];
+            r.py = q[kFusedThreads];
+            r.pz = q[2 * kFusedThreads];
+            r.dx = static_cast<float>(q[3 * kFusedThreads]);
+            r.dy = static_cast<float>(q[4 * kFusedThreads]);
+            r.dz = static_cast<float>(q[5 * kFusedThreads]);
+        }
+        r.opl = 0.0;
+        sp[0] = {static_cast<F>(r.px), static_cast<F>(r.py), static_cast<F>(r.pz)};
+        sd[0] = {r.dx, r.dy, r.dz};
+        SoftT<double> dummy{0.0, kOk};
+#pragma unroll
+        for (int i = 1; i < kInterval; ++i) {
+            if (i < n) {
+                const int s = first + i;
+                const double cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+                int branch;
+                step_surface_mixed(r, thick[s - 1], cs, idx[(s - 1) * L + l], idx[s * L + l],
+                                   soft_mode ? &dummy : nullptr, branch);
+                sp[i] = {static_cast<F>(r.px), static_cast<F>(r.py), static_cast<F>(r.pz)};
+                sd[i] = {r.dx, r.dy, r.dz};
+            }
+        }
+#pragma unroll
+        for (int i = kInterval - 1; i >= 0; --i) {
+            if (i < n) {
+                const int s = first + i;
+                if (s == count - 1) {
+                    if (reached_image && count == S) {
+                        Vec<F> center_adj{0.f, 0.f, 0.f};
+                        F n_image_adj = 0.f;
+                        reference_step_backward<F>(sp[i], sd[i], center,
+                                                   static_cast<F>(idx[(S - 1) * L + l]),
+                                                   image_branch, seed_opl, seed_pen, adj,
+                                                   center_adj, n_image_adj);
+                        const int col = v.col_thickness[S - 1];
+                        if (col >= 0) row[col * ld] = factor * center_adj.z;
+                    }
+                } else {
+                    const int j = s + 1;
+                    const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
+                    const F cj = sphere ? static_cast<F>(curv[j]) : 0.f;
+                    StepAdj<F> par{0.f, 0.f, 0.f, 0.f};
+                    refracting_step_backward<F>(sp[i], sd[i], static_cast<F>(thick[s]), cj,
+                                                static_cast<F>(idx[s * L + l]),
+                                                static_cast<F>(idx[j * L + l]), next_branch,
+                                                seed_opl, seed_pen, adj, par);
+                    if (sphere && v.col_curvature[j] >= 0)
+                        row[v.col_curvature[j] * ld] = factor * par.curvature;
+                    if (v.col_thickness[s] >= 0) row[v.col_thickness[s] * ld] = factor * par.thickness;
+                }
+                next_branch = branch_of(s);
+            }
+        }
+    }
+}
+
 template <class N>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __restrict__ records,
@@ -625,12 +793,21 @@ adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __re
             k = within - l * p.sample_count[f];
             tu = f * p.L + l;
             smp = pupil_sample(p, sh.tab, f, k);
-            fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
-                             br_hi, count, image_branch, status, soft_first, opl, penalty);
+            if constexpr (std::is_same<N, MixedPrecision>::value)
+                fused_forward_mixed(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
+                                    br_hi, count, image_branch, status, soft_first, opl, penalty);
+            else
+                fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
+                                 br_hi, count, image_branch, status, soft_first, opl, penalty);
             if (in_piston(status)) {
-                fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo, br_hi,
-                                  count, image_branch, true, soft_mode, N(1.0), N(0.0), N(1.0),
-                                  row, TS);
+                if constexpr (std::is_same<N, MixedPrecision>::value)
+                    fused_backward_mixed(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                         br_hi, count, image_branch, true, soft_mode, 1.0f, 0.0f,
+                                         1.0f, row, TS);
+                else
+                    fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                      br_hi, count, image_branch, true, soft_mode, N(1.0),
+                                      N(0.0), N(1.0), row, TS);
                 row[P * TS] = opl;
             }
         }
@@ -711,13 +888,21 @@ adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         if (sh.any_failed) {
             for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
             if (q < p.rays && status != kOk) {
-                const N factor = N(p.pscale[tu]) * N(smp.root_weight);
-                if (soft_first != kOk)
-                    fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
-                                      br_hi, count, image_branch, in_piston(status), soft_mode,
-                                      N(0.0), N(1.0), factor, row, TS);
+                const double factor = p.pscale[tu] * smp.root_weight;
+                if (soft_first != kOk) {
+                    if constexpr (std::is_same<N, MixedPrecision>::value)
+                        fused_backward_mixed(p, v, record, lay, f, l, smp, my_ck, stride_ck,
+                                             br_lo, br_hi, count, image_branch, in_piston(status),
+                                             soft_mode, 0.0f, 1.0f, static_cast<float>(factor),
+                                             row, TS);
+                    else
+                        fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                          br_hi, count, image_branch, in_piston(status),
+                                          soft_mode, N(0.0), N(1.0),
+                                          N(p.pscale[tu]) * N(smp.root_weight), row, TS);
+                }
                 const double fp = is_soft(status) ? penalty : penalty + 1.0;
-                row[P * TS] = value_of(factor * N(fp));
+                row[P * TS] = factor * fp;
             }
             __syncthreads();
             accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
@@ -754,13 +939,15 @@ size_t fused_adjoint_smem(const TraceParams& tp, int P) {
 }
 
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, bool exact, cudaStream_t stream) {
+                        double* gram, int precision, cudaStream_t stream) {
     AdjointParams ap;
     ap.t = tp;
     ap.v = vp;
     ap.rows = 0;
     const size_t smem = fused_adjoint_smem(tp, vp.P);
-    auto kernel = exact ? adjoint_gram_kernel<Exact64> : adjoint_gram_kernel<double>;
+    auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
+                  : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>
+                                                     : adjoint_gram_kernel<double>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");

@@ -12,10 +12,10 @@
 namespace mkb {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     int64_t stride, double* opd, uint8_t* status, int precision,
                      cudaStream_t stream);
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 int64_t* hard, void* workspace, size_t ws_bytes, int precision,
                  cudaStream_t stream);
 size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
@@ -382,7 +382,8 @@ int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan*
     TraceParams p;
     int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
         set_error("residuals: precision %d not available for RESIDUALS", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -397,8 +398,7 @@ int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan*
         set_error("residuals: output is null");
         return MKB_ERR_ARGUMENT;
     }
-    return launch_residuals(p, batch->records, residuals, stride, opd, status,
-                            plan->precision == MKB_PRECISION_FP64,
+    return launch_residuals(p, batch->records, residuals, stride, opd, status, plan->precision,
                             static_cast<cudaStream_t>(stream));
 }
 
@@ -413,8 +413,9 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
     TraceParams p;
     int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
-        set_error("merit: precision %d not built yet", plan->precision);
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
+        set_error("merit: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
     if (p.V == 0) return MKB_OK;
@@ -423,8 +424,7 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
         return MKB_ERR_ARGUMENT;
     }
     return launch_merit(p, batch->records, merit, failed, hard_failed, workspace,
-                        workspace_bytes, plan->precision == MKB_PRECISION_FP64,
-                        static_cast<cudaStream_t>(stream));
+                        workspace_bytes, plan->precision, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -19,7 +19,7 @@
 namespace mkb {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     int64_t stride, double* opd, uint8_t* status, int precision,
                      cudaStream_t stream);
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
                  int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
@@ -28,7 +28,7 @@ int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows
 int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
                       const uint8_t* status, double* J, bool exact, cudaStream_t stream);
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, bool exact, cudaStream_t stream);
+                        double* gram, int precision, cudaStream_t stream);
 int pack_rays_default();
 
 namespace {
@@ -280,7 +280,7 @@ int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual
         if (rc != MKB_OK) break;
         TraceParams chunk_tp = tp;
         chunk_tp.V = cnt * n;
-        rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, exact, stream);
+        rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, plan->precision, stream);
         if (rc != MKB_OK) break;
         const int64_t total = static_cast<int64_t>(cnt) * (P + 1) * R;
         const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 64));
@@ -345,7 +345,7 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
     rc = cuda_status(cudaMemsetAsync(J, 0, sizeof(double) * static_cast<size_t>(runs) * vp.P * R,
                                      stream), "adjoint jacobian: clear J");
     if (rc != MKB_OK) return rc;
-    rc = launch_residuals(tp, records, r0, R, nullptr, status, exact, stream);
+    rc = launch_residuals(tp, records, r0, R, nullptr, status, plan->precision, stream);
     if (rc != MKB_OK) return rc;
     rc = launch_adjoint_rows(tp, vp, R, records, J, exact, stream);
     if (rc != MKB_OK) return rc;
@@ -370,7 +370,8 @@ int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
     b.variants = runs;
     rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
         set_error("adjoint normal equations: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -390,8 +391,7 @@ int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
     const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
     if (rc != MKB_OK) return rc;
-    return launch_adjoint_gram(tp, vp, records, gram, plan->precision == MKB_PRECISION_FP64,
-                               stream);
+    return launch_adjoint_gram(tp, vp, records, gram, plan->precision, stream);
 }
 
 }  // extern "C"

@@ -431,10 +431,10 @@ MKB_DEFINE_ERROR_READER(lm_device_error)
 namespace mkb {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     int64_t stride, double* opd, uint8_t* status, int precision,
                      cudaStream_t stream);
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 int64_t* hard, void* workspace, size_t ws_bytes, int precision,
                  cudaStream_t stream);
 size_t merit_workspace_bytes(int V, int n_tuples);
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
@@ -446,7 +446,7 @@ int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
                 bool exact, cudaStream_t stream);
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, bool exact, cudaStream_t stream);
+                        double* gram, int precision, cudaStream_t stream);
 int pack_rays_default();
 
 namespace {
@@ -538,6 +538,7 @@ struct LmSetup {
     VarParams vp;
     LmOptionsDev o;
     bool fd, exact, gram_exact, fused;
+    int precision;
     int64_t R;
 };
 
@@ -555,7 +556,8 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     b.variants = runs;
     int rc = make_trace_params(&b, plan, pack_rays_default(), &s.tp);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
         set_error("lm: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -577,8 +579,14 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
            o.diag_floor, o.reject_new_failures};
     s.fd = o.jacobian == MKB_JACOBIAN_FD;
     s.exact = plan->precision == MKB_PRECISION_FP64;
+    s.precision = plan->precision;
     s.gram_exact = o.gram_exact != 0;
     s.fused = !s.fd && !s.gram_exact;
+    if (plan->precision == MKB_PRECISION_MIXED && !s.fused) {
+        set_error("lm: mixed precision runs with the fused adjoint (jacobian = adjoint, "
+                  "gram_exact = 0)");
+        return MKB_ERR_UNSUPPORTED;
+    }
     s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
     return MKB_OK;
 }
@@ -592,7 +600,7 @@ int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* tem
                           stream);
     if (rc != MKB_OK) return rc;
     return launch_merit(s.tp, L.records, merit, failed, hard, L.merit_ws, L.merit_ws_bytes,
-                        s.exact, stream);
+                        s.precision, stream);
 }
 
 }  // namespace
@@ -656,7 +664,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream);
         if (rc == MKB_OK)
-            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, s.exact, stream);
+            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, s.precision, stream);
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
@@ -665,7 +673,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
             rc = cuda_status(cudaMemsetAsync(L.J, 0, sizeof(double) * size_t(runs) * s.vp.P * s.R,
                                              stream), "lm: clear J");
         if (rc == MKB_OK)
-            rc = launch_residuals(s.tp, L.records, L.r0, s.R, nullptr, L.status, s.exact, stream);
+            rc = launch_residuals(s.tp, L.records, L.r0, s.R, nullptr, L.status, s.precision, stream);
         if (rc == MKB_OK)
             rc = launch_adjoint_rows(s.tp, s.vp, s.R, L.records, L.J, s.exact, stream);
         if (rc == MKB_OK)

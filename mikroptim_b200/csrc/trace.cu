@@ -95,6 +95,55 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const R
     return status;
 }
 
+// Mixed-precision trace of one ray (FP64 geometry and OPL, FP32 directions and refraction).
+__device__ inline int trace_ray_mixed(const TraceParams& p, const double* rec,
+                                      const RecordLayout& lay, int f, int l, const Sample& smp,
+                                      bool soft_mode, double& opl, double& penalty) {
+    const int S = p.S, L = p.L;
+    const double a = rec[lay.pupil];
+    const double st = rec[lay.sin_theta + f];
+    const double ct = rec[lay.cos_theta + f];
+    const double r0 = a * smp.rho;
+    RayMixed r;
+    r.px = r0 * smp.sin_phi;
+    r.py = r0 * smp.cos_phi;
+    r.pz = 0.0;
+    r.dx = 0.0f;
+    r.dy = static_cast<float>(st);
+    r.dz = static_cast<float>(ct);
+    r.opl = r.py * st;
+    SoftT<double> soft{0.0, kOk};
+    SoftT<double>* sp = soft_mode ? &soft : nullptr;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    double n_before = idx[l];
+    for (int s = 1; s < S; ++s) {
+        const double n_after = idx[s * L + l];
+        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        int branch;
+        status = step_surface_mixed(r, thick[s - 1], c, n_before, n_after, sp, branch);
+        if (status != kOk) break;
+        n_before = n_after;
+    }
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > 0.0f)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step_mixed(r, rec[lay.target + f], thick[S - 1], n_before,
+                                                 sp, branch);
+            if (!in_piston(rst)) status = rst;
+            else if (status == kOk) status = rst;
+        }
+    }
+    opl = r.opl;
+    penalty = soft.penalty;
+    return status;
+}
+
 __device__ inline double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -121,10 +170,11 @@ struct TupleOut {
 // order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
-template <bool kResiduals, bool kExact>
+template <bool kResiduals, int kPrecision>
 __global__ void __launch_bounds__(kThreads)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
+    constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
     using N = typename std::conditional<kExact, Exact64, double>::type;
     __shared__ SharedTrace sh;
     const int v = blockIdx.x / p.n_packs;
@@ -156,7 +206,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
+        const int st = kPrecision == MKB_PRECISION_MIXED
+                           ? trace_ray_mixed(p, sh.record, lay, f, l, smp, soft_mode, opl, pen)
+                           : trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
         sh.status[i] = static_cast<uint8_t>(st);
@@ -299,20 +351,22 @@ size_t merit_workspace(int V, int n_tuples) {
 }  // namespace
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, bool exact,
+                     int64_t stride, double* opd, uint8_t* status, int precision,
                      cudaStream_t stream) {
     TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr};
-    const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
-    if (exact)
-        trace_kernel<true, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+    if (precision == MKB_PRECISION_FP64)
+        trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
+    else if (precision == MKB_PRECISION_MIXED)
+        trace_kernel<true, MKB_PRECISION_MIXED><<<blocks, kThreads, 0, stream>>>(p, records, out);
     else
-        trace_kernel<true, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<true, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
     count_launch();
     return cuda_status(cudaGetLastError(), "residuals kernel launch");
 }
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, bool exact,
+                 int64_t* hard, void* workspace, size_t ws_bytes, int precision,
                  cudaStream_t stream) {
     const size_t need = merit_workspace(p.V, p.n_tuples);
     if (workspace == nullptr || ws_bytes < need) {
@@ -324,11 +378,13 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     TupleOut out{nullptr, 0, nullptr, nullptr, reinterpret_cast<double*>(ws),
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
                  reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int)))};
-    const int64_t blocks = static_cast<int64_t>(p.V) * p.n_packs;
-    if (exact)
-        trace_kernel<false, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+    if (precision == MKB_PRECISION_FP64)
+        trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
+    else if (precision == MKB_PRECISION_MIXED)
+        trace_kernel<false, MKB_PRECISION_MIXED><<<blocks, kThreads, 0, stream>>>(p, records, out);
     else
-        trace_kernel<false, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<false, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
     count_launch();
     int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
     if (rc != MKB_OK) return rc;
@@ -397,7 +453,8 @@ extern "C" int mkb_merit_noalloc_device(const mkb_device_batch* batch,
     TraceParams p;
     int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA) {
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
         set_error("no-allocation MERIT: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -418,6 +475,6 @@ extern "C" int mkb_merit_noalloc_device(const mkb_device_batch* batch,
     rc = noalloc_merit_scratch(&scratch);
     if (rc != MKB_OK) return rc;
     return launch_merit(p, batch->records, merit, failed, hard_failed, scratch,
-                        kNoAllocScratchBytes, plan->precision == MKB_PRECISION_FP64,
+                        kNoAllocScratchBytes, plan->precision,
                         static_cast<cudaStream_t>(stream));
 }
