@@ -346,20 +346,27 @@ MKB_DEFINE_ERROR_READER(adjoint_device_error)
 
 namespace mkb {
 // ---- fused adjoint + normal equations ---------------------------------------------------------
-// One CTA per run streams the run's rays in chunks of kFusedThreads (one ray per thread):
-//   A  forward with checkpoints in shared memory, then the OPL-seed reverse sweep writes the
-//      row y_k = [dOPL_k/dx | OPL_k] into shared memory (rays outside the piston: weight 0);
-//   B  per tuple segment of the chunk (threads = columns): weighted mean mu_seg, rows centred
-//      and scaled in place, x_k = s sqrt(W_k) (y_k - mu_seg), and the segment merged into the
-//      tuple's running mean with one extra row s sqrt(W_t W_seg / (W_t + W_seg)) (mu_seg - mu_t)
-//      (Chan, Golub, LeVeque): summed over the chunks, sum x x^T is s^2 sum_k W_k (y_k - ybar)
-//      (y_k - ybar)^T over the tuple -- exactly [J r]^T [J r] of the piston-projected rows
-//      J_k = s sqrt(W_k) (g_k - gbar), r_k = s sqrt(W_k) (OPL_k - piston), without a second
-//      pass over the tuple and without J in memory;
-//   C  FP64 tensor cores accumulate sum x x^T (mma.sync m8n8k4, 8 x 8 tiles of the upper
-//      triangle in registers, owned by the CTA's warps);
-//   D  in soft-failure mode, when the chunk has failed rays, the penalty rows
-//      [s_p sqrt(W) dpi/dx | p_k] (uncentred) are accumulated the same way.
+// Persistent CTAs take runs off a work queue; a CTA streams the run's rays in chunks of
+// kFusedThreads (one ray per thread):
+//   A  forward with checkpoints in shared memory, then ONE reverse sweep carrying two adjoint
+//      vectors (seed OPL = 1 and seed penalty = 1) that share the replay and the step-local
+//      quantities. The OPL row g_k = dOPL_k/dx goes to shared memory (Y, column-major, odd
+//      stride) with OPL_k beside it (Rv); the scaled penalty row s_p sqrt(W) dpi/dx goes to the
+//      CTA's slot of a global scratch buffer (L2-resident, coalesced: column c of thread t at
+//      [c][t]). Warps whose rays have no soft event run the single-seed sweep;
+//   B  per tuple segment of the chunk: weighted column means (a warp per column, shuffle sums)
+//      and the rows centred and scaled in place by all threads, x_k = s sqrt(W_k) (y_k -
+//      mu_seg); the segment is merged into the tuple's running mean with one extra row
+//      s sqrt(W_t W_seg / (W_t + W_seg)) (mu_seg - mu_t) (Chan, Golub, LeVeque). Summed over
+//      the chunks, sum x x^T is s^2 sum_k W_k (y_k - ybar)(y_k - ybar)^T over the tuple --
+//      exactly [J r]^T [J r] of the piston-projected rows J_k = s sqrt(W_k) (g_k - gbar),
+//      r_k = s sqrt(W_k) (OPL_k - piston), with no second pass over the tuple and no J in
+//      memory;
+//   C  FP64 tensor cores accumulate J^T J (mma.sync m8n8k4 on 8 x 8 tiles of the upper
+//      triangle, accumulators in shared memory in fragment order); J^T r and r^T r are
+//      per-thread partial sums (thread = column x row phase) reduced once per run;
+//   D  in soft-failure mode, when the chunk has failed rays, the penalty rows (uncentred, value
+//      s_p sqrt(W) p_k) are loaded from the scratch slot into Y and accumulated the same way.
 // Output: gram [runs][P+1][P+1] as the normal-equation kernels write it.
 namespace {
 
@@ -367,21 +374,33 @@ constexpr int kFusedThreads = 128;
 constexpr int kFusedWarps = kFusedThreads / 32;
 constexpr int kExtraRows = 8;
 constexpr int kFusedMinBlocks = 3;  // CTAs per SM the register budget is sized for
-constexpr int kMaxTileCols = (MKB_MAX_VARIABLES + 1 + 7) / 8;                   // 9
-constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 45
+constexpr int kFusedInterval = 1;   // surfaces per checkpoint segment of the fused sweep
+constexpr bool kFusedDual = true;   // one two-seed sweep for rays with both rows
+constexpr int kMaxTileCols = MKB_MAX_VARIABLES / 8;                              // 8
+constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 36
+constexpr int kMaxFusedSlots = 148 * 8;  // persistent CTAs at most (SMs x resident CTAs)
+
+__host__ __device__ inline int fused_np(int P) { return ((P + 7) / 8) * 8; }
 
 struct FusedShared {
     uint64_t bar;
     SharedTables tab;
     double w[kFusedThreads];      // sample weight if the ray is in the piston, else 0
+    double sw[kFusedThreads];     // sqrt of w
     int tuple[kFusedThreads];     // tuple of the ray (-1 past the end)
-    double seg_w;                 // weight of the current segment
     double open_w;                // running weight of the open tuple
     int open_tuple;               // tuple whose running mean is kept
     int extra;                    // extra rows pending
-    int any_failed;               // chunk has a ray with status != Ok (soft mode)
+    int any_pen;                  // chunk has a penalty row (soft mode)
+    int run;                      // run taken off the queue
     int2 tiles[kMaxTilePairs];    // (row tile, column tile) of every upper-triangle pair
 };
+
+__device__ __forceinline__ double fused_warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -408,6 +427,27 @@ __device__ __forceinline__ void accumulate(const double* xt, int ld, int n, int 
     }
 }
 
+// Partial sums of J^T r (columns c = lane and lane + 32 of the rows r = warp (mod 4)) and of
+// r^T r (lane 0 of every warp).
+__device__ __forceinline__ void accumulate_r(const double* xt, int ld, const double* rv, int n,
+                                             int NP, double& j0, double& j1, double& rr) {
+    const int c = threadIdx.x & 31;
+    for (int r = threadIdx.x >> 5; r < n; r += kFusedWarps) {
+        const double v = rv[r];
+        if (c < NP) j0 += xt[c * ld + r] * v;
+        if (c + 32 < NP) j1 += xt[(c + 32) * ld + r] * v;
+        if (c == 0) rr += v * v;
+    }
+}
+
+// Where the reverse sweep writes: the OPL row (seed 0) and the penalty row (seed 1).
+template <int K>
+struct RowSinks {
+    double factor[K];
+    double* row[K];
+    int ld[K];
+};
+
 template <class N>
 __device__ void fused_forward(const TraceParams& p, const double* rec, const RecordLayout& lay,
                               int f, int l, const Sample& smp, bool soft_mode, double* ck,
@@ -430,15 +470,6 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
     r.opl = r.py * st;
     SoftT<N> soft{zero, kOk};
     SoftT<N>* sp = soft_mode ? &soft : nullptr;
-    auto save = [&](int c) {
-        double* q = ck + c * stride_ck;
-        q[0] = value_of(r.px);
-        q[1 * kFusedThreads] = value_of(r.py);
-        q[2 * kFusedThreads] = value_of(r.pz);
-        q[3 * kFusedThreads] = value_of(r.dx);
-        q[4 * kFusedThreads] = value_of(r.dy);
-        q[5 * kFusedThreads] = value_of(r.dz);
-    };
     br_lo = br_hi = 0;
     count = 1;
     image_branch = kBranchRegular;
@@ -456,7 +487,15 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
         count = s + 1;
         if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
         else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
-        if (s % kInterval == 0) save(s / kInterval);
+        if (s % kFusedInterval == 0) {  // checkpoint s / K (slot s / K - 1; the start ray is recomputed)
+            double* q = ck + (s / kFusedInterval - 1) * stride_ck;
+            q[0] = value_of(r.px);
+            q[1 * kFusedThreads] = value_of(r.py);
+            q[2 * kFusedThreads] = value_of(r.pz);
+            q[3 * kFusedThreads] = value_of(r.dx);
+            q[4 * kFusedThreads] = value_of(r.dy);
+            q[5 * kFusedThreads] = value_of(r.dz);
+        }
         n_before = n_after;
     }
     if (status == kOk && soft_mode) status = soft.first;
@@ -481,44 +520,63 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
     penalty = value_of(soft.penalty);
 }
 
-// Reverse sweep of one seed writing factor * dPhi/dx into row[col * ld]. One out-of-line copy
-// serves both seeds (keeps the kernel's instruction footprint small).
-template <class N>
-__device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v, const double* rec,
-                               const RecordLayout& lay, int f, int l, const Sample& smp,
-                               const double* ck,
-                               int stride_ck, uint64_t br_lo, uint64_t br_hi, int count,
-                               int image_branch, bool reached_image, bool soft_mode, N seed_opl,
-                               N seed_pen, N factor, double* row, int ld) {
+// Reverse sweep with K adjoint vectors (seed k: OPL seed so[k], penalty seed sp[k]) writing
+// factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. One out-of-line copy per K keeps the
+// kernel's instruction footprint small.
+template <class N, int K>
+__device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
+                                            const double* rec, const RecordLayout& lay, int f,
+                                            int l, const Sample& smp, const double* ck,
+                                            int stride_ck, uint64_t br_lo, uint64_t br_hi,
+                                            int count, int image_branch, bool reached_image,
+                                            bool soft_mode, const double (&so)[K],
+                                            const double (&spn)[K], const RowSinks<K>& sinks) {
     const int S = p.S, L = p.L;
     const N zero(0.0);
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
-    RayAdj<N> adj{{zero, zero, zero}, {zero, zero, zero}};
+    N seed_opl[K], seed_pen[K], factor[K];
+    RayAdj<N> adj[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        seed_opl[m] = so[m];
+        seed_pen[m] = spn[m];
+        factor[m] = sinks.factor[m];
+        adj[m] = {{zero, zero, zero}, {zero, zero, zero}};
+    }
     int next_branch = kBranchRegular;
     const Vec<N> center{zero, N(rec[lay.target + f]), N(thick[S - 1])};
     auto branch_of = [&](int s) {
         return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
                       : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
     };
-    for (int c = (count - 1) / kInterval; c >= 0; --c) {
-        const int first = c * kInterval;
-        const int n = (count - first) < kInterval ? (count - first) : kInterval;
-        Vec<N> sp[kInterval], sd[kInterval];
-        if (c == 0) {  // the start ray is recomputed (collimated_ray), not stored
+    // the state that starts segment c: the start ray is recomputed (collimated_ray), the others
+    // are loaded from the checkpoint slots one segment ahead of their use
+    auto segment_start = [&](int c, Vec<N>& p0, Vec<N>& d0) {
+        if (c == 0) {
             const N r0 = N(rec[lay.pupil]) * N(smp.rho);
-            sp[0] = {r0 * N(smp.sin_phi), r0 * N(smp.cos_phi), zero};
-            sd[0] = {zero, N(rec[lay.sin_theta + f]), N(rec[lay.cos_theta + f])};
+            p0 = {r0 * N(smp.sin_phi), r0 * N(smp.cos_phi), zero};
+            d0 = {zero, N(rec[lay.sin_theta + f]), N(rec[lay.cos_theta + f])};
         } else {
-            const double* q = ck + c * stride_ck;
-            sp[0] = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
-            sd[0] = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
+            const double* q = ck + (c - 1) * stride_ck;
+            p0 = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
+            d0 = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
         }
+    };
+    Vec<N> next_p, next_d;
+    segment_start((count - 1) / kFusedInterval, next_p, next_d);
+    for (int c = (count - 1) / kFusedInterval; c >= 0; --c) {
+        const int first = c * kFusedInterval;
+        const int n = (count - first) < kFusedInterval ? (count - first) : kFusedInterval;
+        Vec<N> sp[kFusedInterval], sd[kFusedInterval];
+        sp[0] = next_p;
+        sd[0] = next_d;
+        if (c > 0) segment_start(c - 1, next_p, next_d);
         RayT<N> r{sp[0].x, sp[0].y, sp[0].z, sd[0].x, sd[0].y, sd[0].z, zero};
         SoftT<N> dummy{zero, kOk};
 #pragma unroll
-        for (int i = 1; i < kInterval; ++i) {
+        for (int i = 1; i < kFusedInterval; ++i) {
             if (i < n) {
                 const int s = first + i;
                 const N cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
@@ -530,31 +588,47 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
             }
         }
 #pragma unroll
-        for (int i = kInterval - 1; i >= 0; --i) {
+        for (int i = kFusedInterval - 1; i >= 0; --i) {
             if (i < n) {
                 const int s = first + i;
                 if (s == count - 1) {
                     if (reached_image && count == S) {
-                        Vec<N> center_adj{zero, zero, zero};
-                        N n_image_adj = zero;
-                        reference_step_backward<N>(sp[i], sd[i], center, N(idx[(S - 1) * L + l]),
-                                                   image_branch, seed_opl, seed_pen, adj,
-                                                   center_adj, n_image_adj);
+                        Vec<N> center_adj[K];
+                        N n_image_adj[K];
+#pragma unroll
+                        for (int m = 0; m < K; ++m) {
+                            center_adj[m] = {zero, zero, zero};
+                            n_image_adj[m] = zero;
+                        }
+                        reference_step_backward_k<N, K>(sp[i], sd[i], center,
+                                                        N(idx[(S - 1) * L + l]), image_branch,
+                                                        seed_opl, seed_pen, adj, center_adj,
+                                                        n_image_adj);
                         const int col = v.col_thickness[S - 1];
-                        if (col >= 0) row[col * ld] = value_of(factor * center_adj.z);
+                        if (col >= 0) {
+#pragma unroll
+                            for (int m = 0; m < K; ++m)
+                                sinks.row[m][col * sinks.ld[m]] =
+                                    value_of(factor[m] * center_adj[m].z);
+                        }
                     }
                 } else {
                     const int j = s + 1;
                     const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
                     const N cj = sphere ? curv[j] : 0.0;
-                    StepAdj<N> par{zero, zero, zero, zero};
-                    refracting_step_backward<N>(sp[i], sd[i], N(thick[s]), cj, N(idx[s * L + l]),
-                                                N(idx[j * L + l]), next_branch, seed_opl,
-                                                seed_pen, adj, par);
-                    if (sphere && v.col_curvature[j] >= 0)
-                        row[v.col_curvature[j] * ld] = value_of(factor * par.curvature);
-                    if (v.col_thickness[s] >= 0)
-                        row[v.col_thickness[s] * ld] = value_of(factor * par.thickness);
+                    StepAdj<N> par[K];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) par[m] = {zero, zero, zero, zero};
+                    refracting_step_backward_k<N, K>(sp[i], sd[i], N(thick[s]), cj,
+                                                     N(idx[s * L + l]), N(idx[j * L + l]),
+                                                     next_branch, seed_opl, seed_pen, adj, par);
+                    const int cc = sphere ? v.col_curvature[j] : -1;
+                    const int ct = v.col_thickness[s];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) {
+                        if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = value_of(factor[m] * par[m].curvature);
+                        if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = value_of(factor[m] * par[m].thickness);
+                    }
                 }
                 next_branch = branch_of(s);
             }
@@ -605,8 +679,8 @@ __device__ void fused_forward_mixed(const TraceParams& p, const double* rec,
         count = s + 1;
         if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
         else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
-        if (s % kInterval == 0) {
-            double* q = ck + (s / kInterval) * stride_ck;
+        if (s % kFusedInterval == 0) {
+            double* q = ck + (s / kFusedInterval - 1) * stride_ck;
             q[0] = r.px;
             q[1 * kFusedThreads] = r.py;
             q[2 * kFusedThreads] = r.pz;
@@ -638,54 +712,70 @@ __device__ void fused_forward_mixed(const TraceParams& p, const double* rec,
     penalty = soft.penalty;
 }
 
+template <int K>
 __device__ __noinline__ void fused_backward_mixed(const TraceParams& p, const VarParams& v,
                                                   const double* rec, const RecordLayout& lay,
                                                   int f, int l, const Sample& smp,
                                                   const double* ck, int stride_ck,
                                                   uint64_t br_lo, uint64_t br_hi, int count,
                                                   int image_branch, bool reached_image,
-                                                  bool soft_mode, float seed_opl, float seed_pen,
-                                                  float factor, double* row, int ld) {
+                                                  bool soft_mode, const double (&so)[K],
+                                                  const double (&spn)[K],
+                                                  const RowSinks<K>& sinks) {
     using F = float;
     const int S = p.S, L = p.L;
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
-    RayAdj<F> adj{{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    F seed_opl[K], seed_pen[K], factor[K];
+    RayAdj<F> adj[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        seed_opl[m] = static_cast<F>(so[m]);
+        seed_pen[m] = static_cast<F>(spn[m]);
+        factor[m] = static_cast<F>(sinks.factor[m]);
+        adj[m] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    }
     int next_branch = kBranchRegular;
     const Vec<F> center{0.f, static_cast<F>(rec[lay.target + f]), static_cast<F>(thick[S - 1])};
     auto branch_of = [&](int s) {
         return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
                       : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
     };
-    for (int c = (count - 1) / kInterval; c >= 0; --c) {
-        const int first = c * kInterval;
-        const int n = (count - first) < kInterval ? (count - first) : kInterval;
-        Vec<F> sp[kInterval], sd[kInterval];
-        RayMixed r;
+    // segment start states, loaded one segment ahead of their use (see fused_backward)
+    auto segment_start = [&](int c, RayMixed& r0s) {
         if (c == 0) {
             const double r0 = rec[lay.pupil] * smp.rho;
-            r.px = r0 * smp.sin_phi;
-            r.py = r0 * smp.cos_phi;
-            r.pz = 0.0;
-            r.dx = 0.0f;
-            r.dy = static_cast<float>(rec[lay.sin_theta + f]);
-            r.dz = static_cast<float>(rec[lay.cos_theta + f]);
+            r0s.px = r0 * smp.sin_phi;
+            r0s.py = r0 * smp.cos_phi;
+            r0s.pz = 0.0;
+            r0s.dx = 0.0f;
+            r0s.dy = static_cast<float>(rec[lay.sin_theta + f]);
+            r0s.dz = static_cast<float>(rec[lay.cos_theta + f]);
         } else {
-            const double* q = ck + c * stride_ck;
-            r.px = q[0];
-            r.py = q[kFusedThreads];
-            r.pz = q[2 * kFusedThreads];
-            r.dx = static_cast<float>(q[3 * kFusedThreads]);
-            r.dy = static_cast<float>(q[4 * kFusedThreads]);
-            r.dz = static_cast<float>(q[5 * kFusedThreads]);
+            const double* q = ck + (c - 1) * stride_ck;
+            r0s.px = q[0];
+            r0s.py = q[kFusedThreads];
+            r0s.pz = q[2 * kFusedThreads];
+            r0s.dx = static_cast<float>(q[3 * kFusedThreads]);
+            r0s.dy = static_cast<float>(q[4 * kFusedThreads]);
+            r0s.dz = static_cast<float>(q[5 * kFusedThreads]);
         }
+    };
+    RayMixed next;
+    segment_start((count - 1) / kFusedInterval, next);
+    for (int c = (count - 1) / kFusedInterval; c >= 0; --c) {
+        const int first = c * kFusedInterval;
+        const int n = (count - first) < kFusedInterval ? (count - first) : kFusedInterval;
+        Vec<F> sp[kFusedInterval], sd[kFusedInterval];
+        RayMixed r = next;
+        if (c > 0) segment_start(c - 1, next);
         r.opl = 0.0;
         sp[0] = {static_cast<F>(r.px), static_cast<F>(r.py), static_cast<F>(r.pz)};
         sd[0] = {r.dx, r.dy, r.dz};
         SoftT<double> dummy{0.0, kOk};
 #pragma unroll
-        for (int i = 1; i < kInterval; ++i) {
+        for (int i = 1; i < kFusedInterval; ++i) {
             if (i < n) {
                 const int s = first + i;
                 const double cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
@@ -697,32 +787,47 @@ __device__ __noinline__ void fused_backward_mixed(const TraceParams& p, const Va
             }
         }
 #pragma unroll
-        for (int i = kInterval - 1; i >= 0; --i) {
+        for (int i = kFusedInterval - 1; i >= 0; --i) {
             if (i < n) {
                 const int s = first + i;
                 if (s == count - 1) {
                     if (reached_image && count == S) {
-                        Vec<F> center_adj{0.f, 0.f, 0.f};
-                        F n_image_adj = 0.f;
-                        reference_step_backward<F>(sp[i], sd[i], center,
-                                                   static_cast<F>(idx[(S - 1) * L + l]),
-                                                   image_branch, seed_opl, seed_pen, adj,
-                                                   center_adj, n_image_adj);
+                        Vec<F> center_adj[K];
+                        F n_image_adj[K];
+#pragma unroll
+                        for (int m = 0; m < K; ++m) {
+                            center_adj[m] = {0.f, 0.f, 0.f};
+                            n_image_adj[m] = 0.f;
+                        }
+                        reference_step_backward_k<F, K>(sp[i], sd[i], center,
+                                                        static_cast<F>(idx[(S - 1) * L + l]),
+                                                        image_branch, seed_opl, seed_pen, adj,
+                                                        center_adj, n_image_adj);
                         const int col = v.col_thickness[S - 1];
-                        if (col >= 0) row[col * ld] = factor * center_adj.z;
+                        if (col >= 0) {
+#pragma unroll
+                            for (int m = 0; m < K; ++m)
+                                sinks.row[m][col * sinks.ld[m]] = factor[m] * center_adj[m].z;
+                        }
                     }
                 } else {
                     const int j = s + 1;
                     const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
                     const F cj = sphere ? static_cast<F>(curv[j]) : 0.f;
-                    StepAdj<F> par{0.f, 0.f, 0.f, 0.f};
-                    refracting_step_backward<F>(sp[i], sd[i], static_cast<F>(thick[s]), cj,
-                                                static_cast<F>(idx[s * L + l]),
-                                                static_cast<F>(idx[j * L + l]), next_branch,
-                                                seed_opl, seed_pen, adj, par);
-                    if (sphere && v.col_curvature[j] >= 0)
-                        row[v.col_curvature[j] * ld] = factor * par.curvature;
-                    if (v.col_thickness[s] >= 0) row[v.col_thickness[s] * ld] = factor * par.thickness;
+                    StepAdj<F> par[K];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) par[m] = {0.f, 0.f, 0.f, 0.f};
+                    refracting_step_backward_k<F, K>(sp[i], sd[i], static_cast<F>(thick[s]), cj,
+                                                     static_cast<F>(idx[s * L + l]),
+                                                     static_cast<F>(idx[j * L + l]), next_branch,
+                                                     seed_opl, seed_pen, adj, par);
+                    const int cc = sphere ? v.col_curvature[j] : -1;
+                    const int ct = v.col_thickness[s];
+#pragma unroll
+                    for (int m = 0; m < K; ++m) {
+                        if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = factor[m] * par[m].curvature;
+                        if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = factor[m] * par[m].thickness;
+                    }
                 }
                 next_branch = branch_of(s);
             }
@@ -730,42 +835,59 @@ __device__ __noinline__ void fused_backward_mixed(const TraceParams& p, const Va
     }
 }
 
+template <class N, int K>
+__device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
+                                             const double* rec, const RecordLayout& lay, int f,
+                                             int l, const Sample& smp, const double* ck,
+                                             int stride_ck, uint64_t br_lo, uint64_t br_hi,
+                                             int count, int image_branch, bool reached_image,
+                                             bool soft_mode, const double (&so)[K],
+                                             const double (&spn)[K], const RowSinks<K>& sinks) {
+    if constexpr (std::is_same<N, MixedPrecision>::value)
+        fused_backward_mixed<K>(p, v, rec, lay, f, l, smp, ck, stride_ck, br_lo, br_hi, count,
+                                image_branch, reached_image, soft_mode, so, spn, sinks);
+    else
+        fused_backward<N, K>(p, v, rec, lay, f, l, smp, ck, stride_ck, br_lo, br_hi, count,
+                             image_branch, reached_image, soft_mode, so, spn, sinks);
+}
+
+struct FusedArgs {
+    AdjointParams ap;
+    const double* records;
+    double* gram;
+    double* scratch;       // [slots][slot_doubles]: penalty rows and checkpoints per CTA
+    int64_t slot_doubles;
+    int* queue;            // run counter
+};
+
 template <class N>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
-adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __restrict__ records,
-                    double* __restrict__ gram) {
-    const TraceParams& p = ap.t;
-    const VarParams& v = ap.v;
+adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
+    const TraceParams& p = fa.ap.t;
+    const VarParams& v = fa.ap.v;
     __shared__ FusedShared sh;
     extern __shared__ __align__(16) double dyn[];
     const int P = v.P;
-    const int NP = ((P + 1 + 7) / 8) * 8;
+    const int NP = fused_np(P);
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
-    const int nck = (p.S - 1) / kInterval + 1;
     const int stride_ck = 6 * kFusedThreads;
     constexpr int TS = kFusedThreads + 1;              // column stride of Y (odd: no conflicts)
     constexpr int ES = kExtraRows + 1;                 // column stride of E
     double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
-    double* Y = record + p.stride;                     // column-major [NP][TS]
-    double* E = Y + NP * TS;                           // column-major [NP][ES]
-    double* mu_open = E + NP * ES;                     // [NP]
-    double* mu_seg = mu_open + NP;                     // [NP]
-    double* acc = mu_seg + NP;                         // [pairs][32][2] DMMA accumulators
-    double* ckpt = acc + pairs * 64;                   // [nck][6][T], checkpoint 0 unused
-    const int tid = threadIdx.x;
-    const int run = blockIdx.x;
+    double* Y = record + ((p.stride + 1) & ~1);        // column-major [NP][TS]
+    double* Rv = Y + NP * TS;                          // residual column [TS]
+    double* E = Rv + TS;                               // column-major [NP + 1][ES]
+    double* mu_open = E + (NP + 1) * ES;               // [NP + 1]
+    double* mu_seg = mu_open + NP + 1;                 // [NP + 1]
+    double* acc = mu_seg + NP + 1;                     // [pairs][32][2] DMMA accumulators
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
-    copy_tables(p, sh.tab);
-    if (tid == 0) {
-        sh.open_tuple = -1;
-        sh.open_w = 0.0;
-        sh.extra = 0;
-    }
-    if (!stage_to_shared(record, records + static_cast<int64_t>(run) * p.stride,
-                         static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar))
-        return;
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
+    // this CTA's scratch slot: penalty rows [NP][T], then checkpoints 1 .. [nck - 1][6][T]
+    double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
+    double* ckpt = pen_slot + NP * kFusedThreads;
+    copy_tables(p, sh.tab);
     for (int e = tid; e < pairs; e += kFusedThreads) {
         int j = 0, rem = e;
         while (rem >= j + 1) {
@@ -774,176 +896,254 @@ adjoint_gram_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         }
         sh.tiles[e] = make_int2(rem, j);
     }
-    for (int i = tid; i < pairs * 64; i += kFusedThreads) acc[i] = 0.0;
-    __syncthreads();
     double* my_ck = ckpt + tid;
-    for (int base = 0; base < p.rays; base += kFusedThreads) {
-        const int q = base + tid;
-        double* row = Y + tid;  // this ray's row, column c at row[c * TS]
-        for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
-        int f = 0, l = 0, k = 0, tu = -1;
-        int status = kMissed, soft_first = kOk, count = 0, image_branch = 0;
-        uint64_t br_lo = 0, br_hi = 0;
-        double opl = 0.0, penalty = 0.0;
-        Sample smp{};
-        if (q < p.rays) {
-            while (f + 1 < p.F && q >= p.field_offset[f + 1]) ++f;
-            const int within = q - p.field_offset[f];
-            l = within / p.sample_count[f];
-            k = within - l * p.sample_count[f];
-            tu = f * p.L + l;
-            smp = pupil_sample(p, sh.tab, f, k);
-            if constexpr (std::is_same<N, MixedPrecision>::value)
-                fused_forward_mixed(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
-                                    br_hi, count, image_branch, status, soft_first, opl, penalty);
-            else
-                fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck, br_lo,
-                                 br_hi, count, image_branch, status, soft_first, opl, penalty);
-            if (in_piston(status)) {
-                if constexpr (std::is_same<N, MixedPrecision>::value)
-                    fused_backward_mixed(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
-                                         br_hi, count, image_branch, true, soft_mode, 1.0f, 0.0f,
-                                         1.0f, row, TS);
-                else
-                    fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
-                                      br_hi, count, image_branch, true, soft_mode, N(1.0),
-                                      N(0.0), N(1.0), row, TS);
-                row[P * TS] = opl;
-            }
-        }
-        sh.w[tid] = (q < p.rays && in_piston(status)) ? smp.weight : 0.0;
-        sh.tuple[tid] = tu;
-        if (tid == 0) sh.any_failed = 0;
+    uint32_t uses = 0;
+    for (;;) {
+        __syncthreads();  // the previous run's shared state is consumed
+        if (tid == 0) sh.run = atomicAdd(fa.queue, 1);
         __syncthreads();
-        if (soft_mode && q < p.rays && status != kOk) sh.any_failed = 1;
-        // ---- B: segments (threads = columns) ----
-        const int rows_here = p.rays - base < kFusedThreads ? p.rays - base : kFusedThreads;
-        int start = 0;
-        while (start < rows_here) {
-            const int t = sh.tuple[start];
-            int end = start + 1;
-            while (end < rows_here && sh.tuple[end] == t) ++end;
-            if (tid == 0) {
-                double w = 0.0;
-                for (int r = start; r < end; ++r) w += sh.w[r];
-                sh.seg_w = w;
-            }
-            __syncthreads();
-            const double wseg = sh.seg_w;
-            const double scale = p.scale[t];
-            if (wseg > 0.0) {
-                if (tid < NP) {
-                    double s = 0.0;
-                    double* col = Y + tid * TS;
-                    for (int r = start; r < end; ++r) s += sh.w[r] * col[r];
-                    const double mean = s / wseg;
-                    mu_seg[tid] = mean;
-                    for (int r = start; r < end; ++r) {
-                        const double x = col[r];
-                        col[r] = sh.w[r] > 0.0 ? scale * sqrt(sh.w[r]) * (x - mean) : 0.0;
+        const int run = sh.run;
+        if (run >= p.V) break;
+        if (tid == 0) {
+            sh.open_tuple = -1;
+            sh.open_w = 0.0;
+            sh.extra = 0;
+        }
+        for (int i = tid; i < pairs * 64; i += kFusedThreads) acc[i] = 0.0;
+        if (!stage_to_shared(record, fa.records + static_cast<int64_t>(run) * p.stride,
+                             static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar, uses++))
+            return;
+        double j0 = 0.0, j1 = 0.0, rr = 0.0;
+        for (int base = 0; base < p.rays; base += kFusedThreads) {
+            const int q = base + tid;
+            double* row = Y + tid;  // this ray's row, column c at row[c * TS]
+            for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
+            double* prow = pen_slot + tid;  // this ray's penalty row, column c at prow[c * T]
+            int tu = -1, status = kMissed;
+            bool has_pen = false;
+            double pen_val = 0.0, opl_val = 0.0;
+            Sample smp{};
+            if (q < p.rays) {
+                int f = 0;
+                while (f + 1 < p.F && q >= p.field_offset[f + 1]) ++f;
+                const int within = q - p.field_offset[f];
+                const int l = within / p.sample_count[f];
+                const int k = within - l * p.sample_count[f];
+                tu = f * p.L + l;
+                smp = pupil_sample(p, sh.tab, f, k);
+                int soft_first = kOk, count = 0, image_branch = 0;
+                uint64_t br_lo = 0, br_hi = 0;
+                double opl = 0.0, penalty = 0.0;
+                if constexpr (std::is_same<N, MixedPrecision>::value)
+                    fused_forward_mixed(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck,
+                                        br_lo, br_hi, count, image_branch, status, soft_first,
+                                        opl, penalty);
+                else
+                    fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck,
+                                     br_lo, br_hi, count, image_branch, status, soft_first, opl,
+                                     penalty);
+                const bool piston = in_piston(status);
+                has_pen = soft_mode && status != kOk;
+                const bool pen_sweep = has_pen && soft_first != kOk;
+                const double pfac = has_pen ? p.pscale[tu] * smp.root_weight : 0.0;
+                if (has_pen) {
+                    for (int c = 0; c < NP; ++c) prow[c * kFusedThreads] = 0.0;
+                    pen_val = pfac * (is_soft(status) ? penalty : penalty + 1.0);
+                }
+                if (piston) opl_val = opl;
+                // the OPL row into Y, the penalty row into the scratch slot
+                if (kFusedDual && __any_sync(__activemask(), piston && pen_sweep)) {
+                    if (piston || pen_sweep) {
+                        const double so[2] = {piston ? 1.0 : 0.0, 0.0};
+                        const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
+                        const RowSinks<2> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
+                        run_backward<N, 2>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                           br_hi, count, image_branch, piston, soft_mode, so, sp,
+                                           sinks);
                     }
-                    if (sh.open_tuple == t && sh.open_w > 0.0) {
+                } else if (!(piston && pen_sweep)) {
+                    if (piston || pen_sweep) {  // one row: its seed and its sink
+                        const double so[1] = {piston ? 1.0 : 0.0};
+                        const double sp[1] = {pen_sweep ? 1.0 : 0.0};
+                        const RowSinks<1> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
+                                                {piston ? TS : kFusedThreads}};
+                        run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck,
+                                           br_lo, br_hi, count, image_branch, piston, soft_mode,
+                                           so, sp, sinks);
+                    }
+                } else {  // both rows, one sweep each
+                    const double so0[1] = {1.0}, sp0[1] = {0.0};
+                    const RowSinks<1> s0{{1.0}, {row}, {TS}};
+                    run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                       br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
+                    const double so1[1] = {0.0}, sp1[1] = {1.0};
+                    const RowSinks<1> s1{{pfac}, {prow}, {kFusedThreads}};
+                    run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                                       br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
+                }
+            }
+            Rv[tid] = opl_val;
+            const double wv = (q < p.rays && in_piston(status)) ? smp.weight : 0.0;
+            sh.w[tid] = wv;
+            sh.sw[tid] = sqrt(wv);
+            sh.tuple[tid] = tu;
+            if (tid == 0) sh.any_pen = 0;
+            __syncthreads();
+            if (has_pen) sh.any_pen = 1;
+            // ---- B: centre every tuple segment of the chunk ----
+            const int rows_here = p.rays - base < kFusedThreads ? p.rays - base : kFusedThreads;
+            int start = 0;
+            while (start < rows_here) {
+                const int t = sh.tuple[start];
+                int end = start + 1;
+                while (end < rows_here && sh.tuple[end] == t) ++end;
+                const int len = end - start;
+                double ws = 0.0;
+                for (int r = start + lane; r < end; r += 32) ws += sh.w[r];
+                ws = fused_warp_sum(ws);
+                if (ws > 0.0) {
+                    for (int c = warp; c <= NP; c += kFusedWarps) {
+                        const double* col = c < NP ? Y + c * TS : Rv;
+                        double sum = 0.0;
+                        for (int r = start + lane; r < end; r += 32) sum += sh.w[r] * col[r];
+                        sum = fused_warp_sum(sum);
+                        if (lane == 0) mu_seg[c] = sum / ws;
+                    }
+                }
+                __syncthreads();
+                const bool open = sh.open_tuple == t && sh.open_w > 0.0;
+                const double scale = p.scale[t];
+                for (int e = tid; e < len * (NP + 1); e += kFusedThreads) {
+                    const int c = e / len, r = start + (e - c * len);
+                    double* col = c < NP ? Y + c * TS : Rv;
+                    col[r] = (ws > 0.0 && sh.w[r] > 0.0) ? scale * sh.sw[r] * (col[r] - mu_seg[c])
+                                                         : 0.0;
+                }
+                if (ws > 0.0 && tid <= NP) {
+                    const double mean = mu_seg[tid];
+                    if (open) {
                         const double wt = sh.open_w;
-                        const double fac = scale * sqrt(wt * wseg / (wt + wseg));
+                        const double fac = scale * sqrt(wt * ws / (wt + ws));
                         E[tid * ES + sh.extra] = fac * (mean - mu_open[tid]);
-                        mu_open[tid] += (wseg / (wt + wseg)) * (mean - mu_open[tid]);
+                        mu_open[tid] += (ws / (wt + ws)) * (mean - mu_open[tid]);
                     } else {
                         mu_open[tid] = mean;
                     }
                 }
                 __syncthreads();
-                if (tid == 0) {
-                    if (sh.open_tuple == t && sh.open_w > 0.0) {
+                if (tid == 0 && ws > 0.0) {
+                    if (open) {
                         sh.extra += 1;
-                        sh.open_w += wseg;
+                        sh.open_w += ws;
                     } else {
                         sh.open_tuple = t;
-                        sh.open_w = wseg;
+                        sh.open_w = ws;
                     }
                 }
-            } else if (tid < NP) {
-                for (int r = start; r < end; ++r) Y[tid * TS + r] = 0.0;
-            }
-            __syncthreads();
-            if (sh.extra == kExtraRows) {  // flush the extra rows
-                accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
                 __syncthreads();
-                if (tid == 0) sh.extra = 0;
-                __syncthreads();
-            }
-            start = end;
-        }
-        // ---- C: accumulate the centred rows and the pending extra rows ----
-        for (int r = rows_here + tid; r < ((rows_here + 3) & ~3); r += kFusedThreads)
-            for (int c = 0; c < NP; ++c) Y[c * TS + r] = 0.0;
-        const int ne = sh.extra;
-        for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
-            for (int c = 0; c < NP; ++c) E[c * ES + r] = 0.0;
-        __syncthreads();
-        accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
-        if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
-        __syncthreads();
-        if (tid == 0) sh.extra = 0;
-        // ---- D: penalty rows ----
-        if (sh.any_failed) {
-            for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
-            if (q < p.rays && status != kOk) {
-                const double factor = p.pscale[tu] * smp.root_weight;
-                if (soft_first != kOk) {
-                    if constexpr (std::is_same<N, MixedPrecision>::value)
-                        fused_backward_mixed(p, v, record, lay, f, l, smp, my_ck, stride_ck,
-                                             br_lo, br_hi, count, image_branch, in_piston(status),
-                                             soft_mode, 0.0f, 1.0f, static_cast<float>(factor),
-                                             row, TS);
-                    else
-                        fused_backward<N>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
-                                          br_hi, count, image_branch, in_piston(status),
-                                          soft_mode, N(0.0), N(1.0),
-                                          N(p.pscale[tu]) * N(smp.root_weight), row, TS);
+                if (sh.extra == kExtraRows) {  // flush the extra rows
+                    accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
+                    accumulate_r(E, ES, E + NP * ES, kExtraRows, NP, j0, j1, rr);
+                    __syncthreads();
+                    if (tid == 0) sh.extra = 0;
+                    __syncthreads();
                 }
-                const double fp = is_soft(status) ? penalty : penalty + 1.0;
-                row[P * TS] = factor * fp;
+                start = end;
             }
+            // ---- C: the centred rows and the pending extra rows ----
+            const int ne = sh.extra;
+            for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
+                for (int c = 0; c <= NP; ++c) E[c * ES + r] = 0.0;
             __syncthreads();
             accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+            accumulate_r(Y, TS, Rv, rows_here, NP, j0, j1, rr);
+            if (ne > 0) {
+                accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
+                accumulate_r(E, ES, E + NP * ES, ne, NP, j0, j1, rr);
+            }
+            __syncthreads();
+            if (tid == 0) sh.extra = 0;
+            // ---- D: penalty rows ----
+            if (sh.any_pen) {
+                for (int c = 0; c < NP; ++c) row[c * TS] = has_pen ? prow[c * kFusedThreads] : 0.0;
+                Rv[tid] = pen_val;
+                __syncthreads();
+                accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+                accumulate_r(Y, TS, Rv, rows_here, NP, j0, j1, rr);
+            }
+            __syncthreads();
         }
+        // ---- write the (P+1) x (P+1) symmetric gram ----
+        const int n = P + 1;
+        double* G = fa.gram + static_cast<int64_t>(run) * n * n;
+        for (int i = tid; i < pairs * 64; i += kFusedThreads) {
+            const int e = i / 64, ln = (i / 2) & 31, h = i & 1;
+            const int r = sh.tiles[e].x * 8 + (ln >> 2);
+            const int c = sh.tiles[e].y * 8 + 2 * (ln & 3) + h;
+            if (r < P && c < P) {
+                G[static_cast<int64_t>(c) * n + r] = acc[i];
+                G[static_cast<int64_t>(r) * n + c] = acc[i];
+            }
+        }
+        // J^T r and r^T r: partials of the four row phases reduced through Y
+        double* red = Y;  // [4][64 + 1]
+        red[warp * 65 + lane] = j0;
+        red[warp * 65 + lane + 32] = j1;
+        if (lane == 0) red[warp * 65 + 64] = rr;
         __syncthreads();
-    }
-    // ---- write the (P+1) x (P+1) symmetric gram ----
-    const int n = P + 1;
-    double* G = gram + static_cast<int64_t>(run) * n * n;
-    __syncthreads();
-    for (int i = tid; i < pairs * 64; i += kFusedThreads) {
-        const int e = i / 64, lane = (i / 2) & 31, h = i & 1;
-        const int r = sh.tiles[e].x * 8 + (lane >> 2);
-        const int c = sh.tiles[e].y * 8 + 2 * (lane & 3) + h;
-        if (r < n && c < n) {
-            G[static_cast<int64_t>(c) * n + r] = acc[i];
-            G[static_cast<int64_t>(r) * n + c] = acc[i];
+        if (tid < P) {
+            const double g = (red[tid] + red[65 + tid]) + (red[130 + tid] + red[195 + tid]);
+            G[static_cast<int64_t>(tid) * n + P] = g;
+            G[static_cast<int64_t>(P) * n + tid] = g;
         }
+        if (tid == 0) G[static_cast<int64_t>(P) * n + P] = (red[64] + red[129]) + (red[194] + red[259]);
     }
 }
 
 }  // namespace
 
 size_t fused_adjoint_smem(const TraceParams& tp, int P) {
-    const int NP = ((P + 1 + 7) / 8) * 8;
-    const int nck = (tp.S - 1) / kInterval + 1;
+    const int NP = fused_np(P);
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
-    return sizeof(double) * (static_cast<size_t>(tp.stride) +
-                             static_cast<size_t>(kFusedThreads + 1) * NP +
-                             (kExtraRows + 1) * NP + 2 * NP +
-                             static_cast<size_t>(pairs) * 64 +
-                             static_cast<size_t>(nck) * 6 * kFusedThreads);
+    return sizeof(double) * (static_cast<size_t>((tp.stride + 1) & ~1) +
+                             static_cast<size_t>(kFusedThreads + 1) * (NP + 1) +
+                             (kExtraRows + 1) * (NP + 1) + 2 * (NP + 1) +
+                             static_cast<size_t>(pairs) * 64);
+}
+
+namespace {
+int64_t fused_slot_doubles(int P, int S) {
+    const int checkpoints = (S - 1) / kFusedInterval;  // states after surfaces K, 2K, ...
+    return static_cast<int64_t>(fused_np(P) + 6 * checkpoints) * kFusedThreads;
+}
+}  // namespace
+
+// Global scratch of the fused kernel: the queue counter, then one slot per persistent CTA with
+// its penalty rows and its checkpoints (rewritten for every chunk, so it stays in L2).
+size_t fused_scratch_bytes(int runs, int P, int S) {
+    const size_t slots = static_cast<size_t>(runs < kMaxFusedSlots ? runs : kMaxFusedSlots);
+    return 256 + slots * fused_slot_doubles(P, S) * sizeof(double);
 }
 
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, int precision, cudaStream_t stream) {
-    AdjointParams ap;
-    ap.t = tp;
-    ap.v = vp;
-    ap.rows = 0;
+                        double* gram, void* scratch, size_t scratch_bytes, int precision,
+                        cudaStream_t stream) {
+    if (tp.V <= 0) return MKB_OK;
+    if (scratch == nullptr || scratch_bytes < fused_scratch_bytes(tp.V, vp.P, tp.S)) {
+        set_error("fused adjoint: scratch of %zu bytes needed",
+                  fused_scratch_bytes(tp.V, vp.P, tp.S));
+        return MKB_ERR_WORKSPACE;
+    }
+    FusedArgs fa;
+    fa.ap.t = tp;
+    fa.ap.v = vp;
+    fa.ap.rows = 0;
+    fa.records = records;
+    fa.gram = gram;
+    fa.queue = static_cast<int*>(scratch);
+    fa.scratch = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
+    fa.slot_doubles = fused_slot_doubles(vp.P, tp.S);
     const size_t smem = fused_adjoint_smem(tp, vp.P);
     auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
                   : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>
@@ -951,7 +1151,22 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");
-    kernel<<<tp.V, kFusedThreads, smem, stream>>>(ap, records, gram);
+    int device = 0, sms = 0, per_sm = 0;
+    err = cudaGetDevice(&device);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (err == cudaSuccess)
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFusedThreads, smem);
+    if (err != cudaSuccess) return cuda_status(err, "fused adjoint: occupancy");
+    if (per_sm < 1) {
+        set_error("fused adjoint: %zu bytes of shared memory do not fit an SM", smem);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    int grid = sms * per_sm;
+    if (grid > kMaxFusedSlots) grid = kMaxFusedSlots;
+    if (grid > tp.V) grid = tp.V;
+    err = cudaMemsetAsync(fa.queue, 0, sizeof(int), stream);
+    if (err != cudaSuccess) return cuda_status(err, "fused adjoint: clear queue");
+    kernel<<<grid, kFusedThreads, smem, stream>>>(fa);
     count_launch();
     return cuda_status(cudaGetLastError(), "fused adjoint launch");
 }

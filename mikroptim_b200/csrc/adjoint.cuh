@@ -39,11 +39,17 @@ struct StepAdj {
     N thickness, curvature, n_before, n_after;
 };
 
-template <class N>
-__device__ __forceinline__ void refracting_step_backward(Vec<N> p, Vec<N> d, N t, N c, N n_before,
-                                                         N n_after, int branch, N seed_opl,
-                                                         N seed_pen, RayAdj<N>& adj,
-                                                         StepAdj<N>& out) {
+// K adjoint vectors through one step (K seeds of the same ray: the OPL and the penalty). The
+// forward recompute and the seed-independent reverse quantities are shared; every adjoint
+// vector goes through the reference's statements in the reference's order, so for K = 1 (and
+// for each k) the result equals the single-seed sweep bit for bit.
+template <class N, int K>
+__device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N t, N c,
+                                                           N n_before, N n_after, int branch,
+                                                           const N (&seed_opl)[K],
+                                                           const N (&seed_pen)[K],
+                                                           RayAdj<N> (&adj)[K],
+                                                           StepAdj<N> (&out)[K]) {
     const N zero(0.0), one(1.0), two(2.0);
     // forward recompute of the step's local quantities
     const N z = p.z - t;
@@ -76,91 +82,115 @@ __device__ __forceinline__ void refracting_step_backward(Vec<N> p, Vec<N> d, N t
     const N cos_i = vdot(d, Nv);
     const N sin2 = one - cos_i * cos_i;
     const N k = one - mu * mu * sin2;
-    // reverse
-    const Vec<N> qb_out = adj.p;
-    const Vec<N> d1b = adj.d;
-    RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
-    Vec<N> nb{zero, zero, zero};
-    N cosb = zero, kb = zero, mub = zero;
+    // seed-independent reverse quantities
+    Vec<N> d1{zero, zero, zero};
+    N inv_tau = zero, root_k = zero, a = zero, inv = zero;
     if (tir) {
         const Vec<N> tau = vsub(d, vscale(cos_i, Nv));
-        const N inv_tau = one / vnorm(tau);
-        const Vec<N> d1 = vscale(inv_tau, tau);
-        const Vec<N> taub = vscale(inv_tau, vsub(d1b, vscale(vdot(d1, d1b), d1)));
-        in.d = vadd(in.d, taub);
-        cosb += -vdot(taub, Nv);
-        nb = vadd(nb, vscale(-cos_i, taub));
-        kb += -seed_pen;
+        inv_tau = one / vnorm(tau);
+        d1 = vscale(inv_tau, tau);
     } else {
-        const N root_k = nsqrt(k);
-        const N a = root_k - mu * cos_i;
-        in.d = vadd(in.d, vscale(mu, d1b));
-        nb = vadd(nb, vscale(a, d1b));
-        const N ab = vdot(d1b, Nv);
-        mub += vdot(d1b, d);
-        kb += ab / (two * root_k);
-        mub += -ab * cos_i;
-        cosb += -ab * mu;
+        root_k = nsqrt(k);
+        a = root_k - mu * cos_i;
     }
-    mub += -kb * two * mu * sin2;
-    cosb += kb * two * mu * mu * cos_i;
-    in.d = vadd(in.d, vscale(cosb, Nv));
-    nb = vadd(nb, vscale(cosb, d));
-    out.n_before += mub / n_after;
-    out.n_after += -mub * mu / n_after;
-    Vec<N> nrb = nb;
-    if (missed) nrb = vscale(inv_norm, vsub(nb, vscale(vdot(Nv, nb), Nv)));
-    const Vec<N> qb = vadd(qb_out, vscale(-c, nrb));
-    N cb = -vdot(q, nrb);
-    N xb = qb.x, yb = qb.y;
-    N sb = vdot(qb, d);
-    in.d = vadd(in.d, vscale(s, qb));
-    sb += seed_opl * n_before;
-    N s0b = seed_opl * n_before;
-    out.n_before += seed_opl * (s0 + s);
-    N hb = zero, bb = zero;
-    if (missed) {
-        bb += sb / c;
-        cb += -sb * s / c;
-        const N db = -seed_pen;
-        bb += db * two * B;
-        cb += -db * H;
-        hb += -db * c;
-    } else {
-        const N inv = one / (two * root_d);
-        hb += sb * inv;
-        bb += -sb * s * two * inv;
-        cb += sb * s * s * inv;
+    if (!missed) inv = one / (two * root_d);
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        const Vec<N> qb_out = adj[m].p;
+        const Vec<N> d1b = adj[m].d;
+        RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
+        Vec<N> nb{zero, zero, zero};
+        N cosb = zero, kb = zero, mub = zero;
+        if (tir) {
+            const Vec<N> taub = vscale(inv_tau, vsub(d1b, vscale(vdot(d1, d1b), d1)));
+            in.d = vadd(in.d, taub);
+            cosb += -vdot(taub, Nv);
+            nb = vadd(nb, vscale(-cos_i, taub));
+            kb += -seed_pen[m];
+        } else {
+            in.d = vadd(in.d, vscale(mu, d1b));
+            nb = vadd(nb, vscale(a, d1b));
+            const N ab = vdot(d1b, Nv);
+            mub += vdot(d1b, d);
+            kb += ab / (two * root_k);
+            mub += -ab * cos_i;
+            cosb += -ab * mu;
+        }
+        mub += -kb * two * mu * sin2;
+        cosb += kb * two * mu * mu * cos_i;
+        in.d = vadd(in.d, vscale(cosb, Nv));
+        nb = vadd(nb, vscale(cosb, d));
+        out[m].n_before += mub / n_after;
+        out[m].n_after += -mub * mu / n_after;
+        Vec<N> nrb = nb;
+        if (missed) nrb = vscale(inv_norm, vsub(nb, vscale(vdot(Nv, nb), Nv)));
+        const Vec<N> qb = vadd(qb_out, vscale(-c, nrb));
+        N cb = -vdot(q, nrb);
+        N xb = qb.x, yb = qb.y;
+        N sb = vdot(qb, d);
+        in.d = vadd(in.d, vscale(s, qb));
+        sb += seed_opl[m] * n_before;
+        N s0b = seed_opl[m] * n_before;
+        out[m].n_before += seed_opl[m] * (s0 + s);
+        N hb = zero, bb = zero;
+        if (missed) {
+            bb += sb / c;
+            cb += -sb * s / c;
+            const N db = -seed_pen[m];
+            bb += db * two * B;
+            cb += -db * H;
+            hb += -db * c;
+        } else {
+            hb += sb * inv;
+            bb += -sb * s * two * inv;
+            cb += sb * s * s * inv;
+        }
+        cb += hb * rr;
+        xb += hb * two * c * x;
+        yb += hb * two * c * y;
+        in.d.z += bb;
+        cb += -bb * xd;
+        xb += -bb * c * d.x;
+        yb += -bb * c * d.y;
+        in.d.x += -bb * c * x;
+        in.d.y += -bb * c * y;
+        // transfer: s0 = (t - p_z) / d_z
+        in.p.x += xb;
+        in.p.y += yb;
+        s0b += xb * d.x + yb * d.y;
+        in.d.x += xb * s0;
+        in.d.y += yb * s0;
+        const N qq = s0b / d.z;
+        out[m].thickness += qq;
+        in.p.z += -qq;
+        in.d.z += -qq * s0;
+        out[m].curvature += cb;
+        adj[m] = in;
     }
-    cb += hb * rr;
-    xb += hb * two * c * x;
-    yb += hb * two * c * y;
-    in.d.z += bb;
-    cb += -bb * xd;
-    xb += -bb * c * d.x;
-    yb += -bb * c * d.y;
-    in.d.x += -bb * c * x;
-    in.d.y += -bb * c * y;
-    // transfer: s0 = (t - p_z) / d_z
-    in.p.x += xb;
-    in.p.y += yb;
-    s0b += xb * d.x + yb * d.y;
-    in.d.x += xb * s0;
-    in.d.y += yb * s0;
-    const N qq = s0b / d.z;
-    out.thickness += qq;
-    in.p.z += -qq;
-    in.d.z += -qq * s0;
-    out.curvature += cb;
-    adj = in;
 }
 
-// Step onto the reference sphere through the last vertex about M = (0, h, w).
 template <class N>
-__device__ __forceinline__ void reference_step_backward(Vec<N> p, Vec<N> d, Vec<N> center,
-                                                        N n_image, int branch, N seed_opl,
-                                                        N seed_pen, RayAdj<N>& adj,
-                                                        Vec<N>& center_adj, N& n_image_adj) {
+__device__ __forceinline__ void refracting_step_backward(Vec<N> p, Vec<N> d, N t, N c, N n_before,
+                                                         N n_after, int branch, N seed_opl,
+                                                         N seed_pen, RayAdj<N>& adj,
+                                                         StepAdj<N>& out) {
+    const N so[1] = {seed_opl}, sp[1] = {seed_pen};
+    RayAdj<N> a[1] = {adj};
+    StepAdj<N> o[1] = {out};
+    refracting_step_backward_k<N, 1>(p, d, t, c, n_before, n_after, branch, so, sp, a, o);
+    adj = a[0];
+    out = o[0];
+}
+
+// Step onto the reference sphere through the last vertex about M = (0, h, w), K seeds.
+template <class N, int K>
+__device__ __forceinline__ void reference_step_backward_k(Vec<N> p, Vec<N> d, Vec<N> center,
+                                                          N n_image, int branch,
+                                                          const N (&seed_opl)[K],
+                                                          const N (&seed_pen)[K],
+                                                          RayAdj<N> (&adj)[K],
+                                                          Vec<N> (&center_adj)[K],
+                                                          N (&n_image_adj)[K]) {
     const N zero(0.0), one(1.0), two(2.0);
     const Vec<N> q = vsub(p, center);
     const N b = -vdot(q, d);
@@ -175,29 +205,48 @@ __device__ __forceinline__ void reference_step_backward(Vec<N> p, Vec<N> d, Vec<
         root = nsqrt(disc);
         s = g / (b + sigma * root);
     }
-    const N sb = seed_opl * n_image;
-    n_image_adj += seed_opl * s;
-    N bb, gb;
-    if (missed) {
-        bb = sb;
-        gb = zero;
-        const N radius_sq = vdot(center, center);
-        const N discb = -seed_pen / radius_sq;
-        bb += discb * two * b;
-        gb += -discb;
-        center_adj = vadd(center_adj, vscale(seed_pen * two * disc / (radius_sq * radius_sq),
-                                             center));
-    } else {
-        gb = sb * sigma / (two * root);
-        bb = -sb * sigma * s / root;
+    const N radius_sq = missed ? vdot(center, center) : zero;
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        const N sb = seed_opl[m] * n_image;
+        n_image_adj[m] += seed_opl[m] * s;
+        N bb, gb;
+        if (missed) {
+            bb = sb;
+            gb = zero;
+            const N discb = -seed_pen[m] / radius_sq;
+            bb += discb * two * b;
+            gb += -discb;
+            center_adj[m] = vadd(center_adj[m],
+                                 vscale(seed_pen[m] * two * disc / (radius_sq * radius_sq),
+                                        center));
+        } else {
+            gb = sb * sigma / (two * root);
+            bb = -sb * sigma * s / root;
+        }
+        RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
+        in.p = vadd(in.p, vscale(-bb, d));
+        in.d = vadd(in.d, vscale(-bb, q));
+        center_adj[m] = vadd(center_adj[m], vscale(bb, d));
+        in.p = vadd(in.p, vscale(two * gb, vsub(p, center)));
+        center_adj[m] = vadd(center_adj[m], vscale(N(-2.0) * gb, p));
+        adj[m] = in;
     }
-    RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
-    in.p = vadd(in.p, vscale(-bb, d));
-    in.d = vadd(in.d, vscale(-bb, q));
-    center_adj = vadd(center_adj, vscale(bb, d));
-    in.p = vadd(in.p, vscale(two * gb, vsub(p, center)));
-    center_adj = vadd(center_adj, vscale(N(-2.0) * gb, p));
-    adj = in;
+}
+
+template <class N>
+__device__ __forceinline__ void reference_step_backward(Vec<N> p, Vec<N> d, Vec<N> center,
+                                                        N n_image, int branch, N seed_opl,
+                                                        N seed_pen, RayAdj<N>& adj,
+                                                        Vec<N>& center_adj, N& n_image_adj) {
+    const N so[1] = {seed_opl}, sp[1] = {seed_pen};
+    RayAdj<N> a[1] = {adj};
+    Vec<N> ca[1] = {center_adj};
+    N na[1] = {n_image_adj};
+    reference_step_backward_k<N, 1>(p, d, center, n_image, branch, so, sp, a, ca, na);
+    adj = a[0];
+    center_adj = ca[0];
+    n_image_adj = na[0];
 }
 
 }  // namespace mkb

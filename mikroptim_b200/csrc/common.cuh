@@ -139,16 +139,17 @@ __device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit)
 // memory with one bulk copy issued by thread 0. Every thread of the block calls it. On a
 // timed-out wait the block records MKB_ERR_TIMEOUT, waits once more (bounded) for the copy
 // still in flight, and the function returns false: the caller must return without touching
-// the staged data.
+// the staged data. A block that stages repeatedly through the same barrier passes the number of
+// earlier uses (`use`): the barrier is initialised on the first and waited on by phase parity.
 __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t bytes,
-                                       uint64_t* bar) {
+                                       uint64_t* bar, uint32_t use = 0) {
     // alignment guard: a misaligned bulk copy faults, so record the error and skip it
     if (((smem_addr(dst) | reinterpret_cast<uintptr_t>(src) | bytes) & 15u) != 0 ||
         (smem_addr(bar) & 7u) != 0) {
         if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_ARGUMENT);
         return false;
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && use == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -158,11 +159,11 @@ __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t byte
         bulk_copy_g2s(dst, src, bytes, bar);
     }
     constexpr uint32_t kPolls = 1u << 24;
-    bool ok = mbar_wait(bar, 0, kPolls);
+    bool ok = mbar_wait(bar, use & 1u, kPolls);
     ok = __syncthreads_and(ok);
     if (!ok) {
         if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_TIMEOUT);
-        mbar_wait(bar, 0, kPolls);
+        mbar_wait(bar, use & 1u, kPolls);
         __syncthreads();
     }
     return ok;

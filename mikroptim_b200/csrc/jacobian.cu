@@ -28,7 +28,9 @@ int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows
 int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
                       const uint8_t* status, double* J, bool exact, cudaStream_t stream);
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, int precision, cudaStream_t stream);
+                        double* gram, void* scratch, size_t scratch_bytes, int precision,
+                        cudaStream_t stream);
+size_t fused_scratch_bytes(int runs, int P, int S);
 int pack_rays_default();
 
 namespace {
@@ -300,7 +302,8 @@ int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual
 
 size_t mkb_adjoint_jacobian_workspace_bytes(const mkb_device_batch* templates, int32_t runs) {
     if (templates == nullptr || runs < 0) return 0;
-    return align256(sizeof(double) * static_cast<size_t>(runs) * templates->record_stride);
+    return align256(sizeof(double) * static_cast<size_t>(runs) * templates->record_stride) +
+           fused_scratch_bytes(runs, MKB_MAX_VARIABLES, templates->surfaces);
 }
 
 int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
@@ -391,7 +394,10 @@ int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
     const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
     if (rc != MKB_OK) return rc;
-    return launch_adjoint_gram(tp, vp, records, gram, plan->precision, stream);
+    const size_t rec_bytes = align256(sizeof(double) * static_cast<size_t>(runs) *
+                                      templates->record_stride);
+    return launch_adjoint_gram(tp, vp, records, gram, static_cast<char*>(workspace) + rec_bytes,
+                               workspace_bytes - rec_bytes, plan->precision, stream);
 }
 
 }  // extern "C"

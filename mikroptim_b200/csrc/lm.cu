@@ -446,7 +446,9 @@ int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
                 bool exact, cudaStream_t stream);
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, int precision, cudaStream_t stream);
+                        double* gram, void* scratch, size_t scratch_bytes, int precision,
+                        cudaStream_t stream);
+size_t fused_scratch_bytes(int runs, int P, int S);
 int pack_rays_default();
 
 namespace {
@@ -468,6 +470,8 @@ struct LmLayout {
     int64_t* trial_hard;
     void* fd_ws;
     size_t fd_ws_bytes;
+    void* fused_ws;
+    size_t fused_ws_bytes;
 };
 
 constexpr int kFdChunkRuns = 64;
@@ -522,6 +526,8 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     L.trial_merit = reinterpret_cast<double*>(take(8 * r));
     L.trial_failed = reinterpret_cast<int64_t*>(take(8 * r));
     L.trial_hard = reinterpret_cast<int64_t*>(take(8 * r));
+    L.fused_ws_bytes = fused ? fused_scratch_bytes(runs, P, tp.S) : 0;
+    L.fused_ws = take(L.fused_ws_bytes);
     L.fd_ws_bytes = 0;
     if (fd) {
         mkb_device_batch t = *templates;
@@ -664,7 +670,8 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream);
         if (rc == MKB_OK)
-            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, s.precision, stream);
+            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
+                                     s.precision, stream);
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
