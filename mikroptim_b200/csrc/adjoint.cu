@@ -14,6 +14,7 @@
 // per-surface record in local memory (49 B per surface and ray); here only every K-th state
 // is kept and the rest is recomputed (checkpointing).
 #include "adjoint.cuh"
+#include "launch.cuh"
 #include "pupil.cuh"
 
 #include <type_traits>
@@ -858,6 +859,7 @@ struct FusedArgs {
     double* scratch;       // [slots][slot_doubles]: penalty rows and checkpoints per CTA
     int64_t slot_doubles;
     int* queue;            // run counter
+    const int* run_mask;   // runs to process (null: all)
 };
 
 template <class N>
@@ -904,6 +906,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         __syncthreads();
         const int run = sh.run;
         if (run >= p.V) break;
+        if (fa.run_mask != nullptr && fa.run_mask[run] == 0) continue;
         if (tid == 0) {
             sh.open_tuple = -1;
             sh.open_w = 0.0;
@@ -1128,7 +1131,7 @@ size_t fused_scratch_bytes(int runs, int P, int S) {
 
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, const int* run_mask) {
     if (tp.V <= 0) return MKB_OK;
     if (scratch == nullptr || scratch_bytes < fused_scratch_bytes(tp.V, vp.P, tp.S)) {
         set_error("fused adjoint: scratch of %zu bytes needed",
@@ -1144,6 +1147,7 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.queue = static_cast<int*>(scratch);
     fa.scratch = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
     fa.slot_doubles = fused_slot_doubles(vp.P, tp.S);
+    fa.run_mask = run_mask;
     const size_t smem = fused_adjoint_smem(tp, vp.P);
     auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
                   : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>

@@ -1,6 +1,6 @@
 // C ABI entry points (include/mikroptim_b200.h): argument checks, parameter blocks, pack
 // plans, error reporting. Every check runs on the host before anything is enqueued.
-#include "common.cuh"
+#include "launch.cuh"
 
 #include <atomic>
 #include <cmath>
@@ -10,20 +10,6 @@
 #include <string>
 
 namespace mkb {
-
-int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream);
-int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream);
-size_t merit_workspace_bytes(int V, int n_tuples);
-int pack_rays_default();
-int trace_device_error();
-int gram_device_error();
-int adjoint_device_error();
-int jacobian_device_error();
-int lm_device_error();
 
 namespace {
 thread_local std::string g_error;

@@ -10,7 +10,7 @@
 //   gram_dmma_kernel -- FP64 tensor cores: mma.sync.m8n8k4 (f64) on 8 x 8 output tiles of the
 //     upper triangle, row tiles of J staged in shared memory; fixed k order (deterministic, not
 //     bit-identical to the chain).
-#include "common.cuh"
+#include "launch.cuh"
 
 namespace mkb {
 
@@ -29,9 +29,10 @@ __device__ inline const double* column(const double* J, const double* r, int64_t
 
 __global__ void __launch_bounds__(kGramThreads)
 gram_exact_kernel(const double* __restrict__ J, const double* __restrict__ r, int P, int64_t R,
-                  double* __restrict__ gram) {
+                  double* __restrict__ gram, const int* __restrict__ run_mask) {
     __shared__ double tile[kMaxCols * kExactStride];
     const int64_t run = blockIdx.x;
+    if (run_mask != nullptr && run_mask[run] == 0) return;
     const int n = P + 1;
     const int pairs = n * (n + 1) / 2;
     // pair index -> (p, q), p <= q, row-major over the upper triangle
@@ -93,12 +94,13 @@ __device__ inline void dmma_8x8x4(double& d0, double& d1, double a, double b) {
 
 __global__ void __launch_bounds__(kGramThreads)
 gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int P, int64_t R,
-                 double* __restrict__ gram) {
+                 double* __restrict__ gram, const int* __restrict__ run_mask) {
     // tile[k][c] row-major with a padded row stride (columns of the 8-wide tiles are read
     // across lanes)
     constexpr int kStride = kDmmaMaxTiles * 8 + 1;
     __shared__ double tile[kDmmaRows * kStride];
     const int64_t run = blockIdx.x;
+    if (run_mask != nullptr && run_mask[run] == 0) return;
     const int n = P + 1;
     const int T = (n + 7) / 8;
     const int pairs = T * (T + 1) / 2;
@@ -164,12 +166,12 @@ gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int
 }  // namespace
 
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
-                bool exact, cudaStream_t stream) {
+                bool exact, cudaStream_t stream, const int* run_mask) {
     if (runs <= 0) return MKB_OK;
     if (exact)
-        gram_exact_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram);
+        gram_exact_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask);
     else
-        gram_dmma_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram);
+        gram_dmma_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask);
     count_launch();
     return cuda_status(cudaGetLastError(), "normal equations launch");
 }

@@ -11,27 +11,12 @@
 //
 // Adjoint (reference: DeviceAdjointJacobian::compute, src/cuda/adjoint_jacobian.cu:401):
 //   apply x0 -> RESIDUALS (r0, status) -> adjoint rows -> piston projection.
-#include "common.cuh"
+#include "launch.cuh"
 
 #include <algorithm>
 #include <type_traits>
 
 namespace mkb {
-
-int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream);
-int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
-                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
-int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
-                        const double* records, double* J, bool exact, cudaStream_t stream);
-int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
-                      const uint8_t* status, double* J, bool exact, cudaStream_t stream);
-int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, void* scratch, size_t scratch_bytes, int precision,
-                        cudaStream_t stream);
-size_t fused_scratch_bytes(int runs, int P, int S);
-int pack_rays_default();
 
 namespace {
 
@@ -88,11 +73,13 @@ __global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const do
 __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayout lay,
                                 const double* __restrict__ templates, int n_templates,
                                 const double* __restrict__ x0, const FdPattern* __restrict__ pat,
-                                int first_run, int runs, double* __restrict__ out) {
+                                int first_run, int runs, double* __restrict__ out,
+                                const int* __restrict__ run_mask) {
     const int n = 2 * vp.P + 1;
     const int local = blockIdx.x / n;
     const int j = blockIdx.x - local * n;
     const int run = first_run + local;
+    if (run_mask != nullptr && run_mask[run] == 0) return;
     const double* src = templates + static_cast<int64_t>(n_templates == 1 ? 0 : run) * lay.stride;
     double* dst = out + static_cast<int64_t>(blockIdx.x) * lay.stride;
     for (int i = threadIdx.x; i < lay.stride; i += blockDim.x) dst[i] = src[i];
@@ -115,7 +102,8 @@ __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayo
 template <bool kExact>
 __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPattern* __restrict__ pat,
                                      int P, int64_t R, int first_run, int runs,
-                                     double* __restrict__ J, double* __restrict__ r0) {
+                                     double* __restrict__ J, double* __restrict__ r0,
+                                     const int* __restrict__ run_mask) {
     using N = typename std::conditional<kExact, Exact64, double>::type;
     const int n = 2 * P + 1;
     const int64_t total = static_cast<int64_t>(runs) * (P + 1) * R;
@@ -126,6 +114,7 @@ __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPat
         const int c = static_cast<int>(ck % (P + 1));
         const int local = static_cast<int>(ck / (P + 1));
         const int run = first_run + local;
+        if (run_mask != nullptr && run_mask[run] == 0) continue;
         const double* base = res + static_cast<int64_t>(local) * n * R;
         if (c == P) {
             r0[static_cast<int64_t>(run) * R + r] = base[r];
@@ -205,26 +194,12 @@ MKB_DEFINE_ERROR_READER(jacobian_device_error)
 
 using namespace mkb;
 
-extern "C" {
+namespace mkb {
 
-size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
-                                       const mkb_residual_plan* plan, int32_t P, int32_t runs,
-                                       int32_t runs_per_chunk) {
-    TraceParams tp;
-    if (templates == nullptr || P < 1 || runs < 1 || runs_per_chunk < 1) return 0;
-    mkb_device_batch one = *templates;
-    one.variants = 1;
-    if (make_trace_params(&one, plan, pack_rays_default(), &tp) != MKB_OK) return 0;
-    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
-    const FdSizes z = fd_sizes(tp.stride, P, rows, tp.rays, runs);
-    return z.total_fixed + z.per_run * static_cast<size_t>(runs_per_chunk < runs ? runs_per_chunk : runs);
-}
-
-int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
-                           const mkb_variables* vars, const double* x0, int32_t runs, double* J,
-                           double* r0, int64_t* status_changes, void* workspace,
-                           size_t workspace_bytes, void* stream_ptr) {
-    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                const mkb_variables* vars, const double* x0, int runs, double* J, double* r0,
+                int64_t* status_changes, void* workspace, size_t workspace_bytes,
+                cudaStream_t stream, const int* run_mask) {
     if (runs < 0) {
         set_error("fd jacobian: runs must be >= 0");
         return MKB_ERR_ARGUMENT;
@@ -276,20 +251,21 @@ int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual
         const int cnt = std::min(chunk, runs - first);
         fd_build_kernel<<<cnt * n, 128, 0, stream>>>(vp, lay, templates->records,
                                                      templates->variants, x0, pattern, first,
-                                                     cnt, records);
+                                                     cnt, records, run_mask);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "fd build launch");
         if (rc != MKB_OK) break;
         TraceParams chunk_tp = tp;
         chunk_tp.V = cnt * n;
-        rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, plan->precision, stream);
+        rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, plan->precision, stream,
+                              RunMask{run_mask, n, first});
         if (rc != MKB_OK) break;
         const int64_t total = static_cast<int64_t>(cnt) * (P + 1) * R;
         const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 64));
         if (exact)
-            fd_difference_kernel<true><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0);
+            fd_difference_kernel<true><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0, run_mask);
         else
-            fd_difference_kernel<false><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0);
+            fd_difference_kernel<false><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0, run_mask);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "fd difference launch");
         if (rc != MKB_OK || status_changes == nullptr) continue;
@@ -298,6 +274,31 @@ int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual
         rc = cuda_status(cudaGetLastError(), "fd status-change launch");
     }
     return rc;
+}
+
+}  // namespace mkb
+
+extern "C" {
+
+size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
+                                       const mkb_residual_plan* plan, int32_t P, int32_t runs,
+                                       int32_t runs_per_chunk) {
+    TraceParams tp;
+    if (templates == nullptr || P < 1 || runs < 1 || runs_per_chunk < 1) return 0;
+    mkb_device_batch one = *templates;
+    one.variants = 1;
+    if (make_trace_params(&one, plan, pack_rays_default(), &tp) != MKB_OK) return 0;
+    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const FdSizes z = fd_sizes(tp.stride, P, rows, tp.rays, runs);
+    return z.total_fixed + z.per_run * static_cast<size_t>(runs_per_chunk < runs ? runs_per_chunk : runs);
+}
+
+int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                           const mkb_variables* vars, const double* x0, int32_t runs, double* J,
+                           double* r0, int64_t* status_changes, void* workspace,
+                           size_t workspace_bytes, void* stream_ptr) {
+    return fd_jacobian(templates, plan, vars, x0, runs, J, r0, status_changes, workspace,
+                       workspace_bytes, static_cast<cudaStream_t>(stream_ptr), nullptr);
 }
 
 size_t mkb_adjoint_jacobian_workspace_bytes(const mkb_device_batch* templates, int32_t runs) {

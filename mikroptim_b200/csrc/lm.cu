@@ -13,7 +13,7 @@
 // sequentially), so with bit-identical normal equations and merits the run trajectories equal
 // the reference's host loop bit for bit. One cycle is a fixed sequence of launches with
 // per-run masks (no host decisions), so a cycle can be captured in a CUDA graph.
-#include "common.cuh"
+#include "launch.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -56,9 +56,15 @@ struct LmState {
     int* rejected;
     int* solved;
     int* in_cycle;      // this cycle took a trial step
-    int* evaluate;      // this cycle's trial point is evaluated
+    int* evaluate;      // this cycle's trial point is evaluated (mask of the trial MERIT)
+    int* want_jacobian; // the next cycle computes this run's Jacobian (mask of the Jacobian)
     int* running;       // [1] runs still running after the last cycle
 };
+
+// The next cycle's update reads new normal equations exactly for these runs.
+__device__ __forceinline__ int wants_jacobian(const LmState& st, int run, int max_iterations) {
+    return st.status[run] == 0 && st.need_jacobian[run] && st.iterations[run] < max_iterations;
+}
 
 namespace {
 
@@ -333,6 +339,7 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
     if (run >= runs) return;
     if (!st.in_cycle[run]) {
         if (st.status[run] == kRunning) atomicAdd(st.running, 1);
+        st.want_jacobian[run] = wants_jacobian(st, run, o.max_iterations);
         return;
     }
     st.iterations[run] += 1;
@@ -369,6 +376,7 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
     st.history[static_cast<int64_t>(run) * (o.max_iterations + 1) + st.iterations[run]] =
         st.merit[run];
     if (st.status[run] == kRunning) atomicAdd(st.running, 1);
+    st.want_jacobian[run] = wants_jacobian(st, run, o.max_iterations);
 }
 
 // Start: merit at x0 (already evaluated into merit/failed/hard), status, damping.
@@ -396,6 +404,7 @@ __global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* 
     for (int h = 1; h <= o.max_iterations; ++h)
         st.history[static_cast<int64_t>(run) * (o.max_iterations + 1) + h] = nan("");
     if (status == kRunning) atomicAdd(st.running, 1);
+    st.want_jacobian[run] = wants_jacobian(st, run, o.max_iterations);
 }
 
 }  // namespace
@@ -429,27 +438,6 @@ MKB_DEFINE_ERROR_READER(lm_device_error)
 
 // ---- entry points ------------------------------------------------------------------------------
 namespace mkb {
-
-int launch_residuals(const TraceParams& p, const double* records, double* residuals,
-                     int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream);
-int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
-                 int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream);
-size_t merit_workspace_bytes(int V, int n_tuples);
-int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
-                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
-int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
-                        const double* records, double* J, bool exact, cudaStream_t stream);
-int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
-                      const uint8_t* status, double* J, bool exact, cudaStream_t stream);
-int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
-                bool exact, cudaStream_t stream);
-int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
-                        double* gram, void* scratch, size_t scratch_bytes, int precision,
-                        cudaStream_t stream);
-size_t fused_scratch_bytes(int runs, int P, int S);
-int pack_rays_default();
 
 namespace {
 
@@ -514,6 +502,7 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     L.st.solved = reinterpret_cast<int*>(take(4 * r));
     L.st.in_cycle = reinterpret_cast<int*>(take(4 * r));
     L.st.evaluate = reinterpret_cast<int*>(take(4 * r));
+    L.st.want_jacobian = reinterpret_cast<int*>(take(4 * r));
     L.st.running = reinterpret_cast<int*>(take(4));
     L.gram = reinterpret_cast<double*>(take(8 * r * (P + 1) * (P + 1)));
     const size_t jr = fused ? 0 : r;  // the fused adjoint keeps J out of memory
@@ -600,13 +589,13 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
 // merit at the run points `x` (applied to the templates) into merit/failed/hard
 int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates,
                 const double* x, int runs, double* merit, int64_t* failed, int64_t* hard,
-                cudaStream_t stream) {
+                cudaStream_t stream, const int* run_mask = nullptr) {
     const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
     int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
                           stream);
     if (rc != MKB_OK) return rc;
     return launch_merit(s.tp, L.records, merit, failed, hard, L.merit_ws, L.merit_ws_bytes,
-                        s.precision, stream);
+                        s.precision, stream, RunMask{run_mask, 1, 0});
 }
 
 }  // namespace
@@ -658,20 +647,18 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         set_error("lm: workspace of %zu bytes needed", L.total);
         return MKB_ERR_WORKSPACE;
     }
-    // 1. Jacobian at x (every run; only runs that need one use it) and normal equations
+    // 1. Jacobian and normal equations at x for the runs whose update will read them
+    const int* want = L.st.want_jacobian;
     if (s.fd) {
-        mkb_device_batch t = *templates;
-        mkb_residual_plan pl = *plan;
-        mkb_variables v = *vars;
-        rc = mkb_fd_jacobian_device(&t, &pl, &v, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
-                                    L.fd_ws_bytes, stream);
+        rc = fd_jacobian(templates, plan, vars, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
+                         L.fd_ws_bytes, stream, want);
     } else if (s.fused) {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream);
         if (rc == MKB_OK)
             rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
-                                     s.precision, stream);
+                                     s.precision, stream, want);
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
@@ -680,7 +667,8 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
             rc = cuda_status(cudaMemsetAsync(L.J, 0, sizeof(double) * size_t(runs) * s.vp.P * s.R,
                                              stream), "lm: clear J");
         if (rc == MKB_OK)
-            rc = launch_residuals(s.tp, L.records, L.r0, s.R, nullptr, L.status, s.precision, stream);
+            rc = launch_residuals(s.tp, L.records, L.r0, s.R, nullptr, L.status, s.precision,
+                                  stream, RunMask{want, 1, 0});
         if (rc == MKB_OK)
             rc = launch_adjoint_rows(s.tp, s.vp, s.R, L.records, L.J, s.exact, stream);
         if (rc == MKB_OK)
@@ -688,7 +676,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     }
     if (rc != MKB_OK) return rc;
     if (!s.fused) {
-        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream);
+        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream, want);
         if (rc != MKB_OK) return rc;
     }
     // 2. step
@@ -696,7 +684,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     if (rc != MKB_OK) return rc;
     // 3. trial MERIT, 4. acceptance
     rc = lm_merit_at(s, L, templates, L.st.trial, runs, L.trial_merit, L.trial_failed,
-                     L.trial_hard, stream);
+                     L.trial_hard, stream, L.st.evaluate);
     if (rc != MKB_OK) return rc;
     rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
     if (rc != MKB_OK) return rc;

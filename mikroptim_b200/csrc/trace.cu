@@ -13,7 +13,7 @@
 // Reference behaviour restated: residuals_kernel / merit_kernel + merit_finalize_kernel
 // (src/cuda/residuals.cu:57, src/cuda/merit.cu:62,206), batch_ray_opl (merit/ray_residual.hpp:69),
 // opd_statistics (merit/opd.hpp:37), ray_residual / ray_penalty (merit/ray_residual.hpp:131,199).
-#include "common.cuh"
+#include "launch.cuh"
 #include "pupil.cuh"
 
 #include <cstdio>
@@ -164,6 +164,7 @@ struct TupleOut {
     double* part;       // MERIT: [V][n_tuples] tuple sums
     int* part_failed;   // MERIT: [V][n_tuples]
     int* part_hard;     // MERIT: [V][n_tuples]
+    RunMask mask;       // variants to trace
 };
 
 // kExact: per-ray arithmetic in Exact64 and every tuple sum sequential in ascending sample
@@ -178,6 +179,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     using N = typename std::conditional<kExact, Exact64, double>::type;
     __shared__ SharedTrace sh;
     const int v = blockIdx.x / p.n_packs;
+    if (!run_active(out.mask, v)) return;
     const int pk = blockIdx.x - v * p.n_packs;
     const Pack pack = p.packs[pk];
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
@@ -327,9 +329,10 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
 // merit[v] = sum over tuples in order (f-major, then l); counts likewise.
 __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
                                       const int* part_failed, const int* part_hard,
-                                      double* merit, int64_t* failed, int64_t* hard) {
+                                      double* merit, int64_t* failed, int64_t* hard,
+                                      RunMask mask) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
+    if (v >= V || !run_active(mask, v)) return;
     double sum = 0.0;
     int64_t nf = 0, nh = 0;
     const int64_t o = static_cast<int64_t>(v) * n_tuples;
@@ -352,8 +355,8 @@ size_t merit_workspace(int V, int n_tuples) {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
                      int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream) {
-    TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr};
+                     cudaStream_t stream, RunMask mask) {
+    TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask};
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     if (precision == MKB_PRECISION_FP64)
         trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
@@ -367,7 +370,7 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
                  int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, RunMask mask) {
     const size_t need = merit_workspace(p.V, p.n_tuples);
     if (workspace == nullptr || ws_bytes < need) {
         set_error("merit: workspace of %zu bytes needed, %zu given", need, ws_bytes);
@@ -377,7 +380,7 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     char* ws = static_cast<char*>(workspace);
     TupleOut out{nullptr, 0, nullptr, nullptr, reinterpret_cast<double*>(ws),
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
-                 reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int)))};
+                 reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask};
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     if (precision == MKB_PRECISION_FP64)
         trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
@@ -389,7 +392,7 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
     if (rc != MKB_OK) return rc;
     merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(
-        p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard);
+        p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard, mask);
     count_launch();
     return cuda_status(cudaGetLastError(), "merit finalize launch");
 }
