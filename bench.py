@@ -10,9 +10,12 @@ working distance), soft failure; synthetic seeded inputs.
 
   --workload lm (default): one step = one batched Levenberg-Marquardt cycle of all 4096 runs
       (adjoint Jacobian fused with its FP64-tensor-core normal equations, damped Cholesky step,
-      trial MERIT, acceptance), FP64 with FMA contraction. The same cycle with the central-
-      difference Jacobian (the reference method, 2P + 1 = 59 traced variants per run) is timed
-      on the same GPU beside it (`fd_fp64`), on 512 runs (its cost is linear in the runs).
+      trial MERIT, acceptance), FP64 with FMA contraction, replayed as a CUDA graph. The value is
+      the LM iterations the runs actually took in the timed cycles per second. Beside it: the
+      same LM with the MIXED-precision adjoint (`adjoint_mixed`), with the central-difference
+      Jacobian (the reference method, 2P + 1 = 59 traced variants per run, `fd_fp64`, on 512
+      runs: its cost is linear in the runs), and the OPD error of each precision against the
+      bit-exact FP64 trace.
   --workload merit: one step = one MERIT evaluation of all variants.
 
 N > 1 (torchrun, one rank per GPU): every rank traces its own 4096 variants (weak scaling,
@@ -28,6 +31,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import dataclasses
 import json
 import os
 import statistics
@@ -47,6 +51,9 @@ FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of th
 # DRAM traffic of trace_kernel per variant from the ncu capture summarised in
 # profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
 TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
+# DRAM traffic of adjoint_gram_kernel per run, from the ncu capture summarised in
+# profiles/adjoint_gram_objective1184.md (scaled by the runs of the launch).
+FUSED_TRAFFIC_BYTES_PER_RUN = None
 
 
 def parse():
@@ -289,10 +296,72 @@ def run_b200(args, world, rank, local):
     return out, (b, lay)
 
 
+def _lm_window(lm, steps: int, warmup: int, flush, world, dev, graph: bool = True):
+    """W warm-up cycles, then K cycles timed with CUDA events (L2 flushed before each, outside
+    the events). Returns (ms per cycle, LM iterations performed in the timed cycles, launches
+    per cycle)."""
+    import torch
+    from mikroptim_b200 import _capi
+    lib = _capi.lib()
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        lm.cycle()
+    l0 = lib.mkb_launch_count()
+    g = lm.capture() if graph else None
+    per_cycle = lib.mkb_launch_count() - l0
+    it0 = int(lm.iterations().sum())
+    barrier(world)
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if g is not None:
+            g.replay()
+        else:
+            lm.cycle()
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier(world)
+    iters = int(lm.iterations().sum()) - it0
+    ms = sum(a.elapsed_time(b) for a, b in times)
+    del g
+    return ms / steps, iters, per_cycle
+
+
+def opd_errors(b, st, runs: int = 256):
+    """RMS / max OPD difference (waves at the reference wavelength) of the FP64-FMA and MIXED
+    traces against the bit-exact FP64 trace, over rays in the piston with the same status."""
+    import torch
+    from mikroptim_b200 import engine
+    from mikroptim_b200.batch import ResidualLayout, in_piston
+    sub = b.subset(0, runs)
+    lam_mm = sub.reference_wavelength_nm * 1e-6
+    out = {}
+    res = {}
+    for prec in (0, 2, 1):
+        lay = ResidualLayout(sub.topology, dataclasses.replace(st, precision=prec))
+        r = engine.residuals_device(engine.DeviceSystemBatch(sub), lay, sub)
+        torch.cuda.synchronize()
+        res[prec] = (r.opd.cpu().numpy(), r.status.cpu().numpy())
+    ref_opd, ref_st = res[0]
+    for prec, name in ((2, "fp64_fma"), (1, "mixed")):
+        opd, stt = res[prec]
+        same = (stt == ref_st) & in_piston(ref_st)
+        clean = same & (ref_st == 0)
+        err = (opd - ref_opd) / lam_mm
+        out[name] = {"rms_waves": float(np.sqrt(np.mean(err[same] ** 2))),
+                     "rms_waves_ok_rays": float(np.sqrt(np.mean(err[clean] ** 2))),
+                     "median_abs_waves": float(np.median(np.abs(err[same]))),
+                     "status_agreement": float(np.mean(stt == ref_st))}
+    return out
+
+
 def run_lm(args, world, rank, local):
     import torch
     from mikroptim_b200 import _capi, engine, workloads
-    from mikroptim_b200.batch import PRECISION_FP64_FMA, ResidualLayout
+    from mikroptim_b200.batch import PRECISION_FP64_FMA, PRECISION_MIXED, ResidualLayout
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -301,45 +370,54 @@ def run_lm(args, world, rank, local):
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
     runs = b.variants
+    P = vs.size
     db = engine.DeviceSystemBatch(b, dev)
-    opt = engine.LmOptions(max_iterations=args.warmup + args.steps + 100,
-                           jacobian=engine.JACOBIAN_ADJOINT, gram_exact=False)
-    lm = engine.DeviceLm(db, lay, b, vs, opt, runs)
-    lm.start(x0)
+    max_it = args.warmup + args.steps + 100
+    opt = engine.LmOptions(max_iterations=max_it, jacobian=engine.JACOBIAN_ADJOINT,
+                           gram_exact=False)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
     rays = runs * lay.rays_per_variant
     steps_per_ray = b.surfaces - 1
-    for _ in range(args.warmup):
-        lm.cycle()
-    torch.cuda.synchronize()
-    barrier(world)
-    launches0 = lib.mkb_launch_count()
-    times = []
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        barrier(world)
-        for _ in range(args.steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            lm.cycle()
-            e1.record(stream)
-            times.append((e0, e1))
-        torch.cuda.synchronize()
-        barrier(world)
-    launches = lib.mkb_launch_count() - launches0
-    ms_total = max_over_ranks(sum(a.elapsed_time(c) for a, c in times), world, dev)
-    ms_step = ms_total / args.steps
-    value = world * runs * args.steps / (ms_total / 1e3)
 
-    # the dominant kernel alone: fused adjoint + normal equations at the current points
-    x_now = torch.empty((runs, vs.size), dtype=torch.float64, device=dev)
+    # ---- headline: adjoint (fused with the FP64 tensor-core normal equations) LM cycles ----
+    lm = engine.DeviceLm(db, lay, b, vs, opt, runs)
+    lm.start(x0)
+    with ClockSampler(local) as clocks:
+        ms_cycle, iters, per_cycle = _lm_window(lm, args.steps, args.warmup, flush, world, dev)
+    ms_step = max_over_ranks(ms_cycle, world, dev)
+    iters_all = max_over_ranks(float(iters), world, dev) * world  # equal per rank by seeding
+    value = iters_all / (ms_step * args.steps / 1e3)
+    x_now = torch.empty((runs, P), dtype=torch.float64, device=dev)
     lib.mkb_lm_results_device(*lm._args(), runs, C.c_void_p(lm.workspace.data_ptr()),
                               C.c_void_p(x_now.data_ptr()), *([None] * 10),
                               C.c_void_p(stream.cuda_stream))
     torch.cuda.synchronize()
     x_np = x_now.cpu().numpy()
+    del lm
+
+    # ---- the same LM with the MIXED-precision adjoint ----
+    lay_mixed = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_MIXED))
+    lm_m = engine.DeviceLm(db, lay_mixed, b, vs, opt, runs)
+    lm_m.start(x0)
+    ms_mixed, iters_mixed, _ = _lm_window(lm_m, args.steps, args.warmup, flush, world, dev)
+    mixed_value = world * iters_mixed / (max_over_ranks(ms_mixed, world, dev) * args.steps / 1e3)
+    del lm_m
+
+    # ---- the reference method on the same GPU: FD Jacobian (2P + 1 traced variants), FP64 ----
+    fd_runs = min(512, runs)
+    fd_b = b.subset(0, fd_runs)
+    fd_db = engine.DeviceSystemBatch(fd_b, dev)
+    fd_opt = engine.LmOptions(max_iterations=max_it, jacobian=engine.JACOBIAN_FD,
+                              gram_exact=False)
+    fd = engine.DeviceLm(fd_db, lay, fd_b, vs, fd_opt, fd_runs)
+    fd.start(x0[:fd_runs])
+    fd_steps = max(2, min(args.steps, 10))
+    fd_ms, fd_iters, _ = _lm_window(fd, fd_steps, args.warmup, flush, world, dev)
+    fd_value = fd_iters / (fd_ms * fd_steps / 1e3)
+    del fd
+
+    # ---- the dominant kernel alone: fused adjoint + normal equations at the current points ----
     engine.adjoint_normal_equations_device(db, lay, b, vs, x_np)
     torch.cuda.synchronize()
     kt = []
@@ -354,12 +432,10 @@ def run_lm(args, world, rank, local):
     kernel_ms = min(kt)
     # FLOP model (reference cost model): adjoint = 3 x FLOPeq(ray), FLOPeq = 140 (S_steps + 2),
     # plus 4 P per ray (projection) and 2 P^2 per row (rows: rays and penalty rows)
-    P = vs.size
     flop = rays * (3 * FLOPEQ_PER_RAY_SURFACE * (steps_per_ray + 2) + 4 * P) + \
         2 * P * P * runs * lay.trace_rows
 
-    # MERIT rate (ray-surface hits/s) on the same points
-    mws = None
+    # ---- MERIT rate (ray-surface hits/s) on the same points ----
     engine.merit_device(db, lay, b)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -370,32 +446,13 @@ def run_lm(args, world, rank, local):
     torch.cuda.synchronize()
     merit_ms = e0.elapsed_time(e1) / 3
 
-    # the reference method on the same GPU: FD Jacobian (59 traced variants per run), FP64
-    fd_runs = min(512, runs)
-    fd_b = b.subset(0, fd_runs)
-    fd_db = engine.DeviceSystemBatch(fd_b, dev)
-    fd_opt = engine.LmOptions(max_iterations=100, jacobian=engine.JACOBIAN_FD, gram_exact=False)
-    fd = engine.DeviceLm(fd_db, lay, fd_b, vs, fd_opt, fd_runs)
-    fd.start(x0[:fd_runs])
-    fd.cycle()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(2):
-        fd.cycle()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    fd_ms = e0.elapsed_time(e1) / 2
-    fd_value = fd_runs / (fd_ms / 1e3)
-    del fd
-
-    # end to end through the host-buffer path: pinned x in, cycle, x and merit out per step
+    # ---- end to end through the host-buffer path: pinned x in, cycle, x and merit out ----
     host_x = torch.from_numpy(x_np.copy()).pin_memory()
     host_out = torch.empty((runs, P + 1), dtype=torch.float64).pin_memory()
     dev_x = torch.empty_like(x_now)
     lm2 = engine.DeviceLm(db, lay, b, vs, opt, runs)
     lm2.start(x_np)
-    torch.cuda.synchronize()
+    it0 = int(lm2.iterations().sum())
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -408,8 +465,11 @@ def run_lm(args, world, rank, local):
                                   *([None] * 9), C.c_void_p(stream.cuda_stream))
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+    e2e_iters = int(lm2.iterations().sum()) - it0
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    del lm2
 
+    errors = opd_errors(b, st) if rank == 0 else None
     peak = fp64_peak_tflops(torch) if rank == 0 else None
     achieved = flop / (kernel_ms / 1e3) / 1e12
     if rank != 0:
@@ -417,7 +477,7 @@ def run_lm(args, world, rank, local):
     return {
         "metric": METRIC,
         "value": value,
-        "unit": "LM run-iterations/s",
+        "unit": "LM iterations/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -427,20 +487,29 @@ def run_lm(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generator, configuration-2 shapes)",
-        "config": {"workload": WORKLOAD, "step": "one batched LM cycle of all runs",
+        "config": {"workload": WORKLOAD, "step": "one batched LM cycle of all runs (CUDA graph)",
                    "runs_per_gpu": runs, "variables": P, "rays_per_run": lay.rays_per_variant,
                    "jacobian": "adjoint fused with FP64 tensor-core normal equations",
                    "precision": "FP64 with FMA contraction",
+                   "iterations": "LM iterations actually taken in the timed cycles "
+                                 f"({iters} of {runs * args.steps} run-cycles)",
                    "l2": "flushed (256 MB write) before every timed step"},
-        "gpu_launches": int(launches),
+        "gpu_launches": int(per_cycle * args.steps),
         "ray_surface_hits_per_s": world * rays * steps_per_ray / (merit_ms / 1e3),
-        "fd_fp64": {"value": world * fd_value, "unit": "LM run-iterations/s",
-                    "ms_per_cycle_512_runs": fd_ms, "speedup_adjoint_vs_fd": value / (world * fd_value)},
-        "e2e": {"value": world * runs / (e2e_ms / 1e3), "unit": "LM run-iterations/s",
+        "adjoint_mixed": {"value": mixed_value, "unit": "LM iterations/s",
+                          "ms_per_cycle": ms_mixed},
+        "fd_fp64": {"value": world * fd_value, "unit": "LM iterations/s",
+                    "ms_per_cycle_512_runs": fd_ms, "cycles": fd_steps,
+                    "speedup_adjoint_vs_fd": value / (world * fd_value),
+                    "speedup_adjoint_mixed_vs_fd": mixed_value / (world * fd_value)},
+        "opd_error_vs_fp64": errors,
+        "e2e": {"value": world * e2e_iters / (e2e_ms / 1e3), "unit": "LM iterations/s",
                 "h2d_bytes_per_step": int(runs * P * 8),
                 "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": (FUSED_TRAFFIC_BYTES_PER_RUN * runs
+                                 if FUSED_TRAFFIC_BYTES_PER_RUN else None),
                      "kernel": "adjoint_gram_kernel (fused adjoint + DMMA normal equations)",
                      "kernel_ms": kernel_ms,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",

@@ -106,9 +106,10 @@ int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields)
  * are taken here with the host libm, so the start rays are those of the CPU reference). */
 int mkb_pack_batch_host(const mkb_batch_view* view, double* records);
 
-/* Writes the curvature/thickness/working-distance entries of `x` ([runs][P]) into the
- * packed device records of the matching variants (variant v = first_variant + run) --
- * VariableSet::apply (src/optim/variable_set.cpp:237) for these variable types. */
+/* The LM variables (VariableSet, include/mikroptim/optim/variable_set.hpp:63): curvature,
+ * thickness and working-distance entries of the surface table. The Jacobian and LM entry
+ * points write a run point x [P] into a copy of the run's template record on the device
+ * (VariableSet::apply, src/optim/variable_set.cpp:237). */
 typedef struct mkb_variables {
     int32_t count;                    /* P                                               */
     const int32_t* type;              /* host [P] MKB_VAR_*                              */

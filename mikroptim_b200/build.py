@@ -2,7 +2,8 @@
 
     python -m mikroptim_b200.build [--verbose]
 
-Objects go to mikroptim_b200/_build/, the shared library next to this file. Every .cu file in
+Objects go to mikroptim_b200/_build/, the shared library next to this file, and the C++ host
+layer (host/host.cpp) is linked against it as libmikroptim_b200_host.so. Every .cu file in
 csrc/ is compiled with ``-gencode arch=compute_100a,code=sm_100a -O3 -lineinfo``; the CUDA
 runtime is linked statically so the library does not depend on which libcudart the process
 loaded first.
@@ -55,6 +56,33 @@ def _compile(src: str, verbose: bool) -> tuple[str, str]:
     return obj, res.stdout + res.stderr
 
 
+HOST_DIR = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libmikroptim_b200_host.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def build_host() -> str:
+    """The C++ host layer (host/host.cpp, reference-shaped classes over the C ABI) as
+    libmikroptim_b200_host.so next to the CUDA library, which it links (rpath $ORIGIN)."""
+    srcs = [os.path.join(HOST_DIR, "host.cpp")]
+    deps = srcs + glob.glob(os.path.join(HOST_DIR, "*.hpp")) + [LIB,
+                                                              os.path.join(ROOT, "include",
+                                                                           "mikroptim_b200.h")]
+    if os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= max(
+            os.path.getmtime(p) for p in deps):
+        return HOST_LIB
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", *srcs,
+           "-I", os.path.join(ROOT, "include"), "-I", HOST_DIR,
+           "-I", os.path.join(CUDA_HOME, "include"), "-o", HOST_LIB,
+           "-L", HERE, "-lmikroptim_b200", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"host layer build failed:\n{res.stdout}\n{res.stderr}")
+    return HOST_LIB
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
@@ -71,6 +99,7 @@ def build(verbose: bool = False) -> str:
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    build_host()
     return LIB
 
 

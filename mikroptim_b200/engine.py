@@ -318,6 +318,32 @@ class DeviceLm:
         _capi.check(rc, "lm cycle")
         self.cycles += 1
 
+    def capture(self) -> "torch.cuda.CUDAGraph":
+        """One LM cycle captured as a CUDA graph: a cycle is a fixed launch sequence whose
+        per-run decisions live in device masks, so replaying the graph advances every run by
+        one cycle exactly as cycle() does. Call cycle() at least once first (it sets kernel
+        attributes outside the capture)."""
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            rc = self.lib.mkb_lm_cycle_device(*self._args(), self.runs,
+                                              C.c_void_p(self.workspace.data_ptr()),
+                                              self.workspace.numel(),
+                                              _stream_handle(None))
+        _capi.check(rc, "lm cycle capture")
+        return graph
+
+    def iterations(self) -> np.ndarray:
+        """Per-run iteration counters (synchronising)."""
+        out = np.zeros(self.runs, dtype=np.int32)
+        torch.cuda.synchronize(self.templates.device)
+        rc = self.lib.mkb_lm_results_device(*self._args(), self.runs,
+                                            C.c_void_p(self.workspace.data_ptr()), None, None,
+                                            None, _capi.ptr(out, C.c_int32), *([None] * 7),
+                                            _stream_handle(self.stream))
+        _capi.check(rc, "lm results")
+        torch.cuda.synchronize(self.templates.device)
+        return out
+
     def running(self) -> int:
         out = np.zeros(1, dtype=np.int32)
         torch.cuda.synchronize(self.templates.device)

@@ -1,0 +1,579 @@
+// C++ host layer over the C ABI (see mikroptim_b200.hpp for the reference classes mirrored).
+#include "mikroptim_b200.hpp"
+
+#include <cuda_runtime_api.h>
+
+#include <cmath>
+#include <memory>
+#include <set>
+#include <utility>
+
+#include "gauss_legendre_table.hpp"
+
+namespace mkb {
+
+namespace {
+
+constexpr int kMaxRings = detail::kMaxRings;
+
+int sample_count(int rings, int spokes, PupilMode mode) {
+    return mode == PupilMode::Axis ? rings : rings * spokes;
+}
+
+}  // namespace
+
+// ---- BatchTopology / SystemBatchHost ---------------------------------------------------------
+
+void BatchTopology::validate() const {
+    if (surfaces < 2 || surfaces > MKB_MAX_SURFACES)
+        throw std::invalid_argument("BatchTopology: surfaces must be in [2, 64]");
+    if (wavelengths < 1 || wavelengths > MKB_MAX_WAVELENGTHS)
+        throw std::invalid_argument("BatchTopology: wavelengths must be in [1, 16]");
+    if (fields < 1 || fields > MKB_MAX_FIELDS)
+        throw std::invalid_argument("BatchTopology: fields must be in [1, 16]");
+    if (fields * wavelengths > MKB_MAX_TUPLES)
+        throw std::invalid_argument("BatchTopology: fields * wavelengths must be <= 128");
+    if (static_cast<int>(type.size()) != surfaces)
+        throw std::invalid_argument("BatchTopology: type needs one entry per surface");
+    if (type[0] != SurfaceKind::Stop)
+        throw std::invalid_argument("BatchTopology: surface 0 must be the stop");
+    for (int s = 1; s < surfaces; ++s)
+        if (type[s] != SurfaceKind::Plane && type[s] != SurfaceKind::Sphere)
+            throw std::logic_error("BatchTopology: this build traces stop, plane and sphere "
+                                   "surfaces");
+    if (static_cast<int>(pupil_mode.size()) != fields)
+        throw std::invalid_argument("BatchTopology: pupil_mode needs one entry per field");
+}
+
+SystemBatchHost::SystemBatchHost(BatchTopology topology, int variants)
+    : topology_(std::move(topology)), variants_(variants) {
+    topology_.validate();
+    if (variants < 0) throw std::invalid_argument("SystemBatchHost: variants must be >= 0");
+    const size_t V = static_cast<size_t>(variants);
+    const size_t S = topology_.surfaces, L = topology_.wavelengths, F = topology_.fields;
+    type_.resize(S);
+    for (size_t s = 0; s < S; ++s) type_[s] = static_cast<uint8_t>(topology_.type[s]);
+    wavelength_weight.assign(L, 1.0);
+    field_weight.assign(F, 1.0);
+    curvature_.assign(V * S, 0.0);
+    thickness_.assign(V * S, 0.0);
+    index_.assign(V * S * L, 1.0);
+    pupil_radius_.assign(V, 0.0);
+    field_angle_.assign(V * F, 0.0);
+    field_target_.assign(V * F, 0.0);
+}
+
+size_t SystemBatchHost::check_v(int v) const {
+    if (v < 0 || v >= variants_) throw std::out_of_range("SystemBatchHost: variant out of range");
+    return static_cast<size_t>(v);
+}
+
+size_t SystemBatchHost::index2(int v, int i, int n) const {
+    if (i < 0 || i >= n) throw std::out_of_range("SystemBatchHost: index out of range");
+    return check_v(v) * n + i;
+}
+
+double& SystemBatchHost::index(int v, int s, int l) {
+    if (l < 0 || l >= wavelengths()) throw std::out_of_range("SystemBatchHost: wavelength");
+    return index_.at(index2(v, s, surfaces()) * wavelengths() + l);
+}
+
+void SystemBatchHost::validate_values() const {
+    auto finite = [](const std::vector<double>& a, const char* name) {
+        for (double x : a)
+            if (!std::isfinite(x))
+                throw std::invalid_argument(std::string("SystemBatchHost: ") + name +
+                                            " is not finite");
+    };
+    finite(curvature_, "curvature");
+    finite(thickness_, "thickness");
+    finite(index_, "index");
+    finite(pupil_radius_, "pupil_radius");
+    finite(field_angle_, "field_angle");
+    finite(field_target_, "field_target");
+    finite(wavelength_weight, "wavelength_weight");
+    finite(field_weight, "field_weight");
+    for (double r : pupil_radius_)
+        if (!(r > 0)) throw std::invalid_argument("SystemBatchHost: pupil radius must be > 0");
+    for (double n : index_)
+        if (!(n > 0)) throw std::invalid_argument("SystemBatchHost: refractive indices must be > 0");
+    for (double w : wavelength_weight)
+        if (w < 0) throw std::invalid_argument("SystemBatchHost: weights must be >= 0");
+    for (double w : field_weight)
+        if (w < 0) throw std::invalid_argument("SystemBatchHost: weights must be >= 0");
+    if (!(reference_wavelength_nm > 0))
+        throw std::invalid_argument("SystemBatchHost: reference wavelength must be > 0");
+    for (int f = 0; f < fields(); ++f)
+        if (topology_.pupil_mode[f] == PupilMode::Axis)
+            for (int v = 0; v < variants_; ++v)
+                if (field_angle_[static_cast<size_t>(v) * fields() + f] != 0.0)
+                    throw std::invalid_argument("SystemBatchHost: an axis field has a non-zero "
+                                                "field angle (check_pupil_modes)");
+}
+
+mkb_batch_view SystemBatchHost::view() const {
+    if (static_cast<int>(wavelength_weight.size()) != wavelengths() ||
+        static_cast<int>(field_weight.size()) != fields())
+        throw std::invalid_argument("SystemBatchHost: weight arrays do not match the topology");
+    mkb_batch_view v{};
+    v.variants = variants_;
+    v.surfaces = surfaces();
+    v.wavelengths = wavelengths();
+    v.fields = fields();
+    v.reference_wavelength_nm = reference_wavelength_nm;
+    v.type = type_.data();
+    v.wavelength_weight = wavelength_weight.data();
+    v.field_weight = field_weight.data();
+    v.curvature = curvature_.data();
+    v.thickness = thickness_.data();
+    v.index = index_.data();
+    v.pupil_radius = pupil_radius_.data();
+    v.field_angle = field_angle_.data();
+    v.field_target = field_target_.data();
+    return v;
+}
+
+// ---- ResidualLayout ---------------------------------------------------------------------------
+
+ResidualLayout::ResidualLayout(const BatchTopology& topology, const ResidualSettings& settings)
+    : topology_(topology), settings_(settings) {
+    topology_.validate();
+    if (settings.rings < 1 || settings.rings > kMaxRings)
+        throw std::invalid_argument("ResidualLayout: rings must be in [1, 32]");
+    if (settings.spokes < 1) throw std::invalid_argument("ResidualLayout: spokes must be >= 1");
+    for (PupilMode m : topology.pupil_mode)
+        if (m != PupilMode::Axis && settings.spokes > MKB_MAX_SPOKES)
+            throw std::invalid_argument("ResidualLayout: spokes must be <= 64 in this build");
+    if (!(settings.fail_weight >= 0 && std::isfinite(settings.fail_weight)))
+        throw std::invalid_argument("ResidualLayout: fail_weight must be finite and >= 0");
+    int64_t off = 0;
+    for (int f = 0; f < topology.fields; ++f) {
+        const int n = sample_count(settings.rings, settings.spokes, topology.pupil_mode[f]);
+        samples_.push_back(n);
+        field_offset_.push_back(off);
+        off += static_cast<int64_t>(topology.wavelengths) * n;
+    }
+    rays_ = off;
+}
+
+int64_t ResidualLayout::trace_rows() const {
+    return settings_.failure == FailureMode::Soft ? 2 * rays_ : rays_;
+}
+
+int64_t ResidualLayout::offset(int f, int l) const {
+    if (f < 0 || f >= topology_.fields) throw std::out_of_range("ResidualLayout: field");
+    if (l < 0 || l >= topology_.wavelengths) throw std::out_of_range("ResidualLayout: wavelength");
+    return field_offset_[f] + static_cast<int64_t>(l) * samples_[f];
+}
+
+std::unique_ptr<ResidualPlan> ResidualLayout::plan(const SystemBatchHost& batch) const {
+    if (batch.fields() != topology_.fields || batch.wavelengths() != topology_.wavelengths)
+        throw std::invalid_argument("ResidualLayout: batch does not match the layout");
+    std::unique_ptr<ResidualPlan> p(new ResidualPlan());
+    const int n = settings_.rings;
+    for (int i = 0; i < n; ++i) {
+        p->u_.push_back(detail::kGaussLegendre[n - 1][2 * i]);
+        p->w_.push_back(detail::kGaussLegendre[n - 1][2 * i + 1]);
+    }
+    for (PupilMode m : topology_.pupil_mode) p->modes_.push_back(static_cast<uint8_t>(m));
+    p->field_weight_ = batch.field_weight;
+    p->wavelength_weight_ = batch.wavelength_weight;
+    mkb_residual_plan& c = p->plan_;
+    c.rings = n;
+    c.spokes = settings_.spokes;
+    c.failure = static_cast<int32_t>(settings_.failure);
+    c.precision = static_cast<int32_t>(settings_.precision);
+    c.fail_weight = settings_.fail_weight;
+    c.reference_wavelength_nm = batch.reference_wavelength_nm;
+    c.fields = topology_.fields;
+    c.wavelengths = topology_.wavelengths;
+    c.pupil_mode = p->modes_.data();
+    c.field_weight = p->field_weight_.data();
+    c.wavelength_weight = p->wavelength_weight_.data();
+    c.quad_u = p->u_.data();
+    c.quad_w = p->w_.data();
+    return p;
+}
+
+// ---- VariableSet / LmOptions ----------------------------------------------------------------
+
+VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> variables)
+    : variables_(std::move(variables)) {
+    const int S = topology.surfaces;
+    if (variables_.size() > MKB_MAX_VARIABLES)
+        throw std::invalid_argument("VariableSet: at most 64 variables");
+    std::set<std::pair<bool, int>> seen;
+    for (size_t k = 0; k < variables_.size(); ++k) {
+        Variable& v = variables_[k];
+        if (v.type == VariableType::Curvature) {
+            if (v.surface < 1 || v.surface >= S || topology.type[v.surface] != SurfaceKind::Sphere)
+                throw std::invalid_argument("VariableSet: curvature variable needs a sphere");
+        } else if (v.type == VariableType::Thickness) {
+            if (v.surface < 0 || v.surface >= S - 1)
+                throw std::invalid_argument("VariableSet: thickness surface out of range");
+        } else if (v.type == VariableType::WorkingDistance) {
+            v.surface = S - 1;
+        } else {
+            throw std::logic_error("VariableSet: variable type not traced by this build");
+        }
+        if (!seen.insert({v.type == VariableType::Curvature, v.surface}).second)
+            throw std::invalid_argument("VariableSet: parameter already used by a variable");
+        if (std::isnan(v.lower) || std::isnan(v.upper) || v.lower > v.upper)
+            throw std::invalid_argument("VariableSet: invalid bounds");
+        if (!(v.typical > 0 && std::isfinite(v.typical)))
+            throw std::invalid_argument("VariableSet: typical size must be > 0");
+        type_.push_back(static_cast<int32_t>(v.type));
+        surface_.push_back(v.surface);
+        lower_.push_back(v.lower);
+        upper_.push_back(v.upper);
+        typical_.push_back(v.typical);
+    }
+}
+
+std::vector<double> VariableSet::extract(const SystemBatchHost& batch, int v) const {
+    std::vector<double> x;
+    for (const Variable& var : variables_)
+        x.push_back(var.type == VariableType::Curvature ? batch.curvature(v, var.surface)
+                                                       : batch.thickness(v, var.surface));
+    return x;
+}
+
+void VariableSet::apply(SystemBatchHost& batch, int v, const double* x) const {
+    for (size_t k = 0; k < variables_.size(); ++k) {
+        const Variable& var = variables_[k];
+        if (var.type == VariableType::Curvature) batch.curvature(v, var.surface) = x[k];
+        else batch.thickness(v, var.surface) = x[k];
+    }
+}
+
+mkb_variables VariableSet::c_struct() const {
+    mkb_variables c{};
+    c.count = size();
+    c.type = type_.data();
+    c.surface = surface_.data();
+    c.lower = lower_.data();
+    c.upper = upper_.data();
+    c.typical = typical_.data();
+    return c;
+}
+
+mkb_lm_options LmOptions::c_struct() const {
+    mkb_lm_options o{};
+    o.max_iterations = max_iterations;
+    o.reject_new_failures = reject_new_failures ? 1 : 0;
+    o.ftol = ftol;
+    o.xtol = xtol;
+    o.gtol = gtol;
+    o.initial_damping = initial_damping;
+    o.max_damping = max_damping;
+    o.diag_floor = diag_floor;
+    o.jacobian = static_cast<int32_t>(jacobian);
+    o.gram_exact = gram_exact ? 1 : 0;
+    return o;
+}
+
+// ---- cuda ------------------------------------------------------------------------------------
+namespace cuda {
+
+void check(int status, const char* what) {
+    if (status == MKB_OK) return;
+    const std::string msg = std::string(what) + ": " + mkb_last_error();
+    if (status == MKB_ERR_ARGUMENT) throw std::invalid_argument(msg);
+    if (status == MKB_ERR_UNSUPPORTED) throw std::logic_error(msg);
+    throw CudaError(msg);
+}
+
+namespace {
+
+void cuda_check(cudaError_t err, const char* what) {
+    if (err != cudaSuccess)
+        throw CudaError(std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+template <class T>
+void copy_out(std::vector<T>& dst, const DeviceBuffer& src, size_t count, void* stream) {
+    dst.resize(count);
+    if (count == 0) return;
+    cuda_check(cudaMemcpyAsync(dst.data(), src.get(), count * sizeof(T), cudaMemcpyDeviceToHost,
+                               as_stream(stream)),
+               "download");
+}
+
+template <class T>
+void* upload(DeviceBuffer& dst, const std::vector<T>& src, void* stream) {
+    void* p = dst.reserve(src.size() * sizeof(T));
+    if (!src.empty())
+        cuda_check(cudaMemcpyAsync(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                   as_stream(stream)),
+                   "upload");
+    return p;
+}
+
+}  // namespace
+
+DeviceBuffer::~DeviceBuffer() { release(); }
+
+void* DeviceBuffer::reserve(size_t bytes) {
+    if (bytes <= bytes_ && ptr_ != nullptr) return ptr_;
+    release();
+    if (bytes == 0) return nullptr;
+    cuda_check(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    bytes_ = bytes;
+    return ptr_;
+}
+
+void DeviceBuffer::release() {
+    if (ptr_ != nullptr) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+}
+
+void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
+    batch.validate_values();
+    const mkb_batch_view view = batch.view();
+    const int32_t stride = mkb_record_stride(view.surfaces, view.wavelengths, view.fields);
+    host_records_.assign(static_cast<size_t>(view.variants) * stride, 0.0);
+    check(mkb_pack_batch_host(&view, host_records_.data()), "pack batch");
+    void* d = cuda::upload(records_, host_records_, stream);
+    type_.assign(view.type, view.type + view.surfaces);
+    batch_.variants = view.variants;
+    batch_.surfaces = view.surfaces;
+    batch_.wavelengths = view.wavelengths;
+    batch_.fields = view.fields;
+    batch_.record_stride = stride;
+    batch_.reserved = 0;
+    batch_.records = static_cast<const double*>(d);
+    batch_.type = type_.data();
+}
+
+TraceEngine::TraceEngine(int device) : device_(device) {
+    int count = 0;
+    cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (device < 0 || device >= count)
+        throw std::invalid_argument("TraceEngine: no such CUDA device");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaStream_t s;
+    cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    stream_ = s;
+}
+
+TraceEngine::~TraceEngine() {
+    release();
+    if (stream_ != nullptr) cudaStreamDestroy(as_stream(stream_));
+}
+
+void TraceEngine::release() {
+    out_.release();
+    opd_.release();
+    status_.release();
+    merit_.release();
+    failed_.release();
+    hard_.release();
+    workspace_.release();
+}
+
+void TraceEngine::synchronize() {
+    cuda_check(cudaStreamSynchronize(as_stream(stream_)), "synchronize");
+    check(mkb_device_status(), "device status");
+}
+
+void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
+                      const ResidualSettings& settings, TraceOutput& out) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const ResidualLayout layout(batch.topology(), settings);
+    const auto plan = layout.plan(batch);
+    batch_.upload(batch, stream_);
+    const mkb_device_batch b = batch_.c_struct();
+    const size_t V = static_cast<size_t>(batch.variants());
+    if (mode == TraceMode::Residuals) {
+        const int64_t rows = layout.trace_rows(), rays = layout.rays_per_variant();
+        auto* res = static_cast<double*>(out_.reserve(V * rows * sizeof(double)));
+        auto* opd = static_cast<double*>(opd_.reserve(V * rays * sizeof(double)));
+        auto* st = static_cast<uint8_t*>(status_.reserve(V * rays));
+        check(mkb_residuals_device(&b, plan->get(), res, rows, opd, st, stream_), "residuals");
+        copy_out(out.residuals, out_, V * rows, stream_);
+        copy_out(out.opd, opd_, V * rays, stream_);
+        copy_out(out.status, status_, V * rays, stream_);
+    } else {
+        const size_t ws = mkb_merit_workspace_bytes(batch.variants(), plan->get());
+        workspace_.reserve(ws);
+        auto* merit = static_cast<double*>(merit_.reserve(V * sizeof(double)));
+        auto* failed = static_cast<int64_t*>(failed_.reserve(V * sizeof(int64_t)));
+        auto* hard = static_cast<int64_t*>(hard_.reserve(V * sizeof(int64_t)));
+        check(mkb_merit_device(&b, plan->get(), merit, failed, hard, workspace_.get(),
+                               workspace_.bytes(), stream_),
+              "merit");
+        copy_out(out.merit, merit_, V, stream_);
+        copy_out(out.failed, failed_, V, stream_);
+        copy_out(out.hard_failed, hard_, V, stream_);
+    }
+    synchronize();
+}
+
+namespace {
+
+int runs_of(const VariableSet& variables, const SystemBatchHost& base,
+            const std::vector<double>& x0) {
+    const int P = variables.size();
+    if (P < 1) throw std::invalid_argument("variables: at least one variable");
+    if (x0.size() % P != 0) throw std::invalid_argument("x0: size is not a multiple of P");
+    const int runs = static_cast<int>(x0.size() / P);
+    if (base.variants() != 1 && base.variants() != runs)
+        throw std::invalid_argument("base batch must hold 1 variant or one per run");
+    return runs;
+}
+
+}  // namespace
+
+void DeviceFdJacobian::compute(TraceEngine& engine, const VariableSet& variables,
+                               const SystemBatchHost& base, const std::vector<double>& x0,
+                               const ResidualSettings& settings, JacobianResult& out) {
+    cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
+    const int runs = runs_of(variables, base, x0);
+    const int P = variables.size();
+    const ResidualLayout layout(base.topology(), settings);
+    const auto plan = layout.plan(base);
+    templates_.upload(base, engine.stream());
+    const mkb_device_batch t = templates_.c_struct();
+    const mkb_variables v = variables.c_struct();
+    const int64_t R = layout.trace_rows();
+    const auto* x = static_cast<const double*>(upload(x0_, x0, engine.stream()));
+    auto* J = static_cast<double*>(J_.reserve(sizeof(double) * runs * P * R));
+    auto* r0 = static_cast<double*>(r0_.reserve(sizeof(double) * runs * R));
+    const int chunk = runs < 64 ? runs : 64;
+    const size_t ws = mkb_fd_jacobian_workspace_bytes(&t, plan->get(), P, runs, chunk);
+    if (ws == 0) check(MKB_ERR_ARGUMENT, "fd jacobian workspace");
+    workspace_.reserve(ws);
+    check(mkb_fd_jacobian_device(&t, plan->get(), &v, x, runs, J, r0, nullptr, workspace_.get(),
+                                 workspace_.bytes(), engine.stream()),
+          "fd jacobian");
+    out.runs = runs;
+    out.P = P;
+    out.rows = R;
+    copy_out(out.J, J_, static_cast<size_t>(runs) * P * R, engine.stream());
+    copy_out(out.r0, r0_, static_cast<size_t>(runs) * R, engine.stream());
+    engine.synchronize();
+}
+
+void DeviceAdjointJacobian::compute(TraceEngine& engine, const VariableSet& variables,
+                                    const SystemBatchHost& base, const std::vector<double>& x0,
+                                    const ResidualSettings& settings, JacobianResult& out) {
+    cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
+    const int runs = runs_of(variables, base, x0);
+    const int P = variables.size();
+    const ResidualLayout layout(base.topology(), settings);
+    const auto plan = layout.plan(base);
+    templates_.upload(base, engine.stream());
+    const mkb_device_batch t = templates_.c_struct();
+    const mkb_variables v = variables.c_struct();
+    const int64_t R = layout.trace_rows();
+    const auto* x = static_cast<const double*>(upload(x0_, x0, engine.stream()));
+    auto* J = static_cast<double*>(J_.reserve(sizeof(double) * runs * P * R));
+    auto* r0 = static_cast<double*>(r0_.reserve(sizeof(double) * runs * R));
+    auto* st = static_cast<uint8_t*>(status_.reserve(static_cast<size_t>(runs) *
+                                                     layout.rays_per_variant()));
+    workspace_.reserve(mkb_adjoint_jacobian_workspace_bytes(&t, runs));
+    check(mkb_adjoint_jacobian_device(&t, plan->get(), &v, x, runs, J, r0, st, workspace_.get(),
+                                      workspace_.bytes(), engine.stream()),
+          "adjoint jacobian");
+    out.runs = runs;
+    out.P = P;
+    out.rows = R;
+    copy_out(out.J, J_, static_cast<size_t>(runs) * P * R, engine.stream());
+    copy_out(out.r0, r0_, static_cast<size_t>(runs) * R, engine.stream());
+    engine.synchronize();
+}
+
+void DeviceNormalEquations::compute(TraceEngine& engine, const JacobianResult& jac, bool exact) {
+    cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
+    if (jac.J.size() != static_cast<size_t>(jac.runs) * jac.P * jac.rows ||
+        jac.r0.size() != static_cast<size_t>(jac.runs) * jac.rows)
+        throw std::invalid_argument("normal equations: J / r0 sizes do not match");
+    const auto* J = static_cast<const double*>(upload(J_, jac.J, engine.stream()));
+    const auto* r = static_cast<const double*>(upload(r_, jac.r0, engine.stream()));
+    const size_t n = static_cast<size_t>(jac.P) + 1;
+    auto* g = static_cast<double*>(dgram_.reserve(sizeof(double) * jac.runs * n * n));
+    check(mkb_normal_equations_device(J, r, jac.runs, jac.P, jac.rows, g, exact ? 1 : 0,
+                                      engine.stream()),
+          "normal equations");
+    copy_out(gram_, dgram_, jac.runs * n * n, engine.stream());
+    engine.synchronize();
+    runs_ = jac.runs;
+    P_ = jac.P;
+}
+
+void DeviceNormalEquations::download(std::vector<double>& a, std::vector<double>& g) const {
+    const size_t P = P_, n = P + 1;
+    a.assign(static_cast<size_t>(runs_) * P * P, 0.0);
+    g.assign(static_cast<size_t>(runs_) * P, 0.0);
+    for (size_t run = 0; run < static_cast<size_t>(runs_); ++run) {
+        const double* G = gram_.data() + run * n * n;
+        for (size_t q = 0; q < P; ++q) {
+            for (size_t p = 0; p < P; ++p) a[run * P * P + q * P + p] = G[q * n + p];
+            g[run * P + q] = G[q * n + P];
+        }
+    }
+}
+
+LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
+                         const SystemBatchHost& base, const std::vector<double>& x0,
+                         const LmOptions& options, const ResidualSettings& settings,
+                         LmGpuStats* stats) {
+    cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
+    const int runs = runs_of(variables, base, x0);
+    const int P = variables.size();
+    const ResidualLayout layout(base.topology(), settings);
+    const auto plan = layout.plan(base);
+    DeviceSystemBatch templates;
+    templates.upload(base, engine.stream());
+    const mkb_device_batch t = templates.c_struct();
+    const mkb_variables v = variables.c_struct();
+    const mkb_lm_options o = options.c_struct();
+    DeviceBuffer dx0, ws;
+    const auto* x = static_cast<const double*>(upload(dx0, x0, engine.stream()));
+    const size_t bytes = mkb_lm_workspace_bytes(&t, plan->get(), &v, &o, runs);
+    if (bytes == 0) check(MKB_ERR_ARGUMENT, "lm workspace");
+    ws.reserve(bytes);
+    check(mkb_lm_start_device(&t, plan->get(), &v, &o, x, runs, ws.get(), ws.bytes(),
+                              engine.stream()),
+          "lm start");
+    int32_t running = runs;
+    int cycles = 0;
+    while (running > 0 && cycles <= options.max_iterations) {
+        check(mkb_lm_cycle_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
+                                  engine.stream()),
+              "lm cycle");
+        ++cycles;
+        check(mkb_lm_results_device(&t, plan->get(), &v, &o, runs, ws.get(), nullptr, nullptr,
+                                    nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    nullptr, &running, engine.stream()),
+              "lm results");
+        engine.synchronize();
+    }
+    LmResult r;
+    const size_t R = static_cast<size_t>(runs), H = static_cast<size_t>(options.max_iterations) + 1;
+    r.x.resize(R * P);
+    r.merit.resize(R);
+    r.damping.resize(R);
+    r.history.resize(R * H);
+    r.status.resize(R);
+    r.iterations.resize(R);
+    r.accepted.resize(R);
+    r.jacobians.resize(R);
+    r.failed.resize(R);
+    r.hard_failed.resize(R);
+    check(mkb_lm_results_device(&t, plan->get(), &v, &o, runs, ws.get(), r.x.data(),
+                                r.merit.data(), r.status.data(), r.iterations.data(),
+                                r.accepted.data(), r.jacobians.data(), r.damping.data(),
+                                r.history.data(), r.failed.data(), r.hard_failed.data(), nullptr,
+                                engine.stream()),
+          "lm results");
+    engine.synchronize();
+    if (stats != nullptr) stats->cycles = cycles;
+    return r;
+}
+
+}  // namespace cuda
+}  // namespace mkb

@@ -1,0 +1,305 @@
+// C++ host API of the B200 batched trace-and-optimise path.
+//
+// Mirrors the reference's host classes so that its callers (`mikroptim trace --gpu`,
+// `mikroptim optimize --gpu`) can switch by changing the namespace:
+//   BatchTopology, SystemBatchHost   include/mikroptim/batch/system_batch.hpp:229,268
+//   ResidualSettings, ResidualLayout include/mikroptim/batch/batch_residuals.hpp:24,62
+//   Variable, VariableSet            include/mikroptim/optim/variable_set.hpp:20,63
+//   LmOptions, LmStatus              include/mikroptim/optim/levenberg_marquardt.hpp:26,85
+//   cuda::TraceEngine                include/mikroptim/cuda/trace_engine.hpp
+//   cuda::DeviceFdJacobian, cuda::DeviceAdjointJacobian, cuda::DeviceNormalEquations,
+//   cuda::optimize_lm_gpu            include/mikroptim/cuda/*.hpp
+// Everything runs through the C ABI of libmikroptim_b200.so (include/mikroptim_b200.h).
+// Errors are thrown before any device work: std::invalid_argument for bad arguments,
+// std::out_of_range for indices, std::logic_error for features this build does not trace,
+// cuda::CudaError for device failures -- the reference's exception classes.
+#pragma once
+
+#include <cstdint>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mikroptim_b200.h"
+
+namespace mkb {
+
+enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2 };
+enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
+enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
+enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2 };
+enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2 };
+enum class JacobianMethod : int32_t { FiniteDifference = 0, Adjoint = 1 };
+enum class LmStatus : int32_t {
+    Running = 0, ConvergedMerit = 1, ConvergedStep = 2, ConvergedGradient = 3,
+    ConvergedStall = 4, MaxIterations = 5, DampingLimit = 6, NumericalError = 7
+};
+
+// What every variant of a batch shares (one topology per batch).
+struct BatchTopology {
+    int surfaces = 0, wavelengths = 0, fields = 0;
+    std::vector<SurfaceKind> type;      // [S], type[0] = Stop
+    std::vector<PupilMode> pupil_mode;  // [F]
+    void validate() const;
+};
+
+// V variants as FP64 structure of arrays, variant outermost.
+class SystemBatchHost {
+public:
+    SystemBatchHost(BatchTopology topology, int variants);
+
+    int variants() const { return variants_; }
+    int surfaces() const { return topology_.surfaces; }
+    int wavelengths() const { return topology_.wavelengths; }
+    int fields() const { return topology_.fields; }
+    const BatchTopology& topology() const { return topology_; }
+
+    double& curvature(int v, int s) { return curvature_.at(index2(v, s, surfaces())); }
+    double& thickness(int v, int s) { return thickness_.at(index2(v, s, surfaces())); }
+    double& index(int v, int s, int l);
+    double& pupil_radius(int v) { return pupil_radius_.at(check_v(v)); }
+    double& field_angle(int v, int f) { return field_angle_.at(index2(v, f, fields())); }
+    double& field_target(int v, int f) { return field_target_.at(index2(v, f, fields())); }
+    double curvature(int v, int s) const { return curvature_.at(index2(v, s, surfaces())); }
+    double thickness(int v, int s) const { return thickness_.at(index2(v, s, surfaces())); }
+
+    double reference_wavelength_nm = 0.0;
+    std::vector<double> wavelength_weight;  // [L]
+    std::vector<double> field_weight;       // [F]
+
+    // validate_values (src/batch/system_batch.cpp:558) for the traced fields
+    void validate_values() const;
+    // C view over the arrays (valid while the batch is alive and unresized)
+    mkb_batch_view view() const;
+
+private:
+    size_t check_v(int v) const;
+    size_t index2(int v, int i, int n) const;
+    BatchTopology topology_;
+    int variants_;
+    std::vector<uint8_t> type_;
+    std::vector<double> curvature_, thickness_, index_, pupil_radius_, field_angle_,
+        field_target_;
+};
+
+struct ResidualSettings {
+    int rings = 10;
+    int spokes = 8;
+    FailureMode failure = FailureMode::Soft;
+    double fail_weight = 1e6;  // kDefaultFailWeight (merit/ray_residual.hpp:175)
+    Precision precision = Precision::FP64;
+};
+
+// The C plan for one batch; owns the arrays its pointers reference (not copyable).
+class ResidualPlan {
+public:
+    const mkb_residual_plan* get() const { return &plan_; }
+    ResidualPlan(const ResidualPlan&) = delete;
+    ResidualPlan& operator=(const ResidualPlan&) = delete;
+
+private:
+    friend class ResidualLayout;
+    ResidualPlan() = default;
+    mkb_residual_plan plan_{};
+    std::vector<uint8_t> modes_;
+    std::vector<double> field_weight_, wavelength_weight_, u_, w_;
+};
+
+// Row layout of one variant: tuples (f, l) f-major then l, sample k = i*M + j inside a tuple,
+// penalty rows after the ray rows in soft-failure mode.
+class ResidualLayout {
+public:
+    ResidualLayout(const BatchTopology& topology, const ResidualSettings& settings);
+    int64_t rays_per_variant() const { return rays_; }
+    int64_t trace_rows() const;
+    int64_t offset(int f, int l) const;
+    int samples(int f) const { return samples_.at(f); }
+    const ResidualSettings& settings() const { return settings_; }
+    // the plan is heap-allocated so its internal pointers stay valid
+    std::unique_ptr<ResidualPlan> plan(const SystemBatchHost& batch) const;
+
+private:
+    BatchTopology topology_;
+    ResidualSettings settings_;
+    std::vector<int> samples_;
+    std::vector<int64_t> field_offset_;
+    int64_t rays_ = 0;
+};
+
+struct Variable {
+    VariableType type = VariableType::Curvature;
+    int surface = 0;
+    double lower = -std::numeric_limits<double>::infinity();
+    double upper = std::numeric_limits<double>::infinity();
+    double typical = 1.0;
+};
+
+class VariableSet {
+public:
+    VariableSet(const BatchTopology& topology, std::vector<Variable> variables);
+    int size() const { return static_cast<int>(variables_.size()); }
+    const std::vector<Variable>& variables() const { return variables_; }
+    std::vector<double> extract(const SystemBatchHost& batch, int v) const;
+    void apply(SystemBatchHost& batch, int v, const double* x) const;
+    mkb_variables c_struct() const;
+
+private:
+    std::vector<Variable> variables_;
+    std::vector<int32_t> type_, surface_;
+    std::vector<double> lower_, upper_, typical_;
+};
+
+struct LmOptions {
+    int max_iterations = 100;
+    bool reject_new_failures = true;
+    double ftol = 1e-10, xtol = 1e-10, gtol = 1e-10;
+    double initial_damping = 1e-3;
+    double max_damping = 1e16;
+    double diag_floor = 1e-12;
+    JacobianMethod jacobian = JacobianMethod::Adjoint;
+    bool gram_exact = true;  // false: FP64 tensor cores (with the adjoint: J never in memory)
+    mkb_lm_options c_struct() const;
+};
+
+namespace cuda {
+
+class CudaError : public std::runtime_error {
+public:
+    using std::runtime_error::runtime_error;
+};
+
+// Throws the reference's exception class for a non-zero mkb_status.
+void check(int status, const char* what);
+
+// One device allocation, grown on demand and reused (the reference's buffer reuse).
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) {
+        o.ptr_ = nullptr;
+        o.bytes_ = 0;
+    }
+    ~DeviceBuffer();
+    void* reserve(size_t bytes);
+    void* get() const { return ptr_; }
+    size_t bytes() const { return bytes_; }
+    void release();
+
+private:
+    void* ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+enum class TraceMode { Residuals, Merit };
+
+struct TraceOutput {
+    std::vector<double> residuals;     // RESIDUALS: [V][trace_rows]
+    std::vector<double> opd;           // RESIDUALS: [V][rays]
+    std::vector<uint8_t> status;       // RESIDUALS: [V][rays]
+    std::vector<double> merit;         // MERIT: [V]
+    std::vector<int64_t> failed;       // MERIT: [V]
+    std::vector<int64_t> hard_failed;  // MERIT: [V]
+};
+
+// Device-resident packed batch (records and surface types).
+class DeviceSystemBatch {
+public:
+    DeviceSystemBatch() = default;
+    void upload(const SystemBatchHost& batch, void* stream);
+    mkb_device_batch c_struct() const { return batch_; }
+
+private:
+    mkb_device_batch batch_{};
+    std::vector<uint8_t> type_;
+    std::vector<double> host_records_;
+    DeviceBuffer records_;
+};
+
+class TraceEngine {
+public:
+    explicit TraceEngine(int device = 0);
+    ~TraceEngine();
+    TraceEngine(const TraceEngine&) = delete;
+    TraceEngine& operator=(const TraceEngine&) = delete;
+
+    // TraceEngine::run: validation, upload, RESIDUALS or MERIT, download
+    void run(const SystemBatchHost& batch, TraceMode mode, const ResidualSettings& settings,
+             TraceOutput& out);
+    int device() const { return device_; }
+    void* stream() const { return stream_; }
+    void release();
+    void synchronize();
+
+private:
+    int device_;
+    void* stream_ = nullptr;
+    DeviceSystemBatch batch_;
+    DeviceBuffer out_, opd_, status_, merit_, failed_, hard_, workspace_;
+};
+
+// J [runs][P][R] (column p of run i at (i*P + p)*R) and r0 [runs][R] on the host.
+struct JacobianResult {
+    int runs = 0, P = 0;
+    int64_t rows = 0;
+    std::vector<double> J, r0;
+};
+
+class DeviceFdJacobian {
+public:
+    void compute(TraceEngine& engine, const VariableSet& variables, const SystemBatchHost& base,
+                 const std::vector<double>& x0, const ResidualSettings& settings,
+                 JacobianResult& out);
+
+private:
+    DeviceSystemBatch templates_;
+    DeviceBuffer x0_, J_, r0_, workspace_;
+};
+
+class DeviceAdjointJacobian {
+public:
+    void compute(TraceEngine& engine, const VariableSet& variables, const SystemBatchHost& base,
+                 const std::vector<double>& x0, const ResidualSettings& settings,
+                 JacobianResult& out);
+
+private:
+    DeviceSystemBatch templates_;
+    DeviceBuffer x0_, J_, r0_, status_, workspace_;
+};
+
+class DeviceNormalEquations {
+public:
+    // gram of [J r0] per run; exact: FMA chain in row order (normal_equations_host bit for
+    // bit), else FP64 tensor cores
+    void compute(TraceEngine& engine, const JacobianResult& jac, bool exact);
+    // A [runs][P][P] (column-major per run, as the reference) and g [runs][P]
+    void download(std::vector<double>& a, std::vector<double>& g) const;
+
+private:
+    int runs_ = 0, P_ = 0;
+    std::vector<double> gram_;
+    DeviceBuffer J_, r_, dgram_;
+};
+
+struct LmResult {
+    std::vector<double> x, merit, damping, history;
+    std::vector<int32_t> status, iterations, accepted, jacobians;
+    std::vector<int64_t> failed, hard_failed;
+};
+
+struct LmGpuStats {
+    int cycles = 0;
+};
+
+// Batched LM of the runs x0 [runs][P] on `base` (1 variant for all runs or one per run),
+// one soft-failure penalty pass; the whole loop runs on the device.
+LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
+                         const SystemBatchHost& base, const std::vector<double>& x0,
+                         const LmOptions& options, const ResidualSettings& settings,
+                         LmGpuStats* stats = nullptr);
+
+}  // namespace cuda
+}  // namespace mkb

@@ -1,0 +1,173 @@
+// Test driver of the C++ host layer (mikroptim_b200/host): traces, differentiates and
+// optimises a small singlet batch through the reference-shaped C++ classes and checks every
+// result against the oracle (oracle/liboracle.so, the C restatement of the reference CPU
+// path) -- bit for bit in the FP64 mode. Exit status 0 when every check passes.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "mikroptim_b200.hpp"
+#include "mko_oracle.h"
+
+namespace {
+
+int failures = 0, checks = 0;
+
+void expect(bool ok, const char* what) {
+    ++checks;
+    if (!ok) {
+        ++failures;
+        std::printf("FAIL: %s\n", what);
+    }
+}
+
+template <class T>
+bool same_bits(const std::vector<T>& a, const std::vector<T>& b) {
+    return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(T)) == 0;
+}
+
+mkb::SystemBatchHost singlets(int V) {
+    using namespace mkb;
+    BatchTopology topo;
+    topo.surfaces = 3;
+    topo.wavelengths = 3;
+    topo.fields = 3;
+    topo.type = {SurfaceKind::Stop, SurfaceKind::Sphere, SurfaceKind::Sphere};
+    topo.pupil_mode = {PupilMode::Axis, PupilMode::Half, PupilMode::Half};
+    SystemBatchHost b(topo, V);
+    b.reference_wavelength_nm = 587.6;
+    const double lambda_um[3] = {0.4861, 0.5876, 0.6563};
+    const double angle_deg[3] = {0.0, 0.7, 1.0};
+    const double pi = 3.14159265358979323846;
+    for (int v = 0; v < V; ++v) {
+        b.curvature(v, 1) = (1.0 / 50.0) * (1.0 + 0.03 * v);
+        b.curvature(v, 2) = (-1.0 / 50.0) * (1.0 - 0.02 * v);
+        b.thickness(v, 0) = 0.0;
+        b.thickness(v, 1) = 6.0 * (1.0 + 0.01 * v);
+        b.thickness(v, 2) = 46.0 + 0.5 * v;
+        for (int l = 0; l < 3; ++l) {
+            b.index(v, 0, l) = 1.0;
+            b.index(v, 1, l) = 1.5046 + 0.00420 / (lambda_um[l] * lambda_um[l]);
+            b.index(v, 2, l) = 1.0;
+        }
+        b.pupil_radius(v) = 5.0;
+        for (int f = 0; f < 3; ++f) {
+            b.field_angle(v, f) = angle_deg[f] * pi / 180.0;
+            b.field_target(v, f) = 48.5 * std::tan(angle_deg[f] * pi / 180.0);
+        }
+    }
+    return b;
+}
+
+}  // namespace
+
+int main() {
+    using namespace mkb;
+    const int V = 6;
+    SystemBatchHost batch = singlets(V);
+    ResidualSettings settings;
+    settings.rings = 6;
+    settings.spokes = 12;
+    const ResidualLayout layout(batch.topology(), settings);
+    const auto plan = layout.plan(batch);
+    const mkb_batch_view view = batch.view();
+    const int64_t rays = layout.rays_per_variant(), rows = layout.trace_rows();
+    expect(rays == mko_port_rays_per_variant(plan->get()), "rays per variant");
+
+    cuda::TraceEngine engine(0);
+    // RESIDUALS and MERIT
+    cuda::TraceOutput out;
+    engine.run(batch, cuda::TraceMode::Residuals, settings, out);
+    std::vector<double> res(V * rows), opd(V * rays);
+    std::vector<uint8_t> st(V * rays);
+    expect(mko_port_residuals(&view, plan->get(), res.data(), opd.data(), st.data(), 1) == 0,
+           "oracle residuals");
+    expect(same_bits(out.residuals, res), "RESIDUALS bit-identical to the oracle");
+    expect(same_bits(out.opd, opd), "OPD bit-identical to the oracle");
+    expect(same_bits(out.status, st), "status identical to the oracle");
+    engine.run(batch, cuda::TraceMode::Merit, settings, out);
+    std::vector<double> merit(V);
+    std::vector<int64_t> failed(V), hard(V);
+    expect(mko_port_merit(&view, plan->get(), merit.data(), failed.data(), hard.data(), 1) == 0,
+           "oracle merit");
+    expect(same_bits(out.merit, merit), "MERIT bit-identical to the oracle");
+    expect(same_bits(out.failed, failed) && same_bits(out.hard_failed, hard), "failure counts");
+
+    // Jacobians and normal equations
+    const VariableSet vars(batch.topology(),
+                           {{VariableType::Curvature, 1, -0.2, 0.2, 0.01},
+                            {VariableType::Curvature, 2, -0.2, 0.2, 0.01},
+                            {VariableType::Thickness, 1, 0.5, 20.0, 1.0},
+                            {VariableType::WorkingDistance, 2, 1.0, 500.0, 1.0}});
+    const int P = vars.size();
+    std::vector<double> x0;
+    for (int v = 0; v < V; ++v) {
+        const std::vector<double> x = vars.extract(batch, v);
+        x0.insert(x0.end(), x.begin(), x.end());
+    }
+    const mkb_variables cv = vars.c_struct();
+    std::vector<double> J(static_cast<size_t>(V) * P * rows), r0(static_cast<size_t>(V) * rows);
+    cuda::JacobianResult jac;
+    cuda::DeviceFdJacobian fd;
+    fd.compute(engine, vars, batch, x0, settings, jac);
+    expect(mko_port_fd_jacobian(&view, plan->get(), &cv, x0.data(), V, J.data(), r0.data(),
+                                nullptr, 1) == 0,
+           "oracle fd jacobian");
+    expect(same_bits(jac.J, J) && same_bits(jac.r0, r0), "FD Jacobian bit-identical");
+    cuda::DeviceAdjointJacobian adj;
+    adj.compute(engine, vars, batch, x0, settings, jac);
+    std::vector<uint8_t> jst(static_cast<size_t>(V) * rays);
+    expect(mko_port_adjoint_jacobian(&view, plan->get(), &cv, x0.data(), V, J.data(), r0.data(),
+                                     jst.data(), 1) == 0,
+           "oracle adjoint jacobian");
+    expect(same_bits(jac.J, J) && same_bits(jac.r0, r0), "adjoint Jacobian bit-identical");
+    cuda::DeviceNormalEquations ne;
+    ne.compute(engine, jac, true);
+    std::vector<double> a, g;
+    ne.download(a, g);
+    bool ne_ok = true;
+    for (int run = 0; run < V; ++run) {
+        std::vector<double> A(P * P), gg(P);
+        mko_port_normal_equations(J.data() + static_cast<size_t>(run) * P * rows,
+                                  r0.data() + static_cast<size_t>(run) * rows, P, rows,
+                                  A.data(), gg.data());
+        ne_ok = ne_ok && std::memcmp(A.data(), a.data() + run * P * P, sizeof(double) * P * P) == 0 &&
+                std::memcmp(gg.data(), g.data() + run * P, sizeof(double) * P) == 0;
+    }
+    expect(ne_ok, "normal equations bit-identical");
+
+    // LM on the device
+    LmOptions opt;
+    opt.max_iterations = 25;
+    cuda::LmGpuStats stats;
+    const cuda::LmResult lm = cuda::optimize_lm_gpu(engine, vars, batch, x0, opt, settings, &stats);
+    bool improved = true;
+    for (int run = 0; run < V; ++run)
+        improved = improved && lm.merit[run] < merit[run] && lm.iterations[run] > 0;
+    expect(improved, "LM lowers every run's merit");
+    expect(stats.cycles > 0, "LM ran cycles");
+
+    // argument errors are thrown before any device work
+    bool thrown = false;
+    try {
+        BatchTopology bad = batch.topology();
+        bad.type[0] = SurfaceKind::Sphere;
+        bad.validate();
+    } catch (const std::invalid_argument&) {
+        thrown = true;
+    }
+    expect(thrown, "invalid topology -> std::invalid_argument");
+    thrown = false;
+    try {
+        std::vector<double> short_x(P + 1, 0.0);
+        cuda::optimize_lm_gpu(engine, vars, batch, short_x, opt, settings);
+    } catch (const std::invalid_argument&) {
+        thrown = true;
+    }
+    expect(thrown, "x0 of the wrong size -> std::invalid_argument");
+
+    std::printf("host API: %d of %d checks passed\n", checks - failures, checks);
+    return failures == 0 ? 0 : 1;
+}

@@ -60,3 +60,34 @@ def test_lm_fused_adjoint_fma_reaches_same_optimum():
     assert np.all(g["status"] > 0)
     assert np.allclose(g["merit"], r["merit"], rtol=1e-6, atol=1e-12)
     assert np.allclose(g["x"], r["x"], rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("method", ["adjoint", "fd"])
+def test_lm_cycle_graph_replay_equals_direct_cycles(method):
+    """A cycle is a fixed launch sequence with device masks: replaying its CUDA graph advances
+    the runs exactly as calling the cycle does (bit for bit), FP64 exact path."""
+    import torch
+    b, st, vs, x0 = workloads.singlet(8)
+    lay = ResidualLayout(b.topology, st)
+    opt = engine.LmOptions(max_iterations=30, gram_exact=method == "fd",
+                           jacobian=engine.JACOBIAN_ADJOINT if method == "adjoint"
+                           else engine.JACOBIAN_FD)
+    db = engine.DeviceSystemBatch(b)
+    direct = engine.DeviceLm(db, lay, b, vs, opt, b.variants)
+    direct.start(x0)
+    for _ in range(12):
+        direct.cycle()
+    graphed = engine.DeviceLm(db, lay, b, vs, opt, b.variants)
+    graphed.start(x0)
+    graphed.cycle()
+    graph = graphed.capture()
+    for _ in range(11):
+        graph.replay()
+    torch.cuda.synchronize()
+    a, g = direct.results(), graphed.results()
+    for key in ("x", "merit", "status", "iterations", "accepted", "jacobians", "damping"):
+        assert np.array_equal(a[key], g[key]), key
+    h = ~np.isnan(a["history"])
+    assert np.array_equal(np.isnan(a["history"]), np.isnan(g["history"]))
+    assert np.array_equal(a["history"][h], g["history"][h])
+    assert int(a["iterations"].sum()) > 0
