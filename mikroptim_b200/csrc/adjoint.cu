@@ -349,12 +349,12 @@ namespace mkb {
 // ---- fused adjoint + normal equations ---------------------------------------------------------
 // Persistent CTAs take runs off a work queue; a CTA streams the run's rays in chunks of
 // kFusedThreads (one ray per thread):
-//   A  forward with checkpoints in shared memory, then ONE reverse sweep carrying two adjoint
-//      vectors (seed OPL = 1 and seed penalty = 1) that share the replay and the step-local
-//      quantities. The OPL row g_k = dOPL_k/dx goes to shared memory (Y, column-major, odd
-//      stride) with OPL_k beside it (Rv); the scaled penalty row s_p sqrt(W) dpi/dx goes to the
-//      CTA's slot of a global scratch buffer (L2-resident, coalesced: column c of thread t at
-//      [c][t]). Warps whose rays have no soft event run the single-seed sweep;
+//   A  forward trace that stores the ray state entering every surface in the CTA's slot of an
+//      L2-resident global scratch (thread-minor, coalesced), then ONE reverse sweep over those
+//      states carrying two adjoint vectors (seed OPL = 1 and seed penalty = 1) that share the
+//      step-local quantities (warps whose rays need one row run the single-seed sweep). The row
+//      y_k = [dOPL_k/dx | OPL_k] goes to shared memory (Y, column-major, residual in column
+//      P); the scaled penalty row s_p sqrt(W) dpi/dx goes to the scratch slot;
 //   B  per tuple segment of the chunk: weighted column means (a warp per column, shuffle sums)
 //      and the rows centred and scaled in place by all threads, x_k = s sqrt(W_k) (y_k -
 //      mu_seg); the segment is merged into the tuple's running mean with one extra row
@@ -363,9 +363,8 @@ namespace mkb {
 //      exactly [J r]^T [J r] of the piston-projected rows J_k = s sqrt(W_k) (g_k - gbar),
 //      r_k = s sqrt(W_k) (OPL_k - piston), with no second pass over the tuple and no J in
 //      memory;
-//   C  FP64 tensor cores accumulate J^T J (mma.sync m8n8k4 on 8 x 8 tiles of the upper
-//      triangle, accumulators in shared memory in fragment order); J^T r and r^T r are
-//      per-thread partial sums (thread = column x row phase) reduced once per run;
+//   C  FP64 tensor cores accumulate [J r]^T [J r] (mma.sync m8n8k4 on 8 x 8 tiles of the upper
+//      triangle, accumulators in shared memory in fragment order);
 //   D  in soft-failure mode, when the chunk has failed rays, the penalty rows (uncentred, value
 //      s_p sqrt(W) p_k) are loaded from the scratch slot into Y and accumulated the same way.
 // Output: gram [runs][P+1][P+1] as the normal-equation kernels write it.
@@ -381,7 +380,8 @@ constexpr int kMaxTileCols = MKB_MAX_VARIABLES / 8;                             
 constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 36
 constexpr int kMaxFusedSlots = 148 * 8;  // persistent CTAs at most (SMs x resident CTAs)
 
-__host__ __device__ inline int fused_np(int P) { return ((P + 7) / 8) * 8; }
+// columns of a row: the P derivatives, the residual in column P, zero padding to 8
+__host__ __device__ inline int fused_np(int P) { return ((P + 1 + 7) / 8) * 8; }
 
 struct FusedShared {
     uint64_t bar;
@@ -425,19 +425,6 @@ __device__ __forceinline__ void accumulate(const double* xt, int ld, int n, int 
         for (int k0 = 0; k0 < n; k0 += 4) dmma(d0, d1, ca[k0], cb[k0]);
         a[0] = d0;
         a[1] = d1;
-    }
-}
-
-// Partial sums of J^T r (columns c = lane and lane + 32 of the rows r = warp (mod 4)) and of
-// r^T r (lane 0 of every warp).
-__device__ __forceinline__ void accumulate_r(const double* xt, int ld, const double* rv, int n,
-                                             int NP, double& j0, double& j1, double& rr) {
-    const int c = threadIdx.x & 31;
-    for (int r = threadIdx.x >> 5; r < n; r += kFusedWarps) {
-        const double v = rv[r];
-        if (c < NP) j0 += xt[c * ld + r] * v;
-        if (c + 32 < NP) j1 += xt[(c + 32) * ld + r] * v;
-        if (c == 0) rr += v * v;
     }
 }
 
@@ -522,9 +509,10 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
 }
 
 // Reverse sweep with K adjoint vectors (seed k: OPL seed so[k], penalty seed sp[k]) writing
-// factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. One out-of-line copy per K keeps the
-// kernel's instruction footprint small.
-template <class N, int K>
+// factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
+// quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
+// out-of-line copy per K keeps the kernel's instruction footprint small.
+template <class N, class A, int K>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
                                             const double* rec, const RecordLayout& lay, int f,
                                             int l, const Sample& smp, const double* ck,
@@ -537,14 +525,15 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
-    N seed_opl[K], seed_pen[K], factor[K];
-    RayAdj<N> adj[K];
+    const A zero_a(0.0);
+    A seed_opl[K], seed_pen[K], factor[K];
+    RayAdj<A> adj[K];
 #pragma unroll
     for (int m = 0; m < K; ++m) {
-        seed_opl[m] = so[m];
-        seed_pen[m] = spn[m];
-        factor[m] = sinks.factor[m];
-        adj[m] = {{zero, zero, zero}, {zero, zero, zero}};
+        seed_opl[m] = A(so[m]);
+        seed_pen[m] = A(spn[m]);
+        factor[m] = A(sinks.factor[m]);
+        adj[m] = {{zero_a, zero_a, zero_a}, {zero_a, zero_a, zero_a}};
     }
     int next_branch = kBranchRegular;
     const Vec<N> center{zero, N(rec[lay.target + f]), N(thick[S - 1])};
@@ -594,14 +583,14 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                 const int s = first + i;
                 if (s == count - 1) {
                     if (reached_image && count == S) {
-                        Vec<N> center_adj[K];
-                        N n_image_adj[K];
+                        Vec<A> center_adj[K];
+                        A n_image_adj[K];
 #pragma unroll
                         for (int m = 0; m < K; ++m) {
-                            center_adj[m] = {zero, zero, zero};
-                            n_image_adj[m] = zero;
+                            center_adj[m] = {zero_a, zero_a, zero_a};
+                            n_image_adj[m] = zero_a;
                         }
-                        reference_step_backward_k<N, K>(sp[i], sd[i], center,
+                        reference_step_backward_k<N, A, K>(sp[i], sd[i], center,
                                                         N(idx[(S - 1) * L + l]), image_branch,
                                                         seed_opl, seed_pen, adj, center_adj,
                                                         n_image_adj);
@@ -617,10 +606,10 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                     const int j = s + 1;
                     const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
                     const N cj = sphere ? curv[j] : 0.0;
-                    StepAdj<N> par[K];
+                    StepAdj<A> par[K];
 #pragma unroll
-                    for (int m = 0; m < K; ++m) par[m] = {zero, zero, zero, zero};
-                    refracting_step_backward_k<N, K>(sp[i], sd[i], N(thick[s]), cj,
+                    for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
+                    refracting_step_backward_k<N, A, K>(sp[i], sd[i], N(thick[s]), cj,
                                                      N(idx[s * L + l]), N(idx[j * L + l]),
                                                      next_branch, seed_opl, seed_pen, adj, par);
                     const int cc = sphere ? v.col_curvature[j] : -1;
@@ -637,204 +626,14 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
     }
 }
 
-// Mixed precision: forward in the mixed scheme (FP64 positions, sag root and OPL, FP32
-// directions and refraction; checkpoints keep the FP64 position and the FP32 direction), the
-// reverse sweep entirely in FP32 on the states rounded to FP32.
+// Mixed precision: the forward trace (OPL, piston, merit, the states the sweep is linearised
+// at) in FP64, the reverse sweep in FP32 on those states (an FP32 trace of the rays themselves
+// misses the OPD bar on aberrated systems; the Jacobian tolerates single-precision rounding).
 struct MixedPrecision {};
 
-__device__ void fused_forward_mixed(const TraceParams& p, const double* rec,
-                                    const RecordLayout& lay, int f, int l, const Sample& smp,
-                                    bool soft_mode, double* ck, int stride_ck, uint64_t& br_lo,
-                                    uint64_t& br_hi, int& count, int& image_branch,
-                                    int& status_out, int& soft_first, double& opl,
-                                    double& penalty) {
-    const int S = p.S, L = p.L;
-    const double a = rec[lay.pupil];
-    const double st = rec[lay.sin_theta + f];
-    const double ct = rec[lay.cos_theta + f];
-    const double r0 = a * smp.rho;
-    RayMixed r;
-    r.px = r0 * smp.sin_phi;
-    r.py = r0 * smp.cos_phi;
-    r.pz = 0.0;
-    r.dx = 0.0f;
-    r.dy = static_cast<float>(st);
-    r.dz = static_cast<float>(ct);
-    r.opl = r.py * st;
-    SoftT<double> soft{0.0, kOk};
-    SoftT<double>* sp = soft_mode ? &soft : nullptr;
-    br_lo = br_hi = 0;
-    count = 1;
-    image_branch = kBranchRegular;
-    int status = kOk;
-    const double* curv = rec + lay.curvature;
-    const double* thick = rec + lay.thickness;
-    const double* idx = rec + lay.index;
-    double n_before = idx[l];
-    for (int s = 1; s < S; ++s) {
-        const double n_after = idx[s * L + l];
-        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
-        int branch;
-        status = step_surface_mixed(r, thick[s - 1], c, n_before, n_after, sp, branch);
-        if (status != kOk) break;
-        count = s + 1;
-        if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
-        else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
-        if (s % kFusedInterval == 0) {
-            double* q = ck + (s / kFusedInterval - 1) * stride_ck;
-            q[0] = r.px;
-            q[1 * kFusedThreads] = r.py;
-            q[2 * kFusedThreads] = r.pz;
-            q[3 * kFusedThreads] = r.dx;
-            q[4 * kFusedThreads] = r.dy;
-            q[5 * kFusedThreads] = r.dz;
-        }
-        n_before = n_after;
-    }
-    if (status == kOk && soft_mode) status = soft.first;
-    if (in_piston(status)) {
-        if (!(r.dz > 0.0f)) {
-            status = kBackward;
-        } else {
-            int branch;
-            const int rst = reference_step_mixed(r, rec[lay.target + f], thick[S - 1], n_before,
-                                                 sp, branch);
-            if (!in_piston(rst)) {
-                status = rst;
-            } else {
-                image_branch = branch;
-                if (status == kOk) status = rst;
-            }
-        }
-    }
-    status_out = status;
-    soft_first = soft.first;
-    opl = r.opl;
-    penalty = soft.penalty;
-}
-
-template <int K>
-__device__ __noinline__ void fused_backward_mixed(const TraceParams& p, const VarParams& v,
-                                                  const double* rec, const RecordLayout& lay,
-                                                  int f, int l, const Sample& smp,
-                                                  const double* ck, int stride_ck,
-                                                  uint64_t br_lo, uint64_t br_hi, int count,
-                                                  int image_branch, bool reached_image,
-                                                  bool soft_mode, const double (&so)[K],
-                                                  const double (&spn)[K],
-                                                  const RowSinks<K>& sinks) {
-    using F = float;
-    const int S = p.S, L = p.L;
-    const double* curv = rec + lay.curvature;
-    const double* thick = rec + lay.thickness;
-    const double* idx = rec + lay.index;
-    F seed_opl[K], seed_pen[K], factor[K];
-    RayAdj<F> adj[K];
-#pragma unroll
-    for (int m = 0; m < K; ++m) {
-        seed_opl[m] = static_cast<F>(so[m]);
-        seed_pen[m] = static_cast<F>(spn[m]);
-        factor[m] = static_cast<F>(sinks.factor[m]);
-        adj[m] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-    }
-    int next_branch = kBranchRegular;
-    const Vec<F> center{0.f, static_cast<F>(rec[lay.target + f]), static_cast<F>(thick[S - 1])};
-    auto branch_of = [&](int s) {
-        return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
-                      : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
-    };
-    // segment start states, loaded one segment ahead of their use (see fused_backward)
-    auto segment_start = [&](int c, RayMixed& r0s) {
-        if (c == 0) {
-            const double r0 = rec[lay.pupil] * smp.rho;
-            r0s.px = r0 * smp.sin_phi;
-            r0s.py = r0 * smp.cos_phi;
-            r0s.pz = 0.0;
-            r0s.dx = 0.0f;
-            r0s.dy = static_cast<float>(rec[lay.sin_theta + f]);
-            r0s.dz = static_cast<float>(rec[lay.cos_theta + f]);
-        } else {
-            const double* q = ck + (c - 1) * stride_ck;
-            r0s.px = q[0];
-            r0s.py = q[kFusedThreads];
-            r0s.pz = q[2 * kFusedThreads];
-            r0s.dx = static_cast<float>(q[3 * kFusedThreads]);
-            r0s.dy = static_cast<float>(q[4 * kFusedThreads]);
-            r0s.dz = static_cast<float>(q[5 * kFusedThreads]);
-        }
-    };
-    RayMixed next;
-    segment_start((count - 1) / kFusedInterval, next);
-    for (int c = (count - 1) / kFusedInterval; c >= 0; --c) {
-        const int first = c * kFusedInterval;
-        const int n = (count - first) < kFusedInterval ? (count - first) : kFusedInterval;
-        Vec<F> sp[kFusedInterval], sd[kFusedInterval];
-        RayMixed r = next;
-        if (c > 0) segment_start(c - 1, next);
-        r.opl = 0.0;
-        sp[0] = {static_cast<F>(r.px), static_cast<F>(r.py), static_cast<F>(r.pz)};
-        sd[0] = {r.dx, r.dy, r.dz};
-        SoftT<double> dummy{0.0, kOk};
-#pragma unroll
-        for (int i = 1; i < kFusedInterval; ++i) {
-            if (i < n) {
-                const int s = first + i;
-                const double cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
-                int branch;
-                step_surface_mixed(r, thick[s - 1], cs, idx[(s - 1) * L + l], idx[s * L + l],
-                                   soft_mode ? &dummy : nullptr, branch);
-                sp[i] = {static_cast<F>(r.px), static_cast<F>(r.py), static_cast<F>(r.pz)};
-                sd[i] = {r.dx, r.dy, r.dz};
-            }
-        }
-#pragma unroll
-        for (int i = kFusedInterval - 1; i >= 0; --i) {
-            if (i < n) {
-                const int s = first + i;
-                if (s == count - 1) {
-                    if (reached_image && count == S) {
-                        Vec<F> center_adj[K];
-                        F n_image_adj[K];
-#pragma unroll
-                        for (int m = 0; m < K; ++m) {
-                            center_adj[m] = {0.f, 0.f, 0.f};
-                            n_image_adj[m] = 0.f;
-                        }
-                        reference_step_backward_k<F, K>(sp[i], sd[i], center,
-                                                        static_cast<F>(idx[(S - 1) * L + l]),
-                                                        image_branch, seed_opl, seed_pen, adj,
-                                                        center_adj, n_image_adj);
-                        const int col = v.col_thickness[S - 1];
-                        if (col >= 0) {
-#pragma unroll
-                            for (int m = 0; m < K; ++m)
-                                sinks.row[m][col * sinks.ld[m]] = factor[m] * center_adj[m].z;
-                        }
-                    }
-                } else {
-                    const int j = s + 1;
-                    const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
-                    const F cj = sphere ? static_cast<F>(curv[j]) : 0.f;
-                    StepAdj<F> par[K];
-#pragma unroll
-                    for (int m = 0; m < K; ++m) par[m] = {0.f, 0.f, 0.f, 0.f};
-                    refracting_step_backward_k<F, K>(sp[i], sd[i], static_cast<F>(thick[s]), cj,
-                                                     static_cast<F>(idx[s * L + l]),
-                                                     static_cast<F>(idx[j * L + l]), next_branch,
-                                                     seed_opl, seed_pen, adj, par);
-                    const int cc = sphere ? v.col_curvature[j] : -1;
-                    const int ct = v.col_thickness[s];
-#pragma unroll
-                    for (int m = 0; m < K; ++m) {
-                        if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = factor[m] * par[m].curvature;
-                        if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = factor[m] * par[m].thickness;
-                    }
-                }
-                next_branch = branch_of(s);
-            }
-        }
-    }
-}
+// number types of the forward trace and of the reverse sweep per kernel variant
+template <class N> struct FusedTypes { using Fwd = N; using Adj = N; };
+template <> struct FusedTypes<MixedPrecision> { using Fwd = double; using Adj = float; };
 
 template <class N, int K>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
@@ -844,12 +643,10 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                              int count, int image_branch, bool reached_image,
                                              bool soft_mode, const double (&so)[K],
                                              const double (&spn)[K], const RowSinks<K>& sinks) {
-    if constexpr (std::is_same<N, MixedPrecision>::value)
-        fused_backward_mixed<K>(p, v, rec, lay, f, l, smp, ck, stride_ck, br_lo, br_hi, count,
-                                image_branch, reached_image, soft_mode, so, spn, sinks);
-    else
-        fused_backward<N, K>(p, v, rec, lay, f, l, smp, ck, stride_ck, br_lo, br_hi, count,
-                             image_branch, reached_image, soft_mode, so, spn, sinks);
+    using T = FusedTypes<N>;
+    fused_backward<typename T::Fwd, typename T::Adj, K>(p, v, rec, lay, f, l, smp, ck, stride_ck,
+                                                        br_lo, br_hi, count, image_branch,
+                                                        reached_image, soft_mode, so, spn, sinks);
 }
 
 struct FusedArgs {
@@ -874,15 +671,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
     const int stride_ck = 6 * kFusedThreads;
-    constexpr int TS = kFusedThreads + 1;              // column stride of Y (odd: no conflicts)
-    constexpr int ES = kExtraRows + 1;                 // column stride of E
+    // Column strides = 4 (mod 16) doubles: the 16 lanes of a half-warp reading a DMMA fragment
+    // (8 columns x 4 rows) then hit 16 different bank pairs; lanes that own consecutive rows
+    // of one column (the sweep's writes, the centring) stay conflict-free.
+    constexpr int TS = kFusedThreads + 4;              // column stride of Y
+    constexpr int ES = kExtraRows + 4;                 // column stride of E
     double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
     double* Y = record + ((p.stride + 1) & ~1);        // column-major [NP][TS]
-    double* Rv = Y + NP * TS;                          // residual column [TS]
-    double* E = Rv + TS;                               // column-major [NP + 1][ES]
-    double* mu_open = E + (NP + 1) * ES;               // [NP + 1]
-    double* mu_seg = mu_open + NP + 1;                 // [NP + 1]
-    double* acc = mu_seg + NP + 1;                     // [pairs][32][2] DMMA accumulators
+    double* Rv = Y + P * TS;                           // the residual column of Y
+    double* E = Y + NP * TS;                           // column-major [NP][ES]
+    double* mu_open = E + NP * ES;                     // [NP]
+    double* mu_seg = mu_open + NP;                     // [NP]
+    double* acc = mu_seg + NP;                         // [pairs][32][2] DMMA accumulators
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
@@ -890,6 +690,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
     double* ckpt = pen_slot + NP * kFusedThreads;
     copy_tables(p, sh.tab);
+    for (int i = tid; i < NP * ES; i += kFusedThreads) E[i] = 0.0;  // padding columns stay 0
     for (int e = tid; e < pairs; e += kFusedThreads) {
         int j = 0, rem = e;
         while (rem >= j + 1) {
@@ -916,7 +717,6 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         if (!stage_to_shared(record, fa.records + static_cast<int64_t>(run) * p.stride,
                              static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar, uses++))
             return;
-        double j0 = 0.0, j1 = 0.0, rr = 0.0;
         for (int base = 0; base < p.rays; base += kFusedThreads) {
             const int q = base + tid;
             double* row = Y + tid;  // this ray's row, column c at row[c * TS]
@@ -937,14 +737,10 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                if constexpr (std::is_same<N, MixedPrecision>::value)
-                    fused_forward_mixed(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck,
-                                        br_lo, br_hi, count, image_branch, status, soft_first,
-                                        opl, penalty);
-                else
-                    fused_forward<N>(p, record, lay, f, l, smp, soft_mode, my_ck, stride_ck,
-                                     br_lo, br_hi, count, image_branch, status, soft_first, opl,
-                                     penalty);
+                fused_forward<typename FusedTypes<N>::Fwd>(p, record, lay, f, l, smp, soft_mode,
+                                                           my_ck, stride_ck, br_lo, br_hi, count,
+                                                           image_branch, status, soft_first, opl,
+                                                           penalty);
                 const bool piston = in_piston(status);
                 has_pen = soft_mode && status != kOk;
                 const bool pen_sweep = has_pen && soft_first != kOk;
@@ -1005,8 +801,8 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 for (int r = start + lane; r < end; r += 32) ws += sh.w[r];
                 ws = fused_warp_sum(ws);
                 if (ws > 0.0) {
-                    for (int c = warp; c <= NP; c += kFusedWarps) {
-                        const double* col = c < NP ? Y + c * TS : Rv;
+                    for (int c = warp; c <= P; c += kFusedWarps) {
+                        const double* col = Y + c * TS;
                         double sum = 0.0;
                         for (int r = start + lane; r < end; r += 32) sum += sh.w[r] * col[r];
                         sum = fused_warp_sum(sum);
@@ -1016,13 +812,13 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 __syncthreads();
                 const bool open = sh.open_tuple == t && sh.open_w > 0.0;
                 const double scale = p.scale[t];
-                for (int e = tid; e < len * (NP + 1); e += kFusedThreads) {
+                for (int e = tid; e < len * (P + 1); e += kFusedThreads) {
                     const int c = e / len, r = start + (e - c * len);
-                    double* col = c < NP ? Y + c * TS : Rv;
+                    double* col = Y + c * TS;
                     col[r] = (ws > 0.0 && sh.w[r] > 0.0) ? scale * sh.sw[r] * (col[r] - mu_seg[c])
                                                          : 0.0;
                 }
-                if (ws > 0.0 && tid <= NP) {
+                if (ws > 0.0 && tid <= P) {
                     const double mean = mu_seg[tid];
                     if (open) {
                         const double wt = sh.open_w;
@@ -1046,7 +842,6 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 __syncthreads();
                 if (sh.extra == kExtraRows) {  // flush the extra rows
                     accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
-                    accumulate_r(E, ES, E + NP * ES, kExtraRows, NP, j0, j1, rr);
                     __syncthreads();
                     if (tid == 0) sh.extra = 0;
                     __syncthreads();
@@ -1056,14 +851,10 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             // ---- C: the centred rows and the pending extra rows ----
             const int ne = sh.extra;
             for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
-                for (int c = 0; c <= NP; ++c) E[c * ES + r] = 0.0;
+                for (int c = 0; c <= P; ++c) E[c * ES + r] = 0.0;
             __syncthreads();
             accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
-            accumulate_r(Y, TS, Rv, rows_here, NP, j0, j1, rr);
-            if (ne > 0) {
-                accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
-                accumulate_r(E, ES, E + NP * ES, ne, NP, j0, j1, rr);
-            }
+            if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
             __syncthreads();
             if (tid == 0) sh.extra = 0;
             // ---- D: penalty rows ----
@@ -1072,7 +863,6 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 Rv[tid] = pen_val;
                 __syncthreads();
                 accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
-                accumulate_r(Y, TS, Rv, rows_here, NP, j0, j1, rr);
             }
             __syncthreads();
         }
@@ -1083,23 +873,11 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             const int e = i / 64, ln = (i / 2) & 31, h = i & 1;
             const int r = sh.tiles[e].x * 8 + (ln >> 2);
             const int c = sh.tiles[e].y * 8 + 2 * (ln & 3) + h;
-            if (r < P && c < P) {
+            if (r < n && c < n) {
                 G[static_cast<int64_t>(c) * n + r] = acc[i];
                 G[static_cast<int64_t>(r) * n + c] = acc[i];
             }
         }
-        // J^T r and r^T r: partials of the four row phases reduced through Y
-        double* red = Y;  // [4][64 + 1]
-        red[warp * 65 + lane] = j0;
-        red[warp * 65 + lane + 32] = j1;
-        if (lane == 0) red[warp * 65 + 64] = rr;
-        __syncthreads();
-        if (tid < P) {
-            const double g = (red[tid] + red[65 + tid]) + (red[130 + tid] + red[195 + tid]);
-            G[static_cast<int64_t>(tid) * n + P] = g;
-            G[static_cast<int64_t>(P) * n + tid] = g;
-        }
-        if (tid == 0) G[static_cast<int64_t>(P) * n + P] = (red[64] + red[129]) + (red[194] + red[259]);
     }
 }
 
@@ -1110,9 +888,8 @@ size_t fused_adjoint_smem(const TraceParams& tp, int P) {
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
     return sizeof(double) * (static_cast<size_t>((tp.stride + 1) & ~1) +
-                             static_cast<size_t>(kFusedThreads + 1) * (NP + 1) +
-                             (kExtraRows + 1) * (NP + 1) + 2 * (NP + 1) +
-                             static_cast<size_t>(pairs) * 64);
+                             static_cast<size_t>(kFusedThreads + 4) * NP +
+                             (kExtraRows + 4) * NP + 2 * NP + static_cast<size_t>(pairs) * 64);
 }
 
 namespace {

@@ -39,18 +39,27 @@ struct StepAdj {
     N thickness, curvature, n_before, n_after;
 };
 
+// Conversion of a forward quantity (type N) to the adjoint arithmetic (type A): the identity
+// when N == A, a rounding to float when the reverse sweep runs in FP32 on FP64 states.
+template <class A, class N>
+__device__ __forceinline__ A cv(N x) { return A(value_of(x)); }
+template <class A, class N>
+__device__ __forceinline__ Vec<A> cv(Vec<N> v) { return {cv<A>(v.x), cv<A>(v.y), cv<A>(v.z)}; }
+
 // K adjoint vectors through one step (K seeds of the same ray: the OPL and the penalty). The
-// forward recompute and the seed-independent reverse quantities are shared; every adjoint
-// vector goes through the reference's statements in the reference's order, so for K = 1 (and
-// for each k) the result equals the single-seed sweep bit for bit.
-template <class N, int K>
+// step-local forward quantities are recomputed in N, the adjoint arithmetic runs in A (N for
+// the FP64 paths; float on FP64 states for the mixed path). The forward recompute and the
+// seed-independent reverse quantities are shared; every adjoint vector goes through the
+// reference's statements in the reference's order, so for N == A and K = 1 (and for each k)
+// the result equals the single-seed sweep bit for bit.
+template <class N, class A, int K>
 __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N t, N c,
                                                            N n_before, N n_after, int branch,
-                                                           const N (&seed_opl)[K],
-                                                           const N (&seed_pen)[K],
-                                                           RayAdj<N> (&adj)[K],
-                                                           StepAdj<N> (&out)[K]) {
-    const N zero(0.0), one(1.0), two(2.0);
+                                                           const A (&seed_opl)[K],
+                                                           const A (&seed_pen)[K],
+                                                           RayAdj<A> (&adj)[K],
+                                                           StepAdj<A> (&out)[K]) {
+    const N one(1.0), two(2.0);
     // forward recompute of the step's local quantities
     const N z = p.z - t;
     const N s0 = -z / d.z;
@@ -63,7 +72,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
     const N D = B * B - c * H;
     const bool missed = (branch & kBranchSoftMissed) != 0;
     const bool tir = (branch & kBranchSoftTir) != 0;
-    N root_d = zero, s;
+    N root_d(0.0), s;
     if (missed) {
         s = B / c;
     } else {
@@ -83,8 +92,8 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
     const N sin2 = one - cos_i * cos_i;
     const N k = one - mu * mu * sin2;
     // seed-independent reverse quantities
-    Vec<N> d1{zero, zero, zero};
-    N inv_tau = zero, root_k = zero, a = zero, inv = zero;
+    Vec<N> d1{N(0.0), N(0.0), N(0.0)};
+    N inv_tau(0.0), root_k(0.0), a(0.0), inv(0.0);
     if (tir) {
         const Vec<N> tau = vsub(d, vscale(cos_i, Nv));
         inv_tau = one / vnorm(tau);
@@ -94,76 +103,84 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         a = root_k - mu * cos_i;
     }
     if (!missed) inv = one / (two * root_d);
+    // the same quantities in the adjoint arithmetic
+    const A zero_a(0.0), two_a(2.0);
+    const Vec<A> ad = cv<A>(d), aNv = cv<A>(Nv), aq = cv<A>(q), ad1 = cv<A>(d1);
+    const A ac = cv<A>(c), amu = cv<A>(mu), acos = cv<A>(cos_i), asin2 = cv<A>(sin2);
+    const A ainv_tau = cv<A>(inv_tau), aroot_k = cv<A>(root_k), aa = cv<A>(a);
+    const A ainv_norm = cv<A>(inv_norm), ainv = cv<A>(inv), as = cv<A>(s), as0 = cv<A>(s0);
+    const A ann = cv<A>(n_after), anb = cv<A>(n_before), aB = cv<A>(B), aH = cv<A>(H);
+    const A arr = cv<A>(rr), ax = cv<A>(x), ay = cv<A>(y), axd = cv<A>(xd);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
-        const Vec<N> qb_out = adj[m].p;
-        const Vec<N> d1b = adj[m].d;
-        RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
-        Vec<N> nb{zero, zero, zero};
-        N cosb = zero, kb = zero, mub = zero;
+        const Vec<A> qb_out = adj[m].p;
+        const Vec<A> d1b = adj[m].d;
+        RayAdj<A> in{{zero_a, zero_a, zero_a}, {zero_a, zero_a, zero_a}};
+        Vec<A> nb{zero_a, zero_a, zero_a};
+        A cosb = zero_a, kb = zero_a, mub = zero_a;
         if (tir) {
-            const Vec<N> taub = vscale(inv_tau, vsub(d1b, vscale(vdot(d1, d1b), d1)));
+            const Vec<A> taub = vscale(ainv_tau, vsub(d1b, vscale(vdot(ad1, d1b), ad1)));
             in.d = vadd(in.d, taub);
-            cosb += -vdot(taub, Nv);
-            nb = vadd(nb, vscale(-cos_i, taub));
+            cosb += -vdot(taub, aNv);
+            nb = vadd(nb, vscale(-acos, taub));
             kb += -seed_pen[m];
         } else {
-            in.d = vadd(in.d, vscale(mu, d1b));
-            nb = vadd(nb, vscale(a, d1b));
-            const N ab = vdot(d1b, Nv);
-            mub += vdot(d1b, d);
-            kb += ab / (two * root_k);
-            mub += -ab * cos_i;
-            cosb += -ab * mu;
+            in.d = vadd(in.d, vscale(amu, d1b));
+            nb = vadd(nb, vscale(aa, d1b));
+            const A ab = vdot(d1b, aNv);
+            mub += vdot(d1b, ad);
+            kb += ab / (two_a * aroot_k);
+            mub += -ab * acos;
+            cosb += -ab * amu;
         }
-        mub += -kb * two * mu * sin2;
-        cosb += kb * two * mu * mu * cos_i;
-        in.d = vadd(in.d, vscale(cosb, Nv));
-        nb = vadd(nb, vscale(cosb, d));
-        out[m].n_before += mub / n_after;
-        out[m].n_after += -mub * mu / n_after;
-        Vec<N> nrb = nb;
-        if (missed) nrb = vscale(inv_norm, vsub(nb, vscale(vdot(Nv, nb), Nv)));
-        const Vec<N> qb = vadd(qb_out, vscale(-c, nrb));
-        N cb = -vdot(q, nrb);
-        N xb = qb.x, yb = qb.y;
-        N sb = vdot(qb, d);
-        in.d = vadd(in.d, vscale(s, qb));
-        sb += seed_opl[m] * n_before;
-        N s0b = seed_opl[m] * n_before;
-        out[m].n_before += seed_opl[m] * (s0 + s);
-        N hb = zero, bb = zero;
+        mub += -kb * two_a * amu * asin2;
+        cosb += kb * two_a * amu * amu * acos;
+        in.d = vadd(in.d, vscale(cosb, aNv));
+        nb = vadd(nb, vscale(cosb, ad));
+        out[m].n_before += mub / ann;
+        out[m].n_after += -mub * amu / ann;
+        Vec<A> nrb = nb;
+        if (missed) nrb = vscale(ainv_norm, vsub(nb, vscale(vdot(aNv, nb), aNv)));
+        const Vec<A> qb = vadd(qb_out, vscale(-ac, nrb));
+        A cb = -vdot(aq, nrb);
+        A xb = qb.x, yb = qb.y;
+        A sb = vdot(qb, ad);
+        in.d = vadd(in.d, vscale(as, qb));
+        sb += seed_opl[m] * anb;
+        A s0b = seed_opl[m] * anb;
+        out[m].n_before += seed_opl[m] * (as0 + as);
+        A hb = zero_a, bb = zero_a;
         if (missed) {
-            bb += sb / c;
-            cb += -sb * s / c;
-            const N db = -seed_pen[m];
-            bb += db * two * B;
-            cb += -db * H;
-            hb += -db * c;
+            bb += sb / ac;
+            cb += -sb * as / ac;
+            const A db = -seed_pen[m];
+            bb += db * two_a * aB;
+            cb += -db * aH;
+            hb += -db * ac;
         } else {
-            hb += sb * inv;
-            bb += -sb * s * two * inv;
-            cb += sb * s * s * inv;
+            hb += sb * ainv;
+            bb += -sb * as * two_a * ainv;
+            cb += sb * as * as * ainv;
         }
-        cb += hb * rr;
-        xb += hb * two * c * x;
-        yb += hb * two * c * y;
+        cb += hb * arr;
+        xb += hb * two_a * ac * ax;
+        yb += hb * two_a * ac * ay;
         in.d.z += bb;
-        cb += -bb * xd;
-        xb += -bb * c * d.x;
-        yb += -bb * c * d.y;
-        in.d.x += -bb * c * x;
-        in.d.y += -bb * c * y;
+        cb += -bb * axd;
+        xb += -bb * ac * ad.x;
+        yb += -bb * ac * ad.y;
+        in.d.x += -bb * ac * ax;
+        in.d.y += -bb * ac * ay;
         // transfer: s0 = (t - p_z) / d_z
         in.p.x += xb;
         in.p.y += yb;
-        s0b += xb * d.x + yb * d.y;
-        in.d.x += xb * s0;
-        in.d.y += yb * s0;
-        const N qq = s0b / d.z;
+        s0b += xb * ad.x + yb * ad.y;
+        in.d.x += xb * as0;
+        in.d.y += yb * as0;
+        const A qq = s0b / ad.z;
         out[m].thickness += qq;
         in.p.z += -qq;
-        in.d.z += -qq * s0;
+        in.d.z += -qq * as0;
         out[m].curvature += cb;
         adj[m] = in;
     }
@@ -177,20 +194,21 @@ __device__ __forceinline__ void refracting_step_backward(Vec<N> p, Vec<N> d, N t
     const N so[1] = {seed_opl}, sp[1] = {seed_pen};
     RayAdj<N> a[1] = {adj};
     StepAdj<N> o[1] = {out};
-    refracting_step_backward_k<N, 1>(p, d, t, c, n_before, n_after, branch, so, sp, a, o);
+    refracting_step_backward_k<N, N, 1>(p, d, t, c, n_before, n_after, branch, so, sp, a, o);
     adj = a[0];
     out = o[0];
 }
 
-// Step onto the reference sphere through the last vertex about M = (0, h, w), K seeds.
-template <class N, int K>
+// Step onto the reference sphere through the last vertex about M = (0, h, w), K seeds
+// (forward quantities in N, adjoint arithmetic in A, as above).
+template <class N, class A, int K>
 __device__ __forceinline__ void reference_step_backward_k(Vec<N> p, Vec<N> d, Vec<N> center,
                                                           N n_image, int branch,
-                                                          const N (&seed_opl)[K],
-                                                          const N (&seed_pen)[K],
-                                                          RayAdj<N> (&adj)[K],
-                                                          Vec<N> (&center_adj)[K],
-                                                          N (&n_image_adj)[K]) {
+                                                          const A (&seed_opl)[K],
+                                                          const A (&seed_pen)[K],
+                                                          RayAdj<A> (&adj)[K],
+                                                          Vec<A> (&center_adj)[K],
+                                                          A (&n_image_adj)[K]) {
     const N zero(0.0), one(1.0), two(2.0);
     const Vec<N> q = vsub(p, center);
     const N b = -vdot(q, d);
@@ -206,30 +224,33 @@ __device__ __forceinline__ void reference_step_backward_k(Vec<N> p, Vec<N> d, Ve
         s = g / (b + sigma * root);
     }
     const N radius_sq = missed ? vdot(center, center) : zero;
+    const A zero_a(0.0), two_a(2.0), m2_a(-2.0);
+    const Vec<A> ad = cv<A>(d), aq = cv<A>(q), ap = cv<A>(p), acenter = cv<A>(center);
+    const A as = cv<A>(s), ab = cv<A>(b), adisc = cv<A>(disc), asigma = cv<A>(sigma);
+    const A aroot = cv<A>(root), arsq = cv<A>(radius_sq), an = cv<A>(n_image);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
-        const N sb = seed_opl[m] * n_image;
-        n_image_adj[m] += seed_opl[m] * s;
-        N bb, gb;
+        const A sb = seed_opl[m] * an;
+        n_image_adj[m] += seed_opl[m] * as;
+        A bb, gb;
         if (missed) {
             bb = sb;
-            gb = zero;
-            const N discb = -seed_pen[m] / radius_sq;
-            bb += discb * two * b;
+            gb = zero_a;
+            const A discb = -seed_pen[m] / arsq;
+            bb += discb * two_a * ab;
             gb += -discb;
             center_adj[m] = vadd(center_adj[m],
-                                 vscale(seed_pen[m] * two * disc / (radius_sq * radius_sq),
-                                        center));
+                                 vscale(seed_pen[m] * two_a * adisc / (arsq * arsq), acenter));
         } else {
-            gb = sb * sigma / (two * root);
-            bb = -sb * sigma * s / root;
+            gb = sb * asigma / (two_a * aroot);
+            bb = -sb * asigma * as / aroot;
         }
-        RayAdj<N> in{{zero, zero, zero}, {zero, zero, zero}};
-        in.p = vadd(in.p, vscale(-bb, d));
-        in.d = vadd(in.d, vscale(-bb, q));
-        center_adj[m] = vadd(center_adj[m], vscale(bb, d));
-        in.p = vadd(in.p, vscale(two * gb, vsub(p, center)));
-        center_adj[m] = vadd(center_adj[m], vscale(N(-2.0) * gb, p));
+        RayAdj<A> in{{zero_a, zero_a, zero_a}, {zero_a, zero_a, zero_a}};
+        in.p = vadd(in.p, vscale(-bb, ad));
+        in.d = vadd(in.d, vscale(-bb, aq));
+        center_adj[m] = vadd(center_adj[m], vscale(bb, ad));
+        in.p = vadd(in.p, vscale(two_a * gb, vsub(ap, acenter)));
+        center_adj[m] = vadd(center_adj[m], vscale(m2_a * gb, ap));
         adj[m] = in;
     }
 }
@@ -243,7 +264,7 @@ __device__ __forceinline__ void reference_step_backward(Vec<N> p, Vec<N> d, Vec<
     RayAdj<N> a[1] = {adj};
     Vec<N> ca[1] = {center_adj};
     N na[1] = {n_image_adj};
-    reference_step_backward_k<N, 1>(p, d, center, n_image, branch, so, sp, a, ca, na);
+    reference_step_backward_k<N, N, 1>(p, d, center, n_image, branch, so, sp, a, ca, na);
     adj = a[0];
     center_adj = ca[0];
     n_image_adj = na[0];

@@ -192,6 +192,7 @@ __device__ __forceinline__ bool operator>(Exact64 a, Exact64 b) { return a.v > b
 __device__ __forceinline__ bool operator>=(Exact64 a, Exact64 b) { return a.v >= b.v; }
 __device__ __forceinline__ Exact64 nsqrt(Exact64 a) { return __dsqrt_rn(a.v); }
 __device__ __forceinline__ double nsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float nsqrt(float a) { return sqrtf(a); }
 __device__ __forceinline__ double value_of(double a) { return a; }
 __device__ __forceinline__ double value_of(Exact64 a) { return a.v; }
 
@@ -308,110 +309,6 @@ __device__ __forceinline__ int reference_step(RayT<N>& r, N h, N w, N n_image, S
     r.pz = r.pz + s * r.dz;
     r.opl += n_image * s;
     return kOk;
-}
-
-// ---- mixed precision: FP64 geometry and OPL, FP32 directions and refraction ---------------
-// Position, the transfer to the tangent plane, the cancellation-safe sag root s = H/(B + sqrt D)
-// and the OPL accumulation are FP64. The direction is stored in FP32 and the refraction
-// (normal, cos I, k, new direction) runs in FP32. Before it is used in FP64 the stored direction
-// is renormalised to first order, d64 = d (1 - e/2) with e = |d|^2 - 1 (|d64| = 1 + O(e^2),
-// e ~ 1e-7): the path the OPL accumulates is then a true polygon with unit directions, so the
-// FP32 rounding of the directions enters the OPL only at second order (Fermat), not through
-// the segment lengths.
-struct RayMixed {
-    double px, py, pz;
-    float dx, dy, dz;
-    double opl;
-};
-
-struct Dir64 {
-    double x, y, z;
-};
-
-__device__ __forceinline__ Dir64 unit64(float fx, float fy, float fz) {
-    const double x = fx, y = fy, z = fz;
-    const double e = fma(x, x, fma(y, y, fma(z, z, -1.0)));
-    const double f = 1.0 - 0.5 * e;
-    return {x * f, y * f, z * f};
-}
-
-__device__ __forceinline__ int step_surface_mixed(RayMixed& r, double t, double c, double n_before,
-                                                  double n_after, SoftT<double>* soft,
-                                                  int& branch) {
-    if (!(r.dz > 0.0f)) return kBackward;
-    const Dir64 d = unit64(r.dx, r.dy, r.dz);
-    // transfer to the tangent plane (FP64)
-    r.pz -= t;
-    const double s0 = -r.pz / d.z;
-    r.px = r.px + s0 * d.x;
-    r.py = r.py + s0 * d.y;
-    r.pz = 0.0;
-    // intersection with the sphere (FP64, Spencer-Murty form)
-    const double H = c * (r.px * r.px + r.py * r.py);
-    const double B = d.z - c * (r.px * d.x + r.py * d.y);
-    const double D = B * B - c * H;
-    double s;
-    bool missed = false;
-    if (D < 0.0) {
-        if (soft == nullptr || (!(c > 0.0) && !(c < 0.0))) return kMissed;
-        soft->add(-D, kSoftMissed);
-        s = B / c;
-        missed = true;
-    } else {
-        const double denom = B + sqrt(D);
-        if (!(denom > 0.0)) return kMissed;
-        s = H / denom;
-    }
-    r.px = r.px + s * d.x;
-    r.py = r.py + s * d.y;
-    r.pz = r.pz + s * d.z;
-    r.opl += n_before * (s0 + s);
-    // refraction (FP32)
-    const float cf = static_cast<float>(c);
-    const float mu = static_cast<float>(n_before) / static_cast<float>(n_after);
-    const float dx = static_cast<float>(d.x), dy = static_cast<float>(d.y),
-                dz = static_cast<float>(d.z);
-    float nx = -cf * static_cast<float>(r.px), ny = -cf * static_cast<float>(r.py),
-          nz = 1.0f - cf * static_cast<float>(r.pz);
-    if (missed) {
-        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-        nx *= inv;
-        ny *= inv;
-        nz *= inv;
-    }
-    const float cos_i = dx * nx + dy * ny + dz * nz;
-    const float k = 1.0f - mu * mu * (1.0f - cos_i * cos_i);
-    branch = missed ? kBranchSoftMissed : kBranchRegular;
-    if (k < 0.0f) {
-        if (soft == nullptr) return kTir;
-        soft->add(-static_cast<double>(k), kSoftTir);
-        const float tx = dx - cos_i * nx, ty = dy - cos_i * ny, tz = dz - cos_i * nz;
-        const float inv = rsqrtf(tx * tx + ty * ty + tz * tz);
-        r.dx = inv * tx;
-        r.dy = inv * ty;
-        r.dz = inv * tz;
-        branch |= kBranchSoftTir;
-        return kOk;
-    }
-    const float a = sqrtf(k) - mu * cos_i;
-    r.dx = mu * dx + a * nx;
-    r.dy = mu * dy + a * ny;
-    r.dz = mu * dz + a * nz;
-    return kOk;
-}
-
-// Reference-sphere step in FP64 with the renormalised direction.
-__device__ __forceinline__ int reference_step_mixed(RayMixed& r, double h, double w,
-                                                   double n_image, SoftT<double>* soft,
-                                                   int& branch) {
-    const Dir64 d = unit64(r.dx, r.dy, r.dz);
-    RayT<double> q{r.px, r.py, r.pz, d.x, d.y, d.z, r.opl};
-    const int st = reference_step<double>(q, h, w, n_image, soft, branch);
-    r.px = q.px;
-    r.py = q.py;
-    r.pz = q.pz;
-    r.opl = q.opl;
-    return st;
 }
 
 // ---- optimiser variables (VariableSet, reference include/mikroptim/optim/variable_set.hpp:63)

@@ -95,55 +95,6 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const R
     return status;
 }
 
-// Mixed-precision trace of one ray (FP64 geometry and OPL, FP32 directions and refraction).
-__device__ inline int trace_ray_mixed(const TraceParams& p, const double* rec,
-                                      const RecordLayout& lay, int f, int l, const Sample& smp,
-                                      bool soft_mode, double& opl, double& penalty) {
-    const int S = p.S, L = p.L;
-    const double a = rec[lay.pupil];
-    const double st = rec[lay.sin_theta + f];
-    const double ct = rec[lay.cos_theta + f];
-    const double r0 = a * smp.rho;
-    RayMixed r;
-    r.px = r0 * smp.sin_phi;
-    r.py = r0 * smp.cos_phi;
-    r.pz = 0.0;
-    r.dx = 0.0f;
-    r.dy = static_cast<float>(st);
-    r.dz = static_cast<float>(ct);
-    r.opl = r.py * st;
-    SoftT<double> soft{0.0, kOk};
-    SoftT<double>* sp = soft_mode ? &soft : nullptr;
-    int status = kOk;
-    const double* curv = rec + lay.curvature;
-    const double* thick = rec + lay.thickness;
-    const double* idx = rec + lay.index;
-    double n_before = idx[l];
-    for (int s = 1; s < S; ++s) {
-        const double n_after = idx[s * L + l];
-        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
-        int branch;
-        status = step_surface_mixed(r, thick[s - 1], c, n_before, n_after, sp, branch);
-        if (status != kOk) break;
-        n_before = n_after;
-    }
-    if (status == kOk && soft_mode) status = soft.first;
-    if (in_piston(status)) {
-        if (!(r.dz > 0.0f)) {
-            status = kBackward;
-        } else {
-            int branch;
-            const int rst = reference_step_mixed(r, rec[lay.target + f], thick[S - 1], n_before,
-                                                 sp, branch);
-            if (!in_piston(rst)) status = rst;
-            else if (status == kOk) status = rst;
-        }
-    }
-    opl = r.opl;
-    penalty = soft.penalty;
-    return status;
-}
-
 __device__ inline double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -208,9 +159,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = kPrecision == MKB_PRECISION_MIXED
-                           ? trace_ray_mixed(p, sh.record, lay, f, l, smp, soft_mode, opl, pen)
-                           : trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
+        const int st = trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
         sh.status[i] = static_cast<uint8_t>(st);
@@ -358,10 +307,9 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
                      cudaStream_t stream, RunMask mask) {
     TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask};
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+    // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
     if (precision == MKB_PRECISION_FP64)
         trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
-    else if (precision == MKB_PRECISION_MIXED)
-        trace_kernel<true, MKB_PRECISION_MIXED><<<blocks, kThreads, 0, stream>>>(p, records, out);
     else
         trace_kernel<true, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
     count_launch();
@@ -382,10 +330,9 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
                  reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask};
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+    // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
     if (precision == MKB_PRECISION_FP64)
         trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
-    else if (precision == MKB_PRECISION_MIXED)
-        trace_kernel<false, MKB_PRECISION_MIXED><<<blocks, kThreads, 0, stream>>>(p, records, out);
     else
         trace_kernel<false, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
     count_launch();
