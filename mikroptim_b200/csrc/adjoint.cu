@@ -374,11 +374,14 @@ constexpr int kFusedThreads = 128;
 constexpr int kFusedWarps = kFusedThreads / 32;
 constexpr int kExtraRows = 8;
 constexpr int kFusedMinBlocks = 3;  // CTAs per SM the register budget is sized for
-constexpr int kFusedInterval = 1;   // surfaces per checkpoint segment of the fused sweep
+// Per ray and table surface c the forward pass keeps, in the CTA's scratch slot, the state
+// entering the step c -> c + 1 and that step's StepLocal quantities (kSlotDoubles doubles).
+constexpr int kSlotDoubles = 11;
 constexpr bool kFusedDual = true;   // one two-seed sweep for rays with both rows
 constexpr int kMaxTileCols = MKB_MAX_VARIABLES / 8;                              // 8
 constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 36
 constexpr int kMaxFusedSlots = 148 * 8;  // persistent CTAs at most (SMs x resident CTAs)
+constexpr int kSegBatch = 16;            // tuple segments whose means are held at once
 
 // columns of a row: the P derivatives, the residual in column P, zero padding to 8
 __host__ __device__ inline int fused_np(int P) { return ((P + 1 + 7) / 8) * 8; }
@@ -389,9 +392,8 @@ struct FusedShared {
     double w[kFusedThreads];      // sample weight if the ray is in the piston, else 0
     double sw[kFusedThreads];     // sqrt of w
     int tuple[kFusedThreads];     // tuple of the ray (-1 past the end)
-    double open_w;                // running weight of the open tuple
-    int open_tuple;               // tuple whose running mean is kept
-    int extra;                    // extra rows pending
+    int seg_first[kFusedThreads + 1];  // first row of every tuple segment of the chunk (+ end)
+    int warp_starts[kFusedWarps];      // segments starting in each warp
     int any_pen;                  // chunk has a penalty row (soft mode)
     int run;                      // run taken off the queue
     int2 tiles[kMaxTilePairs];    // (row tile, column tile) of every upper-triangle pair
@@ -466,26 +468,35 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
     N n_before = idx[l];
+    auto keep_state = [&](double* q) {
+        q[0] = value_of(r.px);
+        q[1 * kFusedThreads] = value_of(r.py);
+        q[2 * kFusedThreads] = value_of(r.pz);
+        q[3 * kFusedThreads] = value_of(r.dx);
+        q[4 * kFusedThreads] = value_of(r.dy);
+        q[5 * kFusedThreads] = value_of(r.dz);
+    };
     for (int s = 1; s < S; ++s) {
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        double* q = ck + (s - 1) * stride_ck;  // slot s - 1: the state entering this step
+        keep_state(q);
         int branch;
-        status = step_surface<N>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch);
+        StepLocal<N> loc{zero, zero, zero, zero, zero};
+        status = step_surface<N, true>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch,
+                                       &loc);
         if (status != kOk) break;
+        q[6 * kFusedThreads] = value_of(loc.s0);
+        q[7 * kFusedThreads] = value_of(loc.s);
+        q[8 * kFusedThreads] = value_of(loc.root_d);
+        q[9 * kFusedThreads] = value_of(loc.mu);
+        q[10 * kFusedThreads] = value_of(loc.root_k);
         count = s + 1;
         if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
         else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
-        if (s % kFusedInterval == 0) {  // checkpoint s / K (slot s / K - 1; the start ray is recomputed)
-            double* q = ck + (s / kFusedInterval - 1) * stride_ck;
-            q[0] = value_of(r.px);
-            q[1 * kFusedThreads] = value_of(r.py);
-            q[2 * kFusedThreads] = value_of(r.pz);
-            q[3 * kFusedThreads] = value_of(r.dx);
-            q[4 * kFusedThreads] = value_of(r.dy);
-            q[5 * kFusedThreads] = value_of(r.dz);
-        }
         n_before = n_after;
     }
+    if (count == S) keep_state(ck + (S - 1) * stride_ck);  // the state entering the image step
     if (status == kOk && soft_mode) status = soft.first;
     if (in_piston(status)) {
         if (!(r.dz > zero)) {
@@ -541,88 +552,62 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
         return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
                       : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
     };
-    // the state that starts segment c: the start ray is recomputed (collimated_ray), the others
-    // are loaded from the checkpoint slots one segment ahead of their use
-    auto segment_start = [&](int c, Vec<N>& p0, Vec<N>& d0) {
-        if (c == 0) {
-            const N r0 = N(rec[lay.pupil]) * N(smp.rho);
-            p0 = {r0 * N(smp.sin_phi), r0 * N(smp.cos_phi), zero};
-            d0 = {zero, N(rec[lay.sin_theta + f]), N(rec[lay.cos_theta + f])};
-        } else {
-            const double* q = ck + (c - 1) * stride_ck;
-            p0 = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
-            d0 = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
-        }
+    // slot c: the state entering step c -> c + 1 and the step's local quantities, loaded one
+    // step ahead of their use so the load latency hides behind the current step
+    struct Slot {
+        Vec<N> p, d;
+        StepLocal<N> loc;
     };
-    Vec<N> next_p, next_d;
-    segment_start((count - 1) / kFusedInterval, next_p, next_d);
-    for (int c = (count - 1) / kFusedInterval; c >= 0; --c) {
-        const int first = c * kFusedInterval;
-        const int n = (count - first) < kFusedInterval ? (count - first) : kFusedInterval;
-        Vec<N> sp[kFusedInterval], sd[kFusedInterval];
-        sp[0] = next_p;
-        sd[0] = next_d;
-        if (c > 0) segment_start(c - 1, next_p, next_d);
-        RayT<N> r{sp[0].x, sp[0].y, sp[0].z, sd[0].x, sd[0].y, sd[0].z, zero};
-        SoftT<N> dummy{zero, kOk};
+    auto load = [&](int c, Slot& sl) {
+        const double* q = ck + c * stride_ck;
+        sl.p = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
+        sl.d = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
+        sl.loc = {N(q[6 * kFusedThreads]), N(q[7 * kFusedThreads]), N(q[8 * kFusedThreads]),
+                  N(q[9 * kFusedThreads]), N(q[10 * kFusedThreads])};
+    };
+    Slot next;
+    load(count - 1, next);
+    for (int c = count - 1; c >= 0; --c) {
+        const Slot cur = next;
+        if (c > 0) load(c - 1, next);
+        if (c == count - 1) {
+            if (reached_image && count == S) {
+                Vec<A> center_adj[K];
+                A n_image_adj[K];
 #pragma unroll
-        for (int i = 1; i < kFusedInterval; ++i) {
-            if (i < n) {
-                const int s = first + i;
-                const N cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
-                int branch;
-                step_surface<N>(r, N(thick[s - 1]), cs, N(idx[(s - 1) * L + l]),
-                                N(idx[s * L + l]), soft_mode ? &dummy : nullptr, branch);
-                sp[i] = {r.px, r.py, r.pz};
-                sd[i] = {r.dx, r.dy, r.dz};
-            }
-        }
-#pragma unroll
-        for (int i = kFusedInterval - 1; i >= 0; --i) {
-            if (i < n) {
-                const int s = first + i;
-                if (s == count - 1) {
-                    if (reached_image && count == S) {
-                        Vec<A> center_adj[K];
-                        A n_image_adj[K];
-#pragma unroll
-                        for (int m = 0; m < K; ++m) {
-                            center_adj[m] = {zero_a, zero_a, zero_a};
-                            n_image_adj[m] = zero_a;
-                        }
-                        reference_step_backward_k<N, A, K>(sp[i], sd[i], center,
-                                                        N(idx[(S - 1) * L + l]), image_branch,
-                                                        seed_opl, seed_pen, adj, center_adj,
-                                                        n_image_adj);
-                        const int col = v.col_thickness[S - 1];
-                        if (col >= 0) {
-#pragma unroll
-                            for (int m = 0; m < K; ++m)
-                                sinks.row[m][col * sinks.ld[m]] =
-                                    value_of(factor[m] * center_adj[m].z);
-                        }
-                    }
-                } else {
-                    const int j = s + 1;
-                    const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
-                    const N cj = sphere ? curv[j] : 0.0;
-                    StepAdj<A> par[K];
-#pragma unroll
-                    for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
-                    refracting_step_backward_k<N, A, K>(sp[i], sd[i], N(thick[s]), cj,
-                                                     N(idx[s * L + l]), N(idx[j * L + l]),
-                                                     next_branch, seed_opl, seed_pen, adj, par);
-                    const int cc = sphere ? v.col_curvature[j] : -1;
-                    const int ct = v.col_thickness[s];
-#pragma unroll
-                    for (int m = 0; m < K; ++m) {
-                        if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = value_of(factor[m] * par[m].curvature);
-                        if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = value_of(factor[m] * par[m].thickness);
-                    }
+                for (int m = 0; m < K; ++m) {
+                    center_adj[m] = {zero_a, zero_a, zero_a};
+                    n_image_adj[m] = zero_a;
                 }
-                next_branch = branch_of(s);
+                reference_step_backward_k<N, A, K>(cur.p, cur.d, center, N(idx[(S - 1) * L + l]),
+                                                   image_branch, seed_opl, seed_pen, adj,
+                                                   center_adj, n_image_adj);
+                const int col = v.col_thickness[S - 1];
+                if (col >= 0) {
+#pragma unroll
+                    for (int m = 0; m < K; ++m)
+                        sinks.row[m][col * sinks.ld[m]] = value_of(factor[m] * center_adj[m].z);
+                }
+            }
+        } else {
+            const int j = c + 1;
+            const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
+            const N cj = sphere ? curv[j] : 0.0;
+            StepAdj<A> par[K];
+#pragma unroll
+            for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
+            refracting_step_backward_k<N, A, K>(cur.p, cur.d, N(thick[c]), cj, N(idx[c * L + l]),
+                                                N(idx[j * L + l]), next_branch, seed_opl,
+                                                seed_pen, adj, par, &cur.loc);
+            const int cc = sphere ? v.col_curvature[j] : -1;
+            const int ct = v.col_thickness[c];
+#pragma unroll
+            for (int m = 0; m < K; ++m) {
+                if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = value_of(factor[m] * par[m].curvature);
+                if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = value_of(factor[m] * par[m].thickness);
             }
         }
+        next_branch = branch_of(c);
     }
 }
 
@@ -670,7 +655,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const int NP = fused_np(P);
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
-    const int stride_ck = 6 * kFusedThreads;
+    const int stride_ck = kSlotDoubles * kFusedThreads;
     // Column strides = 4 (mod 16) doubles: the 16 lanes of a half-warp reading a DMMA fragment
     // (8 columns x 4 rows) then hit 16 different bank pairs; lanes that own consecutive rows
     // of one column (the sweep's writes, the centring) stay conflict-free.
@@ -680,13 +665,14 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     double* Y = record + ((p.stride + 1) & ~1);        // column-major [NP][TS]
     double* Rv = Y + P * TS;                           // the residual column of Y
     double* E = Y + NP * TS;                           // column-major [NP][ES]
-    double* mu_open = E + NP * ES;                     // [NP]
-    double* mu_seg = mu_open + NP;                     // [NP]
-    double* acc = mu_seg + NP;                         // [pairs][32][2] DMMA accumulators
+    double* mu_open = E + NP * ES;                     // [NP] running mean of the open tuple
+    double* seg_mean = mu_open + NP;                   // [kSegBatch][NP] segment means
+    double* seg_w = seg_mean + kSegBatch * NP;         // [kSegBatch] segment weights
+    double* acc = seg_w + kSegBatch;                   // [pairs][32][2] DMMA accumulators
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
-    // this CTA's scratch slot: penalty rows [NP][T], then checkpoints 1 .. [nck - 1][6][T]
+    // this CTA's scratch slot: penalty rows [NP][T], then per surface [kSlotDoubles][T]
     double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
     double* ckpt = pen_slot + NP * kFusedThreads;
     copy_tables(p, sh.tab);
@@ -708,11 +694,9 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         const int run = sh.run;
         if (run >= p.V) break;
         if (fa.run_mask != nullptr && fa.run_mask[run] == 0) continue;
-        if (tid == 0) {
-            sh.open_tuple = -1;
-            sh.open_w = 0.0;
-            sh.extra = 0;
-        }
+        // the open tuple (kept identically by every thread): its index, weight, extra rows
+        int open_tuple = -1, extra = 0;
+        double open_w = 0.0;
         for (int i = tid; i < pairs * 64; i += kFusedThreads) acc[i] = 0.0;
         if (!stage_to_shared(record, fa.records + static_cast<int64_t>(run) * p.stride,
                              static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar, uses++))
@@ -791,72 +775,96 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             if (has_pen) sh.any_pen = 1;
             // ---- B: centre every tuple segment of the chunk ----
             const int rows_here = p.rays - base < kFusedThreads ? p.rays - base : kFusedThreads;
-            int start = 0;
-            while (start < rows_here) {
-                const int t = sh.tuple[start];
-                int end = start + 1;
-                while (end < rows_here && sh.tuple[end] == t) ++end;
-                const int len = end - start;
-                double ws = 0.0;
-                for (int r = start + lane; r < end; r += 32) ws += sh.w[r];
-                ws = fused_warp_sum(ws);
-                if (ws > 0.0) {
-                    for (int c = warp; c <= P; c += kFusedWarps) {
-                        const double* col = Y + c * TS;
-                        double sum = 0.0;
-                        for (int r = start + lane; r < end; r += 32) sum += sh.w[r] * col[r];
-                        sum = fused_warp_sum(sum);
-                        if (lane == 0) mu_seg[c] = sum / ws;
+            // B1: segments are the maximal runs of rows of one tuple; a ballot prefix gives
+            // every row its segment and every segment its first row
+            const bool starts = tid < rows_here && (tid == 0 || sh.tuple[tid] != sh.tuple[tid - 1]);
+            const unsigned ball = __ballot_sync(0xffffffffu, starts);
+            if (lane == 0) sh.warp_starts[warp] = __popc(ball);
+            __syncthreads();
+            int before = 0, nseg = 0;
+#pragma unroll
+            for (int w = 0; w < kFusedWarps; ++w) {
+                before += w < warp ? sh.warp_starts[w] : 0;
+                nseg += sh.warp_starts[w];
+            }
+            const int seg = before + __popc(ball & (0xffffffffu >> (31 - lane))) - 1;
+            if (starts) sh.seg_first[seg] = tid;
+            if (tid == 0) sh.seg_first[nseg] = rows_here;
+            __syncthreads();
+            for (int k0 = 0; k0 < nseg; k0 += kSegBatch) {
+                const int kn = nseg - k0 < kSegBatch ? nseg - k0 : kSegBatch;
+                // B2: weight and weighted column means of each segment, a warp per (segment,
+                // column) with lane-strided rows and a shuffle sum
+                for (int pr = warp; pr < kn * (P + 1); pr += kFusedWarps) {
+                    const int k = pr / (P + 1), c = pr - k * (P + 1);
+                    const int a = sh.seg_first[k0 + k], b = sh.seg_first[k0 + k + 1];
+                    const double* col = Y + c * TS;
+                    double sw_sum = 0.0, sum = 0.0;
+                    for (int r = a + lane; r < b; r += 32) {
+                        sw_sum += sh.w[r];
+                        sum += sh.w[r] * col[r];
+                    }
+                    sw_sum = fused_warp_sum(sw_sum);
+                    sum = fused_warp_sum(sum);
+                    if (lane == 0) {
+                        seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
+                        if (c == 0) seg_w[k] = sw_sum;
                     }
                 }
                 __syncthreads();
-                const bool open = sh.open_tuple == t && sh.open_w > 0.0;
-                const double scale = p.scale[t];
-                for (int e = tid; e < len * (P + 1); e += kFusedThreads) {
-                    const int c = e / len, r = start + (e - c * len);
-                    double* col = Y + c * TS;
-                    col[r] = (ws > 0.0 && sh.w[r] > 0.0) ? scale * sh.sw[r] * (col[r] - mu_seg[c])
-                                                         : 0.0;
+                // B3: every row of the batch's segments centred and scaled by its own thread
+                if (tid < rows_here && seg >= k0 && seg < k0 + kn) {
+                    const int k = seg - k0;
+                    const double f = (seg_w[k] > 0.0 && sh.w[tid] > 0.0)
+                                         ? p.scale[sh.tuple[tid]] * sh.sw[tid] : 0.0;
+                    const double* m = seg_mean + k * NP;
+                    for (int c = 0; c <= P; ++c) {
+                        double* y = Y + c * TS + tid;
+                        *y = f != 0.0 ? f * (*y - m[c]) : 0.0;
+                    }
                 }
-                if (ws > 0.0 && tid <= P) {
-                    const double mean = mu_seg[tid];
+                // B4: the segments merged into the open tuple in row order (threads = columns
+                // for the vectors; the scalar state is updated identically by every thread)
+                for (int k = 0; k < kn; ++k) {
+                    const double ws = seg_w[k];
+                    if (!(ws > 0.0)) continue;
+                    const int t = sh.tuple[sh.seg_first[k0 + k]];
+                    const bool open = open_tuple == t && open_w > 0.0;
+                    if (tid <= P) {
+                        const double mean = seg_mean[k * NP + tid];
+                        if (open) {
+                            const double fac = p.scale[t] * sqrt(open_w * ws / (open_w + ws));
+                            E[tid * ES + extra] = fac * (mean - mu_open[tid]);
+                            mu_open[tid] += (ws / (open_w + ws)) * (mean - mu_open[tid]);
+                        } else {
+                            mu_open[tid] = mean;
+                        }
+                    }
                     if (open) {
-                        const double wt = sh.open_w;
-                        const double fac = scale * sqrt(wt * ws / (wt + ws));
-                        E[tid * ES + sh.extra] = fac * (mean - mu_open[tid]);
-                        mu_open[tid] += (ws / (wt + ws)) * (mean - mu_open[tid]);
+                        extra += 1;
+                        open_w += ws;
                     } else {
-                        mu_open[tid] = mean;
+                        open_tuple = t;
+                        open_w = ws;
+                    }
+                    if (extra == kExtraRows) {  // flush the extra rows
+                        __syncthreads();
+                        accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
+                        __syncthreads();
+                        extra = 0;
                     }
                 }
                 __syncthreads();
-                if (tid == 0 && ws > 0.0) {
-                    if (open) {
-                        sh.extra += 1;
-                        sh.open_w += ws;
-                    } else {
-                        sh.open_tuple = t;
-                        sh.open_w = ws;
-                    }
-                }
-                __syncthreads();
-                if (sh.extra == kExtraRows) {  // flush the extra rows
-                    accumulate(E, ES, kExtraRows, pairs, sh.tiles, acc);
-                    __syncthreads();
-                    if (tid == 0) sh.extra = 0;
-                    __syncthreads();
-                }
-                start = end;
             }
             // ---- C: the centred rows and the pending extra rows ----
-            const int ne = sh.extra;
+            const int ne = extra;
             for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
                 for (int c = 0; c <= P; ++c) E[c * ES + r] = 0.0;
             __syncthreads();
             accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
             if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
             __syncthreads();
-            if (tid == 0) sh.extra = 0;
+            extra = 0;
             // ---- D: penalty rows ----
             if (sh.any_pen) {
                 for (int c = 0; c < NP; ++c) row[c * TS] = has_pen ? prow[c * kFusedThreads] : 0.0;
@@ -889,13 +897,13 @@ size_t fused_adjoint_smem(const TraceParams& tp, int P) {
     const int pairs = ncols * (ncols + 1) / 2;
     return sizeof(double) * (static_cast<size_t>((tp.stride + 1) & ~1) +
                              static_cast<size_t>(kFusedThreads + 4) * NP +
-                             (kExtraRows + 4) * NP + 2 * NP + static_cast<size_t>(pairs) * 64);
+                             (kExtraRows + 4) * NP + NP + kSegBatch * (NP + 1) +
+                             static_cast<size_t>(pairs) * 64);
 }
 
 namespace {
 int64_t fused_slot_doubles(int P, int S) {
-    const int checkpoints = (S - 1) / kFusedInterval;  // states after surfaces K, 2K, ...
-    return static_cast<int64_t>(fused_np(P) + 6 * checkpoints) * kFusedThreads;
+    return static_cast<int64_t>(fused_np(P) + kSlotDoubles * S) * kFusedThreads;
 }
 }  // namespace
 

@@ -52,17 +52,20 @@ __device__ __forceinline__ Vec<A> cv(Vec<N> v) { return {cv<A>(v.x), cv<A>(v.y),
 // seed-independent reverse quantities are shared; every adjoint vector goes through the
 // reference's statements in the reference's order, so for N == A and K = 1 (and for each k)
 // the result equals the single-seed sweep bit for bit.
+// `known` (optional): the step's StepLocal quantities kept by the forward pass, used instead
+// of recomputing the divisions and square roots (the values are the same).
 template <class N, class A, int K>
 __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N t, N c,
                                                            N n_before, N n_after, int branch,
                                                            const A (&seed_opl)[K],
                                                            const A (&seed_pen)[K],
                                                            RayAdj<A> (&adj)[K],
-                                                           StepAdj<A> (&out)[K]) {
+                                                           StepAdj<A> (&out)[K],
+                                                           const StepLocal<N>* known = nullptr) {
     const N one(1.0), two(2.0);
     // forward recompute of the step's local quantities
     const N z = p.z - t;
-    const N s0 = -z / d.z;
+    const N s0 = known ? known->s0 : -z / d.z;
     const N x = p.x + s0 * d.x;
     const N y = p.y + s0 * d.y;
     const N rr = x * x + y * y;
@@ -73,7 +76,10 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
     const bool missed = (branch & kBranchSoftMissed) != 0;
     const bool tir = (branch & kBranchSoftTir) != 0;
     N root_d(0.0), s;
-    if (missed) {
+    if (known) {
+        root_d = known->root_d;
+        s = known->s;
+    } else if (missed) {
         s = B / c;
     } else {
         root_d = nsqrt(D);
@@ -87,7 +93,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         inv_norm = one / vnorm(n_raw);
         Nv = vscale(inv_norm, n_raw);
     }
-    const N mu = n_before / n_after;
+    const N mu = known ? known->mu : n_before / n_after;
     const N cos_i = vdot(d, Nv);
     const N sin2 = one - cos_i * cos_i;
     const N k = one - mu * mu * sin2;
@@ -99,7 +105,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         inv_tau = one / vnorm(tau);
         d1 = vscale(inv_tau, tau);
     } else {
-        root_k = nsqrt(k);
+        root_k = known ? known->root_k : nsqrt(k);
         a = root_k - mu * cos_i;
     }
     if (!missed) inv = one / (two * root_d);

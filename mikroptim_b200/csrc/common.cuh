@@ -215,16 +215,27 @@ struct SoftT {
     }
 };
 
-// One surface step (stop/plane: c = 0). Returns the status; `branch` gets the taken
-// soft-failure continuation. With soft == nullptr the hard-failure rules apply.
+// The quantities of one surface step that its reverse sweep needs and that cost a division
+// or a square root: the transfer length s0, the intersection length s, sqrt(D), mu = n / n'
+// and sqrt(k) of the refraction.
 template <class N>
+struct StepLocal {
+    N s0, s, root_d, mu, root_k;
+};
+
+// One surface step (stop/plane: c = 0). Returns the status; `branch` gets the taken
+// soft-failure continuation. With soft == nullptr the hard-failure rules apply. kKeep also
+// returns the step's StepLocal quantities (the arithmetic is the same either way).
+template <class N, bool kKeep = false>
 __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N n_after,
-                                            SoftT<N>* soft, int& branch) {
+                                            SoftT<N>* soft, int& branch,
+                                            StepLocal<N>* keep = nullptr) {
     const N zero(0.0), one(1.0);
     if (!(r.dz > zero)) return kBackward;
     // transfer to the tangent plane
     r.pz -= t;
     const N s0 = -r.pz / r.dz;
+    if constexpr (kKeep) keep->s0 = s0;
     r.px = r.px + s0 * r.dx;
     r.py = r.py + s0 * r.dy;
     r.pz = zero;
@@ -239,17 +250,22 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
         soft->add(-D, kSoftMissed);
         s = B / c;
         missed = true;
+        if constexpr (kKeep) keep->root_d = zero;
     } else {
-        const N denom = B + nsqrt(D);
+        const N root_d = nsqrt(D);
+        const N denom = B + root_d;
         if (!(denom > zero)) return kMissed;
         s = H / denom;
+        if constexpr (kKeep) keep->root_d = root_d;
     }
+    if constexpr (kKeep) keep->s = s;
     r.px = r.px + s * r.dx;
     r.py = r.py + s * r.dy;
     r.pz = r.pz + s * r.dz;
     r.opl += n_before * (s0 + s);
     // refraction, mu = n / n'
     const N mu = n_before / n_after;
+    if constexpr (kKeep) keep->mu = mu;
     N nx = -c * r.px, ny = -c * r.py, nz = one - c * r.pz;
     if (missed) {
         const N inv = one / nsqrt(nx * nx + ny * ny + nz * nz);
@@ -263,6 +279,7 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
     if (k < zero) {
         if (soft == nullptr) return kTir;
         soft->add(-k, kSoftTir);
+        if constexpr (kKeep) keep->root_k = zero;
         const N tx = r.dx - cos_i * nx, ty = r.dy - cos_i * ny, tz = r.dz - cos_i * nz;
         const N inv = one / nsqrt(tx * tx + ty * ty + tz * tz);
         r.dx = inv * tx;
@@ -271,7 +288,9 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
         branch |= kBranchSoftTir;
         return kOk;
     }
-    const N a = nsqrt(k) - mu * cos_i;
+    const N root_k = nsqrt(k);
+    if constexpr (kKeep) keep->root_k = root_k;
+    const N a = root_k - mu * cos_i;
     r.dx = mu * r.dx + a * nx;
     r.dy = mu * r.dy + a * ny;
     r.dz = mu * r.dz + a * nz;
