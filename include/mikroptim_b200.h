@@ -119,6 +119,13 @@ typedef struct mkb_variables {
     const double* typical;            /* host [P] > 0                                    */
 } mkb_variables;
 
+/* VariableSet::apply on the device: records_out [runs][record_stride] = the run's template
+ * record (templates hold 1 variant or one per run) with the run's point x [runs][P] written
+ * into its curvature / thickness / working-distance entries. All pointers except `vars` are
+ * device pointers; records_out is 16-byte aligned. */
+int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_variables* vars,
+                               const double* x, int32_t runs, double* records_out, void* stream);
+
 /* ---- residual plan -----------------------------------------------------------------------
  * ResidualSettings + ResidualLayout (include/mikroptim/batch/batch_residuals.hpp:24,62)
  * plus the shared weights of the batch. quad_u / quad_w are the Gauss-Legendre radial nodes

@@ -161,6 +161,9 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_lm_results_device.restype = c.c_int
     lib.mkb_lm_results_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p] + \
         [c.c_void_p] * 11 + [c.c_void_p]
+    lib.mkb_apply_variables_device.restype = c.c_int
+    lib.mkb_apply_variables_device.argtypes = [PB, PV, c.c_void_p, c.c_int32, c.c_void_p,
+                                               c.c_void_p]
     lib.mkb_normal_equations_device.restype = c.c_int
     lib.mkb_normal_equations_device.argtypes = [c.c_void_p, c.c_void_p, c.c_int32, c.c_int32,
                                                 c.c_int64, c.c_void_p, c.c_int32, c.c_void_p]

@@ -349,6 +349,39 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
     return MKB_OK;
 }
 
+int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_variables* vars,
+                               const double* x, int32_t runs, double* records_out,
+                               void* stream) {
+    if (templates == nullptr || runs < 0 ||
+        (templates->variants != 1 && templates->variants != runs)) {
+        set_error("apply: templates must hold 1 variant or one per run");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (runs == 0) return MKB_OK;
+    if (x == nullptr || records_out == nullptr || templates->records == nullptr ||
+        templates->type == nullptr) {
+        set_error("apply: null pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    const int S = templates->surfaces, L = templates->wavelengths, F = templates->fields;
+    if (S < 2 || S > kMaxSurfaces || L < 1 || L > MKB_MAX_WAVELENGTHS || F < 1 || F > kMaxFields) {
+        set_error("apply: shape out of range (S=%d, L=%d, F=%d)", S, L, F);
+        return MKB_ERR_ARGUMENT;
+    }
+    const RecordLayout lay = record_layout(S, L, F);
+    if (templates->record_stride != lay.stride ||
+        (reinterpret_cast<uintptr_t>(records_out) & 15u) != 0) {
+        set_error("apply: record stride %d (expected %d) or unaligned output",
+                  templates->record_stride, lay.stride);
+        return MKB_ERR_ARGUMENT;
+    }
+    VarParams vp;
+    const int rc = make_var_params(vars, S, templates->type, &vp);
+    if (rc != MKB_OK) return rc;
+    return launch_apply(vp, lay, templates->records, templates->variants, x, records_out, runs,
+                        static_cast<cudaStream_t>(stream));
+}
+
 int64_t mkb_rays_per_variant(const mkb_residual_plan* plan) {
     if (check_plan(plan) != MKB_OK) return MKB_ERR_ARGUMENT;
     int64_t n = 0;
