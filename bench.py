@@ -51,9 +51,10 @@ FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of th
 # DRAM traffic of trace_kernel per variant from the ncu capture summarised in
 # profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
 TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
-# DRAM traffic of adjoint_gram_kernel per run, from the ncu capture summarised in
-# profiles/adjoint_gram_objective1184.md (scaled by the runs of the launch).
-FUSED_TRAFFIC_BYTES_PER_RUN = None
+# DRAM traffic (read + write) of adjoint_gram_kernel per run, from the ncu capture summarised
+# in profiles/adjoint_gram_objective1184.md (1,184 runs: 1.669 GB read, 18.593 GB written),
+# scaled by the runs of the launch.
+FUSED_TRAFFIC_BYTES_PER_RUN = (1.669274e9 + 18.593394e9) / 1184
 
 
 def parse():
