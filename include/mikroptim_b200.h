@@ -97,6 +97,11 @@ typedef struct mkb_device_batch {
     int32_t reserved;
     const double* records;            /* device [V][record_stride], 16-byte aligned     */
     const uint8_t* type;              /* host [S] (copied into the kernel parameters)   */
+    const uint8_t* variant_surfaces;  /* device [V] or NULL: table surfaces each variant
+                                         uses (2 .. S; uneven batches, one launch): its
+                                         surfaces are 0 .. n-1 of the shared table, its
+                                         working distance is thickness[n-1], the entries
+                                         past n are ignored. NULL: every variant uses S. */
 } mkb_device_batch;
 
 /* Doubles per packed variant record for a batch shape (>= 2, even). */
@@ -228,6 +233,10 @@ typedef struct mkb_lm_options {
     int32_t gram_exact;               /* 1: FMA-chain normal equations, 0: FP64 DMMA; with
                                          the adjoint, 0 selects the fused adjoint +
                                          normal-equation kernel (no J in memory) */
+    int32_t per_run_variables;        /* 0: `vars` is one variable set for all runs. 1: `vars`
+                                         points to an array of `runs` sets (uneven batches;
+                                         counts may differ), x0 / x rows are then strided by
+                                         the largest count; needs gram_exact = 0 */
 } mkb_lm_options;
 
 size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,

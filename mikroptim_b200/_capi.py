@@ -54,6 +54,7 @@ class DeviceBatch(C.Structure):
         ("fields", C.c_int32), ("record_stride", C.c_int32), ("reserved", C.c_int32),
         ("records", C.c_void_p),
         ("type", P_uint8),
+        ("variant_surfaces", C.c_void_p),
     ]
 
 
@@ -96,6 +97,7 @@ class LmOptions(C.Structure):
         ("initial_damping", C.c_double), ("max_damping", C.c_double),
         ("diag_floor", C.c_double),
         ("jacobian", C.c_int32), ("gram_exact", C.c_int32),
+        ("per_run_variables", C.c_int32),
     ]
 
 

@@ -101,6 +101,8 @@ class SystemBatchHost:
         self.pupil_radius = np.zeros(variants)
         self.field_angle = np.zeros((variants, F))
         self.field_target = np.zeros((variants, F))
+        # uneven batches: table surfaces each variant uses (2 .. S); None = all use S
+        self.variant_surfaces: np.ndarray | None = None
 
     # ---- shape --------------------------------------------------------------------------
     @property
@@ -132,6 +134,8 @@ class SystemBatchHost:
         for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
                      "field_target"):
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[sl]))
+        if self.variant_surfaces is not None:
+            out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[sl])
         return out
 
     def take(self, variants) -> "SystemBatchHost":
@@ -141,6 +145,8 @@ class SystemBatchHost:
         for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
                      "field_target"):
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
+        if self.variant_surfaces is not None:
+            out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[idx])
         return out
 
     def validate_values(self) -> None:
@@ -159,6 +165,11 @@ class SystemBatchHost:
             raise ValueError("SystemBatchHost: weights must be >= 0")
         if not self.reference_wavelength_nm > 0:
             raise ValueError("SystemBatchHost: reference wavelength must be > 0")
+        if self.variant_surfaces is not None:
+            vsf = np.asarray(self.variant_surfaces)
+            if vsf.shape != (self.variants,) or np.any(vsf < 2) or np.any(vsf > self.surfaces):
+                raise ValueError("SystemBatchHost: variant_surfaces must hold one count in "
+                                 f"[2, {self.surfaces}] per variant")
         for f, m in enumerate(self.topology.pupil_mode):
             if m == PUPIL_AXIS and np.any(self.field_angle[:, f] != 0.0):
                 raise ValueError(f"SystemBatchHost: field {f} is an axis field but a variant "

@@ -287,24 +287,34 @@ __global__ void projection_kernel(const __grid_constant__ AdjointParams ap,
 }
 
 // Writes x_i into a copy of the run's template record (VariableSet::apply): one CTA per run.
+// Uneven batches: run i uses the variables rv.table[i] and the row x + i * rv.stride, and its
+// record's surface count is copied from its template into rv.vsurf_out.
 __global__ void apply_kernel(const __grid_constant__ VarParams vp, RecordLayout lay,
                              const double* __restrict__ templates, int n_templates,
-                             const double* __restrict__ x, double* __restrict__ out, int runs) {
+                             const double* __restrict__ x, double* __restrict__ out, int runs,
+                             RunVars rv) {
     const int run = blockIdx.x;
     if (run >= runs) return;
-    const double* src = templates + static_cast<int64_t>(n_templates == 1 ? 0 : run) * lay.stride;
+    const int t = n_templates == 1 ? 0 : run;
+    const double* src = templates + static_cast<int64_t>(t) * lay.stride;
     double* dst = out + static_cast<int64_t>(run) * lay.stride;
     for (int i = threadIdx.x; i < lay.stride; i += blockDim.x) dst[i] = src[i];
     __syncthreads();
-    if (threadIdx.x == 0) apply_variables(vp, lay, x + static_cast<int64_t>(run) * vp.P, dst);
+    if (threadIdx.x == 0) {
+        const VarParams& v = rv.table != nullptr ? rv.table[run] : vp;
+        const int stride = rv.table != nullptr ? rv.stride : vp.P;
+        apply_variables(v, lay, x + static_cast<int64_t>(run) * stride, dst);
+        if (rv.vsurf_out != nullptr) rv.vsurf_out[run] = rv.tsurf != nullptr ? rv.tsurf[t] : lay.surfaces;
+    }
 }
 
 }  // namespace
 
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
-                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream) {
+                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream,
+                 RunVars rv) {
     if (runs <= 0) return MKB_OK;
-    apply_kernel<<<runs, 128, 0, stream>>>(vp, lay, templates, n_templates, x, out, runs);
+    apply_kernel<<<runs, 128, 0, stream>>>(vp, lay, templates, n_templates, x, out, runs, rv);
     count_launch();
     return cuda_status(cudaGetLastError(), "apply launch");
 }
@@ -440,11 +450,11 @@ struct RowSinks {
 
 template <class N>
 __device__ void fused_forward(const TraceParams& p, const double* rec, const RecordLayout& lay,
-                              int f, int l, const Sample& smp, bool soft_mode, double* ck,
+                              int S, int f, int l, const Sample& smp, bool soft_mode, double* ck,
                               int stride_ck, uint64_t& br_lo, uint64_t& br_hi, int& count,
                               int& image_branch, int& status_out, int& soft_first, double& opl,
                               double& penalty) {
-    const int S = p.S, L = p.L;
+    const int L = p.L;
     const N zero(0.0);
     const N a = rec[lay.pupil];
     const N st = rec[lay.sin_theta + f];
@@ -525,13 +535,13 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
 // out-of-line copy per K keeps the kernel's instruction footprint small.
 template <class N, class A, int K>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
-                                            const double* rec, const RecordLayout& lay, int f,
-                                            int l, const Sample& smp, const double* ck,
+                                            const double* rec, const RecordLayout& lay, int S,
+                                            int f, int l, const Sample& smp, const double* ck,
                                             int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                             int count, int image_branch, bool reached_image,
                                             bool soft_mode, const double (&so)[K],
                                             const double (&spn)[K], const RowSinks<K>& sinks) {
-    const int S = p.S, L = p.L;
+    const int L = p.L;
     const N zero(0.0);
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
@@ -622,14 +632,14 @@ template <> struct FusedTypes<MixedPrecision> { using Fwd = double; using Adj = 
 
 template <class N, int K>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
-                                             const double* rec, const RecordLayout& lay, int f,
-                                             int l, const Sample& smp, const double* ck,
+                                             const double* rec, const RecordLayout& lay, int S,
+                                             int f, int l, const Sample& smp, const double* ck,
                                              int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                              int count, int image_branch, bool reached_image,
                                              bool soft_mode, const double (&so)[K],
                                              const double (&spn)[K], const RowSinks<K>& sinks) {
     using T = FusedTypes<N>;
-    fused_backward<typename T::Fwd, typename T::Adj, K>(p, v, rec, lay, f, l, smp, ck, stride_ck,
+    fused_backward<typename T::Fwd, typename T::Adj, K>(p, v, rec, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
                                                         reached_image, soft_mode, so, spn, sinks);
 }
@@ -642,19 +652,20 @@ struct FusedArgs {
     int64_t slot_doubles;
     int* queue;            // run counter
     const int* run_mask;   // runs to process (null: all)
+    const int* order;      // queue position -> run (null: identity)
+    const VarParams* vt;   // per-run variables (null: ap.v for every run)
+    int p_max;             // the largest P (sizes the shared memory and the scratch slots)
+    int64_t gram_stride;   // doubles per run of `gram`
 };
 
 template <class N>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
-    const VarParams& v = fa.ap.v;
     __shared__ FusedShared sh;
     extern __shared__ __align__(16) double dyn[];
-    const int P = v.P;
-    const int NP = fused_np(P);
-    const int ncols = NP / 8;
-    const int pairs = ncols * (ncols + 1) / 2;
+    const int NPM = fused_np(fa.p_max);  // shared-memory and scratch layout: the largest P
+    const int pairs_max = (NPM / 8) * (NPM / 8 + 1) / 2;
     const int stride_ck = kSlotDoubles * kFusedThreads;
     // Column strides = 4 (mod 16) doubles: the 16 lanes of a half-warp reading a DMMA fragment
     // (8 columns x 4 rows) then hit 16 different bank pairs; lanes that own consecutive rows
@@ -662,22 +673,21 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     constexpr int TS = kFusedThreads + 4;              // column stride of Y
     constexpr int ES = kExtraRows + 4;                 // column stride of E
     double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
-    double* Y = record + ((p.stride + 1) & ~1);        // column-major [NP][TS]
-    double* Rv = Y + P * TS;                           // the residual column of Y
-    double* E = Y + NP * TS;                           // column-major [NP][ES]
-    double* mu_open = E + NP * ES;                     // [NP] running mean of the open tuple
-    double* seg_mean = mu_open + NP;                   // [kSegBatch][NP] segment means
-    double* seg_w = seg_mean + kSegBatch * NP;         // [kSegBatch] segment weights
+    double* Y = record + ((p.stride + 1) & ~1);        // column-major [NPM][TS]
+    double* E = Y + NPM * TS;                          // column-major [NPM][ES]
+    double* mu_open = E + NPM * ES;                    // [NPM] running mean of the open tuple
+    double* seg_mean = mu_open + NPM;                  // [kSegBatch][NPM] segment means
+    double* seg_w = seg_mean + kSegBatch * NPM;        // [kSegBatch] segment weights
     double* acc = seg_w + kSegBatch;                   // [pairs][32][2] DMMA accumulators
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
-    // this CTA's scratch slot: penalty rows [NP][T], then per surface [kSlotDoubles][T]
+    // this CTA's scratch slot: penalty rows [NPM][T], then per surface [kSlotDoubles][T]
     double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
-    double* ckpt = pen_slot + NP * kFusedThreads;
+    double* ckpt = pen_slot + NPM * kFusedThreads;
     copy_tables(p, sh.tab);
-    for (int i = tid; i < NP * ES; i += kFusedThreads) E[i] = 0.0;  // padding columns stay 0
-    for (int e = tid; e < pairs; e += kFusedThreads) {
+    // upper-triangle tile pairs in column order: the pairs of a smaller P are a prefix
+    for (int e = tid; e < pairs_max; e += kFusedThreads) {
         int j = 0, rem = e;
         while (rem >= j + 1) {
             rem -= j + 1;
@@ -691,9 +701,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         __syncthreads();  // the previous run's shared state is consumed
         if (tid == 0) sh.run = atomicAdd(fa.queue, 1);
         __syncthreads();
-        const int run = sh.run;
-        if (run >= p.V) break;
+        if (sh.run >= p.V) break;
+        const int run = fa.order != nullptr ? fa.order[sh.run] : sh.run;
         if (fa.run_mask != nullptr && fa.run_mask[run] == 0) continue;
+        // the run's variables, columns and surfaces
+        const VarParams& v = fa.vt != nullptr ? fa.vt[run] : fa.ap.v;
+        const int P = v.P;
+        const int NP = fused_np(P);
+        const int ncols = NP / 8;
+        const int pairs = ncols * (ncols + 1) / 2;
+        const int S = surfaces_of(p, run);
+        double* Rv = Y + P * TS;  // the residual column of Y
+        for (int i = tid; i < NPM * ES; i += kFusedThreads) E[i] = 0.0;  // padding stays 0
         // the open tuple (kept identically by every thread): its index, weight, extra rows
         int open_tuple = -1, extra = 0;
         double open_w = 0.0;
@@ -721,7 +740,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                fused_forward<typename FusedTypes<N>::Fwd>(p, record, lay, f, l, smp, soft_mode,
+                fused_forward<typename FusedTypes<N>::Fwd>(p, record, lay, S, f, l, smp, soft_mode,
                                                            my_ck, stride_ck, br_lo, br_hi, count,
                                                            image_branch, status, soft_first, opl,
                                                            penalty);
@@ -740,7 +759,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double so[2] = {piston ? 1.0 : 0.0, 0.0};
                         const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
                         const RowSinks<2> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
-                        run_backward<N, 2>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                        run_backward<N, 2>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
                                            sinks);
                     }
@@ -750,18 +769,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double sp[1] = {pen_sweep ? 1.0 : 0.0};
                         const RowSinks<1> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
                                                 {piston ? TS : kFusedThreads}};
-                        run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck,
+                        run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
                                            so, sp, sinks);
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
                     const RowSinks<1> s0{{1.0}, {row}, {TS}};
-                    run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
                     const RowSinks<1> s1{{pfac}, {prow}, {kFusedThreads}};
-                    run_backward<N, 1>(p, v, record, lay, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
                 }
             }
@@ -876,7 +895,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         }
         // ---- write the (P+1) x (P+1) symmetric gram ----
         const int n = P + 1;
-        double* G = fa.gram + static_cast<int64_t>(run) * n * n;
+        double* G = fa.gram + static_cast<int64_t>(run) * fa.gram_stride;
         for (int i = tid; i < pairs * 64; i += kFusedThreads) {
             const int e = i / 64, ln = (i / 2) & 31, h = i & 1;
             const int r = sh.tiles[e].x * 8 + (ln >> 2);
@@ -916,11 +935,13 @@ size_t fused_scratch_bytes(int runs, int P, int S) {
 
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
-                        cudaStream_t stream, const int* run_mask) {
+                        cudaStream_t stream, const int* run_mask, RunVars rv,
+                        const int* order) {
     if (tp.V <= 0) return MKB_OK;
-    if (scratch == nullptr || scratch_bytes < fused_scratch_bytes(tp.V, vp.P, tp.S)) {
+    const int p_max = rv.table != nullptr ? rv.stride : vp.P;
+    if (scratch == nullptr || scratch_bytes < fused_scratch_bytes(tp.V, p_max, tp.S)) {
         set_error("fused adjoint: scratch of %zu bytes needed",
-                  fused_scratch_bytes(tp.V, vp.P, tp.S));
+                  fused_scratch_bytes(tp.V, p_max, tp.S));
         return MKB_ERR_WORKSPACE;
     }
     FusedArgs fa;
@@ -931,9 +952,13 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.gram = gram;
     fa.queue = static_cast<int*>(scratch);
     fa.scratch = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256);
-    fa.slot_doubles = fused_slot_doubles(vp.P, tp.S);
+    fa.slot_doubles = fused_slot_doubles(p_max, tp.S);
     fa.run_mask = run_mask;
-    const size_t smem = fused_adjoint_smem(tp, vp.P);
+    fa.order = order;
+    fa.vt = rv.table;
+    fa.p_max = p_max;
+    fa.gram_stride = static_cast<int64_t>(p_max + 1) * (p_max + 1);
+    const size_t smem = fused_adjoint_smem(tp, p_max);
     auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
                   : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>
                                                      : adjoint_gram_kernel<double>;

@@ -166,6 +166,8 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     std::memset(&p, 0, sizeof(p));
     p.V = batch->variants;
     p.S = S;
+    p.vsurf = batch->variant_surfaces;
+    p.order = nullptr;
     p.L = L;
     p.F = F;
     p.stride = lay.stride;

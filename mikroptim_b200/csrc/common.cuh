@@ -30,11 +30,12 @@ __host__ __device__ inline bool in_piston(int s) { return s == kOk || is_soft(s)
 // ---- record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
 //      sin theta[F] | cos theta[F] | field_target[F] | pad to even --------------------------
 struct RecordLayout {
-    int curvature, thickness, index, pupil, sin_theta, cos_theta, target, stride;
+    int curvature, thickness, index, pupil, sin_theta, cos_theta, target, stride, surfaces;
 };
 
 __host__ __device__ inline RecordLayout record_layout(int S, int L, int F) {
     RecordLayout r;
+    r.surfaces = S;
     r.curvature = 0;
     r.thickness = S;
     r.index = 2 * S;
@@ -75,7 +76,17 @@ struct TraceParams {
     double scale[kMaxTuples];       // residual_scale per tuple
     double pscale[kMaxTuples];      // penalty_scale per tuple
     Pack packs[kMaxPacks];
+    const uint8_t* vsurf;           // device [V] table surfaces of each variant, or null (S)
+    const int* order;               // device [V] processing order of the variants, or null
 };
+
+// Table surfaces variant v traces (uneven batches share the table of the largest; the value
+// is clamped to [2, S] so that no index leaves the record).
+__device__ __forceinline__ int surfaces_of(const TraceParams& p, int v) {
+    if (p.vsurf == nullptr) return p.S;
+    const int n = p.vsurf[v];
+    return n < 2 ? 2 : (n > p.S ? p.S : n);
+}
 
 // ---- error word written by bounded waits that gave up -------------------------------------
 // One word per translation unit (no relocatable device code); each .cu file that launches

@@ -22,17 +22,21 @@ constexpr int kMaxCols = MKB_MAX_VARIABLES + 1;
 constexpr int kExactStride = kExactRows + 1;  // padded column stride (bank spread)
 constexpr int kMaxPairsPerThread = (kMaxCols * (kMaxCols + 1) / 2 + kGramThreads - 1) / kGramThreads;
 
+// Column c of run `run`: J columns are strided by `stride` per run (the largest P of an uneven
+// batch, else P); column P is the residual.
 __device__ inline const double* column(const double* J, const double* r, int64_t run, int c,
-                                       int P, int64_t R) {
-    return c < P ? J + (run * P + c) * R : r + run * R;
+                                       int P, int stride, int64_t R) {
+    return c < P ? J + (run * stride + c) * R : r + run * R;
 }
 
 __global__ void __launch_bounds__(kGramThreads)
-gram_exact_kernel(const double* __restrict__ J, const double* __restrict__ r, int P, int64_t R,
-                  double* __restrict__ gram, const int* __restrict__ run_mask) {
+gram_exact_kernel(const double* __restrict__ J, const double* __restrict__ r, int P_all,
+                  int64_t R, double* __restrict__ gram, const int* __restrict__ run_mask,
+                  const VarParams* __restrict__ vt, int stride) {
     __shared__ double tile[kMaxCols * kExactStride];
     const int64_t run = blockIdx.x;
     if (run_mask != nullptr && run_mask[run] == 0) return;
+    const int P = vt != nullptr ? vt[run].P : P_all;
     const int n = P + 1;
     const int pairs = n * (n + 1) / 2;
     // pair index -> (p, q), p <= q, row-major over the upper triangle
@@ -56,7 +60,7 @@ gram_exact_kernel(const double* __restrict__ J, const double* __restrict__ r, in
         for (int i = threadIdx.x; i < n * kExactRows; i += kGramThreads) {
             const int c = i / kExactRows;
             const int k = i - c * kExactRows;
-            tile[c * kExactStride + k] = k < rows ? column(J, r, run, c, P, R)[r0 + k] : 0.0;
+            tile[c * kExactStride + k] = k < rows ? column(J, r, run, c, P, stride, R)[r0 + k] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -70,7 +74,7 @@ gram_exact_kernel(const double* __restrict__ J, const double* __restrict__ r, in
             }
         }
     }
-    double* g = gram + run * n * n;
+    double* g = gram + run * (stride + 1) * (stride + 1);
     for (int m = 0; m < mine; ++m) {
         g[static_cast<int64_t>(qq[m]) * n + pp[m]] = acc[m];
         g[static_cast<int64_t>(pp[m]) * n + qq[m]] = acc[m];
@@ -93,14 +97,16 @@ __device__ inline void dmma_8x8x4(double& d0, double& d1, double a, double b) {
 }
 
 __global__ void __launch_bounds__(kGramThreads)
-gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int P, int64_t R,
-                 double* __restrict__ gram, const int* __restrict__ run_mask) {
+gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int P_all,
+                 int64_t R, double* __restrict__ gram, const int* __restrict__ run_mask,
+                 const VarParams* __restrict__ vt, int stride) {
     // tile[k][c] row-major with a padded row stride (columns of the 8-wide tiles are read
     // across lanes)
     constexpr int kStride = kDmmaMaxTiles * 8 + 1;
     __shared__ double tile[kDmmaRows * kStride];
     const int64_t run = blockIdx.x;
     if (run_mask != nullptr && run_mask[run] == 0) return;
+    const int P = vt != nullptr ? vt[run].P : P_all;
     const int n = P + 1;
     const int T = (n + 7) / 8;
     const int pairs = T * (T + 1) / 2;
@@ -128,7 +134,7 @@ gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int
             const int c = i / kDmmaRows;
             const int k = i - c * kDmmaRows;
             double v = 0.0;
-            if (c < n && k < rows) v = column(J, r, run, c, P, R)[r0 + k];
+            if (c < n && k < rows) v = column(J, r, run, c, P, stride, R)[r0 + k];
             tile[k * kStride + c] = v;
         }
         __syncthreads();
@@ -148,7 +154,7 @@ gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int
             }
         }
     }
-    double* g = gram + run * n * n;
+    double* g = gram + run * (stride + 1) * (stride + 1);
     for (int m = 0; m < mine; ++m) {
         const int row = ti[m] * 8 + gid;
 #pragma unroll
@@ -166,12 +172,15 @@ gram_dmma_kernel(const double* __restrict__ J, const double* __restrict__ r, int
 }  // namespace
 
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
-                bool exact, cudaStream_t stream, const int* run_mask) {
+                bool exact, cudaStream_t stream, const int* run_mask, RunVars rv) {
     if (runs <= 0) return MKB_OK;
+    const int stride = rv.table != nullptr ? rv.stride : P;
     if (exact)
-        gram_exact_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask);
+        gram_exact_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask, rv.table,
+                                                             stride);
     else
-        gram_dmma_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask);
+        gram_dmma_kernel<<<runs, kGramThreads, 0, stream>>>(J, r, P, R, gram, run_mask, rv.table,
+                                                            stride);
     count_launch();
     return cuda_status(cudaGetLastError(), "normal equations launch");
 }

@@ -29,15 +29,19 @@ struct FdPattern {
 };
 
 // fd_step + fd_pattern (central), every operation separately rounded.
+// Run i's variable k is entry i * pstride + k (pstride = P, or the largest P of an uneven batch
+// whose run i uses vt[i]).
 __global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const double* x0, int runs,
-                                  FdPattern* pattern) {
+                                  FdPattern* pattern, const VarParams* vt, int pstride) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= runs * vp.P) return;
-    const int k = id % vp.P;
+    if (id >= runs * pstride) return;
+    const int run = id / pstride, k = id - run * pstride;
+    const VarParams& v = vt != nullptr ? vt[run] : vp;
+    if (k >= v.P) return;
     const Exact64 x = x0[id];
-    const Exact64 lo = vp.lower[k], up = vp.upper[k];
+    const Exact64 lo = v.lower[k], up = v.upper[k];
     const double ax = fabs(x.v);
-    const double typ = vp.typical[k];
+    const double typ = v.typical[k];
     const Exact64 h = Exact64(6.0554544523933395e-06) * Exact64(ax < typ ? typ : ax);
     const Exact64 plus = x + h, minus = x - h;
     FdPattern out;
@@ -68,31 +72,40 @@ __global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const do
     pattern[id] = out;
 }
 
-// One CTA per FD variant j of run i (variant i*n + j): template record, x0 applied, entry k
-// replaced by x_a (j = 2k + 1) or x_b (j = 2k + 2).
+// One CTA per FD variant j of run i (variant i*n + j, n = 2 pstride + 1): template record, x0
+// applied, entry k replaced by x_a (j = 2k + 1) or x_b (j = 2k + 2). active[variant] tells the
+// trace which variants to trace (the run is wanted and j < 2 P_i + 1); vsurf[variant] is the
+// template's surface count (uneven batches).
 __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayout lay,
                                 const double* __restrict__ templates, int n_templates,
                                 const double* __restrict__ x0, const FdPattern* __restrict__ pat,
                                 int first_run, int runs, double* __restrict__ out,
-                                const int* __restrict__ run_mask) {
-    const int n = 2 * vp.P + 1;
+                                const int* __restrict__ run_mask, const VarParams* vt,
+                                int pstride, const uint8_t* tsurf, int* __restrict__ active,
+                                uint8_t* __restrict__ vsurf) {
+    const int n = 2 * pstride + 1;
     const int local = blockIdx.x / n;
     const int j = blockIdx.x - local * n;
     const int run = first_run + local;
-    if (run_mask != nullptr && run_mask[run] == 0) return;
-    const double* src = templates + static_cast<int64_t>(n_templates == 1 ? 0 : run) * lay.stride;
+    const VarParams& v = vt != nullptr ? vt[run] : vp;
+    const bool on = (run_mask == nullptr || run_mask[run] != 0) && j < 2 * v.P + 1;
+    if (threadIdx.x == 0) active[blockIdx.x] = on ? 1 : 0;
+    if (!on) return;
+    const int t = n_templates == 1 ? 0 : run;
+    if (threadIdx.x == 0 && vsurf != nullptr) vsurf[blockIdx.x] = tsurf != nullptr ? tsurf[t] : lay.surfaces;
+    const double* src = templates + static_cast<int64_t>(t) * lay.stride;
     double* dst = out + static_cast<int64_t>(blockIdx.x) * lay.stride;
     for (int i = threadIdx.x; i < lay.stride; i += blockDim.x) dst[i] = src[i];
     __syncthreads();
     if (threadIdx.x == 0) {
-        const double* x = x0 + static_cast<int64_t>(run) * vp.P;
-        apply_variables(vp, lay, x, dst);
+        const double* x = x0 + static_cast<int64_t>(run) * pstride;
+        apply_variables(v, lay, x, dst);
         if (j > 0) {
             const int k = (j - 1) / 2;
-            const FdPattern& p = pat[static_cast<int64_t>(run) * vp.P + k];
+            const FdPattern& p = pat[static_cast<int64_t>(run) * pstride + k];
             const double y = (j & 1) ? p.xa : p.xb;
-            const int s = vp.surface[k];
-            if (vp.type[k] == MKB_VAR_CURVATURE) dst[lay.curvature + s] = y;
+            const int s = v.surface[k];
+            if (v.type[k] == MKB_VAR_CURVATURE) dst[lay.curvature + s] = y;
             else dst[lay.thickness + s] = y;
         }
     }
@@ -103,7 +116,7 @@ template <bool kExact>
 __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPattern* __restrict__ pat,
                                      int P, int64_t R, int first_run, int runs,
                                      double* __restrict__ J, double* __restrict__ r0,
-                                     const int* __restrict__ run_mask) {
+                                     const int* __restrict__ run_mask, const VarParams* vt) {
     using N = typename std::conditional<kExact, Exact64, double>::type;
     const int n = 2 * P + 1;
     const int64_t total = static_cast<int64_t>(runs) * (P + 1) * R;
@@ -115,6 +128,7 @@ __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPat
         const int local = static_cast<int>(ck / (P + 1));
         const int run = first_run + local;
         if (run_mask != nullptr && run_mask[run] == 0) continue;
+        if (vt != nullptr && c < P && c >= vt[run].P) continue;  // past this run's variables
         const double* base = res + static_cast<int64_t>(local) * n * R;
         if (c == P) {
             r0[static_cast<int64_t>(run) * R + r] = base[r];
@@ -139,10 +153,15 @@ __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPat
 
 // Rays whose validity (status Ok) changes between x0 and a perturbed point of column k.
 __global__ void fd_changes_kernel(const uint8_t* __restrict__ status, int P, int64_t rays,
-                                  int first_run, int64_t* __restrict__ changes) {
+                                  int first_run, int64_t* __restrict__ changes,
+                                  const VarParams* vt) {
     const int n = 2 * P + 1;
     const int local = blockIdx.x / P;
     const int k = blockIdx.x - local * P;
+    if (vt != nullptr && k >= vt[first_run + local].P) {
+        if (threadIdx.x == 0) changes[static_cast<int64_t>(first_run + local) * P + k] = 0;
+        return;
+    }
     const uint8_t* s0 = status + static_cast<int64_t>(local) * n * rays;
     const uint8_t* sa = s0 + static_cast<int64_t>(2 * k + 1) * rays;
     const uint8_t* sb = s0 + static_cast<int64_t>(2 * k + 2) * rays;
@@ -167,14 +186,16 @@ struct FdSizes {
     size_t pattern, records, residuals, status, total_fixed, per_run;
 };
 
+// Workspace of the FD Jacobian: the step patterns of all runs, then per chunk of runs the FD
+// variants' records, residuals, statuses, trace mask and surface counts (each 256-B aligned).
 FdSizes fd_sizes(int stride, int P, int64_t R, int64_t rays, int runs) {
     FdSizes z;
     const int n = 2 * P + 1;
     z.pattern = align256(sizeof(FdPattern) * static_cast<size_t>(runs) * P);
-    z.per_run = align256(sizeof(double) * static_cast<size_t>(n) * stride) +
-                align256(sizeof(double) * static_cast<size_t>(n) * R) +
-                align256(static_cast<size_t>(n) * rays);
-    z.total_fixed = z.pattern;
+    z.per_run = sizeof(double) * static_cast<size_t>(n) * stride +
+                sizeof(double) * static_cast<size_t>(n) * R + static_cast<size_t>(n) * rays +
+                sizeof(int) * static_cast<size_t>(n) + static_cast<size_t>(n);
+    z.total_fixed = z.pattern + 5 * 256;
     return z;
 }
 
@@ -199,7 +220,7 @@ namespace mkb {
 int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                 const mkb_variables* vars, const double* x0, int runs, double* J, double* r0,
                 int64_t* status_changes, void* workspace, size_t workspace_bytes,
-                cudaStream_t stream, const int* run_mask) {
+                cudaStream_t stream, const int* run_mask, RunVars rv) {
     if (runs < 0) {
         set_error("fd jacobian: runs must be >= 0");
         return MKB_ERR_ARGUMENT;
@@ -216,15 +237,17 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
         set_error("fd jacobian: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
-    VarParams vp;
-    rc = make_var_params(vars, tp.S, templates->type, &vp);
-    if (rc != MKB_OK) return rc;
+    VarParams vp{};
+    if (rv.table == nullptr) {
+        rc = make_var_params(vars, tp.S, templates->type, &vp);
+        if (rc != MKB_OK) return rc;
+    }
     if (!x0 || !J || !r0) {
         set_error("fd jacobian: null pointer");
         return MKB_ERR_ARGUMENT;
     }
     const bool exact = plan->precision == MKB_PRECISION_FP64;
-    const int P = vp.P, n = 2 * P + 1;
+    const int P = rv.table != nullptr ? rv.stride : vp.P, n = 2 * P + 1;
     const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
     const FdSizes z = fd_sizes(tp.stride, P, R, tp.rays, runs);
     if (workspace == nullptr || workspace_bytes < z.total_fixed + z.per_run) {
@@ -242,34 +265,45 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
         chunk_base + align256(sizeof(double) * static_cast<size_t>(chunk) * n * tp.stride));
     uint8_t* status = reinterpret_cast<uint8_t*>(
         reinterpret_cast<char*>(res) + align256(sizeof(double) * static_cast<size_t>(chunk) * n * R));
+    int* active = reinterpret_cast<int*>(
+        reinterpret_cast<char*>(status) + align256(static_cast<size_t>(chunk) * n * tp.rays));
+    uint8_t* vsurf = reinterpret_cast<uint8_t*>(
+        reinterpret_cast<char*>(active) + align256(sizeof(int) * static_cast<size_t>(chunk) * n));
     const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    const bool uneven_surfaces = templates->variant_surfaces != nullptr;
 
-    fd_pattern_kernel<<<(runs * P + 127) / 128, 128, 0, stream>>>(vp, x0, runs, pattern);
+    fd_pattern_kernel<<<(runs * P + 127) / 128, 128, 0, stream>>>(vp, x0, runs, pattern,
+                                                                  rv.table, P);
     count_launch();
     rc = cuda_status(cudaGetLastError(), "fd pattern launch");
     for (int first = 0; rc == MKB_OK && first < runs; first += chunk) {
         const int cnt = std::min(chunk, runs - first);
-        fd_build_kernel<<<cnt * n, 128, 0, stream>>>(vp, lay, templates->records,
-                                                     templates->variants, x0, pattern, first,
-                                                     cnt, records, run_mask);
+        fd_build_kernel<<<cnt * n, 128, 0, stream>>>(
+            vp, lay, templates->records, templates->variants, x0, pattern, first, cnt, records,
+            run_mask, rv.table, P, templates->variant_surfaces, active,
+            uneven_surfaces ? vsurf : nullptr);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "fd build launch");
         if (rc != MKB_OK) break;
         TraceParams chunk_tp = tp;
         chunk_tp.V = cnt * n;
+        chunk_tp.vsurf = uneven_surfaces ? vsurf : nullptr;
         rc = launch_residuals(chunk_tp, records, res, R, nullptr, status, plan->precision, stream,
-                              RunMask{run_mask, n, first});
+                              RunMask{active, 1, 0});
         if (rc != MKB_OK) break;
         const int64_t total = static_cast<int64_t>(cnt) * (P + 1) * R;
         const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 64));
         if (exact)
-            fd_difference_kernel<true><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0, run_mask);
+            fd_difference_kernel<true><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt,
+                                                                   J, r0, run_mask, rv.table);
         else
-            fd_difference_kernel<false><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt, J, r0, run_mask);
+            fd_difference_kernel<false><<<blocks, 256, 0, stream>>>(res, pattern, P, R, first, cnt,
+                                                                    J, r0, run_mask, rv.table);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "fd difference launch");
         if (rc != MKB_OK || status_changes == nullptr) continue;
-        fd_changes_kernel<<<cnt * P, 256, 0, stream>>>(status, P, tp.rays, first, status_changes);
+        fd_changes_kernel<<<cnt * P, 256, 0, stream>>>(status, P, tp.rays, first, status_changes,
+                                                       rv.table);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "fd status-change launch");
     }
@@ -298,7 +332,7 @@ int mkb_fd_jacobian_device(const mkb_device_batch* templates, const mkb_residual
                            double* r0, int64_t* status_changes, void* workspace,
                            size_t workspace_bytes, void* stream_ptr) {
     return fd_jacobian(templates, plan, vars, x0, runs, J, r0, status_changes, workspace,
-                       workspace_bytes, static_cast<cudaStream_t>(stream_ptr), nullptr);
+                       workspace_bytes, static_cast<cudaStream_t>(stream_ptr), nullptr, {});
 }
 
 size_t mkb_adjoint_jacobian_workspace_bytes(const mkb_device_batch* templates, int32_t runs) {
@@ -319,6 +353,11 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
     if (runs == 0) return MKB_OK;
     int rc = check_templates(templates, runs);
     if (rc != MKB_OK) return rc;
+    if (templates->variant_surfaces != nullptr) {
+        set_error("adjoint jacobian: uneven batches run with the fused adjoint "
+                  "(mkb_adjoint_normal_equations_device) or finite differences");
+        return MKB_ERR_UNSUPPORTED;
+    }
     TraceParams tp;
     mkb_device_batch b = *templates;
     b.variants = runs;
@@ -369,6 +408,10 @@ int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
     if (runs == 0) return MKB_OK;
     int rc = check_templates(templates, runs);
     if (rc != MKB_OK) return rc;
+    if (templates->variant_surfaces != nullptr && templates->variants != runs) {
+        set_error("adjoint normal equations: uneven templates need one template per run");
+        return MKB_ERR_ARGUMENT;
+    }
     TraceParams tp;
     mkb_device_batch b = *templates;
     b.variants = runs;

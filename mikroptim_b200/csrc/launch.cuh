@@ -20,6 +20,17 @@ __device__ __forceinline__ bool run_active(const RunMask& m, int v) {
     return m.mask == nullptr || m.mask[m.offset + v / m.div] != 0;
 }
 
+// Per-run variables of an uneven batch: run i uses table[i] (device) and the row x + i * stride
+// (stride = the largest P); apply writes each run record's surface count, copied from its
+// template's (tsurf, or the table's S when null), into vsurf_out. A null table: every run uses
+// the launch's VarParams.
+struct RunVars {
+    const VarParams* table = nullptr;
+    int stride = 0;
+    const uint8_t* tsurf = nullptr;
+    uint8_t* vsurf_out = nullptr;
+};
+
 // trace.cu
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
                      int64_t stride, double* opd, uint8_t* status, int precision,
@@ -32,25 +43,27 @@ int pack_rays_default();
 
 // adjoint.cu
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,
-                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream);
+                 int n_templates, const double* x, double* out, int runs, cudaStream_t stream,
+                 RunVars rv = {});
 int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
                         const double* records, double* J, bool exact, cudaStream_t stream);
 int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
                       const uint8_t* status, double* J, bool exact, cudaStream_t stream);
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
-                        cudaStream_t stream, const int* run_mask = nullptr);
+                        cudaStream_t stream, const int* run_mask = nullptr, RunVars rv = {},
+                        const int* order = nullptr);
 size_t fused_scratch_bytes(int runs, int P, int S);
 
 // gram.cu
 int launch_gram(const double* J, const double* r, int runs, int P, int64_t R, double* gram,
-                bool exact, cudaStream_t stream, const int* run_mask = nullptr);
+                bool exact, cudaStream_t stream, const int* run_mask = nullptr, RunVars rv = {});
 
 // jacobian.cu: the FD Jacobian of mkb_fd_jacobian_device for the runs the mask selects
 int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                 const mkb_variables* vars, const double* x0, int runs, double* J, double* r0,
                 int64_t* status_changes, void* workspace, size_t workspace_bytes,
-                cudaStream_t stream, const int* run_mask);
+                cudaStream_t stream, const int* run_mask, RunVars rv);
 
 // device error words, one per translation unit
 int trace_device_error();

@@ -16,6 +16,7 @@
 #include "launch.cuh"
 
 #include <algorithm>
+#include <vector>
 #include <cmath>
 
 namespace mkb {
@@ -59,6 +60,8 @@ struct LmState {
     int* evaluate;      // this cycle's trial point is evaluated (mask of the trial MERIT)
     int* want_jacobian; // the next cycle computes this run's Jacobian (mask of the Jacobian)
     int* running;       // [1] runs still running after the last cycle
+    const VarParams* vt;  // per-run variables (uneven batches) or null: the launch's VarParams
+    int pstride;          // entries per run of x / trial / g / d (the largest P), P*P of a
 };
 
 // The next cycle's update reads new normal equations exactly for these runs.
@@ -226,18 +229,20 @@ lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st
     __shared__ int s_solved, s_status;
     const int run = blockIdx.x;
     if (run >= runs) return;
-    const int n = v.P;
+    const VarParams& vr = st.vt != nullptr ? st.vt[run] : v;
+    const int n = vr.P;
+    const int64_t ps = st.pstride;
     const int tid = threadIdx.x;
-    double* x = st.x + static_cast<int64_t>(run) * n;
-    double* trial = st.trial + static_cast<int64_t>(run) * n;
-    double* a = st.a + static_cast<int64_t>(run) * n * n;
-    double* g = st.g + static_cast<int64_t>(run) * n;
-    double* d = st.d + static_cast<int64_t>(run) * n;
+    double* x = st.x + run * ps;
+    double* trial = st.trial + run * ps;
+    double* a = st.a + run * ps * ps;
+    double* g = st.g + run * ps;
+    double* d = st.d + run * ps;
     int status = st.status[run];
     const double merit = st.merit[run];
     // ---- new normal equations ----
     if (status == kRunning && st.need_jacobian[run] && st.iterations[run] < o.max_iterations) {
-        const double* G = gram + static_cast<int64_t>(run) * (n + 1) * (n + 1);
+        const double* G = gram + run * (ps + 1) * (ps + 1);
         __shared__ int s_finite;
         if (tid == 0) s_finite = 1;
         __syncthreads();
@@ -264,18 +269,18 @@ lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st
             if (tid == 0) {
                 double smax = 0.0;
                 for (int k = 0; k < n; ++k) {
-                    const Exact64 sk = scale_of(x[k], v.typical[k]);
+                    const Exact64 sk = scale_of(x[k], vr.typical[k]);
                     smax = dmax(smax, (Exact64(a[k * n + k]) * sk * sk).v);
                 }
                 double gmax = 0.0;
                 for (int k = 0; k < n; ++k) {
-                    const Exact64 sk = scale_of(x[k], v.typical[k]);
+                    const Exact64 sk = scale_of(x[k], vr.typical[k]);
                     const double akk = a[k * n + k];
                     const double floor = smax > 0.0
                                              ? (Exact64(o.diag_floor) * Exact64(smax) / (sk * sk)).v
                                              : (Exact64(1.0) / (sk * sk)).v;
                     d[k] = dmax(akk, floor);
-                    if (!bound_blocks(v, k, x[k], -g[k])) {
+                    if (!bound_blocks(vr, k, x[k], -g[k])) {
                         const double denom = nsqrt(Exact64(akk) * Exact64(merit)).v;
                         if (denom > 0.0) gmax = dmax(gmax, (Exact64(fabs(g[k])) / Exact64(denom)).v);
                     }
@@ -285,7 +290,7 @@ lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st
             __syncthreads();
             int solved;
             double norm, pred;
-            solve_step(v, a, g, d, x, kModelDamping, trial, sh, solved, norm, pred);
+            solve_step(vr, a, g, d, x, kModelDamping, trial, sh, solved, norm, pred);
             if (tid == 0) {
                 st.model_decrease[run] = solved ? (Exact64(pred) / Exact64(merit)).v : nan("");
                 if (st.gradient_norm[run] <= o.gtol) status = kConvergedGradient;
@@ -307,7 +312,7 @@ lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st
             in_cycle = 1;
             int solved;
             double norm, pred;
-            solve_step(v, a, g, d, x, st.mu[run], trial, sh, solved, norm, pred);
+            solve_step(vr, a, g, d, x, st.mu[run], trial, sh, solved, norm, pred);
             if (tid == 0) {
                 s_solved = solved;
                 s_norm = norm;
@@ -344,6 +349,8 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
     }
     st.iterations[run] += 1;
     bool accept = false;
+    const int n = st.vt != nullptr ? st.vt[run].P : P;
+    const int64_t ps = st.pstride;
     if (st.solved[run]) {
         const double f_new = trial_merit[run];
         const double merit = st.merit[run];
@@ -352,8 +359,7 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
         accept = isfinite(f_new) && pred > 0.0 && f_new < merit &&
                  !(o.reject_new_failures && trial_hard[run] > st.hard[run]);
         if (accept) {
-            for (int k = 0; k < P; ++k)
-                st.x[static_cast<int64_t>(run) * P + k] = st.trial[static_cast<int64_t>(run) * P + k];
+            for (int k = 0; k < n; ++k) st.x[run * ps + k] = st.trial[run * ps + k];
             st.merit[run] = f_new;
             st.failed[run] = trial_failed[run];
             st.hard[run] = trial_hard[run];
@@ -383,10 +389,11 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
 __global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* x0, int runs) {
     const int run = blockIdx.x * blockDim.x + threadIdx.x;
     if (run >= runs) return;
-    for (int k = 0; k < P; ++k) {
-        const double xv = x0[static_cast<int64_t>(run) * P + k];
-        st.x[static_cast<int64_t>(run) * P + k] = xv;
-        st.trial[static_cast<int64_t>(run) * P + k] = xv;
+    const int64_t ps = st.pstride;  // x0 rows have the same stride (P, or the largest P)
+    for (int k = 0; k < ps; ++k) {
+        const double xv = x0[run * ps + k];
+        st.x[run * ps + k] = xv;
+        st.trial[run * ps + k] = xv;
     }
     const double m = st.merit[run];
     int status = kRunning;
@@ -460,13 +467,26 @@ struct LmLayout {
     size_t fd_ws_bytes;
     void* fused_ws;
     size_t fused_ws_bytes;
+    VarParams* vt;      // per-run variables (uneven batches), else null
+    uint8_t* vsurf;     // surface count of each run's record (uneven surfaces), else null
+    int* order;         // runs sorted by surface count, largest first (uneven surfaces)
 };
 
 constexpr int kFdChunkRuns = 64;
 
+struct LmSetup {
+    TraceParams tp;
+    VarParams vp;       // the variables (uniform) or those of run 0 (per run)
+    LmOptionsDev o;
+    bool fd, exact, gram_exact, fused;
+    bool per_run;       // per-run variables
+    int pmax;           // P, or the largest P of the runs
+    int precision;
+    int64_t R;
+};
+
 // Carves the workspace (base may be null to only size it).
-LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_it, bool fd,
-                   bool fused, const mkb_device_batch* templates,
+LmLayout lm_layout(char* base, const LmSetup& s, int runs, const mkb_device_batch* templates,
                    const mkb_residual_plan* plan) {
     LmLayout L{};
     size_t off = 0;
@@ -475,8 +495,11 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
         off += al(bytes);
         return p;
     };
+    const TraceParams& tp = s.tp;
+    const size_t P = static_cast<size_t>(s.pmax);
+    const int max_it = s.o.max_iterations;
     const size_t r = static_cast<size_t>(runs);
-    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const int64_t R = s.R;
     L.st.x = reinterpret_cast<double*>(take(8 * r * P));
     L.st.trial = reinterpret_cast<double*>(take(8 * r * P));
     L.st.a = reinterpret_cast<double*>(take(8 * r * P * P));
@@ -504,8 +527,14 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     L.st.evaluate = reinterpret_cast<int*>(take(4 * r));
     L.st.want_jacobian = reinterpret_cast<int*>(take(4 * r));
     L.st.running = reinterpret_cast<int*>(take(4));
+    L.vt = s.per_run ? reinterpret_cast<VarParams*>(take(sizeof(VarParams) * r)) : nullptr;
+    L.st.vt = L.vt;
+    L.st.pstride = s.pmax;
+    const bool uneven = templates->variant_surfaces != nullptr;
+    L.vsurf = uneven ? reinterpret_cast<uint8_t*>(take(r)) : nullptr;
+    L.order = uneven ? reinterpret_cast<int*>(take(4 * r)) : nullptr;
     L.gram = reinterpret_cast<double*>(take(8 * r * (P + 1) * (P + 1)));
-    const size_t jr = fused ? 0 : r;  // the fused adjoint keeps J out of memory
+    const size_t jr = s.fused ? 0 : r;  // the fused adjoint keeps J out of memory
     L.J = reinterpret_cast<double*>(take(8 * jr * P * R));
     L.r0 = reinterpret_cast<double*>(take(8 * jr * R));
     L.status = reinterpret_cast<uint8_t*>(take(jr * tp.rays));
@@ -515,12 +544,12 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     L.trial_merit = reinterpret_cast<double*>(take(8 * r));
     L.trial_failed = reinterpret_cast<int64_t*>(take(8 * r));
     L.trial_hard = reinterpret_cast<int64_t*>(take(8 * r));
-    L.fused_ws_bytes = fused ? fused_scratch_bytes(runs, P, tp.S) : 0;
+    L.fused_ws_bytes = s.fused ? fused_scratch_bytes(runs, s.pmax, tp.S) : 0;
     L.fused_ws = take(L.fused_ws_bytes);
     L.fd_ws_bytes = 0;
-    if (fd) {
+    if (s.fd) {
         mkb_device_batch t = *templates;
-        L.fd_ws_bytes = mkb_fd_jacobian_workspace_bytes(&t, plan, P, runs,
+        L.fd_ws_bytes = mkb_fd_jacobian_workspace_bytes(&t, plan, s.pmax, runs,
                                                         runs < kFdChunkRuns ? runs : kFdChunkRuns);
         L.fd_ws = take(L.fd_ws_bytes);
     }
@@ -528,19 +557,12 @@ LmLayout lm_layout(char* base, const TraceParams& tp, int P, int runs, int max_i
     return L;
 }
 
-struct LmSetup {
-    TraceParams tp;
-    VarParams vp;
-    LmOptionsDev o;
-    bool fd, exact, gram_exact, fused;
-    int precision;
-    int64_t R;
-};
-
+// table != null (start): every run's variables are validated and built into it.
 int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
-             const mkb_variables* vars, const mkb_lm_options* options, int runs, LmSetup& s) {
-    if (templates == nullptr || options == nullptr || runs < 1) {
-        set_error("lm: null templates/options or runs < 1");
+             const mkb_variables* vars, const mkb_lm_options* options, int runs, LmSetup& s,
+             std::vector<VarParams>* table = nullptr) {
+    if (templates == nullptr || options == nullptr || runs < 1 || vars == nullptr) {
+        set_error("lm: null templates/options/variables or runs < 1");
         return MKB_ERR_ARGUMENT;
     }
     if (templates->variants != 1 && templates->variants != runs) {
@@ -556,9 +578,25 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
         set_error("lm: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
-    rc = make_var_params(vars, s.tp.S, templates->type, &s.vp);
-    if (rc != MKB_OK) return rc;
     const mkb_lm_options& o = *options;
+    s.per_run = o.per_run_variables != 0;
+    rc = make_var_params(&vars[0], s.tp.S, templates->type, &s.vp);
+    if (rc != MKB_OK) return rc;
+    s.pmax = s.vp.P;
+    if (s.per_run) {
+        if (table != nullptr) table->resize(static_cast<size_t>(runs));
+        for (int r = 0; r < runs; ++r) {
+            if (vars[r].count > s.pmax) s.pmax = vars[r].count;
+            if (table != nullptr) {
+                rc = make_var_params(&vars[r], s.tp.S, templates->type, &(*table)[r]);
+                if (rc != MKB_OK) return rc;
+            }
+        }
+        if (s.pmax > MKB_MAX_VARIABLES) {
+            set_error("lm: a run has more than %d variables", MKB_MAX_VARIABLES);
+            return MKB_ERR_ARGUMENT;
+        }
+    }
     auto ok = [](double v) { return std::isfinite(v) && v >= 0.0; };
     if (o.max_iterations < 0 || !ok(o.ftol) || !ok(o.xtol) || !ok(o.gtol) || !ok(o.diag_floor) ||
         !(o.initial_damping > 0.0) || !std::isfinite(o.initial_damping) ||
@@ -582,8 +620,30 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                   "gram_exact = 0)");
         return MKB_ERR_UNSUPPORTED;
     }
+    if (!s.fd && !s.fused && (s.per_run || templates->variant_surfaces != nullptr)) {
+        set_error("lm: uneven batches run with the fused adjoint (gram_exact = 0) or FD");
+        return MKB_ERR_UNSUPPORTED;
+    }
     s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
     return MKB_OK;
+}
+
+// The LM's own records are one per run: their surface counts and processing order are the
+// workspace's.
+TraceParams run_params(const LmSetup& s, const LmLayout& L) {
+    TraceParams tp = s.tp;
+    tp.vsurf = L.vsurf;
+    tp.order = L.order;
+    return tp;
+}
+
+RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates) {
+    RunVars rv;
+    rv.table = L.vt;
+    rv.stride = s.pmax;
+    rv.tsurf = templates->variant_surfaces;
+    rv.vsurf_out = L.vsurf;
+    return rv;
 }
 
 // merit at the run points `x` (applied to the templates) into merit/failed/hard
@@ -592,10 +652,35 @@ int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* tem
                 cudaStream_t stream, const int* run_mask = nullptr) {
     const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
     int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
-                          stream);
+                          stream, run_vars(s, L, templates));
     if (rc != MKB_OK) return rc;
-    return launch_merit(s.tp, L.records, merit, failed, hard, L.merit_ws, L.merit_ws_bytes,
-                        s.precision, stream, RunMask{run_mask, 1, 0});
+    return launch_merit(run_params(s, L), L.records, merit, failed, hard, L.merit_ws,
+                        L.merit_ws_bytes, s.precision, stream, RunMask{run_mask, 1, 0});
+}
+
+// Runs sorted by surface count, largest first (counting sort in one CTA; the order inside a
+// count is not fixed, and only the scheduling depends on it).
+__global__ void order_kernel(const uint8_t* __restrict__ vsurf, int runs, int S,
+                             int* __restrict__ order) {
+    __shared__ int start[MKB_MAX_SURFACES + 1];
+    for (int i = threadIdx.x; i <= MKB_MAX_SURFACES; i += blockDim.x) start[i] = 0;
+    __syncthreads();
+    auto key = [&](int r) {
+        const int n = vsurf[r];
+        return n < 2 ? 2 : (n > S ? S : n);
+    };
+    for (int r = threadIdx.x; r < runs; r += blockDim.x) atomicAdd(&start[key(r)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int at = 0;
+        for (int n = MKB_MAX_SURFACES; n >= 0; --n) {
+            const int c = start[n];
+            start[n] = at;
+            at += c;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < runs; r += blockDim.x) order[atomicAdd(&start[key(r)], 1)] = r;
 }
 
 }  // namespace
@@ -610,7 +695,7 @@ size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_resid
                               int32_t runs) {
     LmSetup s;
     if (lm_setup(templates, plan, vars, options, runs, s) != MKB_OK) return 0;
-    return lm_layout(nullptr, s.tp, s.vp.P, runs, s.o.max_iterations, s.fd, s.fused, templates, plan).total;
+    return lm_layout(nullptr, s, runs, templates, plan).total;
 }
 
 int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
@@ -619,19 +704,35 @@ int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_pl
                         void* stream_ptr) {
     const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     LmSetup s;
-    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    std::vector<VarParams> table;
+    int rc = lm_setup(templates, plan, vars, options, runs, s, &table);
     if (rc != MKB_OK) return rc;
-    const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
-                                 s.o.max_iterations, s.fd, s.fused, templates, plan);
+    const LmLayout L = lm_layout(static_cast<char*>(workspace), s, runs, templates, plan);
     if (workspace == nullptr || workspace_bytes < L.total || x0 == nullptr) {
         set_error("lm: workspace of %zu bytes and x0 needed", L.total);
         return MKB_ERR_WORKSPACE;
+    }
+    if (L.vt != nullptr) {  // pageable source: the copy has consumed it when the call returns
+        rc = cuda_status(cudaMemcpyAsync(L.vt, table.data(), sizeof(VarParams) * table.size(),
+                                         cudaMemcpyHostToDevice, stream),
+                         "lm: upload variables");
+        if (rc != MKB_OK) return rc;
+    }
+    if (L.order != nullptr) {  // surface counts of the runs' records, then their order
+        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        rc = launch_apply(s.vp, lay, templates->records, templates->variants, x0, L.records, runs,
+                          stream, run_vars(s, L, templates));
+        if (rc != MKB_OK) return rc;
+        order_kernel<<<1, 1024, 0, stream>>>(L.vsurf, runs, s.tp.S, L.order);
+        count_launch();
+        rc = cuda_status(cudaGetLastError(), "lm order launch");
+        if (rc != MKB_OK) return rc;
     }
     rc = lm_merit_at(s, L, templates, x0, runs, L.st.merit, L.st.failed, L.st.hard, stream);
     if (rc != MKB_OK) return rc;
     rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
     if (rc != MKB_OK) return rc;
-    return launch_lm_init(s.o, L.st, s.vp.P, x0, runs, stream);
+    return launch_lm_init(s.o, L.st, s.pmax, x0, runs, stream);
 }
 
 int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
@@ -641,24 +742,25 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     LmSetup s;
     int rc = lm_setup(templates, plan, vars, options, runs, s);
     if (rc != MKB_OK) return rc;
-    const LmLayout L = lm_layout(static_cast<char*>(workspace), s.tp, s.vp.P, runs,
-                                 s.o.max_iterations, s.fd, s.fused, templates, plan);
+    const LmLayout L = lm_layout(static_cast<char*>(workspace), s, runs, templates, plan);
     if (workspace == nullptr || workspace_bytes < L.total) {
         set_error("lm: workspace of %zu bytes needed", L.total);
         return MKB_ERR_WORKSPACE;
     }
+    const TraceParams tp = run_params(s, L);
+    const RunVars rv = run_vars(s, L, templates);
     // 1. Jacobian and normal equations at x for the runs whose update will read them
     const int* want = L.st.want_jacobian;
     if (s.fd) {
         rc = fd_jacobian(templates, plan, vars, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
-                         L.fd_ws_bytes, stream, want);
+                         L.fd_ws_bytes, stream, want, rv);
     } else if (s.fused) {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
-                          runs, stream);
+                          runs, stream, rv);
         if (rc == MKB_OK)
-            rc = launch_adjoint_gram(s.tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
-                                     s.precision, stream, want);
+            rc = launch_adjoint_gram(tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
+                                     s.precision, stream, want, rv, L.order);
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
@@ -676,7 +778,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     }
     if (rc != MKB_OK) return rc;
     if (!s.fused) {
-        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream, want);
+        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream, want, rv);
         if (rc != MKB_OK) return rc;
     }
     // 2. step
@@ -702,15 +804,15 @@ int mkb_lm_results_device(const mkb_device_batch* templates, const mkb_residual_
     LmSetup s;
     int rc = lm_setup(templates, plan, vars, options, runs, s);
     if (rc != MKB_OK) return rc;
-    const LmLayout L = lm_layout(static_cast<char*>(const_cast<void*>(workspace)), s.tp, s.vp.P,
-                                 runs, s.o.max_iterations, s.fd, s.fused, templates, plan);
+    const LmLayout L = lm_layout(static_cast<char*>(const_cast<void*>(workspace)), s, runs,
+                                 templates, plan);
     const size_t r = static_cast<size_t>(runs);
     struct Copy {
         void* dst;
         const void* src;
         size_t bytes;
     } copies[] = {
-        {x, L.st.x, 8 * r * s.vp.P},
+        {x, L.st.x, 8 * r * s.pmax},
         {merit, L.st.merit, 8 * r},
         {status, L.st.status, 4 * r},
         {iterations, L.st.iterations, 4 * r},

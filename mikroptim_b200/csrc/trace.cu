@@ -47,9 +47,9 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
 template <class N>
 __device__ inline int trace_ray(const TraceParams& p, const double* rec, const RecordLayout& lay,
-                                int f, int l, const Sample& smp, bool soft_mode, double& opl,
-                                double& penalty) {
-    const int S = p.S, L = p.L;
+                                int S, int f, int l, const Sample& smp, bool soft_mode,
+                                double& opl, double& penalty) {
+    const int L = p.L;
     const N zero(0.0);
     const N a = rec[lay.pupil];
     const N st = rec[lay.sin_theta + f];
@@ -129,9 +129,11 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
     using N = typename std::conditional<kExact, Exact64, double>::type;
     __shared__ SharedTrace sh;
-    const int v = blockIdx.x / p.n_packs;
+    const int slot = blockIdx.x / p.n_packs;
+    const int v = p.order != nullptr ? p.order[slot] : slot;
     if (!run_active(out.mask, v)) return;
-    const int pk = blockIdx.x - v * p.n_packs;
+    const int pk = blockIdx.x - slot * p.n_packs;
+    const int S = surfaces_of(p, v);
     const Pack pack = p.packs[pk];
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
     const double* src = records + static_cast<int64_t>(v) * p.stride;
@@ -159,7 +161,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N>(p, sh.record, lay, f, l, smp, soft_mode, opl, pen);
+        const int st = trace_ray<N>(p, sh.record, lay, S, f, l, smp, soft_mode, opl, pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
         sh.status[i] = static_cast<uint8_t>(st);

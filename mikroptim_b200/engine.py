@@ -60,6 +60,10 @@ class DeviceSystemBatch:
             with torch.cuda.stream(stream) if stream is not None else _nullcontext():
                 self.records[:batch.variants].copy_(self.host_records, non_blocking=True)
         self.type = np.ascontiguousarray(batch.type, dtype=np.uint8)
+        self.variant_surfaces = None
+        if batch.variant_surfaces is not None:
+            self.variant_surfaces = torch.from_numpy(
+                np.ascontiguousarray(batch.variant_surfaces, dtype=np.uint8)).to(self.device)
 
     def c_struct(self, first: int = 0, count: int | None = None) -> _capi.DeviceBatch:
         count = self.variants - first if count is None else count
@@ -72,6 +76,8 @@ class DeviceSystemBatch:
         b.records = C.c_void_p(self.records.data_ptr() + first * self.stride * 8)
         b.type = _capi.ptr(self.type, C.c_uint8)
         b._keep = self.type
+        b.variant_surfaces = (C.c_void_p(self.variant_surfaces.data_ptr() + first)
+                              if self.variant_surfaces is not None else None)
         return b
 
 
@@ -273,12 +279,26 @@ class LmOptions:
         o.diag_floor = self.diag_floor
         o.jacobian = self.jacobian
         o.gram_exact = int(self.gram_exact)
+        o.per_run_variables = 0
         return o
+
+
+def pad_rows(x, runs: int, width: int) -> np.ndarray:
+    """[runs][width] float64 rows: a 2-D array as it is, or a list of rows padded with zeros."""
+    if isinstance(x, (list, tuple)):
+        out = np.zeros((runs, width))
+        for i, row in enumerate(x):
+            out[i, :len(row)] = row
+        return out
+    return np.asarray(x, dtype=np.float64).reshape(runs, width)
 
 
 class DeviceLm:
     """Batched LM state on the device: start(x0), cycle(), results(). One object per problem;
-    the workspace is allocated once and reused by every cycle."""
+    the workspace is allocated once and reused by every cycle.
+
+    `variables` is one VariableSet for all runs, or a list of one VariableSet per run (uneven
+    batches: the counts may differ; x0 / x rows are then padded to the largest count)."""
 
     def __init__(self, templates: DeviceSystemBatch, layout: ResidualLayout,
                  host: SystemBatchHost, variables, options: LmOptions, runs: int,
@@ -289,8 +309,19 @@ class DeviceLm:
         self.stream = stream
         self._b = templates.c_struct()
         self._plan = layout.plan(host)
-        self._vars = variables.c_struct()
         self._opt = options.c_struct()
+        if isinstance(variables, (list, tuple)):
+            if len(variables) != runs:
+                raise ValueError("DeviceLm: one VariableSet per run needed")
+            self.P = max(v.size for v in variables)
+            self._var_list = [v.c_struct() for v in variables]
+            arr = (_capi.Variables * runs)(*self._var_list)
+            self._var_array = arr
+            self._vars = C.cast(arr, C.POINTER(_capi.Variables)).contents
+            self._opt.per_run_variables = 1
+        else:
+            self.P = variables.size
+            self._vars = variables.c_struct()
         need = int(self.lib.mkb_lm_workspace_bytes(C.byref(self._b), C.byref(self._plan),
                                                    C.byref(self._vars), C.byref(self._opt),
                                                    runs))
@@ -303,8 +334,7 @@ class DeviceLm:
         return (C.byref(self._b), C.byref(self._plan), C.byref(self._vars), C.byref(self._opt))
 
     def start(self, x0) -> None:
-        x0 = _dev_f64(np.asarray(x0).reshape(self.runs, self.variables.size),
-                      self.templates.device)
+        x0 = _dev_f64(pad_rows(x0, self.runs, self.P), self.templates.device)
         self._x0 = x0
         rc = self.lib.mkb_lm_start_device(*self._args(), C.c_void_p(x0.data_ptr()), self.runs,
                                           C.c_void_p(self.workspace.data_ptr()),
@@ -356,7 +386,7 @@ class DeviceLm:
         return int(out[0])
 
     def results(self) -> dict:
-        R, P, H = self.runs, self.variables.size, self.options.max_iterations + 1
+        R, P, H = self.runs, self.P, self.options.max_iterations + 1
         out = dict(x=np.zeros((R, P)), merit=np.zeros(R), status=np.zeros(R, np.int32),
                    iterations=np.zeros(R, np.int32), accepted=np.zeros(R, np.int32),
                    jacobians=np.zeros(R, np.int32), damping=np.zeros(R),
@@ -378,13 +408,19 @@ class DeviceLm:
 def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x0,
                     options: LmOptions | None = None, device: int = 0) -> dict:
     """optimize_lm_gpu (include/mikroptim/cuda/levenberg_marquardt.hpp): batched LM of the runs
-    x0 [runs][P] on `batch` (1 variant for all runs or one per run), one penalty pass."""
+    x0 [runs][P] on `batch` (1 variant for all runs or one per run), one penalty pass.
+    `variables` may be a list of one VariableSet per run (uneven batches; x0 rows padded)."""
     options = options or LmOptions()
     dev = _require_cuda(f"cuda:{device}")
-    x0 = np.asarray(x0, dtype=np.float64).reshape(-1, variables.size)
+    if isinstance(variables, (list, tuple)):
+        runs = len(variables)
+        x0 = pad_rows(x0, runs, max(v.size for v in variables))
+    else:
+        x0 = np.asarray(x0, dtype=np.float64).reshape(-1, variables.size)
+        runs = x0.shape[0]
     with torch.cuda.device(dev):
         templates = DeviceSystemBatch(batch, dev)
-        lm = DeviceLm(templates, layout, batch, variables, options, x0.shape[0])
+        lm = DeviceLm(templates, layout, batch, variables, options, runs)
         lm.start(x0)
         while lm.running() > 0:
             lm.cycle()

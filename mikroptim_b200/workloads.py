@@ -243,3 +243,97 @@ def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
     vs = VariableSet(topo, variables)
     x0 = np.stack([vs.extract(b, v) for v in range(variants)])
     return b, settings, vs, x0
+
+
+# ---- configuration 3: uneven systems -----------------------------------------------------------
+
+def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max: int = 30,
+           p_min: int = 8, p_max: int = 64, rings: int = 16, spokes: int = 32,
+           sigma: float = 0.05, failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+    """Configuration 3: variants of uneven surface and variable counts in one batch.
+
+    Variant v has S_v ~ U{s_min .. s_max} table surfaces: the stop, then L = (S_v - 1) // 2
+    biconvex elements in the style of configuration 1 (curvatures +-1/(50 L) and glass
+    6/L mm, perturbed by `sigma` Gaussian noise, air gaps 0.5 mm, Cauchy glass at 7
+    wavelengths 405..700 nm), and -- when S_v - 1 is odd -- a zero-power plate (curvature 0,
+    air on both sides) before the image; the image plane sits at the paraxial focus. All
+    variants share the 30-surface table (`variant_surfaces` holds S_v; the entries past S_v
+    are unused). 5 fields 0..1 degree, all Half pupils 16 x 32, pupil radius 5 mm.
+    Variables of run v: the first P_v ~ U{p_min .. p_max} (at most all of them) of
+    [working distance, element curvatures, glass thicknesses, air gaps].
+    Returns (batch, settings, [VariableSet per run], [x0 row per run])."""
+    S = s_max
+    topo = BatchTopology(surfaces=S, wavelengths=7, fields=5,
+                         type=[SURFACE_STOP] + [SURFACE_SPHERE] * (S - 1),
+                         pupil_mode=[PUPIL_HALF] * 5)
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.6
+    b.wavelength_nm[:] = OBJECTIVE_WAVELENGTHS
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    sv = s_min + np.floor(rng.uniform(1, variants) * (s_max - s_min + 1)).astype(np.int64)
+    pv = p_min + np.floor(rng.uniform(2, variants) * (p_max - p_min + 1)).astype(np.int64)
+    noise = rng.normal(3, variants * 3 * S).reshape(variants, S, 3)
+    n_glass = cauchy_index(OBJECTIVE_WAVELENGTHS)
+    n_glass_ref = float(cauchy_index(587.6))
+    angles = np.deg2rad(np.linspace(0.0, 1.0, 5))
+    variable_sets, x0 = [], []
+    for v in range(variants):
+        n_surf = int(sv[v])
+        elements = (n_surf - 1) // 2
+        c = np.zeros(S)
+        t = np.zeros(S)
+        idx = np.ones((S, 7))
+        n_ref = np.ones(S)
+        t[0] = 0.0  # stop plane at the first vertex
+        for e in range(elements):
+            s1, s2 = 1 + 2 * e, 2 + 2 * e
+            c[s1] = (1.0 / (50.0 * elements)) * (1.0 + sigma * noise[v, s1, 0])
+            c[s2] = (-1.0 / (50.0 * elements)) * (1.0 + sigma * noise[v, s2, 0])
+            t[s1] = (6.0 / elements) * (1.0 + sigma * noise[v, s1, 1])
+            t[s2] = 0.5 * (1.0 + sigma * noise[v, s2, 1])
+            idx[s1, :] = n_glass
+            n_ref[s1] = n_glass_ref
+        # surfaces past the elements (one zero-power plate when S_v - 1 is odd) stay c = 0
+        _, bfd = paraxial(c[None, :n_surf], t[None, :n_surf], n_ref[None, :n_surf])
+        efl, _ = paraxial(c[None, :n_surf], t[None, :n_surf], n_ref[None, :n_surf])
+        t[n_surf - 1] = bfd[0]
+        b.curvature[v] = c
+        b.thickness[v] = t
+        b.index[v] = idx
+        b.pupil_radius[v] = 5.0
+        b.field_angle[v] = angles
+        b.field_target[v] = efl[0] * np.tan(angles)
+        wd = (Variable(VAR_WORKING_DISTANCE, S - 1, 1.0, 500.0, 1.0) if n_surf == S
+              else Variable(VAR_THICKNESS, n_surf - 1, 1.0, 500.0, 1.0))
+        cands = [wd]
+        cands += [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, 1 + 2 * elements)]
+        cands += [Variable(VAR_THICKNESS, 1 + 2 * e, 0.5, 20.0, 1.0) for e in range(elements)]
+        cands += [Variable(VAR_THICKNESS, 2 + 2 * e, 0.1, 20.0, 1.0) for e in range(elements - 1)]
+        vs = VariableSet(topo, cands[:min(int(pv[v]), len(cands))])
+        variable_sets.append(vs)
+        x0.append(vs.extract(b, v))
+    b.variant_surfaces = sv.astype(np.uint8)
+    settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
+    return b, settings, variable_sets, x0
+
+
+def unpad(batch: SystemBatchHost, v: int) -> SystemBatchHost:
+    """Variant v of an uneven batch as a batch of its own S_v surfaces (one variant)."""
+    n = int(batch.variant_surfaces[v]) if batch.variant_surfaces is not None else batch.surfaces
+    topo = BatchTopology(surfaces=n, wavelengths=batch.wavelengths, fields=batch.fields,
+                         type=list(batch.topology.type[:n]),
+                         pupil_mode=list(batch.topology.pupil_mode))
+    out = SystemBatchHost(topo, 1)
+    out.reference_wavelength_nm = batch.reference_wavelength_nm
+    out.wavelength_nm = batch.wavelength_nm.copy()
+    out.wavelength_weight = batch.wavelength_weight.copy()
+    out.field_weight = batch.field_weight.copy()
+    out.curvature[0] = batch.curvature[v, :n]
+    out.thickness[0] = batch.thickness[v, :n]
+    out.index[0] = batch.index[v, :n]
+    out.pupil_radius[0] = batch.pupil_radius[v]
+    out.field_angle[0] = batch.field_angle[v]
+    out.field_target[0] = batch.field_target[v]
+    return out
