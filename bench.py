@@ -63,8 +63,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="lm", choices=["lm", "merit"])
-    ap.add_argument("--variants", type=int, default=4096)
+    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit"])
+    ap.add_argument("--variants", type=int, default=None,
+                    help="runs per GPU (default 8192 for uneven, 4096 otherwise)")
     return ap.parse_args()
 
 
@@ -185,7 +186,8 @@ def run_b200(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     lib = _capi.lib()
-    b, st, vs, x0 = workloads.objective(args.variants, seed=20261203 + 2 + 1000 * rank)
+    b, st, vs, x0 = workloads.objective(args.variants or 4096,
+                                        seed=20261203 + 2 + 1000 * rank)
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
     db = engine.DeviceSystemBatch(b, dev)
@@ -367,7 +369,8 @@ def run_lm(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     lib = _capi.lib()
-    b, st, vs, x0 = workloads.objective(args.variants, seed=20261203 + 2 + 1000 * rank)
+    b, st, vs, x0 = workloads.objective(args.variants or 4096,
+                                        seed=20261203 + 2 + 1000 * rank)
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
     runs = b.variants
@@ -519,6 +522,171 @@ def run_lm(args, world, rank, local):
     }, None
 
 
+WORKLOAD_UNEVEN = ("uneven-8192: 8192 runs, S ~ U{6..30} (stop, 1/50-style biconvex elements, "
+                   "zero-power plates), P ~ U{8..64} (capped by the system), L=7, F=5, "
+                   "16x32 Half pupils (config 3 shape)")
+
+
+def run_uneven(args, world, rank, local):
+    """Configuration 3: batched LM over uneven systems, one launch per kernel per cycle."""
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import PRECISION_FP64_FMA, PRECISION_MIXED, ResidualLayout
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    runs = args.variants or 8192
+    b, st, vss, x0 = workloads.uneven(runs, seed=20261203 + 3 + 1000 * rank)
+    P = max(v.size for v in vss)
+    lay_fma = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP64_FMA))
+    lay_mixed = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_MIXED))
+    db = engine.DeviceSystemBatch(b, dev)
+    max_it = args.warmup + args.steps + 100
+    opt = engine.LmOptions(max_iterations=max_it, jacobian=engine.JACOBIAN_ADJOINT,
+                           gram_exact=False)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    rays = lay_fma.rays_per_variant
+    sv = b.variant_surfaces.astype(np.int64)
+    hits = int(rays * (sv - 1).sum())
+
+    # ---- headline: adjoint (FP64 trace, FP32 reverse sweep) fused with the normal equations
+    lm = engine.DeviceLm(db, lay_mixed, b, vss, opt, runs)
+    lm.start(x0)
+    with ClockSampler(local) as clocks:
+        ms_cycle, iters, per_cycle = _lm_window(lm, args.steps, args.warmup, flush, world, dev)
+    ms_step = max_over_ranks(ms_cycle, world, dev)
+    value = world * iters / (ms_step * args.steps / 1e3)
+    x_now = np.zeros((runs, P))
+    res = lm.results()
+    x_now = res["x"]
+    del lm
+
+    # ---- the same with the FP64-FMA adjoint
+    lm_f = engine.DeviceLm(db, lay_fma, b, vss, opt, runs)
+    lm_f.start(x0)
+    ms_fma, iters_fma, _ = _lm_window(lm_f, args.steps, args.warmup, flush, world, dev)
+    fma_value = world * iters_fma / (max_over_ranks(ms_fma, world, dev) * args.steps / 1e3)
+    del lm_f
+
+    # ---- the reference method on the same GPU: FD Jacobian (2P + 1 traced variants), FP64
+    fd_runs = min(1024, runs)
+    fd_b = b.subset(0, fd_runs)
+    fd_db = engine.DeviceSystemBatch(fd_b, dev)
+    fd_opt = engine.LmOptions(max_iterations=max_it, jacobian=engine.JACOBIAN_FD,
+                              gram_exact=False)
+    fd = engine.DeviceLm(fd_db, lay_fma, fd_b, vss[:fd_runs], fd_opt, fd_runs)
+    fd.start(x0[:fd_runs])
+    fd_steps = max(2, min(args.steps, 10))
+    fd_ms, fd_iters, _ = _lm_window(fd, fd_steps, args.warmup, flush, world, dev)
+    fd_value = fd_iters / (fd_ms * fd_steps / 1e3)
+    del fd
+
+    # ---- the dominant kernel alone: fused adjoint + normal equations of every run
+    # FLOP model per run (reference cost model): 3 x 140 (S_v - 1 + 2) per ray + 4 P per ray +
+    # 2 P^2 per row (rays and penalty rows)
+    pv = np.array([v.size for v in vss], dtype=np.float64)
+    flop = float(np.sum(rays * (3 * FLOPEQ_PER_RAY_SURFACE * (sv - 1 + 2) + 4 * pv) +
+                        2 * pv * pv * lay_mixed.trace_rows))
+    engine.adjoint_normal_equations_runs_device(db, lay_mixed, b, vss, x_now)
+    torch.cuda.synchronize()
+    kt = []
+    for _ in range(3):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        engine.adjoint_normal_equations_runs_device(db, lay_mixed, b, vss, x_now)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kt.append(e0.elapsed_time(e1))
+    kernel_ms = min(kt)
+
+    # ---- MERIT rate (ray-surface hits/s) on the uneven batch
+    engine.merit_device(db, lay_fma, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        engine.merit_device(db, lay_fma, b)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    merit_ms = e0.elapsed_time(e1) / 3
+
+    # ---- end to end through the host-buffer path: pinned x in, cycle, x and merit out
+    host_x = torch.from_numpy(np.ascontiguousarray(x_now)).pin_memory()
+    host_out = torch.empty((runs, P + 1), dtype=torch.float64).pin_memory()
+    dev_x = torch.empty((runs, P), dtype=torch.float64, device=dev)
+    lm2 = engine.DeviceLm(db, lay_mixed, b, vss, opt, runs)
+    lm2.start(x_now)
+    it0 = int(lm2.iterations().sum())
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_x.copy_(host_x, non_blocking=True)
+        lm2.cycle()
+        lib.mkb_lm_results_device(*lm2._args(), runs, C.c_void_p(lm2.workspace.data_ptr()),
+                                  C.c_void_p(host_out.data_ptr()),
+                                  C.c_void_p(host_out.data_ptr() + runs * P * 8),
+                                  *([None] * 9), C.c_void_p(stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_iters = int(lm2.iterations().sum()) - it0
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    del lm2
+
+    errors = opd_errors(b, st, runs=256) if rank == 0 else None
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = flop / (kernel_ms / 1e3) / 1e12
+    if rank != 0:
+        return None, None
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": "LM iterations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-3 shapes)",
+        "config": {"workload": WORKLOAD_UNEVEN,
+                   "step": "one batched LM cycle of all runs in one launch per kernel "
+                           "(CUDA graph), runs ordered by surface count",
+                   "runs_per_gpu": runs, "variables_max": P, "rays_per_run": rays,
+                   "jacobian": "adjoint fused with FP64 tensor-core normal equations",
+                   "precision": "MIXED: FP64 trace and OPD, FP32 adjoint reverse sweep",
+                   "iterations": "LM iterations actually taken in the timed cycles "
+                                 f"({iters} of {runs * args.steps} run-cycles)",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(per_cycle * args.steps),
+        "ray_surface_hits_per_s": world * hits / (merit_ms / 1e3),
+        "adjoint_fp64_fma": {"value": fma_value, "unit": "LM iterations/s",
+                             "ms_per_cycle": ms_fma},
+        "fd_fp64": {"value": world * fd_value, "unit": "LM iterations/s",
+                    "ms_per_cycle_1024_runs": fd_ms, "cycles": fd_steps,
+                    "speedup_adjoint_mixed_vs_fd": value / (world * fd_value),
+                    "speedup_adjoint_fma_vs_fd": fma_value / (world * fd_value)},
+        "opd_error_vs_fp64": errors,
+        "e2e": {"value": world * e2e_iters / (e2e_ms / 1e3), "unit": "LM iterations/s",
+                "h2d_bytes_per_step": int(runs * P * 8),
+                "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "adjoint_gram_kernel<MixedPrecision> (fused adjoint + DMMA "
+                               "normal equations, every run, with its apply kernel)",
+                     "kernel_ms": kernel_ms,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "flop_model": "3 x 140 (S_v-1+2) FLOP-eq per ray + 4P per ray + 2P^2 "
+                                   "per row, summed over the runs"},
+        "clocks": clocks.summary(),
+    }, None
+
+
 # ---- CPU baselines (oracle) ----------------------------------------------------------------
 def cpu_baseline(kind: str, sample_variants: int = 16, seed: int = 20261203 + 2):
     """The reference's own CPU merit (oracle/_ref) or the C restatement, on all host threads,
@@ -563,6 +731,44 @@ def cpu_baseline_lm(kind: str, runs: int = 256, seed: int = 20261203 + 2):
                                      f"1 and 3 cycles, {t2 - t0:.1f} s"}
 
 
+def cpu_baseline_uneven(runs: int = 96, seed: int = 20261203 + 3):
+    """The reference's optimize_lm_cpu on a sample of the uneven runs: the reference needs one
+    topology and one variable set per call, so every run is its own call (its baseline loops
+    over topology groups), the calls spread over all host threads. Three cycles minus one
+    cycle, halved, isolates the cost of a cycle from the start-up."""
+    import concurrent.futures as cf
+    import oracle.pyoracle as po
+    from mikroptim_b200 import workloads
+    from mikroptim_b200.batch import ResidualLayout
+    b, st, vss, x0 = workloads.uneven(runs, seed=seed)
+    ref = po.reference()
+    threads = os.cpu_count() or 1
+    jobs = []
+    for v in range(runs):
+        one = workloads.unpad(b, v)
+        lone = ResidualLayout(one.topology, st)
+        vs = type(vss[v])(one.topology, [
+            type(var)(2 if (var.type == 1 and var.surface == one.surfaces - 1) else var.type,
+                      var.surface, var.lower, var.upper, var.typical)
+            for var in vss[v].variables])
+        jobs.append((one, lone, vs, x0[v][None, :]))
+
+    def run_all(max_it):
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(lambda j: ref.optimize_lm(*j, max_iterations=max_it, method="adjoint",
+                                                  threads=1), jobs))
+    t0 = time.perf_counter()
+    run_all(1)
+    t1 = time.perf_counter()
+    run_all(3)
+    t2 = time.perf_counter()
+    per_cycle = max(((t2 - t1) - (t1 - t0)) / 2, 1e-9)
+    return {"value": runs / per_cycle, "unit": "LM iterations/s", "cores": threads,
+            "kind": "reference", "sample": f"optimize_lm_cpu (adjoint), {runs} of the uneven "
+                                            f"runs one per call, 1 and 3 cycles, "
+                                            f"{t2 - t0:.1f} s"}
+
+
 def reference_kind() -> str:
     import oracle.pyoracle as po
     return "reference" if os.path.exists(po.REF_LIB) else "port"
@@ -572,6 +778,23 @@ def run_reference(args, world, rank):
     if rank != 0:
         return None
     kind = reference_kind()
+    if args.workload == "uneven":
+        if kind != "reference":
+            return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
+        base = cpu_baseline_uneven(runs=96)
+        v = base["value"]
+        return {
+            "metric": METRIC, "value": v, "unit": "LM iterations/s", "impl": "reference",
+            "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, configuration-3 shapes)",
+            "config": {"workload": WORKLOAD_UNEVEN,
+                       "step": "one LM cycle of a 96-run sample on the host"},
+            "cpu_baseline": {"value": v, "unit": "LM iterations/s", "cores": base["cores"],
+                             "kind": kind, "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "LM iterations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
     if args.workload == "lm":
         if kind != "reference":
             return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
@@ -614,6 +837,13 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "uneven":
+        out, _ = run_uneven(args, world, rank, local)
+        if rank == 0 and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline_uneven()
+            except Exception as e:  # the baseline is reported, not required
+                out["cpu_baseline"] = {"value": None, "error": str(e)}
     elif args.workload == "lm":
         out, _ = run_lm(args, world, rank, local)
         if rank == 0 and world == 1:

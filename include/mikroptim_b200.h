@@ -210,6 +210,19 @@ int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
                                         const double* x0, int32_t runs, double* gram,
                                         void* workspace, size_t workspace_bytes, void* stream);
 
+/* The same for an uneven batch: `vars` is an array of `runs` variable sets (one per run; the
+ * counts may differ), x0 rows are strided by the largest count Pmax and gram [runs] slots by
+ * (Pmax + 1)^2 (run i's (P_i + 1)^2 matrix dense at the start of its slot). Templates with
+ * variant_surfaces must hold one template per run. */
+size_t mkb_adjoint_normal_equations_runs_workspace_bytes(const mkb_device_batch* templates,
+                                                         const mkb_variables* vars,
+                                                         int32_t runs);
+int mkb_adjoint_normal_equations_runs_device(const mkb_device_batch* templates,
+                                             const mkb_residual_plan* plan,
+                                             const mkb_variables* vars, const double* x0,
+                                             int32_t runs, double* gram, void* workspace,
+                                             size_t workspace_bytes, void* stream);
+
 /* ---- batched Levenberg-Marquardt ------------------------------------------------------------
  * LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85) for one pass (no outer
  * soft-failure penalty rounds), and the per-run state kept in a caller workspace. The device

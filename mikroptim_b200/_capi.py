@@ -151,6 +151,12 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_adjoint_normal_equations_device.argtypes = [PB, PP, PV, c.c_void_p, c.c_int32,
                                                         c.c_void_p, c.c_void_p, c.c_size_t,
                                                         c.c_void_p]
+    lib.mkb_adjoint_normal_equations_runs_workspace_bytes.restype = c.c_size_t
+    lib.mkb_adjoint_normal_equations_runs_workspace_bytes.argtypes = [PB, PV, c.c_int32]
+    lib.mkb_adjoint_normal_equations_runs_device.restype = c.c_int
+    lib.mkb_adjoint_normal_equations_runs_device.argtypes = [PB, PP, PV, c.c_void_p, c.c_int32,
+                                                             c.c_void_p, c.c_void_p, c.c_size_t,
+                                                             c.c_void_p]
     PO = C.POINTER(LmOptions)
     lib.mkb_lm_workspace_bytes.restype = c.c_size_t
     lib.mkb_lm_workspace_bytes.argtypes = [PB, PP, PV, PO, c.c_int32]

@@ -14,6 +14,7 @@
 #include "launch.cuh"
 
 #include <algorithm>
+#include <vector>
 #include <type_traits>
 
 namespace mkb {
@@ -312,6 +313,88 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
 
 }  // namespace mkb
 
+namespace mkb {
+namespace {
+
+// The fused adjoint + normal equations of mkb_adjoint_normal_equations_device and, with
+// per_run, of mkb_adjoint_normal_equations_runs_device (vars: one set per run).
+int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, bool per_run, const double* x0,
+                             int runs, double* gram, void* workspace, size_t workspace_bytes,
+                             cudaStream_t stream) {
+    if (runs < 0) {
+        set_error("adjoint normal equations: runs must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (runs == 0) return MKB_OK;
+    int rc = check_templates(templates, runs);
+    if (rc != MKB_OK) return rc;
+    if (templates->variant_surfaces != nullptr && templates->variants != runs) {
+        set_error("adjoint normal equations: uneven templates need one template per run");
+        return MKB_ERR_ARGUMENT;
+    }
+    TraceParams tp;
+    mkb_device_batch b = *templates;
+    b.variants = runs;
+    rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
+    if (rc != MKB_OK) return rc;
+    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
+        plan->precision != MKB_PRECISION_MIXED) {
+        set_error("adjoint normal equations: precision %d not available", plan->precision);
+        return MKB_ERR_UNSUPPORTED;
+    }
+    if (vars == nullptr || !x0 || !gram) {
+        set_error("adjoint normal equations: null pointer");
+        return MKB_ERR_ARGUMENT;
+    }
+    VarParams vp;
+    rc = make_var_params(&vars[0], tp.S, templates->type, &vp);
+    if (rc != MKB_OK) return rc;
+    std::vector<VarParams> table;
+    int pmax = vp.P;
+    if (per_run) {
+        table.resize(static_cast<size_t>(runs));
+        for (int r = 0; r < runs; ++r) {
+            rc = make_var_params(&vars[r], tp.S, templates->type, &table[r]);
+            if (rc != MKB_OK) return rc;
+            pmax = table[r].P > pmax ? table[r].P : pmax;
+        }
+    }
+    const size_t need = per_run ? mkb_adjoint_normal_equations_runs_workspace_bytes(templates,
+                                                                                    vars, runs)
+                                : mkb_adjoint_jacobian_workspace_bytes(templates, runs);
+    if (workspace == nullptr || workspace_bytes < need) {
+        set_error("adjoint normal equations: workspace of %zu bytes needed", need);
+        return MKB_ERR_WORKSPACE;
+    }
+    char* ws = static_cast<char*>(workspace);
+    double* records = reinterpret_cast<double*>(ws);
+    const size_t rec_bytes = align256(sizeof(double) * static_cast<size_t>(runs) *
+                                      templates->record_stride);
+    RunVars rv;
+    size_t table_bytes = 0;  // per run: the variable table follows the records
+    if (per_run) {
+        table_bytes = align256(sizeof(VarParams) * static_cast<size_t>(runs));
+        VarParams* dtable = reinterpret_cast<VarParams*>(ws + rec_bytes);
+        rc = cuda_status(cudaMemcpyAsync(dtable, table.data(), sizeof(VarParams) * table.size(),
+                                         cudaMemcpyHostToDevice, stream),
+                         "adjoint normal equations: upload variables");
+        if (rc != MKB_OK) return rc;
+        rv.table = dtable;
+        rv.stride = pmax;
+    }
+    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream,
+                      rv);
+    if (rc != MKB_OK) return rc;
+    return launch_adjoint_gram(tp, vp, records, gram, ws + rec_bytes + table_bytes,
+                               workspace_bytes - rec_bytes - table_bytes, plan->precision,
+                               stream, nullptr, rv);
+}
+
+}  // namespace
+}  // namespace mkb
+
 extern "C" {
 
 size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
@@ -395,53 +478,40 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
     return launch_projection(tp, vp, R, status, J, exact, stream);
 }
 
+int mkb_adjoint_normal_equations_runs_device(const mkb_device_batch* templates,
+                                             const mkb_residual_plan* plan,
+                                             const mkb_variables* vars, const double* x0,
+                                             int32_t runs, double* gram, void* workspace,
+                                             size_t workspace_bytes, void* stream_ptr);
+
 int mkb_adjoint_normal_equations_device(const mkb_device_batch* templates,
                                         const mkb_residual_plan* plan, const mkb_variables* vars,
                                         const double* x0, int32_t runs, double* gram,
                                         void* workspace, size_t workspace_bytes,
                                         void* stream_ptr) {
-    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    if (runs < 0) {
-        set_error("adjoint normal equations: runs must be >= 0");
-        return MKB_ERR_ARGUMENT;
-    }
-    if (runs == 0) return MKB_OK;
-    int rc = check_templates(templates, runs);
-    if (rc != MKB_OK) return rc;
-    if (templates->variant_surfaces != nullptr && templates->variants != runs) {
-        set_error("adjoint normal equations: uneven templates need one template per run");
-        return MKB_ERR_ARGUMENT;
-    }
-    TraceParams tp;
-    mkb_device_batch b = *templates;
-    b.variants = runs;
-    rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
-    if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
-        plan->precision != MKB_PRECISION_MIXED) {
-        set_error("adjoint normal equations: precision %d not available", plan->precision);
-        return MKB_ERR_UNSUPPORTED;
-    }
-    VarParams vp;
-    rc = make_var_params(vars, tp.S, templates->type, &vp);
-    if (rc != MKB_OK) return rc;
-    if (!x0 || !gram) {
-        set_error("adjoint normal equations: null pointer");
-        return MKB_ERR_ARGUMENT;
-    }
-    const size_t need = mkb_adjoint_jacobian_workspace_bytes(templates, runs);
-    if (workspace == nullptr || workspace_bytes < need) {
-        set_error("adjoint normal equations: workspace of %zu bytes needed", need);
-        return MKB_ERR_WORKSPACE;
-    }
-    double* records = static_cast<double*>(workspace);
-    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
-    rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
-    if (rc != MKB_OK) return rc;
-    const size_t rec_bytes = align256(sizeof(double) * static_cast<size_t>(runs) *
-                                      templates->record_stride);
-    return launch_adjoint_gram(tp, vp, records, gram, static_cast<char*>(workspace) + rec_bytes,
-                               workspace_bytes - rec_bytes, plan->precision, stream);
+    return adjoint_normal_equations(templates, plan, vars, false, x0, runs, gram, workspace,
+                                    workspace_bytes, static_cast<cudaStream_t>(stream_ptr));
+}
+
+size_t mkb_adjoint_normal_equations_runs_workspace_bytes(const mkb_device_batch* templates,
+                                                         const mkb_variables* vars,
+                                                         int32_t runs) {
+    if (templates == nullptr || vars == nullptr || runs < 0) return 0;
+    int pmax = 1;
+    for (int r = 0; r < runs; ++r) pmax = vars[r].count > pmax ? vars[r].count : pmax;
+    if (pmax > MKB_MAX_VARIABLES) return 0;
+    return align256(sizeof(double) * static_cast<size_t>(runs) * templates->record_stride) +
+           fused_scratch_bytes(runs, pmax, templates->surfaces) +
+           align256(sizeof(VarParams) * static_cast<size_t>(runs));
+}
+
+int mkb_adjoint_normal_equations_runs_device(const mkb_device_batch* templates,
+                                             const mkb_residual_plan* plan,
+                                             const mkb_variables* vars, const double* x0,
+                                             int32_t runs, double* gram, void* workspace,
+                                             size_t workspace_bytes, void* stream_ptr) {
+    return adjoint_normal_equations(templates, plan, vars, true, x0, runs, gram, workspace,
+                                    workspace_bytes, static_cast<cudaStream_t>(stream_ptr));
 }
 
 }  // extern "C"

@@ -293,6 +293,20 @@ def pad_rows(x, runs: int, width: int) -> np.ndarray:
     return np.asarray(x, dtype=np.float64).reshape(runs, width)
 
 
+def check_start_points(variables, x0: np.ndarray) -> None:
+    """The reference rejects a start value outside its variable's bounds before any work
+    (VariableSet validation in levenberg_marquardt, std::invalid_argument): ValueError."""
+    sets = variables if isinstance(variables, (list, tuple)) else [variables] * len(x0)
+    for i, (vs, row) in enumerate(zip(sets, x0)):
+        lo, up = vs.lower(), vs.upper()
+        x = row[:vs.size]
+        bad = np.nonzero((x < lo) | (x > up))[0]
+        if bad.size:
+            k = int(bad[0])
+            raise ValueError(f"lm: run {i}, variable {k}: start value {x[k]!r} outside "
+                             f"[{lo[k]!r}, {up[k]!r}]")
+
+
 class DeviceLm:
     """Batched LM state on the device: start(x0), cycle(), results(). One object per problem;
     the workspace is allocated once and reused by every cycle.
@@ -334,7 +348,9 @@ class DeviceLm:
         return (C.byref(self._b), C.byref(self._plan), C.byref(self._vars), C.byref(self._opt))
 
     def start(self, x0) -> None:
-        x0 = _dev_f64(pad_rows(x0, self.runs, self.P), self.templates.device)
+        rows = pad_rows(x0, self.runs, self.P)
+        check_start_points(self.variables, rows)
+        x0 = _dev_f64(rows, self.templates.device)
         self._x0 = x0
         rc = self.lib.mkb_lm_start_device(*self._args(), C.c_void_p(x0.data_ptr()), self.runs,
                                           C.c_void_p(self.workspace.data_ptr()),
@@ -450,3 +466,36 @@ def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: Residu
                                                  _stream_handle(stream))
     _capi.check(rc, "adjoint normal equations")
     return gram
+
+
+def adjoint_normal_equations_runs_device(templates: DeviceSystemBatch, layout: ResidualLayout,
+                                         host: SystemBatchHost, variable_sets, x0,
+                                         stream=None):
+    """Fused adjoint + normal equations of an uneven batch: one VariableSet per run, x0 rows
+    padded to the largest P. Returns gram [runs][Pmax+1][Pmax+1]; run i's (P_i+1)^2 matrix is
+    dense at the start of its slot (see gram_block)."""
+    lib = _capi.lib()
+    dev = templates.device
+    runs = len(variable_sets)
+    pmax = max(v.size for v in variable_sets)
+    x = _dev_f64(pad_rows(x0, runs, pmax), dev)
+    b = templates.c_struct()
+    plan = layout.plan(host)
+    keep = [v.c_struct() for v in variable_sets]
+    arr = (_capi.Variables * runs)(*keep)
+    pv = C.cast(arr, C.POINTER(_capi.Variables))
+    need = int(lib.mkb_adjoint_normal_equations_runs_workspace_bytes(C.byref(b), pv, runs))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    gram = torch.zeros((runs, pmax + 1, pmax + 1), dtype=torch.float64, device=dev)
+    rc = lib.mkb_adjoint_normal_equations_runs_device(C.byref(b), C.byref(plan), pv,
+                                                      C.c_void_p(x.data_ptr()), runs,
+                                                      C.c_void_p(gram.data_ptr()),
+                                                      C.c_void_p(ws.data_ptr()), ws.numel(),
+                                                      _stream_handle(stream))
+    _capi.check(rc, "adjoint normal equations (runs)")
+    return gram
+
+
+def gram_block(gram: torch.Tensor, run: int, P: int) -> torch.Tensor:
+    """Run `run`'s (P+1) x (P+1) matrix from a gram of stride (Pmax+1)^2 per run."""
+    return gram[run].reshape(-1)[:(P + 1) * (P + 1)].reshape(P + 1, P + 1)

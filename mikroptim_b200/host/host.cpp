@@ -524,6 +524,15 @@ LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
     cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
     const int runs = runs_of(variables, base, x0);
     const int P = variables.size();
+    for (int r = 0; r < runs; ++r)  // the reference rejects start values outside the bounds
+        for (int k = 0; k < P; ++k) {
+            const double x = x0[static_cast<size_t>(r) * P + k];
+            const Variable& v = variables.variables()[k];
+            if (!(x >= v.lower && x <= v.upper))
+                throw std::invalid_argument("optimize_lm_gpu: start value of variable " +
+                                            std::to_string(k) + " of run " +
+                                            std::to_string(r) + " outside its bounds");
+        }
     const ResidualLayout layout(base.topology(), settings);
     const auto plan = layout.plan(base);
     DeviceSystemBatch templates;

@@ -309,7 +309,7 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
               else Variable(VAR_THICKNESS, n_surf - 1, 1.0, 500.0, 1.0))
         cands = [wd]
         cands += [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, 1 + 2 * elements)]
-        cands += [Variable(VAR_THICKNESS, 1 + 2 * e, 0.5, 20.0, 1.0) for e in range(elements)]
+        cands += [Variable(VAR_THICKNESS, 1 + 2 * e, 0.1, 20.0, 1.0) for e in range(elements)]
         cands += [Variable(VAR_THICKNESS, 2 + 2 * e, 0.1, 20.0, 1.0) for e in range(elements - 1)]
         vs = VariableSet(topo, cands[:min(int(pv[v]), len(cands))])
         variable_sets.append(vs)

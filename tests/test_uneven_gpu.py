@@ -65,3 +65,20 @@ def test_uneven_lm_equals_each_run_alone(method):
         assert together["iterations"][v] == alone["iterations"][0], v
         assert together["status"][v] == alone["status"][0], v
     assert np.all(together["merit"] <= together["history"][:, 0])
+
+
+def test_uneven_fused_normal_equations_equal_each_run_alone():
+    b, st, vss, x0 = _small(8, precision=0)
+    lay = ResidualLayout(b.topology, st)
+    gram = engine.adjoint_normal_equations_runs_device(engine.DeviceSystemBatch(b), lay, b, vss,
+                                                       x0)
+    for v in range(b.variants):
+        one = workloads.unpad(b, v)
+        lone = ResidualLayout(one.topology, st)
+        vs_alone = type(vss[v])(one.topology, [
+            type(var)(2 if (var.type == 1 and var.surface == one.surfaces - 1) else var.type,
+                      var.surface, var.lower, var.upper, var.typical)
+            for var in vss[v].variables])
+        alone = engine.adjoint_normal_equations_device(engine.DeviceSystemBatch(one), lone, one,
+                                                       vs_alone, x0[v][None, :])
+        assert torch.equal(engine.gram_block(gram, v, vss[v].size), alone[0]), v
