@@ -653,6 +653,9 @@ struct FusedArgs {
     int* queue;            // run counter
     const int* run_mask;   // runs to process (null: all)
     const int* order;      // queue position -> run (null: identity)
+    const int* split;      // device: queue positions [0, *split) and [*split, V) are two
+                           // launches (runs with <= 31 and with more variables), or null
+    int part;              // 0 or 1: which of the two ranges this launch takes; -1: all
     const VarParams* vt;   // per-run variables (null: ap.v for every run)
     int p_max;             // the largest P (sizes the shared memory and the scratch slots)
     int64_t gram_stride;   // doubles per run of `gram`
@@ -701,8 +704,14 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         __syncthreads();  // the previous run's shared state is consumed
         if (tid == 0) sh.run = atomicAdd(fa.queue, 1);
         __syncthreads();
-        if (sh.run >= p.V) break;
-        const int run = fa.order != nullptr ? fa.order[sh.run] : sh.run;
+        int lo = 0, hi = p.V;
+        if (fa.split != nullptr && fa.part >= 0) {
+            const int mid = *fa.split;
+            lo = fa.part == 0 ? 0 : mid;
+            hi = fa.part == 0 ? mid : p.V;
+        }
+        if (lo + sh.run >= hi) break;
+        const int run = fa.order != nullptr ? fa.order[lo + sh.run] : lo + sh.run;
         if (fa.run_mask != nullptr && fa.run_mask[run] == 0) continue;
         // the run's variables, columns and surfaces
         const VarParams& v = fa.vt != nullptr ? fa.vt[run] : fa.ap.v;
@@ -936,9 +945,10 @@ size_t fused_scratch_bytes(int runs, int P, int S) {
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
                         cudaStream_t stream, const int* run_mask, RunVars rv,
-                        const int* order) {
+                        const int* order, const int* split, int part, int part_pmax) {
     if (tp.V <= 0) return MKB_OK;
-    const int p_max = rv.table != nullptr ? rv.stride : vp.P;
+    const int p_all = rv.table != nullptr ? rv.stride : vp.P;
+    const int p_max = part_pmax > 0 ? part_pmax : p_all;  // sizes this launch's shared memory
     if (scratch == nullptr || scratch_bytes < fused_scratch_bytes(tp.V, p_max, tp.S)) {
         set_error("fused adjoint: scratch of %zu bytes needed",
                   fused_scratch_bytes(tp.V, p_max, tp.S));
@@ -955,9 +965,11 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.slot_doubles = fused_slot_doubles(p_max, tp.S);
     fa.run_mask = run_mask;
     fa.order = order;
+    fa.split = split;
+    fa.part = part;
     fa.vt = rv.table;
     fa.p_max = p_max;
-    fa.gram_stride = static_cast<int64_t>(p_max + 1) * (p_max + 1);
+    fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
     const size_t smem = fused_adjoint_smem(tp, p_max);
     auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
                   : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>

@@ -372,13 +372,31 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
     const size_t rec_bytes = align256(sizeof(double) * static_cast<size_t>(runs) *
                                       templates->record_stride);
     RunVars rv;
-    size_t table_bytes = 0;  // per run: the variable table follows the records
+    size_t table_bytes = 0;  // per run: the variable table and the run order follow the records
+    int* order = nullptr;
+    constexpr int kSmallP = 31;  // runs with at most this many variables go first, in a launch
+                                 // with a smaller shared-memory footprint
+    std::vector<int> host_order;  // [runs] order, then the size of the first group
     if (per_run) {
-        table_bytes = align256(sizeof(VarParams) * static_cast<size_t>(runs));
+        table_bytes = align256(sizeof(VarParams) * static_cast<size_t>(runs)) +
+                      align256(sizeof(int) * (static_cast<size_t>(runs) + 1));
         VarParams* dtable = reinterpret_cast<VarParams*>(ws + rec_bytes);
+        order = reinterpret_cast<int*>(ws + rec_bytes +
+                                       align256(sizeof(VarParams) * static_cast<size_t>(runs)));
+        for (int r = 0; r < runs; ++r)
+            if (table[r].P <= kSmallP) host_order.push_back(r);
+        const int small = static_cast<int>(host_order.size());
+        for (int r = 0; r < runs; ++r)
+            if (table[r].P > kSmallP) host_order.push_back(r);
+        host_order.push_back(small);
         rc = cuda_status(cudaMemcpyAsync(dtable, table.data(), sizeof(VarParams) * table.size(),
                                          cudaMemcpyHostToDevice, stream),
                          "adjoint normal equations: upload variables");
+        if (rc == MKB_OK)
+            rc = cuda_status(cudaMemcpyAsync(order, host_order.data(),
+                                             sizeof(int) * host_order.size(),
+                                             cudaMemcpyHostToDevice, stream),
+                             "adjoint normal equations: upload order");
         if (rc != MKB_OK) return rc;
         rv.table = dtable;
         rv.stride = pmax;
@@ -387,9 +405,17 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream,
                       rv);
     if (rc != MKB_OK) return rc;
-    return launch_adjoint_gram(tp, vp, records, gram, ws + rec_bytes + table_bytes,
-                               workspace_bytes - rec_bytes - table_bytes, plan->precision,
-                               stream, nullptr, rv);
+    void* scratch = ws + rec_bytes + table_bytes;
+    const size_t scratch_bytes = workspace_bytes - rec_bytes - table_bytes;
+    if (per_run && pmax > kSmallP) {
+        rc = launch_adjoint_gram(tp, vp, records, gram, scratch, scratch_bytes, plan->precision,
+                                 stream, nullptr, rv, order, order + runs, 0, kSmallP);
+        if (rc != MKB_OK) return rc;
+        return launch_adjoint_gram(tp, vp, records, gram, scratch, scratch_bytes, plan->precision,
+                                   stream, nullptr, rv, order, order + runs, 1, pmax);
+    }
+    return launch_adjoint_gram(tp, vp, records, gram, scratch, scratch_bytes, plan->precision,
+                               stream, nullptr, rv, order);
 }
 
 }  // namespace
@@ -502,7 +528,8 @@ size_t mkb_adjoint_normal_equations_runs_workspace_bytes(const mkb_device_batch*
     if (pmax > MKB_MAX_VARIABLES) return 0;
     return align256(sizeof(double) * static_cast<size_t>(runs) * templates->record_stride) +
            fused_scratch_bytes(runs, pmax, templates->surfaces) +
-           align256(sizeof(VarParams) * static_cast<size_t>(runs));
+           align256(sizeof(VarParams) * static_cast<size_t>(runs)) +
+           align256(sizeof(int) * (static_cast<size_t>(runs) + 1));
 }
 
 int mkb_adjoint_normal_equations_runs_device(const mkb_device_batch* templates,

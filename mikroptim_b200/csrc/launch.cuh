@@ -52,7 +52,8 @@ int launch_projection(const TraceParams& tp, const VarParams& vp, int64_t rows,
 int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double* records,
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
                         cudaStream_t stream, const int* run_mask = nullptr, RunVars rv = {},
-                        const int* order = nullptr);
+                        const int* order = nullptr, const int* split = nullptr, int part = -1,
+                        int part_pmax = 0);
 size_t fused_scratch_bytes(int runs, int P, int S);
 
 // gram.cu

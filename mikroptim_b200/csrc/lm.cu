@@ -469,7 +469,8 @@ struct LmLayout {
     size_t fused_ws_bytes;
     VarParams* vt;      // per-run variables (uneven batches), else null
     uint8_t* vsurf;     // surface count of each run's record (uneven surfaces), else null
-    int* order;         // runs sorted by surface count, largest first (uneven surfaces)
+    int* order;         // processing order (uneven batches), else null
+    int* split;         // [1] runs of the first group of `order`
 };
 
 constexpr int kFdChunkRuns = 64;
@@ -532,7 +533,8 @@ LmLayout lm_layout(char* base, const LmSetup& s, int runs, const mkb_device_batc
     L.st.pstride = s.pmax;
     const bool uneven = templates->variant_surfaces != nullptr;
     L.vsurf = uneven ? reinterpret_cast<uint8_t*>(take(r)) : nullptr;
-    L.order = uneven ? reinterpret_cast<int*>(take(4 * r)) : nullptr;
+    L.order = uneven || s.per_run ? reinterpret_cast<int*>(take(4 * r)) : nullptr;
+    L.split = uneven || s.per_run ? reinterpret_cast<int*>(take(4)) : nullptr;
     L.gram = reinterpret_cast<double*>(take(8 * r * (P + 1) * (P + 1)));
     const size_t jr = s.fused ? 0 : r;  // the fused adjoint keeps J out of memory
     L.J = reinterpret_cast<double*>(take(8 * jr * P * R));
@@ -658,24 +660,32 @@ int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* tem
                         L.merit_ws_bytes, s.precision, stream, RunMask{run_mask, 1, 0});
 }
 
-// Runs sorted by surface count, largest first (counting sort in one CTA; the order inside a
-// count is not fixed, and only the scheduling depends on it).
-__global__ void order_kernel(const uint8_t* __restrict__ vsurf, int runs, int S,
-                             int* __restrict__ order) {
-    __shared__ int start[MKB_MAX_SURFACES + 1];
-    for (int i = threadIdx.x; i <= MKB_MAX_SURFACES; i += blockDim.x) start[i] = 0;
+// Processing order of the runs: those with at most kSmallP variables first (their fused
+// adjoint launch needs less shared memory per CTA, so more CTAs fit an SM), each group by
+// surface count, largest first. *split = size of the first group. Counting sort in one CTA;
+// the order inside a bucket is not fixed, and only the scheduling depends on it.
+constexpr int kSmallP = 31;
+constexpr int kBuckets = 2 * (MKB_MAX_SURFACES + 1);
+
+__global__ void order_kernel(const uint8_t* __restrict__ vsurf, const VarParams* vt, int P,
+                             int runs, int S, int* __restrict__ order, int* __restrict__ split) {
+    __shared__ int start[kBuckets];
+    for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) start[i] = 0;
     __syncthreads();
     auto key = [&](int r) {
-        const int n = vsurf[r];
-        return n < 2 ? 2 : (n > S ? S : n);
+        int n = vsurf != nullptr ? vsurf[r] : S;
+        n = n < 2 ? 2 : (n > S ? S : n);
+        const int big = (vt != nullptr ? vt[r].P : P) > kSmallP ? 1 : 0;
+        return big * (MKB_MAX_SURFACES + 1) + (MKB_MAX_SURFACES - n);
     };
     for (int r = threadIdx.x; r < runs; r += blockDim.x) atomicAdd(&start[key(r)], 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         int at = 0;
-        for (int n = MKB_MAX_SURFACES; n >= 0; --n) {
-            const int c = start[n];
-            start[n] = at;
+        for (int k = 0; k < kBuckets; ++k) {
+            if (k == MKB_MAX_SURFACES + 1) *split = at;
+            const int c = start[k];
+            start[k] = at;
             at += c;
         }
     }
@@ -723,7 +733,8 @@ int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_pl
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, x0, L.records, runs,
                           stream, run_vars(s, L, templates));
         if (rc != MKB_OK) return rc;
-        order_kernel<<<1, 1024, 0, stream>>>(L.vsurf, runs, s.tp.S, L.order);
+        order_kernel<<<1, 1024, 0, stream>>>(L.vsurf, L.vt, s.vp.P, runs, s.tp.S, L.order,
+                                             L.split);
         count_launch();
         rc = cuda_status(cudaGetLastError(), "lm order launch");
         if (rc != MKB_OK) return rc;
@@ -758,9 +769,19 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream, rv);
-        if (rc == MKB_OK)
+        if (rc == MKB_OK && L.order != nullptr && s.pmax > kSmallP) {
+            // two launches: the runs with few variables with a smaller shared-memory footprint
+            rc = launch_adjoint_gram(tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
+                                     s.precision, stream, want, rv, L.order, L.split, 0,
+                                     kSmallP);
+            if (rc == MKB_OK)
+                rc = launch_adjoint_gram(tp, s.vp, L.records, L.gram, L.fused_ws,
+                                         L.fused_ws_bytes, s.precision, stream, want, rv, L.order,
+                                         L.split, 1, s.pmax);
+        } else if (rc == MKB_OK) {
             rc = launch_adjoint_gram(tp, s.vp, L.records, L.gram, L.fused_ws, L.fused_ws_bytes,
                                      s.precision, stream, want, rv, L.order);
+        }
     } else {
         const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
