@@ -468,24 +468,35 @@ def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: Residu
     return gram
 
 
+class RunVariables:
+    """One VariableSet per run as the C array the ABI takes (built once, reused)."""
+
+    def __init__(self, variable_sets):
+        self.sets = list(variable_sets)
+        self.runs = len(self.sets)
+        self.pmax = max(v.size for v in self.sets)
+        self._keep = [v.c_struct() for v in self.sets]
+        self._array = (_capi.Variables * self.runs)(*self._keep)
+        self.pointer = C.cast(self._array, C.POINTER(_capi.Variables))
+
+
 def adjoint_normal_equations_runs_device(templates: DeviceSystemBatch, layout: ResidualLayout,
                                          host: SystemBatchHost, variable_sets, x0,
-                                         stream=None):
-    """Fused adjoint + normal equations of an uneven batch: one VariableSet per run, x0 rows
-    padded to the largest P. Returns gram [runs][Pmax+1][Pmax+1]; run i's (P_i+1)^2 matrix is
-    dense at the start of its slot (see gram_block)."""
+                                         stream=None, workspace: torch.Tensor | None = None):
+    """Fused adjoint + normal equations of an uneven batch: one VariableSet per run (a list or
+    a RunVariables), x0 rows padded to the largest P. Returns gram [runs][Pmax+1][Pmax+1]; run
+    i's (P_i+1)^2 matrix is dense at the start of its slot (see gram_block)."""
     lib = _capi.lib()
     dev = templates.device
-    runs = len(variable_sets)
-    pmax = max(v.size for v in variable_sets)
-    x = _dev_f64(pad_rows(x0, runs, pmax), dev)
+    rv = variable_sets if isinstance(variable_sets, RunVariables) else RunVariables(variable_sets)
+    runs, pmax = rv.runs, rv.pmax
+    x = x0 if isinstance(x0, torch.Tensor) else _dev_f64(pad_rows(x0, runs, pmax), dev)
     b = templates.c_struct()
     plan = layout.plan(host)
-    keep = [v.c_struct() for v in variable_sets]
-    arr = (_capi.Variables * runs)(*keep)
-    pv = C.cast(arr, C.POINTER(_capi.Variables))
+    pv = rv.pointer
     need = int(lib.mkb_adjoint_normal_equations_runs_workspace_bytes(C.byref(b), pv, runs))
-    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    ws = workspace if workspace is not None and workspace.numel() >= need else \
+        torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
     gram = torch.zeros((runs, pmax + 1, pmax + 1), dtype=torch.float64, device=dev)
     rc = lib.mkb_adjoint_normal_equations_runs_device(C.byref(b), C.byref(plan), pv,
                                                       C.c_void_p(x.data_ptr()), runs,
