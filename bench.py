@@ -55,6 +55,9 @@ TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
 # in profiles/adjoint_gram_objective1184.md (1,184 runs: 1.669 GB read, 18.593 GB written),
 # scaled by the runs of the launch.
 FUSED_TRAFFIC_BYTES_PER_RUN = (1.669274e9 + 18.593394e9) / 1184
+# The same for the uneven (config-3) runs, MIXED precision, both launches of the call, from
+# profiles/adjoint_gram_uneven1184.md (1,184 runs: 1.992 GB read, 19.288 GB written).
+FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (1.599339e9 + 0.392692e9 + 11.698874e9 + 7.588631e9) / 1184
 
 
 def parse():
@@ -688,7 +691,8 @@ def run_uneven(args, world, rank, local):
                 "h2d_bytes_per_step": int(runs * P * 8),
                 "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN * runs,
                      "kernel": "adjoint_gram_kernel<MixedPrecision> (fused adjoint + DMMA "
                                "normal equations, every run, with its apply kernel)",
                      "kernel_ms": kernel_ms,
