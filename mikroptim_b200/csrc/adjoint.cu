@@ -385,13 +385,14 @@ constexpr int kFusedWarps = kFusedThreads / 32;
 constexpr int kExtraRows = 8;
 constexpr int kFusedMinBlocks = 3;  // CTAs per SM the register budget is sized for
 // Per ray and table surface c the forward pass keeps, in the CTA's scratch slot, the state
-// entering the step c -> c + 1 and that step's StepLocal quantities (kSlotDoubles doubles).
-constexpr int kSlotDoubles = 11;
+// entering the step c -> c + 1 and that step's StepLocal quantities but mu (kSlotDoubles
+// values; mu = n / n' per surface and wavelength is in a shared-memory table of the run).
+constexpr int kSlotDoubles = 10;
 constexpr bool kFusedDual = true;   // one two-seed sweep for rays with both rows
 constexpr int kMaxTileCols = MKB_MAX_VARIABLES / 8;                              // 8
 constexpr int kMaxTilePairs = kMaxTileCols * (kMaxTileCols + 1) / 2;             // 36
 constexpr int kMaxFusedSlots = 148 * 8;  // persistent CTAs at most (SMs x resident CTAs)
-constexpr int kSegBatch = 16;            // tuple segments whose means are held at once
+constexpr int kSegBatch = 8;             // tuple segments whose means are held at once
 
 // columns of a row: the P derivatives, the residual in column P, zero padding to 8
 __host__ __device__ inline int fused_np(int P) { return ((P + 1 + 7) / 8) * 8; }
@@ -408,12 +409,6 @@ struct FusedShared {
     int run;                      // run taken off the queue
     int2 tiles[kMaxTilePairs];    // (row tile, column tile) of every upper-triangle pair
 };
-
-__device__ __forceinline__ double fused_warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -448,9 +443,10 @@ struct RowSinks {
     int ld[K];
 };
 
-template <class N>
-__device__ void fused_forward(const TraceParams& p, const double* rec, const RecordLayout& lay,
-                              int S, int f, int l, const Sample& smp, bool soft_mode, double* ck,
+template <class N, class Q>
+__device__ void fused_forward(const TraceParams& p, const double* rec, const double* mu_tab,
+                              const RecordLayout& lay, int S, int f, int l, const Sample& smp,
+                              bool soft_mode, Q* ck,
                               int stride_ck, uint64_t& br_lo, uint64_t& br_hi, int& count,
                               int& image_branch, int& status_out, int& soft_first, double& opl,
                               double& penalty) {
@@ -478,29 +474,28 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
     N n_before = idx[l];
-    auto keep_state = [&](double* q) {
-        q[0] = value_of(r.px);
-        q[1 * kFusedThreads] = value_of(r.py);
-        q[2 * kFusedThreads] = value_of(r.pz);
-        q[3 * kFusedThreads] = value_of(r.dx);
-        q[4 * kFusedThreads] = value_of(r.dy);
-        q[5 * kFusedThreads] = value_of(r.dz);
+    auto keep_state = [&](Q* q) {
+        q[0] = Q(value_of(r.px));
+        q[1 * kFusedThreads] = Q(value_of(r.py));
+        q[2 * kFusedThreads] = Q(value_of(r.pz));
+        q[3 * kFusedThreads] = Q(value_of(r.dx));
+        q[4 * kFusedThreads] = Q(value_of(r.dy));
+        q[5 * kFusedThreads] = Q(value_of(r.dz));
     };
     for (int s = 1; s < S; ++s) {
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
-        double* q = ck + (s - 1) * stride_ck;  // slot s - 1: the state entering this step
+        Q* q = ck + (s - 1) * stride_ck;  // slot s - 1: the state entering this step
         keep_state(q);
         int branch;
         StepLocal<N> loc{zero, zero, zero, zero, zero};
-        status = step_surface<N, true>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch,
-                                       &loc);
+        status = step_surface_mu<N, true>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
+                                          sp, branch, &loc);
         if (status != kOk) break;
-        q[6 * kFusedThreads] = value_of(loc.s0);
-        q[7 * kFusedThreads] = value_of(loc.s);
-        q[8 * kFusedThreads] = value_of(loc.root_d);
-        q[9 * kFusedThreads] = value_of(loc.mu);
-        q[10 * kFusedThreads] = value_of(loc.root_k);
+        q[6 * kFusedThreads] = Q(value_of(loc.s0));
+        q[7 * kFusedThreads] = Q(value_of(loc.s));
+        q[8 * kFusedThreads] = Q(value_of(loc.root_d));
+        q[9 * kFusedThreads] = Q(value_of(loc.root_k));
         count = s + 1;
         if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
         else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
@@ -533,10 +528,11 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const Rec
 // factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
 // quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
 // out-of-line copy per K keeps the kernel's instruction footprint small.
-template <class N, class A, int K>
+template <class N, class A, int K, class Q>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
-                                            const double* rec, const RecordLayout& lay, int S,
-                                            int f, int l, const Sample& smp, const double* ck,
+                                            const double* rec, const double* mu_tab,
+                                            const RecordLayout& lay, int S,
+                                            int f, int l, const Sample& smp, const Q* ck,
                                             int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                             int count, int image_branch, bool reached_image,
                                             bool soft_mode, const double (&so)[K],
@@ -569,11 +565,11 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
         StepLocal<N> loc;
     };
     auto load = [&](int c, Slot& sl) {
-        const double* q = ck + c * stride_ck;
+        const Q* q = ck + c * stride_ck;
         sl.p = {N(q[0]), N(q[kFusedThreads]), N(q[2 * kFusedThreads])};
         sl.d = {N(q[3 * kFusedThreads]), N(q[4 * kFusedThreads]), N(q[5 * kFusedThreads])};
         sl.loc = {N(q[6 * kFusedThreads]), N(q[7 * kFusedThreads]), N(q[8 * kFusedThreads]),
-                  N(q[9 * kFusedThreads]), N(q[10 * kFusedThreads])};
+                  N(mu_tab[(c + 1) * L + l]), N(q[9 * kFusedThreads])};
     };
     Slot next;
     load(count - 1, next);
@@ -622,24 +618,39 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
 }
 
 // Mixed precision: the forward trace (OPL, piston, merit, the states the sweep is linearised
-// at) in FP64, the reverse sweep in FP32 on those states (an FP32 trace of the rays themselves
-// misses the OPD bar on aberrated systems; the Jacobian tolerates single-precision rounding).
+// at) in FP64, the reverse sweep in FP32 on those states rounded to FP32 when they are kept
+// (an FP32 trace of the rays themselves misses the OPD bar on aberrated systems; the Jacobian
+// tolerates single-precision rounding).
 struct MixedPrecision {};
 
-// number types of the forward trace and of the reverse sweep per kernel variant
-template <class N> struct FusedTypes { using Fwd = N; using Adj = N; };
-template <> struct FusedTypes<MixedPrecision> { using Fwd = double; using Adj = float; };
+// number types per kernel variant: the forward trace (Fwd), the kept states and the
+// quantities the reverse sweep recomputes from them (Bwd), the adjoint arithmetic (Adj), and
+// the type the states are kept in (Keep)
+template <class N> struct FusedTypes {
+    using Fwd = N;
+    using Bwd = N;
+    using Adj = N;
+    using Keep = double;
+};
+template <> struct FusedTypes<MixedPrecision> {
+    using Fwd = double;
+    using Bwd = float;
+    using Adj = float;
+    using Keep = float;
+};
 
 template <class N, int K>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
-                                             const double* rec, const RecordLayout& lay, int S,
-                                             int f, int l, const Sample& smp, const double* ck,
+                                             const double* rec, const double* mu_tab,
+                                             const RecordLayout& lay, int S,
+                                             int f, int l, const Sample& smp,
+                                             const typename FusedTypes<N>::Keep* ck,
                                              int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                              int count, int image_branch, bool reached_image,
                                              bool soft_mode, const double (&so)[K],
                                              const double (&spn)[K], const RowSinks<K>& sinks) {
     using T = FusedTypes<N>;
-    fused_backward<typename T::Fwd, typename T::Adj, K>(p, v, rec, lay, S, f, l, smp, ck, stride_ck,
+    fused_backward<typename T::Bwd, typename T::Adj, K>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
                                                         reached_image, soft_mode, so, spn, sinks);
 }
@@ -662,7 +673,7 @@ struct FusedArgs {
 };
 
 template <class N>
-__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
+__global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ? 4 : kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
     __shared__ FusedShared sh;
@@ -676,7 +687,8 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     constexpr int TS = kFusedThreads + 4;              // column stride of Y
     constexpr int ES = kExtraRows + 4;                 // column stride of E
     double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
-    double* Y = record + ((p.stride + 1) & ~1);        // column-major [NPM][TS]
+    double* mu_tab = record + ((p.stride + 1) & ~1);   // [S + 1][L]: mu of step s - 1 -> s
+    double* Y = mu_tab + (((p.S + 1) * p.L + 1) & ~1); // column-major [NPM][TS]
     double* E = Y + NPM * TS;                          // column-major [NPM][ES]
     double* mu_open = E + NPM * ES;                    // [NPM] running mean of the open tuple
     double* seg_mean = mu_open + NPM;                  // [kSegBatch][NPM] segment means
@@ -686,8 +698,9 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const RecordLayout lay = record_layout(p.S, p.L, p.F);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     // this CTA's scratch slot: penalty rows [NPM][T], then per surface [kSlotDoubles][T]
+    using Keep = typename FusedTypes<N>::Keep;
     double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
-    double* ckpt = pen_slot + NPM * kFusedThreads;
+    Keep* ckpt = reinterpret_cast<Keep*>(pen_slot + NPM * kFusedThreads);
     copy_tables(p, sh.tab);
     // upper-triangle tile pairs in column order: the pairs of a smaller P are a prefix
     for (int e = tid; e < pairs_max; e += kFusedThreads) {
@@ -698,7 +711,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         }
         sh.tiles[e] = make_int2(rem, j);
     }
-    double* my_ck = ckpt + tid;
+    Keep* my_ck = ckpt + tid;
     uint32_t uses = 0;
     for (;;) {
         __syncthreads();  // the previous run's shared state is consumed
@@ -729,6 +742,17 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         if (!stage_to_shared(record, fa.records + static_cast<int64_t>(run) * p.stride,
                              static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar, uses++))
             return;
+        // mu = n_before / n_after of every step and wavelength, divided as the step divides
+        // it (rows 0 and S .. p.S stay 0: no step)
+        for (int i = tid; i < (p.S + 1) * p.L; i += kFusedThreads) {
+            const int s = i / p.L, l = i - s * p.L;
+            using F = typename FusedTypes<N>::Fwd;
+            mu_tab[i] = s >= 1 && s < S
+                            ? value_of(F(record[lay.index + (s - 1) * p.L + l]) /
+                                       F(record[lay.index + s * p.L + l]))
+                            : 0.0;
+        }
+        __syncthreads();
         for (int base = 0; base < p.rays; base += kFusedThreads) {
             const int q = base + tid;
             double* row = Y + tid;  // this ray's row, column c at row[c * TS]
@@ -749,7 +773,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                fused_forward<typename FusedTypes<N>::Fwd>(p, record, lay, S, f, l, smp, soft_mode,
+                fused_forward<typename FusedTypes<N>::Fwd, Keep>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
                                                            my_ck, stride_ck, br_lo, br_hi, count,
                                                            image_branch, status, soft_first, opl,
                                                            penalty);
@@ -768,7 +792,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double so[2] = {piston ? 1.0 : 0.0, 0.0};
                         const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
                         const RowSinks<2> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
-                        run_backward<N, 2>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                        run_backward<N, 2>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
                                            sinks);
                     }
@@ -778,18 +802,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double sp[1] = {pen_sweep ? 1.0 : 0.0};
                         const RowSinks<1> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
                                                 {piston ? TS : kFusedThreads}};
-                        run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck,
+                        run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
                                            so, sp, sinks);
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
                     const RowSinks<1> s0{{1.0}, {row}, {TS}};
-                    run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
                     const RowSinks<1> s1{{pfac}, {prow}, {kFusedThreads}};
-                    run_backward<N, 1>(p, v, record, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
                 }
             }
@@ -821,23 +845,36 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             __syncthreads();
             for (int k0 = 0; k0 < nseg; k0 += kSegBatch) {
                 const int kn = nseg - k0 < kSegBatch ? nseg - k0 : kSegBatch;
-                // B2: weight and weighted column means of each segment, a warp per (segment,
-                // column) with lane-strided rows and a shuffle sum
-                for (int pr = warp; pr < kn * (P + 1); pr += kFusedWarps) {
+                // B2: weight and weighted column means of each segment, a thread per (segment,
+                // column) summing the segment's rows from row c mod n on: neighbouring columns
+                // (column stride 4 mod 16 doubles) then read bank pairs 5c + j mod 16, so the
+                // lanes of a half-warp never share one
+                for (int pr = tid; pr < kn * (P + 1); pr += kFusedThreads) {
                     const int k = pr / (P + 1), c = pr - k * (P + 1);
-                    const int a = sh.seg_first[k0 + k], b = sh.seg_first[k0 + k + 1];
-                    const double* col = Y + c * TS;
-                    double sw_sum = 0.0, sum = 0.0;
-                    for (int r = a + lane; r < b; r += 32) {
-                        sw_sum += sh.w[r];
-                        sum += sh.w[r] * col[r];
+                    const int a = sh.seg_first[k0 + k];
+                    const int n = sh.seg_first[k0 + k + 1] - a;
+                    const double* col = Y + c * TS + a;
+                    const double* wr = sh.w + a;
+                    double sw0 = 0.0, sw1 = 0.0, s0 = 0.0, s1 = 0.0;
+                    int r = c % n;
+                    int j = 0;
+                    for (; j + 1 < n; j += 2) {
+                        const double wa = wr[r], ya = col[r];
+                        r = r + 1 == n ? 0 : r + 1;
+                        const double wb = wr[r], yb = col[r];
+                        r = r + 1 == n ? 0 : r + 1;
+                        sw0 += wa;
+                        s0 += wa * ya;
+                        sw1 += wb;
+                        s1 += wb * yb;
                     }
-                    sw_sum = fused_warp_sum(sw_sum);
-                    sum = fused_warp_sum(sum);
-                    if (lane == 0) {
-                        seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
-                        if (c == 0) seg_w[k] = sw_sum;
+                    if (j < n) {
+                        sw0 += wr[r];
+                        s0 += wr[r] * col[r];
                     }
+                    const double sw_sum = sw0 + sw1, sum = s0 + s1;
+                    seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
+                    if (c == 0) seg_w[k] = sw_sum;
                 }
                 __syncthreads();
                 // B3: every row of the batch's segments centred and scaled by its own thread
@@ -924,6 +961,7 @@ size_t fused_adjoint_smem(const TraceParams& tp, int P) {
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
     return sizeof(double) * (static_cast<size_t>((tp.stride + 1) & ~1) +
+                             static_cast<size_t>(((tp.S + 1) * tp.L + 1) & ~1) +
                              static_cast<size_t>(kFusedThreads + 4) * NP +
                              (kExtraRows + 4) * NP + NP + kSegBatch * (NP + 1) +
                              static_cast<size_t>(pairs) * 64);

@@ -46,6 +46,25 @@ __device__ __forceinline__ A cv(N x) { return A(value_of(x)); }
 template <class A, class N>
 __device__ __forceinline__ Vec<A> cv(Vec<N> v) { return {cv<A>(v.x), cv<A>(v.y), cv<A>(v.z)}; }
 
+// A divisor of the adjoint arithmetic. FP32 (the mixed sweep): the SFU reciprocal, taken once
+// per step and shared by the K seeds, and a multiply -- a few ulp of single precision, inside
+// that sweep's rounding budget. FP64: the rounded division in the reference's order, so the
+// FP64 sweeps stay bit-identical.
+__device__ __forceinline__ float sfu_reciprocal(float x) { return __fdividef(1.0f, x); }
+
+template <class A>
+struct Divisor {
+    A d;
+    __device__ __forceinline__ explicit Divisor(A x) : d(x) {}
+    __device__ __forceinline__ A div(A a) const { return a / d; }
+};
+template <>
+struct Divisor<float> {
+    float r;
+    __device__ __forceinline__ explicit Divisor(float x) : r(sfu_reciprocal(x)) {}
+    __device__ __forceinline__ float div(float a) const { return a * r; }
+};
+
 // K adjoint vectors through one step (K seeds of the same ray: the OPL and the penalty). The
 // step-local forward quantities are recomputed in N, the adjoint arithmetic runs in A (N for
 // the FP64 paths; float on FP64 states for the mixed path). The forward recompute and the
@@ -108,7 +127,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         root_k = known ? known->root_k : nsqrt(k);
         a = root_k - mu * cos_i;
     }
-    if (!missed) inv = one / (two * root_d);
+    if (!missed) inv = Divisor<N>(two * root_d).div(one);
     // the same quantities in the adjoint arithmetic
     const A zero_a(0.0), two_a(2.0);
     const Vec<A> ad = cv<A>(d), aNv = cv<A>(Nv), aq = cv<A>(q), ad1 = cv<A>(d1);
@@ -117,6 +136,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
     const A ainv_norm = cv<A>(inv_norm), ainv = cv<A>(inv), as = cv<A>(s), as0 = cv<A>(s0);
     const A ann = cv<A>(n_after), anb = cv<A>(n_before), aB = cv<A>(B), aH = cv<A>(H);
     const A arr = cv<A>(rr), ax = cv<A>(x), ay = cv<A>(y), axd = cv<A>(xd);
+    const Divisor<A> by_2root_k(two_a * aroot_k), by_n_after(ann), by_c(ac), by_dz(ad.z);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
         const Vec<A> qb_out = adj[m].p;
@@ -135,7 +155,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
             nb = vadd(nb, vscale(aa, d1b));
             const A ab = vdot(d1b, aNv);
             mub += vdot(d1b, ad);
-            kb += ab / (two_a * aroot_k);
+            kb += by_2root_k.div(ab);
             mub += -ab * acos;
             cosb += -ab * amu;
         }
@@ -143,8 +163,8 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         cosb += kb * two_a * amu * amu * acos;
         in.d = vadd(in.d, vscale(cosb, aNv));
         nb = vadd(nb, vscale(cosb, ad));
-        out[m].n_before += mub / ann;
-        out[m].n_after += -mub * amu / ann;
+        out[m].n_before += by_n_after.div(mub);
+        out[m].n_after += by_n_after.div(-mub * amu);
         Vec<A> nrb = nb;
         if (missed) nrb = vscale(ainv_norm, vsub(nb, vscale(vdot(aNv, nb), aNv)));
         const Vec<A> qb = vadd(qb_out, vscale(-ac, nrb));
@@ -157,8 +177,8 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         out[m].n_before += seed_opl[m] * (as0 + as);
         A hb = zero_a, bb = zero_a;
         if (missed) {
-            bb += sb / ac;
-            cb += -sb * as / ac;
+            bb += by_c.div(sb);
+            cb += by_c.div(-sb * as);
             const A db = -seed_pen[m];
             bb += db * two_a * aB;
             cb += -db * aH;
@@ -183,7 +203,7 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
         s0b += xb * ad.x + yb * ad.y;
         in.d.x += xb * as0;
         in.d.y += yb * as0;
-        const A qq = s0b / ad.z;
+        const A qq = by_dz.div(s0b);
         out[m].thickness += qq;
         in.p.z += -qq;
         in.d.z += -qq * as0;

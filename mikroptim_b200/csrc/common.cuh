@@ -206,6 +206,7 @@ __device__ __forceinline__ double nsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float nsqrt(float a) { return sqrtf(a); }
 __device__ __forceinline__ double value_of(double a) { return a; }
 __device__ __forceinline__ double value_of(Exact64 a) { return a.v; }
+__device__ __forceinline__ float value_of(float a) { return a; }
 
 // ---- ray state and surface step -------------------------------------------------------------
 // Formulas and order of operations: transfer_to_tangent_plane, intersect_sphere and
@@ -234,13 +235,15 @@ struct StepLocal {
     N s0, s, root_d, mu, root_k;
 };
 
-// One surface step (stop/plane: c = 0). Returns the status; `branch` gets the taken
-// soft-failure continuation. With soft == nullptr the hard-failure rules apply. kKeep also
-// returns the step's StepLocal quantities (the arithmetic is the same either way).
+// One surface step (stop/plane: c = 0) with mu = n / n' given (the rounded quotient of the
+// two indices, taken once per surface and wavelength by callers that trace many rays).
+// Returns the status; `branch` gets the taken soft-failure continuation. With soft == nullptr
+// the hard-failure rules apply. kKeep also returns the step's StepLocal quantities (the
+// arithmetic is the same either way).
 template <class N, bool kKeep = false>
-__device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N n_after,
-                                            SoftT<N>* soft, int& branch,
-                                            StepLocal<N>* keep = nullptr) {
+__device__ __forceinline__ int step_surface_mu(RayT<N>& r, N t, N c, N n_before, N mu,
+                                               SoftT<N>* soft, int& branch,
+                                               StepLocal<N>* keep = nullptr) {
     const N zero(0.0), one(1.0);
     if (!(r.dz > zero)) return kBackward;
     // transfer to the tangent plane
@@ -275,7 +278,6 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
     r.pz = r.pz + s * r.dz;
     r.opl += n_before * (s0 + s);
     // refraction, mu = n / n'
-    const N mu = n_before / n_after;
     if constexpr (kKeep) keep->mu = mu;
     N nx = -c * r.px, ny = -c * r.py, nz = one - c * r.pz;
     if (missed) {
@@ -306,6 +308,14 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
     r.dy = mu * r.dy + a * ny;
     r.dz = mu * r.dz + a * nz;
     return kOk;
+}
+
+// One surface step with mu = n_before / n_after divided here.
+template <class N, bool kKeep = false>
+__device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N n_after,
+                                            SoftT<N>* soft, int& branch,
+                                            StepLocal<N>* keep = nullptr) {
+    return step_surface_mu<N, kKeep>(r, t, c, n_before, n_before / n_after, soft, branch, keep);
 }
 
 // Step onto the reference sphere about M = (0, h, w) through the vertex of the last surface.
