@@ -27,6 +27,9 @@ namespace {
 constexpr int kThreads = 128;
 constexpr int kRaysPerThread = 4;
 constexpr int kPackRays = kThreads * kRaysPerThread;
+// resident CTAs per SM the register budget is sized for (56 registers, no spills); the shared
+// memory of the workloads' tables fits as many
+constexpr int kTraceBlocksPerSm = 9;
 
 // The bulk-copy destination `record` must start on a 16-byte boundary: it is the first
 // member of a 16-byte aligned struct (checked below).
@@ -45,10 +48,11 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // Trace of one ray to the reference sphere in number type N (trace_to_reference_sphere,
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
+// mu_tab[s * L + l] = n_before / n_after of the step onto surface s (divided in N).
 template <class N>
-__device__ inline int trace_ray(const TraceParams& p, const double* rec, const RecordLayout& lay,
-                                int S, int f, int l, const Sample& smp, bool soft_mode,
-                                double& opl, double& penalty) {
+__device__ inline int trace_ray(const TraceParams& p, const double* rec, const double* mu_tab,
+                                const RecordLayout& lay, int S, int f, int l, const Sample& smp,
+                                bool soft_mode, double& opl, double& penalty) {
     const int L = p.L;
     const N zero(0.0);
     const N a = rec[lay.pupil];
@@ -74,7 +78,8 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const R
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
-        status = step_surface<N>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch);
+        status = step_surface_mu<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]), sp,
+                                    branch);
         if (status != kOk) break;
         n_before = n_after;
     }
@@ -123,7 +128,7 @@ struct TupleOut {
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
 template <bool kResiduals, int kPrecision>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
     constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
@@ -150,6 +155,15 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                          &sh.bar))
         return;
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
+    // mu of every step and wavelength, divided once per CTA as the step would divide it
+    extern __shared__ double mu_tab[];  // [S][L]
+    for (int i = threadIdx.x; i < S * p.L; i += kThreads) {
+        const int s = i / p.L, l = i - s * p.L;
+        mu_tab[i] = s >= 1 ? value_of(N(sh.record[lay.index + (s - 1) * p.L + l]) /
+                                      N(sh.record[lay.index + s * p.L + l]))
+                           : 0.0;
+    }
+    __syncthreads();
 
     // ---- phase 1: trace ---------------------------------------------------------------
     for (int i = threadIdx.x; i < pack.rays; i += kThreads) {
@@ -161,7 +175,8 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N>(p, sh.record, lay, S, f, l, smp, soft_mode, opl, pen);
+        const int st = trace_ray<N>(p, sh.record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
+                                    pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
         sh.status[i] = static_cast<uint8_t>(st);
@@ -297,6 +312,11 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
     hard[v] = nh;
 }
 
+// dynamic shared memory of trace_kernel: the mu table
+size_t trace_smem(const TraceParams& p) {
+    return static_cast<size_t>(p.S) * p.L * sizeof(double);
+}
+
 size_t merit_workspace(int V, int n_tuples) {
     const size_t slots = static_cast<size_t>(V) * n_tuples;
     return slots * (sizeof(double) + 2 * sizeof(int)) + 256;
@@ -311,9 +331,9 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
     if (precision == MKB_PRECISION_FP64)
-        trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
     else
-        trace_kernel<true, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<true, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
     count_launch();
     return cuda_status(cudaGetLastError(), "residuals kernel launch");
 }
@@ -334,9 +354,9 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
     if (precision == MKB_PRECISION_FP64)
-        trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
     else
-        trace_kernel<false, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, 0, stream>>>(p, records, out);
+        trace_kernel<false, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
     count_launch();
     int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
     if (rc != MKB_OK) return rc;
