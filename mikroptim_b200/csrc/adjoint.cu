@@ -435,11 +435,37 @@ __device__ __forceinline__ void accumulate(const double* xt, int ld, int n, int 
     }
 }
 
+// acc += X^T X for the chunk's rows: X(k, c) = Y[c * ld + k] for the derivative columns
+// (type YT) and R[k] for the residual column c = P (FP64 in every variant), k < n (n a
+// multiple of 4). Fragment columns past P read the zero padding of Y.
+template <class YT>
+__device__ __forceinline__ void accumulate_rows(const YT* Y, const double* R, int ld, int P, int n,
+                                                int pairs, const int2* tiles, double* acc) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gid = lane >> 2, tig = lane & 3;
+    for (int e = warp; e < pairs; e += kFusedWarps) {
+        const int col_a = tiles[e].x * 8 + gid, col_b = tiles[e].y * 8 + gid;
+        const YT* ya = Y + col_a * ld + tig;
+        const YT* yb = Y + col_b * ld + tig;
+        const double* r = R + tig;
+        const bool ra = col_a == P, rb = col_b == P;
+        double* a = acc + (e * 32 + lane) * 2;
+        double d0 = a[0], d1 = a[1];
+        for (int k0 = 0; k0 < n; k0 += 4) {
+            const double fa = ra ? r[k0] : static_cast<double>(ya[k0]);
+            const double fb = rb ? r[k0] : static_cast<double>(yb[k0]);
+            dmma(d0, d1, fa, fb);
+        }
+        a[0] = d0;
+        a[1] = d1;
+    }
+}
+
 // Where the reverse sweep writes: the OPL row (seed 0) and the penalty row (seed 1).
-template <int K>
+template <int K, class YT>
 struct RowSinks {
     double factor[K];
-    double* row[K];
+    YT* row[K];
     int ld[K];
 };
 
@@ -528,7 +554,7 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
 // factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
 // quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
 // out-of-line copy per K keeps the kernel's instruction footprint small.
-template <class N, class A, int K, class Q>
+template <class N, class A, int K, class Q, class YT>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
                                             const double* rec, const double* mu_tab,
                                             const RecordLayout& lay, int S,
@@ -536,7 +562,8 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                                             int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                             int count, int image_branch, bool reached_image,
                                             bool soft_mode, const double (&so)[K],
-                                            const double (&spn)[K], const RowSinks<K>& sinks) {
+                                            const double (&spn)[K],
+                                            const RowSinks<K, YT>& sinks) {
     const int L = p.L;
     const N zero(0.0);
     const double* curv = rec + lay.curvature;
@@ -592,7 +619,7 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                 if (col >= 0) {
 #pragma unroll
                     for (int m = 0; m < K; ++m)
-                        sinks.row[m][col * sinks.ld[m]] = value_of(factor[m] * center_adj[m].z);
+                        sinks.row[m][col * sinks.ld[m]] = YT(value_of(factor[m] * center_adj[m].z));
                 }
             }
         } else {
@@ -609,8 +636,10 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
             const int ct = v.col_thickness[c];
 #pragma unroll
             for (int m = 0; m < K; ++m) {
-                if (cc >= 0) sinks.row[m][cc * sinks.ld[m]] = value_of(factor[m] * par[m].curvature);
-                if (ct >= 0) sinks.row[m][ct * sinks.ld[m]] = value_of(factor[m] * par[m].thickness);
+                if (cc >= 0)
+                    sinks.row[m][cc * sinks.ld[m]] = YT(value_of(factor[m] * par[m].curvature));
+                if (ct >= 0)
+                    sinks.row[m][ct * sinks.ld[m]] = YT(value_of(factor[m] * par[m].thickness));
             }
         }
         next_branch = branch_of(c);
@@ -624,19 +653,22 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
 struct MixedPrecision {};
 
 // number types per kernel variant: the forward trace (Fwd), the kept states and the
-// quantities the reverse sweep recomputes from them (Bwd), the adjoint arithmetic (Adj), and
-// the type the states are kept in (Keep)
+// quantities the reverse sweep recomputes from them (Bwd), the adjoint arithmetic (Adj), the
+// type the states are kept in (Keep), and the type of the derivative columns of the rows in
+// shared memory and of the penalty rows in the scratch slot (Row; the residual column is FP64)
 template <class N> struct FusedTypes {
     using Fwd = N;
     using Bwd = N;
     using Adj = N;
     using Keep = double;
+    using Row = double;
 };
 template <> struct FusedTypes<MixedPrecision> {
     using Fwd = double;
     using Bwd = float;
     using Adj = float;
     using Keep = float;
+    using Row = float;
 };
 
 template <class N, int K>
@@ -648,7 +680,8 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                              int stride_ck, uint64_t br_lo, uint64_t br_hi,
                                              int count, int image_branch, bool reached_image,
                                              bool soft_mode, const double (&so)[K],
-                                             const double (&spn)[K], const RowSinks<K>& sinks) {
+                                             const double (&spn)[K],
+                                             const RowSinks<K, typename FusedTypes<N>::Row>& sinks) {
     using T = FusedTypes<N>;
     fused_backward<typename T::Bwd, typename T::Adj, K>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
@@ -681,15 +714,17 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const int NPM = fused_np(fa.p_max);  // shared-memory and scratch layout: the largest P
     const int pairs_max = (NPM / 8) * (NPM / 8 + 1) / 2;
     const int stride_ck = kSlotDoubles * kFusedThreads;
-    // Column strides = 4 (mod 16) doubles: the 16 lanes of a half-warp reading a DMMA fragment
-    // (8 columns x 4 rows) then hit 16 different bank pairs; lanes that own consecutive rows
-    // of one column (the sweep's writes, the centring) stay conflict-free.
+    // Column strides = 4 (mod 16) doubles, 4 (mod 32) floats: the lanes of a (half-)warp
+    // reading a DMMA fragment (8 columns x 4 rows) then hit different banks; lanes that own
+    // consecutive rows of one column (the sweep's writes, the centring) stay conflict-free.
     constexpr int TS = kFusedThreads + 4;              // column stride of Y
     constexpr int ES = kExtraRows + 4;                 // column stride of E
     double* record = dyn;                              // [stride] (bulk-copy target, 16 B aligned)
     double* mu_tab = record + ((p.stride + 1) & ~1);   // [S + 1][L]: mu of step s - 1 -> s
-    double* Y = mu_tab + (((p.S + 1) * p.L + 1) & ~1); // column-major [NPM][TS]
-    double* E = Y + NPM * TS;                          // column-major [NPM][ES]
+    using YT = typename FusedTypes<N>::Row;
+    YT* Y = reinterpret_cast<YT*>(mu_tab + (((p.S + 1) * p.L + 1) & ~1));  // [NPM][TS]
+    double* R = reinterpret_cast<double*>(Y + NPM * TS);  // [TS] the residual column
+    double* E = R + TS;                                // column-major [NPM][ES]
     double* mu_open = E + NPM * ES;                    // [NPM] running mean of the open tuple
     double* seg_mean = mu_open + NPM;                  // [kSegBatch][NPM] segment means
     double* seg_w = seg_mean + kSegBatch * NPM;        // [kSegBatch] segment weights
@@ -699,7 +734,8 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     // this CTA's scratch slot: penalty rows [NPM][T], then per surface [kSlotDoubles][T]
     using Keep = typename FusedTypes<N>::Keep;
-    double* pen_slot = fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles;
+    YT* pen_slot =
+        reinterpret_cast<YT*>(fa.scratch + static_cast<int64_t>(blockIdx.x) * fa.slot_doubles);
     Keep* ckpt = reinterpret_cast<Keep*>(pen_slot + NPM * kFusedThreads);
     copy_tables(p, sh.tab);
     // upper-triangle tile pairs in column order: the pairs of a smaller P are a prefix
@@ -733,7 +769,6 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         const int ncols = NP / 8;
         const int pairs = ncols * (ncols + 1) / 2;
         const int S = surfaces_of(p, run);
-        double* Rv = Y + P * TS;  // the residual column of Y
         for (int i = tid; i < NPM * ES; i += kFusedThreads) E[i] = 0.0;  // padding stays 0
         // the open tuple (kept identically by every thread): its index, weight, extra rows
         int open_tuple = -1, extra = 0;
@@ -755,9 +790,9 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
         __syncthreads();
         for (int base = 0; base < p.rays; base += kFusedThreads) {
             const int q = base + tid;
-            double* row = Y + tid;  // this ray's row, column c at row[c * TS]
-            for (int c = 0; c < NP; ++c) row[c * TS] = 0.0;
-            double* prow = pen_slot + tid;  // this ray's penalty row, column c at prow[c * T]
+            YT* row = Y + tid;  // this ray's row, column c at row[c * TS]
+            for (int c = 0; c < NP; ++c) row[c * TS] = YT(0);
+            YT* prow = pen_slot + tid;  // this ray's penalty row, column c at prow[c * T]
             int tu = -1, status = kMissed;
             bool has_pen = false;
             double pen_val = 0.0, opl_val = 0.0;
@@ -782,7 +817,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 const bool pen_sweep = has_pen && soft_first != kOk;
                 const double pfac = has_pen ? p.pscale[tu] * smp.root_weight : 0.0;
                 if (has_pen) {
-                    for (int c = 0; c < NP; ++c) prow[c * kFusedThreads] = 0.0;
+                    for (int c = 0; c < NP; ++c) prow[c * kFusedThreads] = YT(0);
                     pen_val = pfac * (is_soft(status) ? penalty : penalty + 1.0);
                 }
                 if (piston) opl_val = opl;
@@ -791,7 +826,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     if (piston || pen_sweep) {
                         const double so[2] = {piston ? 1.0 : 0.0, 0.0};
                         const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
-                        const RowSinks<2> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
+                        const RowSinks<2, YT> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
                         run_backward<N, 2>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
                                            sinks);
@@ -800,7 +835,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     if (piston || pen_sweep) {  // one row: its seed and its sink
                         const double so[1] = {piston ? 1.0 : 0.0};
                         const double sp[1] = {pen_sweep ? 1.0 : 0.0};
-                        const RowSinks<1> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
+                        const RowSinks<1, YT> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
                                                 {piston ? TS : kFusedThreads}};
                         run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
@@ -808,16 +843,16 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
-                    const RowSinks<1> s0{{1.0}, {row}, {TS}};
+                    const RowSinks<1, YT> s0{{1.0}, {row}, {TS}};
                     run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
-                    const RowSinks<1> s1{{pfac}, {prow}, {kFusedThreads}};
+                    const RowSinks<1, YT> s1{{pfac}, {prow}, {kFusedThreads}};
                     run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
                 }
             }
-            Rv[tid] = opl_val;
+            R[tid] = opl_val;
             const double wv = (q < p.rays && in_piston(status)) ? smp.weight : 0.0;
             sh.w[tid] = wv;
             sh.sw[tid] = sqrt(wv);
@@ -853,15 +888,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     const int k = pr / (P + 1), c = pr - k * (P + 1);
                     const int a = sh.seg_first[k0 + k];
                     const int n = sh.seg_first[k0 + k + 1] - a;
-                    const double* col = Y + c * TS + a;
+                    const YT* col = Y + c * TS + a;
+                    const double* rcol = R + a;
+                    const bool res = c == P;
+                    auto at = [&](int i) { return res ? rcol[i] : static_cast<double>(col[i]); };
                     const double* wr = sh.w + a;
                     double sw0 = 0.0, sw1 = 0.0, s0 = 0.0, s1 = 0.0;
                     int r = c % n;
                     int j = 0;
                     for (; j + 1 < n; j += 2) {
-                        const double wa = wr[r], ya = col[r];
+                        const double wa = wr[r], ya = at(r);
                         r = r + 1 == n ? 0 : r + 1;
-                        const double wb = wr[r], yb = col[r];
+                        const double wb = wr[r], yb = at(r);
                         r = r + 1 == n ? 0 : r + 1;
                         sw0 += wa;
                         s0 += wa * ya;
@@ -870,7 +908,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     }
                     if (j < n) {
                         sw0 += wr[r];
-                        s0 += wr[r] * col[r];
+                        s0 += wr[r] * at(r);
                     }
                     const double sw_sum = sw0 + sw1, sum = s0 + s1;
                     seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
@@ -883,10 +921,11 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     const double f = (seg_w[k] > 0.0 && sh.w[tid] > 0.0)
                                          ? p.scale[sh.tuple[tid]] * sh.sw[tid] : 0.0;
                     const double* m = seg_mean + k * NP;
-                    for (int c = 0; c <= P; ++c) {
-                        double* y = Y + c * TS + tid;
-                        *y = f != 0.0 ? f * (*y - m[c]) : 0.0;
+                    for (int c = 0; c < P; ++c) {
+                        YT* y = Y + c * TS + tid;
+                        *y = f != 0.0 ? YT(f * (static_cast<double>(*y) - m[c])) : YT(0);
                     }
+                    R[tid] = f != 0.0 ? f * (R[tid] - m[P]) : 0.0;
                 }
                 // B4: the segments merged into the open tuple in row order (threads = columns
                 // for the vectors; the scalar state is updated identically by every thread)
@@ -926,16 +965,16 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
                 for (int c = 0; c <= P; ++c) E[c * ES + r] = 0.0;
             __syncthreads();
-            accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+            accumulate_rows(Y, R, TS, P, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
             if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
             __syncthreads();
             extra = 0;
             // ---- D: penalty rows ----
             if (sh.any_pen) {
-                for (int c = 0; c < NP; ++c) row[c * TS] = has_pen ? prow[c * kFusedThreads] : 0.0;
-                Rv[tid] = pen_val;
+                for (int c = 0; c < NP; ++c) row[c * TS] = has_pen ? prow[c * kFusedThreads] : YT(0);
+                R[tid] = pen_val;
                 __syncthreads();
-                accumulate(Y, TS, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+                accumulate_rows(Y, R, TS, P, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
             }
             __syncthreads();
         }
@@ -956,13 +995,14 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
 
 }  // namespace
 
-size_t fused_adjoint_smem(const TraceParams& tp, int P) {
+size_t fused_adjoint_smem(const TraceParams& tp, int P, size_t row_bytes) {
     const int NP = fused_np(P);
     const int ncols = NP / 8;
     const int pairs = ncols * (ncols + 1) / 2;
+    const size_t rows = (static_cast<size_t>(kFusedThreads + 4) * NP * row_bytes + 7) / 8;
     return sizeof(double) * (static_cast<size_t>((tp.stride + 1) & ~1) +
-                             static_cast<size_t>(((tp.S + 1) * tp.L + 1) & ~1) +
-                             static_cast<size_t>(kFusedThreads + 4) * NP +
+                             static_cast<size_t>(((tp.S + 1) * tp.L + 1) & ~1) + rows +
+                             (kFusedThreads + 4) +
                              (kExtraRows + 4) * NP + NP + kSegBatch * (NP + 1) +
                              static_cast<size_t>(pairs) * 64);
 }
@@ -1008,7 +1048,8 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.vt = rv.table;
     fa.p_max = p_max;
     fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
-    const size_t smem = fused_adjoint_smem(tp, p_max);
+    const size_t smem = fused_adjoint_smem(
+        tp, p_max, precision == MKB_PRECISION_MIXED ? sizeof(float) : sizeof(double));
     auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
                   : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>
                                                      : adjoint_gram_kernel<double>;
