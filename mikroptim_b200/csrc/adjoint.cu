@@ -443,18 +443,24 @@ __device__ __forceinline__ void accumulate_rows(const YT* Y, const double* R, in
                                                 int pairs, const int2* tiles, double* acc) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
+    const int last = P >> 3;  // the column tile holding the residual column
     for (int e = warp; e < pairs; e += kFusedWarps) {
         const int col_a = tiles[e].x * 8 + gid, col_b = tiles[e].y * 8 + gid;
         const YT* ya = Y + col_a * ld + tig;
         const YT* yb = Y + col_b * ld + tig;
-        const double* r = R + tig;
-        const bool ra = col_a == P, rb = col_b == P;
         double* a = acc + (e * 32 + lane) * 2;
         double d0 = a[0], d1 = a[1];
-        for (int k0 = 0; k0 < n; k0 += 4) {
-            const double fa = ra ? r[k0] : static_cast<double>(ya[k0]);
-            const double fb = rb ? r[k0] : static_cast<double>(yb[k0]);
-            dmma(d0, d1, fa, fb);
+        if (tiles[e].y != last) {  // warp-uniform: no residual column in the pair
+            for (int k0 = 0; k0 < n; k0 += 4)
+                dmma(d0, d1, static_cast<double>(ya[k0]), static_cast<double>(yb[k0]));
+        } else {  // upper triangle: x <= y, so column tile x holds P only when x == y == last
+            const double* r = R + tig;
+            const bool ra = col_a == P, rb = col_b == P;
+            for (int k0 = 0; k0 < n; k0 += 4) {
+                const double fa = ra ? r[k0] : static_cast<double>(ya[k0]);
+                const double fb = rb ? r[k0] : static_cast<double>(yb[k0]);
+                dmma(d0, d1, fa, fb);
+            }
         }
         a[0] = d0;
         a[1] = d1;
@@ -880,39 +886,41 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             __syncthreads();
             for (int k0 = 0; k0 < nseg; k0 += kSegBatch) {
                 const int kn = nseg - k0 < kSegBatch ? nseg - k0 : kSegBatch;
-                // B2: weight and weighted column means of each segment, a thread per (segment,
-                // column) summing the segment's rows from row c mod n on: neighbouring columns
-                // (column stride 4 mod 16 doubles) then read bank pairs 5c + j mod 16, so the
-                // lanes of a half-warp never share one
-                for (int pr = tid; pr < kn * (P + 1); pr += kFusedThreads) {
-                    const int k = pr / (P + 1), c = pr - k * (P + 1);
-                    const int a = sh.seg_first[k0 + k];
-                    const int n = sh.seg_first[k0 + k + 1] - a;
-                    const YT* col = Y + c * TS + a;
-                    const double* rcol = R + a;
-                    const bool res = c == P;
-                    auto at = [&](int i) { return res ? rcol[i] : static_cast<double>(col[i]); };
-                    const double* wr = sh.w + a;
-                    double sw0 = 0.0, sw1 = 0.0, s0 = 0.0, s1 = 0.0;
-                    int r = c % n;
-                    int j = 0;
-                    for (; j + 1 < n; j += 2) {
-                        const double wa = wr[r], ya = at(r);
-                        r = r + 1 == n ? 0 : r + 1;
-                        const double wb = wr[r], yb = at(r);
-                        r = r + 1 == n ? 0 : r + 1;
-                        sw0 += wa;
-                        s0 += wa * ya;
-                        sw1 += wb;
-                        s1 += wb * yb;
+                // B2: weight and weighted column means of each segment, four lanes per
+                // (segment, column) taking rows h, h + 4, ... (h = lane mod 4) and a two-step
+                // shuffle sum. The eight columns of a warp and the four row phases then hit
+                // 32 different banks (column stride 4 mod 32 floats).
+                {
+                    const int h = lane & 3;
+                    const unsigned quad = 0xFu << (lane & ~3);
+                    for (int pr = tid >> 2; pr < kn * (P + 1); pr += kFusedThreads / 4) {
+                        const int k = pr / (P + 1), c = pr - k * (P + 1);
+                        const int a = sh.seg_first[k0 + k];
+                        const int n = sh.seg_first[k0 + k + 1] - a;
+                        const YT* col = Y + c * TS + a;
+                        const double* rcol = R + a;
+                        const double* wr = sh.w + a;
+                        double sw_sum = 0.0, sum = 0.0;
+                        if (c != P) {
+                            for (int r = h; r < n; r += 4) {
+                                sw_sum += wr[r];
+                                sum += wr[r] * static_cast<double>(col[r]);
+                            }
+                        } else {
+                            for (int r = h; r < n; r += 4) {
+                                sw_sum += wr[r];
+                                sum += wr[r] * rcol[r];
+                            }
+                        }
+                        sw_sum += __shfl_xor_sync(quad, sw_sum, 1);
+                        sum += __shfl_xor_sync(quad, sum, 1);
+                        sw_sum += __shfl_xor_sync(quad, sw_sum, 2);
+                        sum += __shfl_xor_sync(quad, sum, 2);
+                        if (h == 0) {
+                            seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
+                            if (c == 0) seg_w[k] = sw_sum;
+                        }
                     }
-                    if (j < n) {
-                        sw0 += wr[r];
-                        s0 += wr[r] * at(r);
-                    }
-                    const double sw_sum = sw0 + sw1, sum = s0 + s1;
-                    seg_mean[k * NP + c] = sw_sum > 0.0 ? sum / sw_sum : 0.0;
-                    if (c == 0) seg_w[k] = sw_sum;
                 }
                 __syncthreads();
                 // B3: every row of the batch's segments centred and scaled by its own thread
