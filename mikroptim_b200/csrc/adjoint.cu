@@ -397,14 +397,17 @@ constexpr int kSegBatch = 8;             // tuple segments whose means are held 
 // columns of a row: the P derivatives, the residual in column P, zero padding to 8
 __host__ __device__ inline int fused_np(int P) { return ((P + 1 + 7) / 8) * 8; }
 
+// tuple (f-major, then l) of ray q of a run
+__device__ __forceinline__ int tuple_of(const TraceParams& p, int q) {
+    int f = 0;
+    while (f + 1 < p.F && q >= p.field_offset[f + 1]) ++f;
+    return f * p.L + (q - p.field_offset[f]) / p.sample_count[f];
+}
+
 struct FusedShared {
     uint64_t bar;
     SharedTables tab;
     double w[kFusedThreads];      // sample weight if the ray is in the piston, else 0
-    double sw[kFusedThreads];     // sqrt of w
-    int tuple[kFusedThreads];     // tuple of the ray (-1 past the end)
-    int seg_first[kFusedThreads + 1];  // first row of every tuple segment of the chunk (+ end)
-    int warp_starts[kFusedWarps];      // segments starting in each warp
     int any_pen;                  // chunk has a penalty row (soft mode)
     int run;                      // run taken off the queue
     int2 tiles[kMaxTilePairs];    // (row tile, column tile) of every upper-triangle pair
@@ -860,30 +863,27 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
             }
             R[tid] = opl_val;
             const double wv = (q < p.rays && in_piston(status)) ? smp.weight : 0.0;
+            const double swv = sqrt(wv);
             sh.w[tid] = wv;
-            sh.sw[tid] = sqrt(wv);
-            sh.tuple[tid] = tu;
             if (tid == 0) sh.any_pen = 0;
             __syncthreads();
             if (has_pen) sh.any_pen = 1;
             // ---- B: centre every tuple segment of the chunk ----
             const int rows_here = p.rays - base < kFusedThreads ? p.rays - base : kFusedThreads;
-            // B1: segments are the maximal runs of rows of one tuple; a ballot prefix gives
-            // every row its segment and every segment its first row
-            const bool starts = tid < rows_here && (tid == 0 || sh.tuple[tid] != sh.tuple[tid - 1]);
-            const unsigned ball = __ballot_sync(0xffffffffu, starts);
-            if (lane == 0) sh.warp_starts[warp] = __popc(ball);
-            __syncthreads();
-            int before = 0, nseg = 0;
-#pragma unroll
-            for (int w = 0; w < kFusedWarps; ++w) {
-                before += w < warp ? sh.warp_starts[w] : 0;
-                nseg += sh.warp_starts[w];
-            }
-            const int seg = before + __popc(ball & (0xffffffffu >> (31 - lane))) - 1;
-            if (starts) sh.seg_first[seg] = tid;
-            if (tid == 0) sh.seg_first[nseg] = rows_here;
-            __syncthreads();
+            // Segments are the chunk's pieces of its tuples; rays are ordered by tuple (f-major,
+            // then l), so segment k is tuple t0 + k and its rows follow from the plan alone.
+            const int t0 = tuple_of(p, base);
+            const int nseg = tuple_of(p, base + rows_here - 1) - t0 + 1;
+            const int seg = tid < rows_here ? tu - t0 : -1;
+            auto seg_rows = [&](int k, int& a, int& n) {
+                const int t = t0 + k;
+                const int f = t / p.L;
+                const int start = p.field_offset[f] + (t - f * p.L) * p.sample_count[f] - base;
+                a = start > 0 ? start : 0;
+                const int end = start + p.sample_count[f];
+                n = (end < rows_here ? end : rows_here) - a;
+                if (n < 0) n = 0;
+            };
             for (int k0 = 0; k0 < nseg; k0 += kSegBatch) {
                 const int kn = nseg - k0 < kSegBatch ? nseg - k0 : kSegBatch;
                 // B2: weight and weighted column means of each segment, four lanes per
@@ -895,8 +895,8 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                     const unsigned quad = 0xFu << (lane & ~3);
                     for (int pr = tid >> 2; pr < kn * (P + 1); pr += kFusedThreads / 4) {
                         const int k = pr / (P + 1), c = pr - k * (P + 1);
-                        const int a = sh.seg_first[k0 + k];
-                        const int n = sh.seg_first[k0 + k + 1] - a;
+                        int a, n;
+                        seg_rows(k0 + k, a, n);
                         const YT* col = Y + c * TS + a;
                         const double* rcol = R + a;
                         const double* wr = sh.w + a;
@@ -924,10 +924,9 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 }
                 __syncthreads();
                 // B3: every row of the batch's segments centred and scaled by its own thread
-                if (tid < rows_here && seg >= k0 && seg < k0 + kn) {
+                if (seg >= k0 && seg < k0 + kn) {
                     const int k = seg - k0;
-                    const double f = (seg_w[k] > 0.0 && sh.w[tid] > 0.0)
-                                         ? p.scale[sh.tuple[tid]] * sh.sw[tid] : 0.0;
+                    const double f = (seg_w[k] > 0.0 && wv > 0.0) ? p.scale[tu] * swv : 0.0;
                     const double* m = seg_mean + k * NP;
                     for (int c = 0; c < P; ++c) {
                         YT* y = Y + c * TS + tid;
@@ -940,7 +939,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 for (int k = 0; k < kn; ++k) {
                     const double ws = seg_w[k];
                     if (!(ws > 0.0)) continue;
-                    const int t = sh.tuple[sh.seg_first[k0 + k]];
+                    const int t = t0 + k0 + k;
                     const bool open = open_tuple == t && open_w > 0.0;
                     if (tid <= P) {
                         const double mean = seg_mean[k * NP + tid];
@@ -966,15 +965,15 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         extra = 0;
                     }
                 }
+                // zero padding of the pending extra rows to a multiple of 4 (each column by
+                // the thread that writes it)
+                if (tid <= P)
+                    for (int r = extra; r < ((extra + 3) & ~3); ++r) E[tid * ES + r] = 0.0;
                 __syncthreads();
             }
             // ---- C: the centred rows and the pending extra rows ----
-            const int ne = extra;
-            for (int r = ne + tid; r < ((ne + 3) & ~3); r += kFusedThreads)
-                for (int c = 0; c <= P; ++c) E[c * ES + r] = 0.0;
-            __syncthreads();
             accumulate_rows(Y, R, TS, P, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
-            if (ne > 0) accumulate(E, ES, (ne + 3) & ~3, pairs, sh.tiles, acc);
+            if (extra > 0) accumulate(E, ES, (extra + 3) & ~3, pairs, sh.tiles, acc);
             __syncthreads();
             extra = 0;
             // ---- D: penalty rows ----
@@ -983,8 +982,8 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 R[tid] = pen_val;
                 __syncthreads();
                 accumulate_rows(Y, R, TS, P, (rows_here + 3) & ~3, pairs, sh.tiles, acc);
+                __syncthreads();
             }
-            __syncthreads();
         }
         // ---- write the (P+1) x (P+1) symmetric gram ----
         const int n = P + 1;
