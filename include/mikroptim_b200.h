@@ -85,16 +85,31 @@ typedef struct mkb_batch_view {
     const double* pupil_radius;       /* [V]                                            */
     const double* field_angle;        /* [V][F] radians                                 */
     const double* field_target;       /* [V][F] ideal image height h_f (mm)             */
+    /* Non-coaxial batches (BatchTopology::non_coaxial, system_batch.hpp:45): per surface the
+     * decenter dx, dy (mm) and the tilts alpha about the local x axis and beta about the local
+     * y axis (radians, |.| < pi/2), [V][S][4], rotation R = R_y(beta) R_x(alpha) about the
+     * vertex (trace/surface_transform.hpp:8-14). NULL: coaxial. A non-coaxial batch traces
+     * Full pupils only. */
+    const double* decenter_tilt;
+    /* Ghost plates (surfaces of kind MKB_SURFACE_GHOST_PLATE, numbered in table order): the
+     * Legendre profile coefficients a_1..a_K [V][G][K] (mm), the normalisation radius r_g
+     * [V][G] (mm) and the plate's glass index [V][G][L] (trace/ghost_plate.hpp:24). NULL when
+     * ghost_plates = 0. */
+    const double* ghost_coeff;
+    const double* ghost_norm_radius;
+    const double* ghost_index;
 } mkb_batch_view;
 
 /* The device-resident batch: one 16-byte aligned record of `record_stride` doubles per
  * variant (so that a CTA stages its variant with one bulk copy), plus the shared arrays.
  * Record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
- * sin(field_angle)[F] | cos(field_angle)[F] | field_target[F] | padding. */
+ * sin(field_angle)[F] | cos(field_angle)[F] | field_target[F] | [non-coaxial: per surface
+ * dx, dy, cos alpha, sin alpha, cos beta, sin beta, moved, 0] | [ghost plates:
+ * coefficients [G][K] | normalisation radius [G] | index [G][L]] | padding. */
 typedef struct mkb_device_batch {
     int32_t variants, surfaces, wavelengths, fields;
     int32_t record_stride;            /* doubles per variant, even                      */
-    int32_t reserved;
+    int32_t non_coaxial;              /* 1: the records carry per-surface transforms     */
     const double* records;            /* device [V][record_stride], 16-byte aligned     */
     const uint8_t* type;              /* host [S] (copied into the kernel parameters)   */
     const uint8_t* variant_surfaces;  /* device [V] or NULL: table surfaces each variant
@@ -102,13 +117,20 @@ typedef struct mkb_device_batch {
                                          surfaces are 0 .. n-1 of the shared table, its
                                          working distance is thickness[n-1], the entries
                                          past n are ignored. NULL: every variant uses S. */
+    int32_t ghost_plates, ghost_terms;  /* G, K: the records carry the plates' data       */
 } mkb_device_batch;
 
-/* Doubles per packed variant record for a batch shape (>= 2, even). */
+/* Doubles per packed variant record for a coaxial batch shape without ghost plates (>= 2,
+ * even). */
 int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields);
 
-/* Packs a host SoA view into host records [V][record_stride] (sin/cos of the field angles
- * are taken here with the host libm, so the start rays are those of the CPU reference). */
+/* Doubles per packed variant record for any batch shape. */
+int32_t mkb_record_stride_ext(int32_t surfaces, int32_t wavelengths, int32_t fields,
+                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms);
+
+/* Packs a host SoA view into host records [V][mkb_record_stride_ext(...)] (sin/cos of the
+ * field angles and of the tilts are taken here with the host libm, so the start rays and the
+ * surface transforms are those of the CPU reference). */
 int mkb_pack_batch_host(const mkb_batch_view* view, double* records);
 
 /* The LM variables (VariableSet, include/mikroptim/optim/variable_set.hpp:63): curvature,

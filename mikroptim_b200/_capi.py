@@ -43,6 +43,10 @@ class BatchView(C.Structure):
         ("pupil_radius", P_double),
         ("field_angle", P_double),
         ("field_target", P_double),
+        ("decenter_tilt", P_double),
+        ("ghost_coeff", P_double),
+        ("ghost_norm_radius", P_double),
+        ("ghost_index", P_double),
     ]
 
 
@@ -51,10 +55,11 @@ class DeviceBatch(C.Structure):
 
     _fields_ = [
         ("variants", C.c_int32), ("surfaces", C.c_int32), ("wavelengths", C.c_int32),
-        ("fields", C.c_int32), ("record_stride", C.c_int32), ("reserved", C.c_int32),
+        ("fields", C.c_int32), ("record_stride", C.c_int32), ("non_coaxial", C.c_int32),
         ("records", C.c_void_p),
         ("type", P_uint8),
         ("variant_surfaces", C.c_void_p),
+        ("ghost_plates", C.c_int32), ("ghost_terms", C.c_int32),
     ]
 
 
@@ -112,6 +117,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_launch_count.restype = c.c_int64
     lib.mkb_record_stride.restype = c.c_int32
     lib.mkb_record_stride.argtypes = [c.c_int32, c.c_int32, c.c_int32]
+    lib.mkb_record_stride_ext.restype = c.c_int32
+    lib.mkb_record_stride_ext.argtypes = [c.c_int32] * 6
     lib.mkb_pack_batch_host.restype = c.c_int
     lib.mkb_pack_batch_host.argtypes = [C.POINTER(BatchView), P_double]
     lib.mkb_rays_per_variant.restype = c.c_int64

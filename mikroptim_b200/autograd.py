@@ -51,6 +51,7 @@ class AdjointProblem:
         out = DeviceSystemBatch.__new__(DeviceSystemBatch)
         out.device, out.topology, out.variants = self.device, self.templates.topology, runs
         out.stride, out.type = self.templates.stride, self.templates.type
+        out.non_coaxial = self.templates.non_coaxial
         out.variant_surfaces = None
         out.records = torch.empty((max(runs, 1), out.stride), dtype=torch.float64,
                                   device=self.device)

@@ -1,7 +1,7 @@
 """Host-side batch model mirroring the reference's SystemBatch API.
 
 Names and meaning follow the reference:
-  BatchTopology      include/mikroptim/batch/system_batch.hpp:229
+  BatchTopology      include/mikroptim/batch/system_batch.hpp:229 (non_coaxial: :45)
   SystemBatchHost    include/mikroptim/batch/system_batch.hpp:268 (FP64 SoA, variant-major)
   ResidualSettings   include/mikroptim/batch/batch_residuals.hpp:24
   ResidualLayout     include/mikroptim/batch/batch_residuals.hpp:62 (src/batch/batch_residuals.cpp:25)
@@ -55,6 +55,9 @@ class BatchTopology:
     fields: int
     type: list[int]
     pupil_mode: list[int]
+    # per-surface decenter and tilt (decenter_tilt [V][S][4]); every field then uses the
+    # Full pupil (check_pupil_modes, src/batch/system_batch.cpp:158)
+    non_coaxial: bool = False
 
     def validate(self) -> None:
         if not 2 <= self.surfaces <= MAX_SURFACES:
@@ -79,6 +82,9 @@ class BatchTopology:
         for m in self.pupil_mode:
             if m not in (PUPIL_HALF, PUPIL_FULL, PUPIL_AXIS):
                 raise ValueError("BatchTopology: unknown pupil mode")
+            if self.non_coaxial and m != PUPIL_FULL:
+                raise ValueError("BatchTopology: a non-coaxial batch needs the Full pupil in "
+                                 "every field")
 
 
 class SystemBatchHost:
@@ -101,6 +107,10 @@ class SystemBatchHost:
         self.pupil_radius = np.zeros(variants)
         self.field_angle = np.zeros((variants, F))
         self.field_target = np.zeros((variants, F))
+        # non-coaxial batches: (dx, dy, alpha, beta) per surface, decenter in mm and tilts in
+        # radians (SystemBatchHost::decenter_tilt, system_batch.hpp:156); None when coaxial
+        self.decenter_tilt: np.ndarray | None = (np.zeros((variants, S, 4))
+                                                 if topology.non_coaxial else None)
         # uneven batches: table surfaces each variant uses (2 .. S); None = all use S
         self.variant_surfaces: np.ndarray | None = None
 
@@ -134,6 +144,8 @@ class SystemBatchHost:
         for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
                      "field_target"):
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[sl]))
+        if self.decenter_tilt is not None:
+            out.decenter_tilt = np.ascontiguousarray(self.decenter_tilt[sl])
         if self.variant_surfaces is not None:
             out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[sl])
         return out
@@ -145,18 +157,38 @@ class SystemBatchHost:
         for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
                      "field_target"):
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
+        if self.decenter_tilt is not None:
+            out.decenter_tilt = np.ascontiguousarray(self.decenter_tilt[idx])
         if self.variant_surfaces is not None:
             out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[idx])
         return out
 
+    def set_decenter_tilt(self, v: int, s: int, dx: float, dy: float, alpha: float,
+                          beta: float) -> None:
+        """SystemBatchHost::set_decenter_tilt (src/batch/system_batch.cpp:510)."""
+        if self.decenter_tilt is None:
+            raise ValueError("SystemBatchHost: decenter and tilt need a non-coaxial batch "
+                             "(make_non_coaxial)")
+        if not (0 <= v < self.variants and 0 <= s < self.surfaces):
+            raise IndexError("SystemBatchHost.set_decenter_tilt: index out of range")
+        self.decenter_tilt[v, s] = (dx, dy, alpha, beta)
+
     def validate_values(self) -> None:
         """validate_values (src/batch/system_batch.cpp:558) for the fields traced here."""
-        for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
-                     "field_target", "wavelength_weight", "field_weight"):
+        names = ["curvature", "thickness", "index", "pupil_radius", "field_angle",
+                 "field_target", "wavelength_weight", "field_weight"]
+        if self.decenter_tilt is not None:
+            names.append("decenter_tilt")
+        for name in names:
             a = getattr(self, name)
             if not np.all(np.isfinite(a)):
                 bad = np.argwhere(~np.isfinite(a))[0]
                 raise ValueError(f"SystemBatchHost: {name}{list(bad)} is not finite")
+        if self.decenter_tilt is not None:
+            if self.decenter_tilt.shape != (self.variants, self.surfaces, 4):
+                raise ValueError("SystemBatchHost: decenter_tilt must be [V][S][4]")
+            if not np.all(np.abs(self.decenter_tilt[:, :, 2:]) < math.pi / 2):
+                raise ValueError("SystemBatchHost: tilt angles must be in (-pi/2, pi/2)")
         if np.any(self.pupil_radius <= 0):
             raise ValueError("SystemBatchHost: pupil radius must be > 0")
         if np.any(self.index <= 0):
@@ -195,8 +227,35 @@ class SystemBatchHost:
         for name in ("wavelength_weight", "field_weight", "curvature", "thickness", "index",
                      "pupil_radius", "field_angle", "field_target"):
             setattr(v, name, _capi.ptr(arrays[name]))
+        if self.decenter_tilt is not None:
+            dt = np.ascontiguousarray(self.decenter_tilt, dtype=np.float64)
+            arrays["decenter_tilt"] = dt
+            v.decenter_tilt = _capi.ptr(dt)
         v._keep = arrays  # keep the arrays alive with the struct
         return v
+
+    @property
+    def non_coaxial(self) -> bool:
+        return self.decenter_tilt is not None
+
+
+def make_non_coaxial(batch: SystemBatchHost) -> SystemBatchHost:
+    """Copy of `batch` with a non-coaxial topology: decenter and tilt all zero, every field on
+    the Full pupil (make_non_coaxial, src/batch/system_batch.cpp)."""
+    t = batch.topology
+    topo = BatchTopology(t.surfaces, t.wavelengths, t.fields, list(t.type),
+                         [PUPIL_FULL] * t.fields, non_coaxial=True)
+    out = SystemBatchHost(topo, batch.variants)
+    out.reference_wavelength_nm = batch.reference_wavelength_nm
+    out.wavelength_nm = batch.wavelength_nm.copy()
+    out.wavelength_weight = batch.wavelength_weight.copy()
+    out.field_weight = batch.field_weight.copy()
+    for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                 "field_target"):
+        setattr(out, name, np.array(getattr(batch, name), copy=True))
+    if batch.variant_surfaces is not None:
+        out.variant_surfaces = np.array(batch.variant_surfaces, copy=True)
+    return out
 
 
 @dataclass

@@ -33,13 +33,12 @@ struct AdjointParams {
     int64_t rows;  // R = trace rows per run (J column length)
 };
 
+// the variant's record is the kernel's dynamic shared memory (16-byte aligned, stride doubles)
 struct alignas(16) SharedAdj {
-    double record[2 * kMaxSurfaces + kMaxSurfaces * MKB_MAX_WAVELENGTHS + 1 + 3 * kMaxFields + 1];
     uint64_t bar;
     SharedTables tab;
     int tuple_start[kMaxPackTuples + 1];
 };
-static_assert(offsetof(SharedAdj, record) % 16 == 0, "bulk-copy destination alignment");
 
 // Forward record of one ray: checkpoints of (p, d) after surfaces 0, K, 2K, ... and the
 // branch code of every surface (2 bits, 64 surfaces in 128 bits).
@@ -96,7 +95,8 @@ __device__ int forward_record(const TraceParams& p, const double* rec, const Rec
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
-        status = step_surface<N>(r, N(thick[s - 1]), c, n_before, n_after, sp, branch);
+        status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, n_before / n_after,
+                                    xf_of(rec, lay, s), sp, branch);
         if (status != kOk) break;
         out.count = s + 1;
         out.set_branch(s, branch);
@@ -160,8 +160,9 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                 const int s = first + i;
                 const N cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
                 int branch;
-                step_surface<N>(r, N(thick[s - 1]), cs, N(idx[(s - 1) * L + l]),
-                                N(idx[s * L + l]), soft_mode ? &dummy : nullptr, branch);
+                const N nb = idx[(s - 1) * L + l], na = idx[s * L + l];
+                step_surface_xf<N>(r, N(thick[s - 1]), cs, nb, nb / na, xf_of(rec, lay, s),
+                                   soft_mode ? &dummy : nullptr, branch);
                 sp[i] = {r.px, r.py, r.pz};
                 sd[i] = {r.dx, r.dy, r.dz};
             }
@@ -186,9 +187,24 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                     const bool sphere = p.type[j] == MKB_SURFACE_SPHERE;
                     const N cj = sphere ? curv[j] : 0.0;
                     StepAdj<N> par{zero, zero, zero, zero};
-                    refracting_step_backward<N>(sp[i], sd[i], N(thick[s]), cj,
-                                                N(idx[s * L + l]), N(idx[j * L + l]),
-                                                next_branch, seed_opl, seed_pen, adj, par);
+                    const double* xf = xf_of(rec, lay, j);
+                    const bool moved = xf != nullptr && xf[6] > 0.0;
+                    Vec<N> pl = sp[i], dl = sd[i];
+                    N tl = thick[s];
+                    Transform<N> tr{};
+                    if (moved) {
+                        tr = transform_at<N>(xf);
+                        state_to_surface(tr, pl, dl, tl);
+                        tl = zero;
+                        adjoint_to_surface(tr, adj);
+                    }
+                    refracting_step_backward<N>(pl, dl, tl, cj, N(idx[s * L + l]),
+                                                N(idx[j * L + l]), next_branch, seed_opl,
+                                                seed_pen, adj, par);
+                    if (moved) {
+                        adjoint_from_surface(tr, adj);
+                        par.thickness = -adj.p.z;
+                    }
                     if (sphere) write(v.col_curvature[j], par.curvature);
                     write(v.col_thickness[s], par.thickness);
                 }
@@ -208,7 +224,7 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
     const int v = blockIdx.x / p.n_packs;
     const int pk = blockIdx.x - v * p.n_packs;
     const Pack pack = p.packs[pk];
-    const RecordLayout lay = record_layout(p.S, p.L, p.F);
+    const RecordLayout lay = layout_of(p);
     if (threadIdx.x <= pack.tuples) {
         int start = 0;
         for (int t = 0; t < static_cast<int>(threadIdx.x); ++t)
@@ -216,7 +232,8 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         sh.tuple_start[threadIdx.x] = start;
     }
     copy_tables(p, sh.tab);
-    if (!stage_to_shared(sh.record, records + static_cast<int64_t>(v) * p.stride,
+    extern __shared__ __align__(16) double record[];
+    if (!stage_to_shared(record, records + static_cast<int64_t>(v) * p.stride,
                          static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar))
         return;
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
@@ -231,15 +248,15 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         Record<N> ck;
         int soft_first;
-        const int st = forward_record<N>(p, sh.record, lay, f, l, smp, soft_mode, ck, soft_first);
+        const int st = forward_record<N>(p, record, lay, f, l, smp, soft_mode, ck, soft_first);
         const int64_t row = p.field_offset[f] + static_cast<int64_t>(l) * p.sample_count[f] + k;
         const bool reached = in_piston(st);
         if (reached)
-            backward_sweep<N>(p, ap.v, sh.record, lay, f, l, ck, true, soft_mode, N(1.0), N(0.0),
+            backward_sweep<N>(p, ap.v, record, lay, f, l, ck, true, soft_mode, N(1.0), N(0.0),
                               N(1.0), col0, ap.rows, row);
         if (soft_mode && soft_first != kOk) {
             const N factor = N(p.pscale[tu]) * N(smp.root_weight);
-            backward_sweep<N>(p, ap.v, sh.record, lay, f, l, ck, reached, soft_mode, N(0.0),
+            backward_sweep<N>(p, ap.v, record, lay, f, l, ck, reached, soft_mode, N(0.0),
                               N(1.0), factor, col0, ap.rows, p.rays + row);
         }
     }
@@ -326,10 +343,12 @@ int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows
     ap.v = vp;
     ap.rows = rows;
     const int64_t blocks = static_cast<int64_t>(tp.V) * tp.n_packs;
-    if (exact)
-        adjoint_rows_kernel<true><<<static_cast<unsigned>(blocks), kAdjThreads, 0, stream>>>(ap, records, J);
-    else
-        adjoint_rows_kernel<false><<<static_cast<unsigned>(blocks), kAdjThreads, 0, stream>>>(ap, records, J);
+    const size_t smem = static_cast<size_t>(tp.stride) * sizeof(double);
+    auto kernel = exact ? adjoint_rows_kernel<true> : adjoint_rows_kernel<false>;
+    const cudaError_t err = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (err != cudaSuccess) return cuda_status(err, "adjoint rows: shared memory attribute");
+    kernel<<<static_cast<unsigned>(blocks), kAdjThreads, smem, stream>>>(ap, records, J);
     count_launch();
     return cuda_status(cudaGetLastError(), "adjoint rows launch");
 }
@@ -524,8 +543,8 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
         keep_state(q);
         int branch;
         StepLocal<N> loc{zero, zero, zero, zero, zero};
-        status = step_surface_mu<N, true>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
-                                          sp, branch, &loc);
+        status = step_surface_xf<N, true>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
+                                          xf_of(rec, lay, s), sp, branch, &loc);
         if (status != kOk) break;
         q[6 * kFusedThreads] = Q(value_of(loc.s0));
         q[7 * kFusedThreads] = Q(value_of(loc.s));
@@ -638,9 +657,28 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
             StepAdj<A> par[K];
 #pragma unroll
             for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
-            refracting_step_backward_k<N, A, K>(cur.p, cur.d, N(thick[c]), cj, N(idx[c * L + l]),
-                                                N(idx[j * L + l]), next_branch, seed_opl,
-                                                seed_pen, adj, par, &cur.loc);
+            const double* xf = xf_of(rec, lay, j);
+            if (xf != nullptr && xf[6] > 0.0) {  // decentered / tilted surface
+                const Transform<N> tn = transform_at<N>(xf);
+                const Transform<A> ta = transform_at<A>(xf);
+                Vec<N> pl = cur.p, dl = cur.d;
+                state_to_surface(tn, pl, dl, N(thick[c]));
+#pragma unroll
+                for (int m = 0; m < K; ++m) adjoint_to_surface(ta, adj[m]);
+                refracting_step_backward_k<N, A, K>(pl, dl, zero, cj, N(idx[c * L + l]),
+                                                    N(idx[j * L + l]), next_branch, seed_opl,
+                                                    seed_pen, adj, par, &cur.loc);
+#pragma unroll
+                for (int m = 0; m < K; ++m) {
+                    adjoint_from_surface(ta, adj[m]);
+                    par[m].thickness = -adj[m].p.z;
+                }
+            } else {
+                refracting_step_backward_k<N, A, K>(cur.p, cur.d, N(thick[c]), cj,
+                                                    N(idx[c * L + l]), N(idx[j * L + l]),
+                                                    next_branch, seed_opl, seed_pen, adj, par,
+                                                    &cur.loc);
+            }
             const int cc = sphere ? v.col_curvature[j] : -1;
             const int ct = v.col_thickness[c];
 #pragma unroll
@@ -739,7 +777,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     double* seg_w = seg_mean + kSegBatch * NPM;        // [kSegBatch] segment weights
     double* acc = seg_w + kSegBatch;                   // [pairs][32][2] DMMA accumulators
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const RecordLayout lay = record_layout(p.S, p.L, p.F);
+    const RecordLayout lay = layout_of(p);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     // this CTA's scratch slot: penalty rows [NPM][T], then per surface [kSlotDoubles][T]
     using Keep = typename FusedTypes<N>::Keep;

@@ -46,6 +46,31 @@ __device__ __forceinline__ A cv(N x) { return A(value_of(x)); }
 template <class A, class N>
 __device__ __forceinline__ Vec<A> cv(Vec<N> v) { return {cv<A>(v.x), cv<A>(v.y), cv<A>(v.z)}; }
 
+// Decentered and tilted surfaces (backward_ray, trace/adjoint_backward.hpp:539-569): the step
+// is differentiated in the surface's tilted frame, with the entering state
+// R^T (p - t e_z - D), R^T d and a transfer by 0; the adjoints of the leaving state are turned
+// in with R^T and those of the entering state back with R, and t-bar = -p-bar_z.
+template <class N>
+__device__ __forceinline__ void state_to_surface(const Transform<N>& t, Vec<N>& p, Vec<N>& d,
+                                                 N thickness) {
+    N x = p.x - t.dx, y = p.y - t.dy, z = p.z - thickness;
+    rotate_to(t, x, y, z);
+    p = {x, y, z};
+    rotate_to(t, d.x, d.y, d.z);
+}
+
+template <class A>
+__device__ __forceinline__ void adjoint_to_surface(const Transform<A>& t, RayAdj<A>& a) {
+    rotate_to(t, a.p.x, a.p.y, a.p.z);
+    rotate_to(t, a.d.x, a.d.y, a.d.z);
+}
+
+template <class A>
+__device__ __forceinline__ void adjoint_from_surface(const Transform<A>& t, RayAdj<A>& a) {
+    rotate_from(t, a.p.x, a.p.y, a.p.z);
+    rotate_from(t, a.d.x, a.d.y, a.d.z);
+}
+
 // A divisor of the adjoint arithmetic. FP32 (the mixed sweep): the SFU reciprocal, taken once
 // per step and shared by the K seeds, and a multiply -- a few ulp of single precision, inside
 // that sweep's rounding budget. FP64: the rounded division in the reference's order, so the

@@ -131,12 +131,29 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         set_error("variants must be >= 0");
         return MKB_ERR_ARGUMENT;
     }
-    const RecordLayout lay = record_layout(S, L, F);
+    if (batch->non_coaxial != 0 && batch->non_coaxial != 1) {
+        set_error("non_coaxial must be 0 or 1");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (batch->ghost_plates < 0 || batch->ghost_terms < 0 ||
+        batch->ghost_plates > kMaxSurfaces || batch->ghost_terms > kMaxGhostTerms) {
+        set_error("ghost plates (G=%d, K=%d) out of range [0, %d] x [0, %d]",
+                  batch->ghost_plates, batch->ghost_terms, kMaxSurfaces, kMaxGhostTerms);
+        return MKB_ERR_ARGUMENT;
+    }
+    const RecordLayout lay = record_layout(S, L, F, batch->non_coaxial, batch->ghost_plates,
+                                           batch->ghost_terms);
     if (batch->record_stride != lay.stride) {
         set_error("record_stride %d does not match the shape (expected %d)",
                   batch->record_stride, lay.stride);
         return MKB_ERR_ARGUMENT;
     }
+    if (batch->non_coaxial)
+        for (int f = 0; f < F; ++f)
+            if (plan->pupil_mode[f] != MKB_PUPIL_FULL) {
+                set_error("a non-coaxial batch traces Full pupils only (field %d)", f);
+                return MKB_ERR_ARGUMENT;
+            }
     if (batch->variants > 0 && (batch->records == nullptr ||
                                 (reinterpret_cast<uintptr_t>(batch->records) & 15u) != 0)) {
         set_error("records must be a 16-byte aligned device pointer");
@@ -166,6 +183,9 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     std::memset(&p, 0, sizeof(p));
     p.V = batch->variants;
     p.S = S;
+    p.non_coaxial = batch->non_coaxial;
+    p.G = batch->ghost_plates;
+    p.K = batch->ghost_terms;
     p.vsurf = batch->variant_surfaces;
     p.order = nullptr;
     p.L = L;
@@ -319,6 +339,13 @@ int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields)
     return record_layout(surfaces, wavelengths, fields).stride;
 }
 
+int32_t mkb_record_stride_ext(int32_t surfaces, int32_t wavelengths, int32_t fields,
+                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms) {
+    return record_layout(surfaces, wavelengths, fields, non_coaxial ? 1 : 0,
+                         ghost_plates > 0 ? ghost_plates : 0,
+                         ghost_plates > 0 && ghost_terms > 0 ? ghost_terms : 0).stride;
+}
+
 int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
     if (v == nullptr || records == nullptr) {
         set_error("pack: null argument");
@@ -330,7 +357,14 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
         set_error("pack: shape out of range (S=%d, L=%d, F=%d)", S, L, F);
         return MKB_ERR_ARGUMENT;
     }
-    const RecordLayout lay = record_layout(S, L, F);
+    const int G = v->ghost_plates, K = v->ghost_terms;
+    if (G < 0 || K < 0 || G > kMaxSurfaces || K > kMaxGhostTerms ||
+        (G > 0 && (!v->ghost_coeff || !v->ghost_norm_radius || !v->ghost_index))) {
+        set_error("pack: ghost plates (G=%d, K=%d) out of range or without data", G, K);
+        return MKB_ERR_ARGUMENT;
+    }
+    const int non_coaxial = v->decenter_tilt != nullptr ? 1 : 0;
+    const RecordLayout lay = record_layout(S, L, F, non_coaxial, G, K);
     for (int64_t i = 0; i < v->variants; ++i) {
         double* r = records + i * lay.stride;
         std::memset(r, 0, sizeof(double) * lay.stride);
@@ -346,6 +380,30 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
             r[lay.sin_theta + f] = std::sin(th);
             r[lay.cos_theta + f] = std::cos(th);
             r[lay.target + f] = v->field_target[i * F + f];
+        }
+        // surface transforms (surface_transform_of, trace/surface_transform.hpp:99): a surface
+        // whose four values are all zero is traced coaxially; otherwise the tilt sines and
+        // cosines are taken with the host libm, as the CPU tracer takes them
+        for (int s = 0; non_coaxial && s < S; ++s) {
+            const double* t = v->decenter_tilt + (i * S + s) * 4;
+            double* x = r + lay.xf + s * kXfValues;
+            auto zero = [](double a) { return !(a > 0.0) && !(a < 0.0); };
+            const bool moved = !(zero(t[0]) && zero(t[1]) && zero(t[2]) && zero(t[3]));
+            x[0] = moved ? t[0] : 0.0;
+            x[1] = moved ? t[1] : 0.0;
+            x[2] = moved ? std::cos(t[2]) : 1.0;
+            x[3] = moved ? std::sin(t[2]) : 0.0;
+            x[4] = moved ? std::cos(t[3]) : 1.0;
+            x[5] = moved ? std::sin(t[3]) : 0.0;
+            x[6] = moved ? 1.0 : 0.0;
+            x[7] = 0.0;
+        }
+        for (int g = 0; g < G; ++g) {
+            for (int k = 0; k < K; ++k)
+                r[lay.ghost_coeff + g * K + k] = v->ghost_coeff[(i * G + g) * K + k];
+            r[lay.ghost_radius + g] = v->ghost_norm_radius[i * G + g];
+            for (int l = 0; l < L; ++l)
+                r[lay.ghost_index + g * L + l] = v->ghost_index[(i * G + g) * L + l];
         }
     }
     return MKB_OK;
@@ -370,7 +428,8 @@ int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_vari
         set_error("apply: shape out of range (S=%d, L=%d, F=%d)", S, L, F);
         return MKB_ERR_ARGUMENT;
     }
-    const RecordLayout lay = record_layout(S, L, F);
+    const RecordLayout lay = record_layout(S, L, F, templates->non_coaxial != 0,
+                                           templates->ghost_plates, templates->ghost_terms);
     if (templates->record_stride != lay.stride ||
         (reinterpret_cast<uintptr_t>(records_out) & 15u) != 0) {
         set_error("apply: record stride %d (expected %d) or unaligned output",

@@ -18,6 +18,7 @@ constexpr int kMaxFields = MKB_MAX_FIELDS;
 constexpr int kMaxTuples = MKB_MAX_TUPLES;
 constexpr int kMaxPacks = 256;
 constexpr int kMaxPackTuples = 16;
+constexpr int kMaxGhostTerms = 32;  // kMaxGhostTerms of the reference (trace/surface_table.hpp)
 
 // Trace status and soft-failure branch codes (reference: trace/surface_ops.hpp:24,113).
 enum : int { kOk = 0, kMissed = 1, kTir = 2, kBackward = 3, kUnsupported = 4,
@@ -28,12 +29,22 @@ __host__ __device__ inline bool is_soft(int s) { return s == kSoftMissed || s ==
 __host__ __device__ inline bool in_piston(int s) { return s == kOk || is_soft(s); }
 
 // ---- record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
-//      sin theta[F] | cos theta[F] | field_target[F] | pad to even --------------------------
+//      sin theta[F] | cos theta[F] | field_target[F] | [non-coaxial batches: per surface
+//      kXfValues transform values] | [ghost plates: coefficients [G][K] | normalisation
+//      radius [G] | plate index [G][L]] | pad to even --------------------------------------
+// Transform values of surface s (SurfaceTransform, trace/surface_transform.hpp:27, with the
+// sines and cosines taken on the host): dx, dy, cos a, sin a, cos b, sin b, moved (1 when
+// any of dx, dy, a, b is nonzero, else 0 and the surface is traced coaxially), 0.
+constexpr int kXfValues = 8;
+
 struct RecordLayout {
     int curvature, thickness, index, pupil, sin_theta, cos_theta, target, stride, surfaces;
+    int xf;                                      // transforms, or -1 (coaxial)
+    int ghost_coeff, ghost_radius, ghost_index;  // ghost plate data, or -1 (no plates)
 };
 
-__host__ __device__ inline RecordLayout record_layout(int S, int L, int F) {
+__host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int non_coaxial = 0,
+                                                      int G = 0, int K = 0) {
     RecordLayout r;
     r.surfaces = S;
     r.curvature = 0;
@@ -43,7 +54,18 @@ __host__ __device__ inline RecordLayout record_layout(int S, int L, int F) {
     r.sin_theta = r.pupil + 1;
     r.cos_theta = r.sin_theta + F;
     r.target = r.cos_theta + F;
-    const int n = r.target + F;
+    int n = r.target + F;
+    r.xf = non_coaxial ? n : -1;
+    if (non_coaxial) n += S * kXfValues;
+    r.ghost_coeff = r.ghost_radius = r.ghost_index = -1;
+    if (G > 0) {
+        r.ghost_coeff = n;
+        n += G * K;
+        r.ghost_radius = n;
+        n += G;
+        r.ghost_index = n;
+        n += G * L;
+    }
     r.stride = (n + 1) & ~1;
     return r;
 }
@@ -58,6 +80,8 @@ struct Pack {
 
 struct TraceParams {
     int V, S, L, F;
+    int non_coaxial;        // records carry per-surface transforms
+    int G, K;               // ghost plates and their profile terms
     int stride;             // doubles per variant record
     int failure;            // MKB_FAILURE_*
     int rays;               // rays per variant
@@ -79,6 +103,10 @@ struct TraceParams {
     const uint8_t* vsurf;           // device [V] table surfaces of each variant, or null (S)
     const int* order;               // device [V] processing order of the variants, or null
 };
+
+__host__ __device__ inline RecordLayout layout_of(const TraceParams& p) {
+    return record_layout(p.S, p.L, p.F, p.non_coaxial, p.G, p.K);
+}
 
 // Table surfaces variant v traces (uneven batches share the table of the largest; the value
 // is clamped to [2, S] so that no index leaves the record).
@@ -316,6 +344,88 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
                                             SoftT<N>* soft, int& branch,
                                             StepLocal<N>* keep = nullptr) {
     return step_surface_mu<N, kKeep>(r, t, c, n_before, n_before / n_after, soft, branch, keep);
+}
+
+// ---- decenter and tilt of a surface (trace/surface_transform.hpp:27-85) -----------------
+// R = R_y(b) R_x(a); a point q of the tilted surface frame lies at R q + (dx, dy, 0) in the
+// nominal frame. xf points at the surface's kXfValues record values.
+template <class N>
+struct Transform {
+    N dx, dy, ca, sa, cb, sb;
+};
+
+template <class N>
+__device__ __forceinline__ Transform<N> transform_at(const double* xf) {
+    return {N(xf[0]), N(xf[1]), N(xf[2]), N(xf[3]), N(xf[4]), N(xf[5])};
+}
+
+// R^T v (rotate_to_surface)
+template <class N>
+__device__ __forceinline__ void rotate_to(const Transform<N>& t, N& vx, N& vy, N& vz) {
+    const N x = t.cb * vx - t.sb * vz;
+    const N z = t.sb * vx + t.cb * vz;
+    const N y = t.ca * vy + t.sa * z;
+    vz = t.ca * z - t.sa * vy;
+    vx = x;
+    vy = y;
+}
+
+// R v (rotate_from_surface)
+template <class N>
+__device__ __forceinline__ void rotate_from(const Transform<N>& t, N& vx, N& vy, N& vz) {
+    const N y = t.ca * vy - t.sa * vz;
+    const N z = t.sa * vy + t.ca * vz;
+    const N x = t.cb * vx + t.sb * z;
+    vz = t.cb * z - t.sb * vx;
+    vx = x;
+    vy = y;
+}
+
+// ray_to_surface: p <- R^T (p - D), d <- R^T d
+template <class N>
+__device__ __forceinline__ void ray_to_surface(RayT<N>& r, const Transform<N>& t) {
+    N x = r.px - t.dx, y = r.py - t.dy, z = r.pz;
+    rotate_to(t, x, y, z);
+    r.px = x;
+    r.py = y;
+    r.pz = z;
+    rotate_to(t, r.dx, r.dy, r.dz);
+}
+
+// ray_from_surface: p <- R p + D, d <- R d
+template <class N>
+__device__ __forceinline__ void ray_from_surface(RayT<N>& r, const Transform<N>& t) {
+    N x = r.px, y = r.py, z = r.pz;
+    rotate_from(t, x, y, z);
+    r.px = x + t.dx;
+    r.py = y + t.dy;
+    r.pz = z;
+    rotate_from(t, r.dx, r.dy, r.dz);
+}
+
+// propagate_surface (trace/trace.hpp:233): the step onto surface s with its transform when
+// the batch is non-coaxial and the surface moved (xf = its record values, or null): d_z > 0,
+// z -= t in the nominal frame, into the tilted frame, the local step with t = 0 (its own
+// d_z > 0 check), and back into the nominal frame when it succeeded. The StepLocal values
+// are those of the local step.
+template <class N, bool kKeep = false>
+__device__ __forceinline__ int step_surface_xf(RayT<N>& r, N t, N c, N n_before, N mu,
+                                               const double* xf, SoftT<N>* soft, int& branch,
+                                               StepLocal<N>* keep = nullptr) {
+    if (xf == nullptr || !(xf[6] > 0.0))
+        return step_surface_mu<N, kKeep>(r, t, c, n_before, mu, soft, branch, keep);
+    if (!(r.dz > N(0.0))) return kBackward;
+    r.pz -= t;
+    const Transform<N> tr = transform_at<N>(xf);
+    ray_to_surface(r, tr);
+    const int st = step_surface_mu<N, kKeep>(r, N(0.0), c, n_before, mu, soft, branch, keep);
+    if (st == kOk) ray_from_surface(r, tr);
+    return st;
+}
+
+// Record values of surface s's transform, or null (coaxial batch).
+__device__ __forceinline__ const double* xf_of(const double* rec, const RecordLayout& lay, int s) {
+    return lay.xf >= 0 ? rec + lay.xf + s * kXfValues : nullptr;
 }
 
 // Step onto the reference sphere about M = (0, h, w) through the vertex of the last surface.

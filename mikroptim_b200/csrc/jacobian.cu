@@ -270,7 +270,7 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
         reinterpret_cast<char*>(status) + align256(static_cast<size_t>(chunk) * n * tp.rays));
     uint8_t* vsurf = reinterpret_cast<uint8_t*>(
         reinterpret_cast<char*>(active) + align256(sizeof(int) * static_cast<size_t>(chunk) * n));
-    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    const RecordLayout lay = layout_of(tp);
     const bool uneven_surfaces = templates->variant_surfaces != nullptr;
 
     fd_pattern_kernel<<<(runs * P + 127) / 128, 128, 0, stream>>>(vp, x0, runs, pattern,
@@ -401,7 +401,7 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
         rv.table = dtable;
         rv.stride = pmax;
     }
-    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    const RecordLayout lay = layout_of(tp);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream,
                       rv);
     if (rc != MKB_OK) return rc;
@@ -491,7 +491,7 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
     const bool exact = plan->precision == MKB_PRECISION_FP64;
     const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
     double* records = static_cast<double*>(workspace);
-    const RecordLayout lay = record_layout(tp.S, tp.L, tp.F);
+    const RecordLayout lay = layout_of(tp);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);
     if (rc != MKB_OK) return rc;
     rc = cuda_status(cudaMemsetAsync(J, 0, sizeof(double) * static_cast<size_t>(runs) * vp.P * R,

@@ -652,7 +652,7 @@ RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* te
 int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates,
                 const double* x, int runs, double* merit, int64_t* failed, int64_t* hard,
                 cudaStream_t stream, const int* run_mask = nullptr) {
-    const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+    const RecordLayout lay = layout_of(s.tp);
     int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
                           stream, run_vars(s, L, templates));
     if (rc != MKB_OK) return rc;
@@ -729,7 +729,7 @@ int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_pl
         if (rc != MKB_OK) return rc;
     }
     if (L.order != nullptr) {  // surface counts of the runs' records, then their order
-        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        const RecordLayout lay = layout_of(s.tp);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, x0, L.records, runs,
                           stream, run_vars(s, L, templates));
         if (rc != MKB_OK) return rc;
@@ -766,7 +766,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
         rc = fd_jacobian(templates, plan, vars, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
                          L.fd_ws_bytes, stream, want, rv);
     } else if (s.fused) {
-        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        const RecordLayout lay = layout_of(s.tp);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream, rv);
         if (rc == MKB_OK && L.order != nullptr && s.pmax > kSmallP) {
@@ -783,7 +783,7 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
                                      s.precision, stream, want, rv, L.order);
         }
     } else {
-        const RecordLayout lay = record_layout(s.tp.S, s.tp.L, s.tp.F);
+        const RecordLayout lay = layout_of(s.tp);
         rc = launch_apply(s.vp, lay, templates->records, templates->variants, L.st.x, L.records,
                           runs, stream);
         if (rc == MKB_OK)

@@ -31,10 +31,9 @@ constexpr int kPackRays = kThreads * kRaysPerThread;
 // memory of the workloads' tables fits as many
 constexpr int kTraceBlocksPerSm = 9;
 
-// The bulk-copy destination `record` must start on a 16-byte boundary: it is the first
-// member of a 16-byte aligned struct (checked below).
+// The variant's record (the bulk-copy destination, 16-byte aligned) and the mu table live in
+// dynamic shared memory sized for the batch's record stride (trace_smem).
 struct alignas(16) SharedTrace {
-    double record[2 * kMaxSurfaces + kMaxSurfaces * MKB_MAX_WAVELENGTHS + 1 + 3 * kMaxFields + 1];
     uint64_t bar;
     SharedTables tab;
     double opl[kPackRays];
@@ -42,7 +41,6 @@ struct alignas(16) SharedTrace {
     uint8_t status[kPackRays];
     int tuple_start[kMaxPackTuples + 1];
 };
-static_assert(offsetof(SharedTrace, record) % 16 == 0, "bulk-copy destination alignment");
 static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 
 // Trace of one ray to the reference sphere in number type N (trace_to_reference_sphere,
@@ -78,8 +76,8 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
-        status = step_surface_mu<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]), sp,
-                                    branch);
+        status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
+                                    xf_of(rec, lay, s), sp, branch);
         if (status != kOk) break;
         n_before = n_after;
     }
@@ -140,7 +138,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     const int pk = blockIdx.x - slot * p.n_packs;
     const int S = surfaces_of(p, v);
     const Pack pack = p.packs[pk];
-    const RecordLayout lay = record_layout(p.S, p.L, p.F);
+    const RecordLayout lay = layout_of(p);
     const double* src = records + static_cast<int64_t>(v) * p.stride;
     if (threadIdx.x <= pack.tuples) {
         int start = 0;
@@ -151,16 +149,18 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         sh.tuple_start[threadIdx.x] = start;
     }
     copy_tables(p, sh.tab);
-    if (!stage_to_shared(sh.record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
+    extern __shared__ __align__(16) double dyn[];
+    double* record = dyn;                 // [stride]
+    double* mu_tab = dyn + p.stride;      // [S][L]
+    if (!stage_to_shared(record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
                          &sh.bar))
         return;
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     // mu of every step and wavelength, divided once per CTA as the step would divide it
-    extern __shared__ double mu_tab[];  // [S][L]
     for (int i = threadIdx.x; i < S * p.L; i += kThreads) {
         const int s = i / p.L, l = i - s * p.L;
-        mu_tab[i] = s >= 1 ? value_of(N(sh.record[lay.index + (s - 1) * p.L + l]) /
-                                      N(sh.record[lay.index + s * p.L + l]))
+        mu_tab[i] = s >= 1 ? value_of(N(record[lay.index + (s - 1) * p.L + l]) /
+                                      N(record[lay.index + s * p.L + l]))
                            : 0.0;
     }
     __syncthreads();
@@ -175,7 +175,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N>(p, sh.record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
+        const int st = trace_ray<N>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
                                     pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
@@ -312,9 +312,30 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
     hard[v] = nh;
 }
 
-// dynamic shared memory of trace_kernel: the mu table
+// dynamic shared memory of trace_kernel: the record (stride is even) and the mu table
 size_t trace_smem(const TraceParams& p) {
-    return static_cast<size_t>(p.S) * p.L * sizeof(double);
+    return (static_cast<size_t>(p.stride) + static_cast<size_t>(p.S) * p.L) * sizeof(double);
+}
+
+// Launches trace_kernel<kResiduals, precision> (MIXED traces in FP64 with contraction; its FP32
+// part is the reverse sweep) with the dynamic shared memory the batch needs.
+template <bool kResiduals>
+int launch_trace(const TraceParams& p, const double* records, const TupleOut& out, int precision,
+                 cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+    const size_t smem = trace_smem(p);
+    auto kernel = precision == MKB_PRECISION_FP64
+                      ? trace_kernel<kResiduals, MKB_PRECISION_FP64>
+                      : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA>;
+    if (smem > 48 * 1024) {
+        const cudaError_t err = cudaFuncSetAttribute(
+            kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (err != cudaSuccess) return cuda_status(err, "trace: shared memory attribute");
+    }
+    kernel<<<blocks, kThreads, smem, stream>>>(p, records, out);
+    count_launch();
+    return cuda_status(cudaGetLastError(), kResiduals ? "residuals kernel launch"
+                                                      : "merit kernel launch");
 }
 
 size_t merit_workspace(int V, int n_tuples) {
@@ -328,14 +349,7 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
                      int64_t stride, double* opd, uint8_t* status, int precision,
                      cudaStream_t stream, RunMask mask) {
     TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask};
-    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
-    // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
-    if (precision == MKB_PRECISION_FP64)
-        trace_kernel<true, MKB_PRECISION_FP64><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
-    else
-        trace_kernel<true, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
-    count_launch();
-    return cuda_status(cudaGetLastError(), "residuals kernel launch");
+    return launch_trace<true>(p, records, out, precision, stream);
 }
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
@@ -351,14 +365,7 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     TupleOut out{nullptr, 0, nullptr, nullptr, reinterpret_cast<double*>(ws),
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
                  reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask};
-    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
-    // MIXED traces the rays in FP64 with contraction (its FP32 part is the reverse sweep)
-    if (precision == MKB_PRECISION_FP64)
-        trace_kernel<false, MKB_PRECISION_FP64><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
-    else
-        trace_kernel<false, MKB_PRECISION_FP64_FMA><<<blocks, kThreads, trace_smem(p), stream>>>(p, records, out);
-    count_launch();
-    int rc = cuda_status(cudaGetLastError(), "merit kernel launch");
+    int rc = launch_trace<false>(p, records, out, precision, stream);
     if (rc != MKB_OK) return rc;
     merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(
         p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard, mask);

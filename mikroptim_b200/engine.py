@@ -48,8 +48,9 @@ class DeviceSystemBatch:
         batch.validate_values()
         self.topology = batch.topology
         self.variants = batch.variants
-        self.stride = int(lib.mkb_record_stride(batch.surfaces, batch.wavelengths,
-                                                batch.fields))
+        self.non_coaxial = 1 if batch.non_coaxial else 0
+        self.stride = int(lib.mkb_record_stride_ext(batch.surfaces, batch.wavelengths,
+                                                    batch.fields, self.non_coaxial, 0, 0))
         host = np.zeros((max(batch.variants, 1), self.stride))
         view = batch.view()
         _capi.check(lib.mkb_pack_batch_host(C.byref(view), _capi.ptr(host)), "pack batch")
@@ -73,6 +74,7 @@ class DeviceSystemBatch:
         b.wavelengths = self.topology.wavelengths
         b.fields = self.topology.fields
         b.record_stride = self.stride
+        b.non_coaxial = self.non_coaxial
         b.records = C.c_void_p(self.records.data_ptr() + first * self.stride * 8)
         b.type = _capi.ptr(self.type, C.c_uint8)
         b._keep = self.type

@@ -43,6 +43,11 @@ void BatchTopology::validate() const {
                                    "surfaces");
     if (static_cast<int>(pupil_mode.size()) != fields)
         throw std::invalid_argument("BatchTopology: pupil_mode needs one entry per field");
+    if (non_coaxial)
+        for (PupilMode m : pupil_mode)
+            if (m != PupilMode::Full)
+                throw std::invalid_argument("BatchTopology: a non-coaxial batch needs the Full "
+                                            "pupil in every field");
 }
 
 SystemBatchHost::SystemBatchHost(BatchTopology topology, int variants)
@@ -61,6 +66,46 @@ SystemBatchHost::SystemBatchHost(BatchTopology topology, int variants)
     pupil_radius_.assign(V, 0.0);
     field_angle_.assign(V * F, 0.0);
     field_target_.assign(V * F, 0.0);
+    if (topology_.non_coaxial) decenter_tilt_.assign(V * S * 4, 0.0);
+}
+
+double& SystemBatchHost::decenter_tilt(int v, int s, int k) {
+    if (!topology_.non_coaxial)
+        throw std::invalid_argument("SystemBatchHost: decenter and tilt need a non-coaxial "
+                                    "batch (make_non_coaxial)");
+    if (k < 0 || k >= 4) throw std::out_of_range("SystemBatchHost: decenter_tilt component");
+    return decenter_tilt_.at(index2(v, s, surfaces()) * 4 + k);
+}
+
+double SystemBatchHost::decenter_tilt(int v, int s, int k) const {
+    if (k < 0 || k >= 4) throw std::out_of_range("SystemBatchHost: decenter_tilt component");
+    const size_t i = index2(v, s, surfaces());
+    return topology_.non_coaxial ? decenter_tilt_.at(i * 4 + k) : 0.0;
+}
+
+void SystemBatchHost::set_decenter_tilt(int v, int s, double dx, double dy, double alpha,
+                                        double beta) {
+    decenter_tilt(v, s, 0) = dx;
+    decenter_tilt(v, s, 1) = dy;
+    decenter_tilt(v, s, 2) = alpha;
+    decenter_tilt(v, s, 3) = beta;
+}
+
+SystemBatchHost make_non_coaxial(const SystemBatchHost& batch) {
+    BatchTopology t = batch.topology();
+    t.non_coaxial = true;
+    t.pupil_mode.assign(static_cast<size_t>(t.fields), PupilMode::Full);
+    SystemBatchHost out(t, batch.variants());
+    out.reference_wavelength_nm = batch.reference_wavelength_nm;
+    out.wavelength_weight = batch.wavelength_weight;
+    out.field_weight = batch.field_weight;
+    out.curvature_ = batch.curvature_;
+    out.thickness_ = batch.thickness_;
+    out.index_ = batch.index_;
+    out.pupil_radius_ = batch.pupil_radius_;
+    out.field_angle_ = batch.field_angle_;
+    out.field_target_ = batch.field_target_;
+    return out;
 }
 
 size_t SystemBatchHost::check_v(int v) const {
@@ -93,6 +138,12 @@ void SystemBatchHost::validate_values() const {
     finite(field_target_, "field_target");
     finite(wavelength_weight, "wavelength_weight");
     finite(field_weight, "field_weight");
+    finite(decenter_tilt_, "decenter_tilt");
+    for (size_t i = 2; i < decenter_tilt_.size(); i += 4)
+        for (size_t k = i; k < i + 2; ++k)
+            if (!(std::abs(decenter_tilt_[k]) < 1.5707963267948966))
+                throw std::invalid_argument("SystemBatchHost: tilt angles must be in "
+                                            "(-pi/2, pi/2)");
     for (double r : pupil_radius_)
         if (!(r > 0)) throw std::invalid_argument("SystemBatchHost: pupil radius must be > 0");
     for (double n : index_)
@@ -130,6 +181,7 @@ mkb_batch_view SystemBatchHost::view() const {
     v.pupil_radius = pupil_radius_.data();
     v.field_angle = field_angle_.data();
     v.field_target = field_target_.data();
+    v.decenter_tilt = topology_.non_coaxial ? decenter_tilt_.data() : nullptr;
     return v;
 }
 
@@ -333,7 +385,9 @@ void DeviceBuffer::release() {
 void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     batch.validate_values();
     const mkb_batch_view view = batch.view();
-    const int32_t stride = mkb_record_stride(view.surfaces, view.wavelengths, view.fields);
+    const int32_t non_coaxial = view.decenter_tilt != nullptr ? 1 : 0;
+    const int32_t stride = mkb_record_stride_ext(view.surfaces, view.wavelengths, view.fields,
+                                                 non_coaxial, 0, 0);
     host_records_.assign(static_cast<size_t>(view.variants) * stride, 0.0);
     check(mkb_pack_batch_host(&view, host_records_.data()), "pack batch");
     void* d = cuda::upload(records_, host_records_, stream);
@@ -343,7 +397,9 @@ void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     batch_.wavelengths = view.wavelengths;
     batch_.fields = view.fields;
     batch_.record_stride = stride;
-    batch_.reserved = 0;
+    batch_.non_coaxial = non_coaxial;
+    batch_.ghost_plates = 0;
+    batch_.ghost_terms = 0;
     batch_.records = static_cast<const double*>(d);
     batch_.type = type_.data();
 }

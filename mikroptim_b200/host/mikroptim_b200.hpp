@@ -42,6 +42,8 @@ struct BatchTopology {
     int surfaces = 0, wavelengths = 0, fields = 0;
     std::vector<SurfaceKind> type;      // [S], type[0] = Stop
     std::vector<PupilMode> pupil_mode;  // [F]
+    // per-surface decenter and tilt (system_batch.hpp:45); every field then uses the Full pupil
+    bool non_coaxial = false;
     void validate() const;
 };
 
@@ -64,6 +66,13 @@ public:
     double& field_target(int v, int f) { return field_target_.at(index2(v, f, fields())); }
     double curvature(int v, int s) const { return curvature_.at(index2(v, s, surfaces())); }
     double thickness(int v, int s) const { return thickness_.at(index2(v, s, surfaces())); }
+    // decenter dx, dy [mm] and tilts alpha, beta [rad] of surface s (k = 0..3); writing needs
+    // a non-coaxial topology (std::invalid_argument otherwise), reading a coaxial batch gives 0
+    // (SystemBatchHost::decenter_tilt, system_batch.hpp:156)
+    double& decenter_tilt(int v, int s, int k);
+    double decenter_tilt(int v, int s, int k) const;
+    void set_decenter_tilt(int v, int s, double dx, double dy, double alpha, double beta);
+    bool coaxial() const { return !topology_.non_coaxial; }
 
     double reference_wavelength_nm = 0.0;
     std::vector<double> wavelength_weight;  // [L]
@@ -81,8 +90,12 @@ private:
     int variants_;
     std::vector<uint8_t> type_;
     std::vector<double> curvature_, thickness_, index_, pupil_radius_, field_angle_,
-        field_target_;
+        field_target_, decenter_tilt_;
+    friend SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
 };
+
+// Copy of `batch` with a non-coaxial topology (decenter and tilt zero, Full pupils).
+SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
 
 struct ResidualSettings {
     int rings = 10;

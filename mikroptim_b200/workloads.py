@@ -9,6 +9,7 @@ Box-Muller on it. Seeds: configuration k uses 20261203 + k unless given.
                   n = 1.5046 + 0.00420 / lambda^2 (um) at 486.1 / 587.6 / 656.3 nm, fields
                   0, 0.7, 1.0 degree, pupil radius 5 mm, c1, c2, t perturbed by 5 % Gaussian
                   noise, quadrature 6 rings x 12 spokes.
+  tolerancing(...) configuration 5: perturbed, decentered and tilted copies of one objective.
   objective(...)  4096 seven-element (14-sphere) objectives with curvatures U(-1/15, 1/15),
                   air gaps U(0.1, 5), glass thickness U(1, 8), 3-term Sellmeier glasses fitted
                   to n_d U(1.45, 1.90), V_d U(25, 95), 7 wavelengths 405..700 nm, 5 fields,
@@ -25,7 +26,7 @@ import numpy as np
 from .batch import (BatchTopology, FAILURE_SOFT, PRECISION_FP64, ResidualSettings,
                     SURFACE_SPHERE, SURFACE_STOP, SystemBatchHost, VAR_CURVATURE,
                     VAR_THICKNESS, VAR_WORKING_DISTANCE, Variable, VariableSet)
-from .quadrature import PUPIL_AXIS, PUPIL_HALF
+from .quadrature import PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF
 
 _M64 = (1 << 64) - 1
 _GOLDEN = 0x9E3779B97F4A7C15
@@ -317,6 +318,87 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
     b.variant_surfaces = sv.astype(np.uint8)
     settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
     return b, settings, variable_sets, x0
+
+
+# ---- configuration 5: Monte-Carlo tolerancing of a decentered / tilted objective --------------
+
+ARCMIN = math.pi / 10800.0
+
+
+def tolerancing(variants: int = 262144, seed: int = 20261203 + 5, elements: int = 10,
+                rings: int = 16, spokes: int = 32, decenter_mm: float = 0.005,
+                tilt_rad: float = ARCMIN, radius_rel: float = 0.001, thickness_mm: float = 0.010,
+                index_delta: float = 2e-4, failure: int = FAILURE_SOFT,
+                precision: int = PRECISION_FP64):
+    """Configuration 5: `variants` perturbed copies of one nominal objective of `elements`
+    biconvex elements (2 * elements spheres after the stop; element style of configuration 1:
+    curvatures +-1/(50 E), glass 6/E mm, air 0.5 mm, Cauchy glass at 7 wavelengths, image at
+    the paraxial focus), non-coaxial (every field on the Full pupil, 16 x 32), 5 fields
+    0..1 degree, pupil radius 5 mm. Per variant, in the meaning of the reference's deviate
+    model (tolerance/tolerance_model.hpp: c' = c/(1 + eps), t' = t + delta, n'(lambda) =
+    n(lambda) + dn per glass, per-surface decenter and tilt): eps ~ U(-radius_rel, radius_rel)
+    per sphere, delta ~ N(0, thickness_mm) per element thickness and air gap, dn ~
+    N(0, index_delta) per glass, dx, dy ~ N(0, decenter_mm) and alpha, beta ~ N(0, tilt_rad)
+    per sphere; normal draws are cut at 3 sigma. Variables: every curvature, every thickness
+    between the spheres and the working distance (the design variables; the tolerances are
+    not variables). Returns (batch, settings, variables, x0 [V][P])."""
+    S = 1 + 2 * elements
+    topo = BatchTopology(surfaces=S, wavelengths=7, fields=5,
+                         type=[SURFACE_STOP] + [SURFACE_SPHERE] * (S - 1),
+                         pupil_mode=[PUPIL_FULL] * 5, non_coaxial=True)
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.6
+    b.wavelength_nm[:] = OBJECTIVE_WAVELENGTHS
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    # nominal design (one draw of the configuration-1 style element noise)
+    nom = rng.normal(1, 3 * S).reshape(S, 3)
+    c = np.zeros(S)
+    t = np.zeros(S)
+    idx = np.ones((S, 7))
+    n_ref = np.ones(S)
+    n_glass = cauchy_index(OBJECTIVE_WAVELENGTHS)
+    for e in range(elements):
+        s1, s2 = 1 + 2 * e, 2 + 2 * e
+        c[s1] = (1.0 / (50.0 * elements)) * (1.0 + 0.05 * nom[s1, 0])
+        c[s2] = (-1.0 / (50.0 * elements)) * (1.0 + 0.05 * nom[s2, 0])
+        t[s1] = (6.0 / elements) * (1.0 + 0.05 * nom[s1, 1])
+        t[s2] = 0.5 * (1.0 + 0.05 * nom[s2, 1])
+        idx[s1, :] = n_glass
+        n_ref[s1] = float(cauchy_index(587.6))
+    efl, bfd = paraxial(c[None, :], t[None, :], n_ref[None, :])
+    t[S - 1] = bfd[0]
+
+    def cut_normal(tag, shape, sigma):
+        z = rng.normal(tag, int(np.prod(shape))).reshape(shape)
+        return sigma * np.clip(z, -3.0, 3.0)
+
+    eps = radius_rel * (2.0 * rng.uniform(10, variants * (S - 1)).reshape(variants, S - 1) - 1.0)
+    b.curvature[:, :] = c[None, :]
+    b.curvature[:, 1:] = c[None, 1:] / (1.0 + eps)
+    b.thickness[:, :] = t[None, :]
+    b.thickness[:, 1:S - 1] += cut_normal(11, (variants, S - 2), thickness_mm)
+    b.index[:, :, :] = idx[None, :, :]
+    dn = cut_normal(12, (variants, elements), index_delta)
+    for e in range(elements):
+        b.index[:, 1 + 2 * e, :] += dn[:, e, None]
+    b.decenter_tilt[:, 1:, 0] = cut_normal(13, (variants, S - 1), decenter_mm)
+    b.decenter_tilt[:, 1:, 1] = cut_normal(14, (variants, S - 1), decenter_mm)
+    b.decenter_tilt[:, 1:, 2] = cut_normal(15, (variants, S - 1), tilt_rad)
+    b.decenter_tilt[:, 1:, 3] = cut_normal(16, (variants, S - 1), tilt_rad)
+    angles = np.deg2rad(np.linspace(0.0, 1.0, 5))
+    b.pupil_radius[:] = 5.0
+    b.field_angle[:, :] = angles[None, :]
+    b.field_target[:, :] = efl[0] * np.tan(angles)[None, :]
+    settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
+    variables = [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, S)]
+    variables += [Variable(VAR_THICKNESS, s, 0.05, 50.0, 1.0) for s in range(1, S - 1)]
+    variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1000.0, 1.0)]
+    vs = VariableSet(topo, variables)
+    x0 = (np.stack([vs.extract(b, v) for v in range(variants)]) if variants
+          else np.zeros((0, vs.size)))
+    return b, settings, vs, x0
 
 
 def unpad(batch: SystemBatchHost, v: int) -> SystemBatchHost:

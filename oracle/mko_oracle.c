@@ -175,7 +175,69 @@ typedef struct {
     const double* c;  /* [S] */
     const double* t;  /* [S] */
     const double* n;  /* [S][L] */
+    const double* xf; /* [S][4] dx, dy, alpha, beta, or NULL (coaxial) */
 } table_t;
+
+/* ---- decenter and tilt: trace/surface_transform.hpp:27-140 ---------------------------- */
+typedef struct { double dx, dy, ca, sa, cb, sb; } xform_t;
+
+/* surface_transform_of: 0 when the table is coaxial or the surface's four values are 0 */
+static int transform_of(const table_t* sys, int s, xform_t* t) {
+    if (sys->xf == NULL) return 0;
+    const double* v = sys->xf + (size_t)s * 4;
+#define MKO_ZERO(x) (!((x) > 0.0) && !((x) < 0.0))
+    if (MKO_ZERO(v[0]) && MKO_ZERO(v[1]) && MKO_ZERO(v[2]) && MKO_ZERO(v[3])) return 0;
+#undef MKO_ZERO
+    t->dx = v[0];
+    t->dy = v[1];
+    t->ca = cos(v[2]);
+    t->sa = sin(v[2]);
+    t->cb = cos(v[3]);
+    t->sb = sin(v[3]);
+    return 1;
+}
+
+static vec3 rotate_to_surface(const xform_t* t, vec3 v) {
+    const double x = t->cb * v.x - t->sb * v.z;
+    const double z = t->sb * v.x + t->cb * v.z;
+    vec3 r = {x, t->ca * v.y + t->sa * z, t->ca * z - t->sa * v.y};
+    return r;
+}
+
+static vec3 rotate_from_surface(const xform_t* t, vec3 v) {
+    const double y = t->ca * v.y - t->sa * v.z;
+    const double z = t->sa * v.y + t->ca * v.z;
+    vec3 r = {t->cb * v.x + t->sb * z, y, t->cb * z - t->sb * v.x};
+    return r;
+}
+
+static vec3 point_to_surface(const xform_t* t, vec3 p) {
+    vec3 q = {p.x - t->dx, p.y - t->dy, p.z};
+    return rotate_to_surface(t, q);
+}
+
+static vec3 point_from_surface(const xform_t* t, vec3 q) {
+    const vec3 p = rotate_from_surface(t, q);
+    vec3 r = {p.x + t->dx, p.y + t->dy, p.z};
+    return r;
+}
+
+/* propagate_surface with a transform (trace/trace.hpp:233) */
+static int propagate_surface_xf(ray_t* ray, double t, int kind, double c, double n_before,
+                                double n_after, soft_t* soft, unsigned char* branch,
+                                const xform_t* xf) {
+    if (xf == NULL) return propagate_surface(ray, t, kind, c, n_before, n_after, soft, branch);
+    if (!(ray->d.z > 0.0)) return ST_BACKWARD;
+    ray->p.z -= t;
+    ray->p = point_to_surface(xf, ray->p);
+    ray->d = rotate_to_surface(xf, ray->d);
+    const int st = propagate_surface(ray, 0.0, kind, c, n_before, n_after, soft, branch);
+    if (st == ST_OK) {
+        ray->p = point_from_surface(xf, ray->p);
+        ray->d = rotate_from_surface(xf, ray->d);
+    }
+    return st;
+}
 
 /* Full per-surface record of a ray (AdjointRecord, trace/adjoint_record.hpp:66). */
 typedef struct {
@@ -203,8 +265,10 @@ static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center
         const double n_before = sys->n[(s - 1) * L + l];
         const double n_after = sys->n[s * L + l];
         unsigned char branch = BR_REGULAR;
-        st = propagate_surface(ray, sys->t[s - 1], sys->type[s], sys->c[s], n_before, n_after,
-                               soft, &branch);
+        xform_t xf;
+        const int moved = transform_of(sys, s, &xf);
+        st = propagate_surface_xf(ray, sys->t[s - 1], sys->type[s], sys->c[s], n_before, n_after,
+                                  soft, &branch, moved ? &xf : NULL);
         if (st != ST_OK) break;
         if (rec) {
             rec->count = s + 1;
@@ -320,6 +384,7 @@ static table_t table_of(const mkb_batch_view* v, int var) {
     t.c = v->curvature + (size_t)var * v->surfaces;
     t.t = v->thickness + (size_t)var * v->surfaces;
     t.n = v->index + (size_t)var * v->surfaces * v->wavelengths;
+    t.xf = v->decenter_tilt != NULL ? v->decenter_tilt + (size_t)var * v->surfaces * 4 : NULL;
     return t;
 }
 
@@ -833,8 +898,27 @@ static void backward_ray(const table_t* sys, int l, const record_t* rec, int rea
             const double n_after = sys->n[j * L + l];
             sadj_t par = {0.0, 0.0, 0.0, 0.0};
             const double c = kind == MKB_SURFACE_SPHERE ? sys->c[j] : 0.0;
-            refracting_step_backward(p, d, t, c, n_before, n_after, next_branch, seed_opl,
+            /* decentered / tilted surface: the step in its tilted frame, adjoints turned in
+               with R^T and back with R, t-bar = -p-bar_z (adjoint_backward.hpp:539-569) */
+            xform_t xf;
+            const int moved = transform_of(sys, j, &xf);
+            vec3 pl = p, dl = d;
+            double tl = t;
+            if (moved) {
+                vec3 shifted = {p.x, p.y, p.z - t};
+                pl = point_to_surface(&xf, shifted);
+                dl = rotate_to_surface(&xf, d);
+                tl = 0.0;
+                adj.p = rotate_to_surface(&xf, adj.p);
+                adj.d = rotate_to_surface(&xf, adj.d);
+            }
+            refracting_step_backward(pl, dl, tl, c, n_before, n_after, next_branch, seed_opl,
                                      seed_pen, &adj, &par);
+            if (moved) {
+                adj.p = rotate_from_surface(&xf, adj.p);
+                adj.d = rotate_from_surface(&xf, adj.d);
+                par.thickness = -adj.p.z;
+            }
             if (kind == MKB_SURFACE_SPHERE) w_write(w, w->curvature[j], par.curvature);
             w_write(w, w->thickness[s], par.thickness);
             (void)n_carry; /* index sinks: no glass variables in this build */

@@ -49,6 +49,7 @@ mko::BatchTopology topology_of_view(const mkb_batch_view& v, const mkb_residual_
     t.fields = v.fields;
     t.ghost_plates = 0;
     t.ghost_terms = 0;
+    t.non_coaxial = v.decenter_tilt != nullptr;
     t.source = mko::SourceKind::Collimated;
     for (int s = 0; s < v.surfaces; ++s) {
         t.type.push_back(static_cast<mko::SurfaceKind>(v.type[s]));
@@ -84,6 +85,11 @@ mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_p
             b.field_angle(i, f) = v.field_angle[i * F + f];
             b.field_target(i, f) = v.field_target[i * F + f];
         }
+        if (v.decenter_tilt != nullptr)
+            for (int s = 0; s < S; ++s)
+                for (int k = 0; k < 4; ++k)
+                    b.decenter_tilt(i, s, k) =
+                        v.decenter_tilt[(static_cast<std::size_t>(i) * S + s) * 4 + k];
     }
     return b;
 }

@@ -148,3 +148,45 @@ def test_normal_equations_fma_chain():
     if has_reference_build():
         Ar, gr = po.reference().normal_equations(J, r)
         assert np.array_equal(A, Ar) and np.array_equal(g, gr)
+
+
+@pytest.mark.skipif(not has_reference_build(), reason="reference CPU build not present")
+def test_port_matches_reference_on_decentered_tilted_batch():
+    """Non-coaxial batch (configuration-5 shape, small pupil): restatement and reference
+    agree bit for bit on RESIDUALS, MERIT, the adjoint and the FD Jacobian."""
+    b, st, vs, x0 = workloads.tolerancing(6, rings=6, spokes=12)
+    assert np.any(b.decenter_tilt[:, 1:] != 0.0)
+    lay = ResidualLayout(b.topology, st)
+    P, R = po.port(), po.reference()
+    for a, c in zip(P.residuals(b, lay), R.residuals(b, lay)):
+        assert np.array_equal(a, c)
+    for a, c in zip(P.merit(b, lay), R.merit(b, lay)):
+        assert np.array_equal(a, c)
+    two = b.subset(0, 2)
+    for a, c in zip(P.adjoint_jacobian(two, lay, vs, x0[:2]),
+                    R.adjoint_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
+    for a, c in zip(P.fd_jacobian(two, lay, vs, x0[:2]), R.fd_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
+
+
+def test_zero_transforms_trace_like_the_coaxial_batch():
+    """A non-coaxial copy whose decenters and tilts are all zero traces bit for bit like the
+    coaxial batch (surface_transform_of returns false for all-zero surfaces)."""
+    from mikroptim_b200.batch import BatchTopology, SystemBatchHost, make_non_coaxial
+    b, st, vs, x0 = workloads.tolerancing(3, rings=4, spokes=8)
+    nc = b.subset(0, 3)
+    nc.decenter_tilt[:] = 0.0
+    t = b.topology
+    co = SystemBatchHost(BatchTopology(t.surfaces, t.wavelengths, t.fields, list(t.type),
+                                       list(t.pupil_mode)), 3)
+    for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
+                 "field_target"):
+        setattr(co, name, getattr(nc, name).copy())
+    co.reference_wavelength_nm = nc.reference_wavelength_nm
+    co.wavelength_weight, co.field_weight = nc.wavelength_weight, nc.field_weight
+    assert make_non_coaxial(co).non_coaxial
+    lay = ResidualLayout(b.topology, st)
+    P = po.port()
+    for a, c in zip(P.residuals(nc, lay), P.residuals(co, lay)):
+        assert np.array_equal(a, c)
