@@ -66,9 +66,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit"])
+    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing"])
     ap.add_argument("--variants", type=int, default=None,
-                    help="runs per GPU (default 8192 for uneven, 4096 otherwise)")
+                    help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
+                         "otherwise)")
     return ap.parse_args()
 
 
@@ -848,6 +849,177 @@ def run_reference(args, world, rank):
     }
 
 
+WORKLOAD_TOL = ("tolerancing-{V}: {V} Monte-Carlo perturbations of one 10-element (20-sphere) "
+                "objective, decenter 5 um, tilt 1', dR/R 0.1 %, dt 10 um, dn 2e-4 per glass, "
+                "non-coaxial, L=7, F=5, Full 16x32 pupils, P=40 design variables (config 5 shape)")
+
+
+def run_tolerancing(args, world, rank, local):
+    """Configuration 5: per step, the MERIT of every perturbed variant (FP64 with FMA) and its
+    gradient with respect to the design variables, 2 J^T r, from the fused adjoint normal
+    equations (column P of [J r]^T [J r]; the Gauss-Newton block J^T J comes with it). The
+    gradient's reverse sweep runs in MIXED precision (FP64 trace, FP32 sweep); its error
+    against the FP64_FMA gradient is reported, and the FP64_FMA gradient is timed beside."""
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import PRECISION_FP64_FMA, PRECISION_MIXED, ResidualLayout
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    V = args.variants or 65536
+    b, st, vs, x0 = workloads.tolerancing(V, seed=20261203 + 5 + 1000 * rank)
+    st.precision = PRECISION_FP64_FMA
+    lay = ResidualLayout(b.topology, st)
+    lay_mixed = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_MIXED))
+    db = engine.DeviceSystemBatch(b, dev)
+    P = vs.size
+    cb = db.c_struct()
+    plans = {0: lay.plan(b), 1: lay_mixed.plan(b)}
+    cvars = vs.c_struct()
+    x = torch.from_numpy(np.ascontiguousarray(x0)).to(dev)
+    gram = torch.empty((V, P + 1, P + 1), dtype=torch.float64, device=dev)
+    ws_g = torch.empty(int(lib.mkb_adjoint_jacobian_workspace_bytes(C.byref(cb), V)),
+                       dtype=torch.uint8, device=dev)
+    ws_m = torch.empty(int(lib.mkb_merit_workspace_bytes(V, C.byref(plans[0]))),
+                       dtype=torch.uint8, device=dev)
+    merit = torch.empty(V, dtype=torch.float64, device=dev)
+    failed = torch.empty(V, dtype=torch.int64, device=dev)
+    hard = torch.empty(V, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    sh = C.c_void_p(stream.cuda_stream)
+
+    def merit_call():
+        _capi.check(lib.mkb_merit_device(C.byref(cb), C.byref(plans[0]),
+                                         C.c_void_p(merit.data_ptr()),
+                                         C.c_void_p(failed.data_ptr()),
+                                         C.c_void_p(hard.data_ptr()),
+                                         C.c_void_p(ws_m.data_ptr()), ws_m.numel(), sh), "merit")
+
+    def gram_call(which):
+        _capi.check(lib.mkb_adjoint_normal_equations_device(
+            C.byref(cb), C.byref(plans[which]), C.byref(cvars), C.c_void_p(x.data_ptr()), V,
+            C.c_void_p(gram.data_ptr()), C.c_void_p(ws_g.data_ptr()), ws_g.numel(), sh),
+            "adjoint normal equations")
+
+    def timed(fn, steps):
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in ts) / steps
+
+    def step():
+        merit_call()
+        gram_call(1)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = lib.mkb_launch_count()
+    with ClockSampler(local) as clocks:
+        ms_step = timed(step, args.steps)
+    launches = lib.mkb_launch_count() - l0
+    barrier(world)
+    ms_step = max_over_ranks(ms_step, world, dev)
+    ms_merit = timed(merit_call, 2)
+    ms_gram_fma = timed(lambda: gram_call(0), 2)
+    g_fma = gram[:, :P, P].clone()
+    ms_gram = timed(lambda: gram_call(1), 2)
+    torch.cuda.synchronize()
+    g_mixed = gram[:, :P, P]
+    # MIXED gradient error against the FMA one (relative to |g| per sample)
+    rel = (torch.linalg.vector_norm(g_mixed - g_fma, dim=1) /
+           torch.clamp(torch.linalg.vector_norm(g_fma, dim=1), min=1e-300)).cpu().numpy()
+
+    # end to end: host x in (pinned), merit and gradient out, every step
+    x_host = torch.from_numpy(np.ascontiguousarray(x0)).pin_memory()
+    out_merit = torch.empty(V, dtype=torch.float64).pin_memory()
+    out_grad = torch.empty((V, P), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        x.copy_(x_host, non_blocking=True)
+        step()
+        out_merit.copy_(merit, non_blocking=True)
+        out_grad.copy_(gram[:, :P, P], non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+
+    rays = V * lay.rays_per_variant
+    S = b.surfaces
+    flop = rays * (3 * FLOPEQ_PER_RAY_SURFACE * (S - 1 + 2) + 4 * P) + 2.0 * (P + 1) ** 2 * \
+        V * lay.trace_rows
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = flop / (ms_gram / 1e3) / 1e12
+    if rank != 0:
+        return None, None
+    return {
+        "metric": "MC tolerancing samples/s (MERIT + design-variable gradient)",
+        "value": world * V / (ms_step / 1e3),
+        "unit": "samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-5 shapes)",
+        "config": {"workload": WORKLOAD_TOL.format(V=V),
+                   "step": "MERIT (FP64, FMA) + fused adjoint normal equations (MIXED: FP64 "
+                           "trace, FP32 reverse sweep) of every sample; the gradient is 2 x "
+                           "column P",
+                   "samples_per_gpu": V, "rays_per_sample": lay.rays_per_variant,
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(launches),
+        "ray_surface_hits_per_s": world * rays * (S - 1) / (ms_merit / 1e3),
+        "ms_merit": ms_merit, "ms_gradient_mixed": ms_gram, "ms_gradient_fp64_fma": ms_gram_fma,
+        "fp64_fma_gradient": {"value": world * V / ((ms_merit + ms_gram_fma) / 1e3),
+                              "unit": "samples/s"},
+        "mixed_gradient_rel_error_vs_fp64_fma": {"median": float(np.median(rel)),
+                                                 "p99": float(np.percentile(rel, 99))},
+        "e2e": {"value": world * V / (e2e_ms / 1e3), "unit": "samples/s",
+                "h2d_bytes_per_step": int(V * P * 8),
+                "d2h_bytes_per_step": int(V * (P + 1) * 8)},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "adjoint_gram_kernel<MixedPrecision> (fused adjoint + DMMA "
+                               "normal equations) with its apply kernel",
+                     "kernel_ms": ms_gram,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
+        "clocks": clocks.summary(),
+    }, (b, lay)
+
+
+def cpu_baseline_tolerancing(samples: int = 8):
+    """The reference's CPU MERIT plus adjoint Jacobian (gradient 2 J^T r) of `samples` samples,
+    all host threads (oracle/_ref)."""
+    import oracle.pyoracle as po
+    from mikroptim_b200 import workloads
+    from mikroptim_b200.batch import ResidualLayout
+    b, st, vs, x0 = workloads.tolerancing(samples)
+    lay = ResidualLayout(b.topology, st)
+    ref = po.reference()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref.merit(b, lay, threads=threads)
+    J, r0, _ = ref.adjoint_jacobian(b, lay, vs, x0, threads=threads)
+    np.einsum("ipr,ir->ip", J, r0)
+    dt = time.perf_counter() - t0
+    return {"value": samples / dt, "unit": "samples/s", "cores": threads, "kind": "reference",
+            "sample": f"merit_cpu + adjoint_jacobian_cpu of {samples} samples, {dt:.1f} s"}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -858,6 +1030,13 @@ def main():
         if rank == 0 and world == 1:
             try:
                 out["cpu_baseline"] = cpu_baseline_uneven()
+            except Exception as e:  # the baseline is reported, not required
+                out["cpu_baseline"] = {"value": None, "error": str(e)}
+    elif args.workload == "tolerancing":
+        out, _ = run_tolerancing(args, world, rank, local)
+        if rank == 0 and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline_tolerancing()
             except Exception as e:  # the baseline is reported, not required
                 out["cpu_baseline"] = {"value": None, "error": str(e)}
     elif args.workload == "lm":

@@ -497,7 +497,7 @@ struct RowSinks {
     int ld[K];
 };
 
-template <class N, class Q>
+template <class N, class Q, bool kXf>
 __device__ void fused_forward(const TraceParams& p, const double* rec, const double* mu_tab,
                               const RecordLayout& lay, int S, int f, int l, const Sample& smp,
                               bool soft_mode, Q* ck,
@@ -544,7 +544,7 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
         int branch;
         StepLocal<N> loc{zero, zero, zero, zero, zero};
         status = step_surface_xf<N, true>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
-                                          xf_of(rec, lay, s), sp, branch, &loc);
+                                          xf_at<kXf>(rec, lay, s), sp, branch, &loc);
         if (status != kOk) break;
         q[6 * kFusedThreads] = Q(value_of(loc.s0));
         q[7 * kFusedThreads] = Q(value_of(loc.s));
@@ -582,7 +582,7 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
 // factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
 // quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
 // out-of-line copy per K keeps the kernel's instruction footprint small.
-template <class N, class A, int K, class Q, class YT>
+template <class N, class A, int K, bool kXf, class Q, class YT>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
                                             const double* rec, const double* mu_tab,
                                             const RecordLayout& lay, int S,
@@ -657,7 +657,7 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
             StepAdj<A> par[K];
 #pragma unroll
             for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
-            const double* xf = xf_of(rec, lay, j);
+            const double* xf = xf_at<kXf>(rec, lay, j);
             if (xf != nullptr && xf[6] > 0.0) {  // decentered / tilted surface
                 const Transform<N> tn = transform_at<N>(xf);
                 const Transform<A> ta = transform_at<A>(xf);
@@ -718,7 +718,7 @@ template <> struct FusedTypes<MixedPrecision> {
     using Row = float;
 };
 
-template <class N, int K>
+template <class N, int K, bool kXf>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
                                              const double* rec, const double* mu_tab,
                                              const RecordLayout& lay, int S,
@@ -730,7 +730,7 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                              const double (&spn)[K],
                                              const RowSinks<K, typename FusedTypes<N>::Row>& sinks) {
     using T = FusedTypes<N>;
-    fused_backward<typename T::Bwd, typename T::Adj, K>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
+    fused_backward<typename T::Bwd, typename T::Adj, K, kXf>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
                                                         reached_image, soft_mode, so, spn, sinks);
 }
@@ -752,7 +752,7 @@ struct FusedArgs {
     int64_t gram_stride;   // doubles per run of `gram`
 };
 
-template <class N>
+template <class N, bool kXf>
 __global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ? 4 : kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
@@ -855,7 +855,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                fused_forward<typename FusedTypes<N>::Fwd, Keep>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
+                fused_forward<typename FusedTypes<N>::Fwd, Keep, kXf>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
                                                            my_ck, stride_ck, br_lo, br_hi, count,
                                                            image_branch, status, soft_first, opl,
                                                            penalty);
@@ -874,7 +874,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double so[2] = {piston ? 1.0 : 0.0, 0.0};
                         const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
                         const RowSinks<2, YT> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
-                        run_backward<N, 2>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                        run_backward<N, 2, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
                                            sinks);
                     }
@@ -884,18 +884,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double sp[1] = {pen_sweep ? 1.0 : 0.0};
                         const RowSinks<1, YT> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
                                                 {piston ? TS : kFusedThreads}};
-                        run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
+                        run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
                                            so, sp, sinks);
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
                     const RowSinks<1, YT> s0{{1.0}, {row}, {TS}};
-                    run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
                     const RowSinks<1, YT> s1{{pfac}, {prow}, {kFusedThreads}};
-                    run_backward<N, 1>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
                 }
             }
@@ -1095,9 +1095,13 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
     const size_t smem = fused_adjoint_smem(
         tp, p_max, precision == MKB_PRECISION_MIXED ? sizeof(float) : sizeof(double));
-    auto kernel = precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64>
-                  : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision>
-                                                     : adjoint_gram_kernel<double>;
+    auto kernel = tp.non_coaxial
+                      ? (precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64, true>
+                         : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision, true>
+                                                            : adjoint_gram_kernel<double, true>)
+                      : (precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64, false>
+                         : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision, false>
+                                                            : adjoint_gram_kernel<double, false>);
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");

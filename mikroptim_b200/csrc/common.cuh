@@ -423,6 +423,14 @@ __device__ __forceinline__ int step_surface_xf(RayT<N>& r, N t, N c, N n_before,
     return st;
 }
 
+// Record values of surface s's transform when the kernel was built for non-coaxial records
+// (kXf), else null at compile time: a coaxial launch carries no transform code.
+template <bool kXf>
+__device__ __forceinline__ const double* xf_at(const double* rec, const RecordLayout& lay, int s) {
+    if constexpr (kXf) return rec + lay.xf + s * kXfValues;
+    else return nullptr;
+}
+
 // Record values of surface s's transform, or null (coaxial batch).
 __device__ __forceinline__ const double* xf_of(const double* rec, const RecordLayout& lay, int s) {
     return lay.xf >= 0 ? rec + lay.xf + s * kXfValues : nullptr;

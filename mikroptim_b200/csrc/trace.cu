@@ -47,7 +47,7 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
 // mu_tab[s * L + l] = n_before / n_after of the step onto surface s (divided in N).
-template <class N>
+template <class N, bool kXf>
 __device__ inline int trace_ray(const TraceParams& p, const double* rec, const double* mu_tab,
                                 const RecordLayout& lay, int S, int f, int l, const Sample& smp,
                                 bool soft_mode, double& opl, double& penalty) {
@@ -77,7 +77,7 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
         status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
-                                    xf_of(rec, lay, s), sp, branch);
+                                    xf_at<kXf>(rec, lay, s), sp, branch);
         if (status != kOk) break;
         n_before = n_after;
     }
@@ -125,7 +125,7 @@ struct TupleOut {
 // order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
-template <bool kResiduals, int kPrecision>
+template <bool kResiduals, int kPrecision, bool kXf>
 __global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
@@ -175,7 +175,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
+        const int st = trace_ray<N, kXf>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
                                     pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
@@ -324,9 +324,12 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
                  cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     const size_t smem = trace_smem(p);
-    auto kernel = precision == MKB_PRECISION_FP64
-                      ? trace_kernel<kResiduals, MKB_PRECISION_FP64>
-                      : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA>;
+    const bool exact = precision == MKB_PRECISION_FP64;
+    auto kernel = p.non_coaxial
+                      ? (exact ? trace_kernel<kResiduals, MKB_PRECISION_FP64, true>
+                               : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA, true>)
+                      : (exact ? trace_kernel<kResiduals, MKB_PRECISION_FP64, false>
+                               : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA, false>);
     if (smem > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(
             kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

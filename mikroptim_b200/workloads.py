@@ -396,8 +396,9 @@ def tolerancing(variants: int = 262144, seed: int = 20261203 + 5, elements: int 
     variables += [Variable(VAR_THICKNESS, s, 0.05, 50.0, 1.0) for s in range(1, S - 1)]
     variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1000.0, 1.0)]
     vs = VariableSet(topo, variables)
-    x0 = (np.stack([vs.extract(b, v) for v in range(variants)]) if variants
-          else np.zeros((0, vs.size)))
+    # the variables' values of every variant (VariableSet::extract, in the variables' order)
+    x0 = np.concatenate([b.curvature[:, 1:S], b.thickness[:, 1:S - 1], b.thickness[:, S - 1:S]],
+                        axis=1)
     return b, settings, vs, x0
 
 
