@@ -40,6 +40,8 @@ extern "C" {
 #define MKB_MAX_WAVELENGTHS 16
 #define MKB_MAX_TUPLES 128      /* F * L */
 #define MKB_MAX_VARIABLES 64    /* P */
+#define MKB_MAX_GHOST_PLATES 16 /* G (the reference allows one per table surface) */
+#define MKB_MAX_GHOST_TERMS 32  /* K, kMaxGhostTerms of trace/surface_table.hpp:20 */
 
 /* ---- status codes --------------------------------------------------------------------- */
 typedef enum mkb_status {
@@ -65,7 +67,8 @@ enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_
  * equal within the reference's CPU/GPU tolerances). MIXED: FP32 bulk arithmetic with an FP64
  * sag root and OPL accumulation. */
 enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2 };
-enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2 };
+enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2,
+       MKB_VAR_GHOST_COEFFICIENT = 3 };
                                                        /* VariableType, model/variables.hpp:18 */
 
 /* ---- batch ------------------------------------------------------------------------------
@@ -91,10 +94,11 @@ typedef struct mkb_batch_view {
      * vertex (trace/surface_transform.hpp:8-14). NULL: coaxial. A non-coaxial batch traces
      * Full pupils only. */
     const double* decenter_tilt;
-    /* Ghost plates (surfaces of kind MKB_SURFACE_GHOST_PLATE, numbered in table order): the
-     * Legendre profile coefficients a_1..a_K [V][G][K] (mm), the normalisation radius r_g
-     * [V][G] (mm) and the plate's glass index [V][G][L] (trace/ghost_plate.hpp:24). NULL when
-     * ghost_plates = 0. */
+    /* Ghost plates (surfaces of kind MKB_SURFACE_GHOST_PLATE, numbered in table order; K >= 1
+     * when G > 0): the Legendre profile coefficients a_1..a_K [V][G][K] (mm), the
+     * normalisation radius r_g [G] (mm, shared by the variants as in the reference's
+     * SystemBatchHost::ghost_norm_radius(g)) and the plate's glass index [V][G][L]
+     * (trace/ghost_plate.hpp:24). NULL when ghost_plates = 0. */
     const double* ghost_coeff;
     const double* ghost_norm_radius;
     const double* ghost_index;
@@ -144,6 +148,10 @@ typedef struct mkb_variables {
     const double* lower;              /* host [P] (-inf allowed)                         */
     const double* upper;              /* host [P] (+inf allowed)                         */
     const double* typical;            /* host [P] > 0                                    */
+    /* GhostCoefficient variables (a_k of plate g; their `surface` entry is ignored): host [P]
+     * plate g (0 .. G-1, table order) and order k (1 .. K); NULL when there are none. */
+    const int32_t* ghost_plate;
+    const int32_t* ghost_order;
 } mkb_variables;
 
 /* VariableSet::apply on the device: records_out [runs][record_stride] = the run's template

@@ -81,7 +81,7 @@ class ResidualPlan(C.Structure):
 
 
 class Variables(C.Structure):
-    """mkb_variables (VariableSet for curvature / thickness / working distance)."""
+    """mkb_variables (VariableSet: curvature, thickness, working distance, ghost coefficient)."""
 
     _fields_ = [
         ("count", C.c_int32),
@@ -90,6 +90,8 @@ class Variables(C.Structure):
         ("lower", P_double),
         ("upper", P_double),
         ("typical", P_double),
+        ("ghost_plate", P_int32),
+        ("ghost_order", P_int32),
     ]
 
 

@@ -52,6 +52,8 @@ class AdjointProblem:
         out.device, out.topology, out.variants = self.device, self.templates.topology, runs
         out.stride, out.type = self.templates.stride, self.templates.type
         out.non_coaxial = self.templates.non_coaxial
+        out.ghost_plates = self.templates.ghost_plates
+        out.ghost_terms = self.templates.ghost_terms
         out.variant_surfaces = None
         out.records = torch.empty((max(runs, 1), out.stride), dtype=torch.float64,
                                   device=self.device)

@@ -27,7 +27,8 @@ from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_le
 SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
 FAILURE_SOFT, FAILURE_HARD = 0, 1
 PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA = 0, 1, 2
-VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE = 0, 1, 2
+VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT = 0, 1, 2, 3
+MAX_GHOST_PLATES, MAX_GHOST_TERMS = 16, 32
 
 MAX_SURFACES = 64
 MAX_FIELDS = 16
@@ -58,6 +59,17 @@ class BatchTopology:
     # per-surface decenter and tilt (decenter_tilt [V][S][4]); every field then uses the
     # Full pupil (check_pupil_modes, src/batch/system_batch.cpp:158)
     non_coaxial: bool = False
+    # ghost plates: the surfaces of kind GhostPlate, numbered in table order, and the profile
+    # terms K every plate carries (BatchTopology::ghost_plates / ghost_terms)
+    ghost_terms: int = 0
+
+    @property
+    def ghost_plates(self) -> int:
+        return sum(1 for t in self.type[1:] if t == SURFACE_GHOST_PLATE)
+
+    def ghost_surface(self, g: int) -> int:
+        """Table surface of plate g."""
+        return [s for s, t in enumerate(self.type) if s > 0 and t == SURFACE_GHOST_PLATE][g]
 
     def validate(self) -> None:
         if not 2 <= self.surfaces <= MAX_SURFACES:
@@ -73,10 +85,15 @@ class BatchTopology:
         if self.type[0] != SURFACE_STOP:
             raise ValueError("BatchTopology: surface 0 must be the stop")
         for s, t in enumerate(self.type[1:], start=1):
-            if t not in (SURFACE_PLANE, SURFACE_SPHERE):
-                raise NotImplementedError(
-                    f"BatchTopology: surface {s} has kind {t}; this build traces stop, plane "
-                    "and sphere surfaces")
+            if t not in (SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE):
+                raise ValueError(f"BatchTopology: surface {s} has unknown kind {t}")
+        if self.ghost_plates > MAX_GHOST_PLATES:
+            raise NotImplementedError(f"BatchTopology: at most {MAX_GHOST_PLATES} ghost plates "
+                                      "in this build")
+        if not 0 <= self.ghost_terms <= MAX_GHOST_TERMS:
+            raise ValueError(f"BatchTopology: ghost_terms must be in [0, {MAX_GHOST_TERMS}]")
+        if self.ghost_plates > 0 and self.ghost_terms < 1:
+            raise ValueError("BatchTopology: ghost plates need ghost_terms >= 1")
         if len(self.pupil_mode) != self.fields:
             raise ValueError("BatchTopology: pupil_mode needs one entry per field")
         for m in self.pupil_mode:
@@ -111,6 +128,12 @@ class SystemBatchHost:
         # radians (SystemBatchHost::decenter_tilt, system_batch.hpp:156); None when coaxial
         self.decenter_tilt: np.ndarray | None = (np.zeros((variants, S, 4))
                                                  if topology.non_coaxial else None)
+        # ghost plates (system_batch.hpp:102-131): profile coefficients a_1..a_K [V][G][K]
+        # (mm), normalisation radius r_g [G] (mm, shared), plate glass index [V][G][L]
+        G, K = topology.ghost_plates, topology.ghost_terms
+        self.ghost_coeff = np.zeros((variants, G, K))
+        self.ghost_norm_radius = np.ones(G)
+        self.ghost_index = np.ones((variants, G, L))
         # uneven batches: table surfaces each variant uses (2 .. S); None = all use S
         self.variant_surfaces: np.ndarray | None = None
 
@@ -132,7 +155,7 @@ class SystemBatchHost:
         return self.topology.fields
 
     def subset(self, first: int, count: int) -> "SystemBatchHost":
-        """Variants [first, first + count) as a new batch (assign_variants)."""
+        """Variants [first, first + count) as a new batch with its own arrays (assign_variants)."""
         if first < 0 or count < 0 or first + count > self.variants:
             raise IndexError("SystemBatchHost.subset: range out of bounds")
         out = SystemBatchHost(self.topology, 0)
@@ -143,11 +166,14 @@ class SystemBatchHost:
         sl = slice(first, first + count)
         for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
                      "field_target"):
-            setattr(out, name, np.ascontiguousarray(getattr(self, name)[sl]))
+            setattr(out, name, np.array(getattr(self, name)[sl], copy=True))
         if self.decenter_tilt is not None:
-            out.decenter_tilt = np.ascontiguousarray(self.decenter_tilt[sl])
+            out.decenter_tilt = np.array(self.decenter_tilt[sl])
+        for name in ("ghost_coeff", "ghost_index"):
+            setattr(out, name, np.array(getattr(self, name)[sl], copy=True))
+        out.ghost_norm_radius = self.ghost_norm_radius.copy()
         if self.variant_surfaces is not None:
-            out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[sl])
+            out.variant_surfaces = np.array(self.variant_surfaces[sl])
         return out
 
     def take(self, variants) -> "SystemBatchHost":
@@ -159,6 +185,9 @@ class SystemBatchHost:
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
         if self.decenter_tilt is not None:
             out.decenter_tilt = np.ascontiguousarray(self.decenter_tilt[idx])
+        for name in ("ghost_coeff", "ghost_index"):
+            setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
+        out.ghost_norm_radius = self.ghost_norm_radius.copy()
         if self.variant_surfaces is not None:
             out.variant_surfaces = np.ascontiguousarray(self.variant_surfaces[idx])
         return out
@@ -179,6 +208,12 @@ class SystemBatchHost:
                  "field_target", "wavelength_weight", "field_weight"]
         if self.decenter_tilt is not None:
             names.append("decenter_tilt")
+        names += ["ghost_coeff", "ghost_norm_radius", "ghost_index"]
+        G, K, L = self.topology.ghost_plates, self.topology.ghost_terms, self.wavelengths
+        if (self.ghost_coeff.shape != (self.variants, G, K) or
+                self.ghost_norm_radius.shape != (G,) or
+                self.ghost_index.shape != (self.variants, G, L)):
+            raise ValueError("SystemBatchHost: ghost arrays do not match the topology")
         for name in names:
             a = getattr(self, name)
             if not np.all(np.isfinite(a)):
@@ -189,6 +224,8 @@ class SystemBatchHost:
                 raise ValueError("SystemBatchHost: decenter_tilt must be [V][S][4]")
             if not np.all(np.abs(self.decenter_tilt[:, :, 2:]) < math.pi / 2):
                 raise ValueError("SystemBatchHost: tilt angles must be in (-pi/2, pi/2)")
+        if np.any(self.ghost_norm_radius <= 0) or np.any(self.ghost_index <= 0):
+            raise ValueError("SystemBatchHost: ghost plate radius and index must be > 0")
         if np.any(self.pupil_radius <= 0):
             raise ValueError("SystemBatchHost: pupil radius must be > 0")
         if np.any(self.index <= 0):
@@ -221,7 +258,8 @@ class SystemBatchHost:
         v = _capi.BatchView()
         v.variants = self.variants
         v.surfaces, v.wavelengths, v.fields = self.surfaces, self.wavelengths, self.fields
-        v.ghost_plates = v.ghost_terms = 0
+        v.ghost_plates = self.topology.ghost_plates
+        v.ghost_terms = self.topology.ghost_terms
         v.reference_wavelength_nm = self.reference_wavelength_nm
         v.type = _capi.ptr(arrays["type"], C.c_uint8)
         for name in ("wavelength_weight", "field_weight", "curvature", "thickness", "index",
@@ -231,6 +269,13 @@ class SystemBatchHost:
             dt = np.ascontiguousarray(self.decenter_tilt, dtype=np.float64)
             arrays["decenter_tilt"] = dt
             v.decenter_tilt = _capi.ptr(dt)
+        if self.topology.ghost_plates > 0:
+            for name in ("ghost_coeff", "ghost_norm_radius", "ghost_index"):
+                a = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
+                if a.size == 0:
+                    a = np.zeros(1)
+                arrays[name] = a
+                setattr(v, name, _capi.ptr(a))
         v._keep = arrays  # keep the arrays alive with the struct
         return v
 
@@ -244,14 +289,14 @@ def make_non_coaxial(batch: SystemBatchHost) -> SystemBatchHost:
     the Full pupil (make_non_coaxial, src/batch/system_batch.cpp)."""
     t = batch.topology
     topo = BatchTopology(t.surfaces, t.wavelengths, t.fields, list(t.type),
-                         [PUPIL_FULL] * t.fields, non_coaxial=True)
+                         [PUPIL_FULL] * t.fields, non_coaxial=True, ghost_terms=t.ghost_terms)
     out = SystemBatchHost(topo, batch.variants)
     out.reference_wavelength_nm = batch.reference_wavelength_nm
     out.wavelength_nm = batch.wavelength_nm.copy()
     out.wavelength_weight = batch.wavelength_weight.copy()
     out.field_weight = batch.field_weight.copy()
     for name in ("curvature", "thickness", "index", "pupil_radius", "field_angle",
-                 "field_target"):
+                 "field_target", "ghost_coeff", "ghost_norm_radius", "ghost_index"):
         setattr(out, name, np.array(getattr(batch, name), copy=True))
     if batch.variant_surfaces is not None:
         out.variant_surfaces = np.array(batch.variant_surfaces, copy=True)
@@ -352,6 +397,9 @@ class Variable:
     lower: float = -math.inf
     upper: float = math.inf
     typical: float = 1.0
+    # GhostCoefficient: a_order of plate `plate` (surface is then the plate's table surface)
+    plate: int = -1
+    order: int = 0
 
 
 @dataclass
@@ -375,9 +423,16 @@ class VariableSet:
                     raise ValueError(f"VariableSet: variable {k}: thickness surface out of range")
             elif v.type == VAR_WORKING_DISTANCE:
                 v.surface = S - 1
+            elif v.type == VAR_GHOST_COEFFICIENT:
+                if not (0 <= v.plate < self.topology.ghost_plates and
+                        1 <= v.order <= self.topology.ghost_terms):
+                    raise ValueError(f"VariableSet: variable {k}: ghost coefficient a_{v.order} "
+                                     f"of plate {v.plate} does not exist")
+                v.surface = self.topology.ghost_surface(v.plate)
             else:
                 raise NotImplementedError(f"VariableSet: variable type {v.type}")
-            key = (v.type == VAR_CURVATURE, v.surface)
+            key = ((2, v.plate, v.order) if v.type == VAR_GHOST_COEFFICIENT
+                   else (v.type == VAR_CURVATURE, v.surface))
             if key in seen:
                 raise ValueError(f"VariableSet: parameter of variable {k} already used")
             seen.add(key)
@@ -403,8 +458,11 @@ class VariableSet:
         """x from variant v (VariableSet::extract, variable_set.cpp:222)."""
         x = np.empty(self.size)
         for k, var in enumerate(self.variables):
-            x[k] = (batch.curvature[v, var.surface] if var.type == VAR_CURVATURE
-                    else batch.thickness[v, var.surface])
+            if var.type == VAR_GHOST_COEFFICIENT:
+                x[k] = batch.ghost_coeff[v, var.plate, var.order - 1]
+            else:
+                x[k] = (batch.curvature[v, var.surface] if var.type == VAR_CURVATURE
+                        else batch.thickness[v, var.surface])
         return x
 
     def apply(self, batch: SystemBatchHost, v: int, x) -> None:
@@ -417,6 +475,8 @@ class VariableSet:
         for k, var in enumerate(self.variables):
             if var.type == VAR_CURVATURE:
                 batch.curvature[v, var.surface] = x[k]
+            elif var.type == VAR_GHOST_COEFFICIENT:
+                batch.ghost_coeff[v, var.plate, var.order - 1] = x[k]
             else:
                 batch.thickness[v, var.surface] = x[k]
 
@@ -425,11 +485,15 @@ class VariableSet:
             "type": np.array([v.type for v in self.variables], dtype=np.int32),
             "surface": np.array([v.surface for v in self.variables], dtype=np.int32),
             "lower": self.lower(), "upper": self.upper(), "typical": self.typical(),
+            "ghost_plate": np.array([v.plate for v in self.variables], dtype=np.int32),
+            "ghost_order": np.array([v.order for v in self.variables], dtype=np.int32),
         }
         s = _capi.Variables()
         s.count = self.size
         s.type = _capi.ptr(keep["type"], C.c_int32)
         s.surface = _capi.ptr(keep["surface"], C.c_int32)
+        s.ghost_plate = _capi.ptr(keep["ghost_plate"], C.c_int32)
+        s.ghost_order = _capi.ptr(keep["ghost_order"], C.c_int32)
         s.lower, s.upper, s.typical = (_capi.ptr(keep[n]) for n in ("lower", "upper", "typical"))
         s._keep = keep
         return s

@@ -95,8 +95,11 @@ __device__ int forward_record(const TraceParams& p, const double* rec, const Rec
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
+        GhostData gd;
+        const bool plate = ghost_at<true>(p, rec, lay, s, l, gd);
         status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, n_before / n_after,
-                                    xf_of(rec, lay, s), sp, branch);
+                                    xf_of(rec, lay, s), sp, branch, nullptr,
+                                    plate ? &gd : nullptr, n_after);
         if (status != kOk) break;
         out.count = s + 1;
         out.set_branch(s, branch);
@@ -161,8 +164,11 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                 const N cs = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
                 int branch;
                 const N nb = idx[(s - 1) * L + l], na = idx[s * L + l];
+                GhostData gd;
+                const bool plate = ghost_at<true>(p, rec, lay, s, l, gd);
                 step_surface_xf<N>(r, N(thick[s - 1]), cs, nb, nb / na, xf_of(rec, lay, s),
-                                   soft_mode ? &dummy : nullptr, branch);
+                                   soft_mode ? &dummy : nullptr, branch, nullptr,
+                                   plate ? &gd : nullptr, na);
                 sp[i] = {r.px, r.py, r.pz};
                 sd[i] = {r.dx, r.dy, r.dz};
             }
@@ -198,9 +204,23 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                         tl = zero;
                         adjoint_to_surface(tr, adj);
                     }
-                    refracting_step_backward<N>(pl, dl, tl, cj, N(idx[s * L + l]),
-                                                N(idx[j * L + l]), next_branch, seed_opl,
-                                                seed_pen, adj, par);
+                    GhostData gd;
+                    if (ghost_at<true>(p, rec, lay, j, l, gd)) {
+                        const int g = p.ghost_of[j];
+                        const N so[1] = {seed_opl}, sq[1] = {seed_pen};
+                        RayAdj<N> a[1] = {adj};
+                        StepAdj<N> o[1] = {par};
+                        ghost_step_backward_k<N, N, 1>(
+                            pl, dl, tl, gd, N(idx[s * L + l]), N(idx[j * L + l]), next_branch,
+                            so, sq, a, o,
+                            [&](int, int k, N value) { write(v.col_ghost[g][k], value); });
+                        adj = a[0];
+                        par = o[0];
+                    } else {
+                        refracting_step_backward<N>(pl, dl, tl, cj, N(idx[s * L + l]),
+                                                    N(idx[j * L + l]), next_branch, seed_opl,
+                                                    seed_pen, adj, par);
+                    }
                     if (moved) {
                         adjoint_from_surface(tr, adj);
                         par.thickness = -adj.p.z;
@@ -497,7 +517,7 @@ struct RowSinks {
     int ld[K];
 };
 
-template <class N, class Q, bool kXf>
+template <class N, class Q, int kFeat>
 __device__ void fused_forward(const TraceParams& p, const double* rec, const double* mu_tab,
                               const RecordLayout& lay, int S, int f, int l, const Sample& smp,
                               bool soft_mode, Q* ck,
@@ -543,8 +563,11 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
         keep_state(q);
         int branch;
         StepLocal<N> loc{zero, zero, zero, zero, zero};
+        GhostData gd;
+        const bool plate = ghost_at<(kFeat & 2) != 0>(p, rec, lay, s, l, gd);
         status = step_surface_xf<N, true>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
-                                          xf_at<kXf>(rec, lay, s), sp, branch, &loc);
+                                          xf_at<(kFeat & 1) != 0>(rec, lay, s), sp, branch, &loc,
+                                          plate ? &gd : nullptr, n_after);
         if (status != kOk) break;
         q[6 * kFusedThreads] = Q(value_of(loc.s0));
         q[7 * kFusedThreads] = Q(value_of(loc.s));
@@ -582,7 +605,7 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
 // factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
 // quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
 // out-of-line copy per K keeps the kernel's instruction footprint small.
-template <class N, class A, int K, bool kXf, class Q, class YT>
+template <class N, class A, int K, int kFeat, class Q, class YT>
 __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParams& v,
                                             const double* rec, const double* mu_tab,
                                             const RecordLayout& lay, int S,
@@ -657,7 +680,27 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
             StepAdj<A> par[K];
 #pragma unroll
             for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
-            const double* xf = xf_at<kXf>(rec, lay, j);
+            GhostData gd;
+            const bool plate = ghost_at<(kFeat & 2) != 0>(p, rec, lay, j, l, gd);
+            // the step in the surface's own frame: a ghost plate (its profile coefficients
+            // are variables too) or a refracting sphere / plane
+            auto local = [&](Vec<N> pl, Vec<N> dl, N tl) {
+                if (plate) {
+                    const int g = p.ghost_of[j];
+                    ghost_step_backward_k<N, A, K>(
+                        pl, dl, tl, gd, N(idx[c * L + l]), N(idx[j * L + l]), next_branch,
+                        seed_opl, seed_pen, adj, par, [&](int m, int k, A value) {
+                            const int col = v.col_ghost[g][k];
+                            if (col >= 0)
+                                sinks.row[m][col * sinks.ld[m]] = YT(value_of(factor[m] * value));
+                        });
+                } else {
+                    refracting_step_backward_k<N, A, K>(pl, dl, tl, cj, N(idx[c * L + l]),
+                                                        N(idx[j * L + l]), next_branch, seed_opl,
+                                                        seed_pen, adj, par, &cur.loc);
+                }
+            };
+            const double* xf = xf_at<(kFeat & 1) != 0>(rec, lay, j);
             if (xf != nullptr && xf[6] > 0.0) {  // decentered / tilted surface
                 const Transform<N> tn = transform_at<N>(xf);
                 const Transform<A> ta = transform_at<A>(xf);
@@ -665,19 +708,14 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                 state_to_surface(tn, pl, dl, N(thick[c]));
 #pragma unroll
                 for (int m = 0; m < K; ++m) adjoint_to_surface(ta, adj[m]);
-                refracting_step_backward_k<N, A, K>(pl, dl, zero, cj, N(idx[c * L + l]),
-                                                    N(idx[j * L + l]), next_branch, seed_opl,
-                                                    seed_pen, adj, par, &cur.loc);
+                local(pl, dl, zero);
 #pragma unroll
                 for (int m = 0; m < K; ++m) {
                     adjoint_from_surface(ta, adj[m]);
                     par[m].thickness = -adj[m].p.z;
                 }
             } else {
-                refracting_step_backward_k<N, A, K>(cur.p, cur.d, N(thick[c]), cj,
-                                                    N(idx[c * L + l]), N(idx[j * L + l]),
-                                                    next_branch, seed_opl, seed_pen, adj, par,
-                                                    &cur.loc);
+                local(cur.p, cur.d, N(thick[c]));
             }
             const int cc = sphere ? v.col_curvature[j] : -1;
             const int ct = v.col_thickness[c];
@@ -718,7 +756,7 @@ template <> struct FusedTypes<MixedPrecision> {
     using Row = float;
 };
 
-template <class N, int K, bool kXf>
+template <class N, int K, int kFeat>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
                                              const double* rec, const double* mu_tab,
                                              const RecordLayout& lay, int S,
@@ -730,7 +768,7 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                              const double (&spn)[K],
                                              const RowSinks<K, typename FusedTypes<N>::Row>& sinks) {
     using T = FusedTypes<N>;
-    fused_backward<typename T::Bwd, typename T::Adj, K, kXf>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
+    fused_backward<typename T::Bwd, typename T::Adj, K, kFeat>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
                                                         reached_image, soft_mode, so, spn, sinks);
 }
@@ -752,7 +790,7 @@ struct FusedArgs {
     int64_t gram_stride;   // doubles per run of `gram`
 };
 
-template <class N, bool kXf>
+template <class N, int kFeat>
 __global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ? 4 : kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
@@ -855,7 +893,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                fused_forward<typename FusedTypes<N>::Fwd, Keep, kXf>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
+                fused_forward<typename FusedTypes<N>::Fwd, Keep, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
                                                            my_ck, stride_ck, br_lo, br_hi, count,
                                                            image_branch, status, soft_first, opl,
                                                            penalty);
@@ -874,7 +912,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double so[2] = {piston ? 1.0 : 0.0, 0.0};
                         const double sp[2] = {0.0, pen_sweep ? 1.0 : 0.0};
                         const RowSinks<2, YT> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
-                        run_backward<N, 2, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                        run_backward<N, 2, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
                                            sinks);
                     }
@@ -884,18 +922,18 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const double sp[1] = {pen_sweep ? 1.0 : 0.0};
                         const RowSinks<1, YT> sinks{{piston ? 1.0 : pfac}, {piston ? row : prow},
                                                 {piston ? TS : kFusedThreads}};
-                        run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
+                        run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
                                            so, sp, sinks);
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
                     const RowSinks<1, YT> s0{{1.0}, {row}, {TS}};
-                    run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
                     const RowSinks<1, YT> s1{{pfac}, {prow}, {kFusedThreads}};
-                    run_backward<N, 1, kXf>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
+                    run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                        br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
                 }
             }
@@ -1095,13 +1133,20 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
     const size_t smem = fused_adjoint_smem(
         tp, p_max, precision == MKB_PRECISION_MIXED ? sizeof(float) : sizeof(double));
-    auto kernel = tp.non_coaxial
-                      ? (precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64, true>
-                         : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision, true>
-                                                            : adjoint_gram_kernel<double, true>)
-                      : (precision == MKB_PRECISION_FP64    ? adjoint_gram_kernel<Exact64, false>
-                         : precision == MKB_PRECISION_MIXED ? adjoint_gram_kernel<MixedPrecision, false>
-                                                            : adjoint_gram_kernel<double, false>);
+    // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
+    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0);
+    auto pick = [&](auto f0, auto f1, auto f2, auto f3) {
+        return feat == 0 ? f0 : feat == 1 ? f1 : feat == 2 ? f2 : f3;
+    };
+    auto kernel =
+        precision == MKB_PRECISION_FP64
+            ? pick(adjoint_gram_kernel<Exact64, 0>, adjoint_gram_kernel<Exact64, 1>,
+                   adjoint_gram_kernel<Exact64, 2>, adjoint_gram_kernel<Exact64, 3>)
+        : precision == MKB_PRECISION_MIXED
+            ? pick(adjoint_gram_kernel<MixedPrecision, 0>, adjoint_gram_kernel<MixedPrecision, 1>,
+                   adjoint_gram_kernel<MixedPrecision, 2>, adjoint_gram_kernel<MixedPrecision, 3>)
+            : pick(adjoint_gram_kernel<double, 0>, adjoint_gram_kernel<double, 1>,
+                   adjoint_gram_kernel<double, 2>, adjoint_gram_kernel<double, 3>);
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");

@@ -237,6 +237,136 @@ __device__ __forceinline__ void refracting_step_backward_k(Vec<N> p, Vec<N> d, N
     }
 }
 
+// K adjoint vectors through a ghost-plate step (ghost_step_backward,
+// trace/adjoint_backward.hpp:253): the forward quantities recomputed in N, the adjoint
+// arithmetic in A, every statement in the reference's order. The profile's second derivative
+// comes from P''_{k+1} = P''_{k-1} + (2k + 1) P'_k. coeff(m, k, value) receives the adjoint of
+// a_{k+1} for seed m (k = 0 .. K-1); out[m].curvature is left alone.
+template <class N, class A, int K, class CoeffSink>
+__device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, const GhostData& g,
+                                                      N n_before, N n_after, int branch,
+                                                      const A (&seed_opl)[K],
+                                                      const A (&seed_pen)[K],
+                                                      RayAdj<A> (&adj)[K], StepAdj<A> (&out)[K],
+                                                      CoeffSink&& coeff) {
+    const N one(1.0), two(2.0);
+    // ---- forward ----
+    const N z = p.z - t;
+    const N s0 = -z / d.z;
+    const N x = p.x + s0 * d.x;
+    const N y = p.y + s0 * d.y;
+    const N radius = g.radius;
+    const N inv_r2 = one / (radius * radius);
+    const N u = (x * x + y * y) * inv_r2;
+    const N xi = two * u - one;
+    N prof_t(0.0), sum_dp(0.0), sum_ddp(0.0);
+    {
+        N p_prev = one, p_cur = xi, dp_prev(0.0), dp_cur = one, ddp_prev(0.0), ddp_cur(0.0);
+        for (int k = 1; k <= g.K; ++k) {
+            const N a = g.coeff[k - 1];
+            prof_t += a * p_cur;
+            sum_dp += a * dp_cur;
+            sum_ddp += a * ddp_cur;
+            const N p_next = (N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev) /
+                             N(double(k + 1));
+            const N dp_next = dp_prev + N(double(2 * k + 1)) * p_cur;
+            const N ddp_next = ddp_prev + N(double(2 * k + 1)) * dp_cur;
+            p_prev = p_cur;
+            p_cur = p_next;
+            dp_prev = dp_cur;
+            dp_cur = dp_next;
+            ddp_prev = ddp_cur;
+            ddp_cur = ddp_next;
+        }
+    }
+    const N dt_du = two * sum_dp;
+    const N d2t_du2 = N(4.0) * sum_ddp;
+    const N dn = N(g.n_glass) - n_before;
+    const N radial = dn * dt_du * two * inv_r2;
+    const N dx = (n_before * d.x + radial * x) / n_after;
+    const N dy = (n_before * d.y + radial * y) / n_after;
+    const N radicand = one - dx * dx - dy * dy;
+    const bool tir = (branch & kBranchSoftTir) != 0;
+    N inv_m(0.0), ex(0.0), ey(0.0), root(0.0);
+    if (tir) {
+        inv_m = one / nsqrt(dx * dx + dy * dy);
+        ex = dx * inv_m;
+        ey = dy * inv_m;
+    } else {
+        root = nsqrt(radicand);
+    }
+    // ---- reverse, in A ----
+    const A zero_a(0.0), two_a(2.0);
+    const A adx = cv<A>(dx), ady = cv<A>(dy), ax = cv<A>(x), ay = cv<A>(y);
+    const A ainv_m = cv<A>(inv_m), aex = cv<A>(ex), aey = cv<A>(ey), aroot = cv<A>(root);
+    const A anb = cv<A>(n_before), ana = cv<A>(n_after), ad_x = cv<A>(d.x), ad_y = cv<A>(d.y);
+    const A aradial = cv<A>(radial), as0 = cv<A>(s0), adn = cv<A>(dn), aprof = cv<A>(prof_t);
+    const A adtdu = cv<A>(dt_du), ad2t = cv<A>(d2t_du2), ainv_r2 = cv<A>(inv_r2);
+    const A axi = cv<A>(xi), ad_z = cv<A>(d.z);
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        const Vec<A> qb = adj[m].p;
+        const Vec<A> d1b = adj[m].d;
+        RayAdj<A> in{{zero_a, zero_a, zero_a}, {zero_a, zero_a, zero_a}};
+        A dxb, dyb, radb;
+        if (tir) {
+            const A proj = aex * d1b.x + aey * d1b.y;
+            dxb = (d1b.x - proj * aex) * ainv_m;
+            dyb = (d1b.y - proj * aey) * ainv_m;
+            radb = -seed_pen[m];
+        } else {
+            dxb = d1b.x;
+            dyb = d1b.y;
+            radb = d1b.z / (two_a * aroot);
+        }
+        dxb += -two_a * adx * radb;
+        dyb += -two_a * ady * radb;
+        in.d.x += dxb * anb / ana;
+        in.d.y += dyb * anb / ana;
+        out[m].n_before += (dxb * ad_x + dyb * ad_y) / ana;
+        out[m].n_after += -(dxb * adx + dyb * ady) / ana;
+        const A gxb = dxb / ana;
+        const A gyb = dyb / ana;
+        const A radialb = gxb * ax + gyb * ay;
+        A xb = qb.x + gxb * aradial;
+        A yb = qb.y + gyb * aradial;
+        A s0b = seed_opl[m] * anb;
+        out[m].n_before += seed_opl[m] * as0;
+        const A phaseb = seed_opl[m];
+        const A dnb = phaseb * aprof + radialb * adtdu * two_a * ainv_r2;
+        const A tb = phaseb * adn;
+        const A dtdub = radialb * adn * two_a * ainv_r2;
+        out[m].n_before += -dnb;
+        const A ub = tb * adtdu + dtdub * ad2t;
+        {
+            A p_prev(1.0), p_cur = axi, dp_prev(0.0), dp_cur(1.0);
+            for (int k = 1; k <= g.K; ++k) {
+                coeff(m, k - 1, tb * p_cur + dtdub * two_a * dp_cur);
+                const A p_next = (A(double(2 * k + 1)) * axi * p_cur - A(double(k)) * p_prev) /
+                                 A(double(k + 1));
+                const A dp_next = dp_prev + A(double(2 * k + 1)) * p_cur;
+                p_prev = p_cur;
+                p_cur = p_next;
+                dp_prev = dp_cur;
+                dp_cur = dp_next;
+            }
+        }
+        xb += ub * two_a * ax * ainv_r2;
+        yb += ub * two_a * ay * ainv_r2;
+        // transfer: s0 = (t - p_z) / d_z (transfer_backward, adjoint_backward.hpp:91)
+        in.p.x += xb;
+        in.p.y += yb;
+        s0b += xb * ad_x + yb * ad_y;
+        in.d.x += xb * as0;
+        in.d.y += yb * as0;
+        const A qq = s0b / ad_z;
+        out[m].thickness += qq;
+        in.p.z += -qq;
+        in.d.z += -qq * as0;
+        adj[m] = in;
+    }
+}
+
 template <class N>
 __device__ __forceinline__ void refracting_step_backward(Vec<N> p, Vec<N> d, N t, N c, N n_before,
                                                          N n_after, int branch, N seed_opl,

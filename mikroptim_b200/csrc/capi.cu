@@ -136,9 +136,9 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         return MKB_ERR_ARGUMENT;
     }
     if (batch->ghost_plates < 0 || batch->ghost_terms < 0 ||
-        batch->ghost_plates > kMaxSurfaces || batch->ghost_terms > kMaxGhostTerms) {
+        batch->ghost_plates > kMaxGhostPlates || batch->ghost_terms > kMaxGhostTerms) {
         set_error("ghost plates (G=%d, K=%d) out of range [0, %d] x [0, %d]",
-                  batch->ghost_plates, batch->ghost_terms, kMaxSurfaces, kMaxGhostTerms);
+                  batch->ghost_plates, batch->ghost_terms, kMaxGhostPlates, kMaxGhostTerms);
         return MKB_ERR_ARGUMENT;
     }
     const RecordLayout lay = record_layout(S, L, F, batch->non_coaxial, batch->ghost_plates,
@@ -167,17 +167,26 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         set_error("surface 0 must be the stop");
         return MKB_ERR_ARGUMENT;
     }
+    int plates = 0;
     for (int s = 1; s < S; ++s) {
         const int t = batch->type[s];
         if (t == MKB_SURFACE_GHOST_PLATE) {
-            set_error("surface %d is a ghost plate; this build traces stop, plane and sphere",
-                      s);
-            return MKB_ERR_UNSUPPORTED;
+            ++plates;
+            continue;
         }
         if (t != MKB_SURFACE_PLANE && t != MKB_SURFACE_SPHERE) {
             set_error("surface %d has unknown kind %d", s, t);
             return MKB_ERR_ARGUMENT;
         }
+    }
+    if (plates != batch->ghost_plates) {
+        set_error("the table has %d ghost-plate surfaces but the batch carries %d plates",
+                  plates, batch->ghost_plates);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (plates > kMaxGhostPlates) {
+        set_error("%d ghost plates; this build traces at most %d", plates, kMaxGhostPlates);
+        return MKB_ERR_UNSUPPORTED;
     }
     TraceParams& p = *out;
     std::memset(&p, 0, sizeof(p));
@@ -194,7 +203,12 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     p.failure = plan->failure;
     p.rings = plan->rings;
     p.spokes = plan->spokes;
-    for (int s = 0; s < S; ++s) p.type[s] = batch->type[s];
+    for (int s = 0, g = 0; s < kMaxSurfaces; ++s) {
+        p.ghost_of[s] = -1;
+        if (s >= S) continue;
+        p.type[s] = batch->type[s];
+        if (s > 0 && batch->type[s] == MKB_SURFACE_GHOST_PLATE) p.ghost_of[s] = static_cast<int8_t>(g++);
+    }
     int offset = 0;
     for (int f = 0; f < F; ++f) {
         p.pupil_mode[f] = plan->pupil_mode[f];
@@ -260,7 +274,8 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     return MKB_OK;
 }
 
-int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out) {
+int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out,
+                    int ghost_terms) {
     if (vars == nullptr || vars->count < 1 || vars->count > MKB_MAX_VARIABLES) {
         set_error("variables: count must be in [1, %d]", MKB_MAX_VARIABLES);
         return MKB_ERR_ARGUMENT;
@@ -273,30 +288,53 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
     std::memset(&v, 0, sizeof(v));
     v.P = vars->count;
     for (int s = 0; s < kMaxSurfaces; ++s) v.col_curvature[s] = v.col_thickness[s] = -1;
+    std::memset(v.col_ghost, -1, sizeof(v.col_ghost));
+    // table surface of every ghost plate (plates are numbered in table order)
+    int plate_surface[kMaxGhostPlates];
+    int plates = 0;
+    for (int s = 1; s < S; ++s)
+        if (type[s] == MKB_SURFACE_GHOST_PLATE && plates < kMaxGhostPlates)
+            plate_surface[plates++] = s;
     for (int k = 0; k < v.P; ++k) {
         const int t = vars->type[k];
         int s = vars->surface[k];
         if (t == MKB_VAR_WORKING_DISTANCE) s = S - 1;
-        if (t != MKB_VAR_CURVATURE && t != MKB_VAR_THICKNESS && t != MKB_VAR_WORKING_DISTANCE) {
-            set_error("variable %d: unknown type %d (curvature, thickness, working distance)", k,
-                      t);
+        if (t != MKB_VAR_CURVATURE && t != MKB_VAR_THICKNESS && t != MKB_VAR_WORKING_DISTANCE &&
+            t != MKB_VAR_GHOST_COEFFICIENT) {
+            set_error("variable %d: unknown type %d (curvature, thickness, working distance, "
+                      "ghost coefficient)", k, t);
             return MKB_ERR_UNSUPPORTED;
         }
-        if (s < 0 || s >= S || (t == MKB_VAR_THICKNESS && s == S - 1)) {
-            set_error("variable %d: surface %d out of range", k, s);
+        int8_t* slot;
+        if (t == MKB_VAR_GHOST_COEFFICIENT) {
+            const int g = vars->ghost_plate ? vars->ghost_plate[k] : -1;
+            const int order = vars->ghost_order ? vars->ghost_order[k] : 0;
+            if (g < 0 || g >= plates || order < 1 || order > ghost_terms) {
+                set_error("variable %d: ghost coefficient a_%d of plate %d out of range "
+                          "(%d plates, %d terms)", k, order, g, plates, ghost_terms);
+                return MKB_ERR_ARGUMENT;
+            }
+            s = plate_surface[g];
+            v.ghost_plate[k] = static_cast<int8_t>(g);
+            v.ghost_order[k] = static_cast<int8_t>(order);
+            slot = &v.col_ghost[g][order - 1];
+        } else {
+            if (s < 0 || s >= S || (t == MKB_VAR_THICKNESS && s == S - 1)) {
+                set_error("variable %d: surface %d out of range", k, s);
+                return MKB_ERR_ARGUMENT;
+            }
+            if (t == MKB_VAR_CURVATURE && type[s] != MKB_SURFACE_SPHERE) {
+                set_error("variable %d: curvature of surface %d, which is not a sphere", k, s);
+                return MKB_ERR_ARGUMENT;
+            }
+            slot = t == MKB_VAR_CURVATURE ? &v.col_curvature[s] : &v.col_thickness[s];
+        }
+        if (*slot >= 0) {
+            set_error("variable %d: its parameter already belongs to variable %d", k, *slot);
             return MKB_ERR_ARGUMENT;
         }
-        if (t == MKB_VAR_CURVATURE && type[s] != MKB_SURFACE_SPHERE) {
-            set_error("variable %d: curvature of surface %d, which is not a sphere", k, s);
-            return MKB_ERR_ARGUMENT;
-        }
-        int8_t& slot = t == MKB_VAR_CURVATURE ? v.col_curvature[s] : v.col_thickness[s];
-        if (slot >= 0) {
-            set_error("variable %d: its parameter already belongs to variable %d", k, slot);
-            return MKB_ERR_ARGUMENT;
-        }
-        slot = static_cast<int8_t>(k);
-        v.type[k] = static_cast<int8_t>(t == MKB_VAR_CURVATURE ? MKB_VAR_CURVATURE : MKB_VAR_THICKNESS);
+        *slot = static_cast<int8_t>(k);
+        v.type[k] = static_cast<int8_t>(t == MKB_VAR_WORKING_DISTANCE ? MKB_VAR_THICKNESS : t);
         v.surface[k] = static_cast<int8_t>(s);
         v.lower[k] = vars->lower[k];
         v.upper[k] = vars->upper[k];
@@ -358,7 +396,7 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
         return MKB_ERR_ARGUMENT;
     }
     const int G = v->ghost_plates, K = v->ghost_terms;
-    if (G < 0 || K < 0 || G > kMaxSurfaces || K > kMaxGhostTerms ||
+    if (G < 0 || K < 0 || G > kMaxGhostPlates || K > kMaxGhostTerms ||
         (G > 0 && (!v->ghost_coeff || !v->ghost_norm_radius || !v->ghost_index))) {
         set_error("pack: ghost plates (G=%d, K=%d) out of range or without data", G, K);
         return MKB_ERR_ARGUMENT;
@@ -401,7 +439,7 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
         for (int g = 0; g < G; ++g) {
             for (int k = 0; k < K; ++k)
                 r[lay.ghost_coeff + g * K + k] = v->ghost_coeff[(i * G + g) * K + k];
-            r[lay.ghost_radius + g] = v->ghost_norm_radius[i * G + g];
+            r[lay.ghost_radius + g] = v->ghost_norm_radius[g];
             for (int l = 0; l < L; ++l)
                 r[lay.ghost_index + g * L + l] = v->ghost_index[(i * G + g) * L + l];
         }
@@ -437,7 +475,7 @@ int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_vari
         return MKB_ERR_ARGUMENT;
     }
     VarParams vp;
-    const int rc = make_var_params(vars, S, templates->type, &vp);
+    const int rc = make_var_params(vars, S, templates->type, &vp, templates->ghost_terms);
     if (rc != MKB_OK) return rc;
     return launch_apply(vp, lay, templates->records, templates->variants, x, records_out, runs,
                         static_cast<cudaStream_t>(stream));

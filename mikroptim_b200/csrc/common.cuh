@@ -18,7 +18,8 @@ constexpr int kMaxFields = MKB_MAX_FIELDS;
 constexpr int kMaxTuples = MKB_MAX_TUPLES;
 constexpr int kMaxPacks = 256;
 constexpr int kMaxPackTuples = 16;
-constexpr int kMaxGhostTerms = 32;  // kMaxGhostTerms of the reference (trace/surface_table.hpp)
+constexpr int kMaxGhostTerms = MKB_MAX_GHOST_TERMS;  // the reference's kMaxGhostTerms
+constexpr int kMaxGhostPlates = MKB_MAX_GHOST_PLATES;
 
 // Trace status and soft-failure branch codes (reference: trace/surface_ops.hpp:24,113).
 enum : int { kOk = 0, kMissed = 1, kTir = 2, kBackward = 3, kUnsupported = 4,
@@ -41,6 +42,7 @@ struct RecordLayout {
     int curvature, thickness, index, pupil, sin_theta, cos_theta, target, stride, surfaces;
     int xf;                                      // transforms, or -1 (coaxial)
     int ghost_coeff, ghost_radius, ghost_index;  // ghost plate data, or -1 (no plates)
+    int ghost_terms;                             // K
 };
 
 __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int non_coaxial = 0,
@@ -58,6 +60,7 @@ __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int n
     r.xf = non_coaxial ? n : -1;
     if (non_coaxial) n += S * kXfValues;
     r.ghost_coeff = r.ghost_radius = r.ghost_index = -1;
+    r.ghost_terms = K;
     if (G > 0) {
         r.ghost_coeff = n;
         n += G * K;
@@ -100,6 +103,7 @@ struct TraceParams {
     double scale[kMaxTuples];       // residual_scale per tuple
     double pscale[kMaxTuples];      // penalty_scale per tuple
     Pack packs[kMaxPacks];
+    int8_t ghost_of[kMaxSurfaces];  // plate number of a ghost-plate surface (table order), or -1
     const uint8_t* vsurf;           // device [V] table surfaces of each variant, or null (S)
     const int* order;               // device [V] processing order of the variants, or null
 };
@@ -346,6 +350,102 @@ __device__ __forceinline__ int step_surface(RayT<N>& r, N t, N c, N n_before, N 
     return step_surface_mu<N, kKeep>(r, t, c, n_before, n_before / n_after, soft, branch, keep);
 }
 
+// ---- ghost plates (trace/ghost_plate.hpp) ---------------------------------------------------
+// One plate at one wavelength: profile coefficients a_1..a_K, normalisation radius r_g, glass
+// index n_G (GhostPlateParams, ghost_plate.hpp:24).
+struct GhostData {
+    const double* coeff;
+    int K;
+    double radius;
+    double n_glass;
+};
+
+// The plate data of surface s at wavelength l when the kernel was built for ghost plates
+// (kGhost) and s is one; false otherwise (at compile time for kernels without plates).
+template <bool kGhost>
+__device__ __forceinline__ bool ghost_at(const TraceParams& p, const double* rec,
+                                         const RecordLayout& lay, int s, int l, GhostData& g) {
+    if constexpr (!kGhost) {
+        return false;
+    } else {
+        const int gi = p.ghost_of[s];
+        if (gi < 0) return false;
+        g = {rec + lay.ghost_coeff + gi * p.K, p.K, rec[lay.ghost_radius + gi],
+             rec[lay.ghost_index + gi * p.L + l]};
+        return true;
+    }
+}
+
+// Thickness profile t(u) = sum_k a_k P_k(2u - 1) and dt/du = 2 sum_k a_k P'_k(2u - 1) by the
+// Legendre recurrences in ascending k (ghost_profile, ghost_plate.hpp:67).
+template <class N>
+__device__ __forceinline__ void ghost_profile(const GhostData& g, N u, N& t, N& dt_du) {
+    const N one(1.0), two(2.0);
+    const N xi = two * u - one;
+    N p_prev = one, p_cur = xi, dp_prev(0.0), dp_cur = one;
+    N tt(0.0), dt(0.0);
+    for (int k = 1; k <= g.K; ++k) {
+        const N a = g.coeff[k - 1];
+        tt += a * p_cur;
+        dt += a * dp_cur;
+        const N p_next = (N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev) /
+                         N(double(k + 1));
+        const N dp_next = dp_prev + N(double(2 * k + 1)) * p_cur;
+        p_prev = p_cur;
+        p_cur = p_next;
+        dp_prev = dp_cur;
+        dp_cur = dp_next;
+    }
+    t = tt;
+    dt_du = two * dt;
+}
+
+// The step onto a ghost plate (propagate_surface_local with kind GhostPlate, trace.hpp:191, and
+// ghost_plate_step / phase_surface_step, ghost_plate.hpp:130,159): transfer to the plane z = 0,
+// OPL += n s0, OPL += Phi = (n_G - n) t(u), n' d'_perp = n d_perp + grad Phi, d'_z =
+// sqrt(1 - |d'_perp|^2); a negative radicand is TIR (soft: penalty -radicand, d' in the plane).
+template <class N, bool kKeep = false>
+__device__ __forceinline__ int ghost_step(RayT<N>& r, N t, N n_before, N n_after,
+                                          const GhostData& g, SoftT<N>* soft, int& branch,
+                                          StepLocal<N>* keep = nullptr) {
+    const N zero(0.0), one(1.0), two(2.0);
+    if (!(r.dz > zero)) return kBackward;
+    r.pz -= t;
+    const N s0 = -r.pz / r.dz;
+    r.px = r.px + s0 * r.dx;
+    r.py = r.py + s0 * r.dy;
+    r.pz = zero;
+    r.opl += n_before * s0;
+    const N radius = g.radius;
+    const N inv_r2 = one / (radius * radius);
+    const N u = (r.px * r.px + r.py * r.py) * inv_r2;
+    N prof_t, dt_du;
+    ghost_profile<N>(g, u, prof_t, dt_du);
+    const N dn = N(g.n_glass) - n_before;
+    const N radial = dn * dt_du * two * inv_r2;
+    const N gx = radial * r.px, gy = radial * r.py;
+    r.opl += dn * prof_t;
+    const N dx = (n_before * r.dx + gx) / n_after;
+    const N dy = (n_before * r.dy + gy) / n_after;
+    const N radicand = one - dx * dx - dy * dy;
+    if constexpr (kKeep) *keep = {s0, zero, zero, zero, zero};
+    branch = kBranchRegular;
+    if (radicand < zero) {
+        if (soft == nullptr) return kTir;
+        soft->add(-radicand, kSoftTir);
+        const N inv = one / nsqrt(dx * dx + dy * dy);
+        r.dx = dx * inv;
+        r.dy = dy * inv;
+        r.dz = zero;
+        branch = kBranchSoftTir;
+        return kOk;
+    }
+    r.dx = dx;
+    r.dy = dy;
+    r.dz = nsqrt(radicand);
+    return kOk;
+}
+
 // ---- decenter and tilt of a surface (trace/surface_transform.hpp:27-85) -----------------
 // R = R_y(b) R_x(a); a point q of the tilted surface frame lies at R q + (dx, dy, 0) in the
 // nominal frame. xf points at the surface's kXfValues record values.
@@ -408,17 +508,25 @@ __device__ __forceinline__ void ray_from_surface(RayT<N>& r, const Transform<N>&
 // z -= t in the nominal frame, into the tilted frame, the local step with t = 0 (its own
 // d_z > 0 check), and back into the nominal frame when it succeeded. The StepLocal values
 // are those of the local step.
+// `ghost` (or null): the surface is a ghost plate with these data; the step then divides by
+// n_after itself (mu is not used).
 template <class N, bool kKeep = false>
 __device__ __forceinline__ int step_surface_xf(RayT<N>& r, N t, N c, N n_before, N mu,
                                                const double* xf, SoftT<N>* soft, int& branch,
-                                               StepLocal<N>* keep = nullptr) {
-    if (xf == nullptr || !(xf[6] > 0.0))
-        return step_surface_mu<N, kKeep>(r, t, c, n_before, mu, soft, branch, keep);
+                                               StepLocal<N>* keep = nullptr,
+                                               const GhostData* ghost = nullptr,
+                                               N n_after = N(1.0)) {
+    auto local = [&](N tl) {
+        return ghost != nullptr
+                   ? ghost_step<N, kKeep>(r, tl, n_before, n_after, *ghost, soft, branch, keep)
+                   : step_surface_mu<N, kKeep>(r, tl, c, n_before, mu, soft, branch, keep);
+    };
+    if (xf == nullptr || !(xf[6] > 0.0)) return local(t);
     if (!(r.dz > N(0.0))) return kBackward;
     r.pz -= t;
     const Transform<N> tr = transform_at<N>(xf);
     ray_to_surface(r, tr);
-    const int st = step_surface_mu<N, kKeep>(r, N(0.0), c, n_before, mu, soft, branch, keep);
+    const int st = local(N(0.0));
     if (st == kOk) ray_from_surface(r, tr);
     return st;
 }
@@ -476,20 +584,32 @@ struct VarParams {
     int8_t surface[MKB_MAX_VARIABLES];    // table surface of the parameter
     int8_t col_curvature[kMaxSurfaces];   // column of curvature[s], -1 if none
     int8_t col_thickness[kMaxSurfaces];   // column of thickness[s], -1 if none
+    int8_t ghost_plate[MKB_MAX_VARIABLES];  // GhostCoefficient variables: plate g
+    int8_t ghost_order[MKB_MAX_VARIABLES];  // and order k (1 .. K)
+    int8_t col_ghost[kMaxGhostPlates][kMaxGhostTerms];  // column of a_{k+1} of plate g, or -1
     double lower[MKB_MAX_VARIABLES], upper[MKB_MAX_VARIABLES], typical[MKB_MAX_VARIABLES];
 };
 
 // Builds the variable block for a batch with S surfaces; MKB_OK or MKB_ERR_ARGUMENT.
-int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out);
+// ghost_terms: K of the batch (GhostCoefficient variables need k <= K).
+int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out,
+                    int ghost_terms = 0);
 
 // Writes x into a packed record (VariableSet::apply, src/optim/variable_set.cpp:237).
+// Writes variable k's value into a record (curvature, thickness / working distance, or a ghost
+// plate's profile coefficient).
+__device__ __forceinline__ void write_variable(const VarParams& v, const RecordLayout& lay, int k,
+                                               double x, double* rec) {
+    const int s = v.surface[k];
+    if (v.type[k] == MKB_VAR_CURVATURE) rec[lay.curvature + s] = x;
+    else if (v.type[k] == MKB_VAR_GHOST_COEFFICIENT)
+        rec[lay.ghost_coeff + v.ghost_plate[k] * lay.ghost_terms + v.ghost_order[k] - 1] = x;
+    else rec[lay.thickness + s] = x;
+}
+
 __device__ __forceinline__ void apply_variables(const VarParams& v, const RecordLayout& lay,
                                                 const double* x, double* rec) {
-    for (int k = 0; k < v.P; ++k) {
-        const int s = v.surface[k];
-        if (v.type[k] == MKB_VAR_CURVATURE) rec[lay.curvature + s] = x[k];
-        else rec[lay.thickness + s] = x[k];
-    }
+    for (int k = 0; k < v.P; ++k) write_variable(v, lay, k, x[k], rec);
 }
 
 // ---- launch bookkeeping (host) -------------------------------------------------------------

@@ -105,9 +105,7 @@ __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayo
             const int k = (j - 1) / 2;
             const FdPattern& p = pat[static_cast<int64_t>(run) * pstride + k];
             const double y = (j & 1) ? p.xa : p.xb;
-            const int s = v.surface[k];
-            if (v.type[k] == MKB_VAR_CURVATURE) dst[lay.curvature + s] = y;
-            else dst[lay.thickness + s] = y;
+            write_variable(v, lay, k, y, dst);
         }
     }
 }
@@ -240,7 +238,7 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
     }
     VarParams vp{};
     if (rv.table == nullptr) {
-        rc = make_var_params(vars, tp.S, templates->type, &vp);
+        rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms);
         if (rc != MKB_OK) return rc;
     }
     if (!x0 || !J || !r0) {
@@ -348,14 +346,14 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
         return MKB_ERR_ARGUMENT;
     }
     VarParams vp;
-    rc = make_var_params(&vars[0], tp.S, templates->type, &vp);
+    rc = make_var_params(&vars[0], tp.S, templates->type, &vp, templates->ghost_terms);
     if (rc != MKB_OK) return rc;
     std::vector<VarParams> table;
     int pmax = vp.P;
     if (per_run) {
         table.resize(static_cast<size_t>(runs));
         for (int r = 0; r < runs; ++r) {
-            rc = make_var_params(&vars[r], tp.S, templates->type, &table[r]);
+            rc = make_var_params(&vars[r], tp.S, templates->type, &table[r], templates->ghost_terms);
             if (rc != MKB_OK) return rc;
             pmax = table[r].P > pmax ? table[r].P : pmax;
         }
@@ -477,7 +475,7 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
         return MKB_ERR_UNSUPPORTED;
     }
     VarParams vp;
-    rc = make_var_params(vars, tp.S, templates->type, &vp);
+    rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms);
     if (rc != MKB_OK) return rc;
     if (!x0 || !J || !r0 || !status) {
         set_error("adjoint jacobian: null pointer");

@@ -582,7 +582,7 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     }
     const mkb_lm_options& o = *options;
     s.per_run = o.per_run_variables != 0;
-    rc = make_var_params(&vars[0], s.tp.S, templates->type, &s.vp);
+    rc = make_var_params(&vars[0], s.tp.S, templates->type, &s.vp, templates->ghost_terms);
     if (rc != MKB_OK) return rc;
     s.pmax = s.vp.P;
     if (s.per_run) {
@@ -590,7 +590,7 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
         for (int r = 0; r < runs; ++r) {
             if (vars[r].count > s.pmax) s.pmax = vars[r].count;
             if (table != nullptr) {
-                rc = make_var_params(&vars[r], s.tp.S, templates->type, &(*table)[r]);
+                rc = make_var_params(&vars[r], s.tp.S, templates->type, &(*table)[r], templates->ghost_terms);
                 if (rc != MKB_OK) return rc;
             }
         }

@@ -47,7 +47,7 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
 // mu_tab[s * L + l] = n_before / n_after of the step onto surface s (divided in N).
-template <class N, bool kXf>
+template <class N, int kFeat>
 __device__ inline int trace_ray(const TraceParams& p, const double* rec, const double* mu_tab,
                                 const RecordLayout& lay, int S, int f, int l, const Sample& smp,
                                 bool soft_mode, double& opl, double& penalty) {
@@ -76,8 +76,11 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
         const N n_after = idx[s * L + l];
         const N c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
         int branch;
+        GhostData gd;
+        const bool plate = ghost_at<(kFeat & 2) != 0>(p, rec, lay, s, l, gd);
         status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
-                                    xf_at<kXf>(rec, lay, s), sp, branch);
+                                    xf_at<(kFeat & 1) != 0>(rec, lay, s), sp, branch, nullptr,
+                                    plate ? &gd : nullptr, n_after);
         if (status != kOk) break;
         n_before = n_after;
     }
@@ -125,7 +128,7 @@ struct TupleOut {
 // order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
-template <bool kResiduals, int kPrecision, bool kXf>
+template <bool kResiduals, int kPrecision, int kFeat>
 __global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
@@ -175,7 +178,7 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N, kXf>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
+        const int st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
                                     pen);
         sh.opl[i] = opl;
         sh.pen[i] = pen;
@@ -324,12 +327,18 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
                  cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
     const size_t smem = trace_smem(p);
-    const bool exact = precision == MKB_PRECISION_FP64;
-    auto kernel = p.non_coaxial
-                      ? (exact ? trace_kernel<kResiduals, MKB_PRECISION_FP64, true>
-                               : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA, true>)
-                      : (exact ? trace_kernel<kResiduals, MKB_PRECISION_FP64, false>
-                               : trace_kernel<kResiduals, MKB_PRECISION_FP64_FMA, false>);
+    // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
+    const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
+    constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
+    auto kernel = precision == MKB_PRECISION_FP64
+                      ? (feat == 0   ? trace_kernel<kResiduals, E, 0>
+                         : feat == 1 ? trace_kernel<kResiduals, E, 1>
+                         : feat == 2 ? trace_kernel<kResiduals, E, 2>
+                                     : trace_kernel<kResiduals, E, 3>)
+                      : (feat == 0   ? trace_kernel<kResiduals, F, 0>
+                         : feat == 1 ? trace_kernel<kResiduals, F, 1>
+                         : feat == 2 ? trace_kernel<kResiduals, F, 2>
+                                     : trace_kernel<kResiduals, F, 3>);
     if (smem > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(
             kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

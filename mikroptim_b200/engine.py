@@ -49,8 +49,11 @@ class DeviceSystemBatch:
         self.topology = batch.topology
         self.variants = batch.variants
         self.non_coaxial = 1 if batch.non_coaxial else 0
+        self.ghost_plates = batch.topology.ghost_plates
+        self.ghost_terms = batch.topology.ghost_terms
         self.stride = int(lib.mkb_record_stride_ext(batch.surfaces, batch.wavelengths,
-                                                    batch.fields, self.non_coaxial, 0, 0))
+                                                    batch.fields, self.non_coaxial,
+                                                    self.ghost_plates, self.ghost_terms))
         host = np.zeros((max(batch.variants, 1), self.stride))
         view = batch.view()
         _capi.check(lib.mkb_pack_batch_host(C.byref(view), _capi.ptr(host)), "pack batch")
@@ -75,6 +78,8 @@ class DeviceSystemBatch:
         b.fields = self.topology.fields
         b.record_stride = self.stride
         b.non_coaxial = self.non_coaxial
+        b.ghost_plates = self.ghost_plates
+        b.ghost_terms = self.ghost_terms
         b.records = C.c_void_p(self.records.data_ptr() + first * self.stride * 8)
         b.type = _capi.ptr(self.type, C.c_uint8)
         b._keep = self.type

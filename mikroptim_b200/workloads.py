@@ -320,6 +320,70 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
     return b, settings, variable_sets, x0
 
 
+# ---- ghost plates ------------------------------------------------------------------------------
+
+def ghost(variants: int = 64, seed: int = 20261203 + 11, terms: int = 4,
+          coeff_sigma: float = 2e-4, sigma: float = 0.05, rings: int = 6, spokes: int = 12,
+          failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+    """Two biconvex elements with a ghost plate in the air gap between them (table: stop,
+    2 spheres, plate, 2 spheres): curvatures +1/60, -1/60, +1/70, -1/50 with `sigma` Gaussian
+    noise, glass 5 and 4 mm (Cauchy n = 1.5046 + 0.00420/lambda^2 at 486.1 / 587.6 /
+    656.3 nm), the gap 1 mm before and 1 mm after the plate, image at the paraxial focus of the
+    elements. The plate: `terms` Legendre coefficients ~ N(0, coeff_sigma) mm per variant,
+    normalisation radius 8 mm, glass index that of the elements. Fields 0, 0.7, 1 degree, Half
+    pupils, pupil radius 5 mm. Variables: the four curvatures, both glass thicknesses, the
+    working distance and the plate's coefficients. Returns (batch, settings, variables, x0)."""
+    from .batch import SURFACE_GHOST_PLATE, VAR_GHOST_COEFFICIENT
+    S = 6
+    lam = np.array([486.1, 587.6, 656.3])
+    topo = BatchTopology(surfaces=S, wavelengths=3, fields=3,
+                         type=[SURFACE_STOP, SURFACE_SPHERE, SURFACE_SPHERE, SURFACE_GHOST_PLATE,
+                               SURFACE_SPHERE, SURFACE_SPHERE],
+                         pupil_mode=[PUPIL_HALF] * 3, ghost_terms=terms)
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.6
+    b.wavelength_nm[:] = lam
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    noise = rng.normal(1, variants * 4).reshape(variants, 4)
+    n = cauchy_index(lam)
+    n_ref = float(cauchy_index(587.6))
+    c = np.zeros((variants, S))
+    c[:, 1] = (1.0 / 60.0) * (1.0 + sigma * noise[:, 0])
+    c[:, 2] = (-1.0 / 60.0) * (1.0 + sigma * noise[:, 1])
+    c[:, 4] = (1.0 / 70.0) * (1.0 + sigma * noise[:, 2])
+    c[:, 5] = (-1.0 / 50.0) * (1.0 + sigma * noise[:, 3])
+    t = np.zeros((variants, S))
+    t[:, 1], t[:, 2], t[:, 3], t[:, 4] = 5.0, 1.0, 1.0, 4.0
+    idx = np.ones((variants, S, 3))
+    idx[:, 1, :] = n
+    idx[:, 4, :] = n
+    nr = np.ones((variants, S))
+    nr[:, 1] = nr[:, 4] = n_ref
+    efl, bfd = paraxial(c, t, nr)
+    t[:, S - 1] = bfd
+    b.curvature[:] = c
+    b.thickness[:] = t
+    b.index[:] = idx
+    b.ghost_coeff[:] = coeff_sigma * rng.normal(2, variants * terms).reshape(variants, 1, terms)
+    b.ghost_norm_radius[:] = 8.0
+    b.ghost_index[:] = n[None, None, :]
+    angles = np.deg2rad(np.array([0.0, 0.7, 1.0]))
+    b.pupil_radius[:] = 5.0
+    b.field_angle[:] = angles[None, :]
+    b.field_target[:] = efl[:, None] * np.tan(angles)[None, :]
+    settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
+    variables = [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in (1, 2, 4, 5)]
+    variables += [Variable(VAR_THICKNESS, s, 0.5, 20.0, 1.0) for s in (1, 4)]
+    variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 1.0, 500.0, 1.0)]
+    variables += [Variable(VAR_GHOST_COEFFICIENT, 3, -0.1, 0.1, 1e-4, plate=0, order=k)
+                  for k in range(1, terms + 1)]
+    vs = VariableSet(topo, variables)
+    x0 = np.stack([vs.extract(b, v) for v in range(variants)])
+    return b, settings, vs, x0
+
+
 # ---- configuration 5: Monte-Carlo tolerancing of a decentered / tilted objective --------------
 
 ARCMIN = math.pi / 10800.0

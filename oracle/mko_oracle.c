@@ -121,9 +121,84 @@ static int refract_sphere(ray_t* r, double c, double mu, soft_t* soft, int off_s
     return ST_OK;
 }
 
-/* propagate_surface_local, trace/trace.hpp:174 (stop, plane, sphere) */
-static int propagate_surface(ray_t* ray, double t, int kind, double c, double n_before,
-                             double n_after, soft_t* soft, unsigned char* branch) {
+/* ---- ghost plates: trace/ghost_plate.hpp --------------------------------------------------
+ * One plate at one wavelength (GhostPlateParams, ghost_plate.hpp:24). */
+typedef struct {
+    const double* coeff;  /* a_1 .. a_K */
+    int terms;
+    double norm_radius, n_glass;
+} ghost_t;
+
+/* ghost_profile, ghost_plate.hpp:67: t(u) and dt/du by the Legendre recurrences */
+static void ghost_profile(const ghost_t* g, double u, double* t_out, double* dt_du) {
+    const double xi = 2.0 * u - 1.0;
+    double p_prev = 1.0, p_cur = xi, dp_prev = 0.0, dp_cur = 1.0, t = 0.0, dt = 0.0;
+    for (int k = 1; k <= g->terms; ++k) {
+        const double a = g->coeff[k - 1];
+        t += a * p_cur;
+        dt += a * dp_cur;
+        const double p_next = ((double)(2 * k + 1) * xi * p_cur - (double)k * p_prev) /
+                              (double)(k + 1);
+        const double dp_next = dp_prev + (double)(2 * k + 1) * p_cur;
+        p_prev = p_cur;
+        p_cur = p_next;
+        dp_prev = dp_cur;
+        dp_cur = dp_next;
+    }
+    *t_out = t;
+    *dt_du = 2.0 * dt;
+}
+
+/* phase_surface_step, ghost_plate.hpp:130 */
+static int phase_surface_step(ray_t* ray, double phase, double grad_x, double grad_y,
+                              double n_before, double n_after, soft_t* soft) {
+    ray->opl += phase;
+    const double dx = (n_before * ray->d.x + grad_x) / n_after;
+    const double dy = (n_before * ray->d.y + grad_y) / n_after;
+    const double radicand = 1.0 - dx * dx - dy * dy;
+    if (radicand < 0.0) {
+        if (soft == NULL) return ST_TIR;
+        soft_add(soft, -radicand, ST_SOFT_TIR);
+        const double inv = 1.0 / sqrt(dx * dx + dy * dy);
+        vec3 d = {dx * inv, dy * inv, 0.0};
+        ray->d = d;
+        return ST_SOFT_TIR;
+    }
+    vec3 d = {dx, dy, sqrt(radicand)};
+    ray->d = d;
+    return ST_OK;
+}
+
+/* ghost_plate_step, ghost_plate.hpp:159 */
+static int ghost_plate_step(ray_t* ray, const ghost_t* g, double n_before, double n_after,
+                            soft_t* soft) {
+    const double inv_r2 = 1.0 / (g->norm_radius * g->norm_radius);
+    const double u = (ray->p.x * ray->p.x + ray->p.y * ray->p.y) * inv_r2;
+    double t, dt_du;
+    ghost_profile(g, u, &t, &dt_du);
+    const double dn = g->n_glass - n_before;
+    const double radial = dn * dt_du * 2.0 * inv_r2;
+    return phase_surface_step(ray, dn * t, radial * ray->p.x, radial * ray->p.y, n_before,
+                              n_after, soft);
+}
+
+/* propagate_surface_local, trace/trace.hpp:174 (stop, plane, sphere; ghost plate with `ghost`) */
+static int propagate_surface_g(ray_t* ray, double t, int kind, double c, double n_before,
+                               double n_after, soft_t* soft, unsigned char* branch,
+                               const ghost_t* ghost) {
+    if (kind == MKB_SURFACE_GHOST_PLATE) {
+        if (ghost == NULL) return ST_UNSUPPORTED;
+        if (!(ray->d.z > 0.0)) return ST_BACKWARD;
+        const double s0 = transfer_to_tangent_plane(ray, t);
+        ray->opl += n_before * s0;
+        const int step = ghost_plate_step(ray, ghost, n_before, n_after, soft);
+        if (step == ST_SOFT_TIR) {
+            if (branch != NULL) *branch = BR_SOFT_TIR;
+            return ST_OK;
+        }
+        if (branch != NULL) *branch = BR_REGULAR;
+        return step;
+    }
     double curv;
     if (kind == MKB_SURFACE_STOP || kind == MKB_SURFACE_PLANE) curv = 0.0;
     else if (kind == MKB_SURFACE_SPHERE) curv = c;
@@ -139,6 +214,11 @@ static int propagate_surface(ray_t* ray, double t, int kind, double c, double n_
         *branch = (unsigned char)((hit == ST_SOFT_MISSED ? BR_SOFT_MISSED : BR_REGULAR) |
                                   (refr == ST_SOFT_TIR ? BR_SOFT_TIR : BR_REGULAR));
     return refr == ST_SOFT_TIR ? ST_OK : refr;
+}
+
+static int propagate_surface(ray_t* ray, double t, int kind, double c, double n_before,
+                             double n_after, soft_t* soft, unsigned char* branch) {
+    return propagate_surface_g(ray, t, kind, c, n_before, n_after, soft, branch, NULL);
 }
 
 /* reference_sphere_step, trace/reference_sphere.hpp:55 */
@@ -176,7 +256,18 @@ typedef struct {
     const double* t;  /* [S] */
     const double* n;  /* [S][L] */
     const double* xf; /* [S][4] dx, dy, alpha, beta, or NULL (coaxial) */
+    int G, K;         /* ghost plates (GhostPlate surfaces in table order) and their terms */
+    const double* gcoeff;   /* [G][K] */
+    const double* gradius;  /* [G] */
+    const double* gindex;   /* [G][L] */
 } table_t;
+
+/* plate data of plate g at wavelength l */
+static ghost_t ghost_of(const table_t* sys, int g, int l) {
+    ghost_t r = {sys->gcoeff + (size_t)g * sys->K, sys->K, sys->gradius[g],
+                 sys->gindex[(size_t)g * sys->L + l]};
+    return r;
+}
 
 /* ---- decenter and tilt: trace/surface_transform.hpp:27-140 ---------------------------- */
 typedef struct { double dx, dy, ca, sa, cb, sb; } xform_t;
@@ -225,13 +316,15 @@ static vec3 point_from_surface(const xform_t* t, vec3 q) {
 /* propagate_surface with a transform (trace/trace.hpp:233) */
 static int propagate_surface_xf(ray_t* ray, double t, int kind, double c, double n_before,
                                 double n_after, soft_t* soft, unsigned char* branch,
-                                const xform_t* xf) {
-    if (xf == NULL) return propagate_surface(ray, t, kind, c, n_before, n_after, soft, branch);
+                                const xform_t* xf, const ghost_t* ghost) {
+    if (xf == NULL)
+        return propagate_surface_g(ray, t, kind, c, n_before, n_after, soft, branch, ghost);
     if (!(ray->d.z > 0.0)) return ST_BACKWARD;
     ray->p.z -= t;
     ray->p = point_to_surface(xf, ray->p);
     ray->d = rotate_to_surface(xf, ray->d);
-    const int st = propagate_surface(ray, 0.0, kind, c, n_before, n_after, soft, branch);
+    const int st = propagate_surface_g(ray, 0.0, kind, c, n_before, n_after, soft, branch,
+                                       ghost);
     if (st == ST_OK) {
         ray->p = point_from_surface(xf, ray->p);
         ray->d = rotate_from_surface(xf, ray->d);
@@ -261,15 +354,20 @@ static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center
         rec->image_branch = BR_REGULAR;
     }
     int st = ST_OK;
+    int ghost = 0; /* ghost plates passed (TraceProgress::ghost) */
     for (int s = 1; s < S; ++s) {
         const double n_before = sys->n[(s - 1) * L + l];
         const double n_after = sys->n[s * L + l];
         unsigned char branch = BR_REGULAR;
         xform_t xf;
         const int moved = transform_of(sys, s, &xf);
+        ghost_t gp;
+        const int plate = sys->type[s] == MKB_SURFACE_GHOST_PLATE && ghost < sys->G;
+        if (plate) gp = ghost_of(sys, ghost, l);
         st = propagate_surface_xf(ray, sys->t[s - 1], sys->type[s], sys->c[s], n_before, n_after,
-                                  soft, &branch, moved ? &xf : NULL);
+                                  soft, &branch, moved ? &xf : NULL, plate ? &gp : NULL);
         if (st != ST_OK) break;
+        if (sys->type[s] == MKB_SURFACE_GHOST_PLATE) ++ghost;
         if (rec) {
             rec->count = s + 1;
             rec->p[s] = ray->p;
@@ -385,6 +483,11 @@ static table_t table_of(const mkb_batch_view* v, int var) {
     t.t = v->thickness + (size_t)var * v->surfaces;
     t.n = v->index + (size_t)var * v->surfaces * v->wavelengths;
     t.xf = v->decenter_tilt != NULL ? v->decenter_tilt + (size_t)var * v->surfaces * 4 : NULL;
+    t.G = v->ghost_plates;
+    t.K = v->ghost_terms;
+    t.gcoeff = t.G > 0 ? v->ghost_coeff + (size_t)var * t.G * t.K : NULL;
+    t.gradius = t.G > 0 ? v->ghost_norm_radius : NULL;
+    t.gindex = t.G > 0 ? v->ghost_index + (size_t)var * t.G * t.L : NULL;
     return t;
 }
 
@@ -537,23 +640,36 @@ int mko_port_merit(const mkb_batch_view* view, const mkb_residual_plan* plan, do
 /* ---- variables: VariableSet::apply (src/optim/variable_set.cpp:237) ---------------------- */
 static int check_vars(const mkb_batch_view* v, const mkb_variables* vars) {
     if (!vars || vars->count < 1 || vars->count > MKB_MAX_VARIABLES) return -1;
-    for (int k = 0; k < vars->count; ++k)
-        if (vars->surface[k] < 0 || vars->surface[k] >= v->surfaces) return -1;
+    for (int k = 0; k < vars->count; ++k) {
+        if (vars->type[k] == MKB_VAR_GHOST_COEFFICIENT) {
+            if (!vars->ghost_plate || !vars->ghost_order || vars->ghost_plate[k] < 0 ||
+                vars->ghost_plate[k] >= v->ghost_plates || vars->ghost_order[k] < 1 ||
+                vars->ghost_order[k] > v->ghost_terms)
+                return -1;
+        } else if (vars->surface[k] < 0 || vars->surface[k] >= v->surfaces) {
+            return -1;
+        }
+    }
     return 0;
 }
 
-/* Copy of variant `src` of the view with x applied (curvature / thickness entries). */
+/* Copy of variant `src` of the view with x applied (curvature / thickness / ghost coefficient
+ * entries; VariableSet::apply, src/optim/variable_set.cpp:237). */
 typedef struct {
     double c[MKB_MAX_SURFACES], t[MKB_MAX_SURFACES];
+    double g[MKB_MAX_GHOST_PLATES * MKB_MAX_GHOST_TERMS];
 } params_t;
 
 static void apply_x(const mkb_batch_view* view, int src, const mkb_variables* vars,
                     const double* x, params_t* out) {
-    const int S = view->surfaces;
+    const int S = view->surfaces, GK = view->ghost_plates * view->ghost_terms;
     memcpy(out->c, view->curvature + (size_t)src * S, sizeof(double) * S);
     memcpy(out->t, view->thickness + (size_t)src * S, sizeof(double) * S);
+    if (GK > 0) memcpy(out->g, view->ghost_coeff + (size_t)src * GK, sizeof(double) * GK);
     for (int k = 0; k < vars->count; ++k) {
         if (vars->type[k] == MKB_VAR_CURVATURE) out->c[vars->surface[k]] = x[k];
+        else if (vars->type[k] == MKB_VAR_GHOST_COEFFICIENT)
+            out->g[vars->ghost_plate[k] * view->ghost_terms + vars->ghost_order[k] - 1] = x[k];
         else out->t[vars->surface[k]] = x[k];
     }
 }
@@ -562,6 +678,7 @@ static table_t table_with(const mkb_batch_view* v, int var, const params_t* p) {
     table_t t = table_of(v, var);
     t.c = p->c;
     t.t = p->t;
+    if (t.G > 0) t.gcoeff = p->g;
     return t;
 }
 
@@ -857,14 +974,122 @@ static void reference_step_backward(vec3 p, vec3 d, vec3 center, double n_image,
     *adj = in;
 }
 
+/* ghost_step_backward, trace/adjoint_backward.hpp:253: writes the adjoint of a_{k+1} of the
+ * plate into w->ghost[g0 + k] (see w_write below; declared here, defined after the writer). */
+typedef struct writer_s writer_t;
+static void w_write(const writer_t* w, int p, double value);
+static void ghost_step_backward(vec3 p, vec3 d, double t, const ghost_t* g, double n_before,
+                                double n_after, unsigned char branch, double seed_opl,
+                                double seed_pen, radj_t* adj, sadj_t* out, const writer_t* w,
+                                const int* coeff_cols) {
+    /* forward */
+    const double z = p.z - t;
+    const double s0 = -z / d.z;
+    const double x = p.x + s0 * d.x;
+    const double y = p.y + s0 * d.y;
+    const double inv_r2 = 1.0 / (g->norm_radius * g->norm_radius);
+    const double u = (x * x + y * y) * inv_r2;
+    const double xi = 2.0 * u - 1.0;
+    double prof_t = 0.0, sum_dp = 0.0, sum_ddp = 0.0;
+    {
+        double p_prev = 1.0, p_cur = xi, dp_prev = 0.0, dp_cur = 1.0, ddp_prev = 0.0,
+               ddp_cur = 0.0;
+        for (int k = 1; k <= g->terms; ++k) {
+            const double a = g->coeff[k - 1];
+            prof_t += a * p_cur;
+            sum_dp += a * dp_cur;
+            sum_ddp += a * ddp_cur;
+            const double p_next = ((double)(2 * k + 1) * xi * p_cur - (double)k * p_prev) /
+                                  (double)(k + 1);
+            const double dp_next = dp_prev + (double)(2 * k + 1) * p_cur;
+            const double ddp_next = ddp_prev + (double)(2 * k + 1) * dp_cur;
+            p_prev = p_cur;
+            p_cur = p_next;
+            dp_prev = dp_cur;
+            dp_cur = dp_next;
+            ddp_prev = ddp_cur;
+            ddp_cur = ddp_next;
+        }
+    }
+    const double dt_du = 2.0 * sum_dp;
+    const double d2t_du2 = 4.0 * sum_ddp;
+    const double dn = g->n_glass - n_before;
+    const double radial = dn * dt_du * 2.0 * inv_r2;
+    const double dx = (n_before * d.x + radial * x) / n_after;
+    const double dy = (n_before * d.y + radial * y) / n_after;
+    const double radicand = 1.0 - dx * dx - dy * dy;
+    const int tir = (branch & BR_SOFT_TIR) != 0;
+    /* reverse */
+    const vec3 qb = adj->p, d1b = adj->d;
+    radj_t in = {v_zero(), v_zero()};
+    double dxb, dyb, radb;
+    if (tir) {
+        const double inv_m = 1.0 / sqrt(dx * dx + dy * dy);
+        const double ex = dx * inv_m, ey = dy * inv_m;
+        const double proj = ex * d1b.x + ey * d1b.y;
+        dxb = (d1b.x - proj * ex) * inv_m;
+        dyb = (d1b.y - proj * ey) * inv_m;
+        radb = -seed_pen;
+    } else {
+        dxb = d1b.x;
+        dyb = d1b.y;
+        radb = d1b.z / (2.0 * sqrt(radicand));
+    }
+    dxb += -2.0 * dx * radb;
+    dyb += -2.0 * dy * radb;
+    in.d.x += dxb * n_before / n_after;
+    in.d.y += dyb * n_before / n_after;
+    out->n_before += (dxb * d.x + dyb * d.y) / n_after;
+    out->n_after += -(dxb * dx + dyb * dy) / n_after;
+    const double gxb = dxb / n_after, gyb = dyb / n_after;
+    const double radialb = gxb * x + gyb * y;
+    double xb = qb.x + gxb * radial;
+    double yb = qb.y + gyb * radial;
+    double s0b = seed_opl * n_before;
+    out->n_before += seed_opl * s0;
+    const double phaseb = seed_opl;
+    const double dnb = phaseb * prof_t + radialb * dt_du * 2.0 * inv_r2;
+    const double tb = phaseb * dn;
+    const double dtdub = radialb * dn * 2.0 * inv_r2;
+    out->n_before += -dnb;
+    const double ub = tb * dt_du + dtdub * d2t_du2;
+    {
+        double p_prev = 1.0, p_cur = xi, dp_prev = 0.0, dp_cur = 1.0;
+        for (int k = 1; k <= g->terms; ++k) {
+            w_write(w, coeff_cols[k - 1], tb * p_cur + dtdub * 2.0 * dp_cur);
+            const double p_next = ((double)(2 * k + 1) * xi * p_cur - (double)k * p_prev) /
+                                  (double)(k + 1);
+            const double dp_next = dp_prev + (double)(2 * k + 1) * p_cur;
+            p_prev = p_cur;
+            p_cur = p_next;
+            dp_prev = dp_cur;
+            dp_cur = dp_next;
+        }
+    }
+    xb += ub * 2.0 * x * inv_r2;
+    yb += ub * 2.0 * y * inv_r2;
+    /* transfer_backward, adjoint_backward.hpp:91 */
+    in.p.x += xb;
+    in.p.y += yb;
+    s0b += xb * d.x + yb * d.y;
+    in.d.x += xb * s0;
+    in.d.y += yb * s0;
+    const double q = s0b / d.z;
+    out->thickness += q;
+    in.p.z += -q;
+    in.d.z += -q * s0;
+    *adj = in;
+}
+
 /* Row writer: column map per table parameter (AdjointParameterMap, ray_jacobian.hpp:28). */
-typedef struct {
+struct writer_s {
     int curvature[MKB_MAX_SURFACES];
     int thickness[MKB_MAX_SURFACES];
+    int ghost[MKB_MAX_GHOST_PLATES * MKB_MAX_GHOST_TERMS];  /* ghost_coeff[g][k] */
     double* column0;
     int64_t rows, row;
     double factor;
-} writer_t;
+};
 
 static void w_write(const writer_t* w, int p, double value) {
     if (p >= 0) w->column0[(int64_t)p * w->rows + w->row] = w->factor * value;
@@ -878,6 +1103,9 @@ static void backward_ray(const table_t* sys, int l, const record_t* rec, int rea
     radj_t adj = {v_zero(), v_zero()};
     double n_carry = 0.0;
     unsigned char next_branch = BR_REGULAR;
+    int ghost = 0; /* ghost plates among the surfaces 1 .. count - 1 */
+    for (int j = 1; j < count; ++j)
+        if (sys->type[j] == MKB_SURFACE_GHOST_PLATE) ++ghost;
     for (int s = count - 1; s >= 0; --s) {
         const vec3 p = rec->p[s], d = rec->d[s];
         if (s == count - 1) {
@@ -912,8 +1140,15 @@ static void backward_ray(const table_t* sys, int l, const record_t* rec, int rea
                 adj.p = rotate_to_surface(&xf, adj.p);
                 adj.d = rotate_to_surface(&xf, adj.d);
             }
-            refracting_step_backward(pl, dl, tl, c, n_before, n_after, next_branch, seed_opl,
-                                     seed_pen, &adj, &par);
+            if (kind == MKB_SURFACE_GHOST_PLATE) {
+                --ghost;
+                const ghost_t gp = ghost_of(sys, ghost, l);
+                ghost_step_backward(pl, dl, tl, &gp, n_before, n_after, next_branch, seed_opl,
+                                    seed_pen, &adj, &par, w, w->ghost + ghost * sys->K);
+            } else {
+                refracting_step_backward(pl, dl, tl, c, n_before, n_after, next_branch, seed_opl,
+                                         seed_pen, &adj, &par);
+            }
             if (moved) {
                 adj.p = rotate_from_surface(&xf, adj.p);
                 adj.d = rotate_from_surface(&xf, adj.d);
@@ -967,8 +1202,11 @@ static void adjoint_item(void* pctx, int i) {
     if (status) memcpy(status + (size_t)i * rays, st_all, rays);
     writer_t w;
     for (int s = 0; s < S; ++s) w.curvature[s] = w.thickness[s] = -1;
+    for (int g = 0; g < MKB_MAX_GHOST_PLATES * MKB_MAX_GHOST_TERMS; ++g) w.ghost[g] = -1;
     for (int k = 0; k < P; ++k) {
         if (vars->type[k] == MKB_VAR_CURVATURE) w.curvature[vars->surface[k]] = k;
+        else if (vars->type[k] == MKB_VAR_GHOST_COEFFICIENT)
+            w.ghost[vars->ghost_plate[k] * view->ghost_terms + vars->ghost_order[k] - 1] = k;
         else w.thickness[vars->surface[k]] = k;
     }
     w.column0 = J + (size_t)i * P * R;

@@ -47,8 +47,8 @@ mko::BatchTopology topology_of_view(const mkb_batch_view& v, const mkb_residual_
     t.surfaces = v.surfaces;
     t.wavelengths = v.wavelengths;
     t.fields = v.fields;
-    t.ghost_plates = 0;
-    t.ghost_terms = 0;
+    t.ghost_plates = v.ghost_plates;
+    t.ghost_terms = v.ghost_terms;
     t.non_coaxial = v.decenter_tilt != nullptr;
     t.source = mko::SourceKind::Collimated;
     for (int s = 0; s < v.surfaces; ++s) {
@@ -85,12 +85,22 @@ mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_p
             b.field_angle(i, f) = v.field_angle[i * F + f];
             b.field_target(i, f) = v.field_target[i * F + f];
         }
+        for (int g = 0; g < v.ghost_plates; ++g) {
+            for (int k = 0; k < v.ghost_terms; ++k)
+                b.ghost_coeff(i, g, k) =
+                    v.ghost_coeff[(static_cast<std::size_t>(i) * v.ghost_plates + g) *
+                                      v.ghost_terms + k];
+            for (int l = 0; l < L; ++l)
+                b.ghost_index(i, g, l) =
+                    v.ghost_index[(static_cast<std::size_t>(i) * v.ghost_plates + g) * L + l];
+        }
         if (v.decenter_tilt != nullptr)
             for (int s = 0; s < S; ++s)
                 for (int k = 0; k < 4; ++k)
                     b.decenter_tilt(i, s, k) =
                         v.decenter_tilt[(static_cast<std::size_t>(i) * S + s) * 4 + k];
     }
+    for (int g = 0; g < v.ghost_plates; ++g) b.ghost_norm_radius(g) = v.ghost_norm_radius[g];
     return b;
 }
 

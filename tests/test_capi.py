@@ -92,9 +92,11 @@ def test_bad_arguments_rejected_before_launch(mutate, expect):
     assert expect in msg
 
 
-def test_ghost_plate_reported_unsupported():
+def test_ghost_plate_surface_without_plate_data_rejected():
+    """A GhostPlate surface needs the batch to carry as many plates (ghost_plates) as the
+    table has such surfaces."""
     rc, msg = _bad_call(lambda b, p, t: t.__setitem__(1, 3))
-    assert rc == _capi.MKB_ERR_UNSUPPORTED and "ghost" in msg
+    assert rc == _capi.MKB_ERR_ARGUMENT and "ghost" in msg
 
 
 def test_merit_workspace_checked():
