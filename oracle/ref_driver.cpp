@@ -129,14 +129,39 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
         d.source.field_angles_deg.push_back(b.field_angle(0, f) * 180.0 / M_PI);
         d.source.field_weights.push_back(b.field_weight(f));
     }
-    for (int s = 0; s < b.surfaces(); ++s) {
+    // file surfaces are the table's non-ghost surfaces; a gap with ghost plates is one file
+    // thickness (the sum of its table pieces), each plate at its distance from the gap's
+    // first vertex (make_surface_map, src/model/system.cpp:361)
+    const int S = b.surfaces();
+    std::vector<int> file_of_table(static_cast<std::size_t>(S), -1);
+    std::vector<int> plate_of_table(static_cast<std::size_t>(S), -1);
+    int files = 0, plates = 0;
+    for (int s = 0; s < S; ++s) {
+        if (b.type(s) == mko::SurfaceKind::GhostPlate) plate_of_table[s] = plates++;
+        else file_of_table[s] = files++;
+    }
+    for (int s = 0; s < S; ++s) {
+        if (file_of_table[s] < 0) continue;
         mko::Surface surf;
         const auto kind = b.type(s);
         surf.type = kind == mko::SurfaceKind::Stop    ? mko::SurfaceType::Stop
                     : kind == mko::SurfaceKind::Plane ? mko::SurfaceType::Plane
                                                       : mko::SurfaceType::Sphere;
         surf.curvature = b.curvature(0, s);
-        surf.thickness = b.thickness(0, s);
+        double gap = b.thickness(0, s);
+        for (int q = s + 1; q < S && plate_of_table[q] >= 0; ++q) {
+            mko::GhostPlate gp;
+            gp.after_surface = file_of_table[s];
+            gp.distance = gap;
+            gp.glass.kind = mko::MaterialKind::Constant;
+            gp.glass.n = b.ghost_index(0, plate_of_table[q], 0);
+            gp.norm_radius = b.ghost_norm_radius(plate_of_table[q]);
+            for (int k = 0; k < b.ghost_terms(); ++k)
+                gp.coefficients.push_back(b.ghost_coeff(0, plate_of_table[q], k));
+            d.ghost_plates.push_back(gp);
+            gap += b.thickness(0, q);
+        }
+        surf.thickness = gap;
         const double n = b.index(0, s, 0);
         if (n == 1.0) {
             surf.material.kind = mko::MaterialKind::Air;
@@ -147,7 +172,8 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
         surf.semi_diameter = s == 0 ? b.pupil_radius(0) : 100.0;
         d.surfaces.push_back(surf);
     }
-    // start values of the description = x0 of run 0 (resolve_variables checks the bounds)
+    // start values of the description = x0 of run 0 (resolve_variables checks the bounds);
+    // variables of this driver sit on gaps without plates, so table and file values agree
     mko::Variables items;
     for (int k = 0; k < vars.count; ++k) {
         mko::VariableSpec spec;
@@ -155,17 +181,26 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
         if (vars.type[k] == MKB_VAR_CURVATURE) {
             spec.type = mko::VariableType::Curvature;
             spec.selection = mko::SurfaceSelection::One;
-            spec.surfaces = {s};
-            d.surfaces[s].curvature = x0[k];
+            spec.surfaces = {file_of_table[s]};
+            d.surfaces[file_of_table[s]].curvature = x0[k];
         } else if (vars.type[k] == MKB_VAR_THICKNESS) {
             spec.type = mko::VariableType::Thickness;
             spec.selection = mko::SurfaceSelection::One;
-            spec.surfaces = {s};
-            d.surfaces[s].thickness = x0[k];
+            spec.surfaces = {file_of_table[s]};
+            d.surfaces[file_of_table[s]].thickness = x0[k];
+        } else if (vars.type[k] == MKB_VAR_GHOST_COEFFICIENT) {
+            spec.type = mko::VariableType::GhostCoefficient;
+            spec.selection = mko::SurfaceSelection::None;
+            spec.plate_selection = mko::SurfaceSelection::One;
+            spec.plates = {vars.ghost_plate[k]};
+            spec.order_selection = mko::SurfaceSelection::One;
+            spec.orders = {vars.ghost_order[k]};
+            d.ghost_plates[static_cast<std::size_t>(vars.ghost_plate[k])]
+                .coefficients[static_cast<std::size_t>(vars.ghost_order[k] - 1)] = x0[k];
         } else {
             spec.type = mko::VariableType::WorkingDistance;
             spec.selection = mko::SurfaceSelection::None;
-            d.surfaces[b.surfaces() - 1].thickness = x0[k];
+            d.surfaces[static_cast<std::size_t>(files - 1)].thickness = x0[k];
         }
         if (std::isfinite(vars.lower[k])) {
             spec.min = vars.lower[k];

@@ -195,7 +195,8 @@ def test_zero_transforms_trace_like_the_coaxial_batch():
 @pytest.mark.skipif(not has_reference_build(), reason="reference CPU build not present")
 def test_port_matches_reference_with_ghost_plates():
     """Ghost plates with non-zero Legendre profiles (trace/ghost_plate.hpp): restatement and
-    reference agree bit for bit on RESIDUALS and MERIT."""
+    reference agree bit for bit on RESIDUALS, MERIT and the adjoint and FD Jacobians, whose
+    columns include the plate's profile coefficients (GhostCoefficient variables)."""
     b, st, vs, x0 = workloads.ghost(8)
     assert np.any(b.ghost_coeff != 0.0)
     lay = ResidualLayout(b.topology, st)
@@ -204,18 +205,25 @@ def test_port_matches_reference_with_ghost_plates():
         assert np.array_equal(a, c)
     for a, c in zip(P.merit(b, lay), R.merit(b, lay)):
         assert np.array_equal(a, c)
+    two = b.subset(0, 2)
+    for a, c in zip(P.adjoint_jacobian(two, lay, vs, x0[:2]),
+                    R.adjoint_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
+    for a, c in zip(P.fd_jacobian(two, lay, vs, x0[:2]), R.fd_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
 
 
 def test_port_adjoint_through_ghost_plates_matches_central_differences():
     """The restated reverse step of a ghost plate (ghost_step_backward): derivatives with
     respect to curvatures, thicknesses and the plate's profile coefficients agree with central
-    differences of the pinned forward trace to 1e-7 (truncation error, steps 1e-6 / 1e-5)."""
+    differences of the pinned forward trace to 1e-6 of the column (steps 1e-5, thicknesses
+    1e-4, where the OPL rounding of a smaller step dominates)."""
     b, st, vs, x0 = workloads.ghost(2)
     lay = ResidualLayout(b.topology, st)
     P = po.port()
     J, _, _ = P.adjoint_jacobian(b.subset(0, 1), lay, vs, x0[:1])
     for k in range(vs.size):
-        h = 1e-5 if k >= 7 else 1e-6
+        h = 1e-4 if 4 <= k <= 6 else 1e-5
         bp, bm = b.subset(0, 1), b.subset(0, 1)
         xp, xm = x0[0].copy(), x0[0].copy()
         xp[k] += h
@@ -223,7 +231,7 @@ def test_port_adjoint_through_ghost_plates_matches_central_differences():
         vs.apply(bp, 0, xp)
         vs.apply(bm, 0, xm)
         fd = (P.residuals(bp, lay)[0][0] - P.residuals(bm, lay)[0][0]) / (2 * h)
-        assert np.abs(J[0, k] - fd).max() <= 1e-7 * np.abs(fd).max(), k
+        assert np.abs(J[0, k] - fd).max() <= 1e-6 * np.abs(fd).max(), k
 
 
 def test_subset_owns_its_arrays():
