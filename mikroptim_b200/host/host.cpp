@@ -37,10 +37,19 @@ void BatchTopology::validate() const {
         throw std::invalid_argument("BatchTopology: type needs one entry per surface");
     if (type[0] != SurfaceKind::Stop)
         throw std::invalid_argument("BatchTopology: surface 0 must be the stop");
-    for (int s = 1; s < surfaces; ++s)
-        if (type[s] != SurfaceKind::Plane && type[s] != SurfaceKind::Sphere)
-            throw std::logic_error("BatchTopology: this build traces stop, plane and sphere "
-                                   "surfaces");
+    int plates = 0;
+    for (int s = 1; s < surfaces; ++s) {
+        if (type[s] == SurfaceKind::GhostPlate) ++plates;
+        else if (type[s] != SurfaceKind::Plane && type[s] != SurfaceKind::Sphere)
+            throw std::invalid_argument("BatchTopology: unknown surface kind");
+    }
+    if (plates != ghost_plates)
+        throw std::invalid_argument("BatchTopology: ghost_plates must equal the number of "
+                                    "GhostPlate surfaces");
+    if (ghost_plates > MKB_MAX_GHOST_PLATES)
+        throw std::logic_error("BatchTopology: too many ghost plates for this build");
+    if (ghost_terms < 0 || ghost_terms > MKB_MAX_GHOST_TERMS || (ghost_plates > 0 && ghost_terms < 1))
+        throw std::invalid_argument("BatchTopology: ghost_terms out of range");
     if (static_cast<int>(pupil_mode.size()) != fields)
         throw std::invalid_argument("BatchTopology: pupil_mode needs one entry per field");
     if (non_coaxial)
@@ -67,6 +76,36 @@ SystemBatchHost::SystemBatchHost(BatchTopology topology, int variants)
     field_angle_.assign(V * F, 0.0);
     field_target_.assign(V * F, 0.0);
     if (topology_.non_coaxial) decenter_tilt_.assign(V * S * 4, 0.0);
+    const size_t G = topology_.ghost_plates, K = topology_.ghost_terms;
+    ghost_coeff_.assign(V * G * K, 0.0);
+    ghost_index_.assign(V * G * L, 1.0);
+    ghost_norm_radius_.assign(G, 1.0);
+}
+
+double& SystemBatchHost::ghost_coeff(int v, int g, int k) {
+    if (g < 0 || g >= topology_.ghost_plates || k < 0 || k >= topology_.ghost_terms)
+        throw std::out_of_range("SystemBatchHost: ghost coefficient out of range");
+    return ghost_coeff_.at((check_v(v) * topology_.ghost_plates + g) * topology_.ghost_terms + k);
+}
+
+double& SystemBatchHost::ghost_index(int v, int g, int l) {
+    if (g < 0 || g >= topology_.ghost_plates || l < 0 || l >= wavelengths())
+        throw std::out_of_range("SystemBatchHost: ghost index out of range");
+    return ghost_index_.at((check_v(v) * topology_.ghost_plates + g) * wavelengths() + l);
+}
+
+double& SystemBatchHost::ghost_norm_radius(int g) {
+    if (g < 0 || g >= topology_.ghost_plates)
+        throw std::out_of_range("SystemBatchHost: ghost plate out of range");
+    return ghost_norm_radius_.at(static_cast<size_t>(g));
+}
+
+int SystemBatchHost::ghost_surface(int g) const {
+    if (g < 0 || g >= topology_.ghost_plates)
+        throw std::out_of_range("SystemBatchHost: ghost plate out of range");
+    for (int s = 1, n = 0; s < surfaces(); ++s)
+        if (topology_.type[s] == SurfaceKind::GhostPlate && n++ == g) return s;
+    return -1;
 }
 
 double& SystemBatchHost::decenter_tilt(int v, int s, int k) {
@@ -105,6 +144,9 @@ SystemBatchHost make_non_coaxial(const SystemBatchHost& batch) {
     out.pupil_radius_ = batch.pupil_radius_;
     out.field_angle_ = batch.field_angle_;
     out.field_target_ = batch.field_target_;
+    out.ghost_coeff_ = batch.ghost_coeff_;
+    out.ghost_index_ = batch.ghost_index_;
+    out.ghost_norm_radius_ = batch.ghost_norm_radius_;
     return out;
 }
 
@@ -139,6 +181,11 @@ void SystemBatchHost::validate_values() const {
     finite(wavelength_weight, "wavelength_weight");
     finite(field_weight, "field_weight");
     finite(decenter_tilt_, "decenter_tilt");
+    finite(ghost_coeff_, "ghost_coeff");
+    for (double x : ghost_index_)
+        if (!(x > 0)) throw std::invalid_argument("SystemBatchHost: ghost index must be > 0");
+    for (double x : ghost_norm_radius_)
+        if (!(x > 0)) throw std::invalid_argument("SystemBatchHost: ghost radius must be > 0");
     for (size_t i = 2; i < decenter_tilt_.size(); i += 4)
         for (size_t k = i; k < i + 2; ++k)
             if (!(std::abs(decenter_tilt_[k]) < 1.5707963267948966))
@@ -182,6 +229,13 @@ mkb_batch_view SystemBatchHost::view() const {
     v.field_angle = field_angle_.data();
     v.field_target = field_target_.data();
     v.decenter_tilt = topology_.non_coaxial ? decenter_tilt_.data() : nullptr;
+    v.ghost_plates = topology_.ghost_plates;
+    v.ghost_terms = topology_.ghost_terms;
+    if (topology_.ghost_plates > 0) {
+        v.ghost_coeff = ghost_coeff_.data();
+        v.ghost_norm_radius = ghost_norm_radius_.data();
+        v.ghost_index = ghost_index_.data();
+    }
     return v;
 }
 
@@ -254,7 +308,7 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
     const int S = topology.surfaces;
     if (variables_.size() > MKB_MAX_VARIABLES)
         throw std::invalid_argument("VariableSet: at most 64 variables");
-    std::set<std::pair<bool, int>> seen;
+    std::set<std::pair<int, int>> seen;
     for (size_t k = 0; k < variables_.size(); ++k) {
         Variable& v = variables_[k];
         if (v.type == VariableType::Curvature) {
@@ -265,10 +319,21 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
                 throw std::invalid_argument("VariableSet: thickness surface out of range");
         } else if (v.type == VariableType::WorkingDistance) {
             v.surface = S - 1;
+        } else if (v.type == VariableType::GhostCoefficient) {
+            if (v.ghost_plate < 0 || v.ghost_plate >= topology.ghost_plates ||
+                v.ghost_order < 1 || v.ghost_order > topology.ghost_terms)
+                throw std::invalid_argument("VariableSet: ghost coefficient out of range");
+            for (int s = 1, n = 0; s < S; ++s)
+                if (topology.type[s] == SurfaceKind::GhostPlate && n++ == v.ghost_plate)
+                    v.surface = s;
         } else {
             throw std::logic_error("VariableSet: variable type not traced by this build");
         }
-        if (!seen.insert({v.type == VariableType::Curvature, v.surface}).second)
+        const std::pair<int, int> key =
+            v.type == VariableType::GhostCoefficient
+                ? std::pair<int, int>{2 + v.ghost_plate, v.ghost_order}
+                : std::pair<int, int>{v.type == VariableType::Curvature ? 1 : 0, v.surface};
+        if (!seen.insert(key).second)
             throw std::invalid_argument("VariableSet: parameter already used by a variable");
         if (std::isnan(v.lower) || std::isnan(v.upper) || v.lower > v.upper)
             throw std::invalid_argument("VariableSet: invalid bounds");
@@ -276,6 +341,8 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
             throw std::invalid_argument("VariableSet: typical size must be > 0");
         type_.push_back(static_cast<int32_t>(v.type));
         surface_.push_back(v.surface);
+        ghost_plate_.push_back(v.ghost_plate);
+        ghost_order_.push_back(v.ghost_order);
         lower_.push_back(v.lower);
         upper_.push_back(v.upper);
         typical_.push_back(v.typical);
@@ -286,7 +353,10 @@ std::vector<double> VariableSet::extract(const SystemBatchHost& batch, int v) co
     std::vector<double> x;
     for (const Variable& var : variables_)
         x.push_back(var.type == VariableType::Curvature ? batch.curvature(v, var.surface)
-                                                       : batch.thickness(v, var.surface));
+                    : var.type == VariableType::GhostCoefficient
+                        ? const_cast<SystemBatchHost&>(batch).ghost_coeff(v, var.ghost_plate,
+                                                                          var.ghost_order - 1)
+                        : batch.thickness(v, var.surface));
     return x;
 }
 
@@ -294,6 +364,8 @@ void VariableSet::apply(SystemBatchHost& batch, int v, const double* x) const {
     for (size_t k = 0; k < variables_.size(); ++k) {
         const Variable& var = variables_[k];
         if (var.type == VariableType::Curvature) batch.curvature(v, var.surface) = x[k];
+        else if (var.type == VariableType::GhostCoefficient)
+            batch.ghost_coeff(v, var.ghost_plate, var.ghost_order - 1) = x[k];
         else batch.thickness(v, var.surface) = x[k];
     }
 }
@@ -306,6 +378,8 @@ mkb_variables VariableSet::c_struct() const {
     c.lower = lower_.data();
     c.upper = upper_.data();
     c.typical = typical_.data();
+    c.ghost_plate = ghost_plate_.data();
+    c.ghost_order = ghost_order_.data();
     return c;
 }
 
@@ -387,7 +461,8 @@ void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     const mkb_batch_view view = batch.view();
     const int32_t non_coaxial = view.decenter_tilt != nullptr ? 1 : 0;
     const int32_t stride = mkb_record_stride_ext(view.surfaces, view.wavelengths, view.fields,
-                                                 non_coaxial, 0, 0);
+                                                 non_coaxial, view.ghost_plates,
+                                                 view.ghost_terms);
     host_records_.assign(static_cast<size_t>(view.variants) * stride, 0.0);
     check(mkb_pack_batch_host(&view, host_records_.data()), "pack batch");
     void* d = cuda::upload(records_, host_records_, stream);
@@ -398,8 +473,8 @@ void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     batch_.fields = view.fields;
     batch_.record_stride = stride;
     batch_.non_coaxial = non_coaxial;
-    batch_.ghost_plates = 0;
-    batch_.ghost_terms = 0;
+    batch_.ghost_plates = view.ghost_plates;
+    batch_.ghost_terms = view.ghost_terms;
     batch_.records = static_cast<const double*>(d);
     batch_.type = type_.data();
 }

@@ -26,11 +26,12 @@
 
 namespace mkb {
 
-enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2 };
+enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2, GhostPlate = 3 };
 enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
 enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
 enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2 };
-enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2 };
+enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2,
+                                    GhostCoefficient = 3 };
 enum class JacobianMethod : int32_t { FiniteDifference = 0, Adjoint = 1 };
 enum class LmStatus : int32_t {
     Running = 0, ConvergedMerit = 1, ConvergedStep = 2, ConvergedGradient = 3,
@@ -44,6 +45,9 @@ struct BatchTopology {
     std::vector<PupilMode> pupil_mode;  // [F]
     // per-surface decenter and tilt (system_batch.hpp:45); every field then uses the Full pupil
     bool non_coaxial = false;
+    // ghost plates: one per GhostPlate surface (table order), each with ghost_terms profile
+    // coefficients (BatchTopology::ghost_plates / ghost_terms, system_batch.hpp:30)
+    int ghost_plates = 0, ghost_terms = 0;
     void validate() const;
 };
 
@@ -73,6 +77,12 @@ public:
     double decenter_tilt(int v, int s, int k) const;
     void set_decenter_tilt(int v, int s, double dx, double dy, double alpha, double beta);
     bool coaxial() const { return !topology_.non_coaxial; }
+    // ghost plate g: profile coefficient a_{k+1}, glass index at wavelength l (per variant),
+    // normalisation radius (shared), table surface (system_batch.hpp:102-131)
+    double& ghost_coeff(int v, int g, int k);
+    double& ghost_index(int v, int g, int l);
+    double& ghost_norm_radius(int g);
+    int ghost_surface(int g) const;
 
     double reference_wavelength_nm = 0.0;
     std::vector<double> wavelength_weight;  // [L]
@@ -90,7 +100,7 @@ private:
     int variants_;
     std::vector<uint8_t> type_;
     std::vector<double> curvature_, thickness_, index_, pupil_radius_, field_angle_,
-        field_target_, decenter_tilt_;
+        field_target_, decenter_tilt_, ghost_coeff_, ghost_index_, ghost_norm_radius_;
     friend SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
 };
 
@@ -147,6 +157,8 @@ struct Variable {
     double lower = -std::numeric_limits<double>::infinity();
     double upper = std::numeric_limits<double>::infinity();
     double typical = 1.0;
+    int ghost_plate = -1;  // GhostCoefficient: a_{ghost_order} of plate ghost_plate
+    int ghost_order = 0;
 };
 
 class VariableSet {
@@ -160,7 +172,7 @@ public:
 
 private:
     std::vector<Variable> variables_;
-    std::vector<int32_t> type_, surface_;
+    std::vector<int32_t> type_, surface_, ghost_plate_, ghost_order_;
     std::vector<double> lower_, upper_, typical_;
 };
 
