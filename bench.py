@@ -33,6 +33,7 @@ import argparse
 import ctypes as C
 import dataclasses
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -66,7 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing"])
+    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing", "precision"])
     ap.add_argument("--variants", type=int, default=None,
                     help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
                          "otherwise)")
@@ -1001,6 +1002,126 @@ def run_tolerancing(args, world, rank, local):
     }, (b, lay)
 
 
+WORKLOAD_PREC = ("precision-{V}: {V} systems x 20 surfaces (9 configuration-1 style elements + "
+                 "a zero-power plate), L=9 (405..700 nm), F=5, Half 32x32 pupils (1,024 rays per "
+                 "field and wavelength; config 4 shape)")
+
+
+def run_precision(args, world, rank, local):
+    """Configuration 4: MERIT of every system in FP64 (bit-identical to the reference CPU),
+    FP64_FMA and MIXED, timed; OPD of every ray in all three, in tranches, and the FMA / MIXED
+    OPD error against the FP64 trace (waves at the reference wavelength, over rays whose status
+    agrees and lies in the piston); the normal-equation error of the fused MIXED and FMA
+    adjoint against the exact materialised one on a sample."""
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED,
+                                      ResidualLayout, in_piston)
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    V = args.variants or 65536
+    b, st, vs, x0 = workloads.sweep(V, seed=20261203 + 4 + 1000 * rank)
+    lays = {p: ResidualLayout(b.topology, dataclasses.replace(st, precision=p))
+            for p in (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED)}
+    db = engine.DeviceSystemBatch(b, dev)
+    lay0 = lays[PRECISION_FP64]
+    ws = torch.empty(int(lib.mkb_merit_workspace_bytes(V, C.byref(lay0.plan(b)))),
+                     dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    rays = V * lay0.rays_per_variant
+    hits = rays * (b.surfaces - 1)
+
+    def merit_ms(p, steps):
+        for _ in range(args.warmup):
+            engine.merit_device(db, lays[p], b, workspace=ws)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            engine.merit_device(db, lays[p], b, workspace=ws)
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in ts) / steps
+
+    l0 = lib.mkb_launch_count()
+    with ClockSampler(local) as clocks:
+        ms = {p: merit_ms(p, args.steps) for p in (PRECISION_FP64_FMA, PRECISION_FP64,
+                                                   PRECISION_MIXED)}
+    launches = lib.mkb_launch_count() - l0
+    ms = {p: max_over_ranks(v, world, dev) for p, v in ms.items()}
+
+    # OPD errors over every ray, in tranches of variants
+    lam_mm = b.reference_wavelength_nm * 1e-6
+    acc = {PRECISION_FP64_FMA: [0.0, 0, 0.0, 0, 0], PRECISION_MIXED: [0.0, 0, 0.0, 0, 0]}
+    chunk = 2048
+    for first in range(0, V, chunk):
+        n = min(chunk, V - first)
+        sub = b.subset(first, n)
+        dsub = engine.DeviceSystemBatch(sub, dev)
+        ref = engine.residuals_device(dsub, lay0, sub)
+        ok_ref = ((ref.status == 0) | (ref.status == 5) | (ref.status == 6))
+        for p in (PRECISION_FP64_FMA, PRECISION_MIXED):
+            r = engine.residuals_device(dsub, lays[p], sub)
+            same = (r.status == ref.status) & ok_ref
+            err = ((r.opd - ref.opd) / lam_mm)[same]
+            a = acc[p]
+            a[0] += float((err * err).sum())
+            a[1] += int(err.numel())
+            a[2] = max(a[2], float(err.abs().max()) if err.numel() else 0.0)
+            a[3] += int((r.status == ref.status).sum())
+            a[4] += int(r.status.numel())
+        del dsub, ref
+    errors = {name: {"rms_waves": math.sqrt(acc[p][0] / max(acc[p][1], 1)),
+                     "max_waves": acc[p][2],
+                     "status_agreement": acc[p][3] / max(acc[p][4], 1),
+                     "rays_compared": acc[p][1]}
+              for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed"))}
+
+    # normal equations: fused (FMA, MIXED) against the exact materialised J^T J on a sample
+    sample = b.subset(0, 64)
+    ds = engine.DeviceSystemBatch(sample, dev)
+    J, r0, _ = engine.adjoint_jacobian_device(ds, lay0, sample, vs, x0[:64])
+    exact = engine.normal_equations_device(J, r0, True)
+    del J
+    jerr = {}
+    for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed")):
+        g = engine.adjoint_normal_equations_device(ds, lays[p], sample, vs, x0[:64])
+        d = torch.diagonal(exact, dim1=1, dim2=2).abs()
+        d = torch.maximum(d, 1e-20 * d.max(dim=1, keepdim=True).values + 1e-300)
+        rel = (g - exact).abs() / torch.sqrt(d[:, :, None] * d[:, None, :])
+        jerr[name] = {"median": float(rel.median()), "max": float(rel.max())}
+    if rank != 0:
+        return None, None
+    return {
+        "metric": "ray-surface hits/s (MERIT, FP64_FMA) with the OPD error of FP64_FMA and "
+                  "MIXED against bit-exact FP64",
+        "value": world * hits / (ms[PRECISION_FP64_FMA] / 1e3),
+        "unit": "ray-surface hits/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms[PRECISION_FP64_FMA],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-4 shapes)",
+        "config": {"workload": WORKLOAD_PREC.format(V=V),
+                   "step": "one MERIT evaluation of every system",
+                   "rays_per_evaluation": rays,
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(launches),
+        "merit_ms": {"fp64_fma": ms[PRECISION_FP64_FMA], "fp64_exact": ms[PRECISION_FP64],
+                     "mixed": ms[PRECISION_MIXED]},
+        "opd_error_vs_fp64": errors,
+        "normal_equations_rel_error_vs_exact": jerr,
+        "intercept_error": "not reported: the trace has no intercept output",
+        "e2e": None,
+        "clocks": clocks.summary(),
+    }, (b, lay0)
+
+
 def cpu_baseline_tolerancing(samples: int = 8):
     """The reference's CPU MERIT plus adjoint Jacobian (gradient 2 J^T r) of `samples` samples,
     all host threads (oracle/_ref)."""
@@ -1032,6 +1153,8 @@ def main():
                 out["cpu_baseline"] = cpu_baseline_uneven()
             except Exception as e:  # the baseline is reported, not required
                 out["cpu_baseline"] = {"value": None, "error": str(e)}
+    elif args.workload == "precision":
+        out, _ = run_precision(args, world, rank, local)
     elif args.workload == "tolerancing":
         out, _ = run_tolerancing(args, world, rank, local)
         if rank == 0 and world == 1:

@@ -242,7 +242,10 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
             p.scale[f * L + l] = w > 0.0 ? std::sqrt(w) / lambda_ref_mm : 0.0;
             p.pscale[f * L + l] = w > 0.0 ? std::sqrt(plan->fail_weight * w) : 0.0;
         }
-    // pack plan: consecutive tuples until pack_rays rays or kMaxPackTuples tuples
+    // pack plan: consecutive tuples until pack_rays rays or kMaxPackTuples tuples; a tuple
+    // with more rays than pack_rays (fine pupils) gets a pack of its own
+    for (int t = 0; t < p.n_tuples; ++t)
+        if (p.sample_count[t / L] > pack_rays) pack_rays = p.sample_count[t / L];
     int packs = 0;
     int t = 0;
     while (t < p.n_tuples) {
@@ -258,10 +261,6 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         while (t < p.n_tuples && tuples < kMaxPackTuples) {
             const int n = p.sample_count[t / L];
             if (tuples > 0 && rays + n > pack_rays) break;
-            if (n > pack_rays) {
-                set_error("a tuple has %d rays; at most %d per block", n, pack_rays);
-                return MKB_ERR_UNSUPPORTED;
-            }
             rays += n;
             ++tuples;
             ++t;
@@ -271,6 +270,9 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         ++packs;
     }
     p.n_packs = packs;
+    p.pack_max = 0;
+    for (int k = 0; k < packs; ++k)
+        if (p.packs[k].rays > p.pack_max) p.pack_max = p.packs[k].rays;
     return MKB_OK;
 }
 

@@ -90,6 +90,7 @@ struct TraceParams {
     int rays;               // rays per variant
     int rings, spokes;
     int n_tuples, n_packs;
+    int pack_max;           // rays of the largest pack
     int sample_count[kMaxFields];   // n_f
     int field_offset[kMaxFields];   // ray offset of tuple (f, 0)
     uint8_t pupil_mode[kMaxFields];

@@ -31,14 +31,12 @@ constexpr int kPackRays = kThreads * kRaysPerThread;
 // memory of the workloads' tables fits as many
 constexpr int kTraceBlocksPerSm = 9;
 
-// The variant's record (the bulk-copy destination, 16-byte aligned) and the mu table live in
-// dynamic shared memory sized for the batch's record stride (trace_smem).
+// The variant's record (the bulk-copy destination, 16-byte aligned), the mu table and the
+// pack's per-ray OPL, penalty and status live in dynamic shared memory sized for the batch
+// (trace_smem): record [stride] | mu [S][L] | opl [pack_max] | pen [pack_max] | status.
 struct alignas(16) SharedTrace {
     uint64_t bar;
     SharedTables tab;
-    double opl[kPackRays];
-    double pen[kPackRays];
-    uint8_t status[kPackRays];
     int tuple_start[kMaxPackTuples + 1];
 };
 static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
@@ -155,6 +153,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     extern __shared__ __align__(16) double dyn[];
     double* record = dyn;                 // [stride]
     double* mu_tab = dyn + p.stride;      // [S][L]
+    double* opl_sh = mu_tab + p.S * p.L;  // [pack_max]
+    double* pen_sh = opl_sh + p.pack_max; // [pack_max]
+    uint8_t* status_sh = reinterpret_cast<uint8_t*>(pen_sh + p.pack_max);
     if (!stage_to_shared(record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
                          &sh.bar))
         return;
@@ -180,9 +181,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         double opl, pen;
         const int st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
                                     pen);
-        sh.opl[i] = opl;
-        sh.pen[i] = pen;
-        sh.status[i] = static_cast<uint8_t>(st);
+        opl_sh[i] = opl;
+        pen_sh[i] = pen;
+        status_sh[i] = static_cast<uint8_t>(st);
     }
     __syncthreads();
 
@@ -202,10 +203,10 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
             if (lane == 0) {
                 N w_acc(0.0), s_acc(0.0);
                 for (int k = 0; k < n; ++k) {
-                    if (in_piston(sh.status[base + k])) {
+                    if (in_piston(status_sh[base + k])) {
                         const N w = pupil_sample(p, sh.tab, f, k).weight;
                         w_acc += w;
-                        s_acc += w * N(sh.opl[base + k]);
+                        s_acc += w * N(opl_sh[base + k]);
                     }
                 }
                 vw = value_of(w_acc);
@@ -215,10 +216,10 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
             vs = __shfl_sync(0xffffffffu, vs, 0);
         } else {
             for (int k = lane; k < n; k += 32) {
-                if (in_piston(sh.status[base + k])) {
+                if (in_piston(status_sh[base + k])) {
                     const Sample smp = pupil_sample(p, sh.tab, f, k);
                     vw += smp.weight;
-                    vs += smp.weight * sh.opl[base + k];
+                    vs += smp.weight * opl_sh[base + k];
                 }
             }
             vw = warp_sum(vw);
@@ -231,16 +232,16 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         double sq = 0.0, psq = 0.0;
         int failed = 0, hard = 0;
         for (int k = lane; k < n; k += 32) {
-            const int st = sh.status[base + k];
+            const int st = status_sh[base + k];
             const Sample smp = pupil_sample(p, sh.tab, f, k);
-            const N e = (valid && in_piston(st)) ? N(sh.opl[base + k]) - piston : N(0.0);
+            const N e = (valid && in_piston(st)) ? N(opl_sh[base + k]) - piston : N(0.0);
             const N rw = smp.root_weight;
             const N r = scale * rw * e;
             N pr(0.0);
             if (soft_mode) {
                 const N fp = st == kOk ? N(0.0)
-                             : is_soft(st) ? N(sh.pen[base + k])
-                                           : N(sh.pen[base + k]) + N(1.0);
+                             : is_soft(st) ? N(pen_sh[base + k])
+                                           : N(pen_sh[base + k]) + N(1.0);
                 pr = pscale * rw * fp;
             }
             failed += st != kOk;
@@ -253,8 +254,8 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                 if (out.opd) out.opd[ray] = value_of(e);
                 if (out.status) out.status[ray] = static_cast<uint8_t>(st);
             } else if (kExact) {
-                sh.opl[base + k] = value_of(r);  // each lane rewrites only its own samples
-                sh.pen[base + k] = value_of(pr);
+                opl_sh[base + k] = value_of(r);  // each lane rewrites only its own samples
+                pen_sh[base + k] = value_of(pr);
             } else {
                 sq += value_of(r * r);
                 psq += value_of(pr * pr);
@@ -266,12 +267,12 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                 if (lane == 0) {  // sum_k r_k^2, then sum_k p_k^2, in ascending k
                     N tuple(0.0), pen(0.0);
                     for (int k = 0; k < n; ++k) {
-                        const N x = sh.opl[base + k];
+                        const N x = opl_sh[base + k];
                         tuple += x * x;
                     }
                     if (soft_mode) {
                         for (int k = 0; k < n; ++k) {
-                            const N x = sh.pen[base + k];
+                            const N x = pen_sh[base + k];
                             pen += x * x;
                         }
                         tuple += pen;
@@ -315,9 +316,12 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
     hard[v] = nh;
 }
 
-// dynamic shared memory of trace_kernel: the record (stride is even) and the mu table
+// dynamic shared memory of trace_kernel: the record (stride is even), the mu table and the
+// pack's per-ray OPL, penalty and status
 size_t trace_smem(const TraceParams& p) {
-    return (static_cast<size_t>(p.stride) + static_cast<size_t>(p.S) * p.L) * sizeof(double);
+    return (static_cast<size_t>(p.stride) + static_cast<size_t>(p.S) * p.L +
+            2 * static_cast<size_t>(p.pack_max)) * sizeof(double) +
+           ((static_cast<size_t>(p.pack_max) + 15) & ~size_t(15));
 }
 
 // Launches trace_kernel<kResiduals, precision> (MIXED traces in FP64 with contraction; its FP32

@@ -320,6 +320,64 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
     return b, settings, variable_sets, x0
 
 
+# ---- configuration 4: precision sweep -----------------------------------------------------------
+
+def sweep(variants: int = 65536, seed: int = 20261203 + 4, surfaces: int = 20,
+          wavelengths: int = 9, rings: int = 32, spokes: int = 32, sigma: float = 0.05,
+          failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+    """Configuration 4: `variants` systems of `surfaces` table surfaces in the element style of
+    configuration 1 -- the stop, E = (S - 1) // 2 biconvex elements (curvatures +-1/(50 E),
+    glass 6/E mm, air 0.5 mm, each perturbed by `sigma` Gaussian noise; Cauchy glass) and,
+    when S - 1 is odd, a zero-power plate before the image at the paraxial focus -- at
+    `wavelengths` wavelengths 405..700 nm, 5 fields 0..1 degree, Half pupils rings x spokes
+    (32 x 32 = 1,024 rays per field and wavelength), pupil radius 5 mm. Variables: the working
+    distance, every curvature and every glass thickness. Returns (batch, settings, variables,
+    x0)."""
+    S = surfaces
+    E = (S - 1) // 2
+    lam = np.linspace(405.0, 700.0, wavelengths)
+    topo = BatchTopology(surfaces=S, wavelengths=wavelengths, fields=5,
+                         type=[SURFACE_STOP] + [SURFACE_SPHERE] * (S - 1),
+                         pupil_mode=[PUPIL_HALF] * 5)
+    b = SystemBatchHost(topo, variants)
+    b.reference_wavelength_nm = 587.6
+    b.wavelength_nm[:] = lam
+    b.wavelength_weight[:] = 1.0
+    b.field_weight[:] = 1.0
+    rng = Stream(seed)
+    noise = rng.normal(1, variants * 2 * S).reshape(variants, S, 2)
+    c = np.zeros((variants, S))
+    t = np.zeros((variants, S))
+    nr = np.ones((variants, S))
+    for e in range(E):
+        s1, s2 = 1 + 2 * e, 2 + 2 * e
+        c[:, s1] = (1.0 / (50.0 * E)) * (1.0 + sigma * noise[:, s1, 0])
+        c[:, s2] = (-1.0 / (50.0 * E)) * (1.0 + sigma * noise[:, s2, 0])
+        t[:, s1] = (6.0 / E) * (1.0 + sigma * noise[:, s1, 1])
+        t[:, s2] = 0.5 * (1.0 + sigma * noise[:, s2, 1])
+        nr[:, s1] = float(cauchy_index(587.6))
+    efl, bfd = paraxial(c, t, nr)
+    t[:, S - 1] = bfd
+    b.curvature[:] = c
+    b.thickness[:] = t
+    b.index[:] = 1.0
+    n = cauchy_index(lam)
+    for e in range(E):
+        b.index[:, 1 + 2 * e, :] = n[None, :]
+    angles = np.deg2rad(np.linspace(0.0, 1.0, 5))
+    b.pupil_radius[:] = 5.0
+    b.field_angle[:] = angles[None, :]
+    b.field_target[:] = efl[:, None] * np.tan(angles)[None, :]
+    settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
+    variables = [Variable(VAR_WORKING_DISTANCE, S - 1, 1.0, 500.0, 1.0)]
+    variables += [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, 1 + 2 * E)]
+    variables += [Variable(VAR_THICKNESS, 1 + 2 * e, 0.1, 20.0, 1.0) for e in range(E)]
+    vs = VariableSet(topo, variables)
+    x0 = np.concatenate([b.thickness[:, S - 1:S], b.curvature[:, 1:1 + 2 * E],
+                         b.thickness[:, 1:1 + 2 * E:2]], axis=1)
+    return b, settings, vs, x0
+
+
 # ---- ghost plates ------------------------------------------------------------------------------
 
 def ghost(variants: int = 64, seed: int = 20261203 + 11, terms: int = 4,
