@@ -12,6 +12,7 @@ or without the built library the calls raise.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 from dataclasses import dataclass
 import enum
 
@@ -19,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _capi
-from .batch import ResidualLayout, ResidualSettings, SystemBatchHost
+from .batch import FAILURE_SOFT, ResidualLayout, ResidualSettings, SystemBatchHost
 
 
 class TraceMode(enum.Enum):
@@ -264,7 +265,9 @@ LM_STATUS = {0: "running", 1: "converged_merit", 2: "converged_step", 3: "conver
 
 @dataclass
 class LmOptions:
-    """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85), one penalty pass."""
+    """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85). fail_weight_factor and
+    max_fail_weight drive the outer soft-failure penalty rounds of optimize_lm_gpu
+    (optimize_lm_rounds, src/optim/levenberg_marquardt.cpp:891); a factor <= 1 gives one pass."""
 
     max_iterations: int = 100
     ftol: float = 1e-10
@@ -276,6 +279,8 @@ class LmOptions:
     reject_new_failures: bool = True
     jacobian: int = JACOBIAN_ADJOINT
     gram_exact: bool = True
+    fail_weight_factor: float = 10.0
+    max_fail_weight: float = 1e14
 
     def c_struct(self) -> "_capi.LmOptions":
         o = _capi.LmOptions()
@@ -428,13 +433,8 @@ class DeviceLm:
         return out
 
 
-def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x0,
-                    options: LmOptions | None = None, device: int = 0) -> dict:
-    """optimize_lm_gpu (include/mikroptim/cuda/levenberg_marquardt.hpp): batched LM of the runs
-    x0 [runs][P] on `batch` (1 variant for all runs or one per run), one penalty pass.
-    `variables` may be a list of one VariableSet per run (uneven batches; x0 rows padded)."""
-    options = options or LmOptions()
-    dev = _require_cuda(f"cuda:{device}")
+def _lm_pass(batch, layout, variables, x0, options, dev) -> dict:
+    """One LM pass of every run on the device (levenberg_marquardt with GpuLmBackend)."""
     if isinstance(variables, (list, tuple)):
         runs = len(variables)
         x0 = pad_rows(x0, runs, max(v.size for v in variables))
@@ -451,6 +451,65 @@ def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x
         res["cycles"] = lm.cycles
         _device_status()
         return res
+
+
+LM_NUMERICAL_ERROR = 7  # LmStatus::NumericalError
+
+
+def optimize_lm_gpu(batch: SystemBatchHost, layout: ResidualLayout, variables, x0,
+                    options: LmOptions | None = None, device: int = 0) -> dict:
+    """optimize_lm_gpu (include/mikroptim/cuda/levenberg_marquardt.hpp): batched LM of the runs
+    x0 [runs][P] on `batch` (1 variant for all runs or one per run). `variables` may be a list
+    of one VariableSet per run (uneven batches; x0 rows padded).
+
+    In soft-failure mode the outer penalty rounds follow (optimize_lm_rounds,
+    src/optim/levenberg_marquardt.cpp:891): runs that end with failed rays (and not in
+    NumericalError) restart together from their end point with fail_weight times
+    fail_weight_factor, as long as the weight stays <= max_fail_weight. Per run: x, merit,
+    failed rays, status and damping of the last round; iterations, accepted steps and Jacobians
+    summed; the merit histories of the rounds joined (padded with NaN); fail_weight and
+    penalty_rounds."""
+    options = options or LmOptions()
+    dev = _require_cuda(f"cuda:{device}")
+    res = _lm_pass(batch, layout, variables, x0, options, dev)
+    runs = res["x"].shape[0]
+    weight = layout.settings.fail_weight
+    res["fail_weight"] = np.full(runs, weight)
+    res["penalty_rounds"] = np.ones(runs, np.int32)
+    histories = [[h[~np.isnan(h)]] for h in res["history"]]
+    if not (layout.settings.failure == FAILURE_SOFT and options.fail_weight_factor > 1.0 and
+            weight > 0.0):
+        return res
+    per_run = isinstance(variables, (list, tuple))
+    while True:
+        weight *= options.fail_weight_factor
+        if not weight <= options.max_fail_weight:
+            break
+        again = [i for i in range(runs)
+                 if res["failed"][i] > 0 and res["status"][i] != LM_NUMERICAL_ERROR]
+        if not again:
+            break
+        tmpl = batch if batch.variants == 1 else batch.take(again)
+        lay = ResidualLayout(layout.topology, dataclasses.replace(layout.settings,
+                                                                  fail_weight=weight))
+        vars_again = [variables[i] for i in again] if per_run else variables
+        part = _lm_pass(tmpl, lay, vars_again, res["x"][again], options, dev)
+        for j, i in enumerate(again):
+            for k in ("x", "merit", "failed", "hard_failed", "status", "damping"):
+                res[k][i] = part[k][j]
+            for k in ("iterations", "accepted", "jacobians"):
+                res[k][i] += part[k][j]
+            h = part["history"][j]
+            histories[i].append(h[~np.isnan(h)])
+            res["fail_weight"][i] = weight
+            res["penalty_rounds"][i] += 1
+        res["cycles"] += part["cycles"]
+    joined = [np.concatenate(h) for h in histories]
+    width = max(res["history"].shape[1], max(len(h) for h in joined))
+    res["history"] = np.full((runs, width), np.nan)
+    for i, h in enumerate(joined):
+        res["history"][i, :len(h)] = h
+    return res
 
 
 def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: ResidualLayout,

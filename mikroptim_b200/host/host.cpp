@@ -3,6 +3,7 @@
 
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <set>
@@ -128,6 +129,32 @@ void SystemBatchHost::set_decenter_tilt(int v, int s, double dx, double dy, doub
     decenter_tilt(v, s, 1) = dy;
     decenter_tilt(v, s, 2) = alpha;
     decenter_tilt(v, s, 3) = beta;
+}
+
+SystemBatchHost take_variants(const SystemBatchHost& batch, const std::vector<int>& variants) {
+    SystemBatchHost out(batch.topology(), static_cast<int>(variants.size()));
+    out.reference_wavelength_nm = batch.reference_wavelength_nm;
+    out.wavelength_weight = batch.wavelength_weight;
+    out.field_weight = batch.field_weight;
+    out.ghost_norm_radius_ = batch.ghost_norm_radius_;
+    auto copy = [&](const std::vector<double>& from, std::vector<double>& to, size_t n) {
+        for (size_t j = 0; j < variants.size(); ++j) {
+            const size_t i = batch.check_v(variants[j]);
+            std::copy(from.begin() + i * n, from.begin() + (i + 1) * n, to.begin() + j * n);
+        }
+    };
+    const size_t S = batch.surfaces(), L = batch.wavelengths(), F = batch.fields();
+    const size_t G = batch.topology().ghost_plates, K = batch.topology().ghost_terms;
+    copy(batch.curvature_, out.curvature_, S);
+    copy(batch.thickness_, out.thickness_, S);
+    copy(batch.index_, out.index_, S * L);
+    copy(batch.pupil_radius_, out.pupil_radius_, 1);
+    copy(batch.field_angle_, out.field_angle_, F);
+    copy(batch.field_target_, out.field_target_, F);
+    if (!batch.decenter_tilt_.empty()) copy(batch.decenter_tilt_, out.decenter_tilt_, S * 4);
+    copy(batch.ghost_coeff_, out.ghost_coeff_, G * K);
+    copy(batch.ghost_index_, out.ghost_index_, G * L);
+    return out;
 }
 
 SystemBatchHost make_non_coaxial(const SystemBatchHost& batch) {
@@ -648,10 +675,12 @@ void DeviceNormalEquations::download(std::vector<double>& a, std::vector<double>
     }
 }
 
-LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
-                         const SystemBatchHost& base, const std::vector<double>& x0,
-                         const LmOptions& options, const ResidualSettings& settings,
-                         LmGpuStats* stats) {
+namespace {
+
+// One LM pass of every run on the device.
+LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const SystemBatchHost& base,
+                 const std::vector<double>& x0, const LmOptions& options,
+                 const ResidualSettings& settings, LmGpuStats* stats) {
     cuda_check(cudaSetDevice(engine.device()), "cudaSetDevice");
     const int runs = runs_of(variables, base, x0);
     const int P = variables.size();
@@ -711,7 +740,72 @@ LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
                                 engine.stream()),
           "lm results");
     engine.synchronize();
-    if (stats != nullptr) stats->cycles = cycles;
+    r.history_width = static_cast<int>(H);
+    r.fail_weight.assign(R, settings.fail_weight);
+    r.penalty_rounds.assign(R, 1);
+    if (stats != nullptr) stats->cycles += cycles;
+    return r;
+}
+
+}  // namespace
+
+LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
+                         const SystemBatchHost& base, const std::vector<double>& x0,
+                         const LmOptions& options, const ResidualSettings& settings,
+                         LmGpuStats* stats) {
+    if (stats != nullptr) stats->cycles = 0;
+    LmResult r = lm_pass(engine, variables, base, x0, options, settings, stats);
+    const int P = variables.size();
+    const size_t R = r.merit.size();
+    // the merit history of every round, joined per run
+    std::vector<std::vector<double>> hist(R);
+    auto add_history = [](std::vector<double>& to, const double* h, int width) {
+        for (int k = 0; k < width && !std::isnan(h[k]); ++k) to.push_back(h[k]);
+    };
+    for (size_t i = 0; i < R; ++i)
+        add_history(hist[i], r.history.data() + i * r.history_width, r.history_width);
+    double weight = settings.fail_weight;
+    if (settings.failure == FailureMode::Soft && options.fail_weight_factor > 1.0 &&
+        weight > 0.0) {
+        for (;;) {
+            weight *= options.fail_weight_factor;
+            if (!(weight <= options.max_fail_weight)) break;
+            std::vector<int> again;
+            std::vector<double> xs;
+            for (size_t i = 0; i < R; ++i)
+                if (r.failed[i] > 0 && r.status[i] != static_cast<int32_t>(LmStatus::NumericalError)) {
+                    again.push_back(static_cast<int>(i));
+                    xs.insert(xs.end(), r.x.begin() + i * P, r.x.begin() + (i + 1) * P);
+                }
+            if (again.empty()) break;
+            ResidualSettings round = settings;
+            round.fail_weight = weight;
+            const LmResult q = base.variants() == 1
+                                   ? lm_pass(engine, variables, base, xs, options, round, stats)
+                                   : lm_pass(engine, variables, take_variants(base, again), xs,
+                                             options, round, stats);
+            for (size_t j = 0; j < again.size(); ++j) {
+                const size_t i = static_cast<size_t>(again[j]);
+                std::copy(q.x.begin() + j * P, q.x.begin() + (j + 1) * P, r.x.begin() + i * P);
+                r.merit[i] = q.merit[j];
+                r.failed[i] = q.failed[j];
+                r.hard_failed[i] = q.hard_failed[j];
+                r.status[i] = q.status[j];
+                r.damping[i] = q.damping[j];
+                r.iterations[i] += q.iterations[j];
+                r.accepted[i] += q.accepted[j];
+                r.jacobians[i] += q.jacobians[j];
+                add_history(hist[i], q.history.data() + j * q.history_width, q.history_width);
+                r.fail_weight[i] = weight;
+                ++r.penalty_rounds[i];
+            }
+        }
+    }
+    size_t width = static_cast<size_t>(r.history_width);
+    for (const auto& h : hist) width = std::max(width, h.size());
+    r.history.assign(R * width, std::numeric_limits<double>::quiet_NaN());
+    for (size_t i = 0; i < R; ++i) std::copy(hist[i].begin(), hist[i].end(), r.history.begin() + i * width);
+    r.history_width = static_cast<int>(width);
     return r;
 }
 

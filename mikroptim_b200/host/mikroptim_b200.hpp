@@ -102,7 +102,12 @@ private:
     std::vector<double> curvature_, thickness_, index_, pupil_radius_, field_angle_,
         field_target_, decenter_tilt_, ghost_coeff_, ghost_index_, ghost_norm_radius_;
     friend SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
+    friend SystemBatchHost take_variants(const SystemBatchHost& batch,
+                                         const std::vector<int>& variants);
 };
+
+// Batch of the listed variants of `batch`, in that order (lm_template_batch).
+SystemBatchHost take_variants(const SystemBatchHost& batch, const std::vector<int>& variants);
 
 // Copy of `batch` with a non-coaxial topology (decenter and tilt zero, Full pupils).
 SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
@@ -185,6 +190,10 @@ struct LmOptions {
     double diag_floor = 1e-12;
     JacobianMethod jacobian = JacobianMethod::Adjoint;
     bool gram_exact = true;  // false: FP64 tensor cores (with the adjoint: J never in memory)
+    // outer soft-failure penalty rounds (levenberg_marquardt.hpp:120-125): runs that end with
+    // failed rays restart with w_fail x fail_weight_factor while it stays <= max_fail_weight
+    double fail_weight_factor = 10.0;
+    double max_fail_weight = 1e14;
     mkb_lm_options c_struct() const;
 };
 
@@ -310,17 +319,21 @@ private:
 };
 
 struct LmResult {
-    std::vector<double> x, merit, damping, history;
-    std::vector<int32_t> status, iterations, accepted, jacobians;
+    std::vector<double> x, merit, damping;
+    std::vector<double> history;  // [runs][history_width], the rounds joined, NaN padded
+    int history_width = 0;
+    std::vector<int32_t> status, iterations, accepted, jacobians, penalty_rounds;
     std::vector<int64_t> failed, hard_failed;
+    std::vector<double> fail_weight;
 };
 
 struct LmGpuStats {
     int cycles = 0;
 };
 
-// Batched LM of the runs x0 [runs][P] on `base` (1 variant for all runs or one per run),
-// one soft-failure penalty pass; the whole loop runs on the device.
+// Batched LM of the runs x0 [runs][P] on `base` (1 variant for all runs or one per run); the
+// whole loop runs on the device. In soft-failure mode the outer penalty rounds follow
+// (optimize_lm_rounds, src/optim/levenberg_marquardt.cpp:891).
 LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
                          const SystemBatchHost& base, const std::vector<double>& x0,
                          const LmOptions& options, const ResidualSettings& settings,

@@ -112,7 +112,7 @@ def test_lm_trajectories_bitwise_equal_reference(method):
     b, st, vs, x0, lay = batch(4)
     opt = engine.LmOptions(max_iterations=8,
                            jacobian=engine.JACOBIAN_ADJOINT if method == "adjoint"
-                           else engine.JACOBIAN_FD, gram_exact=True)
+                           else engine.JACOBIAN_FD, gram_exact=True, fail_weight_factor=1.0)
     g = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
     r = po.reference().optimize_lm(b, lay, vs, x0, max_iterations=8, method=method,
                                    penalty_rounds=1, threads=4)

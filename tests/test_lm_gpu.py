@@ -26,7 +26,8 @@ def run_both(method, runs=6, max_iterations=25, gram_exact=True, precision=0):
                                                   failure=st.failure, precision=precision))
     opt = engine.LmOptions(max_iterations=max_iterations,
                            jacobian=engine.JACOBIAN_ADJOINT if method == "adjoint"
-                           else engine.JACOBIAN_FD, gram_exact=gram_exact)
+                           else engine.JACOBIAN_FD, gram_exact=gram_exact,
+                           fail_weight_factor=1.0)
     g = engine.optimize_lm_gpu(b, lay_gpu, vs, x0, opt)
     r = po.reference().optimize_lm(b, lay, vs, x0, max_iterations=max_iterations,
                                    method=method, penalty_rounds=1, threads=4)
@@ -91,3 +92,18 @@ def test_lm_cycle_graph_replay_equals_direct_cycles(method):
     assert np.array_equal(np.isnan(a["history"]), np.isnan(g["history"]))
     assert np.array_equal(a["history"][h], g["history"][h])
     assert int(a["iterations"].sum()) > 0
+
+
+def test_lm_penalty_rounds_bitwise_equal_reference():
+    """Outer soft-failure penalty rounds (optimize_lm_rounds): objectives at NA 0.95 end with
+    vignetted rays, so runs restart with w_fail x 10 up to 1e14; every run's end point, merit,
+    status and summed counters equal the reference's optimize_lm_cpu with its default rounds."""
+    b, st, vs, x0 = workloads.objective(4, rings=3, spokes=6)
+    lay = ResidualLayout(b.topology, st)
+    opt = engine.LmOptions(max_iterations=4, jacobian=engine.JACOBIAN_ADJOINT, gram_exact=True)
+    g = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
+    r = po.reference().optimize_lm(b, lay, vs, x0, max_iterations=4, method="adjoint",
+                                   penalty_rounds=2, threads=4)
+    assert np.any(g["penalty_rounds"] > 1)
+    for k in ("status", "iterations", "accepted", "x", "merit"):
+        assert np.array_equal(g[k], r[k]), k

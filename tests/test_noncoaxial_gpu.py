@@ -99,7 +99,8 @@ def test_mixed_normal_equations_within_the_mixed_bar():
 @pytest.mark.skipif(not has_reference_build(), reason="reference build missing")
 def test_lm_trajectories_bitwise_equal_reference():
     b, st, vs, x0, lay = batch(4, rings=4, spokes=8)
-    opt = engine.LmOptions(max_iterations=6, jacobian=engine.JACOBIAN_ADJOINT, gram_exact=True)
+    opt = engine.LmOptions(max_iterations=6, jacobian=engine.JACOBIAN_ADJOINT, gram_exact=True,
+                           fail_weight_factor=1.0)
     g = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
     r = po.reference().optimize_lm(b, lay, vs, x0, max_iterations=6, method="adjoint",
                                    penalty_rounds=1, threads=4)
