@@ -68,7 +68,7 @@ enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_
  * sag root and OPL accumulation. */
 enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2 };
 enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2,
-       MKB_VAR_GHOST_COEFFICIENT = 3 };
+       MKB_VAR_GHOST_COEFFICIENT = 3, MKB_VAR_GLASS = 4 };
                                                        /* VariableType, model/variables.hpp:18 */
 
 /* ---- batch ------------------------------------------------------------------------------
@@ -102,6 +102,11 @@ typedef struct mkb_batch_view {
     const double* ghost_coeff;
     const double* ghost_norm_radius;
     const double* ghost_index;
+    /* Glass variables: the Buchdahl coefficients (n0, nu1, nu2, nu3) of the medium after every
+     * surface [V][S][4] (SystemBatchHost::buchdahl_coeff, system_batch.hpp:147) and the
+     * wavelengths [L] in nm; NULL when no variable is a glass. */
+    const double* buchdahl_coeff;
+    const double* wavelength_nm;
 } mkb_batch_view;
 
 /* The device-resident batch: one 16-byte aligned record of `record_stride` doubles per
@@ -109,7 +114,8 @@ typedef struct mkb_batch_view {
  * Record layout (doubles): curvature[S] | thickness[S] | index[S*L] | pupil_radius |
  * sin(field_angle)[F] | cos(field_angle)[F] | field_target[F] | [non-coaxial: per surface
  * dx, dy, cos alpha, sin alpha, cos beta, sin beta, moved, 0] | [ghost plates:
- * coefficients [G][K] | normalisation radius [G] | index [G][L]] | padding. */
+ * coefficients [G][K] | normalisation radius [G] | index [G][L]] | [glass: Buchdahl
+ * coefficients [S][4]] | padding. */
 typedef struct mkb_device_batch {
     int32_t variants, surfaces, wavelengths, fields;
     int32_t record_stride;            /* doubles per variant, even                      */
@@ -122,6 +128,8 @@ typedef struct mkb_device_batch {
                                          working distance is thickness[n-1], the entries
                                          past n are ignored. NULL: every variant uses S. */
     int32_t ghost_plates, ghost_terms;  /* G, K: the records carry the plates' data       */
+    int32_t glass;                    /* 1: the records carry Buchdahl coefficients [S][4] */
+    const double* wavelength_nm;      /* host [L] nm; needed when glass = 1              */
 } mkb_device_batch;
 
 /* Doubles per packed variant record for a coaxial batch shape without ghost plates (>= 2,
@@ -130,7 +138,8 @@ int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields)
 
 /* Doubles per packed variant record for any batch shape. */
 int32_t mkb_record_stride_ext(int32_t surfaces, int32_t wavelengths, int32_t fields,
-                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms);
+                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms,
+                              int32_t glass);
 
 /* Packs a host SoA view into host records [V][mkb_record_stride_ext(...)] (sin/cos of the
  * field angles and of the tilts are taken here with the host libm, so the start rays and the
@@ -152,6 +161,11 @@ typedef struct mkb_variables {
      * plate g (0 .. G-1, table order) and order k (1 .. K); NULL when there are none. */
     const int32_t* ghost_plate;
     const int32_t* ghost_order;
+    /* Glass variables (Buchdahl coordinate of the medium after `surface`; the reference's
+     * VariableType::Glass): host [P] component 0 = n0, 1 = nu1, 2 = nu2; NULL when none.
+     * Writing one recomputes that medium's index at every wavelength,
+     * n = n0 + w (nu1 + w (nu2 + w nu3)), w = the Buchdahl coordinate of the wavelength. */
+    const int32_t* glass_component;
 } mkb_variables;
 
 /* VariableSet::apply on the device: records_out [runs][record_stride] = the run's template

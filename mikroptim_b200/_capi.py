@@ -47,6 +47,8 @@ class BatchView(C.Structure):
         ("ghost_coeff", P_double),
         ("ghost_norm_radius", P_double),
         ("ghost_index", P_double),
+        ("buchdahl_coeff", P_double),
+        ("wavelength_nm", P_double),
     ]
 
 
@@ -60,6 +62,8 @@ class DeviceBatch(C.Structure):
         ("type", P_uint8),
         ("variant_surfaces", C.c_void_p),
         ("ghost_plates", C.c_int32), ("ghost_terms", C.c_int32),
+        ("glass", C.c_int32),
+        ("wavelength_nm", P_double),
     ]
 
 
@@ -92,6 +96,7 @@ class Variables(C.Structure):
         ("typical", P_double),
         ("ghost_plate", P_int32),
         ("ghost_order", P_int32),
+        ("glass_component", P_int32),
     ]
 
 
@@ -120,7 +125,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_record_stride.restype = c.c_int32
     lib.mkb_record_stride.argtypes = [c.c_int32, c.c_int32, c.c_int32]
     lib.mkb_record_stride_ext.restype = c.c_int32
-    lib.mkb_record_stride_ext.argtypes = [c.c_int32] * 6
+    lib.mkb_record_stride_ext.argtypes = [c.c_int32] * 7
     lib.mkb_pack_batch_host.restype = c.c_int
     lib.mkb_pack_batch_host.argtypes = [C.POINTER(BatchView), P_double]
     lib.mkb_rays_per_variant.restype = c.c_int64

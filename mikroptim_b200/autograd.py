@@ -54,6 +54,7 @@ class AdjointProblem:
         out.non_coaxial = self.templates.non_coaxial
         out.ghost_plates = self.templates.ghost_plates
         out.ghost_terms = self.templates.ghost_terms
+        out.glass, out.wavelength_nm = self.templates.glass, self.templates.wavelength_nm
         out.variant_surfaces = None
         out.records = torch.empty((max(runs, 1), out.stride), dtype=torch.float64,
                                   device=self.device)

@@ -27,7 +27,8 @@ from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_le
 SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
 FAILURE_SOFT, FAILURE_HARD = 0, 1
 PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA = 0, 1, 2
-VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT = 0, 1, 2, 3
+VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT, VAR_GLASS = 0, 1, 2, 3, 4
+BUCHDAHL_LAMBDA0_UM, BUCHDAHL_ALPHA = 0.546074, 2.5  # glass/dispersion.hpp:13,15
 MAX_GHOST_PLATES, MAX_GHOST_TERMS = 16, 32
 
 MAX_SURFACES = 64
@@ -134,6 +135,9 @@ class SystemBatchHost:
         self.ghost_coeff = np.zeros((variants, G, K))
         self.ghost_norm_radius = np.ones(G)
         self.ghost_index = np.ones((variants, G, L))
+        # glass variables: Buchdahl coefficients (n0, nu1, nu2, nu3) of the medium after every
+        # surface [V][S][4] (SystemBatchHost::buchdahl_coeff); None when no variable is a glass
+        self.buchdahl_coeff: np.ndarray | None = None
         # uneven batches: table surfaces each variant uses (2 .. S); None = all use S
         self.variant_surfaces: np.ndarray | None = None
 
@@ -169,6 +173,8 @@ class SystemBatchHost:
             setattr(out, name, np.array(getattr(self, name)[sl], copy=True))
         if self.decenter_tilt is not None:
             out.decenter_tilt = np.array(self.decenter_tilt[sl])
+        if self.buchdahl_coeff is not None:
+            out.buchdahl_coeff = np.array(self.buchdahl_coeff[sl])
         for name in ("ghost_coeff", "ghost_index"):
             setattr(out, name, np.array(getattr(self, name)[sl], copy=True))
         out.ghost_norm_radius = self.ghost_norm_radius.copy()
@@ -185,6 +191,8 @@ class SystemBatchHost:
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
         if self.decenter_tilt is not None:
             out.decenter_tilt = np.ascontiguousarray(self.decenter_tilt[idx])
+        if self.buchdahl_coeff is not None:
+            out.buchdahl_coeff = np.ascontiguousarray(self.buchdahl_coeff[idx])
         for name in ("ghost_coeff", "ghost_index"):
             setattr(out, name, np.ascontiguousarray(getattr(self, name)[idx]))
         out.ghost_norm_radius = self.ghost_norm_radius.copy()
@@ -269,6 +277,11 @@ class SystemBatchHost:
             dt = np.ascontiguousarray(self.decenter_tilt, dtype=np.float64)
             arrays["decenter_tilt"] = dt
             v.decenter_tilt = _capi.ptr(dt)
+        if self.buchdahl_coeff is not None:
+            for name in ("buchdahl_coeff", "wavelength_nm"):
+                a = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
+                arrays[name] = a
+                setattr(v, name, _capi.ptr(a))
         if self.topology.ghost_plates > 0:
             for name in ("ghost_coeff", "ghost_norm_radius", "ghost_index"):
                 a = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
@@ -282,6 +295,19 @@ class SystemBatchHost:
     @property
     def non_coaxial(self) -> bool:
         return self.decenter_tilt is not None
+
+    def buchdahl_omega(self) -> np.ndarray:
+        """Buchdahl coordinate of every wavelength, dl / (1 + 2.5 dl), dl = lambda [um] -
+        0.546074 (buchdahl_omega, glass/dispersion.hpp:87)."""
+        dl = self.wavelength_nm / 1000.0 - BUCHDAHL_LAMBDA0_UM
+        return dl / (1.0 + BUCHDAHL_ALPHA * dl)
+
+    def refresh_glass_index(self, v: int, s: int) -> None:
+        """index[v][s][:] from the Buchdahl coefficients, n0 + w (nu1 + w (nu2 + w nu3))
+        (buchdahl_index, glass/dispersion.hpp:93)."""
+        n0, nu1, nu2, nu3 = self.buchdahl_coeff[v, s]
+        w = self.buchdahl_omega()
+        self.index[v, s, :] = n0 + w * (nu1 + w * (nu2 + w * nu3))
 
 
 def make_non_coaxial(batch: SystemBatchHost) -> SystemBatchHost:
@@ -400,6 +426,8 @@ class Variable:
     # GhostCoefficient: a_order of plate `plate` (surface is then the plate's table surface)
     plate: int = -1
     order: int = 0
+    # Glass: Buchdahl component (0 n0, 1 nu1, 2 nu2) of the medium after `surface`
+    component: int = -1
 
 
 @dataclass
@@ -423,6 +451,10 @@ class VariableSet:
                     raise ValueError(f"VariableSet: variable {k}: thickness surface out of range")
             elif v.type == VAR_WORKING_DISTANCE:
                 v.surface = S - 1
+            elif v.type == VAR_GLASS:
+                if not (0 <= v.surface < S and 0 <= v.component <= 2):
+                    raise ValueError(f"VariableSet: variable {k}: glass component {v.component} "
+                                     f"of surface {v.surface} does not exist")
             elif v.type == VAR_GHOST_COEFFICIENT:
                 if not (0 <= v.plate < self.topology.ghost_plates and
                         1 <= v.order <= self.topology.ghost_terms):
@@ -432,6 +464,7 @@ class VariableSet:
             else:
                 raise NotImplementedError(f"VariableSet: variable type {v.type}")
             key = ((2, v.plate, v.order) if v.type == VAR_GHOST_COEFFICIENT
+                   else (3, v.surface, v.component) if v.type == VAR_GLASS
                    else (v.type == VAR_CURVATURE, v.surface))
             if key in seen:
                 raise ValueError(f"VariableSet: parameter of variable {k} already used")
@@ -460,6 +493,8 @@ class VariableSet:
         for k, var in enumerate(self.variables):
             if var.type == VAR_GHOST_COEFFICIENT:
                 x[k] = batch.ghost_coeff[v, var.plate, var.order - 1]
+            elif var.type == VAR_GLASS:
+                x[k] = batch.buchdahl_coeff[v, var.surface, var.component]
             else:
                 x[k] = (batch.curvature[v, var.surface] if var.type == VAR_CURVATURE
                         else batch.thickness[v, var.surface])
@@ -477,8 +512,12 @@ class VariableSet:
                 batch.curvature[v, var.surface] = x[k]
             elif var.type == VAR_GHOST_COEFFICIENT:
                 batch.ghost_coeff[v, var.plate, var.order - 1] = x[k]
+            elif var.type == VAR_GLASS:
+                batch.buchdahl_coeff[v, var.surface, var.component] = x[k]
             else:
                 batch.thickness[v, var.surface] = x[k]
+        for s in sorted({var.surface for var in self.variables if var.type == VAR_GLASS}):
+            batch.refresh_glass_index(v, s)
 
     def c_struct(self) -> _capi.Variables:
         keep = {
@@ -487,6 +526,7 @@ class VariableSet:
             "lower": self.lower(), "upper": self.upper(), "typical": self.typical(),
             "ghost_plate": np.array([v.plate for v in self.variables], dtype=np.int32),
             "ghost_order": np.array([v.order for v in self.variables], dtype=np.int32),
+            "glass_component": np.array([v.component for v in self.variables], dtype=np.int32),
         }
         s = _capi.Variables()
         s.count = self.size
@@ -494,6 +534,7 @@ class VariableSet:
         s.surface = _capi.ptr(keep["surface"], C.c_int32)
         s.ghost_plate = _capi.ptr(keep["ghost_plate"], C.c_int32)
         s.ghost_order = _capi.ptr(keep["ghost_order"], C.c_int32)
+        s.glass_component = _capi.ptr(keep["glass_component"], C.c_int32)
         s.lower, s.upper, s.typical = (_capi.ptr(keep[n]) for n in ("lower", "upper", "typical"))
         s._keep = keep
         return s

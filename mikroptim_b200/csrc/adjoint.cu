@@ -148,6 +148,17 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
     auto write = [&](int col, N value) {
         if (col >= 0) col0[static_cast<int64_t>(col) * R + row] = value_of(factor * value);
     };
+    // the index of medium s enters the steps onto s and onto s + 1: its adjoint is summed over
+    // both (a carry) and written to the glass columns of s with dn/d(n0, nu1, nu2) =
+    // (1, w, w^2) at this wavelength (AdjointRowWriter::index, merit/ray_jacobian.hpp:66)
+    N n_carry = zero;
+    auto index_sink = [&](int s, N value) {
+        if (!v.has_glass) return;
+        const double w = v.omega[l];
+        const N slope[3] = {N(1.0), N(w), N(w) * N(w)};
+        for (int c = 0; c < 3; ++c)
+            if (v.col_glass[s][c] >= 0) write(v.col_glass[s][c], value * slope[c]);
+    };
     for (int c = (count - 1) / kInterval; c >= 0; --c) {
         const int first = c * kInterval;
         const int n = (count - first) < kInterval ? (count - first) : kInterval;
@@ -187,6 +198,7 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                                                    seed_opl, seed_pen, adj, center_adj,
                                                    n_image_adj);
                         write(v.col_thickness[S - 1], center_adj.z);
+                        n_carry = n_image_adj;
                     }
                 } else {
                     const int j = s + 1;
@@ -227,11 +239,14 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                     }
                     if (sphere) write(v.col_curvature[j], par.curvature);
                     write(v.col_thickness[s], par.thickness);
+                    index_sink(j, par.n_after + n_carry);
+                    n_carry = par.n_before;
                 }
                 next_branch = ck.branch(s);
             }
         }
     }
+    index_sink(0, n_carry);
 }
 
 template <bool kExact>
@@ -632,6 +647,26 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
     }
     int next_branch = kBranchRegular;
     const Vec<N> center{zero, N(rec[lay.target + f]), N(thick[S - 1])};
+    // glass variables (kernel feature 4): the adjoint of the index of each medium, carried from
+    // the step onto s + 1 to the step onto s and written with dn/d(n0, nu1, nu2) = (1, w, w^2)
+    constexpr bool kGlass = (kFeat & 4) != 0;
+    A n_carry[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) n_carry[m] = zero_a;
+    auto index_sink = [&](int s, const A (&value)[K]) {
+        if constexpr (kGlass) {
+            const double w = v.omega[l];
+            const A slope[3] = {A(1.0), A(w), A(w) * A(w)};
+            for (int c = 0; c < 3; ++c) {
+                const int col = v.col_glass[s][c];
+                if (col < 0) continue;
+#pragma unroll
+                for (int m = 0; m < K; ++m)
+                    sinks.row[m][col * sinks.ld[m]] =
+                        YT(value_of(factor[m] * (value[m] * slope[c])));
+            }
+        }
+    };
     auto branch_of = [&](int s) {
         return s < 32 ? static_cast<int>((br_lo >> (2 * s)) & 3u)
                       : static_cast<int>((br_hi >> (2 * (s - 32))) & 3u);
@@ -671,6 +706,10 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
 #pragma unroll
                     for (int m = 0; m < K; ++m)
                         sinks.row[m][col * sinks.ld[m]] = YT(value_of(factor[m] * center_adj[m].z));
+                }
+                if constexpr (kGlass) {
+#pragma unroll
+                    for (int m = 0; m < K; ++m) n_carry[m] = n_image_adj[m];
                 }
             }
         } else {
@@ -726,9 +765,19 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                 if (ct >= 0)
                     sinks.row[m][ct * sinks.ld[m]] = YT(value_of(factor[m] * par[m].thickness));
             }
+            if constexpr (kGlass) {
+                A value[K];
+#pragma unroll
+                for (int m = 0; m < K; ++m) {
+                    value[m] = par[m].n_after + n_carry[m];
+                    n_carry[m] = par[m].n_before;
+                }
+                index_sink(j, value);
+            }
         }
         next_branch = branch_of(c);
     }
+    index_sink(0, n_carry);
 }
 
 // Mixed precision: the forward trace (OPL, piston, merit, the states the sweep is linearised
@@ -772,6 +821,11 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                                         br_lo, br_hi, count, image_branch,
                                                         reached_image, soft_mode, so, spn, sinks);
 }
+
+template <class T>
+struct TypeTag {
+    using type = T;
+};
 
 struct FusedArgs {
     AdjointParams ap;
@@ -1133,20 +1187,27 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
     const size_t smem = fused_adjoint_smem(
         tp, p_max, precision == MKB_PRECISION_MIXED ? sizeof(float) : sizeof(double));
-    // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
-    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0);
-    auto pick = [&](auto f0, auto f1, auto f2, auto f3) {
-        return feat == 0 ? f0 : feat == 1 ? f1 : feat == 2 ? f2 : f3;
+    // kernel variant per precision and features (1: surface transforms, 2: ghost plates,
+    // 4: glass variables of some run)
+    const bool glass = vp.has_glass != 0 || rv.any_glass != 0;
+    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0);
+    using Fn = void (*)(FusedArgs);
+    auto pick = [&](auto tag) -> Fn {
+        using N = typename decltype(tag)::type;
+        switch (feat) {
+        case 0: return adjoint_gram_kernel<N, 0>;
+        case 1: return adjoint_gram_kernel<N, 1>;
+        case 2: return adjoint_gram_kernel<N, 2>;
+        case 3: return adjoint_gram_kernel<N, 3>;
+        case 4: return adjoint_gram_kernel<N, 4>;
+        case 5: return adjoint_gram_kernel<N, 5>;
+        case 6: return adjoint_gram_kernel<N, 6>;
+        default: return adjoint_gram_kernel<N, 7>;
+        }
     };
-    auto kernel =
-        precision == MKB_PRECISION_FP64
-            ? pick(adjoint_gram_kernel<Exact64, 0>, adjoint_gram_kernel<Exact64, 1>,
-                   adjoint_gram_kernel<Exact64, 2>, adjoint_gram_kernel<Exact64, 3>)
-        : precision == MKB_PRECISION_MIXED
-            ? pick(adjoint_gram_kernel<MixedPrecision, 0>, adjoint_gram_kernel<MixedPrecision, 1>,
-                   adjoint_gram_kernel<MixedPrecision, 2>, adjoint_gram_kernel<MixedPrecision, 3>)
-            : pick(adjoint_gram_kernel<double, 0>, adjoint_gram_kernel<double, 1>,
-                   adjoint_gram_kernel<double, 2>, adjoint_gram_kernel<double, 3>);
+    const Fn kernel = precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
+                      : precision == MKB_PRECISION_MIXED ? pick(TypeTag<MixedPrecision>{})
+                                                         : pick(TypeTag<double>{});
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return cuda_status(err, "fused adjoint: shared memory attribute");

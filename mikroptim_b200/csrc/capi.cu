@@ -142,7 +142,7 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         return MKB_ERR_ARGUMENT;
     }
     const RecordLayout lay = record_layout(S, L, F, batch->non_coaxial, batch->ghost_plates,
-                                           batch->ghost_terms);
+                                           batch->ghost_terms, batch->glass ? 1 : 0);
     if (batch->record_stride != lay.stride) {
         set_error("record_stride %d does not match the shape (expected %d)",
                   batch->record_stride, lay.stride);
@@ -195,6 +195,7 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     p.non_coaxial = batch->non_coaxial;
     p.G = batch->ghost_plates;
     p.K = batch->ghost_terms;
+    p.glass = batch->glass ? 1 : 0;
     p.vsurf = batch->variant_surfaces;
     p.order = nullptr;
     p.L = L;
@@ -277,7 +278,7 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
 }
 
 int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out,
-                    int ghost_terms) {
+                    int ghost_terms, int L, const double* wavelength_nm, int glass) {
     if (vars == nullptr || vars->count < 1 || vars->count > MKB_MAX_VARIABLES) {
         set_error("variables: count must be in [1, %d]", MKB_MAX_VARIABLES);
         return MKB_ERR_ARGUMENT;
@@ -291,6 +292,8 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
     v.P = vars->count;
     for (int s = 0; s < kMaxSurfaces; ++s) v.col_curvature[s] = v.col_thickness[s] = -1;
     std::memset(v.col_ghost, -1, sizeof(v.col_ghost));
+    std::memset(v.col_glass, -1, sizeof(v.col_glass));
+    v.L = L;
     // table surface of every ghost plate (plates are numbered in table order)
     int plate_surface[kMaxGhostPlates];
     int plates = 0;
@@ -302,13 +305,27 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
         int s = vars->surface[k];
         if (t == MKB_VAR_WORKING_DISTANCE) s = S - 1;
         if (t != MKB_VAR_CURVATURE && t != MKB_VAR_THICKNESS && t != MKB_VAR_WORKING_DISTANCE &&
-            t != MKB_VAR_GHOST_COEFFICIENT) {
+            t != MKB_VAR_GHOST_COEFFICIENT && t != MKB_VAR_GLASS) {
             set_error("variable %d: unknown type %d (curvature, thickness, working distance, "
-                      "ghost coefficient)", k, t);
+                      "ghost coefficient, glass)", k, t);
             return MKB_ERR_UNSUPPORTED;
         }
         int8_t* slot;
-        if (t == MKB_VAR_GHOST_COEFFICIENT) {
+        if (t == MKB_VAR_GLASS) {
+            const int c = vars->glass_component ? vars->glass_component[k] : -1;
+            if (!glass || wavelength_nm == nullptr || L < 1 || L > MKB_MAX_WAVELENGTHS) {
+                set_error("variable %d: a glass variable needs the batch's Buchdahl "
+                          "coefficients and wavelengths", k);
+                return MKB_ERR_ARGUMENT;
+            }
+            if (s < 0 || s >= S || c < 0 || c > 2) {
+                set_error("variable %d: glass of surface %d, component %d out of range", k, s, c);
+                return MKB_ERR_ARGUMENT;
+            }
+            v.glass_component[k] = static_cast<int8_t>(c);
+            v.has_glass = 1;
+            slot = &v.col_glass[s][c];
+        } else if (t == MKB_VAR_GHOST_COEFFICIENT) {
             const int g = vars->ghost_plate ? vars->ghost_plate[k] : -1;
             const int order = vars->ghost_order ? vars->ghost_order[k] : 0;
             if (g < 0 || g >= plates || order < 1 || order > ghost_terms) {
@@ -350,6 +367,20 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
             return MKB_ERR_ARGUMENT;
         }
     }
+    if (v.has_glass) {
+        // Buchdahl coordinate w = dl / (1 + 2.5 dl), dl = lambda [um] - 0.546074 um
+        // (buchdahl_omega, glass/dispersion.hpp:87; nm_to_um divides by 1000)
+        for (int l = 0; l < L; ++l) {
+            const double dl = wavelength_nm[l] / 1000.0 - 0.546074;
+            const double den = 1.0 + 2.5 * dl;
+            if (!(den > 0.0)) {
+                set_error("glass variables: the Buchdahl coordinate of %g nm is undefined",
+                          wavelength_nm[l]);
+                return MKB_ERR_ARGUMENT;
+            }
+            v.omega[l] = dl / den;
+        }
+    }
     return MKB_OK;
 }
 
@@ -380,10 +411,12 @@ int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields)
 }
 
 int32_t mkb_record_stride_ext(int32_t surfaces, int32_t wavelengths, int32_t fields,
-                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms) {
+                              int32_t non_coaxial, int32_t ghost_plates, int32_t ghost_terms,
+                              int32_t glass) {
     return record_layout(surfaces, wavelengths, fields, non_coaxial ? 1 : 0,
                          ghost_plates > 0 ? ghost_plates : 0,
-                         ghost_plates > 0 && ghost_terms > 0 ? ghost_terms : 0).stride;
+                         ghost_plates > 0 && ghost_terms > 0 ? ghost_terms : 0,
+                         glass ? 1 : 0).stride;
 }
 
 int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
@@ -404,7 +437,8 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
         return MKB_ERR_ARGUMENT;
     }
     const int non_coaxial = v->decenter_tilt != nullptr ? 1 : 0;
-    const RecordLayout lay = record_layout(S, L, F, non_coaxial, G, K);
+    const int glass = v->buchdahl_coeff != nullptr ? 1 : 0;
+    const RecordLayout lay = record_layout(S, L, F, non_coaxial, G, K, glass);
     for (int64_t i = 0; i < v->variants; ++i) {
         double* r = records + i * lay.stride;
         std::memset(r, 0, sizeof(double) * lay.stride);
@@ -438,6 +472,9 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
             x[6] = moved ? 1.0 : 0.0;
             x[7] = 0.0;
         }
+        for (int s = 0; glass && s < S; ++s)
+            for (int c = 0; c < 4; ++c)
+                r[lay.glass + s * 4 + c] = v->buchdahl_coeff[(i * S + s) * 4 + c];
         for (int g = 0; g < G; ++g) {
             for (int k = 0; k < K; ++k)
                 r[lay.ghost_coeff + g * K + k] = v->ghost_coeff[(i * G + g) * K + k];
@@ -469,7 +506,8 @@ int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_vari
         return MKB_ERR_ARGUMENT;
     }
     const RecordLayout lay = record_layout(S, L, F, templates->non_coaxial != 0,
-                                           templates->ghost_plates, templates->ghost_terms);
+                                           templates->ghost_plates, templates->ghost_terms,
+                                           templates->glass ? 1 : 0);
     if (templates->record_stride != lay.stride ||
         (reinterpret_cast<uintptr_t>(records_out) & 15u) != 0) {
         set_error("apply: record stride %d (expected %d) or unaligned output",
@@ -477,7 +515,9 @@ int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_vari
         return MKB_ERR_ARGUMENT;
     }
     VarParams vp;
-    const int rc = make_var_params(vars, S, templates->type, &vp, templates->ghost_terms);
+    const int rc = make_var_params(vars, S, templates->type, &vp, templates->ghost_terms,
+                         templates->wavelengths, templates->wavelength_nm,
+                         templates->glass);
     if (rc != MKB_OK) return rc;
     return launch_apply(vp, lay, templates->records, templates->variants, x, records_out, runs,
                         static_cast<cudaStream_t>(stream));

@@ -43,10 +43,11 @@ struct RecordLayout {
     int xf;                                      // transforms, or -1 (coaxial)
     int ghost_coeff, ghost_radius, ghost_index;  // ghost plate data, or -1 (no plates)
     int ghost_terms;                             // K
+    int glass;                                   // Buchdahl coefficients [S][4], or -1
 };
 
 __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int non_coaxial = 0,
-                                                      int G = 0, int K = 0) {
+                                                      int G = 0, int K = 0, int glass = 0) {
     RecordLayout r;
     r.surfaces = S;
     r.curvature = 0;
@@ -69,6 +70,8 @@ __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int n
         r.ghost_index = n;
         n += G * L;
     }
+    r.glass = glass ? n : -1;
+    if (glass) n += S * 4;
     r.stride = (n + 1) & ~1;
     return r;
 }
@@ -85,6 +88,7 @@ struct TraceParams {
     int V, S, L, F;
     int non_coaxial;        // records carry per-surface transforms
     int G, K;               // ghost plates and their profile terms
+    int glass;              // records carry Buchdahl coefficients
     int stride;             // doubles per variant record
     int failure;            // MKB_FAILURE_*
     int rays;               // rays per variant
@@ -110,7 +114,7 @@ struct TraceParams {
 };
 
 __host__ __device__ inline RecordLayout layout_of(const TraceParams& p) {
-    return record_layout(p.S, p.L, p.F, p.non_coaxial, p.G, p.K);
+    return record_layout(p.S, p.L, p.F, p.non_coaxial, p.G, p.K, p.glass);
 }
 
 // Table surfaces variant v traces (uneven batches share the table of the largest; the value
@@ -588,13 +592,19 @@ struct VarParams {
     int8_t ghost_plate[MKB_MAX_VARIABLES];  // GhostCoefficient variables: plate g
     int8_t ghost_order[MKB_MAX_VARIABLES];  // and order k (1 .. K)
     int8_t col_ghost[kMaxGhostPlates][kMaxGhostTerms];  // column of a_{k+1} of plate g, or -1
+    int8_t glass_component[MKB_MAX_VARIABLES];  // Glass variables: 0 n0, 1 nu1, 2 nu2
+    int8_t col_glass[kMaxSurfaces][3];          // column of (n0, nu1, nu2) of medium s, or -1
+    int has_glass;                              // any Glass variable
+    int L;                                      // wavelengths (glass index refresh)
+    double omega[MKB_MAX_WAVELENGTHS];          // Buchdahl coordinate of every wavelength
     double lower[MKB_MAX_VARIABLES], upper[MKB_MAX_VARIABLES], typical[MKB_MAX_VARIABLES];
 };
 
 // Builds the variable block for a batch with S surfaces; MKB_OK or MKB_ERR_ARGUMENT.
 // ghost_terms: K of the batch (GhostCoefficient variables need k <= K).
 int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out,
-                    int ghost_terms = 0);
+                    int ghost_terms = 0, int L = 0, const double* wavelength_nm = nullptr,
+                    int glass = 0);
 
 // Writes x into a packed record (VariableSet::apply, src/optim/variable_set.cpp:237).
 // Writes variable k's value into a record (curvature, thickness / working distance, or a ghost
@@ -605,12 +615,32 @@ __device__ __forceinline__ void write_variable(const VarParams& v, const RecordL
     if (v.type[k] == MKB_VAR_CURVATURE) rec[lay.curvature + s] = x;
     else if (v.type[k] == MKB_VAR_GHOST_COEFFICIENT)
         rec[lay.ghost_coeff + v.ghost_plate[k] * lay.ghost_terms + v.ghost_order[k] - 1] = x;
+    else if (v.type[k] == MKB_VAR_GLASS) rec[lay.glass + s * 4 + v.glass_component[k]] = x;
     else rec[lay.thickness + s] = x;
+}
+
+// Recomputes the index of every medium with a glass variable from its Buchdahl coefficients,
+// n = n0 + w (nu1 + w (nu2 + w nu3)) with separately rounded operations (buchdahl_index,
+// glass/dispersion.hpp:93, as VariableSet::apply does on the host).
+__device__ __forceinline__ void refresh_glass(const VarParams& v, const RecordLayout& lay,
+                                              double* rec) {
+    if (!v.has_glass) return;
+    for (int s = 0; s < lay.surfaces; ++s) {
+        if (v.col_glass[s][0] < 0 && v.col_glass[s][1] < 0 && v.col_glass[s][2] < 0) continue;
+        const double* b = rec + lay.glass + s * 4;
+        for (int l = 0; l < v.L; ++l) {
+            const double w = v.omega[l];
+            const double inner = __dadd_rn(b[2], __dmul_rn(w, b[3]));
+            const double mid = __dadd_rn(b[1], __dmul_rn(w, inner));
+            rec[lay.index + s * v.L + l] = __dadd_rn(b[0], __dmul_rn(w, mid));
+        }
+    }
 }
 
 __device__ __forceinline__ void apply_variables(const VarParams& v, const RecordLayout& lay,
                                                 const double* x, double* rec) {
     for (int k = 0; k < v.P; ++k) write_variable(v, lay, k, x[k], rec);
+    refresh_glass(v, lay, rec);
 }
 
 // ---- launch bookkeeping (host) -------------------------------------------------------------

@@ -238,7 +238,9 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
     }
     VarParams vp{};
     if (rv.table == nullptr) {
-        rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms);
+        rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms,
+                             templates->wavelengths, templates->wavelength_nm,
+                             templates->glass);
         if (rc != MKB_OK) return rc;
     }
     if (!x0 || !J || !r0) {
@@ -346,14 +348,18 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
         return MKB_ERR_ARGUMENT;
     }
     VarParams vp;
-    rc = make_var_params(&vars[0], tp.S, templates->type, &vp, templates->ghost_terms);
+    rc = make_var_params(&vars[0], tp.S, templates->type, &vp, templates->ghost_terms,
+                         templates->wavelengths, templates->wavelength_nm,
+                         templates->glass);
     if (rc != MKB_OK) return rc;
     std::vector<VarParams> table;
     int pmax = vp.P;
     if (per_run) {
         table.resize(static_cast<size_t>(runs));
         for (int r = 0; r < runs; ++r) {
-            rc = make_var_params(&vars[r], tp.S, templates->type, &table[r], templates->ghost_terms);
+            rc = make_var_params(&vars[r], tp.S, templates->type, &table[r],
+                                 templates->ghost_terms, templates->wavelengths,
+                                 templates->wavelength_nm, templates->glass);
             if (rc != MKB_OK) return rc;
             pmax = table[r].P > pmax ? table[r].P : pmax;
         }
@@ -398,6 +404,7 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
         if (rc != MKB_OK) return rc;
         rv.table = dtable;
         rv.stride = pmax;
+        for (const VarParams& t : table) rv.any_glass |= t.has_glass;
     }
     const RecordLayout lay = layout_of(tp);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream,
@@ -475,7 +482,9 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
         return MKB_ERR_UNSUPPORTED;
     }
     VarParams vp;
-    rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms);
+    rc = make_var_params(vars, tp.S, templates->type, &vp, templates->ghost_terms,
+                         templates->wavelengths, templates->wavelength_nm,
+                         templates->glass);
     if (rc != MKB_OK) return rc;
     if (!x0 || !J || !r0 || !status) {
         set_error("adjoint jacobian: null pointer");

@@ -29,6 +29,7 @@ struct RunVars {
     int stride = 0;
     const uint8_t* tsurf = nullptr;
     uint8_t* vsurf_out = nullptr;
+    int any_glass = 0;  // some run of the table has glass variables
 };
 
 // trace.cu

@@ -481,6 +481,7 @@ struct LmSetup {
     LmOptionsDev o;
     bool fd, exact, gram_exact, fused;
     bool per_run;       // per-run variables
+    bool any_glass;     // some run has glass variables
     int pmax;           // P, or the largest P of the runs
     int precision;
     int64_t R;
@@ -582,15 +583,22 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     }
     const mkb_lm_options& o = *options;
     s.per_run = o.per_run_variables != 0;
-    rc = make_var_params(&vars[0], s.tp.S, templates->type, &s.vp, templates->ghost_terms);
+    rc = make_var_params(&vars[0], s.tp.S, templates->type, &s.vp, templates->ghost_terms,
+                         templates->wavelengths, templates->wavelength_nm,
+                         templates->glass);
     if (rc != MKB_OK) return rc;
     s.pmax = s.vp.P;
+    s.any_glass = s.vp.has_glass != 0;
     if (s.per_run) {
         if (table != nullptr) table->resize(static_cast<size_t>(runs));
         for (int r = 0; r < runs; ++r) {
             if (vars[r].count > s.pmax) s.pmax = vars[r].count;
+            for (int k = 0; k < vars[r].count; ++k)
+                if (vars[r].type[k] == MKB_VAR_GLASS) s.any_glass = true;
             if (table != nullptr) {
-                rc = make_var_params(&vars[r], s.tp.S, templates->type, &(*table)[r], templates->ghost_terms);
+                rc = make_var_params(&vars[r], s.tp.S, templates->type, &(*table)[r],
+                                     templates->ghost_terms, templates->wavelengths,
+                                     templates->wavelength_nm, templates->glass);
                 if (rc != MKB_OK) return rc;
             }
         }
@@ -645,6 +653,7 @@ RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* te
     rv.stride = s.pmax;
     rv.tsurf = templates->variant_surfaces;
     rv.vsurf_out = L.vsurf;
+    rv.any_glass = s.any_glass ? 1 : 0;
     return rv;
 }
 

@@ -52,9 +52,12 @@ class DeviceSystemBatch:
         self.non_coaxial = 1 if batch.non_coaxial else 0
         self.ghost_plates = batch.topology.ghost_plates
         self.ghost_terms = batch.topology.ghost_terms
+        self.glass = 1 if batch.buchdahl_coeff is not None else 0
+        self.wavelength_nm = np.ascontiguousarray(batch.wavelength_nm, dtype=np.float64)
         self.stride = int(lib.mkb_record_stride_ext(batch.surfaces, batch.wavelengths,
                                                     batch.fields, self.non_coaxial,
-                                                    self.ghost_plates, self.ghost_terms))
+                                                    self.ghost_plates, self.ghost_terms,
+                                                    self.glass))
         host = np.zeros((max(batch.variants, 1), self.stride))
         view = batch.view()
         _capi.check(lib.mkb_pack_batch_host(C.byref(view), _capi.ptr(host)), "pack batch")
@@ -81,9 +84,11 @@ class DeviceSystemBatch:
         b.non_coaxial = self.non_coaxial
         b.ghost_plates = self.ghost_plates
         b.ghost_terms = self.ghost_terms
+        b.glass = self.glass
+        b.wavelength_nm = _capi.ptr(self.wavelength_nm)
         b.records = C.c_void_p(self.records.data_ptr() + first * self.stride * 8)
         b.type = _capi.ptr(self.type, C.c_uint8)
-        b._keep = self.type
+        b._keep = (self.type, self.wavelength_nm)
         b.variant_surfaces = (C.c_void_p(self.variant_surfaces.data_ptr() + first)
                               if self.variant_surfaces is not None else None)
         return b

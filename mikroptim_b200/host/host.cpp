@@ -81,6 +81,27 @@ SystemBatchHost::SystemBatchHost(BatchTopology topology, int variants)
     ghost_coeff_.assign(V * G * K, 0.0);
     ghost_index_.assign(V * G * L, 1.0);
     ghost_norm_radius_.assign(G, 1.0);
+    buchdahl_coeff_.assign(V * S * 4, 0.0);
+    wavelength_nm.assign(L, 0.0);
+}
+
+double& SystemBatchHost::buchdahl_coeff(int v, int s, int j) {
+    if (j < 0 || j >= 4) throw std::out_of_range("SystemBatchHost: Buchdahl coefficient");
+    return buchdahl_coeff_.at(index2(v, s, surfaces()) * 4 + j);
+}
+
+double SystemBatchHost::buchdahl_coeff(int v, int s, int j) const {
+    if (j < 0 || j >= 4) throw std::out_of_range("SystemBatchHost: Buchdahl coefficient");
+    return buchdahl_coeff_.at(index2(v, s, surfaces()) * 4 + j);
+}
+
+void SystemBatchHost::refresh_glass_index(int v, int s) {
+    const double* b = buchdahl_coeff_.data() + index2(v, s, surfaces()) * 4;
+    for (int l = 0; l < wavelengths(); ++l) {
+        const double dl = wavelength_nm.at(static_cast<size_t>(l)) / 1000.0 - 0.546074;
+        const double w = dl / (1.0 + 2.5 * dl);
+        index(v, s, l) = b[0] + w * (b[1] + w * (b[2] + w * b[3]));
+    }
 }
 
 double& SystemBatchHost::ghost_coeff(int v, int g, int k) {
@@ -154,6 +175,9 @@ SystemBatchHost take_variants(const SystemBatchHost& batch, const std::vector<in
     if (!batch.decenter_tilt_.empty()) copy(batch.decenter_tilt_, out.decenter_tilt_, S * 4);
     copy(batch.ghost_coeff_, out.ghost_coeff_, G * K);
     copy(batch.ghost_index_, out.ghost_index_, G * L);
+    copy(batch.buchdahl_coeff_, out.buchdahl_coeff_, S * 4);
+    out.wavelength_nm = batch.wavelength_nm;
+    out.glass = batch.glass;
     return out;
 }
 
@@ -256,6 +280,12 @@ mkb_batch_view SystemBatchHost::view() const {
     v.field_angle = field_angle_.data();
     v.field_target = field_target_.data();
     v.decenter_tilt = topology_.non_coaxial ? decenter_tilt_.data() : nullptr;
+    if (glass) {
+        if (static_cast<int>(wavelength_nm.size()) != wavelengths())
+            throw std::invalid_argument("SystemBatchHost: wavelength_nm does not match");
+        v.buchdahl_coeff = buchdahl_coeff_.data();
+        v.wavelength_nm = wavelength_nm.data();
+    }
     v.ghost_plates = topology_.ghost_plates;
     v.ghost_terms = topology_.ghost_terms;
     if (topology_.ghost_plates > 0) {
@@ -346,6 +376,9 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
                 throw std::invalid_argument("VariableSet: thickness surface out of range");
         } else if (v.type == VariableType::WorkingDistance) {
             v.surface = S - 1;
+        } else if (v.type == VariableType::Glass) {
+            if (v.surface < 0 || v.surface >= S || v.glass_component < 0 || v.glass_component > 2)
+                throw std::invalid_argument("VariableSet: glass variable out of range");
         } else if (v.type == VariableType::GhostCoefficient) {
             if (v.ghost_plate < 0 || v.ghost_plate >= topology.ghost_plates ||
                 v.ghost_order < 1 || v.ghost_order > topology.ghost_terms)
@@ -359,6 +392,8 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
         const std::pair<int, int> key =
             v.type == VariableType::GhostCoefficient
                 ? std::pair<int, int>{2 + v.ghost_plate, v.ghost_order}
+            : v.type == VariableType::Glass
+                ? std::pair<int, int>{100 + v.surface, v.glass_component}
                 : std::pair<int, int>{v.type == VariableType::Curvature ? 1 : 0, v.surface};
         if (!seen.insert(key).second)
             throw std::invalid_argument("VariableSet: parameter already used by a variable");
@@ -370,6 +405,7 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
         surface_.push_back(v.surface);
         ghost_plate_.push_back(v.ghost_plate);
         ghost_order_.push_back(v.ghost_order);
+        glass_component_.push_back(v.glass_component);
         lower_.push_back(v.lower);
         upper_.push_back(v.upper);
         typical_.push_back(v.typical);
@@ -380,6 +416,8 @@ std::vector<double> VariableSet::extract(const SystemBatchHost& batch, int v) co
     std::vector<double> x;
     for (const Variable& var : variables_)
         x.push_back(var.type == VariableType::Curvature ? batch.curvature(v, var.surface)
+                    : var.type == VariableType::Glass
+                        ? batch.buchdahl_coeff(v, var.surface, var.glass_component)
                     : var.type == VariableType::GhostCoefficient
                         ? const_cast<SystemBatchHost&>(batch).ghost_coeff(v, var.ghost_plate,
                                                                           var.ghost_order - 1)
@@ -393,8 +431,14 @@ void VariableSet::apply(SystemBatchHost& batch, int v, const double* x) const {
         if (var.type == VariableType::Curvature) batch.curvature(v, var.surface) = x[k];
         else if (var.type == VariableType::GhostCoefficient)
             batch.ghost_coeff(v, var.ghost_plate, var.ghost_order - 1) = x[k];
+        else if (var.type == VariableType::Glass)
+            batch.buchdahl_coeff(v, var.surface, var.glass_component) = x[k];
         else batch.thickness(v, var.surface) = x[k];
     }
+    std::set<int> glass_surfaces;
+    for (const Variable& var : variables_)
+        if (var.type == VariableType::Glass) glass_surfaces.insert(var.surface);
+    for (int gs : glass_surfaces) batch.refresh_glass_index(v, gs);
 }
 
 mkb_variables VariableSet::c_struct() const {
@@ -407,6 +451,7 @@ mkb_variables VariableSet::c_struct() const {
     c.typical = typical_.data();
     c.ghost_plate = ghost_plate_.data();
     c.ghost_order = ghost_order_.data();
+    c.glass_component = glass_component_.data();
     return c;
 }
 
@@ -487,9 +532,11 @@ void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     batch.validate_values();
     const mkb_batch_view view = batch.view();
     const int32_t non_coaxial = view.decenter_tilt != nullptr ? 1 : 0;
+    const int32_t glass = view.buchdahl_coeff != nullptr ? 1 : 0;
     const int32_t stride = mkb_record_stride_ext(view.surfaces, view.wavelengths, view.fields,
                                                  non_coaxial, view.ghost_plates,
-                                                 view.ghost_terms);
+                                                 view.ghost_terms, glass);
+    wavelength_nm_.assign(batch.wavelength_nm.begin(), batch.wavelength_nm.end());
     host_records_.assign(static_cast<size_t>(view.variants) * stride, 0.0);
     check(mkb_pack_batch_host(&view, host_records_.data()), "pack batch");
     void* d = cuda::upload(records_, host_records_, stream);
@@ -502,6 +549,8 @@ void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
     batch_.non_coaxial = non_coaxial;
     batch_.ghost_plates = view.ghost_plates;
     batch_.ghost_terms = view.ghost_terms;
+    batch_.glass = glass;
+    batch_.wavelength_nm = wavelength_nm_.data();
     batch_.records = static_cast<const double*>(d);
     batch_.type = type_.data();
 }

@@ -31,7 +31,7 @@ enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
 enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
 enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2 };
 enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2,
-                                    GhostCoefficient = 3 };
+                                    GhostCoefficient = 3, Glass = 4 };
 enum class JacobianMethod : int32_t { FiniteDifference = 0, Adjoint = 1 };
 enum class LmStatus : int32_t {
     Running = 0, ConvergedMerit = 1, ConvergedStep = 2, ConvergedGradient = 3,
@@ -83,8 +83,16 @@ public:
     double& ghost_index(int v, int g, int l);
     double& ghost_norm_radius(int g);
     int ghost_surface(int g) const;
+    // Buchdahl coefficients (n0, nu1, nu2, nu3) of the medium after surface s (j = 0..3); set
+    // `glass` to pass them (and wavelength_nm) to the device for glass variables
+    double& buchdahl_coeff(int v, int s, int j);
+    double buchdahl_coeff(int v, int s, int j) const;
+    // index[v][s][:] from the Buchdahl coefficients (buchdahl_index, glass/dispersion.hpp:93)
+    void refresh_glass_index(int v, int s);
 
     double reference_wavelength_nm = 0.0;
+    std::vector<double> wavelength_nm;      // [L] (glass variables)
+    bool glass = false;                     // the batch carries Buchdahl coefficients
     std::vector<double> wavelength_weight;  // [L]
     std::vector<double> field_weight;       // [F]
 
@@ -100,7 +108,8 @@ private:
     int variants_;
     std::vector<uint8_t> type_;
     std::vector<double> curvature_, thickness_, index_, pupil_radius_, field_angle_,
-        field_target_, decenter_tilt_, ghost_coeff_, ghost_index_, ghost_norm_radius_;
+        field_target_, decenter_tilt_, ghost_coeff_, ghost_index_, ghost_norm_radius_,
+        buchdahl_coeff_;
     friend SystemBatchHost make_non_coaxial(const SystemBatchHost& batch);
     friend SystemBatchHost take_variants(const SystemBatchHost& batch,
                                          const std::vector<int>& variants);
@@ -164,6 +173,7 @@ struct Variable {
     double typical = 1.0;
     int ghost_plate = -1;  // GhostCoefficient: a_{ghost_order} of plate ghost_plate
     int ghost_order = 0;
+    int glass_component = -1;  // Glass: 0 n0, 1 nu1, 2 nu2 of the medium after `surface`
 };
 
 class VariableSet {
@@ -177,7 +187,7 @@ public:
 
 private:
     std::vector<Variable> variables_;
-    std::vector<int32_t> type_, surface_, ghost_plate_, ghost_order_;
+    std::vector<int32_t> type_, surface_, ghost_plate_, ghost_order_, glass_component_;
     std::vector<double> lower_, upper_, typical_;
 };
 
@@ -249,6 +259,7 @@ public:
 private:
     mkb_device_batch batch_{};
     std::vector<uint8_t> type_;
+    std::vector<double> wavelength_nm_;
     std::vector<double> host_records_;
     DeviceBuffer records_;
 };

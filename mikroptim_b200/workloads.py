@@ -183,8 +183,14 @@ def sellmeier_fit(nd, vd):
 
 def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
               spokes: int = 32, na: float = 0.95, max_field_deg: float = 1.0,
-              failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
-    """Configuration 2. Returns (batch, settings, variables, x0 [V][P])."""
+              failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64,
+              glass: bool = False):
+    """Configuration 2. Returns (batch, settings, variables, x0 [V][P]).
+
+    glass=True: the first element's glass becomes a Buchdahl glass (n0 = its n_d, nu1 =
+    -0.12, nu2 = 0.03, nu3 = 0; index = n0 + w (nu1 + w (nu2 + w nu3)) at every wavelength)
+    and its three Buchdahl coordinates join the variables (P = 32, the configuration-2 count),
+    with the reference's typical sizes (1, 0.01, 0.001) and no bounds."""
     S = 15
     topo = BatchTopology(surfaces=S, wavelengths=7, fields=5,
                          type=[SURFACE_STOP] + [SURFACE_SPHERE] * 14,
@@ -241,6 +247,19 @@ def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
     variables = [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, S)]
     variables += [Variable(VAR_THICKNESS, s, 0.05, 50.0, 1.0) for s in range(0, S - 1)]
     variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1000.0, 1.0)]
+    if glass:
+        from .batch import VAR_GLASS
+        b.buchdahl_coeff = np.zeros((variants, S, 4))
+        nd = sellmeier_index(*[a[:, 0] for a in sellmeier_fit(
+            1.45 + 0.45 * rng.uniform(104, variants * 7).reshape(variants, 7)[:, :1],
+            25.0 + 70.0 * rng.uniform(105, variants * 7).reshape(variants, 7)[:, :1])], 587.56)
+        b.buchdahl_coeff[:, 1, 0] = nd
+        b.buchdahl_coeff[:, 1, 1] = -0.12
+        b.buchdahl_coeff[:, 1, 2] = 0.03
+        for v in range(variants):
+            b.refresh_glass_index(v, 1)
+        variables += [Variable(VAR_GLASS, 1, -math.inf, math.inf, typ, component=c)
+                      for c, typ in enumerate((1.0, 0.01, 0.001))]
     vs = VariableSet(topo, variables)
     x0 = np.stack([vs.extract(b, v) for v in range(variants)])
     return b, settings, vs, x0

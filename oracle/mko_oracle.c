@@ -658,7 +658,15 @@ static int check_vars(const mkb_batch_view* v, const mkb_variables* vars) {
 typedef struct {
     double c[MKB_MAX_SURFACES], t[MKB_MAX_SURFACES];
     double g[MKB_MAX_GHOST_PLATES * MKB_MAX_GHOST_TERMS];
+    double n[MKB_MAX_SURFACES * MKB_MAX_WAVELENGTHS];  /* index, rewritten by glass variables */
+    double b[MKB_MAX_SURFACES * 4];                      /* Buchdahl coefficients */
 } params_t;
+
+/* buchdahl_omega, glass/dispersion.hpp:87 (nm_to_um divides by 1000) */
+static double buchdahl_omega_nm(double nm) {
+    const double dl = nm / 1000.0 - 0.546074;
+    return dl / (1.0 + 2.5 * dl);
+}
 
 static void apply_x(const mkb_batch_view* view, int src, const mkb_variables* vars,
                     const double* x, params_t* out) {
@@ -666,11 +674,29 @@ static void apply_x(const mkb_batch_view* view, int src, const mkb_variables* va
     memcpy(out->c, view->curvature + (size_t)src * S, sizeof(double) * S);
     memcpy(out->t, view->thickness + (size_t)src * S, sizeof(double) * S);
     if (GK > 0) memcpy(out->g, view->ghost_coeff + (size_t)src * GK, sizeof(double) * GK);
+    const int L = view->wavelengths;
+    memcpy(out->n, view->index + (size_t)src * S * L, sizeof(double) * S * L);
+    if (view->buchdahl_coeff)
+        memcpy(out->b, view->buchdahl_coeff + (size_t)src * S * 4, sizeof(double) * S * 4);
+    int glass_surface[MKB_MAX_SURFACES] = {0};
     for (int k = 0; k < vars->count; ++k) {
         if (vars->type[k] == MKB_VAR_CURVATURE) out->c[vars->surface[k]] = x[k];
         else if (vars->type[k] == MKB_VAR_GHOST_COEFFICIENT)
             out->g[vars->ghost_plate[k] * view->ghost_terms + vars->ghost_order[k] - 1] = x[k];
-        else out->t[vars->surface[k]] = x[k];
+        else if (vars->type[k] == MKB_VAR_GLASS) {
+            out->b[vars->surface[k] * 4 + vars->glass_component[k]] = x[k];
+            glass_surface[vars->surface[k]] = 1;
+        } else out->t[vars->surface[k]] = x[k];
+    }
+    /* the media of the glass variables: n = n0 + w (nu1 + w (nu2 + w nu3)) (VariableSet::apply,
+       src/optim/variable_set.cpp:268, buchdahl_index, glass/dispersion.hpp:93) */
+    for (int s = 0; s < S; ++s) {
+        if (!glass_surface[s]) continue;
+        const double* b = out->b + s * 4;
+        for (int l = 0; l < L; ++l) {
+            const double w = buchdahl_omega_nm(view->wavelength_nm[l]);
+            out->n[s * L + l] = b[0] + w * (b[1] + w * (b[2] + w * b[3]));
+        }
     }
 }
 
@@ -678,6 +704,7 @@ static table_t table_with(const mkb_batch_view* v, int var, const params_t* p) {
     table_t t = table_of(v, var);
     t.c = p->c;
     t.t = p->t;
+    t.n = p->n;
     if (t.G > 0) t.gcoeff = p->g;
     return t;
 }
@@ -1086,6 +1113,9 @@ struct writer_s {
     int curvature[MKB_MAX_SURFACES];
     int thickness[MKB_MAX_SURFACES];
     int ghost[MKB_MAX_GHOST_PLATES * MKB_MAX_GHOST_TERMS];  /* ghost_coeff[g][k] */
+    int glass[MKB_MAX_SURFACES * 3];                       /* (n0, nu1, nu2) of medium s */
+    double slope[MKB_MAX_WAVELENGTHS * 3];                 /* (1, w_l, w_l^2) */
+    int wavelength;
     double* column0;
     int64_t rows, row;
     double factor;
@@ -1093,6 +1123,13 @@ struct writer_s {
 
 static void w_write(const writer_t* w, int p, double value) {
     if (p >= 0) w->column0[(int64_t)p * w->rows + w->row] = w->factor * value;
+}
+
+/* AdjointRowWriter::index (merit/ray_jacobian.hpp:66): the index adjoint of medium s to the
+ * glass columns with dn/d(n0, nu1, nu2) = (1, w, w^2) at the ray's wavelength */
+static void w_index(const writer_t* w, int s, double value) {
+    for (int c = 0; c < 3; ++c)
+        if (w->glass[s * 3 + c] >= 0) w_write(w, w->glass[s * 3 + c], value * w->slope[w->wavelength * 3 + c]);
 }
 
 /* backward_ray, adjoint_backward.hpp:495 (coaxial, LastSurface reference, collimated). */
@@ -1156,11 +1193,12 @@ static void backward_ray(const table_t* sys, int l, const record_t* rec, int rea
             }
             if (kind == MKB_SURFACE_SPHERE) w_write(w, w->curvature[j], par.curvature);
             w_write(w, w->thickness[s], par.thickness);
-            (void)n_carry; /* index sinks: no glass variables in this build */
+            w_index(w, j, par.n_after + n_carry);
             n_carry = par.n_before;
         }
         next_branch = rec->branch[s];
     }
+    w_index(w, 0, n_carry);
 }
 
 typedef struct {
@@ -1207,10 +1245,19 @@ static void adjoint_item(void* pctx, int i) {
         if (vars->type[k] == MKB_VAR_CURVATURE) w.curvature[vars->surface[k]] = k;
         else if (vars->type[k] == MKB_VAR_GHOST_COEFFICIENT)
             w.ghost[vars->ghost_plate[k] * view->ghost_terms + vars->ghost_order[k] - 1] = k;
-        else w.thickness[vars->surface[k]] = k;
+        else if (vars->type[k] != MKB_VAR_GLASS) w.thickness[vars->surface[k]] = k;
     }
     w.column0 = J + (size_t)i * P * R;
     w.rows = R;
+    for (int g = 0; g < MKB_MAX_SURFACES * 3; ++g) w.glass[g] = -1;
+    for (int k = 0; k < P; ++k)
+        if (vars->type[k] == MKB_VAR_GLASS) w.glass[vars->surface[k] * 3 + vars->glass_component[k]] = k;
+    for (int l = 0; l < view->wavelengths; ++l) {
+        const double om = view->wavelength_nm ? buchdahl_omega_nm(view->wavelength_nm[l]) : 0.0;
+        w.slope[l * 3 + 0] = 1.0;
+        w.slope[l * 3 + 1] = om;
+        w.slope[l * 3 + 2] = om * om;
+    }
     record_t* rec = (record_t*)malloc(sizeof(record_t));
     double weight[MKB_MAX_RINGS * MKB_MAX_SPOKES], rootw[MKB_MAX_RINGS * MKB_MAX_SPOKES];
     unsigned char piston[MKB_MAX_RINGS * MKB_MAX_SPOKES];
@@ -1221,6 +1268,7 @@ static void adjoint_item(void* pctx, int i) {
         const double a = view->pupil_radius[tmpl];
         const double theta = view->field_angle[(size_t)tmpl * view->fields + f];
         for (int l = 0; l < plan->wavelengths; ++l) {
+            w.wavelength = l;
             const int64_t offset = tuple_offset(plan, f, l);
             const double scale = residual_scale(plan, f, l);
             const double pscale = soft_mode ? penalty_scale(plan, f, l) : 0.0;

@@ -101,6 +101,14 @@ mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_p
                         v.decenter_tilt[(static_cast<std::size_t>(i) * S + s) * 4 + k];
     }
     for (int g = 0; g < v.ghost_plates; ++g) b.ghost_norm_radius(g) = v.ghost_norm_radius[g];
+    if (v.buchdahl_coeff != nullptr) {
+        for (int l = 0; l < L; ++l) b.wavelength_nm(l) = v.wavelength_nm[l];
+        for (int i = 0; i < v.variants; ++i)
+            for (int s = 0; s < S; ++s)
+                for (int j = 0; j < 4; ++j)
+                    b.buchdahl_coeff(i, s, j) =
+                        v.buchdahl_coeff[(static_cast<std::size_t>(i) * S + s) * 4 + j];
+    }
     return b;
 }
 
@@ -163,7 +171,14 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
         }
         surf.thickness = gap;
         const double n = b.index(0, s, 0);
-        if (n == 1.0) {
+        bool glass_var = false;
+        for (int k = 0; k < vars.count; ++k)
+            glass_var = glass_var || (vars.type[k] == MKB_VAR_GLASS && vars.surface[k] == s);
+        if (glass_var) {  // Buchdahl glass (the material of a glass variable)
+            surf.material.kind = mko::MaterialKind::Buchdahl;
+            surf.material.n0 = b.buchdahl_coeff(0, s, 0);
+            for (int j = 0; j < 3; ++j) surf.material.nu[j] = b.buchdahl_coeff(0, s, j + 1);
+        } else if (n == 1.0) {
             surf.material.kind = mko::MaterialKind::Air;
         } else {
             surf.material.kind = mko::MaterialKind::Constant;
@@ -188,6 +203,19 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
             spec.selection = mko::SurfaceSelection::One;
             spec.surfaces = {file_of_table[s]};
             d.surfaces[file_of_table[s]].thickness = x0[k];
+        } else if (vars.type[k] == MKB_VAR_GLASS) {
+            // one item for the three components n0, nu1, nu2 (listed in that order, no bounds,
+            // the reference's typical sizes)
+            if (vars.glass_component[k] != 0) continue;
+            spec.type = mko::VariableType::Glass;
+            spec.selection = mko::SurfaceSelection::One;
+            spec.surfaces = {file_of_table[s]};
+            auto& mat = d.surfaces[file_of_table[s]].material;
+            mat.n0 = x0[k];
+            mat.nu[0] = x0[k + 1];
+            mat.nu[1] = x0[k + 2];
+            items.items.push_back(spec);
+            continue;
         } else if (vars.type[k] == MKB_VAR_GHOST_COEFFICIENT) {
             spec.type = mko::VariableType::GhostCoefficient;
             spec.selection = mko::SurfaceSelection::None;

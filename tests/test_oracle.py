@@ -241,3 +241,21 @@ def test_subset_owns_its_arrays():
     sub.ghost_coeff[0, 0, 0] += 1.0
     assert b.curvature[0, 1] != sub.curvature[0, 1]
     assert b.ghost_coeff[0, 0, 0] != sub.ghost_coeff[0, 0, 0]
+
+
+@pytest.mark.skipif(not has_reference_build(), reason="reference CPU build not present")
+def test_port_matches_reference_with_glass_variables():
+    """Glass variables (Buchdahl n0, nu1, nu2 of the medium after a surface; the reference's
+    VariableType::Glass): applying x recomputes that medium's index at every wavelength, and the
+    adjoint carries each medium's index adjoint into its glass columns with (1, w, w^2).
+    Restatement and reference agree bit for bit on the adjoint and the FD Jacobians."""
+    b, st, vs, x0 = workloads.objective(4, rings=3, spokes=6, glass=True)
+    assert vs.size == 32
+    lay = ResidualLayout(b.topology, st)
+    P, R = po.port(), po.reference()
+    two = b.subset(0, 2)
+    for a, c in zip(P.adjoint_jacobian(two, lay, vs, x0[:2]),
+                    R.adjoint_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
+    for a, c in zip(P.fd_jacobian(two, lay, vs, x0[:2]), R.fd_jacobian(two, lay, vs, x0[:2])):
+        assert np.array_equal(a, c)
