@@ -106,6 +106,7 @@ __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayo
             const FdPattern& p = pat[static_cast<int64_t>(run) * pstride + k];
             const double y = (j & 1) ? p.xa : p.xb;
             write_variable(v, lay, k, y, dst);
+            refresh_glass(v, lay, dst);  // a perturbed Buchdahl coefficient moves the index
         }
     }
 }
