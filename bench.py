@@ -48,6 +48,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "LM iter/s & ray-surface hits/s: adjoint+mixed vs FP64 FD, at ≤1e-4λ OPD err"
 WORKLOAD = "objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=29 (config 2 shape)"
+WORKLOAD_LM = ("objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=32: 14 "
+               "curvatures, 15 thicknesses and the first element's Buchdahl glass (n0, nu1, nu2) "
+               "(config 2 shape)")
 FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of the reference)
 # DRAM traffic of trace_kernel per variant from the ncu capture summarised in
 # profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
@@ -57,8 +60,8 @@ TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
 # scaled by the runs of the launch.
 FUSED_TRAFFIC_BYTES_PER_RUN = (1.669274e9 + 18.593394e9) / 1184
 # The same for the uneven (config-3) runs, MIXED precision, both launches of the call, from
-# profiles/adjoint_gram_uneven1184.md (1,184 runs: 1.992 GB read, 19.288 GB written).
-FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (1.599339e9 + 0.392692e9 + 11.698874e9 + 7.588631e9) / 1184
+# profiles/adjoint_gram_uneven1184.md (1,184 runs: 22.6 MB read, 1.822 GB written).
+FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (19.521536e6 + 3.077120e6 + 1.344401e9 + 0.477131e9) / 1184
 
 
 def parse():
@@ -375,7 +378,7 @@ def run_lm(args, world, rank, local):
     dev = torch.device("cuda", local)
     lib = _capi.lib()
     b, st, vs, x0 = workloads.objective(args.variants or 4096,
-                                        seed=20261203 + 2 + 1000 * rank)
+                                        seed=20261203 + 2 + 1000 * rank, glass=True)
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
     runs = b.variants
@@ -426,19 +429,28 @@ def run_lm(args, world, rank, local):
     fd_value = fd_iters / (fd_ms * fd_steps / 1e3)
     del fd
 
-    # ---- the dominant kernel alone: fused adjoint + normal equations at the current points ----
-    engine.adjoint_normal_equations_device(db, lay, b, vs, x_np)
+    # ---- the dominant kernel alone: fused adjoint + normal equations at the current points.
+    # The call's host part is enqueued while the previous call runs: the first call is outside
+    # the events, so they see the GPU work only; the L2 flush between calls is taken out.
+    x_dev = x_now.clone()
+    engine.adjoint_normal_equations_device(db, lay, b, vs, x_dev)
     torch.cuda.synchronize()
-    kt = []
-    for _ in range(3):
+    reps = 3
+    engine.adjoint_normal_equations_device(db, lay, b, vs, x_dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
         flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        engine.adjoint_normal_equations_device(db, lay, b, vs, x_np)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        kt.append(e0.elapsed_time(e1))
-    kernel_ms = min(kt)
+        engine.adjoint_normal_equations_device(db, lay, b, vs, x_dev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(reps):
+        flush.zero_()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    kernel_ms = (e0.elapsed_time(e1) - f0.elapsed_time(f1)) / reps
     # FLOP model (reference cost model): adjoint = 3 x FLOPeq(ray), FLOPeq = 140 (S_steps + 2),
     # plus 4 P per ray (projection) and 2 P^2 per row (rows: rays and penalty rows)
     flop = rays * (3 * FLOPEQ_PER_RAY_SURFACE * (steps_per_ray + 2) + 4 * P) + \
@@ -496,7 +508,8 @@ def run_lm(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generator, configuration-2 shapes)",
-        "config": {"workload": WORKLOAD, "step": "one batched LM cycle of all runs (CUDA graph)",
+        "config": {"workload": WORKLOAD_LM,
+                   "step": "one batched LM cycle of all runs (CUDA graph)",
                    "runs_per_gpu": runs, "variables": P, "rays_per_run": lay.rays_per_variant,
                    "jacobian": "adjoint fused with FP64 tensor-core normal equations",
                    "precision": "FP64 with FMA contraction",
@@ -733,7 +746,7 @@ def cpu_baseline_lm(kind: str, runs: int = 256, seed: int = 20261203 + 2):
     import oracle.pyoracle as po
     from mikroptim_b200 import workloads
     from mikroptim_b200.batch import ResidualLayout
-    b, st, vs, x0 = workloads.objective(4096, seed=seed)
+    b, st, vs, x0 = workloads.objective(4096, seed=seed, glass=True)
     b = b.subset(0, runs)
     lay = ResidualLayout(b.topology, st)
     threads = os.cpu_count() or 1
@@ -824,7 +837,8 @@ def run_reference(args, world, rank):
             "n_gpus": world, "steps": len(samples), "warmup": 0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, configuration-2 shapes)",
-            "config": {"workload": WORKLOAD, "step": "one LM cycle of a 128-run sample on the host"},
+            "config": {"workload": WORKLOAD_LM,
+                       "step": "one LM cycle of a 128-run sample on the host"},
             "cpu_baseline": {"value": v, "unit": "LM run-iterations/s", "cores": base["cores"],
                              "kind": kind, "sample": base["sample"]},
             "e2e": {"value": v, "unit": "LM run-iterations/s", "h2d_bytes_per_step": 0,

@@ -196,6 +196,14 @@ def _dev_f64(a, device):
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(device)
 
 
+def _x_rows(x0, P: int, device):
+    """Variable rows [runs][P] on the device: a device tensor is used in place (no copy when
+    it is already contiguous FP64), host arrays are copied."""
+    if isinstance(x0, torch.Tensor):
+        return x0.to(device=device, dtype=torch.float64).reshape(-1, P).contiguous()
+    return _dev_f64(np.asarray(x0).reshape(-1, P), device)
+
+
 def fd_jacobian_device(templates: DeviceSystemBatch, layout: ResidualLayout,
                        host: SystemBatchHost, variables, x0, chunk_runs: int | None = None,
                        stream=None):
@@ -203,7 +211,7 @@ def fd_jacobian_device(templates: DeviceSystemBatch, layout: ResidualLayout,
     Returns device tensors J [runs][P][R], r0 [runs][R], status_changes [runs][P]."""
     lib = _capi.lib()
     dev = templates.device
-    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    x0 = _x_rows(x0, variables.size, dev)
     runs, P = x0.shape
     R = layout.trace_rows
     b = templates.c_struct()
@@ -229,7 +237,7 @@ def adjoint_jacobian_device(templates: DeviceSystemBatch, layout: ResidualLayout
     Returns device tensors J [runs][P][R], r0 [runs][R], status [runs][rays]."""
     lib = _capi.lib()
     dev = templates.device
-    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    x0 = _x_rows(x0, variables.size, dev)
     runs, P = x0.shape
     R = layout.trace_rows
     b = templates.c_struct()
@@ -522,7 +530,7 @@ def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: Residu
     """Fused adjoint + normal equations (FP64_FMA, DMMA): gram [runs][P+1][P+1]."""
     lib = _capi.lib()
     dev = templates.device
-    x0 = _dev_f64(np.asarray(x0).reshape(-1, variables.size), dev)
+    x0 = _x_rows(x0, variables.size, dev)
     runs, P = x0.shape
     b = templates.c_struct()
     plan = layout.plan(host)

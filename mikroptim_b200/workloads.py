@@ -246,7 +246,7 @@ def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
     settings = ResidualSettings(rings=rings, spokes=spokes, failure=failure, precision=precision)
     variables = [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, S)]
     variables += [Variable(VAR_THICKNESS, s, 0.05, 50.0, 1.0) for s in range(0, S - 1)]
-    variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1000.0, 1.0)]
+    variables += [Variable(VAR_WORKING_DISTANCE, S - 1, 0.1, 1.0e4, 1.0)]
     if glass:
         from .batch import VAR_GLASS
         b.buchdahl_coeff = np.zeros((variants, S, 4))
