@@ -214,6 +214,54 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
                      double* merit, int64_t* failed, int64_t* hard_failed,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* Per-run options of the trace (TraceSettings::pack_rays and ::extra_merit,
+ * include/mikroptim/cuda/trace_engine.hpp:58).
+ *   pack_rays    the largest pack of consecutive tuples one CTA traces, in rays; 0 = 512.
+ *                Runtime only: every value gives bit-identical results (a tuple with more rays
+ *                gets a pack of its own; values above 4096 are traced as 4096).
+ *   extra_merit  MERIT only: device [V] or NULL; extra_merit[v] is added to variant v's merit
+ *                after its tuple sums (MeritRunOptions::extra_merit, src/cuda/merit.cu:222). */
+typedef struct mkb_trace_options {
+    int32_t pack_rays;
+    int32_t reserved;                 /* 0                                               */
+    const double* extra_merit;
+} mkb_trace_options;
+
+/* mkb_residuals_device / mkb_merit_device with options (NULL = the defaults). */
+int mkb_residuals_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                            const mkb_trace_options* options, double* residuals, int64_t stride,
+                            double* opd, uint8_t* status, void* stream);
+int mkb_merit_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                        const mkb_trace_options* options, double* merit, int64_t* failed,
+                        int64_t* hard_failed, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* ---- device memory of a TraceEngine run ------------------------------------------------------
+ * The tranche plan of TraceEngine::run / run_on_device / max_variants
+ * (src/cuda/trace_engine.cu:185-268; usable_bytes and max_variants,
+ * include/mikroptim/batch/batch_memory.hpp:119-135), for this library's device layout.
+ *
+ * usable = free - max(reserve_min_bytes, reserve_fraction * free), at least 0; status
+ * MKB_ERR_ARGUMENT when reserve_fraction is outside [0, 1]. */
+int mkb_usable_bytes(size_t free_bytes, size_t reserve_min_bytes, double reserve_fraction,
+                     size_t* usable);
+/* Device bytes a run allocates: `per_variant` for each variant of a tranche (its record, its
+ * outputs and scratch) plus `fixed` once (alignment of the buffers). `shape` describes the
+ * batch (variants and records are not read). merit_mode 0: RESIDUALS with residual rows of
+ * stride trace_rows + extra_residuals, status always, OPD when `opd`; 1: MERIT, with one
+ * double per variant more when `extra_merit`. */
+int mkb_trace_run_bytes(const mkb_device_batch* shape, const mkb_residual_plan* plan,
+                        int32_t merit_mode, int64_t extra_residuals, int32_t opd,
+                        int32_t extra_merit, size_t* per_variant, size_t* fixed);
+/* The largest tranche for `usable` bytes: a multiple of `granularity` (>= 1) with
+ * fixed + tranche * per_variant <= usable and tranche * packs <= 2^31 - 1 CTAs; 0 when not
+ * even `granularity` variants fit; negative status on bad arguments. */
+int64_t mkb_trace_tranche_variants(size_t usable, const mkb_device_batch* shape,
+                                   const mkb_residual_plan* plan,
+                                   const mkb_trace_options* options, int32_t merit_mode,
+                                   int64_t extra_residuals, int32_t opd, int32_t extra_merit,
+                                   int32_t granularity);
+
 /* ---- Jacobians ------------------------------------------------------------------------------
  * Both take `templates` (1 variant for all runs, or one per run), the plan, the variables and
  * the run points x0 [runs][P] (device), and write J [runs][P][R] (column p of run i at

@@ -113,6 +113,13 @@ class LmOptions(C.Structure):
     ]
 
 
+class TraceOptions(C.Structure):
+    """mkb_trace_options (TraceSettings::pack_rays / ::extra_merit, trace_engine.hpp:58)."""
+
+    _fields_ = [("pack_rays", C.c_int32), ("reserved", C.c_int32),
+                ("extra_merit", C.c_void_p)]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -142,6 +149,26 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                      c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
                                      c.c_size_t, c.c_void_p]
+    PT = C.POINTER(TraceOptions)
+    lib.mkb_residuals_ex_device.restype = c.c_int
+    lib.mkb_residuals_ex_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan), PT,
+                                            c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p,
+                                            c.c_void_p]
+    lib.mkb_merit_ex_device.restype = c.c_int
+    lib.mkb_merit_ex_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan), PT,
+                                        c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+                                        c.c_size_t, c.c_void_p]
+    lib.mkb_usable_bytes.restype = c.c_int
+    lib.mkb_usable_bytes.argtypes = [c.c_size_t, c.c_size_t, c.c_double,
+                                     C.POINTER(c.c_size_t)]
+    lib.mkb_trace_run_bytes.restype = c.c_int
+    lib.mkb_trace_run_bytes.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                        c.c_int32, c.c_int64, c.c_int32, c.c_int32,
+                                        C.POINTER(c.c_size_t), C.POINTER(c.c_size_t)]
+    lib.mkb_trace_tranche_variants.restype = c.c_int64
+    lib.mkb_trace_tranche_variants.argtypes = [c.c_size_t, C.POINTER(DeviceBatch),
+                                               C.POINTER(ResidualPlan), PT, c.c_int32,
+                                               c.c_int64, c.c_int32, c.c_int32, c.c_int32]
     lib.mkb_merit_noalloc_device.restype = c.c_int
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]

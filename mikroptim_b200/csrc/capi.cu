@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <string>
 
@@ -536,17 +537,42 @@ int64_t mkb_trace_rows(const mkb_residual_plan* plan) {
     return plan->failure == MKB_FAILURE_SOFT ? 2 * r : r;
 }
 
-int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
-                         double* residuals, int64_t stride, double* opd, uint8_t* status,
-                         void* stream) {
-    TraceParams p;
-    int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
-    if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
-        plan->precision != MKB_PRECISION_MIXED) {
-        set_error("residuals: precision %d not available for RESIDUALS", plan->precision);
+namespace {
+
+// pack_rays of the options (0 or no options: the default), clamped to what the kernels stage
+int options_pack_rays(const mkb_trace_options* options, int* pack_rays) {
+    int v = options != nullptr ? options->pack_rays : 0;
+    if (v < 0) {
+        set_error("pack_rays must be >= 1 (0 = default), got %d", v);
+        return MKB_ERR_ARGUMENT;
+    }
+    if (v == 0) v = pack_rays_default();
+    *pack_rays = v < kMaxPackRaysOption ? v : kMaxPackRaysOption;
+    return MKB_OK;
+}
+
+int check_trace_precision(int precision, const char* what) {
+    if (precision != MKB_PRECISION_FP64 && precision != MKB_PRECISION_FP64_FMA &&
+        precision != MKB_PRECISION_MIXED) {
+        set_error("%s: precision %d not available", what, precision);
         return MKB_ERR_UNSUPPORTED;
     }
+    return MKB_OK;
+}
+
+}  // namespace
+
+int mkb_residuals_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                            const mkb_trace_options* options, double* residuals, int64_t stride,
+                            double* opd, uint8_t* status, void* stream) {
+    int pack_rays = 0;
+    int rc = options_pack_rays(options, &pack_rays);
+    if (rc != MKB_OK) return rc;
+    TraceParams p;
+    rc = make_trace_params(batch, plan, pack_rays, &p);
+    if (rc != MKB_OK) return rc;
+    rc = check_trace_precision(plan->precision, "residuals");
+    if (rc != MKB_OK) return rc;
     const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * static_cast<int64_t>(p.rays) : p.rays;
     if (stride < rows) {
         set_error("residuals: stride %lld < trace rows %lld", static_cast<long long>(stride),
@@ -562,29 +588,145 @@ int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan*
                             static_cast<cudaStream_t>(stream));
 }
 
+int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                         double* residuals, int64_t stride, double* opd, uint8_t* status,
+                         void* stream) {
+    return mkb_residuals_ex_device(batch, plan, nullptr, residuals, stride, opd, status, stream);
+}
+
 size_t mkb_merit_workspace_bytes(int32_t variants, const mkb_residual_plan* plan) {
     if (check_plan(plan) != MKB_OK || variants < 0) return 0;
     return merit_workspace_bytes(variants, plan->fields * plan->wavelengths);
 }
 
-int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* plan, double* merit,
-                     int64_t* failed, int64_t* hard_failed, void* workspace,
-                     size_t workspace_bytes, void* stream) {
-    TraceParams p;
-    int rc = make_trace_params(batch, plan, pack_rays_default(), &p);
+int mkb_merit_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                        const mkb_trace_options* options, double* merit, int64_t* failed,
+                        int64_t* hard_failed, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+    int pack_rays = 0;
+    int rc = options_pack_rays(options, &pack_rays);
     if (rc != MKB_OK) return rc;
-    if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
-        plan->precision != MKB_PRECISION_MIXED) {
-        set_error("merit: precision %d not available", plan->precision);
-        return MKB_ERR_UNSUPPORTED;
-    }
+    TraceParams p;
+    rc = make_trace_params(batch, plan, pack_rays, &p);
+    if (rc != MKB_OK) return rc;
+    rc = check_trace_precision(plan->precision, "merit");
+    if (rc != MKB_OK) return rc;
     if (p.V == 0) return MKB_OK;
     if (!merit || !failed || !hard_failed) {
         set_error("merit: output is null");
         return MKB_ERR_ARGUMENT;
     }
     return launch_merit(p, batch->records, merit, failed, hard_failed, workspace,
-                        workspace_bytes, plan->precision, static_cast<cudaStream_t>(stream));
+                        workspace_bytes, plan->precision, static_cast<cudaStream_t>(stream), {},
+                        options != nullptr ? options->extra_merit : nullptr);
+}
+
+int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* plan, double* merit,
+                     int64_t* failed, int64_t* hard_failed, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+    return mkb_merit_ex_device(batch, plan, nullptr, merit, failed, hard_failed, workspace,
+                               workspace_bytes, stream);
+}
+
+// ---- device memory of a TraceEngine run ----------------------------------------------------
+int mkb_usable_bytes(size_t free_bytes, size_t reserve_min_bytes, double reserve_fraction,
+                     size_t* usable) {
+    if (usable == nullptr || !(reserve_fraction >= 0.0 && reserve_fraction <= 1.0)) {
+        set_error("memory reserve: fraction must be in [0, 1]");
+        return MKB_ERR_ARGUMENT;
+    }
+    const double part = reserve_fraction * static_cast<double>(free_bytes);
+    size_t reserve = part >= static_cast<double>(SIZE_MAX) ? SIZE_MAX : static_cast<size_t>(part);
+    if (reserve < reserve_min_bytes) reserve = reserve_min_bytes;
+    *usable = free_bytes > reserve ? free_bytes - reserve : 0;
+    return MKB_OK;
+}
+
+namespace {
+
+// the trace parameters of a batch shape (its variants and records are not read)
+int shape_params(const mkb_device_batch* shape, const mkb_residual_plan* plan, int pack_rays,
+                 TraceParams* p) {
+    if (shape == nullptr) {
+        set_error("batch shape is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    mkb_device_batch s = *shape;
+    s.variants = 0;
+    s.records = nullptr;
+    return make_trace_params(&s, plan, pack_rays, p);
+}
+
+// one buffer's worth of allocation granularity for each buffer a run holds (records, variant
+// surface counts, up to three outputs, scratch, extra merit)
+constexpr size_t kRunBuffers = 7;
+constexpr size_t kBufferSlack = size_t(2) << 20;
+
+int run_bytes(const TraceParams& p, const mkb_device_batch* shape, const mkb_residual_plan* plan,
+              int merit_mode, int64_t extra_residuals, int opd, int extra_merit,
+              size_t* per_variant, size_t* fixed) {
+    if (extra_residuals < 0) {
+        set_error("extra_residuals must be >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
+    const size_t rays = static_cast<size_t>(p.rays);
+    size_t per = static_cast<size_t>(p.stride) * sizeof(double);
+    if (shape->variant_surfaces != nullptr) per += 1;
+    if (merit_mode) {
+        per += 3 * sizeof(double) + merit_workspace_bytes(1, p.n_tuples);
+        if (extra_merit) per += sizeof(double);
+    } else {
+        const size_t rows = (plan->failure == MKB_FAILURE_SOFT ? 2 * rays : rays) +
+                            static_cast<size_t>(extra_residuals);
+        per += rows * sizeof(double) + rays;  // residual rows and the status bytes
+        if (opd) per += rays * sizeof(double);
+    }
+    *per_variant = per;
+    *fixed = kRunBuffers * kBufferSlack;
+    return MKB_OK;
+}
+
+}  // namespace
+
+int mkb_trace_run_bytes(const mkb_device_batch* shape, const mkb_residual_plan* plan,
+                        int32_t merit_mode, int64_t extra_residuals, int32_t opd,
+                        int32_t extra_merit, size_t* per_variant, size_t* fixed) {
+    if (per_variant == nullptr || fixed == nullptr) {
+        set_error("run bytes: null output");
+        return MKB_ERR_ARGUMENT;
+    }
+    TraceParams p;
+    int rc = shape_params(shape, plan, pack_rays_default(), &p);
+    if (rc != MKB_OK) return rc;
+    return run_bytes(p, shape, plan, merit_mode, extra_residuals, opd, extra_merit, per_variant,
+                     fixed);
+}
+
+int64_t mkb_trace_tranche_variants(size_t usable, const mkb_device_batch* shape,
+                                   const mkb_residual_plan* plan,
+                                   const mkb_trace_options* options, int32_t merit_mode,
+                                   int64_t extra_residuals, int32_t opd, int32_t extra_merit,
+                                   int32_t granularity) {
+    if (granularity < 1) {
+        set_error("granularity must be >= 1");
+        return MKB_ERR_ARGUMENT;
+    }
+    int pack_rays = 0;
+    int rc = options_pack_rays(options, &pack_rays);
+    if (rc != MKB_OK) return rc;
+    TraceParams p;
+    rc = shape_params(shape, plan, pack_rays, &p);
+    if (rc != MKB_OK) return rc;
+    size_t per = 0, fixed = 0;
+    rc = run_bytes(p, shape, plan, merit_mode, extra_residuals, opd, extra_merit, &per, &fixed);
+    if (rc != MKB_OK) return rc;
+    if (usable <= fixed) return 0;
+    int64_t cap = static_cast<int64_t>((usable - fixed) / per);
+    const int64_t grid_cap = static_cast<int64_t>(INT32_MAX) / (p.n_packs > 0 ? p.n_packs : 1);
+    if (cap > grid_cap) cap = grid_cap;
+    if (cap > INT32_MAX) cap = INT32_MAX;
+    cap = cap / granularity * granularity;
+    return cap;
 }
 
 }  // extern "C"

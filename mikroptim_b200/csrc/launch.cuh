@@ -38,9 +38,11 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
                      cudaStream_t stream, RunMask mask = {});
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
                  int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream, RunMask mask = {});
+                 cudaStream_t stream, RunMask mask = {}, const double* extra = nullptr);
 size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
+// largest pack a caller may ask for (mkb_trace_options.pack_rays is clamped to it)
+constexpr int kMaxPackRaysOption = 4096;
 
 // adjoint.cu
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,

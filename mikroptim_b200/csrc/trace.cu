@@ -297,10 +297,12 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
 }
 
 // merit[v] = sum over tuples in order (f-major, then l); counts likewise.
+// extra [V] (or null): added after the tuple sums (MeritRunOptions::extra_merit,
+// src/cuda/merit.cu:222).
 __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
                                       const int* part_failed, const int* part_hard,
                                       double* merit, int64_t* failed, int64_t* hard,
-                                      RunMask mask) {
+                                      RunMask mask, const double* extra) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V || !run_active(mask, v)) return;
     double sum = 0.0;
@@ -311,6 +313,7 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
         nf += part_failed[o + t];
         nh += part_hard[o + t];
     }
+    if (extra != nullptr) sum = __dadd_rn(sum, extra[v]);
     merit[v] = sum;
     failed[v] = nf;
     hard[v] = nh;
@@ -370,7 +373,7 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
                  int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream, RunMask mask) {
+                 cudaStream_t stream, RunMask mask, const double* extra) {
     const size_t need = merit_workspace(p.V, p.n_tuples);
     if (workspace == nullptr || ws_bytes < need) {
         set_error("merit: workspace of %zu bytes needed, %zu given", need, ws_bytes);
@@ -384,7 +387,8 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     int rc = launch_trace<false>(p, records, out, precision, stream);
     if (rc != MKB_OK) return rc;
     merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(
-        p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard, mask);
+        p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard, mask,
+        extra);
     count_launch();
     return cuda_status(cudaGetLastError(), "merit finalize launch");
 }

@@ -41,9 +41,13 @@ def _require_cuda(device) -> torch.device:
 
 
 class DeviceSystemBatch:
-    """A batch resident in device memory as packed per-variant records (16-byte aligned)."""
+    """A batch resident in device memory as packed per-variant records (16-byte aligned).
 
-    def __init__(self, batch: SystemBatchHost, device="cuda", stream=None):
+    `storage` (a uint8 device tensor) lets a caller that keeps its buffers across calls, like
+    TraceEngine, place the records in memory it already holds when it is large enough."""
+
+    def __init__(self, batch: SystemBatchHost, device="cuda", stream=None,
+                 storage: torch.Tensor | None = None):
         self.device = _require_cuda(device)
         lib = _capi.lib()
         batch.validate_values()
@@ -62,8 +66,12 @@ class DeviceSystemBatch:
         view = batch.view()
         _capi.check(lib.mkb_pack_batch_host(C.byref(view), _capi.ptr(host)), "pack batch")
         self.host_records = torch.from_numpy(host[:batch.variants]).pin_memory()
-        self.records = torch.empty((max(batch.variants, 1), self.stride), dtype=torch.float64,
-                                   device=self.device)
+        n = max(batch.variants, 1) * self.stride
+        if storage is not None and storage.numel() >= 8 * n and storage.device == self.device:
+            self.records = storage[:8 * n].view(torch.float64).view(-1, self.stride)
+        else:
+            self.records = torch.empty((max(batch.variants, 1), self.stride),
+                                       dtype=torch.float64, device=self.device)
         if batch.variants:
             with torch.cuda.stream(stream) if stream is not None else _nullcontext():
                 self.records[:batch.variants].copy_(self.host_records, non_blocking=True)
@@ -116,8 +124,16 @@ class MeritOutput:
     hard_failed: np.ndarray | torch.Tensor
 
 
+def _trace_options(pack_rays: int = 0, extra_merit: torch.Tensor | None = None):
+    o = _capi.TraceOptions()
+    o.pack_rays = int(pack_rays)
+    o.reserved = 0
+    o.extra_merit = C.c_void_p(extra_merit.data_ptr()) if extra_merit is not None else None
+    return o
+
+
 def residuals_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: SystemBatchHost,
-                     stream=None) -> ResidualOutput:
+                     stream=None, pack_rays: int = 0) -> ResidualOutput:
     """RESIDUALS on an uploaded batch; outputs stay on the device."""
     lib = _capi.lib()
     V = dbatch.variants
@@ -126,16 +142,20 @@ def residuals_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: Sy
     st = torch.empty((V, layout.rays_per_variant), dtype=torch.uint8, device=dbatch.device)
     b = dbatch.c_struct()
     plan = layout.plan(host)
-    rc = lib.mkb_residuals_device(C.byref(b), C.byref(plan), C.c_void_p(res.data_ptr()),
-                                  layout.trace_rows, C.c_void_p(opd.data_ptr()),
-                                  C.c_void_p(st.data_ptr()), _stream_handle(stream))
+    opts = _trace_options(pack_rays)
+    rc = lib.mkb_residuals_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
+                                     C.c_void_p(res.data_ptr()), layout.trace_rows,
+                                     C.c_void_p(opd.data_ptr()), C.c_void_p(st.data_ptr()),
+                                     _stream_handle(stream))
     _capi.check(rc, "residuals")
     return ResidualOutput(res, opd, st)
 
 
 def merit_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: SystemBatchHost,
-                 stream=None, workspace: torch.Tensor | None = None) -> MeritOutput:
-    """MERIT on an uploaded batch; outputs stay on the device."""
+                 stream=None, workspace: torch.Tensor | None = None, pack_rays: int = 0,
+                 extra_merit: torch.Tensor | None = None) -> MeritOutput:
+    """MERIT on an uploaded batch; outputs stay on the device. extra_merit: device [V] added to
+    each variant's merit after its tuple sums."""
     lib = _capi.lib()
     V = dbatch.variants
     plan = layout.plan(host)
@@ -146,43 +166,426 @@ def merit_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: System
     failed = torch.empty(V, dtype=torch.int64, device=dbatch.device)
     hard = torch.empty(V, dtype=torch.int64, device=dbatch.device)
     b = dbatch.c_struct()
-    rc = lib.mkb_merit_device(C.byref(b), C.byref(plan), C.c_void_p(merit.data_ptr()),
-                              C.c_void_p(failed.data_ptr()), C.c_void_p(hard.data_ptr()),
-                              C.c_void_p(workspace.data_ptr()), workspace.numel(),
-                              _stream_handle(stream))
+    if extra_merit is not None:
+        extra_merit = extra_merit.to(device=dbatch.device, dtype=torch.float64).contiguous()
+        if extra_merit.numel() != V:
+            raise ValueError(f"extra_merit must hold {V} values")
+    opts = _trace_options(pack_rays, extra_merit)
+    rc = lib.mkb_merit_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
+                                 C.c_void_p(merit.data_ptr()), C.c_void_p(failed.data_ptr()),
+                                 C.c_void_p(hard.data_ptr()), C.c_void_p(workspace.data_ptr()),
+                                 workspace.numel(), _stream_handle(stream))
     _capi.check(rc, "merit")
     return MeritOutput(merit, failed, hard)
 
 
+# ---- TraceEngine (include/mikroptim/cuda/trace_engine.hpp) ---------------------------------
+@dataclass
+class MemoryReserve:
+    """MemoryReserve (include/mikroptim/batch/batch_memory.hpp:119): the engine leaves
+    max(min_bytes, fraction * free) of the device memory it sees as free untouched."""
+
+    min_bytes: int = 256 << 20
+    fraction: float = 0.05
+
+
+@dataclass
+class EngineOptions:
+    """EngineOptions (trace_engine.hpp:44). memory_limit_bytes caps the memory the engine
+    regards as available (tranche tests, sharing a GPU); None: the device's free memory."""
+
+    memory_limit_bytes: int | None = None
+    reserve: MemoryReserve = dataclasses.field(default_factory=MemoryReserve)
+
+
+@dataclass
+class TraceSettings:
+    """TraceSettings (trace_engine.hpp:52). opd / status / extra_residuals apply to RESIDUALS
+    (the extra rows follow the ray and penalty rows and are set to 0); extra_merit (host [V] or
+    None) to MERIT, added to each variant's merit after its tuple sums. precision None: the
+    quadrature's. pack_rays changes only the run time (bit-identical results for every value).
+    extrema (per-variant, per-surface maxima) is not built: True raises NotImplementedError."""
+
+    quadrature: ResidualSettings = dataclasses.field(default_factory=ResidualSettings)
+    opd: bool = False
+    status: bool = True
+    extra_residuals: int = 0
+    extrema: bool = False
+    extra_merit: np.ndarray | None = None
+    precision: int | None = None
+    pack_rays: int = 512
+
+
+@dataclass
+class TraceRunInfo:
+    """TraceRunInfo (trace_engine.hpp:93)."""
+
+    variants: int = 0
+    tranches: int = 0
+    tranche_variants: int = 0
+    budget_bytes: int = 0
+    device_bytes: int = 0
+
+
+@dataclass
+class ResidualResult:
+    """ResidualResult (batch_residuals.hpp): residuals [V][stride], opd / status [V][rays]
+    (empty when not requested)."""
+
+    variants: int = 0
+    rays_per_variant: int = 0
+    penalty_rows: int = 0
+    stride: int = 0
+    residuals: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0)))
+    opd: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0)))
+    status: np.ndarray = dataclasses.field(
+        default_factory=lambda: np.zeros((0, 0), dtype=np.uint8))
+
+
+@dataclass
+class MeritResult:
+    """MeritResult (batch_merit.hpp:32)."""
+
+    variants: int = 0
+    rays_per_variant: int = 0
+    merit: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    failed: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, dtype=np.int64))
+    hard_failed: np.ndarray = dataclasses.field(
+        default_factory=lambda: np.zeros(0, dtype=np.int64))
+
+
+@dataclass
+class TraceOutput:
+    """TraceOutput (trace_engine.hpp:103): the result of the run's mode; the other is empty."""
+
+    mode: TraceMode = TraceMode.RESIDUALS
+    layout: ResidualLayout | None = None
+    residuals: ResidualResult = dataclasses.field(default_factory=ResidualResult)
+    merit: MeritResult = dataclasses.field(default_factory=MeritResult)
+    info: TraceRunInfo = dataclasses.field(default_factory=TraceRunInfo)
+
+
+@dataclass
+class DeviceTranche:
+    """DeviceTranche (trace_engine.hpp:117): one tranche's RESIDUALS on the device, views of
+    the engine's buffers valid during the callback only."""
+
+    first: int
+    count: int
+    rays_per_variant: int
+    penalty_rows: int
+    stride: int
+    residuals: torch.Tensor            # [count][stride]
+    status: torch.Tensor               # [count][rays]
+    opd: torch.Tensor | None           # [count][rays] when settings.opd
+
+
+def _as_trace_settings(settings) -> TraceSettings:
+    if settings is None:
+        return TraceSettings()
+    if isinstance(settings, TraceSettings):
+        return settings
+    if isinstance(settings, ResidualSettings):
+        return TraceSettings(quadrature=settings)
+    raise TypeError("settings must be TraceSettings or ResidualSettings")
+
+
 class TraceEngine:
-    """TraceEngine(device): host batch in, host results out (TraceEngine::run)."""
+    """TraceEngine(device, options) (include/mikroptim/cuda/trace_engine.hpp:145): host batch
+    in, host results out. Splits a batch into tranches that fit the device memory it sees
+    (free memory plus its own buffers, at most options.memory_limit_bytes, less the reserve)
+    and keeps its buffers across calls; every variant's results are bit-identical whatever the
+    split (the kernels do not depend on a variant's position in the batch)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, options: EngineOptions | None = None):
         self.device = _require_cuda(f"cuda:{device}")
-        self._workspace = None
+        self.options = options or EngineOptions()
+        self._usable(0)  # checks the reserve (ValueError for a fraction outside [0, 1])
+        self.device_name = torch.cuda.get_device_name(self.device)
+        self._buffers: dict[str, torch.Tensor] = {}
 
-    def run(self, batch: SystemBatchHost, mode: TraceMode,
-            settings: ResidualSettings | None = None):
-        layout = ResidualLayout(batch.topology, settings or ResidualSettings())
+    # ---- memory ---------------------------------------------------------------------------
+    def device_bytes(self) -> int:
+        """Device memory the engine holds now (batch and outputs) [bytes]."""
+        return sum(t.numel() for t in self._buffers.values())
+
+    def release(self) -> None:
+        """Frees every device buffer (the next run allocates them again)."""
+        self._buffers.clear()
+
+    def _usable(self, available: int) -> int:
+        out = C.c_size_t(0)
+        r = self.options.reserve
+        _capi.check(_capi.lib().mkb_usable_bytes(int(available), int(r.min_bytes),
+                                                  float(r.fraction), C.byref(out)),
+                    "memory reserve")
+        return int(out.value)
+
+    def _available(self) -> int:
+        free, _ = torch.cuda.mem_get_info(self.device)
+        cached = (torch.cuda.memory_reserved(self.device) -
+                  torch.cuda.memory_allocated(self.device))
+        available = int(free) + int(cached) + self.device_bytes()
+        if self.options.memory_limit_bytes is not None:
+            available = min(available, int(self.options.memory_limit_bytes))
+        return available
+
+    def _buffer(self, name: str, nbytes: int) -> torch.Tensor:
+        buf = self._buffers.get(name)
+        if buf is None or buf.numel() < nbytes:
+            self._buffers.pop(name, None)  # the old buffer goes before the new one comes
+            buf = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=self.device)
+            self._buffers[name] = buf
+        return buf
+
+    @staticmethod
+    def _shape(topology, glass: bool, variant_surfaces: bool = False) -> _capi.DeviceBatch:
+        lib = _capi.lib()
+        b = _capi.DeviceBatch()
+        b.variants = 0
+        b.surfaces, b.wavelengths, b.fields = (topology.surfaces, topology.wavelengths,
+                                                topology.fields)
+        b.non_coaxial = 1 if topology.non_coaxial else 0
+        b.ghost_plates, b.ghost_terms = topology.ghost_plates, topology.ghost_terms
+        b.glass = 1 if glass else 0
+        b.record_stride = int(lib.mkb_record_stride_ext(b.surfaces, b.wavelengths, b.fields,
+                                                        b.non_coaxial, b.ghost_plates,
+                                                        b.ghost_terms, b.glass))
+        t = np.ascontiguousarray(topology.type, dtype=np.uint8)
+        b.type = _capi.ptr(t, C.c_uint8)
+        b.records = None
+        b.variant_surfaces = C.c_void_p(1) if variant_surfaces else None  # never dereferenced
+        b._keep = (t,)
+        return b
+
+    @staticmethod
+    def _layout(topology, ts: TraceSettings) -> ResidualLayout:
+        q = ts.quadrature
+        if ts.precision is not None:
+            q = dataclasses.replace(q, precision=ts.precision)
+        return ResidualLayout(topology, q)
+
+    @staticmethod
+    def _check(ts: TraceSettings) -> None:
+        if ts.extra_residuals < 0:
+            raise ValueError("TraceEngine: extra_residuals must be >= 0")
+        if ts.pack_rays < 1:
+            raise ValueError("TraceEngine: pack_rays must be >= 1")
+        if ts.extrema:
+            raise NotImplementedError("TraceEngine: per-surface extrema are not built")
+
+    def _tranche(self, shape, layout: ResidualLayout, plan, ts: TraceSettings, merit: bool,
+                 granularity: int, usable: int) -> int:
+        opts = _trace_options(ts.pack_rays)
+        n = int(_capi.lib().mkb_trace_tranche_variants(
+            int(usable), C.byref(shape), C.byref(plan), C.byref(opts), 1 if merit else 0,
+            int(ts.extra_residuals), 1 if ts.opd else 0,
+            1 if (merit and ts.extra_merit is not None) else 0, int(granularity)))
+        if n < 0:
+            _capi.check(n, "tranche plan")
+        return n
+
+    def max_variants(self, topology, mode: TraceMode, settings=None, glass: bool = False) -> int:
+        """Largest tranche for batches of this topology (TraceEngine::max_variants): the free
+        device memory plus the engine's own buffers, at most memory_limit_bytes, less the
+        reserve and the fixed per-run buffers. 0 when not one variant fits."""
+        ts = _as_trace_settings(settings)
+        self._check(ts)
+        layout = self._layout(topology, ts)
+        host = _UnitWeights(topology)
+        return self._tranche(self._shape(topology, glass), layout, layout.plan(host), ts,
+                             mode == TraceMode.MERIT, 1, self._usable(self._available()))
+
+    def _plan(self, batch: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
+              merit: bool, granularity: int) -> tuple[int, int]:
+        shape = self._shape(batch.topology, batch.buchdahl_coeff is not None,
+                            batch.variant_surfaces is not None)
+        plan = layout.plan(batch)
+        # the other mode's buffers stay while the tranche does not shrink because of them
+        other = ("res", "status", "opd") if merit else ("merit", "failed", "hard", "ws", "extra")
+        held = sum(self._buffers[k].numel() for k in other if k in self._buffers)
+        available = self._available()
+        usable = self._usable(available - min(held, available))
+        tranche = self._tranche(shape, layout, plan, ts, merit, granularity, usable)
+        if held and tranche < batch.variants:
+            usable_all = self._usable(available)
+            tranche_all = self._tranche(shape, layout, plan, ts, merit, granularity, usable_all)
+            if tranche_all > tranche:
+                for k in other:
+                    self._buffers.pop(k, None)
+                tranche, usable = tranche_all, usable_all
+        if tranche < 1:
+            what = ("one variant fits" if granularity == 1
+                    else f"{granularity} variants that belong together fit")
+            raise RuntimeError(f"TraceEngine: not even {what} into the device memory "
+                               f"(available {available / 2**20:.1f} MiB, after the reserve "
+                               f"{usable / 2**20:.1f} MiB)")
+        return min(tranche, batch.variants), usable
+
+    # ---- runs -----------------------------------------------------------------------------
+    def run(self, batch: SystemBatchHost, mode: TraceMode, settings=None,
+            out: TraceOutput | None = None) -> TraceOutput:
+        """TraceEngine::run: validate, plan the tranches, then per tranche upload, kernel and
+        download into the host result at the tranche's first variant. Synchronous."""
+        ts = _as_trace_settings(settings)
+        self._check(ts)
+        if not isinstance(mode, TraceMode):
+            raise ValueError("TraceEngine: unknown mode")
+        layout = self._layout(batch.topology, ts)
+        batch.validate_values()
+        V = batch.variants
+        merit = mode == TraceMode.MERIT
+        extra = None
+        if merit and ts.extra_merit is not None:
+            extra = np.ascontiguousarray(ts.extra_merit, dtype=np.float64).reshape(-1)
+            if extra.size != V:
+                raise ValueError(f"TraceEngine: extra_merit must be empty or hold {V} values")
+        out = out if out is not None else TraceOutput()
+        rays = layout.rays_per_variant
+        stride = layout.trace_rows + ts.extra_residuals
+        out.mode, out.layout = mode, layout
+        out.info = TraceRunInfo(variants=V)
+        if merit:
+            out.residuals = ResidualResult()
+            out.merit = MeritResult(V, rays, np.zeros(V), np.zeros(V, dtype=np.int64),
+                                    np.zeros(V, dtype=np.int64))
+        else:
+            out.merit = MeritResult()
+            out.residuals = ResidualResult(
+                V, rays, layout.trace_rows - rays, stride, np.zeros((V, stride)),
+                np.zeros((V, rays) if ts.opd else (0, 0)),
+                np.zeros((V, rays) if ts.status else (0, 0), dtype=np.uint8))
+        if V == 0:
+            out.info.device_bytes = self.device_bytes()
+            return out
         with torch.cuda.device(self.device):
-            dbatch = DeviceSystemBatch(batch, self.device)
-            if mode == TraceMode.RESIDUALS:
-                out = residuals_device(dbatch, layout, batch)
+            tranche, usable = self._plan(batch, layout, ts, merit, 1)
+            for first in range(0, V, tranche):
+                count = min(tranche, V - first)
+                part = batch.subset(first, count) if (first, count) != (0, V) else batch
+                if merit:
+                    m = self._merit_tranche(part, layout, ts,
+                                            None if extra is None else extra[first:first + count])
+                    torch.cuda.synchronize()
+                    out.merit.merit[first:first + count] = m.merit.cpu().numpy()
+                    out.merit.failed[first:first + count] = m.failed.cpu().numpy()
+                    out.merit.hard_failed[first:first + count] = m.hard_failed.cpu().numpy()
+                else:
+                    t = self._residual_tranche(part, layout, ts, first)
+                    torch.cuda.synchronize()
+                    out.residuals.residuals[first:first + count] = t.residuals.cpu().numpy()
+                    if ts.status:
+                        out.residuals.status[first:first + count] = t.status.cpu().numpy()
+                    if ts.opd:
+                        out.residuals.opd[first:first + count] = t.opd.cpu().numpy()
+                _device_status()
+                out.info.tranches += 1
+            out.info.tranche_variants = tranche
+            out.info.budget_bytes = usable
+            out.info.device_bytes = self.device_bytes()
+        return out
+
+    def run_on_device(self, batch: SystemBatchHost, settings, granularity: int,
+                      consume) -> TraceRunInfo:
+        """TraceEngine::run_on_device: RESIDUALS without the download. After each tranche's
+        kernel the engine calls consume(DeviceTranche) with views of its device buffers; the
+        tranche size is a multiple of `granularity` (only the last may be smaller)."""
+        ts = _as_trace_settings(settings)
+        self._check(ts)
+        if granularity < 1:
+            raise ValueError("TraceEngine: granularity must be >= 1")
+        if consume is None:
+            raise ValueError("TraceEngine: run_on_device without a callback")
+        layout = self._layout(batch.topology, ts)
+        batch.validate_values()
+        V = batch.variants
+        info = TraceRunInfo(variants=V)
+        if V == 0:
+            info.device_bytes = self.device_bytes()
+            return info
+        with torch.cuda.device(self.device):
+            tranche, usable = self._plan(batch, layout, ts, False, granularity)
+            for first in range(0, V, tranche):
+                count = min(tranche, V - first)
+                part = batch.subset(first, count) if (first, count) != (0, V) else batch
+                t = self._residual_tranche(part, layout, ts, first)
                 torch.cuda.synchronize()
                 _device_status()
-                return ResidualOutput(out.residuals.cpu().numpy(), out.opd.cpu().numpy(),
-                                      out.status.cpu().numpy())
-            if self._workspace is None:
-                self._workspace = torch.empty(0, dtype=torch.uint8, device=self.device)
-            need = int(_capi.lib().mkb_merit_workspace_bytes(batch.variants,
-                                                            C.byref(layout.plan(batch))))
-            if self._workspace.numel() < need:
-                self._workspace = torch.empty(need, dtype=torch.uint8, device=self.device)
-            out = merit_device(dbatch, layout, batch, workspace=self._workspace)
-            torch.cuda.synchronize()
-            _device_status()
-            return MeritOutput(out.merit.cpu().numpy(), out.failed.cpu().numpy(),
-                               out.hard_failed.cpu().numpy())
+                consume(t)
+                torch.cuda.synchronize()
+                info.tranches += 1
+            info.tranche_variants = tranche
+            info.budget_bytes = usable
+            info.device_bytes = self.device_bytes()
+        return info
+
+    def _residual_tranche(self, part: SystemBatchHost, layout: ResidualLayout,
+                          ts: TraceSettings, first: int) -> DeviceTranche:
+        lib = _capi.lib()
+        n = part.variants
+        rays = layout.rays_per_variant
+        stride = layout.trace_rows + ts.extra_residuals
+        db = DeviceSystemBatch(part, self.device,
+                               storage=self._buffer("records", 8 * n * self._stride_of(part)))
+        res = self._buffer("res", 8 * n * stride)[:8 * n * stride].view(torch.float64)
+        res = res.view(n, stride)
+        st = self._buffer("status", n * rays)[:n * rays].view(n, rays)
+        opd = None
+        if ts.opd:
+            opd = self._buffer("opd", 8 * n * rays)[:8 * n * rays].view(torch.float64)
+            opd = opd.view(n, rays)
+        if ts.extra_residuals:
+            res[:, layout.trace_rows:].zero_()
+        b = db.c_struct()
+        plan = layout.plan(part)
+        opts = _trace_options(ts.pack_rays)
+        rc = lib.mkb_residuals_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
+                                         C.c_void_p(res.data_ptr()), stride,
+                                         C.c_void_p(opd.data_ptr()) if opd is not None else None,
+                                         C.c_void_p(st.data_ptr()), _stream_handle(None))
+        _capi.check(rc, "residuals")
+        return DeviceTranche(first, n, rays, layout.trace_rows - rays, stride, res, st, opd)
+
+    def _merit_tranche(self, part: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
+                       extra: np.ndarray | None) -> MeritOutput:
+        lib = _capi.lib()
+        n = part.variants
+        db = DeviceSystemBatch(part, self.device,
+                               storage=self._buffer("records", 8 * n * self._stride_of(part)))
+        plan = layout.plan(part)
+        ws = self._buffer("ws", int(lib.mkb_merit_workspace_bytes(n, C.byref(plan))))
+        merit = self._buffer("merit", 8 * n)[:8 * n].view(torch.float64)
+        failed = self._buffer("failed", 8 * n)[:8 * n].view(torch.int64)
+        hard = self._buffer("hard", 8 * n)[:8 * n].view(torch.int64)
+        extra_dev = None
+        if extra is not None:
+            extra_dev = self._buffer("extra", 8 * n)[:8 * n].view(torch.float64)
+            extra_dev.copy_(torch.from_numpy(np.ascontiguousarray(extra)))
+        b = db.c_struct()
+        opts = _trace_options(ts.pack_rays, extra_dev)
+        rc = lib.mkb_merit_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
+                                     C.c_void_p(merit.data_ptr()), C.c_void_p(failed.data_ptr()),
+                                     C.c_void_p(hard.data_ptr()), C.c_void_p(ws.data_ptr()),
+                                     ws.numel(), _stream_handle(None))
+        _capi.check(rc, "merit")
+        return MeritOutput(merit, failed, hard)
+
+    @staticmethod
+    def _stride_of(batch: SystemBatchHost) -> int:
+        return int(_capi.lib().mkb_record_stride_ext(
+            batch.surfaces, batch.wavelengths, batch.fields, 1 if batch.non_coaxial else 0,
+            batch.topology.ghost_plates, batch.topology.ghost_terms,
+            1 if batch.buchdahl_coeff is not None else 0))
+
+
+class _UnitWeights:
+    """The weights a plan reads, for sizing a run of a topology alone (sizes do not depend on
+    the weights)."""
+
+    def __init__(self, topology):
+        self.field_weight = np.ones(topology.fields)
+        self.wavelength_weight = np.ones(topology.wavelengths)
+        self.reference_wavelength_nm = 587.56
 
 
 def _device_status() -> None:

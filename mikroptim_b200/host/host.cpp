@@ -332,6 +332,17 @@ int64_t ResidualLayout::offset(int f, int l) const {
 std::unique_ptr<ResidualPlan> ResidualLayout::plan(const SystemBatchHost& batch) const {
     if (batch.fields() != topology_.fields || batch.wavelengths() != topology_.wavelengths)
         throw std::invalid_argument("ResidualLayout: batch does not match the layout");
+    return plan_from(batch.field_weight, batch.wavelength_weight, batch.reference_wavelength_nm);
+}
+
+std::unique_ptr<ResidualPlan> ResidualLayout::plan_for_sizing() const {
+    return plan_from(std::vector<double>(topology_.fields, 1.0),
+                     std::vector<double>(topology_.wavelengths, 1.0), 587.56);
+}
+
+std::unique_ptr<ResidualPlan> ResidualLayout::plan_from(
+    const std::vector<double>& field_weight, const std::vector<double>& wavelength_weight,
+    double reference_wavelength_nm) const {
     std::unique_ptr<ResidualPlan> p(new ResidualPlan());
     const int n = settings_.rings;
     for (int i = 0; i < n; ++i) {
@@ -339,15 +350,15 @@ std::unique_ptr<ResidualPlan> ResidualLayout::plan(const SystemBatchHost& batch)
         p->w_.push_back(detail::kGaussLegendre[n - 1][2 * i + 1]);
     }
     for (PupilMode m : topology_.pupil_mode) p->modes_.push_back(static_cast<uint8_t>(m));
-    p->field_weight_ = batch.field_weight;
-    p->wavelength_weight_ = batch.wavelength_weight;
+    p->field_weight_ = field_weight;
+    p->wavelength_weight_ = wavelength_weight;
     mkb_residual_plan& c = p->plan_;
     c.rings = n;
     c.spokes = settings_.spokes;
     c.failure = static_cast<int32_t>(settings_.failure);
     c.precision = static_cast<int32_t>(settings_.precision);
     c.fail_weight = settings_.fail_weight;
-    c.reference_wavelength_nm = batch.reference_wavelength_nm;
+    c.reference_wavelength_nm = reference_wavelength_nm;
     c.fields = topology_.fields;
     c.wavelengths = topology_.wavelengths;
     c.pupil_mode = p->modes_.data();
@@ -529,38 +540,69 @@ void DeviceBuffer::release() {
 }
 
 void DeviceSystemBatch::upload(const SystemBatchHost& batch, void* stream) {
+    upload(batch, 0, batch.variants(), stream);
+}
+
+void DeviceSystemBatch::upload(const SystemBatchHost& batch, int first, int count,
+                               void* stream) {
     batch.validate_values();
-    const mkb_batch_view view = batch.view();
+    if (first < 0 || count < 0 || first + count > batch.variants())
+        throw std::out_of_range("DeviceSystemBatch: variant range outside the batch");
+    mkb_batch_view view = batch.view();
+    // the tranche's rows of every per-variant array; the shared arrays stay
+    const int S = view.surfaces, L = view.wavelengths, F = view.fields;
+    const int G = view.ghost_plates, K = view.ghost_terms;
+    const size_t v0 = static_cast<size_t>(first);
+    view.variants = count;
+    view.curvature += v0 * S;
+    view.thickness += v0 * S;
+    view.index += v0 * S * L;
+    view.pupil_radius += v0;
+    view.field_angle += v0 * F;
+    view.field_target += v0 * F;
+    if (view.decenter_tilt != nullptr) view.decenter_tilt += v0 * S * 4;
+    if (view.ghost_coeff != nullptr) view.ghost_coeff += v0 * G * K;
+    if (view.ghost_index != nullptr) view.ghost_index += v0 * G * L;
+    if (view.buchdahl_coeff != nullptr) view.buchdahl_coeff += v0 * S * 4;
     const int32_t non_coaxial = view.decenter_tilt != nullptr ? 1 : 0;
     const int32_t glass = view.buchdahl_coeff != nullptr ? 1 : 0;
-    const int32_t stride = mkb_record_stride_ext(view.surfaces, view.wavelengths, view.fields,
-                                                 non_coaxial, view.ghost_plates,
-                                                 view.ghost_terms, glass);
+    const int32_t stride = mkb_record_stride_ext(S, L, F, non_coaxial, G, K, glass);
     wavelength_nm_.assign(batch.wavelength_nm.begin(), batch.wavelength_nm.end());
-    host_records_.assign(static_cast<size_t>(view.variants) * stride, 0.0);
+    host_records_.assign(static_cast<size_t>(count) * stride, 0.0);
     check(mkb_pack_batch_host(&view, host_records_.data()), "pack batch");
     void* d = cuda::upload(records_, host_records_, stream);
-    type_.assign(view.type, view.type + view.surfaces);
-    batch_.variants = view.variants;
-    batch_.surfaces = view.surfaces;
-    batch_.wavelengths = view.wavelengths;
-    batch_.fields = view.fields;
+    type_.assign(view.type, view.type + S);
+    batch_ = mkb_device_batch{};
+    batch_.variants = count;
+    batch_.surfaces = S;
+    batch_.wavelengths = L;
+    batch_.fields = F;
     batch_.record_stride = stride;
     batch_.non_coaxial = non_coaxial;
-    batch_.ghost_plates = view.ghost_plates;
-    batch_.ghost_terms = view.ghost_terms;
+    batch_.ghost_plates = G;
+    batch_.ghost_terms = K;
     batch_.glass = glass;
     batch_.wavelength_nm = wavelength_nm_.data();
     batch_.records = static_cast<const double*>(d);
     batch_.type = type_.data();
 }
 
-TraceEngine::TraceEngine(int device) : device_(device) {
+const char* to_string(TraceMode mode) {
+    return mode == TraceMode::Merit ? "MERIT" : "RESIDUALS";
+}
+
+TraceEngine::TraceEngine(int device, const EngineOptions& options)
+    : device_(device), options_(options) {
     int count = 0;
     cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (count == 0) throw CudaError("TraceEngine: no CUDA device");
     if (device < 0 || device >= count)
         throw std::invalid_argument("TraceEngine: no such CUDA device");
+    (void)usable_bytes(0);  // checks the reserve (std::invalid_argument)
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    device_name_ = prop.name;
     cudaStream_t s;
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = s;
@@ -571,7 +613,8 @@ TraceEngine::~TraceEngine() {
     if (stream_ != nullptr) cudaStreamDestroy(as_stream(stream_));
 }
 
-void TraceEngine::release() {
+void TraceEngine::release() noexcept {
+    batch_.release();
     out_.release();
     opd_.release();
     status_.release();
@@ -579,6 +622,13 @@ void TraceEngine::release() {
     failed_.release();
     hard_.release();
     workspace_.release();
+    extra_.release();
+}
+
+std::size_t TraceEngine::device_bytes() const {
+    return batch_.capacity_bytes() + out_.bytes() + opd_.bytes() + status_.bytes() +
+           merit_.bytes() + failed_.bytes() + hard_.bytes() + workspace_.bytes() +
+           extra_.bytes();
 }
 
 void TraceEngine::synchronize() {
@@ -586,37 +636,287 @@ void TraceEngine::synchronize() {
     check(mkb_device_status(), "device status");
 }
 
-void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
-                      const ResidualSettings& settings, TraceOutput& out) {
+std::size_t TraceEngine::available_bytes() const {
+    size_t free_bytes = 0, total = 0;
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
-    const ResidualLayout layout(batch.topology(), settings);
+    cuda_check(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+    // the engine's own buffers count as available: a run reuses or frees them
+    size_t available = free_bytes + device_bytes();
+    if (options_.memory_limit_bytes) available = std::min(available, *options_.memory_limit_bytes);
+    return available;
+}
+
+std::size_t TraceEngine::usable_bytes(std::size_t available) const {
+    size_t usable = 0;
+    if (mkb_usable_bytes(available, options_.reserve.min_bytes, options_.reserve.fraction,
+                         &usable) != MKB_OK)
+        throw std::invalid_argument("TraceEngine: reserve fraction must be in [0, 1]");
+    return usable;
+}
+
+namespace {
+
+void check_settings(const TraceSettings& settings) {
+    if (settings.extra_residuals < 0)
+        throw std::invalid_argument("TraceEngine: extra_residuals must be >= 0");
+    if (settings.pack_rays < 1) throw std::invalid_argument("TraceEngine: pack_rays must be >= 1");
+    if (settings.extrema) throw std::logic_error("TraceEngine: per-surface extrema are not built");
+}
+
+ResidualSettings quadrature_of(const TraceSettings& settings) {
+    ResidualSettings q = settings.quadrature;
+    if (settings.precision) q.precision = *settings.precision;
+    return q;
+}
+
+mkb_device_batch shape_of(const BatchTopology& t, bool glass, std::vector<uint8_t>& type) {
+    type.clear();
+    for (SurfaceKind k : t.type) type.push_back(static_cast<uint8_t>(k));
+    mkb_device_batch b{};
+    b.surfaces = t.surfaces;
+    b.wavelengths = t.wavelengths;
+    b.fields = t.fields;
+    b.non_coaxial = t.non_coaxial ? 1 : 0;
+    b.ghost_plates = t.ghost_plates;
+    b.ghost_terms = t.ghost_terms;
+    b.glass = glass ? 1 : 0;
+    b.record_stride = mkb_record_stride_ext(b.surfaces, b.wavelengths, b.fields, b.non_coaxial,
+                                            b.ghost_plates, b.ghost_terms, b.glass);
+    b.type = type.data();
+    return b;
+}
+
+int64_t tranche_for(size_t usable, const mkb_device_batch& shape, const mkb_residual_plan* plan,
+                    const TraceSettings& settings, bool merit, int granularity) {
+    mkb_trace_options o{};
+    o.pack_rays = settings.pack_rays;
+    const int64_t n = mkb_trace_tranche_variants(
+        usable, &shape, plan, &o, merit ? 1 : 0, settings.extra_residuals, settings.opd ? 1 : 0,
+        merit && !settings.extra_merit.empty() ? 1 : 0, granularity);
+    if (n < 0) check(static_cast<int>(n), "tranche plan");
+    return n;
+}
+
+}  // namespace
+
+int TraceEngine::max_variants(const BatchTopology& topology, TraceMode mode,
+                              const TraceSettings& settings) const {
+    check_settings(settings);
+    const ResidualLayout layout(topology, quadrature_of(settings));
+    const auto plan = layout.plan_for_sizing();
+    std::vector<uint8_t> type;
+    const mkb_device_batch shape = shape_of(topology, false, type);
+    return static_cast<int>(tranche_for(usable_bytes(available_bytes()), shape, plan->get(),
+                                        settings, mode == TraceMode::Merit, 1));
+}
+
+TraceEngine::TranchePlan TraceEngine::plan_tranches(const SystemBatchHost& batch, TraceMode mode,
+                                                    const ResidualLayout& layout,
+                                                    const TraceSettings& settings,
+                                                    int granularity) {
+    const bool merit = mode == TraceMode::Merit;
     const auto plan = layout.plan(batch);
-    batch_.upload(batch, stream_);
-    const mkb_device_batch b = batch_.c_struct();
-    const size_t V = static_cast<size_t>(batch.variants());
-    if (mode == TraceMode::Residuals) {
-        const int64_t rows = layout.trace_rows(), rays = layout.rays_per_variant();
-        auto* res = static_cast<double*>(out_.reserve(V * rows * sizeof(double)));
-        auto* opd = static_cast<double*>(opd_.reserve(V * rays * sizeof(double)));
-        auto* st = static_cast<uint8_t*>(status_.reserve(V * rays));
-        check(mkb_residuals_device(&b, plan->get(), res, rows, opd, st, stream_), "residuals");
-        copy_out(out.residuals, out_, V * rows, stream_);
-        copy_out(out.opd, opd_, V * rays, stream_);
-        copy_out(out.status, status_, V * rays, stream_);
-    } else {
-        const size_t ws = mkb_merit_workspace_bytes(batch.variants(), plan->get());
-        workspace_.reserve(ws);
-        auto* merit = static_cast<double*>(merit_.reserve(V * sizeof(double)));
-        auto* failed = static_cast<int64_t*>(failed_.reserve(V * sizeof(int64_t)));
-        auto* hard = static_cast<int64_t*>(hard_.reserve(V * sizeof(int64_t)));
-        check(mkb_merit_device(&b, plan->get(), merit, failed, hard, workspace_.get(),
-                               workspace_.bytes(), stream_),
-              "merit");
-        copy_out(out.merit, merit_, V, stream_);
-        copy_out(out.failed, failed_, V, stream_);
-        copy_out(out.hard_failed, hard_, V, stream_);
+    std::vector<uint8_t> type;
+    const mkb_device_batch shape = shape_of(batch.topology(), batch.glass, type);
+    // the other mode's buffers stay while the tranche does not shrink because of them
+    const size_t other = merit ? out_.bytes() + opd_.bytes() + status_.bytes()
+                               : merit_.bytes() + failed_.bytes() + hard_.bytes() +
+                                     workspace_.bytes() + extra_.bytes();
+    const size_t available = available_bytes();
+    size_t usable = usable_bytes(available - std::min(other, available));
+    int64_t tranche = tranche_for(usable, shape, plan->get(), settings, merit, granularity);
+    if (other > 0 && tranche < batch.variants()) {
+        const size_t usable_all = usable_bytes(available);
+        const int64_t tranche_all =
+            tranche_for(usable_all, shape, plan->get(), settings, merit, granularity);
+        if (tranche_all > tranche) {
+            if (merit) {
+                out_.release();
+                opd_.release();
+                status_.release();
+            } else {
+                merit_.release();
+                failed_.release();
+                hard_.release();
+                workspace_.release();
+                extra_.release();
+            }
+            tranche = tranche_all;
+            usable = usable_all;
+        }
     }
+    if (tranche < 1)
+        throw CudaError("TraceEngine: not even " +
+                        (granularity == 1 ? std::string("one variant fits")
+                                          : std::to_string(granularity) +
+                                                " variants that belong together fit") +
+                        " into the device memory (available " + std::to_string(available) +
+                        " B, after the reserve " + std::to_string(usable) + " B)");
+    // buffers that are too small go before the new ones come (old and new never coexist)
+    batch_.release();
+    return TranchePlan{static_cast<int>(std::min<int64_t>(tranche, batch.variants())), usable};
+}
+
+DeviceTranche TraceEngine::residual_tranche(const SystemBatchHost& batch,
+                                            const ResidualLayout& layout,
+                                            const TraceSettings& settings, int first,
+                                            int count) {
+    const int64_t rays = layout.rays_per_variant();
+    const int64_t stride = layout.trace_rows() + settings.extra_residuals;
+    const size_t n = static_cast<size_t>(count);
+    batch_.upload(batch, first, count, stream_);
+    const mkb_device_batch b = batch_.c_struct();
+    const auto plan = layout.plan(batch);
+    auto* res = static_cast<double*>(out_.reserve(n * stride * sizeof(double)));
+    auto* st = static_cast<uint8_t*>(status_.reserve(n * rays));
+    double* opd = settings.opd ? static_cast<double*>(opd_.reserve(n * rays * sizeof(double)))
+                               : nullptr;
+    if (settings.extra_residuals > 0)
+        cuda_check(cudaMemsetAsync(res, 0, n * stride * sizeof(double), as_stream(stream_)),
+                   "clear residuals");
+    mkb_trace_options o{};
+    o.pack_rays = settings.pack_rays;
+    check(mkb_residuals_ex_device(&b, plan->get(), &o, res, stride, opd, st, stream_),
+          "residuals");
     synchronize();
+    DeviceTranche t;
+    t.first = first;
+    t.count = count;
+    t.rays_per_variant = rays;
+    t.penalty_rows = layout.trace_rows() - rays;
+    t.stride = stride;
+    t.residuals = res;
+    t.status = st;
+    t.opd = opd;
+    return t;
+}
+
+TraceOutput TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
+                             const TraceSettings& settings) {
+    TraceOutput out;
+    run(batch, mode, settings, out);
+    return out;
+}
+
+void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
+                      const TraceSettings& settings, TraceOutput& out) {
+    check_settings(settings);
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const ResidualLayout layout(batch.topology(), quadrature_of(settings));
+    batch.validate_values();
+    const int V = batch.variants();
+    const bool merit_mode = mode == TraceMode::Merit;
+    if (merit_mode && !settings.extra_merit.empty() &&
+        settings.extra_merit.size() != static_cast<size_t>(V))
+        throw std::invalid_argument("TraceEngine: extra_merit must be empty or hold " +
+                                    std::to_string(V) + " values");
+    const int64_t rays = layout.rays_per_variant();
+    const int64_t stride = layout.trace_rows() + settings.extra_residuals;
+    const size_t rays_total = static_cast<size_t>(V) * rays;
+    out.mode = mode;
+    out.info = TraceRunInfo{};
+    out.info.variants = V;
+    out.residuals = ResidualResult{};
+    out.merit = MeritResult{};
+    if (merit_mode) {
+        out.merit.variants = V;
+        out.merit.rays_per_variant = rays;
+        out.merit.merit.resize(V);
+        out.merit.failed.resize(V);
+        out.merit.hard_failed.resize(V);
+    } else {
+        out.residuals.variants = V;
+        out.residuals.rays_per_variant = rays;
+        out.residuals.penalty_rows = layout.trace_rows() - rays;
+        out.residuals.stride = stride;
+        out.residuals.residuals.resize(static_cast<size_t>(V) * stride);
+        out.residuals.opd.resize(settings.opd ? rays_total : 0);
+        out.residuals.status.resize(settings.status ? rays_total : 0);
+    }
+    out.layout.emplace(layout);
+    if (V == 0) {
+        out.info.device_bytes = device_bytes();
+        return;
+    }
+    const TranchePlan tp = plan_tranches(batch, mode, layout, settings, 1);
+    const auto plan = layout.plan(batch);
+    for (int first = 0; first < V; first += tp.tranche) {
+        const int count = std::min(tp.tranche, V - first);
+        const size_t v0 = static_cast<size_t>(first), n = static_cast<size_t>(count);
+        auto down = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes > 0)
+                cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost,
+                                           as_stream(stream_)),
+                           "download");
+        };
+        if (merit_mode) {
+            batch_.upload(batch, first, count, stream_);
+            const mkb_device_batch b = batch_.c_struct();
+            workspace_.reserve(mkb_merit_workspace_bytes(count, plan->get()));
+            auto* m = static_cast<double*>(merit_.reserve(n * sizeof(double)));
+            auto* f = static_cast<int64_t*>(failed_.reserve(n * sizeof(int64_t)));
+            auto* h = static_cast<int64_t*>(hard_.reserve(n * sizeof(int64_t)));
+            mkb_trace_options o{};
+            o.pack_rays = settings.pack_rays;
+            if (!settings.extra_merit.empty()) {
+                void* e = extra_.reserve(n * sizeof(double));
+                cuda_check(cudaMemcpyAsync(e, settings.extra_merit.data() + v0,
+                                           n * sizeof(double), cudaMemcpyHostToDevice,
+                                           as_stream(stream_)),
+                           "upload extra_merit");
+                o.extra_merit = static_cast<const double*>(e);
+            }
+            check(mkb_merit_ex_device(&b, plan->get(), &o, m, f, h, workspace_.get(),
+                                      workspace_.bytes(), stream_),
+                  "merit");
+            down(out.merit.merit.data() + v0, m, n * sizeof(double));
+            down(out.merit.failed.data() + v0, f, n * sizeof(int64_t));
+            down(out.merit.hard_failed.data() + v0, h, n * sizeof(int64_t));
+            synchronize();
+        } else {
+            const DeviceTranche t = residual_tranche(batch, layout, settings, first, count);
+            down(out.residuals.residuals.data() + v0 * stride, t.residuals,
+                 n * stride * sizeof(double));
+            if (settings.status)
+                down(out.residuals.status.data() + v0 * rays, t.status, n * rays);
+            if (settings.opd)
+                down(out.residuals.opd.data() + v0 * rays, t.opd, n * rays * sizeof(double));
+            synchronize();
+        }
+        ++out.info.tranches;
+    }
+    out.info.tranche_variants = tp.tranche;
+    out.info.budget_bytes = tp.usable;
+    out.info.device_bytes = device_bytes();
+}
+
+TraceRunInfo TraceEngine::run_on_device(const SystemBatchHost& batch,
+                                        const TraceSettings& settings, int granularity,
+                                        const DeviceTrancheFn& consume) {
+    check_settings(settings);
+    if (granularity < 1) throw std::invalid_argument("TraceEngine: granularity must be >= 1");
+    if (!consume) throw std::invalid_argument("TraceEngine: run_on_device without a callback");
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const ResidualLayout layout(batch.topology(), quadrature_of(settings));
+    batch.validate_values();
+    TraceRunInfo info;
+    info.variants = batch.variants();
+    if (info.variants == 0) {
+        info.device_bytes = device_bytes();
+        return info;
+    }
+    const TranchePlan tp =
+        plan_tranches(batch, TraceMode::Residuals, layout, settings, granularity);
+    for (int first = 0; first < info.variants; first += tp.tranche) {
+        const int count = std::min(tp.tranche, info.variants - first);
+        consume(residual_tranche(batch, layout, settings, first, count));
+        cuda_check(cudaDeviceSynchronize(), "tranche callback");
+        ++info.tranches;
+    }
+    info.tranche_variants = tp.tranche;
+    info.budget_bytes = tp.usable;
+    info.device_bytes = device_bytes();
+    return info;
 }
 
 namespace {

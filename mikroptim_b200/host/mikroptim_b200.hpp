@@ -15,9 +15,13 @@
 // cuda::CudaError for device failures -- the reference's exception classes.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <limits>
 #include <memory>
+#include <optional>
+#include <span>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -156,8 +160,13 @@ public:
     const ResidualSettings& settings() const { return settings_; }
     // the plan is heap-allocated so its internal pointers stay valid
     std::unique_ptr<ResidualPlan> plan(const SystemBatchHost& batch) const;
+    // a plan with unit weights, for sizing runs of the topology (sizes ignore the weights)
+    std::unique_ptr<ResidualPlan> plan_for_sizing() const;
 
 private:
+    std::unique_ptr<ResidualPlan> plan_from(const std::vector<double>& field_weight,
+                                            const std::vector<double>& wavelength_weight,
+                                            double reference_wavelength_nm) const;
     BatchTopology topology_;
     ResidualSettings settings_;
     std::vector<int> samples_;
@@ -239,22 +248,98 @@ private:
 };
 
 enum class TraceMode { Residuals, Merit };
+const char* to_string(TraceMode mode);
 
-struct TraceOutput {
-    std::vector<double> residuals;     // RESIDUALS: [V][trace_rows]
-    std::vector<double> opd;           // RESIDUALS: [V][rays]
-    std::vector<uint8_t> status;       // RESIDUALS: [V][rays]
-    std::vector<double> merit;         // MERIT: [V]
-    std::vector<int64_t> failed;       // MERIT: [V]
-    std::vector<int64_t> hard_failed;  // MERIT: [V]
+// MemoryReserve (include/mikroptim/batch/batch_memory.hpp:119): the engine leaves
+// max(min_bytes, fraction * free) of the memory it sees as free untouched.
+struct MemoryReserve {
+    std::size_t min_bytes = std::size_t{256} << 20;
+    double fraction = 0.05;
 };
+
+// EngineOptions (include/mikroptim/cuda/trace_engine.hpp:44): memory_limit_bytes caps the
+// memory the engine regards as available (tranche tests, sharing a GPU).
+struct EngineOptions {
+    std::optional<std::size_t> memory_limit_bytes;
+    MemoryReserve reserve{};
+};
+
+// TraceSettings (trace_engine.hpp:52). opd / status / extra_residuals apply to RESIDUALS (the
+// extra rows follow the ray and penalty rows and are set to 0); extra_merit (empty or one
+// value per variant, valid until run returns) to MERIT, added to each variant's merit after
+// its tuple sums. precision: empty = the quadrature's. pack_rays changes only the run time.
+// extrema (per-surface maxima) is not built: true throws std::logic_error.
+struct TraceSettings {
+    TraceSettings() = default;
+    TraceSettings(const ResidualSettings& q) : quadrature(q) {}  // NOLINT: implicit on purpose
+    ResidualSettings quadrature{};
+    bool opd = false;
+    bool status = true;
+    int64_t extra_residuals = 0;
+    bool extrema = false;
+    std::span<const double> extra_merit{};
+    std::optional<Precision> precision;
+    int pack_rays = 512;
+};
+
+// TraceRunInfo (trace_engine.hpp:93)
+struct TraceRunInfo {
+    int variants = 0;
+    int tranches = 0;
+    int tranche_variants = 0;
+    std::size_t budget_bytes = 0;
+    std::size_t device_bytes = 0;
+};
+
+struct ResidualResult {
+    int variants = 0;
+    int64_t rays_per_variant = 0, penalty_rows = 0, stride = 0;
+    std::vector<double> residuals;  // [V][stride]
+    std::vector<double> opd;        // [V][rays] when requested
+    std::vector<uint8_t> status;    // [V][rays] when requested
+};
+
+struct MeritResult {
+    int variants = 0;
+    int64_t rays_per_variant = 0;
+    std::vector<double> merit;          // [V]
+    std::vector<int64_t> failed;        // [V]
+    std::vector<int64_t> hard_failed;   // [V]
+};
+
+// TraceOutput (trace_engine.hpp:103): the result of the run's mode; the other is empty.
+struct TraceOutput {
+    TraceMode mode = TraceMode::Residuals;
+    std::optional<ResidualLayout> layout;
+    ResidualResult residuals;
+    MeritResult merit;
+    TraceRunInfo info;
+};
+
+// One tranche's RESIDUALS on the device (DeviceTranche, trace_engine.hpp:117); the pointers
+// are the engine's buffers and valid during the callback only.
+struct DeviceTranche {
+    int first = 0;
+    int count = 0;
+    int64_t rays_per_variant = 0;
+    int64_t penalty_rows = 0;
+    int64_t stride = 0;
+    const double* residuals = nullptr;    // [count][stride]
+    const uint8_t* status = nullptr;      // [count][rays]
+    const double* opd = nullptr;          // [count][rays] with settings.opd
+};
+using DeviceTrancheFn = std::function<void(const DeviceTranche&)>;
 
 // Device-resident packed batch (records and surface types).
 class DeviceSystemBatch {
 public:
     DeviceSystemBatch() = default;
     void upload(const SystemBatchHost& batch, void* stream);
+    // variants [first, first + count) only (a tranche)
+    void upload(const SystemBatchHost& batch, int first, int count, void* stream);
     mkb_device_batch c_struct() const { return batch_; }
+    std::size_t capacity_bytes() const { return records_.bytes(); }
+    void release() { records_.release(); }
 
 private:
     mkb_device_batch batch_{};
@@ -264,26 +349,55 @@ private:
     DeviceBuffer records_;
 };
 
+// TraceEngine (include/mikroptim/cuda/trace_engine.hpp:145): host batch in, host results out.
+// A batch is split into tranches that fit the device memory the engine sees (free memory plus
+// its own buffers, at most memory_limit_bytes, less the reserve); buffers are kept across
+// calls. Every variant's results are bit-identical whatever the split.
 class TraceEngine {
 public:
-    explicit TraceEngine(int device = 0);
+    explicit TraceEngine(int device = 0, const EngineOptions& options = {});
     ~TraceEngine();
     TraceEngine(const TraceEngine&) = delete;
     TraceEngine& operator=(const TraceEngine&) = delete;
 
-    // TraceEngine::run: validation, upload, RESIDUALS or MERIT, download
-    void run(const SystemBatchHost& batch, TraceMode mode, const ResidualSettings& settings,
+    void run(const SystemBatchHost& batch, TraceMode mode, const TraceSettings& settings,
              TraceOutput& out);
+    TraceOutput run(const SystemBatchHost& batch, TraceMode mode,
+                    const TraceSettings& settings = {});
+    // RESIDUALS without the download: consume(tranche) after each tranche's kernel; the tranche
+    // size is a multiple of `granularity` (only the last may be smaller).
+    TraceRunInfo run_on_device(const SystemBatchHost& batch, const TraceSettings& settings,
+                               int granularity, const DeviceTrancheFn& consume);
+    // Largest tranche for batches of this topology; 0 when not one variant fits.
+    int max_variants(const BatchTopology& topology, TraceMode mode,
+                     const TraceSettings& settings = {}) const;
     int device() const { return device_; }
+    const std::string& device_name() const { return device_name_; }
+    const EngineOptions& options() const { return options_; }
+    std::size_t device_bytes() const;
     void* stream() const { return stream_; }
-    void release();
+    void release() noexcept;
     void synchronize();
 
 private:
+    struct TranchePlan {
+        int tranche = 0;
+        std::size_t usable = 0;
+    };
+    std::size_t available_bytes() const;
+    std::size_t usable_bytes(std::size_t available) const;
+    TranchePlan plan_tranches(const SystemBatchHost& batch, TraceMode mode,
+                              const ResidualLayout& layout, const TraceSettings& settings,
+                              int granularity);
+    DeviceTranche residual_tranche(const SystemBatchHost& batch, const ResidualLayout& layout,
+                                   const TraceSettings& settings, int first, int count);
+
     int device_;
+    std::string device_name_;
+    EngineOptions options_;
     void* stream_ = nullptr;
     DeviceSystemBatch batch_;
-    DeviceBuffer out_, opd_, status_, merit_, failed_, hard_, workspace_;
+    DeviceBuffer out_, opd_, status_, merit_, failed_, hard_, workspace_, extra_;
 };
 
 // J [runs][P][R] (column p of run i at (i*P + p)*R) and r0 [runs][R] on the host.

@@ -58,7 +58,7 @@ def merit_sharded(batch: SystemBatchHost, settings, group=None) -> dict[str, np.
     engine = TraceEngine(torch.cuda.current_device())
 
     def fn(shard, first):
-        out = engine.run(shard, TraceMode.MERIT, settings)
+        out = engine.run(shard, TraceMode.MERIT, settings).merit
         return {"merit": out.merit, "failed": out.failed, "hard_failed": out.hard_failed}
     return run_sharded(batch, fn, group)
 

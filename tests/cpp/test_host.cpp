@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cuda_runtime.h>
 #include <stdexcept>
 #include <vector>
 
@@ -79,21 +80,70 @@ int main() {
     cuda::TraceEngine engine(0);
     // RESIDUALS and MERIT
     cuda::TraceOutput out;
-    engine.run(batch, cuda::TraceMode::Residuals, settings, out);
+    cuda::TraceSettings with_opd(settings);
+    with_opd.opd = true;
+    engine.run(batch, cuda::TraceMode::Residuals, with_opd, out);
     std::vector<double> res(V * rows), opd(V * rays);
     std::vector<uint8_t> st(V * rays);
     expect(mko_port_residuals(&view, plan->get(), res.data(), opd.data(), st.data(), 1) == 0,
            "oracle residuals");
-    expect(same_bits(out.residuals, res), "RESIDUALS bit-identical to the oracle");
-    expect(same_bits(out.opd, opd), "OPD bit-identical to the oracle");
-    expect(same_bits(out.status, st), "status identical to the oracle");
+    expect(same_bits(out.residuals.residuals, res), "RESIDUALS bit-identical to the oracle");
+    expect(same_bits(out.residuals.opd, opd), "OPD bit-identical to the oracle");
+    expect(same_bits(out.residuals.status, st), "status identical to the oracle");
+    expect(out.info.tranches == 1 && out.merit.merit.empty(), "one tranche, no MERIT result");
+    // tranches: a memory limit that holds a third of the batch gives bit-identical results
+    {
+        size_t per = 0, fixed = 0;
+        mkb_device_batch shape{};
+        std::vector<uint8_t> type;
+        for (SurfaceKind k : batch.topology().type) type.push_back(static_cast<uint8_t>(k));
+        shape.surfaces = batch.surfaces();
+        shape.wavelengths = batch.wavelengths();
+        shape.fields = batch.fields();
+        shape.record_stride = mkb_record_stride(shape.surfaces, shape.wavelengths, shape.fields);
+        shape.type = type.data();
+        expect(mkb_trace_run_bytes(&shape, plan->get(), 0, 0, 1, 0, &per, &fixed) == 0,
+               "run bytes");
+        cuda::EngineOptions opts;
+        opts.memory_limit_bytes = fixed + per * static_cast<size_t>((V + 2) / 3);
+        opts.reserve = cuda::MemoryReserve{0, 0.0};
+        cuda::TraceEngine small(0, opts);
+        expect(small.max_variants(batch.topology(), cuda::TraceMode::Residuals, with_opd) ==
+                   (V + 2) / 3,
+               "max_variants under the memory limit");
+        const cuda::TraceOutput split = small.run(batch, cuda::TraceMode::Residuals, with_opd);
+        expect(split.info.tranches == 3, "three tranches");
+        expect(same_bits(split.residuals.residuals, res) && same_bits(split.residuals.opd, opd) &&
+                   same_bits(split.residuals.status, st),
+               "tranches bit-identical to the oracle");
+        std::vector<double> gathered(V * rows);
+        const cuda::TraceRunInfo info = small.run_on_device(
+            batch, with_opd, 2, [&](const cuda::DeviceTranche& t) {
+                cudaMemcpy(gathered.data() + static_cast<size_t>(t.first) * t.stride,
+                           t.residuals, sizeof(double) * t.count * t.stride,
+                           cudaMemcpyDeviceToHost);
+            });
+        expect(info.tranches >= 3 && info.tranche_variants % 2 == 0, "run_on_device tranches");
+        expect(same_bits(gathered, res), "run_on_device residuals bit-identical");
+    }
     engine.run(batch, cuda::TraceMode::Merit, settings, out);
     std::vector<double> merit(V);
     std::vector<int64_t> failed(V), hard(V);
     expect(mko_port_merit(&view, plan->get(), merit.data(), failed.data(), hard.data(), 1) == 0,
            "oracle merit");
-    expect(same_bits(out.merit, merit), "MERIT bit-identical to the oracle");
-    expect(same_bits(out.failed, failed) && same_bits(out.hard_failed, hard), "failure counts");
+    expect(same_bits(out.merit.merit, merit), "MERIT bit-identical to the oracle");
+    expect(same_bits(out.merit.failed, failed) && same_bits(out.merit.hard_failed, hard),
+           "failure counts");
+    {
+        std::vector<double> extra(V);
+        for (int v = 0; v < V; ++v) extra[v] = 0.25 * v;
+        cuda::TraceSettings with_extra(settings);
+        with_extra.extra_merit = extra;
+        const cuda::TraceOutput m = engine.run(batch, cuda::TraceMode::Merit, with_extra);
+        bool ok = true;
+        for (int v = 0; v < V; ++v) ok = ok && m.merit.merit[v] == merit[v] + extra[v];
+        expect(ok, "extra_merit added after the tuple sums");
+    }
 
     // Jacobians and normal equations
     const VariableSet vars(batch.topology(),

@@ -36,7 +36,7 @@ def test_merit_forward_equals_trace_of_applied_batch():
     host = b.subset(0, b.variants)
     for v in range(b.variants):
         vs.apply(host, v, x0[v] * 1.001)
-    want = engine.TraceEngine(0).run(host, engine.TraceMode.MERIT, lay.settings).merit
+    want = engine.TraceEngine(0).run(host, engine.TraceMode.MERIT, lay.settings).merit.merit
     got = ag.merit(x, prob).cpu().numpy()
     assert np.array_equal(got, want)
 

@@ -106,3 +106,80 @@ def test_merit_workspace_checked():
     plan = lay.plan(b)
     need = lib.mkb_merit_workspace_bytes(2, C.byref(plan))
     assert need >= 2 * 9 * 16
+
+
+def test_usable_bytes_reserve():
+    """usable = free - max(min, fraction * free), at least 0 (usable_bytes,
+    batch_memory.hpp:125); a fraction outside [0, 1] is an argument error."""
+    lib = _capi.lib()
+    out = C.c_size_t(0)
+    gib = 1 << 30
+    assert lib.mkb_usable_bytes(10 * gib, 256 << 20, 0.05, C.byref(out)) == 0
+    assert out.value == 10 * gib - int(0.05 * 10 * gib)
+    assert lib.mkb_usable_bytes(gib, 256 << 20, 0.05, C.byref(out)) == 0
+    assert out.value == gib - (256 << 20)
+    assert lib.mkb_usable_bytes(100 << 20, 256 << 20, 0.05, C.byref(out)) == 0
+    assert out.value == 0
+    assert lib.mkb_usable_bytes(gib, 0, 1.5, C.byref(out)) == _capi.MKB_ERR_ARGUMENT
+
+
+def _shape_and_plan(make=workloads.singlet):
+    from mikroptim_b200.engine import TraceEngine
+    b, st, vs, x0 = make(4)
+    lay = ResidualLayout(b.topology, st)
+    return b, lay, TraceEngine._shape(b.topology, False), lay.plan(b)
+
+
+def test_trace_run_bytes_per_variant():
+    lib = _capi.lib()
+    b, lay, shape, plan = _shape_and_plan()
+    per, fixed = C.c_size_t(0), C.c_size_t(0)
+    rays, rows = lay.rays_per_variant, lay.trace_rows
+    rec = 8 * shape.record_stride
+    assert lib.mkb_trace_run_bytes(C.byref(shape), C.byref(plan), 0, 5, 1, 0, C.byref(per),
+                                   C.byref(fixed)) == 0
+    assert per.value == rec + 8 * (rows + 5) + rays + 8 * rays
+    assert lib.mkb_trace_run_bytes(C.byref(shape), C.byref(plan), 0, 0, 0, 0, C.byref(per),
+                                   C.byref(fixed)) == 0
+    assert per.value == rec + 8 * rows + rays
+    tuples = b.fields * b.wavelengths
+    assert lib.mkb_trace_run_bytes(C.byref(shape), C.byref(plan), 1, 0, 0, 1, C.byref(per),
+                                   C.byref(fixed)) == 0
+    assert per.value == rec + 24 + int(lib.mkb_merit_workspace_bytes(1, C.byref(plan))) + 8
+    assert per.value >= rec + 24 + 16 * tuples + 8
+    assert lib.mkb_trace_run_bytes(C.byref(shape), C.byref(plan), 0, -1, 0, 0, C.byref(per),
+                                   C.byref(fixed)) == _capi.MKB_ERR_ARGUMENT
+
+
+def test_tranche_variants_fit_the_budget():
+    """The tranche is the largest multiple of `granularity` whose buffers fit the usable bytes;
+    0 when not even `granularity` variants fit."""
+    lib = _capi.lib()
+    b, lay, shape, plan = _shape_and_plan()
+    per, fixed = C.c_size_t(0), C.c_size_t(0)
+    lib.mkb_trace_run_bytes(C.byref(shape), C.byref(plan), 0, 0, 1, 0, C.byref(per),
+                            C.byref(fixed))
+    opts = _capi.TraceOptions()
+
+    def tranche(usable, g=1):
+        return lib.mkb_trace_tranche_variants(usable, C.byref(shape), C.byref(plan),
+                                              C.byref(opts), 0, 0, 1, 0, g)
+    assert tranche(fixed.value + 300 * per.value) == 300
+    assert tranche(fixed.value + 300 * per.value - 1) == 299
+    assert tranche(fixed.value + 300 * per.value, 7) == 294
+    assert tranche(fixed.value + 6 * per.value, 7) == 0
+    assert tranche(fixed.value) == 0
+    assert 0 < tranche(1 << 50) <= (2**31 - 1)  # capped by the CTA count of one launch
+    assert tranche(1 << 30, 0) == _capi.MKB_ERR_ARGUMENT
+    opts.pack_rays = -1
+    assert tranche(1 << 30) == _capi.MKB_ERR_ARGUMENT
+
+
+def test_engine_settings_mirror_the_reference():
+    from mikroptim_b200 import engine
+    ts = engine.TraceSettings()
+    assert (ts.opd, ts.status, ts.extra_residuals, ts.extrema, ts.pack_rays) == \
+        (False, True, 0, False, 512)
+    r = engine.MemoryReserve()
+    assert (r.min_bytes, r.fraction) == (256 << 20, 0.05)
+    assert engine.EngineOptions().memory_limit_bytes is None

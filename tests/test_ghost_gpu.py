@@ -41,8 +41,9 @@ def gram_error(a, b):
 def test_residuals_and_merit_bitwise():
     b, st, vs, x0, lay = batch(64)
     eng = engine.TraceEngine(0)
-    r = eng.run(b, engine.TraceMode.RESIDUALS, lay.settings)
-    m = eng.run(b, engine.TraceMode.MERIT, lay.settings)
+    r = eng.run(b, engine.TraceMode.RESIDUALS,
+                engine.TraceSettings(lay.settings, opd=True)).residuals
+    m = eng.run(b, engine.TraceMode.MERIT, lay.settings).merit
     ro, oo, so = po.port().residuals(b, lay, threads=8)
     mo, fo, ho = po.port().merit(b, lay, threads=8)
     assert np.array_equal(r.residuals, ro) and np.array_equal(r.opd, oo)
@@ -98,7 +99,7 @@ def test_decentered_batch_with_ghost_plates_bitwise():
     nc.decenter_tilt[:, 1:, 2:] = 3e-4 * rng.standard_normal((6, b.surfaces - 1, 2))
     lay = ResidualLayout(nc.topology, st)
     db = engine.DeviceSystemBatch(nc)
-    r = engine.TraceEngine(0).run(nc, engine.TraceMode.RESIDUALS, lay.settings)
+    r = engine.TraceEngine(0).run(nc, engine.TraceMode.RESIDUALS, lay.settings).residuals
     ro, oo, so = po.port().residuals(nc, lay, threads=8)
     assert np.array_equal(r.residuals, ro) and np.array_equal(r.status, so)
     Ja, ra, _ = to_np(*engine.adjoint_jacobian_device(db, lay, nc, vs, x0))

@@ -36,8 +36,9 @@ def to_np(*ts):
 def test_residuals_and_merit_bitwise():
     b, st, vs, x0, lay = batch(32)
     eng = engine.TraceEngine(0)
-    r = eng.run(b, engine.TraceMode.RESIDUALS, lay.settings)
-    m = eng.run(b, engine.TraceMode.MERIT, lay.settings)
+    r = eng.run(b, engine.TraceMode.RESIDUALS,
+                engine.TraceSettings(lay.settings, opd=True)).residuals
+    m = eng.run(b, engine.TraceMode.MERIT, lay.settings).merit
     ro, oo, so = po.port().residuals(b, lay, threads=8)
     mo, fo, ho = po.port().merit(b, lay, threads=8)
     assert np.array_equal(r.residuals, ro) and np.array_equal(r.opd, oo)

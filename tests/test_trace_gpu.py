@@ -30,13 +30,14 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 def gpu_residuals(b, lay):
     eng = engine.TraceEngine(0)
-    out = eng.run(b, engine.TraceMode.RESIDUALS, lay.settings)
+    out = eng.run(b, engine.TraceMode.RESIDUALS,
+                  engine.TraceSettings(lay.settings, opd=True)).residuals
     return out.residuals, out.opd, out.status
 
 
 def gpu_merit(b, lay):
     eng = engine.TraceEngine(0)
-    out = eng.run(b, engine.TraceMode.MERIT, lay.settings)
+    out = eng.run(b, engine.TraceMode.MERIT, lay.settings).merit
     return out.merit, out.failed, out.hard_failed
 
 
