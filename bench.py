@@ -48,6 +48,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "LM iter/s & ray-surface hits/s: adjoint+mixed vs FP64 FD, at ≤1e-4λ OPD err"
 WORKLOAD = "objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=29 (config 2 shape)"
+WORKLOAD_SINGLET = ("singlet-1024: 1024 biconvex singlets (stop plane + 2 spheres), L=3, F=3 "
+                    "(axis 6 rays, two Half 6x12 fields: 150 rays per wavelength), soft "
+                    "failures (config 1 shape)")
 WORKLOAD_LM = ("objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=32: 14 "
                "curvatures, 15 thicknesses and the first element's Buchdahl glass (n0, nu1, nu2) "
                "(config 2 shape)")
@@ -70,7 +73,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing", "precision"])
+    ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing", "precision",
+                             "singlet"])
     ap.add_argument("--variants", type=int, default=None,
                     help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
                          "otherwise)")
@@ -718,6 +722,197 @@ def run_uneven(args, world, rank, local):
     }, None
 
 
+def run_singlet(args, world, rank, local):
+    """Configuration 1: FP64 RESIDUALS + MERIT of 1,024 singlets. One evaluation is ~0.3
+    GFLOP-eq (microseconds of GPU work), so a step is one CUDA-graph replay of many
+    back-to-back evaluations (each: RESIDUALS with OPD and status, then MERIT), with the L2
+    flushed between steps; beside it the same rate over a sweep of batch sizes."""
+    import torch
+    from mikroptim_b200 import _capi, engine, workloads
+    from mikroptim_b200.batch import PRECISION_FP64, PRECISION_FP64_FMA, ResidualLayout
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def graph_of(V, precision, evals, seed):
+        """A CUDA graph of `evals` evaluations of V singlets (outputs preallocated)."""
+        b, st, vs, x0 = workloads.singlet(V, seed=seed)
+        st.precision = precision
+        lay = ResidualLayout(b.topology, st)
+        db = engine.DeviceSystemBatch(b, dev)
+        rows, rays = lay.trace_rows, lay.rays_per_variant
+        res = torch.empty((V, rows), dtype=torch.float64, device=dev)
+        opd = torch.empty((V, rays), dtype=torch.float64, device=dev)
+        stat = torch.empty((V, rays), dtype=torch.uint8, device=dev)
+        merit = torch.empty(V, dtype=torch.float64, device=dev)
+        failed = torch.empty(V, dtype=torch.int64, device=dev)
+        hard = torch.empty(V, dtype=torch.int64, device=dev)
+        plan = lay.plan(b)
+        ws = torch.empty(int(lib.mkb_merit_workspace_bytes(V, C.byref(plan))), dtype=torch.uint8,
+                         device=dev)
+        bst = db.c_struct()
+        opts = engine._trace_options(0)
+
+        def one():
+            h = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            _capi.check(lib.mkb_residuals_ex_device(
+                C.byref(bst), C.byref(plan), C.byref(opts), C.c_void_p(res.data_ptr()), rows,
+                C.c_void_p(opd.data_ptr()), C.c_void_p(stat.data_ptr()), h), "residuals")
+            _capi.check(lib.mkb_merit_ex_device(
+                C.byref(bst), C.byref(plan), C.byref(opts), C.c_void_p(merit.data_ptr()),
+                C.c_void_p(failed.data_ptr()), C.c_void_p(hard.data_ptr()),
+                C.c_void_p(ws.data_ptr()), ws.numel(), h), "merit")
+
+        for _ in range(2):
+            one()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        l0 = lib.mkb_launch_count()
+        with torch.cuda.graph(g):
+            for _ in range(evals):
+                one()
+        per_graph = lib.mkb_launch_count() - l0
+        torch.cuda.synchronize()
+        keep = (b, lay, db, res, opd, stat, merit, failed, hard, ws, plan, bst, opts)
+        hits = 2 * V * rays * (b.surfaces - 1) * evals  # RESIDUALS and MERIT trace each ray
+        flopeq = 2 * V * rays * FLOPEQ_PER_RAY_SURFACE * (b.surfaces - 1 + 2) * evals
+        return g, per_graph, hits, flopeq, keep
+
+    def time_graph(g, steps, warmup):
+        for _ in range(warmup):
+            g.replay()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in times) / steps
+
+    V = args.variants or 1024
+    evals = max(1, 102400 // V)
+    seed = 20261203 + 1 + 1000 * rank
+    g, per_graph, hits, flopeq, keep = graph_of(V, PRECISION_FP64, evals, seed)
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        ms_step = time_graph(g, args.steps, args.warmup)
+    ms_step = max_over_ranks(ms_step, world, dev)
+    value = world * hits / (ms_step / 1e3)
+    b = keep[0]
+    lay = keep[1]
+    del g, keep
+
+    # FP64 with contraction on the same batches, and the size sweep (both precisions)
+    sweep = []
+    fma_value = None
+    for n in (1024, 8192, 65536, 262144):
+        ev = max(1, 102400 // n)
+        row = {"variants": n, "evaluations_per_replay": ev}
+        for name, prec in (("fp64", PRECISION_FP64), ("fp64_fma", PRECISION_FP64_FMA)):
+            gg, _, hh, ff, kk = graph_of(n, prec, ev, seed)
+            ms = time_graph(gg, 3, 2)
+            row[name] = {"ray_surface_hits_per_s": hh / (ms / 1e3),
+                         "tflopeq_per_s": ff / (ms / 1e3) / 1e12, "ms_per_replay": ms}
+            if n == V and prec == PRECISION_FP64_FMA:
+                fma_value = world * hh / (ms / 1e3)
+            del gg, kk
+            torch.cuda.empty_cache()
+        sweep.append(row)
+
+    # end to end through the public API: host batch in, host residuals / OPD / status and merit
+    # out, tranche planning included (TraceEngine.run RESIDUALS then MERIT)
+    eng = engine.TraceEngine(local)
+    ts = engine.TraceSettings(lay.settings, opd=True)
+    for _ in range(2):
+        eng.run(b, engine.TraceMode.RESIDUALS, ts)
+        eng.run(b, engine.TraceMode.MERIT, ts)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.run(b, engine.TraceMode.RESIDUALS, ts)
+        eng.run(b, engine.TraceMode.MERIT, ts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+    rays = lay.rays_per_variant
+    stride = int(lib.mkb_record_stride(3, 3, 3))
+
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved = flopeq / (ms_step / 1e3) / 1e12
+    if rank != 0:
+        return None, None
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": "ray-surface hits/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-1 shapes)",
+        "config": {"workload": WORKLOAD_SINGLET,
+                   "step": f"one CUDA-graph replay of {evals} back-to-back evaluations, each "
+                           "RESIDUALS (with OPD and status) then MERIT of every variant",
+                   "precision": "FP64, every operation separately rounded (bit-identical to "
+                                "the reference CPU)",
+                   "variants_per_gpu": V, "rays_per_variant": rays,
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(per_graph * args.steps),
+        "fp64_fma": {"value": fma_value, "unit": "ray-surface hits/s"},
+        "size_sweep": sweep,
+        "e2e": {"value": world * (hits / evals) / (e2e_ms / 1e3), "unit": "ray-surface hits/s",
+                "h2d_bytes_per_step": int(2 * V * stride * 8),
+                "d2h_bytes_per_step": int(V * (lay.trace_rows * 8 + rays * 9) + V * 24),
+                "path": "TraceEngine.run(RESIDUALS, opd=True) + TraceEngine.run(MERIT) from a "
+                        "host SystemBatchHost, one evaluation per step"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "trace_kernel<1, 0, 0> + trace_kernel<0, 0, 0> + "
+                               "merit_finalize_kernel (graph replay)",
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "flop_model": "2 traces x 140 (S-1+2) FLOP-eq per ray"},
+        "clocks": clocks.summary(),
+    }, None
+
+
+def cpu_baseline_singlet(variants: int = 1024, seed: int = 20261203 + 1):
+    """The reference's own residuals_cpu + merit_cpu (oracle/_ref, or the C restatement when
+    the reference build is missing) over all host threads, repeated for about 2 s."""
+    import oracle.pyoracle as po
+    from mikroptim_b200 import workloads
+    from mikroptim_b200.batch import ResidualLayout
+    b, st, vs, x0 = workloads.singlet(variants, seed=seed)
+    lay = ResidualLayout(b.topology, st)
+    kind = reference_kind()
+    impl = po.reference() if kind == "reference" else po.port()
+    threads = os.cpu_count() or 1
+    impl.residuals(b, lay, threads=threads)
+    impl.merit(b, lay, threads=threads)
+    reps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < 2.0:
+        impl.residuals(b, lay, threads=threads)
+        impl.merit(b, lay, threads=threads)
+        reps += 1
+    dt = time.perf_counter() - t0
+    hits = 2 * b.variants * lay.rays_per_variant * (b.surfaces - 1) * reps
+    return {"value": hits / dt, "unit": "ray-surface hits/s", "cores": threads, "kind": kind,
+            "sample": f"residuals_cpu + merit_cpu of the {variants} singlets, {reps} times, "
+                      f"{dt:.2f} s"}
+
+
 # ---- CPU baselines (oracle) ----------------------------------------------------------------
 def cpu_baseline(kind: str, sample_variants: int = 16, seed: int = 20261203 + 2):
     """The reference's own CPU merit (oracle/_ref) or the C restatement, on all host threads,
@@ -842,6 +1037,21 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": v, "unit": "LM run-iterations/s", "cores": base["cores"],
                              "kind": kind, "sample": base["sample"]},
             "e2e": {"value": v, "unit": "LM run-iterations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+    if args.workload == "singlet":
+        base = cpu_baseline_singlet()
+        v = base["value"]
+        return {
+            "metric": METRIC, "value": v, "unit": "ray-surface hits/s", "impl": "reference",
+            "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, configuration-1 shapes)",
+            "config": {"workload": WORKLOAD_SINGLET,
+                       "step": "residuals_cpu + merit_cpu of the 1024 singlets on the host"},
+            "cpu_baseline": {"value": v, "unit": "ray-surface hits/s", "cores": base["cores"],
+                             "kind": base["kind"], "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "ray-surface hits/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
     samples = []
@@ -1174,6 +1384,13 @@ def main():
         if rank == 0 and world == 1:
             try:
                 out["cpu_baseline"] = cpu_baseline_tolerancing()
+            except Exception as e:  # the baseline is reported, not required
+                out["cpu_baseline"] = {"value": None, "error": str(e)}
+    elif args.workload == "singlet":
+        out, _ = run_singlet(args, world, rank, local)
+        if rank == 0 and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline_singlet()
             except Exception as e:  # the baseline is reported, not required
                 out["cpu_baseline"] = {"value": None, "error": str(e)}
     elif args.workload == "lm":

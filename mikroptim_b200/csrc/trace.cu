@@ -33,7 +33,8 @@ constexpr int kTraceBlocksPerSm = 9;
 
 // The variant's record (the bulk-copy destination, 16-byte aligned), the mu table and the
 // pack's per-ray OPL, penalty and status live in dynamic shared memory sized for the batch
-// (trace_smem): record [stride] | mu [S][L] | opl [pack_max] | pen [pack_max] | status.
+// (trace_smem): record [stride] | mu [S][L] | opl [pack_max] | pen [pack_max] |
+// [FP64: piston terms w [pack_max] | w * opl [pack_max]] | status.
 struct alignas(16) SharedTrace {
     uint64_t bar;
     SharedTables tab;
@@ -155,7 +156,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     double* mu_tab = dyn + p.stride;      // [S][L]
     double* opl_sh = mu_tab + p.S * p.L;  // [pack_max]
     double* pen_sh = opl_sh + p.pack_max; // [pack_max]
-    uint8_t* status_sh = reinterpret_cast<uint8_t*>(pen_sh + p.pack_max);
+    double* w_sh = pen_sh + p.pack_max;   // FP64 only: [pack_max] piston weights
+    double* ws_sh = w_sh + (kExact ? p.pack_max : 0);  // FP64 only: [pack_max] w * opl
+    uint8_t* status_sh = reinterpret_cast<uint8_t*>(kExact ? ws_sh + p.pack_max : w_sh);
     if (!stage_to_shared(record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
                          &sh.bar))
         return;
@@ -200,14 +203,22 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         // piston: valid weight and weighted OPL sum over the rays in the piston
         double vw = 0.0, vs = 0.0;
         if (kExact) {
+            // Every lane forms its samples' terms w_k and w_k * OPL_k (one rounded product, as
+            // the sequential loop forms it; +0 for rays outside the piston, which leaves the
+            // sums' bits unchanged: both start at +0 and never become -0), then lane 0 adds
+            // them in ascending k: the dependent additions are all it executes alone.
+            for (int k = lane; k < n; k += 32) {
+                const bool in = in_piston(status_sh[base + k]);
+                const N w = in ? N(pupil_sample(p, sh.tab, f, k).weight) : N(0.0);
+                w_sh[base + k] = value_of(w);
+                ws_sh[base + k] = in ? value_of(w * N(opl_sh[base + k])) : 0.0;
+            }
+            __syncwarp();
             if (lane == 0) {
                 N w_acc(0.0), s_acc(0.0);
                 for (int k = 0; k < n; ++k) {
-                    if (in_piston(status_sh[base + k])) {
-                        const N w = pupil_sample(p, sh.tab, f, k).weight;
-                        w_acc += w;
-                        s_acc += w * N(opl_sh[base + k]);
-                    }
+                    w_acc += N(w_sh[base + k]);
+                    s_acc += N(ws_sh[base + k]);
                 }
                 vw = value_of(w_acc);
                 vs = value_of(s_acc);
@@ -254,8 +265,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                 if (out.opd) out.opd[ray] = value_of(e);
                 if (out.status) out.status[ray] = static_cast<uint8_t>(st);
             } else if (kExact) {
-                opl_sh[base + k] = value_of(r);  // each lane rewrites only its own samples
-                pen_sh[base + k] = value_of(pr);
+                // each lane rewrites only its own samples, with the rounded squares
+                opl_sh[base + k] = value_of(r * r);
+                pen_sh[base + k] = value_of(pr * pr);
             } else {
                 sq += value_of(r * r);
                 psq += value_of(pr * pr);
@@ -266,15 +278,9 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                 __syncwarp();
                 if (lane == 0) {  // sum_k r_k^2, then sum_k p_k^2, in ascending k
                     N tuple(0.0), pen(0.0);
-                    for (int k = 0; k < n; ++k) {
-                        const N x = opl_sh[base + k];
-                        tuple += x * x;
-                    }
+                    for (int k = 0; k < n; ++k) tuple += N(opl_sh[base + k]);
                     if (soft_mode) {
-                        for (int k = 0; k < n; ++k) {
-                            const N x = pen_sh[base + k];
-                            pen += x * x;
-                        }
+                        for (int k = 0; k < n; ++k) pen += N(pen_sh[base + k]);
                         tuple += pen;
                     }
                     sq = value_of(tuple);
@@ -321,9 +327,9 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
 
 // dynamic shared memory of trace_kernel: the record (stride is even), the mu table and the
 // pack's per-ray OPL, penalty and status
-size_t trace_smem(const TraceParams& p) {
+size_t trace_smem(const TraceParams& p, bool exact) {
     return (static_cast<size_t>(p.stride) + static_cast<size_t>(p.S) * p.L +
-            2 * static_cast<size_t>(p.pack_max)) * sizeof(double) +
+            (exact ? 4 : 2) * static_cast<size_t>(p.pack_max)) * sizeof(double) +
            ((static_cast<size_t>(p.pack_max) + 15) & ~size_t(15));
 }
 
@@ -333,7 +339,7 @@ template <bool kResiduals>
 int launch_trace(const TraceParams& p, const double* records, const TupleOut& out, int precision,
                  cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
-    const size_t smem = trace_smem(p);
+    const size_t smem = trace_smem(p, precision == MKB_PRECISION_FP64);
     // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
     const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
     constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
