@@ -47,7 +47,7 @@ class DeviceSystemBatch:
     TraceEngine, place the records in memory it already holds when it is large enough."""
 
     def __init__(self, batch: SystemBatchHost, device="cuda", stream=None,
-                 storage: torch.Tensor | None = None):
+                 storage: torch.Tensor | None = None, staging: torch.Tensor | None = None):
         self.device = _require_cuda(device)
         lib = _capi.lib()
         batch.validate_values()
@@ -62,10 +62,20 @@ class DeviceSystemBatch:
                                                     batch.fields, self.non_coaxial,
                                                     self.ghost_plates, self.ghost_terms,
                                                     self.glass))
-        host = np.zeros((max(batch.variants, 1), self.stride))
+        n_host = max(batch.variants, 1) * self.stride
+        if staging is not None and staging.numel() >= n_host and staging.is_pinned():
+            # a caller's pinned buffer, reused across calls (pinning memory is slow)
+            self.host_records = staging[:n_host].view(-1, self.stride)
+            host = self.host_records.numpy()
+            host.fill(0.0)
+        else:
+            host = np.zeros((max(batch.variants, 1), self.stride))
+            self.host_records = None
         view = batch.view()
         _capi.check(lib.mkb_pack_batch_host(C.byref(view), _capi.ptr(host)), "pack batch")
-        self.host_records = torch.from_numpy(host[:batch.variants]).pin_memory()
+        if self.host_records is None:
+            self.host_records = torch.from_numpy(host).pin_memory()
+        self.host_records = self.host_records[:batch.variants]
         n = max(batch.variants, 1) * self.stride
         if storage is not None and storage.numel() >= 8 * n and storage.device == self.device:
             self.records = storage[:8 * n].view(torch.float64).view(-1, self.stride)
@@ -303,6 +313,13 @@ class TraceEngine:
         self._usable(0)  # checks the reserve (ValueError for a fraction outside [0, 1])
         self.device_name = torch.cuda.get_device_name(self.device)
         self._buffers: dict[str, torch.Tensor] = {}
+        self._staging: torch.Tensor | None = None  # pinned host records, grown on demand
+        self._last_usable = 0
+
+    def _host_staging(self, doubles: int) -> torch.Tensor:
+        if self._staging is None or self._staging.numel() < doubles:
+            self._staging = torch.empty(max(int(doubles), 1), dtype=torch.float64).pin_memory()
+        return self._staging
 
     # ---- memory ---------------------------------------------------------------------------
     def device_bytes(self) -> int:
@@ -312,6 +329,7 @@ class TraceEngine:
     def release(self) -> None:
         """Frees every device buffer (the next run allocates them again)."""
         self._buffers.clear()
+        self._last_usable = 0
 
     def _usable(self, available: int) -> int:
         out = C.c_size_t(0)
@@ -401,6 +419,20 @@ class TraceEngine:
         shape = self._shape(batch.topology, batch.buchdahl_coeff is not None,
                             batch.variant_surfaces is not None)
         plan = layout.plan(batch)
+        # A batch whose whole run fits the buffers this mode already holds reuses them without
+        # asking the device (cudaMemGetInfo costs about a millisecond): the previous plan
+        # reserved them within the same limits.
+        per, fixed = C.c_size_t(0), C.c_size_t(0)
+        _capi.check(_capi.lib().mkb_trace_run_bytes(
+            C.byref(shape), C.byref(plan), 1 if merit else 0, int(ts.extra_residuals),
+            1 if ts.opd else 0, 1 if (merit and ts.extra_merit is not None) else 0,
+            C.byref(per), C.byref(fixed)), "run bytes")
+        mine = ("records", "merit", "failed", "hard", "ws", "extra") if merit else \
+            ("records", "res", "status", "opd")
+        held_mine = sum(self._buffers[k].numel() for k in mine if k in self._buffers)
+        if self._last_usable and held_mine >= batch.variants * per.value and \
+                self._last_usable >= fixed.value + batch.variants * per.value:
+            return batch.variants, self._last_usable
         # the other mode's buffers stay while the tranche does not shrink because of them
         other = ("res", "status", "opd") if merit else ("merit", "failed", "hard", "ws", "extra")
         held = sum(self._buffers[k].numel() for k in other if k in self._buffers)
@@ -420,6 +452,7 @@ class TraceEngine:
             raise RuntimeError(f"TraceEngine: not even {what} into the device memory "
                                f"(available {available / 2**20:.1f} MiB, after the reserve "
                                f"{usable / 2**20:.1f} MiB)")
+        self._last_usable = usable
         return min(tranche, batch.variants), usable
 
     # ---- runs -----------------------------------------------------------------------------
@@ -440,21 +473,46 @@ class TraceEngine:
             extra = np.ascontiguousarray(ts.extra_merit, dtype=np.float64).reshape(-1)
             if extra.size != V:
                 raise ValueError(f"TraceEngine: extra_merit must be empty or hold {V} values")
+        reuse = out is not None
         out = out if out is not None else TraceOutput()
         rays = layout.rays_per_variant
         stride = layout.trace_rows + ts.extra_residuals
         out.mode, out.layout = mode, layout
         out.info = TraceRunInfo(variants=V)
+        # A loop that passes its `out` back gets its results in pinned memory that `out` keeps
+        # (downloaded straight into, the reference keeps its vectors' capacity likewise); a
+        # call without `out` gets fresh arrays.
+        pin = out.__dict__.setdefault("_pinned", {})
+
+        def host(name, shape, dtype):
+            n = int(np.prod(shape))
+            if not reuse:
+                return torch.empty(shape, dtype=dtype)
+            t = pin.get(name)
+            if t is None or t.numel() < n or t.dtype != dtype:
+                t = torch.empty(max(n, 1), dtype=dtype).pin_memory()
+                pin[name] = t
+            return t[:n].view(*shape)
+
+        hp = {}
         if merit:
+            hp["merit"] = host("merit", (V,), torch.float64)
+            hp["failed"] = host("failed", (V,), torch.int64)
+            hp["hard"] = host("hard", (V,), torch.int64)
             out.residuals = ResidualResult()
-            out.merit = MeritResult(V, rays, np.zeros(V), np.zeros(V, dtype=np.int64),
-                                    np.zeros(V, dtype=np.int64))
+            out.merit = MeritResult(V, rays, hp["merit"].numpy(), hp["failed"].numpy(),
+                                    hp["hard"].numpy())
         else:
+            hp["res"] = host("res", (V, stride), torch.float64)
+            if ts.opd:
+                hp["opd"] = host("opd", (V, rays), torch.float64)
+            if ts.status:
+                hp["status"] = host("status", (V, rays), torch.uint8)
             out.merit = MeritResult()
             out.residuals = ResidualResult(
-                V, rays, layout.trace_rows - rays, stride, np.zeros((V, stride)),
-                np.zeros((V, rays) if ts.opd else (0, 0)),
-                np.zeros((V, rays) if ts.status else (0, 0), dtype=np.uint8))
+                V, rays, layout.trace_rows - rays, stride, hp["res"].numpy(),
+                hp["opd"].numpy() if ts.opd else np.zeros((0, 0)),
+                hp["status"].numpy() if ts.status else np.zeros((0, 0), dtype=np.uint8))
         if V == 0:
             out.info.device_bytes = self.device_bytes()
             return out
@@ -463,21 +521,21 @@ class TraceEngine:
             for first in range(0, V, tranche):
                 count = min(tranche, V - first)
                 part = batch.subset(first, count) if (first, count) != (0, V) else batch
+                sl = slice(first, first + count)
                 if merit:
                     m = self._merit_tranche(part, layout, ts,
                                             None if extra is None else extra[first:first + count])
-                    torch.cuda.synchronize()
-                    out.merit.merit[first:first + count] = m.merit.cpu().numpy()
-                    out.merit.failed[first:first + count] = m.failed.cpu().numpy()
-                    out.merit.hard_failed[first:first + count] = m.hard_failed.cpu().numpy()
+                    hp["merit"][sl].copy_(m.merit, non_blocking=True)
+                    hp["failed"][sl].copy_(m.failed, non_blocking=True)
+                    hp["hard"][sl].copy_(m.hard_failed, non_blocking=True)
                 else:
                     t = self._residual_tranche(part, layout, ts, first)
-                    torch.cuda.synchronize()
-                    out.residuals.residuals[first:first + count] = t.residuals.cpu().numpy()
+                    hp["res"][sl].copy_(t.residuals, non_blocking=True)
                     if ts.status:
-                        out.residuals.status[first:first + count] = t.status.cpu().numpy()
+                        hp["status"][sl].copy_(t.status, non_blocking=True)
                     if ts.opd:
-                        out.residuals.opd[first:first + count] = t.opd.cpu().numpy()
+                        hp["opd"][sl].copy_(t.opd, non_blocking=True)
+                torch.cuda.current_stream(self.device).synchronize()
                 _device_status()
                 out.info.tranches += 1
             out.info.tranche_variants = tranche
@@ -525,8 +583,9 @@ class TraceEngine:
         n = part.variants
         rays = layout.rays_per_variant
         stride = layout.trace_rows + ts.extra_residuals
-        db = DeviceSystemBatch(part, self.device,
-                               storage=self._buffer("records", 8 * n * self._stride_of(part)))
+        sv = n * self._stride_of(part)
+        db = DeviceSystemBatch(part, self.device, storage=self._buffer("records", 8 * sv),
+                               staging=self._host_staging(sv))
         res = self._buffer("res", 8 * n * stride)[:8 * n * stride].view(torch.float64)
         res = res.view(n, stride)
         st = self._buffer("status", n * rays)[:n * rays].view(n, rays)
@@ -550,8 +609,9 @@ class TraceEngine:
                        extra: np.ndarray | None) -> MeritOutput:
         lib = _capi.lib()
         n = part.variants
-        db = DeviceSystemBatch(part, self.device,
-                               storage=self._buffer("records", 8 * n * self._stride_of(part)))
+        sv = n * self._stride_of(part)
+        db = DeviceSystemBatch(part, self.device, storage=self._buffer("records", 8 * sv),
+                               staging=self._host_staging(sv))
         plan = layout.plan(part)
         ws = self._buffer("ws", int(lib.mkb_merit_workspace_bytes(n, C.byref(plan))))
         merit = self._buffer("merit", 8 * n)[:8 * n].view(torch.float64)

@@ -133,3 +133,24 @@ def test_max_variants_and_out_of_memory():
         engine.TraceEngine(0, engine.EngineOptions(reserve=engine.MemoryReserve(0, 2.0)))
     eng.release()
     assert eng.device_bytes() == 0
+
+
+def test_reused_output_and_fresh_results():
+    """A loop that passes its TraceOutput back gets its results in that object's (pinned)
+    arrays; a call without one gets arrays of its own that later runs leave alone."""
+    b1, st, lay = singlets(64)
+    b2, _, _ = singlets(100)
+    eng = engine.TraceEngine(0)
+    ts = engine.TraceSettings(st, opd=True)
+    fresh1 = eng.run(b1, engine.TraceMode.RESIDUALS, ts).residuals
+    keep = fresh1.residuals.copy()
+    out = engine.TraceOutput()
+    for b in (b1, b2, b1):
+        got = eng.run(b, engine.TraceMode.RESIDUALS, ts, out).residuals
+        want = engine.TraceEngine(0).run(b, engine.TraceMode.RESIDUALS, ts).residuals
+        assert np.array_equal(got.residuals, want.residuals)
+        assert np.array_equal(got.opd, want.opd) and np.array_equal(got.status, want.status)
+        m = eng.run(b, engine.TraceMode.MERIT, ts, out).merit
+        assert np.array_equal(m.merit, engine.TraceEngine(0).run(
+            b, engine.TraceMode.MERIT, ts).merit.merit)
+    assert np.array_equal(fresh1.residuals, keep)
