@@ -354,6 +354,68 @@ int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_pl
 int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                         const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
                         void* workspace, size_t workspace_bytes, void* stream);
+
+/* Extra residual rows (the reference's LmOptions::jacobian.extra, ExtraResiduals evaluated on
+ * the host: paraxial constraints and the like, src/optim/levenberg_marquardt.cpp:659,
+ * extra_rows_untraced in src/optim/adjoint_jacobian.cpp:245). A caller with E such rows runs
+ * each cycle in phases instead of mkb_lm_cycle_device:
+ *   1. mkb_lm_cycle_jacobian_device       trace-row Jacobian and normal equations;
+ *      mkb_lm_points_device               want_jacobian [runs] and x [runs][P]: the runs that
+ *                                          got normal equations and their points;
+ *   2. mkb_lm_extra_rows_device           the caller's rows at those points, J_e [runs][P][E]
+ *                                          (column k of run i at (i*P + k)*E) and r_e
+ *                                          [runs][E] (device), appended after the trace rows:
+ *                                          every entry of [J r]^T [J r] continues its fma chain
+ *                                          over e = 0..E-1 (rows of other runs are not read);
+ *   3. mkb_lm_cycle_step_device           damped step and trial point;
+ *      mkb_lm_points_device               evaluate [runs] and trial [runs][P];
+ *   4. mkb_lm_cycle_accept_device         trial MERIT plus extra_merit[run] = sum_e r_e^2 at
+ *                                          the trial point (device [runs]; read for the runs to
+ *                                          evaluate), then acceptance.
+ * mkb_lm_start_ex_device is mkb_lm_start_device with the extra merit at x0 (device [runs]).
+ * The host FD of the extra rows uses mkb_fd_pattern_host / mkb_fd_derivative_host, the
+ * pattern and formula of the FD Jacobian. */
+int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                           const mkb_variables* vars, const mkb_lm_options* options,
+                           const double* x0, const double* extra_merit, int32_t runs,
+                           void* workspace, size_t workspace_bytes, void* stream);
+int mkb_lm_cycle_jacobian_device(const mkb_device_batch* templates,
+                                 const mkb_residual_plan* plan, const mkb_variables* vars,
+                                 const mkb_lm_options* options, int32_t runs, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+int mkb_lm_extra_rows_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             int32_t runs, void* workspace, size_t workspace_bytes,
+                             const double* jacobian, const double* residuals, int32_t rows,
+                             void* stream);
+int mkb_lm_cycle_step_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             int32_t runs, void* workspace, size_t workspace_bytes,
+                             void* stream);
+int mkb_lm_cycle_accept_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                               const mkb_variables* vars, const mkb_lm_options* options,
+                               int32_t runs, void* workspace, size_t workspace_bytes,
+                               const double* extra_merit, void* stream);
+/* Copies want_jacobian [runs], x [runs][P], evaluate [runs] and trial [runs][P] out of the
+ * workspace (any may be NULL; host or device pointers). */
+int mkb_lm_points_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                         const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                         const void* workspace, int32_t* want_jacobian, double* x,
+                         int32_t* evaluate, double* trial, void* stream);
+
+/* FD pattern of run points on the host (fd_step + fd_pattern, central scheme,
+ * src/optim/variant_generator.cpp:177), the same bits as the device FD Jacobian's: for entry
+ * i*P + k the perturbed values x_a (point_plus) and x_b (point_minus), the steps
+ * d_a = x_a - x and d_b = x_b - x, and the stencil (0 central, 1 one-sided, 2 truncated at a
+ * bound). Host arrays [runs][P]. */
+int mkb_fd_pattern_host(const mkb_variables* vars, const double* x, int32_t runs,
+                        double* point_plus, double* point_minus, double* step_plus,
+                        double* step_minus, int32_t* stencil);
+/* fd_derivative (optim/fd_formula.hpp:40) of `rows` values on the host: column[e] from r0[e]
+ * at x, r_plus[e] at x_a and r_minus[e] at x_b. */
+int mkb_fd_derivative_host(int32_t stencil, double step_plus, double step_minus, int32_t rows,
+                           const double* r0, const double* r_plus, const double* r_minus,
+                           double* column);
 /* Copies the run results out of the workspace (any output may be NULL; host or device
  * pointers): x [runs][P], merit, status, iterations, accepted, jacobians, damping mu,
  * history [runs][max_iterations + 1] (NaN-padded), failed / hard-failed rays, and `running`

@@ -207,6 +207,28 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_lm_cycle_device.restype = c.c_int
     lib.mkb_lm_cycle_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,
                                         c.c_void_p]
+    lib.mkb_lm_start_ex_device.restype = c.c_int
+    lib.mkb_lm_start_ex_device.argtypes = [PB, PP, PV, PO, c.c_void_p, c.c_void_p, c.c_int32,
+                                           c.c_void_p, c.c_size_t, c.c_void_p]
+    for name in ("mkb_lm_cycle_jacobian_device", "mkb_lm_cycle_step_device"):
+        getattr(lib, name).restype = c.c_int
+        getattr(lib, name).argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,
+                                       c.c_void_p]
+    lib.mkb_lm_extra_rows_device.restype = c.c_int
+    lib.mkb_lm_extra_rows_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,
+                                             c.c_void_p, c.c_void_p, c.c_int32, c.c_void_p]
+    lib.mkb_lm_cycle_accept_device.restype = c.c_int
+    lib.mkb_lm_cycle_accept_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p,
+                                               c.c_size_t, c.c_void_p, c.c_void_p]
+    lib.mkb_lm_points_device.restype = c.c_int
+    lib.mkb_lm_points_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_void_p,
+                                         c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
+    lib.mkb_fd_pattern_host.restype = c.c_int
+    lib.mkb_fd_pattern_host.argtypes = [PV, P_double, c.c_int32, P_double, P_double, P_double,
+                                        P_double, C.POINTER(c.c_int32)]
+    lib.mkb_fd_derivative_host.restype = c.c_int
+    lib.mkb_fd_derivative_host.argtypes = [c.c_int32, c.c_double, c.c_double, c.c_int32,
+                                           P_double, P_double, P_double, P_double]
     lib.mkb_lm_results_device.restype = c.c_int
     lib.mkb_lm_results_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p] + \
         [c.c_void_p] * 11 + [c.c_void_p]

@@ -29,7 +29,64 @@ struct FdPattern {
     int pad;
 };
 
-// fd_step + fd_pattern (central), every operation separately rounded.
+__host__ __device__ inline double raw(double a) { return a; }
+__host__ __device__ inline double raw(Exact64 a) { return a.v; }
+
+// fd_step + fd_pattern (central) of one variable (src/optim/variant_generator.cpp:177), every
+// operation separately rounded: Exact64 on the device, plain double on the host (x86-64 without
+// contraction), so both give the same bits.
+template <class N>
+__host__ __device__ inline FdPattern fd_pattern_of(double x0, double lower, double upper,
+                                                   double typical) {
+    const N x = x0;
+    const N lo = lower, up = upper;
+    const double ax = fabs(x0);
+    const N h = N(6.0554544523933395e-06) * N(ax < typical ? typical : ax);
+    const N plus = x + h, minus = x - h;
+    FdPattern out;
+    out.stencil = kCentral;
+    out.pad = 0;
+    N a, b;
+    if (raw(plus) <= raw(up) && raw(minus) >= raw(lo)) {
+        a = plus;
+        b = minus;
+    } else {
+        const bool towards_upper = raw(up - x) >= raw(x - lo);
+        const N two_h = N(2.0) * h;
+        const N far = towards_upper ? x + two_h : x - two_h;
+        if (towards_upper ? raw(far) <= raw(up) : raw(far) >= raw(lo)) {
+            out.stencil = kOneSided;
+            a = towards_upper ? plus : minus;
+            b = far;
+        } else {
+            out.stencil = kTruncated;
+            a = raw(plus) <= raw(up) ? plus : up;
+            b = raw(minus) >= raw(lo) ? minus : lo;
+        }
+    }
+    out.xa = raw(a);
+    out.xb = raw(b);
+    out.da = raw(a - x);
+    out.db = raw(b - x);
+    return out;
+}
+
+// fd_derivative (optim/fd_formula.hpp:40)
+template <class N>
+__host__ __device__ inline double fd_derivative_of(int stencil, double r0, double ra, double rb,
+                                                   double da_, double db_) {
+    const N v0 = r0, va = ra, vb = rb, da = da_, db = db_;
+    N d;
+    if (stencil == kOneSided) {
+        const N ga = va - v0;
+        const N gb = vb - v0;
+        d = (db * db * ga - da * da * gb) / (da * db * (db - da));
+    } else {
+        d = (va - vb) / (da - db);
+    }
+    return raw(d);
+}
+
 // Run i's variable k is entry i * pstride + k (pstride = P, or the largest P of an uneven batch
 // whose run i uses vt[i]).
 __global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const double* x0, int runs,
@@ -39,38 +96,7 @@ __global__ void fd_pattern_kernel(const __grid_constant__ VarParams vp, const do
     const int run = id / pstride, k = id - run * pstride;
     const VarParams& v = vt != nullptr ? vt[run] : vp;
     if (k >= v.P) return;
-    const Exact64 x = x0[id];
-    const Exact64 lo = v.lower[k], up = v.upper[k];
-    const double ax = fabs(x.v);
-    const double typ = v.typical[k];
-    const Exact64 h = Exact64(6.0554544523933395e-06) * Exact64(ax < typ ? typ : ax);
-    const Exact64 plus = x + h, minus = x - h;
-    FdPattern out;
-    out.stencil = kCentral;
-    out.pad = 0;
-    Exact64 a, b;
-    if (plus.v <= up.v && minus.v >= lo.v) {
-        a = plus;
-        b = minus;
-    } else {
-        const bool towards_upper = (up - x).v >= (x - lo).v;
-        const Exact64 two_h = Exact64(2.0) * h;
-        const Exact64 far = towards_upper ? x + two_h : x - two_h;
-        if (towards_upper ? far.v <= up.v : far.v >= lo.v) {
-            out.stencil = kOneSided;
-            a = towards_upper ? plus : minus;
-            b = far;
-        } else {
-            out.stencil = kTruncated;
-            a = plus.v <= up.v ? plus : up;
-            b = minus.v >= lo.v ? minus : lo;
-        }
-    }
-    out.xa = a.v;
-    out.xb = b.v;
-    out.da = (a - x).v;
-    out.db = (b - x).v;
-    pattern[id] = out;
+    pattern[id] = fd_pattern_of<Exact64>(x0[id], v.lower[k], v.upper[k], v.typical[k]);
 }
 
 // One CTA per FD variant j of run i (variant i*n + j, n = 2 pstride + 1): template record, x0
@@ -135,19 +161,9 @@ __global__ void fd_difference_kernel(const double* __restrict__ res, const FdPat
             continue;
         }
         const FdPattern p = pat[static_cast<int64_t>(run) * P + c];
-        const N v0 = base[r];
-        const N va = base[static_cast<int64_t>(2 * c + 1) * R + r];
-        const N vb = base[static_cast<int64_t>(2 * c + 2) * R + r];
-        const N da = p.da, db = p.db;
-        N d;
-        if (p.stencil == kOneSided) {
-            const N ga = va - v0;
-            const N gb = vb - v0;
-            d = (db * db * ga - da * da * gb) / (da * db * (db - da));
-        } else {
-            d = (va - vb) / (da - db);
-        }
-        J[(static_cast<int64_t>(run) * P + c) * R + r] = value_of(d);
+        J[(static_cast<int64_t>(run) * P + c) * R + r] = fd_derivative_of<N>(
+            p.stencil, base[r], base[static_cast<int64_t>(2 * c + 1) * R + r],
+            base[static_cast<int64_t>(2 * c + 2) * R + r], p.da, p.db);
     }
 }
 
@@ -428,6 +444,45 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
 }  // namespace mkb
 
 extern "C" {
+
+int mkb_fd_pattern_host(const mkb_variables* vars, const double* x, int32_t runs,
+                        double* point_plus, double* point_minus, double* step_plus,
+                        double* step_minus, int32_t* stencil) {
+    if (vars == nullptr || vars->count < 1 || vars->lower == nullptr || vars->upper == nullptr ||
+        vars->typical == nullptr || x == nullptr || runs < 0 || point_plus == nullptr ||
+        point_minus == nullptr || step_plus == nullptr || step_minus == nullptr ||
+        stencil == nullptr) {
+        set_error("fd pattern: null argument or no variables");
+        return MKB_ERR_ARGUMENT;
+    }
+    const int P = vars->count;
+    for (int64_t i = 0; i < static_cast<int64_t>(runs) * P; ++i) {
+        const int k = static_cast<int>(i % P);
+        const FdPattern f = fd_pattern_of<double>(x[i], vars->lower[k], vars->upper[k],
+                                                  vars->typical[k]);
+        point_plus[i] = f.xa;
+        point_minus[i] = f.xb;
+        step_plus[i] = f.da;
+        step_minus[i] = f.db;
+        stencil[i] = f.stencil;
+    }
+    return MKB_OK;
+}
+
+int mkb_fd_derivative_host(int32_t stencil, double step_plus, double step_minus, int32_t rows,
+                           const double* r0, const double* r_plus, const double* r_minus,
+                           double* column) {
+    if (rows < 0 || (rows > 0 && (r0 == nullptr || r_plus == nullptr || r_minus == nullptr ||
+                                  column == nullptr)) ||
+        stencil < kCentral || stencil > kTruncated) {
+        set_error("fd derivative: bad arguments");
+        return MKB_ERR_ARGUMENT;
+    }
+    for (int e = 0; e < rows; ++e)
+        column[e] = fd_derivative_of<double>(stencil, r0[e], r_plus[e], r_minus[e], step_plus,
+                                             step_minus);
+    return MKB_OK;
+}
 
 size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
                                        const mkb_residual_plan* plan, int32_t P, int32_t runs,

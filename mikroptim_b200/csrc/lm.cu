@@ -414,6 +414,31 @@ __global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* 
     st.want_jacobian[run] = wants_jacobian(st, run, o.max_iterations);
 }
 
+// Rows of the caller's own (the reference's extra residuals, appended after the trace rows):
+// every entry of [J r]^T [J r] of the runs that got normal equations in this cycle continues
+// its chain over the extra rows e = 0 .. E-1, acc = fma(u_e, v_e, acc), as the reference's
+// normal_equations_host does over all rows in ascending order. je [runs][pstride][E] (column
+// k of run i at (i * pstride + k) * E), re [runs][E].
+__global__ void gram_extend_kernel(const VarParams v, LmState st, double* __restrict__ gram,
+                                   const double* __restrict__ je, const double* __restrict__ re,
+                                   int E, int runs) {
+    const int run = blockIdx.x;
+    if (run >= runs || !st.want_jacobian[run]) return;
+    const int n = st.vt != nullptr ? st.vt[run].P : v.P;
+    const int64_t ps = st.pstride;
+    double* G = gram + run * (ps + 1) * (ps + 1);
+    const double* col = je + run * ps * E;
+    const double* r = re + static_cast<int64_t>(run) * E;
+    for (int e = threadIdx.x; e < (n + 1) * (n + 1); e += blockDim.x) {
+        const int q = e / (n + 1), p = e - q * (n + 1);
+        const double* u = q < n ? col + static_cast<int64_t>(q) * E : r;
+        const double* w = p < n ? col + static_cast<int64_t>(p) * E : r;
+        double acc = G[e];
+        for (int k = 0; k < E; ++k) acc = fma(u[k], w[k], acc);
+        G[e] = acc;
+    }
+}
+
 }  // namespace
 
 int launch_lm_init(const LmOptionsDev& o, const LmState& st, int P, const double* x0, int runs,
@@ -440,6 +465,14 @@ int launch_lm_accept(const LmOptionsDev& o, const LmState& st, int P, const doub
 }
 
 MKB_DEFINE_ERROR_READER(lm_device_error)
+
+int launch_gram_extend(const VarParams& v, const LmState& st, double* gram, const double* je,
+                       const double* re, int E, int runs, cudaStream_t stream) {
+    if (runs <= 0 || E <= 0) return MKB_OK;
+    gram_extend_kernel<<<runs, 256, 0, stream>>>(v, st, gram, je, re, E, runs);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "lm extra rows launch");
+}
 
 }  // namespace mkb
 
@@ -660,13 +693,15 @@ RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* te
 // merit at the run points `x` (applied to the templates) into merit/failed/hard
 int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates,
                 const double* x, int runs, double* merit, int64_t* failed, int64_t* hard,
-                cudaStream_t stream, const int* run_mask = nullptr) {
+                cudaStream_t stream, const int* run_mask = nullptr,
+                const double* extra_merit = nullptr) {
     const RecordLayout lay = layout_of(s.tp);
     int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
                           stream, run_vars(s, L, templates));
     if (rc != MKB_OK) return rc;
     return launch_merit(run_params(s, L), L.records, merit, failed, hard, L.merit_ws,
-                        L.merit_ws_bytes, s.precision, stream, RunMask{run_mask, 1, 0});
+                        L.merit_ws_bytes, s.precision, stream, RunMask{run_mask, 1, 0},
+                        extra_merit);
 }
 
 // Processing order of the runs: those with at most kSmallP variables first (their fused
@@ -702,75 +737,36 @@ __global__ void order_kernel(const uint8_t* __restrict__ vsurf, const VarParams*
     for (int r = threadIdx.x; r < runs; r += blockDim.x) order[atomicAdd(&start[key(r)], 1)] = r;
 }
 
-}  // namespace
-}  // namespace mkb
-
-using namespace mkb;
-
-extern "C" {
-
-size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,
-                              const mkb_variables* vars, const mkb_lm_options* options,
-                              int32_t runs) {
+// Everything a phase of a cycle needs, checked once.
+struct LmCall {
     LmSetup s;
-    if (lm_setup(templates, plan, vars, options, runs, s) != MKB_OK) return 0;
-    return lm_layout(nullptr, s, runs, templates, plan).total;
-}
+    LmLayout L;
+};
 
-int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
-                        const mkb_variables* vars, const mkb_lm_options* options,
-                        const double* x0, int32_t runs, void* workspace, size_t workspace_bytes,
-                        void* stream_ptr) {
-    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    LmSetup s;
-    std::vector<VarParams> table;
-    int rc = lm_setup(templates, plan, vars, options, runs, s, &table);
+int lm_call(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+            const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+            void* workspace, size_t workspace_bytes, LmCall& c,
+            std::vector<VarParams>* table = nullptr) {
+    int rc = lm_setup(templates, plan, vars, options, runs, c.s, table);
     if (rc != MKB_OK) return rc;
-    const LmLayout L = lm_layout(static_cast<char*>(workspace), s, runs, templates, plan);
-    if (workspace == nullptr || workspace_bytes < L.total || x0 == nullptr) {
-        set_error("lm: workspace of %zu bytes and x0 needed", L.total);
+    c.L = lm_layout(static_cast<char*>(workspace), c.s, runs, templates, plan);
+    if (workspace == nullptr || workspace_bytes < c.L.total) {
+        set_error("lm: workspace of %zu bytes needed", c.L.total);
         return MKB_ERR_WORKSPACE;
     }
-    if (L.vt != nullptr) {  // pageable source: the copy has consumed it when the call returns
-        rc = cuda_status(cudaMemcpyAsync(L.vt, table.data(), sizeof(VarParams) * table.size(),
-                                         cudaMemcpyHostToDevice, stream),
-                         "lm: upload variables");
-        if (rc != MKB_OK) return rc;
-    }
-    if (L.order != nullptr) {  // surface counts of the runs' records, then their order
-        const RecordLayout lay = layout_of(s.tp);
-        rc = launch_apply(s.vp, lay, templates->records, templates->variants, x0, L.records, runs,
-                          stream, run_vars(s, L, templates));
-        if (rc != MKB_OK) return rc;
-        order_kernel<<<1, 1024, 0, stream>>>(L.vsurf, L.vt, s.vp.P, runs, s.tp.S, L.order,
-                                             L.split);
-        count_launch();
-        rc = cuda_status(cudaGetLastError(), "lm order launch");
-        if (rc != MKB_OK) return rc;
-    }
-    rc = lm_merit_at(s, L, templates, x0, runs, L.st.merit, L.st.failed, L.st.hard, stream);
-    if (rc != MKB_OK) return rc;
-    rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
-    if (rc != MKB_OK) return rc;
-    return launch_lm_init(s.o, L.st, s.pmax, x0, runs, stream);
+    return MKB_OK;
 }
 
-int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
-                        const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
-                        void* workspace, size_t workspace_bytes, void* stream_ptr) {
-    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    LmSetup s;
-    int rc = lm_setup(templates, plan, vars, options, runs, s);
-    if (rc != MKB_OK) return rc;
-    const LmLayout L = lm_layout(static_cast<char*>(workspace), s, runs, templates, plan);
-    if (workspace == nullptr || workspace_bytes < L.total) {
-        set_error("lm: workspace of %zu bytes needed", L.total);
-        return MKB_ERR_WORKSPACE;
-    }
+// 1. Jacobian and normal equations at x for the runs whose update will read them
+int phase_jacobian(const LmCall& c, const mkb_device_batch* templates,
+                   const mkb_residual_plan* plan, const mkb_variables* vars, int32_t runs,
+                   cudaStream_t stream) {
+    const LmSetup& s = c.s;
+    const LmLayout& L = c.L;
     const TraceParams tp = run_params(s, L);
     const RunVars rv = run_vars(s, L, templates);
-    // 1. Jacobian and normal equations at x for the runs whose update will read them
     const int* want = L.st.want_jacobian;
+    int rc;
     if (s.fd) {
         rc = fd_jacobian(templates, plan, vars, L.st.x, runs, L.J, L.r0, nullptr, L.fd_ws,
                          L.fd_ws_bytes, stream, want, rv);
@@ -807,21 +803,177 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
             rc = launch_projection(s.tp, s.vp, s.R, L.status, L.J, s.exact, stream);
     }
     if (rc != MKB_OK) return rc;
-    if (!s.fused) {
-        rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream, want, rv);
-        if (rc != MKB_OK) return rc;
-    }
-    // 2. step
-    rc = launch_lm_update(s.vp, s.o, L.st, L.gram, runs, stream);
-    if (rc != MKB_OK) return rc;
-    // 3. trial MERIT, 4. acceptance
-    rc = lm_merit_at(s, L, templates, L.st.trial, runs, L.trial_merit, L.trial_failed,
-                     L.trial_hard, stream, L.st.evaluate);
+    if (!s.fused) rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream,
+                                   want, rv);
+    return rc;
+}
+
+// 3. trial MERIT (+ the caller's extra merit), 4. acceptance
+int phase_accept(const LmCall& c, const mkb_device_batch* templates, int32_t runs,
+                 const double* extra_merit, cudaStream_t stream) {
+    const LmSetup& s = c.s;
+    const LmLayout& L = c.L;
+    int rc = lm_merit_at(s, L, templates, L.st.trial, runs, L.trial_merit, L.trial_failed,
+                         L.trial_hard, stream, L.st.evaluate, extra_merit);
     if (rc != MKB_OK) return rc;
     rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
     if (rc != MKB_OK) return rc;
     return launch_lm_accept(s.o, L.st, s.vp.P, L.trial_merit, L.trial_failed, L.trial_hard, runs,
                             stream);
+}
+
+}  // namespace
+}  // namespace mkb
+
+using namespace mkb;
+
+extern "C" {
+
+size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                              const mkb_variables* vars, const mkb_lm_options* options,
+                              int32_t runs) {
+    LmSetup s;
+    if (lm_setup(templates, plan, vars, options, runs, s) != MKB_OK) return 0;
+    return lm_layout(nullptr, s, runs, templates, plan).total;
+}
+
+int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                           const mkb_variables* vars, const mkb_lm_options* options,
+                           const double* x0, const double* extra_merit, int32_t runs,
+                           void* workspace, size_t workspace_bytes, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmCall c;
+    std::vector<VarParams> table;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c, &table);
+    if (rc != MKB_OK) return rc;
+    const LmSetup& s = c.s;
+    const LmLayout& L = c.L;
+    if (x0 == nullptr) {
+        set_error("lm: x0 is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    if (L.vt != nullptr) {  // pageable source: the copy has consumed it when the call returns
+        rc = cuda_status(cudaMemcpyAsync(L.vt, table.data(), sizeof(VarParams) * table.size(),
+                                         cudaMemcpyHostToDevice, stream),
+                         "lm: upload variables");
+        if (rc != MKB_OK) return rc;
+    }
+    if (L.order != nullptr) {  // surface counts of the runs' records, then their order
+        const RecordLayout lay = layout_of(s.tp);
+        rc = launch_apply(s.vp, lay, templates->records, templates->variants, x0, L.records, runs,
+                          stream, run_vars(s, L, templates));
+        if (rc != MKB_OK) return rc;
+        order_kernel<<<1, 1024, 0, stream>>>(L.vsurf, L.vt, s.vp.P, runs, s.tp.S, L.order,
+                                             L.split);
+        count_launch();
+        rc = cuda_status(cudaGetLastError(), "lm order launch");
+        if (rc != MKB_OK) return rc;
+    }
+    rc = lm_merit_at(s, L, templates, x0, runs, L.st.merit, L.st.failed, L.st.hard, stream,
+                     nullptr, extra_merit);
+    if (rc != MKB_OK) return rc;
+    rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
+    if (rc != MKB_OK) return rc;
+    return launch_lm_init(s.o, L.st, s.pmax, x0, runs, stream);
+}
+
+int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options,
+                        const double* x0, int32_t runs, void* workspace, size_t workspace_bytes,
+                        void* stream_ptr) {
+    return mkb_lm_start_ex_device(templates, plan, vars, options, x0, nullptr, runs, workspace,
+                                  workspace_bytes, stream_ptr);
+}
+
+int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                        const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                        void* workspace, size_t workspace_bytes, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    rc = phase_jacobian(c, templates, plan, vars, runs, stream);
+    if (rc != MKB_OK) return rc;
+    rc = launch_lm_update(c.s.vp, c.s.o, c.L.st, c.L.gram, runs, stream);  // 2. step
+    if (rc != MKB_OK) return rc;
+    return phase_accept(c, templates, runs, nullptr, stream);
+}
+
+int mkb_lm_cycle_jacobian_device(const mkb_device_batch* templates,
+                                 const mkb_residual_plan* plan, const mkb_variables* vars,
+                                 const mkb_lm_options* options, int32_t runs, void* workspace,
+                                 size_t workspace_bytes, void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    return phase_jacobian(c, templates, plan, vars, runs, static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_extra_rows_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             int32_t runs, void* workspace, size_t workspace_bytes,
+                             const double* jacobian, const double* residuals, int32_t rows,
+                             void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    if (rows < 0 || (rows > 0 && (jacobian == nullptr || residuals == nullptr))) {
+        set_error("lm extra rows: %d rows, jacobian and residuals needed", rows);
+        return MKB_ERR_ARGUMENT;
+    }
+    return launch_gram_extend(c.s.vp, c.L.st, c.L.gram, jacobian, residuals, rows, runs,
+                              static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_cycle_step_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             int32_t runs, void* workspace, size_t workspace_bytes,
+                             void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    return launch_lm_update(c.s.vp, c.s.o, c.L.st, c.L.gram, runs,
+                            static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_cycle_accept_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                               const mkb_variables* vars, const mkb_lm_options* options,
+                               int32_t runs, void* workspace, size_t workspace_bytes,
+                               const double* extra_merit, void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    return phase_accept(c, templates, runs, extra_merit, static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_points_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                         const mkb_variables* vars, const mkb_lm_options* options, int32_t runs,
+                         const void* workspace, int32_t* want_jacobian, double* x,
+                         int32_t* evaluate, double* trial, void* stream_ptr) {
+    const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    LmSetup s;
+    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    if (rc != MKB_OK) return rc;
+    const LmLayout L = lm_layout(static_cast<char*>(const_cast<void*>(workspace)), s, runs,
+                                 templates, plan);
+    const size_t r = static_cast<size_t>(runs);
+    struct Copy {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } copies[] = {
+        {want_jacobian, L.st.want_jacobian, 4 * r},
+        {x, L.st.x, 8 * r * s.pmax},
+        {evaluate, L.st.evaluate, 4 * r},
+        {trial, L.st.trial, 8 * r * s.pmax},
+    };
+    for (const Copy& cp : copies) {
+        if (cp.dst == nullptr) continue;
+        rc = cuda_status(cudaMemcpyAsync(cp.dst, cp.src, cp.bytes, cudaMemcpyDefault, stream),
+                         "lm points copy");
+        if (rc != MKB_OK) return rc;
+    }
+    return MKB_OK;
 }
 
 int mkb_lm_results_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
