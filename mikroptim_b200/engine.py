@@ -739,11 +739,72 @@ LM_STATUS = {0: "running", 1: "converged_merit", 2: "converged_step", 3: "conver
              7: "numerical_error"}
 
 
+class ExtraResiduals:
+    """ExtraResiduals (include/mikroptim/optim/extra_residuals.hpp): `count` residual rows per
+    variant after the trace rows (paraxial constraints and the like). evaluate(batch, v, out)
+    writes variant v's rows of a SystemBatchHost into out (float64 [count]). The LM takes
+    their Jacobian by central differences on the host, with the FD Jacobian's pattern, and adds
+    sum_e r_e^2 to every merit (extra_rows_untraced, src/optim/adjoint_jacobian.cpp:245;
+    extra_merit_values, src/optim/levenberg_marquardt.cpp:659)."""
+
+    def __init__(self, count: int = 0, evaluate=None):
+        if count < 0 or (count > 0 and evaluate is None):
+            raise ValueError("ExtraResiduals: count >= 0 and an evaluate function needed")
+        self.count = count
+        self.evaluate = evaluate
+
+
+def extra_rows_host(host: SystemBatchHost, variables, x0, extra: ExtraResiduals):
+    """The caller's extra rows at run points x0 [runs][P] on the host (extra_rows_untraced,
+    src/optim/adjoint_jacobian.cpp:245): per run, a one-variant copy of its template (`host`
+    holds 1 variant or one per run), the values r at x and J [P][E] by central differences with
+    the FD Jacobian's pattern (each point applied in full, as the reference does). Returns
+    J [runs][P][E], r [runs][E]."""
+    lib = _capi.lib()
+    P, E = variables.size, extra.count
+    x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, P)
+    runs = x0.shape[0]
+    J = np.zeros((runs, P, E))
+    R = np.zeros((runs, E))
+    vc = variables.c_struct()
+    for i in range(runs):
+        one = host.subset(0 if host.variants == 1 else i, 1)
+
+        def evaluate(y):
+            variables.apply(one, 0, y)
+            out = np.zeros(E)
+            extra.evaluate(one, 0, out)
+            return out
+
+        x = x0[i].copy()
+        xp, xm, dp, dm = (np.zeros(P) for _ in range(4))
+        st = np.zeros(P, dtype=np.int32)
+        _capi.check(lib.mkb_fd_pattern_host(C.byref(vc), _capi.ptr(x), 1, _capi.ptr(xp),
+                                            _capi.ptr(xm), _capi.ptr(dp), _capi.ptr(dm),
+                                            _capi.ptr(st, C.c_int32)), "fd pattern")
+        y = x.copy()
+        r0 = evaluate(y)
+        R[i] = r0
+        for k in range(P):
+            y[k] = xp[k]
+            ra = evaluate(y)
+            y[k] = xm[k]
+            rb = evaluate(y)
+            y[k] = x[k]
+            col = np.zeros(E)
+            _capi.check(lib.mkb_fd_derivative_host(int(st[k]), float(dp[k]), float(dm[k]), E,
+                                                   _capi.ptr(r0), _capi.ptr(ra), _capi.ptr(rb),
+                                                   _capi.ptr(col)), "fd derivative")
+            J[i, k] = col
+    return J, R
+
+
 @dataclass
 class LmOptions:
     """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85). fail_weight_factor and
     max_fail_weight drive the outer soft-failure penalty rounds of optimize_lm_gpu
-    (optimize_lm_rounds, src/optim/levenberg_marquardt.cpp:891); a factor <= 1 gives one pass."""
+    (optimize_lm_rounds, src/optim/levenberg_marquardt.cpp:891); a factor <= 1 gives one pass.
+    extra: the caller's extra residual rows (LmOptions::jacobian.extra), or None."""
 
     max_iterations: int = 100
     ftol: float = 1e-10
@@ -757,6 +818,7 @@ class LmOptions:
     gram_exact: bool = True
     fail_weight_factor: float = 10.0
     max_fail_weight: float = 1e14
+    extra: ExtraResiduals | None = None
 
     def c_struct(self) -> "_capi.LmOptions":
         o = _capi.LmOptions()
@@ -840,16 +902,108 @@ class DeviceLm:
         check_start_points(self.variables, rows)
         x0 = _dev_f64(rows, self.templates.device)
         self._x0 = x0
-        rc = self.lib.mkb_lm_start_device(*self._args(), C.c_void_p(x0.data_ptr()), self.runs,
-                                          C.c_void_p(self.workspace.data_ptr()),
-                                          self.workspace.numel(), _stream_handle(self.stream))
+        extra = None
+        if self._extra_rows():
+            extra = _dev_f64([self._extra_merit(i, rows[i]) for i in range(self.runs)],
+                             self.templates.device)
+        rc = self.lib.mkb_lm_start_ex_device(
+            *self._args(), C.c_void_p(x0.data_ptr()),
+            C.c_void_p(extra.data_ptr()) if extra is not None else None, self.runs,
+            C.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
+            _stream_handle(self.stream))
         _capi.check(rc, "lm start")
 
     def cycle(self) -> None:
+        if self._extra_rows():
+            self._cycle_with_extra_rows()
+            return
         rc = self.lib.mkb_lm_cycle_device(*self._args(), self.runs,
                                           C.c_void_p(self.workspace.data_ptr()),
                                           self.workspace.numel(), _stream_handle(self.stream))
         _capi.check(rc, "lm cycle")
+        self.cycles += 1
+
+    # ---- the caller's extra rows (evaluated on the host) ----------------------------------
+    def _extra_rows(self) -> int:
+        e = self.options.extra
+        return e.count if e is not None else 0
+
+    def _var_set(self, i: int):
+        return self.variables[i] if isinstance(self.variables, (list, tuple)) else self.variables
+
+    def _work_batch(self, i: int) -> SystemBatchHost:
+        """A one-variant copy of run i's template (the reference's working variant)."""
+        cache = self.__dict__.setdefault("_work", {})
+        t = 0 if self.host.variants == 1 else i
+        if t not in cache:
+            cache[t] = self.host.subset(t, 1)
+        return cache[t]
+
+    def _evaluate(self, i: int, y) -> np.ndarray:
+        one = self._work_batch(i)
+        self._var_set(i).apply(one, 0, np.asarray(y, dtype=np.float64))
+        out = np.zeros(self.options.extra.count)
+        self.options.extra.evaluate(one, 0, out)
+        return out
+
+    def _extra_merit(self, i: int, x_row) -> float:
+        """sum_e r_e^2 in row order, each product and sum rounded (extra_merit_values)."""
+        s = 0.0
+        for e in self._evaluate(i, x_row[:self._var_set(i).size]):
+            s = s + e * e
+        return s
+
+    def _extra_jacobian(self, i: int, x_row) -> tuple[np.ndarray, np.ndarray]:
+        """J_e [P][E] and r_e [E] of run i at x (extra_rows_host on its template)."""
+        vs = self._var_set(i)
+        t = 0 if self.host.variants == 1 else i
+        J, r = extra_rows_host(self.host.subset(t, 1), vs, x_row[:vs.size], self.options.extra)
+        return J[0], r[0]
+
+    def _points(self, want: bool):
+        flags = np.zeros(self.runs, dtype=np.int32)
+        rows = np.zeros((self.runs, self.P))
+        torch.cuda.synchronize(self.templates.device)
+        args = [None] * 4
+        if want:
+            args[0], args[1] = _capi.ptr(flags, C.c_int32), _capi.ptr(rows)
+        else:
+            args[2], args[3] = _capi.ptr(flags, C.c_int32), _capi.ptr(rows)
+        rc = self.lib.mkb_lm_points_device(*self._args(), self.runs,
+                                           C.c_void_p(self.workspace.data_ptr()), *args,
+                                           _stream_handle(self.stream))
+        _capi.check(rc, "lm points")
+        torch.cuda.synchronize(self.templates.device)
+        return flags, rows
+
+    def _cycle_with_extra_rows(self) -> None:
+        E = self.options.extra.count
+        ws = (C.c_void_p(self.workspace.data_ptr()), self.workspace.numel())
+        h = _stream_handle(self.stream)
+        _capi.check(self.lib.mkb_lm_cycle_jacobian_device(*self._args(), self.runs, *ws, h),
+                    "lm cycle (Jacobian)")
+        want, x = self._points(True)
+        je = np.zeros((self.runs, self.P, E))
+        re = np.zeros((self.runs, E))
+        for i in np.nonzero(want)[0]:
+            J, r = self._extra_jacobian(int(i), x[i])
+            je[i, :J.shape[0]] = J
+            re[i] = r
+        je_d, re_d = _dev_f64(je, self.templates.device), _dev_f64(re, self.templates.device)
+        _capi.check(self.lib.mkb_lm_extra_rows_device(
+            *self._args(), self.runs, *ws, C.c_void_p(je_d.data_ptr()),
+            C.c_void_p(re_d.data_ptr()), E, h), "lm extra rows")
+        _capi.check(self.lib.mkb_lm_cycle_step_device(*self._args(), self.runs, *ws, h),
+                    "lm cycle (step)")
+        evaluate, trial = self._points(False)
+        em = np.zeros(self.runs)
+        for i in np.nonzero(evaluate)[0]:
+            em[i] = self._extra_merit(int(i), trial[i])
+        em_d = _dev_f64(em, self.templates.device)
+        _capi.check(self.lib.mkb_lm_cycle_accept_device(*self._args(), self.runs, *ws,
+                                                        C.c_void_p(em_d.data_ptr()), h),
+                    "lm cycle (acceptance)")
+        torch.cuda.synchronize(self.templates.device)
         self.cycles += 1
 
     def capture(self) -> "torch.cuda.CUDAGraph":
@@ -857,6 +1011,8 @@ class DeviceLm:
         per-run decisions live in device masks, so replaying the graph advances every run by
         one cycle exactly as cycle() does. Call cycle() at least once first (it sets kernel
         attributes outside the capture)."""
+        if self._extra_rows():
+            raise NotImplementedError("DeviceLm.capture: extra rows are evaluated on the host")
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
             rc = self.lib.mkb_lm_cycle_device(*self._args(), self.runs,

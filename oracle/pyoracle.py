@@ -153,8 +153,17 @@ class Reference(_Oracle):
                                                C.c_void_p, C.c_void_p, C.c_int]
         L.mko_ref_optimize_lm.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
-                                          C.c_void_p, C.c_void_p, C.c_void_p]
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.mko_ref_optimize_lm.restype = C.c_int
+        L.mko_ref_paraxial_residuals.argtypes = [_PB, _PP, C.c_int, C.c_int, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p]
+        L.mko_ref_paraxial_residuals.restype = C.c_int
+        L.mko_ref_extra_rows.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
+        L.mko_ref_extra_rows.restype = C.c_int
 
     def error(self) -> str:
         return self.lib.mko_ref_last_error().decode(errors="replace")
@@ -177,8 +186,50 @@ class Reference(_Oracle):
         self._check(rc, "adjoint_jacobian")
         return J, r0, st
 
+    @staticmethod
+    def _constraints(constraints):
+        """[(type, mode, weight, target)] -> the driver's flat arrays (type in ConstraintType
+        order: 0 FocalLength, 1 ParfocalLength, 2 WorkingDistance, 3 ParaxialFocus, 4 Petzval;
+        mode 0 Equal, 1 Min, 2 Max)."""
+        c = list(constraints or [])
+        return (len(c), np.array([k[0] for k in c], dtype=np.int32),
+                np.array([k[1] for k in c], dtype=np.int32),
+                np.array([k[2] for k in c], dtype=np.float64),
+                np.array([k[3] for k in c], dtype=np.float64))
+
+    def _ccall(self, constraints):
+        n, t, m, w, g = self._constraints(constraints)
+        self._keep_c = (t, m, w, g)
+        return (n, t.ctypes.data, m.ctypes.data, w.ctypes.data, g.ctypes.data)
+
+    def paraxial_residuals(self, batch, layout, v: int, constraints) -> np.ndarray:
+        """The reference's paraxial_residuals of variant v (its ExtraResidualFn)."""
+        n, t, m, w, g = self._constraints(constraints)
+        out = np.zeros(n)
+        view, plan = batch.view(), layout.plan(batch)
+        rc = self.lib.mko_ref_paraxial_residuals(C.byref(view), C.byref(plan), v, n,
+                                                 t.ctypes.data, m.ctypes.data, w.ctypes.data,
+                                                 g.ctypes.data, out.ctypes.data)
+        self._check(rc, "paraxial_residuals")
+        return out
+
+    def extra_rows(self, batch, layout, vs, x0, constraints):
+        """The reference's extra_rows_cpu with paraxial constraints: J [runs][P][E], r."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, vs.size)
+        runs = x0.shape[0]
+        n = len(constraints)
+        J = np.zeros((runs, vs.size, n))
+        r = np.zeros((runs, n))
+        view, plan, vars_ = batch.view(), layout.plan(batch), vs.c_struct()
+        rc = self.lib.mko_ref_extra_rows(C.byref(view), C.byref(plan), C.byref(vars_),
+                                         x0.ctypes.data, runs, *self._ccall(constraints),
+                                         J.ctypes.data, r.ctypes.data)
+        self._check(rc, "extra_rows")
+        return J, r
+
     def optimize_lm(self, batch, layout, vs, x0, max_iterations: int = 100,
-                    method: str = "adjoint", penalty_rounds: int = 1, threads: int = 0):
+                    method: str = "adjoint", penalty_rounds: int = 1, threads: int = 0,
+                    constraints=None):
         x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, vs.size)
         runs, P = x0.shape
         x = np.zeros((runs, P))
@@ -192,7 +243,7 @@ class Reference(_Oracle):
             C.byref(view), C.byref(plan), C.byref(vars_), x0.ctypes.data, runs, max_iterations,
             1 if method == "adjoint" else 0, penalty_rounds, threads, x.ctypes.data,
             merit.ctypes.data, status.ctypes.data, its.ctypes.data, acc.ctypes.data,
-            hist.ctypes.data)
+            hist.ctypes.data, *self._ccall(constraints))
         self._check(rc, "optimize_lm")
         return dict(x=x, merit=merit, status=status, iterations=its, accepted=acc,
                     history=hist)

@@ -11,6 +11,7 @@
 //   adjoint_jacobian_cpu   src/optim/adjoint_jacobian.cpp:370
 //   normal_equations_host  include/mikroptim/optim/normal_equations.hpp:33
 //   optimize_lm_cpu        src/optim/levenberg_marquardt.cpp:972
+//   paraxial_residuals     src/optim/paraxial_residuals.cpp:353 (extra residual rows)
 // Only tests/, the golden-fixture script and bench.py's CPU legs load this library.
 
 #include "mikroptim_b200.h"
@@ -23,6 +24,7 @@
 #include "mikroptim/optim/fd_jacobian.hpp"
 #include "mikroptim/optim/levenberg_marquardt.hpp"
 #include "mikroptim/optim/normal_equations.hpp"
+#include "mikroptim/optim/paraxial_residuals.hpp"
 #include "mikroptim/optim/variable_set.hpp"
 #include "optim/parallel_variants.hpp"
 
@@ -243,6 +245,23 @@ mko::SystemDescription description_of(const mko::SystemBatchHost& b, const mkb_v
     return d;
 }
 
+// Paraxial constraints from flat arrays: type (ConstraintType order: 0 FocalLength,
+// 1 ParfocalLength, 2 WorkingDistance, 3 ParaxialFocus, 4 Petzval), mode (0 Equal, 1 Min,
+// 2 Max), weight, target.
+mko::ParaxialConstraints constraints_of(int n, const int32_t* type, const int32_t* mode,
+                                        const double* weight, const double* target) {
+    mko::ParaxialConstraints c;
+    for (int i = 0; i < n; ++i) {
+        mko::ParaxialConstraint k;
+        k.type = static_cast<mko::ConstraintType>(type[i]);
+        k.mode = static_cast<mko::ConstraintMode>(mode[i]);
+        k.weight = weight[i];
+        k.target = target[i];
+        c.items.push_back(k);
+    }
+    return c;
+}
+
 } // namespace
 
 extern "C" {
@@ -354,6 +373,32 @@ int mko_ref_adjoint_jacobian(const mkb_batch_view* view, const mkb_residual_plan
     }
 }
 
+// extra_rows_cpu (src/optim/adjoint_jacobian.cpp:300) with paraxial constraints as the extra
+// rows: J [runs][P][E], r [runs][E].
+int mko_ref_extra_rows(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                       const mkb_variables* vars, const double* x0, int runs, int n,
+                       const int32_t* type, const int32_t* mode, const double* weight,
+                       const double* target, double* J, double* r) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::SystemDescription d = description_of(b, *vars, x0);
+        const mko::VariableSet set(d, b.topology());
+        const mko::ParaxialConstraints c = constraints_of(n, type, mode, weight, target);
+        mko::check_paraxial_constraints(c, b.topology());
+        mko::AdjointJacobianOptions opt;
+        opt.quadrature = settings_of(*plan);
+        opt.extra = mko::make_paraxial_residuals(c);
+        const auto P = static_cast<std::size_t>(vars->count);
+        const mko::ExtraRowsJacobian e = mko::extra_rows_cpu(
+            set, b, std::span<const double>(x0, P * static_cast<std::size_t>(runs)), opt);
+        std::memcpy(J, e.jacobian.data(), sizeof(double) * e.jacobian.size());
+        std::memcpy(r, e.residuals.data(), sizeof(double) * e.residuals.size());
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
 int mko_ref_normal_equations(const double* J, const double* r, int P, int64_t R, double* A,
                              double* g) {
     try {
@@ -368,14 +413,33 @@ int mko_ref_normal_equations(const double* J, const double* r, int P, int64_t R,
     }
 }
 
+// paraxial_residuals of variant v (the reference's ExtraResidualFn for paraxial constraints).
+int mko_ref_paraxial_residuals(const mkb_batch_view* view, const mkb_residual_plan* plan, int v,
+                               int n, const int32_t* type, const int32_t* mode,
+                               const double* weight, const double* target, double* out) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ParaxialConstraints c = constraints_of(n, type, mode, weight, target);
+        mko::check_paraxial_constraints(c, b.topology());
+        mko::paraxial_residuals(c, b, v, std::span<double>(out, static_cast<std::size_t>(n)));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
 // Batched LM on the CPU (optimize_lm_cpu) for `runs` runs. method 0 = FD, 1 = adjoint.
 // Outputs per run: x [runs][P], merit, status (LmStatus value), iterations, accepted and the
 // merit history [runs][max_iterations + 1] padded with NaN (first penalty round only).
+// With n_constraints > 0 the paraxial constraints join as extra residual rows
+// (make_paraxial_residuals, LmOptions::jacobian.extra).
 int mko_ref_optimize_lm(const mkb_batch_view* view, const mkb_residual_plan* plan,
                         const mkb_variables* vars, const double* x0, int runs, int max_iterations,
                         int method, int penalty_rounds, int threads, double* x_out,
                         double* merit_out, int32_t* status_out, int32_t* iterations_out,
-                        int32_t* accepted_out, double* history_out) {
+                        int32_t* accepted_out, double* history_out, int n_constraints,
+                        const int32_t* c_type, const int32_t* c_mode, const double* c_weight,
+                        const double* c_target) {
     try {
         const mko::SystemBatchHost b = batch_of_view(*view, *plan);
         const mko::SystemDescription d = description_of(b, *vars, x0);
@@ -389,6 +453,12 @@ int mko_ref_optimize_lm(const mkb_batch_view* view, const mkb_residual_plan* pla
         opt.jacobian.extra_threads = threads;
         if (penalty_rounds <= 1) {
             opt.fail_weight_factor = 1.0; // one pass, no outer penalty rounds
+        }
+        if (n_constraints > 0) {
+            const mko::ParaxialConstraints c =
+                constraints_of(n_constraints, c_type, c_mode, c_weight, c_target);
+            mko::check_paraxial_constraints(c, b.topology());
+            opt.jacobian.extra = mko::make_paraxial_residuals(c);
         }
         const auto P = static_cast<std::size_t>(vars->count);
         const mko::LmResult res = mko::optimize_lm_cpu(

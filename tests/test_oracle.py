@@ -259,3 +259,22 @@ def test_port_matches_reference_with_glass_variables():
         assert np.array_equal(a, c)
     for a, c in zip(P.fd_jacobian(two, lay, vs, x0[:2]), R.fd_jacobian(two, lay, vs, x0[:2])):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.skipif(not has_reference_build(), reason="reference CPU build not present")
+def test_extra_rows_host_match_reference():
+    """Extra residual rows (paraxial constraints evaluated by the reference's own
+    paraxial_residuals): the host layer's central-difference rows, pattern and formula from the
+    library's host entry points, equal the reference's extra_rows_cpu bit for bit."""
+    from mikroptim_b200 import engine
+    b, st, vs, x0 = workloads.singlet(3)
+    lay = ResidualLayout(b.topology, st)
+    R = po.reference()
+    cons = [(0, 0, 4.0, 48.0), (2, 1, 1.0, 47.5), (4, 2, 1e4, 0.001)]
+    extra = engine.ExtraResiduals(
+        len(cons), lambda one, v, out: out.__setitem__(
+            slice(None), R.paraxial_residuals(one, lay, v, cons)))
+    J, r = engine.extra_rows_host(b, vs, x0[:3], extra)
+    Jr, rr = R.extra_rows(b, lay, vs, x0[:3], cons)
+    assert np.array_equal(r, rr) and np.array_equal(J, Jr)
+    assert np.any(J != 0.0)
