@@ -1027,6 +1027,21 @@ void DeviceNormalEquations::download(std::vector<double>& a, std::vector<double>
 namespace {
 
 // One LM pass of every run on the device.
+// sum_e r_e^2 of run i at x (extra_merit_values, src/optim/levenberg_marquardt.cpp:659)
+double extra_merit_at(const VariableSet& variables, SystemBatchHost& one,
+                      const ExtraResiduals& extra, const double* x) {
+    variables.apply(one, 0, x);
+    std::vector<double> r(static_cast<size_t>(extra.count));
+    extra.evaluate(one, 0, r);
+    double s = 0.0;
+    for (double e : r) s += e * e;
+    return s;
+}
+
+SystemBatchHost run_template(const SystemBatchHost& base, int i) {
+    return take_variants(base, {base.variants() == 1 ? 0 : i});
+}
+
 LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const SystemBatchHost& base,
                  const std::vector<double>& x0, const LmOptions& options,
                  const ResidualSettings& settings, LmGpuStats* stats) {
@@ -1054,15 +1069,74 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
     const size_t bytes = mkb_lm_workspace_bytes(&t, plan->get(), &v, &o, runs);
     if (bytes == 0) check(MKB_ERR_ARGUMENT, "lm workspace");
     ws.reserve(bytes);
-    check(mkb_lm_start_device(&t, plan->get(), &v, &o, x, runs, ws.get(), ws.bytes(),
-                              engine.stream()),
+    const int E = options.extra.count;
+    if (E < 0 || (E > 0 && !options.extra.evaluate))
+        throw std::invalid_argument("optimize_lm_gpu: extra rows need a count >= 0 and a function");
+    std::vector<SystemBatchHost> work;  // one-variant working copies of the run templates
+    DeviceBuffer dextra, dje, dre;
+    std::vector<double> em(static_cast<size_t>(runs), 0.0);
+    if (E > 0) {
+        for (int i = 0; i < runs; ++i) work.push_back(run_template(base, i));
+        for (int i = 0; i < runs; ++i)
+            em[i] = extra_merit_at(variables, work[i], options.extra,
+                                   x0.data() + static_cast<size_t>(i) * P);
+        upload(dextra, em, engine.stream());
+    }
+    check(mkb_lm_start_ex_device(&t, plan->get(), &v, &o, x,
+                                 E > 0 ? static_cast<const double*>(dextra.get()) : nullptr,
+                                 runs, ws.get(), ws.bytes(), engine.stream()),
           "lm start");
     int32_t running = runs;
     int cycles = 0;
     while (running > 0 && cycles <= options.max_iterations) {
-        check(mkb_lm_cycle_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
-                                  engine.stream()),
-              "lm cycle");
+        if (E == 0) {
+            check(mkb_lm_cycle_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
+                                      engine.stream()),
+                  "lm cycle");
+        } else {
+            // phases: trace-row normal equations, the caller's rows at the points that got
+            // them, step, trial merit with the extra merit at the trial points, acceptance
+            check(mkb_lm_cycle_jacobian_device(&t, plan->get(), &v, &o, runs, ws.get(),
+                                               ws.bytes(), engine.stream()),
+                  "lm cycle (Jacobian)");
+            std::vector<int32_t> flags(static_cast<size_t>(runs));
+            std::vector<double> pts(static_cast<size_t>(runs) * P);
+            check(mkb_lm_points_device(&t, plan->get(), &v, &o, runs, ws.get(), flags.data(),
+                                       pts.data(), nullptr, nullptr, engine.stream()),
+                  "lm points");
+            engine.synchronize();
+            std::vector<double> je(static_cast<size_t>(runs) * P * E, 0.0),
+                re(static_cast<size_t>(runs) * E, 0.0);
+            for (int i = 0; i < runs; ++i) {
+                if (!flags[i]) continue;
+                std::vector<double> xi(pts.begin() + static_cast<ptrdiff_t>(i) * P,
+                                       pts.begin() + static_cast<ptrdiff_t>(i + 1) * P);
+                std::vector<double> J1, r1;
+                extra_rows_host(variables, work[i], xi, options.extra, J1, r1);
+                std::copy(J1.begin(), J1.end(), je.begin() + static_cast<ptrdiff_t>(i) * P * E);
+                std::copy(r1.begin(), r1.end(), re.begin() + static_cast<ptrdiff_t>(i) * E);
+            }
+            const auto* dj = static_cast<const double*>(upload(dje, je, engine.stream()));
+            const auto* dr = static_cast<const double*>(upload(dre, re, engine.stream()));
+            check(mkb_lm_extra_rows_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
+                                           dj, dr, E, engine.stream()),
+                  "lm extra rows");
+            check(mkb_lm_cycle_step_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
+                                           engine.stream()),
+                  "lm cycle (step)");
+            check(mkb_lm_points_device(&t, plan->get(), &v, &o, runs, ws.get(), nullptr, nullptr,
+                                       flags.data(), pts.data(), engine.stream()),
+                  "lm points");
+            engine.synchronize();
+            for (int i = 0; i < runs; ++i)
+                em[i] = flags[i] ? extra_merit_at(variables, work[i], options.extra,
+                                                  pts.data() + static_cast<size_t>(i) * P)
+                                 : 0.0;
+            const auto* de = static_cast<const double*>(upload(dextra, em, engine.stream()));
+            check(mkb_lm_cycle_accept_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
+                                             de, engine.stream()),
+                  "lm cycle (acceptance)");
+        }
         ++cycles;
         check(mkb_lm_results_device(&t, plan->get(), &v, &o, runs, ws.get(), nullptr, nullptr,
                                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -1097,6 +1171,46 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
 }
 
 }  // namespace
+
+void extra_rows_host(const VariableSet& variables, const SystemBatchHost& base,
+                     const std::vector<double>& x0, const ExtraResiduals& extra,
+                     std::vector<double>& jacobian, std::vector<double>& residuals) {
+    const int P = variables.size(), E = extra.count;
+    const int runs = runs_of(variables, base, x0);
+    if (E < 0 || (E > 0 && !extra.evaluate))
+        throw std::invalid_argument("extra rows: count >= 0 and an evaluate function needed");
+    jacobian.assign(static_cast<size_t>(runs) * P * E, 0.0);
+    residuals.assign(static_cast<size_t>(runs) * E, 0.0);
+    const mkb_variables vc = variables.c_struct();
+    std::vector<double> xp(P), xm(P), dp(P), dm(P), y(P), r0(E), ra(E), rb(E), col(E);
+    std::vector<int32_t> st(P);
+    for (int i = 0; i < runs; ++i) {
+        SystemBatchHost one = run_template(base, i);
+        const double* x = x0.data() + static_cast<size_t>(i) * P;
+        check(mkb_fd_pattern_host(&vc, x, 1, xp.data(), xm.data(), dp.data(), dm.data(),
+                                  st.data()),
+              "fd pattern");
+        auto evaluate = [&](std::vector<double>& out) {
+            variables.apply(one, 0, y.data());
+            extra.evaluate(one, 0, out);
+        };
+        y.assign(x, x + P);
+        evaluate(r0);
+        std::copy(r0.begin(), r0.end(), residuals.begin() + static_cast<ptrdiff_t>(i) * E);
+        for (int k = 0; k < P; ++k) {
+            y[k] = xp[k];
+            evaluate(ra);
+            y[k] = xm[k];
+            evaluate(rb);
+            y[k] = x[k];
+            check(mkb_fd_derivative_host(st[k], dp[k], dm[k], E, r0.data(), ra.data(), rb.data(),
+                                         col.data()),
+                  "fd derivative");
+            std::copy(col.begin(), col.end(),
+                      jacobian.begin() + (static_cast<ptrdiff_t>(i) * P + k) * E);
+        }
+    }
+}
 
 LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
                          const SystemBatchHost& base, const std::vector<double>& x0,

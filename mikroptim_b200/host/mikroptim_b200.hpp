@@ -200,6 +200,15 @@ private:
     std::vector<double> lower_, upper_, typical_;
 };
 
+// ExtraResiduals (include/mikroptim/optim/extra_residuals.hpp): `count` rows per variant after
+// the trace rows (paraxial constraints and the like); evaluate(batch, v, out) writes variant v's
+// rows. The LM differentiates them centrally on the host with the FD Jacobian's pattern and
+// adds sum_e r_e^2 to every merit (extra_rows_untraced, src/optim/adjoint_jacobian.cpp:245).
+struct ExtraResiduals {
+    int count = 0;
+    std::function<void(const SystemBatchHost& batch, int v, std::span<double> out)> evaluate;
+};
+
 struct LmOptions {
     int max_iterations = 100;
     bool reject_new_failures = true;
@@ -213,10 +222,18 @@ struct LmOptions {
     // failed rays restart with w_fail x fail_weight_factor while it stays <= max_fail_weight
     double fail_weight_factor = 10.0;
     double max_fail_weight = 1e14;
+    ExtraResiduals extra;  // the caller's extra rows (LmOptions::jacobian.extra); count 0: none
     mkb_lm_options c_struct() const;
 };
 
 namespace cuda {
+
+// The extra rows of the runs x0 [runs][P] (`base` holds 1 variant or one per run):
+// jacobian [runs][P][E] and residuals [runs][E], bit-identical to the reference's
+// extra_rows_cpu for the same evaluate function.
+void extra_rows_host(const VariableSet& variables, const SystemBatchHost& base,
+                     const std::vector<double>& x0, const ExtraResiduals& extra,
+                     std::vector<double>& jacobian, std::vector<double>& residuals);
 
 class CudaError : public std::runtime_error {
 public:

@@ -16,6 +16,18 @@ namespace {
 
 int failures = 0, checks = 0;
 
+#ifdef MKB_HAVE_REF
+// the reference's own CPU build (oracle/_ref): paraxial constraints as extra rows
+extern "C" int mko_ref_paraxial_residuals(const mkb_batch_view*, const mkb_residual_plan*, int,
+                                          int, const int32_t*, const int32_t*, const double*,
+                                          const double*, double*);
+extern "C" int mko_ref_optimize_lm(const mkb_batch_view*, const mkb_residual_plan*,
+                                   const mkb_variables*, const double*, int, int, int, int, int,
+                                   double*, double*, int32_t*, int32_t*, int32_t*, double*, int,
+                                   const int32_t*, const int32_t*, const double*,
+                                   const double*);
+#endif
+
 void expect(bool ok, const char* what) {
     ++checks;
     if (!ok) {
@@ -198,6 +210,36 @@ int main() {
         improved = improved && lm.merit[run] < merit[run] && lm.iterations[run] > 0;
     expect(improved, "LM lowers every run's merit");
     expect(stats.cycles > 0, "LM ran cycles");
+
+#ifdef MKB_HAVE_REF
+    {  // extra rows: focal length, working distance, Petzval constraints (the reference's
+       // paraxial_residuals as the evaluate function) against the reference LM with them
+        const int32_t ctype[3] = {0, 2, 4}, cmode[3] = {0, 1, 2};
+        const double cw[3] = {4.0, 1.0, 1e4}, ct[3] = {48.0, 47.5, 0.001};
+        LmOptions xo;
+        xo.max_iterations = 8;
+        xo.fail_weight_factor = 1.0;
+        xo.extra.count = 3;
+        xo.extra.evaluate = [&](const SystemBatchHost& one, int v, std::span<double> out) {
+            const mkb_batch_view w = one.view();
+            const auto p1 = layout.plan(one);
+            if (mko_ref_paraxial_residuals(&w, p1->get(), v, 3, ctype, cmode, cw, ct,
+                                           out.data()) != 0)
+                throw std::runtime_error("reference paraxial_residuals failed");
+        };
+        const cuda::LmResult g = cuda::optimize_lm_gpu(engine, vars, batch, x0, xo, settings);
+        std::vector<double> rx(x0.size()), rm(V), rh(static_cast<size_t>(V) * 9);
+        std::vector<int32_t> rs(V), ri(V), ra(V);
+        expect(mko_ref_optimize_lm(&view, plan->get(), &cv, x0.data(), V, 8, 1, 1, 4, rx.data(),
+                                   rm.data(), rs.data(), ri.data(), ra.data(), rh.data(), 3,
+                                   ctype, cmode, cw, ct) == 0,
+               "reference LM with constraints");
+        std::vector<int32_t> gs(g.status.begin(), g.status.end());
+        expect(same_bits(g.x, rx) && same_bits(g.merit, rm) && same_bits(gs, rs) &&
+                   same_bits(g.iterations, ri) && same_bits(g.accepted, ra),
+               "LM with extra rows bit-identical to the reference");
+    }
+#endif
 
     // argument errors are thrown before any device work
     bool thrown = false;

@@ -35,6 +35,10 @@ def build_driver() -> str:
            "-L", os.path.join(cuda, "lib64"), "-lcudart",
            "-Wl,-rpath," + mbuild.HERE, "-Wl,-rpath," + os.path.dirname(po.PORT_LIB),
            "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    if os.path.exists(po.REF_LIB):  # the reference's CPU build: extra-row checks against it
+        cmd += ["-DMKB_HAVE_REF", "-L", os.path.dirname(po.REF_LIB),
+                "-l:" + os.path.basename(po.REF_LIB),
+                "-Wl,-rpath," + os.path.dirname(po.REF_LIB)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
     return DRIVER
