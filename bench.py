@@ -59,9 +59,9 @@ FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of th
 # profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
 TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
 # DRAM traffic (read + write) of adjoint_gram_kernel per run, from the ncu capture summarised
-# in profiles/adjoint_gram_objective1184.md (1,184 runs: 1.669 GB read, 18.593 GB written),
-# scaled by the runs of the launch.
-FUSED_TRAFFIC_BYTES_PER_RUN = (1.669274e9 + 18.593394e9) / 1184
+# in profiles/adjoint_gram_objective1184.md (1,184 runs of the P = 32 objective with a glass
+# variable: 1.941 GB read, 17.645 GB written), scaled by the runs of the launch.
+FUSED_TRAFFIC_BYTES_PER_RUN = (1.940772e9 + 17.644780e9) / 1184
 # The same for the uneven (config-3) runs, MIXED precision, both launches of the call, from
 # profiles/adjoint_gram_uneven1184.md (1,184 runs: 22.6 MB read, 1.822 GB written).
 FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (19.521536e6 + 3.077120e6 + 1.344401e9 + 0.477131e9) / 1184
