@@ -220,11 +220,18 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
  *                Runtime only: every value gives bit-identical results (a tuple with more rays
  *                gets a pack of its own; values above 4096 are traced as 4096).
  *   extra_merit  MERIT only: device [V] or NULL; extra_merit[v] is added to variant v's merit
- *                after its tuple sums (MeritRunOptions::extra_merit, src/cuda/merit.cu:222). */
+ *                after its tuple sums (MeritRunOptions::extra_merit, src/cuda/merit.cu:222).
+ *   extrema      device [V][S][2] or NULL: per variant and table surface the largest ray
+ *                height sqrt(x^2 + y^2) at the surface and the smallest cos I (d before the
+ *                refraction . surface normal) over the rays with status Ok; surface 0 holds
+ *                the start point and d_z; neutral 0 and 1 without a valid ray
+ *                (SurfaceExtremaResult, include/mikroptim/batch/batch_extrema.hpp, hard
+ *                maxima). Coaxial batches only (MKB_ERR_UNSUPPORTED otherwise). */
 typedef struct mkb_trace_options {
     int32_t pack_rays;
     int32_t reserved;                 /* 0                                               */
     const double* extra_merit;
+    double* extrema;
 } mkb_trace_options;
 
 /* mkb_residuals_device / mkb_merit_device with options (NULL = the defaults). */

@@ -585,7 +585,8 @@ int mkb_residuals_ex_device(const mkb_device_batch* batch, const mkb_residual_pl
         return MKB_ERR_ARGUMENT;
     }
     return launch_residuals(p, batch->records, residuals, stride, opd, status, plan->precision,
-                            static_cast<cudaStream_t>(stream));
+                            static_cast<cudaStream_t>(stream), {},
+                            options != nullptr ? options->extrema : nullptr);
 }
 
 int mkb_residuals_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
@@ -618,7 +619,8 @@ int mkb_merit_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* 
     }
     return launch_merit(p, batch->records, merit, failed, hard_failed, workspace,
                         workspace_bytes, plan->precision, static_cast<cudaStream_t>(stream), {},
-                        options != nullptr ? options->extra_merit : nullptr);
+                        options != nullptr ? options->extra_merit : nullptr,
+                        options != nullptr ? options->extrema : nullptr);
 }
 
 int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* plan, double* merit,

@@ -33,12 +33,15 @@ struct RunVars {
 };
 
 // trace.cu
+// extrema: [V][S][2] per-surface (largest ray height, smallest cos I) of the valid rays, or
+// null (TraceSettings::extrema, include/mikroptim/batch/batch_extrema.hpp)
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
                      int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream, RunMask mask = {});
+                     cudaStream_t stream, RunMask mask = {}, double* extrema = nullptr);
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
                  int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream, RunMask mask = {}, const double* extra = nullptr);
+                 cudaStream_t stream, RunMask mask = {}, const double* extra = nullptr,
+                 double* extrema = nullptr);
 size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
 // largest pack a caller may ask for (mkb_trace_options.pack_rays is clamped to it)

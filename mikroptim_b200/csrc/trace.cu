@@ -46,10 +46,15 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
 // mu_tab[s * L + l] = n_before / n_after of the step onto surface s (divided in N).
-template <class N, int kFeat>
+// kExtrema (coaxial kernels): hsq[s] / cosi[s] get the squared ray height x^2 + y^2 at surface
+// s and cos I = d . N (d before the refraction, N = (-c x, -c y, 1 - c z), c = 0 off spheres)
+// for every surface the ray passed; surface 0 is the start point and cos I = d_z there
+// (RaySurfaceRecord, trace/surface_extrema.hpp; observer calls in trace/trace.hpp:316,346).
+template <class N, int kFeat, bool kExtrema = false>
 __device__ inline int trace_ray(const TraceParams& p, const double* rec, const double* mu_tab,
                                 const RecordLayout& lay, int S, int f, int l, const Sample& smp,
-                                bool soft_mode, double& opl, double& penalty) {
+                                bool soft_mode, double& opl, double& penalty,
+                                double* hsq = nullptr, double* cosi = nullptr) {
     const int L = p.L;
     const N zero(0.0);
     const N a = rec[lay.pupil];
@@ -67,6 +72,10 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
     SoftT<N> soft{zero, kOk};
     SoftT<N>* sp = soft_mode ? &soft : nullptr;
     int status = kOk;
+    if constexpr (kExtrema) {
+        hsq[0] = value_of(r.px * r.px + r.py * r.py);
+        cosi[0] = value_of(r.dz);
+    }
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
@@ -77,10 +86,16 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
         int branch;
         GhostData gd;
         const bool plate = ghost_at<(kFeat & 2) != 0>(p, rec, lay, s, l, gd);
+        const N dbx = r.dx, dby = r.dy, dbz = r.dz;  // direction before the refraction
         status = step_surface_xf<N>(r, N(thick[s - 1]), c, n_before, N(mu_tab[s * L + l]),
                                     xf_at<(kFeat & 1) != 0>(rec, lay, s), sp, branch, nullptr,
                                     plate ? &gd : nullptr, n_after);
         if (status != kOk) break;
+        if constexpr (kExtrema) {
+            hsq[s] = value_of(r.px * r.px + r.py * r.py);
+            const N nx = -c * r.px, ny = -c * r.py, nz = N(1.0) - c * r.pz;
+            cosi[s] = value_of(dbx * nx + dby * ny + dbz * nz);
+        }
         n_before = n_after;
     }
     if (status == kOk && soft_mode) status = soft.first;
@@ -121,13 +136,26 @@ struct TupleOut {
     int* part_failed;   // MERIT: [V][n_tuples]
     int* part_hard;     // MERIT: [V][n_tuples]
     RunMask mask;       // variants to trace
+    unsigned long long* extrema;  // [V][S][2] order-preserving keys of (x^2 + y^2, cos I), or null
 };
+
+// Order-preserving keys: a larger key is a larger double (bits of a non-negative value, all
+// bits flipped for a negative one), so the maximum and minimum over rays are integer atomics
+// and do not depend on their order, as extremum_max / extremum_min do not.
+__device__ inline unsigned long long order_key(double x) {
+    const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ inline double key_value(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double(static_cast<long long>(b));
+}
 
 // kExact: per-ray arithmetic in Exact64 and every tuple sum sequential in ascending sample
 // order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
-template <bool kResiduals, int kPrecision, int kFeat>
+template <bool kResiduals, int kPrecision, int kFeat, bool kExtrema = false>
 __global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
@@ -172,6 +200,18 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     }
     __syncthreads();
 
+    // per-CTA extrema of the pack's valid rays (keys; surface s at [2s], [2s + 1])
+    unsigned long long* ext_sh = nullptr;
+    if constexpr (kExtrema) {
+        __shared__ unsigned long long ext_keys[2 * kMaxSurfaces];
+        ext_sh = ext_keys;
+        for (int i = threadIdx.x; i < S; i += kThreads) {
+            ext_keys[2 * i] = order_key(0.0);      // height^2 0 (neutral_height_sq)
+            ext_keys[2 * i + 1] = order_key(1.0);  // cos I = 1 (neutral_cos_incidence)
+        }
+        __syncthreads();
+    }
+
     // ---- phase 1: trace ---------------------------------------------------------------
     for (int i = threadIdx.x; i < pack.rays; i += kThreads) {
         int t = 0;
@@ -182,13 +222,32 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         const int k = i - sh.tuple_start[t];
         const Sample smp = pupil_sample(p, sh.tab, f, k);
         double opl, pen;
-        const int st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
-                                    pen);
+        int st;
+        if constexpr (kExtrema) {
+            double hsq[kMaxSurfaces], cosi[kMaxSurfaces];
+            st = trace_ray<N, kFeat, true>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl,
+                                           pen, hsq, cosi);
+            if (st == kOk)  // only valid rays count (SurfaceExtrema::add_ray)
+                for (int q = 0; q < S; ++q) {
+                    if (hsq[q] == hsq[q]) atomicMax(&ext_sh[2 * q], order_key(hsq[q]));
+                    if (cosi[q] == cosi[q]) atomicMin(&ext_sh[2 * q + 1], order_key(cosi[q]));
+                }
+        } else {
+            st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl, pen);
+        }
         opl_sh[i] = opl;
         pen_sh[i] = pen;
         status_sh[i] = static_cast<uint8_t>(st);
     }
     __syncthreads();
+
+    if constexpr (kExtrema) {
+        unsigned long long* g = out.extrema + static_cast<int64_t>(v) * p.S * 2;
+        for (int q = threadIdx.x; q < S; q += kThreads) {
+            atomicMax(&g[2 * q], ext_sh[2 * q]);
+            atomicMin(&g[2 * q + 1], ext_sh[2 * q + 1]);
+        }
+    }
 
     // ---- phase 2: one warp per tuple ----------------------------------------------------
     const int warp = threadIdx.x >> 5;
@@ -303,6 +362,26 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
 }
 
 // merit[v] = sum over tuples in order (f-major, then l); counts likewise.
+// Extrema output [V][S][2]: neutral keys before the trace, then the values (sqrt of the largest
+// height^2, smallest cos I) in place.
+__global__ void extrema_init_kernel(unsigned long long* keys, int64_t n, RunMask mask, int S) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        if (!run_active(mask, static_cast<int>(i / (2 * S)))) continue;
+        keys[i] = (i & 1) ? order_key(1.0) : order_key(0.0);
+    }
+}
+
+__global__ void extrema_finalize_kernel(unsigned long long* keys, int64_t n, RunMask mask,
+                                        int S) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        if (!run_active(mask, static_cast<int>(i / (2 * S)))) continue;
+        const double x = key_value(keys[i]);
+        reinterpret_cast<double*>(keys)[i] = (i & 1) ? x : __dsqrt_rn(x);
+    }
+}
+
 // extra [V] (or null): added after the tuple sums (MeritRunOptions::extra_merit,
 // src/cuda/merit.cu:222).
 __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
@@ -352,6 +431,21 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
                          : feat == 1 ? trace_kernel<kResiduals, F, 1>
                          : feat == 2 ? trace_kernel<kResiduals, F, 2>
                                      : trace_kernel<kResiduals, F, 3>);
+    const int64_t n_ext = static_cast<int64_t>(p.V) * p.S * 2;
+    if (out.extrema != nullptr) {
+        // per-surface extrema: coaxial batches (with or without ghost plates)
+        if (feat & 1) {
+            set_error("trace: per-surface extrema of decentered or tilted batches are not built");
+            return MKB_ERR_UNSUPPORTED;
+        }
+        kernel = precision == MKB_PRECISION_FP64
+                     ? (feat == 0 ? trace_kernel<kResiduals, E, 0, true>
+                                  : trace_kernel<kResiduals, E, 2, true>)
+                     : (feat == 0 ? trace_kernel<kResiduals, F, 0, true>
+                                  : trace_kernel<kResiduals, F, 2, true>);
+        extrema_init_kernel<<<592, 256, 0, stream>>>(out.extrema, n_ext, out.mask, p.S);
+        count_launch();
+    }
     if (smem > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(
             kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -359,6 +453,10 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
     }
     kernel<<<blocks, kThreads, smem, stream>>>(p, records, out);
     count_launch();
+    if (out.extrema != nullptr) {
+        extrema_finalize_kernel<<<592, 256, 0, stream>>>(out.extrema, n_ext, out.mask, p.S);
+        count_launch();
+    }
     return cuda_status(cudaGetLastError(), kResiduals ? "residuals kernel launch"
                                                       : "merit kernel launch");
 }
@@ -372,14 +470,15 @@ size_t merit_workspace(int V, int n_tuples) {
 
 int launch_residuals(const TraceParams& p, const double* records, double* residuals,
                      int64_t stride, double* opd, uint8_t* status, int precision,
-                     cudaStream_t stream, RunMask mask) {
-    TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask};
+                     cudaStream_t stream, RunMask mask, double* extrema) {
+    TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask,
+                 reinterpret_cast<unsigned long long*>(extrema)};
     return launch_trace<true>(p, records, out, precision, stream);
 }
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
                  int64_t* hard, void* workspace, size_t ws_bytes, int precision,
-                 cudaStream_t stream, RunMask mask, const double* extra) {
+                 cudaStream_t stream, RunMask mask, const double* extra, double* extrema) {
     const size_t need = merit_workspace(p.V, p.n_tuples);
     if (workspace == nullptr || ws_bytes < need) {
         set_error("merit: workspace of %zu bytes needed, %zu given", need, ws_bytes);
@@ -389,7 +488,8 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
     char* ws = static_cast<char*>(workspace);
     TupleOut out{nullptr, 0, nullptr, nullptr, reinterpret_cast<double*>(ws),
                  reinterpret_cast<int*>(ws + slots * sizeof(double)),
-                 reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask};
+                 reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask,
+                 reinterpret_cast<unsigned long long*>(extrema)};
     int rc = launch_trace<false>(p, records, out, precision, stream);
     if (rc != MKB_OK) return rc;
     merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(

@@ -134,11 +134,13 @@ class MeritOutput:
     hard_failed: np.ndarray | torch.Tensor
 
 
-def _trace_options(pack_rays: int = 0, extra_merit: torch.Tensor | None = None):
+def _trace_options(pack_rays: int = 0, extra_merit: torch.Tensor | None = None,
+                   extrema: torch.Tensor | None = None):
     o = _capi.TraceOptions()
     o.pack_rays = int(pack_rays)
     o.reserved = 0
     o.extra_merit = C.c_void_p(extra_merit.data_ptr()) if extra_merit is not None else None
+    o.extrema = C.c_void_p(extrema.data_ptr()) if extrema is not None else None
     return o
 
 
@@ -214,7 +216,9 @@ class TraceSettings:
     (the extra rows follow the ray and penalty rows and are set to 0); extra_merit (host [V] or
     None) to MERIT, added to each variant's merit after its tuple sums. precision None: the
     quadrature's. pack_rays changes only the run time (bit-identical results for every value).
-    extrema (per-variant, per-surface maxima) is not built: True raises NotImplementedError."""
+    extrema: per variant and surface the largest ray height and the smallest cos I of the valid
+    rays (SurfaceExtremaResult, hard maxima; coaxial batches) in the result's `extrema`
+    [V][S][2]."""
 
     quadrature: ResidualSettings = dataclasses.field(default_factory=ResidualSettings)
     opd: bool = False
@@ -250,6 +254,7 @@ class ResidualResult:
     opd: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0)))
     status: np.ndarray = dataclasses.field(
         default_factory=lambda: np.zeros((0, 0), dtype=np.uint8))
+    extrema: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0, 2)))
 
 
 @dataclass
@@ -262,6 +267,7 @@ class MeritResult:
     failed: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, dtype=np.int64))
     hard_failed: np.ndarray = dataclasses.field(
         default_factory=lambda: np.zeros(0, dtype=np.int64))
+    extrema: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0, 2)))
 
 
 @dataclass
@@ -288,6 +294,7 @@ class DeviceTranche:
     residuals: torch.Tensor            # [count][stride]
     status: torch.Tensor               # [count][rays]
     opd: torch.Tensor | None           # [count][rays] when settings.opd
+    extrema: torch.Tensor | None = None  # [count][S][2] when settings.extrema
 
 
 def _as_trace_settings(settings) -> TraceSettings:
@@ -389,8 +396,6 @@ class TraceEngine:
             raise ValueError("TraceEngine: extra_residuals must be >= 0")
         if ts.pack_rays < 1:
             raise ValueError("TraceEngine: pack_rays must be >= 1")
-        if ts.extrema:
-            raise NotImplementedError("TraceEngine: per-surface extrema are not built")
 
     def _tranche(self, shape, layout: ResidualLayout, plan, ts: TraceSettings, merit: bool,
                  granularity: int, usable: int) -> int:
@@ -495,6 +500,9 @@ class TraceEngine:
             return t[:n].view(*shape)
 
         hp = {}
+        S = batch.surfaces
+        if ts.extrema:
+            hp["extrema"] = host("extrema", (V, S, 2), torch.float64)
         if merit:
             hp["merit"] = host("merit", (V,), torch.float64)
             hp["failed"] = host("failed", (V,), torch.int64)
@@ -502,6 +510,8 @@ class TraceEngine:
             out.residuals = ResidualResult()
             out.merit = MeritResult(V, rays, hp["merit"].numpy(), hp["failed"].numpy(),
                                     hp["hard"].numpy())
+            if ts.extrema:
+                out.merit.extrema = hp["extrema"].numpy()
         else:
             hp["res"] = host("res", (V, stride), torch.float64)
             if ts.opd:
@@ -513,6 +523,8 @@ class TraceEngine:
                 V, rays, layout.trace_rows - rays, stride, hp["res"].numpy(),
                 hp["opd"].numpy() if ts.opd else np.zeros((0, 0)),
                 hp["status"].numpy() if ts.status else np.zeros((0, 0), dtype=np.uint8))
+            if ts.extrema:
+                out.residuals.extrema = hp["extrema"].numpy()
         if V == 0:
             out.info.device_bytes = self.device_bytes()
             return out
@@ -528,6 +540,8 @@ class TraceEngine:
                     hp["merit"][sl].copy_(m.merit, non_blocking=True)
                     hp["failed"][sl].copy_(m.failed, non_blocking=True)
                     hp["hard"][sl].copy_(m.hard_failed, non_blocking=True)
+                    if ts.extrema:
+                        hp["extrema"][sl].copy_(self._last_extrema, non_blocking=True)
                 else:
                     t = self._residual_tranche(part, layout, ts, first)
                     hp["res"][sl].copy_(t.residuals, non_blocking=True)
@@ -535,6 +549,8 @@ class TraceEngine:
                         hp["status"][sl].copy_(t.status, non_blocking=True)
                     if ts.opd:
                         hp["opd"][sl].copy_(t.opd, non_blocking=True)
+                    if ts.extrema:
+                        hp["extrema"][sl].copy_(t.extrema, non_blocking=True)
                 torch.cuda.current_stream(self.device).synchronize()
                 _device_status()
                 out.info.tranches += 1
@@ -597,13 +613,15 @@ class TraceEngine:
             res[:, layout.trace_rows:].zero_()
         b = db.c_struct()
         plan = layout.plan(part)
-        opts = _trace_options(ts.pack_rays)
+        ext = self._extrema_buffer(part, ts)
+        opts = _trace_options(ts.pack_rays, None, ext)
         rc = lib.mkb_residuals_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
                                          C.c_void_p(res.data_ptr()), stride,
                                          C.c_void_p(opd.data_ptr()) if opd is not None else None,
                                          C.c_void_p(st.data_ptr()), _stream_handle(None))
         _capi.check(rc, "residuals")
-        return DeviceTranche(first, n, rays, layout.trace_rows - rays, stride, res, st, opd)
+        return DeviceTranche(first, n, rays, layout.trace_rows - rays, stride, res, st, opd,
+                             ext)
 
     def _merit_tranche(self, part: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
                        extra: np.ndarray | None) -> MeritOutput:
@@ -622,13 +640,22 @@ class TraceEngine:
             extra_dev = self._buffer("extra", 8 * n)[:8 * n].view(torch.float64)
             extra_dev.copy_(torch.from_numpy(np.ascontiguousarray(extra)))
         b = db.c_struct()
-        opts = _trace_options(ts.pack_rays, extra_dev)
+        ext = self._extrema_buffer(part, ts)
+        self._last_extrema = ext
+        opts = _trace_options(ts.pack_rays, extra_dev, ext)
         rc = lib.mkb_merit_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
                                      C.c_void_p(merit.data_ptr()), C.c_void_p(failed.data_ptr()),
                                      C.c_void_p(hard.data_ptr()), C.c_void_p(ws.data_ptr()),
                                      ws.numel(), _stream_handle(None))
         _capi.check(rc, "merit")
         return MeritOutput(merit, failed, hard)
+
+    def _extrema_buffer(self, part: SystemBatchHost, ts: TraceSettings):
+        if not ts.extrema:
+            return None
+        n = part.variants * part.surfaces * 2
+        return self._buffer("extrema", 8 * n)[:8 * n].view(torch.float64).view(
+            part.variants, part.surfaces, 2)
 
     @staticmethod
     def _stride_of(batch: SystemBatchHost) -> int:

@@ -164,6 +164,8 @@ class Reference(_Oracle):
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]
         L.mko_ref_extra_rows.restype = C.c_int
+        L.mko_ref_surface_extrema.argtypes = [_PB, _PP, C.c_void_p]
+        L.mko_ref_surface_extrema.restype = C.c_int
 
     def error(self) -> str:
         return self.lib.mko_ref_last_error().decode(errors="replace")
@@ -211,6 +213,15 @@ class Reference(_Oracle):
                                                  t.ctypes.data, m.ctypes.data, w.ctypes.data,
                                                  g.ctypes.data, out.ctypes.data)
         self._check(rc, "paraxial_residuals")
+        return out
+
+    def surface_extrema(self, batch, layout) -> np.ndarray:
+        """The reference's surface_extrema_cpu (hard): [V][S][2] = (largest ray height,
+        smallest cos I) per variant and surface over the rays with status Ok."""
+        out = np.zeros((batch.variants, batch.surfaces, 2))
+        view, plan = batch.view(), layout.plan(batch)
+        self._check(self.lib.mko_ref_surface_extrema(C.byref(view), C.byref(plan),
+                                                     out.ctypes.data), "surface_extrema")
         return out
 
     def extra_rows(self, batch, layout, vs, x0, constraints):

@@ -16,6 +16,7 @@
 
 #include "mikroptim_b200.h"
 
+#include "mikroptim/batch/batch_extrema.hpp"
 #include "mikroptim/batch/batch_merit.hpp"
 #include "mikroptim/batch/batch_residuals.hpp"
 #include "mikroptim/batch/system_batch.hpp"
@@ -315,6 +316,20 @@ int mko_ref_merit(const mkb_batch_view* view, const mkb_residual_plan* plan, dou
             failed[v] = r.failed[0];
             hard_failed[v] = r.hard_failed[0];
         });
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// surface_extrema_cpu (src/batch/batch_extrema.cpp, hard maxima): out [V][S][2].
+int mko_ref_surface_extrema(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                            double* out) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
+        const mko::SurfaceExtremaResult r = mko::surface_extrema_cpu(b, layout);
+        std::memcpy(out, r.values.data(), sizeof(double) * r.values.size());
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

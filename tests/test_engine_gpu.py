@@ -91,8 +91,6 @@ def test_extra_residuals_and_extra_merit():
     assert np.array_equal(m1.merit, m0.merit + extra)  # one rounded add after the tuple sums
     with pytest.raises(ValueError):
         eng.run(b, engine.TraceMode.MERIT, engine.TraceSettings(st, extra_merit=extra[:3]))
-    with pytest.raises(NotImplementedError):
-        eng.run(b, engine.TraceMode.MERIT, engine.TraceSettings(st, extrema=True))
 
 
 def test_run_on_device_tranches_keep_groups_together():
