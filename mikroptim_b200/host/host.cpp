@@ -623,12 +623,13 @@ void TraceEngine::release() noexcept {
     hard_.release();
     workspace_.release();
     extra_.release();
+    extrema_.release();
 }
 
 std::size_t TraceEngine::device_bytes() const {
     return batch_.capacity_bytes() + out_.bytes() + opd_.bytes() + status_.bytes() +
            merit_.bytes() + failed_.bytes() + hard_.bytes() + workspace_.bytes() +
-           extra_.bytes();
+           extra_.bytes() + extrema_.bytes();
 }
 
 void TraceEngine::synchronize() {
@@ -660,7 +661,6 @@ void check_settings(const TraceSettings& settings) {
     if (settings.extra_residuals < 0)
         throw std::invalid_argument("TraceEngine: extra_residuals must be >= 0");
     if (settings.pack_rays < 1) throw std::invalid_argument("TraceEngine: pack_rays must be >= 1");
-    if (settings.extrema) throw std::logic_error("TraceEngine: per-surface extrema are not built");
 }
 
 ResidualSettings quadrature_of(const TraceSettings& settings) {
@@ -776,6 +776,9 @@ DeviceTranche TraceEngine::residual_tranche(const SystemBatchHost& batch,
                    "clear residuals");
     mkb_trace_options o{};
     o.pack_rays = settings.pack_rays;
+    if (settings.extrema)
+        o.extrema = static_cast<double*>(
+            extrema_.reserve(n * static_cast<size_t>(batch.surfaces()) * 2 * sizeof(double)));
     check(mkb_residuals_ex_device(&b, plan->get(), &o, res, stride, opd, st, stream_),
           "residuals");
     synchronize();
@@ -813,6 +816,7 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
     const int64_t rays = layout.rays_per_variant();
     const int64_t stride = layout.trace_rows() + settings.extra_residuals;
     const size_t rays_total = static_cast<size_t>(V) * rays;
+    const size_t S2 = static_cast<size_t>(batch.surfaces()) * 2;
     out.mode = mode;
     out.info = TraceRunInfo{};
     out.info.variants = V;
@@ -824,6 +828,7 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
         out.merit.merit.resize(V);
         out.merit.failed.resize(V);
         out.merit.hard_failed.resize(V);
+        if (settings.extrema) out.merit.extrema.resize(static_cast<size_t>(V) * S2);
     } else {
         out.residuals.variants = V;
         out.residuals.rays_per_variant = rays;
@@ -832,6 +837,7 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
         out.residuals.residuals.resize(static_cast<size_t>(V) * stride);
         out.residuals.opd.resize(settings.opd ? rays_total : 0);
         out.residuals.status.resize(settings.status ? rays_total : 0);
+        if (settings.extrema) out.residuals.extrema.resize(static_cast<size_t>(V) * S2);
     }
     out.layout.emplace(layout);
     if (V == 0) {
@@ -858,6 +864,9 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
             auto* h = static_cast<int64_t*>(hard_.reserve(n * sizeof(int64_t)));
             mkb_trace_options o{};
             o.pack_rays = settings.pack_rays;
+            if (settings.extrema)
+                o.extrema = static_cast<double*>(extrema_.reserve(
+                    n * static_cast<size_t>(batch.surfaces()) * 2 * sizeof(double)));
             if (!settings.extra_merit.empty()) {
                 void* e = extra_.reserve(n * sizeof(double));
                 cuda_check(cudaMemcpyAsync(e, settings.extra_merit.data() + v0,
@@ -872,6 +881,8 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
             down(out.merit.merit.data() + v0, m, n * sizeof(double));
             down(out.merit.failed.data() + v0, f, n * sizeof(int64_t));
             down(out.merit.hard_failed.data() + v0, h, n * sizeof(int64_t));
+            if (settings.extrema)
+                down(out.merit.extrema.data() + v0 * S2, extrema_.get(), n * S2 * sizeof(double));
             synchronize();
         } else {
             const DeviceTranche t = residual_tranche(batch, layout, settings, first, count);
@@ -881,6 +892,9 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
                 down(out.residuals.status.data() + v0 * rays, t.status, n * rays);
             if (settings.opd)
                 down(out.residuals.opd.data() + v0 * rays, t.opd, n * rays * sizeof(double));
+            if (settings.extrema)
+                down(out.residuals.extrema.data() + v0 * S2, extrema_.get(),
+                     n * S2 * sizeof(double));
             synchronize();
         }
         ++out.info.tranches;

@@ -285,7 +285,8 @@ struct EngineOptions {
 // extra rows follow the ray and penalty rows and are set to 0); extra_merit (empty or one
 // value per variant, valid until run returns) to MERIT, added to each variant's merit after
 // its tuple sums. precision: empty = the quadrature's. pack_rays changes only the run time.
-// extrema (per-surface maxima) is not built: true throws std::logic_error.
+// extrema: per variant and surface the largest ray height and the smallest cos I of the valid
+// rays (SurfaceExtremaResult, hard maxima; coaxial batches, else std::logic_error).
 struct TraceSettings {
     TraceSettings() = default;
     TraceSettings(const ResidualSettings& q) : quadrature(q) {}  // NOLINT: implicit on purpose
@@ -314,6 +315,7 @@ struct ResidualResult {
     std::vector<double> residuals;  // [V][stride]
     std::vector<double> opd;        // [V][rays] when requested
     std::vector<uint8_t> status;    // [V][rays] when requested
+    std::vector<double> extrema;    // [V][S][2] when requested (largest height, smallest cos I)
 };
 
 struct MeritResult {
@@ -322,6 +324,7 @@ struct MeritResult {
     std::vector<double> merit;          // [V]
     std::vector<int64_t> failed;        // [V]
     std::vector<int64_t> hard_failed;   // [V]
+    std::vector<double> extrema;        // [V][S][2] when requested
 };
 
 // TraceOutput (trace_engine.hpp:103): the result of the run's mode; the other is empty.
@@ -414,7 +417,7 @@ private:
     EngineOptions options_;
     void* stream_ = nullptr;
     DeviceSystemBatch batch_;
-    DeviceBuffer out_, opd_, status_, merit_, failed_, hard_, workspace_, extra_;
+    DeviceBuffer out_, opd_, status_, merit_, failed_, hard_, workspace_, extra_, extrema_;
 };
 
 // J [runs][P][R] (column p of run i at (i*P + p)*R) and r0 [runs][R] on the host.

@@ -21,6 +21,8 @@ int failures = 0, checks = 0;
 extern "C" int mko_ref_paraxial_residuals(const mkb_batch_view*, const mkb_residual_plan*, int,
                                           int, const int32_t*, const int32_t*, const double*,
                                           const double*, double*);
+extern "C" int mko_ref_surface_extrema(const mkb_batch_view*, const mkb_residual_plan*,
+                                       double*);
 extern "C" int mko_ref_optimize_lm(const mkb_batch_view*, const mkb_residual_plan*,
                                    const mkb_variables*, const double*, int, int, int, int, int,
                                    double*, double*, int32_t*, int32_t*, int32_t*, double*, int,
@@ -212,6 +214,15 @@ int main() {
     expect(stats.cycles > 0, "LM ran cycles");
 
 #ifdef MKB_HAVE_REF
+    {  // per-surface extrema against the reference's surface_extrema_cpu
+        cuda::TraceSettings es(settings);
+        es.extrema = true;
+        const cuda::TraceOutput eo = engine.run(batch, cuda::TraceMode::Merit, es);
+        std::vector<double> want(static_cast<size_t>(V) * batch.surfaces() * 2);
+        expect(mko_ref_surface_extrema(&view, plan->get(), want.data()) == 0,
+               "reference surface extrema");
+        expect(same_bits(eo.merit.extrema, want), "extrema bit-identical to the reference");
+    }
     {  // extra rows: focal length, working distance, Petzval constraints (the reference's
        // paraxial_residuals as the evaluate function) against the reference LM with them
         const int32_t ctype[3] = {0, 2, 4}, cmode[3] = {0, 1, 2};
