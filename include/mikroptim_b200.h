@@ -379,13 +379,32 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
  *   4. mkb_lm_cycle_accept_device         trial MERIT plus extra_merit[run] = sum_e r_e^2 at
  *                                          the trial point (device [runs]; read for the runs to
  *                                          evaluate), then acceptance.
- * mkb_lm_start_ex_device is mkb_lm_start_device with the extra merit at x0 (device [runs]).
+ * Step 4 may itself run in two parts for rows that depend on the trace (the reference's
+ * trace_extra, TraceExtraResiduals, which read the per-surface extrema of the same trace):
+ *   4a. mkb_lm_cycle_trial_device         trial MERIT (+ extra_merit) and, when `extrema` is
+ *                                          given (device [runs][S][2]), the trial points'
+ *                                          extrema (mkb_trace_options.extrema);
+ *   4b. mkb_lm_cycle_decide_device        acceptance with trace_merit[run] (device [runs]) added
+ *                                          to the trial merit after the kernel's sum, as
+ *                                          GpuLmBackend::merit does (src/cuda/
+ *                                          levenberg_marquardt.cpp:235-240).
+ * mkb_lm_start_ex_device is mkb_lm_start_device with the extra merit at x0 (device [runs], in
+ * the MERIT kernel) and the trace-dependent merit at x0 (added after it); either may be NULL.
  * The host FD of the extra rows uses mkb_fd_pattern_host / mkb_fd_derivative_host, the
  * pattern and formula of the FD Jacobian. */
 int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                            const mkb_variables* vars, const mkb_lm_options* options,
-                           const double* x0, const double* extra_merit, int32_t runs,
-                           void* workspace, size_t workspace_bytes, void* stream);
+                           const double* x0, const double* extra_merit,
+                           const double* trace_merit, int32_t runs, void* workspace,
+                           size_t workspace_bytes, void* stream);
+int mkb_lm_cycle_trial_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                              const mkb_variables* vars, const mkb_lm_options* options,
+                              int32_t runs, void* workspace, size_t workspace_bytes,
+                              const double* extra_merit, double* extrema, void* stream);
+int mkb_lm_cycle_decide_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                               const mkb_variables* vars, const mkb_lm_options* options,
+                               int32_t runs, void* workspace, size_t workspace_bytes,
+                               const double* trace_merit, void* stream);
 int mkb_lm_cycle_jacobian_device(const mkb_device_batch* templates,
                                  const mkb_residual_plan* plan, const mkb_variables* vars,
                                  const mkb_lm_options* options, int32_t runs, void* workspace,

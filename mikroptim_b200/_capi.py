@@ -208,8 +208,14 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_lm_cycle_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,
                                         c.c_void_p]
     lib.mkb_lm_start_ex_device.restype = c.c_int
-    lib.mkb_lm_start_ex_device.argtypes = [PB, PP, PV, PO, c.c_void_p, c.c_void_p, c.c_int32,
-                                           c.c_void_p, c.c_size_t, c.c_void_p]
+    lib.mkb_lm_start_ex_device.argtypes = [PB, PP, PV, PO, c.c_void_p, c.c_void_p, c.c_void_p,
+                                           c.c_int32, c.c_void_p, c.c_size_t, c.c_void_p]
+    lib.mkb_lm_cycle_trial_device.restype = c.c_int
+    lib.mkb_lm_cycle_trial_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p,
+                                              c.c_size_t, c.c_void_p, c.c_void_p, c.c_void_p]
+    lib.mkb_lm_cycle_decide_device.restype = c.c_int
+    lib.mkb_lm_cycle_decide_device.argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p,
+                                               c.c_size_t, c.c_void_p, c.c_void_p]
     for name in ("mkb_lm_cycle_jacobian_device", "mkb_lm_cycle_step_device"):
         getattr(lib, name).restype = c.c_int
         getattr(lib, name).argtypes = [PB, PP, PV, PO, c.c_int32, c.c_void_p, c.c_size_t,

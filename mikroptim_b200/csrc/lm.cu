@@ -337,9 +337,11 @@ lm_update_kernel(const __grid_constant__ VarParams v, LmOptionsDev o, LmState st
 }
 
 // Acceptance (levenberg_marquardt.cpp:518-545) after the trial MERIT.
+// post (or null): the caller's merit share added after the kernel's (trace-dependent extra
+// rows, src/cuda/levenberg_marquardt.cpp:235-240).
 __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double* trial_merit,
                                  const int64_t* trial_failed, const int64_t* trial_hard,
-                                 int runs) {
+                                 int runs, const double* post) {
     const int run = blockIdx.x * blockDim.x + threadIdx.x;
     if (run >= runs) return;
     if (!st.in_cycle[run]) {
@@ -352,7 +354,8 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
     const int n = st.vt != nullptr ? st.vt[run].P : P;
     const int64_t ps = st.pstride;
     if (st.solved[run]) {
-        const double f_new = trial_merit[run];
+        const double f_new = post != nullptr ? __dadd_rn(trial_merit[run], post[run])
+                                             : trial_merit[run];
         const double merit = st.merit[run];
         const double pred = st.predicted[run];
         const double rho = (Exact64(merit) - Exact64(f_new)).v / pred;
@@ -386,9 +389,11 @@ __global__ void lm_accept_kernel(LmOptionsDev o, LmState st, int P, const double
 }
 
 // Start: merit at x0 (already evaluated into merit/failed/hard), status, damping.
-__global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* x0, int runs) {
+__global__ void lm_init_kernel(LmOptionsDev o, LmState st, int P, const double* x0, int runs,
+                               const double* post) {
     const int run = blockIdx.x * blockDim.x + threadIdx.x;
     if (run >= runs) return;
+    if (post != nullptr) st.merit[run] = __dadd_rn(st.merit[run], post[run]);
     const int64_t ps = st.pstride;  // x0 rows have the same stride (P, or the largest P)
     for (int k = 0; k < ps; ++k) {
         const double xv = x0[run * ps + k];
@@ -442,8 +447,8 @@ __global__ void gram_extend_kernel(const VarParams v, LmState st, double* __rest
 }  // namespace
 
 int launch_lm_init(const LmOptionsDev& o, const LmState& st, int P, const double* x0, int runs,
-                   cudaStream_t stream) {
-    lm_init_kernel<<<(runs + 127) / 128, 128, 0, stream>>>(o, st, P, x0, runs);
+                   cudaStream_t stream, const double* post = nullptr) {
+    lm_init_kernel<<<(runs + 127) / 128, 128, 0, stream>>>(o, st, P, x0, runs, post);
     count_launch();
     return cuda_status(cudaGetLastError(), "lm init launch");
 }
@@ -457,9 +462,9 @@ int launch_lm_update(const VarParams& v, const LmOptionsDev& o, const LmState& s
 
 int launch_lm_accept(const LmOptionsDev& o, const LmState& st, int P, const double* trial_merit,
                      const int64_t* trial_failed, const int64_t* trial_hard, int runs,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, const double* post = nullptr) {
     lm_accept_kernel<<<(runs + 127) / 128, 128, 0, stream>>>(o, st, P, trial_merit, trial_failed,
-                                                             trial_hard, runs);
+                                                             trial_hard, runs, post);
     count_launch();
     return cuda_status(cudaGetLastError(), "lm accept launch");
 }
@@ -694,14 +699,14 @@ RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* te
 int lm_merit_at(const LmSetup& s, const LmLayout& L, const mkb_device_batch* templates,
                 const double* x, int runs, double* merit, int64_t* failed, int64_t* hard,
                 cudaStream_t stream, const int* run_mask = nullptr,
-                const double* extra_merit = nullptr) {
+                const double* extra_merit = nullptr, double* extrema = nullptr) {
     const RecordLayout lay = layout_of(s.tp);
     int rc = launch_apply(s.vp, lay, templates->records, templates->variants, x, L.records, runs,
                           stream, run_vars(s, L, templates));
     if (rc != MKB_OK) return rc;
     return launch_merit(run_params(s, L), L.records, merit, failed, hard, L.merit_ws,
                         L.merit_ws_bytes, s.precision, stream, RunMask{run_mask, 1, 0},
-                        extra_merit);
+                        extra_merit, extrema);
 }
 
 // Processing order of the runs: those with at most kSmallP variables first (their fused
@@ -808,18 +813,28 @@ int phase_jacobian(const LmCall& c, const mkb_device_batch* templates,
     return rc;
 }
 
-// 3. trial MERIT (+ the caller's extra merit), 4. acceptance
+// 3. trial MERIT (+ the caller's extra merit; extrema of the trial points when asked)
+int phase_trial(const LmCall& c, const mkb_device_batch* templates, int32_t runs,
+                const double* extra_merit, double* extrema, cudaStream_t stream) {
+    return lm_merit_at(c.s, c.L, templates, c.L.st.trial, runs, c.L.trial_merit,
+                       c.L.trial_failed, c.L.trial_hard, stream, c.L.st.evaluate, extra_merit,
+                       extrema);
+}
+
+// 4. acceptance (post: a merit share added after the trial MERIT's, or null)
+int phase_decide(const LmCall& c, int32_t runs, const double* post, cudaStream_t stream) {
+    int rc = cuda_status(cudaMemsetAsync(c.L.st.running, 0, sizeof(int), stream),
+                         "lm: clear count");
+    if (rc != MKB_OK) return rc;
+    return launch_lm_accept(c.s.o, c.L.st, c.s.vp.P, c.L.trial_merit, c.L.trial_failed,
+                            c.L.trial_hard, runs, stream, post);
+}
+
 int phase_accept(const LmCall& c, const mkb_device_batch* templates, int32_t runs,
                  const double* extra_merit, cudaStream_t stream) {
-    const LmSetup& s = c.s;
-    const LmLayout& L = c.L;
-    int rc = lm_merit_at(s, L, templates, L.st.trial, runs, L.trial_merit, L.trial_failed,
-                         L.trial_hard, stream, L.st.evaluate, extra_merit);
+    int rc = phase_trial(c, templates, runs, extra_merit, nullptr, stream);
     if (rc != MKB_OK) return rc;
-    rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
-    if (rc != MKB_OK) return rc;
-    return launch_lm_accept(s.o, L.st, s.vp.P, L.trial_merit, L.trial_failed, L.trial_hard, runs,
-                            stream);
+    return phase_decide(c, runs, nullptr, stream);
 }
 
 }  // namespace
@@ -839,8 +854,9 @@ size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_resid
 
 int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                            const mkb_variables* vars, const mkb_lm_options* options,
-                           const double* x0, const double* extra_merit, int32_t runs,
-                           void* workspace, size_t workspace_bytes, void* stream_ptr) {
+                           const double* x0, const double* extra_merit,
+                           const double* trace_merit, int32_t runs, void* workspace,
+                           size_t workspace_bytes, void* stream_ptr) {
     const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     LmCall c;
     std::vector<VarParams> table;
@@ -874,15 +890,15 @@ int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual
     if (rc != MKB_OK) return rc;
     rc = cuda_status(cudaMemsetAsync(L.st.running, 0, sizeof(int), stream), "lm: clear count");
     if (rc != MKB_OK) return rc;
-    return launch_lm_init(s.o, L.st, s.pmax, x0, runs, stream);
+    return launch_lm_init(s.o, L.st, s.pmax, x0, runs, stream, trace_merit);
 }
 
 int mkb_lm_start_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                         const mkb_variables* vars, const mkb_lm_options* options,
                         const double* x0, int32_t runs, void* workspace, size_t workspace_bytes,
                         void* stream_ptr) {
-    return mkb_lm_start_ex_device(templates, plan, vars, options, x0, nullptr, runs, workspace,
-                                  workspace_bytes, stream_ptr);
+    return mkb_lm_start_ex_device(templates, plan, vars, options, x0, nullptr, nullptr, runs,
+                                  workspace, workspace_bytes, stream_ptr);
 }
 
 int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
@@ -944,6 +960,27 @@ int mkb_lm_cycle_accept_device(const mkb_device_batch* templates, const mkb_resi
     int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
     if (rc != MKB_OK) return rc;
     return phase_accept(c, templates, runs, extra_merit, static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_cycle_trial_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                              const mkb_variables* vars, const mkb_lm_options* options,
+                              int32_t runs, void* workspace, size_t workspace_bytes,
+                              const double* extra_merit, double* extrema, void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    return phase_trial(c, templates, runs, extra_merit, extrema,
+                       static_cast<cudaStream_t>(stream_ptr));
+}
+
+int mkb_lm_cycle_decide_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                               const mkb_variables* vars, const mkb_lm_options* options,
+                               int32_t runs, void* workspace, size_t workspace_bytes,
+                               const double* trace_merit, void* stream_ptr) {
+    LmCall c;
+    int rc = lm_call(templates, plan, vars, options, runs, workspace, workspace_bytes, c);
+    if (rc != MKB_OK) return rc;
+    return phase_decide(c, runs, trace_merit, static_cast<cudaStream_t>(stream_ptr));
 }
 
 int mkb_lm_points_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,

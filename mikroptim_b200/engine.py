@@ -781,6 +781,21 @@ class ExtraResiduals:
         self.evaluate = evaluate
 
 
+class TraceExtraResiduals:
+    """TraceExtraResiduals (include/mikroptim/optim/trace_extra_residuals.hpp): `count` rows per
+    variant after the ExtraResiduals rows, computed from the per-surface extrema of the same
+    trace (largest ray height, smallest cos I: semi-diameter and incidence-angle constraints).
+    evaluate(batch, v, extrema, out) gets variant v's extrema [S][2] (hard maxima). The LM
+    traces every FD point with extrema to differentiate them and adds sum t^2 to each merit
+    after the MERIT kernel's sum (GpuLmBackend::merit, src/cuda/levenberg_marquardt.cpp:235)."""
+
+    def __init__(self, count: int = 0, evaluate=None):
+        if count < 0 or (count > 0 and evaluate is None):
+            raise ValueError("TraceExtraResiduals: count >= 0 and an evaluate function needed")
+        self.count = count
+        self.evaluate = evaluate
+
+
 def extra_rows_host(host: SystemBatchHost, variables, x0, extra: ExtraResiduals):
     """The caller's extra rows at run points x0 [runs][P] on the host (extra_rows_untraced,
     src/optim/adjoint_jacobian.cpp:245): per run, a one-variant copy of its template (`host`
@@ -831,7 +846,8 @@ class LmOptions:
     """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85). fail_weight_factor and
     max_fail_weight drive the outer soft-failure penalty rounds of optimize_lm_gpu
     (optimize_lm_rounds, src/optim/levenberg_marquardt.cpp:891); a factor <= 1 gives one pass.
-    extra: the caller's extra residual rows (LmOptions::jacobian.extra), or None."""
+    extra / trace_extra: the caller's extra residual rows (LmOptions::jacobian.extra and
+    ::jacobian.trace_extra), or None."""
 
     max_iterations: int = 100
     ftol: float = 1e-10
@@ -846,6 +862,7 @@ class LmOptions:
     fail_weight_factor: float = 10.0
     max_fail_weight: float = 1e14
     extra: ExtraResiduals | None = None
+    trace_extra: TraceExtraResiduals | None = None
 
     def c_struct(self) -> "_capi.LmOptions":
         o = _capi.LmOptions()
@@ -929,13 +946,17 @@ class DeviceLm:
         check_start_points(self.variables, rows)
         x0 = _dev_f64(rows, self.templates.device)
         self._x0 = x0
-        extra = None
-        if self._extra_rows():
+        extra = tmerit = None
+        if self._plain_rows():
             extra = _dev_f64([self._extra_merit(i, rows[i]) for i in range(self.runs)],
                              self.templates.device)
+        if self._trace_rows():
+            tmerit = _dev_f64(self._trace_merits([(i, rows[i]) for i in range(self.runs)]),
+                              self.templates.device)
         rc = self.lib.mkb_lm_start_ex_device(
             *self._args(), C.c_void_p(x0.data_ptr()),
-            C.c_void_p(extra.data_ptr()) if extra is not None else None, self.runs,
+            C.c_void_p(extra.data_ptr()) if extra is not None else None,
+            C.c_void_p(tmerit.data_ptr()) if tmerit is not None else None, self.runs,
             C.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
             _stream_handle(self.stream))
         _capi.check(rc, "lm start")
@@ -951,17 +972,27 @@ class DeviceLm:
         self.cycles += 1
 
     # ---- the caller's extra rows (evaluated on the host) ----------------------------------
-    def _extra_rows(self) -> int:
+    def _plain_rows(self) -> int:
         e = self.options.extra
         return e.count if e is not None else 0
+
+    def _trace_rows(self) -> int:
+        t = self.options.trace_extra
+        return t.count if t is not None else 0
+
+    def _extra_rows(self) -> int:
+        return self._plain_rows() + self._trace_rows()
 
     def _var_set(self, i: int):
         return self.variables[i] if isinstance(self.variables, (list, tuple)) else self.variables
 
+    def _template(self, i: int) -> int:
+        return 0 if self.host.variants == 1 else i
+
     def _work_batch(self, i: int) -> SystemBatchHost:
         """A one-variant copy of run i's template (the reference's working variant)."""
         cache = self.__dict__.setdefault("_work", {})
-        t = 0 if self.host.variants == 1 else i
+        t = self._template(i)
         if t not in cache:
             cache[t] = self.host.subset(t, 1)
         return cache[t]
@@ -973,19 +1004,83 @@ class DeviceLm:
         self.options.extra.evaluate(one, 0, out)
         return out
 
-    def _extra_merit(self, i: int, x_row) -> float:
-        """sum_e r_e^2 in row order, each product and sum rounded (extra_merit_values)."""
+    @staticmethod
+    def _sum_squares(values) -> float:
         s = 0.0
-        for e in self._evaluate(i, x_row[:self._var_set(i).size]):
+        for e in values:
             s = s + e * e
         return s
 
+    def _extra_merit(self, i: int, x_row) -> float:
+        """sum_e r_e^2 in row order, each product and sum rounded (extra_merit_values)."""
+        if not self._plain_rows():
+            return 0.0
+        return self._sum_squares(self._evaluate(i, x_row[:self._var_set(i).size]))
+
+    def _points_extrema(self, pts) -> tuple[SystemBatchHost, np.ndarray]:
+        """The batch of the points [(run, y)] and their extrema [n][S][2] from one MERIT trace
+        (FD points and trial points alike)."""
+        multi = self.host.take([self._template(i) for i, _ in pts])
+        for j, (i, y) in enumerate(pts):
+            vs = self._var_set(i)
+            vs.apply(multi, j, np.asarray(y[:vs.size], dtype=np.float64))
+        eng = self.__dict__.setdefault("_engine", TraceEngine(self.templates.device.index or 0))
+        out = eng.run(multi, TraceMode.MERIT, TraceSettings(self.layout.settings, extrema=True))
+        return multi, out.merit.extrema
+
+    def _trace_values(self, multi, ext, j: int) -> np.ndarray:
+        out = np.zeros(self._trace_rows())
+        self.options.trace_extra.evaluate(multi, j, ext[j], out)
+        return out
+
+    def _trace_merits(self, pts) -> np.ndarray:
+        """sum_i t_i^2 at the points [(run, y)] (trace_extra_merit)."""
+        if not pts:
+            return np.zeros(0)
+        multi, ext = self._points_extrema(pts)
+        return np.array([self._sum_squares(self._trace_values(multi, ext, j))
+                         for j in range(len(pts))])
+
     def _extra_jacobian(self, i: int, x_row) -> tuple[np.ndarray, np.ndarray]:
-        """J_e [P][E] and r_e [E] of run i at x (extra_rows_host on its template)."""
+        """J [P][E + E_t] and r [E + E_t] of run i at x: the ExtraResiduals rows, then the
+        trace-dependent rows, by central differences with the FD Jacobian's pattern
+        (extra_rows_cpu, src/optim/adjoint_jacobian.cpp:300)."""
         vs = self._var_set(i)
-        t = 0 if self.host.variants == 1 else i
-        J, r = extra_rows_host(self.host.subset(t, 1), vs, x_row[:vs.size], self.options.extra)
-        return J[0], r[0]
+        P = vs.size
+        x = np.ascontiguousarray(x_row[:P], dtype=np.float64)
+        parts_J, parts_r = [], []
+        if self._plain_rows():
+            J, r = extra_rows_host(self.host.subset(self._template(i), 1), vs, x,
+                                   self.options.extra)
+            parts_J.append(J[0])
+            parts_r.append(r[0])
+        Et = self._trace_rows()
+        if Et:
+            xp, xm, dp, dm = (np.zeros(P) for _ in range(4))
+            st = np.zeros(P, dtype=np.int32)
+            vc = vs.c_struct()
+            _capi.check(self.lib.mkb_fd_pattern_host(
+                C.byref(vc), _capi.ptr(x), 1, _capi.ptr(xp), _capi.ptr(xm), _capi.ptr(dp),
+                _capi.ptr(dm), _capi.ptr(st, C.c_int32)), "fd pattern")
+            pts = [(i, x)]
+            for k in range(P):
+                for val in (xp[k], xm[k]):
+                    y = x.copy()
+                    y[k] = val
+                    pts.append((i, y))
+            multi, ext = self._points_extrema(pts)
+            vals = [self._trace_values(multi, ext, j) for j in range(len(pts))]
+            J = np.zeros((P, Et))
+            for k in range(P):
+                col = np.zeros(Et)
+                _capi.check(self.lib.mkb_fd_derivative_host(
+                    int(st[k]), float(dp[k]), float(dm[k]), Et, _capi.ptr(vals[0]),
+                    _capi.ptr(vals[1 + 2 * k]), _capi.ptr(vals[2 + 2 * k]), _capi.ptr(col)),
+                    "fd derivative")
+                J[k] = col
+            parts_J.append(J)
+            parts_r.append(vals[0])
+        return np.concatenate(parts_J, axis=1), np.concatenate(parts_r)
 
     def _points(self, want: bool):
         flags = np.zeros(self.runs, dtype=np.int32)
@@ -1004,9 +1099,10 @@ class DeviceLm:
         return flags, rows
 
     def _cycle_with_extra_rows(self) -> None:
-        E = self.options.extra.count
+        E = self._extra_rows()
         ws = (C.c_void_p(self.workspace.data_ptr()), self.workspace.numel())
         h = _stream_handle(self.stream)
+        dev = self.templates.device
         _capi.check(self.lib.mkb_lm_cycle_jacobian_device(*self._args(), self.runs, *ws, h),
                     "lm cycle (Jacobian)")
         want, x = self._points(True)
@@ -1016,7 +1112,7 @@ class DeviceLm:
             J, r = self._extra_jacobian(int(i), x[i])
             je[i, :J.shape[0]] = J
             re[i] = r
-        je_d, re_d = _dev_f64(je, self.templates.device), _dev_f64(re, self.templates.device)
+        je_d, re_d = _dev_f64(je, dev), _dev_f64(re, dev)
         _capi.check(self.lib.mkb_lm_extra_rows_device(
             *self._args(), self.runs, *ws, C.c_void_p(je_d.data_ptr()),
             C.c_void_p(re_d.data_ptr()), E, h), "lm extra rows")
@@ -1026,11 +1122,25 @@ class DeviceLm:
         em = np.zeros(self.runs)
         for i in np.nonzero(evaluate)[0]:
             em[i] = self._extra_merit(int(i), trial[i])
-        em_d = _dev_f64(em, self.templates.device)
-        _capi.check(self.lib.mkb_lm_cycle_accept_device(*self._args(), self.runs, *ws,
-                                                        C.c_void_p(em_d.data_ptr()), h),
-                    "lm cycle (acceptance)")
-        torch.cuda.synchronize(self.templates.device)
+        em_d = _dev_f64(em, dev)
+        if not self._trace_rows():
+            _capi.check(self.lib.mkb_lm_cycle_accept_device(*self._args(), self.runs, *ws,
+                                                            C.c_void_p(em_d.data_ptr()), h),
+                        "lm cycle (acceptance)")
+        else:
+            # the trace-dependent share needs the trial points' own extrema (the reference
+            # takes them from the trial MERIT); they are traced here with the engine
+            _capi.check(self.lib.mkb_lm_cycle_trial_device(
+                *self._args(), self.runs, *ws, C.c_void_p(em_d.data_ptr()), None, h),
+                "lm cycle (trial merit)")
+            idx = [int(i) for i in np.nonzero(evaluate)[0]]
+            tm = np.zeros(self.runs)
+            tm[idx] = self._trace_merits([(i, trial[i]) for i in idx])
+            tm_d = _dev_f64(tm, dev)
+            _capi.check(self.lib.mkb_lm_cycle_decide_device(
+                *self._args(), self.runs, *ws, C.c_void_p(tm_d.data_ptr()), h),
+                "lm cycle (acceptance)")
+        torch.cuda.synchronize(dev)
         self.cycles += 1
 
     def capture(self) -> "torch.cuda.CUDAGraph":

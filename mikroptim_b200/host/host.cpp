@@ -1098,7 +1098,7 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
     }
     check(mkb_lm_start_ex_device(&t, plan->get(), &v, &o, x,
                                  E > 0 ? static_cast<const double*>(dextra.get()) : nullptr,
-                                 runs, ws.get(), ws.bytes(), engine.stream()),
+                                 nullptr, runs, ws.get(), ws.bytes(), engine.stream()),
           "lm start");
     int32_t running = runs;
     int cycles = 0;

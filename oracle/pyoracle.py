@@ -154,7 +154,9 @@ class Reference(_Oracle):
         L.mko_ref_optimize_lm.argtypes = [_PB, _PP, _PV, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
-                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]
         L.mko_ref_optimize_lm.restype = C.c_int
         L.mko_ref_paraxial_residuals.argtypes = [_PB, _PP, C.c_int, C.c_int, C.c_void_p,
                                                  C.c_void_p, C.c_void_p, C.c_void_p,
@@ -204,6 +206,15 @@ class Reference(_Oracle):
         self._keep_c = (t, m, w, g)
         return (n, t.ctypes.data, m.ctypes.data, w.ctypes.data, g.ctypes.data)
 
+    def _tcall(self, tc):
+        tc = list(tc or [])
+        a = (np.array([k[0] for k in tc], dtype=np.int32),
+             np.array([k[1] for k in tc], dtype=np.int32),
+             np.array([k[2] for k in tc], dtype=np.float64),
+             np.array([k[3] for k in tc], dtype=np.float64))
+        self._keep_t = a
+        return (len(tc),) + tuple(x.ctypes.data for x in a)
+
     def paraxial_residuals(self, batch, layout, v: int, constraints) -> np.ndarray:
         """The reference's paraxial_residuals of variant v (its ExtraResidualFn)."""
         n, t, m, w, g = self._constraints(constraints)
@@ -240,7 +251,9 @@ class Reference(_Oracle):
 
     def optimize_lm(self, batch, layout, vs, x0, max_iterations: int = 100,
                     method: str = "adjoint", penalty_rounds: int = 1, threads: int = 0,
-                    constraints=None):
+                    constraints=None, trace_constraints=None):
+        """trace_constraints: [(surface, kind, weight, limit)], rows from the extrema of the
+        trace: kind 0 sqrt(w) max(0, h_s - limit), kind 1 sqrt(w) max(0, limit - cos I_s)."""
         x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, vs.size)
         runs, P = x0.shape
         x = np.zeros((runs, P))
@@ -254,7 +267,7 @@ class Reference(_Oracle):
             C.byref(view), C.byref(plan), C.byref(vars_), x0.ctypes.data, runs, max_iterations,
             1 if method == "adjoint" else 0, penalty_rounds, threads, x.ctypes.data,
             merit.ctypes.data, status.ctypes.data, its.ctypes.data, acc.ctypes.data,
-            hist.ctypes.data, *self._ccall(constraints))
+            hist.ctypes.data, *self._ccall(constraints), *self._tcall(trace_constraints))
         self._check(rc, "optimize_lm")
         return dict(x=x, merit=merit, status=status, iterations=its, accepted=acc,
                     history=hist)

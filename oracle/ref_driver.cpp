@@ -26,9 +26,11 @@
 #include "mikroptim/optim/levenberg_marquardt.hpp"
 #include "mikroptim/optim/normal_equations.hpp"
 #include "mikroptim/optim/paraxial_residuals.hpp"
+#include "mikroptim/optim/trace_extra_residuals.hpp"
 #include "mikroptim/optim/variable_set.hpp"
 #include "optim/parallel_variants.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -454,7 +456,8 @@ int mko_ref_optimize_lm(const mkb_batch_view* view, const mkb_residual_plan* pla
                         double* merit_out, int32_t* status_out, int32_t* iterations_out,
                         int32_t* accepted_out, double* history_out, int n_constraints,
                         const int32_t* c_type, const int32_t* c_mode, const double* c_weight,
-                        const double* c_target) {
+                        const double* c_target, int n_trace, const int32_t* t_surface,
+                        const int32_t* t_kind, const double* t_weight, const double* t_limit) {
     try {
         const mko::SystemBatchHost b = batch_of_view(*view, *plan);
         const mko::SystemDescription d = description_of(b, *vars, x0);
@@ -474,6 +477,23 @@ int mko_ref_optimize_lm(const mkb_batch_view* view, const mkb_residual_plan* pla
                 constraints_of(n_constraints, c_type, c_mode, c_weight, c_target);
             mko::check_paraxial_constraints(c, b.topology());
             opt.jacobian.extra = mko::make_paraxial_residuals(c);
+        }
+        if (n_trace > 0) {
+            // trace-dependent rows from the extrema: kind 0 sqrt(w) max(0, h_s - limit) (a
+            // semi-diameter), kind 1 sqrt(w) max(0, limit - cos I_s) (an incidence angle)
+            std::vector<int32_t> ts(t_surface, t_surface + n_trace), tk(t_kind, t_kind + n_trace);
+            std::vector<double> tw(t_weight, t_weight + n_trace), tl(t_limit, t_limit + n_trace);
+            mko::TraceExtraResiduals te;
+            te.count = n_trace;
+            te.evaluate = [ts, tk, tw, tl](const mko::SystemBatchHost&, int,
+                                           const mko::VariantExtrema& e, std::span<double> out) {
+                for (std::size_t i = 0; i < ts.size(); ++i) {
+                    const double q = tk[i] == 0 ? e.max_height(ts[i]) - tl[i]
+                                                : tl[i] - e.min_cos_incidence(ts[i]);
+                    out[i] = std::sqrt(tw[i]) * std::max(0.0, q);
+                }
+            };
+            opt.jacobian.trace_extra = te;
         }
         const auto P = static_cast<std::size_t>(vars->count);
         const mko::LmResult res = mko::optimize_lm_cpu(

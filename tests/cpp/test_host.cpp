@@ -27,7 +27,8 @@ extern "C" int mko_ref_optimize_lm(const mkb_batch_view*, const mkb_residual_pla
                                    const mkb_variables*, const double*, int, int, int, int, int,
                                    double*, double*, int32_t*, int32_t*, int32_t*, double*, int,
                                    const int32_t*, const int32_t*, const double*,
-                                   const double*);
+                                   const double*, int, const int32_t*, const int32_t*,
+                                   const double*, const double*);
 #endif
 
 void expect(bool ok, const char* what) {
@@ -243,7 +244,8 @@ int main() {
         std::vector<int32_t> rs(V), ri(V), ra(V);
         expect(mko_ref_optimize_lm(&view, plan->get(), &cv, x0.data(), V, 8, 1, 1, 4, rx.data(),
                                    rm.data(), rs.data(), ri.data(), ra.data(), rh.data(), 3,
-                                   ctype, cmode, cw, ct) == 0,
+                                   ctype, cmode, cw, ct, 0, nullptr, nullptr, nullptr,
+                                   nullptr) == 0,
                "reference LM with constraints");
         std::vector<int32_t> gs(g.status.begin(), g.status.end());
         expect(same_bits(g.x, rx) && same_bits(g.merit, rm) && same_bits(gs, rs) &&
