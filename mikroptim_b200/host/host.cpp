@@ -1056,6 +1056,34 @@ SystemBatchHost run_template(const SystemBatchHost& base, int i) {
     return take_variants(base, {base.variants() == 1 ? 0 : i});
 }
 
+// The trace-dependent rows at the points (run i_j, y_j): one MERIT trace with extrema of all of
+// them; values [points][Et].
+std::vector<double> trace_rows_at(TraceEngine& engine, const VariableSet& variables,
+                                  const SystemBatchHost& base, const ResidualSettings& settings,
+                                  const TraceExtraResiduals& te, const std::vector<int>& runs,
+                                  const std::vector<double>& ys) {
+    const int P = variables.size(), n = static_cast<int>(runs.size()), Et = te.count;
+    std::vector<int> tmpl;
+    for (int i : runs) tmpl.push_back(base.variants() == 1 ? 0 : i);
+    SystemBatchHost multi = take_variants(base, tmpl);
+    for (int j = 0; j < n; ++j) variables.apply(multi, j, ys.data() + static_cast<size_t>(j) * P);
+    TraceSettings ts(settings);
+    ts.extrema = true;
+    const TraceOutput out = engine.run(multi, TraceMode::Merit, ts);
+    const size_t S2 = static_cast<size_t>(multi.surfaces()) * 2;
+    std::vector<double> vals(static_cast<size_t>(n) * Et);
+    for (int j = 0; j < n; ++j)
+        te.evaluate(multi, j, std::span<const double>(out.merit.extrema.data() + j * S2, S2),
+                    std::span<double>(vals.data() + static_cast<size_t>(j) * Et, Et));
+    return vals;
+}
+
+double sum_squares(const double* v, int n) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += v[i] * v[i];
+    return s;
+}
+
 LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const SystemBatchHost& base,
                  const std::vector<double>& x0, const LmOptions& options,
                  const ResidualSettings& settings, LmGpuStats* stats) {
@@ -1083,22 +1111,35 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
     const size_t bytes = mkb_lm_workspace_bytes(&t, plan->get(), &v, &o, runs);
     if (bytes == 0) check(MKB_ERR_ARGUMENT, "lm workspace");
     ws.reserve(bytes);
-    const int E = options.extra.count;
-    if (E < 0 || (E > 0 && !options.extra.evaluate))
+    const int E0 = options.extra.count, Et = options.trace_extra.count, E = E0 + Et;
+    if (E0 < 0 || (E0 > 0 && !options.extra.evaluate) || Et < 0 ||
+        (Et > 0 && !options.trace_extra.evaluate))
         throw std::invalid_argument("optimize_lm_gpu: extra rows need a count >= 0 and a function");
+    DeviceBuffer dtrace;
     std::vector<SystemBatchHost> work;  // one-variant working copies of the run templates
     DeviceBuffer dextra, dje, dre;
     std::vector<double> em(static_cast<size_t>(runs), 0.0);
     if (E > 0) {
         for (int i = 0; i < runs; ++i) work.push_back(run_template(base, i));
-        for (int i = 0; i < runs; ++i)
-            em[i] = extra_merit_at(variables, work[i], options.extra,
-                                   x0.data() + static_cast<size_t>(i) * P);
+        if (E0 > 0)
+            for (int i = 0; i < runs; ++i)
+                em[i] = extra_merit_at(variables, work[i], options.extra,
+                                       x0.data() + static_cast<size_t>(i) * P);
         upload(dextra, em, engine.stream());
     }
+    if (Et > 0) {
+        std::vector<int> all(static_cast<size_t>(runs));
+        for (int i = 0; i < runs; ++i) all[i] = i;
+        const std::vector<double> vals =
+            trace_rows_at(engine, variables, base, settings, options.trace_extra, all, x0);
+        std::vector<double> tm(static_cast<size_t>(runs));
+        for (int i = 0; i < runs; ++i) tm[i] = sum_squares(vals.data() + static_cast<size_t>(i) * Et, Et);
+        upload(dtrace, tm, engine.stream());
+    }
     check(mkb_lm_start_ex_device(&t, plan->get(), &v, &o, x,
-                                 E > 0 ? static_cast<const double*>(dextra.get()) : nullptr,
-                                 nullptr, runs, ws.get(), ws.bytes(), engine.stream()),
+                                 E0 > 0 ? static_cast<const double*>(dextra.get()) : nullptr,
+                                 Et > 0 ? static_cast<const double*>(dtrace.get()) : nullptr,
+                                 runs, ws.get(), ws.bytes(), engine.stream()),
           "lm start");
     int32_t running = runs;
     int cycles = 0;
@@ -1125,10 +1166,44 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
                 if (!flags[i]) continue;
                 std::vector<double> xi(pts.begin() + static_cast<ptrdiff_t>(i) * P,
                                        pts.begin() + static_cast<ptrdiff_t>(i + 1) * P);
-                std::vector<double> J1, r1;
-                extra_rows_host(variables, work[i], xi, options.extra, J1, r1);
-                std::copy(J1.begin(), J1.end(), je.begin() + static_cast<ptrdiff_t>(i) * P * E);
-                std::copy(r1.begin(), r1.end(), re.begin() + static_cast<ptrdiff_t>(i) * E);
+                double* Ji = je.data() + static_cast<size_t>(i) * P * E;
+                double* ri = re.data() + static_cast<size_t>(i) * E;
+                if (E0 > 0) {
+                    std::vector<double> J1, r1;
+                    extra_rows_host(variables, work[i], xi, options.extra, J1, r1);
+                    for (int k = 0; k < P; ++k)
+                        for (int e = 0; e < E0; ++e) Ji[k * E + e] = J1[k * E0 + e];
+                    for (int e = 0; e < E0; ++e) ri[e] = r1[e];
+                }
+                if (Et > 0) {  // FD points of run i traced with their extrema
+                    std::vector<double> xp(P), xm(P), dp(P), dm(P);
+                    std::vector<int32_t> st(P);
+                    const mkb_variables vc = variables.c_struct();
+                    check(mkb_fd_pattern_host(&vc, xi.data(), 1, xp.data(), xm.data(), dp.data(),
+                                              dm.data(), st.data()),
+                          "fd pattern");
+                    std::vector<int> who(static_cast<size_t>(2 * P + 1), i);
+                    std::vector<double> ys;
+                    ys.insert(ys.end(), xi.begin(), xi.end());
+                    for (int k = 0; k < P; ++k)
+                        for (double val : {xp[k], xm[k]}) {
+                            std::vector<double> y = xi;
+                            y[k] = val;
+                            ys.insert(ys.end(), y.begin(), y.end());
+                        }
+                    const std::vector<double> vals = trace_rows_at(
+                        engine, variables, base, settings, options.trace_extra, who, ys);
+                    std::vector<double> col(static_cast<size_t>(Et));
+                    for (int k = 0; k < P; ++k) {
+                        check(mkb_fd_derivative_host(
+                                  st[k], dp[k], dm[k], Et, vals.data(),
+                                  vals.data() + static_cast<size_t>(1 + 2 * k) * Et,
+                                  vals.data() + static_cast<size_t>(2 + 2 * k) * Et, col.data()),
+                              "fd derivative");
+                        for (int e = 0; e < Et; ++e) Ji[k * E + E0 + e] = col[e];
+                    }
+                    for (int e = 0; e < Et; ++e) ri[E0 + e] = vals[e];
+                }
             }
             const auto* dj = static_cast<const double*>(upload(dje, je, engine.stream()));
             const auto* dr = static_cast<const double*>(upload(dre, re, engine.stream()));
@@ -1143,13 +1218,39 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
                   "lm points");
             engine.synchronize();
             for (int i = 0; i < runs; ++i)
-                em[i] = flags[i] ? extra_merit_at(variables, work[i], options.extra,
-                                                  pts.data() + static_cast<size_t>(i) * P)
-                                 : 0.0;
+                em[i] = flags[i] && E0 > 0
+                            ? extra_merit_at(variables, work[i], options.extra,
+                                             pts.data() + static_cast<size_t>(i) * P)
+                            : 0.0;
             const auto* de = static_cast<const double*>(upload(dextra, em, engine.stream()));
-            check(mkb_lm_cycle_accept_device(&t, plan->get(), &v, &o, runs, ws.get(), ws.bytes(),
-                                             de, engine.stream()),
-                  "lm cycle (acceptance)");
+            if (Et == 0) {
+                check(mkb_lm_cycle_accept_device(&t, plan->get(), &v, &o, runs, ws.get(),
+                                                 ws.bytes(), de, engine.stream()),
+                      "lm cycle (acceptance)");
+            } else {  // trial MERIT, then the trial points' extrema rows, then acceptance
+                check(mkb_lm_cycle_trial_device(&t, plan->get(), &v, &o, runs, ws.get(),
+                                                ws.bytes(), de, nullptr, engine.stream()),
+                      "lm cycle (trial merit)");
+                std::vector<int> who;
+                std::vector<double> ys;
+                for (int i = 0; i < runs; ++i)
+                    if (flags[i]) {
+                        who.push_back(i);
+                        ys.insert(ys.end(), pts.begin() + static_cast<ptrdiff_t>(i) * P,
+                                  pts.begin() + static_cast<ptrdiff_t>(i + 1) * P);
+                    }
+                std::vector<double> tm(static_cast<size_t>(runs), 0.0);
+                if (!who.empty()) {
+                    const std::vector<double> vals = trace_rows_at(
+                        engine, variables, base, settings, options.trace_extra, who, ys);
+                    for (size_t j = 0; j < who.size(); ++j)
+                        tm[who[j]] = sum_squares(vals.data() + j * Et, Et);
+                }
+                const auto* dt = static_cast<const double*>(upload(dtrace, tm, engine.stream()));
+                check(mkb_lm_cycle_decide_device(&t, plan->get(), &v, &o, runs, ws.get(),
+                                                 ws.bytes(), dt, engine.stream()),
+                      "lm cycle (acceptance)");
+            }
         }
         ++cycles;
         check(mkb_lm_results_device(&t, plan->get(), &v, &o, runs, ws.get(), nullptr, nullptr,

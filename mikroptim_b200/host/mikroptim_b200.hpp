@@ -209,6 +209,17 @@ struct ExtraResiduals {
     std::function<void(const SystemBatchHost& batch, int v, std::span<double> out)> evaluate;
 };
 
+// TraceExtraResiduals (include/mikroptim/optim/trace_extra_residuals.hpp): rows from the
+// per-surface extrema of the same trace (semi-diameter, incidence-angle constraints);
+// evaluate(batch, v, extrema [S][2], out). Every FD point and trial point is traced with its
+// extrema; their sum t^2 is added to the merit after the MERIT kernel's sum.
+struct TraceExtraResiduals {
+    int count = 0;
+    std::function<void(const SystemBatchHost& batch, int v, std::span<const double> extrema,
+                       std::span<double> out)>
+        evaluate;
+};
+
 struct LmOptions {
     int max_iterations = 100;
     bool reject_new_failures = true;
@@ -223,6 +234,7 @@ struct LmOptions {
     double fail_weight_factor = 10.0;
     double max_fail_weight = 1e14;
     ExtraResiduals extra;  // the caller's extra rows (LmOptions::jacobian.extra); count 0: none
+    TraceExtraResiduals trace_extra;  // rows from the trace's extrema (::jacobian.trace_extra)
     mkb_lm_options c_struct() const;
 };
 

@@ -2,6 +2,7 @@
 // optimises a small singlet batch through the reference-shaped C++ classes and checks every
 // result against the oracle (oracle/liboracle.so, the C restatement of the reference CPU
 // path) -- bit for bit in the FP64 mode. Exit status 0 when every check passes.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -251,6 +252,28 @@ int main() {
         expect(same_bits(g.x, rx) && same_bits(g.merit, rm) && same_bits(gs, rs) &&
                    same_bits(g.iterations, ri) && same_bits(g.accepted, ra),
                "LM with extra rows bit-identical to the reference");
+
+        // plus rows from the trace's extrema (semi-diameter and incidence-angle limits)
+        const int32_t tsurf[3] = {1, 2, 2}, tkind[3] = {0, 0, 1};
+        const double tw[3] = {100.0, 50.0, 1e3}, tl[3] = {4.8, 4.7, 0.9995};
+        xo.trace_extra.count = 3;
+        xo.trace_extra.evaluate = [&](const SystemBatchHost&, int, std::span<const double> e,
+                                      std::span<double> out) {
+            for (int i = 0; i < 3; ++i) {
+                const double q = tkind[i] == 0 ? e[2 * tsurf[i]] - tl[i]
+                                               : tl[i] - e[2 * tsurf[i] + 1];
+                out[i] = std::sqrt(tw[i]) * std::max(0.0, q);
+            }
+        };
+        const cuda::LmResult g2 = cuda::optimize_lm_gpu(engine, vars, batch, x0, xo, settings);
+        expect(mko_ref_optimize_lm(&view, plan->get(), &cv, x0.data(), V, 8, 1, 1, 4, rx.data(),
+                                   rm.data(), rs.data(), ri.data(), ra.data(), rh.data(), 3,
+                                   ctype, cmode, cw, ct, 3, tsurf, tkind, tw, tl) == 0,
+               "reference LM with trace rows");
+        std::vector<int32_t> gs2(g2.status.begin(), g2.status.end());
+        expect(same_bits(g2.x, rx) && same_bits(g2.merit, rm) && same_bits(gs2, rs) &&
+                   same_bits(g2.iterations, ri) && same_bits(g2.accepted, ra),
+               "LM with trace-dependent rows bit-identical to the reference");
     }
 #endif
 
