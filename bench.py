@@ -55,17 +55,17 @@ WORKLOAD_LM = ("objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, 
                "curvatures, 15 thicknesses and the first element's Buchdahl glass (n0, nu1, nu2) "
                "(config 2 shape)")
 FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of the reference)
-# DRAM traffic of trace_kernel per variant from the ncu capture summarised in
-# profiles/trace_kernel_objective512.md (512 variants: 668,672 B read, 0 B written).
+# DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) measured once per kernel on a
+# smaller capture of the same workload, per unit, scaled below by the units of the timed launch
+# and reported with "traffic_source": "scaled capture".
+# trace_kernel, objective variants (512 captured: 668,672 B read, 0 B written)
 TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
-# DRAM traffic (read + write) of adjoint_gram_kernel per run, from the ncu capture summarised
-# in profiles/adjoint_gram_objective1184.md (1,184 runs of the P = 32 objective with a glass
-# variable: 1.941 GB read, 17.645 GB written), scaled by the runs of the launch.
+# adjoint_gram_kernel, objective runs with a glass variable, FP64_FMA (1,184 runs captured:
+# 1.941 GB read, 17.645 GB written)
 FUSED_TRAFFIC_BYTES_PER_RUN = (1.940772e9 + 17.644780e9) / 1184
-# The same for the uneven (config-3) runs, MIXED precision, both launches of the call, from
-# profiles/adjoint_gram_uneven1184.md (1,184 runs: 22.6 MB read, 1.822 GB written).
+# adjoint_gram_kernel, uneven runs, MIXED, both launches of a call (1,184 runs captured:
+# 22.6 MB read, 1.822 GB written)
 FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (19.521536e6 + 3.077120e6 + 1.344401e9 + 0.477131e9) / 1184
-
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -301,6 +301,7 @@ def run_b200(args, world, rank, local):
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "traffic": TRAFFIC_BYTES_PER_VARIANT * b.variants,
+                         "traffic_source": "scaled capture",
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                          "flop_model": "140 FLOP-eq per ray-surface step, (S-1)+2 steps per ray"},
             "fp64_exact": {"ms_per_step": exact_ms,
@@ -371,6 +372,98 @@ def opd_errors(b, st, runs: int = 256):
                      "median_abs_waves": float(np.median(np.abs(err[same]))),
                      "status_agreement": float(np.mean(stt == ref_st))}
     return out
+
+
+def gram_errors(ref: np.ndarray, got: np.ndarray) -> np.ndarray:
+    """|got - ref| / sqrt(|A_ii A_jj|) of every entry of one run's (P+1)^2 normal equations."""
+    d = np.abs(np.diagonal(ref))
+    d = np.maximum(d, 1e-20 * d.max() + 1e-300)
+    return (np.abs(got - ref) / np.sqrt(d[:, None] * d[None, :])).ravel()
+
+
+def mixed_accuracy(b, st, vss, x0, runs: int = 256, iterations: int = 100):
+    """What the FP32 reverse sweep costs on uneven runs: (1) the MIXED fused normal equations
+    against the FP64 (separately rounded) fused ones at the start points, per entry relative to
+    sqrt(A_ii A_jj), for the runs with <= 31 variables and the wider ones (each kind has its own
+    launch); (2) the final merit of a 100-iteration MIXED LM against the FP64-FMA LM."""
+    import torch
+    from mikroptim_b200 import engine
+    from mikroptim_b200.batch import (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED,
+                                      ResidualLayout)
+    sub = b.subset(0, runs)
+    vs = vss[:runs]
+    x = x0[:runs]
+    lay = {p: ResidualLayout(sub.topology, dataclasses.replace(st, precision=p))
+           for p in (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED)}
+    db = engine.DeviceSystemBatch(sub)
+    ref = engine.adjoint_normal_equations_runs_device(db, lay[PRECISION_FP64], sub, vs, x)
+    got = engine.adjoint_normal_equations_runs_device(db, lay[PRECISION_MIXED], sub, vs, x)
+    torch.cuda.synchronize()
+    narrow, wide = [], []
+    for i, v in enumerate(vs):
+        e = gram_errors(engine.gram_block(ref, i, v.size).cpu().numpy(),
+                        engine.gram_block(got, i, v.size).cpu().numpy())
+        (wide if v.size > 31 else narrow).append(e)
+
+    def stats(parts):
+        if not parts:
+            return None
+        e = np.concatenate(parts)
+        return {"runs": len(parts), "median": float(np.median(e)),
+                "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
+    opt = engine.LmOptions(max_iterations=iterations, jacobian=engine.JACOBIAN_ADJOINT,
+                           gram_exact=False)
+    m_mixed = engine.optimize_lm_gpu(sub, lay[PRECISION_MIXED], vs, x, opt)
+    m_fma = engine.optimize_lm_gpu(sub, lay[PRECISION_FP64_FMA], vs, x, opt)
+    rel = np.abs(m_mixed["merit"] - m_fma["merit"]) / np.maximum(np.abs(m_fma["merit"]), 1e-300)
+    return {"normal_equations_vs_fp64": {"le31_variables": stats(narrow),
+                                         "gt31_variables": stats(wide),
+                                         "error": "|A_mixed - A_fp64| / sqrt(A_ii A_jj)"},
+            "lm_final_merit_vs_fp64_fma": {
+                "runs": runs, "iterations": iterations,
+                "median_rel": float(np.median(rel)), "p99_rel": float(np.quantile(rel, 0.99)),
+                "max_rel": float(rel.max()),
+                "mixed_not_worse_frac": float(np.mean(m_mixed["merit"] <=
+                                                      m_fma["merit"] * (1 + 1e-6)))}}
+
+
+def e2e_optimize(b, layout, variables, x0, world, dev, iterations: int = 100):
+    """optimize_lm_gpu end to end (the call `optimize --gpu` makes): host batch, variables and
+    start points in, host results out, 100 iterations plus penalty rounds, convergence included.
+    LM iterations taken / wall time (max over ranks); the bytes copied each way are counted
+    from the arrays the call uploads and downloads."""
+    import torch
+    from mikroptim_b200 import _capi, engine
+    opt = engine.LmOptions(max_iterations=iterations, jacobian=engine.JACOBIAN_ADJOINT,
+                           gram_exact=False)
+    runs = b.variants
+    per_run = isinstance(variables, (list, tuple))
+    P = max(v.size for v in variables) if per_run else variables.size
+    stride = int(_capi.lib().mkb_record_stride_ext(b.surfaces, b.wavelengths, b.fields,
+                                                   1 if b.non_coaxial else 0,
+                                                   b.topology.ghost_plates,
+                                                   b.topology.ghost_terms,
+                                                   1 if b.buchdahl_coeff is not None else 0))
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    res = engine.optimize_lm_gpu(b, layout, variables, x0, opt, device=dev.index or 0)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    wall = max_over_ranks(wall, world, dev)
+    iters = int(res["iterations"].sum())
+    rounds = int(res["penalty_rounds"].max())
+    # per pass: records + variant surface counts + x0 + the run-variable table in; x, merit,
+    # status, counters, damping, history, failed counts out
+    h2d = runs * (stride * 8 + P * 8 + ((1 + 1800) if per_run else 0))
+    d2h = runs * (P * 8 + 8 + 4 * 4 + 8 + 8 * (iterations + 1) + 16)
+    return {"value": world * iters / wall, "unit": "LM iterations/s",
+            "h2d_bytes_per_step": int(h2d * rounds), "d2h_bytes_per_step": int(d2h * rounds),
+            "api": "engine.optimize_lm_gpu(host batch, VariableSet(s), x0) -> host results",
+            "wall_s": wall, "iterations": iters, "runs": runs, "penalty_rounds_max": rounds,
+            "cycles": int(res["cycles"]),
+            "converged_runs": int(np.sum(res["status"] != 0)),
+            "step": "one full optimisation (100 iterations, convergence and penalty rounds)"}
 
 
 def run_lm(args, world, rank, local):
@@ -471,28 +564,9 @@ def run_lm(args, world, rank, local):
     torch.cuda.synchronize()
     merit_ms = e0.elapsed_time(e1) / 3
 
-    # ---- end to end through the host-buffer path: pinned x in, cycle, x and merit out ----
-    host_x = torch.from_numpy(x_np.copy()).pin_memory()
-    host_out = torch.empty((runs, P + 1), dtype=torch.float64).pin_memory()
-    dev_x = torch.empty_like(x_now)
-    lm2 = engine.DeviceLm(db, lay, b, vs, opt, runs)
-    lm2.start(x_np)
-    it0 = int(lm2.iterations().sum())
-    barrier(world)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        dev_x.copy_(host_x, non_blocking=True)
-        lm2.cycle()
-        lib.mkb_lm_results_device(*lm2._args(), runs, C.c_void_p(lm2.workspace.data_ptr()),
-                                  C.c_void_p(host_out.data_ptr()),
-                                  C.c_void_p(host_out.data_ptr() + runs * P * 8),
-                                  *([None] * 9), C.c_void_p(stream.cuda_stream))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_iters = int(lm2.iterations().sum()) - it0
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
-    del lm2
+    # ---- end to end through the drop-in API: optimize_lm_gpu(host batch, variables, x0) ->
+    # host results, the full 100-iteration LM with its penalty rounds, convergence included
+    e2e = e2e_optimize(b, lay, vs, x0, world, dev)
 
     errors = opd_errors(b, st) if rank == 0 else None
     peak = fp64_peak_tflops(torch) if rank == 0 else None
@@ -529,13 +603,12 @@ def run_lm(args, world, rank, local):
                     "speedup_adjoint_vs_fd": value / (world * fd_value),
                     "speedup_adjoint_mixed_vs_fd": mixed_value / (world * fd_value)},
         "opd_error_vs_fp64": errors,
-        "e2e": {"value": world * e2e_iters / (e2e_ms / 1e3), "unit": "LM iterations/s",
-                "h2d_bytes_per_step": int(runs * P * 8),
-                "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
+        "e2e": e2e,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": (FUSED_TRAFFIC_BYTES_PER_RUN * runs
                                  if FUSED_TRAFFIC_BYTES_PER_RUN else None),
+                     "traffic_source": "scaled capture",
                      "kernel": "adjoint_gram_kernel (fused adjoint + DMMA normal equations)",
                      "kernel_ms": kernel_ms,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
@@ -647,30 +720,12 @@ def run_uneven(args, world, rank, local):
     torch.cuda.synchronize()
     merit_ms = e0.elapsed_time(e1) / 3
 
-    # ---- end to end through the host-buffer path: pinned x in, cycle, x and merit out
-    host_x = torch.from_numpy(np.ascontiguousarray(x_now)).pin_memory()
-    host_out = torch.empty((runs, P + 1), dtype=torch.float64).pin_memory()
-    dev_x = torch.empty((runs, P), dtype=torch.float64, device=dev)
-    lm2 = engine.DeviceLm(db, lay_mixed, b, vss, opt, runs)
-    lm2.start(x_now)
-    it0 = int(lm2.iterations().sum())
-    barrier(world)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        dev_x.copy_(host_x, non_blocking=True)
-        lm2.cycle()
-        lib.mkb_lm_results_device(*lm2._args(), runs, C.c_void_p(lm2.workspace.data_ptr()),
-                                  C.c_void_p(host_out.data_ptr()),
-                                  C.c_void_p(host_out.data_ptr() + runs * P * 8),
-                                  *([None] * 9), C.c_void_p(stream.cuda_stream))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_iters = int(lm2.iterations().sum()) - it0
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
-    del lm2
+    # ---- end to end through the drop-in API: optimize_lm_gpu(host batch, variables, x0) ->
+    # host results, the full 100-iteration LM with its penalty rounds, convergence included
+    e2e = e2e_optimize(b, lay_mixed, vss, x0, world, dev)
 
     errors = opd_errors(b, st, runs=256) if rank == 0 else None
+    accuracy = mixed_accuracy(b, st, vss, x0, runs=256) if rank == 0 else None
     peak = fp64_peak_tflops(torch) if rank == 0 else None
     achieved = flop / (kernel_ms / 1e3) / 1e12
     if rank != 0:
@@ -686,7 +741,7 @@ def run_uneven(args, world, rank, local):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64+f32-adjoint",
         "data": "synthetic (seeded generator, configuration-3 shapes)",
         "config": {"workload": WORKLOAD_UNEVEN,
                    "step": "one batched LM cycle of all runs in one launch per kernel "
@@ -706,12 +761,12 @@ def run_uneven(args, world, rank, local):
                     "speedup_adjoint_mixed_vs_fd": value / (world * fd_value),
                     "speedup_adjoint_fma_vs_fd": fma_value / (world * fd_value)},
         "opd_error_vs_fp64": errors,
-        "e2e": {"value": world * e2e_iters / (e2e_ms / 1e3), "unit": "LM iterations/s",
-                "h2d_bytes_per_step": int(runs * P * 8),
-                "d2h_bytes_per_step": int(runs * (P + 1) * 8)},
+        "e2e": e2e,
+        "mixed_accuracy": accuracy,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN * runs,
+                     "traffic_source": "scaled capture",
                      "kernel": "adjoint_gram_kernel<MixedPrecision> (fused adjoint + DMMA "
                                "normal equations, every run, with its apply kernel)",
                      "kernel_ms": kernel_ms,
@@ -1199,7 +1254,7 @@ def run_tolerancing(args, world, rank, local):
         "value": world * V / (ms_step / 1e3),
         "unit": "samples/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32-adjoint",
         "data": "synthetic (seeded generator, configuration-5 shapes)",
         "config": {"workload": WORKLOAD_TOL.format(V=V),
                    "step": "MERIT (FP64, FMA) + fused adjoint normal equations (MIXED: FP64 "

@@ -471,9 +471,11 @@ int mkb_normal_equations_device(const double* J, const double* r, int32_t runs, 
  * (every GPU that loads the library keeps it until the process exits). Limit: variants x
  * fields x wavelengths <= MKB_NOALLOC_MERIT_MAX_SLOTS per call; larger batches are rejected
  * with MKB_ERR_ARGUMENT before anything is enqueued. The array is shared by all calls, so
- * calls that overlap on the GPU race: run one at a time per device. The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress, no allocation) with that
- * device current; make that first call before any stream capture. */
+ * calls that overlap on the GPU race: run one at a time per device. Every call made outside
+ * a stream capture looks up the array's device address in the current context
+ * (cudaGetSymbolAddress, no allocation), so switching contexts or resetting the device between
+ * calls is safe; a call made while its stream is captured reuses the address the last
+ * uncaptured call on that device found, and fails with MKB_ERR_ARGUMENT if there was none. */
 #define MKB_NOALLOC_MERIT_MAX_SLOTS 262144
 int mkb_merit_noalloc_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
                              double* merit, int64_t* failed, int64_t* hard_failed, void* stream);
@@ -484,6 +486,14 @@ const char* mkb_version(void);
 /* Reads and clears the device-side error words (synchronising): MKB_OK, or MKB_ERR_TIMEOUT
  * when a bounded wait inside a kernel gave up since the last call. */
 int mkb_device_status(void);
+/* Polls the first wait on a kernel's bulk copy makes before it gives up, records
+ * MKB_ERR_TIMEOUT and leaves the block's outputs unwritten (default MKB_WAIT_POLLS_DEFAULT;
+ * 0 makes every such wait give up at once, which lets a test drive the failure path without a
+ * fault or a hang). The wait that drains the copy after a give-up keeps the default limit.
+ * Synchronising (cudaMemcpyToSymbol per kernel file); set it with no kernel in flight. No
+ * counterpart in the reference, whose waits are not bounded. */
+#define MKB_WAIT_POLLS_DEFAULT (1u << 24)
+int mkb_set_wait_limit(uint32_t polls);
 /* Number of kernel launches this library has enqueued in the calling process. */
 int64_t mkb_launch_count(void);
 

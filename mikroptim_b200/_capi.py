@@ -20,6 +20,7 @@ MKB_ERR_CUDA = -2
 MKB_ERR_WORKSPACE = -3
 MKB_ERR_TIMEOUT = -4
 MKB_ERR_UNSUPPORTED = -5
+MKB_WAIT_POLLS_DEFAULT = 1 << 24
 
 P_double = C.POINTER(C.c_double)
 P_int64 = C.POINTER(C.c_int64)
@@ -173,6 +174,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     lib.mkb_device_status.restype = c.c_int
+    lib.mkb_set_wait_limit.restype = c.c_int
+    lib.mkb_set_wait_limit.argtypes = [c.c_uint32]
     PV = C.POINTER(Variables)
     PB = C.POINTER(DeviceBatch)
     PP = C.POINTER(ResidualPlan)

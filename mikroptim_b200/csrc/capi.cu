@@ -407,6 +407,20 @@ int mkb_device_status(void) {
     return status;
 }
 
+int mkb_set_wait_limit(uint32_t polls) {
+    int (*setters[])(uint32_t) = {trace_device_error_wait_limit, gram_device_error_wait_limit,
+                                  adjoint_device_error_wait_limit,
+                                  jacobian_device_error_wait_limit, lm_device_error_wait_limit};
+    for (auto set : setters) {
+        const int rc = set(polls);
+        if (rc != MKB_OK) {
+            set_error("mkb_set_wait_limit: cudaMemcpyToSymbol failed");
+            return rc;
+        }
+    }
+    return MKB_OK;
+}
+
 int32_t mkb_record_stride(int32_t surfaces, int32_t wavelengths, int32_t fields) {
     return record_layout(surfaces, wavelengths, fields).stride;
 }

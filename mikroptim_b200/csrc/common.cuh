@@ -130,6 +130,10 @@ __device__ __forceinline__ int surfaces_of(const TraceParams& p, int v) {
 // kernels defines a reader with MKB_DEFINE_ERROR_READER and lists it in capi.cu, and
 // mkb_device_status() polls them all.
 static __device__ int g_device_error = 0;
+// Polls the first wait of a bulk copy makes before it gives up (per translation unit, like the
+// error word). mkb_set_wait_limit changes it so that a test can make the wait run out; the wait
+// that drains the copy after a give-up always keeps the full limit.
+static __device__ uint32_t g_wait_polls = MKB_WAIT_POLLS_DEFAULT;
 
 #define MKB_DEFINE_ERROR_READER(name)                                                     \
     int name() {                                                                           \
@@ -141,6 +145,11 @@ static __device__ int g_device_error = 0;
             cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int));                        \
         }                                                                                  \
         return value;                                                                      \
+    }                                                                                      \
+    int name##_wait_limit(uint32_t polls) {                                                \
+        return cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(polls)) == cudaSuccess      \
+                   ? MKB_OK                                                                \
+                   : MKB_ERR_CUDA;                                                         \
     }
 
 // ---- bulk copy into shared memory with an mbarrier (no multicast) ------------------------
@@ -206,12 +215,13 @@ __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t byte
         mbar_expect_tx(bar, bytes);
         bulk_copy_g2s(dst, src, bytes, bar);
     }
-    constexpr uint32_t kPolls = 1u << 24;
-    bool ok = mbar_wait(bar, use & 1u, kPolls);
+    bool ok = mbar_wait(bar, use & 1u, g_wait_polls);
     ok = __syncthreads_and(ok);
     if (!ok) {
         if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_TIMEOUT);
-        mbar_wait(bar, use & 1u, kPolls);
+        // the copy may still be in flight: drain it (bounded, full limit) before the block
+        // leaves, so that no bulk copy writes into shared memory a later block owns
+        mbar_wait(bar, use & 1u, MKB_WAIT_POLLS_DEFAULT);
         __syncthreads();
     }
     return ok;

@@ -521,10 +521,14 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_address[kMaxDevices] = {};
 }  // namespace
 
-// Device address of the scratch array on the current device. In host code the array's name
-// is only a host-side stand-in, so the address is looked up once per device (with that device
-// current) and cached; the lookup itself allocates nothing.
-int noalloc_merit_scratch(void** out) {
+// Device address of the scratch array in the current context. In host code the array's name
+// is only a host-side stand-in, so the address is looked up with the device current. The array
+// lives in the module loaded into each CUDA context, so an address found once is not kept for
+// good: every call made outside a stream capture looks it up again (the lookup allocates
+// nothing), which also covers a caller that switches to a non-primary context or resets the
+// device between calls. A call made while `stream` is being captured cannot look anything up
+// and uses the address that the last call outside a capture found on this device.
+int noalloc_merit_scratch(cudaStream_t stream, void** out) {
     int dev = 0;
     int rc = cuda_status(cudaGetDevice(&dev), "no-allocation MERIT: cudaGetDevice");
     if (rc != MKB_OK) return rc;
@@ -532,13 +536,21 @@ int noalloc_merit_scratch(void** out) {
         set_error("no-allocation MERIT: device %d out of range", dev);
         return MKB_ERR_ARGUMENT;
     }
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    rc = cuda_status(cudaStreamIsCapturing(stream, &capture),
+                     "no-allocation MERIT: cudaStreamIsCapturing");
+    if (rc != MKB_OK) return rc;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_address[dev] == nullptr) {
+    if (capture == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         rc = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_merit_scratch),
                          "no-allocation MERIT: cudaGetSymbolAddress");
         if (rc != MKB_OK) return rc;
         g_noalloc_address[dev] = p;
+    } else if (g_noalloc_address[dev] == nullptr) {
+        set_error("no-allocation MERIT: first call on device %d made during a stream capture; "
+                  "make one call outside the capture first", dev);
+        return MKB_ERR_ARGUMENT;
     }
     *out = g_noalloc_address[dev];
     return MKB_OK;
@@ -577,7 +589,7 @@ extern "C" int mkb_merit_noalloc_device(const mkb_device_batch* batch,
         return MKB_ERR_ARGUMENT;
     }
     void* scratch = nullptr;
-    rc = noalloc_merit_scratch(&scratch);
+    rc = noalloc_merit_scratch(static_cast<cudaStream_t>(stream), &scratch);
     if (rc != MKB_OK) return rc;
     return launch_merit(p, batch->records, merit, failed, hard_failed, scratch,
                         kNoAllocScratchBytes, plan->precision,

@@ -1214,12 +1214,61 @@ def _lm_pass(batch, layout, variables, x0, options, dev) -> dict:
         templates = DeviceSystemBatch(batch, dev)
         lm = DeviceLm(templates, layout, batch, variables, options, runs)
         lm.start(x0)
-        while lm.running() > 0:
-            lm.cycle()
+        if lm._extra_rows():
+            while lm.running() > 0:
+                lm.cycle()
+            cycles = lm.cycles
+        else:
+            cycles = _run_to_end(lm, options.max_iterations + 1)
         res = lm.results()
-        res["cycles"] = lm.cycles
+        res["cycles"] = cycles
         _device_status()
         return res
+
+
+def _run_to_end(lm: DeviceLm, max_cycles: int) -> int:
+    """Cycles until no run is running (or max_cycles): the first cycle directly (it sets kernel
+    attributes outside any capture), the rest as replays of one captured cycle. The count of
+    running runs after cycle k is copied to pinned memory and read while cycle k + 1 runs, so the
+    host never waits for an idle GPU; the one cycle that may run past the end changes nothing
+    (a run that stopped is masked out of every kernel). Returns the cycles that had a running
+    run."""
+    if lm.running() == 0:
+        return 0
+    lm.cycle()
+    done = 1
+    if max_cycles <= 1:
+        return done
+    stream = torch.cuda.current_stream(lm.templates.device)
+    count = torch.zeros(2, dtype=torch.int32).pin_memory()
+    ready = [torch.cuda.Event(), torch.cuda.Event()]
+
+    def read_count(slot: int) -> None:
+        rc = lm.lib.mkb_lm_results_device(*lm._args(), lm.runs,
+                                          C.c_void_p(lm.workspace.data_ptr()),
+                                          *([None] * 10),
+                                          C.c_void_p(count.data_ptr() + 4 * slot),
+                                          _stream_handle(stream))
+        _capi.check(rc, "lm results")
+        ready[slot].record(stream)
+
+    read_count(0)
+    graph = lm.capture()
+    try:
+        pending = 0  # slot holding the count after the last cycle enqueued before this one
+        while done < max_cycles:
+            graph.replay()
+            lm.cycles += 1
+            read_count(1 - pending)
+            ready[pending].synchronize()
+            if int(count[pending]) == 0:
+                break  # the cycle just enqueued found nothing running
+            done += 1
+            pending = 1 - pending
+        torch.cuda.synchronize(lm.templates.device)
+    finally:
+        del graph
+    return done
 
 
 LM_NUMERICAL_ERROR = 7  # LmStatus::NumericalError

@@ -51,25 +51,50 @@ def run_sharded(batch: SystemBatchHost, fn: Callable[[SystemBatchHost, int], dic
     return gather_rows(local, group)
 
 
-def merit_sharded(batch: SystemBatchHost, settings, group=None) -> dict[str, np.ndarray]:
-    """MERIT of all variants, each rank tracing its share on its own GPU."""
-    from .engine import TraceEngine, TraceMode
-    import torch
-    engine = TraceEngine(torch.cuda.current_device())
+def merit_sharded(batch: SystemBatchHost, settings, group=None,
+                  merit: Callable | None = None) -> dict[str, np.ndarray]:
+    """MERIT of all variants, each rank tracing its share on its own GPU.
+
+    `merit(shard, settings) -> (merit, failed, hard_failed)` replaces the trace (default:
+    TraceEngine.run in MERIT mode on the current device); the split and the gather are the
+    same either way."""
+    if merit is None:
+        from .engine import TraceEngine, TraceMode
+        import torch
+        engine = TraceEngine(torch.cuda.current_device())
+
+        def merit(shard, st):
+            out = engine.run(shard, TraceMode.MERIT, st).merit
+            return out.merit, out.failed, out.hard_failed
 
     def fn(shard, first):
-        out = engine.run(shard, TraceMode.MERIT, settings).merit
-        return {"merit": out.merit, "failed": out.failed, "hard_failed": out.hard_failed}
+        m, f, h = merit(shard, settings)
+        return {"merit": m, "failed": f, "hard_failed": h}
     return run_sharded(batch, fn, group)
 
 
 def optimize_lm_sharded(batch: SystemBatchHost, layout, variables, x0, options=None,
-                        group=None) -> dict[str, np.ndarray]:
-    """Batched LM of all runs, each rank optimising its share of the runs on its own GPU."""
-    from .engine import optimize_lm_gpu
-    import torch
+                        group=None, optimize: Callable | None = None) -> dict[str, np.ndarray]:
+    """Batched LM of all runs, each rank optimising its share of the runs on its own GPU.
+
+    `variables` is one VariableSet for all runs or a list of one per run (uneven batches: x0
+    rows padded to the largest count; each rank gets its runs' sets).
+    `optimize(shard, layout, variables, x_shard, options) -> dict` replaces the optimiser
+    (default: optimize_lm_gpu on the current device)."""
+    if optimize is None:
+        from .engine import optimize_lm_gpu
+        import torch
+
+        def optimize(shard, lay, vs, x_shard, opt):
+            return optimize_lm_gpu(shard, lay, vs, x_shard, opt,
+                                   device=torch.cuda.current_device())
+    per_run = isinstance(variables, (list, tuple))
+    width = max(v.size for v in variables) if per_run else variables.size
+    x0 = np.asarray(x0, dtype=np.float64).reshape(-1, width)
 
     def fn(shard, first, x_shard):
-        return optimize_lm_gpu(shard, layout, variables, x_shard, options,
-                               device=torch.cuda.current_device())
-    return run_sharded(batch, fn, group, x0=np.asarray(x0).reshape(-1, variables.size))
+        vs = list(variables[first:first + len(x_shard)]) if per_run else variables
+        out = optimize(shard, layout, vs, x_shard, options)
+        return {k: v for k, v in out.items()
+                if isinstance(v, np.ndarray) and v.ndim >= 1 and len(v) == len(x_shard)}
+    return run_sharded(batch, fn, group, x0=x0)

@@ -18,7 +18,21 @@ from mikroptim_b200.batch import ResidualLayout, SystemBatchHost, VariableSet
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmko_ref.so")
-REFERENCE_TREE = "/root/reference"
+
+
+def _reference_tree() -> str:
+    """The reference source tree: $MKB_REFERENCE_TREE, else the Makefile's default REF."""
+    env = os.environ.get("MKB_REFERENCE_TREE")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as fh:
+        for line in fh:
+            if line.startswith("REF ?="):
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
+REFERENCE_TREE = _reference_tree()
 
 
 def build(reference: bool = True) -> None:
@@ -26,8 +40,8 @@ def build(reference: bool = True) -> None:
     targets = ["oracle"]
     if reference and os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}", *targets],
-                   check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}",
+                    f"REF={REFERENCE_TREE}", *targets], check=True)
 
 
 _PB = C.POINTER(_capi.BatchView)

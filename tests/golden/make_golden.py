@@ -1,6 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in the container that has the reference tree:  python tests/golden/make_golden.py
+Run where the reference tree exists (oracle/Makefile's REF, or $MKB_REFERENCE_TREE):
+    python tests/golden/make_golden.py
 
 * gauss_legendre.json -- the reference's generated Gauss-Legendre table
   (include/mikroptim/pupil/gauss_legendre_table.hpp), read as text: orders 1..16.
@@ -31,7 +32,7 @@ from mikroptim_b200 import workloads  # noqa: E402
 from mikroptim_b200.batch import ResidualLayout  # noqa: E402
 import oracle.pyoracle as po  # noqa: E402
 
-TABLE = "/root/reference/include/mikroptim/pupil/gauss_legendre_table.hpp"
+TABLE = os.path.join(po.REFERENCE_TREE, "include/mikroptim/pupil/gauss_legendre_table.hpp")
 
 
 def gauss_legendre_fixture() -> None:

@@ -2,7 +2,9 @@
 and LM runs over ranks, the gather of the per-variant results in rank order, and a rank that
 fails before the gather -- the other rank's collective ends with an error after the process
 group's timeout instead of waiting for good. The traced work itself is the oracle's (CPU);
-the GPU path behind the same functions is merit_sharded / optimize_lm_sharded.
+merit_sharded / optimize_lm_sharded, the functions the GPU path runs, are driven with the
+oracle's MERIT and the reference's LM in place of the device calls and must give what one rank
+gives alone.
 """
 
 import os
@@ -15,6 +17,7 @@ import numpy as np
 import pytest
 
 from mikroptim_b200.multi import partition
+from conftest import has_reference_build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -47,6 +50,45 @@ WORKER = textwrap.dedent("""
         out = run_sharded(one, lambda shard, first, x: {"x": x * 2.0, "v": np.full(len(x), shard.variants)},
                           x0=x0)
         assert np.array_equal(out["x"], x0 * 2.0) and np.all(out["v"] == 1)
+    elif mode == "merit_sharded":
+        from mikroptim_b200.multi import merit_sharded
+        calls = []
+
+        def oracle_merit(shard, settings):
+            calls.append(shard.variants)
+            return port.merit(shard, ResidualLayout(shard.topology, settings))
+        out = merit_sharded(b, st, merit=oracle_merit)
+        m, f, h = port.merit(b, lay)
+        assert calls == [7 if rank == 0 else 6], calls
+        assert np.array_equal(out["merit"], m) and np.array_equal(out["failed"], f)
+        assert np.array_equal(out["hard_failed"], h)
+    elif mode == "lm_sharded":
+        from mikroptim_b200.multi import optimize_lm_sharded
+        ref = po.reference()
+
+        def oracle_lm(shard, layout, vs, x_shard, opt):
+            return ref.optimize_lm(shard, layout, vs, x_shard, max_iterations=opt)
+        one = b.subset(0, 1)
+        out = optimize_lm_sharded(one, lay, vs, x0, options=6, optimize=oracle_lm)
+        alone = ref.optimize_lm(one, lay, vs, x0, max_iterations=6)
+        for k in ("x", "merit", "status", "iterations", "history"):
+            assert np.array_equal(out[k], alone[k]), k
+        # uneven runs: every rank gets its own runs' variable sets and padded rows
+        ub, ust, uvss, ux0 = workloads.uneven(5, rings=2, spokes=4)
+        width = max(v.size for v in uvss)
+        seen = []
+
+        def sizes(shard, layout, vs, x_shard, opt):
+            seen.append((shard.variants, [v.size for v in vs], x_shard.shape))
+            return {"p": np.array([v.size for v in vs]), "x": x_shard + 1.0}
+        rows = np.stack([np.pad(np.asarray(r, float), (0, width - len(r))) for r in ux0])
+        out = optimize_lm_sharded(ub, ResidualLayout(ub.topology, ust), uvss, rows,
+                                  optimize=sizes)
+        first = 0 if rank == 0 else 3
+        n = 3 if rank == 0 else 2
+        assert seen == [(n, [v.size for v in uvss[first:first + n]], (n, width))], seen
+        assert np.array_equal(out["p"], [v.size for v in uvss])
+        assert np.array_equal(out["x"], rows + 1.0)
     elif mode == "fail":
         if rank == 1:
             raise SystemExit(3)  # leaves before the gather
@@ -97,8 +139,10 @@ def test_partition_contiguous_and_balanced():
         partition(4, 2, 2)
 
 
-@pytest.mark.parametrize("mode", ["merit", "runs"])
+@pytest.mark.parametrize("mode", ["merit", "runs", "merit_sharded", "lm_sharded"])
 def test_two_ranks_gather_in_rank_order(mode):
+    if mode == "lm_sharded" and not has_reference_build():
+        pytest.skip("reference CPU build not available")
     for rc, out, err in launch(mode):
         assert rc == 0, err[-2000:]
         assert "ok" in out

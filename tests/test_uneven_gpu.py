@@ -6,12 +6,14 @@ and its own variables -- bit for bit: the trace (FP64, checked against the oracl
 LM trajectories with the fused adjoint (FP64 with FMA) and with finite differences.
 """
 
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
 
 from mikroptim_b200 import engine, workloads
-from mikroptim_b200.batch import ResidualLayout
+from mikroptim_b200.batch import PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED, ResidualLayout
 import oracle.pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -82,3 +84,54 @@ def test_uneven_fused_normal_equations_equal_each_run_alone():
         alone = engine.adjoint_normal_equations_device(engine.DeviceSystemBatch(one), lone, one,
                                                        vs_alone, x0[v][None, :])
         assert torch.equal(engine.gram_block(gram, v, vss[v].size), alone[0]), v
+
+
+def _gram_errors(ref, got):
+    d = np.abs(np.diagonal(ref))
+    d = np.maximum(d, 1e-20 * d.max() + 1e-300)
+    return (np.abs(got - ref) / np.sqrt(d[:, None] * d[None, :])).ravel()
+
+
+def test_uneven_mixed_fused_normal_equations_both_launches_against_fp64():
+    """The headline kernel instance: the fused adjoint + normal equations in MIXED precision
+    (FP64 trace, FP32 reverse sweep and FP32 derivative rows) on configuration-3 runs with full
+    16 x 32 pupils, through both of its launches -- runs with <= 31 variables, and the launch
+    sized for the widest run -- against the FP64 fused normal equations (separately rounded
+    operations, within 1e-10 of the exact ones). Bar per entry, relative to sqrt(A_ii A_jj):
+    median <= 1e-5 and every entry <= 2e-3, in both launches."""
+    b, st, vss, x0 = workloads.uneven(96)
+    P = np.array([v.size for v in vss])
+    assert (P > 31).sum() >= 16 and (P <= 31).sum() >= 16
+    db = engine.DeviceSystemBatch(b)
+    lay = {p: ResidualLayout(b.topology, dataclasses.replace(st, precision=p))
+           for p in (PRECISION_FP64, PRECISION_MIXED)}
+    ref = engine.adjoint_normal_equations_runs_device(db, lay[PRECISION_FP64], b, vss, x0)
+    got = engine.adjoint_normal_equations_runs_device(db, lay[PRECISION_MIXED], b, vss, x0)
+    torch.cuda.synchronize()
+    errs = {"narrow": [], "wide": []}
+    for v in range(b.variants):
+        r = engine.gram_block(ref, v, vss[v].size).cpu().numpy()
+        g = engine.gram_block(got, v, vss[v].size).cpu().numpy()
+        assert np.isfinite(g).all(), v
+        errs["wide" if vss[v].size > 31 else "narrow"].append(_gram_errors(r, g))
+    for kind, parts in errs.items():
+        e = np.concatenate(parts)
+        assert np.median(e) <= 1e-5, (kind, np.median(e))
+        assert e.max() <= 2e-3, (kind, e.max())
+
+
+def test_uneven_mixed_lm_reaches_the_fp64_fma_optimum_in_100_iterations():
+    """100 LM iterations on configuration-3 runs: with the MIXED adjoint the steps differ from
+    the FP64-FMA adjoint's, the end points do not. Bar: final merits within 1e-6 relative
+    (median) and 1e-3 (every run), and never more than 1e-3 worse."""
+    b, st, vss, x0 = workloads.uneven(48)
+    opt = engine.LmOptions(max_iterations=100, jacobian=engine.JACOBIAN_ADJOINT, gram_exact=False)
+    lay = {p: ResidualLayout(b.topology, dataclasses.replace(st, precision=p))
+           for p in (PRECISION_FP64_FMA, PRECISION_MIXED)}
+    mixed = engine.optimize_lm_gpu(b, lay[PRECISION_MIXED], vss, x0, opt)
+    fma = engine.optimize_lm_gpu(b, lay[PRECISION_FP64_FMA], vss, x0, opt)
+    assert np.all(mixed["merit"] <= mixed["history"][:, 0])
+    rel = np.abs(mixed["merit"] - fma["merit"]) / np.abs(fma["merit"])
+    assert np.median(rel) <= 1e-6, np.median(rel)
+    assert rel.max() <= 1e-3, rel.max()
+    assert np.all(mixed["merit"] <= fma["merit"] * (1 + 1e-3))

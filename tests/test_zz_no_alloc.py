@@ -14,7 +14,8 @@ import pytest
 import torch
 
 from mikroptim_b200 import _capi, engine, workloads
-from mikroptim_b200.batch import PRECISION_FP64, PRECISION_FP64_FMA, ResidualLayout
+from mikroptim_b200.batch import (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED,
+                                  ResidualLayout)
 
 pytestmark = pytest.mark.gpu
 
@@ -54,7 +55,7 @@ def without_allocation(db, plan, dev):
     return m.cpu().numpy(), f.cpu().numpy(), h.cpu().numpy()
 
 
-@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP64_FMA])
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED])
 def test_no_alloc_merit_matches_workspace_entry_point_twice(precision):
     dev = torch.device("cuda", 0)
     for b, st, vs, x0 in (workloads.singlet(1024), workloads.objective(96)):
@@ -89,3 +90,23 @@ def test_no_alloc_merit_rejects_batches_beyond_the_limit():
                                               C.c_void_p(m.data_ptr()), None)
     assert rc == _capi.MKB_ERR_ARGUMENT
     assert "limit" in _capi.lib().mkb_last_error().decode()
+
+
+def test_no_alloc_merit_rejects_null_outputs_before_any_work():
+    dev = torch.device("cuda", 0)
+    b, st, vs, x0 = workloads.singlet(4)
+    lay = ResidualLayout(b.topology, st)
+    plan = lay.plan(b)
+    db = engine.DeviceSystemBatch(b, dev)
+    s = db.c_struct()
+    m = torch.full((4,), -1.0, dtype=torch.float64, device=dev)
+    f = torch.full((4,), -1, dtype=torch.int64, device=dev)
+    lib = _capi.lib()
+    for ptrs in ((None, f.data_ptr(), f.data_ptr()), (m.data_ptr(), None, f.data_ptr()),
+                 (m.data_ptr(), f.data_ptr(), None)):
+        rc = lib.mkb_merit_noalloc_device(C.byref(s), C.byref(plan),
+                                          *[C.c_void_p(p) if p else None for p in ptrs], None)
+        assert rc == _capi.MKB_ERR_ARGUMENT
+        assert "null" in lib.mkb_last_error().decode()
+    torch.cuda.synchronize()
+    assert torch.all(m == -1.0) and torch.all(f == -1)
