@@ -413,18 +413,28 @@ def mixed_accuracy(b, st, vss, x0, runs: int = 256, iterations: int = 100):
                 "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
     opt = engine.LmOptions(max_iterations=iterations, jacobian=engine.JACOBIAN_ADJOINT,
                            gram_exact=False)
-    m_mixed = engine.optimize_lm_gpu(sub, lay[PRECISION_MIXED], vs, x, opt)
-    m_fma = engine.optimize_lm_gpu(sub, lay[PRECISION_FP64_FMA], vs, x, opt)
-    rel = np.abs(m_mixed["merit"] - m_fma["merit"]) / np.maximum(np.abs(m_fma["merit"]), 1e-300)
+    lm = {p: engine.optimize_lm_gpu(sub, lay[p], vs, x, opt)
+          for p in (PRECISION_FP64, PRECISION_FP64_FMA, PRECISION_MIXED)}
+
+    def agreement(a, b_):
+        rel = np.abs(a["merit"] - b_["merit"]) / np.maximum(np.abs(b_["merit"]), 1e-300)
+        ratio = a["merit"] / b_["merit"]
+        conv = (np.isin(a["status"], (1, 2, 3, 4)) & np.isin(b_["status"], (1, 2, 3, 4)))
+        return {"median_rel": float(np.median(rel)), "p90_rel": float(np.quantile(rel, 0.9)),
+                "max_rel": float(rel.max()),
+                "geo_mean_ratio": float(np.exp(np.mean(np.log(ratio)))),
+                "lower_frac": float(np.mean(ratio < 1.0 - 1e-9)),
+                "higher_frac": float(np.mean(ratio > 1.0 + 1e-9)),
+                "converged_in_both": int(conv.sum()),
+                "converged_median_rel": float(np.median(rel[conv])) if conv.any() else None}
     return {"normal_equations_vs_fp64": {"le31_variables": stats(narrow),
                                          "gt31_variables": stats(wide),
                                          "error": "|A_mixed - A_fp64| / sqrt(A_ii A_jj)"},
-            "lm_final_merit_vs_fp64_fma": {
+            "lm_final_merit": {
                 "runs": runs, "iterations": iterations,
-                "median_rel": float(np.median(rel)), "p99_rel": float(np.quantile(rel, 0.99)),
-                "max_rel": float(rel.max()),
-                "mixed_not_worse_frac": float(np.mean(m_mixed["merit"] <=
-                                                      m_fma["merit"] * (1 + 1e-6)))}}
+                "at_iteration_limit_frac": float(np.mean(lm[PRECISION_FP64]["status"] == 5)),
+                "mixed_vs_fp64": agreement(lm[PRECISION_MIXED], lm[PRECISION_FP64]),
+                "fp64_fma_vs_fp64": agreement(lm[PRECISION_FP64_FMA], lm[PRECISION_FP64])}}
 
 
 def e2e_optimize(b, layout, variables, x0, world, dev, iterations: int = 100):

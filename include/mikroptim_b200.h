@@ -480,6 +480,68 @@ int mkb_normal_equations_device(const double* J, const double* r, int32_t runs, 
 int mkb_merit_noalloc_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
                              double* merit, int64_t* failed, int64_t* hard_failed, void* stream);
 
+/* ---- FP32 prefilter of multistart variants ---------------------------------------------------
+ * Replaces DevicePrefilter::run / download (include/mikroptim/cuda/prefilter.hpp,
+ * src/cuda/prefilter.cu:87,193) behind TraceEngine::prefilter_variants, whose CPU reference is
+ * prefilter_stats_cpu (src/batch/batch_prefilter.cpp). Every ray is traced in float with hard
+ * failure (prefilter_ray, include/mikroptim/merit/prefilter_ray.hpp) and carries a margin, the
+ * distance of its tests (d_z, cos I, cos I', the ghost-plate radicand, the reference sphere's
+ * discriminant and denominator) from their failure limits in units of a direction cosine. A
+ * ray is certain when its margin exceeds `boundary` (eta). Per variant: merit = sum over the
+ * tuples of sum_k r_k^2 over the certainly valid rays (piston over those rays, OPL relative to
+ * the tuple's axial optical length), optical_length = the largest |offset| + |OPL - offset| of
+ * a certainly valid ray, and the counts of certainly failed, uncertain valid and uncertain
+ * failed rays. The arithmetic is the reference's float arithmetic in its order (every
+ * operation separately rounded, sums in ascending sample order), so the results equal
+ * prefilter_stats_cpu bit for bit. The values only decide which variants are worth an FP64
+ * evaluation; they never enter a merit, a Jacobian or the optimiser.
+ *
+ * field_trig: device [V][F][2] = sinf, cosf of the field angle rounded to float, filled on the
+ * host by mkb_prefilter_field_trig_host (the reference takes them with the C library's sinf /
+ * cosf). Outputs device [V]. Scratch: mkb_prefilter_workspace_bytes(V, plan) bytes. Status
+ * MKB_ERR_ARGUMENT for a boundary that is negative or not finite. */
+size_t mkb_prefilter_workspace_bytes(int32_t variants, const mkb_residual_plan* plan);
+int mkb_prefilter_field_trig_host(const mkb_batch_view* view, float* field_trig);
+int mkb_prefilter_device(const mkb_device_batch* batch, const mkb_residual_plan* plan,
+                         const float* field_trig, double boundary, double* merit,
+                         double* optical_length, int64_t* failed, int64_t* uncertain_ok,
+                         int64_t* uncertain_failed, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
+/* Criteria and margins of the prefilter decision (PrefilterCriteria, PrefilterMargins,
+ * include/mikroptim/batch/batch_prefilter.hpp:35,52); mkb_prefilter_default_options fills the
+ * reference's defaults (0.5, +inf, +inf; 0.15, 32, 0.01). */
+typedef struct mkb_prefilter_options {
+    double max_failed_fraction;       /* (a) reject when failed > fraction * rays        */
+    double max_merit;                 /* (b) reject when the merit exceeds this          */
+    double max_merit_factor;          /* (c) reject when the merit exceeds factor * best */
+    double boundary;                  /* eta                                             */
+    double opl_error_factor;          /* kappa                                           */
+    double merit_relative;            /* m, in [0, 1)                                    */
+} mkb_prefilter_options;
+enum { MKB_PREFILTER_KEEP = 0, MKB_PREFILTER_FAILED_RAYS = 1, MKB_PREFILTER_MERIT_ABSOLUTE = 2,
+       MKB_PREFILTER_MERIT_RELATIVE = 4 };   /* PrefilterReason, batch_prefilter.hpp:87 */
+void mkb_prefilter_default_options(mkb_prefilter_options* options);
+
+/* The conservative decision from the per-variant results (host arrays; prefilter_decide,
+ * src/batch/batch_prefilter.cpp): bounds merit_lower <= F_FP64 <= merit_upper of the FP64 merit
+ * and the reason mask per variant (0 = keep), the bound of the best merit that criterion (c)
+ * uses and its variant (+inf and -1 when none), and the number kept. extra_merit: [V] or NULL
+ * (merit of further rows, added exactly). The plan's failure mode is the FP64 truth's. */
+int mkb_prefilter_decide_host(const mkb_residual_plan* plan, const mkb_prefilter_options* options,
+                              int32_t variants, const double* merit,
+                              const double* optical_length, const int64_t* failed,
+                              const int64_t* uncertain_ok, const int64_t* uncertain_failed,
+                              const double* extra_merit, double* merit_lower,
+                              double* merit_upper, uint8_t* reject, double* reference_merit,
+                              int32_t* reference_variant, int32_t* kept);
+/* The same rule without margins applied to FP64 merits and failed-ray counts (the truth the
+ * prefilter is tested against; prefilter_decide_exact, src/batch/batch_prefilter.cpp). */
+int mkb_prefilter_decide_exact_host(const mkb_prefilter_options* options, int32_t variants,
+                                    int64_t rays_per_variant, const double* merit,
+                                    const int64_t* failed, const double* extra_merit,
+                                    uint8_t* reject);
+
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);
 const char* mkb_version(void);

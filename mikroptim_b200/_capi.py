@@ -121,6 +121,19 @@ class TraceOptions(C.Structure):
                 ("extra_merit", C.c_void_p), ("extrema", C.c_void_p)]
 
 
+class PrefilterOptions(C.Structure):
+    """mkb_prefilter_options (PrefilterCriteria + PrefilterMargins, batch_prefilter.hpp:35,52)."""
+
+    _fields_ = [("max_failed_fraction", C.c_double), ("max_merit", C.c_double),
+                ("max_merit_factor", C.c_double), ("boundary", C.c_double),
+                ("opl_error_factor", C.c_double), ("merit_relative", C.c_double)]
+
+
+MKB_PREFILTER_KEEP = 0
+MKB_PREFILTER_FAILED_RAYS = 1
+MKB_PREFILTER_MERIT_ABSOLUTE = 2
+MKB_PREFILTER_MERIT_RELATIVE = 4
+
 _lock = threading.Lock()
 _lib = None
 
@@ -174,6 +187,22 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     lib.mkb_device_status.restype = c.c_int
+    PF = C.POINTER(PrefilterOptions)
+    lib.mkb_prefilter_workspace_bytes.restype = c.c_size_t
+    lib.mkb_prefilter_workspace_bytes.argtypes = [c.c_int32, C.POINTER(ResidualPlan)]
+    lib.mkb_prefilter_field_trig_host.restype = c.c_int
+    lib.mkb_prefilter_field_trig_host.argtypes = [C.POINTER(BatchView), c.c_void_p]
+    lib.mkb_prefilter_device.restype = c.c_int
+    lib.mkb_prefilter_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                         c.c_void_p, c.c_double] + [c.c_void_p] * 6 + \
+        [c.c_size_t, c.c_void_p]
+    lib.mkb_prefilter_default_options.restype = None
+    lib.mkb_prefilter_default_options.argtypes = [PF]
+    lib.mkb_prefilter_decide_host.restype = c.c_int
+    lib.mkb_prefilter_decide_host.argtypes = [C.POINTER(ResidualPlan), PF, c.c_int32] + \
+        [c.c_void_p] * 12
+    lib.mkb_prefilter_decide_exact_host.restype = c.c_int
+    lib.mkb_prefilter_decide_exact_host.argtypes = [PF, c.c_int32, c.c_int64] + [c.c_void_p] * 4
     lib.mkb_set_wait_limit.restype = c.c_int
     lib.mkb_set_wait_limit.argtypes = [c.c_uint32]
     PV = C.POINTER(Variables)

@@ -110,6 +110,18 @@ int check_plan(const mkb_residual_plan* plan) {
 
 }  // namespace
 
+int residual_scales(const mkb_residual_plan* plan, double* scale) {
+    const int rc = check_plan(plan);
+    if (rc != MKB_OK) return rc;
+    const double lambda_ref_mm = plan->reference_wavelength_nm * 1e-6;
+    for (int f = 0; f < plan->fields; ++f)
+        for (int l = 0; l < plan->wavelengths; ++l) {
+            const double w = tuple_weight(plan, f, l);
+            scale[f * plan->wavelengths + l] = w > 0.0 ? std::sqrt(w) / lambda_ref_mm : 0.0;
+        }
+    return MKB_OK;
+}
+
 int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* plan,
                       int pack_rays, TraceParams* out) {
     if (batch == nullptr) {
@@ -397,7 +409,7 @@ int64_t mkb_launch_count(void) { return g_launches.load(); }
 
 int mkb_device_status(void) {
     int (*readers[])() = {trace_device_error, gram_device_error, adjoint_device_error,
-                              jacobian_device_error, lm_device_error};
+                              jacobian_device_error, lm_device_error, prefilter_device_error};
     int status = MKB_OK;
     for (auto read : readers) {
         const int v = read();
@@ -410,7 +422,8 @@ int mkb_device_status(void) {
 int mkb_set_wait_limit(uint32_t polls) {
     int (*setters[])(uint32_t) = {trace_device_error_wait_limit, gram_device_error_wait_limit,
                                   adjoint_device_error_wait_limit,
-                                  jacobian_device_error_wait_limit, lm_device_error_wait_limit};
+                                  jacobian_device_error_wait_limit, lm_device_error_wait_limit,
+                                  prefilter_device_error_wait_limit};
     for (auto set : setters) {
         const int rc = set(polls);
         if (rc != MKB_OK) {

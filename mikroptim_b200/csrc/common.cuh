@@ -249,6 +249,27 @@ __device__ __forceinline__ bool operator<(Exact64 a, Exact64 b) { return a.v < b
 __device__ __forceinline__ bool operator>(Exact64 a, Exact64 b) { return a.v > b.v; }
 __device__ __forceinline__ bool operator>=(Exact64 a, Exact64 b) { return a.v >= b.v; }
 __device__ __forceinline__ Exact64 nsqrt(Exact64 a) { return __dsqrt_rn(a.v); }
+
+// `Exact32`: the same for float (the FP32 prefilter): every operation separately rounded,
+// division and square root correctly rounded -- the reference's CPU float arithmetic.
+struct Exact32 {
+    float v;
+    Exact32() = default;
+    __host__ __device__ constexpr Exact32(float x) : v(x) {}
+    __host__ __device__ constexpr Exact32(double x) : v(static_cast<float>(x)) {}
+};
+__device__ __forceinline__ Exact32 operator+(Exact32 a, Exact32 b) { return __fadd_rn(a.v, b.v); }
+__device__ __forceinline__ Exact32 operator-(Exact32 a, Exact32 b) { return __fsub_rn(a.v, b.v); }
+__device__ __forceinline__ Exact32 operator*(Exact32 a, Exact32 b) { return __fmul_rn(a.v, b.v); }
+__device__ __forceinline__ Exact32 operator/(Exact32 a, Exact32 b) { return __fdiv_rn(a.v, b.v); }
+__device__ __forceinline__ Exact32 operator-(Exact32 a) { return -a.v; }
+__device__ __forceinline__ Exact32& operator+=(Exact32& a, Exact32 b) { return a = a + b; }
+__device__ __forceinline__ Exact32& operator-=(Exact32& a, Exact32 b) { return a = a - b; }
+__device__ __forceinline__ bool operator<(Exact32 a, Exact32 b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(Exact32 a, Exact32 b) { return a.v > b.v; }
+__device__ __forceinline__ bool operator>=(Exact32 a, Exact32 b) { return a.v >= b.v; }
+__device__ __forceinline__ Exact32 nsqrt(Exact32 a) { return __fsqrt_rn(a.v); }
+__device__ __forceinline__ float value_of(Exact32 a) { return a.v; }
 __device__ __forceinline__ double nsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float nsqrt(float a) { return sqrtf(a); }
 __device__ __forceinline__ double value_of(double a) { return a; }
@@ -657,6 +678,10 @@ __device__ __forceinline__ void apply_variables(const VarParams& v, const Record
 void count_launch(int n = 1);
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t err, const char* what);
+
+// residual_scale of every tuple (f-major, then l) into scale[F * L], as make_trace_params
+// computes them; checks the plan first (MKB_OK or MKB_ERR_ARGUMENT).
+int residual_scales(const mkb_residual_plan* plan, double* scale);
 
 // Builds the parameter block from the batch and plan; returns MKB_OK or MKB_ERR_ARGUMENT.
 // `pack_rays` = rays one CTA traces (tuples are packed until this many rays).

@@ -78,10 +78,12 @@ int gram_device_error();
 int adjoint_device_error();
 int jacobian_device_error();
 int lm_device_error();
+int prefilter_device_error();
 int trace_device_error_wait_limit(uint32_t polls);
 int gram_device_error_wait_limit(uint32_t polls);
 int adjoint_device_error_wait_limit(uint32_t polls);
 int jacobian_device_error_wait_limit(uint32_t polls);
 int lm_device_error_wait_limit(uint32_t polls);
+int prefilter_device_error_wait_limit(uint32_t polls);
 
 }  // namespace mkb

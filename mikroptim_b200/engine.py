@@ -559,6 +559,18 @@ class TraceEngine:
             out.info.device_bytes = self.device_bytes()
         return out
 
+    def prefilter_variants(self, batch: SystemBatchHost,
+                           settings: "PrefilterSettings | None" = None) -> "PrefilterResult":
+        """FP32 prefilter of all variants (TraceEngine::prefilter_variants,
+        include/mikroptim/cuda/trace_engine.hpp:188): the float trace with margins on the device,
+        then the conservative decision on the host. The values only bound the FP64 merit for
+        the selection; kept variants are evaluated again with run()."""
+        settings = settings or PrefilterSettings()
+        layout = ResidualLayout(batch.topology, settings.quadrature)
+        stats = prefilter_device(DeviceSystemBatch(batch, self.device), layout, batch,
+                                 settings.options.boundary)
+        return prefilter_decide(stats, layout, batch, settings.options, settings.extra_merit)
+
     def run_on_device(self, batch: SystemBatchHost, settings, granularity: int,
                       consume) -> TraceRunInfo:
         """TraceEngine::run_on_device: RESIDUALS without the download. After each tranche's
@@ -663,6 +675,145 @@ class TraceEngine:
             batch.surfaces, batch.wavelengths, batch.fields, 1 if batch.non_coaxial else 0,
             batch.topology.ghost_plates, batch.topology.ghost_terms,
             1 if batch.buchdahl_coeff is not None else 0))
+
+
+@dataclass
+class PrefilterOptions:
+    """PrefilterCriteria + PrefilterMargins (include/mikroptim/batch/batch_prefilter.hpp:35,52)
+    with the reference's defaults."""
+
+    max_failed_fraction: float = 0.5
+    max_merit: float = float("inf")
+    max_merit_factor: float = float("inf")
+    boundary: float = 0.15
+    opl_error_factor: float = 32.0
+    merit_relative: float = 0.01
+
+    def c_struct(self) -> _capi.PrefilterOptions:
+        return _capi.PrefilterOptions(self.max_failed_fraction, self.max_merit,
+                                      self.max_merit_factor, self.boundary,
+                                      self.opl_error_factor, self.merit_relative)
+
+
+@dataclass
+class PrefilterSettings:
+    """PrefilterSettings (trace_engine.hpp:80): the quadrature of the later FP64 run, the
+    options, and an optional FP64 merit share per variant added to both bounds."""
+
+    quadrature: ResidualSettings = dataclasses.field(default_factory=ResidualSettings)
+    options: PrefilterOptions = dataclasses.field(default_factory=PrefilterOptions)
+    extra_merit: np.ndarray | None = None
+
+
+@dataclass
+class PrefilterStats:
+    """PrefilterStats (batch_prefilter.hpp:66): float results per variant, stored as double."""
+
+    variants: int = 0
+    rays_per_variant: int = 0
+    merit: np.ndarray = None
+    optical_length: np.ndarray = None
+    failed: np.ndarray = None
+    uncertain_ok: np.ndarray = None
+    uncertain_failed: np.ndarray = None
+
+    def uncertain(self, v: int) -> int:
+        return int(self.uncertain_ok[v] + self.uncertain_failed[v])
+
+
+@dataclass
+class PrefilterResult:
+    """PrefilterResult (batch_prefilter.hpp:94): bounds of the FP64 merit, the reason mask per
+    variant (0 = keep), the best-merit bound criterion (c) used and its variant, the count
+    kept."""
+
+    stats: PrefilterStats
+    merit_lower: np.ndarray
+    merit_upper: np.ndarray
+    reject: np.ndarray
+    reference_merit: float
+    reference_variant: int
+    kept: int
+
+    def keep(self, v: int) -> bool:
+        return self.reject[v] == _capi.MKB_PREFILTER_KEEP
+
+
+def prefilter_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: SystemBatchHost,
+                     boundary: float = 0.15, stream=None) -> PrefilterStats:
+    """The FP32 prefilter kernel on an uploaded batch (DevicePrefilter::run + download,
+    include/mikroptim/cuda/prefilter.hpp): per-variant raw results, bit-identical to the
+    reference's prefilter_stats_cpu."""
+    lib = _capi.lib()
+    V = dbatch.variants
+    dev = dbatch.device
+    view = host.view()
+    trig = np.zeros((max(V, 1), host.fields, 2), dtype=np.float32)
+    _capi.check(lib.mkb_prefilter_field_trig_host(C.byref(view), trig.ctypes.data),
+                "prefilter field table")
+    trig_d = torch.from_numpy(trig).to(dev)
+    plan = layout.plan(host)
+    outs = [torch.empty(max(V, 1), dtype=t, device=dev)
+            for t in (torch.float64, torch.float64, torch.int64, torch.int64, torch.int64)]
+    need = int(lib.mkb_prefilter_workspace_bytes(V, C.byref(plan)))
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+    b = dbatch.c_struct()
+    rc = lib.mkb_prefilter_device(C.byref(b), C.byref(plan), C.c_void_p(trig_d.data_ptr()),
+                                  float(boundary), *[C.c_void_p(o.data_ptr()) for o in outs],
+                                  C.c_void_p(ws.data_ptr()), ws.numel(), _stream_handle(stream))
+    _capi.check(rc, "prefilter")
+    host_outs = [o[:V].cpu().numpy() for o in outs]
+    return PrefilterStats(V, layout.rays_per_variant, *host_outs)
+
+
+def prefilter_decide(stats: PrefilterStats, layout: ResidualLayout, host: SystemBatchHost,
+                     options: PrefilterOptions | None = None,
+                     extra_merit=None) -> PrefilterResult:
+    """prefilter_decide (src/batch/batch_prefilter.cpp): the conservative decision from the raw
+    results (mkb_prefilter_decide_host)."""
+    lib = _capi.lib()
+    options = options or PrefilterOptions()
+    V = stats.variants
+    if extra_merit is not None:
+        extra_merit = np.ascontiguousarray(extra_merit, dtype=np.float64)
+        if extra_merit.shape != (V,):
+            raise ValueError(f"prefilter: extra_merit must have {V} values")
+    arrs = [np.ascontiguousarray(a, dtype=t) for a, t in (
+        (stats.merit, np.float64), (stats.optical_length, np.float64),
+        (stats.failed, np.int64), (stats.uncertain_ok, np.int64),
+        (stats.uncertain_failed, np.int64))]
+    lower, upper = np.zeros(V), np.zeros(V)
+    reject = np.zeros(V, dtype=np.uint8)
+    ref_m, ref_v, kept = C.c_double(), C.c_int32(), C.c_int32()
+    plan = layout.plan(host)
+    opts = options.c_struct()
+    rc = lib.mkb_prefilter_decide_host(
+        C.byref(plan), C.byref(opts), V, *[a.ctypes.data for a in arrs],
+        extra_merit.ctypes.data if extra_merit is not None else None, lower.ctypes.data,
+        upper.ctypes.data, reject.ctypes.data, C.addressof(ref_m), C.addressof(ref_v),
+        C.addressof(kept))
+    _capi.check(rc, "prefilter decide")
+    stats = dataclasses.replace(stats, merit=arrs[0], optical_length=arrs[1], failed=arrs[2],
+                                uncertain_ok=arrs[3], uncertain_failed=arrs[4])
+    return PrefilterResult(stats, lower, upper, reject, ref_m.value, ref_v.value, kept.value)
+
+
+def prefilter_decide_exact(merit, failed, rays_per_variant: int,
+                           options: PrefilterOptions | None = None, extra_merit=None):
+    """prefilter_decide_exact: the same rule without margins on FP64 merits (the truth)."""
+    lib = _capi.lib()
+    options = options or PrefilterOptions()
+    merit = np.ascontiguousarray(merit, dtype=np.float64)
+    failed = np.ascontiguousarray(failed, dtype=np.int64)
+    ex = None if extra_merit is None else np.ascontiguousarray(extra_merit, dtype=np.float64)
+    reject = np.zeros(len(merit), dtype=np.uint8)
+    opts = options.c_struct()
+    rc = lib.mkb_prefilter_decide_exact_host(C.byref(opts), len(merit), rays_per_variant,
+                                             merit.ctypes.data, failed.ctypes.data,
+                                             ex.ctypes.data if ex is not None else None,
+                                             reject.ctypes.data)
+    _capi.check(rc, "prefilter decide exact")
+    return reject
 
 
 class _UnitWeights:

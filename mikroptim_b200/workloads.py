@@ -543,6 +543,30 @@ def tolerancing(variants: int = 262144, seed: int = 20261203 + 5, elements: int 
     return b, settings, vs, x0
 
 
+def multistart(base: SystemBatchHost, seed: int = 20261203 + 21) -> SystemBatchHost:
+    """Multistart variants of `base` for the FP32 prefilter, in the manner of the reference's
+    acceptance batches (docs/numerik.md, "FP32-Vorfilterung"): every curvature scaled by
+    1 + U(-0.5, 0.5), every thickness between the stop and the working distance by
+    1 + U(-0.3, 0.3), the pupil radius by U(0.5, 2); every seventh variant is extreme (pupil by
+    U(3, 5), curvatures by 1 + U(-1, 1)). Many rays then fail and the merits spread over orders
+    of magnitude. Returns a new batch with the same topology and variant count."""
+    b = base.subset(0, base.variants)
+    V, S = b.variants, b.surfaces
+    rng = Stream(seed)
+    extreme = (np.arange(V) % 7) == 6
+    cu = rng.uniform(1, V * S).reshape(V, S)
+    tu = rng.uniform(2, V * S).reshape(V, S)
+    pu = rng.uniform(3, V)
+    cf = np.where(extreme[:, None], 1.0 + (2.0 * cu - 1.0), 1.0 + (cu - 0.5))
+    b.curvature[:] = b.curvature * cf
+    tf = 1.0 + 0.6 * (tu - 0.5)
+    inner = np.zeros((V, S), dtype=bool)
+    inner[:, 1:S - 1] = True
+    b.thickness[:] = np.where(inner, b.thickness * tf, b.thickness)
+    b.pupil_radius[:] = b.pupil_radius * np.where(extreme, 3.0 + 2.0 * pu, 0.5 + 1.5 * pu)
+    return b
+
+
 def unpad(batch: SystemBatchHost, v: int) -> SystemBatchHost:
     """Variant v of an uneven batch as a batch of its own S_v surfaces (one variant)."""
     n = int(batch.variant_surfaces[v]) if batch.variant_surfaces is not None else batch.surfaces

@@ -182,6 +182,15 @@ class Reference(_Oracle):
         L.mko_ref_extra_rows.restype = C.c_int
         L.mko_ref_surface_extrema.argtypes = [_PB, _PP, C.c_void_p]
         L.mko_ref_surface_extrema.restype = C.c_int
+        _PF = C.POINTER(_capi.PrefilterOptions)
+        L.mko_ref_prefilter.argtypes = [_PB, _PP, _PF] + [C.c_void_p] * 12
+        L.mko_ref_prefilter.restype = C.c_int
+        L.mko_ref_prefilter_decide_exact.argtypes = [_PF, C.c_int32, C.c_int64] + \
+            [C.c_void_p] * 4
+        L.mko_ref_prefilter_decide_exact.restype = C.c_int
+        L.mko_ref_prefilter_rays.argtypes = [_PB, _PP, C.c_int, C.c_double, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+        L.mko_ref_prefilter_rays.restype = C.c_int
 
     def error(self) -> str:
         return self.lib.mko_ref_last_error().decode(errors="replace")
@@ -262,6 +271,54 @@ class Reference(_Oracle):
                                          J.ctypes.data, r.ctypes.data)
         self._check(rc, "extra_rows")
         return J, r
+
+    def prefilter(self, batch, layout, options, extra=None) -> dict:
+        """prefilter_cpu (src/batch/batch_prefilter.cpp): raw per-variant results and the
+        decision. `options` is a _capi.PrefilterOptions."""
+        V = batch.variants
+        out = dict(merit=np.zeros(V), optical_length=np.zeros(V),
+                   failed=np.zeros(V, np.int64), uncertain_ok=np.zeros(V, np.int64),
+                   uncertain_failed=np.zeros(V, np.int64), merit_lower=np.zeros(V),
+                   merit_upper=np.zeros(V), reject=np.zeros(V, np.uint8))
+        ref_m = C.c_double()
+        ref_v = C.c_int32()
+        kept = C.c_int32()
+        ex = None if extra is None else np.ascontiguousarray(extra, dtype=np.float64)
+        view, plan = batch.view(), layout.plan(batch)
+        rc = self.lib.mko_ref_prefilter(
+            C.byref(view), C.byref(plan), C.byref(options),
+            ex.ctypes.data if ex is not None else None,
+            *[out[k].ctypes.data for k in ("merit", "optical_length", "failed", "uncertain_ok",
+                                           "uncertain_failed", "merit_lower", "merit_upper",
+                                           "reject")],
+            C.addressof(ref_m), C.addressof(ref_v), C.addressof(kept))
+        self._check(rc, "prefilter")
+        out.update(reference_merit=ref_m.value, reference_variant=ref_v.value, kept=kept.value)
+        return out
+
+    def prefilter_decide_exact(self, options, merit, failed, rays_per_variant, extra=None):
+        merit = np.ascontiguousarray(merit, dtype=np.float64)
+        failed = np.ascontiguousarray(failed, dtype=np.int64)
+        ex = None if extra is None else np.ascontiguousarray(extra, dtype=np.float64)
+        reject = np.zeros(len(merit), np.uint8)
+        rc = self.lib.mko_ref_prefilter_decide_exact(
+            C.byref(options), len(merit), rays_per_variant, merit.ctypes.data,
+            failed.ctypes.data, ex.ctypes.data if ex is not None else None, reject.ctypes.data)
+        self._check(rc, "prefilter_decide_exact")
+        return reject
+
+    def prefilter_rays(self, batch, layout, v: int, boundary: float):
+        """prefilter_rays_cpu: status, margin and certain flag of variant v's rays."""
+        R = layout.rays_per_variant
+        status = np.zeros(R, np.uint8)
+        margin = np.zeros(R)
+        certain = np.zeros(R, np.uint8)
+        view, plan = batch.view(), layout.plan(batch)
+        rc = self.lib.mko_ref_prefilter_rays(C.byref(view), C.byref(plan), v, boundary,
+                                             status.ctypes.data, margin.ctypes.data,
+                                             certain.ctypes.data)
+        self._check(rc, "prefilter_rays")
+        return status, margin, certain
 
     def optimize_lm(self, batch, layout, vs, x0, max_iterations: int = 100,
                     method: str = "adjoint", penalty_rounds: int = 1, threads: int = 0,

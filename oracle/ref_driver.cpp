@@ -12,12 +12,15 @@
 //   normal_equations_host  include/mikroptim/optim/normal_equations.hpp:33
 //   optimize_lm_cpu        src/optim/levenberg_marquardt.cpp:972
 //   paraxial_residuals     src/optim/paraxial_residuals.cpp:353 (extra residual rows)
+//   prefilter_stats_cpu, prefilter_decide, prefilter_decide_exact, prefilter_rays_cpu
+//                          src/batch/batch_prefilter.cpp (FP32 multistart prefilter)
 // Only tests/, the golden-fixture script and bench.py's CPU legs load this library.
 
 #include "mikroptim_b200.h"
 
 #include "mikroptim/batch/batch_extrema.hpp"
 #include "mikroptim/batch/batch_merit.hpp"
+#include "mikroptim/batch/batch_prefilter.hpp"
 #include "mikroptim/batch/batch_residuals.hpp"
 #include "mikroptim/batch/system_batch.hpp"
 #include "mikroptim/model/system.hpp"
@@ -332,6 +335,90 @@ int mko_ref_surface_extrema(const mkb_batch_view* view, const mkb_residual_plan*
         const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
         const mko::SurfaceExtremaResult r = mko::surface_extrema_cpu(b, layout);
         std::memcpy(out, r.values.data(), sizeof(double) * r.values.size());
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// FP32 prefilter, the reference's CPU path: per-variant raw results (prefilter_stats_cpu) and
+// the decision (prefilter_decide) with the criteria and margins of `o`; extra [V] or null.
+// Outputs [V]: merit, optical_length, failed, uncertain_ok, uncertain_failed, lower, upper,
+// reject; reference merit / variant and kept count.
+int mko_ref_prefilter(const mkb_batch_view* view, const mkb_residual_plan* plan,
+                      const mkb_prefilter_options* o, const double* extra, double* merit,
+                      double* optical_length, int64_t* failed, int64_t* uncertain_ok,
+                      int64_t* uncertain_failed, double* lower, double* upper, uint8_t* reject,
+                      double* reference_merit, int32_t* reference_variant, int32_t* kept) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
+        mko::PrefilterOptions opt;
+        opt.criteria.max_failed_fraction = o->max_failed_fraction;
+        opt.criteria.max_merit = o->max_merit;
+        opt.criteria.max_merit_factor = o->max_merit_factor;
+        opt.margins.boundary = o->boundary;
+        opt.margins.opl_error_factor = o->opl_error_factor;
+        opt.margins.merit_relative = o->merit_relative;
+        const std::size_t V = static_cast<std::size_t>(b.variants());
+        const mko::PrefilterResult r = mko::prefilter_cpu(
+            b, layout, opt,
+            extra != nullptr ? std::span<const double>(extra, V) : std::span<const double>());
+        for (std::size_t v = 0; v < V; ++v) {
+            merit[v] = r.stats.merit[v];
+            optical_length[v] = r.stats.optical_length[v];
+            failed[v] = r.stats.failed[v];
+            uncertain_ok[v] = r.stats.uncertain_ok[v];
+            uncertain_failed[v] = r.stats.uncertain_failed[v];
+            lower[v] = r.merit_lower[v];
+            upper[v] = r.merit_upper[v];
+            reject[v] = r.reject[v];
+        }
+        *reference_merit = r.reference_merit;
+        *reference_variant = r.reference_variant;
+        *kept = r.kept;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// The decision rule on FP64 merits (prefilter_decide_exact).
+int mko_ref_prefilter_decide_exact(const mkb_prefilter_options* o, int32_t V, int64_t rays,
+                                   const double* merit, const int64_t* failed,
+                                   const double* extra, uint8_t* reject) {
+    try {
+        mko::MeritResult m;
+        m.variants = V;
+        m.rays_per_variant = rays;
+        m.merit.assign(merit, merit + V);
+        m.failed.assign(failed, failed + V);
+        m.hard_failed.assign(static_cast<std::size_t>(V), 0);
+        mko::PrefilterCriteria c;
+        c.max_failed_fraction = o->max_failed_fraction;
+        c.max_merit = o->max_merit;
+        c.max_merit_factor = o->max_merit_factor;
+        const std::vector<std::uint8_t> r = mko::prefilter_decide_exact(
+            m, c,
+            extra != nullptr ? std::span<const double>(extra, static_cast<std::size_t>(V))
+                             : std::span<const double>());
+        std::copy(r.begin(), r.end(), reject);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Per-ray prefilter data of variant v (prefilter_rays_cpu): status, margin, certain [rays].
+int mko_ref_prefilter_rays(const mkb_batch_view* view, const mkb_residual_plan* plan, int v,
+                           double boundary, uint8_t* status, double* margin, uint8_t* certain) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        const mko::ResidualLayout layout(b.topology(), settings_of(*plan));
+        const mko::PrefilterRayData d = mko::prefilter_rays_cpu(b, v, layout, boundary);
+        std::copy(d.status.begin(), d.status.end(), status);
+        std::copy(d.margin.begin(), d.margin.end(), margin);
+        std::copy(d.certain.begin(), d.certain.end(), certain);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
