@@ -802,8 +802,10 @@ def run_singlet(args, world, rank, local):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
-    def graph_of(V, precision, evals, seed):
-        """A CUDA graph of `evals` evaluations of V singlets (outputs preallocated)."""
+    def graph_of(V, precision, evals, seed, tplans=None):
+        """A CUDA graph of `evals` evaluations of V singlets (outputs preallocated), RESIDUALS
+        and MERIT launched with the trace plans `tplans` = (residuals plan, merit plan), each
+        (pack_rays, variants_per_cta); None: the defaults."""
         b, st, vs, x0 = workloads.singlet(V, seed=seed)
         st.precision = precision
         lay = ResidualLayout(b.topology, st)
@@ -819,15 +821,16 @@ def run_singlet(args, world, rank, local):
         ws = torch.empty(int(lib.mkb_merit_workspace_bytes(V, C.byref(plan))), dtype=torch.uint8,
                          device=dev)
         bst = db.c_struct()
-        opts = engine._trace_options(0)
+        opts_r, opts_m = [engine._trace_options(0) if tplans is None else engine._trace_options(
+            tp.pack_rays, variants_per_cta=tp.variants_per_cta) for tp in (tplans or (0, 0))]
 
         def one():
             h = C.c_void_p(torch.cuda.current_stream().cuda_stream)
             _capi.check(lib.mkb_residuals_ex_device(
-                C.byref(bst), C.byref(plan), C.byref(opts), C.c_void_p(res.data_ptr()), rows,
+                C.byref(bst), C.byref(plan), C.byref(opts_r), C.c_void_p(res.data_ptr()), rows,
                 C.c_void_p(opd.data_ptr()), C.c_void_p(stat.data_ptr()), h), "residuals")
             _capi.check(lib.mkb_merit_ex_device(
-                C.byref(bst), C.byref(plan), C.byref(opts), C.c_void_p(merit.data_ptr()),
+                C.byref(bst), C.byref(plan), C.byref(opts_m), C.c_void_p(merit.data_ptr()),
                 C.c_void_p(failed.data_ptr()), C.c_void_p(hard.data_ptr()),
                 C.c_void_p(ws.data_ptr()), ws.numel(), h), "merit")
 
@@ -841,7 +844,7 @@ def run_singlet(args, world, rank, local):
                 one()
         per_graph = lib.mkb_launch_count() - l0
         torch.cuda.synchronize()
-        keep = (b, lay, db, res, opd, stat, merit, failed, hard, ws, plan, bst, opts)
+        keep = (b, lay, db, res, opd, stat, merit, failed, hard, ws, plan, bst, opts_r, opts_m)
         hits = 2 * V * rays * (b.surfaces - 1) * evals  # RESIDUALS and MERIT trace each ray
         flopeq = 2 * V * rays * FLOPEQ_PER_RAY_SURFACE * (b.surfaces - 1 + 2) * evals
         return g, per_graph, hits, flopeq, keep
@@ -864,7 +867,19 @@ def run_singlet(args, world, rank, local):
     V = args.variants or 1024
     evals = max(1, 102400 // V)
     seed = 20261203 + 1 + 1000 * rank
-    g, per_graph, hits, flopeq, keep = graph_of(V, PRECISION_FP64, evals, seed)
+    # the autotuner picks the launch shape of each trace (rays per CTA pack and variants per
+    # CTA) for this batch shape, outside the timed region; every plan gives the same bits
+    from mikroptim_b200 import autotune
+    tuner = autotune.TraceAutotuner(launches=20)
+    b0, st0, _, _ = workloads.singlet(V, seed=seed)
+    st0.precision = PRECISION_FP64
+    lay0 = ResidualLayout(b0.topology, st0)
+    tuned = {m: tuner.tune(b0, lay0, m) for m in ("residuals", "merit")}
+    plan_r = autotune.TracePlan(tuned["residuals"]["pack_rays"],
+                                tuned["residuals"]["variants_per_cta"])
+    plan_m = autotune.TracePlan(tuned["merit"]["pack_rays"], tuned["merit"]["variants_per_cta"])
+    g, per_graph, hits, flopeq, keep = graph_of(V, PRECISION_FP64, evals, seed,
+                                                (plan_r, plan_m))
     barrier(world)
     with ClockSampler(local) as clocks:
         ms_step = time_graph(g, args.steps, args.warmup)
@@ -881,14 +896,25 @@ def run_singlet(args, world, rank, local):
         ev = max(1, 102400 // n)
         row = {"variants": n, "evaluations_per_replay": ev}
         for name, prec in (("fp64", PRECISION_FP64), ("fp64_fma", PRECISION_FP64_FMA)):
-            gg, _, hh, ff, kk = graph_of(n, prec, ev, seed)
-            ms = time_graph(gg, 3, 2)
-            row[name] = {"ray_surface_hits_per_s": hh / (ms / 1e3),
-                         "tflopeq_per_s": ff / (ms / 1e3) / 1e12, "ms_per_replay": ms}
-            if n == V and prec == PRECISION_FP64_FMA:
-                fma_value = world * hh / (ms / 1e3)
-            del gg, kk
-            torch.cuda.empty_cache()
+            bn, stn, _, _ = workloads.singlet(n, seed=seed)
+            stn.precision = prec
+            layn = ResidualLayout(bn.topology, stn)
+            sweep_tuner = autotune.TraceAutotuner(launches=max(2, 20480 // n))
+            tp = [sweep_tuner.tune(bn, layn, m) for m in ("residuals", "merit")]
+            tps = tuple(autotune.TracePlan(t["pack_rays"], t["variants_per_cta"]) for t in tp)
+            row[name] = {}
+            for label, plans in (("default", None), ("tuned", tps)):
+                gg, _, hh, ff, kk = graph_of(n, prec, ev, seed, plans)
+                ms = time_graph(gg, 3, 2)
+                row[name][label] = {"ray_surface_hits_per_s": hh / (ms / 1e3),
+                                    "tflopeq_per_s": ff / (ms / 1e3) / 1e12,
+                                    "ms_per_replay": ms}
+                if n == V and prec == PRECISION_FP64_FMA and label == "tuned":
+                    fma_value = world * hh / (ms / 1e3)
+                del gg, kk
+                torch.cuda.empty_cache()
+            row[name]["plans"] = {"residuals": [tps[0].pack_rays, tps[0].variants_per_cta],
+                                  "merit": [tps[1].pack_rays, tps[1].variants_per_cta]}
         sweep.append(row)
 
     # end to end through the public API: host batch in, host residuals / OPD / status and merit
@@ -938,6 +964,12 @@ def run_singlet(args, world, rank, local):
                    "l2": "flushed (256 MB write) before every timed step"},
         "gpu_launches": int(per_graph * args.steps),
         "fp64_fma": {"value": fma_value, "unit": "ray-surface hits/s"},
+        "autotuned": {m: {"pack_rays": tuned[m]["pack_rays"],
+                          "variants_per_cta": tuned[m]["variants_per_cta"],
+                          "ms_per_launch": tuned[m]["ms"],
+                          "default_ms_per_launch": next(t[2] for t in tuned[m]["timings"]
+                                                        if t[0] == 512 and t[1] == 1)}
+                      for m in tuned},
         "size_sweep": sweep,
         "e2e": {"value": world * (hits / evals) / (e2e_ms / 1e3), "unit": "ray-surface hits/s",
                 "h2d_bytes_per_step": int(2 * V * stride * 8),

@@ -221,6 +221,10 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
  *                gets a pack of its own; values above 4096 are traced as 4096).
  *   extra_merit  MERIT only: device [V] or NULL; extra_merit[v] is added to variant v's merit
  *                after its tuple sums (MeritRunOptions::extra_merit, src/cuda/merit.cu:222).
+ *   variants_per_cta  how many variants one CTA traces side by side (0 = 1, at most 8): its
+ *                threads, the per-tuple reductions and the barriers are then shared by the
+ *                packs of several variants. Runtime only, like pack_rays (bit-identical results
+ *                for every value); not with extrema. The trace autotuner picks both.
  *   extrema      device [V][S][2] or NULL: per variant and table surface the largest ray
  *                height sqrt(x^2 + y^2) at the surface and the smallest cos I (d before the
  *                refraction . surface normal) over the rays with status Ok; surface 0 holds
@@ -229,7 +233,7 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
  *                maxima). Coaxial batches only (MKB_ERR_UNSUPPORTED otherwise). */
 typedef struct mkb_trace_options {
     int32_t pack_rays;
-    int32_t reserved;                 /* 0                                               */
+    int32_t variants_per_cta;
     const double* extra_merit;
     double* extrema;
 } mkb_trace_options;

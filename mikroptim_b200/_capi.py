@@ -117,7 +117,7 @@ class LmOptions(C.Structure):
 class TraceOptions(C.Structure):
     """mkb_trace_options (TraceSettings::pack_rays / ::extra_merit, trace_engine.hpp:58)."""
 
-    _fields_ = [("pack_rays", C.c_int32), ("reserved", C.c_int32),
+    _fields_ = [("pack_rays", C.c_int32), ("variants_per_cta", C.c_int32),
                 ("extra_merit", C.c_void_p), ("extrema", C.c_void_p)]
 
 

@@ -284,6 +284,7 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         ++packs;
     }
     p.n_packs = packs;
+    p.vpc = 1;
     p.pack_max = 0;
     for (int k = 0; k < packs; ++k)
         if (p.packs[k].rays > p.pack_max) p.pack_max = p.packs[k].rays;
@@ -578,6 +579,21 @@ int options_pack_rays(const mkb_trace_options* options, int* pack_rays) {
     return MKB_OK;
 }
 
+// variants_per_cta of the options (0 or no options: 1); with extrema it must be 1
+int options_vpc(const mkb_trace_options* options, TraceParams* p) {
+    const int v = options != nullptr ? options->variants_per_cta : 0;
+    if (v < 0 || v > kMaxVariantsPerCta) {
+        set_error("variants_per_cta must be in [1, %d] (0 = 1), got %d", kMaxVariantsPerCta, v);
+        return MKB_ERR_ARGUMENT;
+    }
+    p->vpc = v == 0 ? 1 : v;
+    if (p->vpc > 1 && options->extrema != nullptr) {
+        set_error("variants_per_cta > 1 is not available with extrema");
+        return MKB_ERR_UNSUPPORTED;
+    }
+    return MKB_OK;
+}
+
 int check_trace_precision(int precision, const char* what) {
     if (precision != MKB_PRECISION_FP64 && precision != MKB_PRECISION_FP64_FMA &&
         precision != MKB_PRECISION_MIXED) {
@@ -597,6 +613,8 @@ int mkb_residuals_ex_device(const mkb_device_batch* batch, const mkb_residual_pl
     if (rc != MKB_OK) return rc;
     TraceParams p;
     rc = make_trace_params(batch, plan, pack_rays, &p);
+    if (rc != MKB_OK) return rc;
+    rc = options_vpc(options, &p);
     if (rc != MKB_OK) return rc;
     rc = check_trace_precision(plan->precision, "residuals");
     if (rc != MKB_OK) return rc;
@@ -636,6 +654,8 @@ int mkb_merit_ex_device(const mkb_device_batch* batch, const mkb_residual_plan* 
     if (rc != MKB_OK) return rc;
     TraceParams p;
     rc = make_trace_params(batch, plan, pack_rays, &p);
+    if (rc != MKB_OK) return rc;
+    rc = options_vpc(options, &p);
     if (rc != MKB_OK) return rc;
     rc = check_trace_precision(plan->precision, "merit");
     if (rc != MKB_OK) return rc;

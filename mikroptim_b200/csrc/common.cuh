@@ -95,6 +95,7 @@ struct TraceParams {
     int rings, spokes;
     int n_tuples, n_packs;
     int pack_max;           // rays of the largest pack
+    int vpc;                // variants one CTA traces (its packs side by side), >= 1
     int sample_count[kMaxFields];   // n_f
     int field_offset[kMaxFields];   // ray offset of tuple (f, 0)
     uint8_t pupil_mode[kMaxFields];
@@ -222,6 +223,43 @@ __device__ inline bool stage_to_shared(void* dst, const void* src, uint32_t byte
         // the copy may still be in flight: drain it (bounded, full limit) before the block
         // leaves, so that no bulk copy writes into shared memory a later block owns
         mbar_wait(bar, use & 1u, MKB_WAIT_POLLS_DEFAULT);
+        __syncthreads();
+    }
+    return ok;
+}
+
+// Stages `count` records of `bytes` each (multiple of 16, 16-byte aligned) from src[j] into
+// dst + j * dst_stride doubles with one barrier: thread 0 expects the total and issues one bulk
+// copy per record whose src[j] is not null. Waits and error handling as stage_to_shared.
+__device__ inline bool stage_records(double* dst, int dst_stride, const double* const* src,
+                                     int count, uint32_t bytes, uint64_t* bar) {
+    bool bad = (smem_addr(dst) & 15u) != 0 || (bytes & 15u) != 0 ||
+               ((dst_stride * 8) & 15) != 0 || (smem_addr(bar) & 7u) != 0;
+    uint32_t total = 0;
+    for (int j = 0; j < count; ++j)
+        if (src[j] != nullptr) {
+            bad |= (reinterpret_cast<uintptr_t>(src[j]) & 15u) != 0;
+            total += bytes;
+        }
+    if (bad) {
+        if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_ARGUMENT);
+        return false;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, total);
+        for (int j = 0; j < count; ++j)
+            if (src[j] != nullptr) bulk_copy_g2s(dst + j * dst_stride, src[j], bytes, bar);
+    }
+    bool ok = mbar_wait(bar, 0, g_wait_polls);
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_device_error, MKB_ERR_TIMEOUT);
+        mbar_wait(bar, 0, MKB_WAIT_POLLS_DEFAULT);
         __syncthreads();
     }
     return ok;

@@ -46,6 +46,8 @@ size_t merit_workspace_bytes(int V, int n_tuples);
 int pack_rays_default();
 // largest pack a caller may ask for (mkb_trace_options.pack_rays is clamped to it)
 constexpr int kMaxPackRaysOption = 4096;
+// most variants one trace CTA may take (mkb_trace_options.variants_per_cta)
+constexpr int kMaxVariantsPerCta = 8;
 
 // adjoint.cu
 int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* templates,

@@ -39,6 +39,8 @@ struct alignas(16) SharedTrace {
     uint64_t bar;
     SharedTables tab;
     int tuple_start[kMaxPackTuples + 1];
+    int vs[kMaxVariantsPerCta];  // the CTA's variants (-1: not traced in this launch)
+    int any;
 };
 static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 
@@ -155,21 +157,37 @@ __device__ inline double key_value(unsigned long long k) {
 // order (opd_statistics, merit/opd.hpp:37; variant_merit, src/batch/batch_merit.cpp:12), so
 // RESIDUALS and MERIT equal the reference CPU results bit for bit. Otherwise contracted FP64
 // with lane-strided sums and a fixed shuffle tree (deterministic, not bit-identical to CPU).
-template <bool kResiduals, int kPrecision, int kFeat, bool kExtrema = false>
+// kMulti: the CTA takes p.vpc variants side by side (built for coaxial batches without ghost
+// plates); otherwise one variant, with the leaner indexing of that case.
+template <bool kResiduals, int kPrecision, int kFeat, bool kExtrema = false, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
     constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
     using N = typename std::conditional<kExact, Exact64, double>::type;
     __shared__ SharedTrace sh;
-    const int slot = blockIdx.x / p.n_packs;
-    const int v = p.order != nullptr ? p.order[slot] : slot;
-    if (!run_active(out.mask, v)) return;
-    const int pk = blockIdx.x - slot * p.n_packs;
-    const int S = surfaces_of(p, v);
+    // this CTA: pack pk of the variants in queue slots group * vpc .. + nv - 1
+    const int vpc = kMulti ? p.vpc : 1;
+    const int group = blockIdx.x / p.n_packs;
+    const int pk = blockIdx.x - group * p.n_packs;
+    const int slot0 = group * vpc;
+    const int nv = kMulti ? (p.V - slot0 < vpc ? p.V - slot0 : vpc) : 1;
+    int* vs = sh.vs;
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int j = 0; j < nv; ++j) {
+            const int slot = slot0 + j;
+            int v = p.order != nullptr ? p.order[slot] : slot;
+            if (!run_active(out.mask, v)) v = -1;
+            vs[j] = v;
+            any |= v >= 0;
+        }
+        sh.any = any;
+    }
+    __syncthreads();
+    if (!sh.any) return;
     const Pack pack = p.packs[pk];
     const RecordLayout lay = layout_of(p);
-    const double* src = records + static_cast<int64_t>(v) * p.stride;
     if (threadIdx.x <= pack.tuples) {
         int start = 0;
         for (int t = 0; t < static_cast<int>(threadIdx.x); ++t) {
@@ -179,24 +197,40 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         sh.tuple_start[threadIdx.x] = start;
     }
     copy_tables(p, sh.tab);
+    // dynamic shared memory: per variant of the CTA its record and mu table (rec_sh doubles),
+    // then the per-ray arrays of all its packs (nv * pack.rays entries each)
     extern __shared__ __align__(16) double dyn[];
-    double* record = dyn;                 // [stride]
-    double* mu_tab = dyn + p.stride;      // [S][L]
-    double* opl_sh = mu_tab + p.S * p.L;  // [pack_max]
-    double* pen_sh = opl_sh + p.pack_max; // [pack_max]
-    double* w_sh = pen_sh + p.pack_max;   // FP64 only: [pack_max] piston weights
-    double* ws_sh = w_sh + (kExact ? p.pack_max : 0);  // FP64 only: [pack_max] w * opl
-    uint8_t* status_sh = reinterpret_cast<uint8_t*>(kExact ? ws_sh + p.pack_max : w_sh);
-    if (!stage_to_shared(record, src, static_cast<uint32_t>(p.stride * sizeof(double)),
-                         &sh.bar))
-        return;
+    const int rec_sh = p.stride + ((p.S * p.L + 1) & ~1);
+    const int span = vpc * p.pack_max;
+    double* opl_sh = dyn + vpc * rec_sh;     // [span]
+    double* pen_sh = opl_sh + span;          // [span]
+    double* w_sh = pen_sh + span;            // FP64 only: [span] piston weights
+    double* ws_sh = w_sh + (kExact ? span : 0);  // FP64 only: [span] w * opl
+    uint8_t* status_sh = reinterpret_cast<uint8_t*>(kExact ? ws_sh + span : w_sh);
+    if constexpr (kMulti) {
+        const double* src[kMaxVariantsPerCta];
+        for (int j = 0; j < nv; ++j)
+            src[j] = vs[j] >= 0 ? records + static_cast<int64_t>(vs[j]) * p.stride : nullptr;
+        if (!stage_records(dyn, rec_sh, src, nv,
+                           static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar))
+            return;
+    } else {
+        if (!stage_to_shared(dyn, records + static_cast<int64_t>(vs[0]) * p.stride,
+                             static_cast<uint32_t>(p.stride * sizeof(double)), &sh.bar))
+            return;
+    }
+    const int S0 = surfaces_of(p, vs[0] >= 0 ? vs[0] : 0);
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     // mu of every step and wavelength, divided once per CTA as the step would divide it
-    for (int i = threadIdx.x; i < S * p.L; i += kThreads) {
-        const int s = i / p.L, l = i - s * p.L;
-        mu_tab[i] = s >= 1 ? value_of(N(record[lay.index + (s - 1) * p.L + l]) /
-                                      N(record[lay.index + s * p.L + l]))
-                           : 0.0;
+    for (int i = threadIdx.x; i < nv * p.S * p.L; i += kThreads) {
+        const int j = i / (p.S * p.L), sl = i - j * p.S * p.L;
+        const int s = sl / p.L, l = sl - s * p.L;
+        if (vs[j] < 0) continue;
+        const double* record = dyn + j * rec_sh;
+        dyn[j * rec_sh + p.stride + sl] = s >= 1 && s < (kMulti ? surfaces_of(p, vs[j]) : S0)
+                                    ? value_of(N(record[lay.index + (s - 1) * p.L + l]) /
+                                               N(record[lay.index + s * p.L + l]))
+                                    : 0.0;
     }
     __syncthreads();
 
@@ -205,15 +239,18 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     if constexpr (kExtrema) {
         __shared__ unsigned long long ext_keys[2 * kMaxSurfaces];
         ext_sh = ext_keys;
-        for (int i = threadIdx.x; i < S; i += kThreads) {
+        for (int i = threadIdx.x; i < p.S; i += kThreads) {
             ext_keys[2 * i] = order_key(0.0);      // height^2 0 (neutral_height_sq)
             ext_keys[2 * i + 1] = order_key(1.0);  // cos I = 1 (neutral_cos_incidence)
         }
         __syncthreads();
     }
 
-    // ---- phase 1: trace ---------------------------------------------------------------
-    for (int i = threadIdx.x; i < pack.rays; i += kThreads) {
+    // ---- phase 1: trace (ray ii = variant j's pack ray i) -------------------------------
+    auto trace_one = [&](int j, int i, int ii) {
+        const int S = kMulti ? surfaces_of(p, vs[j]) : S0;
+        const double* record = dyn + j * rec_sh;
+        const double* mu_tab = record + p.stride;
         int t = 0;
         while (t + 1 < pack.tuples && i >= sh.tuple_start[t + 1]) ++t;
         const int tu = pack.first_tuple + t;
@@ -235,32 +272,54 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
         } else {
             st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl, pen);
         }
-        opl_sh[i] = opl;
-        pen_sh[i] = pen;
-        status_sh[i] = static_cast<uint8_t>(st);
+        opl_sh[ii] = opl;
+        pen_sh[ii] = pen;
+        status_sh[ii] = static_cast<uint8_t>(st);
+    };
+    if constexpr (kMulti) {
+        // (j, i) advanced without a division per ray
+        int j = static_cast<int>(threadIdx.x) / pack.rays;
+        int i = static_cast<int>(threadIdx.x) - j * pack.rays;
+        for (int ii = threadIdx.x; ii < nv * pack.rays; ii += kThreads) {
+            const int jj = j, ir = i;
+            i += kThreads;
+            while (i >= pack.rays) {
+                i -= pack.rays;
+                ++j;
+            }
+            if (vs[jj] >= 0) trace_one(jj, ir, ii);
+        }
+    } else {
+        for (int i = threadIdx.x; i < pack.rays; i += kThreads) trace_one(0, i, i);
     }
     __syncthreads();
 
     if constexpr (kExtrema) {
-        unsigned long long* g = out.extrema + static_cast<int64_t>(v) * p.S * 2;
+        const int S = surfaces_of(p, vs[0]);
+        unsigned long long* g = out.extrema + static_cast<int64_t>(vs[0]) * p.S * 2;
         for (int q = threadIdx.x; q < S; q += kThreads) {
             atomicMax(&g[2 * q], ext_sh[2 * q]);
             atomicMin(&g[2 * q + 1], ext_sh[2 * q + 1]);
         }
     }
 
-    // ---- phase 2: one warp per tuple ----------------------------------------------------
+    // ---- phase 2: one warp per (variant, tuple) ------------------------------------------
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    for (int t = warp; t < pack.tuples; t += kThreads / 32) {
+    const int v0 = vs[0];
+    for (int tt = warp; tt < nv * pack.tuples; tt += kThreads / 32) {
+        const int j = kMulti ? tt / pack.tuples : 0;
+        const int t = tt - j * pack.tuples;
+        const int v = kMulti ? vs[j] : v0;
+        if (kMulti && v < 0) continue;
         const int tu = pack.first_tuple + t;
         const int f = tu / p.L;
         const int l = tu - f * p.L;
         const int n = p.sample_count[f];
-        const int base = sh.tuple_start[t];
+        const int base = j * pack.rays + sh.tuple_start[t];
         const int64_t row0 = p.field_offset[f] + static_cast<int64_t>(l) * n;  // in the variant
         // piston: valid weight and weighted OPL sum over the rays in the piston
-        double vw = 0.0, vs = 0.0;
+        double vw = 0.0, vs_ = 0.0;
         if (kExact) {
             // Every lane forms its samples' terms w_k and w_k * OPL_k (one rounded product, as
             // the sequential loop forms it; +0 for rays outside the piston, which leaves the
@@ -280,23 +339,23 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                     s_acc += N(ws_sh[base + k]);
                 }
                 vw = value_of(w_acc);
-                vs = value_of(s_acc);
+                vs_ = value_of(s_acc);
             }
             vw = __shfl_sync(0xffffffffu, vw, 0);
-            vs = __shfl_sync(0xffffffffu, vs, 0);
+            vs_ = __shfl_sync(0xffffffffu, vs_, 0);
         } else {
             for (int k = lane; k < n; k += 32) {
                 if (in_piston(status_sh[base + k])) {
                     const Sample smp = pupil_sample(p, sh.tab, f, k);
                     vw += smp.weight;
-                    vs += smp.weight * opl_sh[base + k];
+                    vs_ += smp.weight * opl_sh[base + k];
                 }
             }
             vw = warp_sum(vw);
-            vs = warp_sum(vs);
+            vs_ = warp_sum(vs_);
         }
         const bool valid = vw > 0.0;
-        const N piston = valid ? value_of(N(vs) / N(vw)) : 0.0;
+        const N piston = valid ? value_of(N(vs_) / N(vw)) : 0.0;
         const N scale = p.scale[tu];
         const N pscale = p.pscale[tu];
         double sq = 0.0, psq = 0.0;
@@ -407,22 +466,31 @@ __global__ void merit_finalize_kernel(int V, int n_tuples, const double* part,
 // dynamic shared memory of trace_kernel: the record (stride is even), the mu table and the
 // pack's per-ray OPL, penalty and status
 size_t trace_smem(const TraceParams& p, bool exact) {
-    return (static_cast<size_t>(p.stride) + static_cast<size_t>(p.S) * p.L +
-            (exact ? 4 : 2) * static_cast<size_t>(p.pack_max)) * sizeof(double) +
-           ((static_cast<size_t>(p.pack_max) + 15) & ~size_t(15));
+    const size_t rec_sh =
+        static_cast<size_t>(p.stride) + ((static_cast<size_t>(p.S) * p.L + 1) & ~size_t(1));
+    const size_t span = static_cast<size_t>(p.vpc) * p.pack_max;
+    return (p.vpc * rec_sh + (exact ? 4 : 2) * span) * sizeof(double) + ((span + 15) & ~size_t(15));
 }
 
 // Launches trace_kernel<kResiduals, precision> (MIXED traces in FP64 with contraction; its FP32
 // part is the reverse sweep) with the dynamic shared memory the batch needs.
 template <bool kResiduals>
-int launch_trace(const TraceParams& p, const double* records, const TupleOut& out, int precision,
-                 cudaStream_t stream) {
-    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_packs);
+int launch_trace(const TraceParams& p_in, const double* records, const TupleOut& out,
+                 int precision, cudaStream_t stream) {
+    TraceParams p = p_in;
+    // several variants per CTA: built for coaxial batches without ghost plates; the others
+    // trace one variant per CTA (the option only shapes the launch)
+    if (p.non_coaxial || p.G > 0) p.vpc = 1;
+    const int64_t groups = (static_cast<int64_t>(p.V) + p.vpc - 1) / p.vpc;
+    const unsigned blocks = static_cast<unsigned>(groups * p.n_packs);
     const size_t smem = trace_smem(p, precision == MKB_PRECISION_FP64);
     // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
     const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
     constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
-    auto kernel = precision == MKB_PRECISION_FP64
+    auto kernel = p.vpc > 1 ? (precision == MKB_PRECISION_FP64
+                                   ? trace_kernel<kResiduals, E, 0, false, true>
+                                   : trace_kernel<kResiduals, F, 0, false, true>)
+                  : precision == MKB_PRECISION_FP64
                       ? (feat == 0   ? trace_kernel<kResiduals, E, 0>
                          : feat == 1 ? trace_kernel<kResiduals, E, 1>
                          : feat == 2 ? trace_kernel<kResiduals, E, 2>
@@ -433,7 +501,12 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
                                      : trace_kernel<kResiduals, F, 3>);
     const int64_t n_ext = static_cast<int64_t>(p.V) * p.S * 2;
     if (out.extrema != nullptr) {
-        // per-surface extrema: coaxial batches (with or without ghost plates)
+        // per-surface extrema: coaxial batches (with or without ghost plates), one variant per
+        // CTA
+        if (p.vpc != 1) {
+            set_error("trace: extrema need one variant per CTA");
+            return MKB_ERR_UNSUPPORTED;
+        }
         if (feat & 1) {
             set_error("trace: per-surface extrema of decentered or tilted batches are not built");
             return MKB_ERR_UNSUPPORTED;
@@ -445,6 +518,20 @@ int launch_trace(const TraceParams& p, const double* records, const TupleOut& ou
                                   : trace_kernel<kResiduals, F, 2, true>);
         extrema_init_kernel<<<592, 256, 0, stream>>>(out.extrema, n_ext, out.mask, p.S);
         count_launch();
+    }
+    if (p.vpc > 1) {  // the caller's choice must fit: larger ones are refused, not clamped
+        int dev = 0, optin = 0;
+        int rc = cuda_status(cudaGetDevice(&dev), "trace: cudaGetDevice");
+        if (rc == MKB_OK)
+            rc = cuda_status(cudaDeviceGetAttribute(&optin,
+                                                    cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                             "trace: shared memory limit");
+        if (rc != MKB_OK) return rc;
+        if (smem + sizeof(SharedTrace) > static_cast<size_t>(optin)) {
+            set_error("trace: %d variants per CTA need %zu bytes of shared memory, the device "
+                      "has %d per block", p.vpc, smem, optin);
+            return MKB_ERR_ARGUMENT;
+        }
     }
     if (smem > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(

@@ -135,17 +135,18 @@ class MeritOutput:
 
 
 def _trace_options(pack_rays: int = 0, extra_merit: torch.Tensor | None = None,
-                   extrema: torch.Tensor | None = None):
+                   extrema: torch.Tensor | None = None, variants_per_cta: int = 0):
     o = _capi.TraceOptions()
     o.pack_rays = int(pack_rays)
-    o.reserved = 0
+    o.variants_per_cta = int(variants_per_cta)
     o.extra_merit = C.c_void_p(extra_merit.data_ptr()) if extra_merit is not None else None
     o.extrema = C.c_void_p(extrema.data_ptr()) if extrema is not None else None
     return o
 
 
 def residuals_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: SystemBatchHost,
-                     stream=None, pack_rays: int = 0) -> ResidualOutput:
+                     stream=None, pack_rays: int = 0,
+                     variants_per_cta: int = 0) -> ResidualOutput:
     """RESIDUALS on an uploaded batch; outputs stay on the device."""
     lib = _capi.lib()
     V = dbatch.variants
@@ -154,7 +155,7 @@ def residuals_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: Sy
     st = torch.empty((V, layout.rays_per_variant), dtype=torch.uint8, device=dbatch.device)
     b = dbatch.c_struct()
     plan = layout.plan(host)
-    opts = _trace_options(pack_rays)
+    opts = _trace_options(pack_rays, variants_per_cta=variants_per_cta)
     rc = lib.mkb_residuals_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
                                      C.c_void_p(res.data_ptr()), layout.trace_rows,
                                      C.c_void_p(opd.data_ptr()), C.c_void_p(st.data_ptr()),
@@ -165,7 +166,8 @@ def residuals_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: Sy
 
 def merit_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: SystemBatchHost,
                  stream=None, workspace: torch.Tensor | None = None, pack_rays: int = 0,
-                 extra_merit: torch.Tensor | None = None) -> MeritOutput:
+                 extra_merit: torch.Tensor | None = None,
+                 variants_per_cta: int = 0) -> MeritOutput:
     """MERIT on an uploaded batch; outputs stay on the device. extra_merit: device [V] added to
     each variant's merit after its tuple sums."""
     lib = _capi.lib()
@@ -182,7 +184,7 @@ def merit_device(dbatch: DeviceSystemBatch, layout: ResidualLayout, host: System
         extra_merit = extra_merit.to(device=dbatch.device, dtype=torch.float64).contiguous()
         if extra_merit.numel() != V:
             raise ValueError(f"extra_merit must hold {V} values")
-    opts = _trace_options(pack_rays, extra_merit)
+    opts = _trace_options(pack_rays, extra_merit, variants_per_cta=variants_per_cta)
     rc = lib.mkb_merit_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
                                  C.c_void_p(merit.data_ptr()), C.c_void_p(failed.data_ptr()),
                                  C.c_void_p(hard.data_ptr()), C.c_void_p(workspace.data_ptr()),
