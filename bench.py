@@ -675,6 +675,19 @@ def run_uneven(args, world, rank, local):
     fma_value = world * iters_fma / (max_over_ranks(ms_fma, world, dev) * args.steps / 1e3)
     del lm_f
 
+    # ---- the same LM with paraxial constraints on the device (image at the paraxial focus,
+    # working distance >= 1 mm, |Petzval curvature| <= 0.02 / mm; analytic adjoint rows): the
+    # constrained cycle stays one graph-captured launch sequence
+    cons = engine.ParaxialConstraints.of([(3, 0, 1.0, 0.0), (2, 1, 1.0, 1.0), (4, 2, 100.0, 0.02)],
+                                         derivative="adjoint")
+    opt_c = dataclasses.replace(opt, paraxial=cons)
+    lm_c = engine.DeviceLm(db, lay_mixed, b, vss, opt_c, runs)
+    lm_c.start(x0)
+    ms_con, iters_con, per_cycle_con = _lm_window(lm_c, args.steps, args.warmup, flush, world,
+                                                  dev)
+    con_value = world * iters_con / (max_over_ranks(ms_con, world, dev) * args.steps / 1e3)
+    del lm_c
+
     # ---- the reference method on the same GPU: FD Jacobian (2P + 1 traced variants), FP64
     fd_runs = min(1024, runs)
     fd_b = b.subset(0, fd_runs)
@@ -766,6 +779,12 @@ def run_uneven(args, world, rank, local):
         "ray_surface_hits_per_s": world * hits / (merit_ms / 1e3),
         "adjoint_fp64_fma": {"value": fma_value, "unit": "LM iterations/s",
                              "ms_per_cycle": ms_fma},
+        "adjoint_mixed_paraxial_constraints": {
+            "value": con_value, "unit": "LM iterations/s", "ms_per_cycle": ms_con,
+            "launches_per_cycle": int(per_cycle_con),
+            "constraints": "paraxial focus (equal), working distance >= 1 mm, |Petzval| <= "
+                           "0.02/mm; rows and analytic adjoint Jacobian on the device, "
+                           "graph-captured cycle"},
         "fd_fp64": {"value": world * fd_value, "unit": "LM iterations/s",
                     "ms_per_cycle_1024_runs": fd_ms, "cycles": fd_steps,
                     "speedup_adjoint_mixed_vs_fd": value / (world * fd_value),

@@ -353,7 +353,59 @@ typedef struct mkb_lm_options {
                                          points to an array of `runs` sets (uneven batches;
                                          counts may differ), x0 / x rows are then strided by
                                          the largest count; needs gram_exact = 0 */
+    /* Paraxial constraints evaluated on the device (ParaxialConstraints as the LM's extra
+     * rows, include/mikroptim/optim/paraxial_residuals.hpp:67): `paraxial_count` rows after
+     * the trace rows of every run, their Jacobian in every cycle and sum r_e^2 in every merit,
+     * with no host phase (a cycle stays one fixed launch sequence). 0 / NULL: none. See
+     * mkb_paraxial_constraint and mkb_paraxial_rows_device. */
+    int32_t paraxial_count;
+    const struct mkb_paraxial_constraint* paraxial;  /* host [paraxial_count] */
+    int32_t paraxial_column;          /* wavelength column holding the paraxial index */
+    int32_t paraxial_derivative;      /* MKB_PARAXIAL_FD or MKB_PARAXIAL_ADJOINT */
 } mkb_lm_options;
+
+/* ---- paraxial constraints on the device -----------------------------------------------------
+ * One constraint (ParaxialConstraint, include/mikroptim/optim/paraxial_residuals.hpp:67), its
+ * residual r = sqrt(weight) * mode(q + shift) from the y-nu trace at the paraxial index
+ * (ynu_trace.hpp; compute_paraxial, src/paraxial/paraxial.cpp:98):
+ *   FOCAL_LENGTH      q = f_s (1 - f_s phi), phi = -C (equal only)
+ *   PARFOCAL_LENGTH   q = offset + sum_{s >= reference_surface} t_s - L_s
+ *   WORKING_DISTANCE  q = t_{S-1} - w_s
+ *   PARAXIAL_FOCUS    q = a (A + t_{S-1} C / n'_L) (equal only, target 0)
+ *   PETZVAL           q = |kappa_P| - kappa_max, kappa_P = -n'_L P (max only)
+ * mode: MKB_MODE_EQUAL q, MIN min(q, 0), MAX max(q, 0); shift moves one-sided limits (0 for
+ * equal). The paraxial index of a medium is its index in wavelength column `paraxial_column`
+ * of the record (the batch's paraxial_index), or, for a medium with glass variables, the
+ * Buchdahl index at the reference wavelength (VariableSet::apply, src/optim/
+ * variable_set.cpp:282). Coaxial batches without ghost plates. Sine-condition and distortion
+ * rows trace real rays and stay host rows. */
+enum { MKB_CONSTRAINT_FOCAL_LENGTH = 0, MKB_CONSTRAINT_PARFOCAL_LENGTH = 1,
+       MKB_CONSTRAINT_WORKING_DISTANCE = 2, MKB_CONSTRAINT_PARAXIAL_FOCUS = 3,
+       MKB_CONSTRAINT_PETZVAL = 4 };          /* ConstraintType, model/constraints.hpp:28 */
+enum { MKB_MODE_EQUAL = 0, MKB_MODE_MIN = 1, MKB_MODE_MAX = 2 };  /* ConstraintMode */
+/* Jacobian of the constraint rows: central differences with the FD Jacobian's pattern (the
+ * reference's extra_rows_cpu, bit for bit), or the analytic adjoint of the y-nu trace (one
+ * reverse sweep of the marginal ray per run; exact derivatives). */
+enum { MKB_PARAXIAL_FD = 0, MKB_PARAXIAL_ADJOINT = 1 };
+#define MKB_MAX_PARAXIAL 16
+typedef struct mkb_paraxial_constraint {
+    int32_t type, mode;
+    double weight, target;
+    int32_t reference_surface;        /* PARFOCAL_LENGTH only: table surface */
+    int32_t reserved;                 /* 0 */
+    double offset;                    /* PARFOCAL_LENGTH only (mm) */
+    double shift;                     /* >= 0; 0 for equal */
+} mkb_paraxial_constraint;
+
+/* The constraint rows of `runs` runs at x [runs][P] on their templates (1 variant for all runs
+ * or one per run): residuals re [runs][E] and Jacobian je [runs][P][E] (column k of run i at
+ * (i * P + k) * E). `options` supplies the constraints, the column and the derivative (its
+ * other fields must be valid LM options); one variable set for all runs (per_run_variables =
+ * 0). Allocates nothing. */
+int mkb_paraxial_rows_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             const double* x, int32_t runs, double* je, double* re,
+                             void* stream);
 
 size_t mkb_lm_workspace_bytes(const mkb_device_batch* templates, const mkb_residual_plan* plan,
                               const mkb_variables* vars, const mkb_lm_options* options,

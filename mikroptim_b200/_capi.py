@@ -101,6 +101,14 @@ class Variables(C.Structure):
     ]
 
 
+class ParaxialConstraint(C.Structure):
+    """mkb_paraxial_constraint (ParaxialConstraint, optim/paraxial_residuals.hpp:67)."""
+
+    _fields_ = [("type", C.c_int32), ("mode", C.c_int32), ("weight", C.c_double),
+                ("target", C.c_double), ("reference_surface", C.c_int32),
+                ("reserved", C.c_int32), ("offset", C.c_double), ("shift", C.c_double)]
+
+
 class LmOptions(C.Structure):
     """mkb_lm_options (LmOptions, levenberg_marquardt.hpp:85)."""
 
@@ -111,7 +119,13 @@ class LmOptions(C.Structure):
         ("diag_floor", C.c_double),
         ("jacobian", C.c_int32), ("gram_exact", C.c_int32),
         ("per_run_variables", C.c_int32),
+        ("paraxial_count", C.c_int32), ("paraxial", C.POINTER(ParaxialConstraint)),
+        ("paraxial_column", C.c_int32), ("paraxial_derivative", C.c_int32),
     ]
+
+
+MKB_PARAXIAL_FD = 0
+MKB_PARAXIAL_ADJOINT = 1
 
 
 class TraceOptions(C.Structure):
@@ -187,6 +201,11 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     lib.mkb_device_status.restype = c.c_int
+    lib.mkb_paraxial_rows_device.restype = c.c_int
+    lib.mkb_paraxial_rows_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
+                                             C.POINTER(Variables), C.POINTER(LmOptions),
+                                             c.c_void_p, c.c_int32, c.c_void_p, c.c_void_p,
+                                             c.c_void_p]
     PF = C.POINTER(PrefilterOptions)
     lib.mkb_prefilter_workspace_bytes.restype = c.c_size_t
     lib.mkb_prefilter_workspace_bytes.argtypes = [c.c_int32, C.POINTER(ResidualPlan)]

@@ -14,6 +14,7 @@
 // the reference's host loop bit for bit. One cycle is a fixed sequence of launches with
 // per-run masks (no host decisions), so a cycle can be captured in a CUDA graph.
 #include "launch.cuh"
+#include "paraxial.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -509,6 +510,9 @@ struct LmLayout {
     uint8_t* vsurf;     // surface count of each run's record (uneven surfaces), else null
     int* order;         // processing order (uneven batches), else null
     int* split;         // [1] runs of the first group of `order`
+    double* px_je;      // device paraxial rows: Jacobian [runs][pmax][E], rows [runs][E],
+    double* px_re;      // and sum r_e^2 at the points of the merit [runs]
+    double* px_merit;
 };
 
 constexpr int kFdChunkRuns = 64;
@@ -523,6 +527,7 @@ struct LmSetup {
     int pmax;           // P, or the largest P of the runs
     int precision;
     int64_t R;
+    ParaxialSpec px;    // paraxial constraints evaluated on the device (px.E = 0: none)
 };
 
 // Carves the workspace (base may be null to only size it).
@@ -594,6 +599,10 @@ LmLayout lm_layout(char* base, const LmSetup& s, int runs, const mkb_device_batc
                                                         runs < kFdChunkRuns ? runs : kFdChunkRuns);
         L.fd_ws = take(L.fd_ws_bytes);
     }
+    const size_t E = static_cast<size_t>(s.px.E);
+    L.px_je = reinterpret_cast<double*>(take(8 * r * P * E));
+    L.px_re = reinterpret_cast<double*>(take(8 * r * E));
+    L.px_merit = E > 0 ? reinterpret_cast<double*>(take(8 * r)) : nullptr;
     L.total = off;
     return L;
 }
@@ -673,7 +682,7 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
         return MKB_ERR_UNSUPPORTED;
     }
     s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
-    return MKB_OK;
+    return make_paraxial_spec(options, templates, plan, &s.px);
 }
 
 // The LM's own records are one per run: their surface counts and processing order are the
@@ -810,12 +819,28 @@ int phase_jacobian(const LmCall& c, const mkb_device_batch* templates,
     if (rc != MKB_OK) return rc;
     if (!s.fused) rc = launch_gram(L.J, L.r0, runs, s.vp.P, s.R, L.gram, s.gram_exact, stream,
                                    want, rv);
-    return rc;
+    if (rc != MKB_OK || s.px.E == 0) return rc;
+    // paraxial constraint rows at x, appended after the trace rows of every entry's chain
+    rc = launch_paraxial_rows(s.px, s.vp, L.vt, s.pmax, templates, L.st.x, runs, want, L.px_je,
+                              L.px_re, stream);
+    if (rc != MKB_OK) return rc;
+    return launch_gram_extend(s.vp, L.st, L.gram, L.px_je, L.px_re, s.px.E, runs, stream);
 }
 
 // 3. trial MERIT (+ the caller's extra merit; extrema of the trial points when asked)
 int phase_trial(const LmCall& c, const mkb_device_batch* templates, int32_t runs,
                 const double* extra_merit, double* extrema, cudaStream_t stream) {
+    if (c.s.px.E > 0) {  // the paraxial rows' sum of squares at the trial points
+        if (extra_merit != nullptr) {
+            set_error("lm: device paraxial constraints and host extra rows cannot be combined");
+            return MKB_ERR_UNSUPPORTED;
+        }
+        const int rc = launch_paraxial_merit(c.s.px, c.s.vp, c.L.vt, c.s.pmax, templates,
+                                             c.L.st.trial, runs, c.L.st.evaluate,
+                                             c.L.px_merit, stream);
+        if (rc != MKB_OK) return rc;
+        extra_merit = c.L.px_merit;
+    }
     return lm_merit_at(c.s, c.L, templates, c.L.st.trial, runs, c.L.trial_merit,
                        c.L.trial_failed, c.L.trial_hard, stream, c.L.st.evaluate, extra_merit,
                        extrema);
@@ -885,6 +910,16 @@ int mkb_lm_start_ex_device(const mkb_device_batch* templates, const mkb_residual
         rc = cuda_status(cudaGetLastError(), "lm order launch");
         if (rc != MKB_OK) return rc;
     }
+    if (s.px.E > 0) {
+        if (extra_merit != nullptr) {
+            set_error("lm: device paraxial constraints and host extra rows cannot be combined");
+            return MKB_ERR_UNSUPPORTED;
+        }
+        rc = launch_paraxial_merit(s.px, s.vp, L.vt, s.pmax, templates, x0, runs, nullptr,
+                                   L.px_merit, stream);
+        if (rc != MKB_OK) return rc;
+        extra_merit = L.px_merit;
+    }
     rc = lm_merit_at(s, L, templates, x0, runs, L.st.merit, L.st.failed, L.st.hard, stream,
                      nullptr, extra_merit);
     if (rc != MKB_OK) return rc;
@@ -913,6 +948,26 @@ int mkb_lm_cycle_device(const mkb_device_batch* templates, const mkb_residual_pl
     rc = launch_lm_update(c.s.vp, c.s.o, c.L.st, c.L.gram, runs, stream);  // 2. step
     if (rc != MKB_OK) return rc;
     return phase_accept(c, templates, runs, nullptr, stream);
+}
+
+int mkb_paraxial_rows_device(const mkb_device_batch* templates, const mkb_residual_plan* plan,
+                             const mkb_variables* vars, const mkb_lm_options* options,
+                             const double* x, int32_t runs, double* je, double* re,
+                             void* stream_ptr) {
+    LmSetup s;
+    int rc = lm_setup(templates, plan, vars, options, runs, s);
+    if (rc != MKB_OK) return rc;
+    if (s.per_run) {
+        set_error("paraxial rows: one variable set for all runs (the LM takes per-run sets)");
+        return MKB_ERR_UNSUPPORTED;
+    }
+    if (s.px.E == 0) return MKB_OK;
+    if (x == nullptr || je == nullptr || re == nullptr) {
+        set_error("paraxial rows: null x, je or re");
+        return MKB_ERR_ARGUMENT;
+    }
+    return launch_paraxial_rows(s.px, s.vp, nullptr, s.pmax, templates, x, runs, nullptr, je, re,
+                                static_cast<cudaStream_t>(stream_ptr));
 }
 
 int mkb_lm_cycle_jacobian_device(const mkb_device_batch* templates,

@@ -994,6 +994,75 @@ def extra_rows_host(host: SystemBatchHost, variables, x0, extra: ExtraResiduals)
     return J, R
 
 
+CONSTRAINT_FOCAL_LENGTH, CONSTRAINT_PARFOCAL_LENGTH, CONSTRAINT_WORKING_DISTANCE = 0, 1, 2
+CONSTRAINT_PARAXIAL_FOCUS, CONSTRAINT_PETZVAL = 3, 4
+MODE_EQUAL, MODE_MIN, MODE_MAX = 0, 1, 2
+
+
+@dataclass
+class ParaxialConstraint:
+    """ParaxialConstraint (include/mikroptim/optim/paraxial_residuals.hpp:67): type and mode
+    as ConstraintType / ConstraintMode, r = sqrt(weight) * mode(q + shift)."""
+
+    type: int
+    mode: int = MODE_EQUAL
+    weight: float = 1.0
+    target: float = 0.0
+    reference_surface: int = 0
+    offset: float = 0.0
+    shift: float = 0.0
+
+
+@dataclass
+class ParaxialConstraints:
+    """Paraxial constraints evaluated on the device as the LM's extra rows (no host phase):
+    `column` is the wavelength column holding the paraxial index (the batch's paraxial_index),
+    `derivative` "fd" (central differences with the FD pattern, the reference's extra rows bit
+    for bit) or "adjoint" (analytic reverse sweep of the y-nu trace)."""
+
+    items: list = dataclasses.field(default_factory=list)
+    column: int = 0
+    derivative: str = "fd"
+
+    @staticmethod
+    def of(tuples, column: int = 0, derivative: str = "fd") -> "ParaxialConstraints":
+        """From (type, mode, weight, target) tuples."""
+        return ParaxialConstraints([ParaxialConstraint(int(t[0]), int(t[1]), float(t[2]),
+                                                       float(t[3])) for t in tuples],
+                                   column, derivative)
+
+    def c_array(self):
+        arr = (_capi.ParaxialConstraint * len(self.items))()
+        for i, c in enumerate(self.items):
+            arr[i] = _capi.ParaxialConstraint(c.type, c.mode, c.weight, c.target,
+                                               c.reference_surface, 0, c.offset, c.shift)
+        return arr
+
+
+def paraxial_rows_device(templates: DeviceSystemBatch, layout: ResidualLayout,
+                         host: SystemBatchHost, variables, x0,
+                         constraints: ParaxialConstraints, stream=None):
+    """The paraxial constraint rows of every run at x0 on the device: (Jacobian [runs][P][E],
+    residuals [runs][E]), by central differences with the FD pattern or by the analytic adjoint
+    (constraints.derivative)."""
+    lib = _capi.lib()
+    dev = templates.device
+    x = _x_rows(x0, variables.size, dev)
+    runs, P = x.shape
+    E = len(constraints.items)
+    je = torch.zeros((runs, P, E), dtype=torch.float64, device=dev)
+    re = torch.zeros((runs, E), dtype=torch.float64, device=dev)
+    opt = LmOptions(paraxial=constraints).c_struct()
+    b = templates.c_struct()
+    plan = layout.plan(host)
+    vs = variables.c_struct()
+    rc = lib.mkb_paraxial_rows_device(C.byref(b), C.byref(plan), C.byref(vs), C.byref(opt),
+                                      C.c_void_p(x.data_ptr()), runs, C.c_void_p(je.data_ptr()),
+                                      C.c_void_p(re.data_ptr()), _stream_handle(stream))
+    _capi.check(rc, "paraxial rows")
+    return je, re
+
+
 @dataclass
 class LmOptions:
     """LmOptions (include/mikroptim/optim/levenberg_marquardt.hpp:85). fail_weight_factor and
@@ -1016,6 +1085,7 @@ class LmOptions:
     max_fail_weight: float = 1e14
     extra: ExtraResiduals | None = None
     trace_extra: TraceExtraResiduals | None = None
+    paraxial: "ParaxialConstraints | None" = None
 
     def c_struct(self) -> "_capi.LmOptions":
         o = _capi.LmOptions()
@@ -1027,6 +1097,15 @@ class LmOptions:
         o.jacobian = self.jacobian
         o.gram_exact = int(self.gram_exact)
         o.per_run_variables = 0
+        if self.paraxial is not None and self.paraxial.items:
+            arr = self.paraxial.c_array()
+            o._keep_paraxial = arr
+            o.paraxial_count = len(self.paraxial.items)
+            o.paraxial = C.cast(arr, C.POINTER(_capi.ParaxialConstraint))
+            o.paraxial_column = self.paraxial.column
+            o.paraxial_derivative = (_capi.MKB_PARAXIAL_ADJOINT
+                                     if self.paraxial.derivative == "adjoint"
+                                     else _capi.MKB_PARAXIAL_FD)
         return o
 
 
