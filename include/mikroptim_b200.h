@@ -598,6 +598,38 @@ int mkb_prefilter_decide_exact_host(const mkb_prefilter_options* options, int32_
                                     const int64_t* failed, const double* extra_merit,
                                     uint8_t* reject);
 
+/* ---- EVAL: evaluation on a dense Cartesian pupil grid -----------------------------------------
+ * Replaces the kernel EVAL behind TraceEngine::evaluate (src/cuda/eval.cu; CPU reference
+ * eval_cpu, src/eval/eval.cpp:307). Every variant, field and wavelength is traced on the grid
+ * of cell centres x_i = (2i + 1 - N)/N inside the unit pupil (every failure hard), to the
+ * image plane (the spot: image point relative to the ideal image point (0, h_f)) and to the
+ * reference sphere about (0, h_f, w): through the paraxial exit pupil (curvature kappa per
+ * variant and field, MKB_EVAL_EXIT_PUPIL), through the vertex of the last surface
+ * (MKB_EVAL_VERTEX), or of infinite radius (MKB_EVAL_INFINITE). OPD = (OPL - OPL_chief) -
+ * piston over the grid weights; four field rays per tuple (chief ray and its neighbours at
+ * +-delta for the focus positions): x, y, d_x, d_y, d_z. Failed rays: NaN values, their status.
+ * Every operation separately rounded and every sum in ascending grid order: bit-identical to
+ * eval_cpu. Outputs are device arrays in the reference's layout: ray (v, f, l, k) at
+ * ((v F + f) L + l) n + k, field ray j at ((v F + f) L + l) 4 + j (values x 5). */
+enum { MKB_EVAL_EXIT_PUPIL = 0, MKB_EVAL_VERTEX = 1, MKB_EVAL_INFINITE = 2 };
+#define MKB_MAX_EVAL_GRID 2048
+/* The grid (make_eval_grid): points [n][3] (x, y, weight) in row order; NULL to count only. */
+int mkb_eval_grid_host(int32_t size, int32_t half_pupil, double* points, int64_t* count);
+/* Reference geometry on the host (eval_reference_geometry): kappa [V][F] and the exit-pupil
+ * position [V] (NaN where not used) from the paraxial chief ray at wavelength column
+ * `paraxial_column` (the batch's paraxial index). MKB_ERR_ARGUMENT when the image point lies
+ * in the exit pupil. */
+int mkb_eval_reference_host(const mkb_batch_view* view, int32_t reference,
+                            int32_t paraxial_column, double* kappa, double* exit_pupil);
+size_t mkb_eval_workspace_bytes(const mkb_device_batch* batch);
+/* grid, kappa: device arrays from the two host calls above; half_pupil as for the grid;
+ * outputs device [V F L n] (opd, spot_x, spot_y, status) and [V F L 4] x 5 / [V F L 4]. */
+int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double field_ray_offset,
+                    const double* grid, int64_t n, const double* kappa, double* opd,
+                    double* spot_x, double* spot_y, uint8_t* status, double* field_rays,
+                    uint8_t* field_status, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);
 const char* mkb_version(void);

@@ -201,6 +201,17 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_merit_noalloc_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     lib.mkb_device_status.restype = c.c_int
+    lib.mkb_eval_grid_host.restype = c.c_int
+    lib.mkb_eval_grid_host.argtypes = [c.c_int32, c.c_int32, c.c_void_p, C.POINTER(c.c_int64)]
+    lib.mkb_eval_reference_host.restype = c.c_int
+    lib.mkb_eval_reference_host.argtypes = [C.POINTER(BatchView), c.c_int32, c.c_int32,
+                                            c.c_void_p, c.c_void_p]
+    lib.mkb_eval_workspace_bytes.restype = c.c_size_t
+    lib.mkb_eval_workspace_bytes.argtypes = [C.POINTER(DeviceBatch)]
+    lib.mkb_eval_device.restype = c.c_int
+    lib.mkb_eval_device.argtypes = [C.POINTER(DeviceBatch), c.c_int32, c.c_double, c.c_void_p,
+                                    c.c_int64, c.c_void_p] + [c.c_void_p] * 6 + \
+        [c.c_void_p, c.c_size_t, c.c_void_p]
     lib.mkb_paraxial_rows_device.restype = c.c_int
     lib.mkb_paraxial_rows_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              C.POINTER(Variables), C.POINTER(LmOptions),

@@ -573,6 +573,11 @@ class TraceEngine:
                                  settings.options.boundary)
         return prefilter_decide(stats, layout, batch, settings.options, settings.extra_merit)
 
+    def evaluate(self, batch: SystemBatchHost, settings: "EvalSettings | None" = None):
+        """Mode EVAL (TraceEngine::evaluate, include/mikroptim/cuda/trace_engine.hpp:193): OPD
+        maps, spots and field rays of every variant on the dense pupil grid."""
+        return evaluate_device(DeviceSystemBatch(batch, self.device), batch, settings)
+
     def run_on_device(self, batch: SystemBatchHost, settings, granularity: int,
                       consume) -> TraceRunInfo:
         """TraceEngine::run_on_device: RESIDUALS without the download. After each tranche's
@@ -816,6 +821,98 @@ def prefilter_decide_exact(merit, failed, rays_per_variant: int,
                                              reject.ctypes.data)
     _capi.check(rc, "prefilter decide exact")
     return reject
+
+
+EVAL_EXIT_PUPIL, EVAL_VERTEX, EVAL_INFINITE = 0, 1, 2
+
+
+@dataclass
+class EvalSettings:
+    """EvalSettings (include/mikroptim/eval/eval.hpp:27): grid edge N, half pupil (x >= 0),
+    the reference sphere (EVAL_EXIT_PUPIL, EVAL_VERTEX, EVAL_INFINITE), the field-ray offset;
+    paraxial_column: the wavelength column holding the paraxial index (exit-pupil position)."""
+
+    grid: int = 64
+    half_pupil: bool = False
+    reference: int = EVAL_EXIT_PUPIL
+    field_ray_offset: float = 1e-3
+    paraxial_column: int = 0
+
+
+@dataclass
+class EvalResult:
+    """EvalResult (eval.hpp:96): ray (v, f, l, k) at ((v F + f) L + l) n + k; field ray j at
+    ((v F + f) L + l) 4 + j with values (x, y, d_x, d_y, d_z). OPD and spot in mm (spot
+    relative to the ideal image point); failed rays NaN with their status."""
+
+    variants: int
+    fields: int
+    wavelengths: int
+    grid: np.ndarray              # [n][3] x, y, weight
+    reference_curvature: np.ndarray
+    exit_pupil_position: np.ndarray
+    opd: np.ndarray
+    spot_x: np.ndarray
+    spot_y: np.ndarray
+    status: np.ndarray
+    field_rays: np.ndarray
+    field_status: np.ndarray
+
+    @property
+    def samples(self) -> int:
+        return self.grid.shape[0]
+
+
+def eval_grid(size: int, half_pupil: bool = False) -> np.ndarray:
+    """make_eval_grid: cell centres inside the unit pupil with their weights, [n][3]."""
+    lib = _capi.lib()
+    n = C.c_int64()
+    _capi.check(lib.mkb_eval_grid_host(size, int(half_pupil), None, C.byref(n)), "eval grid")
+    pts = np.zeros((n.value, 3))
+    _capi.check(lib.mkb_eval_grid_host(size, int(half_pupil), pts.ctypes.data, C.byref(n)),
+                "eval grid")
+    return pts
+
+
+def evaluate_device(dbatch: "DeviceSystemBatch", host: SystemBatchHost,
+                    settings: EvalSettings | None = None, stream=None) -> EvalResult:
+    """EVAL on an uploaded batch (TraceEngine::evaluate, the kernel EVAL): bit-identical to
+    the reference's eval_cpu."""
+    lib = _capi.lib()
+    settings = settings or EvalSettings()
+    if settings.half_pupil and host.non_coaxial:
+        raise ValueError("EVAL: half pupil only for coaxial systems")
+    dev = dbatch.device
+    V, F, L = host.variants, host.fields, host.wavelengths
+    pts = eval_grid(settings.grid, settings.half_pupil)
+    n = pts.shape[0]
+    kappa = np.zeros((V, F))
+    z_ap = np.zeros(V)
+    view = host.view()
+    _capi.check(lib.mkb_eval_reference_host(C.byref(view), settings.reference,
+                                            settings.paraxial_column, kappa.ctypes.data,
+                                            z_ap.ctypes.data), "eval reference")
+    T = V * F * L
+    out = dict(opd=torch.empty(T * n, dtype=torch.float64, device=dev),
+               sx=torch.empty(T * n, dtype=torch.float64, device=dev),
+               sy=torch.empty(T * n, dtype=torch.float64, device=dev),
+               st=torch.empty(T * n, dtype=torch.uint8, device=dev),
+               fr=torch.empty(T * 20, dtype=torch.float64, device=dev),
+               fs=torch.empty(T * 4, dtype=torch.uint8, device=dev))
+    grid_d = torch.from_numpy(pts).to(dev)
+    kappa_d = torch.from_numpy(kappa).to(dev)
+    b = dbatch.c_struct()
+    ws = torch.empty(int(lib.mkb_eval_workspace_bytes(C.byref(b))), dtype=torch.uint8,
+                     device=dev)
+    rc = lib.mkb_eval_device(C.byref(b), settings.reference, settings.field_ray_offset,
+                             C.c_void_p(grid_d.data_ptr()), n, C.c_void_p(kappa_d.data_ptr()),
+                             *[C.c_void_p(out[k].data_ptr()) for k in
+                               ("opd", "sx", "sy", "st", "fr", "fs")],
+                             C.c_void_p(ws.data_ptr()), ws.numel(), _stream_handle(stream))
+    _capi.check(rc, "eval")
+    h = {k: v.cpu().numpy() for k, v in out.items()}
+    return EvalResult(V, F, L, pts, kappa.reshape(-1), z_ap, h["opd"], h["sx"], h["sy"], h["st"],
+                      h["fr"], h["fs"])
 
 
 class _UnitWeights:

@@ -272,6 +272,32 @@ class Reference(_Oracle):
         self._check(rc, "extra_rows")
         return J, r
 
+    def eval(self, batch, layout, grid: int = 64, half: bool = False, reference: int = 0,
+             delta: float = 1e-3) -> dict:
+        """eval_cpu (src/eval/eval.cpp:307) in the reference's layout."""
+        L = self.lib
+        L.mko_ref_eval.argtypes = [_PB, _PP, C.c_int, C.c_int, C.c_int, C.c_double,
+                                   C.c_void_p] + [C.c_void_p] * 8
+        L.mko_ref_eval.restype = C.c_int
+        view, plan = batch.view(), layout.plan(batch)
+        n = C.c_int64()
+        rc = L.mko_ref_eval(C.byref(view), C.byref(plan), grid, int(half), reference, delta,
+                            C.addressof(n), *([None] * 8))
+        self._check(rc, "eval")
+        T = batch.variants * batch.fields * batch.wavelengths
+        N = n.value
+        out = dict(opd=np.zeros(T * N), spot_x=np.zeros(T * N), spot_y=np.zeros(T * N),
+                   status=np.zeros(T * N, np.uint8), field_rays=np.zeros(T * 20),
+                   field_status=np.zeros(T * 4, np.uint8),
+                   kappa=np.zeros(batch.variants * batch.fields),
+                   exit_pupil=np.zeros(batch.variants))
+        rc = L.mko_ref_eval(C.byref(view), C.byref(plan), grid, int(half), reference, delta,
+                            C.addressof(n), *[out[k].ctypes.data for k in (
+                                "opd", "spot_x", "spot_y", "status", "field_rays",
+                                "field_status", "kappa", "exit_pupil")])
+        self._check(rc, "eval")
+        return out
+
     def prefilter(self, batch, layout, options, extra=None) -> dict:
         """prefilter_cpu (src/batch/batch_prefilter.cpp): raw per-variant results and the
         decision. `options` is a _capi.PrefilterOptions."""

@@ -14,6 +14,7 @@
 //   paraxial_residuals     src/optim/paraxial_residuals.cpp:353 (extra residual rows)
 //   prefilter_stats_cpu, prefilter_decide, prefilter_decide_exact, prefilter_rays_cpu
 //                          src/batch/batch_prefilter.cpp (FP32 multistart prefilter)
+//   eval_cpu               src/eval/eval.cpp:307 (EVAL on the dense pupil grid)
 // Only tests/, the golden-fixture script and bench.py's CPU legs load this library.
 
 #include "mikroptim_b200.h"
@@ -21,6 +22,7 @@
 #include "mikroptim/batch/batch_extrema.hpp"
 #include "mikroptim/batch/batch_merit.hpp"
 #include "mikroptim/batch/batch_prefilter.hpp"
+#include "mikroptim/eval/eval.hpp"
 #include "mikroptim/batch/batch_residuals.hpp"
 #include "mikroptim/batch/system_batch.hpp"
 #include "mikroptim/model/system.hpp"
@@ -419,6 +421,39 @@ int mko_ref_prefilter_rays(const mkb_batch_view* view, const mkb_residual_plan* 
         std::copy(d.status.begin(), d.status.end(), status);
         std::copy(d.margin.begin(), d.margin.end(), margin);
         std::copy(d.certain.begin(), d.certain.end(), certain);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// eval_cpu: grid points n (out), then the arrays in the reference's layout when `opd` is not
+// null (call twice: sizes first). reference: 0 ExitPupil, 1 Vertex, 2 Infinite.
+int mko_ref_eval(const mkb_batch_view* view, const mkb_residual_plan* plan, int grid, int half,
+                 int reference, double delta, int64_t* n, double* opd, double* spot_x,
+                 double* spot_y, uint8_t* status, double* field_rays, uint8_t* field_status,
+                 double* kappa, double* exit_pupil) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        mko::EvalSettings s;
+        s.grid = grid;
+        s.half_pupil = half != 0;
+        s.reference = static_cast<mko::EvalReference>(reference);
+        s.field_ray_offset = delta;
+        if (opd == nullptr) {
+            *n = mko::make_eval_grid(grid, half != 0).samples();
+            return 0;
+        }
+        const mko::EvalResult r = mko::eval_cpu(b, s);
+        *n = r.samples();
+        std::copy(r.opd.begin(), r.opd.end(), opd);
+        std::copy(r.spot_x.begin(), r.spot_x.end(), spot_x);
+        std::copy(r.spot_y.begin(), r.spot_y.end(), spot_y);
+        std::copy(r.status.begin(), r.status.end(), status);
+        std::copy(r.field_rays.begin(), r.field_rays.end(), field_rays);
+        std::copy(r.field_status.begin(), r.field_status.end(), field_status);
+        std::copy(r.reference_curvature.begin(), r.reference_curvature.end(), kappa);
+        std::copy(r.exit_pupil_position.begin(), r.exit_pupil_position.end(), exit_pupil);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
