@@ -191,9 +191,21 @@ typedef struct mkb_residual_plan {
     const double* wavelength_weight;  /* host [L]                                        */
     const double* quad_u;             /* host [rings]                                    */
     const double* quad_w;             /* host [rings]                                    */
+    /* Transverse ray errors as residual rows (>= 0; 0 = none). No counterpart in the
+     * reference, whose residual rows are OPD only: after the ray rows and the penalty rows,
+     * 2 x rays rows -- the x errors of every ray in the ray-row order, then the y errors --
+     * r_x = sqrt(transverse_weight * w_(f,l)) sqrt(W_k) (x_k - 0), r_y likewise with
+     * (y_k - h_f), where (x_k, y_k) is the ray's intersection with the image plane
+     * (thickness[S-1] behind the last vertex, transfer_to_image_plane,
+     * include/mikroptim/trace/trace.hpp:402), w_(f,l) the tuple weight and W_k the pupil
+     * weight; 0 for a ray that failed hard. Units: waves^2 per mm^2 (the merit's unit per
+     * squared image-plane error). MERIT adds sum_k r_x^2, then sum_k r_y^2 after each tuple's
+     * OPD and penalty sums. RESIDUALS, MERIT and the FD Jacobian; the adjoint paths refuse it. */
+    double transverse_weight;
 } mkb_residual_plan;
 
-/* Rays per variant (ResidualLayout::rays_per_variant) and trace rows (rays + penalty rows). */
+/* Rays per variant (ResidualLayout::rays_per_variant) and trace rows (rays, penalty rows in soft
+ * mode, transverse rows with transverse_weight > 0). */
 int64_t mkb_rays_per_variant(const mkb_residual_plan* plan);
 int64_t mkb_trace_rows(const mkb_residual_plan* plan);
 
@@ -623,12 +635,14 @@ int mkb_eval_reference_host(const mkb_batch_view* view, int32_t reference,
                             int32_t paraxial_column, double* kappa, double* exit_pupil);
 size_t mkb_eval_workspace_bytes(const mkb_device_batch* batch);
 /* grid, kappa: device arrays from the two host calls above; half_pupil as for the grid;
- * outputs device [V F L n] (opd, spot_x, spot_y, status) and [V F L 4] x 5 / [V F L 4]. */
+ * outputs device [V F L n] (opd, spot_x, spot_y, status) and [V F L 4] x 5 / [V F L 4].
+ * precision: MKB_PRECISION_FP64 (the reference's arithmetic) or MKB_PRECISION_FP64_FMA
+ * (contracted; the forward of the MIXED mode), for intercept and OPD errors. */
 int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double field_ray_offset,
-                    const double* grid, int64_t n, const double* kappa, double* opd,
-                    double* spot_x, double* spot_y, uint8_t* status, double* field_rays,
-                    uint8_t* field_status, void* workspace, size_t workspace_bytes,
-                    void* stream);
+                    int32_t precision, const double* grid, int64_t n, const double* kappa,
+                    double* opd, double* spot_x, double* spot_y, uint8_t* status,
+                    double* field_rays, uint8_t* field_status, void* workspace,
+                    size_t workspace_bytes, void* stream);
 
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);

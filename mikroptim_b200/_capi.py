@@ -82,6 +82,7 @@ class ResidualPlan(C.Structure):
         ("wavelength_weight", P_double),
         ("quad_u", P_double),
         ("quad_w", P_double),
+        ("transverse_weight", C.c_double),
     ]
 
 
@@ -209,8 +210,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_eval_workspace_bytes.restype = c.c_size_t
     lib.mkb_eval_workspace_bytes.argtypes = [C.POINTER(DeviceBatch)]
     lib.mkb_eval_device.restype = c.c_int
-    lib.mkb_eval_device.argtypes = [C.POINTER(DeviceBatch), c.c_int32, c.c_double, c.c_void_p,
-                                    c.c_int64, c.c_void_p] + [c.c_void_p] * 6 + \
+    lib.mkb_eval_device.argtypes = [C.POINTER(DeviceBatch), c.c_int32, c.c_double, c.c_int32,
+                                    c.c_void_p, c.c_int64, c.c_void_p] + [c.c_void_p] * 6 + \
         [c.c_void_p, c.c_size_t, c.c_void_p]
     lib.mkb_paraxial_rows_device.restype = c.c_int
     lib.mkb_paraxial_rows_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),

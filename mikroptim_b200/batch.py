@@ -331,13 +331,17 @@ def make_non_coaxial(batch: SystemBatchHost) -> SystemBatchHost:
 
 @dataclass
 class ResidualSettings:
-    """ResidualSettings (batch_residuals.hpp:24)."""
+    """ResidualSettings (batch_residuals.hpp:24). transverse_weight (>= 0, waves^2 / mm^2; not
+    in the reference, whose rows are OPD only): with a positive weight every variant's residual
+    vector ends with 2 x rays transverse ray-error rows (image-plane x errors, then y errors,
+    relative to the ideal image point (0, h_f); mkb_residual_plan.transverse_weight)."""
 
     rings: int = 10
     spokes: int = 8
     failure: int = FAILURE_SOFT
     fail_weight: float = DEFAULT_FAIL_WEIGHT
     precision: int = PRECISION_FP64
+    transverse_weight: float = 0.0
 
 
 class ResidualLayout:
@@ -358,6 +362,8 @@ class ResidualLayout:
             raise ValueError("ResidualLayout: fail_weight must be finite and >= 0")
         if settings.precision not in (PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA):
             raise ValueError("ResidualLayout: unknown precision")
+        if not (settings.transverse_weight >= 0 and math.isfinite(settings.transverse_weight)):
+            raise ValueError("ResidualLayout: transverse_weight must be finite and >= 0")
         self.topology = topology
         self.settings = settings
         self.fields = topology.fields
@@ -387,8 +393,12 @@ class ResidualLayout:
         return self.rays_per_variant if self.soft_failure else 0
 
     @property
+    def transverse_rows(self) -> int:
+        return 2 * self.rays_per_variant if self.settings.transverse_weight > 0 else 0
+
+    @property
     def trace_rows(self) -> int:
-        return self.rays_per_variant + self.penalty_rows
+        return self.rays_per_variant + self.penalty_rows + self.transverse_rows
 
     def plan(self, batch: SystemBatchHost) -> _capi.ResidualPlan:
         """mkb_residual_plan for this layout and the shared weights of `batch`."""
@@ -405,6 +415,7 @@ class ResidualLayout:
         p.rings, p.spokes = self.settings.rings, self.settings.spokes
         p.failure, p.precision = self.settings.failure, self.settings.precision
         p.fail_weight = self.settings.fail_weight
+        p.transverse_weight = self.settings.transverse_weight
         p.reference_wavelength_nm = batch.reference_wavelength_nm
         p.fields, p.wavelengths = self.fields, self.wavelengths
         p.pupil_mode = _capi.ptr(keep["pupil_mode"], C.c_uint8)

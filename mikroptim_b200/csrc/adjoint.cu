@@ -373,6 +373,10 @@ int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* tem
 
 int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
                         const double* records, double* J, bool exact, cudaStream_t stream) {
+    if (tp.transverse) {
+        set_error("adjoint Jacobian: transverse ray-error rows have no adjoint (use FD)");
+        return MKB_ERR_UNSUPPORTED;
+    }
     AdjointParams ap;
     ap.t = tp;
     ap.v = vp;
@@ -1161,6 +1165,10 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
                         double* gram, void* scratch, size_t scratch_bytes, int precision,
                         cudaStream_t stream, const int* run_mask, RunVars rv,
                         const int* order, const int* split, int part, int part_pmax) {
+    if (tp.transverse) {
+        set_error("fused adjoint: transverse ray-error rows have no adjoint (use FD)");
+        return MKB_ERR_UNSUPPORTED;
+    }
     if (tp.V <= 0) return MKB_OK;
     const int p_all = rv.table != nullptr ? rv.stride : vp.P;
     const int p_max = part_pmax > 0 ? part_pmax : p_all;  // sizes this launch's shared memory

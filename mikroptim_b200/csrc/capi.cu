@@ -80,6 +80,10 @@ int check_plan(const mkb_residual_plan* plan) {
         set_error("fail_weight must be finite and >= 0");
         return MKB_ERR_ARGUMENT;
     }
+    if (!(plan->transverse_weight >= 0.0) || !std::isfinite(plan->transverse_weight)) {
+        set_error("transverse_weight must be finite and >= 0");
+        return MKB_ERR_ARGUMENT;
+    }
     if (!(plan->reference_wavelength_nm > 0.0) || !std::isfinite(plan->reference_wavelength_nm)) {
         set_error("reference wavelength must be > 0");
         return MKB_ERR_ARGUMENT;
@@ -109,6 +113,11 @@ int check_plan(const mkb_residual_plan* plan) {
 }
 
 }  // namespace
+
+int64_t trace_rows_of(const mkb_residual_plan* plan, int64_t rays) {
+    return rays * (1 + (plan->failure == MKB_FAILURE_SOFT ? 1 : 0) +
+                   (plan->transverse_weight > 0.0 ? 2 : 0));
+}
 
 int residual_scales(const mkb_residual_plan* plan, double* scale) {
     const int rc = check_plan(plan);
@@ -255,7 +264,9 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
             const double w = tuple_weight(plan, f, l);
             p.scale[f * L + l] = w > 0.0 ? std::sqrt(w) / lambda_ref_mm : 0.0;
             p.pscale[f * L + l] = w > 0.0 ? std::sqrt(plan->fail_weight * w) : 0.0;
+            p.tscale[f * L + l] = w > 0.0 ? std::sqrt(plan->transverse_weight * w) : 0.0;
         }
+    p.transverse = plan->transverse_weight > 0.0 ? 1 : 0;
     // pack plan: consecutive tuples until pack_rays rays or kMaxPackTuples tuples; a tuple
     // with more rays than pack_rays (fine pupils) gets a pack of its own
     for (int t = 0; t < p.n_tuples; ++t)
@@ -562,7 +573,7 @@ int64_t mkb_rays_per_variant(const mkb_residual_plan* plan) {
 int64_t mkb_trace_rows(const mkb_residual_plan* plan) {
     const int64_t r = mkb_rays_per_variant(plan);
     if (r < 0) return r;
-    return plan->failure == MKB_FAILURE_SOFT ? 2 * r : r;
+    return trace_rows_of(plan, r);
 }
 
 namespace {
@@ -618,7 +629,7 @@ int mkb_residuals_ex_device(const mkb_device_batch* batch, const mkb_residual_pl
     if (rc != MKB_OK) return rc;
     rc = check_trace_precision(plan->precision, "residuals");
     if (rc != MKB_OK) return rc;
-    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * static_cast<int64_t>(p.rays) : p.rays;
+    const int64_t rows = trace_rows_of(plan, p.rays);
     if (stride < rows) {
         set_error("residuals: stride %lld < trace rows %lld", static_cast<long long>(stride),
                   static_cast<long long>(rows));
@@ -725,7 +736,7 @@ int run_bytes(const TraceParams& p, const mkb_device_batch* shape, const mkb_res
         per += 3 * sizeof(double) + merit_workspace_bytes(1, p.n_tuples);
         if (extra_merit) per += sizeof(double);
     } else {
-        const size_t rows = (plan->failure == MKB_FAILURE_SOFT ? 2 * rays : rays) +
+        const size_t rows = static_cast<size_t>(trace_rows_of(plan, p.rays)) +
                             static_cast<size_t>(extra_residuals);
         per += rows * sizeof(double) + rays;  // residual rows and the status bytes
         if (opd) per += rays * sizeof(double);

@@ -108,6 +108,8 @@ struct TraceParams {
     double sin_full[kMaxSpokes], cos_full[kMaxSpokes];
     double scale[kMaxTuples];       // residual_scale per tuple
     double pscale[kMaxTuples];      // penalty_scale per tuple
+    double tscale[kMaxTuples];      // sqrt(transverse_weight * tuple weight) per tuple
+    int transverse;                 // transverse ray-error rows (plan transverse_weight > 0)
     Pack packs[kMaxPacks];
     int8_t ghost_of[kMaxSurfaces];  // plate number of a ghost-plate surface (table order), or -1
     const uint8_t* vsurf;           // device [V] table surfaces of each variant, or null (S)
@@ -716,6 +718,9 @@ __device__ __forceinline__ void apply_variables(const VarParams& v, const Record
 void count_launch(int n = 1);
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t err, const char* what);
+
+// Rows of one variant's residual vector: rays, penalty rows (soft failure), transverse rows.
+int64_t trace_rows_of(const mkb_residual_plan* plan, int64_t rays);
 
 // residual_scale of every tuple (f-major, then l) into scale[F * L], as make_trace_params
 // computes them; checks the plan first (MKB_OK or MKB_ERR_ARGUMENT).

@@ -27,6 +27,11 @@ namespace mkb {
 namespace {
 
 constexpr int kFieldRays = 4;
+
+template <class T>
+struct NumTag {
+    using type = T;
+};
 constexpr int kFieldValues = 5;
 
 struct EvalParams {
@@ -43,9 +48,8 @@ struct EvalRayOut {
 
 // exit_pupil_sphere_step (eval_ray.hpp:104): s + sigma R = b - kappa t / (sqrt(1 + kappa^2 t)
 // + 1) with q = p - M, b = -q.d, t = -|q x d|^2; only the OPL moves.
-__device__ inline int exit_pupil_step(RayT<Exact64>& r, Exact64 h, Exact64 w, Exact64 kappa,
-                                      Exact64 n_image) {
-    using N = Exact64;
+template <class N>
+__device__ inline int exit_pupil_step(RayT<N>& r, N h, N w, N kappa, N n_image) {
     const N qx = r.px - N(0.0), qy = r.py - h, qz = r.pz - w;
     const N b = -(qx * r.dx + qy * r.dy + qz * r.dz);
     const N cx = qy * r.dz - qz * r.dy;
@@ -53,18 +57,19 @@ __device__ inline int exit_pupil_step(RayT<Exact64>& r, Exact64 h, Exact64 w, Ex
     const N cz = qx * r.dy - qy * r.dx;
     const N t = -(cx * cx + cy * cy + cz * cz);
     const N disc = N(1.0) + kappa * kappa * t;
-    if (!(disc.v >= 0.0)) return kMissed;
+    if (!(value_of(disc) >= 0.0)) return kMissed;
     const N step = b - kappa * t / (nsqrt(disc) + N(1.0));
-    if (!(step.v == step.v)) return kMissed;
+    if (!(value_of(step) == value_of(step))) return kMissed;
     r.opl += n_image * step;
     return kOk;
 }
 
-// eval_ray (eval_ray.hpp:152) of pupil point (x, y) of variant v, field f, wavelength l
-template <int kFeat>
+// eval_ray (eval_ray.hpp:152) of pupil point (x, y) of variant v, field f, wavelength l, in
+// number type N (Exact64: the reference's arithmetic; double: contracted, for the precision
+// sweep's intercept errors)
+template <class N, int kFeat>
 __device__ inline EvalRayOut eval_ray(const EvalParams& e, const double* rec, int v, int f,
                                       int l, double x, double y, double kappa) {
-    using N = Exact64;
     const TraceParams& p = e.t;
     const RecordLayout lay = layout_of(p);
     const int S = surfaces_of(p, v);
@@ -96,29 +101,29 @@ __device__ inline EvalRayOut eval_ray(const EvalParams& e, const double* rec, in
         if (st != kOk) break;
         n_before = n_after;
     }
-    if (st == kOk && !(r.dz.v > 0.0)) st = kBackward;
+    if (st == kOk && !(value_of(r.dz) > 0.0)) st = kBackward;
     if (st == kOk) {
         // transfer_to_image_plane on a copy
         const N z = r.pz - N(thick[S - 1]);
         const N s0 = -z / r.dz;
-        out.ix = (r.px + s0 * r.dx).v;
-        out.iy = (r.py + s0 * r.dy).v;
-        out.dx = r.dx.v;
-        out.dy = r.dy.v;
-        out.dz = r.dz.v;
+        out.ix = value_of(r.px + s0 * r.dx);
+        out.iy = value_of(r.py + s0 * r.dy);
+        out.dx = value_of(r.dx);
+        out.dy = value_of(r.dy);
+        out.dz = value_of(r.dz);
         const N h = N(rec[lay.target + f]);
         const N w = N(thick[S - 1]);
         int branch;
         st = e.reference == MKB_EVAL_VERTEX
                  ? reference_step<N>(r, h, w, n_before, nullptr, branch)
-                 : exit_pupil_step(r, h, w, N(kappa), n_before);
+                 : exit_pupil_step<N>(r, h, w, N(kappa), n_before);
     }
     out.status = st;
-    out.opl = r.opl.v;
+    out.opl = value_of(r.opl);
     return out;
 }
 
-template <int kFeat>
+template <class N, int kFeat>
 __global__ void eval_field_kernel(const __grid_constant__ EvalParams e,
                                   const double* __restrict__ records,
                                   const double* __restrict__ kappa, double* __restrict__ fr,
@@ -135,7 +140,8 @@ __global__ void eval_field_kernel(const __grid_constant__ EvalParams e,
     const double x = j == 3 ? e.delta : 0.0;
     const double y = j == 1 ? e.delta : (j == 2 ? -e.delta : 0.0);
     const double* rec = records + static_cast<int64_t>(v) * e.t.stride;
-    const EvalRayOut r = eval_ray<kFeat>(e, rec, v, f, l, x, y, kappa[int64_t(v) * e.t.F + f]);
+    const EvalRayOut r =
+        eval_ray<N, kFeat>(e, rec, v, f, l, x, y, kappa[int64_t(v) * e.t.F + f]);
     const bool ok = r.status == kOk;
     const double nan = __longlong_as_double(0x7ff8000000000000ll);
     const double h = rec[layout_of(e.t).target + f];
@@ -149,7 +155,7 @@ __global__ void eval_field_kernel(const __grid_constant__ EvalParams e,
     if (j == 0) offset[t] = ok ? r.opl : 0.0;
 }
 
-template <int kFeat>
+template <class N, int kFeat>
 __global__ void eval_grid_kernel(const __grid_constant__ EvalParams e,
                                  const double* __restrict__ records,
                                  const double* __restrict__ grid,
@@ -167,7 +173,7 @@ __global__ void eval_grid_kernel(const __grid_constant__ EvalParams e,
         const int fl = static_cast<int>(t - int64_t(v) * e.t.F * e.t.L);
         const int f = fl / e.t.L, l = fl - f * e.t.L;
         const double* rec = records + static_cast<int64_t>(v) * e.t.stride;
-        const EvalRayOut r = eval_ray<kFeat>(e, rec, v, f, l, grid[3 * k], grid[3 * k + 1],
+        const EvalRayOut r = eval_ray<N, kFeat>(e, rec, v, f, l, grid[3 * k], grid[3 * k + 1],
                                              kappa[int64_t(v) * e.t.F + f]);
         const bool ok = r.status == kOk;
         const double h = rec[layout_of(e.t).target + f];
@@ -325,10 +331,10 @@ size_t mkb_eval_workspace_bytes(const mkb_device_batch* batch) {
 }
 
 int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double field_ray_offset,
-                    const double* grid, int64_t n, const double* kappa, double* opd,
-                    double* spot_x, double* spot_y, uint8_t* status, double* field_rays,
-                    uint8_t* field_status, void* workspace, size_t workspace_bytes,
-                    void* stream_ptr) {
+                    int32_t precision, const double* grid, int64_t n, const double* kappa,
+                    double* opd, double* spot_x, double* spot_y, uint8_t* status,
+                    double* field_rays, uint8_t* field_status, void* workspace,
+                    size_t workspace_bytes, void* stream_ptr) {
     const cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     if (batch == nullptr) {
         set_error("eval: batch is null");
@@ -337,6 +343,10 @@ int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double fie
     if (reference < MKB_EVAL_EXIT_PUPIL || reference > MKB_EVAL_INFINITE) {
         set_error("eval: unknown reference %d", reference);
         return MKB_ERR_ARGUMENT;
+    }
+    if (precision != MKB_PRECISION_FP64 && precision != MKB_PRECISION_FP64_FMA) {
+        set_error("eval: precision %d not available (FP64 or FP64_FMA)", precision);
+        return MKB_ERR_UNSUPPORTED;
     }
     if (batch->variant_surfaces != nullptr) {
         set_error("eval: batches of uneven surface counts are not built (one table per batch)");
@@ -380,17 +390,22 @@ int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double fie
     const int feat = (e.t.non_coaxial ? 1 : 0) | (e.t.G > 0 ? 2 : 0);
     const int64_t nf = tuples * kFieldRays;
     const unsigned fb = static_cast<unsigned>((nf + 127) / 128);
-auto launch = [&](auto feat_tag) {
+    auto launch = [&](auto feat_tag, auto num_tag) {
         constexpr int F_ = decltype(feat_tag)::value;
-        eval_field_kernel<F_><<<fb, 128, 0, stream>>>(e, batch->records, kappa, field_rays,
-                                                       field_status, offset);
-        eval_grid_kernel<F_><<<148 * 16, 128, 0, stream>>>(e, batch->records, grid, kappa,
-                                                            offset, opd, spot_x, spot_y, status);
+        using N = typename decltype(num_tag)::type;
+        eval_field_kernel<N, F_><<<fb, 128, 0, stream>>>(e, batch->records, kappa, field_rays,
+                                                          field_status, offset);
+        eval_grid_kernel<N, F_><<<148 * 16, 128, 0, stream>>>(
+            e, batch->records, grid, kappa, offset, opd, spot_x, spot_y, status);
     };
-    if (feat == 0) launch(std::integral_constant<int, 0>{});
-    else if (feat == 1) launch(std::integral_constant<int, 1>{});
-    else if (feat == 2) launch(std::integral_constant<int, 2>{});
-    else launch(std::integral_constant<int, 3>{});
+    auto by_feat = [&](auto num_tag) {
+        if (feat == 0) launch(std::integral_constant<int, 0>{}, num_tag);
+        else if (feat == 1) launch(std::integral_constant<int, 1>{}, num_tag);
+        else if (feat == 2) launch(std::integral_constant<int, 2>{}, num_tag);
+        else launch(std::integral_constant<int, 3>{}, num_tag);
+    };
+    if (precision == MKB_PRECISION_FP64) by_feat(NumTag<Exact64>{});
+    else by_feat(NumTag<double>{});
     count_launch(2);
     eval_piston_kernel<<<static_cast<unsigned>((tuples + 127) / 128), 128, 0, stream>>>(
         tuples, n, grid, opd, status, piston);

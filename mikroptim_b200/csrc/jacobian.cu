@@ -201,7 +201,7 @@ int fd_jacobian(const mkb_device_batch* templates, const mkb_residual_plan* plan
     }
     const bool exact = plan->precision == MKB_PRECISION_FP64;
     const int P = rv.table != nullptr ? rv.stride : vp.P, n = 2 * P + 1;
-    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const int64_t R = trace_rows_of(plan, tp.rays);
     const FdSizes z = fd_sizes(tp.stride, P, R, tp.rays, runs);
     if (workspace == nullptr || workspace_bytes < z.total_fixed + z.per_run) {
         set_error("fd jacobian: workspace of at least %zu bytes needed (one run per chunk)",
@@ -427,7 +427,7 @@ size_t mkb_fd_jacobian_workspace_bytes(const mkb_device_batch* templates,
     mkb_device_batch one = *templates;
     one.variants = 1;
     if (make_trace_params(&one, plan, pack_rays_default(), &tp) != MKB_OK) return 0;
-    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const int64_t rows = trace_rows_of(plan, tp.rays);
     const FdSizes z = fd_sizes(tp.stride, P, rows, tp.rays, runs);
     return z.total_fixed + z.per_run * static_cast<size_t>(runs_per_chunk < runs ? runs_per_chunk : runs);
 }
@@ -487,7 +487,7 @@ int mkb_adjoint_jacobian_device(const mkb_device_batch* templates, const mkb_res
         return MKB_ERR_WORKSPACE;
     }
     const bool exact = plan->precision == MKB_PRECISION_FP64;
-    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(tp.rays) : tp.rays;
+    const int64_t R = trace_rows_of(plan, tp.rays);
     double* records = static_cast<double*>(workspace);
     const RecordLayout lay = layout_of(tp);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream);

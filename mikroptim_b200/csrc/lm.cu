@@ -681,7 +681,11 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
         set_error("lm: uneven batches run with the fused adjoint (gram_exact = 0) or FD");
         return MKB_ERR_UNSUPPORTED;
     }
-    s.R = plan->failure == MKB_FAILURE_SOFT ? 2 * int64_t(s.tp.rays) : s.tp.rays;
+    s.R = trace_rows_of(plan, s.tp.rays);
+    if (s.tp.transverse && !s.fd) {
+        set_error("lm: transverse ray-error rows have no adjoint; use the FD Jacobian");
+        return MKB_ERR_UNSUPPORTED;
+    }
     return make_paraxial_spec(options, templates, plan, &s.px);
 }
 

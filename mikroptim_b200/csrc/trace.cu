@@ -52,11 +52,15 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // s and cos I = d . N (d before the refraction, N = (-c x, -c y, 1 - c z), c = 0 off spheres)
 // for every surface the ray passed; surface 0 is the start point and cos I = d_z there
 // (RaySurfaceRecord, trace/surface_extrema.hpp; observer calls in trace/trace.hpp:316,346).
-template <class N, int kFeat, bool kExtrema = false>
+// kImage: img gets the ray's intersection (x, y) with the image plane, thickness[S - 1] behind
+// the last vertex (transfer_to_image_plane, trace/trace.hpp:402, on a copy), for rays in the
+// piston.
+template <class N, int kFeat, bool kExtrema = false, bool kImage = false>
 __device__ inline int trace_ray(const TraceParams& p, const double* rec, const double* mu_tab,
                                 const RecordLayout& lay, int S, int f, int l, const Sample& smp,
                                 bool soft_mode, double& opl, double& penalty,
-                                double* hsq = nullptr, double* cosi = nullptr) {
+                                double* hsq = nullptr, double* cosi = nullptr,
+                                double* img = nullptr) {
     const int L = p.L;
     const N zero(0.0);
     const N a = rec[lay.pupil];
@@ -105,6 +109,12 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
         if (!(r.dz > zero)) {
             status = kBackward;
         } else {
+            if constexpr (kImage) {
+                const N z = r.pz - N(thick[S - 1]);
+                const N s0 = -z / r.dz;
+                img[0] = value_of(r.px + s0 * r.dx);
+                img[1] = value_of(r.py + s0 * r.dy);
+            }
             int branch;
             const int rst = reference_step<N>(r, N(rec[lay.target + f]), N(thick[S - 1]),
                                               n_before, sp, branch);
@@ -420,6 +430,111 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
     }
 }
 
+// Transverse ray-error rows (plan transverse_weight > 0): one CTA per (variant, tuple) traces
+// the tuple's rays again with their image-plane intersection and writes the rows
+// r_x = t_s sqrt(W) (x - 0), r_y = t_s sqrt(W) (y - h_f) (0 for rays that failed hard) after
+// the ray and penalty rows (RESIDUALS), or adds sum_k r_x^2, then sum_k r_y^2, in ascending k
+// to the tuple's MERIT partial sum. The arithmetic and the status of every ray are those of
+// trace_kernel.
+template <int kPrecision, int kFeat, bool kResiduals>
+__global__ void __launch_bounds__(kThreads)
+transverse_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
+                  TupleOut out) {
+    constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
+    using N = typename std::conditional<kExact, Exact64, double>::type;
+    __shared__ SharedTables tab;
+    const int slot = blockIdx.x / p.n_tuples;
+    const int tu = blockIdx.x - slot * p.n_tuples;
+    const int v = p.order != nullptr ? p.order[slot] : slot;
+    if (!run_active(out.mask, v)) return;
+    copy_tables(p, tab);
+    extern __shared__ __align__(16) double dyn[];
+    double* mu_tab = dyn;                              // [S][L]
+    double* sq = dyn + ((p.S * p.L + 1) & ~1);         // MERIT: [2 n] squares
+    const int S = surfaces_of(p, v);
+    const RecordLayout lay = layout_of(p);
+    const double* rec = records + static_cast<int64_t>(v) * p.stride;
+    for (int i = threadIdx.x; i < S * p.L; i += kThreads) {
+        const int s = i / p.L, l = i - s * p.L;
+        mu_tab[i] = s >= 1 ? value_of(N(rec[lay.index + (s - 1) * p.L + l]) /
+                                      N(rec[lay.index + s * p.L + l]))
+                           : 0.0;
+    }
+    __syncthreads();
+    const int f = tu / p.L, l = tu - f * p.L;
+    const int n = p.sample_count[f];
+    const int64_t row0 = p.field_offset[f] + static_cast<int64_t>(l) * n;
+    const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
+    const int64_t base = static_cast<int64_t>(p.rays) * (soft_mode ? 2 : 1);
+    const N ts = p.tscale[tu];
+    const N h = rec[lay.target + f];
+    for (int k = threadIdx.x; k < n; k += kThreads) {
+        const Sample smp = pupil_sample(p, tab, f, k);
+        double opl, pen, img[2] = {0.0, 0.0};
+        const int st = trace_ray<N, kFeat, false, true>(p, rec, mu_tab, lay, S, f, l, smp,
+                                                        soft_mode, opl, pen, nullptr, nullptr,
+                                                        img);
+        const bool in = in_piston(st);
+        const N ex = in ? N(img[0]) - N(0.0) : N(0.0);
+        const N ey = in ? N(img[1]) - h : N(0.0);
+        const N rw = smp.root_weight;
+        const N rx = ts * rw * ex, ry = ts * rw * ey;
+        if constexpr (kResiduals) {
+            const int64_t row = static_cast<int64_t>(v) * out.stride + base + row0 + k;
+            out.residuals[row] = value_of(rx);
+            out.residuals[row + p.rays] = value_of(ry);
+        } else {
+            sq[k] = value_of(rx * rx);
+            sq[n + k] = value_of(ry * ry);
+        }
+    }
+    if constexpr (!kResiduals) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            N tx(0.0), ty(0.0);
+            for (int k = 0; k < n; ++k) tx += N(sq[k]);
+            for (int k = 0; k < n; ++k) ty += N(sq[n + k]);
+            const int64_t slot_t = static_cast<int64_t>(v) * p.n_tuples + tu;
+            N part = out.part[slot_t];
+            part += tx;
+            part += ty;
+            out.part[slot_t] = value_of(part);
+        }
+    }
+}
+
+template <bool kResiduals>
+int launch_transverse(const TraceParams& p, const double* records, const TupleOut& out,
+                      int precision, cudaStream_t stream) {
+    if (!p.transverse || p.V == 0) return MKB_OK;
+    int max_n = 0;
+    for (int f = 0; f < p.F; ++f) max_n = p.sample_count[f] > max_n ? p.sample_count[f] : max_n;
+    const size_t smem = (static_cast<size_t>((p.S * p.L + 1) & ~1) +
+                         (kResiduals ? 0 : 2 * static_cast<size_t>(max_n))) * sizeof(double);
+    const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
+    constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
+    auto kernel = precision == MKB_PRECISION_FP64
+                      ? (feat == 0   ? transverse_kernel<E, 0, kResiduals>
+                         : feat == 1 ? transverse_kernel<E, 1, kResiduals>
+                         : feat == 2 ? transverse_kernel<E, 2, kResiduals>
+                                     : transverse_kernel<E, 3, kResiduals>)
+                      : (feat == 0   ? transverse_kernel<F, 0, kResiduals>
+                         : feat == 1 ? transverse_kernel<F, 1, kResiduals>
+                         : feat == 2 ? transverse_kernel<F, 2, kResiduals>
+                                     : transverse_kernel<F, 3, kResiduals>);
+    if (smem > 48 * 1024) {
+        const int rc = cuda_status(cudaFuncSetAttribute(
+                                       kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)),
+                                   "transverse rows: shared memory attribute");
+        if (rc != MKB_OK) return rc;
+    }
+    const unsigned blocks = static_cast<unsigned>(static_cast<int64_t>(p.V) * p.n_tuples);
+    kernel<<<blocks, kThreads, smem, stream>>>(p, records, out);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "transverse rows launch");
+}
+
 // merit[v] = sum over tuples in order (f-major, then l); counts likewise.
 // Extrema output [V][S][2]: neutral keys before the trace, then the values (sqrt of the largest
 // height^2, smallest cos I) in place.
@@ -560,7 +675,9 @@ int launch_residuals(const TraceParams& p, const double* records, double* residu
                      cudaStream_t stream, RunMask mask, double* extrema) {
     TupleOut out{residuals, stride, opd, status, nullptr, nullptr, nullptr, mask,
                  reinterpret_cast<unsigned long long*>(extrema)};
-    return launch_trace<true>(p, records, out, precision, stream);
+    const int rc = launch_trace<true>(p, records, out, precision, stream);
+    if (rc != MKB_OK) return rc;
+    return launch_transverse<true>(p, records, out, precision, stream);
 }
 
 int launch_merit(const TraceParams& p, const double* records, double* merit, int64_t* failed,
@@ -578,6 +695,8 @@ int launch_merit(const TraceParams& p, const double* records, double* merit, int
                  reinterpret_cast<int*>(ws + slots * (sizeof(double) + sizeof(int))), mask,
                  reinterpret_cast<unsigned long long*>(extrema)};
     int rc = launch_trace<false>(p, records, out, precision, stream);
+    if (rc != MKB_OK) return rc;
+    rc = launch_transverse<false>(p, records, out, precision, stream);
     if (rc != MKB_OK) return rc;
     merit_finalize_kernel<<<(p.V + 255) / 256, 256, 0, stream>>>(
         p.V, p.n_tuples, out.part, out.part_failed, out.part_hard, merit, failed, hard, mask,

@@ -522,7 +522,7 @@ class TraceEngine:
                 hp["status"] = host("status", (V, rays), torch.uint8)
             out.merit = MeritResult()
             out.residuals = ResidualResult(
-                V, rays, layout.trace_rows - rays, stride, hp["res"].numpy(),
+                V, rays, layout.penalty_rows, stride, hp["res"].numpy(),
                 hp["opd"].numpy() if ts.opd else np.zeros((0, 0)),
                 hp["status"].numpy() if ts.status else np.zeros((0, 0), dtype=np.uint8))
             if ts.extrema:
@@ -639,7 +639,7 @@ class TraceEngine:
                                          C.c_void_p(opd.data_ptr()) if opd is not None else None,
                                          C.c_void_p(st.data_ptr()), _stream_handle(None))
         _capi.check(rc, "residuals")
-        return DeviceTranche(first, n, rays, layout.trace_rows - rays, stride, res, st, opd,
+        return DeviceTranche(first, n, rays, layout.penalty_rows, stride, res, st, opd,
                              ext)
 
     def _merit_tranche(self, part: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
@@ -837,6 +837,7 @@ class EvalSettings:
     reference: int = EVAL_EXIT_PUPIL
     field_ray_offset: float = 1e-3
     paraxial_column: int = 0
+    precision: int = 0  # PRECISION_FP64 (the reference's arithmetic) or PRECISION_FP64_FMA
 
 
 @dataclass
@@ -905,7 +906,7 @@ def evaluate_device(dbatch: "DeviceSystemBatch", host: SystemBatchHost,
     ws = torch.empty(int(lib.mkb_eval_workspace_bytes(C.byref(b))), dtype=torch.uint8,
                      device=dev)
     rc = lib.mkb_eval_device(C.byref(b), settings.reference, settings.field_ray_offset,
-                             C.c_void_p(grid_d.data_ptr()), n, C.c_void_p(kappa_d.data_ptr()),
+                             settings.precision, C.c_void_p(grid_d.data_ptr()), n, C.c_void_p(kappa_d.data_ptr()),
                              *[C.c_void_p(out[k].data_ptr()) for k in
                                ("opd", "sx", "sy", "st", "fr", "fs")],
                              C.c_void_p(ws.data_ptr()), ws.numel(), _stream_handle(stream))

@@ -343,8 +343,11 @@ typedef struct {
 
 /* trace_to_reference_sphere, reference_sphere.hpp:181 (with trace_ray_recorded,
  * trace.hpp:301, and trace_segment, trace.hpp:275). */
-static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center, soft_t* soft,
-                              record_t* rec) {
+/* img (or NULL): the intersection (x, y) with the image plane thickness[S-1] behind the last
+ * vertex (transfer_to_image_plane, trace.hpp:402, on a copy), for rays in the piston: the
+ * transverse ray-error rows of this build (no reference counterpart). */
+static int trace_to_reference_img(const table_t* sys, int l, ray_t* ray, vec3 center,
+                                  soft_t* soft, record_t* rec, double* img) {
     const int S = sys->S, L = sys->L;
     if (rec) {
         rec->count = 1;
@@ -378,6 +381,12 @@ static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center
     if (st == ST_OK && soft != NULL) st = soft->first;
     if (is_hard(st)) return st;
     if (!(ray->d.z > 0.0)) return ST_BACKWARD;
+    if (img) {
+        ray_t copy = *ray;
+        transfer_to_tangent_plane(&copy, sys->t[S - 1]);
+        img[0] = copy.p.x;
+        img[1] = copy.p.y;
+    }
     const double n_image = sys->n[(S - 1) * L + l];
     double s_ref = 0.0;
     const int rst = reference_sphere_step(ray, center, n_image, &s_ref, soft);
@@ -385,6 +394,11 @@ static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center
     if (rec) rec->image_branch = rst == ST_SOFT_MISSED ? BR_SOFT_MISSED : BR_REGULAR;
     if (st != ST_OK) return st;
     return rst;
+}
+
+static int trace_to_reference(const table_t* sys, int l, ray_t* ray, vec3 center, soft_t* soft,
+                              record_t* rec) {
+    return trace_to_reference_img(sys, l, ray, center, soft, rec, NULL);
 }
 
 /* ---- pupil samples: pupil/quadrature.hpp:71,103,112 ------------------------------------ */
@@ -501,6 +515,8 @@ static void variant_residuals(const mkb_batch_view* view, const table_t* table, 
     const int S = table->S;
     double opl[MKB_MAX_RINGS * MKB_MAX_SPOKES];
     double penalty[MKB_MAX_RINGS * MKB_MAX_SPOKES];
+    double img[MKB_MAX_RINGS * MKB_MAX_SPOKES][2];
+    const int transverse = plan->transverse_weight > 0.0;
     int st[MKB_MAX_RINGS * MKB_MAX_SPOKES];
     sample_t pupil[MKB_MAX_RINGS * MKB_MAX_SPOKES];
     for (int f = 0; f < plan->fields; ++f) {
@@ -514,7 +530,9 @@ static void variant_residuals(const mkb_batch_view* view, const table_t* table, 
             for (int k = 0; k < n; ++k) {
                 soft_t soft = {0.0, ST_OK};
                 ray_t ray = collimated_ray(a, theta, pupil[k].rho, pupil[k].phi);
-                st[k] = trace_to_reference(table, l, &ray, center, soft_mode ? &soft : NULL, NULL);
+                img[k][0] = img[k][1] = 0.0;
+                st[k] = trace_to_reference_img(table, l, &ray, center, soft_mode ? &soft : NULL,
+                                               NULL, transverse ? img[k] : NULL);
                 opl[k] = ray.opl;
                 penalty[k] = soft.penalty;
             }
@@ -542,6 +560,18 @@ static void variant_residuals(const mkb_batch_view* view, const table_t* table, 
                 for (int k = 0; k < n; ++k)
                     residuals[rays + o + k] =
                         pscale * sqrt(pupil[k].weight) * failure_penalty(st[k], penalty[k]);
+            }
+            if (transverse) { /* transverse ray errors after the ray and penalty rows */
+                const double w = tuple_weight(plan, f, l);
+                const double ts = w > 0.0 ? sqrt(plan->transverse_weight * w) : 0.0;
+                const int64_t base = rays * (soft_mode ? 2 : 1);
+                for (int k = 0; k < n; ++k) {
+                    const int in = in_piston(st[k]);
+                    const double ex = in ? img[k][0] - 0.0 : 0.0;
+                    const double ey = in ? img[k][1] - center.y : 0.0;
+                    residuals[base + o + k] = ts * sqrt(pupil[k].weight) * ex;
+                    residuals[base + rays + o + k] = ts * sqrt(pupil[k].weight) * ey;
+                }
             }
         }
     }
@@ -572,7 +602,8 @@ int mko_port_residuals(const mkb_batch_view* view, const mkb_residual_plan* plan
                        double* residuals, double* opd, uint8_t* status, int threads) {
     if (check_plan(view, plan)) return -1;
     const int64_t rays = mko_port_rays_per_variant(plan);
-    const int64_t rows = plan->failure == MKB_FAILURE_SOFT ? 2 * rays : rays;
+    const int64_t rows = rays * (1 + (plan->failure == MKB_FAILURE_SOFT) +
+                                 2 * (plan->transverse_weight > 0.0));
     res_ctx_t ctx = {view, plan, residuals, opd, status, rays, rows};
     parallel_for(view->variants, threads, residuals_item, &ctx);
     return 0;
@@ -596,7 +627,8 @@ static void merit_item(void* pctx, int v) {
     int64_t* hard_failed = c->hard_failed;
     const int64_t rays = mko_port_rays_per_variant(plan);
     const int soft_mode = plan->failure == MKB_FAILURE_SOFT;
-    const int64_t rows = soft_mode ? 2 * rays : rays;
+    const int transverse = plan->transverse_weight > 0.0;
+    const int64_t rows = rays * (1 + soft_mode + 2 * transverse);
     double* r = (double*)malloc(sizeof(double) * rows);
     double* e = (double*)malloc(sizeof(double) * rays);
     uint8_t* s = (uint8_t*)malloc(rays);
@@ -613,6 +645,14 @@ static void merit_item(void* pctx, int v) {
                 double pen = 0.0;
                 for (int k = 0; k < n; ++k) pen += r[rays + o + k] * r[rays + o + k];
                 tuple += pen;
+            }
+            if (transverse) { /* sum_k r_x^2, then sum_k r_y^2 */
+                const int64_t base = rays * (1 + soft_mode);
+                double tx = 0.0, ty = 0.0;
+                for (int k = 0; k < n; ++k) tx += r[base + o + k] * r[base + o + k];
+                for (int k = 0; k < n; ++k) ty += r[base + rays + o + k] * r[base + rays + o + k];
+                tuple += tx;
+                tuple += ty;
             }
             sum += tuple;
         }
@@ -836,7 +876,8 @@ int mko_port_fd_jacobian(const mkb_batch_view* view, const mkb_residual_plan* pl
         return -1;
     const int P = vars->count;
     const int64_t rays = mko_port_rays_per_variant(plan);
-    const int64_t R = plan->failure == MKB_FAILURE_SOFT ? 2 * rays : rays;
+    const int64_t R = rays * (1 + (plan->failure == MKB_FAILURE_SOFT) +
+                              2 * (plan->transverse_weight > 0.0));
     fd_ctx_t ctx = {view, plan, vars, x0, J, r0, status_changes, P, rays, R};
     parallel_for(runs, threads, fd_item, &ctx);
     return 0;
@@ -1319,6 +1360,7 @@ static void adjoint_item(void* pctx, int i) {
 int mko_port_adjoint_jacobian(const mkb_batch_view* view, const mkb_residual_plan* plan,
                               const mkb_variables* vars, const double* x0, int runs, double* J,
                               double* r0, uint8_t* status, int threads) {
+    if (plan->transverse_weight > 0.0) return -1; /* transverse rows: FD only */
     if (check_plan(view, plan) || check_vars(view, vars) || runs < 1 ||
         (view->variants != 1 && view->variants != runs))
         return -1;

@@ -53,3 +53,17 @@ def test_eval_ghost_plates_and_decentered_bitwise_equal_reference():
     _check(b, st, engine.EvalSettings(grid=24, reference=engine.EVAL_VERTEX))
     b, st, _, _ = workloads.tolerancing(4, elements=3, rings=4, spokes=8)
     _check(b, st, engine.EvalSettings(grid=24))
+
+
+def test_eval_contracted_close_to_exact():
+    """EVAL in FP64 with contraction (the forward of the MIXED mode): the same statuses, and
+    intercepts and OPD within 1e-9 mm of the bit-exact evaluation on the objectives."""
+    b, st, _, _ = workloads.objective(6, rings=3, spokes=6)
+    db = engine.DeviceSystemBatch(b)
+    ex = engine.evaluate_device(db, b, engine.EvalSettings(grid=40))
+    fm = engine.evaluate_device(db, b, engine.EvalSettings(grid=40, precision=2))
+    assert np.array_equal(ex.status, fm.status)
+    ok = ex.status == 0
+    assert np.abs(fm.spot_x[ok] - ex.spot_x[ok]).max() <= 1e-9
+    assert np.abs(fm.spot_y[ok] - ex.spot_y[ok]).max() <= 1e-9
+    assert np.nanmax(np.abs(fm.opd - ex.opd)) <= 1e-9
