@@ -1390,16 +1390,20 @@ def run_precision(args, world, rank, local):
         torch.cuda.synchronize()
         return sum(a.elapsed_time(c) for a, c in ts) / steps
 
+    from mikroptim_b200.batch import PRECISION_DF64
+    lays[PRECISION_DF64] = ResidualLayout(b.topology,
+                                          dataclasses.replace(st, precision=PRECISION_DF64))
     l0 = lib.mkb_launch_count()
     with ClockSampler(local) as clocks:
         ms = {p: merit_ms(p, args.steps) for p in (PRECISION_FP64_FMA, PRECISION_FP64,
-                                                   PRECISION_MIXED)}
+                                                   PRECISION_MIXED, PRECISION_DF64)}
     launches = lib.mkb_launch_count() - l0
     ms = {p: max_over_ranks(v, world, dev) for p, v in ms.items()}
 
     # OPD errors over every ray, in tranches of variants
     lam_mm = b.reference_wavelength_nm * 1e-6
-    acc = {PRECISION_FP64_FMA: [0.0, 0, 0.0, 0, 0], PRECISION_MIXED: [0.0, 0, 0.0, 0, 0]}
+    acc = {PRECISION_FP64_FMA: [0.0, 0, 0.0, 0, 0], PRECISION_MIXED: [0.0, 0, 0.0, 0, 0],
+           PRECISION_DF64: [0.0, 0, 0.0, 0, 0]}
     chunk = 2048
     for first in range(0, V, chunk):
         n = min(chunk, V - first)
@@ -1407,7 +1411,7 @@ def run_precision(args, world, rank, local):
         dsub = engine.DeviceSystemBatch(sub, dev)
         ref = engine.residuals_device(dsub, lay0, sub)
         ok_ref = ((ref.status == 0) | (ref.status == 5) | (ref.status == 6))
-        for p in (PRECISION_FP64_FMA, PRECISION_MIXED):
+        for p in (PRECISION_FP64_FMA, PRECISION_MIXED, PRECISION_DF64):
             r = engine.residuals_device(dsub, lays[p], sub)
             same = (r.status == ref.status) & ok_ref
             err = ((r.opd - ref.opd) / lam_mm)[same]
@@ -1422,7 +1426,8 @@ def run_precision(args, world, rank, local):
                      "max_waves": acc[p][2],
                      "status_agreement": acc[p][3] / max(acc[p][4], 1),
                      "rays_compared": acc[p][1]}
-              for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed"))}
+              for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed"),
+                              (PRECISION_DF64, "df64"))}
 
     # normal equations: fused (FMA, MIXED) against the exact materialised J^T J on a sample
     sample = b.subset(0, 64)
@@ -1470,7 +1475,8 @@ def run_precision(args, world, rank, local):
                    "l2": "flushed (256 MB write) before every timed step"},
         "gpu_launches": int(launches),
         "merit_ms": {"fp64_fma": ms[PRECISION_FP64_FMA], "fp64_exact": ms[PRECISION_FP64],
-                     "mixed": ms[PRECISION_MIXED]},
+                     "mixed": ms[PRECISION_MIXED], "df64": ms[PRECISION_DF64]},
+        "df64_vs_fp64_fma_time": ms[PRECISION_DF64] / ms[PRECISION_FP64_FMA],
         "opd_error_vs_fp64": errors,
         "normal_equations_rel_error_vs_exact": jerr,
         "intercept_error_vs_fp64": intercepts,

@@ -66,7 +66,11 @@ enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_
  * the reference CPU build. FP64_FMA: FP64 with a*b+c contracted to FMA and tree sums (faster,
  * equal within the reference's CPU/GPU tolerances). MIXED: FP32 bulk arithmetic with an FP64
  * sag root and OPL accumulation. */
-enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2 };
+enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2,
+       MKB_PRECISION_DF64 = 3 };
+/* DF64 (RESIDUALS and MERIT only): the reference's reduced-precision trace type
+ * (include/mikroptim/math/df64.hpp:108): every per-ray operation in double-float arithmetic
+ * (a pair of floats, about 48 bits) on the FP32 pipes, the tuple sums in FP64. */
 enum { MKB_VAR_CURVATURE = 0, MKB_VAR_THICKNESS = 1, MKB_VAR_WORKING_DISTANCE = 2,
        MKB_VAR_GHOST_COEFFICIENT = 3, MKB_VAR_GLASS = 4 };
                                                        /* VariableType, model/variables.hpp:18 */

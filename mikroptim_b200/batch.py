@@ -26,7 +26,7 @@ from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_le
 
 SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
 FAILURE_SOFT, FAILURE_HARD = 0, 1
-PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA, PRECISION_DF64 = 0, 1, 2, 3
 VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT, VAR_GLASS = 0, 1, 2, 3, 4
 BUCHDAHL_LAMBDA0_UM, BUCHDAHL_ALPHA = 0.546074, 2.5  # glass/dispersion.hpp:13,15
 MAX_GHOST_PLATES, MAX_GHOST_TERMS = 16, 32
@@ -360,7 +360,8 @@ class ResidualLayout:
             raise ValueError("ResidualLayout: unknown failure mode")
         if not (settings.fail_weight >= 0 and math.isfinite(settings.fail_weight)):
             raise ValueError("ResidualLayout: fail_weight must be finite and >= 0")
-        if settings.precision not in (PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA):
+        if settings.precision not in (PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA,
+                                      PRECISION_DF64):
             raise ValueError("ResidualLayout: unknown precision")
         if not (settings.transverse_weight >= 0 and math.isfinite(settings.transverse_weight)):
             raise ValueError("ResidualLayout: transverse_weight must be finite and >= 0")

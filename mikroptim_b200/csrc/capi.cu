@@ -607,7 +607,7 @@ int options_vpc(const mkb_trace_options* options, TraceParams* p) {
 
 int check_trace_precision(int precision, const char* what) {
     if (precision != MKB_PRECISION_FP64 && precision != MKB_PRECISION_FP64_FMA &&
-        precision != MKB_PRECISION_MIXED) {
+        precision != MKB_PRECISION_MIXED && precision != MKB_PRECISION_DF64) {
         set_error("%s: precision %d not available", what, precision);
         return MKB_ERR_UNSUPPORTED;
     }

@@ -13,6 +13,7 @@
 // Reference behaviour restated: residuals_kernel / merit_kernel + merit_finalize_kernel
 // (src/cuda/residuals.cu:57, src/cuda/merit.cu:62,206), batch_ray_opl (merit/ray_residual.hpp:69),
 // opd_statistics (merit/opd.hpp:37), ray_residual / ray_penalty (merit/ray_residual.hpp:131,199).
+#include "df64.cuh"
 #include "launch.cuh"
 #include "pupil.cuh"
 
@@ -174,7 +175,9 @@ __global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
     constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
-    using N = typename std::conditional<kExact, Exact64, double>::type;
+    using N = typename std::conditional<
+        kExact, Exact64,
+        typename std::conditional<kPrecision == MKB_PRECISION_DF64, Df64, double>::type>::type;
     __shared__ SharedTrace sh;
     // this CTA: pack pk of the variants in queue slots group * vpc .. + nv - 1
     const int vpc = kMulti ? p.vpc : 1;
@@ -507,6 +510,10 @@ template <bool kResiduals>
 int launch_transverse(const TraceParams& p, const double* records, const TupleOut& out,
                       int precision, cudaStream_t stream) {
     if (!p.transverse || p.V == 0) return MKB_OK;
+    if (precision == MKB_PRECISION_DF64) {
+        set_error("transverse rows: not built for DF64");
+        return MKB_ERR_UNSUPPORTED;
+    }
     int max_n = 0;
     for (int f = 0; f < p.F; ++f) max_n = p.sample_count[f] > max_n ? p.sample_count[f] : max_n;
     const size_t smem = (static_cast<size_t>((p.S * p.L + 1) & ~1) +
@@ -593,18 +600,24 @@ template <bool kResiduals>
 int launch_trace(const TraceParams& p_in, const double* records, const TupleOut& out,
                  int precision, cudaStream_t stream) {
     TraceParams p = p_in;
-    // several variants per CTA: built for coaxial batches without ghost plates; the others
-    // trace one variant per CTA (the option only shapes the launch)
-    if (p.non_coaxial || p.G > 0) p.vpc = 1;
+    // several variants per CTA: built for coaxial batches without ghost plates in FP64; the
+    // others trace one variant per CTA (the option only shapes the launch)
+    if (p.non_coaxial || p.G > 0 || precision == MKB_PRECISION_DF64) p.vpc = 1;
     const int64_t groups = (static_cast<int64_t>(p.V) + p.vpc - 1) / p.vpc;
     const unsigned blocks = static_cast<unsigned>(groups * p.n_packs);
     const size_t smem = trace_smem(p, precision == MKB_PRECISION_FP64);
     // kernel variant per precision and features (1: surface transforms, 2: ghost plates)
     const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
     constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
+    constexpr int D = MKB_PRECISION_DF64;
     auto kernel = p.vpc > 1 ? (precision == MKB_PRECISION_FP64
                                    ? trace_kernel<kResiduals, E, 0, false, true>
                                    : trace_kernel<kResiduals, F, 0, false, true>)
+                  : precision == MKB_PRECISION_DF64
+                      ? (feat == 0   ? trace_kernel<kResiduals, D, 0>
+                         : feat == 1 ? trace_kernel<kResiduals, D, 1>
+                         : feat == 2 ? trace_kernel<kResiduals, D, 2>
+                                     : trace_kernel<kResiduals, D, 3>)
                   : precision == MKB_PRECISION_FP64
                       ? (feat == 0   ? trace_kernel<kResiduals, E, 0>
                          : feat == 1 ? trace_kernel<kResiduals, E, 1>
@@ -617,7 +630,11 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
     const int64_t n_ext = static_cast<int64_t>(p.V) * p.S * 2;
     if (out.extrema != nullptr) {
         // per-surface extrema: coaxial batches (with or without ghost plates), one variant per
-        // CTA
+        // CTA, FP64
+        if (precision == MKB_PRECISION_DF64) {
+            set_error("trace: extrema are not built for DF64");
+            return MKB_ERR_UNSUPPORTED;
+        }
         if (p.vpc != 1) {
             set_error("trace: extrema need one variant per CTA");
             return MKB_ERR_UNSUPPORTED;
