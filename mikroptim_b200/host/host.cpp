@@ -320,7 +320,8 @@ ResidualLayout::ResidualLayout(const BatchTopology& topology, const ResidualSett
 }
 
 int64_t ResidualLayout::trace_rows() const {
-    return settings_.failure == FailureMode::Soft ? 2 * rays_ : rays_;
+    return rays_ * (1 + (settings_.failure == FailureMode::Soft ? 1 : 0) +
+                    (settings_.transverse_weight > 0.0 ? 2 : 0));
 }
 
 int64_t ResidualLayout::offset(int f, int l) const {
@@ -358,6 +359,7 @@ std::unique_ptr<ResidualPlan> ResidualLayout::plan_from(
     c.failure = static_cast<int32_t>(settings_.failure);
     c.precision = static_cast<int32_t>(settings_.precision);
     c.fail_weight = settings_.fail_weight;
+    c.transverse_weight = settings_.transverse_weight;
     c.reference_wavelength_nm = reference_wavelength_nm;
     c.fields = topology_.fields;
     c.wavelengths = topology_.wavelengths;
@@ -466,7 +468,7 @@ mkb_variables VariableSet::c_struct() const {
     return c;
 }
 
-mkb_lm_options LmOptions::c_struct() const {
+mkb_lm_options LmOptions::c_struct(std::vector<mkb_paraxial_constraint>* storage) const {
     mkb_lm_options o{};
     o.max_iterations = max_iterations;
     o.reject_new_failures = reject_new_failures ? 1 : 0;
@@ -478,6 +480,19 @@ mkb_lm_options LmOptions::c_struct() const {
     o.diag_floor = diag_floor;
     o.jacobian = static_cast<int32_t>(jacobian);
     o.gram_exact = gram_exact ? 1 : 0;
+    if (!paraxial.items.empty()) {
+        if (storage == nullptr)
+            throw std::invalid_argument("LmOptions: paraxial constraints need a storage vector");
+        storage->clear();
+        for (const ParaxialConstraint& c : paraxial.items)
+            storage->push_back(mkb_paraxial_constraint{c.type, c.mode, c.weight, c.target,
+                                                       c.reference_surface, 0, c.offset,
+                                                       c.shift});
+        o.paraxial_count = static_cast<int32_t>(storage->size());
+        o.paraxial = storage->data();
+        o.paraxial_column = paraxial.column;
+        o.paraxial_derivative = paraxial.analytic ? MKB_PARAXIAL_ADJOINT : MKB_PARAXIAL_FD;
+    }
     return o;
 }
 
@@ -776,6 +791,7 @@ DeviceTranche TraceEngine::residual_tranche(const SystemBatchHost& batch,
                    "clear residuals");
     mkb_trace_options o{};
     o.pack_rays = settings.pack_rays;
+    o.variants_per_cta = settings.variants_per_cta;
     if (settings.extrema)
         o.extrema = static_cast<double*>(
             extrema_.reserve(n * static_cast<size_t>(batch.surfaces()) * 2 * sizeof(double)));
@@ -786,7 +802,7 @@ DeviceTranche TraceEngine::residual_tranche(const SystemBatchHost& batch,
     t.first = first;
     t.count = count;
     t.rays_per_variant = rays;
-    t.penalty_rows = layout.trace_rows() - rays;
+    t.penalty_rows = settings.quadrature.failure == FailureMode::Soft ? rays : 0;
     t.stride = stride;
     t.residuals = res;
     t.status = st;
@@ -832,7 +848,7 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
     } else {
         out.residuals.variants = V;
         out.residuals.rays_per_variant = rays;
-        out.residuals.penalty_rows = layout.trace_rows() - rays;
+        out.residuals.penalty_rows = settings.quadrature.failure == FailureMode::Soft ? rays : 0;
         out.residuals.stride = stride;
         out.residuals.residuals.resize(static_cast<size_t>(V) * stride);
         out.residuals.opd.resize(settings.opd ? rays_total : 0);
@@ -864,6 +880,7 @@ void TraceEngine::run(const SystemBatchHost& batch, TraceMode mode,
             auto* h = static_cast<int64_t*>(hard_.reserve(n * sizeof(int64_t)));
             mkb_trace_options o{};
             o.pack_rays = settings.pack_rays;
+            o.variants_per_cta = settings.variants_per_cta;
             if (settings.extrema)
                 o.extrema = static_cast<double*>(extrema_.reserve(
                     n * static_cast<size_t>(batch.surfaces()) * 2 * sizeof(double)));
@@ -1105,7 +1122,8 @@ LmResult lm_pass(TraceEngine& engine, const VariableSet& variables, const System
     templates.upload(base, engine.stream());
     const mkb_device_batch t = templates.c_struct();
     const mkb_variables v = variables.c_struct();
-    const mkb_lm_options o = options.c_struct();
+    std::vector<mkb_paraxial_constraint> paraxial_storage;
+    const mkb_lm_options o = options.c_struct(&paraxial_storage);
     DeviceBuffer dx0, ws;
     const auto* x = static_cast<const double*>(upload(dx0, x0, engine.stream()));
     const size_t bytes = mkb_lm_workspace_bytes(&t, plan->get(), &v, &o, runs);
@@ -1325,6 +1343,149 @@ void extra_rows_host(const VariableSet& variables, const SystemBatchHost& base,
                       jacobian.begin() + (static_cast<ptrdiff_t>(i) * P + k) * E);
         }
     }
+}
+
+PrefilterResult TraceEngine::prefilter_variants(const SystemBatchHost& batch,
+                                                const PrefilterSettings& settings) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    batch.validate_values();
+    const ResidualLayout layout(batch.topology(), settings.quadrature);
+    const auto plan = layout.plan(batch);
+    const int V = batch.variants();
+    const mkb_prefilter_options o{settings.options.criteria.max_failed_fraction,
+                                  settings.options.criteria.max_merit,
+                                  settings.options.criteria.max_merit_factor,
+                                  settings.options.margins.boundary,
+                                  settings.options.margins.opl_error_factor,
+                                  settings.options.margins.merit_relative};
+    if (!settings.extra_merit.empty() && settings.extra_merit.size() != static_cast<size_t>(V))
+        throw std::invalid_argument("prefilter: extra_merit must be empty or hold one value per "
+                                    "variant");
+    PrefilterResult r;
+    PrefilterStats& st = r.stats;
+    st.variants = V;
+    st.rays_per_variant = layout.rays_per_variant();
+    const size_t n = static_cast<size_t>(V);
+    st.merit.assign(n, 0.0);
+    st.optical_length.assign(n, 0.0);
+    st.failed.assign(n, 0);
+    st.uncertain_ok.assign(n, 0);
+    st.uncertain_failed.assign(n, 0);
+    if (V > 0) {
+        batch_.upload(batch, stream_);
+        const mkb_device_batch b = batch_.c_struct();
+        const mkb_batch_view view = batch.view();
+        std::vector<float> trig(n * static_cast<size_t>(batch.fields()) * 2);
+        check(mkb_prefilter_field_trig_host(&view, trig.data()), "prefilter field table");
+        DeviceBuffer dtrig, dout, ws;
+        void* t = dtrig.reserve(trig.size() * sizeof(float));
+        cuda_check(cudaMemcpyAsync(t, trig.data(), trig.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream_)),
+                   "prefilter upload");
+        char* out = static_cast<char*>(dout.reserve(5 * n * 8));
+        void* w = ws.reserve(mkb_prefilter_workspace_bytes(V, plan->get()));
+        check(mkb_prefilter_device(&b, plan->get(), static_cast<const float*>(t),
+                                   o.boundary, reinterpret_cast<double*>(out),
+                                   reinterpret_cast<double*>(out + 8 * n),
+                                   reinterpret_cast<int64_t*>(out + 16 * n),
+                                   reinterpret_cast<int64_t*>(out + 24 * n),
+                                   reinterpret_cast<int64_t*>(out + 32 * n), w, ws.bytes(),
+                                   stream_),
+              "prefilter");
+        void* dst[5] = {st.merit.data(), st.optical_length.data(), st.failed.data(),
+                        st.uncertain_ok.data(), st.uncertain_failed.data()};
+        for (int k = 0; k < 5; ++k)
+            cuda_check(cudaMemcpyAsync(dst[k], out + k * 8 * n, 8 * n, cudaMemcpyDeviceToHost,
+                                       static_cast<cudaStream_t>(stream_)),
+                       "prefilter download");
+        synchronize();
+    }
+    r.merit_lower.assign(n, 0.0);
+    r.merit_upper.assign(n, 0.0);
+    r.reject.assign(n, 0);
+    int32_t ref_v = -1, kept = 0;
+    check(mkb_prefilter_decide_host(plan->get(), &o, V, st.merit.data(), st.optical_length.data(),
+                                    st.failed.data(), st.uncertain_ok.data(),
+                                    st.uncertain_failed.data(),
+                                    settings.extra_merit.empty() ? nullptr
+                                                                 : settings.extra_merit.data(),
+                                    r.merit_lower.data(), r.merit_upper.data(), r.reject.data(),
+                                    &r.reference_merit, &ref_v, &kept),
+          "prefilter decide");
+    r.reference_variant = ref_v;
+    r.kept = kept;
+    return r;
+}
+
+EvalResult TraceEngine::evaluate(const SystemBatchHost& batch, const EvalSettings& settings) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    batch.validate_values();
+    if (settings.half_pupil && !batch.coaxial())
+        throw std::invalid_argument("EVAL: half pupil only for coaxial systems");
+    EvalResult r;
+    r.variants = batch.variants();
+    r.fields = batch.fields();
+    r.wavelengths = batch.wavelengths();
+    int64_t n = 0;
+    check(mkb_eval_grid_host(settings.grid, settings.half_pupil ? 1 : 0, nullptr, &n),
+          "eval grid");
+    r.samples = n;
+    r.grid.resize(static_cast<size_t>(3 * n));
+    check(mkb_eval_grid_host(settings.grid, settings.half_pupil ? 1 : 0, r.grid.data(), &n),
+          "eval grid");
+    const size_t V = static_cast<size_t>(r.variants), F = static_cast<size_t>(r.fields);
+    r.reference_curvature.assign(V * F, 0.0);
+    r.exit_pupil_position.assign(V, 0.0);
+    const mkb_batch_view view = batch.view();
+    check(mkb_eval_reference_host(&view, static_cast<int32_t>(settings.reference),
+                                  settings.paraxial_column, r.reference_curvature.data(),
+                                  r.exit_pupil_position.data()),
+          "eval reference");
+    const size_t T = V * F * static_cast<size_t>(r.wavelengths);
+    const size_t rays = T * static_cast<size_t>(n);
+    r.opd.resize(rays);
+    r.spot_x.resize(rays);
+    r.spot_y.resize(rays);
+    r.status.resize(rays);
+    r.field_rays.resize(T * 20);
+    r.field_status.resize(T * 4);
+    if (V == 0) return r;
+    batch_.upload(batch, stream_);
+    const mkb_device_batch b = batch_.c_struct();
+    const cudaStream_t s = static_cast<cudaStream_t>(stream_);
+    DeviceBuffer dgrid, dkappa, dout, ws;
+    void* g = dgrid.reserve(r.grid.size() * sizeof(double));
+    void* k = dkappa.reserve(r.reference_curvature.size() * sizeof(double));
+    cuda_check(cudaMemcpyAsync(g, r.grid.data(), r.grid.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, s), "eval upload");
+    cuda_check(cudaMemcpyAsync(k, r.reference_curvature.data(),
+                               r.reference_curvature.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, s), "eval upload");
+    char* out = static_cast<char*>(dout.reserve(rays * 25 + T * 164 + 64));
+    double* opd = reinterpret_cast<double*>(out);
+    double* sx = opd + rays;
+    double* sy = sx + rays;
+    double* fr = sy + rays;
+    uint8_t* st = reinterpret_cast<uint8_t*>(fr + T * 20);
+    uint8_t* fs = st + rays;
+    void* w = ws.reserve(mkb_eval_workspace_bytes(&b));
+    check(mkb_eval_device(&b, static_cast<int32_t>(settings.reference),
+                          settings.field_ray_offset, static_cast<int32_t>(settings.precision),
+                          static_cast<const double*>(g), n, static_cast<const double*>(k), opd,
+                          sx, sy, st, fr, fs, w, ws.bytes(), stream_),
+          "eval");
+    struct Copy {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } copies[] = {{r.opd.data(), opd, rays * 8},         {r.spot_x.data(), sx, rays * 8},
+                  {r.spot_y.data(), sy, rays * 8},       {r.status.data(), st, rays},
+                  {r.field_rays.data(), fr, T * 160},    {r.field_status.data(), fs, T * 4}};
+    for (const Copy& c : copies)
+        cuda_check(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, s),
+                   "eval download");
+    synchronize();
+    return r;
 }
 
 LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,

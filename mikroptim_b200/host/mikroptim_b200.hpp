@@ -33,7 +33,7 @@ namespace mkb {
 enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2, GhostPlate = 3 };
 enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
 enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
-enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2 };
+enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2, DF64 = 3 };
 enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2,
                                     GhostCoefficient = 3, Glass = 4 };
 enum class JacobianMethod : int32_t { FiniteDifference = 0, Adjoint = 1 };
@@ -131,6 +131,9 @@ struct ResidualSettings {
     FailureMode failure = FailureMode::Soft;
     double fail_weight = 1e6;  // kDefaultFailWeight (merit/ray_residual.hpp:175)
     Precision precision = Precision::FP64;
+    // transverse ray-error rows after the ray and penalty rows (no reference counterpart:
+    // mkb_residual_plan.transverse_weight); 0 = none
+    double transverse_weight = 0.0;
 };
 
 // The C plan for one batch; owns the arrays its pointers reference (not copyable).
@@ -220,6 +223,23 @@ struct TraceExtraResiduals {
         evaluate;
 };
 
+// Paraxial constraints evaluated on the device as the LM's extra rows (ParaxialConstraint,
+// include/mikroptim/optim/paraxial_residuals.hpp:67; mkb_paraxial_constraint): no host phase
+// in a cycle. column: the wavelength column of the paraxial index; analytic: the adjoint
+// Jacobian of the y-nu trace instead of the reference's central differences.
+struct ParaxialConstraint {
+    int type = MKB_CONSTRAINT_FOCAL_LENGTH;  // ConstraintType order
+    int mode = MKB_MODE_EQUAL;
+    double weight = 1.0, target = 0.0;
+    int reference_surface = 0;
+    double offset = 0.0, shift = 0.0;
+};
+struct ParaxialConstraints {
+    std::vector<ParaxialConstraint> items;
+    int column = 0;
+    bool analytic = false;
+};
+
 struct LmOptions {
     int max_iterations = 100;
     bool reject_new_failures = true;
@@ -235,7 +255,9 @@ struct LmOptions {
     double max_fail_weight = 1e14;
     ExtraResiduals extra;  // the caller's extra rows (LmOptions::jacobian.extra); count 0: none
     TraceExtraResiduals trace_extra;  // rows from the trace's extrema (::jacobian.trace_extra)
-    mkb_lm_options c_struct() const;
+    ParaxialConstraints paraxial;     // constraints on the device (no host phase)
+    // the C struct; its constraint pointer refers to `storage`, which must outlive it
+    mkb_lm_options c_struct(std::vector<mkb_paraxial_constraint>* storage = nullptr) const;
 };
 
 namespace cuda {
@@ -310,6 +332,7 @@ struct TraceSettings {
     std::span<const double> extra_merit{};
     std::optional<Precision> precision;
     int pack_rays = 512;
+    int variants_per_cta = 1;  // runtime only, like pack_rays (the autotuner's second knob)
 };
 
 // TraceRunInfo (trace_engine.hpp:93)
@@ -346,6 +369,64 @@ struct TraceOutput {
     ResidualResult residuals;
     MeritResult merit;
     TraceRunInfo info;
+};
+
+// ---- FP32 prefilter of multistart variants (batch_prefilter.hpp) ----------------------------
+struct PrefilterCriteria {  // batch_prefilter.hpp:35
+    double max_failed_fraction = 0.5;
+    double max_merit = std::numeric_limits<double>::infinity();
+    double max_merit_factor = std::numeric_limits<double>::infinity();
+};
+struct PrefilterMargins {  // batch_prefilter.hpp:52
+    double boundary = 0.15;
+    double opl_error_factor = 32.0;
+    double merit_relative = 0.01;
+};
+struct PrefilterOptions {
+    PrefilterCriteria criteria{};
+    PrefilterMargins margins{};
+};
+// PrefilterSettings (trace_engine.hpp:80)
+struct PrefilterSettings {
+    ResidualSettings quadrature{};
+    PrefilterOptions options{};
+    std::span<const double> extra_merit{};
+};
+struct PrefilterStats {  // batch_prefilter.hpp:66
+    int variants = 0;
+    int64_t rays_per_variant = 0;
+    std::vector<double> merit, optical_length;
+    std::vector<int64_t> failed, uncertain_ok, uncertain_failed;
+};
+enum PrefilterReason : uint8_t { kPrefilterKeep = 0, kPrefilterFailedRays = 1,
+                                 kPrefilterMeritAbsolute = 2, kPrefilterMeritRelative = 4 };
+struct PrefilterResult {  // batch_prefilter.hpp:94
+    PrefilterStats stats;
+    std::vector<double> merit_lower, merit_upper;
+    std::vector<uint8_t> reject;
+    double reference_merit = std::numeric_limits<double>::infinity();
+    int reference_variant = -1;
+    int kept = 0;
+    bool keep(int v) const { return reject.at(static_cast<size_t>(v)) == kPrefilterKeep; }
+};
+
+// ---- EVAL on the dense pupil grid (include/mikroptim/eval/eval.hpp) -----------------------
+enum class EvalReference : int32_t { ExitPupil = 0, Vertex = 1, Infinite = 2 };
+struct EvalSettings {  // eval.hpp:27
+    int grid = 64;
+    bool half_pupil = false;
+    EvalReference reference = EvalReference::ExitPupil;
+    double field_ray_offset = 1e-3;
+    int paraxial_column = 0;  // wavelength column holding the paraxial index
+    Precision precision = Precision::FP64;  // FP64 or FP64_FMA
+};
+struct EvalResult {  // eval.hpp:96, the reference's layout
+    int variants = 0, fields = 0, wavelengths = 0;
+    int64_t samples = 0;
+    std::vector<double> grid;  // [n][3] x, y, weight
+    std::vector<double> reference_curvature, exit_pupil_position;
+    std::vector<double> opd, spot_x, spot_y, field_rays;
+    std::vector<uint8_t> status, field_status;
 };
 
 // One tranche's RESIDUALS on the device (DeviceTranche, trace_engine.hpp:117); the pointers
@@ -400,6 +481,13 @@ public:
     // size is a multiple of `granularity` (only the last may be smaller).
     TraceRunInfo run_on_device(const SystemBatchHost& batch, const TraceSettings& settings,
                                int granularity, const DeviceTrancheFn& consume);
+    // FP32 prefilter (TraceEngine::prefilter_variants, trace_engine.hpp:188): the float trace
+    // with margins on the device, the conservative decision on the host (bit-identical to the
+    // reference's prefilter_cpu).
+    PrefilterResult prefilter_variants(const SystemBatchHost& batch,
+                                       const PrefilterSettings& settings = {});
+    // Mode EVAL (TraceEngine::evaluate, trace_engine.hpp:193), bit-identical to eval_cpu.
+    EvalResult evaluate(const SystemBatchHost& batch, const EvalSettings& settings = {});
     // Largest tranche for batches of this topology; 0 when not one variant fits.
     int max_variants(const BatchTopology& topology, TraceMode mode,
                      const TraceSettings& settings = {}) const;

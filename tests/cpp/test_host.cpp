@@ -24,6 +24,13 @@ extern "C" int mko_ref_paraxial_residuals(const mkb_batch_view*, const mkb_resid
                                           const double*, double*);
 extern "C" int mko_ref_surface_extrema(const mkb_batch_view*, const mkb_residual_plan*,
                                        double*);
+extern "C" int mko_ref_prefilter(const mkb_batch_view*, const mkb_residual_plan*,
+                                 const mkb_prefilter_options*, const double*, double*, double*,
+                                 int64_t*, int64_t*, int64_t*, double*, double*, uint8_t*,
+                                 double*, int32_t*, int32_t*);
+extern "C" int mko_ref_eval(const mkb_batch_view*, const mkb_residual_plan*, int, int, int, double,
+                            int64_t*, double*, double*, double*, uint8_t*, double*, uint8_t*,
+                            double*, double*);
 extern "C" int mko_ref_optimize_lm(const mkb_batch_view*, const mkb_residual_plan*,
                                    const mkb_variables*, const double*, int, int, int, int, int,
                                    double*, double*, int32_t*, int32_t*, int32_t*, double*, int,
@@ -43,6 +50,16 @@ void expect(bool ok, const char* what) {
 template <class T>
 bool same_bits(const std::vector<T>& a, const std::vector<T>& b) {
     return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(T)) == 0;
+}
+
+// equal values, NaN where the other holds NaN (payloads aside)
+bool same_values(const std::vector<double>& a, const std::vector<double>& b) {
+    if (a.size() != b.size()) return false;
+    for (size_t i = 0; i < a.size(); ++i)
+        if (!(std::isnan(a[i]) && std::isnan(b[i])) &&
+            std::memcmp(&a[i], &b[i], sizeof(double)) != 0)
+            return false;
+    return true;
 }
 
 mkb::SystemBatchHost singlets(int V) {
@@ -161,6 +178,21 @@ int main() {
         expect(ok, "extra_merit added after the tuple sums");
     }
 
+    {  // transverse ray-error rows beside the OPD rows
+        ResidualSettings ts = settings;
+        ts.transverse_weight = 0.5;
+        const ResidualLayout tl(batch.topology(), ts);
+        const auto tp = tl.plan(batch);
+        const int64_t trows = tl.trace_rows();
+        expect(trows == rows + 2 * rays, "transverse rows: two per ray");
+        const cuda::TraceOutput t = engine.run(batch, cuda::TraceMode::Residuals, ts);
+        std::vector<double> want(static_cast<size_t>(V) * trows), wopd(V * rays);
+        std::vector<uint8_t> wst(V * rays);
+        expect(mko_port_residuals(&view, tp->get(), want.data(), wopd.data(), wst.data(), 1) == 0,
+               "oracle transverse residuals");
+        expect(same_bits(t.residuals.residuals, want), "transverse rows bit-identical");
+    }
+
     // Jacobians and normal equations
     const VariableSet vars(batch.topology(),
                            {{VariableType::Curvature, 1, -0.2, 0.2, 0.01},
@@ -274,6 +306,77 @@ int main() {
         expect(same_bits(g2.x, rx) && same_bits(g2.merit, rm) && same_bits(gs2, rs) &&
                    same_bits(g2.iterations, ri) && same_bits(g2.accepted, ra),
                "LM with trace-dependent rows bit-identical to the reference");
+
+        // the same three constraints evaluated on the device (no host phase in the cycle)
+        LmOptions po;
+        po.max_iterations = 8;
+        po.fail_weight_factor = 1.0;
+        for (int i = 0; i < 3; ++i) {
+            ParaxialConstraint c;
+            c.type = ctype[i];
+            c.mode = cmode[i];
+            c.weight = cw[i];
+            c.target = ct[i];
+            po.paraxial.items.push_back(c);
+        }
+        const cuda::LmResult g3 = cuda::optimize_lm_gpu(engine, vars, batch, x0, po, settings);
+        expect(mko_ref_optimize_lm(&view, plan->get(), &cv, x0.data(), V, 8, 1, 1, 4, rx.data(),
+                                   rm.data(), rs.data(), ri.data(), ra.data(), rh.data(), 3,
+                                   ctype, cmode, cw, ct, 0, nullptr, nullptr, nullptr,
+                                   nullptr) == 0,
+               "reference LM with constraints");
+        std::vector<int32_t> gs3(g3.status.begin(), g3.status.end());
+        expect(same_bits(g3.x, rx) && same_bits(g3.merit, rm) && same_bits(gs3, rs) &&
+                   same_bits(g3.iterations, ri) && same_bits(g3.accepted, ra),
+               "LM with device paraxial constraints bit-identical to the reference");
+    }
+    {  // FP32 prefilter against the reference's prefilter_cpu
+        cuda::PrefilterSettings ps;
+        ps.quadrature = settings;
+        ps.options.criteria.max_merit_factor = 3.0;
+        const cuda::PrefilterResult pr = engine.prefilter_variants(batch, ps);
+        mkb_prefilter_options o{0.5, INFINITY, 3.0, 0.15, 32.0, 0.01};
+        std::vector<double> m(V), opl(V), lo(V), hi(V);
+        std::vector<int64_t> fl(V), uo(V), uf(V);
+        std::vector<uint8_t> rej(V);
+        double rmerit = 0.0;
+        int32_t rv = 0, kept = 0;
+        expect(mko_ref_prefilter(&view, plan->get(), &o, nullptr, m.data(), opl.data(), fl.data(),
+                                 uo.data(), uf.data(), lo.data(), hi.data(), rej.data(), &rmerit,
+                                 &rv, &kept) == 0,
+               "reference prefilter");
+        expect(same_bits(pr.stats.merit, m) && same_bits(pr.stats.optical_length, opl) &&
+                   same_bits(pr.stats.failed, fl) && same_bits(pr.stats.uncertain_ok, uo) &&
+                   same_bits(pr.stats.uncertain_failed, uf),
+               "prefilter statistics bit-identical to the reference");
+        std::vector<uint8_t> got(pr.reject.begin(), pr.reject.end());
+        expect(same_bits(pr.merit_lower, lo) && same_bits(pr.merit_upper, hi) &&
+                   same_bits(got, rej) && pr.kept == kept && pr.reference_variant == rv,
+               "prefilter decision identical to the reference");
+    }
+    for (int reference = 0; reference < 3; ++reference) {  // EVAL against eval_cpu
+        cuda::EvalSettings es;
+        es.grid = 16;
+        es.reference = static_cast<cuda::EvalReference>(reference);
+        const cuda::EvalResult e = engine.evaluate(batch, es);
+        int64_t n = 0;
+        expect(mko_ref_eval(&view, plan->get(), 16, 0, reference, 1e-3, &n, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr) == 0 &&
+                   n == e.samples,
+               "reference EVAL grid");
+        const size_t T = static_cast<size_t>(V) * 3 * 3, N = static_cast<size_t>(n);
+        std::vector<double> opd(T * N), sx(T * N), sy(T * N), fr(T * 20), k(V * 3), zp(V);
+        std::vector<uint8_t> est(T * N), fs(T * 4);
+        expect(mko_ref_eval(&view, plan->get(), 16, 0, reference, 1e-3, &n, opd.data(),
+                            sx.data(), sy.data(), est.data(), fr.data(), fs.data(), k.data(),
+                            zp.data()) == 0,
+               "reference EVAL");
+        expect(same_values(e.opd, opd) && same_values(e.spot_x, sx) &&
+                   same_values(e.spot_y, sy) && same_bits(e.status, est) &&
+                   same_values(e.field_rays, fr) && same_bits(e.field_status, fs) &&
+                   same_values(e.reference_curvature, k) &&
+                   same_values(e.exit_pupil_position, zp),
+               "EVAL bit-identical to the reference");
     }
 #endif
 

@@ -1,6 +1,7 @@
 """The C++ host layer (mikroptim_b200/host): reference-shaped SystemBatchHost / ResidualLayout /
-VariableSet / TraceEngine / DeviceFdJacobian / DeviceAdjointJacobian / DeviceNormalEquations /
-optimize_lm_gpu over the C ABI.
+VariableSet / TraceEngine (RESIDUALS, MERIT, prefilter, EVAL) / DeviceFdJacobian /
+DeviceAdjointJacobian / DeviceNormalEquations / optimize_lm_gpu (with paraxial constraints on the
+device) over the C ABI.
 
 CPU: the layer builds, exports its classes, and the test driver (tests/cpp/test_host.cpp)
 compiles and links against it and the oracle. GPU: the driver traces, differentiates and
@@ -50,7 +51,9 @@ def test_host_layer_builds_and_exports_classes():
     for name in ("mkb::SystemBatchHost::validate_values", "mkb::ResidualLayout::plan",
                  "mkb::VariableSet::VariableSet", "mkb::cuda::TraceEngine::run",
                  "mkb::cuda::DeviceFdJacobian::compute", "mkb::cuda::DeviceAdjointJacobian::compute",
-                 "mkb::cuda::DeviceNormalEquations::compute", "mkb::cuda::optimize_lm_gpu"):
+                 "mkb::cuda::DeviceNormalEquations::compute", "mkb::cuda::optimize_lm_gpu",
+                 "mkb::cuda::TraceEngine::prefilter_variants", "mkb::cuda::TraceEngine::evaluate",
+                 "mkb::LmOptions::c_struct"):
         assert name in syms, name
 
 
