@@ -64,8 +64,8 @@ enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_
                                                        /* TraceStatus, surface_ops.hpp:24 */
 /* FP64: every operation separately rounded, sums in the reference's order -- bit-identical to
  * the reference CPU build. FP64_FMA: FP64 with a*b+c contracted to FMA and tree sums (faster,
- * equal within the reference's CPU/GPU tolerances). MIXED: FP32 bulk arithmetic with an FP64
- * sag root and OPL accumulation. */
+ * equal within the reference's CPU/GPU tolerances). MIXED: the trace (OPL, piston, merit and
+ * the ray states) as FP64_FMA, the adjoint reverse sweep in FP32 on those states. */
 enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2,
        MKB_PRECISION_DF64 = 3 };
 /* DF64 (RESIDUALS and MERIT only): the reference's reduced-precision trace type
