@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing", "precision",
-                             "singlet"])
+                             "singlet", "psf"])
     ap.add_argument("--variants", type=int, default=None,
                     help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
                          "otherwise)")
@@ -1485,6 +1485,159 @@ def run_precision(args, world, rank, local):
     }, (b, lay0)
 
 
+WORKLOAD_PSF = ("psf-{V}: EVAL of {V} objectives (config-2 shape: 15 surfaces, L=7, F=5) on a "
+                "{N} x {N} pupil grid, then the scalar PSF and MTF of every (variant, field, "
+                "wavelength) tuple with FFT size {M} (zero padding 4), NA {NA} given")
+
+
+def hbm_peak_gbs() -> tuple[float, str]:
+    """The measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json beside this
+    file), else the earlier measurement."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_psf(args, world, rank, local):
+    """Scalar PSF and MTF (PsfEngine): one step = the device chain for every tuple -- OPD maps
+    from EVAL's device outputs (mkb_psf_maps_device), then mkb_psf_device (row FFTs, column
+    FFTs with the intensity, the centred PSF and the projections, MTF cuts); EVAL itself runs
+    once before the timed steps. e2e: PsfEngine.compute on host pupils (maps up, PSF and MTF
+    down, finish_psf on the host) for a sample of the tuples."""
+    import torch
+    from mikroptim_b200 import _capi, engine, psf, workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    V = args.variants or 512
+    N, NA = 64, 0.25
+    M = psf.psf_fft_size(N, 4.0)
+    b, st, _, _ = workloads.objective(V, seed=20261203 + 6 + 1000 * rank)
+    db = engine.DeviceSystemBatch(b, dev)
+    settings = engine.EvalSettings(grid=N)
+    pts, _, _, out = engine.evaluate_device_tensors(db, b, settings)
+    res = engine.evaluate_device(db, b, settings)
+    col, row, full, half = psf.grid_cells(res)
+    T = V * b.fields * b.wavelengths
+    n = pts.shape[0]
+    params = []
+    for v in range(V):
+        for f in range(b.fields):
+            for l in range(b.wavelengths):
+                params.append(_capi.PsfPupilParams(b.wavelength_nm[l] * 1e-6,
+                                                   1.0 / (float(full) * full), 1, 1))
+    pa = (_capi.PsfPupilParams * T)(*params)
+    pd = torch.frombuffer(bytearray(pa), dtype=torch.uint8).to(dev)
+    cold = torch.from_numpy(col).to(dev)
+    rowd = torch.from_numpy(row).to(dev)
+    maps = torch.empty((T, N, N), dtype=torch.float64, device=dev)
+    P = torch.empty((T, M, M), dtype=torch.float64, device=dev)
+    mtf = torch.empty((T, 2, N + 1), dtype=torch.float64, device=dev)
+    nbytes = int(lib.mkb_psf_workspace_bytes(T, N, M))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        _capi.check(lib.mkb_psf_maps_device(T, N, n, int(half), C.c_void_p(out["opd"].data_ptr()),
+                                            C.c_void_p(out["st"].data_ptr()),
+                                            C.c_void_p(cold.data_ptr()),
+                                            C.c_void_p(rowd.data_ptr()),
+                                            C.c_void_p(maps.data_ptr()), None), "psf maps")
+        _capi.check(lib.mkb_psf_device(T, N, M, C.c_void_p(maps.data_ptr()),
+                                       C.c_void_p(pd.data_ptr()), C.c_void_p(P.data_ptr()),
+                                       C.c_void_p(mtf.data_ptr()), C.c_void_p(ws.data_ptr()),
+                                       nbytes, None), "psf")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.mkb_launch_count()
+    ts = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+    launches = lib.mkb_launch_count() - l0
+    ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ts) / args.steps, world, dev)
+    # bytes one step must move: the maps in (EVAL's OPD and status read, maps written and
+    # read), the N x M complex row spectra out and back in (the field does not fit on chip),
+    # the PSF and MTF out
+    per_tuple = (n * 9 + 2 * N * N * 8 + 2 * N * M * 16 + M * M * 8 + 2 * (N + 1) * 8)
+    peak, peak_src = hbm_peak_gbs()
+    achieved = T * per_tuple / (ms / 1e3) / 1e9
+    # e2e through PsfEngine.compute (host pupils in, host results out with finish_psf)
+    sample = min(T, 1024)
+    pupils = []
+    for t in range(sample):
+        v, rem = divmod(t, b.fields * b.wavelengths)
+        f, l = divmod(rem, b.wavelengths)
+        p = psf.make_psf_pupil(b, res, v, f, l, psf.PsfSettings(numerical_aperture=NA))
+        pupils.append(p)
+    eng = psf.PsfEngine(local)
+    eng.compute(pupils[:8], M)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.compute(pupils, M)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if rank != 0:
+        return None, None
+    cpu = None
+    try:
+        cpu = cpu_baseline_psf(pupils[:16], M)
+    except Exception as e:  # the baseline is reported, not required
+        cpu = {"value": None, "error": str(e)}
+    return {
+        "metric": "PSF tuples/s (scalar PSF + MTF cuts from EVAL OPD maps)",
+        "value": world * T / (ms / 1e3),
+        "unit": "PSF tuples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration-2 shapes)",
+        "config": {"workload": WORKLOAD_PSF.format(V=V, N=N, M=M, NA=NA), "tuples": T,
+                   "step": "maps from the device EVAL output + mkb_psf_device for every tuple",
+                   "l2": "flushed (256 MB write) before every timed step; a step writes about "
+                         "10 GB (inputs larger than L2)"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "bytes_model": "per tuple: EVAL OPD + status read (9 B/point), map write "
+                                    "+ read (2 N^2 x 8), row spectra write + read "
+                                    "(2 N M x 16), PSF write (M^2 x 8), MTF"},
+        "e2e": {"value": sample / e2e_s, "unit": "PSF tuples/s",
+                "h2d_bytes_per_step": sample * (N * N * 8 + 24),
+                "d2h_bytes_per_step": sample * (M * M * 8 + 2 * (N + 1) * 8),
+                "api": "psf.PsfEngine.compute(host pupils, M) -> PSF, MTF and figures",
+                "tuples": sample},
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }, None
+
+
+def cpu_baseline_psf(pupils, M: int):
+    """The reference's psf_cpu (own radix-2 FFT, one thread) on a sample of the tuples."""
+    import oracle.pyoracle as po
+    ref = po.reference()
+    t0 = time.perf_counter()
+    for p in pupils:
+        ref.psf_pupil(p.grid, M, p.opd, p.full_count, p.wavelength_nm, p.na_x, p.na_y,
+                      p.flip_x, p.flip_y)
+    dt = time.perf_counter() - t0
+    return {"value": len(pupils) / dt, "unit": "PSF tuples/s", "cores": 1,
+            "kind": "reference",
+            "sample": f"psf_cpu of {len(pupils)} tuples (FFT {M}), {dt:.1f} s"}
+
+
 def cpu_baseline_tolerancing(samples: int = 8):
     """The reference's CPU MERIT plus adjoint Jacobian (gradient 2 J^T r) of `samples` samples,
     all host threads (oracle/_ref)."""
@@ -1518,6 +1671,8 @@ def main():
                 out["cpu_baseline"] = {"value": None, "error": str(e)}
     elif args.workload == "precision":
         out, _ = run_precision(args, world, rank, local)
+    elif args.workload == "psf":
+        out, _ = run_psf(args, world, rank, local)
     elif args.workload == "tolerancing":
         out, _ = run_tolerancing(args, world, rank, local)
         if rank == 0 and world == 1:

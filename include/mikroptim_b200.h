@@ -648,6 +648,63 @@ int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double fie
                     double* field_rays, uint8_t* field_status, void* workspace,
                     size_t workspace_bytes, void* stream);
 
+/* ---- PSF and MTF from EVAL OPD maps ------------------------------------------------------
+ * Replaces PsfEngine::compute (src/cuda/psf.cu; include/mikroptim/cuda/psf.hpp:44) and the
+ * CPU reference psf_cpu (src/eval/psf.cpp:330): per tuple the pupil function
+ * P = exp(2 pi i OPD / lambda) of its N x N OPD map (NaN: no transmission) in the corner of an
+ * M x M field, the PSF I = |FFT2(P)|^2 / n_full^2 centred at (M/2, M/2) (mirrored along an axis
+ * whose sign is -1: a divergent wave), and the MTF cuts |OTF(k, 0)| / OTF(0) (sagittal) and
+ * |OTF(0, k)| / OTF(0) (tangential), k = 0 .. N, with OTF = FFT2^-1(I). The transform is this
+ * library's own shared-memory FFT (no cuFFT). Outputs are device arrays in the reference's
+ * layout: psf [T][M][M] (psf[j M + i] at ((i - M/2) dx, (j - M/2) dy)), mtf [T][2][N + 1]. */
+#define MKB_MAX_PSF_FFT 8192
+/* PsfPupilParams (include/mikroptim/eval/psf_ops.hpp:48): vacuum wavelength [mm],
+ * 1 / n_full^2, +1 (convergent) or -1 (divergent, mirrored) per axis. */
+typedef struct mkb_psf_pupil_params {
+    double lambda_mm;
+    double scale;
+    int32_t sign_x, sign_y;
+} mkb_psf_pupil_params;
+/* The figures of PsfResult (include/mikroptim/eval/psf.hpp:95) that finish_psf and
+ * prepare_psf_result fill. */
+typedef struct mkb_psf_metrics {
+    int64_t transmitted;
+    double energy, strehl_fft, strehl_origin, strehl, reference_x, reference_y;
+    double peak, peak_x, peak_y;
+    double dx, dy, airy_radius;
+} mkb_psf_metrics;
+/* psf_fft_size (src/eval/psf.cpp:168): the smallest power of two >= max(2N, ceil(padding N));
+ * MKB_ERR_ARGUMENT for N outside [1, MKB_MAX_EVAL_GRID], padding < 2 or M > MKB_MAX_PSF_FFT. */
+int mkb_psf_fft_size_host(int32_t grid, double padding, int32_t* fft_size);
+/* Workspace of mkb_psf_device: twiddles, the N x M row spectra and the projections of every
+ * tuple (0 for invalid sizes). */
+size_t mkb_psf_workspace_bytes(int32_t tuples, int32_t grid, int32_t fft_size);
+/* maps [T][N][N] and params [T] on the device; fft_size a power of two in [2N, 8192]. */
+int mkb_psf_device(int32_t tuples, int32_t grid, int32_t fft_size, const double* maps,
+                   const mkb_psf_pupil_params* params, double* psf, double* mtf, void* workspace,
+                   size_t workspace_bytes, void* stream);
+/* OPD maps from EVAL's device outputs without a host round trip (eval_opd_map with piston
+ * removal, src/eval/eval.cpp:512): maps [T][N][N] NaN, then the OPD of every ray with status Ok
+ * at (row[k], column[k]) of its grid point, also at column N - 1 - column[k] for a half pupil.
+ * opd, status [T][samples] as mkb_eval_device writes them; column, row [samples] device. */
+int mkb_psf_maps_device(int32_t tuples, int32_t grid, int64_t samples, int32_t half_pupil,
+                        const double* opd, const uint8_t* status, const int32_t* column,
+                        const int32_t* row, double* maps, void* stream);
+/* The NA of the pupil imaging of one tuple from its four EVAL field rays (make_psf_pupil,
+ * src/eval/psf.cpp:196): field_rays [4][5], field_status [4], n_image = index of the image
+ * space at the tuple's wavelength; numerical_aperture > 0 overrides the field rays. Sets the
+ * mirror flags of a divergent wave. MKB_ERR_ARGUMENT when the NA is undetermined. */
+int mkb_psf_aperture_host(const double* field_rays, const uint8_t* field_status, double n_image,
+                          double field_ray_offset, double numerical_aperture, double* na_x,
+                          double* na_y, int32_t* flip_x, int32_t* flip_y);
+/* finish_psf and the geometry of prepare_psf_result (src/eval/psf.cpp:262,290) on the host for
+ * one tuple: transmitted points, energy, Strehl from the FFT, direct Strehl before and after
+ * the least-squares tilt, the tilt's reference point, the peak; host arrays opd_map [N][N] and
+ * psf [M][M]. Bit-identical to the reference's finish_psf on the same PSF. */
+int mkb_psf_finish_host(int32_t grid, int32_t fft_size, const double* opd_map, int32_t full_count,
+                        double wavelength_nm, double na_x, double na_y, int32_t flip_x,
+                        int32_t flip_y, const double* psf, mkb_psf_metrics* out);
+
 /* ---- diagnostics ----------------------------------------------------------------------- */
 const char* mkb_last_error(void);
 const char* mkb_version(void);

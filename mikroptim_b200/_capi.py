@@ -68,6 +68,22 @@ class DeviceBatch(C.Structure):
     ]
 
 
+class PsfPupilParams(C.Structure):
+    """mkb_psf_pupil_params (PsfPupilParams, include/mikroptim/eval/psf_ops.hpp:48)."""
+
+    _fields_ = [("lambda_mm", C.c_double), ("scale", C.c_double),
+                ("sign_x", C.c_int32), ("sign_y", C.c_int32)]
+
+
+class PsfMetrics(C.Structure):
+    """mkb_psf_metrics: the figures of PsfResult (include/mikroptim/eval/psf.hpp:95)."""
+
+    _fields_ = [("transmitted", C.c_int64)] + [
+        (k, C.c_double) for k in ("energy", "strehl_fft", "strehl_origin", "strehl",
+                                  "reference_x", "reference_y", "peak", "peak_x", "peak_y",
+                                  "dx", "dy", "airy_radius")]
+
+
 class ResidualPlan(C.Structure):
     """mkb_residual_plan (ResidualSettings + ResidualLayout, batch_residuals.hpp:24,62)."""
 
@@ -213,6 +229,23 @@ def _declare(lib: C.CDLL) -> None:
     lib.mkb_eval_device.argtypes = [C.POINTER(DeviceBatch), c.c_int32, c.c_double, c.c_int32,
                                     c.c_void_p, c.c_int64, c.c_void_p] + [c.c_void_p] * 6 + \
         [c.c_void_p, c.c_size_t, c.c_void_p]
+    lib.mkb_psf_fft_size_host.restype = c.c_int
+    lib.mkb_psf_fft_size_host.argtypes = [c.c_int32, c.c_double, P_int32]
+    lib.mkb_psf_workspace_bytes.restype = c.c_size_t
+    lib.mkb_psf_workspace_bytes.argtypes = [c.c_int32, c.c_int32, c.c_int32]
+    lib.mkb_psf_device.restype = c.c_int
+    lib.mkb_psf_device.argtypes = [c.c_int32, c.c_int32, c.c_int32] + [c.c_void_p] * 5 + \
+        [c.c_size_t, c.c_void_p]
+    lib.mkb_psf_maps_device.restype = c.c_int
+    lib.mkb_psf_maps_device.argtypes = [c.c_int32, c.c_int32, c.c_int64, c.c_int32] + \
+        [c.c_void_p] * 6
+    lib.mkb_psf_aperture_host.restype = c.c_int
+    lib.mkb_psf_aperture_host.argtypes = [c.c_void_p, c.c_void_p, c.c_double, c.c_double,
+                                          c.c_double, P_double, P_double, P_int32, P_int32]
+    lib.mkb_psf_finish_host.restype = c.c_int
+    lib.mkb_psf_finish_host.argtypes = [c.c_int32, c.c_int32, c.c_void_p, c.c_int32, c.c_double,
+                                        c.c_double, c.c_double, c.c_int32, c.c_int32,
+                                        c.c_void_p, C.POINTER(PsfMetrics)]
     lib.mkb_paraxial_rows_device.restype = c.c_int
     lib.mkb_paraxial_rows_device.argtypes = [C.POINTER(DeviceBatch), C.POINTER(ResidualPlan),
                                              C.POINTER(Variables), C.POINTER(LmOptions),

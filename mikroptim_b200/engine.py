@@ -858,6 +858,9 @@ class EvalResult:
     status: np.ndarray
     field_rays: np.ndarray
     field_status: np.ndarray
+    grid_size: int = 0        # N
+    half_pupil: bool = False
+    field_ray_offset: float = 1e-3
 
     @property
     def samples(self) -> int:
@@ -879,6 +882,19 @@ def evaluate_device(dbatch: "DeviceSystemBatch", host: SystemBatchHost,
                     settings: EvalSettings | None = None, stream=None) -> EvalResult:
     """EVAL on an uploaded batch (TraceEngine::evaluate, the kernel EVAL): bit-identical to
     the reference's eval_cpu."""
+    settings = settings or EvalSettings()
+    pts, kappa, z_ap, out = evaluate_device_tensors(dbatch, host, settings, stream)
+    h = {k: v.cpu().numpy() for k, v in out.items()}
+    return EvalResult(host.variants, host.fields, host.wavelengths, pts, kappa.reshape(-1), z_ap,
+                      h["opd"], h["sx"], h["sy"], h["st"], h["fr"], h["fs"], settings.grid,
+                      settings.half_pupil, settings.field_ray_offset)
+
+
+def evaluate_device_tensors(dbatch: "DeviceSystemBatch", host: SystemBatchHost,
+                            settings: EvalSettings | None = None, stream=None):
+    """EVAL leaving its outputs on the device: grid points [n][3], kappa [V][F], exit-pupil
+    positions [V] (host) and the device tensors opd, sx, sy, st [V F L n], fr [V F L 4 5],
+    fs [V F L 4]."""
     lib = _capi.lib()
     settings = settings or EvalSettings()
     if settings.half_pupil and host.non_coaxial:
@@ -911,9 +927,7 @@ def evaluate_device(dbatch: "DeviceSystemBatch", host: SystemBatchHost,
                                ("opd", "sx", "sy", "st", "fr", "fs")],
                              C.c_void_p(ws.data_ptr()), ws.numel(), _stream_handle(stream))
     _capi.check(rc, "eval")
-    h = {k: v.cpu().numpy() for k, v in out.items()}
-    return EvalResult(V, F, L, pts, kappa.reshape(-1), z_ap, h["opd"], h["sx"], h["sy"], h["st"],
-                      h["fr"], h["fs"])
+    return pts, kappa, z_ap, out
 
 
 class _UnitWeights:

@@ -298,6 +298,75 @@ class Reference(_Oracle):
         self._check(rc, "eval")
         return out
 
+    PSF_METRICS = ("transmitted", "energy", "strehl_fft", "strehl_origin", "strehl",
+                   "reference_x", "reference_y", "peak", "peak_x", "peak_y", "dx", "dy",
+                   "airy_radius")
+
+    def psf(self, batch, layout, v: int = 0, grid: int = 32, half: bool = False,
+            reference: int = 0, delta: float = 1e-3, padding: float = 4.0,
+            na: float = 0.0) -> dict:
+        """eval_cpu, make_psf_pupils and psf_cpu (src/eval/psf.cpp:196,330) of variant v: the
+        pupils' maps, NA and flips, PSF [T][M][M], MTF [T][2][N + 1] and the figures."""
+        L = self.lib
+        L.mko_ref_psf.argtypes = [_PB, _PP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p] + \
+            [C.c_void_p] * 6
+        L.mko_ref_psf.restype = C.c_int
+        view, plan = batch.view(), layout.plan(batch)
+        lam = np.ascontiguousarray(batch.wavelength_nm, dtype=np.float64)
+        view.wavelength_nm = lam.ctypes.data_as(C.POINTER(C.c_double))
+        m, full = C.c_int(), C.c_int()
+        rc = L.mko_ref_psf(C.byref(view), C.byref(plan), grid, int(half), reference, delta, v,
+                           padding, na, C.addressof(m), C.addressof(full), *([None] * 6))
+        self._check(rc, "psf")
+        T, M = batch.fields * batch.wavelengths, m.value
+        out = dict(fft_size=M, full_count=full.value, maps=np.zeros((T, grid * grid)),
+                   na=np.zeros((T, 2)), flips=np.zeros((T, 2), np.int32),
+                   psf=np.zeros((T, M * M)), mtf=np.zeros((T, 2, grid + 1)),
+                   metrics=np.zeros((T, 13)))
+        rc = L.mko_ref_psf(C.byref(view), C.byref(plan), grid, int(half), reference, delta, v,
+                           padding, na, C.addressof(m), C.addressof(full),
+                           *[out[k].ctypes.data for k in ("maps", "na", "flips", "psf", "mtf",
+                                                          "metrics")])
+        self._check(rc, "psf")
+        return out
+
+    def psf_pupil(self, grid: int, fft_size: int, opd_map, full_count: int,
+                  wavelength_nm: float, na_x: float, na_y: float, flip_x: bool = False,
+                  flip_y: bool = False) -> dict:
+        """psf_cpu (src/eval/psf.cpp:330) of one given pupil map."""
+        L = self.lib
+        L.mko_ref_psf_pupil.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double,
+                                        C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
+        L.mko_ref_psf_pupil.restype = C.c_int
+        opd = np.ascontiguousarray(opd_map, dtype=np.float64)
+        out = dict(psf=np.zeros(fft_size * fft_size), mtf=np.zeros((2, grid + 1)),
+                   metrics=np.zeros(13))
+        rc = L.mko_ref_psf_pupil(grid, fft_size, opd.ctypes.data, full_count, wavelength_nm,
+                                 na_x, na_y, int(flip_x), int(flip_y), out["psf"].ctypes.data,
+                                 out["mtf"].ctypes.data, out["metrics"].ctypes.data)
+        self._check(rc, "psf_pupil")
+        return out
+
+    def psf_finish(self, grid: int, fft_size: int, opd_map, full_count: int,
+                   wavelength_nm: float, na_x: float, na_y: float, flip_x: bool, flip_y: bool,
+                   psf) -> np.ndarray:
+        """finish_psf (src/eval/psf.cpp:290) on a given PSF: the 13 figures."""
+        L = self.lib
+        L.mko_ref_psf_finish.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double,
+                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_void_p]
+        L.mko_ref_psf_finish.restype = C.c_int
+        opd = np.ascontiguousarray(opd_map, dtype=np.float64)
+        p = np.ascontiguousarray(psf, dtype=np.float64)
+        out = np.zeros(13)
+        rc = L.mko_ref_psf_finish(grid, fft_size, opd.ctypes.data, full_count, wavelength_nm,
+                                  na_x, na_y, int(flip_x), int(flip_y), p.ctypes.data,
+                                  out.ctypes.data)
+        self._check(rc, "psf_finish")
+        return out
+
     def prefilter(self, batch, layout, options, extra=None) -> dict:
         """prefilter_cpu (src/batch/batch_prefilter.cpp): raw per-variant results and the
         decision. `options` is a _capi.PrefilterOptions."""

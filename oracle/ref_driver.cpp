@@ -15,6 +15,8 @@
 //   prefilter_stats_cpu, prefilter_decide, prefilter_decide_exact, prefilter_rays_cpu
 //                          src/batch/batch_prefilter.cpp (FP32 multistart prefilter)
 //   eval_cpu               src/eval/eval.cpp:307 (EVAL on the dense pupil grid)
+//   make_psf_pupils, psf_cpu, finish_psf
+//                          src/eval/psf.cpp:196,330,290 (scalar PSF and MTF, own radix-2 FFT)
 // Only tests/, the golden-fixture script and bench.py's CPU legs load this library.
 
 #include "mikroptim_b200.h"
@@ -23,6 +25,7 @@
 #include "mikroptim/batch/batch_merit.hpp"
 #include "mikroptim/batch/batch_prefilter.hpp"
 #include "mikroptim/eval/eval.hpp"
+#include "mikroptim/eval/psf.hpp"
 #include "mikroptim/batch/batch_residuals.hpp"
 #include "mikroptim/batch/system_batch.hpp"
 #include "mikroptim/model/system.hpp"
@@ -76,7 +79,8 @@ mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_p
     b.reference_wavelength_nm = v.reference_wavelength_nm;
     for (int l = 0; l < L; ++l) {
         b.wavelength_weight(l) = v.wavelength_weight[l];
-        b.wavelength_nm(l) = 500.0 + l; // not read by the trace (index is given directly)
+        // the trace reads the indices directly; the wavelengths matter to EVAL's PSF only
+        b.wavelength_nm(l) = v.wavelength_nm != nullptr ? v.wavelength_nm[l] : 500.0 + l;
     }
     for (int f = 0; f < F; ++f) {
         b.field_weight(f) = v.field_weight[f];
@@ -454,6 +458,109 @@ int mko_ref_eval(const mkb_batch_view* view, const mkb_residual_plan* plan, int 
         std::copy(r.field_status.begin(), r.field_status.end(), field_status);
         std::copy(r.reference_curvature.begin(), r.reference_curvature.end(), kappa);
         std::copy(r.exit_pupil_position.begin(), r.exit_pupil_position.end(), exit_pupil);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Scalar PSF of variant v: EVAL (grid, half, reference, delta) then make_psf_pupils and
+// psf_cpu with (padding, na). Per tuple t = f L + l: maps [T][N][N], na [T][2], flips [T][2],
+// psf [T][M][M], mtf [T][2][N + 1], metrics [T][13] in mkb_psf_metrics order (transmitted as
+// a double); *fft_size and *full_count out. With psf == nullptr only the sizes are returned.
+int mko_ref_psf(const mkb_batch_view* view, const mkb_residual_plan* plan, int grid, int half,
+                int reference, double delta, int v, double padding, double na, int* fft_size,
+                int* full_count, double* maps, double* na_out, int* flips, double* psf,
+                double* mtf, double* metrics) {
+    try {
+        const mko::SystemBatchHost b = batch_of_view(*view, *plan);
+        mko::EvalSettings es;
+        es.grid = grid;
+        es.half_pupil = half != 0;
+        es.reference = static_cast<mko::EvalReference>(reference);
+        es.field_ray_offset = delta;
+        mko::PsfSettings ps;
+        ps.padding = padding;
+        ps.numerical_aperture = na;
+        *fft_size = mko::psf_fft_size(grid, padding);
+        *full_count = mko::make_eval_grid(grid, half != 0).full_count;
+        if (psf == nullptr) return 0;
+        const mko::EvalResult r = mko::eval_cpu(b, es);
+        const std::vector<mko::PsfPupil> pupils = mko::make_psf_pupils(b, r, v, ps);
+        const size_t n2 = size_t(grid) * grid, m2 = size_t(*fft_size) * (*fft_size);
+        for (size_t t = 0; t < pupils.size(); ++t) {
+            const mko::PsfPupil& p = pupils[t];
+            const mko::PsfResult q = mko::psf_cpu(p, *fft_size);
+            std::copy(p.opd.begin(), p.opd.end(), maps + t * n2);
+            na_out[2 * t] = p.na_x;
+            na_out[2 * t + 1] = p.na_y;
+            flips[2 * t] = p.flip_x ? 1 : 0;
+            flips[2 * t + 1] = p.flip_y ? 1 : 0;
+            std::copy(q.psf.begin(), q.psf.end(), psf + t * m2);
+            const size_t per = size_t(grid) + 1;
+            std::copy(q.mtf_sagittal.begin(), q.mtf_sagittal.end(), mtf + t * 2 * per);
+            std::copy(q.mtf_tangential.begin(), q.mtf_tangential.end(), mtf + t * 2 * per + per);
+            const double m[13] = {static_cast<double>(q.transmitted), q.energy, q.strehl_fft,
+                                  q.strehl_origin, q.strehl, q.reference_x, q.reference_y,
+                                  q.peak, q.peak_x, q.peak_y, q.dx, q.dy, q.airy_radius};
+            std::copy(m, m + 13, metrics + t * 13);
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// psf_cpu of one given pupil (map [N][N], NaN: no transmission): psf [M][M], mtf [2][N + 1],
+// metrics [13].
+int mko_ref_psf_pupil(int grid, int fft_size, const double* map, int full_count,
+                      double wavelength_nm, double na_x, double na_y, int flip_x, int flip_y,
+                      double* psf, double* mtf, double* metrics) {
+    try {
+        mko::PsfPupil p;
+        p.grid = grid;
+        p.full_count = full_count;
+        p.wavelength_nm = wavelength_nm;
+        p.na_x = na_x;
+        p.na_y = na_y;
+        p.flip_x = flip_x != 0;
+        p.flip_y = flip_y != 0;
+        p.opd.assign(map, map + size_t(grid) * grid);
+        const mko::PsfResult q = mko::psf_cpu(p, fft_size);
+        std::copy(q.psf.begin(), q.psf.end(), psf);
+        std::copy(q.mtf_sagittal.begin(), q.mtf_sagittal.end(), mtf);
+        std::copy(q.mtf_tangential.begin(), q.mtf_tangential.end(), mtf + grid + 1);
+        const double m[13] = {static_cast<double>(q.transmitted), q.energy, q.strehl_fft,
+                              q.strehl_origin, q.strehl, q.reference_x, q.reference_y, q.peak,
+                              q.peak_x, q.peak_y, q.dx, q.dy, q.airy_radius};
+        std::copy(m, m + 13, metrics);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// finish_psf (and prepare_psf_result's geometry) on a given PSF [M][M] of a pupil map.
+int mko_ref_psf_finish(int grid, int fft_size, const double* map, int full_count,
+                       double wavelength_nm, double na_x, double na_y, int flip_x, int flip_y,
+                       const double* psf, double* metrics) {
+    try {
+        mko::PsfPupil p;
+        p.grid = grid;
+        p.full_count = full_count;
+        p.wavelength_nm = wavelength_nm;
+        p.na_x = na_x;
+        p.na_y = na_y;
+        p.flip_x = flip_x != 0;
+        p.flip_y = flip_y != 0;
+        p.opd.assign(map, map + size_t(grid) * grid);
+        mko::PsfResult q = mko::prepare_psf_result(p, fft_size);
+        std::copy(psf, psf + size_t(fft_size) * fft_size, q.psf.begin());
+        mko::finish_psf(q, p);
+        const double m[13] = {static_cast<double>(q.transmitted), q.energy, q.strehl_fft,
+                              q.strehl_origin, q.strehl, q.reference_x, q.reference_y, q.peak,
+                              q.peak_x, q.peak_y, q.dx, q.dy, q.airy_radius};
+        std::copy(m, m + 13, metrics);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
