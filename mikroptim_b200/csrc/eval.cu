@@ -7,7 +7,7 @@
 //                       OPL offset
 //   eval_grid_kernel    grid-stride over (tuple, point): status, spot, OPL - offset (kept in
 //                       the OPD output until the piston is known)
-//   eval_piston_kernel  one thread per tuple: weight and weighted OPL sums in ascending point
+//   eval_piston_kernel  one warp per tuple: weight and weighted OPL sums in ascending point
 //                       order (opd_statistics, include/mikroptim/merit/opd.hpp:43)
 //   eval_opd_kernel     grid-stride: OPD = (OPL - offset) - piston, NaN for failed rays
 // Arithmetic in Exact64 in the reference's order: bit-identical to eval_cpu
@@ -184,21 +184,41 @@ __global__ void eval_grid_kernel(const __grid_constant__ EvalParams e,
     }
 }
 
-__global__ void eval_piston_kernel(int64_t tuples, int64_t n, const double* __restrict__ grid,
-                                   const double* __restrict__ opl,
-                                   const uint8_t* __restrict__ status,
-                                   double* __restrict__ piston) {
-    const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (t >= tuples) return;
+// One warp per tuple: the lanes load 32 consecutive points at a time (coalesced) and form the
+// terms w and w * OPL (each one rounded product, as in the sequential loop); lane 0 then adds
+// them in ascending point order from shared memory, so the two sums keep the reference's
+// order and bits while the loads of the next 32 points are already in flight.
+constexpr int kPistonWarps = 8;
+
+__global__ void __launch_bounds__(32 * kPistonWarps)
+eval_piston_kernel(int64_t tuples, int64_t n, const double* __restrict__ grid,
+                   const double* __restrict__ opl, const uint8_t* __restrict__ status,
+                   double* __restrict__ piston) {
+    __shared__ double ws[kPistonWarps][32], ts[kPistonWarps][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t t = blockIdx.x * int64_t(kPistonWarps) + warp;
+    if (t >= tuples) return;  // warp-uniform
     double wsum = 0.0, sum = 0.0;
-    for (int64_t k = 0; k < n; ++k) {
-        if (status[t * n + k] != kOk) continue;  // hard failure: in the piston = Ok
-        const double w = grid[3 * k + 2];
-        wsum = __dadd_rn(wsum, w);
-        sum = __dadd_rn(sum, __dmul_rn(w, opl[t * n + k]));
+    for (int64_t k0 = 0; k0 < n; k0 += 32) {
+        const int64_t k = k0 + lane;
+        const bool ok = k < n && status[t * n + k] == kOk;  // hard failure: in piston = Ok
+        const double w = ok ? grid[3 * k + 2] : 0.0;
+        ws[warp][lane] = w;
+        ts[warp][lane] = ok ? __dmul_rn(w, opl[t * n + k]) : 0.0;
+        const unsigned mask = __ballot_sync(0xffffffffu, ok);
+        __syncwarp();
+        if (lane == 0) {
+            for (int j = 0; j < 32; ++j) {
+                if (!((mask >> j) & 1u)) continue;
+                wsum = __dadd_rn(wsum, ws[warp][j]);
+                sum = __dadd_rn(sum, ts[warp][j]);
+            }
+        }
+        __syncwarp();
     }
     // piston, and NaN as the mark of a tuple without a valid ray
-    piston[t] = wsum > 0.0 ? __ddiv_rn(sum, wsum) : __longlong_as_double(0x7ff8000000000000ll);
+    if (lane == 0)
+        piston[t] = wsum > 0.0 ? __ddiv_rn(sum, wsum) : __longlong_as_double(0x7ff8000000000000ll);
 }
 
 __global__ void eval_opd_kernel(int64_t total, int64_t n, const double* __restrict__ piston,
@@ -407,8 +427,8 @@ int mkb_eval_device(const mkb_device_batch* batch, int32_t reference, double fie
     if (precision == MKB_PRECISION_FP64) by_feat(NumTag<Exact64>{});
     else by_feat(NumTag<double>{});
     count_launch(2);
-    eval_piston_kernel<<<static_cast<unsigned>((tuples + 127) / 128), 128, 0, stream>>>(
-        tuples, n, grid, opd, status, piston);
+    eval_piston_kernel<<<static_cast<unsigned>((tuples + kPistonWarps - 1) / kPistonWarps),
+                         32 * kPistonWarps, 0, stream>>>(tuples, n, grid, opd, status, piston);
     eval_opd_kernel<<<148 * 16, 256, 0, stream>>>(tuples * n, n, piston, status, opd);
     count_launch(2);
     return cuda_status(cudaGetLastError(), "eval launch");

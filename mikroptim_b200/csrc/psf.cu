@@ -71,8 +71,11 @@ __device__ __forceinline__ int bit_reverse(int i, int log_m) {
 // radix-2 stages run in passes of up to four: a thread loads the 2^NS elements one butterfly
 // group of the pass touches into registers, runs the NS stages there and stores them back, so
 // shared memory is read and written once per pass instead of once per stage.
-template <int NS>
-__device__ __forceinline__ void fft_pass(double2* a, int M, int count, int s, const double2* tw) {
+// kFirst: the pass reads its inputs through load(c, i) (the value at bit-reversed position i
+// of sequence c) instead of from shared memory.
+template <int NS, bool kFirst, class Load>
+__device__ __forceinline__ void fft_pass(double2* a, int M, int count, int s, const double2* tw,
+                                         const Load& load) {
     constexpr int R = 1 << NS;
     const int total = (M >> NS) * count;
     const int h0 = 1 << s;
@@ -82,7 +85,8 @@ __device__ __forceinline__ void fft_pass(double2* a, int M, int count, int s, co
         const int base = ((g >> s) << (s + NS)) + pos;
         double2 x[R];
 #pragma unroll
-        for (int k = 0; k < R; ++k) x[k] = a[(base + k * h0) * count + c];
+        for (int k = 0; k < R; ++k)
+            x[k] = kFirst ? load(c, base + k * h0) : a[(base + k * h0) * count + c];
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
             const int hj = 1 << j;
@@ -104,15 +108,34 @@ __device__ __forceinline__ void fft_pass(double2* a, int M, int count, int s, co
     __syncthreads();
 }
 
-__device__ void fft_shared(double2* a, int M, int log_m, int count, const double2* tw) {
-    for (int s = 0; s < log_m; s += 4) {
+struct FromShared {
+    __device__ double2 operator()(int, int) const { return make_double2(0.0, 0.0); }
+};
+
+// The whole transform; the first pass takes its inputs from load (kFirst) or shared memory.
+template <bool kFirst, class Load>
+__device__ void fft_shared(double2* a, int M, int log_m, int count, const double2* tw,
+                           const Load& load) {
+    switch (log_m < 4 ? log_m : 4) {
+    case 1: fft_pass<1, kFirst>(a, M, count, 0, tw, load); break;
+    case 2: fft_pass<2, kFirst>(a, M, count, 0, tw, load); break;
+    case 3: fft_pass<3, kFirst>(a, M, count, 0, tw, load); break;
+    default: fft_pass<4, kFirst>(a, M, count, 0, tw, load); break;
+    }
+    const FromShared none;
+    for (int s = 4; s < log_m; s += 4) {
         switch (log_m - s < 4 ? log_m - s : 4) {
-        case 1: fft_pass<1>(a, M, count, s, tw); break;
-        case 2: fft_pass<2>(a, M, count, s, tw); break;
-        case 3: fft_pass<3>(a, M, count, s, tw); break;
-        default: fft_pass<4>(a, M, count, s, tw); break;
+        case 1: fft_pass<1, false>(a, M, count, s, tw, none); break;
+        case 2: fft_pass<2, false>(a, M, count, s, tw, none); break;
+        case 3: fft_pass<3, false>(a, M, count, s, tw, none); break;
+        default: fft_pass<4, false>(a, M, count, s, tw, none); break;
         }
     }
+}
+
+// the twiddle table into shared memory (read by every butterfly)
+__device__ __forceinline__ void stage_twiddles(double2* tws, const double2* tw, int M) {
+    for (int k = threadIdx.x; k < (M >> 1); k += blockDim.x) tws[k] = tw[k];
 }
 
 __global__ void psf_twiddle_kernel(double2* tw, int M) {
@@ -123,22 +146,25 @@ __global__ void psf_twiddle_kernel(double2* tw, int M) {
     tw[k] = make_double2(c, -s);
 }
 
-// The pupil function of rows [r0, r0 + R) of tuple t, transformed along x. Row r's element i
-// sits at sm[i * R + r]; the spectra go out column-major per tuple, spec[t][q][j], so that the
-// column pass reads each column's N values contiguously.
+// The pupil function of rows [r0, r0 + R) of tuple t, transformed along x (R = kRows, rows past
+// N are zero and not written). Row r's element i sits at sm[i * R + r]; the spectra go out
+// column-major per tuple, spec[t][q][j], so that the column pass reads each column's N values
+// contiguously.
+template <int kRows>
 __global__ void __launch_bounds__(kPsfThreads, 2) psf_rows_kernel(const PsfArgs a) {
     extern __shared__ double2 sm[];
-    const int per_t = (a.N + a.rows_per_cta - 1) / a.rows_per_cta;
+    const int per_t = (a.N + kRows - 1) / kRows;
     const int t = blockIdx.x / per_t;
-    const int r0 = (blockIdx.x - t * per_t) * a.rows_per_cta;
-    const int R = min(a.rows_per_cta, a.N - r0);
-    const int M = a.M, N = a.N;
+    const int r0 = (blockIdx.x - t * per_t) * kRows;
+    const int M = a.M, N = a.N, lm = a.log_m;
     const double lambda = a.params[t].lambda_mm;
     const double* map = a.maps + (static_cast<int64_t>(t) * N + r0) * N;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, i = e - r * M;
+    double2* tws = sm + kRows * M;
+    stage_twiddles(tws, a.tw, M);
+    for (int e = threadIdx.x; e < kRows * M; e += blockDim.x) {
+        const int r = e >> lm, i = e & (M - 1);
         double2 v = make_double2(0.0, 0.0);
-        if (i < N) {
+        if (i < N && r0 + r < N) {
             const double opd = map[static_cast<int64_t>(r) * N + i];
             if (opd == opd) {  // NaN: outside the pupil or a failed ray
                 const double phase = 6.283185307179586 * (opd / lambda);
@@ -147,76 +173,76 @@ __global__ void __launch_bounds__(kPsfThreads, 2) psf_rows_kernel(const PsfArgs 
                 v = make_double2(c, s);
             }
         }
-        sm[bit_reverse(i, a.log_m) * R + r] = v;
+        sm[bit_reverse(i, lm) * kRows + r] = v;
     }
     __syncthreads();
-    fft_shared(sm, M, a.log_m, R, a.tw);
+    fft_shared<false>(sm, M, lm, kRows, tws, FromShared{});
+    const int R = min(kRows, N - r0);
     double2* out = a.spec + static_cast<int64_t>(t) * M * N + r0;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int q = e / R, r = e - q * R;
-        out[static_cast<int64_t>(q) * N + r] = sm[e];
+    for (int e = threadIdx.x; e < kRows * M; e += blockDim.x) {
+        const int q = e / kRows, r = e - q * kRows;
+        if (r < R) out[static_cast<int64_t>(q) * N + r] = sm[e];
     }
 }
 
-// Columns [q0, q0 + C) of tuple t: transform along y, intensity, centred PSF, projections.
+// Columns [q0, q0 + C) of tuple t (C = kCols): transform along y, then one pass over the
+// result for the intensity, the centred PSF and the two projections.
+template <int kCols>
 __global__ void __launch_bounds__(kPsfThreads, 2) psf_cols_kernel(const PsfArgs a) {
+    constexpr int C = kCols;
     extern __shared__ double2 sm[];
-    __shared__ double wsum[kPsfThreads / 32][16];
-    const int C = a.cols_per_cta, M = a.M, N = a.N;
+    __shared__ double wsum[kPsfThreads / 32][C];
+    const int M = a.M, N = a.N, lm = a.log_m;
     const int t = blockIdx.x / a.tiles;
     const int tile = blockIdx.x - t * a.tiles;
     const int q0 = tile * C;
     const double2* in = a.spec + (static_cast<int64_t>(t) * M + q0) * N;
-    // the N non-zero entries of each column (contiguous in the spectra), bit-reversed ...
-    for (int e = threadIdx.x; e < C * N; e += blockDim.x) {
-        const int c = e / N, j = e - c * N;
-        sm[bit_reverse(j, a.log_m) * C + c] = in[e];
-    }
-    // ... and zeros at the positions of rows N .. M - 1
-    for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
-        const int i = e / C;
-        if (bit_reverse(i, a.log_m) >= N) sm[e] = make_double2(0.0, 0.0);
-    }
+    double2* tws = sm + C * M;
+    stage_twiddles(tws, a.tw, M);
     __syncthreads();
-    fft_shared(sm, M, a.log_m, C, a.tw);
+    // the first pass reads the column's entries straight from the spectra (contiguous per
+    // column, cached in L1 across the pass): position i holds row brev(i), zero past N
+    auto load = [&](int c, int i) {
+        const int j = bit_reverse(i, lm);
+        return j < N ? in[c * N + j] : make_double2(0.0, 0.0);
+    };
+    fft_shared<true>(sm, M, lm, C, tws, load);
     const mkb_psf_pupil_params p = a.params[t];
     double* psf = a.psf + static_cast<int64_t>(t) * M * M;
-    // intensity in place (the real part), the PSF at its centred, possibly mirrored position:
-    // output index o = (M / 2 + sign q) mod M of FFT index q (psf_output_index, psf_ops.hpp)
-    for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
-        const int qj = e / C, c = e - qj * C, qi = q0 + c;
-        const double2 u = sm[e];
-        const double I = (u.x * u.x + u.y * u.y) * p.scale;
-        sm[e].x = I;
-        const int oi = ((M >> 1) + p.sign_x * qi) & (M - 1);
-        const int oj = ((M >> 1) + p.sign_y * qj) & (M - 1);
-        psf[static_cast<int64_t>(oj) * M + oi] = I;
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // column sums: thread (g, c) adds rows g, g + G, ... of column c (G = 256 / C); lanes of a
-    // warp with the same column, then the warps in ascending order -- a fixed order
-    {
-        const int c = threadIdx.x % C, g = threadIdx.x / C, G = kPsfThreads / C;
-        double s = 0.0;
-        for (int qj = g; qj < M; qj += G) s += sm[qj * C + c].x;
-        for (int o = 16; o >= C; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane < C) wsum[warp][lane] = s;
-        __syncthreads();
-        if (threadIdx.x < C) {
-            double tot = 0.0;
-            for (int w = 0; w < kPsfThreads / 32; ++w) tot += wsum[w][threadIdx.x];
-            a.colsum[static_cast<int64_t>(t) * M + q0 + threadIdx.x] = tot;
-        }
-    }
-    // row partials: C lanes per row, a fixed xor tree over the tile's columns
     double* part = a.rowpart + (static_cast<int64_t>(t) * a.tiles + tile) * M;
-    const int total = M * C;  // a multiple of C: a row's lanes are never split
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // e = (qj, c), c fastest: a thread keeps one column (256 is a multiple of C) and adds its
+    // rows in ascending order; the C lanes of a row add the row in a fixed xor tree. The PSF
+    // element goes to its centred, possibly mirrored position: output index
+    // o = (M / 2 + sign q) mod M of FFT index q (psf_output_index, psf_ops.hpp).
+    const int total = M * C;
+    double col_acc = 0.0;
     for (int e0 = threadIdx.x - lane; e0 < total; e0 += blockDim.x) {  // warp-uniform bound
         const int e = e0 + lane;
-        double s = e < total ? sm[e].x : 0.0;
-        for (int o = C >> 1; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (e < total && e % C == 0) part[e / C] = s;
+        double I = 0.0;
+        if (e < total) {
+            const int qj = e / C, qi = q0 + (e - qj * C);
+            const double2 u = sm[e];
+            I = (u.x * u.x + u.y * u.y) * p.scale;
+            col_acc += I;
+            const int oi = ((M >> 1) + p.sign_x * qi) & (M - 1);
+            const int oj = ((M >> 1) + p.sign_y * qj) & (M - 1);
+            psf[static_cast<int64_t>(oj) * M + oi] = I;
+        }
+        double r = I;
+#pragma unroll
+        for (int o = C >> 1; o >= 1; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        if (e < total && e % C == 0) part[e / C] = r;
+    }
+    // column sums: the lanes of a warp with the same column, then the warps in ascending order
+#pragma unroll
+    for (int o = 16; o >= C; o >>= 1) col_acc += __shfl_xor_sync(0xffffffffu, col_acc, o);
+    if (lane < C) wsum[warp][lane] = col_acc;
+    __syncthreads();
+    if (threadIdx.x < C) {
+        double tot = 0.0;
+        for (int w = 0; w < kPsfThreads / 32; ++w) tot += wsum[w][threadIdx.x];
+        a.colsum[static_cast<int64_t>(t) * M + q0 + threadIdx.x] = tot;
     }
 }
 
@@ -466,7 +492,7 @@ int mkb_psf_device(int32_t tuples, int32_t grid, int32_t fft_size, const double*
     a.N = grid;
     a.M = fft_size;
     a.log_m = log_m;
-    a.rows_per_cta = R;
+    a.rows_per_cta = C;
     a.cols_per_cta = C;
     a.tiles = fft_size / C;
     a.maps = maps;
@@ -481,24 +507,28 @@ int mkb_psf_device(int32_t tuples, int32_t grid, int32_t fft_size, const double*
     psf_twiddle_kernel<<<(half + 255) / 256, 256, 0, stream>>>(
         reinterpret_cast<double2*>(ws + off[0]), fft_size);
     count_launch();
-    const size_t smem_rows = sizeof(double2) * static_cast<size_t>(R) * fft_size;
-    const size_t smem_cols = sizeof(double2) * static_cast<size_t>(C) * fft_size;
+    // data [C][M] and the twiddles [M / 2]
+    const size_t smem_rows = sizeof(double2) * (static_cast<size_t>(C) * fft_size + fft_size / 2);
+    const size_t smem_cols = smem_rows;
     const size_t smem_mtf = sizeof(double) * 2 * static_cast<size_t>(fft_size);
-    cudaError_t err = cudaFuncSetAttribute(psf_rows_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+    using Fn = void (*)(PsfArgs);
+    Fn rows = C == 16 ? psf_rows_kernel<16> : C == 8 ? psf_rows_kernel<8>
+            : C == 4 ? psf_rows_kernel<4> : C == 2 ? psf_rows_kernel<2> : psf_rows_kernel<1>;
+    Fn cols = C == 16 ? psf_cols_kernel<16> : C == 8 ? psf_cols_kernel<8>
+            : C == 4 ? psf_cols_kernel<4> : C == 2 ? psf_cols_kernel<2> : psf_cols_kernel<1>;
+    cudaError_t err = cudaFuncSetAttribute(rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem_rows));
     if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(psf_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        err = cudaFuncSetAttribute(cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem_cols));
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(psf_mtf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem_mtf));
     if (err != cudaSuccess) return cuda_status(err, "psf: shared memory attribute");
-    const int per_t = (grid + R - 1) / R;
-    psf_rows_kernel<<<static_cast<unsigned>(tuples) * per_t, kPsfThreads, smem_rows, stream>>>(a);
+    const int per_t = (grid + C - 1) / C;
+    rows<<<static_cast<unsigned>(tuples) * per_t, kPsfThreads, smem_rows, stream>>>(a);
     count_launch();
-    psf_cols_kernel<<<static_cast<unsigned>(tuples) * a.tiles, kPsfThreads, smem_cols, stream>>>(
-        a);
+    cols<<<static_cast<unsigned>(tuples) * a.tiles, kPsfThreads, smem_cols, stream>>>(a);
     count_launch();
     psf_mtf_kernel<<<static_cast<unsigned>(tuples), kPsfThreads, smem_mtf, stream>>>(a);
     count_launch();

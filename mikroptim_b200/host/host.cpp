@@ -1426,6 +1426,9 @@ EvalResult TraceEngine::evaluate(const SystemBatchHost& batch, const EvalSetting
     r.variants = batch.variants();
     r.fields = batch.fields();
     r.wavelengths = batch.wavelengths();
+    r.grid_size = settings.grid;
+    r.half_pupil = settings.half_pupil;
+    r.field_ray_offset = settings.field_ray_offset;
     int64_t n = 0;
     check(mkb_eval_grid_host(settings.grid, settings.half_pupil ? 1 : 0, nullptr, &n),
           "eval grid");
@@ -1546,6 +1549,235 @@ LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
     for (size_t i = 0; i < R; ++i) std::copy(hist[i].begin(), hist[i].end(), r.history.begin() + i * width);
     r.history_width = static_cast<int>(width);
     return r;
+}
+
+
+// ---- scalar PSF and MTF ---------------------------------------------------------------------
+
+int psf_fft_size(int grid, double padding) {
+    int32_t m = 0;
+    check(mkb_psf_fft_size_host(grid, padding, &m), "psf_fft_size");
+    return m;
+}
+
+namespace {
+
+// column i and row j of grid point k (x = (2i + 1 - N) / N) and the points of the full pupil
+void grid_cells(const EvalResult& r, std::vector<int32_t>& col, std::vector<int32_t>& row,
+                int& full) {
+    const int n = r.grid_size;
+    if (n < 1) throw std::invalid_argument("PSF: the EVAL result carries no grid edge");
+    col.resize(static_cast<size_t>(r.samples));
+    row.resize(static_cast<size_t>(r.samples));
+    for (int64_t k = 0; k < r.samples; ++k) {
+        col[static_cast<size_t>(k)] =
+            static_cast<int32_t>(std::lround((r.grid[3 * k] * n + n - 1) / 2.0));
+        row[static_cast<size_t>(k)] =
+            static_cast<int32_t>(std::lround((r.grid[3 * k + 1] * n + n - 1) / 2.0));
+    }
+    full = 0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int64_t a = 2 * i + 1 - n, b = 2 * j + 1 - n;
+            full += a * a + b * b <= int64_t(n) * n ? 1 : 0;
+        }
+}
+
+}  // namespace
+
+std::vector<double> eval_opd_map(const EvalResult& r, int v, int f, int l) {
+    if (v < 0 || v >= r.variants || f < 0 || f >= r.fields || l < 0 || l >= r.wavelengths)
+        throw std::out_of_range("EVAL: tuple does not exist");
+    std::vector<int32_t> col, row;
+    int full = 0;
+    grid_cells(r, col, row, full);
+    const size_t n = static_cast<size_t>(r.grid_size);
+    std::vector<double> map(n * n, std::numeric_limits<double>::quiet_NaN());
+    const size_t t = (static_cast<size_t>(v) * r.fields + f) * r.wavelengths + l;
+    const size_t k0 = t * static_cast<size_t>(r.samples);
+    for (int64_t k = 0; k < r.samples; ++k) {
+        if (r.status[k0 + k] != MKB_STATUS_OK) continue;
+        const size_t c = static_cast<size_t>(col[k]), j = static_cast<size_t>(row[k]);
+        map[j * n + c] = r.opd[k0 + k];
+        if (r.half_pupil) map[j * n + (n - 1 - c)] = r.opd[k0 + k];
+    }
+    return map;
+}
+
+PsfPupil make_psf_pupil(const SystemBatchHost& batch, const EvalResult& r, int v, int f, int l,
+                        const PsfSettings& settings) {
+    if (!(settings.padding >= 2.0) || !std::isfinite(settings.padding))
+        throw std::invalid_argument("PSF: zero-padding factor must be >= 2");
+    if (batch.variants() != r.variants || batch.fields() != r.fields ||
+        batch.wavelengths() != r.wavelengths)
+        throw std::invalid_argument("PSF: batch does not match the EVAL result");
+    PsfPupil p;
+    p.field = f;
+    p.wavelength = l;
+    p.grid = r.grid_size;
+    p.opd = eval_opd_map(r, v, f, l);
+    std::vector<int32_t> col, row;
+    grid_cells(r, col, row, p.full_count);
+    p.wavelength_nm = batch.wavelength_nm.at(static_cast<size_t>(l));
+    const mkb_batch_view view = batch.view();
+    const int S = batch.surfaces(), L = batch.wavelengths();
+    const double n_image = view.index[(static_cast<size_t>(v) * S + S - 1) * L + l];
+    const size_t t = (static_cast<size_t>(v) * r.fields + f) * r.wavelengths + l;
+    int32_t fx = 0, fy = 0;
+    check(mkb_psf_aperture_host(r.field_rays.data() + 20 * t, r.field_status.data() + 4 * t,
+                                      n_image, r.field_ray_offset, settings.numerical_aperture,
+                                      &p.na_x, &p.na_y, &fx, &fy),
+                "psf aperture");
+    p.flip_x = fx != 0;
+    p.flip_y = fy != 0;
+    return p;
+}
+
+std::vector<PsfPupil> make_psf_pupils(const SystemBatchHost& batch, const EvalResult& r, int v,
+                                      const PsfSettings& settings) {
+    std::vector<PsfPupil> out;
+    for (int f = 0; f < r.fields; ++f)
+        for (int l = 0; l < r.wavelengths; ++l)
+            out.push_back(make_psf_pupil(batch, r, v, f, l, settings));
+    return out;
+}
+
+PsfEngine::PsfEngine(int device, const EngineOptions& options)
+    : device_(device), options_(options) {
+    int count = 0;
+    cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (count == 0) throw CudaError("PsfEngine: no CUDA device");
+    if (device < 0 || device >= count) throw std::invalid_argument("PsfEngine: no such device");
+    size_t usable = 0;
+    if (mkb_usable_bytes(0, options_.reserve.min_bytes, options_.reserve.fraction, &usable) !=
+        MKB_OK)
+        throw std::invalid_argument("PsfEngine: reserve fraction must be in [0, 1]");
+}
+
+size_t PsfEngine::device_bytes() const {
+    return maps_.bytes() + params_.bytes() + psf_.bytes() + mtf_.bytes() + work_.bytes();
+}
+
+void PsfEngine::release() {
+    maps_.release();
+    params_.release();
+    psf_.release();
+    mtf_.release();
+    work_.release();
+}
+
+std::vector<PsfResult> PsfEngine::compute(const SystemBatchHost& batch, const EvalResult& result,
+                                          int v, const PsfSettings& settings) {
+    const std::vector<PsfPupil> pupils = make_psf_pupils(batch, result, v, settings);
+    return compute(pupils, psf_fft_size(result.grid_size, settings.padding));
+}
+
+std::vector<PsfResult> PsfEngine::compute(std::span<const PsfPupil> pupils, int fft_size) {
+    std::vector<PsfResult> out;
+    info_ = PsfRunInfo{};
+    info_.pupils = static_cast<int>(pupils.size());
+    for (const PsfPupil& p : pupils) {  // every check before any device work
+        if (p.grid != pupils.front().grid)
+            throw std::invalid_argument("PsfEngine: every pupil needs the same grid edge");
+        if (fft_size < 2 * p.grid || fft_size > MKB_MAX_PSF_FFT || (fft_size & (fft_size - 1)))
+            throw std::invalid_argument("PSF: FFT size must be a power of two in [2N, 8192]");
+        if (p.opd.size() != static_cast<size_t>(p.grid) * p.grid || p.full_count < 1 ||
+            !(p.wavelength_nm > 0.0) || !(p.na_x > 0.0) || !(p.na_y > 0.0))
+            throw std::invalid_argument("PSF: incomplete pupil");
+        PsfResult r;
+        r.field = p.field;
+        r.wavelength = p.wavelength;
+        r.grid = p.grid;
+        r.fft_size = fft_size;
+        r.wavelength_nm = p.wavelength_nm;
+        r.na_x = p.na_x;
+        r.na_y = p.na_y;
+        out.push_back(std::move(r));
+    }
+    if (pupils.empty()) return out;
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const int n = pupils.front().grid, m = fft_size, count = static_cast<int>(pupils.size());
+    const size_t n2 = static_cast<size_t>(n) * n, m2 = static_cast<size_t>(m) * m;
+    const size_t per_mtf = 2 * (static_cast<size_t>(n) + 1);
+    auto tranche_bytes = [&](int t) {
+        return static_cast<size_t>(t) * (n2 * 8 + sizeof(mkb_psf_pupil_params) + m2 * 8 +
+                                         per_mtf * 8) +
+               mkb_psf_workspace_bytes(t, n, m);
+    };
+    size_t free_bytes = 0, total = 0;
+    cuda_check(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+    size_t available = free_bytes + device_bytes();
+    if (options_.memory_limit_bytes) available = std::min(available, *options_.memory_limit_bytes);
+    size_t usable = 0;
+    check(mkb_usable_bytes(available, options_.reserve.min_bytes, options_.reserve.fraction,
+                           &usable),
+          "psf reserve");
+    int tranche = count;
+    while (tranche >= 1 && tranche_bytes(tranche) > usable)
+        tranche = tranche > 1 ? std::max(1, tranche * 3 / 4) : 0;
+    if (tranche < 1) throw CudaError("PsfEngine: not one pupil fits the device memory");
+    auto* maps = static_cast<double*>(maps_.reserve(tranche * n2 * 8));
+    auto* params = static_cast<mkb_psf_pupil_params*>(
+        params_.reserve(tranche * sizeof(mkb_psf_pupil_params)));
+    auto* psf = static_cast<double*>(psf_.reserve(tranche * m2 * 8));
+    auto* mtf = static_cast<double*>(mtf_.reserve(tranche * per_mtf * 8));
+    const size_t wbytes = mkb_psf_workspace_bytes(tranche, n, m);
+    void* work = work_.reserve(wbytes);
+    std::vector<double> stage(static_cast<size_t>(tranche) * n2), mtf_h(tranche * per_mtf);
+    std::vector<mkb_psf_pupil_params> ph(static_cast<size_t>(tranche));
+    for (int first = 0; first < count; first += tranche) {
+        const int used = std::min(tranche, count - first);
+        for (int t = 0; t < used; ++t) {
+            const PsfPupil& p = pupils[static_cast<size_t>(first + t)];
+            std::copy(p.opd.begin(), p.opd.end(), stage.begin() + t * n2);
+            const double full = static_cast<double>(p.full_count);
+            ph[t] = {p.wavelength_mm(), 1.0 / (full * full), p.flip_x ? -1 : 1,
+                     p.flip_y ? -1 : 1};
+        }
+        cuda_check(cudaMemcpy(maps, stage.data(), used * n2 * 8, cudaMemcpyHostToDevice),
+                   "psf upload");
+        cuda_check(cudaMemcpy(params, ph.data(), used * sizeof(mkb_psf_pupil_params),
+                              cudaMemcpyHostToDevice),
+                   "psf upload");
+        check(mkb_psf_device(used, n, m, maps, params, psf, mtf, work, wbytes, nullptr), "psf");
+        cuda_check(cudaDeviceSynchronize(), "psf");
+        cuda_check(cudaMemcpy(mtf_h.data(), mtf, used * per_mtf * 8, cudaMemcpyDeviceToHost),
+                   "psf download");
+        for (int t = 0; t < used; ++t) {
+            PsfResult& r = out[static_cast<size_t>(first + t)];
+            const PsfPupil& p = pupils[static_cast<size_t>(first + t)];
+            r.psf.resize(m2);
+            cuda_check(cudaMemcpy(r.psf.data(), psf + t * m2, m2 * 8, cudaMemcpyDeviceToHost),
+                       "psf download");
+            const double* mt = mtf_h.data() + t * per_mtf;
+            r.mtf_sagittal.assign(mt, mt + n + 1);
+            r.mtf_tangential.assign(mt + n + 1, mt + 2 * (n + 1));
+            mkb_psf_metrics q{};
+            check(mkb_psf_finish_host(n, m, p.opd.data(), p.full_count, p.wavelength_nm, p.na_x,
+                                      p.na_y, p.flip_x ? 1 : 0, p.flip_y ? 1 : 0, r.psf.data(),
+                                      &q),
+                  "psf finish");
+            r.transmitted = q.transmitted;
+            r.energy = q.energy;
+            r.strehl_fft = q.strehl_fft;
+            r.strehl_origin = q.strehl_origin;
+            r.strehl = q.strehl;
+            r.reference_x = q.reference_x;
+            r.reference_y = q.reference_y;
+            r.peak = q.peak;
+            r.peak_x = q.peak_x;
+            r.peak_y = q.peak_y;
+            r.dx = q.dx;
+            r.dy = q.dy;
+            r.airy_radius = q.airy_radius;
+        }
+        ++info_.tranches;
+    }
+    info_.tranche = tranche;
+    info_.work_bytes = wbytes;
+    info_.device_bytes = device_bytes();
+    info_.budget_bytes = usable;
+    return out;
 }
 
 }  // namespace cuda

@@ -423,6 +423,9 @@ struct EvalSettings {  // eval.hpp:27
 struct EvalResult {  // eval.hpp:96, the reference's layout
     int variants = 0, fields = 0, wavelengths = 0;
     int64_t samples = 0;
+    int grid_size = 0;  // N (EvalSettings::grid)
+    bool half_pupil = false;
+    double field_ray_offset = 1e-3;
     std::vector<double> grid;  // [n][3] x, y, weight
     std::vector<double> reference_curvature, exit_pupil_position;
     std::vector<double> opd, spot_x, spot_y, field_rays;
@@ -584,5 +587,66 @@ LmResult optimize_lm_gpu(TraceEngine& engine, const VariableSet& variables,
                          const LmOptions& options, const ResidualSettings& settings,
                          LmGpuStats* stats = nullptr);
 
+
+// ---- scalar PSF and MTF (include/mikroptim/eval/psf.hpp, include/mikroptim/cuda/psf.hpp) ----
+struct PsfSettings {  // psf.hpp:33
+    double padding = 4.0;
+    double numerical_aperture = 0.0;  // > 0: given; 0: from the field rays
+};
+struct PsfPupil {  // psf.hpp:57
+    int field = 0, wavelength = 0, grid = 0, full_count = 0;
+    double wavelength_nm = 0.0, na_x = 0.0, na_y = 0.0;
+    bool flip_x = false, flip_y = false;
+    std::vector<double> opd;  // [N * N], NaN: no transmission
+    double wavelength_mm() const { return wavelength_nm * 1e-6; }
+};
+struct PsfResult {  // psf.hpp:95
+    int field = 0, wavelength = 0, grid = 0, fft_size = 0;
+    double wavelength_nm = 0.0, na_x = 0.0, na_y = 0.0, dx = 0.0, dy = 0.0, airy_radius = 0.0;
+    std::vector<double> psf, mtf_sagittal, mtf_tangential;
+    int64_t transmitted = 0;
+    double energy = 0.0, strehl_fft = 0.0, strehl_origin = 0.0, strehl = 0.0;
+    double reference_x = 0.0, reference_y = 0.0, peak = 0.0, peak_x = 0.0, peak_y = 0.0;
+    double psf_at(int i, int j) const {
+        return psf[static_cast<size_t>(j) * static_cast<size_t>(fft_size) +
+                   static_cast<size_t>(i)];
+    }
+};
+// psf_fft_size (src/eval/psf.cpp:168); std::invalid_argument for invalid sizes
+int psf_fft_size(int grid, double padding);
+// eval_opd_map with piston removal and make_psf_pupil(s) (src/eval/eval.cpp:512,
+// src/eval/psf.cpp:196)
+std::vector<double> eval_opd_map(const EvalResult& result, int v, int f, int l);
+PsfPupil make_psf_pupil(const SystemBatchHost& batch, const EvalResult& result, int v, int f,
+                        int l, const PsfSettings& settings = {});
+std::vector<PsfPupil> make_psf_pupils(const SystemBatchHost& batch, const EvalResult& result,
+                                      int v, const PsfSettings& settings = {});
+
+struct PsfRunInfo {  // cuda/psf.hpp:22; work_bytes: the FFT workspace
+    int pupils = 0, tranche = 0, tranches = 0;
+    size_t work_bytes = 0, device_bytes = 0, budget_bytes = 0;
+};
+// PsfEngine (include/mikroptim/cuda/psf.hpp:37): PSF, MTF and figures of pupils of one grid
+// edge in tranches sized against the device memory; buffers kept across calls; the device
+// work is mkb_psf_device, the figures mkb_psf_finish_host.
+class PsfEngine {
+public:
+    explicit PsfEngine(int device = 0, const EngineOptions& options = {});
+    PsfEngine(const PsfEngine&) = delete;
+    PsfEngine& operator=(const PsfEngine&) = delete;
+    std::vector<PsfResult> compute(std::span<const PsfPupil> pupils, int fft_size);
+    std::vector<PsfResult> compute(const SystemBatchHost& batch, const EvalResult& result, int v,
+                                   const PsfSettings& settings = {});
+    const PsfRunInfo& last_run() const { return info_; }
+    int device() const { return device_; }
+    size_t device_bytes() const;
+    void release();
+
+private:
+    int device_ = 0;
+    EngineOptions options_;
+    PsfRunInfo info_;
+    DeviceBuffer maps_, params_, psf_, mtf_, work_;
+};
 }  // namespace cuda
 }  // namespace mkb

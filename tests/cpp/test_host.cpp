@@ -31,6 +31,9 @@ extern "C" int mko_ref_prefilter(const mkb_batch_view*, const mkb_residual_plan*
 extern "C" int mko_ref_eval(const mkb_batch_view*, const mkb_residual_plan*, int, int, int, double,
                             int64_t*, double*, double*, double*, uint8_t*, double*, uint8_t*,
                             double*, double*);
+extern "C" int mko_ref_psf(const mkb_batch_view*, const mkb_residual_plan*, int, int, int, double,
+                           int, double, double, int*, int*, double*, double*, int*, double*,
+                           double*, double*);
 extern "C" int mko_ref_optimize_lm(const mkb_batch_view*, const mkb_residual_plan*,
                                    const mkb_variables*, const double*, int, int, int, int, int,
                                    double*, double*, int32_t*, int32_t*, int32_t*, double*, int,
@@ -72,6 +75,7 @@ mkb::SystemBatchHost singlets(int V) {
     topo.pupil_mode = {PupilMode::Axis, PupilMode::Half, PupilMode::Half};
     SystemBatchHost b(topo, V);
     b.reference_wavelength_nm = 587.6;
+    b.wavelength_nm = {486.1, 587.6, 656.3};
     const double lambda_um[3] = {0.4861, 0.5876, 0.6563};
     const double angle_deg[3] = {0.0, 0.7, 1.0};
     const double pi = 3.14159265358979323846;
@@ -377,6 +381,44 @@ int main() {
                    same_values(e.reference_curvature, k) &&
                    same_values(e.exit_pupil_position, zp),
                "EVAL bit-identical to the reference");
+    }
+    {  // scalar PSF and MTF against the reference's psf_cpu (its CPU/GPU bar: 1e-13)
+        cuda::EvalSettings es;
+        es.grid = 16;
+        const cuda::EvalResult e = engine.evaluate(batch, es);
+        cuda::PsfEngine pe(0);
+        mkb_batch_view pv = view;
+        pv.wavelength_nm = batch.wavelength_nm.data();
+        bool ok = true;
+        for (int v = 0; v < V; ++v) {
+            const std::vector<cuda::PsfResult> got = pe.compute(batch, e, v);
+            int M = 0, full = 0;
+            expect(mko_ref_psf(&pv, plan->get(), 16, 0, 0, 1e-3, v, 4.0, 0.0, &M, &full, nullptr,
+                               nullptr, nullptr, nullptr, nullptr, nullptr) == 0,
+                   "reference PSF sizes");
+            const size_t T = 9, m2 = size_t(M) * M;
+            std::vector<double> maps(T * 256), na(2 * T), psf(T * m2), mtf(T * 34), fig(T * 13);
+            std::vector<int> flips(2 * T);
+            expect(mko_ref_psf(&pv, plan->get(), 16, 0, 0, 1e-3, v, 4.0, 0.0, &M, &full,
+                               maps.data(), na.data(), flips.data(), psf.data(), mtf.data(),
+                               fig.data()) == 0,
+                   "reference PSF");
+            ok = ok && got.size() == T;
+            for (size_t t = 0; ok && t < T; ++t) {
+                const cuda::PsfResult& r = got[t];
+                for (size_t k = 0; k < m2; ++k) ok = ok && std::abs(r.psf[k] - psf[t * m2 + k]) <= 1e-13;
+                for (int k = 0; k <= 16; ++k)
+                    ok = ok && std::abs(r.mtf_sagittal[k] - mtf[t * 34 + k]) <= 1e-13 &&
+                         std::abs(r.mtf_tangential[k] - mtf[t * 34 + 17 + k]) <= 1e-13;
+                const double* q = fig.data() + t * 13;
+                ok = ok && double(r.transmitted) == q[0] && std::abs(r.energy - q[1]) <= 1e-13 &&
+                     std::abs(r.strehl_fft - q[2]) <= 1e-13 && r.strehl_origin == q[3] &&
+                     r.strehl == q[4] && r.reference_x == q[5] && r.reference_y == q[6] &&
+                     r.dx == q[10] && r.dy == q[11] && r.airy_radius == q[12];
+            }
+        }
+        expect(ok, "PSF and MTF within 1e-13 of the reference, figures equal");
+        expect(pe.last_run().pupils == 9 && pe.last_run().tranches == 1, "PSF run info");
     }
 #endif
 

@@ -1,5 +1,5 @@
 """The C++ host layer (mikroptim_b200/host): reference-shaped SystemBatchHost / ResidualLayout /
-VariableSet / TraceEngine (RESIDUALS, MERIT, prefilter, EVAL) / DeviceFdJacobian /
+VariableSet / TraceEngine (RESIDUALS, MERIT, prefilter, EVAL) / PsfEngine / DeviceFdJacobian /
 DeviceAdjointJacobian / DeviceNormalEquations / optimize_lm_gpu (with paraxial constraints on the
 device) over the C ABI.
 
@@ -53,7 +53,8 @@ def test_host_layer_builds_and_exports_classes():
                  "mkb::cuda::DeviceFdJacobian::compute", "mkb::cuda::DeviceAdjointJacobian::compute",
                  "mkb::cuda::DeviceNormalEquations::compute", "mkb::cuda::optimize_lm_gpu",
                  "mkb::cuda::TraceEngine::prefilter_variants", "mkb::cuda::TraceEngine::evaluate",
-                 "mkb::LmOptions::c_struct"):
+                 "mkb::LmOptions::c_struct", "mkb::cuda::PsfEngine::compute",
+                 "mkb::cuda::make_psf_pupils"):
         assert name in syms, name
 
 
