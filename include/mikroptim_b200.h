@@ -56,6 +56,17 @@ typedef enum mkb_status {
 /* Values are stable and equal to the reference enums. */
 enum { MKB_SURFACE_STOP = 0, MKB_SURFACE_PLANE = 1, MKB_SURFACE_SPHERE = 2,
        MKB_SURFACE_GHOST_PLATE = 3 };                  /* SurfaceKind, surface_table.hpp:25 */
+/* An aperture stop inside the system (no counterpart in the reference, whose stop is always
+ * table surface 0, docs/adr/0006-blende-erste-flaeche.md): a plane at table surface s_a,
+ * 1 <= s_a <= S - 2, at most one per table, whose curvature slot holds the stop's
+ * semi-aperture R. Table surface 0 is then the entrance pupil, placed by paraxial ray aiming
+ * wherever a record is packed or a variable written: with the y-u trace of the paraxial index
+ * (wavelength column 0) from surface 1 to the stop, y_A the stop height of the ray (y = 1,
+ * u = 0) and y_B that of the ray (y = 0, u = 1), the pupil radius becomes R / |y_A| and
+ * thickness[0] becomes -y_B / y_A (the entrance pupil's distance before surface 1). Every
+ * operation separately rounded. Coaxial batches of one table, without ghost plates;
+ * thickness[0] is no variable then. */
+enum { MKB_SURFACE_APERTURE_STOP = 4 };
 enum { MKB_PUPIL_HALF = 0, MKB_PUPIL_FULL = 1, MKB_PUPIL_AXIS = 2 };
                                                        /* PupilMode, pupil/quadrature.hpp:24 */
 enum { MKB_FAILURE_SOFT = 0, MKB_FAILURE_HARD = 1 };   /* FailureMode, surface_ops.hpp:74 */

@@ -25,6 +25,10 @@ from .quadrature import (MAX_RINGS, PUPIL_AXIS, PUPIL_FULL, PUPIL_HALF, gauss_le
                          sample_count)
 
 SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
+# an aperture stop inside the system (no reference counterpart): a plane whose curvature slot
+# holds the stop's semi-aperture; surface 0 is then the entrance pupil, placed by paraxial ray
+# aiming (MKB_SURFACE_APERTURE_STOP, include/mikroptim_b200.h)
+SURFACE_APERTURE_STOP = 4
 FAILURE_SOFT, FAILURE_HARD = 0, 1
 PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA, PRECISION_DF64 = 0, 1, 2, 3
 VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT, VAR_GLASS = 0, 1, 2, 3, 4
@@ -68,6 +72,12 @@ class BatchTopology:
     def ghost_plates(self) -> int:
         return sum(1 for t in self.type[1:] if t == SURFACE_GHOST_PLATE)
 
+    @property
+    def stop_surface(self) -> int:
+        """The interior aperture stop's table surface, or 0 (the stop is surface 0)."""
+        return next((s for s, t in enumerate(self.type) if s > 0 and t == SURFACE_APERTURE_STOP),
+                    0)
+
     def ghost_surface(self, g: int) -> int:
         """Table surface of plate g."""
         return [s for s, t in enumerate(self.type) if s > 0 and t == SURFACE_GHOST_PLATE][g]
@@ -86,8 +96,16 @@ class BatchTopology:
         if self.type[0] != SURFACE_STOP:
             raise ValueError("BatchTopology: surface 0 must be the stop")
         for s, t in enumerate(self.type[1:], start=1):
-            if t not in (SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE):
+            if t not in (SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE,
+                         SURFACE_APERTURE_STOP):
                 raise ValueError(f"BatchTopology: surface {s} has unknown kind {t}")
+        stops = [s for s, t in enumerate(self.type) if s > 0 and t == SURFACE_APERTURE_STOP]
+        if len(stops) > 1 or (stops and not 1 <= stops[0] <= self.surfaces - 2):
+            raise ValueError("BatchTopology: at most one interior aperture stop, at "
+                             "1 <= s <= S - 2")
+        if stops and (self.non_coaxial or self.ghost_plates > 0):
+            raise NotImplementedError("BatchTopology: an interior aperture stop is traced in "
+                                      "coaxial batches without ghost plates")
         if self.ghost_plates > MAX_GHOST_PLATES:
             raise NotImplementedError(f"BatchTopology: at most {MAX_GHOST_PLATES} ghost plates "
                                       "in this build")
@@ -461,6 +479,9 @@ class VariableSet:
             elif v.type == VAR_THICKNESS:
                 if not 0 <= v.surface < S - 1:
                     raise ValueError(f"VariableSet: variable {k}: thickness surface out of range")
+                if v.surface == 0 and self.topology.stop_surface > 0:
+                    raise ValueError(f"VariableSet: variable {k}: thickness[0] follows the "
+                                     "interior stop's entrance pupil")
             elif v.type == VAR_WORKING_DISTANCE:
                 v.surface = S - 1
             elif v.type == VAR_GLASS:

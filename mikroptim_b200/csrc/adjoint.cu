@@ -131,11 +131,14 @@ __device__ int forward_record(const TraceParams& p, const double* rec, const Rec
 
 // Reverse sweep of one seed (backward_ray): writes factor * dPhi/dx into row `row` of the
 // run's columns col0[c * R + row] for every variable whose parameter is reached.
+// start[0..2] (when not null) get the adjoint of the start point's x and y and the derivative
+// with respect to thickness[0] (the entrance pupil's distance), unscaled, for the aiming fold.
 template <class N>
 __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const double* rec,
                                const RecordLayout& lay, int f, int l, const Record<N>& ck,
                                bool reached_image, bool soft_mode, N seed_opl, N seed_pen,
-                               N factor, double* col0, int64_t R, int64_t row) {
+                               N factor, double* col0, int64_t R, int64_t row,
+                               double* start = nullptr) {
     const int S = p.S, L = p.L;
     const N zero(0.0);
     const double* curv = rec + lay.curvature;
@@ -239,6 +242,7 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
                     }
                     if (sphere) write(v.col_curvature[j], par.curvature);
                     write(v.col_thickness[s], par.thickness);
+                    if (s == 0 && start != nullptr) start[2] = value_of(par.thickness);
                     index_sink(j, par.n_after + n_carry);
                     n_carry = par.n_before;
                 }
@@ -247,6 +251,20 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
         }
     }
     index_sink(0, n_carry);
+    if (start != nullptr) {
+        start[0] = value_of(adj.p.x);
+        start[1] = value_of(adj.p.y);
+    }
+}
+
+// The aiming fold of one row: the entrance pupil's radius a and distance t0 follow the
+// variables (aim_record), so every column j gains dPhi/da da/dx_j + dPhi/dt0 dt0/dx_j with
+// dPhi/da = rho (sin phi, cos phi) . adj(p0) + seed_opl rho cos phi sin theta (the start point
+// a rho (sin phi, cos phi, 0) and its optical path p0 . d0).
+__device__ __forceinline__ double aim_start_adjoint(const double* start, const Sample& smp,
+                                                    double sin_theta, double seed_opl) {
+    return smp.rho * (smp.sin_phi * start[0] + smp.cos_phi * start[1]) +
+           seed_opl * smp.rho * smp.cos_phi * sin_theta;
 }
 
 template <bool kExact>
@@ -273,6 +291,20 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         return;
     const bool soft_mode = p.failure == MKB_FAILURE_SOFT;
     double* col0 = J + static_cast<int64_t>(v) * ap.v.P * ap.rows;
+    // an interior stop: d(a, t0)/dx of the variant's aimed entrance pupil
+    __shared__ double aim_da[MKB_MAX_VARIABLES], aim_dt[MKB_MAX_VARIABLES];
+    if (lay.stop > 0) {
+        for (int k = threadIdx.x; k < ap.v.P; k += kAdjThreads)
+            aim_sensitivity(record, lay, ap.v, k, aim_da[k], aim_dt[k]);
+        __syncthreads();
+    }
+    auto aim_fold = [&](const double* start, const Sample& smp, int f, double seed_opl,
+                        double factor, int64_t row) {
+        const double ga = aim_start_adjoint(start, smp, record[lay.sin_theta + f], seed_opl);
+        for (int k = 0; k < ap.v.P; ++k)
+            col0[static_cast<int64_t>(k) * ap.rows + row] +=
+                factor * (ga * aim_da[k] + start[2] * aim_dt[k]);
+    };
     for (int i = threadIdx.x; i < pack.rays; i += kAdjThreads) {
         int t = 0;
         while (t + 1 < pack.tuples && i >= sh.tuple_start[t + 1]) ++t;
@@ -286,13 +318,18 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
         const int st = forward_record<N>(p, record, lay, f, l, smp, soft_mode, ck, soft_first);
         const int64_t row = p.field_offset[f] + static_cast<int64_t>(l) * p.sample_count[f] + k;
         const bool reached = in_piston(st);
-        if (reached)
+        double start[3] = {0.0, 0.0, 0.0};
+        double* aim = lay.stop > 0 ? start : nullptr;
+        if (reached) {
             backward_sweep<N>(p, ap.v, record, lay, f, l, ck, true, soft_mode, N(1.0), N(0.0),
-                              N(1.0), col0, ap.rows, row);
+                              N(1.0), col0, ap.rows, row, aim);
+            if (aim) aim_fold(start, smp, f, 1.0, 1.0, row);
+        }
         if (soft_mode && soft_first != kOk) {
             const N factor = N(p.pscale[tu]) * N(smp.root_weight);
             backward_sweep<N>(p, ap.v, record, lay, f, l, ck, reached, soft_mode, N(0.0),
-                              N(1.0), factor, col0, ap.rows, p.rays + row);
+                              N(1.0), factor, col0, ap.rows, p.rays + row, aim);
+            if (aim) aim_fold(start, smp, f, 0.0, value_of(factor), p.rays + row);
         }
     }
 }
@@ -633,9 +670,15 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                                             int count, int image_branch, bool reached_image,
                                             bool soft_mode, const double (&so)[K],
                                             const double (&spn)[K],
-                                            const RowSinks<K, YT>& sinks) {
+                                            const RowSinks<K, YT>& sinks,
+                                            const double* aim_sens) {
     const int L = p.L;
     const N zero(0.0);
+    // interior stop (kernel feature 8): the aimed entrance pupil follows the variables
+    constexpr bool kAim = (kFeat & 8) != 0;
+    A t0_adj[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) t0_adj[m] = A(0.0);
     const double* curv = rec + lay.curvature;
     const double* thick = rec + lay.thickness;
     const double* idx = rec + lay.index;
@@ -768,6 +811,7 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
                     sinks.row[m][cc * sinks.ld[m]] = YT(value_of(factor[m] * par[m].curvature));
                 if (ct >= 0)
                     sinks.row[m][ct * sinks.ld[m]] = YT(value_of(factor[m] * par[m].thickness));
+                if (kAim && c == 0) t0_adj[m] = par[m].thickness;
             }
             if constexpr (kGlass) {
                 A value[K];
@@ -782,6 +826,20 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
         next_branch = branch_of(c);
     }
     index_sink(0, n_carry);
+    if constexpr (kAim) {
+        // every column gains dPhi/da da/dx_j + dPhi/dt0 dt0/dx_j (aim_start_adjoint)
+        const A st = A(rec[lay.sin_theta + f]);
+        const A rho = A(smp.rho), sp = A(smp.sin_phi), cp = A(smp.cos_phi);
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            const A ga = rho * (sp * adj[m].p.x + cp * adj[m].p.y) + seed_opl[m] * rho * cp * st;
+            for (int k = 0; k < v.P; ++k) {
+                YT& y = sinks.row[m][k * sinks.ld[m]];
+                y = YT(value_of(A(y) + factor[m] * (ga * A(aim_sens[k]) +
+                                                    t0_adj[m] * A(aim_sens[MKB_MAX_VARIABLES + k]))));
+            }
+        }
+    }
 }
 
 // Mixed precision: the forward trace (OPL, piston, merit, the states the sweep is linearised
@@ -819,11 +877,13 @@ __device__ __forceinline__ void run_backward(const TraceParams& p, const VarPara
                                              int count, int image_branch, bool reached_image,
                                              bool soft_mode, const double (&so)[K],
                                              const double (&spn)[K],
-                                             const RowSinks<K, typename FusedTypes<N>::Row>& sinks) {
+                                             const RowSinks<K, typename FusedTypes<N>::Row>& sinks,
+                                             const double* aim_sens) {
     using T = FusedTypes<N>;
     fused_backward<typename T::Bwd, typename T::Adj, K, kFeat>(p, v, rec, mu_tab, lay, S, f, l, smp, ck, stride_ck,
                                                         br_lo, br_hi, count, image_branch,
-                                                        reached_image, soft_mode, so, spn, sinks);
+                                                        reached_image, soft_mode, so, spn, sinks,
+                                                        aim_sens);
 }
 
 template <class T>
@@ -853,6 +913,7 @@ __global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
     __shared__ FusedShared sh;
+    __shared__ double aim_sens[(kFeat & 8) != 0 ? 2 * MKB_MAX_VARIABLES : 1];
     extern __shared__ __align__(16) double dyn[];
     const int NPM = fused_np(fa.p_max);  // shared-memory and scratch layout: the largest P
     const int pairs_max = (NPM / 8) * (NPM / 8 + 1) / 2;
@@ -930,6 +991,9 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                                        F(record[lay.index + s * p.L + l]))
                             : 0.0;
         }
+        if constexpr ((kFeat & 8) != 0)  // interior stop: d(a, t0)/dx of the aimed pupil
+            for (int k = tid; k < P; k += kFusedThreads)
+                aim_sensitivity(record, lay, v, k, aim_sens[k], aim_sens[MKB_MAX_VARIABLES + k]);
         __syncthreads();
         for (int base = 0; base < p.rays; base += kFusedThreads) {
             const int q = base + tid;
@@ -972,7 +1036,7 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                         const RowSinks<2, YT> sinks{{1.0, pfac}, {row, prow}, {TS, kFusedThreads}};
                         run_backward<N, 2, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
                                            br_hi, count, image_branch, piston, soft_mode, so, sp,
-                                           sinks);
+                                           sinks, aim_sens);
                     }
                 } else if (!(piston && pen_sweep)) {
                     if (piston || pen_sweep) {  // one row: its seed and its sink
@@ -982,17 +1046,19 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                                                 {piston ? TS : kFusedThreads}};
                         run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck,
                                            br_lo, br_hi, count, image_branch, piston, soft_mode,
-                                           so, sp, sinks);
+                                           so, sp, sinks, aim_sens);
                     }
                 } else {  // both rows, one sweep each
                     const double so0[1] = {1.0}, sp0[1] = {0.0};
                     const RowSinks<1, YT> s0{{1.0}, {row}, {TS}};
                     run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
-                                       br_hi, count, image_branch, true, soft_mode, so0, sp0, s0);
+                                       br_hi, count, image_branch, true, soft_mode, so0, sp0, s0,
+                                       aim_sens);
                     const double so1[1] = {0.0}, sp1[1] = {1.0};
                     const RowSinks<1, YT> s1{{pfac}, {prow}, {kFusedThreads}};
                     run_backward<N, 1, kFeat>(p, v, record, mu_tab, lay, S, f, l, smp, my_ck, stride_ck, br_lo,
-                                       br_hi, count, image_branch, true, soft_mode, so1, sp1, s1);
+                                       br_hi, count, image_branch, true, soft_mode, so1, sp1, s1,
+                                       aim_sens);
                 }
             }
             R[tid] = opl_val;
@@ -1198,7 +1264,9 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     // kernel variant per precision and features (1: surface transforms, 2: ghost plates,
     // 4: glass variables of some run)
     const bool glass = vp.has_glass != 0 || rv.any_glass != 0;
-    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0);
+    // 8: an interior aperture stop (coaxial, no ghost plates: the batch check refuses others)
+    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0) |
+                     (tp.stop > 0 ? 8 : 0);
     using Fn = void (*)(FusedArgs);
     auto pick = [&](auto tag) -> Fn {
         using N = typename decltype(tag)::type;
@@ -1210,6 +1278,8 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
         case 4: return adjoint_gram_kernel<N, 4>;
         case 5: return adjoint_gram_kernel<N, 5>;
         case 6: return adjoint_gram_kernel<N, 6>;
+        case 8: return adjoint_gram_kernel<N, 8>;
+        case 12: return adjoint_gram_kernel<N, 12>;
         default: return adjoint_gram_kernel<N, 7>;
         }
     };

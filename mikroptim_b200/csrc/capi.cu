@@ -189,17 +189,31 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
         set_error("surface 0 must be the stop");
         return MKB_ERR_ARGUMENT;
     }
-    int plates = 0;
+    int plates = 0, stop = 0;
     for (int s = 1; s < S; ++s) {
         const int t = batch->type[s];
         if (t == MKB_SURFACE_GHOST_PLATE) {
             ++plates;
             continue;
         }
+        if (t == MKB_SURFACE_APERTURE_STOP) {
+            if (stop != 0 || s > S - 2) {
+                set_error("an interior aperture stop lies at 1 <= s <= S - 2, at most one "
+                          "per table (surface %d)", s);
+                return MKB_ERR_ARGUMENT;
+            }
+            stop = s;
+            continue;
+        }
         if (t != MKB_SURFACE_PLANE && t != MKB_SURFACE_SPHERE) {
             set_error("surface %d has unknown kind %d", s, t);
             return MKB_ERR_ARGUMENT;
         }
+    }
+    if (stop > 0 && (batch->non_coaxial || plates > 0 || batch->variant_surfaces != nullptr)) {
+        set_error("an interior aperture stop is traced in coaxial batches of one table without "
+                  "ghost plates");
+        return MKB_ERR_UNSUPPORTED;
     }
     if (plates != batch->ghost_plates) {
         set_error("the table has %d ghost-plate surfaces but the batch carries %d plates",
@@ -220,6 +234,10 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     p.glass = batch->glass ? 1 : 0;
     p.vsurf = batch->variant_surfaces;
     p.order = nullptr;
+    p.stop = stop;
+    p.spheres = 0;
+    for (int s = 0; s < S && s < 64; ++s)
+        if (batch->type[s] == MKB_SURFACE_SPHERE) p.spheres |= uint64_t(1) << s;
     p.L = L;
     p.F = F;
     p.stride = lay.stride;
@@ -371,6 +389,15 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
                 set_error("variable %d: curvature of surface %d, which is not a sphere", k, s);
                 return MKB_ERR_ARGUMENT;
             }
+            if (t == MKB_VAR_THICKNESS && s == 0) {
+                bool stop = false;
+                for (int u = 1; u < S; ++u) stop = stop || type[u] == MKB_SURFACE_APERTURE_STOP;
+                if (stop) {
+                    set_error("variable %d: thickness[0] follows the interior stop's entrance "
+                              "pupil and is no variable", k);
+                    return MKB_ERR_ARGUMENT;
+                }
+            }
             slot = t == MKB_VAR_CURVATURE ? &v.col_curvature[s] : &v.col_thickness[s];
         }
         if (*slot >= 0) {
@@ -478,7 +505,11 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
     }
     const int non_coaxial = v->decenter_tilt != nullptr ? 1 : 0;
     const int glass = v->buchdahl_coeff != nullptr ? 1 : 0;
-    const RecordLayout lay = record_layout(S, L, F, non_coaxial, G, K, glass);
+    if (v->type == nullptr) {
+        set_error("pack: type array is null");
+        return MKB_ERR_ARGUMENT;
+    }
+    const RecordLayout lay = with_stop(record_layout(S, L, F, non_coaxial, G, K, glass), v->type, S);
     for (int64_t i = 0; i < v->variants; ++i) {
         double* r = records + i * lay.stride;
         std::memset(r, 0, sizeof(double) * lay.stride);
@@ -522,6 +553,12 @@ int mkb_pack_batch_host(const mkb_batch_view* v, double* records) {
             for (int l = 0; l < L; ++l)
                 r[lay.ghost_index + g * L + l] = v->ghost_index[(i * G + g) * L + l];
         }
+        // an interior stop: the entrance pupil from paraxial ray aiming
+        if (lay.stop > 0 && !aim_record(lay, r)) {
+            set_error("pack: variant %lld: the interior stop's paraxial image is at infinity "
+                      "or not finite", static_cast<long long>(i));
+            return MKB_ERR_ARGUMENT;
+        }
     }
     return MKB_OK;
 }
@@ -545,9 +582,11 @@ int mkb_apply_variables_device(const mkb_device_batch* templates, const mkb_vari
         set_error("apply: shape out of range (S=%d, L=%d, F=%d)", S, L, F);
         return MKB_ERR_ARGUMENT;
     }
-    const RecordLayout lay = record_layout(S, L, F, templates->non_coaxial != 0,
-                                           templates->ghost_plates, templates->ghost_terms,
-                                           templates->glass ? 1 : 0);
+    const RecordLayout lay = with_stop(record_layout(S, L, F, templates->non_coaxial != 0,
+                                                     templates->ghost_plates,
+                                                     templates->ghost_terms,
+                                                     templates->glass ? 1 : 0),
+                                       templates->type, S);
     if (templates->record_stride != lay.stride ||
         (reinterpret_cast<uintptr_t>(records_out) & 15u) != 0) {
         set_error("apply: record stride %d (expected %d) or unaligned output",

@@ -44,6 +44,9 @@ struct RecordLayout {
     int ghost_coeff, ghost_radius, ghost_index;  // ghost plate data, or -1 (no plates)
     int ghost_terms;                             // K
     int glass;                                   // Buchdahl coefficients [S][4], or -1
+    int stop;                                    // interior aperture stop s_a, or 0 (none)
+    int L;                                       // wavelengths (index columns)
+    uint64_t spheres;                            // bit s: surface s is a sphere (s < 64)
 };
 
 __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int non_coaxial = 0,
@@ -73,6 +76,9 @@ __host__ __device__ inline RecordLayout record_layout(int S, int L, int F, int n
     r.glass = glass ? n : -1;
     if (glass) n += S * 4;
     r.stride = (n + 1) & ~1;
+    r.stop = 0;
+    r.L = L;
+    r.spheres = 0;
     return r;
 }
 
@@ -114,10 +120,95 @@ struct TraceParams {
     int8_t ghost_of[kMaxSurfaces];  // plate number of a ghost-plate surface (table order), or -1
     const uint8_t* vsurf;           // device [V] table surfaces of each variant, or null (S)
     const int* order;               // device [V] processing order of the variants, or null
+    int stop;                       // interior aperture stop s_a (MKB_SURFACE_APERTURE_STOP), or 0
+    uint64_t spheres;               // bit s: surface s is a sphere
 };
 
 __host__ __device__ inline RecordLayout layout_of(const TraceParams& p) {
-    return record_layout(p.S, p.L, p.F, p.non_coaxial, p.G, p.K, p.glass);
+    RecordLayout r = record_layout(p.S, p.L, p.F, p.non_coaxial, p.G, p.K, p.glass);
+    r.stop = p.stop;
+    r.spheres = p.spheres;
+    return r;
+}
+
+// ---- paraxial ray aiming for an interior aperture stop ----------------------------------------
+// Separately rounded operations on host and device (the host side is compiled without
+// contraction), so the packed and the device-applied records agree bit for bit.
+__host__ __device__ __forceinline__ double aim_mul(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double aim_add(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ __forceinline__ double aim_sub(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+__host__ __device__ __forceinline__ double aim_div(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __ddiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+
+// The stop heights y_A (ray y = 1, u = 0 at surface 1) and y_B (ray y = 0, u = 1) of the y-u
+// trace from surface 1 to the stop s_a at the index of wavelength column 0: at surface s,
+// u' = (n u - y c (n' - n)) / n' (c = 0 off spheres), then y += thickness[s] u'.
+__host__ __device__ inline void aim_heights(const double* rec, const RecordLayout& lay,
+                                            double& ya, double& yb) {
+    double y1 = 1.0, u1 = 0.0, y2 = 0.0, u2 = 1.0;
+    double n = rec[lay.index];
+    for (int s = 1; s < lay.stop; ++s) {
+        const double n2 = rec[lay.index + s * lay.L];
+        const double c = (lay.spheres >> s) & 1u ? rec[lay.curvature + s] : 0.0;
+        const double phi = aim_mul(c, aim_sub(n2, n));
+        u1 = aim_div(aim_sub(aim_mul(n, u1), aim_mul(y1, phi)), n2);
+        u2 = aim_div(aim_sub(aim_mul(n, u2), aim_mul(y2, phi)), n2);
+        const double t = rec[lay.thickness + s];
+        y1 = aim_add(y1, aim_mul(t, u1));
+        y2 = aim_add(y2, aim_mul(t, u2));
+        n = n2;
+    }
+    ya = y1;
+    yb = y2;
+}
+
+// The layout with the table's interior stop and sphere mask filled in from its surface kinds.
+inline RecordLayout with_stop(RecordLayout lay, const uint8_t* type, int S) {
+    lay.stop = 0;
+    lay.spheres = 0;
+    for (int s = 0; s < S && s < 64; ++s) {
+        if (type[s] == MKB_SURFACE_SPHERE) lay.spheres |= uint64_t(1) << s;
+        if (s > 0 && type[s] == MKB_SURFACE_APERTURE_STOP) lay.stop = s;
+    }
+    return lay;
+}
+
+// Writes the entrance pupil (radius R / |y_A|, thickness[0] = -y_B / y_A) into a record whose
+// table has an interior stop; R is the stop surface's curvature slot. Returns false when the
+// stop's image is at infinity (y_A = 0) or a value is not finite (the record is then left with
+// those non-finite values, which fail every ray).
+__host__ __device__ inline bool aim_record(const RecordLayout& lay, double* rec) {
+    double ya, yb;
+    aim_heights(rec, lay, ya, yb);
+    const double R = rec[lay.curvature + lay.stop];
+    const double a = aim_div(R, ya < 0.0 ? -ya : ya);
+    const double t0 = -aim_div(yb, ya);
+    rec[lay.pupil] = a;
+    rec[lay.thickness] = t0;
+    return ya != 0.0 && a == a && t0 == t0 && a - a == 0.0 && t0 - t0 == 0.0;
 }
 
 // Table surfaces variant v traces (uneven batches share the table of the largest; the value
@@ -712,6 +803,54 @@ __device__ __forceinline__ void apply_variables(const VarParams& v, const Record
                                                 const double* x, double* rec) {
     for (int k = 0; k < v.P; ++k) write_variable(v, lay, k, x[k], rec);
     refresh_glass(v, lay, rec);
+    if (lay.stop > 0) aim_record(lay, rec);  // the entrance pupil follows the variables
+}
+
+// d(a, t0)/dx_k of the aimed entrance pupil (aim_record) for variable k: the y-u trace of
+// aim_heights carrying every quantity's derivative with respect to x_k (a curvature or a
+// thickness of a surface before the stop, or a Buchdahl component of a medium before it, whose
+// index at wavelength column 0 moves with slope w^c); 0 for every other variable. Forward-mode
+// derivatives of the same arithmetic (contraction allowed: the adjoint rows are not bit-exact).
+__device__ inline void aim_sensitivity(const double* rec, const RecordLayout& lay,
+                                       const VarParams& v, int k, double& da, double& dt0) {
+    const int type = v.type[k], sk = v.surface[k];
+    double slope = 0.0;
+    if (type == MKB_VAR_GLASS) {
+        const double w = v.omega[0];
+        slope = v.glass_component[k] == 0 ? 1.0 : v.glass_component[k] == 1 ? w : w * w;
+    }
+    double y1 = 1.0, u1 = 0.0, y2 = 0.0, u2 = 1.0;
+    double dy1 = 0.0, du1 = 0.0, dy2 = 0.0, du2 = 0.0;
+    double n = rec[lay.index];
+    double dn = type == MKB_VAR_GLASS && sk == 0 ? slope : 0.0;
+    for (int s = 1; s < lay.stop; ++s) {
+        const double n2 = rec[lay.index + s * lay.L];
+        const double dn2 = type == MKB_VAR_GLASS && sk == s ? slope : 0.0;
+        const bool sphere = (lay.spheres >> s) & 1u;
+        const double c = sphere ? rec[lay.curvature + s] : 0.0;
+        const double dc = sphere && type == MKB_VAR_CURVATURE && sk == s ? 1.0 : 0.0;
+        const double phi = c * (n2 - n);
+        const double dphi = dc * (n2 - n) + c * (dn2 - dn);
+        const double a1 = n * u1 - y1 * phi, a2 = n * u2 - y2 * phi;
+        const double da1 = dn * u1 + n * du1 - dy1 * phi - y1 * dphi;
+        const double da2 = dn * u2 + n * du2 - dy2 * phi - y2 * dphi;
+        u1 = a1 / n2;
+        u2 = a2 / n2;
+        du1 = (da1 - u1 * dn2) / n2;
+        du2 = (da2 - u2 * dn2) / n2;
+        const double t = rec[lay.thickness + s];
+        const double dt = type == MKB_VAR_THICKNESS && sk == s ? 1.0 : 0.0;
+        dy1 += dt * u1 + t * du1;
+        dy2 += dt * u2 + t * du2;
+        y1 += t * u1;
+        y2 += t * u2;
+        n = n2;
+        dn = dn2;
+    }
+    const double R = rec[lay.curvature + lay.stop];
+    const double sgn = y1 < 0.0 ? -1.0 : 1.0;
+    da = -R * sgn * dy1 / (y1 * y1);
+    dt0 = -(dy2 * y1 - y2 * dy1) / (y1 * y1);
 }
 
 // ---- launch bookkeeping (host) -------------------------------------------------------------

@@ -68,6 +68,7 @@ __global__ void fd_build_kernel(const __grid_constant__ VarParams vp, RecordLayo
             const double y = (j & 1) ? p.xa : p.xb;
             write_variable(v, lay, k, y, dst);
             refresh_glass(v, lay, dst);  // a perturbed Buchdahl coefficient moves the index
+            if (lay.stop > 0) aim_record(lay, dst);  // and the entrance pupil follows
         }
     }
 }

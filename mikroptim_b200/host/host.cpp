@@ -38,12 +38,19 @@ void BatchTopology::validate() const {
         throw std::invalid_argument("BatchTopology: type needs one entry per surface");
     if (type[0] != SurfaceKind::Stop)
         throw std::invalid_argument("BatchTopology: surface 0 must be the stop");
-    int plates = 0;
+    int plates = 0, stops = 0;
     for (int s = 1; s < surfaces; ++s) {
         if (type[s] == SurfaceKind::GhostPlate) ++plates;
-        else if (type[s] != SurfaceKind::Plane && type[s] != SurfaceKind::Sphere)
+        else if (type[s] == SurfaceKind::ApertureStop) {
+            if (++stops > 1 || s > surfaces - 2)
+                throw std::invalid_argument("BatchTopology: at most one interior aperture stop, "
+                                            "at 1 <= s <= S - 2");
+        } else if (type[s] != SurfaceKind::Plane && type[s] != SurfaceKind::Sphere)
             throw std::invalid_argument("BatchTopology: unknown surface kind");
     }
+    if (stops > 0 && (non_coaxial || plates > 0))
+        throw std::logic_error("BatchTopology: an interior aperture stop is traced in coaxial "
+                               "batches without ghost plates");
     if (plates != ghost_plates)
         throw std::invalid_argument("BatchTopology: ghost_plates must equal the number of "
                                     "GhostPlate surfaces");
@@ -387,6 +394,11 @@ VariableSet::VariableSet(const BatchTopology& topology, std::vector<Variable> va
         } else if (v.type == VariableType::Thickness) {
             if (v.surface < 0 || v.surface >= S - 1)
                 throw std::invalid_argument("VariableSet: thickness surface out of range");
+            if (v.surface == 0)
+                for (int s = 1; s < S; ++s)
+                    if (topology.type[s] == SurfaceKind::ApertureStop)
+                        throw std::invalid_argument("VariableSet: thickness[0] follows the "
+                                                    "interior stop's entrance pupil");
         } else if (v.type == VariableType::WorkingDistance) {
             v.surface = S - 1;
         } else if (v.type == VariableType::Glass) {

@@ -30,7 +30,11 @@
 
 namespace mkb {
 
-enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2, GhostPlate = 3 };
+// ApertureStop: an aperture stop inside the system (no reference counterpart; its curvature
+// slot holds the semi-aperture, surface 0 becomes the aimed entrance pupil,
+// MKB_SURFACE_APERTURE_STOP)
+enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2, GhostPlate = 3,
+                                   ApertureStop = 4 };
 enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
 enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
 enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2, DF64 = 3 };

@@ -265,6 +265,70 @@ def objective(variants: int = 4096, seed: int = 20261203 + 2, rings: int = 16,
     return b, settings, vs, x0
 
 
+def stop_heights(batch: SystemBatchHost, stop: int) -> tuple[np.ndarray, np.ndarray]:
+    """y_A, y_B [V] of the aiming y-u trace (MKB_SURFACE_APERTURE_STOP): rays (y = 1, u = 0)
+    and (y = 0, u = 1) at surface 1 traced to the stop at wavelength column 0."""
+    V = batch.variants
+    y1, u1, y2, u2 = np.ones(V), np.zeros(V), np.zeros(V), np.ones(V)
+    n = batch.index[:, 0, 0].copy()
+    for s in range(1, stop):
+        n2 = batch.index[:, s, 0]
+        c = batch.curvature[:, s] if batch.type[s] == SURFACE_SPHERE else np.zeros(V)
+        phi = c * (n2 - n)
+        u1 = (n * u1 - y1 * phi) / n2
+        u2 = (n * u2 - y2 * phi) / n2
+        y1 = y1 + batch.thickness[:, s] * u1
+        y2 = y2 + batch.thickness[:, s] * u2
+        n = n2
+    return y1, y2
+
+
+def with_aperture_stop(batch: SystemBatchHost, settings: ResidualSettings,
+                       variables: VariableSet, stop: int):
+    """The same systems with an aperture stop inside: a plane of kind SURFACE_APERTURE_STOP
+    inserted as table surface `stop` at the vertex plane of the old surface `stop` (the old
+    thickness[stop - 1] now leads to the stop, which is 0 ahead of the next surface and sits
+    in the same medium). Its semi-aperture is chosen so that the aimed entrance pupil keeps the
+    old pupil radius; surface 0 becomes that entrance pupil, so thickness[0] leaves the
+    variables, and the stop's own gap to the next surface stays fixed (0). Returns (batch,
+    settings, variables, x0). Coaxial batches of one table without ghost plates."""
+    from .batch import SURFACE_APERTURE_STOP
+    old = batch.topology
+    if not 1 <= stop <= old.surfaces - 1:
+        raise ValueError("with_aperture_stop: the stop goes between surfaces 1 and S - 1")
+    S = old.surfaces + 1
+    kinds = list(old.type[:stop]) + [SURFACE_APERTURE_STOP] + list(old.type[stop:])
+    topo = BatchTopology(surfaces=S, wavelengths=old.wavelengths, fields=old.fields,
+                         type=kinds, pupil_mode=list(old.pupil_mode))
+    V = batch.variants
+    b = SystemBatchHost(topo, V)
+    b.reference_wavelength_nm = batch.reference_wavelength_nm
+    b.wavelength_nm[:] = batch.wavelength_nm
+    b.wavelength_weight[:] = batch.wavelength_weight
+    b.field_weight[:] = batch.field_weight
+    ins = lambda a, value: np.concatenate([a[:, :stop], value, a[:, stop:]], axis=1)
+    b.curvature = ins(batch.curvature, np.zeros((V, 1)))
+    b.thickness = ins(batch.thickness, np.zeros((V, 1)))
+    b.index = ins(batch.index, batch.index[:, stop - 1:stop, :])
+    if batch.buchdahl_coeff is not None:
+        b.buchdahl_coeff = ins(batch.buchdahl_coeff, np.zeros((V, 1, 4)))
+    b.pupil_radius = batch.pupil_radius.copy()
+    b.field_angle = batch.field_angle.copy()
+    b.field_target = batch.field_target.copy()
+    ya, _ = stop_heights(b, stop)
+    b.curvature[:, stop] = batch.pupil_radius * np.abs(ya)  # the stop's semi-aperture R
+    moved = []
+    for v in variables.variables:
+        if v.type == VAR_THICKNESS and v.surface == 0:
+            continue  # follows the entrance pupil now
+        s_new = v.surface + (1 if v.surface >= stop else 0)
+        moved.append(Variable(v.type, s_new, v.lower, v.upper, v.typical, plate=v.plate,
+                              order=v.order, component=v.component))
+    vs = VariableSet(topo, moved)
+    x0 = np.stack([vs.extract(b, k) for k in range(V)]) if V else np.zeros((0, vs.size))
+    return b, settings, vs, x0
+
+
 # ---- configuration 3: uneven systems -----------------------------------------------------------
 
 def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max: int = 30,

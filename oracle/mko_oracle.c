@@ -468,6 +468,34 @@ static double failure_penalty(int st, double soft_penalty) {
 }
 
 /* ---- layout: src/batch/batch_residuals.cpp:25 ------------------------------------------- */
+int mko_port_aim(const mkb_batch_view* v, double* pupil, double* thickness0) {
+    if (v == NULL || pupil == NULL || thickness0 == NULL) return -1;
+    const int S = v->surfaces, L = v->wavelengths;
+    int stop = 0;
+    for (int s = 1; s < S; ++s)
+        if (v->type[s] == 4) stop = s; /* MKB_SURFACE_APERTURE_STOP */
+    if (stop == 0) return -1;
+    for (int i = 0; i < v->variants; ++i) {
+        const double* c = v->curvature + (size_t)i * S;
+        const double* t = v->thickness + (size_t)i * S;
+        const double* n_of = v->index + (size_t)i * S * L; /* column 0: n_of[s * L] */
+        double y1 = 1.0, u1 = 0.0, y2 = 0.0, u2 = 1.0, n = n_of[0];
+        for (int s = 1; s < stop; ++s) {
+            const double n2 = n_of[(size_t)s * L];
+            const double cs = v->type[s] == 2 ? c[s] : 0.0; /* spheres only */
+            const double phi = cs * (n2 - n);
+            u1 = (n * u1 - y1 * phi) / n2;
+            u2 = (n * u2 - y2 * phi) / n2;
+            y1 = y1 + t[s] * u1;
+            y2 = y2 + t[s] * u2;
+            n = n2;
+        }
+        pupil[i] = c[stop] / (y1 < 0.0 ? -y1 : y1);
+        thickness0[i] = -(y2 / y1);
+    }
+    return 0;
+}
+
 int64_t mko_port_rays_per_variant(const mkb_residual_plan* plan) {
     int64_t off = 0;
     for (int f = 0; f < plan->fields; ++f) off += (int64_t)plan->wavelengths * field_samples(plan, f);

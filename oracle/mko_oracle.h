@@ -17,6 +17,12 @@ extern "C" {
 
 int64_t mko_port_rays_per_variant(const mkb_residual_plan* plan);
 
+/* Paraxial ray aiming of an interior aperture stop (MKB_SURFACE_APERTURE_STOP; this build's
+ * own definition, the reference's stop is always surface 0): per variant the entrance pupil
+ * radius R / |y_A| and thickness[0] = -y_B / y_A from the y-u trace of wavelength column 0
+ * from surface 1 to the stop. Restated here as the checker of the packed records. */
+int mko_port_aim(const mkb_batch_view* view, double* pupil, double* thickness0);
+
 /* residuals_cpu (src/batch/batch_residuals.cpp:272): residuals [V][trace_rows],
  * opd [V][rays], status [V][rays] (opd, status may be NULL). */
 int mko_port_residuals(const mkb_batch_view* view, const mkb_residual_plan* plan,

@@ -142,6 +142,34 @@ class Port(_Oracle):
         self._check(rc, "fd_jacobian")
         return J, r0, ch
 
+    def aim(self, batch) -> tuple[np.ndarray, np.ndarray]:
+        """The entrance pupil of an interior aperture stop (mko_port_aim): radius [V] and
+        thickness[0] [V]."""
+        self.lib.mko_port_aim.argtypes = [_PB, C.c_void_p, C.c_void_p]
+        self.lib.mko_port_aim.restype = C.c_int
+        view = batch.view()
+        a = np.zeros(batch.variants)
+        t0 = np.zeros(batch.variants)
+        self._check(self.lib.mko_port_aim(C.byref(view), a.ctypes.data, t0.ctypes.data), "aim")
+        return a, t0
+
+    def aimed_equivalent(self, batch):
+        """The batch the reference traces like an aimed one: the interior stop as a plane,
+        surface 0 at the aimed entrance pupil."""
+        from mikroptim_b200.batch import BatchTopology, SURFACE_APERTURE_STOP, SURFACE_PLANE
+        import copy
+        a, t0 = self.aim(batch)
+        out = copy.deepcopy(batch)
+        kinds = [SURFACE_PLANE if k == SURFACE_APERTURE_STOP else k for k in batch.topology.type]
+        out.topology = BatchTopology(**{**batch.topology.__dict__, "type": kinds})
+        out.type = np.asarray(kinds, dtype=np.uint8)
+        out.pupil_radius = a
+        out.thickness = batch.thickness.copy()
+        out.thickness[:, 0] = t0
+        out.curvature = batch.curvature.copy()
+        out.curvature[:, batch.topology.stop_surface] = 0.0  # the stop's slot held R
+        return out
+
     def adjoint_jacobian(self, batch, layout, vs, x0, threads: int = 1):
         x0, runs, R, J, r0, view, plan, vars_ = self._jac_args(batch, layout, vs, x0)
         st = np.zeros((runs, layout.rays_per_variant), dtype=np.uint8)
