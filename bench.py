@@ -54,6 +54,11 @@ WORKLOAD_SINGLET = ("singlet-1024: 1024 biconvex singlets (stop plane + 2 sphere
 WORKLOAD_LM = ("objective-4096: 4096 runs x 15 surfaces, L=7, F=5, 16x32 pupil, P=32: 14 "
                "curvatures, 15 thicknesses and the first element's Buchdahl glass (n0, nu1, nu2) "
                "(config 2 shape)")
+WORKLOAD_LM_STOP = ("objective-4096: 4096 runs x 16 surfaces (15 of configuration 2 with its "
+                    "aperture stop inserted as table surface {stop}; the entrance pupil by "
+                    "paraxial ray aiming), L=7, F=5, 16x32 pupil, P={P}: 14 curvatures, 14 "
+                    "thicknesses (thickness[0] follows the pupil) and the first element's "
+                    "Buchdahl glass (config 2 shape)")
 FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of the reference)
 # DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) measured once per kernel on a
 # smaller capture of the same workload, per unit, scaled below by the units of the timed launch
@@ -75,6 +80,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="uneven", choices=["uneven", "lm", "merit", "tolerancing", "precision",
                              "singlet", "psf"])
+    ap.add_argument("--stop", type=int, default=8,
+                    help="--workload lm: table surface of the aperture stop inside the "
+                         "objective (paraxial ray aiming); 0: the stop at surface 0")
     ap.add_argument("--variants", type=int, default=None,
                     help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
                          "otherwise)")
@@ -486,6 +494,8 @@ def run_lm(args, world, rank, local):
     lib = _capi.lib()
     b, st, vs, x0 = workloads.objective(args.variants or 4096,
                                         seed=20261203 + 2 + 1000 * rank, glass=True)
+    if args.stop > 0:  # configuration 2's stop at surface 8: an aimed entrance pupil
+        b, st, vs, x0 = workloads.with_aperture_stop(b, st, vs, args.stop)
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
     runs = b.variants
@@ -596,7 +606,8 @@ def run_lm(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generator, configuration-2 shapes)",
-        "config": {"workload": WORKLOAD_LM,
+        "config": {"workload": WORKLOAD_LM if args.stop <= 0 else WORKLOAD_LM_STOP.format(
+                       stop=args.stop, P=P),
                    "step": "one batched LM cycle of all runs (CUDA graph)",
                    "runs_per_gpu": runs, "variables": P, "rays_per_run": lay.rays_per_variant,
                    "jacobian": "adjoint fused with FP64 tensor-core normal equations",
