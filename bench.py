@@ -355,8 +355,9 @@ def _lm_window(lm, steps: int, warmup: int, flush, world, dev, graph: bool = Tru
 
 
 def opd_errors(b, st, runs: int = 256):
-    """RMS / max OPD difference (waves at the reference wavelength) of the FP64-FMA and MIXED
-    traces against the bit-exact FP64 trace, over rays in the piston with the same status."""
+    """RMS / max OPD difference (waves at the reference wavelength) of the FP64-FMA, MIXED and
+    (coaxial batches without plates) FP32-bulk traces against the bit-exact FP64 trace, over
+    rays in the piston with the same status."""
     import torch
     from mikroptim_b200 import engine
     from mikroptim_b200.batch import ResidualLayout, in_piston
@@ -364,13 +365,17 @@ def opd_errors(b, st, runs: int = 256):
     lam_mm = sub.reference_wavelength_nm * 1e-6
     out = {}
     res = {}
-    for prec in (0, 2, 1):
+    bulk = not sub.topology.non_coaxial and sub.topology.ghost_plates == 0
+    precs = (0, 2, 1, 4) if bulk else (0, 2, 1)
+    for prec in precs:
         lay = ResidualLayout(sub.topology, dataclasses.replace(st, precision=prec))
         r = engine.residuals_device(engine.DeviceSystemBatch(sub), lay, sub)
         torch.cuda.synchronize()
         res[prec] = (r.opd.cpu().numpy(), r.status.cpu().numpy())
     ref_opd, ref_st = res[0]
-    for prec, name in ((2, "fp64_fma"), (1, "mixed")):
+    for prec, name in ((2, "fp64_fma"), (1, "mixed"), (4, "fp32_bulk")):
+        if prec not in res:
+            continue
         opd, stt = res[prec]
         same = (stt == ref_st) & in_piston(ref_st)
         clean = same & (ref_st == 0)
@@ -686,6 +691,16 @@ def run_uneven(args, world, rank, local):
     fma_value = world * iters_fma / (max_over_ranks(ms_fma, world, dev) * args.steps / 1e3)
     del lm_f
 
+    # ---- the same with the FP32-bulk forward (directions and refraction in FP32; positions,
+    # intersection and optical path in FP64) and the FP32 reverse sweep
+    from mikroptim_b200.batch import PRECISION_FP32_BULK
+    lay_bulk = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP32_BULK))
+    lm_b = engine.DeviceLm(db, lay_bulk, b, vss, opt, runs)
+    lm_b.start(x0)
+    ms_bulk, iters_bulk, _ = _lm_window(lm_b, args.steps, args.warmup, flush, world, dev)
+    bulk_value = world * iters_bulk / (max_over_ranks(ms_bulk, world, dev) * args.steps / 1e3)
+    del lm_b
+
     # ---- the same LM with paraxial constraints on the device (image at the paraxial focus,
     # working distance >= 1 mm, |Petzval curvature| <= 0.02 / mm; analytic adjoint rows): the
     # constrained cycle stays one graph-captured launch sequence
@@ -790,6 +805,12 @@ def run_uneven(args, world, rank, local):
         "ray_surface_hits_per_s": world * hits / (merit_ms / 1e3),
         "adjoint_fp64_fma": {"value": fma_value, "unit": "LM iterations/s",
                              "ms_per_cycle": ms_fma},
+        "adjoint_fp32_bulk": {"value": bulk_value, "unit": "LM iterations/s",
+                              "ms_per_cycle": ms_bulk,
+                              "precision": "FP32_BULK: forward with FP32 directions and "
+                                           "refraction (FP64 positions, intersection, optical "
+                                           "path), FP32 reverse sweep; its OPD error in "
+                                           "opd_error_vs_fp64.fp32_bulk"},
         "adjoint_mixed_paraxial_constraints": {
             "value": con_value, "unit": "LM iterations/s", "ms_per_cycle": ms_con,
             "launches_per_cycle": int(per_cycle_con),
@@ -1401,20 +1422,21 @@ def run_precision(args, world, rank, local):
         torch.cuda.synchronize()
         return sum(a.elapsed_time(c) for a, c in ts) / steps
 
-    from mikroptim_b200.batch import PRECISION_DF64
-    lays[PRECISION_DF64] = ResidualLayout(b.topology,
-                                          dataclasses.replace(st, precision=PRECISION_DF64))
+    from mikroptim_b200.batch import PRECISION_DF64, PRECISION_FP32_BULK
+    for extra in (PRECISION_DF64, PRECISION_FP32_BULK):
+        lays[extra] = ResidualLayout(b.topology, dataclasses.replace(st, precision=extra))
     l0 = lib.mkb_launch_count()
     with ClockSampler(local) as clocks:
         ms = {p: merit_ms(p, args.steps) for p in (PRECISION_FP64_FMA, PRECISION_FP64,
-                                                   PRECISION_MIXED, PRECISION_DF64)}
+                                                   PRECISION_MIXED, PRECISION_DF64,
+                                                   PRECISION_FP32_BULK)}
     launches = lib.mkb_launch_count() - l0
     ms = {p: max_over_ranks(v, world, dev) for p, v in ms.items()}
 
     # OPD errors over every ray, in tranches of variants
     lam_mm = b.reference_wavelength_nm * 1e-6
     acc = {PRECISION_FP64_FMA: [0.0, 0, 0.0, 0, 0], PRECISION_MIXED: [0.0, 0, 0.0, 0, 0],
-           PRECISION_DF64: [0.0, 0, 0.0, 0, 0]}
+           PRECISION_DF64: [0.0, 0, 0.0, 0, 0], PRECISION_FP32_BULK: [0.0, 0, 0.0, 0, 0]}
     chunk = 2048
     for first in range(0, V, chunk):
         n = min(chunk, V - first)
@@ -1422,7 +1444,7 @@ def run_precision(args, world, rank, local):
         dsub = engine.DeviceSystemBatch(sub, dev)
         ref = engine.residuals_device(dsub, lay0, sub)
         ok_ref = ((ref.status == 0) | (ref.status == 5) | (ref.status == 6))
-        for p in (PRECISION_FP64_FMA, PRECISION_MIXED, PRECISION_DF64):
+        for p in (PRECISION_FP64_FMA, PRECISION_MIXED, PRECISION_DF64, PRECISION_FP32_BULK):
             r = engine.residuals_device(dsub, lays[p], sub)
             same = (r.status == ref.status) & ok_ref
             err = ((r.opd - ref.opd) / lam_mm)[same]
@@ -1438,7 +1460,7 @@ def run_precision(args, world, rank, local):
                      "status_agreement": acc[p][3] / max(acc[p][4], 1),
                      "rays_compared": acc[p][1]}
               for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed"),
-                              (PRECISION_DF64, "df64"))}
+                              (PRECISION_DF64, "df64"), (PRECISION_FP32_BULK, "fp32_bulk"))}
 
     # normal equations: fused (FMA, MIXED) against the exact materialised J^T J on a sample
     sample = b.subset(0, 64)
@@ -1486,7 +1508,8 @@ def run_precision(args, world, rank, local):
                    "l2": "flushed (256 MB write) before every timed step"},
         "gpu_launches": int(launches),
         "merit_ms": {"fp64_fma": ms[PRECISION_FP64_FMA], "fp64_exact": ms[PRECISION_FP64],
-                     "mixed": ms[PRECISION_MIXED], "df64": ms[PRECISION_DF64]},
+                     "mixed": ms[PRECISION_MIXED], "df64": ms[PRECISION_DF64],
+                     "fp32_bulk": ms[PRECISION_FP32_BULK]},
         "df64_vs_fp64_fma_time": ms[PRECISION_DF64] / ms[PRECISION_FP64_FMA],
         "opd_error_vs_fp64": errors,
         "normal_equations_rel_error_vs_exact": jerr,

@@ -78,7 +78,15 @@ enum { MKB_STATUS_OK = 0, MKB_STATUS_MISSED = 1, MKB_STATUS_TIR = 2, MKB_STATUS_
  * equal within the reference's CPU/GPU tolerances). MIXED: the trace (OPL, piston, merit and
  * the ray states) as FP64_FMA, the adjoint reverse sweep in FP32 on those states. */
 enum { MKB_PRECISION_FP64 = 0, MKB_PRECISION_MIXED = 1, MKB_PRECISION_FP64_FMA = 2,
-       MKB_PRECISION_DF64 = 3 };
+       MKB_PRECISION_DF64 = 3, MKB_PRECISION_FP32_BULK = 4 };
+/* FP32_BULK (no counterpart in the reference): the trace with its directions and refraction in
+ * FP32 (normal, cos I, sqrt k, the refracted direction, renormalised to first order) and in
+ * FP64 only what stability needs -- the ray's position and the transfer to the tangent plane,
+ * the cancellation-safe sphere intersection s = H / (B + sqrt D), the optical path along the
+ * ray, the reference-sphere step and the tuple sums. RESIDUALS, MERIT and the optimiser (the
+ * fused adjoint's forward and the LM's trial MERIT; the reverse sweep in FP32 as in MIXED) of
+ * coaxial batches without ghost plates; its OPD error against FP64 is stated per workload (tens
+ * of nanowaves on singlet-style systems, far more on strongly aberrated ones). */
 /* DF64 (RESIDUALS and MERIT only): the reference's reduced-precision trace type
  * (include/mikroptim/math/df64.hpp:108): every per-ray operation in double-float arithmetic
  * (a pair of floats, about 48 bits) on the FP32 pipes, the tuple sums in FP64. */

@@ -31,6 +31,9 @@ SURFACE_STOP, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_GHOST_PLATE = 0, 1, 2, 3
 SURFACE_APERTURE_STOP = 4
 FAILURE_SOFT, FAILURE_HARD = 0, 1
 PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA, PRECISION_DF64 = 0, 1, 2, 3
+# directions and refraction in FP32, positions, intersection and optical path in FP64
+# (MKB_PRECISION_FP32_BULK; coaxial batches without ghost plates)
+PRECISION_FP32_BULK = 4
 VAR_CURVATURE, VAR_THICKNESS, VAR_WORKING_DISTANCE, VAR_GHOST_COEFFICIENT, VAR_GLASS = 0, 1, 2, 3, 4
 BUCHDAHL_LAMBDA0_UM, BUCHDAHL_ALPHA = 0.546074, 2.5  # glass/dispersion.hpp:13,15
 MAX_GHOST_PLATES, MAX_GHOST_TERMS = 16, 32
@@ -379,7 +382,7 @@ class ResidualLayout:
         if not (settings.fail_weight >= 0 and math.isfinite(settings.fail_weight)):
             raise ValueError("ResidualLayout: fail_weight must be finite and >= 0")
         if settings.precision not in (PRECISION_FP64, PRECISION_MIXED, PRECISION_FP64_FMA,
-                                      PRECISION_DF64):
+                                      PRECISION_DF64, PRECISION_FP32_BULK):
             raise ValueError("ResidualLayout: unknown precision")
         if not (settings.transverse_weight >= 0 and math.isfinite(settings.transverse_weight)):
             raise ValueError("ResidualLayout: transverse_weight must be finite and >= 0")

@@ -657,6 +657,87 @@ __device__ void fused_forward(const TraceParams& p, const double* rec, const dou
     penalty = value_of(soft.penalty);
 }
 
+// fused_forward in MKB_PRECISION_FP32_BULK (coaxial, no ghost plates): the same kept states and
+// step quantities (float slots), traced with step_surface_bulk.
+template <class Q>
+__device__ void fused_forward_bulk(const TraceParams& p, const double* rec, const double* mu_tab,
+                                   const RecordLayout& lay, int S, int f, int l,
+                                   const Sample& smp, bool soft_mode, Q* ck, int stride_ck,
+                                   uint64_t& br_lo, uint64_t& br_hi, int& count,
+                                   int& image_branch, int& status_out, int& soft_first,
+                                   double& opl, double& penalty) {
+    const int L = p.L;
+    const double a = rec[lay.pupil];
+    const double st = rec[lay.sin_theta + f];
+    const double ct = rec[lay.cos_theta + f];
+    const double r0 = a * smp.rho;
+    RayBulk r;
+    r.px = r0 * smp.sin_phi;
+    r.py = r0 * smp.cos_phi;
+    r.pz = 0.0;
+    r.dx = 0.0f;
+    r.dy = static_cast<float>(st);
+    r.dz = static_cast<float>(ct);
+    r.opl = r.py * st;
+    SoftT<double> soft{0.0, kOk};
+    SoftT<double>* sp = soft_mode ? &soft : nullptr;
+    br_lo = br_hi = 0;
+    count = 1;
+    image_branch = kBranchRegular;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    double n_before = idx[l];
+    auto keep_state = [&](Q* q) {
+        q[0] = Q(r.px);
+        q[1 * kFusedThreads] = Q(r.py);
+        q[2 * kFusedThreads] = Q(r.pz);
+        q[3 * kFusedThreads] = Q(r.dx);
+        q[4 * kFusedThreads] = Q(r.dy);
+        q[5 * kFusedThreads] = Q(r.dz);
+    };
+    for (int s = 1; s < S; ++s) {
+        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        Q* q = ck + (s - 1) * stride_ck;
+        keep_state(q);
+        int branch;
+        StepLocal<float> loc{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        status = step_surface_bulk<true>(r, thick[s - 1], c, n_before,
+                                         static_cast<float>(mu_tab[s * L + l]), sp, branch, &loc);
+        if (status != kOk) break;
+        q[6 * kFusedThreads] = Q(loc.s0);
+        q[7 * kFusedThreads] = Q(loc.s);
+        q[8 * kFusedThreads] = Q(loc.root_d);
+        q[9 * kFusedThreads] = Q(loc.root_k);
+        count = s + 1;
+        if (s < 32) br_lo |= static_cast<uint64_t>(branch) << (2 * s);
+        else br_hi |= static_cast<uint64_t>(branch) << (2 * (s - 32));
+        n_before = idx[s * L + l];
+    }
+    if (count == S) keep_state(ck + (S - 1) * stride_ck);
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > 0.0f)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step_bulk(r, rec[lay.target + f], thick[S - 1], n_before,
+                                                sp, branch);
+            if (!in_piston(rst)) {
+                status = rst;
+            } else {
+                image_branch = branch;
+                if (status == kOk) status = rst;
+            }
+        }
+    }
+    status_out = status;
+    soft_first = soft.first;
+    opl = r.opl;
+    penalty = soft.penalty;
+}
+
 // Reverse sweep with K adjoint vectors (seed k: OPL seed so[k], penalty seed sp[k]) writing
 // factor_k * dPhi_k/dx into sinks.row[k][col * ld_k]. The states and the step-local
 // quantities are in N, the adjoint arithmetic in A (N, or float for the mixed precision). One
@@ -847,6 +928,9 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
 // (an FP32 trace of the rays themselves misses the OPD bar on aberrated systems; the Jacobian
 // tolerates single-precision rounding).
 struct MixedPrecision {};
+// FP32_BULK: as MIXED, with the forward traced by step_surface_bulk (directions and refraction
+// in FP32, positions, intersection and optical path in FP64)
+struct BulkPrecision {};
 
 // number types per kernel variant: the forward trace (Fwd), the kept states and the
 // quantities the reverse sweep recomputes from them (Bwd), the adjoint arithmetic (Adj), the
@@ -866,6 +950,7 @@ template <> struct FusedTypes<MixedPrecision> {
     using Keep = float;
     using Row = float;
 };
+template <> struct FusedTypes<BulkPrecision> : FusedTypes<MixedPrecision> {};
 
 template <class N, int K, int kFeat>
 __device__ __forceinline__ void run_backward(const TraceParams& p, const VarParams& v,
@@ -909,7 +994,10 @@ struct FusedArgs {
 };
 
 template <class N, int kFeat>
-__global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ? 4 : kFusedMinBlocks)
+__global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ||
+                                                           std::is_same<N, BulkPrecision>::value
+                                                       ? 4
+                                                       : kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
     __shared__ FusedShared sh;
@@ -1015,7 +1103,12 @@ adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
                 int soft_first = kOk, count = 0, image_branch = 0;
                 uint64_t br_lo = 0, br_hi = 0;
                 double opl = 0.0, penalty = 0.0;
-                fused_forward<typename FusedTypes<N>::Fwd, Keep, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
+                if constexpr (std::is_same<N, BulkPrecision>::value)
+                    fused_forward_bulk<Keep>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
+                                             my_ck, stride_ck, br_lo, br_hi, count,
+                                             image_branch, status, soft_first, opl, penalty);
+                else
+                    fused_forward<typename FusedTypes<N>::Fwd, Keep, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode,
                                                            my_ck, stride_ck, br_lo, br_hi, count,
                                                            image_branch, status, soft_first, opl,
                                                            penalty);
@@ -1259,8 +1352,13 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     fa.vt = rv.table;
     fa.p_max = p_max;
     fa.gram_stride = static_cast<int64_t>(p_all + 1) * (p_all + 1);
-    const size_t smem = fused_adjoint_smem(
-        tp, p_max, precision == MKB_PRECISION_MIXED ? sizeof(float) : sizeof(double));
+    const bool float_rows =
+        precision == MKB_PRECISION_MIXED || precision == MKB_PRECISION_FP32_BULK;
+    const size_t smem = fused_adjoint_smem(tp, p_max, float_rows ? sizeof(float) : sizeof(double));
+    if (precision == MKB_PRECISION_FP32_BULK && (tp.non_coaxial || tp.G > 0)) {
+        set_error("fused adjoint: FP32_BULK is built for coaxial batches without ghost plates");
+        return MKB_ERR_UNSUPPORTED;
+    }
     // kernel variant per precision and features (1: surface transforms, 2: ghost plates,
     // 4: glass variables of some run)
     const bool glass = vp.has_glass != 0 || rv.any_glass != 0;
@@ -1283,8 +1381,18 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
         default: return adjoint_gram_kernel<N, 7>;
         }
     };
+    // FP32_BULK: coaxial without plates only (features 0, 4, 8, 12)
+    auto pick_bulk = [&]() -> Fn {
+        switch (feat) {
+        case 4: return adjoint_gram_kernel<BulkPrecision, 4>;
+        case 8: return adjoint_gram_kernel<BulkPrecision, 8>;
+        case 12: return adjoint_gram_kernel<BulkPrecision, 12>;
+        default: return adjoint_gram_kernel<BulkPrecision, 0>;
+        }
+    };
     const Fn kernel = precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
                       : precision == MKB_PRECISION_MIXED ? pick(TypeTag<MixedPrecision>{})
+                      : precision == MKB_PRECISION_FP32_BULK ? pick_bulk()
                                                          : pick(TypeTag<double>{});
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));

@@ -646,7 +646,8 @@ int options_vpc(const mkb_trace_options* options, TraceParams* p) {
 
 int check_trace_precision(int precision, const char* what) {
     if (precision != MKB_PRECISION_FP64 && precision != MKB_PRECISION_FP64_FMA &&
-        precision != MKB_PRECISION_MIXED && precision != MKB_PRECISION_DF64) {
+        precision != MKB_PRECISION_MIXED && precision != MKB_PRECISION_DF64 &&
+        precision != MKB_PRECISION_FP32_BULK) {
         set_error("%s: precision %d not available", what, precision);
         return MKB_ERR_UNSUPPORTED;
     }

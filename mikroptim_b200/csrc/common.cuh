@@ -744,6 +744,107 @@ __device__ __forceinline__ int reference_step(RayT<N>& r, N h, N w, N n_image, S
     return kOk;
 }
 
+// ---- FP32-bulk trace (MKB_PRECISION_FP32_BULK) -------------------------------------------------
+// The ray's position, its optical path and the steps that need FP64 for stability in double;
+// its direction and the refraction in float. Same formulas and branches as step_surface_mu.
+struct RayBulk {
+    double px, py, pz;
+    float dx, dy, dz;
+    double opl;
+};
+
+// kKeep: the step's quantities for the reverse sweep (s0, s, sqrt D, sqrt k; mu is the
+// caller's), rounded to float as the MIXED sweep keeps them.
+template <bool kKeep = false>
+__device__ __forceinline__ int step_surface_bulk(RayBulk& r, double t, double c, double n_before,
+                                                 float mu, SoftT<double>* soft, int& branch,
+                                                 StepLocal<float>* keep = nullptr) {
+    if (!(r.dz > 0.0f)) return kBackward;
+    // transfer to the tangent plane (FP64: the point must land on z = 0)
+    r.pz -= t;
+    const double dxd = r.dx, dyd = r.dy, dzd = r.dz;
+    const double s0 = -r.pz / dzd;
+    if constexpr (kKeep) keep->s0 = static_cast<float>(s0);
+    r.px = r.px + s0 * dxd;
+    r.py = r.py + s0 * dyd;
+    r.pz = 0.0;
+    // the cancellation-safe intersection with the sphere (FP64)
+    const double H = c * (r.px * r.px + r.py * r.py);
+    const double B = dzd - c * (r.px * dxd + r.py * dyd);
+    const double D = B * B - c * H;
+    double s;
+    bool missed = false;
+    if (D < 0.0) {
+        if (soft == nullptr || (!(c > 0.0) && !(c < 0.0))) return kMissed;
+        soft->add(-D, kSoftMissed);
+        s = B / c;
+        missed = true;
+        if constexpr (kKeep) keep->root_d = 0.0f;
+    } else {
+        const double root_d = sqrt(D);
+        const double denom = B + root_d;
+        if (!(denom > 0.0)) return kMissed;
+        s = H / denom;
+        if constexpr (kKeep) keep->root_d = static_cast<float>(root_d);
+    }
+    if constexpr (kKeep) keep->s = static_cast<float>(s);
+    r.px = r.px + s * dxd;
+    r.py = r.py + s * dyd;
+    r.pz = r.pz + s * dzd;
+    r.opl += n_before * (s0 + s);
+    // refraction in FP32, mu = n / n'
+    const float cf = static_cast<float>(c);
+    float nx = -cf * static_cast<float>(r.px), ny = -cf * static_cast<float>(r.py);
+    float nz = 1.0f - cf * static_cast<float>(r.pz);
+    if (missed) {
+        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        nx *= inv;
+        ny *= inv;
+        nz *= inv;
+    }
+    const float cos_i = r.dx * nx + r.dy * ny + r.dz * nz;
+    const float k = 1.0f - mu * mu * (1.0f - cos_i * cos_i);
+    branch = missed ? kBranchSoftMissed : kBranchRegular;
+    float ex, ey, ez;
+    if (k < 0.0f) {
+        if (soft == nullptr) return kTir;
+        soft->add(-static_cast<double>(k), kSoftTir);
+        if constexpr (kKeep) keep->root_k = 0.0f;
+        ex = r.dx - cos_i * nx;
+        ey = r.dy - cos_i * ny;
+        ez = r.dz - cos_i * nz;
+        branch |= kBranchSoftTir;
+    } else {
+        const float root_k = sqrtf(k);
+        if constexpr (kKeep) keep->root_k = root_k;
+        const float a = root_k - mu * cos_i;
+        ex = mu * r.dx + a * nx;
+        ey = mu * r.dy + a * ny;
+        ez = mu * r.dz + a * nz;
+    }
+    // unit length: one Newton step of 1 / |e| from 1 (|e| = 1 up to float rounding after a
+    // refraction; the TIR tangent needs the full normalisation)
+    const float e2 = ex * ex + ey * ey + ez * ez;
+    const float inv = k < 0.0f ? rsqrtf(e2) : 1.5f - 0.5f * e2;
+    r.dx = inv * ex;
+    r.dy = inv * ey;
+    r.dz = inv * ez;
+    return kOk;
+}
+
+// reference_step with the float direction (FP64 arithmetic).
+__device__ __forceinline__ int reference_step_bulk(RayBulk& r, double h, double w,
+                                                   double n_image, SoftT<double>* soft,
+                                                   int& branch) {
+    RayT<double> q{r.px, r.py, r.pz, r.dx, r.dy, r.dz, r.opl};
+    const int st = reference_step<double>(q, h, w, n_image, soft, branch);
+    r.px = q.px;
+    r.py = q.py;
+    r.pz = q.pz;
+    r.opl = q.opl;
+    return st;
+}
+
 // ---- optimiser variables (VariableSet, reference include/mikroptim/optim/variable_set.hpp:63)
 struct VarParams {
     int P;

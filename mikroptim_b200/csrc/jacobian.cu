@@ -292,7 +292,7 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
     rc = make_trace_params(&b, plan, pack_rays_default(), &tp);
     if (rc != MKB_OK) return rc;
     if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
-        plan->precision != MKB_PRECISION_MIXED) {
+        plan->precision != MKB_PRECISION_MIXED && plan->precision != MKB_PRECISION_FP32_BULK) {
         set_error("adjoint normal equations: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }

@@ -624,7 +624,7 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     int rc = make_trace_params(&b, plan, pack_rays_default(), &s.tp);
     if (rc != MKB_OK) return rc;
     if (plan->precision != MKB_PRECISION_FP64 && plan->precision != MKB_PRECISION_FP64_FMA &&
-        plan->precision != MKB_PRECISION_MIXED) {
+        plan->precision != MKB_PRECISION_MIXED && plan->precision != MKB_PRECISION_FP32_BULK) {
         set_error("lm: precision %d not available", plan->precision);
         return MKB_ERR_UNSUPPORTED;
     }
@@ -672,7 +672,8 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     s.precision = plan->precision;
     s.gram_exact = o.gram_exact != 0;
     s.fused = !s.fd && !s.gram_exact;
-    if (plan->precision == MKB_PRECISION_MIXED && !s.fused) {
+    if ((plan->precision == MKB_PRECISION_MIXED || plan->precision == MKB_PRECISION_FP32_BULK) &&
+        !s.fused) {
         set_error("lm: mixed precision runs with the fused adjoint (jacobian = adjoint, "
                   "gram_exact = 0)");
         return MKB_ERR_UNSUPPORTED;

@@ -128,6 +128,57 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
     return status;
 }
 
+// trace_ray in MKB_PRECISION_FP32_BULK (coaxial, no ghost plates): the start ray and the
+// surface loop with step_surface_bulk, the reference sphere in FP64.
+__device__ inline int trace_ray_bulk(const TraceParams& p, const double* rec, const double* mu_tab,
+                                     const RecordLayout& lay, int S, int f, int l,
+                                     const Sample& smp, bool soft_mode, double& opl,
+                                     double& penalty) {
+    const int L = p.L;
+    const double a = rec[lay.pupil];
+    const double st = rec[lay.sin_theta + f];
+    const double ct = rec[lay.cos_theta + f];
+    const double r0 = a * smp.rho;
+    RayBulk r;
+    r.px = r0 * smp.sin_phi;
+    r.py = r0 * smp.cos_phi;
+    r.pz = 0.0;
+    r.dx = 0.0f;
+    r.dy = static_cast<float>(st);
+    r.dz = static_cast<float>(ct);
+    r.opl = r.py * st;  // p . d with p_z = d_x = 0 (the exact start direction)
+    SoftT<double> soft{0.0, kOk};
+    SoftT<double>* sp = soft_mode ? &soft : nullptr;
+    int status = kOk;
+    const double* curv = rec + lay.curvature;
+    const double* thick = rec + lay.thickness;
+    const double* idx = rec + lay.index;
+    double n_before = idx[l];
+    for (int s = 1; s < S; ++s) {
+        const double c = p.type[s] == MKB_SURFACE_SPHERE ? curv[s] : 0.0;
+        int branch;
+        status = step_surface_bulk(r, thick[s - 1], c, n_before,
+                                   static_cast<float>(mu_tab[s * L + l]), sp, branch);
+        if (status != kOk) break;
+        n_before = idx[s * L + l];
+    }
+    if (status == kOk && soft_mode) status = soft.first;
+    if (in_piston(status)) {
+        if (!(r.dz > 0.0f)) {
+            status = kBackward;
+        } else {
+            int branch;
+            const int rst = reference_step_bulk(r, rec[lay.target + f], thick[S - 1], n_before,
+                                                sp, branch);
+            if (!in_piston(rst)) status = rst;
+            else if (status == kOk) status = rst;
+        }
+    }
+    opl = r.opl;
+    penalty = soft.penalty;
+    return status;
+}
+
 __device__ inline double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -282,6 +333,8 @@ trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ r
                     if (hsq[q] == hsq[q]) atomicMax(&ext_sh[2 * q], order_key(hsq[q]));
                     if (cosi[q] == cosi[q]) atomicMin(&ext_sh[2 * q + 1], order_key(cosi[q]));
                 }
+        } else if constexpr (kPrecision == MKB_PRECISION_FP32_BULK) {
+            st = trace_ray_bulk(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl, pen);
         } else {
             st = trace_ray<N, kFeat>(p, record, mu_tab, lay, S, f, l, smp, soft_mode, opl, pen);
         }
@@ -510,8 +563,8 @@ template <bool kResiduals>
 int launch_transverse(const TraceParams& p, const double* records, const TupleOut& out,
                       int precision, cudaStream_t stream) {
     if (!p.transverse || p.V == 0) return MKB_OK;
-    if (precision == MKB_PRECISION_DF64) {
-        set_error("transverse rows: not built for DF64");
+    if (precision == MKB_PRECISION_DF64 || precision == MKB_PRECISION_FP32_BULK) {
+        set_error("transverse rows: not built for DF64 or FP32_BULK");
         return MKB_ERR_UNSUPPORTED;
     }
     int max_n = 0;
@@ -602,7 +655,9 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
     TraceParams p = p_in;
     // several variants per CTA: built for coaxial batches without ghost plates in FP64; the
     // others trace one variant per CTA (the option only shapes the launch)
-    if (p.non_coaxial || p.G > 0 || precision == MKB_PRECISION_DF64) p.vpc = 1;
+    if (p.non_coaxial || p.G > 0 || precision == MKB_PRECISION_DF64 ||
+        precision == MKB_PRECISION_FP32_BULK)
+        p.vpc = 1;
     const int64_t groups = (static_cast<int64_t>(p.V) + p.vpc - 1) / p.vpc;
     const unsigned blocks = static_cast<unsigned>(groups * p.n_packs);
     const size_t smem = trace_smem(p, precision == MKB_PRECISION_FP64);
@@ -610,7 +665,14 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
     const int feat = (p.non_coaxial ? 1 : 0) | (p.G > 0 ? 2 : 0);
     constexpr int E = MKB_PRECISION_FP64, F = MKB_PRECISION_FP64_FMA;
     constexpr int D = MKB_PRECISION_DF64;
-    auto kernel = p.vpc > 1 ? (precision == MKB_PRECISION_FP64
+    constexpr int B = MKB_PRECISION_FP32_BULK;
+    if (precision == B && (feat != 0 || out.extrema != nullptr)) {
+        set_error("trace: FP32_BULK is built for coaxial batches without ghost plates or "
+                  "extrema");
+        return MKB_ERR_UNSUPPORTED;
+    }
+    auto kernel = precision == B ? trace_kernel<kResiduals, B, 0>
+                  : p.vpc > 1 ? (precision == MKB_PRECISION_FP64
                                    ? trace_kernel<kResiduals, E, 0, false, true>
                                    : trace_kernel<kResiduals, F, 0, false, true>)
                   : precision == MKB_PRECISION_DF64

@@ -37,7 +37,7 @@ enum class SurfaceKind : uint8_t { Stop = 0, Plane = 1, Sphere = 2, GhostPlate =
                                    ApertureStop = 4 };
 enum class PupilMode : uint8_t { Half = 0, Full = 1, Axis = 2 };
 enum class FailureMode : int32_t { Soft = 0, Hard = 1 };
-enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2, DF64 = 3 };
+enum class Precision : int32_t { FP64 = 0, Mixed = 1, FP64_FMA = 2, DF64 = 3, FP32_Bulk = 4 };
 enum class VariableType : int32_t { Curvature = 0, Thickness = 1, WorkingDistance = 2,
                                     GhostCoefficient = 3, Glass = 4 };
 enum class JacobianMethod : int32_t { FiniteDifference = 0, Adjoint = 1 };

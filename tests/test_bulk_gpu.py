@@ -1,0 +1,81 @@
+"""FP32_BULK: the trace with its directions and refraction in FP32 and in FP64 only the ray's
+position, the cancellation-safe sphere intersection, the optical path and the reference-sphere
+step (the split the optimiser's mixed mode was specified with). Measured against the bit-exact
+FP64 trace on one B200 it misses the 1e-4 wave OPD bar of the optimiser -- the FP32 direction
+carries a tilt of ~1e-7 rad into the wavefront, 1.6e-4 to 3e-4 waves RMS on singlet-style
+systems and far more on strongly aberrated objectives -- and is no faster than FP64_FMA (the
+divisions and roots it keeps dominate the step), so MIXED stays the optimiser's mode. The
+stated tolerances here hold that measurement: OPD RMS <= 1e-3 waves and every status equal on
+singlet-style and uneven systems, merit within 1e-4 relative, the fused normal equations within
+the MIXED bars, and the LM with it lowers every run's merit."""
+
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from mikroptim_b200 import engine, workloads
+from mikroptim_b200.batch import (PRECISION_FP32_BULK, PRECISION_FP64, PRECISION_FP64_FMA,
+                                  ResidualLayout)
+
+pytestmark = pytest.mark.gpu
+
+
+def traced(b, st, precision):
+    lay = ResidualLayout(b.topology, dataclasses.replace(st, precision=precision))
+    db = engine.DeviceSystemBatch(b)
+    r = engine.residuals_device(db, lay, b)
+    m = engine.merit_device(db, lay, b)
+    torch.cuda.synchronize()
+    return r.opd.cpu().numpy(), r.status.cpu().numpy(), m.merit.cpu().numpy()
+
+
+@pytest.mark.parametrize("make", [lambda: workloads.singlet(128), lambda: workloads.sweep(16),
+                                  lambda: workloads.uneven(64)])
+def test_bulk_trace_within_its_stated_tolerance(make):
+    b, st, _, _ = make()
+    lam = b.reference_wavelength_nm * 1e-6
+    o0, s0, m0 = traced(b, st, PRECISION_FP64)
+    o, s, m = traced(b, st, PRECISION_FP32_BULK)
+    assert np.array_equal(s, s0)
+    ok = (s0 == 0) | (s0 == 5) | (s0 == 6)
+    err = (o - o0)[ok] / lam
+    assert np.sqrt(np.mean(err ** 2)) <= 1e-3 and np.abs(err).max() <= 5e-3
+    assert np.median(np.abs(m - m0) / np.abs(m0)) <= 1e-4
+
+
+def test_bulk_fused_normal_equations_within_the_mixed_bars():
+    b, st, vs, x0 = workloads.singlet(64)
+    lay = ResidualLayout(b.topology, st)
+    db = engine.DeviceSystemBatch(b)
+    J, r0, _ = engine.adjoint_jacobian_device(db, lay, b, vs, x0)
+    ref = engine.normal_equations_device(J, r0, True).cpu().numpy()
+    lb = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP32_BULK))
+    got = engine.adjoint_normal_equations_device(db, lb, b, vs, x0).cpu().numpy()
+    d = np.abs(np.diagonal(ref, axis1=1, axis2=2))
+    d = np.maximum(d, 1e-20 * d.max(axis=1, keepdims=True) + 1e-300)
+    err = np.abs(got - ref) / np.sqrt(d[:, :, None] * d[:, None, :])
+    assert np.median(err) <= 1e-4 and err.max() <= 1e-3, (np.median(err), err.max())
+
+
+def test_bulk_lm_lowers_every_merit():
+    b, st, vs, x0 = workloads.singlet(32)
+    lay = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP32_BULK))
+    opt = engine.LmOptions(max_iterations=20, jacobian=engine.JACOBIAN_ADJOINT,
+                           gram_exact=False, fail_weight_factor=1.0)
+    out = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
+    fma = engine.optimize_lm_gpu(b, ResidualLayout(b.topology, dataclasses.replace(
+        st, precision=PRECISION_FP64_FMA)), vs, x0, opt)
+    assert np.all(out["merit"] <= out["history"][:, 0])
+    # the bulk merit is the FP64 one up to its own error; both end near the same optimum
+    assert np.median(np.abs(np.log(out["merit"] / fma["merit"]))) <= 0.05
+
+
+def test_bulk_refuses_plates_and_tilts():
+    for make in (lambda: workloads.ghost(4), lambda: workloads.tolerancing(4, elements=2,
+                                                                            rings=4, spokes=8)):
+        b, st, _, _ = make()
+        lay = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP32_BULK))
+        with pytest.raises(NotImplementedError):
+            engine.residuals_device(engine.DeviceSystemBatch(b), lay, b)
