@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import math
 from dataclasses import dataclass
 import enum
 
@@ -1361,13 +1362,29 @@ class DeviceLm:
             return 0.0
         return self._sum_squares(self._evaluate(i, x_row[:self._var_set(i).size]))
 
-    def _points_extrema(self, pts) -> tuple[SystemBatchHost, np.ndarray]:
+    def _points_extrema(self, pts, invalid=None) -> tuple[SystemBatchHost, np.ndarray]:
         """The batch of the points [(run, y)] and their extrema [n][S][2] from one MERIT trace
-        (FD points and trial points alike)."""
+        (FD points and trial points alike). A point whose system is not valid (a glass step
+        that drives an index to <= 0, say) is traced at its template instead and marked in
+        `invalid` (a bool array the caller passes), so one bad trial point cannot stop the
+        batch."""
         multi = self.host.take([self._template(i) for i, _ in pts])
+        keep = self.host.take([self._template(i) for i, _ in pts])
         for j, (i, y) in enumerate(pts):
             vs = self._var_set(i)
             vs.apply(multi, j, np.asarray(y[:vs.size], dtype=np.float64))
+        bad = ~np.all(multi.index.reshape(len(pts), -1) > 0, axis=1)
+        bad |= ~np.all(np.isfinite(multi.curvature) & np.isfinite(multi.thickness), axis=1)
+        if np.any(bad):
+            for name in ("curvature", "thickness", "index", "pupil_radius"):
+                getattr(multi, name)[bad] = getattr(keep, name)[bad]
+            if multi.buchdahl_coeff is not None:
+                multi.buchdahl_coeff[bad] = keep.buchdahl_coeff[bad]
+        if invalid is not None:
+            invalid[:] = bad
+        elif np.any(bad):
+            raise ValueError("LM: a difference point of the trace-dependent rows is not a valid "
+                             "system")
         eng = self.__dict__.setdefault("_engine", TraceEngine(self.templates.device.index or 0))
         out = eng.run(multi, TraceMode.MERIT, TraceSettings(self.layout.settings, extrema=True))
         return multi, out.merit.extrema
@@ -1381,8 +1398,11 @@ class DeviceLm:
         """sum_i t_i^2 at the points [(run, y)] (trace_extra_merit)."""
         if not pts:
             return np.zeros(0)
-        multi, ext = self._points_extrema(pts)
-        return np.array([self._sum_squares(self._trace_values(multi, ext, j))
+        invalid = np.zeros(len(pts), dtype=bool)
+        multi, ext = self._points_extrema(pts, invalid)
+        # an invalid trial point gets an infinite merit: the LM rejects the step
+        return np.array([math.inf if invalid[j] else
+                         self._sum_squares(self._trace_values(multi, ext, j))
                          for j in range(len(pts))])
 
     def _extra_jacobian(self, i: int, x_row) -> tuple[np.ndarray, np.ndarray]:
