@@ -1467,7 +1467,15 @@ def run_precision(args, world, rank, local):
     ds = engine.DeviceSystemBatch(sample, dev)
     J, r0, _ = engine.adjoint_jacobian_device(ds, lay0, sample, vs, x0[:64])
     exact = engine.normal_equations_device(J, r0, True)
-    del J
+    # Jacobian entries: the contracted adjoint J against the bit-exact one, each entry relative
+    # to its column's largest entry (the precisions whose J is materialised)
+    Jf, _, _ = engine.adjoint_jacobian_device(ds, lays[PRECISION_FP64_FMA], sample, vs, x0[:64])
+    colmax = J.abs().amax(dim=2, keepdim=True).clamp_min(1e-300)
+    jrel = ((Jf - J).abs() / colmax)
+    jac_entries = {"fp64_fma": {"median": float(jrel.median()), "max": float(jrel.max()),
+                                "entries": int(jrel.numel()),
+                                "relative_to": "the largest entry of the column"}}
+    del J, Jf, jrel
     jerr = {}
     for p, name in ((PRECISION_FP64_FMA, "fp64_fma"), (PRECISION_MIXED, "mixed")):
         g = engine.adjoint_normal_equations_device(ds, lays[p], sample, vs, x0[:64])
@@ -1513,6 +1521,7 @@ def run_precision(args, world, rank, local):
         "df64_vs_fp64_fma_time": ms[PRECISION_DF64] / ms[PRECISION_FP64_FMA],
         "opd_error_vs_fp64": errors,
         "normal_equations_rel_error_vs_exact": jerr,
+        "jacobian_entry_rel_error_vs_exact": jac_entries,
         "intercept_error_vs_fp64": intercepts,
         "e2e": None,
         "clocks": clocks.summary(),
