@@ -112,25 +112,37 @@ struct FromShared {
     __device__ double2 operator()(int, int) const { return make_double2(0.0, 0.0); }
 };
 
-// The whole transform; the first pass takes its inputs from load (kFirst) or shared memory.
+// The whole transform in passes of at most kPassStages radix-2 stages (2^kPassStages values
+// per thread in registers); the first pass takes its inputs from load (kFirst) or shared memory.
+constexpr int kPassStages = 3;
+
+template <bool kFirst, class Load>
+__device__ __forceinline__ void fft_pass_n(int n, double2* a, int M, int count, int s,
+                                           const double2* tw, const Load& load) {
+    switch (n) {
+    case 1: fft_pass<1, kFirst>(a, M, count, s, tw, load); break;
+    case 2: fft_pass<2, kFirst>(a, M, count, s, tw, load); break;
+    default:
+        if constexpr (kPassStages >= 4) {
+            if (n == 4) {
+                fft_pass<(kPassStages >= 4 ? 4 : 3), kFirst>(a, M, count, s, tw, load);
+                break;
+            }
+        }
+        fft_pass<3, kFirst>(a, M, count, s, tw, load);
+        break;
+    }
+}
+
 template <bool kFirst, class Load>
 __device__ void fft_shared(double2* a, int M, int log_m, int count, const double2* tw,
                            const Load& load) {
-    switch (log_m < 4 ? log_m : 4) {
-    case 1: fft_pass<1, kFirst>(a, M, count, 0, tw, load); break;
-    case 2: fft_pass<2, kFirst>(a, M, count, 0, tw, load); break;
-    case 3: fft_pass<3, kFirst>(a, M, count, 0, tw, load); break;
-    default: fft_pass<4, kFirst>(a, M, count, 0, tw, load); break;
-    }
+    const int n0 = log_m < kPassStages ? log_m : kPassStages;
+    if (n0 > 0) fft_pass_n<kFirst>(n0, a, M, count, 0, tw, load);
     const FromShared none;
-    for (int s = 4; s < log_m; s += 4) {
-        switch (log_m - s < 4 ? log_m - s : 4) {
-        case 1: fft_pass<1, false>(a, M, count, s, tw, none); break;
-        case 2: fft_pass<2, false>(a, M, count, s, tw, none); break;
-        case 3: fft_pass<3, false>(a, M, count, s, tw, none); break;
-        default: fft_pass<4, false>(a, M, count, s, tw, none); break;
-        }
-    }
+    for (int s = n0; s < log_m; s += kPassStages)
+        fft_pass_n<false>(log_m - s < kPassStages ? log_m - s : kPassStages, a, M, count, s, tw,
+                          none);
 }
 
 // the twiddle table into shared memory (read by every butterfly)
@@ -151,7 +163,7 @@ __global__ void psf_twiddle_kernel(double2* tw, int M) {
 // column-major per tuple, spec[t][q][j], so that the column pass reads each column's N values
 // contiguously.
 template <int kRows>
-__global__ void __launch_bounds__(kPsfThreads, 2) psf_rows_kernel(const PsfArgs a) {
+__global__ void __launch_bounds__(kPsfThreads, 3) psf_rows_kernel(const PsfArgs a) {
     extern __shared__ double2 sm[];
     const int per_t = (a.N + kRows - 1) / kRows;
     const int t = blockIdx.x / per_t;
@@ -188,7 +200,7 @@ __global__ void __launch_bounds__(kPsfThreads, 2) psf_rows_kernel(const PsfArgs 
 // Columns [q0, q0 + C) of tuple t (C = kCols): transform along y, then one pass over the
 // result for the intensity, the centred PSF and the two projections.
 template <int kCols>
-__global__ void __launch_bounds__(kPsfThreads, 2) psf_cols_kernel(const PsfArgs a) {
+__global__ void __launch_bounds__(kPsfThreads, 3) psf_cols_kernel(const PsfArgs a) {
     constexpr int C = kCols;
     extern __shared__ double2 sm[];
     __shared__ double wsum[kPsfThreads / 32][C];
