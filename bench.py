@@ -68,9 +68,10 @@ TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
 # adjoint_gram_kernel, objective runs with a glass variable, FP64_FMA (1,184 runs captured:
 # 1.941 GB read, 17.645 GB written)
 FUSED_TRAFFIC_BYTES_PER_RUN = (1.940772e9 + 17.644780e9) / 1184
-# adjoint_gram_kernel, uneven runs, MIXED, both launches of a call (1,184 runs captured:
-# 22.6 MB read, 1.822 GB written)
-FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (19.521536e6 + 3.077120e6 + 1.344401e9 + 0.477131e9) / 1184
+# adjoint_gram_kernel<MixedPrecision, 2> (the ghost-plate variant), uneven runs with the
+# zero-power plate at surface 1, both launches of a call (1,184 runs captured: 58.6 MB read,
+# 2.975 GB written)
+FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (54.299392e6 + 4.300032e6 + 2.273197e9 + 0.701928e9) / 1184
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -643,9 +644,10 @@ def run_lm(args, world, rank, local):
     }, None
 
 
-WORKLOAD_UNEVEN = ("uneven-8192: 8192 runs, S ~ U{6..30} (stop, 1/50-style biconvex elements, "
-                   "zero-power plates), P ~ U{8..64} (capped by the system), L=7, F=5, "
-                   "16x32 Half pupils (config 3 shape)")
+WORKLOAD_UNEVEN = ("uneven-8192: 8192 runs, S ~ U{6..30} (stop, a zero-power ghost plate at "
+                   "surface 1, 1/50-style biconvex elements, a zero-curvature surface where the "
+                   "count is odd), P ~ U{8..64} (capped by the system), L=7, F=5, 16x32 Half "
+                   "pupils (config 3 shape)")
 
 
 def run_uneven(args, world, rank, local):
@@ -693,13 +695,17 @@ def run_uneven(args, world, rank, local):
 
     # ---- the same with the FP32-bulk forward (directions and refraction in FP32; positions,
     # intersection and optical path in FP64) and the FP32 reverse sweep
+    # (built for batches without ghost plates: measured then, else reported as not run)
     from mikroptim_b200.batch import PRECISION_FP32_BULK
-    lay_bulk = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP32_BULK))
-    lm_b = engine.DeviceLm(db, lay_bulk, b, vss, opt, runs)
-    lm_b.start(x0)
-    ms_bulk, iters_bulk, _ = _lm_window(lm_b, args.steps, args.warmup, flush, world, dev)
-    bulk_value = world * iters_bulk / (max_over_ranks(ms_bulk, world, dev) * args.steps / 1e3)
-    del lm_b
+    bulk_value = ms_bulk = None
+    if b.topology.ghost_plates == 0:
+        lay_bulk = ResidualLayout(b.topology,
+                                  dataclasses.replace(st, precision=PRECISION_FP32_BULK))
+        lm_b = engine.DeviceLm(db, lay_bulk, b, vss, opt, runs)
+        lm_b.start(x0)
+        ms_bulk, iters_bulk, _ = _lm_window(lm_b, args.steps, args.warmup, flush, world, dev)
+        bulk_value = world * iters_bulk / (max_over_ranks(ms_bulk, world, dev) * args.steps / 1e3)
+        del lm_b
 
     # ---- the same LM with paraxial constraints on the device (image at the paraxial focus,
     # working distance >= 1 mm, |Petzval curvature| <= 0.02 / mm; analytic adjoint rows): the
@@ -810,7 +816,8 @@ def run_uneven(args, world, rank, local):
                               "precision": "FP32_BULK: forward with FP32 directions and "
                                            "refraction (FP64 positions, intersection, optical "
                                            "path), FP32 reverse sweep; its OPD error in "
-                                           "opd_error_vs_fp64.fp32_bulk"},
+                                           "opd_error_vs_fp64.fp32_bulk; not run (null) on "
+                                           "batches with ghost plates, which it does not trace"},
         "adjoint_mixed_paraxial_constraints": {
             "value": con_value, "unit": "LM iterations/s", "ms_per_cycle": ms_con,
             "launches_per_cycle": int(per_cycle_con),

@@ -412,8 +412,11 @@ typedef struct mkb_lm_options {
  * equal). The paraxial index of a medium is its index in wavelength column `paraxial_column`
  * of the record (the batch's paraxial_index), or, for a medium with glass variables, the
  * Buchdahl index at the reference wavelength (VariableSet::apply, src/optim/
- * variable_set.cpp:282). Coaxial batches without ghost plates. Sine-condition and distortion
- * rows trace real rays and stay host rows. */
+ * variable_set.cpp:282). A ghost plate is a thin element in the medium n_m of its gap
+ * (batch_paraxial, src/batch/system_batch.cpp:965): its power -2 (n_G - n_m) t2 (t2 from its
+ * Legendre coefficients, n_G its glass index in the same column) joins the surface's power and
+ * that power / (n_m n_G) the Petzval sum; a parfocal reference surface must not be a plate.
+ * Coaxial batches. Sine-condition and distortion rows trace real rays and stay host rows. */
 enum { MKB_CONSTRAINT_FOCAL_LENGTH = 0, MKB_CONSTRAINT_PARFOCAL_LENGTH = 1,
        MKB_CONSTRAINT_WORKING_DISTANCE = 2, MKB_CONSTRAINT_PARAXIAL_FOCUS = 3,
        MKB_CONSTRAINT_PETZVAL = 4 };          /* ConstraintType, model/constraints.hpp:28 */

@@ -812,11 +812,14 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
         sl.loc = {N(q[6 * kFusedThreads]), N(q[7 * kFusedThreads]), N(q[8 * kFusedThreads]),
                   N(mu_tab[(c + 1) * L + l]), N(q[9 * kFusedThreads])};
     };
+    // the steps below the lowest one that writes a column feed no variable (with the aimed
+    // pupil, every column takes the start's adjoint: the sweep runs to the start)
+    const int floor_c = kAim ? 0 : v.sweep_floor;
     Slot next;
     load(count - 1, next);
-    for (int c = count - 1; c >= 0; --c) {
+    for (int c = count - 1; c >= floor_c; --c) {
         const Slot cur = next;
-        if (c > 0) load(c - 1, next);
+        if (c > floor_c) load(c - 1, next);
         if (c == count - 1) {
             if (reached_image && count == S) {
                 Vec<A> center_adj[K];

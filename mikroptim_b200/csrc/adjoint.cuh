@@ -256,7 +256,7 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
     const N x = p.x + s0 * d.x;
     const N y = p.y + s0 * d.y;
     const N radius = g.radius;
-    const N inv_r2 = one / (radius * radius);
+    const N inv_r2 = Divisor<N>(radius * radius).div(one);
     const N u = (x * x + y * y) * inv_r2;
     const N xi = two * u - one;
     N prof_t(0.0), sum_dp(0.0), sum_ddp(0.0);
@@ -267,8 +267,8 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
             prof_t += a * p_cur;
             sum_dp += a * dp_cur;
             sum_ddp += a * ddp_cur;
-            const N p_next = (N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev) /
-                             N(double(k + 1));
+            const N p_next =
+                legendre_div<N>(N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev, k);
             const N dp_next = dp_prev + N(double(2 * k + 1)) * p_cur;
             const N ddp_next = ddp_prev + N(double(2 * k + 1)) * dp_cur;
             p_prev = p_cur;
@@ -283,8 +283,15 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
     const N d2t_du2 = N(4.0) * sum_ddp;
     const N dn = N(g.n_glass) - n_before;
     const N radial = dn * dt_du * two * inv_r2;
-    const N dx = (n_before * d.x + radial * x) / n_after;
-    const N dy = (n_before * d.y + radial * y) / n_after;
+    N dx, dy;
+    if constexpr (kMulByReciprocal<N>) {  // as ghost_step forms them
+        const N inv_after = one / n_after;
+        dx = (n_before * d.x + radial * x) * inv_after;
+        dy = (n_before * d.y + radial * y) * inv_after;
+    } else {
+        dx = (n_before * d.x + radial * x) / n_after;
+        dy = (n_before * d.y + radial * y) / n_after;
+    }
     const N radicand = one - dx * dx - dy * dy;
     const bool tir = (branch & kBranchSoftTir) != 0;
     N inv_m(0.0), ex(0.0), ey(0.0), root(0.0);
@@ -303,6 +310,8 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
     const A aradial = cv<A>(radial), as0 = cv<A>(s0), adn = cv<A>(dn), aprof = cv<A>(prof_t);
     const A adtdu = cv<A>(dt_du), ad2t = cv<A>(d2t_du2), ainv_r2 = cv<A>(inv_r2);
     const A axi = cv<A>(xi), ad_z = cv<A>(d.z);
+    // the seed-independent divisors (FP32: one SFU reciprocal each, shared by the K seeds)
+    const Divisor<A> by_2root(two_a * aroot), by_after(ana), by_dz(ad_z);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
         const Vec<A> qb = adj[m].p;
@@ -317,16 +326,16 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
         } else {
             dxb = d1b.x;
             dyb = d1b.y;
-            radb = d1b.z / (two_a * aroot);
+            radb = by_2root.div(d1b.z);
         }
         dxb += -two_a * adx * radb;
         dyb += -two_a * ady * radb;
-        in.d.x += dxb * anb / ana;
-        in.d.y += dyb * anb / ana;
-        out[m].n_before += (dxb * ad_x + dyb * ad_y) / ana;
-        out[m].n_after += -(dxb * adx + dyb * ady) / ana;
-        const A gxb = dxb / ana;
-        const A gyb = dyb / ana;
+        in.d.x += by_after.div(dxb * anb);
+        in.d.y += by_after.div(dyb * anb);
+        out[m].n_before += by_after.div(dxb * ad_x + dyb * ad_y);
+        out[m].n_after += by_after.div(-(dxb * adx + dyb * ady));
+        const A gxb = by_after.div(dxb);
+        const A gyb = by_after.div(dyb);
         const A radialb = gxb * ax + gyb * ay;
         A xb = qb.x + gxb * aradial;
         A yb = qb.y + gyb * aradial;
@@ -342,8 +351,8 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
             A p_prev(1.0), p_cur = axi, dp_prev(0.0), dp_cur(1.0);
             for (int k = 1; k <= g.K; ++k) {
                 coeff(m, k - 1, tb * p_cur + dtdub * two_a * dp_cur);
-                const A p_next = (A(double(2 * k + 1)) * axi * p_cur - A(double(k)) * p_prev) /
-                                 A(double(k + 1));
+                const A p_next =
+                    legendre_div<A>(A(double(2 * k + 1)) * axi * p_cur - A(double(k)) * p_prev, k);
                 const A dp_next = dp_prev + A(double(2 * k + 1)) * p_cur;
                 p_prev = p_cur;
                 p_cur = p_next;
@@ -359,7 +368,7 @@ __device__ __forceinline__ void ghost_step_backward_k(Vec<N> p, Vec<N> d, N t, c
         s0b += xb * ad_x + yb * ad_y;
         in.d.x += xb * as0;
         in.d.y += yb * as0;
-        const A qq = s0b / ad_z;
+        const A qq = by_dz.div(s0b);
         out[m].thickness += qq;
         in.p.z += -qq;
         in.d.z += -qq * as0;

@@ -419,6 +419,15 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
             return MKB_ERR_ARGUMENT;
         }
     }
+    // the reverse step onto surface c + 1 writes the columns of curvature[c + 1] and of plate
+    // c + 1's coefficients, of thickness[c] (the working distance in the image step, c = S - 1)
+    // and of the media c and c + 1 (medium 0 in the step onto surface 1)
+    v.sweep_floor = kMaxSurfaces;
+    for (int k = 0; k < v.P; ++k) {
+        const int s = v.surface[k];
+        const int c = v.type[k] == MKB_VAR_THICKNESS ? s : (s > 0 ? s - 1 : 0);
+        if (c < v.sweep_floor) v.sweep_floor = c;
+    }
     if (v.has_glass) {
         // Buchdahl coordinate w = dl / (1 + 2.5 dl), dl = lambda [um] - 0.546074 um
         // (buchdahl_omega, glass/dispersion.hpp:87; nm_to_um divides by 1000)

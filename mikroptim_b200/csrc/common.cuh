@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace mkb {
 
 // ---- limits ------------------------------------------------------------------------------
@@ -543,6 +545,29 @@ __device__ __forceinline__ bool ghost_at(const TraceParams& p, const double* rec
     }
 }
 
+// The plain double and float steps divide by a quantity that does not depend on the ray (a
+// small integer, a refractive index) by multiplying with its rounded reciprocal: within an ulp
+// of the division and off the ray's dependent chain. Exact64 (the reference's order of
+// operations) and Df64 keep the division.
+template <class N>
+constexpr bool kMulByReciprocal = std::is_same<N, double>::value || std::is_same<N, float>::value;
+
+// 1 / k for k = 1 .. 36, rounded at compile time (the Legendre recurrences' 1 / (k + 1))
+#define MKB_RECIP4(k) 1.0 / (k), 1.0 / ((k) + 1), 1.0 / ((k) + 2), 1.0 / ((k) + 3)
+static __constant__ double kRecipInt[37] = {0.0,            MKB_RECIP4(1),  MKB_RECIP4(5),
+                                            MKB_RECIP4(9),  MKB_RECIP4(13), MKB_RECIP4(17),
+                                            MKB_RECIP4(21), MKB_RECIP4(25), MKB_RECIP4(29),
+                                            MKB_RECIP4(33)};
+#undef MKB_RECIP4
+static_assert(kMaxGhostTerms + 1 <= 36, "kRecipInt covers 1 / (k + 1) for k <= kMaxGhostTerms");
+
+// x / (k + 1) in the Legendre recurrence
+template <class N>
+__device__ __forceinline__ N legendre_div(N x, int k) {
+    if constexpr (kMulByReciprocal<N>) return x * N(kRecipInt[k + 1]);
+    else return x / N(double(k + 1));
+}
+
 // Thickness profile t(u) = sum_k a_k P_k(2u - 1) and dt/du = 2 sum_k a_k P'_k(2u - 1) by the
 // Legendre recurrences in ascending k (ghost_profile, ghost_plate.hpp:67).
 template <class N>
@@ -555,8 +580,8 @@ __device__ __forceinline__ void ghost_profile(const GhostData& g, N u, N& t, N& 
         const N a = g.coeff[k - 1];
         tt += a * p_cur;
         dt += a * dp_cur;
-        const N p_next = (N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev) /
-                         N(double(k + 1));
+        const N p_next = legendre_div<N>(N(double(2 * k + 1)) * xi * p_cur - N(double(k)) * p_prev,
+                                         k);
         const N dp_next = dp_prev + N(double(2 * k + 1)) * p_cur;
         p_prev = p_cur;
         p_cur = p_next;
@@ -592,8 +617,15 @@ __device__ __forceinline__ int ghost_step(RayT<N>& r, N t, N n_before, N n_after
     const N radial = dn * dt_du * two * inv_r2;
     const N gx = radial * r.px, gy = radial * r.py;
     r.opl += dn * prof_t;
-    const N dx = (n_before * r.dx + gx) / n_after;
-    const N dy = (n_before * r.dy + gy) / n_after;
+    N dx, dy;
+    if constexpr (kMulByReciprocal<N>) {
+        const N inv_after = one / n_after;
+        dx = (n_before * r.dx + gx) * inv_after;
+        dy = (n_before * r.dy + gy) * inv_after;
+    } else {
+        dx = (n_before * r.dx + gx) / n_after;
+        dy = (n_before * r.dy + gy) / n_after;
+    }
     const N radicand = one - dx * dx - dy * dy;
     if constexpr (kKeep) *keep = {s0, zero, zero, zero, zero};
     branch = kBranchRegular;
@@ -858,6 +890,9 @@ struct VarParams {
     int8_t glass_component[MKB_MAX_VARIABLES];  // Glass variables: 0 n0, 1 nu1, 2 nu2
     int8_t col_glass[kMaxSurfaces][3];          // column of (n0, nu1, nu2) of medium s, or -1
     int has_glass;                              // any Glass variable
+    // the lowest slot c (the step onto surface c + 1) whose reverse step writes a column:
+    // the reverse sweep of the fused kernel ends there, the steps below it feed no variable
+    int sweep_floor;
     int L;                                      // wavelengths (glass index refresh)
     double omega[MKB_MAX_WAVELENGTHS];          // Buchdahl coordinate of every wavelength
     double lower[MKB_MAX_VARIABLES], upper[MKB_MAX_VARIABLES], typical[MKB_MAX_VARIABLES];

@@ -11,6 +11,9 @@
 //     src/optim/adjoint_jacobian.cpp:270), bit for bit the reference's extra rows; or
 //   * MKB_PARAXIAL_ADJOINT: the analytic derivatives, from one reverse sweep of the marginal
 //     ray per run (seeds dA and dC) and the closed-form derivatives of the Petzval sum.
+// Ghost plates enter as thin elements in the medium of their gap (batch_paraxial,
+// src/batch/system_batch.cpp:965): power phi_G = -2 (n_G - n_m) t2 added to the surface's power
+// and phi_G / (n_m n_G) added to the Petzval sum, t2 from the plate's Legendre coefficients.
 // Kernels: paraxial_rows_kernel (rows and Jacobian of the runs a mask selects) and
 // paraxial_merit_kernel (sum r_e^2 at the points a mask selects, added to the MERIT).
 #include "fd.cuh"
@@ -31,13 +34,55 @@ struct Paraxial {
     double A, C, power, kappa;
 };
 
-__device__ inline Paraxial ynu(const double* c, const double* t, const double* n, int S) {
+// The ghost plates of one point: the template's plate data with the run's GhostCoefficient
+// variables at x applied; variable `pk` (or -1) takes the value `pv` instead of x[pk].
+struct Plates {
+    const ParaxialSpec* sp;
+    const VarParams* v;
+    const double* tmpl;
+    const double* x;
+    RecordLayout lay;
+    int L, pk;
+    double pv;
+
+    __device__ double coefficient(int g, int j) const {
+        const int col = v->col_ghost[g][j];
+        if (col < 0) return tmpl[lay.ghost_coeff + g * sp->K + j];
+        return col == pk ? pv : x[col];
+    }
+    // ghost_profile_t2 (include/mikroptim/trace/ghost_plate.hpp:95)
+    __device__ double t2(int g) const {
+        double sum = 0.0;
+        for (int k = 1; k <= sp->K; ++k) {
+            const double term = __dmul_rn(coefficient(g, k - 1), static_cast<double>(k * (k + 1)));
+            sum = __dadd_rn(sum, (k & 1) ? term : -term);
+        }
+        const double r = tmpl[lay.ghost_radius + g];
+        return __ddiv_rn(sum, __dmul_rn(r, r));
+    }
+    __device__ double glass(int g) const { return tmpl[lay.ghost_index + g * L + sp->column]; }
+    // ghost_plate_power / ghost_plate_petzval (ghost_plate.hpp:107,114) of surface s in the
+    // medium n_m; 0 and 0 on a surface without a plate
+    __device__ void at(int s, double n_m, double& power, double& petzval) const {
+        power = petzval = 0.0;
+        const int g = sp->ghost_of[s];
+        if (g < 0) return;
+        const double n_g = glass(g);
+        power = __dmul_rn(__dmul_rn(-2.0, __dsub_rn(n_g, n_m)), t2(g));
+        petzval = __ddiv_rn(power, __dmul_rn(n_m, n_g));
+    }
+};
+
+__device__ inline Paraxial ynu(const double* c, const double* t, const double* n, int S,
+                               const Plates& pl) {
     using N = Exact64;
     N y(1.0), u(0.0), nb(1.0);
     for (int s = 0; s < S; ++s) {
         if (s > 0) y = y + N(t[s - 1]) * u;
         N phi = N(c[s]) * (N(n[s]) - nb);
-        phi = phi + N(0.0);  // the plates' extra power (none here), added as the reference adds
+        double pw, pz;
+        pl.at(s, n[s], pw, pz);
+        phi = phi + N(pw);  // the plates' extra power (0 elsewhere), added as the reference adds
         u = (nb * u - y * phi) / N(n[s]);
         nb = n[s];
     }
@@ -45,7 +90,9 @@ __device__ inline Paraxial ynu(const double* c, const double* t, const double* n
     nb = N(1.0);
     for (int s = 0; s < S; ++s) {
         p = p + (N(c[s]) * (N(n[s]) - nb)) / (nb * N(n[s]));
-        p = p + N(0.0);
+        double pw, pz;
+        pl.at(s, n[s], pw, pz);
+        p = p + N(pz);
         nb = n[s];
     }
     Paraxial out;
@@ -96,8 +143,9 @@ __device__ inline double mode_of(int mode, double q) {
 }
 
 __device__ inline void residuals_at(const ParaxialSpec& sp, const double* c, const double* t,
-                                    const double* n, int S, double a, double* r) {
-    const Paraxial px = ynu(c, t, n, S);
+                                    const double* n, int S, const Plates& pl, double a,
+                                    double* r) {
+    const Paraxial px = ynu(c, t, n, S, pl);
     for (int e = 0; e < sp.E; ++e)
         r[e] = __dmul_rn(sp.root_w[e], mode_of(sp.mode[e], deviation(sp, e, px, t, n, S, a)));
 }
@@ -166,6 +214,7 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
                 t[s] = t0[s];
                 n[s] = n0[s];
             }
+            Plates pl{&sp, &v, tmpl, xr, lay, L, -1, 0.0};
             if (j > 0) {
                 const int k = (j - 1) / 2;
                 const double val = (j & 1) ? pat[k].xa : pat[k].xb;
@@ -176,11 +225,14 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
                     double b[4] = {bu0[4 * s], bu0[4 * s + 1], bu0[4 * s + 2], bu0[4 * s + 3]};
                     b[v.glass_component[k]] = val;
                     n[s] = buchdahl(b, sp.omega_ref);
-                } else if (v.type[k] != MKB_VAR_GHOST_COEFFICIENT) {
+                } else if (v.type[k] == MKB_VAR_GHOST_COEFFICIENT) {
+                    pl.pk = k;
+                    pl.pv = val;
+                } else {
                     t[s] = val;
                 }
             }
-            residuals_at(sp, c, t, n, S, a, rs + j * E);
+            residuals_at(sp, c, t, n, S, pl, a, rs + j * E);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < v.P * E; i += kRowThreads) {
@@ -195,24 +247,29 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
     }
     // ---- analytic: thread 0 per run (S <= 64 steps, a handful of rows) ------------------
     if (threadIdx.x != 0) return;
+    const Plates pl{&sp, &v, tmpl, xr, lay, L, -1, 0.0};
     double y[kMaxSurfaces], u[kMaxSurfaces];  // marginal height at s, angle after s
+    double pw[kMaxSurfaces];                  // the plates' extra power (0 elsewhere)
     {
         double yy = 1.0, uu = 0.0, nb = 1.0;
         for (int s = 0; s < S; ++s) {
+            double pz;
+            pl.at(s, n0[s], pw[s], pz);
             if (s > 0) yy = yy + t0[s - 1] * uu;
-            const double phi = c0[s] * (n0[s] - nb);
+            const double phi = c0[s] * (n0[s] - nb) + pw[s];
             uu = (nb * uu - yy * phi) / n0[s];
             y[s] = yy;
             u[s] = uu;
             nb = n0[s];
         }
     }
-    const Paraxial px = ynu(c0, t0, n0, S);
+    const Paraxial px = ynu(c0, t0, n0, S, pl);
     // gradients of A = y_{S-1} and C = n_{S-1} u_{S-1} with respect to c_s, t_s, n_s by one
     // reverse sweep carrying both seeds; gradient of the Petzval sum in closed form
-    double gA_c[kMaxSurfaces], gA_t[kMaxSurfaces], gA_n[kMaxSurfaces];
-    double gC_c[kMaxSurfaces], gC_t[kMaxSurfaces], gC_n[kMaxSurfaces];
-    for (int s = 0; s < S; ++s) gA_c[s] = gA_t[s] = gA_n[s] = gC_c[s] = gC_t[s] = gC_n[s] = 0.0;
+    double gA_c[kMaxSurfaces], gA_t[kMaxSurfaces], gA_n[kMaxSurfaces], gA_p[kMaxSurfaces];
+    double gC_c[kMaxSurfaces], gC_t[kMaxSurfaces], gC_n[kMaxSurfaces], gC_p[kMaxSurfaces];
+    for (int s = 0; s < S; ++s)
+        gA_c[s] = gA_t[s] = gA_n[s] = gA_p[s] = gC_c[s] = gC_t[s] = gC_n[s] = gC_p[s] = 0.0;
     {
         double ay[2] = {1.0, 0.0};           // adjoint of y_s (seed A, seed C)
         double au[2] = {0.0, n0[S - 1]};     // adjoint of u_s
@@ -220,10 +277,11 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
         for (int s = S - 1; s >= 0; --s) {
             const double nb = s > 0 ? n0[s - 1] : 1.0;
             const double u_in = s > 0 ? u[s - 1] : 0.0;
-            const double phi = c0[s] * (n0[s] - nb);
+            const double phi = c0[s] * (n0[s] - nb) + pw[s];
             double* gc[2] = {gA_c, gC_c};
             double* gt[2] = {gA_t, gC_t};
             double* gn[2] = {gA_n, gC_n};
+            double* gp[2] = {gA_p, gC_p};
             for (int q = 0; q < 2; ++q) {
                 // u_s = (nb u_in - y_s phi) / n_s
                 const double w = au[q] / n0[s];
@@ -232,7 +290,8 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
                 const double a_phi = -w * y[s];
                 gn[q][s] += -w * u[s];  // d/dn_s of 1/n_s
                 double a_nb = w * u_in;
-                // phi = c_s (n_s - nb)
+                // phi = c_s (n_s - nb) + the plate's power
+                gp[q][s] += a_phi;
                 gc[q][s] += a_phi * (n0[s] - nb);
                 gn[q][s] += a_phi * c0[s];
                 a_nb += -a_phi * c0[s];
@@ -247,13 +306,22 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
             }
         }
     }
-    // dP/dc_s = 1/nb - 1/n_s; dP/dn_s = c_s / n_s^2 - c_{s+1} / n_s^2
+    // dP/dc_s = 1/nb - 1/n_s; dP/dn_s = c_s / n_s^2 - c_{s+1} / n_s^2; a plate on surface s
+    // adds through its medium n_m = n_s: d(phi_G)/dn_m = 2 t2 and
+    // d(phi_G / (n_m n_G))/dn_m = 2 t2 / (n_m n_G) - phi_G / (n_m^2 n_G)
     double gP_c[kMaxSurfaces], gP_n[kMaxSurfaces];
     {
         double nb = 1.0;
         for (int s = 0; s < S; ++s) {
             gP_c[s] = 1.0 / nb - 1.0 / n0[s];
             gP_n[s] = c0[s] / (n0[s] * n0[s]) - (s + 1 < S ? c0[s + 1] / (n0[s] * n0[s]) : 0.0);
+            const int g = sp.ghost_of[s];
+            if (g >= 0) {
+                const double ng = pl.glass(g), dpw = 2.0 * pl.t2(g);
+                gA_n[s] += gA_p[s] * dpw;
+                gC_n[s] += gC_p[s] * dpw;
+                gP_n[s] += dpw / (n0[s] * ng) - pw[s] / (n0[s] * n0[s] * ng);
+            }
             nb = n0[s];
         }
     }
@@ -293,6 +361,18 @@ paraxial_rows_kernel(const __grid_constant__ ParaxialSpec sp, const __grid_const
                 dC = gC_n[s] * slope;
                 dP = gP_n[s] * slope;
                 dn_last = s == S - 1 ? slope : 0.0;
+            } else {
+                // coefficient a_o of plate g: dt2/da_o = (-1)^{o+1} o (o + 1) / r^2
+                const int g = v.ghost_plate[k], o = v.ghost_order[k];
+                const int sg = sp.ghost_surface[g];
+                if (sg < S) {
+                    const double r = tmpl[lay.ghost_radius + g], ng = pl.glass(g);
+                    const double dt2 = ((o & 1) ? 1.0 : -1.0) * o * (o + 1) / (r * r);
+                    const double dpw = -2.0 * (ng - n0[sg]) * dt2;
+                    dA = gA_p[sg] * dpw;
+                    dC = gC_p[sg] * dpw;
+                    dP = dpw / (n0[sg] * ng);
+                }
             }
             double dq = 0.0;
             switch (sp.type[e]) {
@@ -336,9 +416,10 @@ __global__ void paraxial_merit_kernel(const __grid_constant__ ParaxialSpec sp,
     int S = tsurf != nullptr ? tsurf[tmpl_i] : S_table;
     S = S < 2 ? 2 : (S > S_table ? S_table : S);
     double c[kMaxSurfaces], t[kMaxSurfaces], n[kMaxSurfaces], bu[4 * kMaxSurfaces];
-    build_point(sp, v, lay, tmpl, S, L, x + static_cast<int64_t>(run) * pstride, c, t, n, bu);
+    const double* xr = x + static_cast<int64_t>(run) * pstride;
+    build_point(sp, v, lay, tmpl, S, L, xr, c, t, n, bu);
     double r[MKB_MAX_PARAXIAL];
-    residuals_at(sp, c, t, n, S, tmpl[lay.pupil], r);
+    residuals_at(sp, c, t, n, S, Plates{&sp, &v, tmpl, xr, lay, L, -1, 0.0}, tmpl[lay.pupil], r);
     double sum = 0.0;
     for (int e = 0; e < sp.E; ++e) sum = __dadd_rn(sum, __dmul_rn(r[e], r[e]));
     out[run] = sum;
@@ -356,9 +437,15 @@ int make_paraxial_spec(const mkb_lm_options* o, const mkb_device_batch* b,
                   MKB_MAX_PARAXIAL);
         return MKB_ERR_ARGUMENT;
     }
-    if (b->non_coaxial || b->ghost_plates > 0) {
-        set_error("paraxial constraints on the device: coaxial batches without ghost plates");
+    if (b->non_coaxial) {
+        set_error("paraxial constraints on the device: coaxial batches");
         return MKB_ERR_UNSUPPORTED;
+    }
+    if (b->ghost_plates < 0 || b->ghost_plates > kMaxGhostPlates || b->ghost_terms < 0 ||
+        b->ghost_terms > kMaxGhostTerms || b->surfaces > kMaxSurfaces) {
+        set_error("paraxial constraints: ghost plates (G=%d, K=%d) or %d surfaces out of range",
+                  b->ghost_plates, b->ghost_terms, b->surfaces);
+        return MKB_ERR_ARGUMENT;
     }
     if (o->paraxial_column < 0 || o->paraxial_column >= b->wavelengths) {
         set_error("paraxial constraints: column %d outside [0, %d)", o->paraxial_column,
@@ -371,6 +458,16 @@ int make_paraxial_spec(const mkb_lm_options* o, const mkb_device_batch* b,
     }
     sp->E = E;
     sp->column = o->paraxial_column;
+    // the plates in table order (the surface table's ghost_of)
+    sp->G = b->ghost_plates;
+    sp->K = b->ghost_terms;
+    for (int s = 0; s < kMaxSurfaces; ++s) sp->ghost_of[s] = -1;
+    for (int g = 0; g < kMaxGhostPlates; ++g) sp->ghost_surface[g] = kMaxSurfaces;
+    for (int s = 1, g = 0; s < b->surfaces; ++s)
+        if (b->type[s] == MKB_SURFACE_GHOST_PLATE && g < sp->G) {
+            sp->ghost_of[s] = static_cast<int8_t>(g);
+            sp->ghost_surface[g++] = static_cast<int8_t>(s);
+        }
     sp->analytic = o->paraxial_derivative == MKB_PARAXIAL_ADJOINT ? 1 : 0;
     // the Buchdahl coordinate of the reference wavelength (buchdahl_omega,
     // glass/dispersion.hpp:87), as make_var_params forms it for the batch's wavelengths
@@ -401,6 +498,9 @@ int make_paraxial_spec(const mkb_lm_options* o, const mkb_device_batch* b,
             (c.reference_surface < 0 || c.reference_surface >= b->surfaces ||
              !std::isfinite(c.offset)))
             return fail("parfocal length: reference surface outside the table");
+        if (c.type == MKB_CONSTRAINT_PARFOCAL_LENGTH &&
+            b->type[c.reference_surface] == MKB_SURFACE_GHOST_PLATE)
+            return fail("parfocal length: the reference surface is a ghost plate");
         sp->type[e] = c.type;
         sp->mode[e] = c.mode;
         sp->root_w[e] = std::sqrt(c.weight);

@@ -16,6 +16,11 @@ struct ParaxialSpec {
     int type[MKB_MAX_PARAXIAL], mode[MKB_MAX_PARAXIAL], ref_surface[MKB_MAX_PARAXIAL];
     double root_w[MKB_MAX_PARAXIAL], target[MKB_MAX_PARAXIAL], offset[MKB_MAX_PARAXIAL];
     double shift[MKB_MAX_PARAXIAL];
+    // ghost plates: G plates of K profile terms; the plate of a table surface (or -1) and the
+    // table surface of a plate
+    int G, K;
+    int8_t ghost_of[kMaxSurfaces];
+    int8_t ghost_surface[kMaxGhostPlates];
 };
 
 // buchdahl_index (glass/dispersion.hpp:93): n0 + w (nu1 + w (nu2 + w nu3)), each operation

@@ -333,7 +333,8 @@ def with_aperture_stop(batch: SystemBatchHost, settings: ResidualSettings,
 
 def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max: int = 30,
            p_min: int = 8, p_max: int = 64, rings: int = 16, spokes: int = 32,
-           sigma: float = 0.05, failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64):
+           sigma: float = 0.05, failure: int = FAILURE_SOFT, precision: int = PRECISION_FP64,
+           plate: bool = True):
     """Configuration 3: variants of uneven surface and variable counts in one batch.
 
     Variant v has S_v ~ U{s_min .. s_max} table surfaces: the stop, then L = (S_v - 1) // 2
@@ -343,14 +344,26 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
     air on both sides) before the image; the image plane sits at the paraxial focus. All
     variants share the 30-surface table (`variant_surfaces` holds S_v; the entries past S_v
     are unused). 5 fields 0..1 degree, all Half pupils 16 x 32, pupil radius 5 mm.
+    plate=True: table surface 1 of every variant is a ghost plate of zero power (its K = 2
+    Legendre coefficients 0, radius 8 mm, glass index 1.5) 0.5 mm after the stop, so every
+    variant's count includes one zero-power ghost plate and the plate kernels run; the elements
+    then start at surface 2 (L = (S_v - 2) // 2, the zero-curvature surface when S_v - 2 is
+    odd).
     Variables of run v: the first P_v ~ U{p_min .. p_max} (at most all of them) of
     [working distance, element curvatures, glass thicknesses, air gaps].
     Returns (batch, settings, [VariableSet per run], [x0 row per run])."""
     S = s_max
-    topo = BatchTopology(surfaces=S, wavelengths=7, fields=5,
-                         type=[SURFACE_STOP] + [SURFACE_SPHERE] * (S - 1),
-                         pupil_mode=[PUPIL_HALF] * 5)
+    from .batch import SURFACE_GHOST_PLATE
+    first = 2 if plate else 1  # table surface of the first element
+    kinds = ([SURFACE_STOP, SURFACE_GHOST_PLATE] + [SURFACE_SPHERE] * (S - 2) if plate
+             else [SURFACE_STOP] + [SURFACE_SPHERE] * (S - 1))
+    topo = BatchTopology(surfaces=S, wavelengths=7, fields=5, type=kinds,
+                         pupil_mode=[PUPIL_HALF] * 5, ghost_terms=2 if plate else 0)
     b = SystemBatchHost(topo, variants)
+    if plate:
+        b.ghost_coeff[:] = 0.0
+        b.ghost_norm_radius[:] = 8.0
+        b.ghost_index[:] = 1.5
     b.reference_wavelength_nm = 587.6
     b.wavelength_nm[:] = OBJECTIVE_WAVELENGTHS
     b.wavelength_weight[:] = 1.0
@@ -365,14 +378,14 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
     variable_sets, x0 = [], []
     for v in range(variants):
         n_surf = int(sv[v])
-        elements = (n_surf - 1) // 2
+        elements = (n_surf - first) // 2
         c = np.zeros(S)
         t = np.zeros(S)
         idx = np.ones((S, 7))
         n_ref = np.ones(S)
-        t[0] = 0.0  # stop plane at the first vertex
+        t[0] = 0.5 if plate else 0.0  # stop plane at the first vertex (or 0.5 mm to the plate)
         for e in range(elements):
-            s1, s2 = 1 + 2 * e, 2 + 2 * e
+            s1, s2 = first + 2 * e, first + 1 + 2 * e
             c[s1] = (1.0 / (50.0 * elements)) * (1.0 + sigma * noise[v, s1, 0])
             c[s2] = (-1.0 / (50.0 * elements)) * (1.0 + sigma * noise[v, s2, 0])
             t[s1] = (6.0 / elements) * (1.0 + sigma * noise[v, s1, 1])
@@ -392,9 +405,12 @@ def uneven(variants: int = 8192, seed: int = 20261203 + 3, s_min: int = 6, s_max
         wd = (Variable(VAR_WORKING_DISTANCE, S - 1, 1.0, 500.0, 1.0) if n_surf == S
               else Variable(VAR_THICKNESS, n_surf - 1, 1.0, 500.0, 1.0))
         cands = [wd]
-        cands += [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01) for s in range(1, 1 + 2 * elements)]
-        cands += [Variable(VAR_THICKNESS, 1 + 2 * e, 0.1, 20.0, 1.0) for e in range(elements)]
-        cands += [Variable(VAR_THICKNESS, 2 + 2 * e, 0.1, 20.0, 1.0) for e in range(elements - 1)]
+        cands += [Variable(VAR_CURVATURE, s, -0.2, 0.2, 0.01)
+                  for s in range(first, first + 2 * elements)]
+        cands += [Variable(VAR_THICKNESS, first + 2 * e, 0.1, 20.0, 1.0)
+                  for e in range(elements)]
+        cands += [Variable(VAR_THICKNESS, first + 1 + 2 * e, 0.1, 20.0, 1.0)
+                  for e in range(elements - 1)]
         vs = VariableSet(topo, cands[:min(int(pv[v]), len(cands))])
         variable_sets.append(vs)
         x0.append(vs.extract(b, v))
@@ -634,10 +650,17 @@ def multistart(base: SystemBatchHost, seed: int = 20261203 + 21) -> SystemBatchH
 def unpad(batch: SystemBatchHost, v: int) -> SystemBatchHost:
     """Variant v of an uneven batch as a batch of its own S_v surfaces (one variant)."""
     n = int(batch.variant_surfaces[v]) if batch.variant_surfaces is not None else batch.surfaces
+    kinds = list(batch.topology.type[:n])
+    from .batch import SURFACE_GHOST_PLATE
+    plates = sum(1 for k in kinds[1:] if k == SURFACE_GHOST_PLATE)  # the first plates of the table
     topo = BatchTopology(surfaces=n, wavelengths=batch.wavelengths, fields=batch.fields,
-                         type=list(batch.topology.type[:n]),
-                         pupil_mode=list(batch.topology.pupil_mode))
+                         type=kinds, pupil_mode=list(batch.topology.pupil_mode),
+                         ghost_terms=batch.topology.ghost_terms if plates else 0)
     out = SystemBatchHost(topo, 1)
+    if plates:
+        out.ghost_coeff[0] = batch.ghost_coeff[v, :plates]
+        out.ghost_norm_radius[:] = batch.ghost_norm_radius[:plates]
+        out.ghost_index[0] = batch.ghost_index[v, :plates]
     out.reference_wavelength_nm = batch.reference_wavelength_nm
     out.wavelength_nm = batch.wavelength_nm.copy()
     out.wavelength_weight = batch.wavelength_weight.copy()

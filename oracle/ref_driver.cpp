@@ -107,6 +107,9 @@ mko::SystemBatchHost batch_of_view(const mkb_batch_view& v, const mkb_residual_p
             for (int l = 0; l < L; ++l)
                 b.ghost_index(i, g, l) =
                     v.ghost_index[(static_cast<std::size_t>(i) * v.ghost_plates + g) * L + l];
+            // the plate's paraxial glass index: column 0, like paraxial_index
+            b.paraxial_ghost_index(i, g) =
+                v.ghost_index[(static_cast<std::size_t>(i) * v.ghost_plates + g) * L];
         }
         if (v.decenter_tilt != nullptr)
             for (int s = 0; s < S; ++s)

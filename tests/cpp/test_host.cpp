@@ -197,6 +197,60 @@ int main() {
         expect(same_bits(t.residuals.residuals, want), "transverse rows bit-identical");
     }
 
+    {  // an aperture stop inside the singlet (between its spheres): the packed entrance pupil
+       // and the trace equal the oracle's aiming and its trace of the equivalent batch
+        BatchTopology at = batch.topology();
+        at.surfaces = 4;
+        at.type = {SurfaceKind::Stop, SurfaceKind::Sphere, SurfaceKind::ApertureStop,
+                   SurfaceKind::Sphere};
+        SystemBatchHost ab(at, V);
+        ab.reference_wavelength_nm = batch.reference_wavelength_nm;
+        ab.wavelength_nm = batch.wavelength_nm;
+        ab.wavelength_weight = batch.wavelength_weight;
+        ab.field_weight = batch.field_weight;
+        for (int v = 0; v < V; ++v) {
+            const int map[4] = {0, 1, -1, 2};
+            for (int s = 0; s < 4; ++s) {
+                const int o = map[s] < 0 ? 1 : map[s];
+                ab.curvature(v, s) = map[s] < 0 ? 4.0 : batch.curvature(v, o);  // R = 4 mm
+                ab.thickness(v, s) = s == 1 ? 0.6 * batch.thickness(v, 1)
+                                     : s == 2 ? 0.4 * batch.thickness(v, 1)
+                                     : batch.thickness(v, o);
+                for (int l = 0; l < 3; ++l) ab.index(v, s, l) = batch.view().index[
+                    (static_cast<size_t>(v) * 3 + o) * 3 + l];
+            }
+            ab.pupil_radius(v) = 5.0;
+            for (int f = 0; f < 3; ++f) {
+                ab.field_angle(v, f) = batch.view().field_angle[v * 3 + f];
+                ab.field_target(v, f) = batch.view().field_target[v * 3 + f];
+            }
+        }
+        const ResidualLayout al(ab.topology(), settings);
+        const cuda::TraceOutput t = engine.run(ab, cuda::TraceMode::Residuals, settings);
+        // the equivalent batch: the stop as a plane, surface 0 at the oracle's pupil
+        mkb_batch_view ev = ab.view();
+        std::vector<double> a(V), t0(V);
+        expect(mko_port_aim(&ev, a.data(), t0.data()) == 0, "oracle aiming");
+        std::vector<uint8_t> etype = {MKB_SURFACE_STOP, MKB_SURFACE_SPHERE, MKB_SURFACE_PLANE,
+                                      MKB_SURFACE_SPHERE};
+        std::vector<double> ec(ev.curvature, ev.curvature + 4 * V), et(ev.thickness,
+                                                                       ev.thickness + 4 * V);
+        for (int v = 0; v < V; ++v) {
+            ec[v * 4 + 2] = 0.0;
+            et[v * 4] = t0[v];
+        }
+        ev.type = etype.data();
+        ev.curvature = ec.data();
+        ev.thickness = et.data();
+        ev.pupil_radius = a.data();
+        const auto ap = al.plan(ab);
+        std::vector<double> want(static_cast<size_t>(V) * al.trace_rows());
+        expect(mko_port_residuals(&ev, ap->get(), want.data(), nullptr, nullptr, 1) == 0,
+               "oracle residuals of the equivalent batch");
+        expect(same_bits(t.residuals.residuals, want),
+               "interior stop: RESIDUALS bit-identical to the oracle on the aimed pupil");
+    }
+
     // Jacobians and normal equations
     const VariableSet vars(batch.topology(),
                            {{VariableType::Curvature, 1, -0.2, 0.2, 0.01},

@@ -32,7 +32,7 @@ def traced(b, st, precision):
 
 
 @pytest.mark.parametrize("make", [lambda: workloads.singlet(128), lambda: workloads.sweep(16),
-                                  lambda: workloads.uneven(64)])
+                                  lambda: workloads.uneven(64, plate=False)])
 def test_bulk_trace_within_its_stated_tolerance(make):
     b, st, _, _ = make()
     lam = b.reference_wavelength_nm * 1e-6

@@ -6,10 +6,14 @@ length, working distance, paraxial focus, Petzval curvature).
   whose paraxial index follows the glass).
 * The analytic adjoint Jacobian of the y-nu trace agrees with the central differences to the
   differences' own error.
+* Ghost plates are thin elements of power -2 (n_G - n_m) t2 in the y-nu trace and the Petzval
+  sum: the rows and the Jacobian's coefficient columns equal the reference's bit for bit too.
 * LM trajectories with the constraints on the device equal the reference's optimize_lm_cpu
   with the same constraints bit for bit, with no host phase in the cycle: a cycle is one
   fixed launch sequence and replays from a CUDA graph.
 """
+
+import copy
 
 import numpy as np
 import pytest
@@ -38,7 +42,16 @@ def _objective(n=5):
     return b, ResidualLayout(b.topology, st), vs, x0
 
 
-@pytest.mark.parametrize("make, cons", [(_singlet, SINGLET), (_objective, OBJECTIVE)])
+def _ghost(n=5):
+    # coefficients ~ N(0, 2e-3) mm: the plate's power moves the rows well above rounding
+    b, st, vs, x0 = workloads.ghost(n, rings=3, spokes=6, coeff_sigma=2e-3)
+    return b, ResidualLayout(b.topology, st), vs, x0
+
+
+CASES = [(_singlet, SINGLET), (_objective, OBJECTIVE), (_ghost, SINGLET)]
+
+
+@pytest.mark.parametrize("make, cons", CASES)
 def test_fd_rows_bitwise_equal_reference(make, cons):
     b, lay, vs, x0 = make()
     J, r = engine.paraxial_rows_device(engine.DeviceSystemBatch(b), lay, b, vs, x0,
@@ -48,7 +61,7 @@ def test_fd_rows_bitwise_equal_reference(make, cons):
     assert np.array_equal(J.cpu().numpy(), Jr.reshape(J.shape))
 
 
-@pytest.mark.parametrize("make, cons", [(_singlet, SINGLET), (_objective, OBJECTIVE)])
+@pytest.mark.parametrize("make, cons", CASES)
 def test_adjoint_rows_agree_with_central_differences(make, cons):
     b, lay, vs, x0 = make()
     db = engine.DeviceSystemBatch(b)
@@ -63,9 +76,32 @@ def test_adjoint_rows_agree_with_central_differences(make, cons):
     assert err.max() <= 1e-6, err.max()
 
 
+def test_ghost_plates_change_the_rows():
+    b, lay, vs, x0 = _ghost()
+    cons = engine.ParaxialConstraints.of(SINGLET)
+    _, r = engine.paraxial_rows_device(engine.DeviceSystemBatch(b), lay, b, vs, x0, cons)
+    flat = copy.deepcopy(b)
+    flat.ghost_coeff[:] = 0.0
+    x_flat = np.stack([vs.extract(flat, v) for v in range(b.variants)])
+    _, r0 = engine.paraxial_rows_device(engine.DeviceSystemBatch(flat), lay, flat, vs, x_flat,
+                                        cons)
+    # focal length, Petzval and paraxial focus follow the plate's power
+    d = np.abs(r.cpu().numpy() - r0.cpu().numpy())
+    assert d[:, [0, 3]].min() > 1e-6
+
+
+def test_parfocal_reference_on_a_ghost_plate_is_refused():
+    b, lay, vs, x0 = _ghost(2)
+    cons = engine.ParaxialConstraints([engine.ParaxialConstraint(1, 0, 1.0, 50.0,
+                                                                 reference_surface=3)])
+    with pytest.raises(Exception, match="ghost plate"):
+        engine.paraxial_rows_device(engine.DeviceSystemBatch(b), lay, b, vs, x0, cons)
+
+
+@pytest.mark.parametrize("make", [_singlet, _ghost])
 @pytest.mark.parametrize("method", ["adjoint", "fd"])
-def test_lm_with_device_constraints_bitwise_equal_reference(method):
-    b, lay, vs, x0 = _singlet(4)
+def test_lm_with_device_constraints_bitwise_equal_reference(method, make):
+    b, lay, vs, x0 = make(4)
     cons = SINGLET[:3]
     opt = engine.LmOptions(max_iterations=8,
                            jacobian=engine.JACOBIAN_ADJOINT if method == "adjoint"
