@@ -48,10 +48,12 @@ class DeviceSystemBatch:
     TraceEngine, place the records in memory it already holds when it is large enough."""
 
     def __init__(self, batch: SystemBatchHost, device="cuda", stream=None,
-                 storage: torch.Tensor | None = None, staging: torch.Tensor | None = None):
+                 storage: torch.Tensor | None = None, staging: torch.Tensor | None = None,
+                 validated: bool = False):
         self.device = _require_cuda(device)
         lib = _capi.lib()
-        batch.validate_values()
+        if not validated:  # a caller that has just validated the batch skips the second pass
+            batch.validate_values()
         self.topology = batch.topology
         self.variants = batch.variants
         self.non_coaxial = 1 if batch.non_coaxial else 0
@@ -423,10 +425,10 @@ class TraceEngine:
                              mode == TraceMode.MERIT, 1, self._usable(self._available()))
 
     def _plan(self, batch: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
-              merit: bool, granularity: int) -> tuple[int, int]:
+              merit: bool, granularity: int, plan=None) -> tuple[int, int]:
         shape = self._shape(batch.topology, batch.buchdahl_coeff is not None,
                             batch.variant_surfaces is not None)
-        plan = layout.plan(batch)
+        plan = plan if plan is not None else layout.plan(batch)
         # A batch whose whole run fits the buffers this mode already holds reuses them without
         # asking the device (cudaMemGetInfo costs about a millisecond): the previous plan
         # reserved them within the same limits.
@@ -532,21 +534,23 @@ class TraceEngine:
             out.info.device_bytes = self.device_bytes()
             return out
         with torch.cuda.device(self.device):
-            tranche, usable = self._plan(batch, layout, ts, merit, 1)
+            plan = layout.plan(batch)  # one plan per call (the tranches share its weights)
+            tranche, usable = self._plan(batch, layout, ts, merit, 1, plan)
             for first in range(0, V, tranche):
                 count = min(tranche, V - first)
                 part = batch.subset(first, count) if (first, count) != (0, V) else batch
                 sl = slice(first, first + count)
                 if merit:
                     m = self._merit_tranche(part, layout, ts,
-                                            None if extra is None else extra[first:first + count])
+                                            None if extra is None else extra[first:first + count],
+                                            plan)
                     hp["merit"][sl].copy_(m.merit, non_blocking=True)
                     hp["failed"][sl].copy_(m.failed, non_blocking=True)
                     hp["hard"][sl].copy_(m.hard_failed, non_blocking=True)
                     if ts.extrema:
                         hp["extrema"][sl].copy_(self._last_extrema, non_blocking=True)
                 else:
-                    t = self._residual_tranche(part, layout, ts, first)
+                    t = self._residual_tranche(part, layout, ts, first, plan)
                     hp["res"][sl].copy_(t.residuals, non_blocking=True)
                     if ts.status:
                         hp["status"][sl].copy_(t.status, non_blocking=True)
@@ -598,11 +602,12 @@ class TraceEngine:
             info.device_bytes = self.device_bytes()
             return info
         with torch.cuda.device(self.device):
-            tranche, usable = self._plan(batch, layout, ts, False, granularity)
+            plan = layout.plan(batch)
+            tranche, usable = self._plan(batch, layout, ts, False, granularity, plan)
             for first in range(0, V, tranche):
                 count = min(tranche, V - first)
                 part = batch.subset(first, count) if (first, count) != (0, V) else batch
-                t = self._residual_tranche(part, layout, ts, first)
+                t = self._residual_tranche(part, layout, ts, first, plan)
                 torch.cuda.synchronize()
                 _device_status()
                 consume(t)
@@ -614,14 +619,16 @@ class TraceEngine:
         return info
 
     def _residual_tranche(self, part: SystemBatchHost, layout: ResidualLayout,
-                          ts: TraceSettings, first: int) -> DeviceTranche:
+                          ts: TraceSettings, first: int, plan=None) -> DeviceTranche:
+        """One tranche's RESIDUALS on the device; `part` was validated by the caller and `plan`
+        (or None) is the run's plan, whose weights every tranche shares."""
         lib = _capi.lib()
         n = part.variants
         rays = layout.rays_per_variant
         stride = layout.trace_rows + ts.extra_residuals
         sv = n * self._stride_of(part)
         db = DeviceSystemBatch(part, self.device, storage=self._buffer("records", 8 * sv),
-                               staging=self._host_staging(sv))
+                               staging=self._host_staging(sv), validated=True)
         res = self._buffer("res", 8 * n * stride)[:8 * n * stride].view(torch.float64)
         res = res.view(n, stride)
         st = self._buffer("status", n * rays)[:n * rays].view(n, rays)
@@ -632,7 +639,7 @@ class TraceEngine:
         if ts.extra_residuals:
             res[:, layout.trace_rows:].zero_()
         b = db.c_struct()
-        plan = layout.plan(part)
+        plan = plan if plan is not None else layout.plan(part)
         ext = self._extrema_buffer(part, ts)
         opts = _trace_options(ts.pack_rays, None, ext)
         rc = lib.mkb_residuals_ex_device(C.byref(b), C.byref(plan), C.byref(opts),
@@ -644,13 +651,15 @@ class TraceEngine:
                              ext)
 
     def _merit_tranche(self, part: SystemBatchHost, layout: ResidualLayout, ts: TraceSettings,
-                       extra: np.ndarray | None) -> MeritOutput:
+                       extra: np.ndarray | None, plan=None) -> MeritOutput:
+        """One tranche's MERIT on the device (`part` validated by the caller, `plan` as in
+        _residual_tranche)."""
         lib = _capi.lib()
         n = part.variants
         sv = n * self._stride_of(part)
         db = DeviceSystemBatch(part, self.device, storage=self._buffer("records", 8 * sv),
-                               staging=self._host_staging(sv))
-        plan = layout.plan(part)
+                               staging=self._host_staging(sv), validated=True)
+        plan = plan if plan is not None else layout.plan(part)
         ws = self._buffer("ws", int(lib.mkb_merit_workspace_bytes(n, C.byref(plan))))
         merit = self._buffer("merit", 8 * n)[:8 * n].view(torch.float64)
         failed = self._buffer("failed", 8 * n)[:8 * n].view(torch.int64)
