@@ -85,7 +85,7 @@ def parse():
                     help="--workload lm: table surface of the aperture stop inside the "
                          "objective (paraxial ray aiming); 0: the stop at surface 0")
     ap.add_argument("--variants", type=int, default=None,
-                    help="runs per GPU (default 8192 for uneven, 65536 for tolerancing, 4096 "
+                    help="runs per GPU (default 8192 for uneven, 262144 for tolerancing, 4096 "
                          "otherwise)")
     return ap.parse_args()
 
@@ -1248,7 +1248,7 @@ def run_tolerancing(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     lib = _capi.lib()
-    V = args.variants or 65536
+    V = args.variants or 262144
     b, st, vs, x0 = workloads.tolerancing(V, seed=20261203 + 5 + 1000 * rank)
     st.precision = PRECISION_FP64_FMA
     lay = ResidualLayout(b.topology, st)
