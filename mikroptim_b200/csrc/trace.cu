@@ -29,8 +29,11 @@ constexpr int kThreads = 128;
 constexpr int kRaysPerThread = 4;
 constexpr int kPackRays = kThreads * kRaysPerThread;
 // resident CTAs per SM the register budget is sized for (56 registers, no spills); the shared
-// memory of the workloads' tables fits as many
+// memory of the workloads' tables fits as many. The variants with surface transforms or ghost
+// plates (feature bits 1, 2) carry more state per step and take 64 registers at 8 CTAs.
 constexpr int kTraceBlocksPerSm = 9;
+template <int kFeat>
+constexpr int trace_blocks_per_sm = (kFeat & 3) != 0 ? 8 : kTraceBlocksPerSm;
 
 // The variant's record (the bulk-copy destination, 16-byte aligned), the mu table and the
 // pack's per-ray OPL, penalty and status live in dynamic shared memory sized for the batch
@@ -222,7 +225,7 @@ __device__ inline double key_value(unsigned long long k) {
 // kMulti: the CTA takes p.vpc variants side by side (built for coaxial batches without ghost
 // plates); otherwise one variant, with the leaner indexing of that case.
 template <bool kResiduals, int kPrecision, int kFeat, bool kExtrema = false, bool kMulti = false>
-__global__ void __launch_bounds__(kThreads, kTraceBlocksPerSm)
+__global__ void __launch_bounds__(kThreads, trace_blocks_per_sm<kFeat>)
 trace_kernel(const __grid_constant__ TraceParams p, const double* __restrict__ records,
              TupleOut out) {
     constexpr bool kExact = kPrecision == MKB_PRECISION_FP64;
