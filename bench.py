@@ -1059,9 +1059,9 @@ def run_singlet(args, world, rank, local):
     }, None
 
 
-def cpu_baseline_singlet(variants: int = 1024, seed: int = 20261203 + 1):
+def cpu_baseline_singlet(variants: int = 1024, seed: int = 20261203 + 1, window: float = 2.0):
     """The reference's own residuals_cpu + merit_cpu (oracle/_ref, or the C restatement when
-    the reference build is missing) over all host threads, repeated for about 2 s."""
+    the reference build is missing) over all host threads, repeated for about `window` s."""
     import oracle.pyoracle as po
     from mikroptim_b200 import workloads
     from mikroptim_b200.batch import ResidualLayout
@@ -1073,7 +1073,7 @@ def cpu_baseline_singlet(variants: int = 1024, seed: int = 20261203 + 1):
     impl.residuals(b, lay, threads=threads)
     impl.merit(b, lay, threads=threads)
     reps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < 2.0:
+    while time.perf_counter() - t0 < window:
         impl.residuals(b, lay, threads=threads)
         impl.merit(b, lay, threads=threads)
         reps += 1
@@ -1128,11 +1128,12 @@ def cpu_baseline_lm(kind: str, runs: int = 256, seed: int = 20261203 + 2):
                                      f"1 and 3 cycles, {t2 - t0:.1f} s"}
 
 
-def cpu_baseline_uneven(runs: int = 96, seed: int = 20261203 + 3):
+def uneven_reference_sampler(runs: int = 96, seed: int = 20261203 + 3):
     """The reference's optimize_lm_cpu on a sample of the uneven runs: the reference needs one
     topology and one variable set per call, so every run is its own call (its baseline loops
-    over topology groups), the calls spread over all host threads. Three cycles minus one
-    cycle, halved, isolates the cost of a cycle from the start-up."""
+    over topology groups), the calls spread over all host threads. Returns (sample, threads):
+    sample() times one step -- 1 then 3 cycles of every run; three cycles minus one, halved,
+    isolates the cost of a cycle from the start-up -- and returns (LM iterations/s, seconds)."""
     import concurrent.futures as cf
     import oracle.pyoracle as po
     from mikroptim_b200 import workloads
@@ -1154,21 +1155,41 @@ def cpu_baseline_uneven(runs: int = 96, seed: int = 20261203 + 3):
         with cf.ThreadPoolExecutor(max_workers=threads) as ex:
             list(ex.map(lambda j: ref.optimize_lm(*j, max_iterations=max_it, method="adjoint",
                                                   threads=1), jobs))
-    t0 = time.perf_counter()
-    run_all(1)
-    t1 = time.perf_counter()
-    run_all(3)
-    t2 = time.perf_counter()
-    per_cycle = max(((t2 - t1) - (t1 - t0)) / 2, 1e-9)
-    return {"value": runs / per_cycle, "unit": "LM iterations/s", "cores": threads,
-            "kind": "reference", "sample": f"optimize_lm_cpu (adjoint), {runs} of the uneven "
-                                            f"runs one per call, 1 and 3 cycles, "
-                                            f"{t2 - t0:.1f} s"}
+
+    def sample():
+        t0 = time.perf_counter()
+        run_all(1)
+        t1 = time.perf_counter()
+        run_all(3)
+        t2 = time.perf_counter()
+        per_cycle = max(((t2 - t1) - (t1 - t0)) / 2, 1e-9)
+        return runs / per_cycle, t2 - t0
+    return sample, threads
+
+
+def cpu_baseline_uneven(runs: int = 96, seed: int = 20261203 + 3):
+    """One sample of uneven_reference_sampler, as the cpu_baseline of the GPU line."""
+    sample, threads = uneven_reference_sampler(runs, seed)
+    v, sec = sample()
+    return {"value": v, "unit": "LM iterations/s", "cores": threads, "kind": "reference",
+            "sample": f"optimize_lm_cpu (adjoint), {runs} of the uneven runs one per call, "
+                      f"1 and 3 cycles, {sec:.1f} s"}
 
 
 def reference_kind() -> str:
     import oracle.pyoracle as po
     return "reference" if os.path.exists(po.REF_LIB) else "port"
+
+
+def repeated_samples(fn, warmup: int, steps: int):
+    """W untimed and K timed calls of a bounded CPU sample fn() -> dict with "value"; returns
+    (median of the K values, the last dict)."""
+    vals, last = [], None
+    for i in range(warmup + steps):
+        last = fn()
+        if i >= warmup:
+            vals.append(last["value"])
+    return statistics.median(vals), last
 
 
 def run_reference(args, world, rank):
@@ -1178,44 +1199,61 @@ def run_reference(args, world, rank):
     if args.workload == "uneven":
         if kind != "reference":
             return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
-        base = cpu_baseline_uneven(runs=96)
-        v = base["value"]
+        # W warm-up and K timed steps, each a bounded sample (96 runs; fewer when K + W > 30,
+        # so the whole run stays within a few minutes); the value is the median of the K
+        n_steps = args.warmup + args.steps
+        runs = 96 if n_steps <= 30 else max(24, 96 * 30 // n_steps)
+        sample, threads = uneven_reference_sampler(runs)
+        rates, total = [], 0.0
+        for i in range(n_steps):
+            r, sec = sample()
+            total += sec
+            if i >= args.warmup:
+                rates.append(r)
+        v = statistics.median(rates)
         return {
             "metric": METRIC, "value": v, "unit": "LM iterations/s", "impl": "reference",
-            "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, configuration-3 shapes)",
             "config": {"workload": WORKLOAD_UNEVEN,
-                       "step": "one LM cycle of a 96-run sample on the host"},
-            "cpu_baseline": {"value": v, "unit": "LM iterations/s", "cores": base["cores"],
-                             "kind": kind, "sample": base["sample"]},
+                       "step": f"LM cycles of a {runs}-run sample on the host (1 and 3 cycles of "
+                               f"every run; the median of the timed steps)"},
+            "cpu_baseline": {"value": v, "unit": "LM iterations/s", "cores": threads,
+                             "kind": kind,
+                             "sample": f"optimize_lm_cpu (adjoint), {runs} of the uneven runs "
+                                       f"one per call, {n_steps} steps, {total:.1f} s"},
             "e2e": {"value": v, "unit": "LM iterations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
     if args.workload == "lm":
         if kind != "reference":
             return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
-        base = cpu_baseline_lm(kind, runs=128)
-        samples = [base["value"]]
-        v = base["value"]
+        n_steps = args.warmup + args.steps  # bounded: fewer runs per step for long runs
+        runs = 128 if n_steps <= 30 else max(32, 128 * 30 // n_steps)
+        v, base = repeated_samples(lambda: cpu_baseline_lm(kind, runs=runs), args.warmup,
+                                   args.steps)
         return {
             "metric": METRIC, "value": v, "unit": "LM run-iterations/s", "impl": "reference",
-            "n_gpus": world, "steps": len(samples), "warmup": 0, "higher_is_better": True,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, configuration-2 shapes)",
             "config": {"workload": WORKLOAD_LM,
-                       "step": "one LM cycle of a 128-run sample on the host"},
+                       "step": f"LM cycles of a {runs}-run sample on the host (the median of "
+                               f"the timed steps)"},
             "cpu_baseline": {"value": v, "unit": "LM run-iterations/s", "cores": base["cores"],
                              "kind": kind, "sample": base["sample"]},
             "e2e": {"value": v, "unit": "LM run-iterations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
     if args.workload == "singlet":
-        base = cpu_baseline_singlet()
-        v = base["value"]
+        n_steps = args.warmup + args.steps
+        window = 2.0 if n_steps <= 30 else 2.0 * 30 / n_steps
+        v, base = repeated_samples(lambda: cpu_baseline_singlet(window=window), args.warmup,
+                                   args.steps)
         return {
             "metric": METRIC, "value": v, "unit": "ray-surface hits/s", "impl": "reference",
-            "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": True,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, configuration-1 shapes)",
             "config": {"workload": WORKLOAD_SINGLET,
