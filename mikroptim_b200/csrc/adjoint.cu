@@ -996,11 +996,14 @@ struct FusedArgs {
     int64_t gram_stride;   // doubles per run of `gram`
 };
 
-template <class N, int kFeat>
-__global__ void __launch_bounds__(kFusedThreads, std::is_same<N, MixedPrecision>::value ||
-                                                           std::is_same<N, BulkPrecision>::value
-                                                       ? 4
-                                                       : kFusedMinBlocks)
+// kWide: the instance for the runs with more than 31 variables in MIXED; their shared memory
+// (64 Gram columns) holds three CTAs per SM, so the register budget is that of three CTAs
+template <class N, int kFeat, bool kWide = false>
+__global__ void __launch_bounds__(kFusedThreads, (std::is_same<N, MixedPrecision>::value ||
+                                                  std::is_same<N, BulkPrecision>::value) &&
+                                                         !kWide
+                                                     ? 4
+                                                     : kFusedMinBlocks)
 adjoint_gram_kernel(const __grid_constant__ FusedArgs fa) {
     const TraceParams& p = fa.ap.t;
     __shared__ FusedShared sh;
@@ -1393,7 +1396,12 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
         default: return adjoint_gram_kernel<BulkPrecision, 0>;
         }
     };
-    const Fn kernel = precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
+    // MIXED runs with more than 31 variables (three CTAs per SM by shared memory) on the
+    // coaxial features: the instance with the three-CTA register budget
+    const bool wide = precision == MKB_PRECISION_MIXED && p_max > 31 && (feat == 0 || feat == 2);
+    const Fn kernel = wide ? (feat == 0 ? adjoint_gram_kernel<MixedPrecision, 0, true>
+                                        : adjoint_gram_kernel<MixedPrecision, 2, true>)
+                      : precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
                       : precision == MKB_PRECISION_MIXED ? pick(TypeTag<MixedPrecision>{})
                       : precision == MKB_PRECISION_FP32_BULK ? pick_bulk()
                                                          : pick(TypeTag<double>{});
