@@ -223,7 +223,8 @@ typedef struct mkb_residual_plan {
      * include/mikroptim/trace/trace.hpp:402), w_(f,l) the tuple weight and W_k the pupil
      * weight; 0 for a ray that failed hard. Units: waves^2 per mm^2 (the merit's unit per
      * squared image-plane error). MERIT adds sum_k r_x^2, then sum_k r_y^2 after each tuple's
-     * OPD and penalty sums. RESIDUALS, MERIT and the FD Jacobian; the adjoint paths refuse it. */
+     * OPD and penalty sums. RESIDUALS, MERIT, the FD Jacobian and the materialised adjoint
+     * Jacobian (its sweep seeded at the image-plane intercept); the fused adjoint refuses it. */
     double transverse_weight;
 } mkb_residual_plan;
 

@@ -133,12 +133,15 @@ __device__ int forward_record(const TraceParams& p, const double* rec, const Rec
 // run's columns col0[c * R + row] for every variable whose parameter is reached.
 // start[0..2] (when not null) get the adjoint of the start point's x and y and the derivative
 // with respect to thickness[0] (the entrance pupil's distance), unscaled, for the aiming fold.
+// img_seed (when not null): Phi is g_x x + g_y y of the ray's intersection (x, y) with the
+// image plane, thickness[S - 1] behind the last vertex (the transverse ray-error rows), in
+// place of the optical path to the reference sphere; seed_opl and seed_pen are then 0.
 template <class N>
 __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const double* rec,
                                const RecordLayout& lay, int f, int l, const Record<N>& ck,
                                bool reached_image, bool soft_mode, N seed_opl, N seed_pen,
                                N factor, double* col0, int64_t R, int64_t row,
-                               double* start = nullptr) {
+                               double* start = nullptr, const double* img_seed = nullptr) {
     const int S = p.S, L = p.L;
     const N zero(0.0);
     const double* curv = rec + lay.curvature;
@@ -193,7 +196,17 @@ __device__ void backward_sweep(const TraceParams& p, const VarParams& v, const d
             if (i < n) {
                 const int s = first + i;
                 if (s == count - 1) {
-                    if (reached_image && count == S) {
+                    if (reached_image && count == S && img_seed != nullptr) {
+                        // (x, y) = p + s0 (d_x, d_y), s0 = (w - p_z) / d_z (the forward's
+                        // transfer_to_image_plane on a copy of the state)
+                        const N gx(img_seed[0]), gy(img_seed[1]);
+                        const N w = thick[S - 1];
+                        const N s0 = (w - sp[i].z) / sd[i].z;
+                        const N s0b = gx * sd[i].x + gy * sd[i].y;
+                        adj.p = {gx, gy, -s0b / sd[i].z};
+                        adj.d = {gx * s0, gy * s0, -(s0b * s0) / sd[i].z};
+                        write(v.col_thickness[S - 1], s0b / sd[i].z);
+                    } else if (reached_image && count == S) {
                         Vec<N> center_adj{zero, zero, zero};
                         N n_image_adj = zero;
                         reference_step_backward<N>(sp[i], sd[i], center,
@@ -331,6 +344,19 @@ adjoint_rows_kernel(const __grid_constant__ AdjointParams ap, const double* __re
                               N(1.0), factor, col0, ap.rows, p.rays + row, aim);
             if (aim) aim_fold(start, smp, f, 0.0, value_of(factor), p.rays + row);
         }
+        if (reached && p.transverse) {
+            // the transverse rows (x errors, then y errors, after the ray and penalty rows):
+            // sqrt(w_t W_(f,l)) sqrt(W_k) times the intercept's derivative
+            const int64_t base = static_cast<int64_t>(p.rays) * (soft_mode ? 2 : 1);
+            const N factor = N(p.tscale[tu]) * N(smp.root_weight);
+            for (int axis = 0; axis < 2; ++axis) {
+                const double g[2] = {axis == 0 ? 1.0 : 0.0, axis == 1 ? 1.0 : 0.0};
+                const int64_t trow = base + axis * p.rays + row;
+                backward_sweep<N>(p, ap.v, record, lay, f, l, ck, true, soft_mode, N(0.0),
+                                  N(0.0), factor, col0, ap.rows, trow, aim, g);
+                if (aim) aim_fold(start, smp, f, 0.0, value_of(factor), trow);
+            }
+        }
     }
 }
 
@@ -410,10 +436,6 @@ int launch_apply(const VarParams& vp, const RecordLayout& lay, const double* tem
 
 int launch_adjoint_rows(const TraceParams& tp, const VarParams& vp, int64_t rows,
                         const double* records, double* J, bool exact, cudaStream_t stream) {
-    if (tp.transverse) {
-        set_error("adjoint Jacobian: transverse ray-error rows have no adjoint (use FD)");
-        return MKB_ERR_UNSUPPORTED;
-    }
     AdjointParams ap;
     ap.t = tp;
     ap.v = vp;
@@ -1331,7 +1353,8 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
                         cudaStream_t stream, const int* run_mask, RunVars rv,
                         const int* order, const int* split, int part, int part_pmax) {
     if (tp.transverse) {
-        set_error("fused adjoint: transverse ray-error rows have no adjoint (use FD)");
+        set_error("fused adjoint: transverse ray-error rows have no fused adjoint (use the "
+                  "materialised adjoint Jacobian or FD)");
         return MKB_ERR_UNSUPPORTED;
     }
     if (tp.V <= 0) return MKB_OK;

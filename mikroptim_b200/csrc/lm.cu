@@ -683,8 +683,9 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
         return MKB_ERR_UNSUPPORTED;
     }
     s.R = trace_rows_of(plan, s.tp.rays);
-    if (s.tp.transverse && !s.fd) {
-        set_error("lm: transverse ray-error rows have no adjoint; use the FD Jacobian");
+    if (s.tp.transverse && s.fused) {
+        set_error("lm: transverse ray-error rows have no fused adjoint; use the materialised "
+                  "adjoint (gram_exact = 1) or the FD Jacobian");
         return MKB_ERR_UNSUPPORTED;
     }
     return make_paraxial_spec(options, templates, plan, &s.px);

@@ -3,7 +3,9 @@
 have no reference counterpart: they are defined in include/mikroptim_b200.h
 (mkb_residual_plan.transverse_weight) and checked bit for bit against the oracle's C
 restatement of that definition; the OPD and penalty rows stay those of the reference. The FD
-Jacobian and the LM with the FD Jacobian carry the rows; the adjoint paths refuse them.
+Jacobian and the LM with the FD Jacobian carry the rows; the materialised adjoint Jacobian
+differentiates them too (the image-plane intercept's reverse step seeds the sweep) and agrees
+with the central differences to their own error; the fused adjoint refuses them.
 """
 
 import dataclasses
@@ -62,12 +64,35 @@ def test_fd_jacobian_and_lm_carry_the_transverse_rows():
     J, r0, _ = engine.fd_jacobian_device(db, lay, b, vs, x0)
     Jo, ro, _ = po.port().fd_jacobian(b, lay, vs, x0)
     assert np.array_equal(J.cpu().numpy(), Jo) and np.array_equal(r0.cpu().numpy(), ro)
-    with pytest.raises(NotImplementedError):
-        engine.adjoint_jacobian_device(db, lay, b, vs, x0)
     opt = engine.LmOptions(max_iterations=15, jacobian=engine.JACOBIAN_FD, gram_exact=True,
                            fail_weight_factor=1.0)
     res = engine.optimize_lm_gpu(b, lay, vs, x0, opt)
     assert np.all(res["merit"] < res["history"][:, 0])
-    with pytest.raises((ValueError, NotImplementedError), match="no adjoint"):
+    # the materialised adjoint carries them as well (the fused adjoint does not)
+    ada = engine.optimize_lm_gpu(b, lay, vs, x0, dataclasses.replace(
+        opt, jacobian=engine.JACOBIAN_ADJOINT))
+    assert np.all(ada["merit"] < ada["history"][:, 0])
+    with pytest.raises((ValueError, NotImplementedError), match="no fused adjoint"):
         engine.optimize_lm_gpu(b, lay, vs, x0, dataclasses.replace(
-            opt, jacobian=engine.JACOBIAN_ADJOINT))
+            opt, jacobian=engine.JACOBIAN_ADJOINT, gram_exact=False))
+
+
+@pytest.mark.parametrize("case", ["singlet", "objective", "ghost", "decentered"])
+def test_adjoint_transverse_rows_agree_with_central_differences(case):
+    name, b, st, vs, x0 = next(c for c in _cases() if c[0] == case)
+    st = dataclasses.replace(st, transverse_weight=1e4, precision=PRECISION_FP64)
+    lay = ResidualLayout(b.topology, st)
+    db = engine.DeviceSystemBatch(b)
+    Jf, rf, sf = engine.fd_jacobian_device(db, lay, b, vs, x0)
+    Ja, ra, sa = engine.adjoint_jacobian_device(db, lay, b, vs, x0)
+    assert np.array_equal(ra.cpu().numpy(), rf.cpu().numpy())
+    Jf, Ja = Jf.cpu().numpy(), Ja.cpu().numpy()
+    t0 = lay.rays_per_variant + lay.penalty_rows  # the transverse rows
+    tf, ta = Jf[:, :, t0:], Ja[:, :, t0:]
+    assert np.abs(ta).max() > 0
+    # per column relative to its largest entry (central differences: O(h^2), ~1e-10 on
+    # smooth rays; rays near a soft boundary leave a few larger differences)
+    scale = np.maximum(np.abs(tf).max(axis=2, keepdims=True), 1e-300)
+    err = np.abs(ta - tf) / scale
+    assert np.median(err) <= 1e-8 and np.quantile(err, 0.99) <= 1e-4, (
+        np.median(err), np.quantile(err, 0.99), err.max())
