@@ -68,10 +68,11 @@ TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
 # adjoint_gram_kernel, objective runs with a glass variable, FP64_FMA (1,184 runs captured:
 # 1.941 GB read, 17.645 GB written)
 FUSED_TRAFFIC_BYTES_PER_RUN = (1.940772e9 + 17.644780e9) / 1184
-# adjoint_gram_kernel<MixedPrecision, 2, *> (the ghost-plate variant; the three-CTA instance
-# for the runs with more than 31 variables), uneven runs with the zero-power plate at surface
-# 1, both launches of a call (1,184 runs captured: 59.9 MB read, 2.785 GB written)
-FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (55.828480e6 + 4.068608e6 + 2.303337e9 + 0.481604e9) / 1184
+# adjoint_gram_kernel<MixedPrecision, 18, *> (plates in the forward trace only: every plate
+# lies below every run's sweep floor; the three-CTA instance for the runs with more than 31
+# variables), uneven runs with the zero-power plate at surface 1, both launches of a call
+# (1,184 runs captured: 34.8 MB read, 2.343 GB written)
+FUSED_TRAFFIC_UNEVEN_BYTES_PER_RUN = (31.629056e6 + 3.127808e6 + 1.787534e9 + 0.555371e9) / 1184
 
 def parse():
     ap = argparse.ArgumentParser()

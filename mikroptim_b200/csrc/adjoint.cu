@@ -873,7 +873,9 @@ __device__ __noinline__ void fused_backward(const TraceParams& p, const VarParam
 #pragma unroll
             for (int m = 0; m < K; ++m) par[m] = {zero_a, zero_a, zero_a, zero_a};
             GhostData gd;
-            const bool plate = ghost_at<(kFeat & 2) != 0>(p, rec, lay, j, l, gd);
+            // feature 16: every plate lies below the sweep floor, so no reverse step is one
+            const bool plate =
+                ghost_at<(kFeat & 2) != 0 && (kFeat & 16) == 0>(p, rec, lay, j, l, gd);
             // the step in the surface's own frame: a ghost plate (its profile coefficients
             // are variables too) or a refracting sphere / plane
             auto local = [&](Vec<N> pl, Vec<N> dl, N tl) {
@@ -1392,8 +1394,17 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     // 4: glass variables of some run)
     const bool glass = vp.has_glass != 0 || rv.any_glass != 0;
     // 8: an interior aperture stop (coaxial, no ghost plates: the batch check refuses others)
-    const int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0) |
-                     (tp.stop > 0 ? 8 : 0);
+    int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0) |
+               (tp.stop > 0 ? 8 : 0);
+    // 16 (MIXED, coaxial plates): every plate sits at or below every run's sweep floor, so the
+    // reverse sweep never reaches one -- the instance without the plate's reverse step
+    if (precision == MKB_PRECISION_MIXED && feat == 2) {
+        int plate_max = 0;
+        for (int s = 0; s < tp.S && s < kMaxSurfaces; ++s)
+            if (tp.ghost_of[s] >= 0) plate_max = s;
+        const int floor_min = rv.table != nullptr ? rv.min_floor : vp.sweep_floor;
+        if (floor_min >= plate_max) feat = 18;
+    }
     using Fn = void (*)(FusedArgs);
     auto pick = [&](auto tag) -> Fn {
         using N = typename decltype(tag)::type;
@@ -1421,9 +1432,12 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     };
     // MIXED runs with more than 31 variables (three CTAs per SM by shared memory) on the
     // coaxial features: the instance with the three-CTA register budget
-    const bool wide = precision == MKB_PRECISION_MIXED && p_max > 31 && (feat == 0 || feat == 2);
-    const Fn kernel = wide ? (feat == 0 ? adjoint_gram_kernel<MixedPrecision, 0, true>
-                                        : adjoint_gram_kernel<MixedPrecision, 2, true>)
+    const bool wide = precision == MKB_PRECISION_MIXED && p_max > 31 &&
+                      (feat == 0 || feat == 2 || feat == 18);
+    const Fn kernel = wide ? (feat == 0   ? adjoint_gram_kernel<MixedPrecision, 0, true>
+                              : feat == 2 ? adjoint_gram_kernel<MixedPrecision, 2, true>
+                                          : adjoint_gram_kernel<MixedPrecision, 18, true>)
+                      : feat == 18 ? adjoint_gram_kernel<MixedPrecision, 18>
                       : precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
                       : precision == MKB_PRECISION_MIXED ? pick(TypeTag<MixedPrecision>{})
                       : precision == MKB_PRECISION_FP32_BULK ? pick_bulk()

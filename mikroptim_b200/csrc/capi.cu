@@ -320,6 +320,32 @@ int make_trace_params(const mkb_device_batch* batch, const mkb_residual_plan* pl
     return MKB_OK;
 }
 
+int sweep_floor_of(const mkb_variables* vars, int S, const uint8_t* type) {
+    int plate_surface[kMaxGhostPlates];
+    int plates = 0;
+    for (int s = 1; s < S; ++s)
+        if (type[s] == MKB_SURFACE_GHOST_PLATE && plates < kMaxGhostPlates)
+            plate_surface[plates++] = s;
+    int floor = kMaxSurfaces;
+    for (int k = 0; k < vars->count; ++k) {
+        const int t = vars->type[k];
+        int s = vars->surface[k], c;
+        if (t == MKB_VAR_WORKING_DISTANCE) {
+            c = S - 1;
+        } else if (t == MKB_VAR_THICKNESS) {
+            c = s;
+        } else {
+            if (t == MKB_VAR_GHOST_COEFFICIENT) {
+                const int g = vars->ghost_plate ? vars->ghost_plate[k] : 0;
+                s = g >= 0 && g < plates ? plate_surface[g] : 1;
+            }
+            c = s > 0 ? s - 1 : 0;
+        }
+        if (c < floor) floor = c;
+    }
+    return floor;
+}
+
 int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarParams* out,
                     int ghost_terms, int L, const double* wavelength_nm, int glass) {
     if (vars == nullptr || vars->count < 1 || vars->count > MKB_MAX_VARIABLES) {

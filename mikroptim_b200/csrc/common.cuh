@@ -904,6 +904,10 @@ int make_var_params(const mkb_variables* vars, int S, const uint8_t* type, VarPa
                     int ghost_terms = 0, int L = 0, const double* wavelength_nm = nullptr,
                     int glass = 0);
 
+// The sweep floor (VarParams::sweep_floor) of a variable set, from its raw arrays (the same
+// rule make_var_params applies; the set must be valid).
+int sweep_floor_of(const mkb_variables* vars, int S, const uint8_t* type);
+
 // Writes x into a packed record (VariableSet::apply, src/optim/variable_set.cpp:237).
 // Writes variable k's value into a record (curvature, thickness / working distance, or a ghost
 // plate's profile coefficient).

@@ -357,7 +357,11 @@ int adjoint_normal_equations(const mkb_device_batch* templates, const mkb_residu
         if (rc != MKB_OK) return rc;
         rv.table = dtable;
         rv.stride = pmax;
-        for (const VarParams& t : table) rv.any_glass |= t.has_glass;
+        rv.min_floor = kMaxSurfaces;
+        for (const VarParams& t : table) {
+            rv.any_glass |= t.has_glass;
+            rv.min_floor = t.sweep_floor < rv.min_floor ? t.sweep_floor : rv.min_floor;
+        }
     }
     const RecordLayout lay = layout_of(tp);
     rc = launch_apply(vp, lay, templates->records, templates->variants, x0, records, runs, stream,

@@ -30,6 +30,7 @@ struct RunVars {
     const uint8_t* tsurf = nullptr;
     uint8_t* vsurf_out = nullptr;
     int any_glass = 0;  // some run of the table has glass variables
+    int min_floor = 0;  // the smallest sweep floor of the table's runs (0: not known)
 };
 
 // trace.cu

@@ -524,6 +524,7 @@ struct LmSetup {
     bool fd, exact, gram_exact, fused;
     bool per_run;       // per-run variables
     bool any_glass;     // some run has glass variables
+    int min_floor;      // the smallest sweep floor of the runs' variable sets
     int pmax;           // P, or the largest P of the runs
     int precision;
     int64_t R;
@@ -636,10 +637,15 @@ int lm_setup(const mkb_device_batch* templates, const mkb_residual_plan* plan,
     if (rc != MKB_OK) return rc;
     s.pmax = s.vp.P;
     s.any_glass = s.vp.has_glass != 0;
+    s.min_floor = s.vp.sweep_floor;
     if (s.per_run) {
         if (table != nullptr) table->resize(static_cast<size_t>(runs));
         for (int r = 0; r < runs; ++r) {
             if (vars[r].count > s.pmax) s.pmax = vars[r].count;
+            if (vars[r].count >= 1 && vars[r].type != nullptr && vars[r].surface != nullptr) {
+                const int fl = sweep_floor_of(&vars[r], s.tp.S, templates->type);
+                if (fl < s.min_floor) s.min_floor = fl;
+            }
             for (int k = 0; k < vars[r].count; ++k)
                 if (vars[r].type[k] == MKB_VAR_GLASS) s.any_glass = true;
             if (table != nullptr) {
@@ -707,6 +713,7 @@ RunVars run_vars(const LmSetup& s, const LmLayout& L, const mkb_device_batch* te
     rv.tsurf = templates->variant_surfaces;
     rv.vsurf_out = L.vsurf;
     rv.any_glass = s.any_glass ? 1 : 0;
+    rv.min_floor = s.min_floor;
     return rv;
 }
 
