@@ -142,3 +142,29 @@ def test_uneven_mixed_lm_ends_where_the_fp64_lm_does():
     ratio = mixed["merit"] / fp64["merit"]
     assert np.mean(np.log(ratio)) <= 0.03, ratio  # MIXED may end lower, not 3 % higher
     assert np.mean(ratio <= 1.0 + 1e-9) >= 1.0 / 3.0, ratio
+
+
+def test_instance_without_the_plate_reverse_step_equals_the_full_one():
+    """Every run's variables lie behind the ghost plate at surface 1, so the MIXED launch takes
+    the fused instance without the plate's reverse step; a thickness[0] variable in run 0 puts
+    the plate on that run's sweep and the launch back on the full instance. The other runs'
+    normal equations are the same bits either way."""
+    from mikroptim_b200.batch import SURFACE_GHOST_PLATE, VAR_THICKNESS, Variable, VariableSet
+    b, st, vss, x0 = _small(24, precision=PRECISION_MIXED)
+    assert b.topology.ghost_plates == 1 and b.topology.type[1] == SURFACE_GHOST_PLATE
+    lay = ResidualLayout(b.topology, st)
+    db = engine.DeviceSystemBatch(b)
+    g_cut = engine.adjoint_normal_equations_runs_device(db, lay, b, vss, x0)
+    vss2, x2 = list(vss), list(x0)
+    vss2[0] = VariableSet(vss[0].topology, list(vss[0].variables) +
+                          [Variable(VAR_THICKNESS, 0, 0.1, 5.0, 1.0)])
+    x2[0] = vss2[0].extract(b, 0)
+    g_full = engine.adjoint_normal_equations_runs_device(db, lay, b, vss2, x2)
+    torch.cuda.synchronize()
+    for i in range(1, b.variants):
+        P = vss[i].size
+        assert np.array_equal(engine.gram_block(g_cut, i, P).cpu().numpy(),
+                              engine.gram_block(g_full, i, P).cpu().numpy()), i
+    # run 0 gained the column of thickness[0]: its block is one wider and not zero there
+    blk = engine.gram_block(g_full, 0, vss2[0].size).cpu().numpy()
+    assert blk[vss2[0].size - 1, vss2[0].size - 1] > 0
