@@ -248,7 +248,7 @@ static __device__ uint32_t g_wait_polls = MKB_WAIT_POLLS_DEFAULT;
                    : MKB_ERR_CUDA;                                                         \
     }
 
-// ---- bulk copy into shared memory with an mbarrier (no multicast) ------------------------
+// ---- bulk copy into shared memory with an mbarrier (each CTA its own copy) --------------
 __device__ inline uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
