@@ -1396,10 +1396,12 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
     // 8: an interior aperture stop (coaxial, no ghost plates: the batch check refuses others)
     int feat = (tp.non_coaxial ? 1 : 0) | (tp.G > 0 ? 2 : 0) | (glass ? 4 : 0) |
                (tp.stop > 0 ? 8 : 0);
-    // 16 (MIXED or FP64_FMA, coaxial plates): every plate sits at or below every run's sweep
-    // floor, so the reverse sweep never reaches one -- the instance without the plate's
-    // reverse step
-    if ((precision == MKB_PRECISION_MIXED || precision == MKB_PRECISION_FP64_FMA) && feat == 2) {
+    // 16 (MIXED, FP64_FMA or FP64, coaxial plates): every plate sits at or below every run's
+    // sweep floor, so the reverse sweep never reaches one -- the instance without the plate's
+    // reverse step (the same arithmetic for every run: the skipped code is never reached)
+    if ((precision == MKB_PRECISION_MIXED || precision == MKB_PRECISION_FP64_FMA ||
+         precision == MKB_PRECISION_FP64) &&
+        feat == 2) {
         int plate_max = 0;
         for (int s = 0; s < tp.S && s < kMaxSurfaces; ++s)
             if (tp.ghost_of[s] >= 0) plate_max = s;
@@ -1440,6 +1442,8 @@ int launch_adjoint_gram(const TraceParams& tp, const VarParams& vp, const double
                                           : adjoint_gram_kernel<MixedPrecision, 18, true>)
                       : feat == 18 ? (precision == MKB_PRECISION_MIXED
                                           ? adjoint_gram_kernel<MixedPrecision, 18>
+                                      : precision == MKB_PRECISION_FP64
+                                          ? adjoint_gram_kernel<Exact64, 18>
                                           : adjoint_gram_kernel<double, 18>)
                       : precision == MKB_PRECISION_FP64    ? pick(TypeTag<Exact64>{})
                       : precision == MKB_PRECISION_MIXED ? pick(TypeTag<MixedPrecision>{})

@@ -144,13 +144,14 @@ def test_uneven_mixed_lm_ends_where_the_fp64_lm_does():
     assert np.mean(ratio <= 1.0 + 1e-9) >= 1.0 / 3.0, ratio
 
 
-def test_instance_without_the_plate_reverse_step_equals_the_full_one():
-    """Every run's variables lie behind the ghost plate at surface 1, so the MIXED launch takes
-    the fused instance without the plate's reverse step; a thickness[0] variable in run 0 puts
-    the plate on that run's sweep and the launch back on the full instance. The other runs'
+@pytest.mark.parametrize("precision", [PRECISION_MIXED, PRECISION_FP64_FMA, PRECISION_FP64])
+def test_instance_without_the_plate_reverse_step_equals_the_full_one(precision):
+    """Every run's variables lie behind the ghost plate at surface 1, so the launch takes the
+    fused instance without the plate's reverse step; a thickness[0] variable in run 0 puts the
+    plate on that run's sweep and the launch back on the full instance. The other runs'
     normal equations are the same bits either way."""
     from mikroptim_b200.batch import SURFACE_GHOST_PLATE, VAR_THICKNESS, Variable, VariableSet
-    b, st, vss, x0 = _small(24, precision=PRECISION_MIXED)
+    b, st, vss, x0 = _small(24, precision=precision)
     assert b.topology.ghost_plates == 1 and b.topology.type[1] == SURFACE_GHOST_PLATE
     lay = ResidualLayout(b.topology, st)
     db = engine.DeviceSystemBatch(b)
