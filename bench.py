@@ -503,7 +503,11 @@ def run_lm(args, world, rank, local):
                                         seed=20261203 + 2 + 1000 * rank, glass=True)
     if args.stop > 0:  # configuration 2's stop at surface 8: an aimed entrance pupil
         b, st, vs, x0 = workloads.with_aperture_stop(b, st, vs, args.stop)
-    st.precision = PRECISION_FP64_FMA
+    # the headline runs bit-exact FP64 (every operation separately rounded, as the reference
+    # CPU): on these NA 0.95 objectives FP64 with contraction misses the 1e-4 wave OPD bar on
+    # grazing rays (opd_error_vs_fp64), so FP64_FMA and MIXED are reported beside it
+    from mikroptim_b200.batch import PRECISION_FP64
+    st.precision = PRECISION_FP64
     lay = ResidualLayout(b.topology, st)
     runs = b.variants
     P = vs.size
@@ -540,16 +544,14 @@ def run_lm(args, world, rank, local):
     mixed_value = world * iters_mixed / (max_over_ranks(ms_mixed, world, dev) * args.steps / 1e3)
     del lm_m
 
-    # ---- the same LM in bit-exact FP64 (trace, MERIT and adjoint separately rounded, as the
-    # reference CPU computes them): no OPD error against the FP64 oracle, where FP64 with
-    # contraction misses the 1e-4 wave bar on the grazing rays of these NA 0.95 objectives
-    from mikroptim_b200.batch import PRECISION_FP64
-    lay_exact = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP64))
-    lm_e = engine.DeviceLm(db, lay_exact, b, vs, opt, runs)
-    lm_e.start(x0)
-    ms_exact, iters_exact, _ = _lm_window(lm_e, args.steps, args.warmup, flush, world, dev)
-    exact_value = world * iters_exact / (max_over_ranks(ms_exact, world, dev) * args.steps / 1e3)
-    del lm_e
+    # ---- the same LM in FP64 with FMA contraction (faster; its OPD error in
+    # opd_error_vs_fp64.fp64_fma)
+    lay_fma = ResidualLayout(b.topology, dataclasses.replace(st, precision=PRECISION_FP64_FMA))
+    lm_f = engine.DeviceLm(db, lay_fma, b, vs, opt, runs)
+    lm_f.start(x0)
+    ms_fma, iters_fma, _ = _lm_window(lm_f, args.steps, args.warmup, flush, world, dev)
+    fma_value = world * iters_fma / (max_over_ranks(ms_fma, world, dev) * args.steps / 1e3)
+    del lm_f
 
     # ---- the reference method on the same GPU: FD Jacobian (2P + 1 traced variants), FP64 ----
     fd_runs = min(512, runs)
@@ -629,7 +631,8 @@ def run_lm(args, world, rank, local):
                    "step": "one batched LM cycle of all runs (CUDA graph)",
                    "runs_per_gpu": runs, "variables": P, "rays_per_run": lay.rays_per_variant,
                    "jacobian": "adjoint fused with FP64 tensor-core normal equations",
-                   "precision": "FP64 with FMA contraction",
+                   "precision": "FP64, every operation separately rounded (bit-identical to "
+                                "the reference CPU: no OPD error)",
                    "iterations": "LM iterations actually taken in the timed cycles "
                                  f"({iters} of {runs * args.steps} run-cycles)",
                    "l2": "flushed (256 MB write) before every timed step"},
@@ -637,10 +640,9 @@ def run_lm(args, world, rank, local):
         "ray_surface_hits_per_s": world * rays * steps_per_ray / (merit_ms / 1e3),
         "adjoint_mixed": {"value": mixed_value, "unit": "LM iterations/s",
                           "ms_per_cycle": ms_mixed},
-        "adjoint_fp64_exact": {"value": exact_value, "unit": "LM iterations/s",
-                               "ms_per_cycle": ms_exact,
-                               "opd_error_vs_fp64": "0 (bit-identical to the FP64 oracle)",
-                               "speedup_vs_fd": exact_value / (world * fd_value)},
+        "adjoint_fp64_fma": {"value": fma_value, "unit": "LM iterations/s",
+                             "ms_per_cycle": ms_fma,
+                             "speedup_vs_fd": fma_value / (world * fd_value)},
         "fd_fp64": {"value": world * fd_value, "unit": "LM iterations/s",
                     "ms_per_cycle_512_runs": fd_ms, "cycles": fd_steps,
                     "speedup_adjoint_vs_fd": value / (world * fd_value),
@@ -651,7 +653,8 @@ def run_lm(args, world, rank, local):
                      "frac": achieved / peak if peak else None,
                      "traffic": (FUSED_TRAFFIC_BYTES_PER_RUN * runs
                                  if FUSED_TRAFFIC_BYTES_PER_RUN else None),
-                     "traffic_source": "scaled capture",
+                     "traffic_source": "scaled capture of the FP64_FMA instance (the same "
+                                       "FP64 kept-state layout)",
                      "kernel": "adjoint_gram_kernel (fused adjoint + DMMA normal equations)",
                      "kernel_ms": kernel_ms,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
