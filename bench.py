@@ -65,9 +65,9 @@ FLOPEQ_PER_RAY_SURFACE = 140  # reference cost model (docs/hardware.md:138 of th
 # and reported with "traffic_source": "scaled capture".
 # trace_kernel, objective variants (512 captured: 668,672 B read, 0 B written)
 TRAFFIC_BYTES_PER_VARIANT = 668672 / 512
-# adjoint_gram_kernel, objective runs with a glass variable, FP64_FMA (1,184 runs captured:
-# 1.941 GB read, 17.645 GB written)
-FUSED_TRAFFIC_BYTES_PER_RUN = (1.940772e9 + 17.644780e9) / 1184
+# adjoint_gram_kernel<Exact64, 12> (bit-exact FP64; glass variable and the aimed stop at
+# surface 8), configuration-2 objectives (1,184 runs captured: 2.070 GB read, 19.238 GB written)
+FUSED_TRAFFIC_BYTES_PER_RUN = (2.069940e9 + 19.237769e9) / 1184
 # adjoint_gram_kernel<MixedPrecision, 18, *> (plates in the forward trace only: every plate
 # lies below every run's sweep floor; the three-CTA instance for the runs with more than 31
 # variables), uneven runs with the zero-power plate at surface 1, both launches of a call
@@ -653,8 +653,7 @@ def run_lm(args, world, rank, local):
                      "frac": achieved / peak if peak else None,
                      "traffic": (FUSED_TRAFFIC_BYTES_PER_RUN * runs
                                  if FUSED_TRAFFIC_BYTES_PER_RUN else None),
-                     "traffic_source": "scaled capture of the FP64_FMA instance (the same "
-                                       "FP64 kept-state layout)",
+                     "traffic_source": "scaled capture",
                      "kernel": "adjoint_gram_kernel (fused adjoint + DMMA normal equations)",
                      "kernel_ms": kernel_ms,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
