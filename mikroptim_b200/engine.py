@@ -1241,9 +1241,20 @@ def pad_rows(x, runs: int, width: int) -> np.ndarray:
     return np.asarray(x, dtype=np.float64).reshape(runs, width)
 
 
-def check_start_points(variables, x0: np.ndarray) -> None:
+def check_start_points(variables, x0: np.ndarray, run_variables=None) -> None:
     """The reference rejects a start value outside its variable's bounds before any work
-    (VariableSet validation in levenberg_marquardt, std::invalid_argument): ValueError."""
+    (VariableSet validation in levenberg_marquardt, std::invalid_argument): ValueError. With
+    run_variables (the RunVariables of a per-run list) the check runs on whole arrays."""
+    if run_variables is not None:
+        lo, up = run_variables.bounds()
+        x = np.asarray(x0, dtype=np.float64)[:, :run_variables.pmax]
+        bad = (x < lo) | (x > up)
+        if bad.any():
+            i = int(np.nonzero(bad.any(axis=1))[0][0])
+            k = int(np.nonzero(bad[i])[0][0])
+            raise ValueError(f"lm: run {i}, variable {k}: start value {x[i, k]!r} outside "
+                             f"[{lo[i, k]!r}, {up[i, k]!r}]")
+        return
     sets = variables if isinstance(variables, (list, tuple)) else [variables] * len(x0)
     for i, (vs, row) in enumerate(zip(sets, x0)):
         lo, up = vs.lower(), vs.upper()
@@ -1275,13 +1286,12 @@ class DeviceLm:
         if isinstance(variables, (list, tuple)):
             if len(variables) != runs:
                 raise ValueError("DeviceLm: one VariableSet per run needed")
-            self.P = max(v.size for v in variables)
-            self._var_list = [v.c_struct() for v in variables]
-            arr = (_capi.Variables * runs)(*self._var_list)
-            self._var_array = arr
-            self._vars = C.cast(arr, C.POINTER(_capi.Variables)).contents
+            self._run_vars = RunVariables(variables)
+            self.P = self._run_vars.pmax
+            self._vars = self._run_vars.pointer.contents
             self._opt.per_run_variables = 1
         else:
+            self._run_vars = None
             self.P = variables.size
             self._vars = variables.c_struct()
         need = int(self.lib.mkb_lm_workspace_bytes(C.byref(self._b), C.byref(self._plan),
@@ -1297,7 +1307,7 @@ class DeviceLm:
 
     def start(self, x0) -> None:
         rows = pad_rows(x0, self.runs, self.P)
-        check_start_points(self.variables, rows)
+        check_start_points(self.variables, rows, self._run_vars)
         x0 = _dev_f64(rows, self.templates.device)
         self._x0 = x0
         extra = tmerit = None
@@ -1726,15 +1736,53 @@ def adjoint_normal_equations_device(templates: DeviceSystemBatch, layout: Residu
 
 
 class RunVariables:
-    """One VariableSet per run as the C array the ABI takes (built once, reused)."""
+    """One VariableSet per run as the C array the ABI takes (built once, reused): every run's
+    variable fields in flat arrays, and one mkb_variables record per run pointing into them (a
+    structured array laid out as the C struct), so thousands of runs take milliseconds."""
 
     def __init__(self, variable_sets):
         self.sets = list(variable_sets)
         self.runs = len(self.sets)
-        self.pmax = max(v.size for v in self.sets)
-        self._keep = [v.c_struct() for v in self.sets]
-        self._array = (_capi.Variables * self.runs)(*self._keep)
-        self.pointer = C.cast(self._array, C.POINTER(_capi.Variables))
+        counts = np.fromiter((v.size for v in self.sets), dtype=np.int64, count=self.runs)
+        self.pmax = int(counts.max()) if self.runs else 0
+        flat = [var for v in self.sets for var in v.variables]
+        n = len(flat)
+
+        def column(attr, dtype):
+            return np.fromiter((getattr(x, attr) for x in flat), dtype=dtype, count=n)
+        self.fields = {"type": column("type", np.int32), "surface": column("surface", np.int32),
+                       "lower": column("lower", np.float64), "upper": column("upper", np.float64),
+                       "typical": column("typical", np.float64),
+                       "ghost_plate": column("plate", np.int32),
+                       "ghost_order": column("order", np.int32),
+                       "glass_component": column("component", np.int32)}
+        starts = np.zeros(self.runs, dtype=np.int64)
+        if self.runs > 1:
+            starts[1:] = np.cumsum(counts)[:-1]
+        self.counts, self.starts = counts, starts
+        rec = _capi.Variables
+        names = [f[0] for f in rec._fields_]
+        layout = np.dtype({"names": names,
+                           "formats": [np.int32] + [np.uint64] * (len(names) - 1),
+                           "offsets": [getattr(rec, f).offset for f in names],
+                           "itemsize": C.sizeof(rec)})
+        self._array = np.zeros(max(self.runs, 1), dtype=layout)
+        self._array["count"][:self.runs] = counts
+        for name, a in self.fields.items():
+            self._array[name][:self.runs] = a.ctypes.data + starts * a.itemsize
+        self.pointer = C.cast(self._array.ctypes.data, C.POINTER(rec))
+
+    def bounds(self):
+        """(lower, upper) padded to [runs][pmax] with -inf / +inf past each run's count."""
+        k = np.arange(self.pmax)[None, :]
+        valid = k < self.counts[:, None]
+        idx = np.where(valid, self.starts[:, None] + k, 0)
+        if self.fields["lower"].size == 0:
+            full = np.zeros((self.runs, self.pmax))
+            return full - np.inf, full + np.inf
+        lo = np.where(valid, self.fields["lower"][idx], -np.inf)
+        up = np.where(valid, self.fields["upper"][idx], np.inf)
+        return lo, up
 
 
 def adjoint_normal_equations_runs_device(templates: DeviceSystemBatch, layout: ResidualLayout,
