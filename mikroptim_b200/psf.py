@@ -12,6 +12,8 @@ EVAL -> PSF chain on the device (maps built from EVAL's device outputs).
 from __future__ import annotations
 
 import ctypes as C
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -348,7 +350,16 @@ class PsfEngine:
                     r.psf = psf_h[t].reshape(-1)
                     r.mtf_sagittal = mtf_h[t, 0].copy()
                     r.mtf_tangential = mtf_h[t, 1].copy()
-                    finish_psf(r, p)
+                # the figures of every tuple on the host threads (the finish runs in the
+                # library with the interpreter lock released; each tuple is independent)
+                items = [(out[first + t], p) for t, p in enumerate(part)]
+                workers = min(len(items), os.cpu_count() or 1)
+                if workers > 1:
+                    with ThreadPoolExecutor(max_workers=workers) as ex:
+                        list(ex.map(lambda rp: finish_psf(*rp), items))
+                else:
+                    for r, p in items:
+                        finish_psf(r, p)
                 self.last_run.tranches += 1
         self.last_run.tranche = tranche
         self.last_run.work_bytes = int(_capi.lib().mkb_psf_workspace_bytes(tranche, n, m))
