@@ -266,7 +266,8 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
  *                refraction . surface normal) over the rays with status Ok; surface 0 holds
  *                the start point and d_z; neutral 0 and 1 without a valid ray
  *                (SurfaceExtremaResult, include/mikroptim/batch/batch_extrema.hpp, hard
- *                maxima). Coaxial batches only (MKB_ERR_UNSUPPORTED otherwise). */
+ *                maxima); at a decentered or tilted surface the height and incidence in the
+ *                surface's own frame. FP64 and FP64_FMA. */
 typedef struct mkb_trace_options {
     int32_t pack_rays;
     int32_t variants_per_cta;

@@ -52,7 +52,7 @@ static_assert(offsetof(SharedTrace, bar) % 8 == 0, "mbarrier alignment");
 // reference_sphere.hpp:181, with batch_ray_opl and collimated_ray, merit/ray_residual.hpp:69,
 // trace/trace.hpp:109): returns the status, the OPL and the soft penalty.
 // mu_tab[s * L + l] = n_before / n_after of the step onto surface s (divided in N).
-// kExtrema (coaxial kernels): hsq[s] / cosi[s] get the squared ray height x^2 + y^2 at surface
+// kExtrema: hsq[s] / cosi[s] get the squared ray height x^2 + y^2 at surface
 // s and cos I = d . N (d before the refraction, N = (-c x, -c y, 1 - c z), c = 0 off spheres)
 // for every surface the ray passed; surface 0 is the start point and cos I = d_z there
 // (RaySurfaceRecord, trace/surface_extrema.hpp; observer calls in trace/trace.hpp:316,346).
@@ -102,9 +102,24 @@ __device__ inline int trace_ray(const TraceParams& p, const double* rec, const d
                                     plate ? &gd : nullptr, n_after);
         if (status != kOk) break;
         if constexpr (kExtrema) {
-            hsq[s] = value_of(r.px * r.px + r.py * r.py);
-            const N nx = -c * r.px, ny = -c * r.py, nz = N(1.0) - c * r.pz;
-            cosi[s] = value_of(dbx * nx + dby * ny + dbz * nz);
+            const double* xs = xf_at<(kFeat & 1) != 0>(rec, lay, s);
+            if (xs != nullptr && xs[6] > 0.0) {
+                // a decentered or tilted surface: height and incidence in its own frame -- the
+                // state taken back into it and the direction before the step rotated into it
+                // (trace_segment's observer, trace/trace.hpp:330)
+                const Transform<N> tr = transform_at<N>(xs);
+                RayT<N> loc = r;
+                ray_to_surface(loc, tr);
+                N ux = dbx, uy = dby, uz = dbz;
+                rotate_to(tr, ux, uy, uz);
+                hsq[s] = value_of(loc.px * loc.px + loc.py * loc.py);
+                const N nx = -c * loc.px, ny = -c * loc.py, nz = N(1.0) - c * loc.pz;
+                cosi[s] = value_of(ux * nx + uy * ny + uz * nz);
+            } else {
+                hsq[s] = value_of(r.px * r.px + r.py * r.py);
+                const N nx = -c * r.px, ny = -c * r.py, nz = N(1.0) - c * r.pz;
+                cosi[s] = value_of(dbx * nx + dby * ny + dbz * nz);
+            }
         }
         n_before = n_after;
     }
@@ -694,8 +709,8 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
                                      : trace_kernel<kResiduals, F, 3>);
     const int64_t n_ext = static_cast<int64_t>(p.V) * p.S * 2;
     if (out.extrema != nullptr) {
-        // per-surface extrema: coaxial batches (with or without ghost plates), one variant per
-        // CTA, FP64
+        // per-surface extrema: one variant per CTA, FP64 (a decentered or tilted surface's in
+        // its own frame)
         if (precision == MKB_PRECISION_DF64) {
             set_error("trace: extrema are not built for DF64");
             return MKB_ERR_UNSUPPORTED;
@@ -704,15 +719,15 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
             set_error("trace: extrema need one variant per CTA");
             return MKB_ERR_UNSUPPORTED;
         }
-        if (feat & 1) {
-            set_error("trace: per-surface extrema of decentered or tilted batches are not built");
-            return MKB_ERR_UNSUPPORTED;
-        }
         kernel = precision == MKB_PRECISION_FP64
-                     ? (feat == 0 ? trace_kernel<kResiduals, E, 0, true>
-                                  : trace_kernel<kResiduals, E, 2, true>)
-                     : (feat == 0 ? trace_kernel<kResiduals, F, 0, true>
-                                  : trace_kernel<kResiduals, F, 2, true>);
+                     ? (feat == 0   ? trace_kernel<kResiduals, E, 0, true>
+                        : feat == 1 ? trace_kernel<kResiduals, E, 1, true>
+                        : feat == 2 ? trace_kernel<kResiduals, E, 2, true>
+                                    : trace_kernel<kResiduals, E, 3, true>)
+                     : (feat == 0   ? trace_kernel<kResiduals, F, 0, true>
+                        : feat == 1 ? trace_kernel<kResiduals, F, 1, true>
+                        : feat == 2 ? trace_kernel<kResiduals, F, 2, true>
+                                    : trace_kernel<kResiduals, F, 3, true>);
         extrema_init_kernel<<<592, 256, 0, stream>>>(out.extrema, n_ext, out.mask, p.S);
         count_launch();
     }

@@ -222,8 +222,8 @@ class TraceSettings:
     None) to MERIT, added to each variant's merit after its tuple sums. precision None: the
     quadrature's. pack_rays changes only the run time (bit-identical results for every value).
     extrema: per variant and surface the largest ray height and the smallest cos I of the valid
-    rays (SurfaceExtremaResult, hard maxima; coaxial batches) in the result's `extrema`
-    [V][S][2]."""
+    rays (SurfaceExtremaResult, hard maxima; a tilted surface's in its own frame) in the
+    result's `extrema` [V][S][2]."""
 
     quadrature: ResidualSettings = dataclasses.field(default_factory=ResidualSettings)
     opd: bool = False
