@@ -286,9 +286,11 @@ int mkb_eval_reference_host(const mkb_batch_view* view, int32_t reference,
                   view->wavelengths);
         return MKB_ERR_ARGUMENT;
     }
-    if (reference == MKB_EVAL_EXIT_PUPIL && view->ghost_plates > 0) {
-        set_error("eval reference: the exit pupil of systems with ghost plates is not built");
-        return MKB_ERR_UNSUPPORTED;
+    if (reference == MKB_EVAL_EXIT_PUPIL && view->ghost_plates > 0 &&
+        (view->type == nullptr || view->ghost_coeff == nullptr ||
+         view->ghost_norm_radius == nullptr || view->ghost_index == nullptr)) {
+        set_error("eval reference: ghost plates without their data");
+        return MKB_ERR_ARGUMENT;
     }
     const int V = view->variants, S = view->surfaces, L = view->wavelengths, F = view->fields;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -300,13 +302,32 @@ int mkb_eval_reference_host(const mkb_batch_view* view, int32_t reference,
         if (reference == MKB_EVAL_EXIT_PUPIL) {
             // the paraxial chief ray (y0 = 0, u0 = 1) of compute_paraxial
             // (src/paraxial/paraxial.cpp:130): exit pupil at -y / u' after the last surface
+            // a ghost plate is a thin element in the medium of its gap (batch_paraxial,
+            // src/batch/system_batch.cpp:980): power -2 (n_G - n_m) t2 joins the surface's
+            const int G = view->ghost_plates, K = view->ghost_terms;
             double y = 0.0, u = 1.0, nb = 1.0;
-            for (int s = 0; s < S; ++s) {
+            for (int s = 0, g = 0; s < S; ++s) {
                 const double c = view->curvature[int64_t(v) * S + s];
                 const double n = view->index[(int64_t(v) * S + s) * L + paraxial_column];
                 if (s > 0) y += view->thickness[int64_t(v) * S + s - 1] * u;
                 double phi = c * (n - nb);
-                phi += 0.0;
+                double power = 0.0;
+                if (s > 0 && G > 0 && view->type[s] == MKB_SURFACE_GHOST_PLATE && g < G) {
+                    // ghost_profile_t2 and ghost_plate_power (trace/ghost_plate.hpp:95,107)
+                    const double* a = view->ghost_coeff + (int64_t(v) * G + g) * K;
+                    double sum = 0.0;
+                    for (int k = 1; k <= K; ++k) {
+                        const double term = a[k - 1] * static_cast<double>(k * (k + 1));
+                        sum += (k % 2 == 1) ? term : -term;
+                    }
+                    const double r = view->ghost_norm_radius[g];
+                    const double t2 = sum / (r * r);
+                    const double n_glass =
+                        view->ghost_index[(int64_t(v) * G + g) * L + paraxial_column];
+                    power = -2.0 * (n_glass - n) * t2;
+                    ++g;
+                }
+                phi += power;
                 u = (nb * u - y * phi) / n;
                 nb = n;
             }

@@ -51,6 +51,10 @@ def test_eval_objectives_with_failed_rays_bitwise_equal_reference():
 def test_eval_ghost_plates_and_decentered_bitwise_equal_reference():
     b, st, _, _ = workloads.ghost(5)
     _check(b, st, engine.EvalSettings(grid=24, reference=engine.EVAL_VERTEX))
+    # the exit pupil of systems with ghost plates: the plates' paraxial power in the chief ray
+    _check(b, st, engine.EvalSettings(grid=24, reference=engine.EVAL_EXIT_PUPIL))
+    strong, st2, _, _ = workloads.ghost(5, coeff_sigma=2e-2)
+    _check(strong, st2, engine.EvalSettings(grid=24, reference=engine.EVAL_EXIT_PUPIL))
     b, st, _, _ = workloads.tolerancing(4, elements=3, rings=4, spokes=8)
     _check(b, st, engine.EvalSettings(grid=24))
 
