@@ -267,7 +267,7 @@ int mkb_merit_device(const mkb_device_batch* batch, const mkb_residual_plan* pla
  *                the start point and d_z; neutral 0 and 1 without a valid ray
  *                (SurfaceExtremaResult, include/mikroptim/batch/batch_extrema.hpp, hard
  *                maxima); at a decentered or tilted surface the height and incidence in the
- *                surface's own frame. FP64 and FP64_FMA. */
+ *                surface's own frame. FP64, FP64_FMA and DF64. */
 typedef struct mkb_trace_options {
     int32_t pack_rays;
     int32_t variants_per_cta;

@@ -709,12 +709,8 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
                                      : trace_kernel<kResiduals, F, 3>);
     const int64_t n_ext = static_cast<int64_t>(p.V) * p.S * 2;
     if (out.extrema != nullptr) {
-        // per-surface extrema: one variant per CTA, FP64 (a decentered or tilted surface's in
-        // its own frame)
-        if (precision == MKB_PRECISION_DF64) {
-            set_error("trace: extrema are not built for DF64");
-            return MKB_ERR_UNSUPPORTED;
-        }
+        // per-surface extrema: one variant per CTA, FP64 / FP64_FMA / DF64 (a decentered or
+        // tilted surface's in its own frame)
         if (p.vpc != 1) {
             set_error("trace: extrema need one variant per CTA");
             return MKB_ERR_UNSUPPORTED;
@@ -724,6 +720,11 @@ int launch_trace(const TraceParams& p_in, const double* records, const TupleOut&
                         : feat == 1 ? trace_kernel<kResiduals, E, 1, true>
                         : feat == 2 ? trace_kernel<kResiduals, E, 2, true>
                                     : trace_kernel<kResiduals, E, 3, true>)
+                 : precision == MKB_PRECISION_DF64
+                     ? (feat == 0   ? trace_kernel<kResiduals, D, 0, true>
+                        : feat == 1 ? trace_kernel<kResiduals, D, 1, true>
+                        : feat == 2 ? trace_kernel<kResiduals, D, 2, true>
+                                    : trace_kernel<kResiduals, D, 3, true>)
                      : (feat == 0   ? trace_kernel<kResiduals, F, 0, true>
                         : feat == 1 ? trace_kernel<kResiduals, F, 1, true>
                         : feat == 2 ? trace_kernel<kResiduals, F, 2, true>

@@ -44,3 +44,24 @@ def test_df64_trace_within_the_references_bar(make):
     if clean.any():
         rel = np.abs(md - m64)[clean] / np.maximum(m64[clean], 1e-300)
         assert rel.max() <= 1e-9, rel.max()
+
+
+@pytest.mark.parametrize("make", [lambda: workloads.objective(8, rings=4, spokes=8),
+                                  lambda: workloads.ghost(8),
+                                  lambda: workloads.tolerancing(4, elements=3, rings=4,
+                                                                spokes=8)])
+def test_df64_extrema_within_the_bar(make):
+    """Per-surface extrema in DF64 (the reference's merit kernel reduces them for df64 too):
+    the largest heights within 1e-9 relative and the smallest cos I within 1e-9 of the FP64
+    ones."""
+    b, st, _, _ = make()
+    eng = engine.TraceEngine(0)
+    got = {}
+    for p in (PRECISION_FP64, PRECISION_DF64):
+        ts = engine.TraceSettings(dataclasses.replace(st, precision=p), extrema=True)
+        got[p] = eng.run(b, engine.TraceMode.MERIT, ts).merit.extrema
+    e, d = got[PRECISION_FP64], got[PRECISION_DF64]
+    assert np.any(e[:, 1:, 0] > 0.0)
+    h = np.abs(d[..., 0] - e[..., 0]) / np.maximum(np.abs(e[..., 0]), 1e-300)
+    assert h.max() <= 1e-9, h.max()
+    assert np.abs(d[..., 1] - e[..., 1]).max() <= 1e-9
